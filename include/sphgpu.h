@@ -1,0 +1,201 @@
+/*
+ * sphgpu.h -- C ABI of the B200 (sm_100a) time-step engine for the multi-phase
+ * SPH solver wodexinxin2015/MultiPhase-SPH-Solver.
+ *
+ * The engine owns one particle system in device memory (structure of arrays,
+ * FP64) and runs the reference's per-step particle loop on the GPU.  Every
+ * entry point takes plain pointers and sizes; no C++ or torch types cross the
+ * boundary.  Return value convention (all int-returning entry points):
+ *     0            success
+ *     3            a particle left the cell grid       (reference: parttocell)
+ *     5            a particle has more than 99 neighbours (partisearching)
+ *     >= 100       engine errors (SPHGPU_E_*)
+ * These are the integers the reference returns from the methods this layer
+ * replaces, so a caller's Err_Deal() keeps working unchanged.
+ *
+ * Reference interfaces replaced (file:line in the reference project):
+ *   clNNPS_Fun::celllist_ini1/ini2/parttocell/partisearching
+ *                                         Class_Functions.h:41-59, CPP_3-NNPS.cpp:96-374
+ *   clDensity_Fun::density                Class_Functions.h:61-67, CPP_6-density.cpp:11-189
+ *   clStraStre_Fun::strain_noreg/eos/strain_to_stress/free_surface_check/
+ *                   Stress_eigValue/stress_regu/strain_regu
+ *                                         Class_Functions.h:69-82
+ *   clInterFor_Fun::cal_permeability/interact1
+ *                                         Class_Functions.h:106-119
+ *   clAcce_Fun::fluid_acceleration_*, soil_acceleration_noreg,
+ *               structure_acceleration_noreg, boundary_moving_stress_effect,
+ *               artificial_viscosity      Class_Functions.h:121-150
+ *   clVel_Fun::veocity_update/xsph        Class_Functions.h:156-162
+ *   clUpdate_Fun::update/timestep         Class_Functions.h:164-169
+ *   clBndy_Fun::tmboundary/check_domain   Class_Functions.h:171-185
+ *   the step sequence of SPH_Calculation  CPP_1-SPHLoops.cpp:478-775
+ */
+#ifndef SPHGPU_H_INCLUDED
+#define SPHGPU_H_INCLUDED
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPHGPU_ABI_VERSION 1
+#define SPHGPU_MAX_NEIGHBORS 99   /* Par_Cell::influ[100] is 1-based: Class_NNPS.h:71 */
+
+/* error codes beyond the reference's own (which are 1..42) */
+#define SPHGPU_E_ARG        100   /* bad argument / unknown field name          */
+#define SPHGPU_E_CUDA       101   /* a CUDA runtime call failed                 */
+#define SPHGPU_E_NODEVICE   102   /* no CUDA device or the kernels failed to load */
+#define SPHGPU_E_UNSUPPORTED 103  /* a flag combination this engine does not run */
+#define SPHGPU_E_STATE      104   /* call order (e.g. step before upload)        */
+
+/* Para_Fluid, field for field (Class_ParticleProperty.h:107-133). */
+typedef struct sphgpu_fluid {
+    double vis, vpu, dens, paa0, porosity, fai, c;
+    int    bhtype, press_type, acc_type;
+    double pre_coe, strain_min;
+} sphgpu_fluid;
+
+/* Para_Soil, field for field (Class_ParticleProperty.h:33-105). */
+typedef struct sphgpu_soil {
+    double e, poi, eps0, dens, damp1, damp2, cop, ramda, kapa, zmf;
+    double ann, bnn, beta, sitas, sitar, epsr, epss, sd, sw, kse;
+    double c1, c2, c3, fai, c, ocr, sme0, mzm, azm, r0;
+    double bl, bz, zet, vpu, porosity, fs, etao, g0, ds, damp_coe;
+} sphgpu_soil;
+
+/* Para_Structure (Class_ParticleProperty.h:135-151). */
+typedef struct sphgpu_structure {
+    double dens, eps0, e, poi, vpu, porosity, cop;
+} sphgpu_structure;
+
+/*
+ * Run parameters: the union of Para_FL, Para_Pro, Para_Inter, Para_SSInter,
+ * Para_Boundary, Para_GF and Cell_Con (Class_Problem.h:10-140,
+ * Class_NNPS.h:12-37) that the step loop reads, plus the free-surface
+ * thresholds SPH_Calculation keeps as locals (CPP_1-SPHLoops.cpp:81-84).
+ */
+typedef struct sphgpu_params {
+    int    ndim;              /* 2 or 3 */
+    int    ntotal;            /* particles */
+    /* Para_FL */
+    int    fla, fls, flr, fli, flv, fleob, flts, flspv, flknl, flbndy;
+    /* Para_Pro */
+    int    inip, step_regu, loop, fop;
+    double dr, dt;
+    double xsph[3];
+    double art_vis[3][2];
+    double art_stre_coe;
+    /* Para_GF */
+    double gx, gy, gz;
+    /* free surface colour thresholds (input block PR) */
+    double threshold_min, threshold_max;
+    /* Para_Inter */
+    double interc;
+    int    permtype;
+    double pers, perl, perm;
+    /* Para_SSInter */
+    int    ss_type;
+    double ss_myu, ss_zeta;
+    int    ss_acc_type;
+    /* Para_Boundary */
+    double coe_bndy;
+    int    if_cal, if_move;
+    double move_vx[3];
+    /* Cell_Con: domain box and cell counts (celllist_ini1, CPP_3-NNPS.cpp:96-121) */
+    double xmin, xmax, ymin, ymax, zmin, zmax;
+    int    cxm, cym, czm, ctotal;
+    /* Para_Model / Para_Fluid switches the loop branches on */
+    int    flagum;
+    double alphats;
+    int    water_acc_type;    /* pWater[0].acc_type: 0 plus-form, 1 minus-form */
+    int    air_acc_type;      /* pAir->acc_type */
+    sphgpu_structure structure;
+} sphgpu_params;
+
+typedef struct sphgpu_ctx sphgpu_ctx;
+
+/* Library / device. */
+int         sphgpu_abi_version(void);
+int         sphgpu_device_count(void);
+const char* sphgpu_error_string(int code);
+
+/*
+ * Context lifetime.  sphgpu_create copies *params, allocates every device
+ * buffer for params->ntotal particles and params->ctotal cells on `device`,
+ * and creates the context's CUDA stream.  Returns NULL on failure; the reason
+ * is available from sphgpu_last_create_error().
+ */
+sphgpu_ctx* sphgpu_create(const sphgpu_params* params, int device);
+int         sphgpu_last_create_error(void);
+void        sphgpu_destroy(sphgpu_ctx* ctx);
+int         sphgpu_get_params(const sphgpu_ctx* ctx, sphgpu_params* out);
+/* Current step counter l (Para_Pro::l); starts at 1 like the reference. */
+int         sphgpu_get_step(const sphgpu_ctx* ctx);
+int         sphgpu_set_step(sphgpu_ctx* ctx, int l);
+
+/*
+ * Field transfer, structure of arrays.  `name` is a Particle member
+ * (Class_particle.h:13-103): "xp", "vx", "sig", "rho", "type", ...
+ * sphgpu_field_info reports the component count and element type
+ * (0 = double, 1 = int32).  Host layout is particle-major
+ * (host[i * ncomp + k]), as the members are laid out in Particle.
+ */
+int sphgpu_field_info(const char* name, int* ncomp, int* elem_type);
+int sphgpu_set_field(sphgpu_ctx* ctx, const char* name, const void* host, size_t count);
+int sphgpu_get_field(sphgpu_ctx* ctx, const char* name, void* host, size_t count);
+
+/*
+ * Per-particle material records, as SPH_Calculation keeps them
+ * (pVFluid / pParti_ConsPara, CPP_1-SPHLoops.cpp:371-372; filled by
+ * setting_vis_cons, CPP_2-initialf.cpp:1021-1058).  Either pointer may be
+ * NULL (the corresponding records stay zero).
+ */
+int sphgpu_set_materials(sphgpu_ctx* ctx, const sphgpu_fluid* fluid,
+                         const sphgpu_soil* soil, int n);
+
+/*
+ * Whole-record transfer in the reference's Particle layout
+ * (Class_particle.h:13-103, 1064 bytes per particle, 8-byte aligned doubles,
+ * four trailing ints).  `stride` is sizeof(Particle) on the caller's side and
+ * must be >= 1064.  Download writes only the members the device owns.
+ */
+int sphgpu_upload_particles(sphgpu_ctx* ctx, const void* particles, int n, size_t stride);
+int sphgpu_download_particles(sphgpu_ctx* ctx, void* particles, int n, size_t stride);
+
+/*
+ * One or more complete time steps: the body of the main loop of
+ * SPH_Calculation (CPP_1-SPHLoops.cpp:523-753) for steps l, l+1, ...
+ * Host-side work the loop interleaves (rain, excavation, output) is the
+ * caller's.  Returns 0 or the first error code raised; on error the step
+ * counter stays at the failing step.
+ */
+int sphgpu_step(sphgpu_ctx* ctx, int nsteps);
+
+/*
+ * The NNPS stage alone (parttocell + partisearching for step l), leaving the
+ * neighbour lists on the device; ninflu[n] and influ[n * 100] (1-based slots
+ * 1..ninflu, as Par_Cell::influ) are copied out if non-NULL.
+ */
+int sphgpu_nnps(sphgpu_ctx* ctx, int* ninflu, int* influ);
+
+/* Block until the context's stream is idle; returns the sticky error, if any. */
+int sphgpu_synchronize(sphgpu_ctx* ctx);
+
+/*
+ * Timing: CUDA-event duration of the last sphgpu_step call (milliseconds), and
+ * the number of kernels that call launched.
+ */
+double sphgpu_last_step_ms(const sphgpu_ctx* ctx);
+long   sphgpu_last_step_launches(const sphgpu_ctx* ctx);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own
+ * work after the engine's. */
+void*  sphgpu_stream(sphgpu_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPHGPU_H_INCLUDED */

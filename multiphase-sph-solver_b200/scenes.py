@@ -1,0 +1,554 @@
+"""Synthetic scenes for the SPH engine, in the reference solver's own terms.
+
+A scene is the content of the reference's ``input.dat`` (flag, problem,
+material and particle blocks read by ``clFIni_Fun::initial_pro``,
+``initial_mat`` and ``input_par``, CPP_2-initialf.cpp:22-1018) held as numpy
+arrays and plain dicts.  From it this module
+
+* writes the ``input.dat`` text the reference parses (``write_input_dat``),
+  so the reference solver can be run on exactly the same case, and
+* computes the initial particle state that ``setting_vis_cons`` /
+  ``setting_par`` / ``celllist_ini1`` produce (``initialise``,
+  CPP_2-initialf.cpp:1021-1381, CPP_3-NNPS.cpp:96-121), so the GPU engine can
+  be started without the reference present.
+
+The generators build the workloads the engine is measured on: a 2-D water dam
+break in a walled tank, and a 3-D saturated soil column (Drucker-Prager soil
+with co-located pore water) collapsing in a walled box.  Lattice sites sit at
+cell centres ``(i + 1/2) dx``; nothing is random.
+"""
+from __future__ import annotations
+
+import copy
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# Para_Fluid / Para_Soil / Para_Structure member order (Class_ParticleProperty.h)
+FLUID_FIELDS = ("vis", "vpu", "dens", "paa0", "porosity", "fai", "c",
+                "bhtype", "press_type", "acc_type", "pre_coe", "strain_min")
+SOIL_FIELDS = ("e", "poi", "eps0", "dens", "damp1", "damp2", "cop", "ramda", "kapa", "zmf",
+               "ann", "bnn", "beta", "sitas", "sitar", "epsr", "epss", "sd", "sw", "kse",
+               "c1", "c2", "c3", "fai", "c", "ocr", "sme0", "mzm", "azm", "r0",
+               "bl", "bz", "zet", "vpu", "porosity", "fs", "etao", "g0", "ds", "damp_coe")
+STRUCT_FIELDS = ("dens", "eps0", "e", "poi", "vpu", "porosity", "cop")
+
+
+def fluid_default() -> dict:
+    """Para_Fluid::Para_Fluid (Class_ParticleProperty.cpp)."""
+    d = {k: 0.0 for k in FLUID_FIELDS}
+    d.update(bhtype=0, press_type=0, acc_type=0, strain_min=1.0)
+    return d
+
+
+def soil_default() -> dict:
+    """Para_Soil::Para_Soil (Class_ParticleProperty.cpp): fs = ds = 1."""
+    d = {k: 0.0 for k in SOIL_FIELDS}
+    d.update(fs=1.0, ds=1.0)
+    return d
+
+
+@dataclass
+class Scene:
+    """One reference input deck."""
+    name: str
+    ndim: int
+    dr: float
+    dt: float
+    loop: int
+    xp: np.ndarray            # (n, 3) float64, z = 0 in 2-D
+    vxp: np.ndarray           # (n, 3)
+    ptype: np.ndarray         # (n,) int32  Particle::type
+    matype: np.ndarray        # (n,) int32
+    permtype: np.ndarray      # (n,) int32
+    etype: np.ndarray         # (n,) int32
+    flags: dict = field(default_factory=dict)     # block FL
+    problem: dict = field(default_factory=dict)   # blocks PR XP AT GF IP BP
+    water: list = field(default_factory=list)     # 3 Para_Fluid dicts (block WP)
+    air: dict | None = None                       # block AP
+    model_flags: tuple = (0,) * 10                # block MS: em sb dp um am bui pl ve focc ep
+    soils: dict = field(default_factory=dict)     # {index: Para_Soil dict}, index = layer*10 + model
+    structure: dict | None = None                 # block SM
+
+    @property
+    def n(self) -> int:
+        return int(self.xp.shape[0])
+
+    def n_active(self) -> int:
+        """Particles of types 1-4 (water, soil, air, structure)."""
+        t = self.ptype
+        return int(np.count_nonzero((t >= 1) & (t <= 4)))
+
+
+# --------------------------------------------------------------------------
+# lattice helpers
+
+def _grid(nx, ny, nz, dx, origin):
+    """Cell-centre lattice, x fastest, z slowest.  (nx, ny, nz) >= 1."""
+    ix = (np.arange(nx, dtype=np.float64) + 0.5) * dx + origin[0]
+    iy = (np.arange(ny, dtype=np.float64) + 0.5) * dx + origin[1]
+    iz = (np.arange(nz, dtype=np.float64) + 0.5) * dx + origin[2]
+    Z, Y, X = np.meshgrid(iz, iy, ix, indexing="ij")
+    return np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+
+
+def _grid2(nx, ny, dx, origin):
+    ix = (np.arange(nx, dtype=np.float64) + 0.5) * dx + origin[0]
+    iy = (np.arange(ny, dtype=np.float64) + 0.5) * dx + origin[1]
+    Y, X = np.meshgrid(iy, ix, indexing="ij")
+    return np.stack([X.ravel(), Y.ravel(), np.zeros(X.size)], axis=1)
+
+
+def _assemble(parts):
+    xp = np.concatenate([p[0] for p in parts]).astype(np.float64)
+    n = xp.shape[0]
+    ptype = np.concatenate([np.full(p[0].shape[0], p[1], np.int32) for p in parts])
+    matype = np.concatenate([np.full(p[0].shape[0], p[2], np.int32) for p in parts])
+    return xp, np.zeros((n, 3)), ptype, matype, np.zeros(n, np.int32), np.ones(n, np.int32)
+
+
+# --------------------------------------------------------------------------
+# scenes
+
+def dam_break_2d(dx: float = 0.005, water=(0.4, 0.8), tank=(1.6, 1.0), layers: int = 3,
+                 steps: int = 2000, c0_factor: float = 10.0, alpha: float = 0.1,
+                 eps_xsph: float = 0.5, cfl: float = 0.2) -> Scene:
+    """2-D weakly compressible dam break: a water column (type 1) against the
+    left wall of a tank of 3 wall layers (type 0, matype 0).
+
+    Tait-like EOS with B = rho0 c0^2 / 7 is expressed through the reference's
+    press_type 0 (prep = rhop g dr pre_coe, CPP_2-initialf.cpp:1301-1302) with
+    pre_coe = c0^2 / (7 g dr).  The reference ties h to the particle spacing
+    (hl = dr), so h = dx here.  fls = 1 with a dummy elastic soil material of
+    void ratio 1e8 keeps the fluid porosity at 1 - 1e-8: with fls = 0 every
+    fluid porosity is exactly 1 and the porosity term of the continuity
+    equation is 0/0 at step 1 (CPP_6-density.cpp:153-156)."""
+    g = 9.81
+    H = water[1]
+    c0 = c0_factor * math.sqrt(2.0 * g * H)
+    dt = cfl * dx / c0
+    nwx, nwy = int(round(water[0] / dx)), int(round(water[1] / dx))
+    ntx, nty = int(round(tank[0] / dx)), int(round(tank[1] / dx))
+    parts = [(_grid2(nwx, nwy, dx, (0.0, 0.0)), 1, 0)]
+    floor = _grid2(ntx + 2 * layers, layers, dx, (-layers * dx, -layers * dx))
+    left = _grid2(layers, nty, dx, (-layers * dx, 0.0))
+    right = _grid2(layers, nty, dx, (ntx * dx, 0.0))
+    parts += [(floor, 0, 0), (left, 0, 0), (right, 0, 0)]
+    xp, vxp, ptype, matype, permtype, etype = _assemble(parts)
+    w = fluid_default()
+    w.update(dens=1000.0, vis=1.0e-3, vpu=c0, press_type=0, acc_type=0, bhtype=0,
+             pre_coe=c0 * c0 / (7.0 * g * dx), strain_min=1.0e-3)
+    wmin = copy.deepcopy(w)
+    dummy = soil_default()
+    dummy.update(kapa=0.05, poi=0.3, dens=2000.0, cop=1.0e-4, eps0=1.0e8, e=1.0e7, ds=1.0e-3)
+    return Scene(
+        name=f"dam_break_2d_dx{dx:g}", ndim=2, dr=dx, dt=dt, loop=steps,
+        xp=xp, vxp=vxp, ptype=ptype, matype=matype, permtype=permtype, etype=etype,
+        flags=dict(fla=0, fls=1, flr=0, fli=0, flv=0, fleob=0, flts=0, flspv=0, flknl=1,
+                   ntd=1, flbndy=1),
+        problem=dict(threshold_min=0.1, threshold_max=0.12, fop=max(steps, 1), inip=0,
+                     step_regu=100000000, dttype=1,
+                     xsph=(eps_xsph, 0.0, 0.0), art_vis=((alpha, 0.0), (0.0, 0.0), (0.0, 0.0)),
+                     art_stre_coe=0.0, g=(0.0, -g, 0.0),
+                     interc=0.0, permtype=0, pers=0.0, perl=0.0, perm=0.0,
+                     ss=(0, 0.0, 0.0, 0), if_cal=0, if_move=0, coe_bndy=0.3),
+        water=[w, copy.deepcopy(wmin), copy.deepcopy(wmin)],
+        model_flags=(1, 0, 0, 0, 0, 0, 0, 0, 0, 0),
+        soils={0: dummy},
+    )
+
+
+def soil_column_3d(dx: float = 0.005, block=(1.0, 0.5, 0.5), box=(2.0, 0.5, 0.6),
+                   layers: int = 3, steps: int = 5000, with_water: bool = True) -> Scene:
+    """3-D saturated soil column collapse: a Drucker-Prager soil block
+    (type 2, matype 2: E = 10 MPa, nu = 0.3, phi = 30 deg, c = 0,
+    rho_s = 2650, e0 = 0.6667 so porosity 0.4) overlapped site for site by
+    pore water (type 1), standing against the back wall of a box with a
+    3-layer floor, back wall and two side walls (type 0).  Darcy drag
+    (fli = 1, permeability 1e-4 m/s), gravity -z, and the reference's
+    variable time step (dttype = 2: dt = 0.25 dr / 600,
+    CPP_12-2-dt.cpp:13-20)."""
+    g = 9.81
+    nbx, nby, nbz = (int(round(b / dx)) for b in block)
+    nox, noy, noz = (int(round(b / dx)) for b in box)
+    L = layers
+    soil = _grid(nbx, nby, nbz, dx, (0.0, 0.0, 0.0))
+    parts = [(soil, 2, 2)]
+    if with_water:
+        parts.append((soil.copy(), 1, 0))
+    floor = _grid(nox + L, noy + 2 * L, L, dx, (-L * dx, -L * dx, -L * dx))
+    back = _grid(L, noy + 2 * L, noz, dx, (-L * dx, -L * dx, 0.0))
+    side0 = _grid(nox, L, noz, dx, (0.0, -L * dx, 0.0))
+    side1 = _grid(nox, L, noz, dx, (0.0, noy * dx, 0.0))
+    parts += [(floor, 0, 0), (back, 0, 0), (side0, 0, 0), (side1, 0, 0)]
+    xp, vxp, ptype, matype, permtype, etype = _assemble(parts)
+    dt_var = 0.25 * dx / 600.0
+    w = fluid_default()
+    w.update(dens=1000.0, vis=1.0e-3, vpu=30.0, press_type=0, acc_type=0, bhtype=0,
+             pre_coe=30.0 * 30.0 / (7.0 * g * dx), strain_min=1.0e-3)
+    dp = soil_default()
+    dp.update(kapa=0.05, poi=0.3, dens=2650.0, c=0.0, fai=30.0, fs=1.0,
+              damp1=0.0, damp2=0.0, cop=1.0e-4, eps0=0.6667, e=1.0e7, ds=1.0e-3)
+    return Scene(
+        name=f"soil_column_3d_dx{dx:g}", ndim=3, dr=dx,
+        dt=dt_var * steps,            # dttype 2: the input dt is the total time
+        loop=steps,
+        xp=xp, vxp=vxp, ptype=ptype, matype=matype, permtype=permtype, etype=etype,
+        flags=dict(fla=0, fls=1, flr=0, fli=1, flv=0, fleob=0, flts=0, flspv=0, flknl=1,
+                   ntd=1, flbndy=1),
+        problem=dict(threshold_min=0.1, threshold_max=0.12, fop=max(steps, 1), inip=0,
+                     step_regu=100000000, dttype=2,
+                     xsph=(0.5, 0.1, 0.0), art_vis=((0.1, 0.0), (0.1, 0.0), (0.0, 0.0)),
+                     art_stre_coe=0.0, g=(0.0, 0.0, -g),
+                     interc=1.0, permtype=0, pers=1.0e-4, perl=1.0e-4, perm=1.0e-4,
+                     ss=(0, 0.0, 0.0, 0), if_cal=0, if_move=0, coe_bndy=0.3),
+        water=[w, copy.deepcopy(w), copy.deepcopy(w)],
+        model_flags=(0, 0, 1, 0, 0, 0, 0, 0, 0, 0),
+        soils={2: dp},
+    )
+
+
+def scaled_loop(scene: Scene) -> int:
+    """Steps the reference will run: for dttype 2 the loop count is
+    int(tt / dt) + 1 with tt the input dt (CPP_12-2-dt.cpp:13-20)."""
+    if scene.problem["dttype"] == 2:
+        dtv = 0.25 * scene.dr / 600.0
+        return int(scene.dt / dtv) + 1
+    return scene.loop
+
+
+# --------------------------------------------------------------------------
+# input.dat writer (the format initial_pro / initial_mat / input_par scan)
+
+def _f(v) -> str:
+    return repr(float(v))
+
+
+def write_input_dat(scene: Scene, path: str, ntd: int = 1) -> None:
+    """Write ``scene`` as a reference input deck.  Block markers are two
+    characters or more ('A data', 'E end'): the reference's scanner
+    (``%c%*[^\\n]%*c``) mis-reads one-character lines."""
+    P, F = scene.problem, scene.flags
+    L = []
+    add = L.append
+    add("FL flags")
+    add("A data")
+    add(" ".join(str(F[k]) for k in ("fla", "fls", "flr", "fli", "flv", "fleob", "flts", "flspv", "flknl")))
+    add(f"{ntd} {F['flbndy']}")
+    add("E end")
+    add("PR problem")
+    add("A data")
+    add(f"{scene.ndim} {_f(P['threshold_min'])} {_f(P['threshold_max'])}")
+    add(f"{P['fop']} {P['inip']} {scene.loop} {scene.n} {P['step_regu']}")
+    add(f"{P['dttype']} {_f(scene.dr)} {_f(scene.dt)}")
+    add("E end")
+    add("XP xsph")
+    add("A data")
+    add(" ".join(_f(v) for v in P["xsph"]))
+    add("E end")
+    add("AT artificial viscosity")
+    add("A data")
+    av = P["art_vis"]
+    add(f"{_f(av[0][0])} {_f(av[0][1])}")
+    add(f"{_f(av[1][0])} {_f(av[1][1])} {_f(P['art_stre_coe'])}")
+    add(f"{_f(av[2][0])} {_f(av[2][1])}")
+    add("E end")
+    add("GF gravity")
+    add("A data")
+    add(" ".join(_f(v) for v in P["g"]))
+    add("E end")
+    add("IP interaction")
+    add("A data")
+    add(_f(P["interc"]))
+    add(f"{P['permtype']} {_f(P['pers'])} {_f(P['perl'])} {_f(P['perm'])}")
+    ss = P["ss"]
+    add(f"{ss[0]} {_f(ss[1])} {_f(ss[2])} {ss[3]}")
+    add("E end")
+    add("BP boundary")
+    add("A data")
+    add(f"{P['if_cal']} {P['if_move']} {_f(P['coe_bndy'])}")
+    if P["if_move"] >= 1:
+        add(" ".join(_f(v) for v in P.get("move_vx", (0.0, 0.0, 0.0))))
+    add("E end")
+    add("WP water")
+    add("A data")
+    w0 = scene.water[0]
+    add(" ".join([_f(w0["dens"]), _f(w0["vis"]), _f(w0["fai"]), _f(w0["c"]), _f(w0["vpu"]),
+                  str(w0["press_type"]), str(w0["acc_type"]), str(w0["bhtype"]),
+                  _f(w0["pre_coe"]), _f(w0["strain_min"])]))
+    for w in scene.water[1:3]:
+        add(" ".join(_f(w[k]) for k in ("dens", "vis", "fai", "c", "vpu")))
+    add("E end")
+    if scene.air is not None:
+        a = scene.air
+        add("AP air")
+        add("A data")
+        add(" ".join([_f(a["dens"]), _f(a["paa0"]), _f(a["vis"]), _f(a["vpu"]),
+                      str(a["press_type"]), str(a["acc_type"]), _f(a["pre_coe"])]))
+        add("E end")
+    add("MS soil models")
+    add("A data")
+    add(" ".join(str(v) for v in scene.model_flags))
+    add("E end")
+    mf = scene.model_flags
+    if mf[0] >= 1:
+        add("EM elastic")
+        add("A data")
+        for layer in range(mf[0]):
+            s = scene.soils[layer * 10 + 0]
+            add(" ".join(_f(s[k]) for k in ("kapa", "poi", "dens")))
+            add(" ".join(_f(s[k]) for k in ("damp1", "damp2", "cop", "eps0")))
+            add(" ".join(_f(s[k]) for k in ("e", "ds")))
+        add("E end")
+    if mf[2] >= 1:
+        add("DP drucker prager")
+        add("A data")
+        for layer in range(mf[2]):
+            s = scene.soils[layer * 10 + 2]
+            add(" ".join(_f(s[k]) for k in ("kapa", "poi", "dens", "c", "fai", "fs")))
+            add(" ".join(_f(s[k]) for k in ("damp1", "damp2", "cop", "eps0")))
+            add(" ".join(_f(s[k]) for k in ("e", "ds")))
+        add("E end")
+    if mf[5] >= 1:
+        add("BU bui drucker prager")
+        add("A data")
+        for layer in range(mf[5]):
+            s = scene.soils[layer * 10 + 5]
+            add(" ".join(_f(s[k]) for k in ("kapa", "poi", "dens", "c", "fai", "beta", "fs")))
+            add(" ".join(_f(s[k]) for k in ("damp1", "damp2", "cop", "eps0")))
+            add(" ".join(_f(s[k]) for k in ("e", "ds")))
+        add("E end")
+    if scene.structure is not None:
+        st = scene.structure
+        add("SM structure")
+        add("A data")
+        add(" ".join(_f(st[k]) for k in ("dens", "eps0", "cop")))
+        add(" ".join(_f(st[k]) for k in ("e", "poi")))
+        add("E end")
+    add("PA particles")
+    add("A data")
+    xp, vxp = scene.xp, scene.vxp
+    rows = []
+    if scene.ndim == 2:
+        for i in range(scene.n):
+            rows.append(f"{_f(xp[i, 0])} {_f(xp[i, 1])} {_f(vxp[i, 0])} {_f(vxp[i, 1])} "
+                        f"{scene.ptype[i]} {scene.matype[i]} {scene.permtype[i]} {scene.etype[i]}")
+    else:
+        for i in range(scene.n):
+            rows.append(f"{_f(xp[i, 0])} {_f(xp[i, 1])} {_f(xp[i, 2])} {_f(vxp[i, 0])} {_f(vxp[i, 1])} "
+                        f"{_f(vxp[i, 2])} {scene.ptype[i]} {scene.matype[i]} {scene.permtype[i]} {scene.etype[i]}")
+    L.extend(rows)
+    add("E end")
+    with open(path, "w") as fh:
+        fh.write("\n".join(L) + "\n")
+
+
+# --------------------------------------------------------------------------
+# initial state: initial_mat tail, setting_vis_cons, setting_par, input_par's
+# domain box and celllist_ini1
+
+def material_tables(scene: Scene):
+    """The 30 Para_Soil slots, 3 water and 1 air Para_Fluid records after
+    initial_mat (CPP_2-initialf.cpp:797-839)."""
+    soils = [soil_default() for _ in range(30)]
+    for idx, s in scene.soils.items():
+        soils[idx] = dict(s)
+    for s in soils:
+        s["vpu"] = 600.0
+        s["damp_coe"] = 0.0
+    water = [dict(fluid_default(), **w) for w in scene.water]
+    for k in (1, 2):
+        for key in ("press_type", "bhtype", "pre_coe", "strain_min"):
+            water[k][key] = water[0][key]
+    air = dict(fluid_default(), **(scene.air or {}))
+    if scene.flags["fls"] == 0:
+        por = 1.0
+        for w in water:
+            w["porosity"] = 1.0
+        air["porosity"] = 1.0
+    else:
+        for s in soils:
+            s["porosity"] = s["eps0"] / (1 + s["eps0"])
+        por = 0.0
+        for s in soils:
+            por = max(por, s["porosity"])
+        for w in water:
+            w["porosity"] = por
+        air["porosity"] = por
+    for w in water:
+        if w["dens"] <= 0.0:
+            w["dens"] = 1000.0
+    if air["dens"] <= 0.0:
+        air["dens"] = 1.293
+    st = dict({k: 0.0 for k in STRUCT_FIELDS}, **(scene.structure or {}))
+    st["vpu"] = 600.0
+    st["porosity"] = st["eps0"] / (1 + st["eps0"])
+    return soils, water, air, st
+
+
+@dataclass
+class InitialState:
+    params: dict          # sphgpu_params members
+    fields: dict          # Particle member name -> array (n,) or (n, ncomp)
+    fluid: np.ndarray     # (n, 12) records as sphgpu_fluid (structured dtype)
+    soil: np.ndarray      # (n,) structured sphgpu_soil
+
+
+FLUID_DTYPE = np.dtype([(k, np.int32 if k in ("bhtype", "press_type", "acc_type") else np.float64)
+                        for k in FLUID_FIELDS], align=True)
+SOIL_DTYPE = np.dtype([(k, np.float64) for k in SOIL_FIELDS], align=True)
+
+
+def initialise(scene: Scene) -> InitialState:
+    """Initial particle state as the reference's initialisation leaves it."""
+    n, dim, dr = scene.n, scene.ndim, scene.dr
+    soils, water, air, st = material_tables(scene)
+    P = scene.problem
+    gx, gy, gz = P["g"]
+    # setting_vis_cons (CPP_2-initialf.cpp:1021-1058)
+    fl = np.zeros(n, FLUID_DTYPE)
+    so = np.zeros(n, SOIL_DTYPE)
+    fdef = fluid_default()
+    for k in FLUID_FIELDS:
+        fl[k] = fdef[k]
+    sdef = soil_default()
+    for k in SOIL_FIELDS:
+        so[k] = sdef[k]
+    t, mt, et = scene.ptype, scene.matype, scene.etype
+    for i in range(n):
+        if t[i] == 1 or (t[i] == 7 and et[i] == 1):
+            rec = water[mt[i]]
+            fl[i] = tuple(rec[k] for k in FLUID_FIELDS)
+        elif t[i] == 3:
+            fl[i] = tuple(air[k] for k in FLUID_FIELDS)
+        if t[i] == 2 or (t[i] == 7 and et[i] == 2):
+            idx = mt[i] if mt[i] < 30 else (mt[i] % 10 if mt[i] >= 50 else None)
+            if idx is not None:
+                so[i] = tuple(soils[idx][k] for k in SOIL_FIELDS)
+    f = {name: np.zeros((n, nc)) for name, nc in
+         (("x", 3), ("vx", 3), ("ax", 3), ("axp", 3), ("ux", 3), ("strep", 3), ("interf", 3),
+          ("interfss", 3), ("eps", 6), ("sig", 6), ("adps", 6))}
+    for name in ("rho", "rhop", "mass", "hl", "pre", "prep", "e", "satu", "cop", "porosity", "cd",
+                 "poro_cop", "prew", "prea", "vsig", "veps", "divq", "divr", "meps"):
+        f[name] = np.zeros(n)
+    f["xp"] = scene.xp.copy()
+    f["vxp"] = scene.vxp.copy()
+    f["type"], f["matype"] = t.copy(), mt.copy()
+    f["permtype"], f["etype"] = scene.permtype.copy(), et.copy()
+    sitas = max(s["sitas"] for s in soils)
+    hmaxw, hminw, hmaxs, hmins = -100000.0, 100000.0, -100000.0, 100000.0
+    g_axp = np.array([gx, gy, gz])
+    for i in range(n):   # setting_par first loop (:1088-1282)
+        ti = t[i]
+        if ti == 0:
+            f["rhop"][i] = 1500.0
+            f["satu"][i] = sitas
+            f["hl"][i] = dr
+            if mt[i] == 5:
+                f["axp"][i] = g_axp
+        elif ti == 1 or (ti == 7 and et[i] == 1):
+            f["rhop"][i] = fl["porosity"][i] * fl["dens"][i]
+            f["satu"][i] = sitas
+            f["hl"][i] = dr
+            f["axp"][i] = g_axp
+            f["porosity"][i] = fl["porosity"][i]
+            if ti == 1:
+                hmaxw = max(hmaxw, scene.xp[i, dim - 1])
+                hminw = min(hminw, scene.xp[i, dim - 1])
+        elif ti == 2 or (ti == 7 and et[i] == 2):
+            por = so["porosity"][i]
+            f["rhop"][i] = (1 - por) * so["dens"][i]
+            f["satu"][i] = so["sitar"][i] if (mt[i] % 10 == 3 and mt[i] < 60) else 1.0
+            if mt[i] % 10 == 1:
+                f["roue"] = f.get("roue", np.zeros(n))
+                f["roue"][i] = (so["ramda"][i] - so["kapa"][i]) * math.log(so["ocr"][i])
+            if ti == 2:
+                hmaxs = max(hmaxs, scene.xp[i, dim - 1])
+                hmins = min(hmins, scene.xp[i, dim - 1])
+            else:
+                f["cop"][i] = so["cop"][i]
+            f["e"][i] = so["eps0"][i]
+            f["porosity"][i] = por
+            f["hl"][i] = dr
+            f["axp"][i] = g_axp
+            f["cd"][i] = so["damp_coe"][i] * math.sqrt(so["e"][i] / f["rhop"][i] / f["hl"][i] / f["hl"][i])
+        elif ti == 3:
+            f["rhop"][i] = fl["porosity"][i] * fl["dens"][i]
+            f["hl"][i] = dr
+            f["axp"][i] = g_axp
+        elif ti == 4:
+            f["rhop"][i] = (1 - st["porosity"]) * st["dens"]
+            f["satu"][i] = 1.0
+            f["e"][i] = st["eps0"]
+            f["hl"][i] = dr
+            f["axp"][i] = g_axp
+            f["cd"][i] = so["damp_coe"][i] * math.sqrt(st["e"] / f["rhop"][i] / f["hl"][i] / f["hl"][i])
+        if ti in (0, 1, 2, 3, 4) or (ti == 7 and et[i] in (1, 2)):
+            h = f["hl"][i]
+            f["mass"][i] = f["rhop"][i] * h * h if dim == 2 else f["rhop"][i] * h * h * h
+        f["rho"][i] = f["rhop"][i]
+    g = gy if dim == 2 else gz
+    for i in range(n):   # setting_par second loop (:1291-1369)
+        ti = t[i]
+        if ti == 0:
+            f["prep"][i] = 1500.0 * (-g) * abs(hmaxw - hminw) * 0.5
+            f["pre"][i] = f["prep"][i]
+        if ti == 1:
+            pc = fl["pre_coe"][i]
+            if fl["press_type"][i] == 0:
+                f["prep"][i] = f["rhop"][i] * (-g) * dr * pc
+            else:
+                f["prep"][i] = f["rhop"][i] * (-g) * abs(scene.xp[i, dim - 1] - hmaxw - pc * dr)
+            f["pre"][i] = f["prep"][i]
+        if ti == 7 and et[i] == 1:
+            f["prep"][i] = f["rhop"][i] * (-g) * dr * fl["pre_coe"][i]
+            f["pre"][i] = f["prep"][i]
+        if ti == 2 or (ti == 7 and et[i] == 2):
+            if abs(so["sme0"][i]) > 1.0e-3:
+                f["sig"][i, 0:3] = -so["sme0"][i]
+            elif ti == 2:
+                v = f["rho"][i] * g * (hmaxs - hmins) * 0.5
+                f["sig"][i, 0:3] = v
+        if ti == 3:
+            if fl["press_type"][i] == 0:
+                f["prep"][i] = fl["paa0"][i]
+            else:
+                f["prep"][i] = fl["dens"][i] * (-g) * abs(scene.xp[i, dim - 1] - hmaxw - fl["pre_coe"][i] * dr)
+            f["pre"][i] = f["prep"][i]
+    f.pop("roue", None)
+    # input_par domain box (:917-1002) and celllist_ini1 (CPP_3-NNPS.cpp:96-121)
+    bmax = np.maximum(scene.xp.max(axis=0), -10000.0)
+    bmin = np.minimum(scene.xp.min(axis=0), 10000.0)
+    for j in range(dim):
+        bmax[j] = bmax[j] + 2.0 * dr
+        bmin[j] = bmin[j] - 2.0 * dr
+    cdr = 2.0 * dr
+    cxm = int((bmax[0] - bmin[0]) / cdr + 3.0)
+    cym = int((bmax[1] - bmin[1]) / cdr + 3.0)
+    czm = int((bmax[2] - bmin[2]) / cdr + 3.0) if dim == 3 else 1
+    dttype = P["dttype"]
+    dt, loop = scene.dt, scene.loop
+    if dttype == 2:
+        tt = dt
+        dt = 0.25 * dr / 600.0
+        loop = int(tt / dt) + 1
+    params = dict(
+        ndim=dim, ntotal=n, fla=scene.flags["fla"], fls=scene.flags["fls"], flr=scene.flags["flr"],
+        fli=scene.flags["fli"], flv=scene.flags["flv"], fleob=scene.flags["fleob"],
+        flts=scene.flags["flts"], flspv=scene.flags["flspv"], flknl=scene.flags["flknl"],
+        flbndy=scene.flags["flbndy"], inip=P["inip"], step_regu=P["step_regu"], loop=loop,
+        fop=P["fop"], dr=dr, dt=dt, xsph=tuple(P["xsph"]), art_vis=tuple(map(tuple, P["art_vis"])),
+        art_stre_coe=P["art_stre_coe"], gx=gx, gy=gy, gz=gz,
+        threshold_min=P["threshold_min"], threshold_max=P["threshold_max"],
+        interc=P["interc"], permtype=P["permtype"], pers=P["pers"], perl=P["perl"], perm=P["perm"],
+        ss_type=P["ss"][0], ss_myu=P["ss"][1], ss_zeta=P["ss"][2], ss_acc_type=P["ss"][3],
+        coe_bndy=P["coe_bndy"], if_cal=P["if_cal"], if_move=P["if_move"],
+        move_vx=tuple(P.get("move_vx", (0.0, 0.0, 0.0))),
+        xmin=bmin[0], xmax=bmax[0], ymin=bmin[1], ymax=bmax[1], zmin=bmin[2], zmax=bmax[2],
+        cxm=cxm, cym=cym, czm=czm, ctotal=cxm * cym * czm,
+        flagum=scene.model_flags[3], alphats=0.0,
+        water_acc_type=water[0]["acc_type"], air_acc_type=air["acc_type"],
+        structure=st,
+    )
+    return InitialState(params=params, fields=f, fluid=fl, soil=so)

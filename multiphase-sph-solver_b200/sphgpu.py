@@ -1,0 +1,245 @@
+"""Python host binding of the sphgpu C ABI (include/sphgpu.h).
+
+This is the call a Python user makes: build a parameter record, create an
+engine on a device, upload the particle state and the per-particle material
+records, and step.  The shared library is the in-tree
+``multiphase-sph-solver_b200/libsphgpu.so`` built by ``build.py``; importing
+this module does not load it, constructing an ``Engine`` does, and raises if
+it is missing or no CUDA device is present (there is no CPU fallback).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsphgpu.so")
+
+FLUID_FIELDS = ("vis", "vpu", "dens", "paa0", "porosity", "fai", "c",
+                "bhtype", "press_type", "acc_type", "pre_coe", "strain_min")
+_FLUID_INTS = {"bhtype", "press_type", "acc_type"}
+
+
+class Fluid(C.Structure):
+    _fields_ = [(k, C.c_int if k in _FLUID_INTS else C.c_double) for k in FLUID_FIELDS]
+
+
+SOIL_FIELDS = ("e", "poi", "eps0", "dens", "damp1", "damp2", "cop", "ramda", "kapa", "zmf",
+               "ann", "bnn", "beta", "sitas", "sitar", "epsr", "epss", "sd", "sw", "kse",
+               "c1", "c2", "c3", "fai", "c", "ocr", "sme0", "mzm", "azm", "r0",
+               "bl", "bz", "zet", "vpu", "porosity", "fs", "etao", "g0", "ds", "damp_coe")
+
+
+class Soil(C.Structure):
+    _fields_ = [(k, C.c_double) for k in SOIL_FIELDS]
+
+
+class Structure(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("dens", "eps0", "e", "poi", "vpu", "porosity", "cop")]
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("ndim", C.c_int), ("ntotal", C.c_int),
+        ("fla", C.c_int), ("fls", C.c_int), ("flr", C.c_int), ("fli", C.c_int), ("flv", C.c_int),
+        ("fleob", C.c_int), ("flts", C.c_int), ("flspv", C.c_int), ("flknl", C.c_int), ("flbndy", C.c_int),
+        ("inip", C.c_int), ("step_regu", C.c_int), ("loop", C.c_int), ("fop", C.c_int),
+        ("dr", C.c_double), ("dt", C.c_double),
+        ("xsph", C.c_double * 3),
+        ("art_vis", (C.c_double * 2) * 3),
+        ("art_stre_coe", C.c_double),
+        ("gx", C.c_double), ("gy", C.c_double), ("gz", C.c_double),
+        ("threshold_min", C.c_double), ("threshold_max", C.c_double),
+        ("interc", C.c_double), ("permtype", C.c_int),
+        ("pers", C.c_double), ("perl", C.c_double), ("perm", C.c_double),
+        ("ss_type", C.c_int), ("ss_myu", C.c_double), ("ss_zeta", C.c_double), ("ss_acc_type", C.c_int),
+        ("coe_bndy", C.c_double), ("if_cal", C.c_int), ("if_move", C.c_int),
+        ("move_vx", C.c_double * 3),
+        ("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double), ("ymax", C.c_double),
+        ("zmin", C.c_double), ("zmax", C.c_double),
+        ("cxm", C.c_int), ("cym", C.c_int), ("czm", C.c_int), ("ctotal", C.c_int),
+        ("flagum", C.c_int), ("alphats", C.c_double),
+        ("water_acc_type", C.c_int), ("air_acc_type", C.c_int),
+        ("structure", Structure),
+    ]
+
+
+def params_from_dict(d: dict) -> Params:
+    p = Params()
+    for name, ctype in Params._fields_:
+        if name not in d:
+            continue
+        v = d[name]
+        if name == "xsph" or name == "move_vx":
+            for k in range(3):
+                getattr(p, name)[k] = float(v[k])
+        elif name == "art_vis":
+            for a in range(3):
+                for b in range(2):
+                    p.art_vis[a][b] = float(v[a][b])
+        elif name == "structure":
+            for k, _ in Structure._fields_:
+                setattr(p.structure, k, float(v.get(k, 0.0)))
+        else:
+            setattr(p, name, v if ctype is C.c_int else float(v))
+    return p
+
+
+def params_to_dict(p: Params) -> dict:
+    d = {}
+    for name, ctype in Params._fields_:
+        v = getattr(p, name)
+        if name in ("xsph", "move_vx"):
+            v = tuple(v[k] for k in range(3))
+        elif name == "art_vis":
+            v = tuple(tuple(v[a][b] for b in range(2)) for a in range(3))
+        elif name == "structure":
+            v = {k: getattr(v, k) for k, _ in Structure._fields_}
+        d[name] = v
+    return d
+
+
+# Particle members the engine transfers: name -> components.  Integers are
+# the four trailing members of Particle (Class_particle.h:87-94).
+FIELDS = {
+    "x": 3, "xp": 3, "vx": 3, "vxp": 3, "ax": 3, "axp": 3, "ux": 3, "strep": 3,
+    "interf": 3, "interfss": 3, "rho": 1, "rhop": 1, "mass": 1, "hl": 1, "pre": 1, "prep": 1,
+    "e": 1, "eps": 6, "sig": 6, "adps": 6, "satu": 1, "cop": 1, "vsig": 1, "veps": 1,
+    "divq": 1, "divr": 1, "meps": 1, "prew": 1, "prea": 1, "porosity": 1, "poro_cop": 1,
+    "type": 1, "matype": 1, "permtype": 1, "etype": 1,
+}
+INT_FIELDS = {"type", "matype", "permtype", "etype"}
+
+ERRORS = {0: "ok", 3: "particle outside the cell grid", 5: "more than 99 neighbours",
+          100: "bad argument", 101: "CUDA error", 102: "no CUDA device", 103: "unsupported flags",
+          104: "call order"}
+
+
+class SPHError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        super().__init__(f"{what}: error {code} ({ERRORS.get(code, 'unknown')})")
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Load libsphgpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is not built; run __graft_entry__.build()")
+    lib = C.CDLL(path)
+    lib.sphgpu_abi_version.restype = C.c_int
+    lib.sphgpu_device_count.restype = C.c_int
+    lib.sphgpu_error_string.restype = C.c_char_p
+    lib.sphgpu_error_string.argtypes = [C.c_int]
+    lib.sphgpu_create.restype = C.c_void_p
+    lib.sphgpu_create.argtypes = [C.POINTER(Params), C.c_int]
+    lib.sphgpu_last_create_error.restype = C.c_int
+    lib.sphgpu_destroy.argtypes = [C.c_void_p]
+    lib.sphgpu_get_params.argtypes = [C.c_void_p, C.POINTER(Params)]
+    lib.sphgpu_get_step.argtypes = [C.c_void_p]
+    lib.sphgpu_set_step.argtypes = [C.c_void_p, C.c_int]
+    lib.sphgpu_field_info.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    lib.sphgpu_set_field.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t]
+    lib.sphgpu_get_field.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t]
+    lib.sphgpu_set_materials.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+    lib.sphgpu_upload_particles.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_size_t]
+    lib.sphgpu_download_particles.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_size_t]
+    lib.sphgpu_step.argtypes = [C.c_void_p, C.c_int]
+    lib.sphgpu_nnps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.sphgpu_synchronize.argtypes = [C.c_void_p]
+    lib.sphgpu_last_step_ms.restype = C.c_double
+    lib.sphgpu_last_step_ms.argtypes = [C.c_void_p]
+    lib.sphgpu_last_step_launches.restype = C.c_long
+    lib.sphgpu_last_step_launches.argtypes = [C.c_void_p]
+    lib.sphgpu_stream.restype = C.c_void_p
+    lib.sphgpu_stream.argtypes = [C.c_void_p]
+    _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+class Engine:
+    """One particle system on one GPU (sphgpu_ctx)."""
+
+    def __init__(self, params: dict | Params, device: int = 0):
+        self.lib = load_library()
+        if self.lib.sphgpu_device_count() <= 0:
+            raise SPHError(102, "sphgpu_device_count")
+        self.params = params if isinstance(params, Params) else params_from_dict(params)
+        h = self.lib.sphgpu_create(C.byref(self.params), int(device))
+        if not h:
+            raise SPHError(self.lib.sphgpu_last_create_error(), "sphgpu_create")
+        self.h = C.c_void_p(h)
+        self.n = int(self.params.ntotal)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sphgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, code: int, what: str):
+        if code != 0:
+            raise SPHError(code, what)
+
+    def set_field(self, name: str, values) -> None:
+        nc = FIELDS[name]
+        dt = np.int32 if name in INT_FIELDS else np.float64
+        a = np.ascontiguousarray(np.asarray(values, dtype=dt).reshape(self.n * nc))
+        self._check(self.lib.sphgpu_set_field(self.h, name.encode(), _ptr(a), a.size), f"set_field({name})")
+
+    def get_field(self, name: str) -> np.ndarray:
+        nc = FIELDS[name]
+        dt = np.int32 if name in INT_FIELDS else np.float64
+        a = np.empty(self.n * nc, dtype=dt)
+        self._check(self.lib.sphgpu_get_field(self.h, name.encode(), _ptr(a), a.size), f"get_field({name})")
+        return a if nc == 1 else a.reshape(self.n, nc)
+
+    def set_materials(self, fluid: np.ndarray | None, soil: np.ndarray | None) -> None:
+        fp = _ptr(np.ascontiguousarray(fluid)) if fluid is not None else None
+        sp = _ptr(np.ascontiguousarray(soil)) if soil is not None else None
+        self._check(self.lib.sphgpu_set_materials(self.h, fp, sp, self.n), "set_materials")
+
+    def load_state(self, fields: dict, fluid=None, soil=None) -> None:
+        for name, v in fields.items():
+            if name in FIELDS:
+                self.set_field(name, v)
+        if fluid is not None or soil is not None:
+            self.set_materials(fluid, soil)
+
+    def step(self, nsteps: int = 1) -> None:
+        self._check(self.lib.sphgpu_step(self.h, int(nsteps)), "sphgpu_step")
+
+    def nnps(self):
+        ninflu = np.zeros(self.n, np.int32)
+        influ = np.zeros(self.n * 100, np.int32)
+        self._check(self.lib.sphgpu_nnps(self.h, _ptr(ninflu), _ptr(influ)), "sphgpu_nnps")
+        return ninflu, influ.reshape(self.n, 100)
+
+    def synchronize(self) -> None:
+        self._check(self.lib.sphgpu_synchronize(self.h), "sphgpu_synchronize")
+
+    @property
+    def step_index(self) -> int:
+        return int(self.lib.sphgpu_get_step(self.h))
+
+    def last_step_ms(self) -> float:
+        return float(self.lib.sphgpu_last_step_ms(self.h))
+
+    def last_step_launches(self) -> int:
+        return int(self.lib.sphgpu_last_step_launches(self.h))

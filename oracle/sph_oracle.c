@@ -1,0 +1,1432 @@
+/*
+ * sph_oracle.c -- CPU restatement (checker) of the reference's per-step
+ * particle loop.  TEST INFRASTRUCTURE ONLY: see sph_oracle.h.
+ *
+ * Every function below names the reference function and file:line range it
+ * restates.  Arithmetic is written in the reference's operation order so that
+ * a build with the same compiler settings (no FMA contraction, no fast-math)
+ * reproduces the reference bit for bit; the Jacobi/in-place switch is the one
+ * intended difference (sph_oracle.h).
+ */
+#include "sph_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define NB 100               /* Par_Cell::influ[100], wij[100][4] (Class_NNPS.h:71-72) */
+
+struct orc_ctx {
+    sphgpu_params P;
+    int n, l, mode;
+    double t;
+    /* Particle members (Class_particle.h:13-103), particle-major */
+    double *x, *xp, *vx, *vxp, *ax, *axp, *ux, *strep, *divx, *interf, *interfss;
+    double *rho, *rhop, *mass, *hl, *pre, *prep, *e;
+    double *eps, *deps, *sig, *dsig, *weps, *adps;
+    double *satu, *dsatu, *suct, *cop, *vsig, *veps, *divq, *divr, *meps;
+    double *prew, *prea, *porosity, *cd, *poro_cop, *beta, *beta_ts;
+    int *type, *matype, *permtype, *etype;
+    /* per-particle material records (pVFluid, pParti_ConsPara) */
+    sphgpu_fluid* fl;
+    sphgpu_soil* so;
+    /* NNPS (Class_NNPS.h) */
+    int k, size_m;
+    int *pc_cell_id, *ninflu, *influ;   /* Par_Cell */
+    double* wij;
+    int *srt_cell, *srt_pid, *tmp_cell, *tmp_pid;   /* parti_cellid sorted / temp */
+    int *ci_start, *ci_end;             /* cell_info[ctotal + 4] */
+    /* scratch */
+    double* vx_temp;
+    double* snap;                        /* Jacobi snapshots */
+};
+
+/* ------------------------------------------------------------------------- */
+/* field table                                                               */
+
+typedef struct { const char* name; int ncomp; int is_int; size_t off; } field_desc;
+
+#define FD(nm, nc) { #nm, nc, 0, offsetof(struct orc_ctx, nm) }
+#define FI(nm) { #nm, 1, 1, offsetof(struct orc_ctx, nm) }
+static const field_desc k_fields[] = {
+    FD(x, 3), FD(xp, 3), FD(vx, 3), FD(vxp, 3), FD(ax, 3), FD(axp, 3), FD(ux, 3),
+    FD(strep, 3), FD(divx, 9), FD(interf, 3), FD(interfss, 3),
+    FD(rho, 1), FD(rhop, 1), FD(mass, 1), FD(hl, 1), FD(pre, 1), FD(prep, 1), FD(e, 1),
+    FD(eps, 6), FD(deps, 6), FD(sig, 6), FD(dsig, 6), FD(weps, 9), FD(adps, 6),
+    FD(satu, 1), FD(dsatu, 1), FD(suct, 1), FD(cop, 1), FD(vsig, 1), FD(veps, 1),
+    FD(divq, 1), FD(divr, 1), FD(meps, 1), FD(prew, 1), FD(prea, 1), FD(porosity, 1),
+    FD(cd, 1), FD(poro_cop, 1), FD(beta, 9), FD(beta_ts, 9),
+    FI(type), FI(matype), FI(permtype), FI(etype),
+};
+#define NFIELDS (sizeof(k_fields) / sizeof(k_fields[0]))
+
+static const field_desc* find_field(const char* name)
+{
+    for (size_t i = 0; i < NFIELDS; i++)
+        if (strcmp(k_fields[i].name, name) == 0) return &k_fields[i];
+    return NULL;
+}
+
+orc_ctx* orc_create(const sphgpu_params* p)
+{
+    if (!p || p->ntotal <= 0) return NULL;
+    orc_ctx* c = (orc_ctx*)calloc(1, sizeof(orc_ctx));
+    c->P = *p;
+    c->n = p->ntotal;
+    c->l = 1;   /* Para_Pro::l starts at 1 (Class_Problem.cpp:66) */
+    c->mode = ORC_JACOBI;
+    int n = c->n;
+    for (size_t f = 0; f < NFIELDS; f++) {
+        void** slot = (void**)((char*)c + k_fields[f].off);
+        *slot = calloc((size_t)n * k_fields[f].ncomp, k_fields[f].is_int ? sizeof(int) : sizeof(double));
+    }
+    c->fl = (sphgpu_fluid*)calloc(n, sizeof(sphgpu_fluid));
+    c->so = (sphgpu_soil*)calloc(n, sizeof(sphgpu_soil));
+    for (int i = 0; i < n; i++) {
+        c->fl[i].strain_min = 1.0;   /* Para_Fluid() (Class_ParticleProperty.cpp) */
+        c->so[i].fs = 1.0;            /* Para_Soil()  */
+        c->so[i].ds = 1.0;
+    }
+    /* allocation sizes of SPH_Calculation (CPP_1-SPHLoops.cpp:355-376) */
+    c->k = (int)log2((double)n) + 1;
+    c->size_m = 1 << c->k;
+    c->pc_cell_id = (int*)malloc(sizeof(int) * n);
+    for (int i = 0; i < n; i++) c->pc_cell_id[i] = -1;
+    c->ninflu = (int*)calloc(n, sizeof(int));
+    c->influ = (int*)calloc((size_t)n * NB, sizeof(int));
+    c->wij = (double*)calloc((size_t)n * NB * 4, sizeof(double));
+    c->srt_cell = (int*)malloc(sizeof(int) * c->size_m);
+    c->srt_pid = (int*)malloc(sizeof(int) * c->size_m);
+    c->tmp_cell = (int*)malloc(sizeof(int) * c->size_m);
+    c->tmp_pid = (int*)malloc(sizeof(int) * c->size_m);
+    for (int i = 0; i < c->size_m; i++) {   /* parti_cellid() (Class_NNPS.cpp:48-52) */
+        c->srt_cell[i] = 10000000; c->srt_pid[i] = 10000000;
+        c->tmp_cell[i] = 10000000; c->tmp_pid[i] = 10000000;
+    }
+    int nc = p->ctotal + 4;
+    c->ci_start = (int*)malloc(sizeof(int) * nc);
+    c->ci_end = (int*)malloc(sizeof(int) * nc);
+    for (int i = 0; i < nc; i++) { c->ci_start[i] = 2000000; c->ci_end[i] = -2000000; } /* cell_info() */
+    c->vx_temp = (double*)calloc((size_t)n * 3, sizeof(double));
+    c->snap = (double*)calloc((size_t)n * 6, sizeof(double));
+    return c;
+}
+
+void orc_destroy(orc_ctx* c)
+{
+    if (!c) return;
+    for (size_t f = 0; f < NFIELDS; f++) free(*(void**)((char*)c + k_fields[f].off));
+    free(c->fl); free(c->so); free(c->pc_cell_id); free(c->ninflu); free(c->influ); free(c->wij);
+    free(c->srt_cell); free(c->srt_pid); free(c->tmp_cell); free(c->tmp_pid);
+    free(c->ci_start); free(c->ci_end); free(c->vx_temp); free(c->snap);
+    free(c);
+}
+
+int orc_set_field(orc_ctx* c, const char* name, const void* host, size_t count)
+{
+    const field_desc* f = find_field(name);
+    if (!f || !host) return SPHGPU_E_ARG;
+    size_t want = (size_t)c->n * f->ncomp;
+    if (count != want) return SPHGPU_E_ARG;
+    memcpy(*(void**)((char*)c + f->off), host, want * (f->is_int ? sizeof(int) : sizeof(double)));
+    return 0;
+}
+
+int orc_get_field(orc_ctx* c, const char* name, void* host, size_t count)
+{
+    const field_desc* f = find_field(name);
+    if (!f || !host) return SPHGPU_E_ARG;
+    size_t want = (size_t)c->n * f->ncomp;
+    if (count != want) return SPHGPU_E_ARG;
+    memcpy(host, *(void**)((char*)c + f->off), want * (f->is_int ? sizeof(int) : sizeof(double)));
+    return 0;
+}
+
+int orc_set_materials(orc_ctx* c, const sphgpu_fluid* fluid, const sphgpu_soil* soil, int n)
+{
+    if (n != c->n) return SPHGPU_E_ARG;
+    if (fluid) memcpy(c->fl, fluid, sizeof(sphgpu_fluid) * n);
+    if (soil) memcpy(c->so, soil, sizeof(sphgpu_soil) * n);
+    return 0;
+}
+
+void orc_set_mode(orc_ctx* c, int mode) { c->mode = mode; }
+int orc_get_step(const orc_ctx* c) { return c->l; }
+
+/* ------------------------------------------------------------------------- */
+/* NNPS                                                                       */
+
+/* weight(): cubic B-spline value and gradient, CPP_3-NNPS.cpp:17-48 */
+static void weight(double dst, double ra, const double dx[], double* w1ij, int ndim)
+{
+    double a1, s;
+    int k;
+    s = dst / ra;
+    a1 = 0.0;
+    if (ndim == 2) {
+        a1 = 0.682092613250980 / ra / ra;
+        w1ij[ndim] = 0.0;
+    }
+    if (ndim == 3) a1 = 0.477464829275686 / ra / ra / ra;
+    if (s == 0.0) {
+        for (k = 0; k < ndim; k++) w1ij[k] = 0.0;
+        w1ij[3] = a1 * (0.66666667 - s * s + 0.5 * s * s * s);
+    }
+    if (s > 0.0 && s <= 1.0) {
+        for (k = 0; k < ndim; k++) w1ij[k] = a1 * dx[k] * (-2 * s + 1.5 * s * s) / (ra * dst);
+        w1ij[3] = a1 * (0.66666667 - s * s + 0.5 * s * s * s);
+    } else if (s > 1.0 && s <= 2.0) {
+        for (k = 0; k < ndim; k++) w1ij[k] = a1 * (-0.5) * dx[k] * (2.0 - s) * (2.0 - s) / (ra * dst);
+        w1ij[3] = a1 * (2.0 - s) * (2.0 - s) * (2.0 - s) / 6.0;
+    }
+}
+
+/* weight2(): Yang & Liu kernel, CPP_3-NNPS.cpp:51-82 */
+static void weight2(double dst, double ra, const double dx[], double* w1ij, int ndim)
+{
+    double a1, s;
+    int k;
+    s = dst / ra;
+    a1 = 0.0;
+    if (ndim == 2) {
+        a1 = 0.106103295394597 / (ra * ra);
+        w1ij[ndim] = 0.0;
+    }
+    if (ndim == 3) a1 = 0.077010456334788 / (ra * ra * ra);
+    if (s == 0.0) {
+        for (k = 0; k < ndim; k++) w1ij[k] = 0.0;
+        w1ij[3] = a1 * (6.0 - 6.0 * s + 1.0 * s * s * s);
+    }
+    if (s > 0.0 && s <= 1.0) {
+        for (k = 0; k < ndim; k++) w1ij[k] = a1 * dx[k] * (-6.0 + 3.0 * s * s) / (ra * dst);
+        w1ij[3] = a1 * (6.0 - 6.0 * s + 1.0 * s * s * s);
+    } else if (s > 1.0 && s <= 2.0) {
+        for (k = 0; k < ndim; k++) w1ij[k] = a1 * (-3.0) * dx[k] * (2.0 - s) * (2.0 - s) / (ra * dst);
+        w1ij[3] = a1 * (2.0 - s) * (2.0 - s) * (2.0 - s);
+    }
+}
+
+/* cell_link entries, celllist_ini2 (CPP_3-NNPS.cpp:124-171): stencil slot p of
+ * cell i, 0 when outside [0, m]. */
+static int cell_link(const sphgpu_params* P, int i, int p)
+{
+    int m = P->ctotal, v;
+    if (P->ndim == 2) {
+        int ky = p / 3 + 1, kx = p % 3 + 1;
+        v = (kx - 2) * P->cym + ky - 2 + i;
+    } else {
+        int kz = p / 9 + 1, kx = (p / 3) % 3 + 1, ky = p % 3 + 1;
+        v = (ky - 2) * P->cxm * P->czm + (kx - 2) * P->czm + kz - 2 + i;
+    }
+    if (v < 0 || v > m) v = 0;
+    return v;
+}
+
+/* Merge_CellID: CPP_3-NNPS.cpp:561-594 (right element taken on equal keys) */
+static void merge_cells(orc_ctx* c, int start, int mid, int end)
+{
+    int i, j, k;
+    for (i = start; i <= end; i++) { c->tmp_cell[i] = c->srt_cell[i]; c->tmp_pid[i] = c->srt_pid[i]; }
+    i = start; j = mid + 1; k = start;
+    while (i < mid + 1 && j <= end) {
+        if (c->tmp_cell[i] < c->tmp_cell[j]) { c->srt_cell[k] = c->tmp_cell[i]; c->srt_pid[k++] = c->tmp_pid[i++]; }
+        else { c->srt_cell[k] = c->tmp_cell[j]; c->srt_pid[k++] = c->tmp_pid[j++]; }
+    }
+    while (i < mid + 1) { c->srt_cell[k] = c->tmp_cell[i]; c->srt_pid[k++] = c->tmp_pid[i++]; }
+    while (j <= end) { c->srt_cell[k] = c->tmp_cell[j]; c->srt_pid[k++] = c->tmp_pid[j++]; }
+}
+
+/* Binary_Sort: bottom-up merge passes and the cell_info scan,
+ * CPP_3-NNPS.cpp:597-630 */
+static void binary_sort(orc_ctx* c)
+{
+    for (int i_k = 1; i_k <= c->k; i_k++) {
+        int interval = 1 << i_k;
+        int group_num = c->size_m / interval;
+        for (int g = 0; g < group_num; g++) {
+            int start = g * interval, end = (g + 1) * interval - 1;
+            merge_cells(c, start, (start + end) >> 1, end);
+        }
+    }
+    for (int i = 0; i < c->n; i++) {
+        int cid = c->srt_cell[i];
+        if (i < c->ci_start[cid]) c->ci_start[cid] = i;
+        if (i > c->ci_end[cid]) c->ci_end[cid] = i;
+    }
+}
+
+/* parttocell: CPP_3-NNPS.cpp:175-263 */
+static int parttocell(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    int m = P->ctotal, t = 0;
+    double xmin[3] = {P->xmin, P->ymin, P->zmin};
+    double dr = 2.0 * P->dr;
+    for (int i = 0; i < m; i++) { c->ci_start[i] = 10000000; c->ci_end[i] = -10000000; }
+    for (int i = 0; i < c->n; i++) {
+        int nx_t[3];
+        for (int j = 0; j < P->ndim; j++) {
+            double nx = fabs(c->xp[i * 3 + j] - xmin[j]) / dr + 2.0;
+            nx_t[j] = (int)(nx);
+            if (nx_t[j] < 2) nx_t[j] = 2;
+        }
+        if (P->ndim == 2) c->srt_cell[i] = P->cym * (nx_t[0] - 1) + nx_t[1];
+        else c->srt_cell[i] = P->cxm * P->czm * (nx_t[1] - 1) + P->czm * (nx_t[0] - 1) + nx_t[2];
+        c->srt_pid[i] = i;
+    }
+    /* positions >= ntotal keep the padding records (10000000, 10000000) */
+    for (int i = c->n; i < c->size_m; i++) { c->srt_cell[i] = 10000000; c->srt_pid[i] = 10000000; }
+    for (int i = 0; i < c->n; i++) {
+        if (c->srt_cell[i] > 0 && c->srt_cell[i] <= m) c->pc_cell_id[i] = c->srt_cell[i];
+        else t = 3;
+    }
+    if (t > 0) return t;
+    binary_sort(c);
+    return t;
+}
+
+/* partisearching: CPP_3-NNPS.cpp:265-374 */
+static int partisearching(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    int dim = P->ndim, temp = (dim == 2) ? 9 : 27, t = 0;
+    for (int i = 0; i < c->n; i++) c->ninflu[i] = 0;
+    for (int i = 0; i < c->n; i++) {
+        if (c->type[i] == 7) continue;
+        int nc = c->pc_cell_id[i];
+        for (int nj = 0; nj < temp; nj++) {
+            int nl = cell_link(P, nc, nj);
+            if (nl <= 0) continue;
+            int start = c->ci_start[nl], end = c->ci_end[nl];
+            for (int np = start; np <= end; np++) {
+                int j = c->srt_pid[np];
+                double dst = 0.0, dx[3];
+                for (int k = 0; k < dim; k++) {
+                    dst = dst + (c->xp[i * 3 + k] - c->xp[j * 3 + k]) * (c->xp[i * 3 + k] - c->xp[j * 3 + k]);
+                    dx[k] = c->xp[i * 3 + k] - c->xp[j * 3 + k];
+                }
+                dst = sqrt(dst);
+                double ra = (c->hl[i] + c->hl[j]) / 2;
+                if (dst <= 2 * ra && i != j) {
+                    c->ninflu[i] += 1;
+                    int p = c->ninflu[i];
+                    if (p <= 99) {
+                        c->influ[i * NB + p] = j;
+                        if (P->flknl == 1 || P->flknl == 3) weight(dst, ra, dx, &c->wij[(i * NB + p) * 4], dim);
+                        else weight2(dst, ra, dx, &c->wij[(i * NB + p) * 4], dim);
+                    } else
+                        t = 5;
+                }
+            }
+        }
+    }
+    return t;
+}
+
+#define W(i, nj, k) (c->wij[((size_t)(i) * NB + (nj)) * 4 + (k)])
+#define NBR(i, nj) (c->influ[(size_t)(i) * NB + (nj)])
+
+/* ------------------------------------------------------------------------- */
+/* density: CPP_6-density.cpp:11-189                                          */
+static void density(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    int n = c->n, ndim = P->ndim, l = c->l, bndytype = P->flbndy;
+    double dt = P->dt;
+    /* fluid porosity from soil neighbours (:25-54) */
+    for (int i = 0; i < n; i++) {
+        double up = 0.0, down = 0.0;
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj);
+            if (c->type[i] != c->type[j] && c->type[i] == 1 && c->type[j] == 2) {
+                up = up + c->mass[j] * c->porosity[j] / c->rho[j] * W(i, nj, 3);
+                down = down + c->mass[j] / c->rho[j] * W(i, nj, 3);
+            }
+        }
+        if (c->type[i] == 1 && fabs(down) > 1.0e-7) {
+            c->poro_cop[i] = c->porosity[i];
+            c->porosity[i] = up / down;
+            if (l == 1) c->poro_cop[i] = c->porosity[i];
+        } else if (c->type[i] == 1 && fabs(down) <= 1.0e-7) {
+            c->poro_cop[i] = c->porosity[i];
+        }
+    }
+    /* continuity (:57-165) */
+    for (int i = 0; i < n; i++) {
+        double drhot = 0.0, up[3] = {0, 0, 0}, down[3] = {0, 0, 0}, vxj[3];
+        int ti = c->type[i];
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj), k;
+            if (ti == c->type[j] && ti != 7 && ti != 0) {
+                if (ti == 2 || ti == 4) {
+                    for (k = 0; k < ndim; k++) {
+                        up[k] = up[k] + c->mass[j] * (c->vxp[i * 3 + k] - c->vxp[j * 3 + k]) * W(i, nj, k);
+                        down[k] = down[k] + c->mass[j] * (c->xp[i * 3 + k] - c->xp[j * 3 + k]) * W(i, nj, k);
+                    }
+                }
+                if (ti == 1 || ti == 3) {
+                    for (k = 0; k < ndim; k++)
+                        up[k] = up[k] + c->mass[j] * (c->vxp[i * 3 + k] - c->vxp[j * 3 + k]) * W(i, nj, k);
+                }
+            } else if ((ti == 1 || ti == 2 || ti == 3 || ti == 4) && c->type[j] == 0) {
+                vxj[0] = vxj[1] = vxj[2] = 0.0;
+                if (bndytype == 1) {
+                    vxj[0] = c->vxp[i * 3 + 0]; vxj[1] = c->vxp[i * 3 + 1]; vxj[2] = c->vxp[i * 3 + 2];
+                }
+                /* bndytype 2/3/4/13/14 read clVar_Boundary: not restated (flbndy 1 only) */
+                if (ti == 2 || ti == 4) {
+                    for (k = 0; k < ndim; k++) {
+                        up[k] = up[k] + c->mass[j] * (c->vxp[i * 3 + k] - vxj[k]) * W(i, nj, k);
+                        down[k] = down[k] + c->mass[j] * (c->xp[i * 3 + k] - c->xp[j * 3 + k]) * W(i, nj, k);
+                    }
+                }
+                if (ti == 1 || ti == 3) {
+                    for (k = 0; k < ndim; k++)
+                        up[k] = up[k] + c->mass[j] * (c->vxp[i * 3 + k] - vxj[k]) * W(i, nj, k);
+                }
+            }
+        }
+        if (ti != 7) {
+            int k;
+            if (ti == 2 || ti == 4) {
+                for (k = 0; k < ndim; k++) {
+                    if (fabs(down[k]) > 1.0e-7) drhot -= up[k] / down[k];
+                    else drhot += up[k];
+                }
+            }
+            if (ti == 1 || ti == 3)
+                for (k = 0; k < ndim; k++) drhot += up[k];
+            if (ti == 1) {
+                if (fabs(c->porosity[i]) > 0.0001)
+                    c->rho[i] = c->rhop[i] + drhot * dt + c->rhop[i] * (c->porosity[i] - c->poro_cop[i]) / (1.0 - c->poro_cop[i]);
+                else
+                    c->rho[i] = c->rhop[i] + drhot * dt;
+            } else {
+                c->rho[i] = c->rhop[i] + drhot * dt;
+            }
+        }
+    }
+    /* Shepard filter (:168-188).  Reference: in place; Jacobi: snapshot. */
+    const double* rho_src = c->rho;
+    if (c->mode == ORC_JACOBI) {
+        memcpy(c->snap, c->rho, sizeof(double) * n);
+        rho_src = c->snap;
+    }
+    for (int i = 0; i < n; i++) {
+        double up = 0.0, down = 0.0;
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj);
+            if (c->type[i] == c->type[j]) {
+                up = up + c->mass[j] * W(i, nj, 3);
+                down = down + c->mass[j] / rho_src[j] * W(i, nj, 3);
+            }
+        }
+        if (c->type[i] != 7 && fabs(down) > 1.0e-7) c->rho[i] = up / down;
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+/* strain_noreg: CPP_7-1-strain.cpp:20-220                                    */
+static void strain_noreg(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    int n = c->n, dim = P->ndim, bndytype = P->flbndy;
+    for (int i = 0; i < n; i++) {
+        double dvx[3], up[9], vxj[3], down[3];
+        int j, k;
+        if (c->l == P->inip)
+            for (j = 0; j < 6; j++) c->eps[i * 6 + j] = 0.0;
+        for (j = 0; j < 6; j++) { c->deps[i * 6 + j] = 0.0; c->dsig[i * 6 + j] = 0.0; }
+        for (j = 0; j < 9; j++) { c->weps[i * 9 + j] = 0.0; c->divx[i * 9 + j] = 0.0; up[j] = 0.0; }
+        for (j = 0; j < 3; j++) down[j] = 0;
+        int ti = c->type[i];
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            for (k = 0; k < 3; k++) dvx[k] = 0.0;
+            j = NBR(i, nj);
+            int touch = 0;
+            if (ti == c->type[j] && ti != 7 && ti != 0) {
+                for (k = 0; k < 3; k++) dvx[k] = c->vxp[i * 3 + k] - c->vxp[j * 3 + k];
+                touch = 1;
+            } else if ((ti == 1 || ti == 2 || ti == 3 || ti == 4) && c->type[j] == 0) {
+                vxj[0] = vxj[1] = vxj[2] = 0.0;
+                if (bndytype == 1) {
+                    vxj[0] = c->vxp[i * 3 + 0]; vxj[1] = c->vxp[i * 3 + 1]; vxj[2] = c->vxp[i * 3 + 2];
+                }
+                for (k = 0; k < 3; k++) dvx[k] = c->vxp[i * 3 + k] - vxj[k];
+                touch = 1;
+            }
+            if (!touch) continue;
+            double mr = c->mass[j];
+            double rj = c->rho[j];
+            up[0] = up[0] + mr / rj * dvx[0] * W(i, nj, 0);
+            up[1] = up[1] + mr / rj * dvx[0] * W(i, nj, 1);
+            up[2] = up[2] + mr / rj * dvx[0] * W(i, nj, 2);
+            up[3] = up[3] + mr / rj * dvx[1] * W(i, nj, 0);
+            up[4] = up[4] + mr / rj * dvx[1] * W(i, nj, 1);
+            up[5] = up[5] + mr / rj * dvx[1] * W(i, nj, 2);
+            up[6] = up[6] + mr / rj * dvx[2] * W(i, nj, 0);
+            up[7] = up[7] + mr / rj * dvx[2] * W(i, nj, 1);
+            up[8] = up[8] + mr / rj * dvx[2] * W(i, nj, 2);
+            if (ti == 2 || ti == 4) {
+                down[0] = down[0] + mr / rj * (c->xp[i * 3 + 0] - c->xp[j * 3 + 0]) * W(i, nj, 0);
+                down[1] = down[1] + mr / rj * (c->xp[i * 3 + 1] - c->xp[j * 3 + 1]) * W(i, nj, 1);
+                down[2] = down[2] + mr / rj * (c->xp[i * 3 + 2] - c->xp[j * 3 + 2]) * W(i, nj, 2);
+            }
+        }
+        double* dv = &c->divx[i * 9];   /* divx[a][b] = dv[a*3+b] */
+        if (ti == 1 || ti == 3) {
+            dv[0] = up[0]; dv[3] = up[3]; dv[6] = up[6];
+            dv[1] = up[1]; dv[4] = up[4]; dv[7] = up[7];
+            dv[2] = up[2]; dv[5] = up[5]; dv[8] = up[8];
+        } else {
+            if (fabs(down[0]) > 1.0e-7) { dv[0] = up[0] / down[0]; dv[3] = up[3] / down[0]; dv[6] = up[6] / down[0]; }
+            if (fabs(down[1]) > 1.0e-7) { dv[1] = up[1] / down[1]; dv[4] = up[4] / down[1]; dv[7] = up[7] / down[1]; }
+            if (fabs(down[2]) > 1.0e-7) { dv[2] = up[2] / down[2]; dv[5] = up[5] / down[2]; dv[8] = up[8] / down[2]; }
+        }
+        double* de = &c->deps[i * 6];
+        de[0] = dv[0];
+        de[1] = dv[4];
+        de[2] = dv[8];
+        de[3] = dv[1] + dv[3];
+        de[4] = dv[5] + dv[7];
+        de[5] = dv[6] + dv[2];
+        if (dim == 2) { de[2] = 0.0; de[4] = 0.0; de[5] = 0.0; }
+        double* we = &c->weps[i * 9];
+        we[0] = 0.0;
+        we[1] = 0.5 * (dv[1] - dv[3]);
+        we[2] = 0.5 * (dv[2] - dv[6]);
+        we[3] = 0.5 * (dv[3] - dv[1]);
+        we[4] = 0.0;
+        we[5] = 0.5 * (dv[5] - dv[7]);
+        we[6] = 0.5 * (dv[6] - dv[2]);
+        we[7] = 0.5 * (dv[7] - dv[5]);
+        we[8] = 0.0;
+        if (dim == 2) { we[2] = 0.0; we[5] = 0.0; we[6] = 0.0; we[7] = 0.0; we[8] = 0.0; }
+    }
+}
+
+/* Shepard smoothing of eps or sig: strain_regu / stress_regu,
+ * CPP_7-2-constitutive.cpp:385-450 (in place in the reference) */
+static void regularise(orc_ctx* c, double* f)
+{
+    int n = c->n;
+    const double* src = f;
+    if (c->mode == ORC_JACOBI) {
+        memcpy(c->snap, f, sizeof(double) * 6 * n);
+        src = c->snap;
+    }
+    for (int i = 0; i < n; i++) {
+        double up[6] = {0, 0, 0, 0, 0, 0}, down = 0.0;
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj);
+            if (c->type[i] == c->type[j]) {
+                for (int q = 0; q < 6; q++) up[q] = up[q] + c->mass[j] / c->rho[j] * W(i, nj, 3) * src[j * 6 + q];
+                down = down + c->mass[j] / c->rho[j] * W(i, nj, 3);
+            }
+        }
+        if (fabs(down) > 1.0e-6)
+            for (int q = 0; q < 6; q++) f[i * 6 + q] = up[q] / down;
+    }
+}
+
+/* cal_permeability: CPP_7-2-constitutive.cpp:355-382 (Particle::permeablel /
+ * permeabletl: Class_particle.cpp:147-173) */
+static void cal_permeability(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    for (int i = 0; i < c->n; i++) {
+        if (c->type[i] != 2) continue;
+        if (P->permtype == 0) c->cop[i] = c->so[i].cop;
+        else if (P->permtype == 1) c->cop[i] = P->pers;
+        else if (P->permtype == 2) {
+            double sitas = c->so[i].sitas, sitar = c->so[i].sitar;
+            if (c->satu[i] < sitar) c->cop[i] = P->pers;
+            else if (c->satu[i] > sitas) c->cop[i] = P->perl;
+            else c->cop[i] = (P->perl - P->pers) * c->satu[i] / (sitas - sitar) + P->pers;
+        } else if (P->permtype == 3) {
+            if (c->permtype[i] == 1) c->cop[i] = P->pers;
+            if (c->permtype[i] == 2) c->cop[i] = P->perm;
+            if (c->permtype[i] == 3) c->cop[i] = P->perl;
+        }
+    }
+}
+
+/* eos: CPP_7-1-eos_CR.cpp:12-178 */
+static void eos(orc_ctx* c)
+{
+    int n = c->n;
+    for (int i = 0; i < n; i++) {
+        if (c->type[i] == 1) {
+            c->pre[i] = c->prep[i] * (pow(c->rho[i] / c->fl[i].dens / c->fl[i].porosity, 7.0) - 1.0);
+            c->pre[i] = c->pre[i] + c->prep[i];
+        }
+        if (c->type[i] == 3) {
+            /* the reference's comma expression evaluates to -1.0 (:34) */
+            c->pre[i] = 1.403 * c->prep[i] * (-1.0);
+            c->pre[i] = c->pre[i] + c->prep[i];
+        }
+        if (c->type[i] == 0 && c->matype[i] == 1) {
+            c->pre[i] = c->prep[i] * (pow(c->rho[i] / c->rhop[i], 7.0) - 1.0);
+            c->pre[i] = c->pre[i] + c->prep[i];
+        }
+    }
+    /* the gathered pressures and wall stresses are all written after the
+     * loop reads them only from other types, so one buffer suffices */
+    double* sig_new = c->snap;   /* wall stresses: soil sig is read, wall sig written */
+    for (int i = 0; i < n; i++) {
+        double u1 = 0, u2 = 0, u3 = 0, u4 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, us[6] = {0, 0, 0, 0, 0, 0}, ds = 0;
+        int ti = c->type[i];
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj), tj = c->type[j];
+            if (ti == tj) continue;
+            double m = c->mass[j], w = W(i, nj, 3), r = c->rho[j];
+            if (ti == 2 && tj == 1) { u1 = u1 + m * c->pre[j] * w / r; d1 = d1 + m * w / r; }
+            if (ti == 2 && tj == 3) { u2 = u2 + m * c->pre[j] * w / r; d2 = d2 + m * w / r; }
+            if (ti == 4 && tj == 1) { u3 = u3 + m * c->pre[j] * w / r; d3 = d3 + m * w / r; }
+            if (ti == 4 && tj == 3) { u4 = u4 + m * c->pre[j] * w / r; d4 = d4 + m * w / r; }
+            if (ti == 0 && tj == 1) { u1 = u1 + m * c->pre[j] * w / r; d1 = d1 + m * w / r; }
+            if (ti == 0 && tj == 3) { u2 = u2 + m * c->pre[j] * w / r; d2 = d2 + m * w / r; }
+            if (ti == 0 && tj == 2) {
+                for (int q = 0; q < 6; q++) us[q] = us[q] + m * c->sig[j * 6 + q] * w / r;
+                ds = ds + m * w / r;
+            }
+        }
+        if (ti == 2) {
+            c->prew[i] = (d1 != 0.0) ? u1 / d1 : u1;
+            c->prea[i] = (d2 != 0.0) ? u2 / d2 : u2;
+        } else if (ti == 0) {
+            c->prew[i] = (d1 != 0.0) ? u1 / d1 : u1;
+            c->prea[i] = (d2 != 0.0) ? u2 / d2 : u2;
+            for (int q = 0; q < 6; q++) sig_new[i * 6 + q] = (ds != 0.0) ? us[q] / ds : us[q];
+        } else if (ti == 4) {
+            c->prew[i] = (d3 != 0.0) ? u3 / d3 : u3;
+            c->prea[i] = (d4 != 0.0) ? u4 / d4 : u4;
+        }
+    }
+    for (int i = 0; i < n; i++)
+        if (c->type[i] == 0)
+            for (int q = 0; q < 6; q++) c->sig[i * 6 + q] = sig_new[i * 6 + q];
+}
+
+/* Particle::deq, shearstrain, poro_cal, stress_adjust:
+ * Class_particle.cpp:121-143, 175-215 */
+static void deq(orc_ctx* c, int i)
+{
+    double* s = &c->sig[i * 6];
+    double* ep = &c->eps[i * 6];
+    c->veps[i] = ep[0] + ep[1] + ep[2];
+    c->vsig[i] = (s[0] + s[1] + s[2]) / 3;
+    c->divq[i] = 0.0;
+    double sxx = s[0] - c->vsig[i], syy = s[1] - c->vsig[i], szz = s[2] - c->vsig[i];
+    double j2 = 0.5 * (sxx * sxx + syy * syy + szz * szz) + s[3] * s[3] + s[4] * s[4] + s[5] * s[5];
+    c->divq[i] = sqrt(3 * fabs(j2));
+    if (c->vsig[i] != 0.0) c->divr[i] = fabs(c->divq[i] / c->vsig[i]);
+    else c->divr[i] = 0.0;
+}
+
+static void shearstrain(orc_ctx* c, int i)
+{
+    double* ep = &c->eps[i * 6];
+    double sxx = ep[0] - c->veps[i] / 3.0, syy = ep[1] - c->veps[i] / 3.0, szz = ep[2] - c->veps[i] / 3.0;
+    double j2 = 0.5 * (sxx * sxx + syy * syy + szz * szz) + ep[3] * ep[3] + ep[4] * ep[4] + ep[5] * ep[5];
+    c->meps[i] = sqrt(2.0 * fabs(j2));
+}
+
+static void poro_cal(orc_ctx* c, int i, double dt)
+{
+    double* de = &c->deps[i * 6];
+    double d = (1 + c->e[i]) * (de[0] + de[1] + de[2]) * dt;
+    double et = c->e[i] + d;
+    if (et < 0.0) et = 0.0;
+    c->porosity[i] = et / (1 + et);
+    c->e[i] = et;
+}
+
+static void stress_adjust(orc_ctx* c, int i)
+{
+    if (c->vsig[i] > 0.0) {
+        double temp = -c->vsig[i];
+        double* s = &c->sig[i * 6];
+        s[0] = s[0] + temp; s[1] = s[1] + temp; s[2] = s[2] + temp;
+        s[3] = 0.0; s[4] = 0.0; s[5] = 0.0;
+    }
+}
+
+/* elastic D matrix shared by elastic() / dpmodel1() / dpmodel_bui():
+ * CPP_8-1-consfactor.cpp:17-59, 301-334, 468-501 */
+static void elastic_d(double dept[6][6], const double* sig, const sphgpu_soil* so, double* dlam_o, double* dmu_o, double* sm_o)
+{
+    double sigct[6], sm, e0, dlam, dmu, dmu2;
+    double poi = so->poi, eps0 = so->eps0, zkapa = so->kapa;
+    for (int a = 0; a < 6; a++) {
+        sigct[a] = -sig[a];
+        for (int b = 0; b < 6; b++) dept[a][b] = 0.0;
+    }
+    sm = (sigct[0] + sigct[1] + sigct[2]) * 0.3333333333;
+    if (sm < 1.0) sm = 1.0;
+    if (so->e > 1.0) e0 = so->e;
+    else e0 = 3 * (1 - 2 * poi) * (1 + eps0) * fabs(sm) / zkapa;
+    dlam = e0 * poi / (1.0 + poi) / (1.0 - 2.0 * poi);
+    dmu = e0 * 0.5 / (1.0 + poi);
+    dmu2 = dmu * 2.0;
+    dept[0][0] = dlam + dmu2; dept[1][1] = dlam + dmu2; dept[2][2] = dlam + dmu2;
+    dept[0][1] = dlam; dept[0][2] = dlam; dept[1][0] = dlam;
+    dept[1][2] = dlam; dept[2][0] = dlam; dept[2][1] = dlam;
+    dept[3][3] = dmu; dept[4][4] = dmu; dept[5][5] = dmu;
+    *dlam_o = dlam; *dmu_o = dmu; *sm_o = sm;
+}
+
+/* dpmodel1 (yalf_dil = 0) and dpmodel_bui (yalf_dil from beta):
+ * CPP_8-1-consfactor.cpp:284-448 and 451-615 */
+static void dpmodel(double dept[6][6], const double* sig, const double* deps, const sphgpu_soil* so, double* adps, int bui)
+{
+    double dlam, dmu, sm;
+    elastic_d(dept, sig, so, &dlam, &dmu, &sm);
+    double dmu2 = dmu * 2.0;
+    double fai = atan(tan(so->fai * 0.0174532925166667) / so->fs);
+    double fai_dil = atan(tan(so->beta * 0.0174532925166667) / so->fs);
+    double ci = so->c / so->fs;
+    double sigct[6];
+    for (int a = 0; a < 6; a++) sigct[a] = -sig[a];
+    double dx = sigct[0] - sm, dy = sigct[1] - sm, dz = sigct[2] - sm;
+    double dxy = sigct[3], dyz = sigct[4], dzx = sigct[5];
+    double sjj = 0.5 * (dx * dx + dy * dy + dz * dz) + dxy * dxy + dyz * dyz + dzx * dzx;
+    double sj = sqrt(sjj);
+    double yalf = sin(fai) / sqrt(9.0 + 3.0 * sin(fai) * sin(fai));
+    double ykap = 3.0 * ci * cos(fai) / sqrt(9.0 + 3.0 * sin(fai) * sin(fai));
+    if ((sj - yalf * sm * 3.0 - ykap) >= 0.0) {
+        double f11 = -yalf + dx / sj * 0.5, f22 = -yalf + dy / sj * 0.5, f33 = -yalf + dz / sj * 0.5;
+        double f12 = dxy / sj * 0.5, f23 = dyz / sj * 0.5, f31 = dzx / sj * 0.5;
+        double fkk = f11 + f22 + f33;
+        double yalf_dil = bui ? sin(fai_dil) / sqrt(9.0 + 3.0 * sin(fai_dil) * sin(fai_dil)) : 0.0;
+        double g11 = -yalf_dil + dx / sj * 0.5, g22 = -yalf_dil + dy / sj * 0.5, g33 = -yalf_dil + dz / sj * 0.5;
+        double g12 = dxy / sj * 0.5, g23 = dyz / sj * 0.5, g31 = dzx / sj * 0.5;
+        double hdd = g11 + g22 + g33;
+        double fij = 2.0 * (f11 * g11 + f22 * g22 + f33 * g33) + f12 * g12 + f23 * g23 + f31 * g31;
+        double cc7 = dlam * (fkk * hdd) + dmu * fij + hdd;
+        double d = 1.0 / cc7;
+        double df = dlam * fkk, dg = dlam * hdd;
+        double ramda = (dmu2 * f11 - 3.0 * dlam * yalf) * deps[0]
+            + (dmu2 * f22 - 3.0 * dlam * yalf) * deps[1]
+            + (dmu2 * f33 - 3.0 * dlam * yalf) * deps[2]
+            + dmu * (f12 * deps[3] + f23 * deps[4] + f31 * deps[5]);
+        double ttt = ramda * d;
+        if (ttt < 0.0) {
+            double ww[6] = {dg + dmu2 * g11, dg + dmu2 * g22, dg + dmu2 * g33, dmu * g12, dmu * g23, dmu * g31};
+            double zz[6] = {df + dmu2 * f11, df + dmu2 * f22, df + dmu2 * f33, dmu * f12, dmu * f23, dmu * f31};
+            for (int a = 0; a < 6; a++)
+                for (int b = 0; b < 6; b++) dept[a][b] = dept[a][b] - d * ww[a] * zz[b];
+            adps[0] = ramda * d * f11; adps[1] = ramda * d * f22; adps[2] = ramda * d * f33;
+            adps[3] = ramda * d * f12; adps[4] = ramda * d * f23; adps[5] = ramda * d * f31;
+        }
+    }
+}
+
+/* DPModel_check: stress-scaling return, CPP_8-1-consfactor.cpp:779-819 */
+static void dp_check(double* sig, double* dsig, const sphgpu_soil* so, double dt)
+{
+    double ts[6];
+    double fai = atan(tan(so->fai * 0.0174532925166667) / so->fs);
+    double ci = so->c / so->fs;
+    double sm = (sig[0] + sig[1] + sig[2]) / 3.0;
+    double dx = sig[0] - sm, dy = sig[1] - sm, dz = sig[2] - sm;
+    double sj_2 = 0.5 * (dx * dx + dy * dy + dz * dz) + sig[3] * sig[3] + sig[4] * sig[4] + sig[5] * sig[5];
+    double sj = sqrt(sj_2);
+    for (int a = 0; a < 6; a++) ts[a] = sig[a] + dsig[a] * dt;
+    double i_1 = ts[0] + ts[1] + ts[2];
+    double alpha_fai = sin(fai) / sqrt(9.0 + 3.0 * sin(fai) * sin(fai));
+    double k_c = 3.0 * ci * cos(fai) / sqrt(9.0 + 3.0 * sin(fai) * sin(fai));
+    double rn = (-alpha_fai * i_1 + k_c) / sj;
+    if (rn < 1.0) {
+        ts[0] = rn * (ts[0] - i_1 / 3.0) + i_1 / 3.0;
+        ts[1] = rn * (ts[1] - i_1 / 3.0) + i_1 / 3.0;
+        ts[2] = rn * (ts[2] - i_1 / 3.0) + i_1 / 3.0;
+        ts[3] = rn * ts[3];
+        ts[4] = rn * ts[4];
+        ts[5] = rn * ts[5];
+    }
+    for (int a = 0; a < 6; a++) dsig[a] = (ts[a] - sig[a]) / dt;
+}
+
+/* Jaumann rate terms: CPP_7-2-constitutive.cpp:236-253 (also 297-307) */
+static void jaumann(double* ds, const double* s, const double* w)
+{
+#define WE(a, b) w[(a) * 3 + (b)]
+    ds[0] = ds[0] + (WE(0, 0) * s[0] + WE(0, 1) * s[3] + WE(0, 2) * s[5]) - (s[0] * WE(0, 0) + s[3] * WE(1, 0) + s[5] * WE(2, 0));
+    ds[1] = ds[1] + (WE(1, 0) * s[3] + WE(1, 1) * s[1] + WE(1, 2) * s[4]) - (s[3] * WE(0, 1) + s[1] * WE(1, 1) + s[4] * WE(2, 1));
+    ds[2] = ds[2] + (WE(2, 0) * s[5] + WE(2, 1) * s[4] + WE(2, 2) * s[2]) - (s[5] * WE(0, 2) + s[4] * WE(1, 2) + s[2] * WE(2, 2));
+    ds[3] = ds[3] + (WE(0, 0) * s[3] + WE(0, 1) * s[1] + WE(0, 2) * s[4]) - (s[0] * WE(0, 1) + s[3] * WE(1, 1) + s[5] * WE(2, 1));
+    ds[4] = ds[4] + (WE(1, 0) * s[5] + WE(1, 1) * s[4] + WE(1, 2) * s[2]) - (s[3] * WE(0, 2) + s[1] * WE(1, 2) + s[4] * WE(2, 2));
+    ds[5] = ds[5] + (WE(0, 0) * s[5] + WE(0, 1) * s[4] + WE(0, 2) * s[2]) - (s[0] * WE(0, 2) + s[3] * WE(1, 2) + s[5] * WE(2, 2));
+#undef WE
+}
+
+/* strain_to_stress: CPP_7-2-constitutive.cpp:13-321.  Soil models restated:
+ * elastic (matype%10 = 0, 6), Drucker-Prager (2, with DPModel_check), Bui DP
+ * (5, with DPModel_check). */
+static int strain_to_stress(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    double dt = P->dt;
+    for (int i = 0; i < c->n; i++) {
+        int ti = c->type[i];
+        double* s = &c->sig[i * 6];
+        double* de = &c->deps[i * 6];
+        double* ep = &c->eps[i * 6];
+        if (ti == 1) {
+            double strain_min = c->fl[i].strain_min, viscos1, d[6];
+            double depsmax = (de[0] + de[1] + de[2]) / 3.0;
+            ep[0] = de[0] - depsmax;
+            ep[1] = de[1] - depsmax;
+            ep[2] = de[2] - depsmax;
+            depsmax = 0.666666666666667 * (ep[0] * ep[0] + ep[1] * ep[1]
+                + ep[2] * ep[2] + de[3] * de[3] * 0.25 +
+                de[4] * de[4] * 0.25 + de[5] * de[5] * 0.25);
+            depsmax = sqrt(depsmax);
+            if (c->fl[i].bhtype == 1) {
+                double fai = c->fl[i].fai * 0.0174532925199;
+                double tao = c->pre[i] * tan(fai) + c->fl[i].c;
+                if (depsmax < strain_min) viscos1 = c->fl[i].vis + tao / strain_min;
+                else viscos1 = c->fl[i].vis + tao / depsmax;
+            } else
+                viscos1 = c->fl[i].vis;
+            d[0] = 2.0 * de[0] - 2.0 * (de[0] + de[1] + de[2]) / 3.0;
+            d[1] = 2.0 * de[1] - 2.0 * (de[0] + de[1] + de[2]) / 3.0;
+            d[2] = 2.0 * de[2] - 2.0 * (de[0] + de[1] + de[2]) / 3.0;
+            d[3] = de[3]; d[4] = de[4]; d[5] = de[5];
+            for (int a = 0; a < 6; a++) s[a] = (a < 3) ? -c->pre[i] - viscos1 * d[a] : -viscos1 * d[a];
+        } else if (ti == 3) {
+            double viscos1 = c->fl[i].vis, d[6];
+            d[0] = 2.0 * de[0] - 2.0 * (de[0] + de[1] + de[2]) / 3.0;
+            d[1] = 2.0 * de[1] - 2.0 * (de[0] + de[1] + de[2]) / 3.0;
+            d[2] = 2.0 * de[2] - 2.0 * (de[0] + de[1] + de[2]) / 3.0;
+            d[3] = de[3]; d[4] = de[4]; d[5] = de[5];
+            for (int a = 0; a < 6; a++) s[a] = (a < 3) ? -c->pre[i] - viscos1 * d[a] : -viscos1 * d[a];
+        } else if (ti == 2) {
+            double dept[6][6], adps[6] = {0, 0, 0, 0, 0, 0}, erfs[6] = {0, 0, 0, 0, 0, 0};
+            double dl, dm, sm;
+            double* ds = &c->dsig[i * 6];
+            int mt = c->matype[i] % 10;
+            if (P->flts >= 1) return SPHGPU_E_UNSUPPORTED;
+            if (c->l < P->inip || mt == 0 || mt == 6) {
+                elastic_d(dept, s, &c->so[i], &dl, &dm, &sm);
+            } else if (mt == 2 || mt == 5) {
+                dpmodel(dept, s, de, &c->so[i], adps, mt == 5);
+            } else {
+                return SPHGPU_E_UNSUPPORTED;
+            }
+            for (int a = 0; a < 6; a++)
+                for (int b = 0; b < 6; b++) ds[a] += dept[a][b] * de[b];
+            if (!(c->l < P->inip) && (mt == 2 || mt == 5)) dp_check(s, ds, &c->so[i], dt);
+            jaumann(ds, s, &c->weps[i * 9]);
+            for (int a = 0; a < 6; a++) {
+                c->adps[i * 6 + a] = c->adps[i * 6 + a] + adps[a] * dt;
+                ep[a] = ep[a] + de[a] * dt;
+                s[a] = s[a] + ds[a] * dt + erfs[a];
+            }
+            deq(c, i);
+            shearstrain(c, i);
+            poro_cal(c, i, dt);
+        } else if (ti == 4) {
+            double dept[6][6], e0 = P->structure.e, poi = P->structure.poi;
+            double* ds = &c->dsig[i * 6];
+            for (int a = 0; a < 6; a++) for (int b = 0; b < 6; b++) dept[a][b] = 0.0;
+            double dlam = e0 * poi / (1.0 + poi) / (1.0 - 2.0 * poi);
+            double dmu = e0 * 0.5 / (1.0 + poi), dmu2 = dmu * 2.0;
+            dept[0][0] = dlam + dmu2; dept[1][1] = dlam + dmu2; dept[2][2] = dlam + dmu2;
+            dept[0][1] = dlam; dept[0][2] = dlam; dept[1][0] = dlam;
+            dept[1][2] = dlam; dept[2][0] = dlam; dept[2][1] = dlam;
+            dept[3][3] = dmu; dept[4][4] = dmu; dept[5][5] = dmu;
+            for (int a = 0; a < 6; a++)
+                for (int b = 0; b < 6; b++) ds[a] += dept[a][b] * de[b];
+            jaumann(ds, s, &c->weps[i * 9]);
+            for (int a = 0; a < 6; a++) {
+                ep[a] = ep[a] + de[a] * dt;
+                s[a] = s[a] + ds[a] * dt;
+            }
+            deq(c, i);
+            shearstrain(c, i);
+            poro_cal(c, i, dt);
+        }
+    }
+    return 0;
+}
+
+/* free_surface_check: CPP_7-2-constitutive.cpp:453-506 */
+static void free_surface_check(orc_ctx* c)
+{
+    double tmax = c->P.threshold_max, tmin = c->P.threshold_min, incline = tmax - tmin;
+    for (int i = 0; i < c->n; i++) {
+        double color = 0.0;
+        int ti = c->type[i];
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj), tj = c->type[j];
+            if (ti == tj && (ti != 0 && ti != 7))
+                color = color + c->mass[j] / c->rho[j] * 1.0 * W(i, nj, 3);
+            else if (ti != tj && (ti > 0 && ti < 5)) {
+                if (tj == 0) color = color + c->mass[j] / c->rho[j] * 1.0 * W(i, nj, 3);
+            }
+        }
+        double* s = &c->sig[i * 6];
+        if (ti == 1) {
+            if (color < tmin / 2.0) {
+                for (int k = 0; k < 3; k++) s[k] = -1.0;
+                for (int k = 3; k < 6; k++) s[k] = 0.0;
+            } else if (color >= tmin / 2.0 && color < tmax / 2.0) {
+                double xishu = (2.0 * color - tmin) / incline;
+                for (int k = 0; k < 6; k++) s[k] = xishu * s[k];
+            }
+        } else if (ti == 2) {
+            if (color < tmin) {
+                for (int k = 0; k < 3; k++) s[k] = -1.0;
+                for (int k = 3; k < 6; k++) s[k] = 0.0;
+            } else if (color >= tmin && color < tmax) {
+                double xishu = (color - tmin) / incline * 1.0;
+                for (int k = 0; k < 6; k++) s[k] = xishu * s[k];
+            }
+            stress_adjust(c, i);
+            deq(c, i);
+        }
+    }
+}
+
+/* eejcb: Jacobi eigen-solver, CPP_7-1-strain.cpp:341-437 */
+static int eejcb(double a[], int n, double v[], double eps, int jt)
+{
+    int i, j, p = 0, q = 0, u, w, t, s, l = 1;
+    double fm, cn, sn, omega, x, y, d;
+    for (i = 0; i <= n - 1; i++) {
+        v[i * n + i] = 1.0;
+        for (j = 0; j <= n - 1; j++)
+            if (i != j) v[i * n + j] = 0.0;
+    }
+    while (1) {
+        fm = 0.0;
+        for (i = 0; i <= n - 1; i++)
+            for (j = 0; j <= n - 1; j++) {
+                d = fabs(a[i * n + j]);
+                if ((i != j) && (d > fm)) { fm = d; p = i; q = j; }
+            }
+        if (fm < eps) return 1;
+        if (l > jt) return -1;
+        l = l + 1;
+        u = p * n + q; w = p * n + p; t = q * n + p; s = q * n + q;
+        x = -a[u];
+        y = (a[s] - a[w]) / 2.0;
+        omega = x / sqrt(x * x + y * y);
+        if (y < 0.0) omega = -omega;
+        sn = 1.0 + sqrt(1.0 - omega * omega);
+        sn = omega / sqrt(2.0 * sn);
+        cn = sqrt(1.0 - sn * sn);
+        fm = a[w];
+        a[w] = fm * cn * cn + a[s] * sn * sn + a[u] * omega;
+        a[s] = fm * sn * sn + a[s] * cn * cn - a[u] * omega;
+        a[u] = 0.0;
+        a[t] = 0.0;
+        for (j = 0; j <= n - 1; j++)
+            if ((j != p) && (j != q)) {
+                u = p * n + j; w = q * n + j;
+                fm = a[u];
+                a[u] = fm * cn + a[w] * sn;
+                a[w] = -fm * sn + a[w] * cn;
+            }
+        for (i = 0; i <= n - 1; i++)
+            if ((i != p) && (i != q)) {
+                u = i * n + p; w = i * n + q;
+                fm = a[u];
+                a[u] = fm * cn + a[w] * sn;
+                a[w] = -fm * sn + a[w] * cn;
+            }
+        for (i = 0; i <= n - 1; i++) {
+            u = i * n + p; w = i * n + q;
+            fm = v[u];
+            v[u] = fm * cn + v[w] * sn;
+            v[w] = -fm * sn + v[w] * cn;
+        }
+    }
+    return 1;
+}
+
+/* Stress_eigValue: CPP_7-1-strain.cpp:283-332 */
+static void stress_eig(orc_ctx* c)
+{
+    for (int i = 0; i < c->n; i++) {
+        double st[9], ev[9];
+        const double* s = &c->sig[i * 6];
+        for (int k = 0; k < 9; k++) ev[k] = 0.0;
+        st[0] = s[0]; st[1] = s[3]; st[2] = s[5];
+        st[3] = s[3]; st[4] = s[1]; st[5] = s[4];
+        st[6] = s[5]; st[7] = s[4]; st[8] = s[2];
+        eejcb(st, 3, ev, 0.001, 7);
+        for (int k = 0; k < 3; k++) c->strep[i * 3 + k] = st[k * 3 + k];
+        for (int k = 0; k < 3; k++) {
+            c->beta_ts[i * 9 + k * 3 + 0] = ev[k * 3];
+            c->beta_ts[i * 9 + k * 3 + 1] = ev[k * 3 + 1];
+            c->beta_ts[i * 9 + k * 3 + 2] = ev[k * 3 + 2];
+            c->beta[i * 9 + 0 * 3 + k] = ev[k * 3];
+            c->beta[i * 9 + 1 * 3 + k] = ev[k * 3 + 1];
+            c->beta[i * 9 + 2 * 3 + k] = ev[k * 3 + 2];
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+/* momentum: CPP_9-4-derivation_stress.cpp                                   */
+
+/* one pair of the symmetric stress-divergence sum, the 9 lines shared by
+ * fluid_acceleration_water/air (:55-65) and the soil/structure forms */
+static void stress_pair(double tu[3][3], double mj, const double* aj, const double* ai,
+                        double rj, double ri, const double* w, double sgn)
+{
+    if (sgn > 0) {
+        tu[0][0] = tu[0][0] + mj * (aj[0] / rj / rj + ai[0] / ri / ri) * w[0];
+        tu[0][1] = tu[0][1] + mj * (aj[3] / rj / rj + ai[3] / ri / ri) * w[1];
+        tu[0][2] = tu[0][2] + mj * (aj[5] / rj / rj + ai[5] / ri / ri) * w[2];
+        tu[1][0] = tu[1][0] + mj * (aj[3] / rj / rj + ai[3] / ri / ri) * w[0];
+        tu[1][1] = tu[1][1] + mj * (aj[1] / rj / rj + ai[1] / ri / ri) * w[1];
+        tu[1][2] = tu[1][2] + mj * (aj[4] / rj / rj + ai[4] / ri / ri) * w[2];
+        tu[2][0] = tu[2][0] + mj * (aj[5] / rj / rj + ai[5] / ri / ri) * w[0];
+        tu[2][1] = tu[2][1] + mj * (aj[4] / rj / rj + ai[4] / ri / ri) * w[1];
+        tu[2][2] = tu[2][2] + mj * (aj[2] / rj / rj + ai[2] / ri / ri) * w[2];
+    } else {
+        tu[0][0] = tu[0][0] + mj * (aj[0] / rj / rj - ai[0] / ri / ri) * w[0];
+        tu[0][1] = tu[0][1] + mj * (aj[3] / rj / rj - ai[3] / ri / ri) * w[1];
+        tu[0][2] = tu[0][2] + mj * (aj[5] / rj / rj - ai[5] / ri / ri) * w[2];
+        tu[1][0] = tu[1][0] + mj * (aj[3] / rj / rj - ai[3] / ri / ri) * w[0];
+        tu[1][1] = tu[1][1] + mj * (aj[1] / rj / rj - ai[1] / ri / ri) * w[1];
+        tu[1][2] = tu[1][2] + mj * (aj[4] / rj / rj - ai[4] / ri / ri) * w[2];
+        tu[2][0] = tu[2][0] + mj * (aj[5] / rj / rj - ai[5] / ri / ri) * w[0];
+        tu[2][1] = tu[2][1] + mj * (aj[4] / rj / rj - ai[4] / ri / ri) * w[1];
+        tu[2][2] = tu[2][2] + mj * (aj[2] / rj / rj - ai[2] / ri / ri) * w[2];
+    }
+}
+
+/* fluid_acceleration_water / _air and the minor forms: :12-351 */
+static void fluid_acceleration(orc_ctx* c, int me, int other, int minor)
+{
+    double g[3] = {c->P.gx, c->P.gy, c->P.gz};
+    for (int i = 0; i < c->n; i++) {
+        if (c->type[i] != me) continue;
+        double poro = c->fl[i].porosity, tu[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int k = 0; k < 3; k++) c->ax[i * 3 + k] = g[k];
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj);
+            if (c->type[i] == c->type[j] || c->type[j] == other) {
+                double ai[6], aj[6];
+                for (int k = 0; k < 6; k++) { ai[k] = poro * c->sig[i * 6 + k]; aj[k] = poro * c->sig[j * 6 + k]; }
+                stress_pair(tu, c->mass[j], aj, ai, c->rho[j], c->rho[i], &W(i, nj, 0), minor ? -1.0 : 1.0);
+            }
+        }
+        c->ax[i * 3 + 0] += tu[0][0] + tu[0][1] + tu[0][2];
+        c->ax[i * 3 + 1] += tu[1][0] + tu[1][1] + tu[1][2];
+        c->ax[i * 3 + 2] += tu[2][0] + tu[2][1] + tu[2][2];
+    }
+}
+
+/* soil_acceleration_noreg: :354-428 */
+static void soil_acceleration(orc_ctx* c)
+{
+    double g[3] = {c->P.gx, c->P.gy, c->P.gz};
+    for (int i = 0; i < c->n; i++) {
+        if (c->type[i] != 2) continue;
+        double poro = c->so[i].porosity, tu[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int k = 0; k < 3; k++) c->ax[i * 3 + k] = g[k];
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj);
+            if (c->type[i] != c->type[j]) continue;
+            double satu = c->satu[j], prei[3], prej[3];
+            const double* w = &W(i, nj, 0);
+            for (int k = 0; k < 3; k++) {
+                prei[k] = (1 - poro) * (-satu * c->prew[i] + (1 - satu) * c->prea[i]);
+                prej[k] = (1 - poro) * (-satu * c->prew[j] + (1 - satu) * c->prea[j]);
+            }
+            stress_pair(tu, c->mass[j], &c->sig[j * 6], &c->sig[i * 6], c->rho[j], c->rho[i], w, 1.0);
+            double mj = c->mass[j], rj = c->rho[j], di = c->so[i].dens;
+            tu[0][0] = tu[0][0] + mj * (prej[0] / rj / rj + prei[0] / di / di) * w[0];
+            tu[1][1] = tu[1][1] + mj * (prej[1] / rj / rj + prei[1] / di / di) * w[1];
+            tu[2][2] = tu[2][2] + mj * (prej[2] / rj / rj + prei[2] / di / di) * w[2];
+        }
+        c->ax[i * 3 + 0] += tu[0][0] + tu[0][1] + tu[0][2];
+        c->ax[i * 3 + 1] += tu[1][0] + tu[1][1] + tu[1][2];
+        c->ax[i * 3 + 2] += tu[2][0] + tu[2][1] + tu[2][2];
+    }
+}
+
+/* structure_acceleration_noreg: :431-505 */
+static void structure_acceleration(orc_ctx* c)
+{
+    double g[3] = {c->P.gx, c->P.gy, c->P.gz};
+    for (int i = 0; i < c->n; i++) {
+        if (c->type[i] != 4) continue;
+        double tu[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int k = 0; k < 3; k++) c->ax[i * 3 + k] = g[k];
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj);
+            if (c->type[i] != c->type[j]) continue;
+            double satu = c->satu[j], prei[3], prej[3];
+            const double* w = &W(i, nj, 0);
+            for (int k = 0; k < 3; k++) {
+                prei[k] = -satu * c->prew[i] + (1 - satu) * c->prea[i];
+                prej[k] = -satu * c->prew[j] + (1 - satu) * c->prea[j];
+            }
+            stress_pair(tu, c->mass[j], &c->sig[j * 6], &c->sig[i * 6], c->rho[j], c->rho[i], w, 1.0);
+            double mj = c->mass[j], rj = c->rho[j], ri = c->rho[i];
+            tu[0][0] = tu[0][0] + mj * (prej[0] / rj / rj - prei[0] / ri / ri) * w[0];
+            tu[1][1] = tu[1][1] + mj * (prej[1] / rj / rj - prei[1] / ri / ri) * w[1];
+            tu[2][2] = tu[2][2] + mj * (prej[2] / rj / rj - prei[2] / ri / ri) * w[2];
+        }
+        c->ax[i * 3 + 0] += tu[0][0] + tu[0][1] + tu[0][2];
+        c->ax[i * 3 + 1] += tu[1][0] + tu[1][1] + tu[1][2];
+        c->ax[i * 3 + 2] += tu[2][0] + tu[2][1] + tu[2][2];
+    }
+}
+
+/* artificial_viscosity: CPP_9-3-artificialvis.cpp:12-99 */
+static void artificial_viscosity(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    int ndim = P->ndim;
+    for (int i = 0; i < c->n; i++) {
+        double tu[3] = {0, 0, 0};
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj), k;
+            if (!(c->type[i] == c->type[j] && c->type[i] != 7)) continue;
+            double a = 0.0, b = 0.0, cc = 0.0, inprod = 0.0, dst = 0.0, myu, paix, dvx[3], dx[3];
+            for (k = 0; k < ndim; k++) {
+                dvx[k] = c->vxp[i * 3 + k] - c->vxp[j * 3 + k];
+                dx[k] = c->xp[i * 3 + k] - c->xp[j * 3 + k];
+                dst = dst + dx[k] * dx[k];
+                inprod = inprod + dvx[k] * dx[k];
+            }
+            double hl = (c->hl[j] + c->hl[i]) * 0.5;
+            double rou = (c->rho[j] + c->rho[i]) * 0.5;
+            if (c->type[i] == 1) { cc = c->fl[i].vpu; a = P->art_vis[0][0]; b = P->art_vis[0][1]; }
+            if (c->type[i] == 2) { cc = c->so[i].vpu; a = P->art_vis[1][0]; b = P->art_vis[1][1]; }
+            if (c->type[i] == 3) { cc = c->fl[i].vpu; a = P->art_vis[2][0]; b = P->art_vis[2][1]; }
+            if (inprod < 0.0) {
+                dst = sqrt(dst);
+                myu = hl * inprod / (dst * dst + 0.01 * hl * hl);
+                paix = (-a * cc * myu + b * myu * myu) / rou;
+            } else
+                paix = 0.0;
+            for (k = 0; k < ndim; k++) tu[k] = tu[k] + c->mass[j] * paix * W(i, nj, k);
+        }
+        if (c->type[i] != 7)
+            for (int k = 0; k < ndim; k++) c->ax[i * 3 + k] = c->ax[i * 3 + k] - tu[k];
+    }
+}
+
+/* boundary_moving_stress_effect: CPP_9-4-derivation_stress.cpp:631-721 */
+static void boundary_moving_stress_effect(orc_ctx* c)
+{
+    for (int i = 0; i < c->n; i++) {
+        int ti = c->type[i];
+        if (ti == 0 || ti == 7) continue;
+        double tu[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj);
+            if (c->type[j] != 0) continue;
+            double a[6] = {0, 0, 0, 0, 0, 0};
+            const double* s = &c->sig[i * 6];
+            if (ti == 1 || ti == 3) {
+                for (int k = 0; k < 6; k++) a[k] = s[k];
+            } else if (ti == 2 || ti == 4) {
+                double satu = c->satu[i];
+                a[0] = s[0] - satu * c->prew[i] + (1 - satu) * c->prea[i];
+                a[1] = s[1] - satu * c->prew[i] + (1 - satu) * c->prea[i];
+                a[2] = s[2] - satu * c->prew[i] + (1 - satu) * c->prea[i];
+                a[3] = s[3]; a[4] = s[4]; a[5] = s[5];
+            }
+            stress_pair(tu, c->mass[j], a, a, c->rho[j], c->rho[i], &W(i, nj, 0), 1.0);
+        }
+        c->ax[i * 3 + 0] += tu[0][0] + tu[0][1] + tu[0][2];
+        c->ax[i * 3 + 1] += tu[1][0] + tu[1][1] + tu[1][2];
+        c->ax[i * 3 + 2] += tu[2][0] + tu[2][1] + tu[2][2];
+    }
+}
+
+/* interact1: Darcy drag, CPP_10-interact1.cpp:15-110 */
+static void interact1(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    int ndim = P->ndim;
+    double xishu = P->interc, dt = P->dt;
+    double g_acc = sqrt(P->gx * P->gx + P->gy * P->gy + P->gz * P->gz);
+    for (int i = 0; i < c->n; i++) {
+        double tu[3] = {0, 0, 0};
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj), k;
+            if (c->type[i] == c->type[j]) continue;
+            double inprod = 0.0, dx[3], dvx[3];
+            for (k = 0; k < ndim; k++) {
+                dx[k] = c->xp[i * 3 + k] - c->xp[j * 3 + k];
+                dvx[k] = c->vxp[i * 3 + k] - c->vxp[j * 3 + k];
+                inprod = inprod + dx[k] * dvx[k];
+            }
+            if (!(inprod < 0)) continue;
+            int ti = c->type[i], tj = c->type[j];
+            double w3 = W(i, nj, 3);
+            if (ti == 2 && tj == 1) {
+                for (k = 0; k < ndim; k++)
+                    tu[k] = tu[k] + c->satu[i] * c->satu[i] * c->porosity[i] * c->porosity[i] * c->fl[j].dens * g_acc * dvx[k] / c->cop[i] * c->mass[j] / c->rho[j] * w3;
+            } else if (ti == 1 && tj == 2) {
+                for (k = 0; k < ndim; k++)
+                    tu[k] = tu[k] + c->satu[j] * c->satu[j] * c->porosity[j] * c->porosity[j] * c->fl[i].dens * g_acc * dvx[k] / c->cop[j] * c->mass[j] / c->rho[j] * w3;
+            } else if (ti == 2 && tj == 3) {
+                for (k = 0; k < ndim; k++)
+                    tu[k] = tu[k] + (1 - c->satu[i]) * (1 - c->satu[i]) * c->porosity[i] * c->porosity[i] * c->fl[j].dens * g_acc * dvx[k] * 2000 * c->mass[j] / c->rho[j] * w3;
+            } else if (ti == 3 && tj == 2) {
+                for (k = 0; k < ndim; k++)
+                    tu[k] = tu[k] + (1 - c->satu[j]) * (1 - c->satu[j]) * c->porosity[j] * c->porosity[j] * c->fl[i].dens * g_acc * dvx[k] * 2000 * c->mass[j] / c->rho[j] * w3;
+            }
+        }
+        if (c->type[i] != 0 && c->type[i] != 7) {
+            for (int k = 0; k < ndim; k++) {
+                double* ax = &c->ax[i * 3 + k];
+                double axp = c->axp[i * 3 + k], vxp = c->vxp[i * 3 + k];
+                c->interf[i * 3 + k] = tu[k];
+                double vx1 = vxp + 0.5 * (axp + *ax) * dt;
+                double vx2 = vxp + 0.5 * (axp + *ax - c->interf[i * 3 + k] * xishu / c->rho[i]) * dt;
+                if (vx1 * vx2 <= 0.0) {
+                    c->interf[i * 3 + k] = 0.0;
+                    *ax = -2.0 * vxp / dt - axp;
+                } else
+                    *ax -= c->interf[i * 3 + k] * xishu / c->rho[i];
+            }
+        }
+    }
+}
+
+/* veocity_update: CPP_11-xsph.cpp:11-142 */
+static void velocity_update(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    int ndim = P->ndim, l = c->l, inip = P->inip;
+    double dt = P->dt;
+    for (int i = 0; i < c->n; i++) {
+        int ti = c->type[i], mt = c->matype[i];
+        double *vx = &c->vx[i * 3], *vxp = &c->vxp[i * 3], *ax = &c->ax[i * 3], *axp = &c->axp[i * 3];
+        double *itf = &c->interf[i * 3], *itss = &c->interfss[i * 3];
+        if (P->if_move == 0) {
+            if (ti == 0 && mt < 2) {
+                for (int k = 0; k < ndim; k++) { itf[k] = 0.0; double ath = (itf[k] + itf[k]) * 0.5; itss[k] = itss[k] + ath * dt; }
+            } else if (ti == 0 && mt == 3) {
+                for (int k = 0; k < ndim; k++) { double ath = (itf[k] + itf[k]) * 0.5; itss[k] = itss[k] + ath * dt; }
+            } else if (ti == 0 && mt == 5 && P->flv == 1) {
+                for (int k = 0; k < ndim; k++) { double ath = (itf[k] + itf[k]) * 0.5; itss[k] = itss[k] + ath * dt; }
+            } else if (ti != 0) {
+                for (int k = 0; k < ndim; k++) { double ath = (axp[k] + ax[k]) * 0.5; vx[k] = vxp[k] + ath * dt; }
+            }
+        } else if (P->if_move == 1) {
+            if ((ti == 0 && mt == 2) && l > inip) {
+                for (int k = 0; k < ndim; k++) itss[k] = P->move_vx[k];
+            } else if (ti == 0) {
+                for (int k = 0; k < ndim; k++) itss[k] = 0.0;
+            } else {
+                for (int k = 0; k < ndim; k++) { double ath = (axp[k] + ax[k]) * 0.5; vx[k] = vxp[k] + ath * dt; }
+            }
+        } else if (P->if_move == 2 || P->if_move == 3) {
+            int tmove = (P->if_move == 2) ? 2 : 4;
+            if ((ti == tmove && c->etype[i] == 5) && l > inip) {
+                for (int k = 0; k < ndim; k++) { axp[k] = 0.0; vxp[k] = P->move_vx[k]; vx[k] = P->move_vx[k]; ax[k] = 0.0; }
+            }
+            for (int k = 0; k < ndim; k++) { double ath = (axp[k] + ax[k]) * 0.5; vx[k] = vxp[k] + ath * dt; }
+        }
+    }
+}
+
+/* xsph: CPP_11-xsph.cpp:145-256 (flbndy 1 virtual-velocity form) */
+static void xsph(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    int ndim = P->ndim, bndytype = P->flbndy;
+    for (int i = 0; i < c->n; i++) {
+        double tu[3] = {0, 0, 0}, down = 0.0, xishu = 0.0, vxj[3];
+        int ti = c->type[i];
+        for (int k = 0; k < ndim; k++) c->vx_temp[i * 3 + k] = 0.0;
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj), tj = c->type[j], k;
+            double w3 = W(i, nj, 3);
+            if (ti == tj && (ti != 0 && ti != 7)) {
+                if (ti == 1) xishu = P->xsph[0];
+                else if (ti == 2) xishu = P->xsph[1];
+                else if (ti == 3) xishu = P->xsph[2];
+                else if (ti == 4) xishu = P->xsph[1];
+                for (k = 0; k < ndim; k++)
+                    tu[k] = tu[k] + xishu * c->mass[j] * (c->vx[j * 3 + k] - c->vx[i * 3 + k]) * w3 / c->rho[j];
+                down = down + c->mass[j] * w3 / c->rho[j];
+            } else if ((ti == 1 || ti == 2 || ti == 3 || ti == 4) && tj == 0) {
+                vxj[0] = vxj[1] = vxj[2] = 0.0;
+                if (bndytype == 1) { vxj[0] = c->vx[i * 3]; vxj[1] = c->vx[i * 3 + 1]; vxj[2] = c->vx[i * 3 + 2]; }
+                (void)vxj;   /* computed and unused by the reference (:187-233) */
+                if (ti == 1) xishu = 0.006;
+                else if (ti == 2) xishu = P->xsph[1] / 5.0;
+                else if (ti == 3) xishu = 0.006;
+                else if (ti == 4) xishu = P->xsph[1] / 5.0;
+                for (k = 0; k < ndim; k++)
+                    tu[k] = tu[k] + xishu * c->mass[j] * (c->vx[j * 3 + k] - c->vx[i * 3 + k]) * w3 / c->rho[j];
+                down = down + c->mass[j] * w3 / c->rho[j];
+            }
+        }
+        if (ti != 0 && ti != 7) {
+            if (fabs(down) > 1.0e-7 && (ti == 2 || ti == 4))
+                for (int k = 0; k < ndim; k++) c->vx_temp[i * 3 + k] = c->vx[i * 3 + k] + tu[k] / down;
+            else
+                for (int k = 0; k < ndim; k++) c->vx_temp[i * 3 + k] = c->vx[i * 3 + k] + tu[k];
+        }
+    }
+    for (int i = 0; i < c->n; i++)
+        if (c->type[i] != 0 && c->type[i] != 7)
+            for (int k = 0; k < ndim; k++) c->vx[i * 3 + k] = c->vx_temp[i * 3 + k];
+}
+
+/* tmboundary: CPP_13-boundary.cpp:125-177 */
+static void tmboundary(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    int ndim = P->ndim;
+    double dr = P->dr, a = 0.30, b = 0.30;
+    for (int i = 0; i < c->n; i++) {
+        if (c->type[i] == 0 || c->type[i] == 7) continue;
+        double tu[3] = {0, 0, 0};
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj), k;
+            if (c->type[j] != 0) continue;
+            double inprod = 0.0, dst = 0.0;
+            for (k = 0; k < ndim; k++) {
+                inprod = inprod + (c->vx[i * 3 + k] - c->interfss[j * 3 + k]) * (c->xp[i * 3 + k] - c->xp[j * 3 + k]);
+                dst = dst + (c->xp[i * 3 + k] - c->xp[j * 3 + k]) * (c->xp[i * 3 + k] - c->xp[j * 3 + k]);
+            }
+            if (inprod < 0.0) {
+                dst = sqrt(dst);
+                double db = a * dr;
+                double beta = 1 + db / (dst - b * dr);
+                beta = fmin(1.5, beta);
+                for (k = 0; k < ndim; k++)
+                    tu[k] = tu[k] + (1 - beta) * (c->xp[i * 3 + k] - c->xp[j * 3 + k]) * inprod / dst / dst;
+            }
+        }
+        for (int k = 0; k < ndim; k++) c->vx[i * 3 + k] = c->vx[i * 3 + k] + tu[k];
+    }
+}
+
+/* check_domain: CPP_13-boundary.cpp:20-68, in the sequential order (vbx is
+ * taken from the first wall particle with matype > 2 and applies to the
+ * particles after it) */
+static void check_domain(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    double bmax[3] = {P->xmax, P->ymax, P->zmax}, bmin[3] = {P->xmin, P->ymin, P->zmin};
+    double vbx[3] = {0, 0, 0}, dr = P->dr;
+    int flag = 0, dim = P->ndim;
+    for (int i = 0; i < c->n; i++) {
+        int ti = c->type[i];
+        if (ti != 0 && ti != 7) {
+            const double* xp = &c->xp[i * 3];
+            int hit = 0;
+            if (xp[0] - bmax[0] >= -0.5 * dr) hit = 1;
+            if (xp[0] - bmin[0] <= 0.5 * dr) hit = 1;
+            if (xp[1] - bmax[1] >= -0.5 * dr) hit = 1;
+            if (xp[1] - bmin[1] <= 0.5 * dr) hit = 1;
+            if (xp[2] - bmax[2] >= -0.5 * dr && dim == 3) hit = 1;
+            if (xp[2] - bmin[2] <= 0.5 * dr && dim == 3) hit = 1;
+            if (hit) for (int k = 0; k < 3; k++) c->vx[i * 3 + k] = vbx[k];
+        } else if (ti == 0 && c->matype[i] > 2 && flag == 0) {
+            flag = 1;
+            for (int k = 0; k < 3; k++) vbx[k] = c->interfss[i * 3 + k];
+        }
+    }
+}
+
+/* update: CPP_12-1-update.cpp:11-55 */
+static void update(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    int ndim = P->ndim, loop = c->l - P->inip;
+    double dt = P->dt;
+    for (int i = 0; i < c->n; i++) {
+        for (int k = 0; k < ndim; k++) {
+            if (c->type[i] != 0) {
+                double s = (c->vx[i * 3 + k] + c->vxp[i * 3 + k]) * dt * 0.5;
+                c->x[i * 3 + k] = c->xp[i * 3 + k] + s;
+                if (loop == 0) c->ux[i * 3 + k] = 0.0;
+                else c->ux[i * 3 + k] = c->ux[i * 3 + k] + (c->vx[i * 3 + k] + c->vxp[i * 3 + k]) * dt * 0.5;
+                c->xp[i * 3 + k] = c->x[i * 3 + k];
+                c->vxp[i * 3 + k] = c->vx[i * 3 + k];
+                c->axp[i * 3 + k] = c->ax[i * 3 + k];
+                c->rhop[i] = c->rho[i];
+            } else {
+                int mt = c->matype[i];
+                if (mt == 2 || mt == 3 || mt == 4 || mt == 5) {
+                    c->x[i * 3 + k] = c->xp[i * 3 + k] + (c->interfss[i * 3 + k] + c->interfss[i * 3 + k]) * dt * 0.5;
+                    c->ux[i * 3 + k] = c->ux[i * 3 + k] + (c->interfss[i * 3 + k] + c->interfss[i * 3 + k]) * dt * 0.5;
+                    c->xp[i * 3 + k] = c->x[i * 3 + k];
+                    c->rhop[i] = c->rho[i];
+                    c->prep[i] = c->pre[i];
+                }
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+
+int orc_nnps(orc_ctx* c, int* ninflu, int* influ, double* wij)
+{
+    int err = parttocell(c);
+    if (err) return err;
+    err = partisearching(c);
+    if (ninflu) memcpy(ninflu, c->ninflu, sizeof(int) * c->n);
+    if (influ) memcpy(influ, c->influ, sizeof(int) * (size_t)c->n * NB);
+    if (wij) memcpy(wij, c->wij, sizeof(double) * (size_t)c->n * NB * 4);
+    return err;
+}
+
+static int check_supported(const sphgpu_params* P)
+{
+    if (P->flbndy != 1) return SPHGPU_E_UNSUPPORTED;
+    if (P->flknl > 2) return SPHGPU_E_UNSUPPORTED;
+    if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
+    if (P->art_stre_coe > 0.0) return SPHGPU_E_UNSUPPORTED;
+    if (P->fli > 1 || P->ss_type != 0) return SPHGPU_E_UNSUPPORTED;
+    return 0;
+}
+
+/* one pass of the main loop body, CPP_1-SPHLoops.cpp:523-753 */
+int orc_step(orc_ctx* c, int nsteps)
+{
+    const sphgpu_params* P = &c->P;
+    int err = check_supported(P);
+    if (err) return err;
+    for (int s = 0; s < nsteps; s++) {
+        c->t = c->t + P->dt;
+        err = parttocell(c);
+        if (err) return err;
+        err = partisearching(c);
+        if (err) return err;
+        density(c);
+        strain_noreg(c);
+        if (c->l % P->step_regu == 0) regularise(c, c->eps);
+        if (P->fli == 1) cal_permeability(c);
+        eos(c);
+        err = strain_to_stress(c);
+        if (err) return err;
+        if (c->l % P->step_regu == 0) regularise(c, c->sig);
+        free_surface_check(c);
+        stress_eig(c);
+        fluid_acceleration(c, 1, 3, P->water_acc_type != 0);
+        fluid_acceleration(c, 3, 1, P->air_acc_type != 0);
+        soil_acceleration(c);
+        structure_acceleration(c);
+        artificial_viscosity(c);
+        boundary_moving_stress_effect(c);    /* flv == 0, flbndy 1 */
+        if (P->fli == 1) interact1(c);
+        velocity_update(c);
+        if (P->if_move != 2) xsph(c);
+        tmboundary(c);                        /* flbndy == 1 */
+        check_domain(c);
+        update(c);
+        c->l++;
+    }
+    return 0;
+}

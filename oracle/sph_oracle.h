@@ -1,0 +1,50 @@
+/*
+ * sph_oracle.h -- CPU restatement of the reference's per-step particle loop.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker for the GPU engine:
+ * tests/, __graft_entry__.smoke() and the cpu_baseline leg of bench.py may
+ * load it; the engine (libsphgpu) never links or calls it.
+ *
+ * It restates, in plain C over structure-of-arrays state, the functions of
+ * wodexinxin2015/MultiPhase-SPH-Solver that SPH_Calculation calls each step
+ * (CPP_1-SPHLoops.cpp:523-753), each function citing the reference
+ * file:line it follows.  It is single-threaded and deterministic.  Two
+ * orders are available for the passes the reference runs in place
+ * (Shepard density filter, stress/strain regularisation):
+ *   ORC_INPLACE  - sequential in-place update in particle order, which is
+ *                  what the reference computes when run with one thread;
+ *   ORC_JACOBI   - every particle reads the values from before the pass,
+ *                  which is the order the GPU engine implements.
+ * The restatement is pinned against the reference itself (compiled here
+ * from its own sources into oracle/_ref) by tests/test_oracle_vs_reference.py.
+ */
+#ifndef SPH_ORACLE_H
+#define SPH_ORACLE_H
+
+#include "../include/sphgpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_JACOBI  0
+#define ORC_INPLACE 1
+
+typedef struct orc_ctx orc_ctx;
+
+orc_ctx* orc_create(const sphgpu_params* p);
+void     orc_destroy(orc_ctx* c);
+int      orc_set_field(orc_ctx* c, const char* name, const void* host, size_t count);
+int      orc_get_field(orc_ctx* c, const char* name, void* host, size_t count);
+int      orc_set_materials(orc_ctx* c, const sphgpu_fluid* fluid, const sphgpu_soil* soil, int n);
+void     orc_set_mode(orc_ctx* c, int mode);
+int      orc_get_step(const orc_ctx* c);
+/* parttocell + partisearching for the current step; neighbour lists copied
+ * out as in Par_Cell (influ 1-based, 100 slots per particle). */
+int      orc_nnps(orc_ctx* c, int* ninflu, int* influ, double* wij);
+int      orc_step(orc_ctx* c, int nsteps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

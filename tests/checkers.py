@@ -1,0 +1,199 @@
+"""ctypes bindings of the two checkers (test infrastructure only):
+
+* ``Oracle``    -- oracle/liboracle.so, the C restatement of the reference's
+                   step loop (sph_oracle.c);
+* ``Reference`` -- oracle/_ref/libsphref.so, the reference solver compiled
+                   from its own sources with ref_driver.cpp.  Present only
+                   where it was built (from the reference tree).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(REPO, "multiphase-sph-solver_b200")
+if PKG not in sys.path:
+    sys.path.insert(0, PKG)
+
+import sphgpu  # noqa: E402
+from sphgpu import FIELDS, INT_FIELDS, Params  # noqa: E402
+
+ORACLE_SO = os.path.join(REPO, "oracle", "liboracle.so")
+REF_SO = os.path.join(REPO, "oracle", "_ref", "libsphref.so")
+
+ORC_JACOBI, ORC_INPLACE = 0, 1
+
+ORACLE_FIELDS = dict(FIELDS)
+ORACLE_FIELDS.update({"divx": 9, "deps": 6, "dsig": 6, "weps": 9, "dsatu": 1, "suct": 1,
+                      "cd": 1, "beta": 9, "beta_ts": 9})
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+_olib = None
+
+
+def oracle_lib():
+    global _olib
+    if _olib is None:
+        if not os.path.exists(ORACLE_SO):
+            raise FileNotFoundError(f"{ORACLE_SO} missing: run make -C oracle")
+        lib = C.CDLL(ORACLE_SO)
+        lib.orc_create.restype = C.c_void_p
+        lib.orc_create.argtypes = [C.POINTER(Params)]
+        lib.orc_destroy.argtypes = [C.c_void_p]
+        lib.orc_set_field.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t]
+        lib.orc_get_field.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t]
+        lib.orc_set_materials.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        lib.orc_set_mode.argtypes = [C.c_void_p, C.c_int]
+        lib.orc_get_step.argtypes = [C.c_void_p]
+        lib.orc_nnps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.orc_step.argtypes = [C.c_void_p, C.c_int]
+        _olib = lib
+    return _olib
+
+
+class Oracle:
+    def __init__(self, params: dict | Params, mode: int = ORC_JACOBI):
+        self.lib = oracle_lib()
+        self.params = params if isinstance(params, Params) else sphgpu.params_from_dict(params)
+        self.h = C.c_void_p(self.lib.orc_create(C.byref(self.params)))
+        if not self.h:
+            raise RuntimeError("orc_create failed")
+        self.n = int(self.params.ntotal)
+        self.lib.orc_set_mode(self.h, mode)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.orc_destroy(self.h)
+            self.h = None
+
+    def set_field(self, name, values):
+        nc = ORACLE_FIELDS[name]
+        dt = np.int32 if name in INT_FIELDS else np.float64
+        a = np.ascontiguousarray(np.asarray(values, dtype=dt).reshape(self.n * nc))
+        assert self.lib.orc_set_field(self.h, name.encode(), _ptr(a), a.size) == 0, name
+
+    def get_field(self, name):
+        nc = ORACLE_FIELDS[name]
+        dt = np.int32 if name in INT_FIELDS else np.float64
+        a = np.empty(self.n * nc, dtype=dt)
+        assert self.lib.orc_get_field(self.h, name.encode(), _ptr(a), a.size) == 0, name
+        return a if nc == 1 else a.reshape(self.n, nc)
+
+    def set_materials(self, fluid, soil):
+        fp = _ptr(np.ascontiguousarray(fluid)) if fluid is not None else None
+        sp = _ptr(np.ascontiguousarray(soil)) if soil is not None else None
+        assert self.lib.orc_set_materials(self.h, fp, sp, self.n) == 0
+
+    def load_state(self, fields, fluid=None, soil=None):
+        for name, v in fields.items():
+            if name in ORACLE_FIELDS:
+                self.set_field(name, v)
+        self.set_materials(fluid, soil)
+
+    def step(self, nsteps=1):
+        return self.lib.orc_step(self.h, int(nsteps))
+
+    def nnps(self, with_wij=False):
+        ninflu = np.zeros(self.n, np.int32)
+        influ = np.zeros(self.n * 100, np.int32)
+        wij = np.zeros(self.n * 400) if with_wij else None
+        err = self.lib.orc_nnps(self.h, _ptr(ninflu), _ptr(influ), _ptr(wij) if with_wij else None)
+        return err, ninflu, influ.reshape(self.n, 100), (wij.reshape(self.n, 100, 4) if with_wij else None)
+
+
+_rlib = None
+
+
+def have_reference() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def reference_lib():
+    global _rlib
+    if _rlib is None:
+        lib = C.CDLL(REF_SO)
+        lib.ref_create.restype = C.c_void_p
+        lib.ref_create.argtypes = [C.c_char_p, C.c_int]
+        lib.ref_last_error.restype = C.c_int
+        lib.ref_set_threads.argtypes = [C.c_void_p, C.c_int]
+        lib.ref_get_params.argtypes = [C.c_void_p, C.POINTER(Params)]
+        lib.ref_get_materials.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.ref_get_field.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
+        lib.ref_particles.restype = C.c_void_p
+        lib.ref_particles.argtypes = [C.c_void_p]
+        lib.ref_particle_size.restype = C.c_size_t
+        lib.ref_nnps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.ref_step.argtypes = [C.c_void_p, C.c_int]
+        lib.ref_get_step.argtypes = [C.c_void_p]
+        lib.ref_destroy.argtypes = [C.c_void_p]
+        _rlib = lib
+    return _rlib
+
+
+class Reference:
+    """The reference solver, initialised from an input.dat by its own code."""
+
+    def __init__(self, input_dat: str, nthreads: int = 1):
+        self.lib = reference_lib()
+        h = self.lib.ref_create(input_dat.encode(), int(nthreads))
+        if not h:
+            raise RuntimeError(f"ref_create failed: {self.lib.ref_last_error()}")
+        self.h = C.c_void_p(h)
+        self.params = Params()
+        self.lib.ref_get_params(self.h, C.byref(self.params))
+        self.n = int(self.params.ntotal)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.ref_destroy(self.h)
+            self.h = None
+
+    def get_field(self, name):
+        nc = ORACLE_FIELDS[name]
+        dt = np.int32 if name in INT_FIELDS else np.float64
+        a = np.empty(self.n * nc, dtype=dt)
+        assert self.lib.ref_get_field(self.h, name.encode(), _ptr(a)) == 0, name
+        return a if nc == 1 else a.reshape(self.n, nc)
+
+    def materials(self):
+        from scenes import FLUID_DTYPE, SOIL_DTYPE
+        fl = np.zeros(self.n, FLUID_DTYPE)
+        so = np.zeros(self.n, SOIL_DTYPE)
+        self.lib.ref_get_materials(self.h, _ptr(fl), _ptr(so))
+        return fl, so
+
+    def set_threads(self, n):
+        self.lib.ref_set_threads(self.h, int(n))
+
+    def step(self, nsteps=1):
+        return self.lib.ref_step(self.h, int(nsteps))
+
+    def nnps(self, with_wij=False):
+        ninflu = np.zeros(self.n, np.int32)
+        influ = np.zeros(self.n * 100, np.int32)
+        wij = np.zeros(self.n * 400) if with_wij else None
+        err = self.lib.ref_nnps(self.h, _ptr(ninflu), _ptr(influ), _ptr(wij) if with_wij else None)
+        return err, ninflu, influ.reshape(self.n, 100), (wij.reshape(self.n, 100, 4) if with_wij else None)
+
+    def particles_bytes(self):
+        size = self.lib.ref_particle_size()
+        ptr = self.lib.ref_particles(self.h)
+        return size, C.string_at(ptr, size * self.n)
+
+
+STATE_FIELDS = ("x", "xp", "vx", "vxp", "ax", "axp", "ux", "strep", "interf", "interfss", "rho",
+                "rhop", "mass", "hl", "pre", "prep", "e", "eps", "sig", "adps", "satu", "cop",
+                "vsig", "veps", "divq", "divr", "meps", "prew", "prea", "porosity", "poro_cop",
+                "type", "matype", "permtype", "etype")
+
+
+def snapshot(obj, names=STATE_FIELDS):
+    return {k: obj.get_field(k) for k in names}
