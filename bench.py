@@ -1,0 +1,368 @@
+#!/usr/bin/env python3
+"""Benchmark: particle-updates/s of the SPH time step on B200.
+
+Workload (the reference's second configuration): a 3-D saturated soil column
+collapse -- a 1.0 x 0.5 x 0.5 m Drucker-Prager soil block at dx = 5 mm
+(2,000,000 soil particles, E = 10 MPa, nu = 0.3, phi = 30 deg, c = 0,
+rho_s = 2650, porosity 0.4) overlapped by 2,000,000 pore-water particles,
+Darcy drag with k = 1e-4 m/s, in a 3-layer walled box (452,072 wall
+particles), dt = 0.25 dr / 600.  Synthetic lattice input, FP64 throughout.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours       K steps of the engine (CUDA graph per step) timed with CUDA events
+           on the engine's stream, state resident in HBM; value =
+           active particles (types 1-4) x K / time.  e2e: the same K steps
+           through the C ABI from host buffers (state upload before, full
+           state download after, inside the timed region).
+reference  the reference solver itself (oracle/_ref, compiled from its own
+           sources) on the host cores, same workload and metric.
+With torchrun (N > 1) every rank runs an independent replica of the workload
+(the path has no exchange step); value is the sum over ranks divided by the
+slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "multiphase-sph-solver_b200")
+sys.path.insert(0, PKG)
+
+import numpy as np  # noqa: E402
+
+import scenes  # noqa: E402
+
+METRIC = "particle-updates/s"
+WORKLOAD = "3d_saturated_soil_column_collapse"
+
+# Algorithmic bytes per particle and launch (FP64, 3-D), each kernel reading
+# its own particle's fields and neighbour-list row once and writing its
+# outputs once; neighbour fields are counted as cache-served.  NB is the mean
+# listed neighbours per particle (65 for co-located soil and water).
+NB_MEAN = 65
+
+
+def algorithmic_bytes(stage: str, nb: float = NB_MEAN) -> float:
+    row = 4.0 * nb                       # the particle's neighbour-list row
+    table = {
+        "k_cellkey": 24 + 12,                                   # xp -> cell, key, value
+        "radix_sort": 3 * 16,                                   # 3 digit passes of (key, value) in+out
+        "k_cellrange": 4 + 8,
+        "k_nnps": 24 + 8 + 8 + 4 + 4 + 4 + row,                 # xp, hl, cell, type, pid | count, list
+        "k_density": 4 + 4 + 8 + 24 + 24 + 8 + 8 + 8 + 8 + 8 + row + 8 + 16,
+        "k_shepard_eos": 4 + 4 + 8 + 8 + 8 + 8 + 8 + 8 + row + 8 + 8,
+        "k_strain_stress": 4 + 4 + 4 + 48 + 48 + 24 + 24 + 8 + 8 + 24 + 32 + 24 + 48 + 8 + 8 + row
+                           + 48 + 48 + 24 + 16 + 48 + 16 + 40,
+        "k_accel": 4 + 4 + 48 + 8 + 24 + 24 + 8 + 8 + 8 + 8 + 8 + 8 + 24 + 24 + 24 + row + 24 + 24 + 24,
+        "k_xsph_update": 4 + 4 + 24 + 24 + 24 + 24 + 24 + 8 + 8 + row + 24 + 24 + 24 + 24 + 8,
+    }
+    return float(table.get(stage, 0.0))
+
+
+def measured_peaks() -> tuple[dict, str]:
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            return json.load(fh), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def ncu_traffic() -> dict:
+    """Per-particle DRAM bytes per kernel from the committed ncu summary."""
+    p = os.path.join(REPO, "profiles", "ncu_traffic_per_particle.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            return json.load(fh)
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 200 ms during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.fh = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        self.fh.flush()
+        self.fh.seek(0)
+        sm, smax, reasons = [], [], set()
+        for line in self.fh.read().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"),
+                               f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.fh.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_sum(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# --------------------------------------------------------------------------
+# reference solver on the host cores
+
+def run_reference(scene, steps: int, warmup: int, threads: int) -> dict:
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    from checkers import Reference, have_reference
+    if not have_reference():
+        return {"unavailable": "oracle/_ref/libsphref.so was not built (needs the reference source tree)"}
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "input.dat")
+        scenes.write_input_dat(scene, path, ntd=threads)
+        t0 = time.perf_counter()
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        saved = os.dup(1)
+        os.dup2(devnull, 1)          # the reference prints progress to stdout
+        try:
+            ref = Reference(path, threads)
+            t_init = time.perf_counter() - t0
+            err = ref.step(warmup) if warmup else 0
+            t1 = time.perf_counter()
+            err = err or ref.step(steps)
+            t_steps = time.perf_counter() - t1
+        finally:
+            os.dup2(saved, 1)
+            os.close(devnull)
+            os.close(saved)
+    return {"init_s": t_init, "step_s": t_steps / max(steps, 1), "err": err,
+            "value": scene.n_active() * steps / t_steps if t_steps > 0 else None}
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    full = scenes.soil_column_3d(dx=args.dx, steps=5000)
+    need_gb = full.n * 8.0e3 / 1e9
+    try:
+        import psutil
+        avail_gb = psutil.virtual_memory().available / 1e9
+    except Exception:
+        avail_gb = float("inf")
+    steps = max(1, min(args.steps, 3))
+    warm = min(args.warmup, 1)
+    threads = host_threads()
+    if avail_gb < need_gb * 1.3:
+        scene = scenes.soil_column_3d(dx=2 * args.dx, steps=5000)
+        sample = (f"{steps} steps of the same scene at dx={2 * args.dx:g} ({scene.n} particles); "
+                  f"full size needs ~{need_gb:.0f} GB host RAM, {avail_gb:.0f} GB free")
+    else:
+        scene = full
+        sample = f"{steps} steps (after {warm} warm-up) of the full workload, {scene.n} particles"
+    r = run_reference(scene, steps, warm, threads)
+    if "unavailable" in r:
+        print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}))
+        return 0
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": "particle-updates/s",
+        "n_gpus": 0, "steps": steps, "warmup": warm, "ms_per_step": r["step_s"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "dx": scene.dr, "particles": scene.n,
+                   "active_particles": scene.n_active(), "host_threads": threads,
+                   "reference_init_s": round(r["init_s"], 2)},
+        "cpu_baseline": {"value": r["value"], "unit": "particle-updates/s", "cores": threads,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": r["value"], "unit": "particle-updates/s",
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# --------------------------------------------------------------------------
+# engine arm
+
+STATE_UP = ("xp", "vxp", "axp", "ax", "vx", "ux", "rho", "rhop", "mass", "hl", "pre", "prep", "e",
+            "eps", "sig", "adps", "satu", "cop", "porosity", "poro_cop", "cd", "interf", "interfss",
+            "type", "matype", "permtype", "etype")
+STATE_DOWN = ("xp", "vxp", "axp", "ax", "vx", "ux", "rho", "rhop", "pre", "prep", "e", "eps", "sig",
+              "adps", "satu", "cop", "porosity", "poro_cop", "prew", "prea", "strep", "interf",
+              "interfss", "vsig", "veps", "divq", "divr", "meps")
+
+
+def engine_arm(args, world, rank, local):
+    import sphgpu
+    scene = scenes.soil_column_3d(dx=args.dx, steps=5000)
+    st = scenes.initialise(scene)
+    n_active = scene.n_active()
+    eng = sphgpu.Engine(st.params, device=local if world > 1 else args.device)
+    eng.load_state(st.fields, st.fluid, st.soil)
+    eng.step(args.warmup)
+    barrier(world)
+    eng.synchronize()
+    clocks = ClockSampler(local if world > 1 else args.device)
+    time.sleep(0.3)
+    eng.step(args.steps)                              # timed: CUDA events on the engine stream
+    ms = eng.last_step_ms()
+    launches = eng.last_step_launches()
+    clk = clocks.stop()
+    ms_max = dist_max(ms, world)
+    total_active = dist_sum(float(n_active), world)
+    value = total_active * args.steps / (ms_max / 1e3)
+
+    # stage durations with an event between stages, over the same number of steps
+    prof = eng.step_profiled(args.steps)
+    dominant = max((k for k in prof if k != "k_step_done"), key=lambda k: prof[k])
+    avg_ms = prof[dominant] / args.steps
+    peaks, peak_kind = measured_peaks()
+    alg = algorithmic_bytes(dominant) * scene.n
+    achieved = alg / (avg_ms / 1e3) / 1e9
+    traffic = ncu_traffic().get(dominant)
+
+    # end to end through the C ABI from host buffers
+    host = {k: np.ascontiguousarray(st.fields[k]) for k in STATE_UP}
+    fluid, soil = st.fluid, st.soil
+    eng2 = sphgpu.Engine(st.params, device=local if world > 1 else args.device)
+    barrier(world)
+    t0 = time.perf_counter()
+    eng2.load_state(host, fluid, soil)
+    eng2.step(args.steps)
+    out = {k: eng2.get_field(k) for k in STATE_DOWN}
+    t_e2e = time.perf_counter() - t0
+    t_e2e = dist_max(t_e2e, world)
+    h2d = sum(v.nbytes for v in host.values()) + fluid.nbytes + soil.nbytes
+    d2h = sum(v.nbytes for v in out.values())
+    e2e_value = total_active * args.steps / t_e2e
+    eng2.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        small = scenes.soil_column_3d(dx=2 * args.dx, steps=5000)
+        thr = host_threads()
+        r = run_reference(small, 2, 1, thr)
+        if "unavailable" not in r:
+            cpu = {"value": r["value"], "unit": "particle-updates/s", "cores": thr, "kind": "reference",
+                   "sample": f"2 steps (after 1 warm-up) of the same scene at dx={2 * args.dx:g} "
+                             f"({small.n} particles, {small.n_active()} active)"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "particle-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "dx": args.dx, "particles_per_gpu": scene.n,
+                       "active_particles_per_gpu": n_active, "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (state ~%.1f GB per GPU)" % (scene.n * 1.0e3 / 1e9),
+                       "timing": "CUDA events on the engine stream around K graph launches"},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved,
+                         "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                         "frac": achieved / peaks.get("hbm_gbs"), "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
+                         "traffic": (traffic * scene.n) if traffic else None},
+            "stage_ms_per_step": {k: v / args.steps for k, v in prof.items()},
+            "e2e": {"value": e2e_value, "unit": "particle-updates/s",
+                    "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+                    "what": "state upload + K steps + full state download through the C ABI"},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    eng.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--dx", type=float, default=0.005)
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        # host-only arm: rank 0 runs it, the other ranks exit without work
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        return reference_arm(args, world, int(os.environ.get("RANK", "0")))
+    world, rank, local = dist_setup()
+    try:
+        rc = engine_arm(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())

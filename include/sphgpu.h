@@ -194,6 +194,17 @@ long   sphgpu_last_step_launches(const sphgpu_ctx* ctx);
  * work after the engine's. */
 void*  sphgpu_stream(sphgpu_ctx* ctx);
 
+/*
+ * Stage-level profile: runs nsteps like sphgpu_step, but launching each stage
+ * directly on the context's stream with a CUDA event between consecutive
+ * stages, and adds each stage's duration (ms, summed over the steps) to
+ * stage_ms[0 .. sphgpu_stage_count()-1].  Stage k is named by
+ * sphgpu_stage_name(k) (the kernel names, plus "radix_sort").
+ */
+int         sphgpu_stage_count(void);
+const char* sphgpu_stage_name(int k);
+int         sphgpu_step_profiled(sphgpu_ctx* ctx, int nsteps, double* stage_ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,671 @@
+// sph_capi.cu -- host side of the sphgpu C ABI (include/sphgpu.h).
+//
+// Owns the device buffers of one particle system, converts between the
+// caller's particle-major arrays / Particle records and the device's
+// component-major layout, evaluates the per-particle material constants, and
+// runs time steps as CUDA graphs (one graph per step, two variants that
+// alternate the ping-pong buffers of positions and stresses).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/sphgpu.h"
+#include "sph_device.cuh"
+
+extern "C" size_t sphk_sort_temp_bytes(int N, int end_bit);
+extern "C" int sphk_enqueue_nnps(const Dev* d, void* sort_tmp, size_t sort_bytes, int end_bit, cudaStream_t st,
+                                 cudaEvent_t* ev);
+extern "C" int sphk_enqueue_physics(const Dev* d, cudaStream_t st, cudaEvent_t* ev);
+extern "C" const char* const sphk_stage_names[];
+#define SPHK_NSTAGES 11
+
+namespace {
+
+thread_local int g_create_error = 0;
+
+struct FieldDef {
+    const char* name;
+    int ncomp;
+    int is_int;
+};
+
+// Particle members the device owns (Class_particle.h:13-103)
+const FieldDef kFields[] = {
+    {"x", 3, 0}, {"xp", 3, 0}, {"vx", 3, 0}, {"vxp", 3, 0}, {"ax", 3, 0}, {"axp", 3, 0},
+    {"ux", 3, 0}, {"strep", 3, 0}, {"interf", 3, 0}, {"interfss", 3, 0},
+    {"rho", 1, 0}, {"rhop", 1, 0}, {"mass", 1, 0}, {"hl", 1, 0}, {"pre", 1, 0}, {"prep", 1, 0},
+    {"e", 1, 0}, {"eps", 6, 0}, {"sig", 6, 0}, {"adps", 6, 0}, {"satu", 1, 0}, {"cop", 1, 0},
+    {"vsig", 1, 0}, {"veps", 1, 0}, {"divq", 1, 0}, {"divr", 1, 0}, {"meps", 1, 0},
+    {"prew", 1, 0}, {"prea", 1, 0}, {"porosity", 1, 0}, {"poro_cop", 1, 0}, {"cd", 1, 0},
+    {"type", 1, 1}, {"matype", 1, 1}, {"permtype", 1, 1}, {"etype", 1, 1},
+};
+
+const FieldDef* find_field(const char* name)
+{
+    if (!name) return nullptr;
+    for (const FieldDef& f : kFields)
+        if (std::strcmp(f.name, name) == 0) return &f;
+    return nullptr;
+}
+
+// byte offsets of the members in the reference's Particle (1064 bytes)
+struct AosMember { const char* name; size_t off; };
+const AosMember kAos[] = {
+    {"x", 0}, {"xp", 24}, {"vx", 48}, {"vxp", 72}, {"ax", 96}, {"axp", 120}, {"ux", 144},
+    {"strep", 168}, {"interf", 264}, {"interfss", 288}, {"rho", 312}, {"rhop", 320},
+    {"mass", 328}, {"hl", 336}, {"pre", 344}, {"prep", 352}, {"e", 360}, {"eps", 368},
+    {"sig", 464}, {"adps", 656}, {"satu", 760}, {"cop", 784}, {"vsig", 792}, {"veps", 800},
+    {"divq", 808}, {"divr", 816}, {"meps", 824}, {"prew", 864}, {"prea", 872},
+    {"porosity", 880}, {"cd", 888}, {"poro_cop", 896}, {"type", 1048}, {"matype", 1052},
+    {"permtype", 1056}, {"etype", 1060},
+};
+constexpr size_t kParticleBytes = 1064;
+
+}  // namespace
+
+struct sphgpu_ctx {
+    sphgpu_params P;
+    int device = 0;
+    int N = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    Dev d[2];              // parity variants: d[p] reads buffers "cur" of parity p
+    int parity = 0;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    void* sort_tmp = nullptr;
+    size_t sort_bytes = 0;
+    int end_bit = 1;
+    std::vector<void*> allocs;
+    std::vector<int> h_type, h_matype;
+    std::vector<double> h_x;          // x as uploaded (the reference writes it only in update)
+    bool x_tracked = false;
+    int l_host = 1;
+    double last_ms = 0.0;
+    long launches_per_step = 0;
+    long last_launches = 0;
+    int sticky = 0;
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+};
+
+namespace {
+
+int cuda_fail(sphgpu_ctx* c, cudaError_t e, const char* what)
+{
+    if (e == cudaSuccess) return 0;
+    std::fprintf(stderr, "sphgpu: %s: %s\n", what, cudaGetErrorString(e));
+    if (c) c->sticky = SPHGPU_E_CUDA;
+    return SPHGPU_E_CUDA;
+}
+#define CK(call) do { int _r = cuda_fail(c, (call), #call); if (_r) return _r; } while (0)
+
+template <typename T>
+int dalloc(sphgpu_ctx* c, T** p, size_t count)
+{
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 16);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc");
+    cudaMemsetAsync(q, 0, count * sizeof(T) + 16, c->st);
+    c->allocs.push_back(q);
+    *p = (T*)q;
+    return 0;
+}
+
+int check_params(const sphgpu_params* P)
+{
+    if (!P) return SPHGPU_E_ARG;
+    if (P->ndim != 2 && P->ndim != 3) return SPHGPU_E_ARG;
+    if (P->ntotal <= 0 || P->ctotal <= 0 || P->cxm <= 0 || P->cym <= 0 || P->czm <= 0) return SPHGPU_E_ARG;
+    if ((long long)P->cxm * P->cym * P->czm != P->ctotal) return SPHGPU_E_ARG;
+    if (!(P->dr > 0.0) || !(P->dt > 0.0)) return SPHGPU_E_ARG;
+    if (P->step_regu <= 0) return SPHGPU_E_ARG;
+    // flag combinations this engine runs (the others are rejected loudly)
+    if (P->flbndy != 1) return SPHGPU_E_UNSUPPORTED;
+    if (P->flknl != 1 && P->flknl != 2) return SPHGPU_E_UNSUPPORTED;
+    if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
+    if (P->art_stre_coe > 0.0) return SPHGPU_E_UNSUPPORTED;
+    if (P->fli != 0 && P->fli != 1) return SPHGPU_E_UNSUPPORTED;
+    if (P->ss_type != 0) return SPHGPU_E_UNSUPPORTED;
+    if (P->if_move != 0 && P->if_move != 1) return SPHGPU_E_UNSUPPORTED;
+    return 0;
+}
+
+int end_bit_for(int m)
+{
+    int b = 1;
+    while (b < 32 && (1u << b) <= (unsigned)m) b++;
+    return b;
+}
+
+// (re)build the two step graphs: NNPS + physics for parity 0 and 1
+int build_graphs(sphgpu_ctx* c)
+{
+    for (int p = 0; p < 2; p++) {
+        if (c->exec[p]) { cudaGraphExecDestroy(c->exec[p]); c->exec[p] = nullptr; }
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+        int n = sphk_enqueue_nnps(&c->d[p], c->sort_tmp, c->sort_bytes, c->end_bit, c->st, nullptr);
+        n += sphk_enqueue_physics(&c->d[p], c->st, nullptr);
+        cudaError_t e = cudaStreamEndCapture(c->st, &g);
+        if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&c->exec[p], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+        c->launches_per_step = n;
+    }
+    return 0;
+}
+
+void invalidate_graphs(sphgpu_ctx* c)
+{
+    for (int p = 0; p < 2; p++)
+        if (c->exec[p]) { cudaGraphExecDestroy(c->exec[p]); c->exec[p] = nullptr; }
+}
+
+int ensure_pinned(sphgpu_ctx* c, size_t bytes)
+{
+    if (c->pinned_bytes >= bytes) return 0;
+    if (c->pinned) cudaFreeHost(c->pinned);
+    c->pinned = nullptr;
+    c->pinned_bytes = 0;
+    CK(cudaMallocHost(&c->pinned, bytes));
+    c->pinned_bytes = bytes;
+    return 0;
+}
+
+// device pointer behind a field name for the current parity
+void* field_ptr(sphgpu_ctx* c, const char* name)
+{
+    DevState& s = c->d[c->parity].s;
+    struct { const char* n; void* p; } tab[] = {
+        {"xp", s.xp}, {"vx", s.vx}, {"vxp", s.vxp}, {"ax", s.ax}, {"axp", s.axp}, {"ux", s.ux},
+        {"strep", s.strep}, {"interf", s.interf}, {"interfss", s.interfss}, {"rho", s.rho},
+        {"rhop", s.rhop}, {"mass", s.mass}, {"hl", s.hl}, {"pre", s.pre}, {"prep", s.prep},
+        {"e", s.e}, {"eps", s.eps}, {"sig", s.sig}, {"adps", s.adps}, {"satu", s.satu}, {"cop", s.cop},
+        {"vsig", s.vsig}, {"veps", s.veps}, {"divq", s.divq}, {"divr", s.divr}, {"meps", s.meps},
+        {"prew", s.prew}, {"prea", s.prea}, {"porosity", s.porosity}, {"poro_cop", s.poro_cop},
+        {"cd", s.cd}, {"type", s.type}, {"matype", s.matype}, {"permtype", s.permtype}, {"etype", s.etype},
+    };
+    for (auto& t : tab)
+        if (std::strcmp(t.n, name) == 0) return t.p;
+    return nullptr;
+}
+
+void update_static_params(sphgpu_ctx* c)
+{
+    int w0 = c->N;
+    if (!c->h_type.empty() && !c->h_matype.empty())
+        for (int i = 0; i < c->N; i++)
+            if (c->h_type[i] == 0 && c->h_matype[i] > 2) { w0 = i; break; }
+    for (int p = 0; p < 2; p++) c->d[p].p.first_vbx_wall = w0;
+    invalidate_graphs(c);
+}
+
+int check_particles(sphgpu_ctx* c)
+{
+    if (c->h_type.empty() || c->h_matype.empty()) return SPHGPU_E_STATE;
+    for (int i = 0; i < c->N; i++) {
+        const int t = c->h_type[i], m = c->h_matype[i];
+        if (t == 2) {
+            const int mt = m % 10;
+            if (!(mt == 0 || mt == 2 || mt == 5 || mt == 6) || (m >= 30 && m < 50) || m >= 60)
+                return SPHGPU_E_UNSUPPORTED;
+        }
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sphgpu_abi_version(void) { return SPHGPU_ABI_VERSION; }
+
+int sphgpu_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+const char* sphgpu_error_string(int code)
+{
+    switch (code) {
+    case 0: return "no error";
+    case 3: return "particle outside the cell grid (parttocell)";
+    case 5: return "more than 99 neighbours (partisearching)";
+    case SPHGPU_E_ARG: return "bad argument";
+    case SPHGPU_E_CUDA: return "CUDA runtime error";
+    case SPHGPU_E_NODEVICE: return "no CUDA device";
+    case SPHGPU_E_UNSUPPORTED: return "flag combination not supported by the engine";
+    case SPHGPU_E_STATE: return "call order (state not uploaded)";
+    default: return "unknown error";
+    }
+}
+
+int sphgpu_last_create_error(void) { return g_create_error; }
+
+sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
+{
+    g_create_error = check_params(P);
+    if (g_create_error) return nullptr;
+    int ndev = sphgpu_device_count();
+    if (ndev <= 0 || device < 0 || device >= ndev) { g_create_error = SPHGPU_E_NODEVICE; return nullptr; }
+    sphgpu_ctx* c = new sphgpu_ctx();
+    c->P = *P;
+    c->device = device;
+    c->N = P->ntotal;
+    auto fail = [&](int code) { g_create_error = code; sphgpu_destroy(c); return (sphgpu_ctx*)nullptr; };
+    if (cudaSetDevice(device) != cudaSuccess) return fail(SPHGPU_E_NODEVICE);
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) return fail(SPHGPU_E_CUDA);
+    cudaEventCreate(&c->ev0);
+    cudaEventCreate(&c->ev1);
+    const int N = c->N, M = P->ctotal + 4;
+    Dev& d = c->d[0];
+    DevParams& p = d.p;
+    p.N = N; p.ndim = P->ndim; p.flknl = P->flknl; p.flbndy = P->flbndy; p.fli = P->fli;
+    p.if_move = P->if_move; p.flv = P->flv; p.inip = P->inip; p.step_regu = P->step_regu;
+    p.cxm = P->cxm; p.cym = P->cym; p.czm = P->czm; p.ctotal = P->ctotal;
+    p.water_minor = P->water_acc_type != 0; p.air_minor = P->air_acc_type != 0;
+    p.first_vbx_wall = N;
+    p.dr = P->dr; p.dt = P->dt;
+    p.xsph0 = P->xsph[0]; p.xsph1 = P->xsph[1]; p.xsph2 = P->xsph[2];
+    for (int a = 0; a < 3; a++) for (int b = 0; b < 2; b++) p.av[a][b] = P->art_vis[a][b];
+    p.gx = P->gx; p.gy = P->gy; p.gz = P->gz;
+    p.thr_min = P->threshold_min; p.thr_max = P->threshold_max;
+    p.interc = P->interc; p.pers = P->pers; p.perl = P->perl; p.perm = P->perm; p.permtype = P->permtype;
+    p.coe_bndy = P->coe_bndy;
+    for (int k = 0; k < 3; k++) p.move_vx[k] = P->move_vx[k];
+    p.xmin = P->xmin; p.xmax = P->xmax; p.ymin = P->ymin; p.ymax = P->ymax; p.zmin = P->zmin; p.zmax = P->zmax;
+    p.st_e = P->structure.e; p.st_poi = P->structure.poi;
+    p.g_acc = std::sqrt(P->gx * P->gx + P->gy * P->gy + P->gz * P->gz);   // CPP_10-interact1.cpp:28
+    DevState& s = d.s;
+    int r = 0;
+    r |= dalloc(c, &s.type, N); r |= dalloc(c, &s.matype, N); r |= dalloc(c, &s.etype, N); r |= dalloc(c, &s.permtype, N);
+    r |= dalloc(c, &s.mass, N); r |= dalloc(c, &s.hl, N); r |= dalloc(c, &s.cd, N);
+    r |= dalloc(c, &s.f_dens, N); r |= dalloc(c, &s.f_por, N); r |= dalloc(c, &s.f_vpu, N); r |= dalloc(c, &s.f_vis, N);
+    r |= dalloc(c, &s.f_c, N); r |= dalloc(c, &s.f_smin, N); r |= dalloc(c, &s.f_tanfai, N); r |= dalloc(c, &s.f_bhtype, N);
+    r |= dalloc(c, &s.s_e, N); r |= dalloc(c, &s.s_poi, N); r |= dalloc(c, &s.s_eps0, N); r |= dalloc(c, &s.s_dens, N);
+    r |= dalloc(c, &s.s_kapa, N); r |= dalloc(c, &s.s_por, N); r |= dalloc(c, &s.s_vpu, N); r |= dalloc(c, &s.s_cop, N);
+    r |= dalloc(c, &s.s_sitas, N); r |= dalloc(c, &s.s_sitar, N);
+    r |= dalloc(c, &s.s_yalf, N); r |= dalloc(c, &s.s_ykap, N); r |= dalloc(c, &s.s_yalf_dil, N);
+    r |= dalloc(c, &s.xp, 3 * (size_t)N); r |= dalloc(c, &s.xp_next, 3 * (size_t)N);
+    r |= dalloc(c, &s.vx, 3 * (size_t)N); r |= dalloc(c, &s.vx_next, 3 * (size_t)N);
+    r |= dalloc(c, &s.vxp, 3 * (size_t)N); r |= dalloc(c, &s.axp, 3 * (size_t)N); r |= dalloc(c, &s.ax, 3 * (size_t)N);
+    r |= dalloc(c, &s.ux, 3 * (size_t)N);
+    s.x = nullptr;
+    r |= dalloc(c, &s.rho, N); r |= dalloc(c, &s.rho_c, N); r |= dalloc(c, &s.rhop, N); r |= dalloc(c, &s.pre, N);
+    r |= dalloc(c, &s.prep, N); r |= dalloc(c, &s.porosity, N); r |= dalloc(c, &s.poro_cop, N); r |= dalloc(c, &s.e, N);
+    r |= dalloc(c, &s.sig, 6 * (size_t)N); r |= dalloc(c, &s.sig_next, 6 * (size_t)N);
+    r |= dalloc(c, &s.eps, 6 * (size_t)N); r |= dalloc(c, &s.adps, 6 * (size_t)N);
+    r |= dalloc(c, &s.satu, N); r |= dalloc(c, &s.cop, N); r |= dalloc(c, &s.prew, N); r |= dalloc(c, &s.prea, N);
+    r |= dalloc(c, &s.interf, 3 * (size_t)N); r |= dalloc(c, &s.interfss, 3 * (size_t)N); r |= dalloc(c, &s.strep, 3 * (size_t)N);
+    r |= dalloc(c, &s.vsig, N); r |= dalloc(c, &s.veps, N); r |= dalloc(c, &s.divq, N); r |= dalloc(c, &s.divr, N);
+    r |= dalloc(c, &s.meps, N);
+    r |= dalloc(c, &s.cell, N); r |= dalloc(c, &s.key_in, N); r |= dalloc(c, &s.key_out, N);
+    r |= dalloc(c, &s.val_in, N); r |= dalloc(c, &s.pid_sorted, N);
+    r |= dalloc(c, &s.cstart, M); r |= dalloc(c, &s.cend, M);
+    r |= dalloc(c, &s.nnb, N); r |= dalloc(c, &s.nbr, (size_t)SPH_NB_CAP * N);
+    r |= dalloc(c, &s.err, 1); r |= dalloc(c, &s.step, 1);
+    if (r) return fail(SPHGPU_E_CUDA);
+    // cell_info() constructor values (Class_NNPS.cpp:68-72): the range of the
+    // last cell, which the reference never resets, starts from them
+    std::vector<int> st(M, 2000000), en(M, -2000000);
+    if (cudaMemcpyAsync(s.cstart, st.data(), sizeof(int) * M, cudaMemcpyHostToDevice, c->st) != cudaSuccess ||
+        cudaMemcpyAsync(s.cend, en.data(), sizeof(int) * M, cudaMemcpyHostToDevice, c->st) != cudaSuccess)
+        return fail(SPHGPU_E_CUDA);
+    int one = 1;
+    if (cudaMemcpyAsync(s.step, &one, sizeof(int), cudaMemcpyHostToDevice, c->st) != cudaSuccess)
+        return fail(SPHGPU_E_CUDA);
+    c->end_bit = end_bit_for(P->ctotal);
+    c->sort_bytes = sphk_sort_temp_bytes(N, c->end_bit);
+    if (cudaMalloc(&c->sort_tmp, c->sort_bytes + 256) != cudaSuccess) return fail(SPHGPU_E_CUDA);
+    c->allocs.push_back(c->sort_tmp);
+    c->d[1] = c->d[0];
+    std::swap(c->d[1].s.xp, c->d[1].s.xp_next);
+    std::swap(c->d[1].s.sig, c->d[1].s.sig_next);
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return fail(SPHGPU_E_CUDA);
+    return c;
+}
+
+void sphgpu_destroy(sphgpu_ctx* c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->st) cudaStreamSynchronize(c->st);
+    invalidate_graphs(c);
+    for (void* p : c->allocs) cudaFree(p);
+    if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+}
+
+int sphgpu_get_params(const sphgpu_ctx* c, sphgpu_params* out)
+{
+    if (!c || !out) return SPHGPU_E_ARG;
+    *out = c->P;
+    return 0;
+}
+
+int sphgpu_get_step(const sphgpu_ctx* c) { return c ? c->l_host : -1; }
+
+int sphgpu_set_step(sphgpu_ctx* c, int l)
+{
+    if (!c) return SPHGPU_E_ARG;
+    cudaSetDevice(c->device);
+    CK(cudaMemcpyAsync(c->d[0].s.step, &l, sizeof(int), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->l_host = l;
+    return 0;
+}
+
+int sphgpu_field_info(const char* name, int* ncomp, int* elem_type)
+{
+    const FieldDef* f = find_field(name);
+    if (!f) return SPHGPU_E_ARG;
+    if (ncomp) *ncomp = f->ncomp;
+    if (elem_type) *elem_type = f->is_int;
+    return 0;
+}
+
+int sphgpu_set_field(sphgpu_ctx* c, const char* name, const void* host, size_t count)
+{
+    const FieldDef* f = find_field(name);
+    if (!c || !f || !host) return SPHGPU_E_ARG;
+    const int N = c->N, nc = f->ncomp;
+    if (count != (size_t)N * nc) return SPHGPU_E_ARG;
+    cudaSetDevice(c->device);
+    if (std::strcmp(name, "x") == 0) {
+        c->h_x.assign((const double*)host, (const double*)host + (size_t)N * 3);
+        c->x_tracked = true;
+        return 0;
+    }
+    const size_t esz = f->is_int ? 4 : 8;
+    int r = ensure_pinned(c, count * esz);
+    if (r) return r;
+    // particle-major -> component-major
+    if (f->is_int) {
+        std::memcpy(c->pinned, host, count * esz);
+        const int* h = (const int*)host;
+        if (std::strcmp(name, "type") == 0) { c->h_type.assign(h, h + N); update_static_params(c); }
+        if (std::strcmp(name, "matype") == 0) { c->h_matype.assign(h, h + N); update_static_params(c); }
+    } else {
+        const double* h = (const double*)host;
+        double* o = (double*)c->pinned;
+        for (int k = 0; k < nc; k++)
+            for (int i = 0; i < N; i++) o[(size_t)k * N + i] = h[(size_t)i * nc + k];
+    }
+    void* dst = field_ptr(c, name);
+    if (!dst) return SPHGPU_E_ARG;
+    CK(cudaMemcpyAsync(dst, c->pinned, count * esz, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+int sphgpu_get_field(sphgpu_ctx* c, const char* name, void* host, size_t count)
+{
+    const FieldDef* f = find_field(name);
+    if (!c || !f || !host) return SPHGPU_E_ARG;
+    const int N = c->N, nc = f->ncomp;
+    if (count != (size_t)N * nc) return SPHGPU_E_ARG;
+    cudaSetDevice(c->device);
+    if (std::strcmp(name, "x") == 0) {
+        // Particle::x is written only by update (CPP_12-1-update.cpp:30-47):
+        // after a step it equals xp for moving particles and keeps its
+        // uploaded value for the rest
+        std::vector<double> xp((size_t)N * 3);
+        int r = sphgpu_get_field(c, "xp", xp.data(), xp.size());
+        if (r) return r;
+        double* o = (double*)host;
+        for (size_t q = 0; q < xp.size(); q++) o[q] = c->x_tracked ? c->h_x[q] : 0.0;
+        if (c->l_host > 1 && !c->h_type.empty()) {
+            for (int i = 0; i < N; i++) {
+                const int t = c->h_type[i], m = c->h_matype.empty() ? 0 : c->h_matype[i];
+                if (t != 0 || m == 2 || m == 3 || m == 4 || m == 5)
+                    for (int k = 0; k < c->P.ndim; k++) o[(size_t)i * 3 + k] = xp[(size_t)i * 3 + k];
+            }
+        }
+        return 0;
+    }
+    const size_t esz = f->is_int ? 4 : 8;
+    int r = ensure_pinned(c, count * esz);
+    if (r) return r;
+    void* src = field_ptr(c, name);
+    if (!src) return SPHGPU_E_ARG;
+    CK(cudaMemcpyAsync(c->pinned, src, count * esz, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (f->is_int) {
+        std::memcpy(host, c->pinned, count * esz);
+    } else {
+        const double* s = (const double*)c->pinned;
+        double* o = (double*)host;
+        for (int k = 0; k < nc; k++)
+            for (int i = 0; i < N; i++) o[(size_t)i * nc + k] = s[(size_t)k * N + i];
+    }
+    return 0;
+}
+
+int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soil* so, int n)
+{
+    if (!c || n != c->N) return SPHGPU_E_ARG;
+    cudaSetDevice(c->device);
+    const int N = c->N;
+    DevState& s = c->d[0].s;
+    std::vector<double> buf((size_t)N);
+    std::vector<int> ibuf((size_t)N);
+    auto put = [&](double* dst) -> int {
+        CK(cudaMemcpyAsync(dst, buf.data(), sizeof(double) * N, cudaMemcpyHostToDevice, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        return 0;
+    };
+    int r = 0;
+    if (fl) {
+        for (int i = 0; i < N; i++) buf[i] = fl[i].dens; r |= put(s.f_dens);
+        for (int i = 0; i < N; i++) buf[i] = fl[i].porosity; r |= put(s.f_por);
+        for (int i = 0; i < N; i++) buf[i] = fl[i].vpu; r |= put(s.f_vpu);
+        for (int i = 0; i < N; i++) buf[i] = fl[i].vis; r |= put(s.f_vis);
+        for (int i = 0; i < N; i++) buf[i] = fl[i].c; r |= put(s.f_c);
+        for (int i = 0; i < N; i++) buf[i] = fl[i].strain_min; r |= put(s.f_smin);
+        // Bingham friction: tan of the angle, CPP_7-2-constitutive.cpp:42-43
+        for (int i = 0; i < N; i++) buf[i] = std::tan(fl[i].fai * 0.0174532925199); r |= put(s.f_tanfai);
+        for (int i = 0; i < N; i++) ibuf[i] = fl[i].bhtype;
+        CK(cudaMemcpyAsync(s.f_bhtype, ibuf.data(), sizeof(int) * N, cudaMemcpyHostToDevice, c->st));
+        CK(cudaStreamSynchronize(c->st));
+    }
+    if (so) {
+        for (int i = 0; i < N; i++) buf[i] = so[i].e; r |= put(s.s_e);
+        for (int i = 0; i < N; i++) buf[i] = so[i].poi; r |= put(s.s_poi);
+        for (int i = 0; i < N; i++) buf[i] = so[i].eps0; r |= put(s.s_eps0);
+        for (int i = 0; i < N; i++) buf[i] = so[i].dens; r |= put(s.s_dens);
+        for (int i = 0; i < N; i++) buf[i] = so[i].kapa; r |= put(s.s_kapa);
+        for (int i = 0; i < N; i++) buf[i] = so[i].porosity; r |= put(s.s_por);
+        for (int i = 0; i < N; i++) buf[i] = so[i].vpu; r |= put(s.s_vpu);
+        for (int i = 0; i < N; i++) buf[i] = so[i].cop; r |= put(s.s_cop);
+        for (int i = 0; i < N; i++) buf[i] = so[i].sitas; r |= put(s.s_sitas);
+        for (int i = 0; i < N; i++) buf[i] = so[i].sitar; r |= put(s.s_sitar);
+        // Drucker-Prager cone constants with the reference's own libm calls
+        // (dpmodel1 / dpmodel_bui / DPModel_check, CPP_8-1-consfactor.cpp:294-349,
+        // 461-529, 783-803); they depend only on the material record.
+        std::vector<double> ya(N), yk(N), yd(N);
+        for (int i = 0; i < N; i++) {
+            const double fai = std::atan(std::tan(so[i].fai * 0.0174532925166667) / so[i].fs);
+            const double fai_dil = std::atan(std::tan(so[i].beta * 0.0174532925166667) / so[i].fs);
+            const double ci = so[i].c / so[i].fs;
+            ya[i] = std::sin(fai) / std::sqrt(9.0 + 3.0 * std::sin(fai) * std::sin(fai));
+            yk[i] = 3.0 * ci * std::cos(fai) / std::sqrt(9.0 + 3.0 * std::sin(fai) * std::sin(fai));
+            // dilatancy slope, used by the Bui form (matype % 10 == 5) only
+            yd[i] = std::sin(fai_dil) / std::sqrt(9.0 + 3.0 * std::sin(fai_dil) * std::sin(fai_dil));
+        }
+        buf = ya; r |= put(s.s_yalf);
+        buf = yk; r |= put(s.s_ykap);
+        buf = yd; r |= put(s.s_yalf_dil);
+    }
+    return r ? SPHGPU_E_CUDA : 0;
+}
+
+int sphgpu_upload_particles(sphgpu_ctx* c, const void* particles, int n, size_t stride)
+{
+    if (!c || !particles || n != c->N || stride < kParticleBytes) return SPHGPU_E_ARG;
+    const char* base = (const char*)particles;
+    for (const AosMember& m : kAos) {
+        const FieldDef* f = find_field(m.name);
+        const size_t nc = f->ncomp;
+        if (f->is_int) {
+            std::vector<int> v((size_t)n);
+            for (int i = 0; i < n; i++) std::memcpy(&v[i], base + (size_t)i * stride + m.off, 4);
+            int r = sphgpu_set_field(c, m.name, v.data(), v.size());
+            if (r) return r;
+        } else {
+            std::vector<double> v((size_t)n * nc);
+            for (int i = 0; i < n; i++) std::memcpy(&v[(size_t)i * nc], base + (size_t)i * stride + m.off, 8 * nc);
+            int r = sphgpu_set_field(c, m.name, v.data(), v.size());
+            if (r) return r;
+        }
+    }
+    return 0;
+}
+
+int sphgpu_download_particles(sphgpu_ctx* c, void* particles, int n, size_t stride)
+{
+    if (!c || !particles || n != c->N || stride < kParticleBytes) return SPHGPU_E_ARG;
+    char* base = (char*)particles;
+    for (const AosMember& m : kAos) {
+        const FieldDef* f = find_field(m.name);
+        const size_t nc = f->ncomp;
+        if (f->is_int) {
+            std::vector<int> v((size_t)n);
+            int r = sphgpu_get_field(c, m.name, v.data(), v.size());
+            if (r) return r;
+            for (int i = 0; i < n; i++) std::memcpy(base + (size_t)i * stride + m.off, &v[i], 4);
+        } else {
+            std::vector<double> v((size_t)n * nc);
+            int r = sphgpu_get_field(c, m.name, v.data(), v.size());
+            if (r) return r;
+            for (int i = 0; i < n; i++) std::memcpy(base + (size_t)i * stride + m.off, &v[(size_t)i * nc], 8 * nc);
+        }
+    }
+    return 0;
+}
+
+int sphgpu_step(sphgpu_ctx* c, int nsteps)
+{
+    if (!c || nsteps < 0) return SPHGPU_E_ARG;
+    if (c->sticky) return c->sticky;
+    if (nsteps == 0) return 0;
+    int r = check_particles(c);
+    if (r) return r;
+    // regularisation passes (strain_regu / stress_regu) are not part of this engine
+    for (int l = c->l_host; l < c->l_host + nsteps; l++)
+        if (l % c->P.step_regu == 0) return SPHGPU_E_UNSUPPORTED;
+    cudaSetDevice(c->device);
+    if (!c->exec[0] || !c->exec[1]) {
+        r = build_graphs(c);
+        if (r) return r;
+    }
+    const int l0 = c->l_host;
+    CK(cudaEventRecord(c->ev0, c->st));
+    for (int s = 0; s < nsteps; s++) CK(cudaGraphLaunch(c->exec[(c->parity + s) & 1], c->st));
+    CK(cudaEventRecord(c->ev1, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->last_ms = ms;
+    c->last_launches = c->launches_per_step * nsteps;
+    int err = 0, l = 0;
+    CK(cudaMemcpy(&err, c->d[0].s.err, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&l, c->d[0].s.step, sizeof(int), cudaMemcpyDeviceToHost));
+    c->parity = (c->parity + (l - l0)) & 1;
+    c->l_host = l;
+    return err;
+}
+
+int sphgpu_nnps(sphgpu_ctx* c, int* ninflu, int* influ)
+{
+    if (!c) return SPHGPU_E_ARG;
+    if (c->sticky) return c->sticky;
+    cudaSetDevice(c->device);
+    sphk_enqueue_nnps(&c->d[c->parity], c->sort_tmp, c->sort_bytes, c->end_bit, c->st, nullptr);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->st));
+    int err = 0;
+    CK(cudaMemcpy(&err, c->d[0].s.err, sizeof(int), cudaMemcpyDeviceToHost));
+    const int N = c->N;
+    if (ninflu) CK(cudaMemcpy(ninflu, c->d[0].s.nnb, sizeof(int) * N, cudaMemcpyDeviceToHost));
+    if (influ) {
+        std::vector<int> cnt(N), nb((size_t)SPH_NB_CAP * N);
+        CK(cudaMemcpy(cnt.data(), c->d[0].s.nnb, sizeof(int) * N, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(nb.data(), c->d[0].s.nbr, sizeof(int) * nb.size(), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < N; i++) {
+            int* row = influ + (size_t)i * 100;
+            std::memset(row, 0, sizeof(int) * 100);
+            const int m = cnt[i] < SPH_NB_CAP ? cnt[i] : SPH_NB_CAP;
+            for (int s = 0; s < m; s++) row[s + 1] = nb[(size_t)s * N + i];
+        }
+    }
+    return err;
+}
+
+int sphgpu_synchronize(sphgpu_ctx* c)
+{
+    if (!c) return SPHGPU_E_ARG;
+    cudaSetDevice(c->device);
+    CK(cudaStreamSynchronize(c->st));
+    return c->sticky;
+}
+
+int sphgpu_stage_count(void) { return SPHK_NSTAGES; }
+
+const char* sphgpu_stage_name(int k)
+{
+    return (k >= 0 && k < SPHK_NSTAGES) ? sphk_stage_names[k] : nullptr;
+}
+
+int sphgpu_step_profiled(sphgpu_ctx* c, int nsteps, double* stage_ms)
+{
+    if (!c || nsteps < 0 || !stage_ms) return SPHGPU_E_ARG;
+    if (c->sticky) return c->sticky;
+    int r = check_particles(c);
+    if (r) return r;
+    for (int l = c->l_host; l < c->l_host + nsteps; l++)
+        if (l % c->P.step_regu == 0) return SPHGPU_E_UNSUPPORTED;
+    cudaSetDevice(c->device);
+    cudaEvent_t ev[SPHK_NSTAGES + 1];
+    for (int k = 0; k <= SPHK_NSTAGES; k++) CK(cudaEventCreate(&ev[k]));
+    for (int k = 0; k < SPHK_NSTAGES; k++) stage_ms[k] = 0.0;
+    int err = 0;
+    for (int s = 0; s < nsteps && err == 0; s++) {
+        const Dev* d = &c->d[c->parity];
+        sphk_enqueue_nnps(d, c->sort_tmp, c->sort_bytes, c->end_bit, c->st, ev);
+        sphk_enqueue_physics(d, c->st, ev);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(c->st));
+        for (int k = 0; k < SPHK_NSTAGES; k++) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+            stage_ms[k] += ms;
+        }
+        int l = 0;
+        CK(cudaMemcpy(&err, c->d[0].s.err, sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&l, c->d[0].s.step, sizeof(int), cudaMemcpyDeviceToHost));
+        c->parity = (c->parity + (l - c->l_host)) & 1;
+        c->l_host = l;
+    }
+    for (int k = 0; k <= SPHK_NSTAGES; k++) cudaEventDestroy(ev[k]);
+    return err;
+}
+
+double sphgpu_last_step_ms(const sphgpu_ctx* c) { return c ? c->last_ms : 0.0; }
+long sphgpu_last_step_launches(const sphgpu_ctx* c) { return c ? c->last_launches : 0; }
+void* sphgpu_stream(sphgpu_ctx* c) { return c ? (void*)c->st : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,1097 @@
+// sph_kernels.cu -- the per-step particle loop of the multi-phase SPH solver
+// as sm_100a kernels (FP64 drop-in form).
+//
+// One time step (the body of SPH_Calculation's main loop,
+// CPP_1-SPHLoops.cpp:523-753) is seven kernels plus a radix sort, one kernel
+// per level of the neighbour-data dependency chain:
+//
+//   k_cellkey      parttocell: cell key per particle            (CPP_3-NNPS.cpp:175-257)
+//   radix sort     Binary_Sort's order: cell ascending, index descending
+//   k_cellreset/k_cellrange  cell_info start/end                (CPP_3-NNPS.cpp:196-201, 621-629)
+//   k_nnps         partisearching: stencil scan, FP64 distance test, neighbour list
+//   k_density      fluid porosity + continuity                  (CPP_6-density.cpp:25-165)
+//   k_shepard_eos  Shepard filter (Jacobi) + local EOS          (CPP_6-density.cpp:168-188, CPP_7-1-eos_CR.cpp:22-43)
+//   k_strain_stress strain rate, gathered pressures / wall stress, permeability,
+//                  constitutive update, free-surface correction, principal stresses
+//   k_accel        momentum (fluid / soil / structure), artificial viscosity,
+//                  wall stress, Darcy drag, velocity update
+//   k_xsph_update  XSPH, wall velocity correction, domain check, position update
+//
+// Every pair sum is gathered by the particle that owns it, in the reference's
+// neighbour order, with no atomics: results are deterministic and, with
+// -fmad=false, equal to the reference's FP64 arithmetic.  Kernel values are
+// recomputed per pair from the positions (sph_pair_w) instead of being stored.
+// All kernels return immediately once an error code is set, so a failing step
+// leaves the state as the reference leaves it when it returns the code.
+#include <cub/cub.cuh>
+#include <climits>
+#include "sph_device.cuh"
+
+#define IDX (blockIdx.x * blockDim.x + threadIdx.x)
+
+__device__ __forceinline__ void raise_err(int* err, int code) { atomicCAS(err, 0, code); }
+
+// x86-64 cvttsd2si semantics for the reference's (int) casts of FP64 cell
+// coordinates: NaN and out-of-range values become INT_MIN.
+__device__ __forceinline__ int to_int_x86(double v)
+{
+    return (v >= -2147483648.0 && v < 2147483648.0) ? (int)v : INT_MIN;
+}
+
+// cell_link slot p of cell c (celllist_ini2, CPP_3-NNPS.cpp:124-171).
+__device__ __forceinline__ int cell_link(const DevParams& p, int c, int slot)
+{
+    int v;
+    if (p.ndim == 2) {
+        int ky = slot / 3 + 1, kx = slot % 3 + 1;
+        v = (kx - 2) * p.cym + ky - 2 + c;
+    } else {
+        int kz = slot / 9 + 1, kx = (slot / 3) % 3 + 1, ky = slot % 3 + 1;
+        v = (ky - 2) * p.cxm * p.czm + (kx - 2) * p.czm + kz - 2 + c;
+    }
+    return (v < 0 || v > p.ctotal) ? 0 : v;
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_cellkey(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    const double xmin[3] = {d.p.xmin, d.p.ymin, d.p.zmin};
+    const double dr = 2.0 * d.p.dr;
+    int nx_t[3] = {0, 0, 0};
+    for (int j = 0; j < d.p.ndim; j++) {
+        double nx = fabs(d.s.xp[j * N + i] - xmin[j]) / dr + 2.0;
+        nx_t[j] = to_int_x86(nx);
+        if (nx_t[j] < 2) nx_t[j] = 2;
+    }
+    unsigned key;
+    if (d.p.ndim == 2)
+        key = (unsigned)d.p.cym * (unsigned)(nx_t[0] - 1) + (unsigned)nx_t[1];
+    else
+        key = (unsigned)d.p.cxm * (unsigned)d.p.czm * (unsigned)(nx_t[1] - 1) +
+              (unsigned)d.p.czm * (unsigned)(nx_t[0] - 1) + (unsigned)nx_t[2];
+    int c = (int)key;
+    if (!(c > 0 && c <= d.p.ctotal)) {
+        raise_err(d.s.err, SPH_ERR_CELL);
+        c = 0;
+    }
+    d.s.cell[i] = c;
+    // reversed input order: the stable radix sort then keeps equal keys in
+    // descending particle index, the order Binary_Sort's merge produces
+    d.s.key_in[N - 1 - i] = (uint32_t)c;
+    d.s.val_in[N - 1 - i] = i;
+}
+
+__global__ void k_cellreset(Dev d)
+{
+    const int c = IDX;
+    if (c >= d.p.ctotal || *d.s.err) return;
+    d.s.cstart[c] = 10000000;
+    d.s.cend[c] = -10000000;
+}
+
+// cell_info start/end.  Cell ctotal is never reset by the reference (its
+// reset loop stops at ctotal - 1), so its range accumulates across steps.
+__global__ void k_cellrange(Dev d)
+{
+    const int q = IDX, N = d.p.N;
+    if (q >= N || *d.s.err) return;
+    const uint32_t c = d.s.key_out[q];
+    const bool first = (q == 0) || d.s.key_out[q - 1] != c;
+    const bool last = (q == N - 1) || d.s.key_out[q + 1] != c;
+    if ((int)c == d.p.ctotal) {
+        if (first) atomicMin(&d.s.cstart[c], q);
+        if (last) atomicMax(&d.s.cend[c], q);
+    } else {
+        if (first) d.s.cstart[c] = q;
+        if (last) d.s.cend[c] = q;
+    }
+}
+
+// partisearching (CPP_3-NNPS.cpp:265-374): neighbours of i in stencil order,
+// descending index inside each cell; inclusion test dst <= h_i + h_j in FP64.
+__global__ void __launch_bounds__(128) k_nnps(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    int cnt = 0;
+    if (d.s.type[i] != 7) {
+        const int nd = d.p.ndim, nst = (nd == 2) ? 9 : 27, nc = d.s.cell[i];
+        double xi[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < nd; k++) xi[k] = d.s.xp[k * N + i];
+        const double hi = d.s.hl[i];
+        for (int nj = 0; nj < nst; nj++) {
+            const int nl = cell_link(d.p, nc, nj);
+            if (nl <= 0) continue;
+            const int start = d.s.cstart[nl], end = d.s.cend[nl];
+            for (int q = start; q <= end; q++) {
+                const int j = d.s.pid_sorted[q];
+                double dst = 0.0;
+                for (int k = 0; k < nd; k++) {
+                    double xj = d.s.xp[k * N + j];
+                    dst = dst + (xi[k] - xj) * (xi[k] - xj);
+                }
+                dst = sqrt(dst);
+                const double ra = (hi + d.s.hl[j]) / 2;
+                if (dst <= 2 * ra && i != j) {
+                    cnt++;
+                    if (cnt <= SPH_NB_CAP) d.s.nbr[(size_t)(cnt - 1) * N + i] = j;
+                    else raise_err(d.s.err, SPH_ERR_NEIGH);
+                }
+            }
+        }
+    }
+    d.s.nnb[i] = cnt;
+}
+
+__device__ __forceinline__ int nbr_count(const Dev& d, int i)
+{
+    int c = d.s.nnb[i];
+    return c > SPH_NB_CAP ? SPH_NB_CAP : c;
+}
+
+// ---------------------------------------------------------------------------
+// density(): fluid porosity (:25-54) and continuity (:57-165) -> rho_c
+__global__ void __launch_bounds__(128) k_density(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    const int ti = d.s.type[i], nd = d.p.ndim, nn = nbr_count(d, i);
+    const int l = *d.s.step;
+    double por = d.s.porosity[i];
+    double pcop = d.s.poro_cop[i];
+    if (ti == 1) {
+        double up = 0.0, down = 0.0;
+        for (int s = 0; s < nn; s++) {
+            const int j = d.s.nbr[(size_t)s * N + i];
+            if (d.s.type[j] == 2) {
+                double w[4];
+                sph_pair_w(d, i, j, w);
+                up = up + d.s.mass[j] * d.s.porosity[j] / d.s.rho[j] * w[3];
+                down = down + d.s.mass[j] / d.s.rho[j] * w[3];
+            }
+        }
+        if (fabs(down) > 1.0e-7) {
+            pcop = por;
+            por = up / down;
+            if (l == 1) pcop = por;
+        } else {
+            pcop = por;
+        }
+        d.s.porosity[i] = por;
+        d.s.poro_cop[i] = pcop;
+    }
+    double rnew = d.s.rho[i];
+    if (ti != 7) {
+        double up[3] = {0.0, 0.0, 0.0}, down[3] = {0.0, 0.0, 0.0};
+        double vi[3], xi[3];
+        for (int k = 0; k < 3; k++) { vi[k] = d.s.vxp[k * N + i]; xi[k] = d.s.xp[k * N + i]; }
+        const bool solid = (ti == 2 || ti == 4), fluid = (ti == 1 || ti == 3);
+        const bool moving = (ti >= 1 && ti <= 4);
+        for (int s = 0; s < nn; s++) {
+            const int j = d.s.nbr[(size_t)s * N + i];
+            const int tj = d.s.type[j];
+            double vxj[3];
+            if (ti == tj && ti != 0) {
+                for (int k = 0; k < 3; k++) vxj[k] = d.s.vxp[k * N + j];
+            } else if (moving && tj == 0) {
+                // virtual wall velocity, flbndy 1: the particle's own (:94-98)
+                for (int k = 0; k < 3; k++) vxj[k] = (d.p.flbndy == 1) ? vi[k] : 0.0;
+            } else {
+                continue;
+            }
+            double w[4];
+            sph_pair_w(d, i, j, w);
+            const double mj = d.s.mass[j];
+            if (solid) {
+                for (int k = 0; k < nd; k++) {
+                    up[k] = up[k] + mj * (vi[k] - vxj[k]) * w[k];
+                    down[k] = down[k] + mj * (xi[k] - d.s.xp[k * N + j]) * w[k];
+                }
+            }
+            if (fluid) {
+                for (int k = 0; k < nd; k++) up[k] = up[k] + mj * (vi[k] - vxj[k]) * w[k];
+            }
+        }
+        double drhot = 0.0;
+        if (solid) {
+            for (int k = 0; k < nd; k++) {
+                if (fabs(down[k]) > 1.0e-7) drhot -= up[k] / down[k];
+                else drhot += up[k];
+            }
+        }
+        if (fluid)
+            for (int k = 0; k < nd; k++) drhot += up[k];
+        const double rhop = d.s.rhop[i], dt = d.p.dt;
+        if (ti == 1 && fabs(por) > 0.0001)
+            rnew = rhop + drhot * dt + rhop * (por - pcop) / (1.0 - pcop);
+        else
+            rnew = rhop + drhot * dt;
+    }
+    d.s.rho_c[i] = rnew;
+}
+
+// Shepard filter (:168-188) reading every neighbour's continuity density
+// (Jacobi order), then the local equation of state (CPP_7-1-eos_CR.cpp:22-43).
+__global__ void __launch_bounds__(128) k_shepard_eos(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    const int ti = d.s.type[i], nn = nbr_count(d, i);
+    double up = 0.0, down = 0.0;
+    for (int s = 0; s < nn; s++) {
+        const int j = d.s.nbr[(size_t)s * N + i];
+        if (d.s.type[j] == ti) {
+            double w[4];
+            sph_pair_w(d, i, j, w);
+            up = up + d.s.mass[j] * w[3];
+            down = down + d.s.mass[j] / d.s.rho_c[j] * w[3];
+        }
+    }
+    double r = d.s.rho_c[i];
+    if (ti != 7 && fabs(down) > 1.0e-7) r = up / down;
+    d.s.rho[i] = r;
+    const double prep = d.s.prep[i];
+    if (ti == 1) {
+        double pr = prep * (pow7(r / d.s.f_dens[i] / d.s.f_por[i]) - 1.0);
+        d.s.pre[i] = pr + prep;
+    } else if (ti == 3) {
+        // the reference's comma expression evaluates to -1.0 (:34)
+        double pr = 1.403 * prep * (-1.0);
+        d.s.pre[i] = pr + prep;
+    } else if (ti == 0 && d.s.matype[i] == 1) {
+        double pr = prep * (pow7(r / d.s.rhop[i]) - 1.0);
+        d.s.pre[i] = pr + prep;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// constitutive helpers (CPP_8-1-consfactor.cpp, CPP_7-2-constitutive.cpp)
+
+__device__ __forceinline__ void jaumann(double ds[6], const double s[6], const double we[9])
+{
+#define WE(a, b) we[(a) * 3 + (b)]
+    ds[0] = ds[0] + (WE(0, 0) * s[0] + WE(0, 1) * s[3] + WE(0, 2) * s[5]) - (s[0] * WE(0, 0) + s[3] * WE(1, 0) + s[5] * WE(2, 0));
+    ds[1] = ds[1] + (WE(1, 0) * s[3] + WE(1, 1) * s[1] + WE(1, 2) * s[4]) - (s[3] * WE(0, 1) + s[1] * WE(1, 1) + s[4] * WE(2, 1));
+    ds[2] = ds[2] + (WE(2, 0) * s[5] + WE(2, 1) * s[4] + WE(2, 2) * s[2]) - (s[5] * WE(0, 2) + s[4] * WE(1, 2) + s[2] * WE(2, 2));
+    ds[3] = ds[3] + (WE(0, 0) * s[3] + WE(0, 1) * s[1] + WE(0, 2) * s[4]) - (s[0] * WE(0, 1) + s[3] * WE(1, 1) + s[5] * WE(2, 1));
+    ds[4] = ds[4] + (WE(1, 0) * s[5] + WE(1, 1) * s[4] + WE(1, 2) * s[2]) - (s[3] * WE(0, 2) + s[1] * WE(1, 2) + s[4] * WE(2, 2));
+    ds[5] = ds[5] + (WE(0, 0) * s[5] + WE(0, 1) * s[4] + WE(0, 2) * s[2]) - (s[0] * WE(0, 2) + s[3] * WE(1, 2) + s[5] * WE(2, 2));
+#undef WE
+}
+
+// elastic D (only its nonzero pattern is kept: dlam, dmu) -- elastic(),
+// dpmodel1(), dpmodel_bui() share it (:17-59, :301-334, :468-501)
+__device__ __forceinline__ void elastic_consts(const double s[6], double E, double poi, double eps0, double kapa,
+                                               double* dlam, double* dmu, double* sm_out)
+{
+    double sm = (-s[0] + -s[1] + -s[2]) * 0.3333333333;
+    if (sm < 1.0) sm = 1.0;
+    double e0;
+    if (E > 1.0) e0 = E;
+    else e0 = 3 * (1 - 2 * poi) * (1 + eps0) * fabs(sm) / kapa;
+    *dlam = e0 * poi / (1.0 + poi) / (1.0 - 2.0 * poi);
+    *dmu = e0 * 0.5 / (1.0 + poi);
+    *sm_out = sm;
+}
+
+// dsig += D deps, in the reference's dept[ki][kj] * deps[kj] loop order over a
+// dense 6x6 with the zero entries included (0 * x terms keep signed-zero and
+// NaN behaviour identical).
+__device__ __forceinline__ void add_dense(double ds[6], const double D[6][6], const double de[6])
+{
+    for (int a = 0; a < 6; a++)
+        for (int b = 0; b < 6; b++) ds[a] += D[a][b] * de[b];
+}
+
+__device__ __forceinline__ void fill_elastic(double D[6][6], double dlam, double dmu)
+{
+    const double dmu2 = dmu * 2.0;
+    for (int a = 0; a < 6; a++)
+        for (int b = 0; b < 6; b++) D[a][b] = 0.0;
+    D[0][0] = dlam + dmu2; D[1][1] = dlam + dmu2; D[2][2] = dlam + dmu2;
+    D[0][1] = dlam; D[0][2] = dlam; D[1][0] = dlam;
+    D[1][2] = dlam; D[2][0] = dlam; D[2][1] = dlam;
+    D[3][3] = dmu; D[4][4] = dmu; D[5][5] = dmu;
+}
+
+// Drucker-Prager continuum tangent (dpmodel1 / dpmodel_bui, :284-448 /
+// :451-615).  yalf, ykap, yalf_dil are the material constants the reference
+// evaluates with atan/tan/sin/cos each call; they are evaluated once per
+// particle by the host with the same libm calls.
+__device__ __forceinline__ void dp_tangent(double D[6][6], double adps[6], const double s[6], const double de[6],
+                                           double dlam, double dmu, double sm,
+                                           double yalf, double ykap, double yalf_dil)
+{
+    const double dmu2 = dmu * 2.0;
+    double sig0 = -s[0], sig1 = -s[1], sig2 = -s[2];
+    double dx = sig0 - sm, dy = sig1 - sm, dz = sig2 - sm;
+    double dxy = -s[3], dyz = -s[4], dzx = -s[5];
+    double sjj = 0.5 * (dx * dx + dy * dy + dz * dz) + dxy * dxy + dyz * dyz + dzx * dzx;
+    double sj = sqrt(sjj);
+    if ((sj - yalf * sm * 3.0 - ykap) >= 0.0) {
+        double f11 = -yalf + dx / sj * 0.5, f22 = -yalf + dy / sj * 0.5, f33 = -yalf + dz / sj * 0.5;
+        double f12 = dxy / sj * 0.5, f23 = dyz / sj * 0.5, f31 = dzx / sj * 0.5;
+        double fkk = f11 + f22 + f33;
+        double g11 = -yalf_dil + dx / sj * 0.5, g22 = -yalf_dil + dy / sj * 0.5, g33 = -yalf_dil + dz / sj * 0.5;
+        double g12 = dxy / sj * 0.5, g23 = dyz / sj * 0.5, g31 = dzx / sj * 0.5;
+        double hdd = g11 + g22 + g33;
+        double fij = 2.0 * (f11 * g11 + f22 * g22 + f33 * g33) + f12 * g12 + f23 * g23 + f31 * g31;
+        double cc7 = dlam * (fkk * hdd) + dmu * fij + hdd;
+        double dd_ = 1.0 / cc7;
+        double df = dlam * fkk, dg = dlam * hdd;
+        double ramda = (dmu2 * f11 - 3.0 * dlam * yalf) * de[0]
+            + (dmu2 * f22 - 3.0 * dlam * yalf) * de[1]
+            + (dmu2 * f33 - 3.0 * dlam * yalf) * de[2]
+            + dmu * (f12 * de[3] + f23 * de[4] + f31 * de[5]);
+        double ttt = ramda * dd_;
+        if (ttt < 0.0) {
+            double ww[6] = {dg + dmu2 * g11, dg + dmu2 * g22, dg + dmu2 * g33, dmu * g12, dmu * g23, dmu * g31};
+            double zz[6] = {df + dmu2 * f11, df + dmu2 * f22, df + dmu2 * f33, dmu * f12, dmu * f23, dmu * f31};
+            for (int a = 0; a < 6; a++)
+                for (int b = 0; b < 6; b++) D[a][b] = D[a][b] - dd_ * ww[a] * zz[b];
+            adps[0] = ramda * dd_ * f11; adps[1] = ramda * dd_ * f22; adps[2] = ramda * dd_ * f33;
+            adps[3] = ramda * dd_ * f12; adps[4] = ramda * dd_ * f23; adps[5] = ramda * dd_ * f31;
+        }
+    }
+}
+
+// DPModel_check: stress-scaling return onto the cone (:779-819)
+__device__ __forceinline__ void dp_check(const double s[6], double ds[6], double alpha_fai, double k_c, double dt)
+{
+    double ts[6];
+    double sm = (s[0] + s[1] + s[2]) / 3.0;
+    double dx = s[0] - sm, dy = s[1] - sm, dz = s[2] - sm;
+    double sj_2 = 0.5 * (dx * dx + dy * dy + dz * dz) + s[3] * s[3] + s[4] * s[4] + s[5] * s[5];
+    double sj = sqrt(sj_2);
+    for (int a = 0; a < 6; a++) ts[a] = s[a] + ds[a] * dt;
+    double i_1 = ts[0] + ts[1] + ts[2];
+    double rn = (-alpha_fai * i_1 + k_c) / sj;
+    if (rn < 1.0) {
+        ts[0] = rn * (ts[0] - i_1 / 3.0) + i_1 / 3.0;
+        ts[1] = rn * (ts[1] - i_1 / 3.0) + i_1 / 3.0;
+        ts[2] = rn * (ts[2] - i_1 / 3.0) + i_1 / 3.0;
+        ts[3] = rn * ts[3];
+        ts[4] = rn * ts[4];
+        ts[5] = rn * ts[5];
+    }
+    for (int a = 0; a < 6; a++) ds[a] = (ts[a] - s[a]) / dt;
+}
+
+// Particle::deq (Class_particle.cpp:121-143): vsig, veps, divq, divr
+__device__ __forceinline__ void deq(const double s[6], const double ep[6], double* vsig, double* veps,
+                                    double* divq, double* divr)
+{
+    *veps = ep[0] + ep[1] + ep[2];
+    double vs = (s[0] + s[1] + s[2]) / 3;
+    double sxx = s[0] - vs, syy = s[1] - vs, szz = s[2] - vs;
+    double j2 = 0.5 * (sxx * sxx + syy * syy + szz * szz) + s[3] * s[3] + s[4] * s[4] + s[5] * s[5];
+    double q = sqrt(3 * fabs(j2));
+    *vsig = vs;
+    *divq = q;
+    *divr = (vs != 0.0) ? fabs(q / vs) : 0.0;
+}
+
+// Particle::shearstrain (Class_particle.cpp:175-192)
+__device__ __forceinline__ double shearstrain(const double ep[6], double veps)
+{
+    double sxx = ep[0] - veps / 3.0, syy = ep[1] - veps / 3.0, szz = ep[2] - veps / 3.0;
+    double j2 = 0.5 * (sxx * sxx + syy * syy + szz * szz) + ep[3] * ep[3] + ep[4] * ep[4] + ep[5] * ep[5];
+    return sqrt(2.0 * fabs(j2));
+}
+
+// eejcb Jacobi rotations, eps = 1e-3, at most 7 (CPP_7-1-strain.cpp:341-437);
+// returns the diagonal (principal stresses strep).
+__device__ __forceinline__ void eig3(const double s[6], double strep[3])
+{
+    double a[9] = {s[0], s[3], s[5], s[3], s[1], s[4], s[5], s[4], s[2]};
+    const int n = 3;
+    int p = 0, q = 0, l = 1;
+    while (true) {
+        double fm = 0.0;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                double dd_ = fabs(a[i * n + j]);
+                if ((i != j) && (dd_ > fm)) { fm = dd_; p = i; q = j; }
+            }
+        if (fm < 0.001) break;
+        if (l > 7) break;
+        l = l + 1;
+        int u = p * n + q, w = p * n + p, t = q * n + p, sidx = q * n + q;
+        double x = -a[u];
+        double y = (a[sidx] - a[w]) / 2.0;
+        double omega = x / sqrt(x * x + y * y);
+        if (y < 0.0) omega = -omega;
+        double sn = 1.0 + sqrt(1.0 - omega * omega);
+        sn = omega / sqrt(2.0 * sn);
+        double cn = sqrt(1.0 - sn * sn);
+        fm = a[w];
+        a[w] = fm * cn * cn + a[sidx] * sn * sn + a[u] * omega;
+        a[sidx] = fm * sn * sn + a[sidx] * cn * cn - a[u] * omega;
+        a[u] = 0.0;
+        a[t] = 0.0;
+        for (int j = 0; j < n; j++)
+            if ((j != p) && (j != q)) {
+                int uu = p * n + j, ww = q * n + j;
+                fm = a[uu];
+                a[uu] = fm * cn + a[ww] * sn;
+                a[ww] = -fm * sn + a[ww] * cn;
+            }
+        for (int i = 0; i < n; i++)
+            if ((i != p) && (i != q)) {
+                int uu = i * n + p, ww = i * n + q;
+                fm = a[uu];
+                a[uu] = fm * cn + a[ww] * sn;
+                a[ww] = -fm * sn + a[ww] * cn;
+            }
+    }
+    strep[0] = a[0]; strep[1] = a[4]; strep[2] = a[8];
+}
+
+// strain_noreg (CPP_7-1-strain.cpp:20-220), the gathered pore pressures and
+// wall stresses of eos (CPP_7-1-eos_CR.cpp:46-177), cal_permeability
+// (CPP_7-2-constitutive.cpp:355-382), strain_to_stress (:13-321),
+// free_surface_check (:453-506) and Stress_eigValue (CPP_7-1-strain.cpp:283-332).
+// The three neighbour sums share one pass over the list, each in list order.
+// Reads sig (stresses of the previous step), writes sig_next.
+__global__ void __launch_bounds__(128) k_strain_stress(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    const int ti = d.s.type[i], nd = d.p.ndim, nn = nbr_count(d, i), l = *d.s.step;
+    const double dt = d.p.dt;
+    double ep[6], s[6];
+    for (int k = 0; k < 6; k++) { ep[k] = d.s.eps[k * N + i]; s[k] = d.s.sig[k * N + i]; }
+    if (l == d.p.inip)
+        for (int k = 0; k < 6; k++) ep[k] = 0.0;
+    double vi[3], xi[3];
+    for (int k = 0; k < 3; k++) { vi[k] = d.s.vxp[k * N + i]; xi[k] = d.s.xp[k * N + i]; }
+    const bool solid = (ti == 2 || ti == 4);
+    const bool moving = (ti >= 1 && ti <= 4);
+    double up[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, down[3] = {0, 0, 0};
+    double u1 = 0, u2 = 0, u3 = 0, u4 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0;
+    double us[6] = {0, 0, 0, 0, 0, 0}, dsw = 0;
+    double color = 0.0;
+    for (int q = 0; q < nn; q++) {
+        const int j = d.s.nbr[(size_t)q * N + i];
+        const int tj = d.s.type[j];
+        const bool same = (ti == tj && ti != 7 && ti != 0);
+        const bool wallj = (moving && tj == 0);
+        const bool gath = (ti != tj) && ((ti == 2 || ti == 4 || ti == 0) && (tj == 1 || tj == 3 || (ti == 0 && tj == 2)));
+        if (!(same || wallj || gath)) continue;
+        double w[4];
+        sph_pair_w(d, i, j, w);
+        const double mj = d.s.mass[j], rj = d.s.rho[j];
+        if (same || wallj) {
+            double dvx[3];
+            for (int k = 0; k < 3; k++) {
+                double vj = same ? d.s.vxp[k * N + j] : ((d.p.flbndy == 1) ? vi[k] : 0.0);
+                dvx[k] = vi[k] - vj;
+            }
+            up[0] = up[0] + mj / rj * dvx[0] * w[0];
+            up[1] = up[1] + mj / rj * dvx[0] * w[1];
+            up[2] = up[2] + mj / rj * dvx[0] * w[2];
+            up[3] = up[3] + mj / rj * dvx[1] * w[0];
+            up[4] = up[4] + mj / rj * dvx[1] * w[1];
+            up[5] = up[5] + mj / rj * dvx[1] * w[2];
+            up[6] = up[6] + mj / rj * dvx[2] * w[0];
+            up[7] = up[7] + mj / rj * dvx[2] * w[1];
+            up[8] = up[8] + mj / rj * dvx[2] * w[2];
+            if (solid) {
+                down[0] = down[0] + mj / rj * (xi[0] - d.s.xp[0 * N + j]) * w[0];
+                down[1] = down[1] + mj / rj * (xi[1] - d.s.xp[1 * N + j]) * w[1];
+                down[2] = down[2] + mj / rj * (xi[2] - d.s.xp[2 * N + j]) * w[2];
+            }
+            color = color + mj / rj * 1.0 * w[3];
+        }
+        if (gath) {
+            const double w3 = w[3];
+            if (ti == 2 && tj == 1) { u1 = u1 + mj * d.s.pre[j] * w3 / rj; d1 = d1 + mj * w3 / rj; }
+            if (ti == 2 && tj == 3) { u2 = u2 + mj * d.s.pre[j] * w3 / rj; d2 = d2 + mj * w3 / rj; }
+            if (ti == 4 && tj == 1) { u3 = u3 + mj * d.s.pre[j] * w3 / rj; d3 = d3 + mj * w3 / rj; }
+            if (ti == 4 && tj == 3) { u4 = u4 + mj * d.s.pre[j] * w3 / rj; d4 = d4 + mj * w3 / rj; }
+            if (ti == 0 && tj == 1) { u1 = u1 + mj * d.s.pre[j] * w3 / rj; d1 = d1 + mj * w3 / rj; }
+            if (ti == 0 && tj == 3) { u2 = u2 + mj * d.s.pre[j] * w3 / rj; d2 = d2 + mj * w3 / rj; }
+            if (ti == 0 && tj == 2) {
+                for (int k = 0; k < 6; k++) us[k] = us[k] + mj * d.s.sig[k * N + j] * w3 / rj;
+                dsw = dsw + mj * w3 / rj;
+            }
+        }
+    }
+    // velocity gradient (:148-181), strain rate and spin (:183-218)
+    double dv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (ti == 1 || ti == 3) {
+        for (int k = 0; k < 9; k++) dv[k] = up[k];
+    } else {
+        if (fabs(down[0]) > 1.0e-7) { dv[0] = up[0] / down[0]; dv[3] = up[3] / down[0]; dv[6] = up[6] / down[0]; }
+        if (fabs(down[1]) > 1.0e-7) { dv[1] = up[1] / down[1]; dv[4] = up[4] / down[1]; dv[7] = up[7] / down[1]; }
+        if (fabs(down[2]) > 1.0e-7) { dv[2] = up[2] / down[2]; dv[5] = up[5] / down[2]; dv[8] = up[8] / down[2]; }
+    }
+    double de[6] = {dv[0], dv[4], dv[8], dv[1] + dv[3], dv[5] + dv[7], dv[6] + dv[2]};
+    double we[9] = {0.0, 0.5 * (dv[1] - dv[3]), 0.5 * (dv[2] - dv[6]),
+                    0.5 * (dv[3] - dv[1]), 0.0, 0.5 * (dv[5] - dv[7]),
+                    0.5 * (dv[6] - dv[2]), 0.5 * (dv[7] - dv[5]), 0.0};
+    if (nd == 2) {
+        de[2] = 0.0; de[4] = 0.0; de[5] = 0.0;
+        we[2] = 0.0; we[5] = 0.0; we[6] = 0.0; we[7] = 0.0; we[8] = 0.0;
+    }
+    // gathered pressures (eos :122-176)
+    if (ti == 2 || ti == 0) {
+        d.s.prew[i] = (d1 != 0.0) ? u1 / d1 : u1;
+        d.s.prea[i] = (d2 != 0.0) ? u2 / d2 : u2;
+        if (ti == 0)
+            for (int k = 0; k < 6; k++) s[k] = (dsw != 0.0) ? us[k] / dsw : us[k];
+    } else if (ti == 4) {
+        d.s.prew[i] = (d3 != 0.0) ? u3 / d3 : u3;
+        d.s.prea[i] = (d4 != 0.0) ? u4 / d4 : u4;
+    }
+    // permeability (fli == 1)
+    if (d.p.fli == 1 && ti == 2) {
+        double cop = d.s.cop[i];
+        const int pt = d.p.permtype;
+        if (pt == 0) cop = d.s.s_cop[i];
+        else if (pt == 1) cop = d.p.pers;
+        else if (pt == 2) {
+            double sitas = d.s.s_sitas[i], sitar = d.s.s_sitar[i], sat = d.s.satu[i];
+            if (sat < sitar) cop = d.p.pers;
+            else if (sat > sitas) cop = d.p.perl;
+            else cop = (d.p.perl - d.p.pers) * sat / (sitas - sitar) + d.p.pers;
+        } else if (pt == 3) {
+            const int pm = d.s.permtype[i];
+            if (pm == 1) cop = d.p.pers;
+            if (pm == 2) cop = d.p.perm;
+            if (pm == 3) cop = d.p.perl;
+        }
+        d.s.cop[i] = cop;
+    }
+    // strain_to_stress
+    double vsig = 0, veps = 0, divq = 0, divr = 0, meps = 0;
+    bool have_deq = false;
+    if (ti == 1 || ti == 3) {
+        double viscos1 = d.s.f_vis[i];
+        if (ti == 1) {
+            const double smin = d.s.f_smin[i];
+            double depsmax = (de[0] + de[1] + de[2]) / 3.0;
+            ep[0] = de[0] - depsmax;
+            ep[1] = de[1] - depsmax;
+            ep[2] = de[2] - depsmax;
+            depsmax = 0.666666666666667 * (ep[0] * ep[0] + ep[1] * ep[1]
+                + ep[2] * ep[2] + de[3] * de[3] * 0.25 +
+                de[4] * de[4] * 0.25 + de[5] * de[5] * 0.25);
+            depsmax = sqrt(depsmax);
+            if (d.s.f_bhtype[i] == 1) {
+                double tao = d.s.pre[i] * d.s.f_tanfai[i] + d.s.f_c[i];
+                if (depsmax < smin) viscos1 = d.s.f_vis[i] + tao / smin;
+                else viscos1 = d.s.f_vis[i] + tao / depsmax;
+            }
+        }
+        double dd_[6];
+        dd_[0] = 2.0 * de[0] - 2.0 * (de[0] + de[1] + de[2]) / 3.0;
+        dd_[1] = 2.0 * de[1] - 2.0 * (de[0] + de[1] + de[2]) / 3.0;
+        dd_[2] = 2.0 * de[2] - 2.0 * (de[0] + de[1] + de[2]) / 3.0;
+        dd_[3] = de[3]; dd_[4] = de[4]; dd_[5] = de[5];
+        const double pr = d.s.pre[i];
+        for (int a = 0; a < 6; a++) s[a] = (a < 3) ? -pr - viscos1 * dd_[a] : -viscos1 * dd_[a];
+    } else if (ti == 2 || ti == 4) {
+        double D[6][6], adps[6] = {0, 0, 0, 0, 0, 0}, ds[6] = {0, 0, 0, 0, 0, 0};
+        double dlam, dmu, sm;
+        const int mt = d.s.matype[i] % 10;
+        const bool dp = (ti == 2) && !(l < d.p.inip) && (mt == 2 || mt == 5);
+        if (ti == 2) {
+            elastic_consts(s, d.s.s_e[i], d.s.s_poi[i], d.s.s_eps0[i], d.s.s_kapa[i], &dlam, &dmu, &sm);
+        } else {
+            const double e0 = d.p.st_e, poi = d.p.st_poi;
+            dlam = e0 * poi / (1.0 + poi) / (1.0 - 2.0 * poi);
+            dmu = e0 * 0.5 / (1.0 + poi);
+            sm = 0.0;
+        }
+        fill_elastic(D, dlam, dmu);
+        if (dp) dp_tangent(D, adps, s, de, dlam, dmu, sm, d.s.s_yalf[i], d.s.s_ykap[i], (mt == 5) ? d.s.s_yalf_dil[i] : 0.0);
+        add_dense(ds, D, de);
+        if (dp) dp_check(s, ds, d.s.s_yalf[i], d.s.s_ykap[i], dt);
+        jaumann(ds, s, we);
+        if (ti == 2) {
+            for (int a = 0; a < 6; a++) {
+                double ad = d.s.adps[a * N + i];
+                d.s.adps[a * N + i] = ad + adps[a] * dt;
+                ep[a] = ep[a] + de[a] * dt;
+                s[a] = s[a] + ds[a] * dt + 0.0;
+            }
+        } else {
+            for (int a = 0; a < 6; a++) {
+                ep[a] = ep[a] + de[a] * dt;
+                s[a] = s[a] + ds[a] * dt;
+            }
+        }
+        deq(s, ep, &vsig, &veps, &divq, &divr);
+        meps = shearstrain(ep, veps);
+        have_deq = true;
+        // poro_cal (Class_particle.cpp:194-203)
+        double e = d.s.e[i];
+        double dE = (1 + e) * (de[0] + de[1] + de[2]) * dt;
+        double et = e + dE;
+        if (et < 0.0) et = 0.0;
+        d.s.porosity[i] = et / (1 + et);
+        d.s.e[i] = et;
+    }
+    // free_surface_check (:453-506)
+    const double tmax = d.p.thr_max, tmin = d.p.thr_min, incline = tmax - tmin;
+    if (ti == 1) {
+        if (color < tmin / 2.0) {
+            s[0] = s[1] = s[2] = -1.0;
+            s[3] = s[4] = s[5] = 0.0;
+        } else if (color >= tmin / 2.0 && color < tmax / 2.0) {
+            double xishu = (2.0 * color - tmin) / incline;
+            for (int k = 0; k < 6; k++) s[k] = xishu * s[k];
+        }
+    } else if (ti == 2) {
+        if (color < tmin) {
+            s[0] = s[1] = s[2] = -1.0;
+            s[3] = s[4] = s[5] = 0.0;
+        } else if (color >= tmin && color < tmax) {
+            double xishu = (color - tmin) / incline * 1.0;
+            for (int k = 0; k < 6; k++) s[k] = xishu * s[k];
+        }
+        // Particle::stress_adjust (Class_particle.cpp:205-215) on the vsig of the last deq
+        if (vsig > 0.0) {
+            double temp = -vsig;
+            s[0] = s[0] + temp; s[1] = s[1] + temp; s[2] = s[2] + temp;
+            s[3] = 0.0; s[4] = 0.0; s[5] = 0.0;
+        }
+        deq(s, ep, &vsig, &veps, &divq, &divr);
+    }
+    if (have_deq || ti == 2) {
+        d.s.vsig[i] = vsig; d.s.veps[i] = veps; d.s.divq[i] = divq; d.s.divr[i] = divr;
+        d.s.meps[i] = meps;
+    }
+    double sp[3];
+    eig3(s, sp);
+    for (int k = 0; k < 3; k++) d.s.strep[k * N + i] = sp[k];
+    for (int k = 0; k < 6; k++) {
+        d.s.sig_next[k * N + i] = s[k];
+        d.s.eps[k * N + i] = ep[k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// symmetric stress-divergence pair term (CPP_9-4-derivation_stress.cpp:55-65)
+__device__ __forceinline__ void stress_pair(double tu[3][3], double mj, const double aj[6], const double ai[6],
+                                            double rj, double ri, const double w[4], bool plus)
+{
+    if (plus) {
+        tu[0][0] = tu[0][0] + mj * (aj[0] / rj / rj + ai[0] / ri / ri) * w[0];
+        tu[0][1] = tu[0][1] + mj * (aj[3] / rj / rj + ai[3] / ri / ri) * w[1];
+        tu[0][2] = tu[0][2] + mj * (aj[5] / rj / rj + ai[5] / ri / ri) * w[2];
+        tu[1][0] = tu[1][0] + mj * (aj[3] / rj / rj + ai[3] / ri / ri) * w[0];
+        tu[1][1] = tu[1][1] + mj * (aj[1] / rj / rj + ai[1] / ri / ri) * w[1];
+        tu[1][2] = tu[1][2] + mj * (aj[4] / rj / rj + ai[4] / ri / ri) * w[2];
+        tu[2][0] = tu[2][0] + mj * (aj[5] / rj / rj + ai[5] / ri / ri) * w[0];
+        tu[2][1] = tu[2][1] + mj * (aj[4] / rj / rj + ai[4] / ri / ri) * w[1];
+        tu[2][2] = tu[2][2] + mj * (aj[2] / rj / rj + ai[2] / ri / ri) * w[2];
+    } else {
+        tu[0][0] = tu[0][0] + mj * (aj[0] / rj / rj - ai[0] / ri / ri) * w[0];
+        tu[0][1] = tu[0][1] + mj * (aj[3] / rj / rj - ai[3] / ri / ri) * w[1];
+        tu[0][2] = tu[0][2] + mj * (aj[5] / rj / rj - ai[5] / ri / ri) * w[2];
+        tu[1][0] = tu[1][0] + mj * (aj[3] / rj / rj - ai[3] / ri / ri) * w[0];
+        tu[1][1] = tu[1][1] + mj * (aj[1] / rj / rj - ai[1] / ri / ri) * w[1];
+        tu[1][2] = tu[1][2] + mj * (aj[4] / rj / rj - ai[4] / ri / ri) * w[2];
+        tu[2][0] = tu[2][0] + mj * (aj[5] / rj / rj - ai[5] / ri / ri) * w[0];
+        tu[2][1] = tu[2][1] + mj * (aj[4] / rj / rj - ai[4] / ri / ri) * w[1];
+        tu[2][2] = tu[2][2] + mj * (aj[2] / rj / rj - ai[2] / ri / ri) * w[2];
+    }
+}
+
+// fluid_acceleration_water/air (+ minor forms), soil_acceleration_noreg,
+// structure_acceleration_noreg (CPP_9-4-derivation_stress.cpp:12-505),
+// artificial_viscosity (CPP_9-3-artificialvis.cpp:12-99),
+// boundary_moving_stress_effect (CPP_9-4:631-721), interact1
+// (CPP_10-interact1.cpp:15-110) and veocity_update (CPP_11-xsph.cpp:11-142):
+// one pass over the neighbour list with one accumulator set per sum, combined
+// afterwards in the reference's call order.  Writes ax, interf, interfss and
+// the updated velocity into vmid (state vx of the reference before XSPH).
+__global__ void __launch_bounds__(128) k_accel(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    const int ti = d.s.type[i], nd = d.p.ndim, nn = nbr_count(d, i);
+    const double g[3] = {d.p.gx, d.p.gy, d.p.gz};
+    double si[6];
+    for (int k = 0; k < 6; k++) si[k] = d.s.sig_next[k * N + i];
+    const double ri = d.s.rho[i];
+    double vi[3], xi[3];
+    for (int k = 0; k < 3; k++) { vi[k] = d.s.vxp[k * N + i]; xi[k] = d.s.xp[k * N + i]; }
+    const bool fluid = (ti == 1 || ti == 3);
+    const int other = (ti == 1) ? 3 : 1;
+    const bool minor = (ti == 1) ? d.p.water_minor : d.p.air_minor;
+    const bool moving = (ti >= 1 && ti <= 4);
+    double tf[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};   // stress divergence
+    double tb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};   // wall stress
+    double tav[3] = {0, 0, 0}, tin[3] = {0, 0, 0}, tdm[3] = {0, 0, 0};
+    const bool damping = (*d.s.step <= d.p.inip) && (ti == 2 || ti == 4);
+    const double cdi = damping ? d.s.cd[i] : 0.0;
+    // artificial viscosity coefficients of particle i
+    double ca = 0.0, aa = 0.0, bb = 0.0;
+    if (ti == 1) { ca = d.s.f_vpu[i]; aa = d.p.av[0][0]; bb = d.p.av[0][1]; }
+    if (ti == 2) { ca = d.s.s_vpu[i]; aa = d.p.av[1][0]; bb = d.p.av[1][1]; }
+    if (ti == 3) { ca = d.s.f_vpu[i]; aa = d.p.av[2][0]; bb = d.p.av[2][1]; }
+    // wall-stress operand of particle i (:668-700)
+    double ab[6] = {0, 0, 0, 0, 0, 0};
+    if (fluid) {
+        for (int k = 0; k < 6; k++) ab[k] = si[k];
+    } else if (ti == 2 || ti == 4) {
+        const double satu = d.s.satu[i], pw = d.s.prew[i], pa = d.s.prea[i];
+        ab[0] = si[0] - satu * pw + (1 - satu) * pa;
+        ab[1] = si[1] - satu * pw + (1 - satu) * pa;
+        ab[2] = si[2] - satu * pw + (1 - satu) * pa;
+        ab[3] = si[3]; ab[4] = si[4]; ab[5] = si[5];
+    }
+    const double poro_f = fluid ? d.s.f_por[i] : 0.0;
+    const double poro_s = (ti == 2) ? d.s.s_por[i] : 0.0;
+    const double dens_s = (ti == 2) ? d.s.s_dens[i] : 0.0;
+    for (int q = 0; q < nn; q++) {
+        const int j = d.s.nbr[(size_t)q * N + i];
+        const int tj = d.s.type[j];
+        const bool f_pair = fluid && (tj == ti || tj == other);
+        const bool s_pair = (ti == 2 || ti == 4) && tj == ti;
+        const bool av_pair = (ti == tj && ti != 7);
+        const bool b_pair = moving && tj == 0;
+        const bool in_pair = d.p.fli == 1 && ti != tj;
+        const bool dm_pair = damping && tj == ti;
+        if (!(f_pair || s_pair || av_pair || b_pair || in_pair || dm_pair)) continue;
+        double w[4];
+        sph_pair_w(d, i, j, w);
+        const double mj = d.s.mass[j], rj = d.s.rho[j];
+        if (f_pair) {
+            double ai[6], aj[6];
+            for (int k = 0; k < 6; k++) { ai[k] = poro_f * si[k]; aj[k] = poro_f * d.s.sig_next[k * N + j]; }
+            stress_pair(tf, mj, aj, ai, rj, ri, w, !minor);
+        }
+        if (s_pair) {
+            double sj[6];
+            for (int k = 0; k < 6; k++) sj[k] = d.s.sig_next[k * N + j];
+            const double satu = d.s.satu[j];
+            stress_pair(tf, mj, sj, si, rj, ri, w, true);
+            if (ti == 2) {
+                const double pi_ = (1 - poro_s) * (-satu * d.s.prew[i] + (1 - satu) * d.s.prea[i]);
+                const double pj_ = (1 - poro_s) * (-satu * d.s.prew[j] + (1 - satu) * d.s.prea[j]);
+                tf[0][0] = tf[0][0] + mj * (pj_ / rj / rj + pi_ / dens_s / dens_s) * w[0];
+                tf[1][1] = tf[1][1] + mj * (pj_ / rj / rj + pi_ / dens_s / dens_s) * w[1];
+                tf[2][2] = tf[2][2] + mj * (pj_ / rj / rj + pi_ / dens_s / dens_s) * w[2];
+            } else {
+                const double pi_ = -satu * d.s.prew[i] + (1 - satu) * d.s.prea[i];
+                const double pj_ = -satu * d.s.prew[j] + (1 - satu) * d.s.prea[j];
+                tf[0][0] = tf[0][0] + mj * (pj_ / rj / rj - pi_ / ri / ri) * w[0];
+                tf[1][1] = tf[1][1] + mj * (pj_ / rj / rj - pi_ / ri / ri) * w[1];
+                tf[2][2] = tf[2][2] + mj * (pj_ / rj / rj - pi_ / ri / ri) * w[2];
+            }
+        }
+        if (av_pair) {
+            double inprod = 0.0, dst = 0.0, dx[3];
+            for (int k = 0; k < nd; k++) {
+                double dvx = vi[k] - d.s.vxp[k * N + j];
+                dx[k] = xi[k] - d.s.xp[k * N + j];
+                dst = dst + dx[k] * dx[k];
+                inprod = inprod + dvx * dx[k];
+            }
+            const double hl = (d.s.hl[j] + d.s.hl[i]) * 0.5;
+            const double rou = (rj + ri) * 0.5;
+            double paix;
+            if (inprod < 0.0) {
+                dst = sqrt(dst);
+                double myu = hl * inprod / (dst * dst + 0.01 * hl * hl);
+                paix = (-aa * ca * myu + bb * myu * myu) / rou;
+            } else
+                paix = 0.0;
+            for (int k = 0; k < nd; k++) tav[k] = tav[k] + mj * paix * w[k];
+        }
+        if (b_pair) stress_pair(tb, mj, ab, ab, rj, ri, w, true);
+        if (dm_pair)
+            for (int k = 0; k < nd; k++)
+                tdm[k] = tdm[k] + mj / rj * cdi * (vi[k] - d.s.vxp[k * N + j]) * w[3];
+        if (in_pair) {
+            double inprod = 0.0, dvx[3];
+            for (int k = 0; k < nd; k++) {
+                double dxk = xi[k] - d.s.xp[k * N + j];
+                dvx[k] = vi[k] - d.s.vxp[k * N + j];
+                inprod = inprod + dxk * dvx[k];
+            }
+            if (inprod < 0) {
+                const double w3 = w[3], ga = d.p.g_acc;
+                if (ti == 2 && tj == 1) {
+                    const double sa = d.s.satu[i], po = d.s.porosity[i], cp = d.s.cop[i], fd = d.s.f_dens[j];
+                    for (int k = 0; k < nd; k++)
+                        tin[k] = tin[k] + sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3;
+                } else if (ti == 1 && tj == 2) {
+                    const double sa = d.s.satu[j], po = d.s.porosity[j], cp = d.s.cop[j], fd = d.s.f_dens[i];
+                    for (int k = 0; k < nd; k++)
+                        tin[k] = tin[k] + sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3;
+                } else if (ti == 2 && tj == 3) {
+                    const double sa = d.s.satu[i], po = d.s.porosity[i], fd = d.s.f_dens[j];
+                    for (int k = 0; k < nd; k++)
+                        tin[k] = tin[k] + (1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3;
+                } else if (ti == 3 && tj == 2) {
+                    const double sa = d.s.satu[j], po = d.s.porosity[j], fd = d.s.f_dens[i];
+                    for (int k = 0; k < nd; k++)
+                        tin[k] = tin[k] + (1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3;
+                }
+            }
+        }
+    }
+    double ax[3];
+    for (int k = 0; k < 3; k++) ax[k] = d.s.ax[k * N + i];
+    if (ti >= 1 && ti <= 4) {
+        for (int k = 0; k < 3; k++) ax[k] = g[k];
+        ax[0] += tf[0][0] + tf[0][1] + tf[0][2];
+        ax[1] += tf[1][0] + tf[1][1] + tf[1][2];
+        ax[2] += tf[2][0] + tf[2][1] + tf[2][2];
+    }
+    if (ti != 7)
+        for (int k = 0; k < nd; k++) ax[k] = ax[k] - tav[k];
+    if (moving) {
+        ax[0] += tb[0][0] + tb[0][1] + tb[0][2];
+        ax[1] += tb[1][0] + tb[1][1] + tb[1][2];
+        ax[2] += tb[2][0] + tb[2][1] + tb[2][2];
+    }
+    const double dt = d.p.dt;
+    double axp[3];
+    for (int k = 0; k < 3; k++) axp[k] = d.s.axp[k * N + i];
+    if (d.p.fli == 1 && moving) {
+        const double xishu = d.p.interc;
+        for (int k = 0; k < nd; k++) {
+            double itf = tin[k];
+            double vx1 = vi[k] + 0.5 * (axp[k] + ax[k]) * dt;
+            double vx2 = vi[k] + 0.5 * (axp[k] + ax[k] - itf * xishu / ri) * dt;
+            if (vx1 * vx2 <= 0.0) {
+                itf = 0.0;
+                ax[k] = -2.0 * vi[k] / dt - axp[k];
+            } else
+                ax[k] -= itf * xishu / ri;
+            d.s.interf[k * N + i] = itf;
+        }
+    }
+    // soil_damping_geostress while l <= inip (CPP_9-4-derivation_stress.cpp:849-896)
+    if (damping) {
+        for (int k = 0; k < nd; k++) {
+            double vx1 = vi[k] + 0.5 * (axp[k] + ax[k]) * dt;
+            double vx2 = vi[k] + 0.5 * (axp[k] + ax[k] - tdm[k]) * dt;
+            if (vx1 * vx2 <= 0.0) ax[k] = -2.0 * vi[k] / dt - axp[k];
+            else ax[k] -= tdm[k];
+        }
+    }
+    // veocity_update, if_move 0 and 1
+    double vout[3];
+    for (int k = 0; k < 3; k++) vout[k] = d.s.vx[k * N + i];
+    const int mt = d.s.matype[i];
+    if (d.p.if_move == 0) {
+        if (ti == 0 && mt < 2) {
+            for (int k = 0; k < nd; k++) {
+                d.s.interf[k * N + i] = 0.0;
+                double ath = (0.0 + 0.0) * 0.5;
+                d.s.interfss[k * N + i] = d.s.interfss[k * N + i] + ath * dt;
+            }
+        } else if (ti == 0 && (mt == 3 || (mt == 5 && d.p.flv == 1))) {
+            for (int k = 0; k < nd; k++) {
+                double itf = d.s.interf[k * N + i];
+                double ath = (itf + itf) * 0.5;
+                d.s.interfss[k * N + i] = d.s.interfss[k * N + i] + ath * dt;
+            }
+        } else if (ti != 0) {
+            for (int k = 0; k < nd; k++) {
+                double ath = (axp[k] + ax[k]) * 0.5;
+                vout[k] = vi[k] + ath * dt;
+            }
+        }
+    } else {   // if_move == 1 (2 and 3 are rejected at create)
+        if (ti == 0 && mt == 2 && *d.s.step > d.p.inip) {
+            for (int k = 0; k < nd; k++) d.s.interfss[k * N + i] = d.p.move_vx[k];
+        } else if (ti == 0) {
+            for (int k = 0; k < nd; k++) d.s.interfss[k * N + i] = 0.0;
+        } else {
+            for (int k = 0; k < nd; k++) {
+                double ath = (axp[k] + ax[k]) * 0.5;
+                vout[k] = vi[k] + ath * dt;
+            }
+        }
+    }
+    for (int k = 0; k < 3; k++) {
+        d.s.ax[k * N + i] = ax[k];
+        d.s.vx_next[k * N + i] = vout[k];   // velocity before XSPH
+    }
+}
+
+// xsph (CPP_11-xsph.cpp:145-256, Jacobi by construction: reads the velocities
+// before XSPH), tmboundary (CPP_13-boundary.cpp:125-177), check_domain
+// (CPP_13-boundary.cpp:20-68) and update (CPP_12-1-update.cpp:11-55).
+// Reads xp / vx_next, writes xp_next / vx.
+__global__ void __launch_bounds__(128) k_xsph_update(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    const int ti = d.s.type[i], nd = d.p.ndim, nn = nbr_count(d, i);
+    const double dt = d.p.dt;
+    double vm[3], xi[3];
+    for (int k = 0; k < 3; k++) { vm[k] = d.s.vx_next[k * N + i]; xi[k] = d.s.xp[k * N + i]; }
+    const bool moving = (ti >= 1 && ti <= 4);
+    double vn[3] = {vm[0], vm[1], vm[2]};
+    if (d.p.if_move != 2 && moving) {
+        double tu[3] = {0, 0, 0}, down = 0.0;
+        for (int q = 0; q < nn; q++) {
+            const int j = d.s.nbr[(size_t)q * N + i];
+            const int tj = d.s.type[j];
+            double xishu;
+            if (ti == tj) {
+                xishu = (ti == 1) ? d.p.xsph0 : (ti == 3) ? d.p.xsph2 : d.p.xsph1;
+            } else if (tj == 0) {
+                xishu = (ti == 1 || ti == 3) ? 0.006 : d.p.xsph1 / 5.0;
+            } else {
+                continue;
+            }
+            double w[4];
+            sph_pair_w(d, i, j, w);
+            const double mj = d.s.mass[j], rj = d.s.rho[j];
+            for (int k = 0; k < nd; k++)
+                tu[k] = tu[k] + xishu * mj * (d.s.vx_next[k * N + j] - vm[k]) * w[3] / rj;
+            down = down + mj * w[3] / rj;
+        }
+        if (fabs(down) > 1.0e-7 && (ti == 2 || ti == 4))
+            for (int k = 0; k < nd; k++) vn[k] = vm[k] + tu[k] / down;
+        else
+            for (int k = 0; k < nd; k++) vn[k] = vm[k] + tu[k];
+    }
+    if (moving && d.p.flbndy == 1) {
+        const double a = 0.30, b = 0.30, dr = d.p.dr;
+        double tb[3] = {0, 0, 0};
+        for (int q = 0; q < nn; q++) {
+            const int j = d.s.nbr[(size_t)q * N + i];
+            if (d.s.type[j] != 0) continue;
+            double inprod = 0.0, dst = 0.0;
+            for (int k = 0; k < nd; k++) {
+                const double xj = d.s.xp[k * N + j];
+                inprod = inprod + (vn[k] - d.s.interfss[k * N + j]) * (xi[k] - xj);
+                dst = dst + (xi[k] - xj) * (xi[k] - xj);
+            }
+            if (inprod < 0.0) {
+                dst = sqrt(dst);
+                const double db = a * dr;
+                double beta = 1 + db / (dst - b * dr);
+                beta = fmin(1.5, beta);
+                for (int k = 0; k < nd; k++)
+                    tb[k] = tb[k] + (1 - beta) * (xi[k] - d.s.xp[k * N + j]) * inprod / dst / dst;
+            }
+        }
+        for (int k = 0; k < nd; k++) vn[k] = vn[k] + tb[k];
+    }
+    if (ti != 0 && ti != 7) {
+        const double dr = d.p.dr;
+        const double bmax[3] = {d.p.xmax, d.p.ymax, d.p.zmax}, bmin[3] = {d.p.xmin, d.p.ymin, d.p.zmin};
+        bool hit = false;
+        if (xi[0] - bmax[0] >= -0.5 * dr) hit = true;
+        if (xi[0] - bmin[0] <= 0.5 * dr) hit = true;
+        if (xi[1] - bmax[1] >= -0.5 * dr) hit = true;
+        if (xi[1] - bmin[1] <= 0.5 * dr) hit = true;
+        if (xi[2] - bmax[2] >= -0.5 * dr && nd == 3) hit = true;
+        if (xi[2] - bmin[2] <= 0.5 * dr && nd == 3) hit = true;
+        if (hit) {
+            const int w0 = d.p.first_vbx_wall;
+            for (int k = 0; k < 3; k++) vn[k] = (i > w0) ? d.s.interfss[k * N + w0] : 0.0;
+        }
+    }
+    // update
+    const int loop = *d.s.step - d.p.inip;
+    double xn[3] = {xi[0], xi[1], xi[2]};
+    if (ti != 0) {
+        for (int k = 0; k < nd; k++) {
+            const double vp = d.s.vxp[k * N + i];
+            xn[k] = xi[k] + (vn[k] + vp) * dt * 0.5;
+            double u = d.s.ux[k * N + i];
+            u = (loop == 0) ? 0.0 : u + (vn[k] + vp) * dt * 0.5;
+            d.s.ux[k * N + i] = u;
+            d.s.vxp[k * N + i] = vn[k];
+            d.s.axp[k * N + i] = d.s.ax[k * N + i];
+        }
+        if (nd > 0) d.s.rhop[i] = d.s.rho[i];
+    } else {
+        const int mt = d.s.matype[i];
+        if (mt == 2 || mt == 3 || mt == 4 || mt == 5) {
+            for (int k = 0; k < nd; k++) {
+                const double its = d.s.interfss[k * N + i];
+                xn[k] = xi[k] + (its + its) * dt * 0.5;
+                d.s.ux[k * N + i] = d.s.ux[k * N + i] + (its + its) * dt * 0.5;
+            }
+            d.s.rhop[i] = d.s.rho[i];
+            d.s.prep[i] = d.s.pre[i];
+        }
+    }
+    for (int k = 0; k < 3; k++) {
+        d.s.xp_next[k * N + i] = xn[k];
+        d.s.vx[k * N + i] = vn[k];
+    }
+}
+
+__global__ void k_step_done(Dev d)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0 && *d.s.err == 0) *d.s.step += 1;
+}
+
+// ---------------------------------------------------------------------------
+// host-side launch sequences (enqueued on `st`, capturable into a graph)
+
+static inline unsigned nblk(long n, int b) { return (unsigned)((n + b - 1) / b); }
+
+extern "C" size_t sphk_sort_temp_bytes(int N, int end_bit)
+{
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                    (const int*)nullptr, (int*)nullptr, N, 0, end_bit);
+    return bytes;
+}
+
+// Stage names, in launch order; with `ev` non-null, event ev[k] is recorded
+// before stage k and ev[SPHK_NSTAGES] after the last one.
+extern "C" const char* const sphk_stage_names[] = {
+    "k_cellkey", "radix_sort", "k_cellreset", "k_cellrange", "k_nnps",
+    "k_density", "k_shepard_eos", "k_strain_stress", "k_accel", "k_xsph_update", "k_step_done"};
+#define SPHK_NSTAGES 11
+#define REC(k) do { if (ev) cudaEventRecord(ev[k], st); } while (0)
+
+// the NNPS stage; returns the number of this library's kernels it launched
+extern "C" int sphk_enqueue_nnps(const Dev* dp, void* sort_tmp, size_t sort_bytes, int end_bit, cudaStream_t st,
+                                 cudaEvent_t* ev)
+{
+    const Dev& d = *dp;
+    const int N = d.p.N;
+    REC(0);
+    k_cellkey<<<nblk(N, 256), 256, 0, st>>>(d);
+    REC(1);
+    size_t bytes = sort_bytes;
+    cub::DeviceRadixSort::SortPairs(sort_tmp, bytes, d.s.key_in, d.s.key_out, d.s.val_in, d.s.pid_sorted,
+                                    N, 0, end_bit, st);
+    REC(2);
+    k_cellreset<<<nblk(d.p.ctotal, 256), 256, 0, st>>>(d);
+    REC(3);
+    k_cellrange<<<nblk(N, 256), 256, 0, st>>>(d);
+    REC(4);
+    k_nnps<<<nblk(N, 128), 128, 0, st>>>(d);
+    return 4;
+}
+
+extern "C" int sphk_enqueue_physics(const Dev* dp, cudaStream_t st, cudaEvent_t* ev)
+{
+    const Dev& d = *dp;
+    const int N = d.p.N;
+    REC(5);
+    k_density<<<nblk(N, 128), 128, 0, st>>>(d);
+    REC(6);
+    k_shepard_eos<<<nblk(N, 128), 128, 0, st>>>(d);
+    REC(7);
+    k_strain_stress<<<nblk(N, 128), 128, 0, st>>>(d);
+    REC(8);
+    k_accel<<<nblk(N, 128), 128, 0, st>>>(d);
+    REC(9);
+    k_xsph_update<<<nblk(N, 128), 128, 0, st>>>(d);
+    REC(10);
+    k_step_done<<<1, 32, 0, st>>>(d);
+    REC(11);
+    return 6;
+}

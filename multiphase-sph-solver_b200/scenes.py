@@ -401,31 +401,36 @@ SOIL_DTYPE = np.dtype([(k, np.float64) for k in SOIL_FIELDS], align=True)
 
 
 def initialise(scene: Scene) -> InitialState:
-    """Initial particle state as the reference's initialisation leaves it."""
+    """Initial particle state as the reference's initialisation leaves it
+    (vectorised; every expression keeps the reference's operation order)."""
     n, dim, dr = scene.n, scene.ndim, scene.dr
     soils, water, air, st = material_tables(scene)
     P = scene.problem
     gx, gy, gz = P["g"]
+    t, mt, et = scene.ptype, scene.matype, scene.etype
     # setting_vis_cons (CPP_2-initialf.cpp:1021-1058)
-    fl = np.zeros(n, FLUID_DTYPE)
-    so = np.zeros(n, SOIL_DTYPE)
     fdef = fluid_default()
+    fl = np.zeros(n, FLUID_DTYPE)
     for k in FLUID_FIELDS:
         fl[k] = fdef[k]
+    water_tab = np.zeros(3, FLUID_DTYPE)
+    for q in range(3):
+        water_tab[q] = tuple(water[q][k] for k in FLUID_FIELDS)
+    is_w = (t == 1) | ((t == 7) & (et == 1))
+    fl[is_w] = water_tab[np.clip(mt[is_w], 0, 2)]
+    fl[t == 3] = tuple(air[k] for k in FLUID_FIELDS)
     sdef = soil_default()
+    so = np.zeros(n, SOIL_DTYPE)
     for k in SOIL_FIELDS:
         so[k] = sdef[k]
-    t, mt, et = scene.ptype, scene.matype, scene.etype
-    for i in range(n):
-        if t[i] == 1 or (t[i] == 7 and et[i] == 1):
-            rec = water[mt[i]]
-            fl[i] = tuple(rec[k] for k in FLUID_FIELDS)
-        elif t[i] == 3:
-            fl[i] = tuple(air[k] for k in FLUID_FIELDS)
-        if t[i] == 2 or (t[i] == 7 and et[i] == 2):
-            idx = mt[i] if mt[i] < 30 else (mt[i] % 10 if mt[i] >= 50 else None)
-            if idx is not None:
-                so[i] = tuple(soils[idx][k] for k in SOIL_FIELDS)
+    soil_tab = np.zeros(30, SOIL_DTYPE)
+    for q in range(30):
+        soil_tab[q] = tuple(soils[q][k] for k in SOIL_FIELDS)
+    is_s = (t == 2) | ((t == 7) & (et == 2))
+    idx = np.where(mt < 30, mt, np.where(mt >= 50, mt % 10, -1))
+    sel = is_s & (idx >= 0)
+    so[sel] = soil_tab[idx[sel]]
+
     f = {name: np.zeros((n, nc)) for name, nc in
          (("x", 3), ("vx", 3), ("ax", 3), ("axp", 3), ("ux", 3), ("strep", 3), ("interf", 3),
           ("interfss", 3), ("eps", 6), ("sig", 6), ("adps", 6))}
@@ -436,86 +441,85 @@ def initialise(scene: Scene) -> InitialState:
     f["vxp"] = scene.vxp.copy()
     f["type"], f["matype"] = t.copy(), mt.copy()
     f["permtype"], f["etype"] = scene.permtype.copy(), et.copy()
-    sitas = max(s["sitas"] for s in soils)
-    hmaxw, hminw, hmaxs, hmins = -100000.0, 100000.0, -100000.0, 100000.0
+    sitas = max(s_["sitas"] for s_ in soils)
     g_axp = np.array([gx, gy, gz])
-    for i in range(n):   # setting_par first loop (:1088-1282)
-        ti = t[i]
-        if ti == 0:
-            f["rhop"][i] = 1500.0
-            f["satu"][i] = sitas
-            f["hl"][i] = dr
-            if mt[i] == 5:
-                f["axp"][i] = g_axp
-        elif ti == 1 or (ti == 7 and et[i] == 1):
-            f["rhop"][i] = fl["porosity"][i] * fl["dens"][i]
-            f["satu"][i] = sitas
-            f["hl"][i] = dr
-            f["axp"][i] = g_axp
-            f["porosity"][i] = fl["porosity"][i]
-            if ti == 1:
-                hmaxw = max(hmaxw, scene.xp[i, dim - 1])
-                hminw = min(hminw, scene.xp[i, dim - 1])
-        elif ti == 2 or (ti == 7 and et[i] == 2):
-            por = so["porosity"][i]
-            f["rhop"][i] = (1 - por) * so["dens"][i]
-            f["satu"][i] = so["sitar"][i] if (mt[i] % 10 == 3 and mt[i] < 60) else 1.0
-            if mt[i] % 10 == 1:
-                f["roue"] = f.get("roue", np.zeros(n))
-                f["roue"][i] = (so["ramda"][i] - so["kapa"][i]) * math.log(so["ocr"][i])
-            if ti == 2:
-                hmaxs = max(hmaxs, scene.xp[i, dim - 1])
-                hmins = min(hmins, scene.xp[i, dim - 1])
-            else:
-                f["cop"][i] = so["cop"][i]
-            f["e"][i] = so["eps0"][i]
-            f["porosity"][i] = por
-            f["hl"][i] = dr
-            f["axp"][i] = g_axp
-            f["cd"][i] = so["damp_coe"][i] * math.sqrt(so["e"][i] / f["rhop"][i] / f["hl"][i] / f["hl"][i])
-        elif ti == 3:
-            f["rhop"][i] = fl["porosity"][i] * fl["dens"][i]
-            f["hl"][i] = dr
-            f["axp"][i] = g_axp
-        elif ti == 4:
-            f["rhop"][i] = (1 - st["porosity"]) * st["dens"]
-            f["satu"][i] = 1.0
-            f["e"][i] = st["eps0"]
-            f["hl"][i] = dr
-            f["axp"][i] = g_axp
-            f["cd"][i] = so["damp_coe"][i] * math.sqrt(st["e"] / f["rhop"][i] / f["hl"][i] / f["hl"][i])
-        if ti in (0, 1, 2, 3, 4) or (ti == 7 and et[i] in (1, 2)):
-            h = f["hl"][i]
-            f["mass"][i] = f["rhop"][i] * h * h if dim == 2 else f["rhop"][i] * h * h * h
-        f["rho"][i] = f["rhop"][i]
+    # setting_par first loop (:1088-1282)
+    wall = t == 0
+    f["rhop"][wall] = 1500.0
+    f["satu"][wall] = sitas
+    f["hl"][wall] = dr
+    f["axp"][wall & (mt == 5)] = g_axp
+    f["rhop"][is_w] = fl["porosity"][is_w] * fl["dens"][is_w]
+    f["satu"][is_w] = sitas
+    f["hl"][is_w] = dr
+    f["axp"][is_w] = g_axp
+    f["porosity"][is_w] = fl["porosity"][is_w]
+    por = so["porosity"]
+    f["rhop"][is_s] = (1 - por[is_s]) * so["dens"][is_s]
+    m10 = mt % 10
+    f["satu"][is_s] = 1.0
+    um = is_s & np.isin(mt, (3, 13, 23, 53))
+    f["satu"][um] = so["sitar"][um]
+    f["e"][is_s] = so["eps0"][is_s]
+    f["porosity"][is_s] = por[is_s]
+    f["hl"][is_s] = dr
+    f["axp"][is_s] = g_axp
+    s7 = (t == 7) & (et == 2)
+    f["cop"][s7] = so["cop"][s7]
+    air_ = t == 3
+    f["rhop"][air_] = fl["porosity"][air_] * fl["dens"][air_]
+    f["hl"][air_] = dr
+    f["axp"][air_] = g_axp
+    stc = t == 4
+    f["rhop"][stc] = (1 - st["porosity"]) * st["dens"]
+    f["satu"][stc] = 1.0
+    f["e"][stc] = st["eps0"]
+    f["hl"][stc] = dr
+    f["axp"][stc] = g_axp
+    has_mass = (t == 0) | (t == 1) | (t == 2) | (t == 3) | (t == 4) | is_w | is_s
+    h = f["hl"]
+    if dim == 2:
+        mass = f["rhop"] * h * h
+    else:
+        mass = f["rhop"] * h * h * h
+    f["mass"][has_mass] = mass[has_mass]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        cd_s = so["damp_coe"] * np.sqrt(so["e"] / f["rhop"] / h / h)
+        cd_t = so["damp_coe"] * np.sqrt(st["e"] / f["rhop"] / h / h)
+    f["cd"][is_s] = cd_s[is_s]
+    f["cd"][stc] = cd_t[stc]
+    f["rho"][:] = f["rhop"]
+    z = scene.xp[:, dim - 1]
+    hmaxw = max(-100000.0, float(z[t == 1].max())) if np.any(t == 1) else -100000.0
+    hminw = min(100000.0, float(z[t == 1].min())) if np.any(t == 1) else 100000.0
+    hmaxs = max(-100000.0, float(z[t == 2].max())) if np.any(t == 2) else -100000.0
+    hmins = min(100000.0, float(z[t == 2].min())) if np.any(t == 2) else 100000.0
     g = gy if dim == 2 else gz
-    for i in range(n):   # setting_par second loop (:1291-1369)
-        ti = t[i]
-        if ti == 0:
-            f["prep"][i] = 1500.0 * (-g) * abs(hmaxw - hminw) * 0.5
-            f["pre"][i] = f["prep"][i]
-        if ti == 1:
-            pc = fl["pre_coe"][i]
-            if fl["press_type"][i] == 0:
-                f["prep"][i] = f["rhop"][i] * (-g) * dr * pc
-            else:
-                f["prep"][i] = f["rhop"][i] * (-g) * abs(scene.xp[i, dim - 1] - hmaxw - pc * dr)
-            f["pre"][i] = f["prep"][i]
-        if ti == 7 and et[i] == 1:
-            f["prep"][i] = f["rhop"][i] * (-g) * dr * fl["pre_coe"][i]
-            f["pre"][i] = f["prep"][i]
-        if ti == 2 or (ti == 7 and et[i] == 2):
-            if abs(so["sme0"][i]) > 1.0e-3:
-                f["sig"][i, 0:3] = -so["sme0"][i]
-            elif ti == 2:
-                v = f["rho"][i] * g * (hmaxs - hmins) * 0.5
-                f["sig"][i, 0:3] = v
-        if ti == 3:
-            if fl["press_type"][i] == 0:
-                f["prep"][i] = fl["paa0"][i]
-            else:
-                f["prep"][i] = fl["dens"][i] * (-g) * abs(scene.xp[i, dim - 1] - hmaxw - fl["pre_coe"][i] * dr)
-            f["pre"][i] = f["prep"][i]
+    # setting_par second loop (:1291-1369)
+    f["prep"][wall] = 1500.0 * (-g) * abs(hmaxw - hminw) * 0.5
+    f["pre"][wall] = f["prep"][wall]
+    w1 = t == 1
+    pc = fl["pre_coe"]
+    pt0 = w1 & (fl["press_type"] == 0)
+    f["prep"][pt0] = f["rhop"][pt0] * (-g) * dr * pc[pt0]
+    pt1 = w1 & (fl["press_type"] != 0)
+    f["prep"][pt1] = f["rhop"][pt1] * (-g) * np.abs(z[pt1] - hmaxw - pc[pt1] * dr)
+    f["pre"][w1] = f["prep"][w1]
+    w7 = (t == 7) & (et == 1)
+    f["prep"][w7] = f["rhop"][w7] * (-g) * dr * pc[w7]
+    f["pre"][w7] = f["prep"][w7]
+    big = is_s & (np.abs(so["sme0"]) > 1.0e-3)
+    for k in range(3):
+        f["sig"][big, k] = -so["sme0"][big]
+    geo = (t == 2) & ~big
+    v = f["rho"][geo] * g * (hmaxs - hmins) * 0.5
+    for k in range(3):
+        f["sig"][geo, k] = v
+    a0 = air_ & (fl["press_type"] == 0)
+    f["prep"][a0] = fl["paa0"][a0]
+    a1 = air_ & (fl["press_type"] != 0)
+    f["prep"][a1] = fl["dens"][a1] * (-g) * np.abs(z[a1] - hmaxw - fl["pre_coe"][a1] * dr)
+    f["pre"][air_] = f["prep"][air_]
     f.pop("roue", None)
     # input_par domain box (:917-1002) and celllist_ini1 (CPP_3-NNPS.cpp:96-121)
     bmax = np.maximum(scene.xp.max(axis=0), -10000.0)

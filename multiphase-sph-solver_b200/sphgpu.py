@@ -108,7 +108,7 @@ FIELDS = {
     "interf": 3, "interfss": 3, "rho": 1, "rhop": 1, "mass": 1, "hl": 1, "pre": 1, "prep": 1,
     "e": 1, "eps": 6, "sig": 6, "adps": 6, "satu": 1, "cop": 1, "vsig": 1, "veps": 1,
     "divq": 1, "divr": 1, "meps": 1, "prew": 1, "prea": 1, "porosity": 1, "poro_cop": 1,
-    "type": 1, "matype": 1, "permtype": 1, "etype": 1,
+    "cd": 1, "type": 1, "matype": 1, "permtype": 1, "etype": 1,
 }
 INT_FIELDS = {"type", "matype", "permtype", "etype"}
 
@@ -160,6 +160,10 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_last_step_launches.argtypes = [C.c_void_p]
     lib.sphgpu_stream.restype = C.c_void_p
     lib.sphgpu_stream.argtypes = [C.c_void_p]
+    lib.sphgpu_stage_count.restype = C.c_int
+    lib.sphgpu_stage_name.restype = C.c_char_p
+    lib.sphgpu_stage_name.argtypes = [C.c_int]
+    lib.sphgpu_step_profiled.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
     _lib = lib
     return lib
 
@@ -243,3 +247,11 @@ class Engine:
 
     def last_step_launches(self) -> int:
         return int(self.lib.sphgpu_last_step_launches(self.h))
+
+    def step_profiled(self, nsteps: int) -> dict:
+        """Run nsteps with a CUDA event between stages; returns {stage: ms
+        summed over the steps}."""
+        k = self.lib.sphgpu_stage_count()
+        ms = np.zeros(k)
+        self._check(self.lib.sphgpu_step_profiled(self.h, int(nsteps), _ptr(ms)), "sphgpu_step_profiled")
+        return {self.lib.sphgpu_stage_name(i).decode(): float(ms[i]) for i in range(k)}

@@ -18,7 +18,7 @@
 
 struct orc_ctx {
     sphgpu_params P;
-    int n, l, mode;
+    int n, l, mode, pow_mode;
     double t;
     /* Particle members (Class_particle.h:13-103), particle-major */
     double *x, *xp, *vx, *vxp, *ax, *axp, *ux, *strep, *divx, *interf, *interfss;
@@ -151,6 +151,34 @@ int orc_set_materials(orc_ctx* c, const sphgpu_fluid* fluid, const sphgpu_soil* 
 }
 
 void orc_set_mode(orc_ctx* c, int mode) { c->mode = mode; }
+void orc_set_pow_mode(orc_ctx* c, int pow_mode) { c->pow_mode = pow_mode; }
+
+/* x^7 from Dekker products (fma gives each product's exact error term); the
+ * double-double chain carries ~100 bits, so the final sum is the correctly
+ * rounded x^7 unless x^7 sits within ~2^-48 ulp of a rounding midpoint. */
+typedef struct { double h, l; } orc_dd;
+static orc_dd orc_dd_mul(orc_dd a, orc_dd b)
+{
+    double p = a.h * b.h;
+    double e = fma(a.h, b.h, -p);
+    e = e + (a.h * b.l + a.l * b.h);
+    double s = p + e;
+    orc_dd r = {s, e - (s - p)};
+    return r;
+}
+double orc_pow7(double x)
+{
+    orc_dd x1 = {x, 0.0};
+    orc_dd x2 = orc_dd_mul(x1, x1);
+    orc_dd x4 = orc_dd_mul(x2, x2);
+    orc_dd x6 = orc_dd_mul(x4, x2);
+    orc_dd x7 = orc_dd_mul(x6, x1);
+    return x7.h + x7.l;
+}
+static double eos_pow7(const orc_ctx* c, double x)
+{
+    return c->pow_mode == ORC_POW_CR ? orc_pow7(x) : pow(x, 7.0);
+}
 int orc_get_step(const orc_ctx* c) { return c->l; }
 
 /* ------------------------------------------------------------------------- */
@@ -557,7 +585,7 @@ static void eos(orc_ctx* c)
     int n = c->n;
     for (int i = 0; i < n; i++) {
         if (c->type[i] == 1) {
-            c->pre[i] = c->prep[i] * (pow(c->rho[i] / c->fl[i].dens / c->fl[i].porosity, 7.0) - 1.0);
+            c->pre[i] = c->prep[i] * (eos_pow7(c, c->rho[i] / c->fl[i].dens / c->fl[i].porosity) - 1.0);
             c->pre[i] = c->pre[i] + c->prep[i];
         }
         if (c->type[i] == 3) {
@@ -566,7 +594,7 @@ static void eos(orc_ctx* c)
             c->pre[i] = c->pre[i] + c->prep[i];
         }
         if (c->type[i] == 0 && c->matype[i] == 1) {
-            c->pre[i] = c->prep[i] * (pow(c->rho[i] / c->rhop[i], 7.0) - 1.0);
+            c->pre[i] = c->prep[i] * (eos_pow7(c, c->rho[i] / c->rhop[i]) - 1.0);
             c->pre[i] = c->pre[i] + c->prep[i];
         }
     }
@@ -1197,6 +1225,31 @@ static void interact1(orc_ctx* c)
     }
 }
 
+/* soil_damping_geostress: CPP_9-4-derivation_stress.cpp:849-896 */
+static void soil_damping_geostress(orc_ctx* c)
+{
+    int ndim = c->P.ndim;
+    double dt = c->P.dt;
+    for (int i = 0; i < c->n; i++) {
+        if (!(c->type[i] == 2 || c->type[i] == 4)) continue;
+        double cd = c->cd[i], damp[3] = {0, 0, 0};
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj);
+            if (c->type[i] == c->type[j])
+                for (int k = 0; k < ndim; k++)
+                    damp[k] = damp[k] + c->mass[j] / c->rho[j] * cd * (c->vxp[i * 3 + k] - c->vxp[j * 3 + k]) * W(i, nj, 3);
+        }
+        for (int k = 0; k < ndim; k++) {
+            double* ax = &c->ax[i * 3 + k];
+            double axp = c->axp[i * 3 + k], vxp = c->vxp[i * 3 + k];
+            double vx1 = vxp + 0.5 * (axp + *ax) * dt;
+            double vx2 = vxp + 0.5 * (axp + *ax - damp[k]) * dt;
+            if (vx1 * vx2 <= 0.0) *ax = -2.0 * vxp / dt - axp;
+            else *ax -= damp[k];
+        }
+    }
+}
+
 /* veocity_update: CPP_11-xsph.cpp:11-142 */
 static void velocity_update(orc_ctx* c)
 {
@@ -1421,6 +1474,7 @@ int orc_step(orc_ctx* c, int nsteps)
         artificial_viscosity(c);
         boundary_moving_stress_effect(c);    /* flv == 0, flbndy 1 */
         if (P->fli == 1) interact1(c);
+        if (c->l <= P->inip) soil_damping_geostress(c);
         velocity_update(c);
         if (P->if_move != 2) xsph(c);
         tmboundary(c);                        /* flbndy == 1 */

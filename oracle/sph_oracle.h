@@ -30,6 +30,15 @@ extern "C" {
 #define ORC_JACOBI  0
 #define ORC_INPLACE 1
 
+/* Evaluation of the equation of state's pow(x, 7.0) (CPP_7-1-eos_CR.cpp:28,40):
+ *   ORC_POW_LIBM - the C library's pow(), as the reference calls it;
+ *   ORC_POW_CR   - x^7 correctly rounded (double-double product chain), the
+ *                  value the GPU engine computes.  glibc's pow differs from
+ *                  the correctly rounded value on about 0.1% of inputs near 1
+ *                  by one unit in the last place. */
+#define ORC_POW_LIBM 0
+#define ORC_POW_CR   1
+
 typedef struct orc_ctx orc_ctx;
 
 orc_ctx* orc_create(const sphgpu_params* p);
@@ -38,6 +47,8 @@ int      orc_set_field(orc_ctx* c, const char* name, const void* host, size_t co
 int      orc_get_field(orc_ctx* c, const char* name, void* host, size_t count);
 int      orc_set_materials(orc_ctx* c, const sphgpu_fluid* fluid, const sphgpu_soil* soil, int n);
 void     orc_set_mode(orc_ctx* c, int mode);
+void     orc_set_pow_mode(orc_ctx* c, int pow_mode);
+double   orc_pow7(double x);   /* the ORC_POW_CR evaluation */
 int      orc_get_step(const orc_ctx* c);
 /* parttocell + partisearching for the current step; neighbour lists copied
  * out as in Par_Cell (influ 1-based, 100 slots per particle). */

@@ -26,6 +26,7 @@ ORACLE_SO = os.path.join(REPO, "oracle", "liboracle.so")
 REF_SO = os.path.join(REPO, "oracle", "_ref", "libsphref.so")
 
 ORC_JACOBI, ORC_INPLACE = 0, 1
+ORC_POW_LIBM, ORC_POW_CR = 0, 1
 
 ORACLE_FIELDS = dict(FIELDS)
 ORACLE_FIELDS.update({"divx": 9, "deps": 6, "dsig": 6, "weps": 9, "dsatu": 1, "suct": 1,
@@ -52,6 +53,9 @@ def oracle_lib():
         lib.orc_get_field.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t]
         lib.orc_set_materials.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         lib.orc_set_mode.argtypes = [C.c_void_p, C.c_int]
+        lib.orc_set_pow_mode.argtypes = [C.c_void_p, C.c_int]
+        lib.orc_pow7.restype = C.c_double
+        lib.orc_pow7.argtypes = [C.c_double]
         lib.orc_get_step.argtypes = [C.c_void_p]
         lib.orc_nnps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.orc_step.argtypes = [C.c_void_p, C.c_int]
@@ -60,7 +64,7 @@ def oracle_lib():
 
 
 class Oracle:
-    def __init__(self, params: dict | Params, mode: int = ORC_JACOBI):
+    def __init__(self, params: dict | Params, mode: int = ORC_JACOBI, pow_mode: int = ORC_POW_LIBM):
         self.lib = oracle_lib()
         self.params = params if isinstance(params, Params) else sphgpu.params_from_dict(params)
         self.h = C.c_void_p(self.lib.orc_create(C.byref(self.params)))
@@ -68,6 +72,11 @@ class Oracle:
             raise RuntimeError("orc_create failed")
         self.n = int(self.params.ntotal)
         self.lib.orc_set_mode(self.h, mode)
+        self.lib.orc_set_pow_mode(self.h, pow_mode)
+
+    @property
+    def step_index(self):
+        return int(self.lib.orc_get_step(self.h))
 
     def __del__(self):
         if getattr(self, "h", None):
