@@ -22,7 +22,7 @@ extern "C" int sphk_enqueue_nnps(const Dev* d, void* sort_tmp, size_t sort_bytes
                                  cudaEvent_t* ev);
 extern "C" int sphk_enqueue_physics(const Dev* d, cudaStream_t st, cudaEvent_t* ev);
 extern "C" const char* const sphk_stage_names[];
-#define SPHK_NSTAGES 11
+#define SPHK_NSTAGES 13
 
 namespace {
 
@@ -183,9 +183,9 @@ void* field_ptr(sphgpu_ctx* c, const char* name)
 {
     DevState& s = c->d[c->parity].s;
     struct { const char* n; void* p; } tab[] = {
-        {"xp", s.xp}, {"vx", s.vx}, {"vxp", s.vxp}, {"ax", s.ax}, {"axp", s.axp}, {"ux", s.ux},
+        {"vx", s.vx}, {"vxp", s.vxp}, {"ax", s.ax}, {"axp", s.axp}, {"ux", s.ux},
         {"strep", s.strep}, {"interf", s.interf}, {"interfss", s.interfss}, {"rho", s.rho},
-        {"rhop", s.rhop}, {"mass", s.mass}, {"hl", s.hl}, {"pre", s.pre}, {"prep", s.prep},
+        {"rhop", s.rhop}, {"mass", s.mass}, {"pre", s.pre}, {"prep", s.prep},
         {"e", s.e}, {"eps", s.eps}, {"sig", s.sig}, {"adps", s.adps}, {"satu", s.satu}, {"cop", s.cop},
         {"vsig", s.vsig}, {"veps", s.veps}, {"divq", s.divq}, {"divr", s.divr}, {"meps", s.meps},
         {"prew", s.prew}, {"prea", s.prea}, {"porosity", s.porosity}, {"poro_cop", s.poro_cop},
@@ -290,18 +290,19 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     DevState& s = d.s;
     int r = 0;
     r |= dalloc(c, &s.type, N); r |= dalloc(c, &s.matype, N); r |= dalloc(c, &s.etype, N); r |= dalloc(c, &s.permtype, N);
-    r |= dalloc(c, &s.mass, N); r |= dalloc(c, &s.hl, N); r |= dalloc(c, &s.cd, N);
+    r |= dalloc(c, &s.mass, N); r |= dalloc(c, &s.cd, N);
     r |= dalloc(c, &s.f_dens, N); r |= dalloc(c, &s.f_por, N); r |= dalloc(c, &s.f_vpu, N); r |= dalloc(c, &s.f_vis, N);
     r |= dalloc(c, &s.f_c, N); r |= dalloc(c, &s.f_smin, N); r |= dalloc(c, &s.f_tanfai, N); r |= dalloc(c, &s.f_bhtype, N);
     r |= dalloc(c, &s.s_e, N); r |= dalloc(c, &s.s_poi, N); r |= dalloc(c, &s.s_eps0, N); r |= dalloc(c, &s.s_dens, N);
     r |= dalloc(c, &s.s_kapa, N); r |= dalloc(c, &s.s_por, N); r |= dalloc(c, &s.s_vpu, N); r |= dalloc(c, &s.s_cop, N);
     r |= dalloc(c, &s.s_sitas, N); r |= dalloc(c, &s.s_sitar, N);
     r |= dalloc(c, &s.s_yalf, N); r |= dalloc(c, &s.s_ykap, N); r |= dalloc(c, &s.s_yalf_dil, N);
-    r |= dalloc(c, &s.xp, 3 * (size_t)N); r |= dalloc(c, &s.xp_next, 3 * (size_t)N);
+    r |= dalloc(c, &s.xh, 4 * (size_t)N); r |= dalloc(c, &s.xh_next, 4 * (size_t)N); r |= dalloc(c, &s.xs, 4 * (size_t)N);
+    r |= dalloc(c, &s.de, 6 * (size_t)N); r |= dalloc(c, &s.we, 6 * (size_t)N); r |= dalloc(c, &s.color, N);
+    r |= dalloc(c, &s.sr, 6 * (size_t)N); r |= dalloc(c, &s.pp, N);
     r |= dalloc(c, &s.vx, 3 * (size_t)N); r |= dalloc(c, &s.vx_next, 3 * (size_t)N);
     r |= dalloc(c, &s.vxp, 3 * (size_t)N); r |= dalloc(c, &s.axp, 3 * (size_t)N); r |= dalloc(c, &s.ax, 3 * (size_t)N);
     r |= dalloc(c, &s.ux, 3 * (size_t)N);
-    s.x = nullptr;
     r |= dalloc(c, &s.rho, N); r |= dalloc(c, &s.rho_c, N); r |= dalloc(c, &s.rhop, N); r |= dalloc(c, &s.pre, N);
     r |= dalloc(c, &s.prep, N); r |= dalloc(c, &s.porosity, N); r |= dalloc(c, &s.poro_cop, N); r |= dalloc(c, &s.e, N);
     r |= dalloc(c, &s.sig, 6 * (size_t)N); r |= dalloc(c, &s.sig_next, 6 * (size_t)N);
@@ -330,7 +331,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     if (cudaMalloc(&c->sort_tmp, c->sort_bytes + 256) != cudaSuccess) return fail(SPHGPU_E_CUDA);
     c->allocs.push_back(c->sort_tmp);
     c->d[1] = c->d[0];
-    std::swap(c->d[1].s.xp, c->d[1].s.xp_next);
+    std::swap(c->d[1].s.xh, c->d[1].s.xh_next);
     std::swap(c->d[1].s.sig, c->d[1].s.sig_next);
     if (cudaStreamSynchronize(c->st) != cudaSuccess) return fail(SPHGPU_E_CUDA);
     return c;
@@ -390,6 +391,21 @@ int sphgpu_set_field(sphgpu_ctx* c, const char* name, const void* host, size_t c
         c->x_tracked = true;
         return 0;
     }
+    if (std::strcmp(name, "xp") == 0 || std::strcmp(name, "hl") == 0) {
+        // (x, y, z, h) records: read-modify-write of the current buffer
+        std::vector<double> rec((size_t)N * 4);
+        double* xh = c->d[c->parity].s.xh;
+        CK(cudaMemcpy(rec.data(), xh, sizeof(double) * rec.size(), cudaMemcpyDeviceToHost));
+        const double* h = (const double*)host;
+        if (nc == 3) {
+            for (int i = 0; i < N; i++)
+                for (int k = 0; k < 3; k++) rec[(size_t)i * 4 + k] = h[(size_t)i * 3 + k];
+        } else {
+            for (int i = 0; i < N; i++) rec[(size_t)i * 4 + 3] = h[i];
+        }
+        CK(cudaMemcpy(xh, rec.data(), sizeof(double) * rec.size(), cudaMemcpyHostToDevice));
+        return 0;
+    }
     const size_t esz = f->is_int ? 4 : 8;
     int r = ensure_pinned(c, count * esz);
     if (r) return r;
@@ -434,6 +450,18 @@ int sphgpu_get_field(sphgpu_ctx* c, const char* name, void* host, size_t count)
                 if (t != 0 || m == 2 || m == 3 || m == 4 || m == 5)
                     for (int k = 0; k < c->P.ndim; k++) o[(size_t)i * 3 + k] = xp[(size_t)i * 3 + k];
             }
+        }
+        return 0;
+    }
+    if (std::strcmp(name, "xp") == 0 || std::strcmp(name, "hl") == 0) {
+        std::vector<double> rec((size_t)N * 4);
+        CK(cudaMemcpy(rec.data(), c->d[c->parity].s.xh, sizeof(double) * rec.size(), cudaMemcpyDeviceToHost));
+        double* o = (double*)host;
+        if (nc == 3) {
+            for (int i = 0; i < N; i++)
+                for (int k = 0; k < 3; k++) o[(size_t)i * 3 + k] = rec[(size_t)i * 4 + k];
+        } else {
+            for (int i = 0; i < N; i++) o[i] = rec[(size_t)i * 4 + 3];
         }
         return 0;
     }

@@ -1,20 +1,27 @@
 // sph_device.cuh -- device state and per-pair helpers of the sm_100a SPH step.
 //
-// Layout in HBM (all particle arrays indexed by the reference particle index
-// i, i.e. the order of the caller's Particle array):
+// Layout in HBM (particle arrays indexed by the reference particle index i,
+// i.e. the order of the caller's Particle array):
+//   * positions: double xh[4 * N], particle-major records (x, y, z, h) --
+//                one 32-byte sector per neighbour gather; xs[4 * N] is the
+//                same records in cell-sorted order, streamed by the NNPS scan
 //   * scalars:   T a[N]
 //   * vectors:   double a[3 * N], component k of particle i at a[k * N + i]
 //   * tensors:   double a[6 * N] (Voigt order xx yy zz xy yz zx, as
 //                Particle::sig), component k at a[k * N + i]
 //   * neighbour lists: int nbr[SPH_NB_CAP * N], slot s of particle i at
-//                nbr[s * N + i] (reference index of the neighbour), so that
-//                the threads of a warp read consecutive words per slot.
-// Component-major storage makes every per-particle load of one component a
+//                nbr[s * N + i], so the threads of a warp read consecutive
+//                words per slot.
+// Component-major storage makes every own-particle load of one component a
 // coalesced 8-byte-per-lane access.
 //
 // Arithmetic follows the reference's operation order; the library is built
 // with -fmad=false so no multiply-add is contracted, which keeps the FP64
-// results identical to the reference's x86-64 build (no FMA).
+// results identical to the reference's x86-64 build (no FMA).  Where a
+// subexpression that the reference evaluates per pair depends on one particle
+// only, it is evaluated once per particle and reused when a bitwise guard
+// shows the operands are the same (e.g. equal porosities), which yields the
+// same rounded value.
 #pragma once
 #include <cstdint>
 
@@ -44,23 +51,31 @@ struct DevParams {
 struct DevState {
     // static per particle
     int *type, *matype, *etype, *permtype;
-    double *mass, *hl, *cd;
+    double *mass, *cd;
     // fluid material record (pVFluid) used by the step
     double *f_dens, *f_por, *f_vpu, *f_vis, *f_c, *f_smin, *f_tanfai;
     int *f_bhtype;
     // soil material record (pParti_ConsPara) used by the step
     double *s_e, *s_poi, *s_eps0, *s_dens, *s_kapa, *s_por, *s_vpu, *s_cop, *s_sitas, *s_sitar;
     double *s_yalf, *s_ykap, *s_yalf_dil;   // Drucker-Prager constants, host-evaluated
+    // positions (x, y, z, h) records, ping-pong
+    double *xh, *xh_next;
+    double *xs;                // xh in cell-sorted order (NNPS scan)
     // dynamic state
-    double *xp, *xp_next;      // 3N each, swapped every step
-    double *vx, *vx_next;      // 3N each, swapped every step
-    double *vxp, *axp, *ax, *ux, *x;
+    double *vx, *vx_next;      // vx: velocity after the step; vx_next: before XSPH
+    double *vxp, *axp, *ax, *ux;
     double *rho, *rho_c, *rhop, *pre, *prep, *porosity, *poro_cop, *e;
-    double *sig, *sig_next;    // 6N each, swapped every step
+    double *sig, *sig_next;    // 6N each, ping-pong
     double *eps, *adps;
     double *satu, *cop, *prew, *prea;
     double *interf, *interfss, *strep;
     double *vsig, *veps, *divq, *divr, *meps;
+    // per-step intermediates
+    double *de;                // strain rate, 6N
+    double *we;                // spin, off-diagonal entries (0,1)(0,2)(1,0)(1,2)(2,0)(2,1): 6N
+    double *color;             // free-surface colour sum
+    double *sr;                // stress / rho^2 as the momentum pass uses it, 6N
+    double *pp;                // pore-pressure term / rho^2, N
     // NNPS
     int *cell;                 // cell id per particle
     uint32_t *key_in, *key_out;
@@ -78,68 +93,97 @@ struct Dev {
     DevState s;
 };
 
-// ---------------------------------------------------------------------------
-// per-pair kernel value and gradient: weight() / weight2(),
-// CPP_3-NNPS.cpp:17-82.  w[0..2] gradient, w[3] value.
-__device__ __forceinline__ void sph_weight(double dst, double ra, const double dx[3], double w[4],
-                                           int ndim, int flknl)
+struct Pos { double x, y, z, h; };
+
+__device__ __forceinline__ Pos load_pos(const double* xh, int i)
 {
-    double a1, s;
-    s = dst / ra;
-    a1 = 0.0;
+    const double2* p = reinterpret_cast<const double2*>(xh) + 2 * (size_t)i;
+    double2 a = p[0], b = p[1];
+    return Pos{a.x, a.y, b.x, b.y};
+}
+
+__device__ __forceinline__ void store_pos(double* xh, int i, const Pos& q)
+{
+    double2* p = reinterpret_cast<double2*>(xh) + 2 * (size_t)i;
+    p[0] = make_double2(q.x, q.y);
+    p[1] = make_double2(q.z, q.h);
+}
+
+// the normalisation constant a1 of weight() / weight2() for support ra
+// (CPP_3-NNPS.cpp:24-29, 58-63)
+__device__ __forceinline__ double kernel_a1(double ra, int ndim, int flknl)
+{
+    if (flknl == 1 || flknl == 3)
+        return (ndim == 2) ? 0.682092613250980 / ra / ra : 0.477464829275686 / ra / ra / ra;
+    return (ndim == 2) ? 0.106103295394597 / (ra * ra) : 0.077010456334788 / (ra * ra * ra);
+}
+
+// Particle i's side of every pair: position, h and a1 for ra = h_i (the
+// reference's ra = (h_i + h_j) / 2 equals h_i exactly when h_j == h_i).
+struct PairI {
+    double x[3];
+    double h, a1;
+};
+
+template <int ND>
+__device__ __forceinline__ PairI pair_i(const Dev& d, int i)
+{
+    Pos q = load_pos(d.s.xh, i);
+    PairI I;
+    I.x[0] = q.x; I.x[1] = q.y; I.x[2] = q.z; I.h = q.h;
+    I.a1 = kernel_a1(q.h, ND, d.p.flknl);
+    return I;
+}
+
+// Kernel value and gradient of pair (i, j) exactly as partisearching stored
+// them: weight() / weight2() (CPP_3-NNPS.cpp:17-82) with the same
+// differences, summation order and sqrt, recomputed from this step's
+// positions.  w[0..2] gradient, w[3] value.
+template <int ND>
+__device__ __forceinline__ void pair_w(const Dev& d, const PairI& I, const Pos& pj, double w[4])
+{
+    constexpr int nd = ND;
+    const double xj[3] = {pj.x, pj.y, pj.z};
+    double dx[3] = {0.0, 0.0, 0.0}, dst = 0.0;
+    for (int k = 0; k < nd; k++) {
+        dst = dst + (I.x[k] - xj[k]) * (I.x[k] - xj[k]);
+        dx[k] = I.x[k] - xj[k];
+    }
+    dst = sqrt(dst);
+    const double ra = (pj.h == I.h) ? I.h : (I.h + pj.h) / 2;
+    const double a1 = (pj.h == I.h) ? I.a1 : kernel_a1(ra, nd, d.p.flknl);
+    const double s = dst / ra;
     w[0] = w[1] = w[2] = w[3] = 0.0;
-    if (flknl == 1 || flknl == 3) {
-        if (ndim == 2) a1 = 0.682092613250980 / ra / ra;
-        else a1 = 0.477464829275686 / ra / ra / ra;
+    if (d.p.flknl == 1 || d.p.flknl == 3) {
         if (s == 0.0) {
             w[3] = a1 * (0.66666667 - s * s + 0.5 * s * s * s);
         }
         if (s > 0.0 && s <= 1.0) {
-            for (int k = 0; k < ndim; k++) w[k] = a1 * dx[k] * (-2 * s + 1.5 * s * s) / (ra * dst);
+            for (int k = 0; k < nd; k++) w[k] = a1 * dx[k] * (-2 * s + 1.5 * s * s) / (ra * dst);
             w[3] = a1 * (0.66666667 - s * s + 0.5 * s * s * s);
         } else if (s > 1.0 && s <= 2.0) {
-            for (int k = 0; k < ndim; k++) w[k] = a1 * (-0.5) * dx[k] * (2.0 - s) * (2.0 - s) / (ra * dst);
+            for (int k = 0; k < nd; k++) w[k] = a1 * (-0.5) * dx[k] * (2.0 - s) * (2.0 - s) / (ra * dst);
             w[3] = a1 * (2.0 - s) * (2.0 - s) * (2.0 - s) / 6.0;
         }
     } else {
-        if (ndim == 2) a1 = 0.106103295394597 / (ra * ra);
-        else a1 = 0.077010456334788 / (ra * ra * ra);
         if (s == 0.0) {
             w[3] = a1 * (6.0 - 6.0 * s + 1.0 * s * s * s);
         }
         if (s > 0.0 && s <= 1.0) {
-            for (int k = 0; k < ndim; k++) w[k] = a1 * dx[k] * (-6.0 + 3.0 * s * s) / (ra * dst);
+            for (int k = 0; k < nd; k++) w[k] = a1 * dx[k] * (-6.0 + 3.0 * s * s) / (ra * dst);
             w[3] = a1 * (6.0 - 6.0 * s + 1.0 * s * s * s);
         } else if (s > 1.0 && s <= 2.0) {
-            for (int k = 0; k < ndim; k++) w[k] = a1 * (-3.0) * dx[k] * (2.0 - s) * (2.0 - s) / (ra * dst);
+            for (int k = 0; k < nd; k++) w[k] = a1 * (-3.0) * dx[k] * (2.0 - s) * (2.0 - s) / (ra * dst);
             w[3] = a1 * (2.0 - s) * (2.0 - s) * (2.0 - s);
         }
     }
-}
-
-// The kernel values of pair (i, j) exactly as partisearching stored them
-// (same differences, same summation order, same sqrt), recomputed from the
-// positions of this step instead of being stored per pair.
-__device__ __forceinline__ void sph_pair_w(const Dev& d, int i, int j, double w[4])
-{
-    const int N = d.p.N, nd = d.p.ndim;
-    double dx[3] = {0.0, 0.0, 0.0}, dst = 0.0;
-    for (int k = 0; k < nd; k++) {
-        double xi = d.s.xp[k * N + i], xj = d.s.xp[k * N + j];
-        dst = dst + (xi - xj) * (xi - xj);
-        dx[k] = xi - xj;
-    }
-    dst = sqrt(dst);
-    double ra = (d.s.hl[i] + d.s.hl[j]) / 2;
-    sph_weight(dst, ra, dx, w, nd, d.p.flknl);
 }
 
 // x^7 rounded to nearest from a double-double product chain (Dekker's exact
 // product via fma; relative error of the chain below 2^-100), so the result
 // is the correctly rounded power except when x^7 lies within ~2^-48 ulp of a
 // rounding midpoint.  Stands in for the reference's pow(x, 7.0) in the
-// equation of state (CPP_7-1-eos_CR.cpp:28,40), whose libm result is the
-// correctly rounded value on the same inputs (checked on the CPU in tests).
+// equation of state (CPP_7-1-eos_CR.cpp:28,40).
 struct dd { double h, l; };
 __device__ __forceinline__ dd dd_mul(dd a, dd b)
 {

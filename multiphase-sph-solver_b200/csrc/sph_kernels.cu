@@ -2,34 +2,51 @@
 // as sm_100a kernels (FP64 drop-in form).
 //
 // One time step (the body of SPH_Calculation's main loop,
-// CPP_1-SPHLoops.cpp:523-753) is seven kernels plus a radix sort, one kernel
-// per level of the neighbour-data dependency chain:
+// CPP_1-SPHLoops.cpp:523-753), one kernel per level of the neighbour-data
+// dependency chain:
 //
 //   k_cellkey      parttocell: cell key per particle            (CPP_3-NNPS.cpp:175-257)
 //   radix sort     Binary_Sort's order: cell ascending, index descending
-//   k_cellreset/k_cellrange  cell_info start/end                (CPP_3-NNPS.cpp:196-201, 621-629)
+//   k_cellreset    cell_info reset                              (CPP_3-NNPS.cpp:196-201)
+//   k_cellrange    cell_info start/end (:621-629) + the cell-sorted copy of positions
 //   k_nnps         partisearching: stencil scan, FP64 distance test, neighbour list
 //   k_density      fluid porosity + continuity                  (CPP_6-density.cpp:25-165)
 //   k_shepard_eos  Shepard filter (Jacobi) + local EOS          (CPP_6-density.cpp:168-188, CPP_7-1-eos_CR.cpp:22-43)
-//   k_strain_stress strain rate, gathered pressures / wall stress, permeability,
-//                  constitutive update, free-surface correction, principal stresses
+//   k_strain       velocity gradient, strain rate and spin, gathered pore pressures and
+//                  wall stresses, free-surface colour          (CPP_7-1-strain.cpp:20-220, CPP_7-1-eos_CR.cpp:46-177)
+//   k_stress       permeability, constitutive update, free-surface correction,
+//                  principal stresses (per particle)           (CPP_7-2-constitutive.cpp, CPP_8-1-consfactor.cpp)
 //   k_accel        momentum (fluid / soil / structure), artificial viscosity,
-//                  wall stress, Darcy drag, velocity update
+//                  wall stress, Darcy drag, geostatic damping, velocity update
 //   k_xsph_update  XSPH, wall velocity correction, domain check, position update
 //
 // Every pair sum is gathered by the particle that owns it, in the reference's
 // neighbour order, with no atomics: results are deterministic and, with
 // -fmad=false, equal to the reference's FP64 arithmetic.  Kernel values are
-// recomputed per pair from the positions (sph_pair_w) instead of being stored.
+// recomputed per pair from the positions (pair_w) instead of being stored.
 // All kernels return immediately once an error code is set, so a failing step
 // leaves the state as the reference leaves it when it returns the code.
 #include <cub/cub.cuh>
 #include <climits>
 #include "sph_device.cuh"
+#include "sph_constitutive.cuh"
 
 #define IDX (blockIdx.x * blockDim.x + threadIdx.x)
 
+// minimum resident 128-thread blocks per SM requested from the register
+// allocator for the neighbour-loop kernels (an occupancy / spill trade-off)
+// (4 measured fastest on B200 for the 3-D soil column: 49.9 ms vs 55.0 ms per
+// step at 1, 2 or 3)
+#ifndef SPH_MINB
+#define SPH_MINB 4
+#endif
+
 __device__ __forceinline__ void raise_err(int* err, int code) { atomicCAS(err, 0, code); }
+
+__device__ __forceinline__ bool same_bits(double a, double b)
+{
+    return __double_as_longlong(a) == __double_as_longlong(b);
+}
 
 // x86-64 cvttsd2si semantics for the reference's (int) casts of FP64 cell
 // coordinates: NaN and out-of-range values become INT_MIN.
@@ -52,21 +69,30 @@ __device__ __forceinline__ int cell_link(const DevParams& p, int c, int slot)
     return (v < 0 || v > p.ctotal) ? 0 : v;
 }
 
+__device__ __forceinline__ int nbr_count(const Dev& d, int i)
+{
+    int c = d.s.nnb[i];
+    return c > SPH_NB_CAP ? SPH_NB_CAP : c;
+}
+
 // ---------------------------------------------------------------------------
+template <int ND>
 __global__ void k_cellkey(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
+    const Pos q = load_pos(d.s.xh, i);
+    const double xp[3] = {q.x, q.y, q.z};
     const double xmin[3] = {d.p.xmin, d.p.ymin, d.p.zmin};
     const double dr = 2.0 * d.p.dr;
     int nx_t[3] = {0, 0, 0};
-    for (int j = 0; j < d.p.ndim; j++) {
-        double nx = fabs(d.s.xp[j * N + i] - xmin[j]) / dr + 2.0;
+    for (int j = 0; j < ND; j++) {
+        double nx = fabs(xp[j] - xmin[j]) / dr + 2.0;
         nx_t[j] = to_int_x86(nx);
         if (nx_t[j] < 2) nx_t[j] = 2;
     }
     unsigned key;
-    if (d.p.ndim == 2)
+    if (ND == 2)
         key = (unsigned)d.p.cym * (unsigned)(nx_t[0] - 1) + (unsigned)nx_t[1];
     else
         key = (unsigned)d.p.cxm * (unsigned)d.p.czm * (unsigned)(nx_t[1] - 1) +
@@ -91,8 +117,9 @@ __global__ void k_cellreset(Dev d)
     d.s.cend[c] = -10000000;
 }
 
-// cell_info start/end.  Cell ctotal is never reset by the reference (its
-// reset loop stops at ctotal - 1), so its range accumulates across steps.
+// cell_info start/end, and the positions in cell-sorted order.  Cell ctotal
+// is never reset by the reference (its reset loop stops at ctotal - 1), so its
+// range accumulates across steps.
 __global__ void k_cellrange(Dev d)
 {
     const int q = IDX, N = d.p.N;
@@ -107,37 +134,46 @@ __global__ void k_cellrange(Dev d)
         if (first) d.s.cstart[c] = q;
         if (last) d.s.cend[c] = q;
     }
+    store_pos(d.s.xs, q, load_pos(d.s.xh, d.s.pid_sorted[q]));
 }
 
 // partisearching (CPP_3-NNPS.cpp:265-374): neighbours of i in stencil order,
-// descending index inside each cell; inclusion test dst <= h_i + h_j in FP64.
-__global__ void __launch_bounds__(128) k_nnps(Dev d)
+// descending index inside each cell; inclusion dst <= h_i + h_j decided as the
+// reference decides it (sqrt of the FP64 sum of squares), with the sqrt only
+// evaluated when the squared distance is within 1e-10 of the squared radius.
+template <int ND>
+__global__ void __launch_bounds__(128, SPH_MINB) k_nnps(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
     int cnt = 0;
     if (d.s.type[i] != 7) {
-        const int nd = d.p.ndim, nst = (nd == 2) ? 9 : 27, nc = d.s.cell[i];
-        double xi[3] = {0.0, 0.0, 0.0};
-        for (int k = 0; k < nd; k++) xi[k] = d.s.xp[k * N + i];
-        const double hi = d.s.hl[i];
+        constexpr int nd = ND, nst = (ND == 2) ? 9 : 27;
+        const int nc = d.s.cell[i];
+        const Pos pi = load_pos(d.s.xh, i);
+        const double xi[3] = {pi.x, pi.y, pi.z};
         for (int nj = 0; nj < nst; nj++) {
             const int nl = cell_link(d.p, nc, nj);
             if (nl <= 0) continue;
             const int start = d.s.cstart[nl], end = d.s.cend[nl];
             for (int q = start; q <= end; q++) {
-                const int j = d.s.pid_sorted[q];
-                double dst = 0.0;
-                for (int k = 0; k < nd; k++) {
-                    double xj = d.s.xp[k * N + j];
-                    dst = dst + (xi[k] - xj) * (xi[k] - xj);
-                }
-                dst = sqrt(dst);
-                const double ra = (hi + d.s.hl[j]) / 2;
-                if (dst <= 2 * ra && i != j) {
-                    cnt++;
-                    if (cnt <= SPH_NB_CAP) d.s.nbr[(size_t)(cnt - 1) * N + i] = j;
-                    else raise_err(d.s.err, SPH_ERR_NEIGH);
+                const Pos pj = load_pos(d.s.xs, q);
+                const double xj[3] = {pj.x, pj.y, pj.z};
+                double d2 = 0.0;
+                for (int k = 0; k < nd; k++) d2 = d2 + (xi[k] - xj[k]) * (xi[k] - xj[k]);
+                const double ra = (pi.h + pj.h) / 2;
+                const double T = 2 * ra, T2 = T * T;
+                bool in;
+                if (d2 < T2 * (1.0 - 1.0e-10)) in = true;
+                else if (d2 > T2 * (1.0 + 1.0e-10)) in = false;
+                else in = (sqrt(d2) <= T);
+                if (in) {
+                    const int j = d.s.pid_sorted[q];
+                    if (i != j) {
+                        cnt++;
+                        if (cnt <= SPH_NB_CAP) d.s.nbr[(size_t)(cnt - 1) * N + i] = j;
+                        else raise_err(d.s.err, SPH_ERR_NEIGH);
+                    }
                 }
             }
         }
@@ -145,20 +181,17 @@ __global__ void __launch_bounds__(128) k_nnps(Dev d)
     d.s.nnb[i] = cnt;
 }
 
-__device__ __forceinline__ int nbr_count(const Dev& d, int i)
-{
-    int c = d.s.nnb[i];
-    return c > SPH_NB_CAP ? SPH_NB_CAP : c;
-}
-
 // ---------------------------------------------------------------------------
 // density(): fluid porosity (:25-54) and continuity (:57-165) -> rho_c
-__global__ void __launch_bounds__(128) k_density(Dev d)
+template <int ND>
+__global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
-    const int ti = d.s.type[i], nd = d.p.ndim, nn = nbr_count(d, i);
+    constexpr int nd = ND;
+    const int ti = d.s.type[i], nn = nbr_count(d, i);
     const int l = *d.s.step;
+    const PairI I = pair_i<ND>(d, i);
     double por = d.s.porosity[i];
     double pcop = d.s.poro_cop[i];
     if (ti == 1) {
@@ -167,7 +200,7 @@ __global__ void __launch_bounds__(128) k_density(Dev d)
             const int j = d.s.nbr[(size_t)s * N + i];
             if (d.s.type[j] == 2) {
                 double w[4];
-                sph_pair_w(d, i, j, w);
+                pair_w<ND>(d, I, load_pos(d.s.xh, j), w);
                 up = up + d.s.mass[j] * d.s.porosity[j] / d.s.rho[j] * w[3];
                 down = down + d.s.mass[j] / d.s.rho[j] * w[3];
             }
@@ -185,8 +218,8 @@ __global__ void __launch_bounds__(128) k_density(Dev d)
     double rnew = d.s.rho[i];
     if (ti != 7) {
         double up[3] = {0.0, 0.0, 0.0}, down[3] = {0.0, 0.0, 0.0};
-        double vi[3], xi[3];
-        for (int k = 0; k < 3; k++) { vi[k] = d.s.vxp[k * N + i]; xi[k] = d.s.xp[k * N + i]; }
+        double vi[3];
+        for (int k = 0; k < 3; k++) vi[k] = d.s.vxp[k * N + i];
         const bool solid = (ti == 2 || ti == 4), fluid = (ti == 1 || ti == 3);
         const bool moving = (ti >= 1 && ti <= 4);
         for (int s = 0; s < nn; s++) {
@@ -201,13 +234,15 @@ __global__ void __launch_bounds__(128) k_density(Dev d)
             } else {
                 continue;
             }
+            const Pos pj = load_pos(d.s.xh, j);
+            const double xj[3] = {pj.x, pj.y, pj.z};
             double w[4];
-            sph_pair_w(d, i, j, w);
+            pair_w<ND>(d, I, pj, w);
             const double mj = d.s.mass[j];
             if (solid) {
                 for (int k = 0; k < nd; k++) {
                     up[k] = up[k] + mj * (vi[k] - vxj[k]) * w[k];
-                    down[k] = down[k] + mj * (xi[k] - d.s.xp[k * N + j]) * w[k];
+                    down[k] = down[k] + mj * (I.x[k] - xj[k]) * w[k];
                 }
             }
             if (fluid) {
@@ -234,17 +269,19 @@ __global__ void __launch_bounds__(128) k_density(Dev d)
 
 // Shepard filter (:168-188) reading every neighbour's continuity density
 // (Jacobi order), then the local equation of state (CPP_7-1-eos_CR.cpp:22-43).
-__global__ void __launch_bounds__(128) k_shepard_eos(Dev d)
+template <int ND>
+__global__ void __launch_bounds__(128, SPH_MINB) k_shepard_eos(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
     const int ti = d.s.type[i], nn = nbr_count(d, i);
+    const PairI I = pair_i<ND>(d, i);
     double up = 0.0, down = 0.0;
     for (int s = 0; s < nn; s++) {
         const int j = d.s.nbr[(size_t)s * N + i];
         if (d.s.type[j] == ti) {
             double w[4];
-            sph_pair_w(d, i, j, w);
+            pair_w<ND>(d, I, load_pos(d.s.xh, j), w);
             up = up + d.s.mass[j] * w[3];
             down = down + d.s.mass[j] / d.s.rho_c[j] * w[3];
         }
@@ -267,206 +304,22 @@ __global__ void __launch_bounds__(128) k_shepard_eos(Dev d)
 }
 
 // ---------------------------------------------------------------------------
-// constitutive helpers (CPP_8-1-consfactor.cpp, CPP_7-2-constitutive.cpp)
-
-__device__ __forceinline__ void jaumann(double ds[6], const double s[6], const double we[9])
-{
-#define WE(a, b) we[(a) * 3 + (b)]
-    ds[0] = ds[0] + (WE(0, 0) * s[0] + WE(0, 1) * s[3] + WE(0, 2) * s[5]) - (s[0] * WE(0, 0) + s[3] * WE(1, 0) + s[5] * WE(2, 0));
-    ds[1] = ds[1] + (WE(1, 0) * s[3] + WE(1, 1) * s[1] + WE(1, 2) * s[4]) - (s[3] * WE(0, 1) + s[1] * WE(1, 1) + s[4] * WE(2, 1));
-    ds[2] = ds[2] + (WE(2, 0) * s[5] + WE(2, 1) * s[4] + WE(2, 2) * s[2]) - (s[5] * WE(0, 2) + s[4] * WE(1, 2) + s[2] * WE(2, 2));
-    ds[3] = ds[3] + (WE(0, 0) * s[3] + WE(0, 1) * s[1] + WE(0, 2) * s[4]) - (s[0] * WE(0, 1) + s[3] * WE(1, 1) + s[5] * WE(2, 1));
-    ds[4] = ds[4] + (WE(1, 0) * s[5] + WE(1, 1) * s[4] + WE(1, 2) * s[2]) - (s[3] * WE(0, 2) + s[1] * WE(1, 2) + s[4] * WE(2, 2));
-    ds[5] = ds[5] + (WE(0, 0) * s[5] + WE(0, 1) * s[4] + WE(0, 2) * s[2]) - (s[0] * WE(0, 2) + s[3] * WE(1, 2) + s[5] * WE(2, 2));
-#undef WE
-}
-
-// elastic D (only its nonzero pattern is kept: dlam, dmu) -- elastic(),
-// dpmodel1(), dpmodel_bui() share it (:17-59, :301-334, :468-501)
-__device__ __forceinline__ void elastic_consts(const double s[6], double E, double poi, double eps0, double kapa,
-                                               double* dlam, double* dmu, double* sm_out)
-{
-    double sm = (-s[0] + -s[1] + -s[2]) * 0.3333333333;
-    if (sm < 1.0) sm = 1.0;
-    double e0;
-    if (E > 1.0) e0 = E;
-    else e0 = 3 * (1 - 2 * poi) * (1 + eps0) * fabs(sm) / kapa;
-    *dlam = e0 * poi / (1.0 + poi) / (1.0 - 2.0 * poi);
-    *dmu = e0 * 0.5 / (1.0 + poi);
-    *sm_out = sm;
-}
-
-// dsig += D deps, in the reference's dept[ki][kj] * deps[kj] loop order over a
-// dense 6x6 with the zero entries included (0 * x terms keep signed-zero and
-// NaN behaviour identical).
-__device__ __forceinline__ void add_dense(double ds[6], const double D[6][6], const double de[6])
-{
-    for (int a = 0; a < 6; a++)
-        for (int b = 0; b < 6; b++) ds[a] += D[a][b] * de[b];
-}
-
-__device__ __forceinline__ void fill_elastic(double D[6][6], double dlam, double dmu)
-{
-    const double dmu2 = dmu * 2.0;
-    for (int a = 0; a < 6; a++)
-        for (int b = 0; b < 6; b++) D[a][b] = 0.0;
-    D[0][0] = dlam + dmu2; D[1][1] = dlam + dmu2; D[2][2] = dlam + dmu2;
-    D[0][1] = dlam; D[0][2] = dlam; D[1][0] = dlam;
-    D[1][2] = dlam; D[2][0] = dlam; D[2][1] = dlam;
-    D[3][3] = dmu; D[4][4] = dmu; D[5][5] = dmu;
-}
-
-// Drucker-Prager continuum tangent (dpmodel1 / dpmodel_bui, :284-448 /
-// :451-615).  yalf, ykap, yalf_dil are the material constants the reference
-// evaluates with atan/tan/sin/cos each call; they are evaluated once per
-// particle by the host with the same libm calls.
-__device__ __forceinline__ void dp_tangent(double D[6][6], double adps[6], const double s[6], const double de[6],
-                                           double dlam, double dmu, double sm,
-                                           double yalf, double ykap, double yalf_dil)
-{
-    const double dmu2 = dmu * 2.0;
-    double sig0 = -s[0], sig1 = -s[1], sig2 = -s[2];
-    double dx = sig0 - sm, dy = sig1 - sm, dz = sig2 - sm;
-    double dxy = -s[3], dyz = -s[4], dzx = -s[5];
-    double sjj = 0.5 * (dx * dx + dy * dy + dz * dz) + dxy * dxy + dyz * dyz + dzx * dzx;
-    double sj = sqrt(sjj);
-    if ((sj - yalf * sm * 3.0 - ykap) >= 0.0) {
-        double f11 = -yalf + dx / sj * 0.5, f22 = -yalf + dy / sj * 0.5, f33 = -yalf + dz / sj * 0.5;
-        double f12 = dxy / sj * 0.5, f23 = dyz / sj * 0.5, f31 = dzx / sj * 0.5;
-        double fkk = f11 + f22 + f33;
-        double g11 = -yalf_dil + dx / sj * 0.5, g22 = -yalf_dil + dy / sj * 0.5, g33 = -yalf_dil + dz / sj * 0.5;
-        double g12 = dxy / sj * 0.5, g23 = dyz / sj * 0.5, g31 = dzx / sj * 0.5;
-        double hdd = g11 + g22 + g33;
-        double fij = 2.0 * (f11 * g11 + f22 * g22 + f33 * g33) + f12 * g12 + f23 * g23 + f31 * g31;
-        double cc7 = dlam * (fkk * hdd) + dmu * fij + hdd;
-        double dd_ = 1.0 / cc7;
-        double df = dlam * fkk, dg = dlam * hdd;
-        double ramda = (dmu2 * f11 - 3.0 * dlam * yalf) * de[0]
-            + (dmu2 * f22 - 3.0 * dlam * yalf) * de[1]
-            + (dmu2 * f33 - 3.0 * dlam * yalf) * de[2]
-            + dmu * (f12 * de[3] + f23 * de[4] + f31 * de[5]);
-        double ttt = ramda * dd_;
-        if (ttt < 0.0) {
-            double ww[6] = {dg + dmu2 * g11, dg + dmu2 * g22, dg + dmu2 * g33, dmu * g12, dmu * g23, dmu * g31};
-            double zz[6] = {df + dmu2 * f11, df + dmu2 * f22, df + dmu2 * f33, dmu * f12, dmu * f23, dmu * f31};
-            for (int a = 0; a < 6; a++)
-                for (int b = 0; b < 6; b++) D[a][b] = D[a][b] - dd_ * ww[a] * zz[b];
-            adps[0] = ramda * dd_ * f11; adps[1] = ramda * dd_ * f22; adps[2] = ramda * dd_ * f33;
-            adps[3] = ramda * dd_ * f12; adps[4] = ramda * dd_ * f23; adps[5] = ramda * dd_ * f31;
-        }
-    }
-}
-
-// DPModel_check: stress-scaling return onto the cone (:779-819)
-__device__ __forceinline__ void dp_check(const double s[6], double ds[6], double alpha_fai, double k_c, double dt)
-{
-    double ts[6];
-    double sm = (s[0] + s[1] + s[2]) / 3.0;
-    double dx = s[0] - sm, dy = s[1] - sm, dz = s[2] - sm;
-    double sj_2 = 0.5 * (dx * dx + dy * dy + dz * dz) + s[3] * s[3] + s[4] * s[4] + s[5] * s[5];
-    double sj = sqrt(sj_2);
-    for (int a = 0; a < 6; a++) ts[a] = s[a] + ds[a] * dt;
-    double i_1 = ts[0] + ts[1] + ts[2];
-    double rn = (-alpha_fai * i_1 + k_c) / sj;
-    if (rn < 1.0) {
-        ts[0] = rn * (ts[0] - i_1 / 3.0) + i_1 / 3.0;
-        ts[1] = rn * (ts[1] - i_1 / 3.0) + i_1 / 3.0;
-        ts[2] = rn * (ts[2] - i_1 / 3.0) + i_1 / 3.0;
-        ts[3] = rn * ts[3];
-        ts[4] = rn * ts[4];
-        ts[5] = rn * ts[5];
-    }
-    for (int a = 0; a < 6; a++) ds[a] = (ts[a] - s[a]) / dt;
-}
-
-// Particle::deq (Class_particle.cpp:121-143): vsig, veps, divq, divr
-__device__ __forceinline__ void deq(const double s[6], const double ep[6], double* vsig, double* veps,
-                                    double* divq, double* divr)
-{
-    *veps = ep[0] + ep[1] + ep[2];
-    double vs = (s[0] + s[1] + s[2]) / 3;
-    double sxx = s[0] - vs, syy = s[1] - vs, szz = s[2] - vs;
-    double j2 = 0.5 * (sxx * sxx + syy * syy + szz * szz) + s[3] * s[3] + s[4] * s[4] + s[5] * s[5];
-    double q = sqrt(3 * fabs(j2));
-    *vsig = vs;
-    *divq = q;
-    *divr = (vs != 0.0) ? fabs(q / vs) : 0.0;
-}
-
-// Particle::shearstrain (Class_particle.cpp:175-192)
-__device__ __forceinline__ double shearstrain(const double ep[6], double veps)
-{
-    double sxx = ep[0] - veps / 3.0, syy = ep[1] - veps / 3.0, szz = ep[2] - veps / 3.0;
-    double j2 = 0.5 * (sxx * sxx + syy * syy + szz * szz) + ep[3] * ep[3] + ep[4] * ep[4] + ep[5] * ep[5];
-    return sqrt(2.0 * fabs(j2));
-}
-
-// eejcb Jacobi rotations, eps = 1e-3, at most 7 (CPP_7-1-strain.cpp:341-437);
-// returns the diagonal (principal stresses strep).
-__device__ __forceinline__ void eig3(const double s[6], double strep[3])
-{
-    double a[9] = {s[0], s[3], s[5], s[3], s[1], s[4], s[5], s[4], s[2]};
-    const int n = 3;
-    int p = 0, q = 0, l = 1;
-    while (true) {
-        double fm = 0.0;
-        for (int i = 0; i < n; i++)
-            for (int j = 0; j < n; j++) {
-                double dd_ = fabs(a[i * n + j]);
-                if ((i != j) && (dd_ > fm)) { fm = dd_; p = i; q = j; }
-            }
-        if (fm < 0.001) break;
-        if (l > 7) break;
-        l = l + 1;
-        int u = p * n + q, w = p * n + p, t = q * n + p, sidx = q * n + q;
-        double x = -a[u];
-        double y = (a[sidx] - a[w]) / 2.0;
-        double omega = x / sqrt(x * x + y * y);
-        if (y < 0.0) omega = -omega;
-        double sn = 1.0 + sqrt(1.0 - omega * omega);
-        sn = omega / sqrt(2.0 * sn);
-        double cn = sqrt(1.0 - sn * sn);
-        fm = a[w];
-        a[w] = fm * cn * cn + a[sidx] * sn * sn + a[u] * omega;
-        a[sidx] = fm * sn * sn + a[sidx] * cn * cn - a[u] * omega;
-        a[u] = 0.0;
-        a[t] = 0.0;
-        for (int j = 0; j < n; j++)
-            if ((j != p) && (j != q)) {
-                int uu = p * n + j, ww = q * n + j;
-                fm = a[uu];
-                a[uu] = fm * cn + a[ww] * sn;
-                a[ww] = -fm * sn + a[ww] * cn;
-            }
-        for (int i = 0; i < n; i++)
-            if ((i != p) && (i != q)) {
-                int uu = i * n + p, ww = i * n + q;
-                fm = a[uu];
-                a[uu] = fm * cn + a[ww] * sn;
-                a[ww] = -fm * sn + a[ww] * cn;
-            }
-    }
-    strep[0] = a[0]; strep[1] = a[4]; strep[2] = a[8];
-}
-
 // strain_noreg (CPP_7-1-strain.cpp:20-220), the gathered pore pressures and
-// wall stresses of eos (CPP_7-1-eos_CR.cpp:46-177), cal_permeability
-// (CPP_7-2-constitutive.cpp:355-382), strain_to_stress (:13-321),
-// free_surface_check (:453-506) and Stress_eigValue (CPP_7-1-strain.cpp:283-332).
-// The three neighbour sums share one pass over the list, each in list order.
-// Reads sig (stresses of the previous step), writes sig_next.
-__global__ void __launch_bounds__(128) k_strain_stress(Dev d)
+// wall stresses of eos (CPP_7-1-eos_CR.cpp:46-177) and the colour sum of
+// free_surface_check (CPP_7-2-constitutive.cpp:462-480): one pass over the
+// neighbour list, each sum in list order.  Writes de, we, color, prew, prea,
+// and the walls' gathered stress into sig_next (reads the soil stresses of
+// the previous step from sig).
+template <int ND>
+__global__ void __launch_bounds__(128, SPH_MINB) k_strain(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
-    const int ti = d.s.type[i], nd = d.p.ndim, nn = nbr_count(d, i), l = *d.s.step;
-    const double dt = d.p.dt;
-    double ep[6], s[6];
-    for (int k = 0; k < 6; k++) { ep[k] = d.s.eps[k * N + i]; s[k] = d.s.sig[k * N + i]; }
-    if (l == d.p.inip)
-        for (int k = 0; k < 6; k++) ep[k] = 0.0;
-    double vi[3], xi[3];
-    for (int k = 0; k < 3; k++) { vi[k] = d.s.vxp[k * N + i]; xi[k] = d.s.xp[k * N + i]; }
+    constexpr int nd = ND;
+    const int ti = d.s.type[i], nn = nbr_count(d, i);
+    const PairI I = pair_i<ND>(d, i);
+    double vi[3];
+    for (int k = 0; k < 3; k++) vi[k] = d.s.vxp[k * N + i];
     const bool solid = (ti == 2 || ti == 4);
     const bool moving = (ti >= 1 && ti <= 4);
     double up[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, down[3] = {0, 0, 0};
@@ -480,8 +333,9 @@ __global__ void __launch_bounds__(128) k_strain_stress(Dev d)
         const bool wallj = (moving && tj == 0);
         const bool gath = (ti != tj) && ((ti == 2 || ti == 4 || ti == 0) && (tj == 1 || tj == 3 || (ti == 0 && tj == 2)));
         if (!(same || wallj || gath)) continue;
+        const Pos pj = load_pos(d.s.xh, j);
         double w[4];
-        sph_pair_w(d, i, j, w);
+        pair_w<ND>(d, I, pj, w);
         const double mj = d.s.mass[j], rj = d.s.rho[j];
         if (same || wallj) {
             double dvx[3];
@@ -499,9 +353,9 @@ __global__ void __launch_bounds__(128) k_strain_stress(Dev d)
             up[7] = up[7] + mj / rj * dvx[2] * w[1];
             up[8] = up[8] + mj / rj * dvx[2] * w[2];
             if (solid) {
-                down[0] = down[0] + mj / rj * (xi[0] - d.s.xp[0 * N + j]) * w[0];
-                down[1] = down[1] + mj / rj * (xi[1] - d.s.xp[1 * N + j]) * w[1];
-                down[2] = down[2] + mj / rj * (xi[2] - d.s.xp[2 * N + j]) * w[2];
+                down[0] = down[0] + mj / rj * (I.x[0] - pj.x) * w[0];
+                down[1] = down[1] + mj / rj * (I.x[1] - pj.y) * w[1];
+                down[2] = down[2] + mj / rj * (I.x[2] - pj.z) * w[2];
             }
             color = color + mj / rj * 1.0 * w[3];
         }
@@ -529,24 +383,55 @@ __global__ void __launch_bounds__(128) k_strain_stress(Dev d)
         if (fabs(down[2]) > 1.0e-7) { dv[2] = up[2] / down[2]; dv[5] = up[5] / down[2]; dv[8] = up[8] / down[2]; }
     }
     double de[6] = {dv[0], dv[4], dv[8], dv[1] + dv[3], dv[5] + dv[7], dv[6] + dv[2]};
-    double we[9] = {0.0, 0.5 * (dv[1] - dv[3]), 0.5 * (dv[2] - dv[6]),
-                    0.5 * (dv[3] - dv[1]), 0.0, 0.5 * (dv[5] - dv[7]),
-                    0.5 * (dv[6] - dv[2]), 0.5 * (dv[7] - dv[5]), 0.0};
+    double we[6] = {0.5 * (dv[1] - dv[3]), 0.5 * (dv[2] - dv[6]), 0.5 * (dv[3] - dv[1]),
+                    0.5 * (dv[5] - dv[7]), 0.5 * (dv[6] - dv[2]), 0.5 * (dv[7] - dv[5])};
     if (nd == 2) {
         de[2] = 0.0; de[4] = 0.0; de[5] = 0.0;
-        we[2] = 0.0; we[5] = 0.0; we[6] = 0.0; we[7] = 0.0; we[8] = 0.0;
+        we[1] = 0.0; we[3] = 0.0; we[4] = 0.0; we[5] = 0.0;
     }
+    for (int k = 0; k < 6; k++) {
+        d.s.de[k * N + i] = de[k];
+        d.s.we[k * N + i] = we[k];
+    }
+    d.s.color[i] = color;
     // gathered pressures (eos :122-176)
     if (ti == 2 || ti == 0) {
         d.s.prew[i] = (d1 != 0.0) ? u1 / d1 : u1;
         d.s.prea[i] = (d2 != 0.0) ? u2 / d2 : u2;
         if (ti == 0)
-            for (int k = 0; k < 6; k++) s[k] = (dsw != 0.0) ? us[k] / dsw : us[k];
+            for (int k = 0; k < 6; k++) d.s.sig_next[k * N + i] = (dsw != 0.0) ? us[k] / dsw : us[k];
     } else if (ti == 4) {
         d.s.prew[i] = (d3 != 0.0) ? u3 / d3 : u3;
         d.s.prea[i] = (d4 != 0.0) ? u4 / d4 : u4;
     }
-    // permeability (fli == 1)
+}
+
+// cal_permeability (CPP_7-2-constitutive.cpp:355-382), strain_to_stress
+// (:13-321), free_surface_check's correction (:482-504) and Stress_eigValue
+// (CPP_7-1-strain.cpp:283-332), per particle.  Also evaluates the particle's
+// own stress / rho^2 and pore-pressure / rho^2 terms the momentum pass uses.
+template <int ND>
+__global__ void __launch_bounds__(128, SPH_MINB) k_stress(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    const int ti = d.s.type[i], l = *d.s.step;
+    const double dt = d.p.dt;
+    double s[6], ep[6], de[6], we9[9];
+    for (int k = 0; k < 6; k++) {
+        s[k] = (ti == 0) ? d.s.sig_next[k * N + i] : d.s.sig[k * N + i];
+        ep[k] = d.s.eps[k * N + i];
+        de[k] = d.s.de[k * N + i];
+    }
+    if (l == d.p.inip)
+        for (int k = 0; k < 6; k++) ep[k] = 0.0;
+    {
+        double w6[6];
+        for (int k = 0; k < 6; k++) w6[k] = d.s.we[k * N + i];
+        we9[0] = 0.0; we9[1] = w6[0]; we9[2] = w6[1];
+        we9[3] = w6[2]; we9[4] = 0.0; we9[5] = w6[3];
+        we9[6] = w6[4]; we9[7] = w6[5]; we9[8] = 0.0;
+    }
     if (d.p.fli == 1 && ti == 2) {
         double cop = d.s.cop[i];
         const int pt = d.p.permtype;
@@ -565,7 +450,6 @@ __global__ void __launch_bounds__(128) k_strain_stress(Dev d)
         }
         d.s.cop[i] = cop;
     }
-    // strain_to_stress
     double vsig = 0, veps = 0, divq = 0, divr = 0, meps = 0;
     bool have_deq = false;
     if (ti == 1 || ti == 3) {
@@ -610,7 +494,7 @@ __global__ void __launch_bounds__(128) k_strain_stress(Dev d)
         if (dp) dp_tangent(D, adps, s, de, dlam, dmu, sm, d.s.s_yalf[i], d.s.s_ykap[i], (mt == 5) ? d.s.s_yalf_dil[i] : 0.0);
         add_dense(ds, D, de);
         if (dp) dp_check(s, ds, d.s.s_yalf[i], d.s.s_ykap[i], dt);
-        jaumann(ds, s, we);
+        jaumann(ds, s, we9);
         if (ti == 2) {
             for (int a = 0; a < 6; a++) {
                 double ad = d.s.adps[a * N + i];
@@ -635,7 +519,8 @@ __global__ void __launch_bounds__(128) k_strain_stress(Dev d)
         d.s.porosity[i] = et / (1 + et);
         d.s.e[i] = et;
     }
-    // free_surface_check (:453-506)
+    // free_surface_check correction (:482-504)
+    const double color = d.s.color[i];
     const double tmax = d.p.thr_max, tmin = d.p.thr_min, incline = tmax - tmin;
     if (ti == 1) {
         if (color < tmin / 2.0) {
@@ -668,133 +553,200 @@ __global__ void __launch_bounds__(128) k_strain_stress(Dev d)
     double sp[3];
     eig3(s, sp);
     for (int k = 0; k < 3; k++) d.s.strep[k * N + i] = sp[k];
+    // own halves of the momentum pair terms (CPP_9-4-derivation_stress.cpp):
+    // fluids use porosity * sigma / rho / rho, soil and structure sigma / rho / rho
+    const double r = d.s.rho[i];
+    const double pf = (ti == 1 || ti == 3) ? d.s.f_por[i] : 0.0;
     for (int k = 0; k < 6; k++) {
         d.s.sig_next[k * N + i] = s[k];
         d.s.eps[k * N + i] = ep[k];
+        d.s.sr[k * N + i] = (ti == 1 || ti == 3) ? pf * s[k] / r / r : s[k] / r / r;
     }
+    double pp = 0.0;
+    if (ti == 2) {
+        const double satu = d.s.satu[i], por = d.s.s_por[i];
+        pp = (1 - por) * (-satu * d.s.prew[i] + (1 - satu) * d.s.prea[i]) / r / r;
+    } else if (ti == 4) {
+        const double satu = d.s.satu[i];
+        pp = (-satu * d.s.prew[i] + (1 - satu) * d.s.prea[i]) / r / r;
+    }
+    d.s.pp[i] = pp;
 }
 
 // ---------------------------------------------------------------------------
-// symmetric stress-divergence pair term (CPP_9-4-derivation_stress.cpp:55-65)
-__device__ __forceinline__ void stress_pair(double tu[3][3], double mj, const double aj[6], const double ai[6],
-                                            double rj, double ri, const double w[4], bool plus)
-{
-    if (plus) {
-        tu[0][0] = tu[0][0] + mj * (aj[0] / rj / rj + ai[0] / ri / ri) * w[0];
-        tu[0][1] = tu[0][1] + mj * (aj[3] / rj / rj + ai[3] / ri / ri) * w[1];
-        tu[0][2] = tu[0][2] + mj * (aj[5] / rj / rj + ai[5] / ri / ri) * w[2];
-        tu[1][0] = tu[1][0] + mj * (aj[3] / rj / rj + ai[3] / ri / ri) * w[0];
-        tu[1][1] = tu[1][1] + mj * (aj[1] / rj / rj + ai[1] / ri / ri) * w[1];
-        tu[1][2] = tu[1][2] + mj * (aj[4] / rj / rj + ai[4] / ri / ri) * w[2];
-        tu[2][0] = tu[2][0] + mj * (aj[5] / rj / rj + ai[5] / ri / ri) * w[0];
-        tu[2][1] = tu[2][1] + mj * (aj[4] / rj / rj + ai[4] / ri / ri) * w[1];
-        tu[2][2] = tu[2][2] + mj * (aj[2] / rj / rj + ai[2] / ri / ri) * w[2];
-    } else {
-        tu[0][0] = tu[0][0] + mj * (aj[0] / rj / rj - ai[0] / ri / ri) * w[0];
-        tu[0][1] = tu[0][1] + mj * (aj[3] / rj / rj - ai[3] / ri / ri) * w[1];
-        tu[0][2] = tu[0][2] + mj * (aj[5] / rj / rj - ai[5] / ri / ri) * w[2];
-        tu[1][0] = tu[1][0] + mj * (aj[3] / rj / rj - ai[3] / ri / ri) * w[0];
-        tu[1][1] = tu[1][1] + mj * (aj[1] / rj / rj - ai[1] / ri / ri) * w[1];
-        tu[1][2] = tu[1][2] + mj * (aj[4] / rj / rj - ai[4] / ri / ri) * w[2];
-        tu[2][0] = tu[2][0] + mj * (aj[5] / rj / rj - ai[5] / ri / ri) * w[0];
-        tu[2][1] = tu[2][1] + mj * (aj[4] / rj / rj - ai[4] / ri / ri) * w[1];
-        tu[2][2] = tu[2][2] + mj * (aj[2] / rj / rj - ai[2] / ri / ri) * w[2];
-    }
-}
-
-// fluid_acceleration_water/air (+ minor forms), soil_acceleration_noreg,
-// structure_acceleration_noreg (CPP_9-4-derivation_stress.cpp:12-505),
-// artificial_viscosity (CPP_9-3-artificialvis.cpp:12-99),
-// boundary_moving_stress_effect (CPP_9-4:631-721), interact1
-// (CPP_10-interact1.cpp:15-110) and veocity_update (CPP_11-xsph.cpp:11-142):
-// one pass over the neighbour list with one accumulator set per sum, combined
-// afterwards in the reference's call order.  Writes ax, interf, interfss and
-// the updated velocity into vmid (state vx of the reference before XSPH).
-__global__ void __launch_bounds__(128) k_accel(Dev d)
+// fluid_acceleration_water/air (+ minor forms), soil_acceleration_noreg and
+// structure_acceleration_noreg (CPP_9-4-derivation_stress.cpp:12-505): the
+// stress-divergence sums, whose per-pair stress / rho^2 halves were evaluated
+// once per particle by k_stress.  Writes ax = g + sums for particle types 1-4;
+// k_accel_b continues from this value in the reference's order.
+template <int ND>
+__global__ void __launch_bounds__(128, SPH_MINB) k_accel_a(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
-    const int ti = d.s.type[i], nd = d.p.ndim, nn = nbr_count(d, i);
-    const double g[3] = {d.p.gx, d.p.gy, d.p.gz};
-    double si[6];
-    for (int k = 0; k < 6; k++) si[k] = d.s.sig_next[k * N + i];
-    const double ri = d.s.rho[i];
-    double vi[3], xi[3];
-    for (int k = 0; k < 3; k++) { vi[k] = d.s.vxp[k * N + i]; xi[k] = d.s.xp[k * N + i]; }
+    const int ti = d.s.type[i];
     const bool fluid = (ti == 1 || ti == 3);
+    const bool solid = (ti == 2 || ti == 4);
+    if (!fluid && !solid) return;
+    const int nn = nbr_count(d, i);
+    const PairI I = pair_i<ND>(d, i);
+    const double ri = d.s.rho[i];
     const int other = (ti == 1) ? 3 : 1;
     const bool minor = (ti == 1) ? d.p.water_minor : d.p.air_minor;
+    double sri[6];
+    for (int k = 0; k < 6; k++) sri[k] = d.s.sr[k * N + i];
+    double tf[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    const double satu_i = d.s.satu[i];
+    const double prew_i = solid ? d.s.prew[i] : 0.0, prea_i = solid ? d.s.prea[i] : 0.0;
+    const double poro_f = fluid ? d.s.f_por[i] : 0.0;
+    const double poro_s = (ti == 2) ? d.s.s_por[i] : 0.0;
+    const double dens_s = (ti == 2) ? d.s.s_dens[i] : 1.0;
+    // own pore term with the particle's own saturation (used when the
+    // neighbour's saturation is the same)
+    double pi_own = 0.0;
+    if (ti == 2) pi_own = (1 - poro_s) * (-satu_i * prew_i + (1 - satu_i) * prea_i) / dens_s / dens_s;
+    if (ti == 4) pi_own = (-satu_i * prew_i + (1 - satu_i) * prea_i) / ri / ri;
+    for (int q = 0; q < nn; q++) {
+        const int j = d.s.nbr[(size_t)q * N + i];
+        const int tj = d.s.type[j];
+        const bool f_pair = fluid && (tj == ti || tj == other);
+        const bool s_pair = solid && tj == ti;
+        if (!(f_pair || s_pair)) continue;
+        double w[4];
+        pair_w<ND>(d, I, load_pos(d.s.xh, j), w);
+        const double mj = d.s.mass[j];
+        double srj[6];
+        if (s_pair || same_bits(d.s.f_por[j], poro_f)) {
+            for (int k = 0; k < 6; k++) srj[k] = d.s.sr[k * N + j];
+        } else {
+            const double rj = d.s.rho[j];
+            for (int k = 0; k < 6; k++) srj[k] = poro_f * d.s.sig_next[k * N + j] / rj / rj;
+        }
+        if (f_pair && minor) {
+            tf[0][0] = tf[0][0] + mj * (srj[0] - sri[0]) * w[0];
+            tf[0][1] = tf[0][1] + mj * (srj[3] - sri[3]) * w[1];
+            tf[0][2] = tf[0][2] + mj * (srj[5] - sri[5]) * w[2];
+            tf[1][0] = tf[1][0] + mj * (srj[3] - sri[3]) * w[0];
+            tf[1][1] = tf[1][1] + mj * (srj[1] - sri[1]) * w[1];
+            tf[1][2] = tf[1][2] + mj * (srj[4] - sri[4]) * w[2];
+            tf[2][0] = tf[2][0] + mj * (srj[5] - sri[5]) * w[0];
+            tf[2][1] = tf[2][1] + mj * (srj[4] - sri[4]) * w[1];
+            tf[2][2] = tf[2][2] + mj * (srj[2] - sri[2]) * w[2];
+        } else {
+            tf[0][0] = tf[0][0] + mj * (srj[0] + sri[0]) * w[0];
+            tf[0][1] = tf[0][1] + mj * (srj[3] + sri[3]) * w[1];
+            tf[0][2] = tf[0][2] + mj * (srj[5] + sri[5]) * w[2];
+            tf[1][0] = tf[1][0] + mj * (srj[3] + sri[3]) * w[0];
+            tf[1][1] = tf[1][1] + mj * (srj[1] + sri[1]) * w[1];
+            tf[1][2] = tf[1][2] + mj * (srj[4] + sri[4]) * w[2];
+            tf[2][0] = tf[2][0] + mj * (srj[5] + sri[5]) * w[0];
+            tf[2][1] = tf[2][1] + mj * (srj[4] + sri[4]) * w[1];
+            tf[2][2] = tf[2][2] + mj * (srj[2] + sri[2]) * w[2];
+        }
+        if (s_pair) {
+            const double satu = d.s.satu[j];
+            if (ti == 2) {
+                double pj_, pi_;
+                if (same_bits(d.s.s_por[j], poro_s)) {
+                    pj_ = d.s.pp[j];
+                } else {
+                    const double rj = d.s.rho[j];
+                    pj_ = (1 - poro_s) * (-satu * d.s.prew[j] + (1 - satu) * d.s.prea[j]) / rj / rj;
+                }
+                pi_ = same_bits(satu, satu_i) ? pi_own
+                    : (1 - poro_s) * (-satu * prew_i + (1 - satu) * prea_i) / dens_s / dens_s;
+                tf[0][0] = tf[0][0] + mj * (pj_ + pi_) * w[0];
+                tf[1][1] = tf[1][1] + mj * (pj_ + pi_) * w[1];
+                tf[2][2] = tf[2][2] + mj * (pj_ + pi_) * w[2];
+            } else {
+                const double pj_ = d.s.pp[j];
+                const double pi_ = same_bits(satu, satu_i) ? pi_own
+                    : (-satu * prew_i + (1 - satu) * prea_i) / ri / ri;
+                tf[0][0] = tf[0][0] + mj * (pj_ - pi_) * w[0];
+                tf[1][1] = tf[1][1] + mj * (pj_ - pi_) * w[1];
+                tf[2][2] = tf[2][2] + mj * (pj_ - pi_) * w[2];
+            }
+        }
+    }
+    const double g[3] = {d.p.gx, d.p.gy, d.p.gz};
+    double ax[3];
+    for (int k = 0; k < 3; k++) ax[k] = g[k];
+    ax[0] += tf[0][0] + tf[0][1] + tf[0][2];
+    ax[1] += tf[1][0] + tf[1][1] + tf[1][2];
+    ax[2] += tf[2][0] + tf[2][1] + tf[2][2];
+    for (int k = 0; k < 3; k++) d.s.ax[k * N + i] = ax[k];
+}
+
+// artificial_viscosity (CPP_9-3-artificialvis.cpp:12-99),
+// boundary_moving_stress_effect (CPP_9-4-derivation_stress.cpp:631-721),
+// interact1 (CPP_10-interact1.cpp:15-110), soil_damping_geostress
+// (CPP_9-4:849-896) and veocity_update (CPP_11-xsph.cpp:11-142): one pass
+// over the neighbour list with one accumulator set per sum, combined with the
+// stress-divergence result of k_accel_a in the reference's call order.
+// Writes ax, interf, interfss and the updated velocity into vx_next (the
+// reference's vx before XSPH).
+template <int ND>
+__global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    constexpr int nd = ND;
+    const int ti = d.s.type[i], nn = nbr_count(d, i);
+    const PairI I = pair_i<ND>(d, i);
+    const double ri = d.s.rho[i];
+    double vi[3];
+    for (int k = 0; k < 3; k++) vi[k] = d.s.vxp[k * N + i];
+    const bool fluid = (ti == 1 || ti == 3);
+    const bool solid = (ti == 2 || ti == 4);
     const bool moving = (ti >= 1 && ti <= 4);
-    double tf[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};   // stress divergence
     double tb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};   // wall stress
     double tav[3] = {0, 0, 0}, tin[3] = {0, 0, 0}, tdm[3] = {0, 0, 0};
-    const bool damping = (*d.s.step <= d.p.inip) && (ti == 2 || ti == 4);
+    const bool damping = (*d.s.step <= d.p.inip) && solid;
     const double cdi = damping ? d.s.cd[i] : 0.0;
     // artificial viscosity coefficients of particle i
     double ca = 0.0, aa = 0.0, bb = 0.0;
     if (ti == 1) { ca = d.s.f_vpu[i]; aa = d.p.av[0][0]; bb = d.p.av[0][1]; }
     if (ti == 2) { ca = d.s.s_vpu[i]; aa = d.p.av[1][0]; bb = d.p.av[1][1]; }
     if (ti == 3) { ca = d.s.f_vpu[i]; aa = d.p.av[2][0]; bb = d.p.av[2][1]; }
-    // wall-stress operand of particle i (:668-700)
-    double ab[6] = {0, 0, 0, 0, 0, 0};
-    if (fluid) {
-        for (int k = 0; k < 6; k++) ab[k] = si[k];
-    } else if (ti == 2 || ti == 4) {
-        const double satu = d.s.satu[i], pw = d.s.prew[i], pa = d.s.prea[i];
-        ab[0] = si[0] - satu * pw + (1 - satu) * pa;
-        ab[1] = si[1] - satu * pw + (1 - satu) * pa;
-        ab[2] = si[2] - satu * pw + (1 - satu) * pa;
-        ab[3] = si[3]; ab[4] = si[4]; ab[5] = si[5];
+    // wall-stress operand of particle i (:668-700) and its own half
+    double ab[6] = {0, 0, 0, 0, 0, 0}, abr[6] = {0, 0, 0, 0, 0, 0};
+    const double satu_i = d.s.satu[i];
+    if (moving) {
+        double si[6];
+        for (int k = 0; k < 6; k++) si[k] = d.s.sig_next[k * N + i];
+        if (fluid) {
+            for (int k = 0; k < 6; k++) ab[k] = si[k];
+        } else {
+            const double prew_i = d.s.prew[i], prea_i = d.s.prea[i];
+            ab[0] = si[0] - satu_i * prew_i + (1 - satu_i) * prea_i;
+            ab[1] = si[1] - satu_i * prew_i + (1 - satu_i) * prea_i;
+            ab[2] = si[2] - satu_i * prew_i + (1 - satu_i) * prea_i;
+            ab[3] = si[3]; ab[4] = si[4]; ab[5] = si[5];
+        }
+        for (int k = 0; k < 6; k++) abr[k] = ab[k] / ri / ri;
     }
-    const double poro_f = fluid ? d.s.f_por[i] : 0.0;
-    const double poro_s = (ti == 2) ? d.s.s_por[i] : 0.0;
-    const double dens_s = (ti == 2) ? d.s.s_dens[i] : 0.0;
     for (int q = 0; q < nn; q++) {
         const int j = d.s.nbr[(size_t)q * N + i];
         const int tj = d.s.type[j];
-        const bool f_pair = fluid && (tj == ti || tj == other);
-        const bool s_pair = (ti == 2 || ti == 4) && tj == ti;
         const bool av_pair = (ti == tj && ti != 7);
         const bool b_pair = moving && tj == 0;
         const bool in_pair = d.p.fli == 1 && ti != tj;
         const bool dm_pair = damping && tj == ti;
-        if (!(f_pair || s_pair || av_pair || b_pair || in_pair || dm_pair)) continue;
+        if (!(av_pair || b_pair || in_pair || dm_pair)) continue;
+        const Pos pj = load_pos(d.s.xh, j);
         double w[4];
-        sph_pair_w(d, i, j, w);
+        pair_w<ND>(d, I, pj, w);
         const double mj = d.s.mass[j], rj = d.s.rho[j];
-        if (f_pair) {
-            double ai[6], aj[6];
-            for (int k = 0; k < 6; k++) { ai[k] = poro_f * si[k]; aj[k] = poro_f * d.s.sig_next[k * N + j]; }
-            stress_pair(tf, mj, aj, ai, rj, ri, w, !minor);
-        }
-        if (s_pair) {
-            double sj[6];
-            for (int k = 0; k < 6; k++) sj[k] = d.s.sig_next[k * N + j];
-            const double satu = d.s.satu[j];
-            stress_pair(tf, mj, sj, si, rj, ri, w, true);
-            if (ti == 2) {
-                const double pi_ = (1 - poro_s) * (-satu * d.s.prew[i] + (1 - satu) * d.s.prea[i]);
-                const double pj_ = (1 - poro_s) * (-satu * d.s.prew[j] + (1 - satu) * d.s.prea[j]);
-                tf[0][0] = tf[0][0] + mj * (pj_ / rj / rj + pi_ / dens_s / dens_s) * w[0];
-                tf[1][1] = tf[1][1] + mj * (pj_ / rj / rj + pi_ / dens_s / dens_s) * w[1];
-                tf[2][2] = tf[2][2] + mj * (pj_ / rj / rj + pi_ / dens_s / dens_s) * w[2];
-            } else {
-                const double pi_ = -satu * d.s.prew[i] + (1 - satu) * d.s.prea[i];
-                const double pj_ = -satu * d.s.prew[j] + (1 - satu) * d.s.prea[j];
-                tf[0][0] = tf[0][0] + mj * (pj_ / rj / rj - pi_ / ri / ri) * w[0];
-                tf[1][1] = tf[1][1] + mj * (pj_ / rj / rj - pi_ / ri / ri) * w[1];
-                tf[2][2] = tf[2][2] + mj * (pj_ / rj / rj - pi_ / ri / ri) * w[2];
-            }
-        }
+        const double xj[3] = {pj.x, pj.y, pj.z};
         if (av_pair) {
             double inprod = 0.0, dst = 0.0, dx[3];
             for (int k = 0; k < nd; k++) {
                 double dvx = vi[k] - d.s.vxp[k * N + j];
-                dx[k] = xi[k] - d.s.xp[k * N + j];
+                dx[k] = I.x[k] - xj[k];
                 dst = dst + dx[k] * dx[k];
                 inprod = inprod + dvx * dx[k];
             }
-            const double hl = (d.s.hl[j] + d.s.hl[i]) * 0.5;
+            const double hl = (pj.h + I.h) * 0.5;
             const double rou = (rj + ri) * 0.5;
             double paix;
             if (inprod < 0.0) {
@@ -805,21 +757,30 @@ __global__ void __launch_bounds__(128) k_accel(Dev d)
                 paix = 0.0;
             for (int k = 0; k < nd; k++) tav[k] = tav[k] + mj * paix * w[k];
         }
-        if (b_pair) stress_pair(tb, mj, ab, ab, rj, ri, w, true);
-        if (dm_pair)
-            for (int k = 0; k < nd; k++)
-                tdm[k] = tdm[k] + mj / rj * cdi * (vi[k] - d.s.vxp[k * N + j]) * w[3];
+        if (b_pair) {
+            double abj[6];
+            for (int k = 0; k < 6; k++) abj[k] = ab[k] / rj / rj;
+            tb[0][0] = tb[0][0] + mj * (abj[0] + abr[0]) * w[0];
+            tb[0][1] = tb[0][1] + mj * (abj[3] + abr[3]) * w[1];
+            tb[0][2] = tb[0][2] + mj * (abj[5] + abr[5]) * w[2];
+            tb[1][0] = tb[1][0] + mj * (abj[3] + abr[3]) * w[0];
+            tb[1][1] = tb[1][1] + mj * (abj[1] + abr[1]) * w[1];
+            tb[1][2] = tb[1][2] + mj * (abj[4] + abr[4]) * w[2];
+            tb[2][0] = tb[2][0] + mj * (abj[5] + abr[5]) * w[0];
+            tb[2][1] = tb[2][1] + mj * (abj[4] + abr[4]) * w[1];
+            tb[2][2] = tb[2][2] + mj * (abj[2] + abr[2]) * w[2];
+        }
         if (in_pair) {
             double inprod = 0.0, dvx[3];
             for (int k = 0; k < nd; k++) {
-                double dxk = xi[k] - d.s.xp[k * N + j];
+                double dxk = I.x[k] - xj[k];
                 dvx[k] = vi[k] - d.s.vxp[k * N + j];
                 inprod = inprod + dxk * dvx[k];
             }
             if (inprod < 0) {
                 const double w3 = w[3], ga = d.p.g_acc;
                 if (ti == 2 && tj == 1) {
-                    const double sa = d.s.satu[i], po = d.s.porosity[i], cp = d.s.cop[i], fd = d.s.f_dens[j];
+                    const double sa = satu_i, po = d.s.porosity[i], cp = d.s.cop[i], fd = d.s.f_dens[j];
                     for (int k = 0; k < nd; k++)
                         tin[k] = tin[k] + sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3;
                 } else if (ti == 1 && tj == 2) {
@@ -827,7 +788,7 @@ __global__ void __launch_bounds__(128) k_accel(Dev d)
                     for (int k = 0; k < nd; k++)
                         tin[k] = tin[k] + sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3;
                 } else if (ti == 2 && tj == 3) {
-                    const double sa = d.s.satu[i], po = d.s.porosity[i], fd = d.s.f_dens[j];
+                    const double sa = satu_i, po = d.s.porosity[i], fd = d.s.f_dens[j];
                     for (int k = 0; k < nd; k++)
                         tin[k] = tin[k] + (1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3;
                 } else if (ti == 3 && tj == 2) {
@@ -837,15 +798,12 @@ __global__ void __launch_bounds__(128) k_accel(Dev d)
                 }
             }
         }
+        if (dm_pair)
+            for (int k = 0; k < nd; k++)
+                tdm[k] = tdm[k] + mj / rj * cdi * (vi[k] - d.s.vxp[k * N + j]) * w[3];
     }
     double ax[3];
-    for (int k = 0; k < 3; k++) ax[k] = d.s.ax[k * N + i];
-    if (ti >= 1 && ti <= 4) {
-        for (int k = 0; k < 3; k++) ax[k] = g[k];
-        ax[0] += tf[0][0] + tf[0][1] + tf[0][2];
-        ax[1] += tf[1][0] + tf[1][1] + tf[1][2];
-        ax[2] += tf[2][0] + tf[2][1] + tf[2][2];
-    }
+    for (int k = 0; k < 3; k++) ax[k] = d.s.ax[k * N + i];   // g + stress divergence (k_accel_a) or the old value
     if (ti != 7)
         for (int k = 0; k < nd; k++) ax[k] = ax[k] - tav[k];
     if (moving) {
@@ -870,7 +828,6 @@ __global__ void __launch_bounds__(128) k_accel(Dev d)
             d.s.interf[k * N + i] = itf;
         }
     }
-    // soil_damping_geostress while l <= inip (CPP_9-4-derivation_stress.cpp:849-896)
     if (damping) {
         for (int k = 0; k < nd; k++) {
             double vx1 = vi[k] + 0.5 * (axp[k] + ax[k]) * dt;
@@ -923,15 +880,18 @@ __global__ void __launch_bounds__(128) k_accel(Dev d)
 // xsph (CPP_11-xsph.cpp:145-256, Jacobi by construction: reads the velocities
 // before XSPH), tmboundary (CPP_13-boundary.cpp:125-177), check_domain
 // (CPP_13-boundary.cpp:20-68) and update (CPP_12-1-update.cpp:11-55).
-// Reads xp / vx_next, writes xp_next / vx.
-__global__ void __launch_bounds__(128) k_xsph_update(Dev d)
+// Reads xh / vx_next, writes xh_next / vx.
+template <int ND>
+__global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
-    const int ti = d.s.type[i], nd = d.p.ndim, nn = nbr_count(d, i);
+    constexpr int nd = ND;
+    const int ti = d.s.type[i], nn = nbr_count(d, i);
     const double dt = d.p.dt;
-    double vm[3], xi[3];
-    for (int k = 0; k < 3; k++) { vm[k] = d.s.vx_next[k * N + i]; xi[k] = d.s.xp[k * N + i]; }
+    const PairI I = pair_i<ND>(d, i);
+    double vm[3];
+    for (int k = 0; k < 3; k++) vm[k] = d.s.vx_next[k * N + i];
     const bool moving = (ti >= 1 && ti <= 4);
     double vn[3] = {vm[0], vm[1], vm[2]};
     if (d.p.if_move != 2 && moving) {
@@ -948,7 +908,7 @@ __global__ void __launch_bounds__(128) k_xsph_update(Dev d)
                 continue;
             }
             double w[4];
-            sph_pair_w(d, i, j, w);
+            pair_w<ND>(d, I, load_pos(d.s.xh, j), w);
             const double mj = d.s.mass[j], rj = d.s.rho[j];
             for (int k = 0; k < nd; k++)
                 tu[k] = tu[k] + xishu * mj * (d.s.vx_next[k * N + j] - vm[k]) * w[3] / rj;
@@ -965,11 +925,12 @@ __global__ void __launch_bounds__(128) k_xsph_update(Dev d)
         for (int q = 0; q < nn; q++) {
             const int j = d.s.nbr[(size_t)q * N + i];
             if (d.s.type[j] != 0) continue;
+            const Pos pj = load_pos(d.s.xh, j);
+            const double xj[3] = {pj.x, pj.y, pj.z};
             double inprod = 0.0, dst = 0.0;
             for (int k = 0; k < nd; k++) {
-                const double xj = d.s.xp[k * N + j];
-                inprod = inprod + (vn[k] - d.s.interfss[k * N + j]) * (xi[k] - xj);
-                dst = dst + (xi[k] - xj) * (xi[k] - xj);
+                inprod = inprod + (vn[k] - d.s.interfss[k * N + j]) * (I.x[k] - xj[k]);
+                dst = dst + (I.x[k] - xj[k]) * (I.x[k] - xj[k]);
             }
             if (inprod < 0.0) {
                 dst = sqrt(dst);
@@ -977,7 +938,7 @@ __global__ void __launch_bounds__(128) k_xsph_update(Dev d)
                 double beta = 1 + db / (dst - b * dr);
                 beta = fmin(1.5, beta);
                 for (int k = 0; k < nd; k++)
-                    tb[k] = tb[k] + (1 - beta) * (xi[k] - d.s.xp[k * N + j]) * inprod / dst / dst;
+                    tb[k] = tb[k] + (1 - beta) * (I.x[k] - xj[k]) * inprod / dst / dst;
             }
         }
         for (int k = 0; k < nd; k++) vn[k] = vn[k] + tb[k];
@@ -986,12 +947,12 @@ __global__ void __launch_bounds__(128) k_xsph_update(Dev d)
         const double dr = d.p.dr;
         const double bmax[3] = {d.p.xmax, d.p.ymax, d.p.zmax}, bmin[3] = {d.p.xmin, d.p.ymin, d.p.zmin};
         bool hit = false;
-        if (xi[0] - bmax[0] >= -0.5 * dr) hit = true;
-        if (xi[0] - bmin[0] <= 0.5 * dr) hit = true;
-        if (xi[1] - bmax[1] >= -0.5 * dr) hit = true;
-        if (xi[1] - bmin[1] <= 0.5 * dr) hit = true;
-        if (xi[2] - bmax[2] >= -0.5 * dr && nd == 3) hit = true;
-        if (xi[2] - bmin[2] <= 0.5 * dr && nd == 3) hit = true;
+        if (I.x[0] - bmax[0] >= -0.5 * dr) hit = true;
+        if (I.x[0] - bmin[0] <= 0.5 * dr) hit = true;
+        if (I.x[1] - bmax[1] >= -0.5 * dr) hit = true;
+        if (I.x[1] - bmin[1] <= 0.5 * dr) hit = true;
+        if (I.x[2] - bmax[2] >= -0.5 * dr && nd == 3) hit = true;
+        if (I.x[2] - bmin[2] <= 0.5 * dr && nd == 3) hit = true;
         if (hit) {
             const int w0 = d.p.first_vbx_wall;
             for (int k = 0; k < 3; k++) vn[k] = (i > w0) ? d.s.interfss[k * N + w0] : 0.0;
@@ -999,11 +960,11 @@ __global__ void __launch_bounds__(128) k_xsph_update(Dev d)
     }
     // update
     const int loop = *d.s.step - d.p.inip;
-    double xn[3] = {xi[0], xi[1], xi[2]};
+    double xn[3] = {I.x[0], I.x[1], I.x[2]};
     if (ti != 0) {
         for (int k = 0; k < nd; k++) {
             const double vp = d.s.vxp[k * N + i];
-            xn[k] = xi[k] + (vn[k] + vp) * dt * 0.5;
+            xn[k] = I.x[k] + (vn[k] + vp) * dt * 0.5;
             double u = d.s.ux[k * N + i];
             u = (loop == 0) ? 0.0 : u + (vn[k] + vp) * dt * 0.5;
             d.s.ux[k * N + i] = u;
@@ -1016,17 +977,15 @@ __global__ void __launch_bounds__(128) k_xsph_update(Dev d)
         if (mt == 2 || mt == 3 || mt == 4 || mt == 5) {
             for (int k = 0; k < nd; k++) {
                 const double its = d.s.interfss[k * N + i];
-                xn[k] = xi[k] + (its + its) * dt * 0.5;
+                xn[k] = I.x[k] + (its + its) * dt * 0.5;
                 d.s.ux[k * N + i] = d.s.ux[k * N + i] + (its + its) * dt * 0.5;
             }
             d.s.rhop[i] = d.s.rho[i];
             d.s.prep[i] = d.s.pre[i];
         }
     }
-    for (int k = 0; k < 3; k++) {
-        d.s.xp_next[k * N + i] = xn[k];
-        d.s.vx[k * N + i] = vn[k];
-    }
+    store_pos(d.s.xh_next, i, Pos{xn[0], xn[1], xn[2], I.h});
+    for (int k = 0; k < 3; k++) d.s.vx[k * N + i] = vn[k];
 }
 
 __global__ void k_step_done(Dev d)
@@ -1051,8 +1010,9 @@ extern "C" size_t sphk_sort_temp_bytes(int N, int end_bit)
 // before stage k and ev[SPHK_NSTAGES] after the last one.
 extern "C" const char* const sphk_stage_names[] = {
     "k_cellkey", "radix_sort", "k_cellreset", "k_cellrange", "k_nnps",
-    "k_density", "k_shepard_eos", "k_strain_stress", "k_accel", "k_xsph_update", "k_step_done"};
-#define SPHK_NSTAGES 11
+    "k_density", "k_shepard_eos", "k_strain", "k_stress", "k_accel_a", "k_accel_b", "k_xsph_update",
+    "k_step_done"};
+#define SPHK_NSTAGES 13
 #define REC(k) do { if (ev) cudaEventRecord(ev[k], st); } while (0)
 
 // the NNPS stage; returns the number of this library's kernels it launched
@@ -1062,7 +1022,7 @@ extern "C" int sphk_enqueue_nnps(const Dev* dp, void* sort_tmp, size_t sort_byte
     const Dev& d = *dp;
     const int N = d.p.N;
     REC(0);
-    k_cellkey<<<nblk(N, 256), 256, 0, st>>>(d);
+    if (d.p.ndim == 2) k_cellkey<2><<<nblk(N, 256), 256, 0, st>>>(d); else k_cellkey<3><<<nblk(N, 256), 256, 0, st>>>(d);
     REC(1);
     size_t bytes = sort_bytes;
     cub::DeviceRadixSort::SortPairs(sort_tmp, bytes, d.s.key_in, d.s.key_out, d.s.val_in, d.s.pid_sorted,
@@ -1072,7 +1032,7 @@ extern "C" int sphk_enqueue_nnps(const Dev* dp, void* sort_tmp, size_t sort_byte
     REC(3);
     k_cellrange<<<nblk(N, 256), 256, 0, st>>>(d);
     REC(4);
-    k_nnps<<<nblk(N, 128), 128, 0, st>>>(d);
+    if (d.p.ndim == 2) k_nnps<2><<<nblk(N, 128), 128, 0, st>>>(d); else k_nnps<3><<<nblk(N, 128), 128, 0, st>>>(d);
     return 4;
 }
 
@@ -1081,17 +1041,21 @@ extern "C" int sphk_enqueue_physics(const Dev* dp, cudaStream_t st, cudaEvent_t*
     const Dev& d = *dp;
     const int N = d.p.N;
     REC(5);
-    k_density<<<nblk(N, 128), 128, 0, st>>>(d);
+    if (d.p.ndim == 2) k_density<2><<<nblk(N, 128), 128, 0, st>>>(d); else k_density<3><<<nblk(N, 128), 128, 0, st>>>(d);
     REC(6);
-    k_shepard_eos<<<nblk(N, 128), 128, 0, st>>>(d);
+    if (d.p.ndim == 2) k_shepard_eos<2><<<nblk(N, 128), 128, 0, st>>>(d); else k_shepard_eos<3><<<nblk(N, 128), 128, 0, st>>>(d);
     REC(7);
-    k_strain_stress<<<nblk(N, 128), 128, 0, st>>>(d);
+    if (d.p.ndim == 2) k_strain<2><<<nblk(N, 128), 128, 0, st>>>(d); else k_strain<3><<<nblk(N, 128), 128, 0, st>>>(d);
     REC(8);
-    k_accel<<<nblk(N, 128), 128, 0, st>>>(d);
+    if (d.p.ndim == 2) k_stress<2><<<nblk(N, 128), 128, 0, st>>>(d); else k_stress<3><<<nblk(N, 128), 128, 0, st>>>(d);
     REC(9);
-    k_xsph_update<<<nblk(N, 128), 128, 0, st>>>(d);
+    if (d.p.ndim == 2) k_accel_a<2><<<nblk(N, 128), 128, 0, st>>>(d); else k_accel_a<3><<<nblk(N, 128), 128, 0, st>>>(d);
     REC(10);
-    k_step_done<<<1, 32, 0, st>>>(d);
+    if (d.p.ndim == 2) k_accel_b<2><<<nblk(N, 128), 128, 0, st>>>(d); else k_accel_b<3><<<nblk(N, 128), 128, 0, st>>>(d);
     REC(11);
-    return 6;
+    if (d.p.ndim == 2) k_xsph_update<2><<<nblk(N, 128), 128, 0, st>>>(d); else k_xsph_update<3><<<nblk(N, 128), 128, 0, st>>>(d);
+    REC(12);
+    k_step_done<<<1, 32, 0, st>>>(d);
+    REC(13);
+    return 8;
 }

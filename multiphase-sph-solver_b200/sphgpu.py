@@ -15,7 +15,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libsphgpu.so")
+LIB_PATH = os.environ.get("SPHGPU_LIB", os.path.join(HERE, "libsphgpu.so"))
 
 FLUID_FIELDS = ("vis", "vpu", "dens", "paa0", "porosity", "fai", "c",
                 "bhtype", "press_type", "acc_type", "pre_coe", "strain_min")
