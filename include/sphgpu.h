@@ -163,6 +163,9 @@ int sphgpu_set_materials(sphgpu_ctx* ctx, const sphgpu_fluid* fluid,
  */
 int sphgpu_upload_particles(sphgpu_ctx* ctx, const void* particles, int n, size_t stride);
 int sphgpu_download_particles(sphgpu_ctx* ctx, void* particles, int n, size_t stride);
+/* Byte offset and component count of a Particle member in the record layout
+ * the two calls above use; returns SPHGPU_E_ARG for members they skip. */
+int sphgpu_particle_layout(const char* name, size_t* offset, int* ncomp);
 
 /*
  * One or more complete time steps: the body of the main loop of

@@ -541,6 +541,18 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
     return r ? SPHGPU_E_CUDA : 0;
 }
 
+int sphgpu_particle_layout(const char* name, size_t* offset, int* ncomp)
+{
+    if (!name) return SPHGPU_E_ARG;
+    for (const AosMember& m : kAos)
+        if (std::strcmp(m.name, name) == 0) {
+            if (offset) *offset = m.off;
+            if (ncomp) *ncomp = find_field(name)->ncomp;
+            return 0;
+        }
+    return SPHGPU_E_ARG;
+}
+
 int sphgpu_upload_particles(sphgpu_ctx* c, const void* particles, int n, size_t stride)
 {
     if (!c || !particles || n != c->N || stride < kParticleBytes) return SPHGPU_E_ARG;

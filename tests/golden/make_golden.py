@@ -1,0 +1,74 @@
+"""Generate the golden fixtures of tests/golden/ by running the reference solver.
+
+    python tests/golden/make_golden.py
+
+Needs oracle/_ref/libsphref.so, i.e. the reference solver compiled from its own
+sources (make -C oracle ref, which reads the reference source tree).  For each
+case the reference parses the input deck written by scenes.write_input_dat,
+initialises itself, and runs one thread (its deterministic, sequential order).
+Saved per case (.npz): the input deck parameters the reference parsed, the
+initial state, the neighbour lists of step 1 (counts, indices, kernel values),
+and the state after STEPS steps.  The fixtures let the CPU tests pin the
+oracle against the reference where the reference itself is not available.
+"""
+from __future__ import annotations
+
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path[:0] = [os.path.join(REPO, "multiphase-sph-solver_b200"), os.path.join(REPO, "tests")]
+
+import scenes  # noqa: E402
+import sphgpu  # noqa: E402
+from checkers import STATE_FIELDS, Reference  # noqa: E402
+
+CASES = {
+    # name: (scene factory, steps)
+    "dam_break_2d_dx0.04": (lambda: scenes.dam_break_2d(dx=0.04, steps=200), 25),
+    "soil_column_3d_dx0.1": (lambda: scenes.soil_column_3d(dx=0.1, steps=200), 15),
+}
+
+
+def make(name: str) -> str:
+    factory, steps = CASES[name]
+    sc = factory()
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "input.dat")
+        scenes.write_input_dat(sc, path)
+        ref = Reference(path, 1)
+        out["params"] = np.frombuffer(bytes(ref.params), dtype=np.uint8)
+        fl, so = ref.materials()
+        out["fluid"], out["soil"] = fl, so
+        for k in STATE_FIELDS:
+            out["init_" + k] = ref.get_field(k)
+        err, ninflu, influ, wij = ref.nnps(with_wij=True)
+        assert err == 0
+        out["nnps_ninflu"] = ninflu
+        mask = np.arange(100)[None, :] <= ninflu[:, None]
+        out["nnps_influ"] = np.where(mask, influ, 0)
+        out["nnps_wij"] = np.where(mask[:, :, None], wij, 0.0)
+        assert ref.step(steps) == 0
+        out["steps"] = np.array(steps)
+        for k in STATE_FIELDS:
+            out["final_" + k] = ref.get_field(k)
+    fn = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(fn, **out)
+    return fn
+
+
+if __name__ == "__main__":
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    saved = os.dup(1)
+    os.dup2(devnull, 1)   # the reference prints progress lines
+    try:
+        files = [make(n) for n in CASES]
+    finally:
+        os.dup2(saved, 1)
+    for f in files:
+        print(f, os.path.getsize(f))
