@@ -53,16 +53,19 @@ NB_MEAN = 65
 def algorithmic_bytes(stage: str, nb: float = NB_MEAN) -> float:
     row = 4.0 * nb                       # the particle's neighbour-list row
     table = {
-        "k_cellkey": 24 + 12,                                   # xp -> cell, key, value
-        "radix_sort": 3 * 16,                                   # 3 digit passes of (key, value) in+out
-        "k_cellrange": 4 + 8,
-        "k_nnps": 24 + 8 + 8 + 4 + 4 + 4 + row,                 # xp, hl, cell, type, pid | count, list
-        "k_density": 4 + 4 + 8 + 24 + 24 + 8 + 8 + 8 + 8 + 8 + row + 8 + 16,
-        "k_shepard_eos": 4 + 4 + 8 + 8 + 8 + 8 + 8 + 8 + row + 8 + 8,
-        "k_strain_stress": 4 + 4 + 4 + 48 + 48 + 24 + 24 + 8 + 8 + 24 + 32 + 24 + 48 + 8 + 8 + row
-                           + 48 + 48 + 24 + 16 + 48 + 16 + 40,
-        "k_accel": 4 + 4 + 48 + 8 + 24 + 24 + 8 + 8 + 8 + 8 + 8 + 8 + 24 + 24 + 24 + row + 24 + 24 + 24,
-        "k_xsph_update": 4 + 4 + 24 + 24 + 24 + 24 + 24 + 8 + 8 + row + 24 + 24 + 24 + 24 + 8,
+        # reads | writes
+        "k_cellkey": 32 + 12,                                   # (x,y,z,h) | cell, key, value
+        "radix_sort": 3 * 16,                                   # 3 digit passes of (key, value) in + out
+        "k_cellrange": 4 + 4 + 32 + 32 + 8,                     # key, pid, record | sorted record, range
+        "k_nnps": 32 + 4 + 4 + 4 + row,                         # record, cell, type | count, list row
+        "k_density": 4 + 4 + 32 + 8 + 8 + 8 + 24 + 8 + row + 8 + 16,
+        "k_shepard_eos": 4 + 4 + 32 + 8 + 8 + 8 + 8 + row + 8 + 8,
+        "k_strain": 4 + 4 + 32 + 24 + row + 48 + 48 + 8 + 16,
+        "k_stress": 48 + 48 + 48 + 48 + 8 + 4 + 4 + 8 + 8 + 88 + 48 + 8
+                    + 48 + 48 + 48 + 8 + 8 + 40 + 24 + 48 + 8,
+        "k_accel_a": 4 + 4 + 32 + 8 + 48 + 8 + 8 + 8 + 8 + 8 + row + 24,
+        "k_accel_b": 4 + 4 + 32 + 8 + 24 + 48 + 24 + 24 + 24 + 24 + 4 + 8 + 8 + 8 + 24 + row + 24 + 24 + 24,
+        "k_xsph_update": 4 + 4 + 32 + 24 + 24 + 24 + 24 + 8 + 8 + 8 + 8 + 4 + row + 32 + 24 + 24 + 24 + 24 + 8,
     }
     return float(table.get(stage, 0.0))
 
