@@ -208,6 +208,38 @@ int         sphgpu_stage_count(void);
 const char* sphgpu_stage_name(int k);
 int         sphgpu_step_profiled(sphgpu_ctx* ctx, int nsteps, double* stage_ms);
 
+/*
+ * Neighbour search that allocates no device memory (no counterpart in the
+ * reference: an addition of this library).
+ *
+ * For callers that cannot call cudaMalloc where they need neighbour lists --
+ * code under a device-memory pool or budget that forbids new allocations, a
+ * real-time loop that must stay out of the driver's allocator, or a host
+ * application that owns every device buffer and only lends pointers.  The
+ * caller passes device pointers: d_xp (n * 3 doubles, particle-major, as
+ * Particle::xp), d_hl (n doubles), d_type (n ints) in, and d_ninflu (n ints)
+ * and d_influ (n * 100 ints, Par_Cell::influ layout: slots 1..ninflu) out;
+ * `grid` supplies ndim, dr, xmin/ymin/zmin and cxm/cym/czm/ctotal.  The
+ * result equals sphgpu_nnps on the same positions (parttocell +
+ * partisearching, CPP_3-NNPS.cpp:175-374).
+ *
+ * Every intermediate lives in one fixed device array of
+ * sphgpu_nnps_noalloc_scratch_bytes() bytes inside the library, held by each
+ * GPU that loads the library until the process exits; n is limited to
+ * SPHGPU_NOALLOC_MAX_PARTICLES and ctotal to SPHGPU_NOALLOC_MAX_CELLS (larger
+ * sizes return SPHGPU_E_ARG).  The first call on a device looks the array up
+ * with that device current; make it before any stream capture.  All calls on
+ * a device share the array: calls that overlap on the GPU race and must not
+ * be issued.  The call runs on `stream` (a cudaStream_t, NULL for the default
+ * stream), waits for it, and returns 0, 3 (a particle outside the grid; the
+ * outputs are not written) or 5 (more than 99 neighbours).
+ */
+#define SPHGPU_NOALLOC_MAX_PARTICLES 65536
+#define SPHGPU_NOALLOC_MAX_CELLS     262144
+int    sphgpu_nnps_noalloc(const sphgpu_params* grid, int n, const double* d_xp, const double* d_hl,
+                           const int* d_type, int* d_ninflu, int* d_influ, void* stream);
+size_t sphgpu_nnps_noalloc_scratch_bytes(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,8 +17,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsphgpu.so")
-SOURCES = ["sph_kernels.cu", "sph_capi.cu"]
-HEADERS = ["sph_device.cuh", os.path.join("..", "..", "include", "sphgpu.h")]
+SOURCES = ["sph_kernels.cu", "sph_capi.cu", "sph_noalloc.cu"]
+HEADERS = ["sph_device.cuh", "sph_constitutive.cuh", os.path.join("..", "..", "include", "sphgpu.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
