@@ -20,9 +20,9 @@
 extern "C" size_t sphk_sort_temp_bytes(int N, int end_bit);
 extern "C" int sphk_enqueue_nnps(const Dev* d, void* sort_tmp, size_t sort_bytes, int end_bit, cudaStream_t st,
                                  cudaEvent_t* ev);
-extern "C" int sphk_enqueue_physics(const Dev* d, cudaStream_t st, cudaEvent_t* ev);
+extern "C" int sphk_enqueue_physics(const Dev* d, cudaStream_t st, cudaEvent_t* ev, int regu);
 extern "C" const char* const sphk_stage_names[];
-#define SPHK_NSTAGES 13
+#define SPHK_NSTAGES 17
 
 namespace {
 
@@ -91,6 +91,7 @@ struct sphgpu_ctx {
     int sticky = 0;
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
+    bool regu = false;     // graphs include the strain/stress regularisation passes
 };
 
 namespace {
@@ -126,7 +127,7 @@ int check_params(const sphgpu_params* P)
     if (P->step_regu <= 0) return SPHGPU_E_ARG;
     // flag combinations this engine runs (the others are rejected loudly)
     if (P->flbndy != 1) return SPHGPU_E_UNSUPPORTED;
-    if (P->flknl != 1 && P->flknl != 2) return SPHGPU_E_UNSUPPORTED;
+    if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
     if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
     if (P->art_stre_coe > 0.0) return SPHGPU_E_UNSUPPORTED;
     if (P->fli != 0 && P->fli != 1) return SPHGPU_E_UNSUPPORTED;
@@ -150,7 +151,7 @@ int build_graphs(sphgpu_ctx* c)
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
         int n = sphk_enqueue_nnps(&c->d[p], c->sort_tmp, c->sort_bytes, c->end_bit, c->st, nullptr);
-        n += sphk_enqueue_physics(&c->d[p], c->st, nullptr);
+        n += sphk_enqueue_physics(&c->d[p], c->st, nullptr, c->regu ? 1 : 0);
         cudaError_t e = cudaStreamEndCapture(c->st, &g);
         if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
         e = cudaGraphInstantiate(&c->exec[p], g, 0);
@@ -300,6 +301,8 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.xh, 4 * (size_t)N); r |= dalloc(c, &s.xh_next, 4 * (size_t)N); r |= dalloc(c, &s.xs, 4 * (size_t)N);
     r |= dalloc(c, &s.de, 6 * (size_t)N); r |= dalloc(c, &s.we, 6 * (size_t)N); r |= dalloc(c, &s.color, N);
     r |= dalloc(c, &s.sr, 6 * (size_t)N); r |= dalloc(c, &s.pp, N);
+    r |= dalloc(c, &s.eps_tmp, 6 * (size_t)N); r |= dalloc(c, &s.sig_tmp, 6 * (size_t)N);
+    if (P->flknl > 2) r |= dalloc(c, &s.lmat, 9 * (size_t)N);
     r |= dalloc(c, &s.vx, 3 * (size_t)N); r |= dalloc(c, &s.vx_next, 3 * (size_t)N);
     r |= dalloc(c, &s.vxp, 3 * (size_t)N); r |= dalloc(c, &s.axp, 3 * (size_t)N); r |= dalloc(c, &s.ax, 3 * (size_t)N);
     r |= dalloc(c, &s.ux, 3 * (size_t)N);
@@ -604,9 +607,11 @@ int sphgpu_step(sphgpu_ctx* c, int nsteps)
     if (nsteps == 0) return 0;
     int r = check_particles(c);
     if (r) return r;
-    // regularisation passes (strain_regu / stress_regu) are not part of this engine
-    for (int l = c->l_host; l < c->l_host + nsteps; l++)
-        if (l % c->P.step_regu == 0) return SPHGPU_E_UNSUPPORTED;
+    // the regularisation passes (strain_regu / stress_regu) join the step
+    // graphs from the first call whose steps include one with l % step_regu == 0
+    if (!c->regu)
+        for (long long l = c->l_host; l < (long long)c->l_host + nsteps; l++)
+            if (l % c->P.step_regu == 0) { c->regu = true; invalidate_graphs(c); break; }
     cudaSetDevice(c->device);
     if (!c->exec[0] || !c->exec[1]) {
         r = build_graphs(c);
@@ -676,8 +681,9 @@ int sphgpu_step_profiled(sphgpu_ctx* c, int nsteps, double* stage_ms)
     if (c->sticky) return c->sticky;
     int r = check_particles(c);
     if (r) return r;
-    for (int l = c->l_host; l < c->l_host + nsteps; l++)
-        if (l % c->P.step_regu == 0) return SPHGPU_E_UNSUPPORTED;
+    if (!c->regu)
+        for (long long l = c->l_host; l < (long long)c->l_host + nsteps; l++)
+            if (l % c->P.step_regu == 0) { c->regu = true; invalidate_graphs(c); break; }
     cudaSetDevice(c->device);
     cudaEvent_t ev[SPHK_NSTAGES + 1];
     for (int k = 0; k <= SPHK_NSTAGES; k++) CK(cudaEventCreate(&ev[k]));
@@ -686,7 +692,7 @@ int sphgpu_step_profiled(sphgpu_ctx* c, int nsteps, double* stage_ms)
     for (int s = 0; s < nsteps && err == 0; s++) {
         const Dev* d = &c->d[c->parity];
         sphk_enqueue_nnps(d, c->sort_tmp, c->sort_bytes, c->end_bit, c->st, ev);
-        sphk_enqueue_physics(d, c->st, ev);
+        sphk_enqueue_physics(d, c->st, ev, c->regu ? 1 : 0);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(c->st));
         for (int k = 0; k < SPHK_NSTAGES; k++) {

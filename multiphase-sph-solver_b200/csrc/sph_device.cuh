@@ -76,6 +76,9 @@ struct DevState {
     double *color;             // free-surface colour sum
     double *sr;                // stress / rho^2 as the momentum pass uses it, 6N
     double *pp;                // pore-pressure term / rho^2, N
+    double *eps_in;            // strain the constitutive pass starts from: eps, or eps_tmp after strain_regu
+    double *eps_tmp, *sig_tmp; // outputs of the regularisation passes, 6N each
+    double *lmat;              // inverse CSPM matrix per soil/structure particle, 9N (flknl 3/4)
     // NNPS
     int *cell;                 // cell id per particle
     uint32_t *key_in, *key_out;
@@ -123,15 +126,23 @@ __device__ __forceinline__ double kernel_a1(double ra, int ndim, int flknl)
 struct PairI {
     double x[3];
     double h, a1;
+    bool corr;                 // kernel gradient correction applies (flknl 3/4, soil or structure)
+    double L[9];               // its inverse CSPM matrix, row-major
 };
 
-template <int ND>
+template <int ND, int KGC>
 __device__ __forceinline__ PairI pair_i(const Dev& d, int i)
 {
     Pos q = load_pos(d.s.xh, i);
     PairI I;
     I.x[0] = q.x; I.x[1] = q.y; I.x[2] = q.z; I.h = q.h;
     I.a1 = kernel_a1(q.h, ND, d.p.flknl);
+    I.corr = false;
+    if (KGC) {
+        const int t = d.s.type[i];
+        I.corr = (t == 2 || t == 4);
+        for (int k = 0; k < 9; k++) I.L[k] = I.corr ? d.s.lmat[(size_t)k * d.p.N + i] : 0.0;
+    }
     return I;
 }
 
@@ -140,7 +151,27 @@ __device__ __forceinline__ PairI pair_i(const Dev& d, int i)
 // differences, summation order and sqrt, recomputed from this step's
 // positions.  w[0..2] gradient, w[3] value.
 template <int ND>
+__device__ __forceinline__ void pair_w_raw(const Dev& d, const PairI& I, const Pos& pj, double w[4]);
+
+// Kernel value and gradient as the consumers read them: with flknl 3/4 the
+// gradient of a soil or structure particle's pairs is corrected in place by
+// kernel_gradient_correction (CPP_3-NNPS.cpp:464-493): grad' = L^-1 grad,
+// in mat_multiply's order (:85-90).
+template <int ND, int KGC>
 __device__ __forceinline__ void pair_w(const Dev& d, const PairI& I, const Pos& pj, double w[4])
+{
+    pair_w_raw<ND>(d, I, pj, w);
+    if (KGC && I.corr) {
+        const double* a = I.L;
+        double c0 = a[0] * w[0] + a[1] * w[1] + a[2] * w[2];
+        double c1 = a[3] * w[0] + a[4] * w[1] + a[5] * w[2];
+        double c2 = a[6] * w[0] + a[7] * w[1] + a[8] * w[2];
+        w[0] = c0; w[1] = c1; w[2] = c2;
+    }
+}
+
+template <int ND>
+__device__ __forceinline__ void pair_w_raw(const Dev& d, const PairI& I, const Pos& pj, double w[4])
 {
     constexpr int nd = ND;
     const double xj[3] = {pj.x, pj.y, pj.z};

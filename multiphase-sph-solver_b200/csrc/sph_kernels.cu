@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_nnps(Dev d)
 
 // ---------------------------------------------------------------------------
 // density(): fluid porosity (:25-54) and continuity (:57-165) -> rho_c
-template <int ND>
+template <int ND, int KGC>
 __global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
 {
     const int i = IDX, N = d.p.N;
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
     constexpr int nd = ND;
     const int ti = d.s.type[i], nn = nbr_count(d, i);
     const int l = *d.s.step;
-    const PairI I = pair_i<ND>(d, i);
+    const PairI I = pair_i<ND, KGC>(d, i);
     double por = d.s.porosity[i];
     double pcop = d.s.poro_cop[i];
     if (ti == 1) {
@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
             const int j = d.s.nbr[(size_t)s * N + i];
             if (d.s.type[j] == 2) {
                 double w[4];
-                pair_w<ND>(d, I, load_pos(d.s.xh, j), w);
+                pair_w<ND, KGC>(d, I, load_pos(d.s.xh, j), w);
                 up = up + d.s.mass[j] * d.s.porosity[j] / d.s.rho[j] * w[3];
                 down = down + d.s.mass[j] / d.s.rho[j] * w[3];
             }
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
             const Pos pj = load_pos(d.s.xh, j);
             const double xj[3] = {pj.x, pj.y, pj.z};
             double w[4];
-            pair_w<ND>(d, I, pj, w);
+            pair_w<ND, KGC>(d, I, pj, w);
             const double mj = d.s.mass[j];
             if (solid) {
                 for (int k = 0; k < nd; k++) {
@@ -269,19 +269,19 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
 
 // Shepard filter (:168-188) reading every neighbour's continuity density
 // (Jacobi order), then the local equation of state (CPP_7-1-eos_CR.cpp:22-43).
-template <int ND>
+template <int ND, int KGC>
 __global__ void __launch_bounds__(128, SPH_MINB) k_shepard_eos(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
     const int ti = d.s.type[i], nn = nbr_count(d, i);
-    const PairI I = pair_i<ND>(d, i);
+    const PairI I = pair_i<ND, KGC>(d, i);
     double up = 0.0, down = 0.0;
     for (int s = 0; s < nn; s++) {
         const int j = d.s.nbr[(size_t)s * N + i];
         if (d.s.type[j] == ti) {
             double w[4];
-            pair_w<ND>(d, I, load_pos(d.s.xh, j), w);
+            pair_w<ND, KGC>(d, I, load_pos(d.s.xh, j), w);
             up = up + d.s.mass[j] * w[3];
             down = down + d.s.mass[j] / d.s.rho_c[j] * w[3];
         }
@@ -310,14 +310,14 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_shepard_eos(Dev d)
 // neighbour list, each sum in list order.  Writes de, we, color, prew, prea,
 // and the walls' gathered stress into sig_next (reads the soil stresses of
 // the previous step from sig).
-template <int ND>
+template <int ND, int KGC>
 __global__ void __launch_bounds__(128, SPH_MINB) k_strain(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
     constexpr int nd = ND;
     const int ti = d.s.type[i], nn = nbr_count(d, i);
-    const PairI I = pair_i<ND>(d, i);
+    const PairI I = pair_i<ND, KGC>(d, i);
     double vi[3];
     for (int k = 0; k < 3; k++) vi[k] = d.s.vxp[k * N + i];
     const bool solid = (ti == 2 || ti == 4);
@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_strain(Dev d)
         if (!(same || wallj || gath)) continue;
         const Pos pj = load_pos(d.s.xh, j);
         double w[4];
-        pair_w<ND>(d, I, pj, w);
+        pair_w<ND, KGC>(d, I, pj, w);
         const double mj = d.s.mass[j], rj = d.s.rho[j];
         if (same || wallj) {
             double dvx[3];
@@ -410,7 +410,10 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_strain(Dev d)
 // (:13-321), free_surface_check's correction (:482-504) and Stress_eigValue
 // (CPP_7-1-strain.cpp:283-332), per particle.  Also evaluates the particle's
 // own stress / rho^2 and pore-pressure / rho^2 terms the momentum pass uses.
-template <int ND>
+// PHASE 0 does all of it.  Where stress_regu can run (step_regu within the
+// run), PHASE 1 stops after the constitutive update (writing sig_next), the
+// smoothing pass runs, and PHASE 2 continues from the smoothed stresses.
+template <int ND, int PHASE>
 __global__ void __launch_bounds__(128, SPH_MINB) k_stress(Dev d)
 {
     const int i = IDX, N = d.p.N;
@@ -419,12 +422,16 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_stress(Dev d)
     const double dt = d.p.dt;
     double s[6], ep[6], de[6], we9[9];
     for (int k = 0; k < 6; k++) {
-        s[k] = (ti == 0) ? d.s.sig_next[k * N + i] : d.s.sig[k * N + i];
-        ep[k] = d.s.eps[k * N + i];
+        if (PHASE == 2) s[k] = d.s.sig_tmp[k * N + i];
+        else s[k] = (ti == 0) ? d.s.sig_next[k * N + i] : d.s.sig[k * N + i];
+        ep[k] = (PHASE == 2) ? d.s.eps[k * N + i] : d.s.eps_in[k * N + i];
         de[k] = d.s.de[k * N + i];
     }
-    if (l == d.p.inip)
+    if (PHASE != 2 && l == d.p.inip)
         for (int k = 0; k < 6; k++) ep[k] = 0.0;
+    double vsig = 0, veps = 0, divq = 0, divr = 0, meps = 0;
+    bool have_deq = false;
+    if (PHASE != 2) {
     {
         double w6[6];
         for (int k = 0; k < 6; k++) w6[k] = d.s.we[k * N + i];
@@ -450,8 +457,6 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_stress(Dev d)
         }
         d.s.cop[i] = cop;
     }
-    double vsig = 0, veps = 0, divq = 0, divr = 0, meps = 0;
-    bool have_deq = false;
     if (ti == 1 || ti == 3) {
         double viscos1 = d.s.f_vis[i];
         if (ti == 1) {
@@ -519,6 +524,24 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_stress(Dev d)
         d.s.porosity[i] = et / (1 + et);
         d.s.e[i] = et;
     }
+    }   // PHASE != 2
+    if (PHASE == 1) {
+        // stresses before stress_regu, and the invariants of the last deq
+        for (int k = 0; k < 6; k++) {
+            d.s.sig_next[k * N + i] = s[k];
+            d.s.eps[k * N + i] = ep[k];
+        }
+        if (have_deq) {
+            d.s.vsig[i] = vsig; d.s.veps[i] = veps; d.s.divq[i] = divq; d.s.divr[i] = divr;
+            d.s.meps[i] = meps;
+        }
+        return;
+    }
+    if (PHASE == 2 && (ti == 2 || ti == 4)) {
+        vsig = d.s.vsig[i]; veps = d.s.veps[i]; divq = d.s.divq[i]; divr = d.s.divr[i];
+        meps = d.s.meps[i];
+        have_deq = true;
+    }
     // free_surface_check correction (:482-504)
     const double color = d.s.color[i];
     const double tmax = d.p.thr_max, tmin = d.p.thr_min, incline = tmax - tmin;
@@ -579,7 +602,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_stress(Dev d)
 // stress-divergence sums, whose per-pair stress / rho^2 halves were evaluated
 // once per particle by k_stress.  Writes ax = g + sums for particle types 1-4;
 // k_accel_b continues from this value in the reference's order.
-template <int ND>
+template <int ND, int KGC>
 __global__ void __launch_bounds__(128, SPH_MINB) k_accel_a(Dev d)
 {
     const int i = IDX, N = d.p.N;
@@ -589,7 +612,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_a(Dev d)
     const bool solid = (ti == 2 || ti == 4);
     if (!fluid && !solid) return;
     const int nn = nbr_count(d, i);
-    const PairI I = pair_i<ND>(d, i);
+    const PairI I = pair_i<ND, KGC>(d, i);
     const double ri = d.s.rho[i];
     const int other = (ti == 1) ? 3 : 1;
     const bool minor = (ti == 1) ? d.p.water_minor : d.p.air_minor;
@@ -613,7 +636,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_a(Dev d)
         const bool s_pair = solid && tj == ti;
         if (!(f_pair || s_pair)) continue;
         double w[4];
-        pair_w<ND>(d, I, load_pos(d.s.xh, j), w);
+        pair_w<ND, KGC>(d, I, load_pos(d.s.xh, j), w);
         const double mj = d.s.mass[j];
         double srj[6];
         if (s_pair || same_bits(d.s.f_por[j], poro_f)) {
@@ -685,14 +708,14 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_a(Dev d)
 // stress-divergence result of k_accel_a in the reference's call order.
 // Writes ax, interf, interfss and the updated velocity into vx_next (the
 // reference's vx before XSPH).
-template <int ND>
+template <int ND, int KGC>
 __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
     constexpr int nd = ND;
     const int ti = d.s.type[i], nn = nbr_count(d, i);
-    const PairI I = pair_i<ND>(d, i);
+    const PairI I = pair_i<ND, KGC>(d, i);
     const double ri = d.s.rho[i];
     double vi[3];
     for (int k = 0; k < 3; k++) vi[k] = d.s.vxp[k * N + i];
@@ -735,7 +758,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
         if (!(av_pair || b_pair || in_pair || dm_pair)) continue;
         const Pos pj = load_pos(d.s.xh, j);
         double w[4];
-        pair_w<ND>(d, I, pj, w);
+        pair_w<ND, KGC>(d, I, pj, w);
         const double mj = d.s.mass[j], rj = d.s.rho[j];
         const double xj[3] = {pj.x, pj.y, pj.z};
         if (av_pair) {
@@ -881,7 +904,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
 // before XSPH), tmboundary (CPP_13-boundary.cpp:125-177), check_domain
 // (CPP_13-boundary.cpp:20-68) and update (CPP_12-1-update.cpp:11-55).
 // Reads xh / vx_next, writes xh_next / vx.
-template <int ND>
+template <int ND, int KGC>
 __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
 {
     const int i = IDX, N = d.p.N;
@@ -889,7 +912,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
     constexpr int nd = ND;
     const int ti = d.s.type[i], nn = nbr_count(d, i);
     const double dt = d.p.dt;
-    const PairI I = pair_i<ND>(d, i);
+    const PairI I = pair_i<ND, KGC>(d, i);
     double vm[3];
     for (int k = 0; k < 3; k++) vm[k] = d.s.vx_next[k * N + i];
     const bool moving = (ti >= 1 && ti <= 4);
@@ -908,7 +931,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
                 continue;
             }
             double w[4];
-            pair_w<ND>(d, I, load_pos(d.s.xh, j), w);
+            pair_w<ND, KGC>(d, I, load_pos(d.s.xh, j), w);
             const double mj = d.s.mass[j], rj = d.s.rho[j];
             for (int k = 0; k < nd; k++)
                 tu[k] = tu[k] + xishu * mj * (d.s.vx_next[k * N + j] - vm[k]) * w[3] / rj;
@@ -993,6 +1016,98 @@ __global__ void k_step_done(Dev d)
     if (threadIdx.x == 0 && blockIdx.x == 0 && *d.s.err == 0) *d.s.step += 1;
 }
 
+// kernel_gradient_correction (CPP_3-NNPS.cpp:376-496): the inverse of
+// L = sum_j m_j / rho_j (x_j - x_i) (x) grad W_ij over same-phase, wall and
+// soil/structure neighbours of each soil (type 2) or structure (type 4)
+// particle, inverted as inverse_mat_2D / inverse_mat_3D do (:499-558); the
+// pair kernels apply it to the gradients (pair_w).  Uses the densities of the
+// previous step, as the reference does (it runs before density()).
+template <int ND>
+__global__ void __launch_bounds__(128, SPH_MINB) k_kgc(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    const int ti = d.s.type[i];
+    if (!(ti == 2 || ti == 4)) return;
+    const int nn = nbr_count(d, i);
+    const PairI I = pair_i<ND, 0>(d, i);
+    double L[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int q = 0; q < nn; q++) {
+        const int j = d.s.nbr[(size_t)q * N + i];
+        const int tj = d.s.type[j];
+        const bool take = (ti == 2 && (tj == 2 || tj == 0 || tj == 4)) || (ti == 4 && (tj == 4 || tj == 0 || tj == 2));
+        if (!take) continue;
+        const Pos pj = load_pos(d.s.xh, j);
+        const double xj[3] = {pj.x, pj.y, pj.z};
+        double w[4];
+        pair_w<ND, 0>(d, I, pj, w);
+        const double mr = d.s.mass[j] / d.s.rho[j];
+        double xij[3];
+        for (int k = 0; k < ND; k++) xij[k] = xj[k] - I.x[k];
+        for (int a = 0; a < ND; a++)
+            for (int b = 0; b < ND; b++) L[a][b] = L[a][b] + mr * xij[a] * w[b];
+    }
+    double B[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    if (ND == 2) {
+        const double det = L[0][0] * L[1][1] - L[0][1] * L[1][0];
+        if (fabs(det) > 1.0e-5) {
+            B[0][0] = L[1][1] / det; B[0][1] = -L[0][1] / det;
+            B[1][0] = -L[1][0] / det; B[1][1] = L[0][0] / det;
+        } else {
+            B[0][0] = 1.0; B[1][1] = 1.0;
+        }
+    } else {
+        const double det = L[0][0] * (L[1][1] * L[2][2] - L[1][2] * L[2][1]) - L[1][0] * (L[0][1] * L[2][2] - L[0][2] * L[2][1])
+            + L[2][0] * (L[0][1] * L[1][2] - L[0][2] * L[1][1]);
+        if (fabs(det) > 1.0e-5) {
+            B[0][0] = (L[1][1] * L[2][2] - L[1][2] * L[2][1]) / det;
+            B[0][1] = (L[0][2] * L[2][1] - L[0][1] * L[2][2]) / det;
+            B[0][2] = (L[0][1] * L[1][2] - L[0][2] * L[1][1]) / det;
+            B[1][0] = (L[1][2] * L[2][0] - L[1][0] * L[2][2]) / det;
+            B[1][1] = (L[0][0] * L[2][2] - L[0][2] * L[2][0]) / det;
+            B[1][2] = (L[1][0] * L[0][2] - L[0][0] * L[1][2]) / det;
+            B[2][0] = (L[1][0] * L[2][1] - L[1][1] * L[2][0]) / det;
+            B[2][1] = (L[0][1] * L[2][0] - L[0][0] * L[2][1]) / det;
+            B[2][2] = (L[0][0] * L[1][1] - L[1][0] * L[0][1]) / det;
+        } else {
+            B[0][0] = 1.0; B[1][1] = 1.0; B[2][2] = 1.0;
+        }
+    }
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) d.s.lmat[(size_t)(a * 3 + b) * N + i] = B[a][b];
+}
+
+// strain_regu / stress_regu (CPP_7-2-constitutive.cpp:385-450) in Jacobi
+// order: on steps with l % step_regu == 0, dst = the same-phase Shepard
+// average of src; otherwise dst = src.  For the strain, the values read are
+// those after strain_noreg's reset at l == inip (zero_at_inip).
+template <int ND, int KGC>
+__global__ void __launch_bounds__(128, SPH_MINB) k_regu(Dev d, const double* src, double* dst, int zero_at_inip)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    const int l = *d.s.step;
+    const bool zero = zero_at_inip && l == d.p.inip;
+    if (l % d.p.step_regu != 0) {
+        for (int k = 0; k < 6; k++) dst[(size_t)k * N + i] = zero ? 0.0 : src[(size_t)k * N + i];
+        return;
+    }
+    const int ti = d.s.type[i], nn = nbr_count(d, i);
+    const PairI I = pair_i<ND, 0>(d, i);
+    double up[6] = {0, 0, 0, 0, 0, 0}, down = 0.0;
+    for (int q = 0; q < nn; q++) {
+        const int j = d.s.nbr[(size_t)q * N + i];
+        if (d.s.type[j] != ti) continue;
+        double w[4];
+        pair_w<ND, 0>(d, I, load_pos(d.s.xh, j), w);
+        const double mr = d.s.mass[j] / d.s.rho[j];
+        for (int k = 0; k < 6; k++) up[k] = up[k] + mr * w[3] * (zero ? 0.0 : src[(size_t)k * N + j]);
+        down = down + mr * w[3];
+    }
+    for (int k = 0; k < 6; k++)
+        dst[(size_t)k * N + i] = (fabs(down) > 1.0e-6) ? up[k] / down : (zero ? 0.0 : src[(size_t)k * N + i]);
+}
+
 // ---------------------------------------------------------------------------
 // host-side launch sequences (enqueued on `st`, capturable into a graph)
 
@@ -1007,55 +1122,99 @@ extern "C" size_t sphk_sort_temp_bytes(int N, int end_bit)
 }
 
 // Stage names, in launch order; with `ev` non-null, event ev[k] is recorded
-// before stage k and ev[SPHK_NSTAGES] after the last one.
+// before stage k and ev[SPHK_NSTAGES] after the last one (stages a run does
+// not need are recorded with no work between their events).
 extern "C" const char* const sphk_stage_names[] = {
-    "k_cellkey", "radix_sort", "k_cellreset", "k_cellrange", "k_nnps",
-    "k_density", "k_shepard_eos", "k_strain", "k_stress", "k_accel_a", "k_accel_b", "k_xsph_update",
-    "k_step_done"};
-#define SPHK_NSTAGES 13
+    "k_cellkey", "radix_sort", "k_cellreset", "k_cellrange", "k_nnps", "k_kgc",
+    "k_density", "k_shepard_eos", "k_strain", "k_regu_eps", "k_stress", "k_regu_sig", "k_stress_2",
+    "k_accel_a", "k_accel_b", "k_xsph_update", "k_step_done"};
+#define SPHK_NSTAGES 17
 #define REC(k) do { if (ev) cudaEventRecord(ev[k], st); } while (0)
 
-// the NNPS stage; returns the number of this library's kernels it launched
+// launch K<ND> or K<ND, KGC> for the run's dimension and kernel-gradient mode
+#define LAUNCH_ND(K, blocks, threads, ...)                                          \
+    do {                                                                           \
+        if (d.p.ndim == 2) K<2><<<blocks, threads, 0, st>>>(__VA_ARGS__);          \
+        else K<3><<<blocks, threads, 0, st>>>(__VA_ARGS__);                        \
+    } while (0)
+#define LAUNCH_PAIR(K, blocks, threads, ...)                                        \
+    do {                                                                           \
+        const bool kgc = d.p.flknl > 2;                                            \
+        if (d.p.ndim == 2) {                                                       \
+            if (kgc) K<2, 1><<<blocks, threads, 0, st>>>(__VA_ARGS__);             \
+            else K<2, 0><<<blocks, threads, 0, st>>>(__VA_ARGS__);                 \
+        } else {                                                                   \
+            if (kgc) K<3, 1><<<blocks, threads, 0, st>>>(__VA_ARGS__);             \
+            else K<3, 0><<<blocks, threads, 0, st>>>(__VA_ARGS__);                 \
+        }                                                                          \
+    } while (0)
+
+// the NNPS stage (+ kernel gradient correction); returns the number of this
+// library's kernels it launched
 extern "C" int sphk_enqueue_nnps(const Dev* dp, void* sort_tmp, size_t sort_bytes, int end_bit, cudaStream_t st,
                                  cudaEvent_t* ev)
 {
     const Dev& d = *dp;
     const int N = d.p.N;
+    int n = 0;
     REC(0);
-    if (d.p.ndim == 2) k_cellkey<2><<<nblk(N, 256), 256, 0, st>>>(d); else k_cellkey<3><<<nblk(N, 256), 256, 0, st>>>(d);
+    LAUNCH_ND(k_cellkey, nblk(N, 256), 256, d); n++;
     REC(1);
     size_t bytes = sort_bytes;
     cub::DeviceRadixSort::SortPairs(sort_tmp, bytes, d.s.key_in, d.s.key_out, d.s.val_in, d.s.pid_sorted,
                                     N, 0, end_bit, st);
     REC(2);
-    k_cellreset<<<nblk(d.p.ctotal, 256), 256, 0, st>>>(d);
+    k_cellreset<<<nblk(d.p.ctotal, 256), 256, 0, st>>>(d); n++;
     REC(3);
-    k_cellrange<<<nblk(N, 256), 256, 0, st>>>(d);
+    k_cellrange<<<nblk(N, 256), 256, 0, st>>>(d); n++;
     REC(4);
-    if (d.p.ndim == 2) k_nnps<2><<<nblk(N, 128), 128, 0, st>>>(d); else k_nnps<3><<<nblk(N, 128), 128, 0, st>>>(d);
-    return 4;
+    LAUNCH_ND(k_nnps, nblk(N, 128), 128, d); n++;
+    REC(5);
+    if (d.p.flknl > 2) { LAUNCH_ND(k_kgc, nblk(N, 128), 128, d); n++; }
+    return n;
 }
 
-extern "C" int sphk_enqueue_physics(const Dev* dp, cudaStream_t st, cudaEvent_t* ev)
+// the rest of the step; `regu` includes the strain/stress regularisation
+// passes (which act on steps l with l % step_regu == 0)
+extern "C" int sphk_enqueue_physics(const Dev* dp, cudaStream_t st, cudaEvent_t* ev, int regu)
 {
-    const Dev& d = *dp;
+    Dev d = *dp;
+    d.s.eps_in = regu ? d.s.eps_tmp : d.s.eps;
     const int N = d.p.N;
-    REC(5);
-    if (d.p.ndim == 2) k_density<2><<<nblk(N, 128), 128, 0, st>>>(d); else k_density<3><<<nblk(N, 128), 128, 0, st>>>(d);
+    int n = 0;
     REC(6);
-    if (d.p.ndim == 2) k_shepard_eos<2><<<nblk(N, 128), 128, 0, st>>>(d); else k_shepard_eos<3><<<nblk(N, 128), 128, 0, st>>>(d);
+    LAUNCH_PAIR(k_density, nblk(N, 128), 128, d); n++;
     REC(7);
-    if (d.p.ndim == 2) k_strain<2><<<nblk(N, 128), 128, 0, st>>>(d); else k_strain<3><<<nblk(N, 128), 128, 0, st>>>(d);
+    LAUNCH_PAIR(k_shepard_eos, nblk(N, 128), 128, d); n++;
     REC(8);
-    if (d.p.ndim == 2) k_stress<2><<<nblk(N, 128), 128, 0, st>>>(d); else k_stress<3><<<nblk(N, 128), 128, 0, st>>>(d);
+    LAUNCH_PAIR(k_strain, nblk(N, 128), 128, d); n++;
     REC(9);
-    if (d.p.ndim == 2) k_accel_a<2><<<nblk(N, 128), 128, 0, st>>>(d); else k_accel_a<3><<<nblk(N, 128), 128, 0, st>>>(d);
+    if (regu) { LAUNCH_PAIR(k_regu, nblk(N, 128), 128, d, d.s.eps, d.s.eps_tmp, 1); n++; }
     REC(10);
-    if (d.p.ndim == 2) k_accel_b<2><<<nblk(N, 128), 128, 0, st>>>(d); else k_accel_b<3><<<nblk(N, 128), 128, 0, st>>>(d);
+    if (regu) {
+        if (d.p.ndim == 2) k_stress<2, 1><<<nblk(N, 128), 128, 0, st>>>(d);
+        else k_stress<3, 1><<<nblk(N, 128), 128, 0, st>>>(d);
+    } else {
+        if (d.p.ndim == 2) k_stress<2, 0><<<nblk(N, 128), 128, 0, st>>>(d);
+        else k_stress<3, 0><<<nblk(N, 128), 128, 0, st>>>(d);
+    }
+    n++;
     REC(11);
-    if (d.p.ndim == 2) k_xsph_update<2><<<nblk(N, 128), 128, 0, st>>>(d); else k_xsph_update<3><<<nblk(N, 128), 128, 0, st>>>(d);
+    if (regu) { LAUNCH_PAIR(k_regu, nblk(N, 128), 128, d, d.s.sig_next, d.s.sig_tmp, 0); n++; }
     REC(12);
-    k_step_done<<<1, 32, 0, st>>>(d);
+    if (regu) {
+        if (d.p.ndim == 2) k_stress<2, 2><<<nblk(N, 128), 128, 0, st>>>(d);
+        else k_stress<3, 2><<<nblk(N, 128), 128, 0, st>>>(d);
+        n++;
+    }
     REC(13);
-    return 8;
+    LAUNCH_PAIR(k_accel_a, nblk(N, 128), 128, d); n++;
+    REC(14);
+    LAUNCH_PAIR(k_accel_b, nblk(N, 128), 128, d); n++;
+    REC(15);
+    LAUNCH_PAIR(k_xsph_update, nblk(N, 128), 128, d); n++;
+    REC(16);
+    k_step_done<<<1, 32, 0, st>>>(d); n++;
+    REC(17);
+    return n;
 }

@@ -1435,10 +1435,75 @@ int orc_nnps(orc_ctx* c, int* ninflu, int* influ, double* wij)
     return err;
 }
 
+/* inverse_mat_2D / inverse_mat_3D: CPP_3-NNPS.cpp:499-558 */
+static void inverse_2d(double A[3][3], double B[3][3])
+{
+    double det = A[0][0] * A[1][1] - A[0][1] * A[1][0];
+    if (fabs(det) > 1.0e-5) {
+        B[0][0] = A[1][1] / det; B[0][1] = -A[0][1] / det;
+        B[1][0] = -A[1][0] / det; B[1][1] = A[0][0] / det;
+    } else {
+        B[0][0] = 1.0; B[0][1] = 0.0; B[1][0] = 0.0; B[1][1] = 1.0;
+    }
+}
+
+static void inverse_3d(double A[3][3], double B[3][3])
+{
+    double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) - A[1][0] * (A[0][1] * A[2][2] - A[0][2] * A[2][1])
+        + A[2][0] * (A[0][1] * A[1][2] - A[0][2] * A[1][1]);
+    if (fabs(det) > 1.0e-5) {
+        B[0][0] = (A[1][1] * A[2][2] - A[1][2] * A[2][1]) / det;
+        B[0][1] = (A[0][2] * A[2][1] - A[0][1] * A[2][2]) / det;
+        B[0][2] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]) / det;
+        B[1][0] = (A[1][2] * A[2][0] - A[1][0] * A[2][2]) / det;
+        B[1][1] = (A[0][0] * A[2][2] - A[0][2] * A[2][0]) / det;
+        B[1][2] = (A[1][0] * A[0][2] - A[0][0] * A[1][2]) / det;
+        B[2][0] = (A[1][0] * A[2][1] - A[1][1] * A[2][0]) / det;
+        B[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) / det;
+        B[2][2] = (A[0][0] * A[1][1] - A[1][0] * A[0][1]) / det;
+    } else {
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) B[a][b] = (a == b) ? 1.0 : 0.0;
+    }
+}
+
+/* kernel_gradient_correction: CPP_3-NNPS.cpp:376-496.  For soil and structure
+ * particles, the kernel gradients of every pair are multiplied by the inverse
+ * of L = sum_j m_j / rho_j (x_j - x_i) (x) grad W_ij over same-phase, wall and
+ * soil/structure neighbours. */
+static void kernel_gradient_correction(orc_ctx* c)
+{
+    int ndim = c->P.ndim;
+    for (int i = 0; i < c->n; i++) {
+        int ti = c->type[i];
+        if (!(ti == 2 || ti == 4)) continue;
+        double L[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, Li[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj), tj = c->type[j];
+            int take = (ti == 2 && (tj == 2 || tj == 0 || tj == 4)) || (ti == 4 && (tj == 4 || tj == 0 || tj == 2));
+            if (!take) continue;
+            double xij[3];
+            for (int k = 0; k < ndim; k++) xij[k] = c->xp[j * 3 + k] - c->xp[i * 3 + k];
+            for (int a = 0; a < ndim; a++)
+                for (int b = 0; b < ndim; b++)
+                    L[a][b] = L[a][b] + c->mass[j] / c->rho[j] * xij[a] * W(i, nj, b);
+        }
+        if (ndim == 2) inverse_2d(L, Li);
+        else inverse_3d(L, Li);
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            double* w = &W(i, nj, 0);
+            double r0 = Li[0][0] * w[0] + Li[0][1] * w[1] + Li[0][2] * w[2];
+            double r1 = Li[1][0] * w[0] + Li[1][1] * w[1] + Li[1][2] * w[2];
+            double r2 = Li[2][0] * w[0] + Li[2][1] * w[1] + Li[2][2] * w[2];
+            w[0] = r0; w[1] = r1; w[2] = r2;
+        }
+    }
+}
+
 static int check_supported(const sphgpu_params* P)
 {
     if (P->flbndy != 1) return SPHGPU_E_UNSUPPORTED;
-    if (P->flknl > 2) return SPHGPU_E_UNSUPPORTED;
+    if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
     if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
     if (P->art_stre_coe > 0.0) return SPHGPU_E_UNSUPPORTED;
     if (P->fli > 1 || P->ss_type != 0) return SPHGPU_E_UNSUPPORTED;
@@ -1457,6 +1522,7 @@ int orc_step(orc_ctx* c, int nsteps)
         if (err) return err;
         err = partisearching(c);
         if (err) return err;
+        if (P->flknl > 2) kernel_gradient_correction(c);
         density(c);
         strain_noreg(c);
         if (c->l % P->step_regu == 0) regularise(c, c->eps);

@@ -4,7 +4,8 @@ import sys
 import pytest
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-for p in (os.path.join(REPO, "multiphase-sph-solver_b200"), os.path.join(REPO, "tests"), REPO):
+for p in (os.path.join(REPO, "multiphase-sph-solver_b200"), os.path.join(REPO, "tests"),
+          os.path.join(REPO, "tests", "golden"), REPO):
     if p not in sys.path:
         sys.path.insert(0, p)
 

@@ -27,10 +27,20 @@ import scenes  # noqa: E402
 import sphgpu  # noqa: E402
 from checkers import STATE_FIELDS, Reference  # noqa: E402
 
+def _kgc_regu():
+    """The soil column with the Yang-Liu kernel, kernel gradient correction
+    (flknl 4) and strain/stress regularisation every 2 steps."""
+    sc = scenes.soil_column_3d(dx=0.1, steps=200)
+    sc.flags["flknl"] = 4
+    sc.problem["step_regu"] = 2
+    return sc
+
+
 CASES = {
     # name: (scene factory, steps)
     "dam_break_2d_dx0.04": (lambda: scenes.dam_break_2d(dx=0.04, steps=200), 25),
     "soil_column_3d_dx0.1": (lambda: scenes.soil_column_3d(dx=0.1, steps=200), 15),
+    "soil_column_3d_dx0.1_kgc_regu": (_kgc_regu, 9),
 }
 
 

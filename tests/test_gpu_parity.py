@@ -107,6 +107,22 @@ def test_n_steps(name, steps):
     _neighbours_equal(eng, orc)
 
 
+@pytest.mark.parametrize("flknl,step_regu", [(2, 100000000), (3, 4), (4, 3), (1, 1)])
+@pytest.mark.parametrize("name,steps", [("dam_break_2d", 12), ("soil_column_3d", 9)])
+def test_kernel_and_regularisation_variants(name, steps, flknl, step_regu):
+    """Yang-Liu kernel (flknl 2/4), kernel gradient correction (flknl 3/4)
+    and strain/stress regularisation every step_regu steps: bit-identical to
+    the oracle (whose same runs are bit-identical to the reference)."""
+    sc = SCENES[name]()
+    sc.flags["flknl"] = flknl
+    sc.problem["step_regu"] = step_regu
+    _, eng, orc = _engine_and_oracle(sc)
+    for chunk in (2, steps - 2):
+        eng.step(chunk)
+        assert orc.step(chunk) == 0
+    _compare(eng, orc)
+
+
 @pytest.mark.parametrize("name,steps", [("dam_break_2d", 60), ("soil_column_3d", 40)])
 def test_n_steps_vs_libm_pow(name, steps):
     """Against the oracle that calls the C library's pow like the reference."""

@@ -14,7 +14,7 @@ from checkers import (ORC_INPLACE, ORC_JACOBI, ORC_POW_CR, ORC_POW_LIBM, STATE_F
                       Params, Reference, have_reference)
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-CASES = ["dam_break_2d_dx0.04", "soil_column_3d_dx0.1"]
+CASES = ["dam_break_2d_dx0.04", "soil_column_3d_dx0.1", "soil_column_3d_dx0.1_kgc_regu"]
 
 
 def _golden(name):
@@ -61,8 +61,8 @@ def test_golden_initial_state_from_scene(name):
     """scenes.initialise (the engine's host-side set-up) reproduces the
     reference's own initialisation bit for bit."""
     g, p = _golden(name)
-    sc = {"dam_break_2d_dx0.04": lambda: scenes.dam_break_2d(dx=0.04, steps=200),
-          "soil_column_3d_dx0.1": lambda: scenes.soil_column_3d(dx=0.1, steps=200)}[name]()
+    import make_golden
+    sc = make_golden.CASES[name][0]()
     st = scenes.initialise(sc)
     assert bytes(sphgpu.params_from_dict(st.params)) == bytes(p)
     assert np.array_equal(st.fluid, g["fluid"]) and np.array_equal(st.soil, g["soil"])
@@ -159,6 +159,34 @@ def _live(sc, nthreads=1):
     path = os.path.join(d, "input.dat")
     scenes.write_input_dat(sc, path)
     return Reference(path, nthreads)
+
+
+def _variant(factory, flknl, step_regu):
+    sc = factory()
+    sc.flags["flknl"] = flknl
+    sc.problem["step_regu"] = step_regu
+    return sc
+
+
+@needs_ref
+@pytest.mark.parametrize("flknl,step_regu", [(2, 100000000), (3, 4), (4, 3), (1, 1)])
+@pytest.mark.parametrize("factory,steps", [
+    (lambda: scenes.dam_break_2d(dx=0.02, steps=100), 12),
+    (lambda: scenes.soil_column_3d(dx=0.05, steps=100), 8),
+])
+def test_live_reference_kernel_and_regularisation_variants(factory, steps, flknl, step_regu):
+    """Yang-Liu kernel (flknl 2/4), kernel gradient correction (flknl 3/4,
+    CPP_3-NNPS.cpp:376-496) and strain/stress regularisation every step_regu
+    steps (CPP_7-2-constitutive.cpp:385-450): bit-identical to the reference."""
+    sc = _variant(factory, flknl, step_regu)
+    ref = _live(sc)
+    fl, so = ref.materials()
+    orc = Oracle(ref.params, ORC_INPLACE)
+    orc.load_state({k: ref.get_field(k) for k in STATE_FIELDS}, fl, so)
+    assert ref.step(steps) == 0
+    assert orc.step(steps) == 0
+    for k in STATE_FIELDS:
+        assert np.array_equal(orc.get_field(k), ref.get_field(k)), k
 
 
 @needs_ref
