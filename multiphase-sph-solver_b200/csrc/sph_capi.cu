@@ -22,7 +22,6 @@ extern "C" int sphk_enqueue_nnps(const Dev* d, void* sort_tmp, size_t sort_bytes
                                  cudaEvent_t* ev);
 extern "C" int sphk_enqueue_physics(const Dev* d, cudaStream_t st, cudaEvent_t* ev, int regu);
 extern "C" const char* const sphk_stage_names[];
-#define SPHK_NSTAGES 17
 
 namespace {
 
@@ -129,7 +128,6 @@ int check_params(const sphgpu_params* P)
     if (P->flbndy != 1) return SPHGPU_E_UNSUPPORTED;
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
     if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
-    if (P->art_stre_coe > 0.0) return SPHGPU_E_UNSUPPORTED;
     if (P->fli != 0 && P->fli != 1) return SPHGPU_E_UNSUPPORTED;
     if (P->ss_type != 0) return SPHGPU_E_UNSUPPORTED;
     if (P->if_move != 0 && P->if_move != 1) return SPHGPU_E_UNSUPPORTED;
@@ -288,6 +286,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     p.xmin = P->xmin; p.xmax = P->xmax; p.ymin = P->ymin; p.ymax = P->ymax; p.zmin = P->zmin; p.zmax = P->zmax;
     p.st_e = P->structure.e; p.st_poi = P->structure.poi;
     p.g_acc = std::sqrt(P->gx * P->gx + P->gy * P->gy + P->gz * P->gz);   // CPP_10-interact1.cpp:28
+    p.art_stre_coe = P->art_stre_coe;
     DevState& s = d.s;
     int r = 0;
     r |= dalloc(c, &s.type, N); r |= dalloc(c, &s.matype, N); r |= dalloc(c, &s.etype, N); r |= dalloc(c, &s.permtype, N);
@@ -303,6 +302,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.sr, 6 * (size_t)N); r |= dalloc(c, &s.pp, N);
     r |= dalloc(c, &s.eps_tmp, 6 * (size_t)N); r |= dalloc(c, &s.sig_tmp, 6 * (size_t)N);
     if (P->flknl > 2) r |= dalloc(c, &s.lmat, 9 * (size_t)N);
+    if (P->art_stre_coe > 0.0) r |= dalloc(c, &s.rij, 9 * (size_t)N);
     r |= dalloc(c, &s.vx, 3 * (size_t)N); r |= dalloc(c, &s.vx_next, 3 * (size_t)N);
     r |= dalloc(c, &s.vxp, 3 * (size_t)N); r |= dalloc(c, &s.axp, 3 * (size_t)N); r |= dalloc(c, &s.ax, 3 * (size_t)N);
     r |= dalloc(c, &s.ux, 3 * (size_t)N);

@@ -136,6 +136,88 @@ __device__ __forceinline__ double shearstrain(const double ep[6], double veps)
     return sqrt(2.0 * fabs(j2));
 }
 
+// eejcb with its eigenvector matrix v (row-major, v[i*3+j]), as
+// Stress_eigValue uses it for beta / beta_ts (CPP_7-1-strain.cpp:311-330,
+// 341-437).
+__device__ __forceinline__ void eig3v(const double s[6], double strep[3], double v[9])
+{
+    double a[9] = {s[0], s[3], s[5], s[3], s[1], s[4], s[5], s[4], s[2]};
+    const int n = 3;
+    for (int i = 0; i < 9; i++) v[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    int p = 0, q = 0, l = 1;
+    while (true) {
+        double fm = 0.0;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                double dd_ = fabs(a[i * n + j]);
+                if ((i != j) && (dd_ > fm)) { fm = dd_; p = i; q = j; }
+            }
+        if (fm < 0.001) break;
+        if (l > 7) break;
+        l = l + 1;
+        int u = p * n + q, w = p * n + p, t = q * n + p, sidx = q * n + q;
+        double x = -a[u];
+        double y = (a[sidx] - a[w]) / 2.0;
+        double omega = x / sqrt(x * x + y * y);
+        if (y < 0.0) omega = -omega;
+        double sn = 1.0 + sqrt(1.0 - omega * omega);
+        sn = omega / sqrt(2.0 * sn);
+        double cn = sqrt(1.0 - sn * sn);
+        fm = a[w];
+        a[w] = fm * cn * cn + a[sidx] * sn * sn + a[u] * omega;
+        a[sidx] = fm * sn * sn + a[sidx] * cn * cn - a[u] * omega;
+        a[u] = 0.0;
+        a[t] = 0.0;
+        for (int j = 0; j < n; j++)
+            if ((j != p) && (j != q)) {
+                int uu = p * n + j, ww = q * n + j;
+                fm = a[uu];
+                a[uu] = fm * cn + a[ww] * sn;
+                a[ww] = -fm * sn + a[ww] * cn;
+            }
+        for (int i = 0; i < n; i++)
+            if ((i != p) && (i != q)) {
+                int uu = i * n + p, ww = i * n + q;
+                fm = a[uu];
+                a[uu] = fm * cn + a[ww] * sn;
+                a[ww] = -fm * sn + a[ww] * cn;
+            }
+        for (int i = 0; i < n; i++) {
+            int uu = i * n + p, ww = i * n + q;
+            fm = v[uu];
+            v[uu] = fm * cn + v[ww] * sn;
+            v[ww] = -fm * sn + v[ww] * cn;
+        }
+    }
+    strep[0] = a[0]; strep[1] = a[4]; strep[2] = a[8];
+}
+
+// inverse_mat of the artificial stress (CPP_9-5-artificialstress.cpp:297-317):
+// B is left unchanged (zero) when |det| <= 1e-5
+__device__ __forceinline__ void inv3_or_keep(const double A[9], double B[9])
+{
+    const double det = A[0] * (A[4] * A[8] - A[5] * A[7]) - A[3] * (A[1] * A[8] - A[2] * A[7])
+        + A[6] * (A[1] * A[5] - A[2] * A[4]);
+    if (fabs(det) > 1.0e-5) {
+        B[0] = (A[4] * A[8] - A[5] * A[7]) / det;
+        B[1] = (A[2] * A[7] - A[1] * A[8]) / det;
+        B[2] = (A[1] * A[5] - A[2] * A[4]) / det;
+        B[3] = (A[5] * A[6] - A[3] * A[8]) / det;
+        B[4] = (A[0] * A[8] - A[2] * A[6]) / det;
+        B[5] = (A[3] * A[2] - A[0] * A[5]) / det;
+        B[6] = (A[3] * A[7] - A[4] * A[6]) / det;
+        B[7] = (A[1] * A[6] - A[0] * A[7]) / det;
+        B[8] = (A[0] * A[4] - A[3] * A[1]) / det;
+    }
+}
+
+// matrix_multiply (CPP_9-5-artificialstress.cpp:13-26), row-major 3x3
+__device__ __forceinline__ void mul3(const double a[9], const double b[9], double c[9])
+{
+    for (int r = 0; r < 3; r++)
+        for (int q = 0; q < 3; q++) c[r * 3 + q] = a[r * 3] * b[q] + a[r * 3 + 1] * b[3 + q] + a[r * 3 + 2] * b[6 + q];
+}
+
 // eejcb Jacobi rotations, eps = 1e-3, at most 7 (CPP_7-1-strain.cpp:341-437);
 // returns the diagonal (principal stresses strep).
 __device__ __forceinline__ void eig3(const double s[6], double strep[3])

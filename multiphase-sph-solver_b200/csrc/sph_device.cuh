@@ -28,6 +28,7 @@
 #define SPH_NB_CAP 99          // Par_Cell::influ[100], slots 1..99 (Class_NNPS.h:71)
 #define SPH_ERR_CELL 3         // parttocell, CPP_3-NNPS.cpp:247-257
 #define SPH_ERR_NEIGH 5        // partisearching, CPP_3-NNPS.cpp:313-319
+#define SPHK_NSTAGES 18        // entries of sphk_stage_names (one event bracket each)
 
 struct DevParams {
     int N, ndim, flknl, flbndy, fli, if_move, flv, inip, step_regu;
@@ -46,6 +47,7 @@ struct DevParams {
     double xmin, xmax, ymin, ymax, zmin, zmax;
     double st_e, st_poi;       // Para_Structure elastic constants
     double g_acc;              // |g|, interact1 (CPP_10-interact1.cpp:28)
+    double art_stre_coe;       // artificial stress coefficient (0: off)
 };
 
 struct DevState {
@@ -79,6 +81,7 @@ struct DevState {
     double *eps_in;            // strain the constitutive pass starts from: eps, or eps_tmp after strain_regu
     double *eps_tmp, *sig_tmp; // outputs of the regularisation passes, 6N each
     double *lmat;              // inverse CSPM matrix per soil/structure particle, 9N (flknl 3/4)
+    double *rij;               // artificial stress tensor R per soil particle, 9N row-major (art_stre_coe > 0)
     // NNPS
     int *cell;                 // cell id per particle
     uint32_t *key_in, *key_out;

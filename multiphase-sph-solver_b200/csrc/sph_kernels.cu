@@ -596,6 +596,56 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_stress(Dev d)
     d.s.pp[i] = pp;
 }
 
+// The per-particle tensor R_i of artificial_stress_2d / artificial_stress_3d
+// (CPP_9-5-artificialstress.cpp:50-86, 180-234) for soil particles, from the
+// stresses k_stress finished with: in 2-D from the in-plane principal
+// direction, in 3-D R_i = beta^-1 diag(r) beta_ts^-1 with beta = v^T and
+// beta_ts = v the eigenvectors of Stress_eigValue (CPP_7-1-strain.cpp:311-330)
+// and r_k = -coe sigma_k / rho^2 for the tensile principal stresses.
+// Only run when art_stre_coe > 0.
+template <int ND>
+__global__ void __launch_bounds__(128) k_art_rij(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    if (d.s.type[i] != 2) return;
+    double s[6];
+    for (int k = 0; k < 6; k++) s[k] = d.s.sig_next[k * N + i];
+    const double xishu = d.p.art_stre_coe, r = d.s.rho[i];
+    if (ND == 3) {
+        double sp[3], v[9], bt[9], bi[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, bti[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        eig3v(s, sp, v);
+        double st[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, tmp[9], R[9];
+        for (int k = 0; k < 3; k++) st[k * 4] = (sp[k] > 0.0) ? -xishu * sp[k] / r / r : 0.0;
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) bt[a * 3 + b] = v[b * 3 + a];
+        inv3_or_keep(bt, bi);
+        inv3_or_keep(v, bti);
+        mul3(bi, st, tmp);
+        mul3(tmp, bti, R);
+        for (int k = 0; k < 9; k++) d.s.rij[k * N + i] = R[k];
+    } else {
+        const double pi_ = 3.141592653;   // Header_Parameters.h:10
+        double sita;
+        if (fabs(s[0] - s[1]) < 1.0e-6) {
+            if (s[3] > 0.0) sita = -pi_ * 0.78539816325;
+            else if (s[3] < 0.0) sita = pi_ * 0.78539816325;
+            else sita = 0.0;
+        } else
+            sita = 0.5 * atan(2.0 * s[3] / (s[0] - s[1]));
+        const double cs = cos(sita), sn = sin(sita);
+        const double sxx = cs * cs * s[0] + 2.0 * sn * cs * s[3] + sn * sn * s[1];
+        const double syy = sn * sn * s[0] - 2.0 * sn * cs * s[3] + cs * cs * s[1];
+        const double rxx = (sxx > 0.0) ? -xishu * sxx / r / r : 0.0;
+        const double ryy = (syy > 0.0) ? -xishu * syy / r / r : 0.0;
+        const double r01 = (rxx - ryy) * sn * cs;
+        d.s.rij[0 * N + i] = rxx * cs * cs + ryy * sn * sn;
+        d.s.rij[1 * N + i] = r01;
+        d.s.rij[3 * N + i] = r01;
+        d.s.rij[4 * N + i] = rxx * sn * sn + ryy * cs * cs;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // fluid_acceleration_water/air (+ minor forms), soil_acceleration_noreg and
 // structure_acceleration_noreg (CPP_9-4-derivation_stress.cpp:12-505): the
@@ -700,7 +750,8 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_a(Dev d)
     for (int k = 0; k < 3; k++) d.s.ax[k * N + i] = ax[k];
 }
 
-// artificial_viscosity (CPP_9-3-artificialvis.cpp:12-99),
+// artificial_viscosity (CPP_9-3-artificialvis.cpp:12-99), the pair sum of
+// artificial_stress_2d/_3d (CPP_9-5-artificialstress.cpp, ART = 1),
 // boundary_moving_stress_effect (CPP_9-4-derivation_stress.cpp:631-721),
 // interact1 (CPP_10-interact1.cpp:15-110), soil_damping_geostress
 // (CPP_9-4:849-896) and veocity_update (CPP_11-xsph.cpp:11-142): one pass
@@ -708,7 +759,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_a(Dev d)
 // stress-divergence result of k_accel_a in the reference's call order.
 // Writes ax, interf, interfss and the updated velocity into vx_next (the
 // reference's vx before XSPH).
-template <int ND, int KGC>
+template <int ND, int KGC, int ART = 0>
 __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
 {
     const int i = IDX, N = d.p.N;
@@ -723,8 +774,9 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
     const bool solid = (ti == 2 || ti == 4);
     const bool moving = (ti >= 1 && ti <= 4);
     double tb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};   // wall stress
-    double tav[3] = {0, 0, 0}, tin[3] = {0, 0, 0}, tdm[3] = {0, 0, 0};
+    double tav[3] = {0, 0, 0}, tin[3] = {0, 0, 0}, tdm[3] = {0, 0, 0}, tu[3] = {0, 0, 0};
     const bool damping = (*d.s.step <= d.p.inip) && solid;
+    const bool art = ART && ti == 2;   // artificial stress (art_stre_coe > 0)
     const double cdi = damping ? d.s.cd[i] : 0.0;
     // artificial viscosity coefficients of particle i
     double ca = 0.0, aa = 0.0, bb = 0.0;
@@ -755,6 +807,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
         const bool b_pair = moving && tj == 0;
         const bool in_pair = d.p.fli == 1 && ti != tj;
         const bool dm_pair = damping && tj == ti;
+        const bool as_pair = art && tj == 2;
         if (!(av_pair || b_pair || in_pair || dm_pair)) continue;
         const Pos pj = load_pos(d.s.xh, j);
         double w[4];
@@ -824,11 +877,35 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
         if (dm_pair)
             for (int k = 0; k < nd; k++)
                 tdm[k] = tdm[k] + mj / rj * cdi * (vi[k] - d.s.vxp[k * N + j]) * w[3];
+        if (as_pair) {
+            // artificial_stress_2d/_3d pair sum (CPP_9-5-artificialstress.cpp:
+            // 100-140, 248-290): f_ij = (W(q) / W(dr))^2.55 of the cubic
+            // spline, m_j f_ij (R_i + R_j) grad W_ij
+            double dst = 0.0;
+            for (int k = 0; k < 3; k++) dst = dst + (I.x[k] - xj[k]) * (I.x[k] - xj[k]);
+            dst = sqrt(dst);
+            const double hl = (I.h + pj.h) * 0.5;
+            const double qd = dst / hl;
+            double f;
+            if (qd >= 0.0 && qd < 1.0) f = pow((0.666666666666667 - qd * qd + 0.5 * qd * qd * qd) * 3.82300884955752, 2.55);
+            else if (qd >= 1.0 && qd < 2.0) f = pow((2.0 - qd) * (2.0 - qd) * (2.0 - qd) * 0.629737609329447, 2.55);
+            else f = 0.0;
+            for (int a = 0; a < nd; a++) {
+                double acc = tu[a];
+                for (int b = 0; b < nd; b++) {
+                    const int c = a * 3 + b;
+                    acc = acc + mj * f * (d.s.rij[(size_t)c * N + i] + d.s.rij[(size_t)c * N + j]) * w[b];
+                }
+                tu[a] = acc;
+            }
+        }
     }
     double ax[3];
     for (int k = 0; k < 3; k++) ax[k] = d.s.ax[k * N + i];   // g + stress divergence (k_accel_a) or the old value
     if (ti != 7)
         for (int k = 0; k < nd; k++) ax[k] = ax[k] - tav[k];
+    if (art)
+        for (int k = 0; k < nd; k++) ax[k] = ax[k] + tu[k];
     if (moving) {
         ax[0] += tb[0][0] + tb[0][1] + tb[0][2];
         ax[1] += tb[1][0] + tb[1][1] + tb[1][2];
@@ -1127,8 +1204,8 @@ extern "C" size_t sphk_sort_temp_bytes(int N, int end_bit)
 extern "C" const char* const sphk_stage_names[] = {
     "k_cellkey", "radix_sort", "k_cellreset", "k_cellrange", "k_nnps", "k_kgc",
     "k_density", "k_shepard_eos", "k_strain", "k_regu_eps", "k_stress", "k_regu_sig", "k_stress_2",
-    "k_accel_a", "k_accel_b", "k_xsph_update", "k_step_done"};
-#define SPHK_NSTAGES 17
+    "k_art_rij", "k_accel_a", "k_accel_b", "k_xsph_update", "k_step_done"};
+static_assert(sizeof(sphk_stage_names) / sizeof(sphk_stage_names[0]) == SPHK_NSTAGES, "stage table");
 #define REC(k) do { if (ev) cudaEventRecord(ev[k], st); } while (0)
 
 // launch K<ND> or K<ND, KGC> for the run's dimension and kernel-gradient mode
@@ -1208,13 +1285,28 @@ extern "C" int sphk_enqueue_physics(const Dev* dp, cudaStream_t st, cudaEvent_t*
         n++;
     }
     REC(13);
-    LAUNCH_PAIR(k_accel_a, nblk(N, 128), 128, d); n++;
+    const bool art = d.p.art_stre_coe > 0.0;
+    if (art) { LAUNCH_ND(k_art_rij, nblk(N, 128), 128, d); n++; }
     REC(14);
-    LAUNCH_PAIR(k_accel_b, nblk(N, 128), 128, d); n++;
+    LAUNCH_PAIR(k_accel_a, nblk(N, 128), 128, d); n++;
     REC(15);
-    LAUNCH_PAIR(k_xsph_update, nblk(N, 128), 128, d); n++;
+    if (art) {
+        const bool kgc = d.p.flknl > 2;
+        if (d.p.ndim == 2) {
+            if (kgc) k_accel_b<2, 1, 1><<<nblk(N, 128), 128, 0, st>>>(d);
+            else k_accel_b<2, 0, 1><<<nblk(N, 128), 128, 0, st>>>(d);
+        } else {
+            if (kgc) k_accel_b<3, 1, 1><<<nblk(N, 128), 128, 0, st>>>(d);
+            else k_accel_b<3, 0, 1><<<nblk(N, 128), 128, 0, st>>>(d);
+        }
+    } else {
+        LAUNCH_PAIR(k_accel_b, nblk(N, 128), 128, d);
+    }
+    n++;
     REC(16);
-    k_step_done<<<1, 32, 0, st>>>(d); n++;
+    LAUNCH_PAIR(k_xsph_update, nblk(N, 128), 128, d); n++;
     REC(17);
+    k_step_done<<<1, 32, 0, st>>>(d); n++;
+    REC(18);
     return n;
 }

@@ -209,6 +209,65 @@ def soil_column_3d(dx: float = 0.005, block=(1.0, 0.5, 0.5), box=(2.0, 0.5, 0.6)
     )
 
 
+def slope_2d(H: float = 5.0, dx: float = 0.05, crest: float = 6.25, gradient: float = 1.5,
+             runout: float | None = None, layers: int = 3, steps: int = 20000, c: float = 10.0e3,
+             fai: float = 25.0, E: float = 2.0e7, art_stre_coe: float = 0.0, matype: int = 2) -> Scene:
+    """2-D cohesive-frictional slope: a soil body (type 2, Drucker-Prager,
+    rho = 2000, E = 20 MPa, nu = 0.3, dry) of height H with a crest of
+    `crest` metres behind a 1:`gradient` face, on a 3-layer floor between a
+    back wall and a far wall (type 0).  Soil area = crest H + gradient H^2 / 2
+    (20,000 particles at H = 5, dx = 0.05)."""
+    g = 9.81
+    if runout is None:
+        runout = max(1.0, 0.5 * H)
+    L = crest + gradient * H + runout
+    nx, ny = int(round(L / dx)), int(round((H + 2 * dx) / dx))
+    grid = _grid2(nx, ny, dx, (0.0, 0.0))
+    x, y = grid[:, 0], grid[:, 1]
+    inside = (y < H) & ((x < crest) | (y < H - (x - crest) / gradient))
+    soil = grid[inside]
+    wall_h = H + 4 * dx
+    nwy = int(round(wall_h / dx))
+    parts = [(soil, 2, matype)]
+    parts.append((_grid2(nx + 2 * layers, layers, dx, (-layers * dx, -layers * dx)), 0, 0))
+    parts.append((_grid2(layers, nwy, dx, (-layers * dx, 0.0)), 0, 0))
+    parts.append((_grid2(layers, nwy, dx, (nx * dx, 0.0)), 0, 0))
+    xp, vxp, ptype, mt, permtype, etype = _assemble(parts)
+    dp = soil_default()
+    dp.update(kapa=0.05, poi=0.3, dens=2000.0, c=c, fai=fai, fs=1.0, beta=0.0,
+              damp1=0.0, damp2=0.0, cop=1.0e-4, eps0=0.0, e=E, ds=1.0e-3)
+    w = fluid_default()
+    w.update(dens=1000.0, vis=1.0e-3, vpu=30.0, press_type=0, acc_type=0, bhtype=0,
+             pre_coe=30.0 * 30.0 / (7.0 * g * dx), strain_min=1.0e-3)
+    mflags = [0] * 10
+    mflags[matype % 10] = 1
+    return Scene(
+        name=f"slope_2d_H{H:g}_dx{dx:g}", ndim=2, dr=dx, dt=0.25 * dx / 600.0 * steps, loop=steps,
+        xp=xp, vxp=vxp, ptype=ptype, matype=mt, permtype=permtype, etype=etype,
+        flags=dict(fla=0, fls=1, flr=0, fli=0, flv=0, fleob=0, flts=0, flspv=0, flknl=1,
+                   ntd=1, flbndy=1),
+        problem=dict(threshold_min=0.1, threshold_max=0.12, fop=max(steps, 1), inip=0,
+                     step_regu=100000000, dttype=2,
+                     xsph=(0.5, 0.1, 0.0), art_vis=((0.1, 0.0), (0.1, 0.0), (0.0, 0.0)),
+                     art_stre_coe=art_stre_coe, g=(0.0, -g, 0.0),
+                     interc=0.0, permtype=0, pers=0.0, perl=0.0, perm=0.0,
+                     ss=(0, 0.0, 0.0, 0), if_cal=0, if_move=0, coe_bndy=0.3),
+        water=[w, copy.deepcopy(w), copy.deepcopy(w)],
+        model_flags=tuple(mflags),
+        soils={matype: dp},
+    )
+
+
+def uplift(scene: Scene, axis: int, above: float, v: float = 0.5) -> Scene:
+    """Give the soil particles (type 2) above coordinate `above` along `axis`
+    an initial velocity v along that axis, which stretches the soil body and
+    puts its upper part in tension (used with art_stre_coe > 0 so that the
+    tensile branch of the artificial stress acts)."""
+    up = (scene.ptype == 2) & (scene.xp[:, axis] > above)
+    scene.vxp[up, axis] = v
+    return scene
+
+
 def scaled_loop(scene: Scene) -> int:
     """Steps the reference will run: for dttype 2 the loop count is
     int(tt / dt) + 1 with tt the input dt (CPP_12-2-dt.cpp:13-20)."""

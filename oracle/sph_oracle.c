@@ -39,6 +39,7 @@ struct orc_ctx {
     /* scratch */
     double* vx_temp;
     double* snap;                        /* Jacobi snapshots */
+    double* rij;                         /* clRaij per particle (9), persistent */
 };
 
 /* ------------------------------------------------------------------------- */
@@ -109,6 +110,7 @@ orc_ctx* orc_create(const sphgpu_params* p)
     for (int i = 0; i < nc; i++) { c->ci_start[i] = 2000000; c->ci_end[i] = -2000000; } /* cell_info() */
     c->vx_temp = (double*)calloc((size_t)n * 3, sizeof(double));
     c->snap = (double*)calloc((size_t)n * 6, sizeof(double));
+    c->rij = (double*)calloc((size_t)n * 9, sizeof(double));   /* clRaij() zeroes Rij */
     return c;
 }
 
@@ -118,7 +120,7 @@ void orc_destroy(orc_ctx* c)
     for (size_t f = 0; f < NFIELDS; f++) free(*(void**)((char*)c + k_fields[f].off));
     free(c->fl); free(c->so); free(c->pc_cell_id); free(c->ninflu); free(c->influ); free(c->wij);
     free(c->srt_cell); free(c->srt_pid); free(c->tmp_cell); free(c->tmp_pid);
-    free(c->ci_start); free(c->ci_end); free(c->vx_temp); free(c->snap);
+    free(c->ci_start); free(c->ci_end); free(c->vx_temp); free(c->snap); free(c->rij);
     free(c);
 }
 
@@ -1144,6 +1146,113 @@ static void artificial_viscosity(orc_ctx* c)
     }
 }
 
+/* matrix_multiply / inverse_mat of the artificial stress:
+ * CPP_9-5-artificialstress.cpp:13-26, 297-317 (the inverse is left zero when
+ * |det| <= 1e-5) */
+static void mat3_mul(double a[3][3], double b[3][3], double c[3][3])
+{
+    for (int r = 0; r < 3; r++)
+        for (int q = 0; q < 3; q++) c[r][q] = a[r][0] * b[0][q] + a[r][1] * b[1][q] + a[r][2] * b[2][q];
+}
+
+static void mat3_inv(double A[3][3], double B[3][3])
+{
+    double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) - A[1][0] * (A[0][1] * A[2][2] - A[0][2] * A[2][1])
+        + A[2][0] * (A[0][1] * A[1][2] - A[0][2] * A[1][1]);
+    if (fabs(det) > 1.0e-5) {
+        B[0][0] = (A[1][1] * A[2][2] - A[1][2] * A[2][1]) / det;
+        B[0][1] = (A[0][2] * A[2][1] - A[0][1] * A[2][2]) / det;
+        B[0][2] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]) / det;
+        B[1][0] = (A[1][2] * A[2][0] - A[1][0] * A[2][2]) / det;
+        B[1][1] = (A[0][0] * A[2][2] - A[0][2] * A[2][0]) / det;
+        B[1][2] = (A[1][0] * A[0][2] - A[0][0] * A[1][2]) / det;
+        B[2][0] = (A[1][0] * A[2][1] - A[1][1] * A[2][0]) / det;
+        B[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) / det;
+        B[2][2] = (A[0][0] * A[1][1] - A[1][0] * A[0][1]) / det;
+    }
+}
+
+/* artificial_stress_2d / artificial_stress_3d: CPP_9-5-artificialstress.cpp:28-295.
+ * R_i from the tensile principal stresses of each soil particle, then
+ * a_i += sum_j m_j f_ij^n (R_i + R_j) grad W_ij over soil neighbours, with
+ * f_ij^n = (W(q) / W(dr))^2.55. */
+static void artificial_stress(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    int ndim = P->ndim;
+    double xishu = P->art_stre_coe;
+    const double pi_ = 3.141592653;   /* Header_Parameters.h:10 */
+    for (int i = 0; i < c->n; i++) {
+        if (c->type[i] != 2) continue;
+        double R[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        const double* s = &c->sig[i * 6];
+        double rho = c->rho[i];
+        if (ndim == 2) {
+            double sita;
+            if (fabs(s[0] - s[1]) < 1.0e-6) {
+                if (s[3] > 0.0) sita = -pi_ * 0.78539816325;
+                else if (s[3] < 0.0) sita = pi_ * 0.78539816325;
+                else sita = 0.0;
+            } else
+                sita = 0.5 * atan(2.0 * s[3] / (s[0] - s[1]));
+            double sxx = cos(sita) * cos(sita) * s[0] + 2.0 * sin(sita) * cos(sita) * s[3] + sin(sita) * sin(sita) * s[1];
+            double syy = sin(sita) * sin(sita) * s[0] - 2.0 * sin(sita) * cos(sita) * s[3] + cos(sita) * cos(sita) * s[1];
+            double rxx = (sxx > 0.0) ? -xishu * sxx / rho / rho : 0.0;
+            double ryy = (syy > 0.0) ? -xishu * syy / rho / rho : 0.0;
+            R[0][0] = rxx * cos(sita) * cos(sita) + ryy * sin(sita) * sin(sita);
+            R[1][1] = rxx * sin(sita) * sin(sita) + ryy * cos(sita) * cos(sita);
+            R[0][1] = (rxx - ryy) * sin(sita) * cos(sita);
+            R[1][0] = R[0][1];
+        } else {
+            double sp[3] = {c->strep[i * 3], c->strep[i * 3 + 1], c->strep[i * 3 + 2]}, r[3];
+            for (int k = 0; k < 3; k++) r[k] = (sp[k] > 0.0) ? -xishu * sp[k] / rho / rho : 0.0;
+            double bi[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, bti[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            double tmp[3][3], st[3][3] = {{r[0], 0, 0}, {0, r[1], 0}, {0, 0, r[2]}};
+            double be[3][3], bt[3][3];
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++) {
+                    be[a][b] = c->beta[i * 9 + a * 3 + b];
+                    bt[a][b] = c->beta_ts[i * 9 + a * 3 + b];
+                }
+            mat3_inv(be, bi);
+            mat3_inv(bt, bti);
+            mat3_mul(bi, st, tmp);
+            mat3_mul(tmp, bti, R);
+        }
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) c->rij[i * 9 + a * 3 + b] = R[a][b];
+    }
+    for (int i = 0; i < c->n; i++) {
+        if (c->type[i] != 2) continue;
+        double tu[3] = {0, 0, 0};
+        const double* Ri = &c->rij[i * 9];
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj);
+            if (c->type[j] != 2) continue;
+            double dst = 0.0;
+            for (int k = 0; k < 3; k++) dst = dst + (c->xp[i * 3 + k] - c->xp[j * 3 + k]) * (c->xp[i * 3 + k] - c->xp[j * 3 + k]);
+            dst = sqrt(dst);
+            double hl = (c->hl[i] + c->hl[j]) * 0.5;
+            double q = dst / hl, f;
+            if (q >= 0.0 && q < 1.0) f = pow((0.666666666666667 - q * q + 0.5 * q * q * q) * 3.82300884955752, 2.55);
+            else if (q >= 1.0 && q < 2.0) f = pow((2.0 - q) * (2.0 - q) * (2.0 - q) * 0.629737609329447, 2.55);
+            else f = 0.0;
+            const double* Rj = &c->rij[j * 9];
+            const double* w = &W(i, nj, 0);
+            double m = c->mass[j];
+            if (ndim == 2) {
+                tu[0] = tu[0] + m * f * (Ri[0] + Rj[0]) * w[0] + m * f * (Ri[1] + Rj[1]) * w[1];
+                tu[1] = tu[1] + m * f * (Ri[3] + Rj[3]) * w[0] + m * f * (Ri[4] + Rj[4]) * w[1];
+            } else {
+                for (int a = 0; a < 3; a++)
+                    tu[a] = tu[a] + m * f * (Ri[a * 3] + Rj[a * 3]) * w[0] + m * f * (Ri[a * 3 + 1] + Rj[a * 3 + 1]) * w[1]
+                        + m * f * (Ri[a * 3 + 2] + Rj[a * 3 + 2]) * w[2];
+            }
+        }
+        for (int k = 0; k < ndim; k++) c->ax[i * 3 + k] = c->ax[i * 3 + k] + tu[k];
+    }
+}
+
 /* boundary_moving_stress_effect: CPP_9-4-derivation_stress.cpp:631-721 */
 static void boundary_moving_stress_effect(orc_ctx* c)
 {
@@ -1505,7 +1614,6 @@ static int check_supported(const sphgpu_params* P)
     if (P->flbndy != 1) return SPHGPU_E_UNSUPPORTED;
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
     if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
-    if (P->art_stre_coe > 0.0) return SPHGPU_E_UNSUPPORTED;
     if (P->fli > 1 || P->ss_type != 0) return SPHGPU_E_UNSUPPORTED;
     return 0;
 }
@@ -1538,6 +1646,7 @@ int orc_step(orc_ctx* c, int nsteps)
         soil_acceleration(c);
         structure_acceleration(c);
         artificial_viscosity(c);
+        if (P->art_stre_coe > 0.0) artificial_stress(c);
         boundary_moving_stress_effect(c);    /* flv == 0, flbndy 1 */
         if (P->fli == 1) interact1(c);
         if (c->l <= P->inip) soil_damping_geostress(c);

@@ -1,6 +1,6 @@
 """Generate the golden fixtures of tests/golden/ by running the reference solver.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]     (default: every case)
 
 Needs oracle/_ref/libsphref.so, i.e. the reference solver compiled from its own
 sources (make -C oracle ref, which reads the reference source tree).  For each
@@ -36,11 +36,30 @@ def _kgc_regu():
     return sc
 
 
+def _slope_art_stress():
+    """A 2-D cohesive slope with artificial stress (art_stre_coe 0.5); the upper
+    half of the soil starts moving up at 0.5 m/s (scenes.uplift), which puts
+    its top in tension so that the tensile branch of the artificial stress
+    acts."""
+    return scenes.uplift(scenes.slope_2d(H=1.0, dx=0.05, art_stre_coe=0.5), 1, 0.5)
+
+
+def _column_art_stress():
+    """The soil column (cohesion 20 kPa) with artificial stress; soil above
+    z = 0.25 starts moving up at 0.5 m/s."""
+    sc = scenes.soil_column_3d(dx=0.1, steps=200)
+    sc.soils[2]["c"] = 20.0e3
+    sc.problem["art_stre_coe"] = 0.5
+    return scenes.uplift(sc, 2, 0.25)
+
+
 CASES = {
     # name: (scene factory, steps)
     "dam_break_2d_dx0.04": (lambda: scenes.dam_break_2d(dx=0.04, steps=200), 25),
     "soil_column_3d_dx0.1": (lambda: scenes.soil_column_3d(dx=0.1, steps=200), 15),
     "soil_column_3d_dx0.1_kgc_regu": (_kgc_regu, 9),
+    "slope_2d_H1_dx0.05_art_stress": (_slope_art_stress, 30),
+    "soil_column_3d_dx0.1_art_stress": (_column_art_stress, 12),
 }
 
 
@@ -77,7 +96,7 @@ if __name__ == "__main__":
     saved = os.dup(1)
     os.dup2(devnull, 1)   # the reference prints progress lines
     try:
-        files = [make(n) for n in CASES]
+        files = [make(n) for n in (sys.argv[1:] or CASES)]
     finally:
         os.dup2(saved, 1)
     for f in files:

@@ -196,3 +196,41 @@ def test_particle_records_roundtrip():
         assert np.array_equal(eng.get_field(k), eng2.get_field(k)), k
     rho = np.frombuffer(buf.tobytes(), dtype=np.float64).reshape(n, 133)[:, 312 // 8]
     assert np.array_equal(rho, eng.get_field("rho"))
+
+
+# Artificial stress evaluates atan, sin and cos (2-D principal directions) and
+# pow(f, 2.55) per soil pair; CUDA's double-precision versions of these and the
+# C library's may differ in the last bit, so this run is compared with a
+# tolerance relative to each field's magnitude.
+ART_REL_TOL = 1e-9
+
+
+def _art_scene(name):
+    if name == "slope_2d":
+        return scenes.uplift(scenes.slope_2d(H=1.0, dx=0.025, art_stre_coe=0.5), 1, 0.5)
+    sc = scenes.soil_column_3d(dx=0.05, steps=100)
+    sc.soils[2]["c"] = 20.0e3
+    sc.problem["art_stre_coe"] = 0.5
+    return scenes.uplift(sc, 2, 0.25)
+
+
+@pytest.mark.parametrize("name,steps", [("slope_2d", 20), ("soil_column_3d", 12)])
+def test_artificial_stress(name, steps):
+    """Artificial stress on soil in tension (art_stre_coe 0.5) against the
+    oracle, and the same run without it: the term moves the result by far
+    more than the tolerance."""
+    _, eng, orc = _engine_and_oracle(_art_scene(name))
+    eng.step(steps)
+    assert orc.step(steps) == 0
+    worst = _compare(eng, orc, tol=ART_REL_TOL)
+    print("artificial stress, worst relative error per field:", max(worst.values()))
+    strep, t = eng.get_field("strep"), eng.get_field("type")
+    assert (strep[t == 2] > 0.0).any()
+    sc = _art_scene(name)
+    sc.problem["art_stre_coe"] = 0.0
+    st = scenes.initialise(sc)
+    off = sphgpu.Engine(st.params, device=0)
+    off.load_state(st.fields, st.fluid, st.soil)
+    off.step(steps)
+    a, b = eng.get_field("vx"), off.get_field("vx")
+    assert float(np.abs(a - b).max()) > 1e3 * ART_REL_TOL * float(np.abs(b).max())

@@ -14,7 +14,8 @@ from checkers import (ORC_INPLACE, ORC_JACOBI, ORC_POW_CR, ORC_POW_LIBM, STATE_F
                       Params, Reference, have_reference)
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-CASES = ["dam_break_2d_dx0.04", "soil_column_3d_dx0.1", "soil_column_3d_dx0.1_kgc_regu"]
+CASES = ["dam_break_2d_dx0.04", "soil_column_3d_dx0.1", "soil_column_3d_dx0.1_kgc_regu",
+         "slope_2d_H1_dx0.05_art_stress", "soil_column_3d_dx0.1_art_stress"]
 
 
 def _golden(name):
@@ -207,3 +208,35 @@ def test_live_reference_bit_identical(factory, steps):
         a, b = orc.get_field(k), ref.get_field(k)
         same = (a == b) | (np.isnan(a) & np.isnan(b)) if a.dtype.kind == "f" else (a == b)
         assert same.all(), k
+
+
+def _stretched_column(dx):
+    sc = scenes.soil_column_3d(dx=dx, steps=100)
+    sc.soils[2]["c"] = 20.0e3
+    sc.problem["art_stre_coe"] = 0.5
+    return scenes.uplift(sc, 2, 0.25)
+
+
+def _stretched_slope(dx):
+    return scenes.uplift(scenes.slope_2d(H=1.0, dx=dx, art_stre_coe=0.5), 1, 0.5)
+
+
+@needs_ref
+@pytest.mark.parametrize("factory,steps", [
+    (lambda: _stretched_slope(0.025), 20),
+    (lambda: _stretched_column(0.05), 12),
+])
+def test_live_reference_artificial_stress(factory, steps):
+    """Artificial stress (CPP_9-5-artificialstress.cpp) on soil in tension:
+    bit-identical to the reference, and the tensile branch is reached."""
+    sc = factory()
+    ref = _live(sc)
+    fl, so = ref.materials()
+    orc = Oracle(ref.params, ORC_INPLACE)
+    orc.load_state({k: ref.get_field(k) for k in STATE_FIELDS}, fl, so)
+    assert ref.step(steps) == 0
+    assert orc.step(steps) == 0
+    for k in STATE_FIELDS:
+        assert np.array_equal(orc.get_field(k), ref.get_field(k)), k
+    strep, t = ref.get_field("strep"), ref.get_field("type")
+    assert (strep[t == 2] > 0.0).any()
