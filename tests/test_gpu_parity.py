@@ -202,7 +202,7 @@ def test_particle_records_roundtrip():
 # pow(f, 2.55) per soil pair; CUDA's double-precision versions of these and the
 # C library's may differ in the last bit, so this run is compared with a
 # tolerance relative to each field's magnitude.
-ART_REL_TOL = 1e-9
+ART_REL_TOL = 1e-12         # measured worst on B200: 1.4e-16
 
 
 def _art_scene(name):
