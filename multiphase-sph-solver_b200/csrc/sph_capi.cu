@@ -128,7 +128,7 @@ int check_params(const sphgpu_params* P)
     if (P->flbndy != 1) return SPHGPU_E_UNSUPPORTED;
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
     if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
-    if (P->fli != 0 && P->fli != 1) return SPHGPU_E_UNSUPPORTED;
+    if (P->fli < 0 || P->fli > 3) return SPHGPU_E_UNSUPPORTED;
     if (P->ss_type != 0) return SPHGPU_E_UNSUPPORTED;
     if (P->if_move != 0 && P->if_move != 1) return SPHGPU_E_UNSUPPORTED;
     return 0;
@@ -295,7 +295,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.f_c, N); r |= dalloc(c, &s.f_smin, N); r |= dalloc(c, &s.f_tanfai, N); r |= dalloc(c, &s.f_bhtype, N);
     r |= dalloc(c, &s.s_e, N); r |= dalloc(c, &s.s_poi, N); r |= dalloc(c, &s.s_eps0, N); r |= dalloc(c, &s.s_dens, N);
     r |= dalloc(c, &s.s_kapa, N); r |= dalloc(c, &s.s_por, N); r |= dalloc(c, &s.s_vpu, N); r |= dalloc(c, &s.s_cop, N);
-    r |= dalloc(c, &s.s_sitas, N); r |= dalloc(c, &s.s_sitar, N);
+    r |= dalloc(c, &s.s_sitas, N); r |= dalloc(c, &s.s_sitar, N); r |= dalloc(c, &s.s_ds, N);
     r |= dalloc(c, &s.s_yalf, N); r |= dalloc(c, &s.s_ykap, N); r |= dalloc(c, &s.s_yalf_dil, N);
     r |= dalloc(c, &s.xh, 4 * (size_t)N); r |= dalloc(c, &s.xh_next, 4 * (size_t)N); r |= dalloc(c, &s.xs, 4 * (size_t)N);
     r |= dalloc(c, &s.de, 6 * (size_t)N); r |= dalloc(c, &s.we, 6 * (size_t)N); r |= dalloc(c, &s.color, N);
@@ -524,6 +524,7 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
         for (int i = 0; i < N; i++) buf[i] = so[i].cop; r |= put(s.s_cop);
         for (int i = 0; i < N; i++) buf[i] = so[i].sitas; r |= put(s.s_sitas);
         for (int i = 0; i < N; i++) buf[i] = so[i].sitar; r |= put(s.s_sitar);
+        for (int i = 0; i < N; i++) buf[i] = so[i].ds; r |= put(s.s_ds);
         // Drucker-Prager cone constants with the reference's own libm calls
         // (dpmodel1 / dpmodel_bui / DPModel_check, CPP_8-1-consfactor.cpp:294-349,
         // 461-529, 783-803); they depend only on the material record.

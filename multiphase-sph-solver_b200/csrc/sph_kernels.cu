@@ -750,10 +750,39 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_a(Dev d)
     for (int k = 0; k < 3; k++) d.s.ax[k * N + i] = ax[k];
 }
 
+// Soil-water drag coefficient of interact2 (Tsuji / Shi, form 2,
+// CPP_10-interact1.cpp:154-176) and interact3 (Peng, form 3, :294-306) for
+// a soil particle of porosity por and grain diameter ds in water of density
+// dens and viscosity vis, at relative speed mag_v; rho_w is the density the
+// reference reads there.  Out of line: only fli 2/3 call it, and its pow calls
+// would otherwise widen the register budget of every run.
+__device__ __noinline__ double drag_beta(int form, double por, double ds, double dens, double vis, double mag_v,
+                                         double rho_w)
+{
+    double re, cd, beta;
+    if (form == 2) {
+        re = mag_v * dens * por * ds / vis;
+        if (re > 1000.0) cd = 0.43;
+        else if (fabs(re) > 0.0001) cd = 24.0 * (1.0 + 0.15 * pow(re, 0.687)) / re;
+        else cd = 0.0;
+        if (por <= 0.8) {
+            beta = 150.0 * (1.0 - por) * (1.0 - por) / por / por / ds / ds * vis;
+            beta = beta + 1.75 * (1.0 - por) / ds / por * dens * mag_v;
+        } else
+            beta = 0.75 * cd * mag_v * dens * (1.0 - por) / ds * pow(por, -2.7);
+    } else {
+        re = mag_v * dens * ds / vis;
+        cd = por * por * por * ds * ds * 0.0066666667 / (1.0 - por) / (1.0 - por);
+        if (re > 60.0) beta = vis / cd + 1.75 / sqrt(150.0) * rho_w * mag_v / sqrt(cd) / pow(por, 1.5);
+        else beta = vis / cd;
+    }
+    return beta;
+}
+
 // artificial_viscosity (CPP_9-3-artificialvis.cpp:12-99), the pair sum of
 // artificial_stress_2d/_3d (CPP_9-5-artificialstress.cpp, ART = 1),
 // boundary_moving_stress_effect (CPP_9-4-derivation_stress.cpp:631-721),
-// interact1 (CPP_10-interact1.cpp:15-110), soil_damping_geostress
+// interact1/2/3 (CPP_10-interact1.cpp:15-405), soil_damping_geostress
 // (CPP_9-4:849-896) and veocity_update (CPP_11-xsph.cpp:11-142): one pass
 // over the neighbour list with one accumulator set per sum, combined with the
 // stress-divergence result of k_accel_a in the reference's call order.
@@ -805,7 +834,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
         const int tj = d.s.type[j];
         const bool av_pair = (ti == tj && ti != 7);
         const bool b_pair = moving && tj == 0;
-        const bool in_pair = d.p.fli == 1 && ti != tj;
+        const bool in_pair = d.p.fli >= 1 && ti != tj;
         const bool dm_pair = damping && tj == ti;
         const bool as_pair = art && tj == 2;
         if (!(av_pair || b_pair || in_pair || dm_pair)) continue;
@@ -855,7 +884,16 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
             }
             if (inprod < 0) {
                 const double w3 = w[3], ga = d.p.g_acc;
-                if (ti == 2 && tj == 1) {
+                if (d.p.fli > 1 && ((ti == 2 && tj == 1) || (ti == 1 && tj == 2))) {
+                    // interact2/3 soil-water drag, m_j / rho_j W beta (v_i - v_j)
+                    double mv = 0.0;
+                    for (int k = 0; k < nd; k++) mv = mv + dvx[k] * dvx[k];
+                    mv = sqrt(mv);
+                    const int so = (ti == 2) ? i : j, wa = (ti == 2) ? j : i;
+                    const double beta = drag_beta(d.p.fli, d.s.porosity[so], d.s.s_ds[so], d.s.f_dens[wa],
+                                                  d.s.f_vis[wa], mv, (ti == 2) ? rj : ri);
+                    for (int k = 0; k < nd; k++) tin[k] = tin[k] + mj / rj * w3 * beta * dvx[k];
+                } else if (ti == 2 && tj == 1) {
                     const double sa = satu_i, po = d.s.porosity[i], cp = d.s.cop[i], fd = d.s.f_dens[j];
                     for (int k = 0; k < nd; k++)
                         tin[k] = tin[k] + sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3;
@@ -914,7 +952,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
     const double dt = d.p.dt;
     double axp[3];
     for (int k = 0; k < 3; k++) axp[k] = d.s.axp[k * N + i];
-    if (d.p.fli == 1 && moving) {
+    if (d.p.fli >= 1 && moving) {
         const double xishu = d.p.interc;
         for (int k = 0; k < nd; k++) {
             double itf = tin[k];

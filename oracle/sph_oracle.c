@@ -1282,8 +1282,37 @@ static void boundary_moving_stress_effect(orc_ctx* c)
     }
 }
 
-/* interact1: Darcy drag, CPP_10-interact1.cpp:15-110 */
-static void interact1(orc_ctx* c)
+/* Soil-water drag coefficient beta of interact2 (Tsuji et al. 1993 / Shi et al.
+ * 2018, CPP_10-interact1.cpp:154-176) and interact3 (Peng et al. 2017,
+ * :294-306), for soil particle s and water particle w; rho_w is the density
+ * the reference reads (pPar[j].rho with i soil, pPar[i].rho with i water). */
+static double drag_beta(const orc_ctx* c, int form, int s, int w, double mag_v, double rho_w)
+{
+    double por = c->porosity[s], ds = c->so[s].ds, dens = c->fl[w].dens, vis = c->fl[w].vis;
+    double re, cd, beta;
+    if (form == 2) {
+        re = mag_v * dens * por * ds / vis;
+        if (re > 1000.0) cd = 0.43;
+        else if (fabs(re) > 0.0001) cd = 24.0 * (1.0 + 0.15 * pow(re, 0.687)) / re;
+        else cd = 0.0;
+        if (por <= 0.8) {
+            beta = 150.0 * (1.0 - por) * (1.0 - por) / por / por / ds / ds * vis;
+            beta = beta + 1.75 * (1.0 - por) / ds / por * dens * mag_v;
+        } else
+            beta = 0.75 * cd * mag_v * dens * (1.0 - por) / ds * pow(por, -2.7);
+    } else {
+        re = mag_v * dens * ds / vis;
+        cd = por * por * por * ds * ds * 0.0066666667 / (1.0 - por) / (1.0 - por);
+        if (re > 60.0) beta = vis / cd + 1.75 / sqrt(150.0) * rho_w * mag_v / sqrt(cd) / pow(por, 1.5);
+        else beta = vis / cd;
+    }
+    return beta;
+}
+
+/* interact1 (Darcy, CPP_10-interact1.cpp:15-110), interact2 (Tsuji, :114-263)
+ * and interact3 (Peng, :267-405): the same pass, limiter and soil-air term;
+ * they differ in the soil-water pair term. */
+static void interact(orc_ctx* c, int form)
 {
     const sphgpu_params* P = &c->P;
     int ndim = P->ndim;
@@ -1294,16 +1323,22 @@ static void interact1(orc_ctx* c)
         for (int nj = 1; nj <= c->ninflu[i]; nj++) {
             int j = NBR(i, nj), k;
             if (c->type[i] == c->type[j]) continue;
-            double inprod = 0.0, dx[3], dvx[3];
+            double inprod = 0.0, mag_v = 0.0, dx[3], dvx[3];
             for (k = 0; k < ndim; k++) {
                 dx[k] = c->xp[i * 3 + k] - c->xp[j * 3 + k];
                 dvx[k] = c->vxp[i * 3 + k] - c->vxp[j * 3 + k];
+                mag_v = mag_v + dvx[k] * dvx[k];
                 inprod = inprod + dx[k] * dvx[k];
             }
+            mag_v = sqrt(mag_v);
             if (!(inprod < 0)) continue;
             int ti = c->type[i], tj = c->type[j];
             double w3 = W(i, nj, 3);
-            if (ti == 2 && tj == 1) {
+            if (form > 1 && ((ti == 2 && tj == 1) || (ti == 1 && tj == 2))) {
+                double beta = (ti == 2) ? drag_beta(c, form, i, j, mag_v, c->rho[j]) : drag_beta(c, form, j, i, mag_v, c->rho[i]);
+                for (k = 0; k < ndim; k++)
+                    tu[k] = tu[k] + c->mass[j] / c->rho[j] * w3 * beta * (c->vxp[i * 3 + k] - c->vxp[j * 3 + k]);
+            } else if (ti == 2 && tj == 1) {
                 for (k = 0; k < ndim; k++)
                     tu[k] = tu[k] + c->satu[i] * c->satu[i] * c->porosity[i] * c->porosity[i] * c->fl[j].dens * g_acc * dvx[k] / c->cop[i] * c->mass[j] / c->rho[j] * w3;
             } else if (ti == 1 && tj == 2) {
@@ -1614,7 +1649,7 @@ static int check_supported(const sphgpu_params* P)
     if (P->flbndy != 1) return SPHGPU_E_UNSUPPORTED;
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
     if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
-    if (P->fli > 1 || P->ss_type != 0) return SPHGPU_E_UNSUPPORTED;
+    if (P->fli < 0 || P->fli > 3 || P->ss_type != 0) return SPHGPU_E_UNSUPPORTED;
     return 0;
 }
 
@@ -1648,7 +1683,7 @@ int orc_step(orc_ctx* c, int nsteps)
         artificial_viscosity(c);
         if (P->art_stre_coe > 0.0) artificial_stress(c);
         boundary_moving_stress_effect(c);    /* flv == 0, flbndy 1 */
-        if (P->fli == 1) interact1(c);
+        if (P->fli >= 1) interact(c, P->fli);
         if (c->l <= P->inip) soil_damping_geostress(c);
         velocity_update(c);
         if (P->if_move != 2) xsph(c);

@@ -53,6 +53,21 @@ def _column_art_stress():
     return scenes.uplift(sc, 2, 0.25)
 
 
+def _column_drag(fli, eps0, vw):
+    """The soil column with the Tsuji/Shi (fli 2) or Peng (fli 3) soil-water
+    drag; void ratio eps0 (5.0 gives porosity 0.83, the dilute branch of
+    fli 2), and the pore water starting at x-velocities 0, vw, 2 vw, 3 vw in
+    turn so that every Reynolds-number branch is reached."""
+    def make():
+        sc = scenes.soil_column_3d(dx=0.1, steps=200)
+        sc.flags["fli"] = fli
+        sc.soils[2]["eps0"] = eps0
+        w = np.flatnonzero(sc.ptype == 1)
+        sc.vxp[w, 0] = vw * (np.arange(len(w)) % 4)
+        return sc
+    return make
+
+
 CASES = {
     # name: (scene factory, steps)
     "dam_break_2d_dx0.04": (lambda: scenes.dam_break_2d(dx=0.04, steps=200), 25),
@@ -60,6 +75,8 @@ CASES = {
     "soil_column_3d_dx0.1_kgc_regu": (_kgc_regu, 9),
     "slope_2d_H1_dx0.05_art_stress": (_slope_art_stress, 30),
     "soil_column_3d_dx0.1_art_stress": (_column_art_stress, 12),
+    "soil_column_3d_dx0.1_drag_tsuji_dilute": (_column_drag(2, 5.0, 1.0), 10),
+    "soil_column_3d_dx0.1_drag_peng": (_column_drag(3, 0.6667, 0.05), 10),
 }
 
 

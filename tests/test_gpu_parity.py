@@ -234,3 +234,24 @@ def test_artificial_stress(name, steps):
     off.step(steps)
     a, b = eng.get_field("vx"), off.get_field("vx")
     assert float(np.abs(a - b).max()) > 1e3 * ART_REL_TOL * float(np.abs(b).max())
+
+
+# interact2/3 evaluate pow(Re, 0.687), pow(n, -2.7) and pow(n, 1.5), whose
+# CUDA and C library results may differ by an ulp: held to a tolerance.
+DRAG_REL_TOL = 1e-12
+
+
+@pytest.mark.parametrize("fli,eps0,vw", [(2, 0.6667, 0.05), (2, 5.0, 1.0), (3, 0.6667, 0.05)])
+def test_drag_forms(fli, eps0, vw):
+    """Tsuji/Shi (fli 2: Ergun below porosity 0.8, Wen-Yu above) and Peng
+    (fli 3: laminar and turbulent) soil-water drag against the oracle."""
+    sc = scenes.soil_column_3d(dx=0.05, steps=100)
+    sc.flags["fli"], sc.soils[2]["eps0"] = fli, eps0
+    w = np.flatnonzero(sc.ptype == 1)
+    sc.vxp[w, 0] = vw * (np.arange(len(w)) % 4)
+    _, eng, orc = _engine_and_oracle(sc)
+    eng.step(10)
+    assert orc.step(10) == 0
+    worst = _compare(eng, orc, tol=DRAG_REL_TOL)
+    print(f"drag fli={fli}, worst relative error per field:", max(worst.values()))
+    assert np.abs(eng.get_field("interf")).max() > 0.0

@@ -15,7 +15,8 @@ from checkers import (ORC_INPLACE, ORC_JACOBI, ORC_POW_CR, ORC_POW_LIBM, STATE_F
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ["dam_break_2d_dx0.04", "soil_column_3d_dx0.1", "soil_column_3d_dx0.1_kgc_regu",
-         "slope_2d_H1_dx0.05_art_stress", "soil_column_3d_dx0.1_art_stress"]
+         "slope_2d_H1_dx0.05_art_stress", "soil_column_3d_dx0.1_art_stress",
+         "soil_column_3d_dx0.1_drag_tsuji_dilute", "soil_column_3d_dx0.1_drag_peng"]
 
 
 def _golden(name):
@@ -240,3 +241,24 @@ def test_live_reference_artificial_stress(factory, steps):
         assert np.array_equal(orc.get_field(k), ref.get_field(k)), k
     strep, t = ref.get_field("strep"), ref.get_field("type")
     assert (strep[t == 2] > 0.0).any()
+
+
+@needs_ref
+@pytest.mark.parametrize("fli,eps0,vw", [(2, 0.6667, 0.05), (2, 5.0, 1.0), (3, 0.6667, 0.05), (3, 0.6667, 0.0)])
+def test_live_reference_drag_forms(fli, eps0, vw):
+    """interact2 (Tsuji/Shi: Ergun below porosity 0.8, Wen-Yu above) and
+    interact3 (Peng: laminar below Re 60, turbulent above), CPP_10-interact1.cpp:
+    114-405, bit-identical to the reference."""
+    sc = scenes.soil_column_3d(dx=0.05, steps=100)
+    sc.flags["fli"], sc.soils[2]["eps0"] = fli, eps0
+    w = np.flatnonzero(sc.ptype == 1)
+    sc.vxp[w, 0] = vw * (np.arange(len(w)) % 4)
+    ref = _live(sc)
+    fl, so = ref.materials()
+    orc = Oracle(ref.params, ORC_INPLACE)
+    orc.load_state({k: ref.get_field(k) for k in STATE_FIELDS}, fl, so)
+    assert ref.step(10) == 0
+    assert orc.step(10) == 0
+    for k in STATE_FIELDS:
+        assert np.array_equal(orc.get_field(k), ref.get_field(k)), k
+    assert np.abs(ref.get_field("interf")).max() > 0.0
