@@ -212,7 +212,8 @@ int check_particles(sphgpu_ctx* c)
         const int t = c->h_type[i], m = c->h_matype[i];
         if (t == 2) {
             const int mt = m % 10;
-            if (!(mt == 0 || mt == 2 || mt == 5 || mt == 6) || (m >= 30 && m < 50) || m >= 60)
+            if (!(mt == 0 || mt == 1 || mt == 2 || mt == 5 || mt == 6 || mt == 7 || mt == 9) || (m >= 30 && m < 50) ||
+                m >= 60)
                 return SPHGPU_E_UNSUPPORTED;
         }
     }
@@ -296,6 +297,8 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.s_e, N); r |= dalloc(c, &s.s_poi, N); r |= dalloc(c, &s.s_eps0, N); r |= dalloc(c, &s.s_dens, N);
     r |= dalloc(c, &s.s_kapa, N); r |= dalloc(c, &s.s_por, N); r |= dalloc(c, &s.s_vpu, N); r |= dalloc(c, &s.s_cop, N);
     r |= dalloc(c, &s.s_sitas, N); r |= dalloc(c, &s.s_sitar, N); r |= dalloc(c, &s.s_ds, N);
+    r |= dalloc(c, &s.s_c, N); r |= dalloc(c, &s.s_fs, N);
+    r |= dalloc(c, &s.s_ann, N); r |= dalloc(c, &s.s_zmf, N); r |= dalloc(c, &s.s_ramda, N); r |= dalloc(c, &s.s_sme0, N);
     r |= dalloc(c, &s.s_yalf, N); r |= dalloc(c, &s.s_ykap, N); r |= dalloc(c, &s.s_yalf_dil, N);
     r |= dalloc(c, &s.xh, 4 * (size_t)N); r |= dalloc(c, &s.xh_next, 4 * (size_t)N); r |= dalloc(c, &s.xs, 4 * (size_t)N);
     r |= dalloc(c, &s.de, 6 * (size_t)N); r |= dalloc(c, &s.we, 6 * (size_t)N); r |= dalloc(c, &s.color, N);
@@ -525,6 +528,12 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
         for (int i = 0; i < N; i++) buf[i] = so[i].sitas; r |= put(s.s_sitas);
         for (int i = 0; i < N; i++) buf[i] = so[i].sitar; r |= put(s.s_sitar);
         for (int i = 0; i < N; i++) buf[i] = so[i].ds; r |= put(s.s_ds);
+        for (int i = 0; i < N; i++) buf[i] = so[i].c; r |= put(s.s_c);
+        for (int i = 0; i < N; i++) buf[i] = so[i].fs; r |= put(s.s_fs);
+        for (int i = 0; i < N; i++) buf[i] = so[i].ann; r |= put(s.s_ann);
+        for (int i = 0; i < N; i++) buf[i] = so[i].zmf; r |= put(s.s_zmf);
+        for (int i = 0; i < N; i++) buf[i] = so[i].ramda; r |= put(s.s_ramda);
+        for (int i = 0; i < N; i++) buf[i] = so[i].sme0; r |= put(s.s_sme0);
         // Drucker-Prager cone constants with the reference's own libm calls
         // (dpmodel1 / dpmodel_bui / DPModel_check, CPP_8-1-consfactor.cpp:294-349,
         // 461-529, 783-803); they depend only on the material record.

@@ -18,14 +18,27 @@ __device__ __forceinline__ void jaumann(double ds[6], const double s[6], const d
 
 // elastic D (only its nonzero pattern is kept: dlam, dmu) -- elastic(),
 // dpmodel1(), dpmodel_bui() share it (:17-59, :301-334, :468-501)
-__device__ __forceinline__ void elastic_consts(const double s[6], double E, double poi, double eps0, double kapa,
-                                               double* dlam, double* dmu, double* sm_out)
+// (elastic_plastic, :618-660, takes the mean stress with third = 0.333333333)
+// The elastic modulus: the material's E, or 3 (1 - 2 nu) (1 + e0) |p| / kappa
+// when E <= 1 (p = mean compression, at least 1).
+__device__ __forceinline__ double elastic_e0(const double s[6], double E, double poi, double eps0, double kapa,
+                                             double* sm_out, double third = 0.3333333333)
 {
-    double sm = (-s[0] + -s[1] + -s[2]) * 0.3333333333;
+    double sm = (-s[0] + -s[1] + -s[2]) * third;
     if (sm < 1.0) sm = 1.0;
     double e0;
     if (E > 1.0) e0 = E;
     else e0 = 3 * (1 - 2 * poi) * (1 + eps0) * fabs(sm) / kapa;
+    *sm_out = sm;
+    return e0;
+}
+
+__device__ __forceinline__ void elastic_consts(const double s[6], double E, double poi, double eps0, double kapa,
+                                               double* dlam, double* dmu, double* sm_out,
+                                               double third = 0.3333333333)
+{
+    double sm;
+    const double e0 = elastic_e0(s, E, poi, eps0, kapa, &sm, third);
     *dlam = e0 * poi / (1.0 + poi) / (1.0 - 2.0 * poi);
     *dmu = e0 * 0.5 / (1.0 + poi);
     *sm_out = sm;
@@ -52,9 +65,12 @@ __device__ __forceinline__ void fill_elastic(double D[6][6], double dlam, double
 }
 
 // Drucker-Prager continuum tangent (dpmodel1 / dpmodel_bui, :284-448 /
-// :451-615).  yalf, ykap, yalf_dil are the material constants the reference
-// evaluates with atan/tan/sin/cos each call; they are evaluated once per
-// particle by the host with the same libm calls.
+// :451-615) and, with MC = true, the Mohr-Coulomb form of elastic_plastic
+// (:618-777: plastic potential without dilatancy and no hardening term in
+// the denominator).  yalf, ykap, yalf_dil are the material constants the
+// reference evaluates with atan/tan/sin/cos each call; they are evaluated once
+// per particle by the host with the same libm calls.
+template <bool MC = false>
 __device__ __forceinline__ void dp_tangent(double D[6][6], double adps[6], const double s[6], const double de[6],
                                            double dlam, double dmu, double sm,
                                            double yalf, double ykap, double yalf_dil)
@@ -69,11 +85,13 @@ __device__ __forceinline__ void dp_tangent(double D[6][6], double adps[6], const
         double f11 = -yalf + dx / sj * 0.5, f22 = -yalf + dy / sj * 0.5, f33 = -yalf + dz / sj * 0.5;
         double f12 = dxy / sj * 0.5, f23 = dyz / sj * 0.5, f31 = dzx / sj * 0.5;
         double fkk = f11 + f22 + f33;
-        double g11 = -yalf_dil + dx / sj * 0.5, g22 = -yalf_dil + dy / sj * 0.5, g33 = -yalf_dil + dz / sj * 0.5;
+        double g11 = MC ? dx / sj * 0.5 : -yalf_dil + dx / sj * 0.5;
+        double g22 = MC ? dy / sj * 0.5 : -yalf_dil + dy / sj * 0.5;
+        double g33 = MC ? dz / sj * 0.5 : -yalf_dil + dz / sj * 0.5;
         double g12 = dxy / sj * 0.5, g23 = dyz / sj * 0.5, g31 = dzx / sj * 0.5;
         double hdd = g11 + g22 + g33;
         double fij = 2.0 * (f11 * g11 + f22 * g22 + f33 * g33) + f12 * g12 + f23 * g23 + f31 * g31;
-        double cc7 = dlam * (fkk * hdd) + dmu * fij + hdd;
+        double cc7 = MC ? dlam * (fkk * hdd) + dmu * fij : dlam * (fkk * hdd) + dmu * fij + hdd;
         double dd_ = 1.0 / cc7;
         double df = dlam * fkk, dg = dlam * hdd;
         double ramda = (dmu2 * f11 - 3.0 * dlam * yalf) * de[0]
@@ -90,6 +108,59 @@ __device__ __forceinline__ void dp_tangent(double D[6][6], double adps[6], const
             adps[3] = ramda * dd_ * f12; adps[4] = ramda * dd_ * f23; adps[5] = ramda * dd_ * f31;
         }
     }
+}
+
+// sub_camclay: subloading Cam-clay tangent (:129-281).  ymf from the
+// critical-state ratio zmf; the subloading ratio term roue from log(sme0 / sm).
+__device__ __forceinline__ void subcam_tangent(double D[6][6], double adps[6], const double s[6], const double de[6],
+                                               double dlam, double dmu, double sm, double ann, double zmf,
+                                               double zramda, double zkapa, double eps0, double sme0, double fs)
+{
+    const double dmu2 = dmu * 2.0;
+    const double ymf = 3.0 * (zmf - 1.0) / (zmf + 2.0) / fs;
+    const double hee = (zramda - zkapa) / (1.0 + eps0);
+    double dx = -s[0] - sm, dy = -s[1] - sm, dz = -s[2] - sm;
+    double dxy = -s[3], dyz = -s[4], dzx = -s[5];
+    double sjj = 0.5 * (dx * dx + dy * dy + dz * dz) + dxy * dxy + dyz * dyz + dzx * dzx;
+    double tt1 = 1.0 / (ymf * ymf * sm * sm + 3.0 * sjj);
+    double tt2 = 2.0 * ymf * ymf * sm * tt1 - 1.0 / sm;
+    double f11 = tt2 / 3.0 + dx * tt1 * 3.0;
+    double f22 = tt2 / 3.0 + dy * tt1 * 3.0;
+    double f33 = tt2 / 3.0 + dz * tt1 * 3.0;
+    double f12 = 3.0 * dxy * tt1, f23 = 3.0 * dyz * tt1, f31 = 3.0 * dzx * tt1;
+    double roue = (1 + eps0) * log(sme0 / sm);
+    if (roue < 0.0) roue = 0.0;
+    double ttt = ann * roue * roue;
+    double hdd = f11 + f22 + f33 + ttt / sm;
+    double fkk = f11 + f22 + f33;
+    double fij = 2.0 * (f11 * f11 + f22 * f22 + f33 * f33) + f12 * f12 + f23 * f23 + f31 * f31;
+    double cc7 = dlam * (fkk * fkk) + dmu * fij + hdd / hee;
+    double dd_ = 1.0 / cc7;
+    double df = dlam * fkk, dg = dlam * fkk;
+    double ramda = (dmu2 * f11 + dlam * fkk) * de[0] + (dmu2 * f22 + dlam * fkk) * de[1]
+        + (dmu2 * f33 + dlam * fkk) * de[2] + dmu * (f12 * de[3] + f23 * de[4] + f31 * de[5]);
+    if (ramda < 0.0) {
+        double ww[6] = {dg + dmu2 * f11, dg + dmu2 * f22, dg + dmu2 * f33, dmu * f12, dmu * f23, dmu * f31};
+        double zz[6] = {df + dmu2 * f11, df + dmu2 * f22, df + dmu2 * f33, dmu * f12, dmu * f23, dmu * f31};
+        for (int a = 0; a < 6; a++)
+            for (int b = 0; b < 6; b++) D[a][b] = D[a][b] - dd_ * ww[a] * zz[b];
+        adps[0] = ramda * dd_ * f11; adps[1] = ramda * dd_ * f22; adps[2] = ramda * dd_ * f33;
+        adps[3] = ramda * dd_ * f12; adps[4] = ramda * dd_ * f23; adps[5] = ramda * dd_ * f31;
+    }
+}
+
+// viscous_elastic (:88-126): dsig set directly, bulk modulus from the
+// elastic modulus, shear modulus g = the material's c
+__device__ __forceinline__ void visco_elastic(double ds[6], const double de[6], double e0, double poi, double g)
+{
+    const double k = e0 * 0.3333333333 / (1.0 - 2.0 * poi);
+    const double epkk = de[0] + de[1] + de[2];
+    ds[0] = 2.0 * g * (de[0] - epkk * 0.3333333333) + k * epkk;
+    ds[1] = 2.0 * g * (de[1] - epkk * 0.3333333333) + k * epkk;
+    ds[2] = 2.0 * g * (de[2] - epkk * 0.3333333333) + k * epkk;
+    ds[3] = 2.0 * g * de[3];
+    ds[4] = 2.0 * g * de[4];
+    ds[5] = 2.0 * g * de[5];
 }
 
 // DPModel_check: stress-scaling return onto the cone (:779-819)

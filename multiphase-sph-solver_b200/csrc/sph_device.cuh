@@ -60,6 +60,8 @@ struct DevState {
     // soil material record (pParti_ConsPara) used by the step
     double *s_e, *s_poi, *s_eps0, *s_dens, *s_kapa, *s_por, *s_vpu, *s_cop, *s_sitas, *s_sitar;
     double *s_ds;              // mean grain diameter (interact2/3 drag)
+    double *s_c, *s_fs;        // cohesion (viscous-elastic: shear modulus), strength reduction factor
+    double *s_ann, *s_zmf, *s_ramda, *s_sme0;   // subloading Cam-clay
     double *s_yalf, *s_ykap, *s_yalf_dil;   // Drucker-Prager constants, host-evaluated
     // positions (x, y, z, h) records, ping-pong
     double *xh, *xh_next;

@@ -40,6 +40,11 @@
 #ifndef SPH_MINB
 #define SPH_MINB 4
 #endif
+// the constitutive pass keeps a dense 6x6 tangent per thread: 2 blocks of
+// 128 threads per SM leave it 222 registers and no spills
+#ifndef SPH_MINB_STRESS
+#define SPH_MINB_STRESS 2
+#endif
 
 __device__ __forceinline__ void raise_err(int* err, int code) { atomicCAS(err, 0, code); }
 
@@ -414,7 +419,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_strain(Dev d)
 // run), PHASE 1 stops after the constitutive update (writing sig_next), the
 // smoothing pass runs, and PHASE 2 continues from the smoothed stresses.
 template <int ND, int PHASE>
-__global__ void __launch_bounds__(128, SPH_MINB) k_stress(Dev d)
+__global__ void __launch_bounds__(128, SPH_MINB_STRESS) k_stress(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
@@ -486,9 +491,12 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_stress(Dev d)
         double D[6][6], adps[6] = {0, 0, 0, 0, 0, 0}, ds[6] = {0, 0, 0, 0, 0, 0};
         double dlam, dmu, sm;
         const int mt = d.s.matype[i] % 10;
-        const bool dp = (ti == 2) && !(l < d.p.inip) && (mt == 2 || mt == 5);
+        const bool plastic = (ti == 2) && !(l < d.p.inip);
+        const bool dp = plastic && (mt == 2 || mt == 5);
         if (ti == 2) {
-            elastic_consts(s, d.s.s_e[i], d.s.s_poi[i], d.s.s_eps0[i], d.s.s_kapa[i], &dlam, &dmu, &sm);
+            // elastic_plastic (M-C, matype 9) takes its mean stress with 0.333333333
+            elastic_consts(s, d.s.s_e[i], d.s.s_poi[i], d.s.s_eps0[i], d.s.s_kapa[i], &dlam, &dmu, &sm,
+                           (plastic && mt == 9) ? 0.333333333 : 0.3333333333);
         } else {
             const double e0 = d.p.st_e, poi = d.p.st_poi;
             dlam = e0 * poi / (1.0 + poi) / (1.0 - 2.0 * poi);
@@ -497,7 +505,16 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_stress(Dev d)
         }
         fill_elastic(D, dlam, dmu);
         if (dp) dp_tangent(D, adps, s, de, dlam, dmu, sm, d.s.s_yalf[i], d.s.s_ykap[i], (mt == 5) ? d.s.s_yalf_dil[i] : 0.0);
-        add_dense(ds, D, de);
+        if (plastic && mt == 9) dp_tangent<true>(D, adps, s, de, dlam, dmu, sm, d.s.s_yalf[i], d.s.s_ykap[i], 0.0);
+        if (plastic && mt == 1)
+            subcam_tangent(D, adps, s, de, dlam, dmu, sm, d.s.s_ann[i], d.s.s_zmf[i], d.s.s_ramda[i], d.s.s_kapa[i],
+                           d.s.s_eps0[i], d.s.s_sme0[i], d.s.s_fs[i]);
+        if (plastic && mt == 7) {
+            double smv;
+            const double e0 = elastic_e0(s, d.s.s_e[i], d.s.s_poi[i], d.s.s_eps0[i], d.s.s_kapa[i], &smv);
+            visco_elastic(ds, de, e0, d.s.s_poi[i], d.s.s_c[i]);
+        } else
+            add_dense(ds, D, de);
         if (dp) dp_check(s, ds, d.s.s_yalf[i], d.s.s_ykap[i], dt);
         jaumann(ds, s, we9);
         if (ti == 2) {

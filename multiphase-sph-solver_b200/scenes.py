@@ -268,6 +268,41 @@ def uplift(scene: Scene, axis: int, above: float, v: float = 0.5) -> Scene:
     return scene
 
 
+# Para_Soil members each soil model's input block sets (CPP_2-initialf.cpp:
+# 490-805); the others keep Para_Soil's defaults
+_BASE = ("damp1", "damp2", "cop", "eps0", "e", "ds")
+MODEL_FIELDS = {
+    0: ("kapa", "poi", "dens") + _BASE,
+    1: ("poi", "dens", "eps0", "zmf", "sme0", "fs", "ramda", "kapa", "damp1", "damp2", "cop", "ann", "ocr", "e", "ds"),
+    2: ("kapa", "poi", "dens", "c", "fai", "fs") + _BASE,
+    5: ("kapa", "poi", "dens", "c", "fai", "beta", "fs") + _BASE,
+    6: ("kapa", "poi", "dens") + _BASE,
+    7: ("kapa", "poi", "dens", "c") + _BASE,
+    9: ("kapa", "poi", "dens", "c", "fai", "fs") + _BASE,
+}
+
+
+def set_soil_model(scene: Scene, matype: int, **record) -> Scene:
+    """Switch every soil particle (type 2) to constitutive model `matype`
+    (0 elastic, 1 subloading Cam-clay, 2 Drucker-Prager, 5 Bui DP, 6 elastic,
+    7 viscous-elastic, 9 Mohr-Coulomb; one layer).  The record holds the
+    members that model's input block reads, from `record`, else from the
+    previous soil record; the others keep Para_Soil's defaults."""
+    old = next(iter(scene.soils.values())) if scene.soils else soil_default()
+    rec = soil_default()
+    for k in MODEL_FIELDS[matype % 10]:      # what the model's input block sets
+        rec[k] = record.get(k, old.get(k, rec[k]))
+    unknown = set(record) - set(MODEL_FIELDS[matype % 10])
+    if unknown:
+        raise ValueError(f"model {matype} does not read {sorted(unknown)}")
+    scene.matype[scene.ptype == 2] = matype
+    scene.soils = {matype: rec}
+    flags = [0] * 10
+    flags[matype % 10] = 1
+    scene.model_flags = tuple(flags)
+    return scene
+
+
 def scaled_loop(scene: Scene) -> int:
     """Steps the reference will run: for dttype 2 the loop count is
     int(tt / dt) + 1 with tt the input dt (CPP_12-2-dt.cpp:13-20)."""
@@ -360,6 +395,16 @@ def write_input_dat(scene: Scene, path: str, ntd: int = 1) -> None:
             add(" ".join(_f(s[k]) for k in ("damp1", "damp2", "cop", "eps0")))
             add(" ".join(_f(s[k]) for k in ("e", "ds")))
         add("E end")
+    if mf[1] >= 1:
+        add("SB subloading cam-clay")
+        add("A data")
+        for layer in range(mf[1]):
+            s = scene.soils[layer * 10 + 1]
+            add(" ".join(_f(s[k]) for k in ("poi", "dens", "eps0", "zmf", "sme0", "fs")))
+            add(" ".join(_f(s[k]) for k in ("ramda", "kapa", "damp1", "damp2", "cop")))
+            add(" ".join(_f(s[k]) for k in ("ann", "ocr")))
+            add(" ".join(_f(s[k]) for k in ("e", "ds")))
+        add("E end")
     if mf[2] >= 1:
         add("DP drucker prager")
         add("A data")
@@ -378,6 +423,20 @@ def write_input_dat(scene: Scene, path: str, ntd: int = 1) -> None:
             add(" ".join(_f(s[k]) for k in ("damp1", "damp2", "cop", "eps0")))
             add(" ".join(_f(s[k]) for k in ("e", "ds")))
         add("E end")
+    # PP (elastic record read for index 6), VE (viscous-elastic, c = shear
+    # modulus) and EP (Mohr-Coulomb), CPP_2-initialf.cpp:666-805
+    for flag, code, title, first in ((6, "PP", "plastic", ("kapa", "poi", "dens")),
+                                     (7, "VE", "viscous elastic", ("kapa", "poi", "dens", "c")),
+                                     (9, "EP", "elastic perfectly plastic", ("kapa", "poi", "dens", "c", "fai", "fs"))):
+        if mf[flag] >= 1:
+            add(f"{code} {title}")
+            add("A data")
+            for layer in range(mf[flag]):
+                s = scene.soils[layer * 10 + flag]
+                add(" ".join(_f(s[k]) for k in first))
+                add(" ".join(_f(s[k]) for k in ("damp1", "damp2", "cop", "eps0")))
+                add(" ".join(_f(s[k]) for k in ("e", "ds")))
+            add("E end")
     if scene.structure is not None:
         st = scene.structure
         add("SM structure")

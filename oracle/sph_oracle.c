@@ -706,6 +706,127 @@ static void elastic_d(double dept[6][6], const double* sig, const sphgpu_soil* s
     *dlam_o = dlam; *dmu_o = dmu; *sm_o = sm;
 }
 
+/* Rank-one plastic correction shared by sub_camclay and elastic_plastic:
+ * dept[a][b] -= d * ww[a] * zz[b] (CPP_8-1-consfactor.cpp:228-273, 723-768) */
+static void plastic_update(double dept[6][6], double d, const double ww[6], const double zz[6])
+{
+    for (int a = 0; a < 6; a++)
+        for (int b = 0; b < 6; b++) dept[a][b] = dept[a][b] - d * ww[a] * zz[b];
+}
+
+/* sub_camclay: subloading Cam-clay, CPP_8-1-consfactor.cpp:129-281 */
+static void sub_camclay(double dept[6][6], const double* sig, const double* deps, const sphgpu_soil* so, double* adps)
+{
+    double dlam, dmu, sm;
+    double ann = so->ann, zmf = so->zmf, zramda = so->ramda, zkapa = so->kapa, eps0 = so->eps0;
+    elastic_d(dept, sig, so, &dlam, &dmu, &sm);
+    double dmu2 = dmu * 2.0;
+    double sigct[6];
+    for (int a = 0; a < 6; a++) sigct[a] = -sig[a];
+    double ymf = 3.0 * (zmf - 1.0) / (zmf + 2.0) / so->fs;
+    double hee = (zramda - zkapa) / (1.0 + eps0);
+    double dx = sigct[0] - sm, dy = sigct[1] - sm, dz = sigct[2] - sm;
+    double dxy = sigct[3], dyz = sigct[4], dzx = sigct[5];
+    double sjj = 0.5 * (dx * dx + dy * dy + dz * dz) + dxy * dxy + dyz * dyz + dzx * dzx;
+    double tt1 = 1.0 / (ymf * ymf * sm * sm + 3.0 * sjj);
+    double tt2 = 2.0 * ymf * ymf * sm * tt1 - 1.0 / sm;
+    double f11 = tt2 / 3.0 + dx * tt1 * 3.0;
+    double f22 = tt2 / 3.0 + dy * tt1 * 3.0;
+    double f33 = tt2 / 3.0 + dz * tt1 * 3.0;
+    double f12 = 3.0 * dxy * tt1, f23 = 3.0 * dyz * tt1, f31 = 3.0 * dzx * tt1;
+    double roue = (1 + eps0) * log(so->sme0 / sm);
+    if (roue < 0.0) roue = 0.0;
+    double ttt = ann * roue * roue;
+    double hdd = f11 + f22 + f33 + ttt / sm;
+    double fkk = f11 + f22 + f33;
+    double fij = 2.0 * (f11 * f11 + f22 * f22 + f33 * f33) + f12 * f12 + f23 * f23 + f31 * f31;
+    double cc7 = dlam * (fkk * fkk) + dmu * fij + hdd / hee;
+    double d = 1.0 / cc7;
+    double df = dlam * fkk, dg = dlam * fkk;
+    double ramda = (dmu2 * f11 + dlam * fkk) * deps[0] + (dmu2 * f22 + dlam * fkk) * deps[1]
+        + (dmu2 * f33 + dlam * fkk) * deps[2] + dmu * (f12 * deps[3] + f23 * deps[4] + f31 * deps[5]);
+    if (ramda < 0.0) {
+        double ww[6] = {dg + dmu2 * f11, dg + dmu2 * f22, dg + dmu2 * f33, dmu * f12, dmu * f23, dmu * f31};
+        double zz[6] = {df + dmu2 * f11, df + dmu2 * f22, df + dmu2 * f33, dmu * f12, dmu * f23, dmu * f31};
+        plastic_update(dept, d, ww, zz);
+        adps[0] = ramda * d * f11; adps[1] = ramda * d * f22; adps[2] = ramda * d * f33;
+        adps[3] = ramda * d * f12; adps[4] = ramda * d * f23; adps[5] = ramda * d * f31;
+    }
+}
+
+/* elastic_plastic: Mohr-Coulomb (Drucker-Prager circumscribed cone with a
+ * non-associated flow), CPP_8-1-consfactor.cpp:618-777.  Its mean stress uses
+ * 0.333333333 (nine 3s) where the other models use ten. */
+static void mc_model(double dept[6][6], const double* sig, const double* deps, const sphgpu_soil* so, double* adps)
+{
+    double sigct[6], e0, poi = so->poi, eps0 = so->eps0, zkapa = so->kapa;
+    double fai = atan(tan(so->fai * 0.0174532925166667) / so->fs);
+    double ci = so->c / so->fs;
+    for (int a = 0; a < 6; a++) {
+        sigct[a] = -sig[a];
+        for (int b = 0; b < 6; b++) dept[a][b] = 0.0;
+    }
+    double sm = (sigct[0] + sigct[1] + sigct[2]) * 0.333333333;
+    if (sm < 1.0) sm = 1.0;
+    if (so->e > 1.0) e0 = so->e;
+    else e0 = 3 * (1 - 2 * poi) * (1 + eps0) * fabs(sm) / zkapa;
+    double dlam = e0 * poi / (1.0 + poi) / (1.0 - 2.0 * poi);
+    double dmu = e0 * 0.5 / (1.0 + poi), dmu2 = dmu * 2.0;
+    dept[0][0] = dlam + dmu2; dept[1][1] = dlam + dmu2; dept[2][2] = dlam + dmu2;
+    dept[0][1] = dlam; dept[0][2] = dlam; dept[1][0] = dlam;
+    dept[1][2] = dlam; dept[2][0] = dlam; dept[2][1] = dlam;
+    dept[3][3] = dmu; dept[4][4] = dmu; dept[5][5] = dmu;
+    double dx = sigct[0] - sm, dy = sigct[1] - sm, dz = sigct[2] - sm;
+    double dxy = sigct[3], dyz = sigct[4], dzx = sigct[5];
+    double sjj = 0.5 * (dx * dx + dy * dy + dz * dz) + dxy * dxy + dyz * dyz + dzx * dzx;
+    double sj = sqrt(sjj);
+    double yalf = sin(fai) / sqrt(9.0 + 3.0 * sin(fai) * sin(fai));
+    double ykap = 3.0 * ci * cos(fai) / sqrt(9.0 + 3.0 * sin(fai) * sin(fai));
+    if ((sj - yalf * sm * 3.0 - ykap) >= 0.0) {
+        double f11 = -yalf + dx / sj * 0.5, f22 = -yalf + dy / sj * 0.5, f33 = -yalf + dz / sj * 0.5;
+        double f12 = dxy / sj * 0.5, f23 = dyz / sj * 0.5, f31 = dzx / sj * 0.5;
+        double fkk = f11 + f22 + f33;
+        double g11 = dx / sj * 0.5, g22 = dy / sj * 0.5, g33 = dz / sj * 0.5;
+        double g12 = dxy / sj * 0.5, g23 = dyz / sj * 0.5, g31 = dzx / sj * 0.5;
+        double hdd = g11 + g22 + g33;
+        double fij = 2.0 * (f11 * g11 + f22 * g22 + f33 * g33) + f12 * g12 + f23 * g23 + f31 * g31;
+        double cc7 = dlam * (fkk * hdd) + dmu * fij;
+        double d = 1.0 / cc7;
+        double df = dlam * fkk, dg = dlam * hdd;
+        double ramda = (dmu2 * f11 - 3.0 * dlam * yalf) * deps[0] + (dmu2 * f22 - 3.0 * dlam * yalf) * deps[1]
+            + (dmu2 * f33 - 3.0 * dlam * yalf) * deps[2] + dmu * (f12 * deps[3] + f23 * deps[4] + f31 * deps[5]);
+        double ttt = ramda * d;
+        if (ttt < 0.0) {
+            double ww[6] = {dg + dmu2 * g11, dg + dmu2 * g22, dg + dmu2 * g33, dmu * g12, dmu * g23, dmu * g31};
+            double zz[6] = {df + dmu2 * f11, df + dmu2 * f22, df + dmu2 * f33, dmu * f12, dmu * f23, dmu * f31};
+            plastic_update(dept, d, ww, zz);
+            adps[0] = ramda * d * f11; adps[1] = ramda * d * f22; adps[2] = ramda * d * f33;
+            adps[3] = ramda * d * f12; adps[4] = ramda * d * f23; adps[5] = ramda * d * f31;
+        }
+    }
+}
+
+/* viscous_elastic: CPP_8-1-consfactor.cpp:88-126 (sets dsig directly; the
+ * shear modulus is the material's c) */
+static void visco_elastic(double* ds, const double* sig, const double* deps, const sphgpu_soil* so)
+{
+    double sigct[6], e0, poi = so->poi, eps0 = so->eps0, zkapa = so->kapa;
+    for (int a = 0; a < 6; a++) sigct[a] = -sig[a];
+    double sm = (sigct[0] + sigct[1] + sigct[2]) * 0.3333333333;
+    if (sm < 1.0) sm = 1.0;
+    if (so->e > 1.0) e0 = so->e;
+    else e0 = 3 * (1 - 2 * poi) * (1 + eps0) * fabs(sm) / zkapa;
+    double k = e0 * 0.3333333333 / (1.0 - 2.0 * poi);
+    double g = so->c;
+    double epkk = deps[0] + deps[1] + deps[2];
+    ds[0] = 2.0 * g * (deps[0] - epkk * 0.3333333333) + k * epkk;
+    ds[1] = 2.0 * g * (deps[1] - epkk * 0.3333333333) + k * epkk;
+    ds[2] = 2.0 * g * (deps[2] - epkk * 0.3333333333) + k * epkk;
+    ds[3] = 2.0 * g * deps[3];
+    ds[4] = 2.0 * g * deps[4];
+    ds[5] = 2.0 * g * deps[5];
+}
+
 /* dpmodel1 (yalf_dil = 0) and dpmodel_bui (yalf_dil from beta):
  * CPP_8-1-consfactor.cpp:284-448 and 451-615 */
 static void dpmodel(double dept[6][6], const double* sig, const double* deps, const sphgpu_soil* so, double* adps, int bui)
@@ -792,8 +913,9 @@ static void jaumann(double* ds, const double* s, const double* w)
 }
 
 /* strain_to_stress: CPP_7-2-constitutive.cpp:13-321.  Soil models restated:
- * elastic (matype%10 = 0, 6), Drucker-Prager (2, with DPModel_check), Bui DP
- * (5, with DPModel_check). */
+ * elastic (matype%10 = 0, 6), subloading Cam-clay (1), Drucker-Prager (2,
+ * with DPModel_check), Bui DP (5, with DPModel_check), viscous-elastic (7) and
+ * Mohr-Coulomb (9). */
 static int strain_to_stress(orc_ctx* c)
 {
     const sphgpu_params* P = &c->P;
@@ -838,15 +960,24 @@ static int strain_to_stress(orc_ctx* c)
             double* ds = &c->dsig[i * 6];
             int mt = c->matype[i] % 10;
             if (P->flts >= 1) return SPHGPU_E_UNSUPPORTED;
+            /* matype 30-49 and >= 60 match no branch of the reference's dispatch */
+            if ((c->matype[i] >= 30 && c->matype[i] < 50) || c->matype[i] >= 60) return SPHGPU_E_UNSUPPORTED;
             if (c->l < P->inip || mt == 0 || mt == 6) {
                 elastic_d(dept, s, &c->so[i], &dl, &dm, &sm);
+            } else if (mt == 1) {
+                sub_camclay(dept, s, de, &c->so[i], adps);
             } else if (mt == 2 || mt == 5) {
                 dpmodel(dept, s, de, &c->so[i], adps, mt == 5);
+            } else if (mt == 9) {
+                mc_model(dept, s, de, &c->so[i], adps);
+            } else if (mt == 7) {
+                visco_elastic(ds, s, de, &c->so[i]);
             } else {
                 return SPHGPU_E_UNSUPPORTED;
             }
-            for (int a = 0; a < 6; a++)
-                for (int b = 0; b < 6; b++) ds[a] += dept[a][b] * de[b];
+            if (c->l < P->inip || mt != 7)
+                for (int a = 0; a < 6; a++)
+                    for (int b = 0; b < 6; b++) ds[a] += dept[a][b] * de[b];
             if (!(c->l < P->inip) && (mt == 2 || mt == 5)) dp_check(s, ds, &c->so[i], dt);
             jaumann(ds, s, &c->weps[i * 9]);
             for (int a = 0; a < 6; a++) {

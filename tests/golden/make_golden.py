@@ -68,6 +68,16 @@ def _column_drag(fli, eps0, vw):
     return make
 
 
+MCC = dict(ramda=0.2, kapa=0.04, zmf=1.2, eps0=0.9, poi=0.3, sme0=50.0e3, ann=1.0, ocr=1.5, e=0.0, fs=1.0)
+
+
+def _column_model(matype, **record):
+    """The soil column with its soil switched to another constitutive model:
+    subloading Cam-clay (1; lambda 0.2, kappa 0.04, M 1.2, e0 0.9, p0 50 kPa,
+    E from kappa and p), viscous-elastic (7) or Mohr-Coulomb (9)."""
+    return lambda: scenes.set_soil_model(scenes.soil_column_3d(dx=0.1, steps=200), matype, **record)
+
+
 CASES = {
     # name: (scene factory, steps)
     "dam_break_2d_dx0.04": (lambda: scenes.dam_break_2d(dx=0.04, steps=200), 25),
@@ -77,6 +87,9 @@ CASES = {
     "soil_column_3d_dx0.1_art_stress": (_column_art_stress, 12),
     "soil_column_3d_dx0.1_drag_tsuji_dilute": (_column_drag(2, 5.0, 1.0), 10),
     "soil_column_3d_dx0.1_drag_peng": (_column_drag(3, 0.6667, 0.05), 10),
+    "soil_column_3d_dx0.1_camclay": (_column_model(1, **MCC), 20),
+    "soil_column_3d_dx0.1_mohr_coulomb": (_column_model(9, c=0.0, fai=30.0, e=1.0e7), 20),
+    "soil_column_3d_dx0.1_visco_elastic": (_column_model(7, c=1.0e5, e=1.0e7), 20),
 }
 
 

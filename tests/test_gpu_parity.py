@@ -255,3 +255,30 @@ def test_drag_forms(fli, eps0, vw):
     worst = _compare(eng, orc, tol=DRAG_REL_TOL)
     print(f"drag fli={fli}, worst relative error per field:", max(worst.values()))
     assert np.abs(eng.get_field("interf")).max() > 0.0
+
+
+MCC = dict(ramda=0.2, kapa=0.04, zmf=1.2, eps0=0.9, poi=0.3, sme0=50.0e3, ann=1.0, ocr=1.5, e=0.0, fs=1.0)
+# sub_camclay's subloading ratio takes log(p0 / p): CUDA's and the C
+# library's log may differ by an ulp, so that model is held to a tolerance;
+# Mohr-Coulomb and viscous-elastic use no transcendental function on the
+# device and are compared bit for bit.
+MCC_REL_TOL = 1e-12
+
+
+@pytest.mark.parametrize("label,factory,steps,tol", [
+    ("camclay", lambda: scenes.set_soil_model(scenes.soil_column_3d(dx=0.05, steps=100), 1, **MCC), 20, MCC_REL_TOL),
+    ("camclay_2d", lambda: scenes.set_soil_model(scenes.slope_2d(H=1.0, dx=0.05), 1, **MCC), 30, MCC_REL_TOL),
+    ("mohr_coulomb", lambda: scenes.set_soil_model(scenes.soil_column_3d(dx=0.05, steps=100), 9,
+                                                   c=0.0, fai=30.0, e=1.0e7), 20, 0.0),
+    ("visco_elastic", lambda: scenes.set_soil_model(scenes.soil_column_3d(dx=0.05, steps=100), 7,
+                                                    c=1.0e5, e=1.0e7), 20, 0.0),
+])
+def test_soil_models(label, factory, steps, tol):
+    """Subloading Cam-clay, Mohr-Coulomb and viscous-elastic soil against the
+    oracle (whose same runs are bit-identical to the reference)."""
+    _, eng, orc = _engine_and_oracle(factory())
+    eng.step(steps)
+    assert orc.step(steps) == 0
+    worst = _compare(eng, orc, tol=tol)
+    if worst:
+        print(f"soil model {label}, worst relative error per field:", max(worst.values()))

@@ -16,7 +16,8 @@ from checkers import (ORC_INPLACE, ORC_JACOBI, ORC_POW_CR, ORC_POW_LIBM, STATE_F
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ["dam_break_2d_dx0.04", "soil_column_3d_dx0.1", "soil_column_3d_dx0.1_kgc_regu",
          "slope_2d_H1_dx0.05_art_stress", "soil_column_3d_dx0.1_art_stress",
-         "soil_column_3d_dx0.1_drag_tsuji_dilute", "soil_column_3d_dx0.1_drag_peng"]
+         "soil_column_3d_dx0.1_drag_tsuji_dilute", "soil_column_3d_dx0.1_drag_peng",
+         "soil_column_3d_dx0.1_camclay", "soil_column_3d_dx0.1_mohr_coulomb", "soil_column_3d_dx0.1_visco_elastic"]
 
 
 def _golden(name):
@@ -262,3 +263,36 @@ def test_live_reference_drag_forms(fli, eps0, vw):
     for k in STATE_FIELDS:
         assert np.array_equal(orc.get_field(k), ref.get_field(k)), k
     assert np.abs(ref.get_field("interf")).max() > 0.0
+
+
+MCC = dict(ramda=0.2, kapa=0.04, zmf=1.2, eps0=0.9, poi=0.3, sme0=50.0e3, ann=1.0, ocr=1.5, e=0.0, fs=1.0)
+
+
+@needs_ref
+@pytest.mark.parametrize("label,factory,steps", [
+    ("camclay", lambda: scenes.set_soil_model(scenes.soil_column_3d(dx=0.05, steps=100), 1, **MCC), 20),
+    ("camclay_2d", lambda: scenes.set_soil_model(scenes.slope_2d(H=1.0, dx=0.05), 1, **MCC), 30),
+    ("mohr_coulomb", lambda: scenes.set_soil_model(scenes.soil_column_3d(dx=0.05, steps=100), 9,
+                                                   c=0.0, fai=30.0, e=1.0e7), 20),
+    ("mohr_coulomb_cohesive", lambda: scenes.set_soil_model(scenes.soil_column_3d(dx=0.05, steps=100), 9,
+                                                            c=5.0e3, fai=25.0, e=1.0e7), 20),
+    ("visco_elastic", lambda: scenes.set_soil_model(scenes.soil_column_3d(dx=0.05, steps=100), 7,
+                                                    c=1.0e5, e=1.0e7), 20),
+])
+def test_live_reference_soil_models(label, factory, steps):
+    """sub_camclay, elastic_plastic (M-C) and viscous_elastic
+    (CPP_8-1-consfactor.cpp:88-281, 618-777): bit-identical to the reference;
+    the plastic branch is reached for the Cam-clay and cohesionless M-C
+    cases."""
+    sc = factory()
+    ref = _live(sc)
+    fl, so = ref.materials()
+    orc = Oracle(ref.params, ORC_INPLACE)
+    orc.load_state({k: ref.get_field(k) for k in STATE_FIELDS}, fl, so)
+    assert ref.step(steps) == 0
+    assert orc.step(steps) == 0
+    for k in STATE_FIELDS:
+        assert np.array_equal(orc.get_field(k), ref.get_field(k)), k
+    if label in ("camclay", "camclay_2d", "mohr_coulomb"):
+        t = ref.get_field("type")
+        assert (np.abs(ref.get_field("adps")[t == 2]).sum(axis=1) > 0).any()
