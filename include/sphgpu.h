@@ -136,6 +136,24 @@ int         sphgpu_get_step(const sphgpu_ctx* ctx);
 int         sphgpu_set_step(sphgpu_ctx* ctx, int l);
 
 /*
+ * Precision form of the step (the reference has one, FP64: every method of
+ * clDensity_Fun / clStraStre_Fun / clAcce_Fun / clVel_Fun, Class_Functions.h:61-162).
+ *   SPHGPU_PREC_FP64       the drop-in: the reference's FP64 arithmetic, operation
+ *                          for operation (the default)
+ *   SPHGPU_PREC_FP32_BULK  pair arithmetic of the neighbour passes (kernel values
+ *                          and gradients, pair terms and their sums) in FP32 with
+ *                          Kahan-compensated sums; positions, velocities, densities,
+ *                          stresses, time integration, the constitutive update and
+ *                          the neighbour search stay FP64, so neighbour lists are
+ *                          identical in both forms
+ * May be switched between steps; the state carries over.
+ */
+#define SPHGPU_PREC_FP64      0
+#define SPHGPU_PREC_FP32_BULK 1
+int         sphgpu_set_precision(sphgpu_ctx* ctx, int mode);
+int         sphgpu_get_precision(const sphgpu_ctx* ctx);
+
+/*
  * Field transfer, structure of arrays.  `name` is a Particle member
  * (Class_particle.h:13-103): "xp", "vx", "sig", "rho", "type", ...
  * sphgpu_field_info reports the component count and element type

@@ -5,8 +5,9 @@
 nvcc compiles the kernels and the C-ABI host code into one shared library next
 to this file.  -fmad=false keeps every FP64 multiply and add separately
 rounded (no contraction into fused multiply-adds), as the reference's x86-64
-build rounds them; the engine's results therefore follow the reference's
-arithmetic operation for operation.
+build rounds them; the FP64 drop-in form therefore follows the reference's
+arithmetic operation for operation.  The FP32-bulk form
+(sph_kernels_bulk32.cu) is compiled with contraction allowed.
 """
 from __future__ import annotations
 
@@ -17,15 +18,15 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsphgpu.so")
-SOURCES = ["sph_kernels.cu", "sph_capi.cu", "sph_noalloc.cu"]
+SOURCES = ["sph_kernels.cu", "sph_capi.cu", "sph_noalloc.cu", "sph_kernels_bulk32.cu"]
+# per-source flags on top of NVCC_FLAGS
+SOURCE_FLAGS = {"sph_kernels_bulk32.cu": ["-fmad=true"]}
 HEADERS = ["sph_device.cuh", "sph_constitutive.cuh", os.path.join("..", "..", "include", "sphgpu.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
-    "-fmad=false",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
-    "-shared",
 ]
 
 
@@ -41,11 +42,22 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + ["-o", LIB] + [os.path.join(CSRC, s) for s in SOURCES]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    procs, objs = [], []
+    for src in SOURCES:
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        flags = SOURCE_FLAGS.get(src, ["-fmad=false"])
+        cmd = [nvcc] + NVCC_FLAGS + flags + ["-c", "-o", obj, os.path.join(CSRC, src)]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+            print(" ".join(cmd))
+        procs.append(subprocess.Popen(cmd))
+        objs.append(obj)
+    for p in procs:
+        if p.wait() != 0:
+            raise subprocess.CalledProcessError(p.returncode, "nvcc")
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB] + objs, check=True)
     return LIB
 
 

@@ -21,6 +21,7 @@ extern "C" size_t sphk_sort_temp_bytes(int N, int end_bit);
 extern "C" int sphk_enqueue_nnps(const Dev* d, void* sort_tmp, size_t sort_bytes, int end_bit, cudaStream_t st,
                                  cudaEvent_t* ev);
 extern "C" int sphk_enqueue_physics(const Dev* d, cudaStream_t st, cudaEvent_t* ev, int regu);
+extern "C" int sphk_enqueue_physics_bulk32(const Dev* d, cudaStream_t st, cudaEvent_t* ev, int regu);
 extern "C" const char* const sphk_stage_names[];
 
 namespace {
@@ -91,6 +92,7 @@ struct sphgpu_ctx {
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
     bool regu = false;     // graphs include the strain/stress regularisation passes
+    int precision = SPHGPU_PREC_FP64;
 };
 
 namespace {
@@ -141,6 +143,14 @@ int end_bit_for(int m)
     return b;
 }
 
+// the physics stages of one step in the context's precision form
+int enqueue_physics(const sphgpu_ctx* c, const Dev* d, cudaEvent_t* ev)
+{
+    const int regu = c->regu ? 1 : 0;
+    if (c->precision == SPHGPU_PREC_FP32_BULK) return sphk_enqueue_physics_bulk32(d, c->st, ev, regu);
+    return sphk_enqueue_physics(d, c->st, ev, regu);
+}
+
 // (re)build the two step graphs: NNPS + physics for parity 0 and 1
 int build_graphs(sphgpu_ctx* c)
 {
@@ -149,7 +159,7 @@ int build_graphs(sphgpu_ctx* c)
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
         int n = sphk_enqueue_nnps(&c->d[p], c->sort_tmp, c->sort_bytes, c->end_bit, c->st, nullptr);
-        n += sphk_enqueue_physics(&c->d[p], c->st, nullptr, c->regu ? 1 : 0);
+        n += enqueue_physics(c, &c->d[p], nullptr);
         cudaError_t e = cudaStreamEndCapture(c->st, &g);
         if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
         e = cudaGraphInstantiate(&c->exec[p], g, 0);
@@ -300,11 +310,10 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.s_c, N); r |= dalloc(c, &s.s_fs, N);
     r |= dalloc(c, &s.s_ann, N); r |= dalloc(c, &s.s_zmf, N); r |= dalloc(c, &s.s_ramda, N); r |= dalloc(c, &s.s_sme0, N);
     r |= dalloc(c, &s.s_yalf, N); r |= dalloc(c, &s.s_ykap, N); r |= dalloc(c, &s.s_yalf_dil, N);
-    r |= dalloc(c, &s.xh, 4 * (size_t)N); r |= dalloc(c, &s.xh_next, 4 * (size_t)N); r |= dalloc(c, &s.xs, 4 * (size_t)N);
+    r |= dalloc(c, &s.xh, 4 * (size_t)N); r |= dalloc(c, &s.xh_next, 4 * (size_t)N); r |= dalloc(c, &s.xs, 4 * (size_t)N); r |= dalloc(c, &s.xsf, 4 * (size_t)N);
     r |= dalloc(c, &s.de, 6 * (size_t)N); r |= dalloc(c, &s.we, 6 * (size_t)N); r |= dalloc(c, &s.color, N);
     r |= dalloc(c, &s.sr, 6 * (size_t)N); r |= dalloc(c, &s.pp, N);
     r |= dalloc(c, &s.eps_tmp, 6 * (size_t)N); r |= dalloc(c, &s.sig_tmp, 6 * (size_t)N);
-    if (P->flknl > 2) r |= dalloc(c, &s.lmat, 9 * (size_t)N);
     if (P->art_stre_coe > 0.0) r |= dalloc(c, &s.rij, 9 * (size_t)N);
     r |= dalloc(c, &s.vx, 3 * (size_t)N); r |= dalloc(c, &s.vx_next, 3 * (size_t)N);
     r |= dalloc(c, &s.vxp, 3 * (size_t)N); r |= dalloc(c, &s.axp, 3 * (size_t)N); r |= dalloc(c, &s.ax, 3 * (size_t)N);
@@ -321,6 +330,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.val_in, N); r |= dalloc(c, &s.pid_sorted, N);
     r |= dalloc(c, &s.cstart, M); r |= dalloc(c, &s.cend, M);
     r |= dalloc(c, &s.nnb, N); r |= dalloc(c, &s.nbr, (size_t)SPH_NB_CAP * N);
+    r |= dalloc(c, &s.nbw, 4 * (size_t)SPH_NB_CAP * N);
     r |= dalloc(c, &s.err, 1); r |= dalloc(c, &s.step, 1);
     if (r) return fail(SPHGPU_E_CUDA);
     // cell_info() constructor values (Class_NNPS.cpp:68-72): the range of the
@@ -365,6 +375,21 @@ int sphgpu_get_params(const sphgpu_ctx* c, sphgpu_params* out)
 }
 
 int sphgpu_get_step(const sphgpu_ctx* c) { return c ? c->l_host : -1; }
+
+int sphgpu_set_precision(sphgpu_ctx* c, int mode)
+{
+    if (!c || (mode != SPHGPU_PREC_FP64 && mode != SPHGPU_PREC_FP32_BULK)) return SPHGPU_E_ARG;
+    if (mode != c->precision) {
+        cudaSetDevice(c->device);
+        CK(cudaStreamSynchronize(c->st));
+        c->precision = mode;
+        for (int p = 0; p < 2; p++) c->d[p].p.bulk = (mode == SPHGPU_PREC_FP32_BULK) ? 1 : 0;
+        invalidate_graphs(c);
+    }
+    return 0;
+}
+
+int sphgpu_get_precision(const sphgpu_ctx* c) { return c ? c->precision : -1; }
 
 int sphgpu_set_step(sphgpu_ctx* c, int l)
 {
@@ -702,7 +727,7 @@ int sphgpu_step_profiled(sphgpu_ctx* c, int nsteps, double* stage_ms)
     for (int s = 0; s < nsteps && err == 0; s++) {
         const Dev* d = &c->d[c->parity];
         sphk_enqueue_nnps(d, c->sort_tmp, c->sort_bytes, c->end_bit, c->st, ev);
-        sphk_enqueue_physics(d, c->st, ev, c->regu ? 1 : 0);
+        enqueue_physics(c, d, ev);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(c->st));
         for (int k = 0; k < SPHK_NSTAGES; k++) {

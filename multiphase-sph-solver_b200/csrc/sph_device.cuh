@@ -11,7 +11,9 @@
 //                Particle::sig), component k at a[k * N + i]
 //   * neighbour lists: int nbr[SPH_NB_CAP * N], slot s of particle i at
 //                nbr[s * N + i], so the threads of a warp read consecutive
-//                words per slot.
+//                words per slot; the pair's kernel gradient and value
+//                (Par_Cell::wij) in the same slot order, nbw[s * N + i], as a
+//                32-byte FP64 record or a 16-byte FP32 record (bulk form).
 // Component-major storage makes every own-particle load of one component a
 // coalesced 8-byte-per-lane access.
 //
@@ -28,7 +30,7 @@
 #define SPH_NB_CAP 99          // Par_Cell::influ[100], slots 1..99 (Class_NNPS.h:71)
 #define SPH_ERR_CELL 3         // parttocell, CPP_3-NNPS.cpp:247-257
 #define SPH_ERR_NEIGH 5        // partisearching, CPP_3-NNPS.cpp:313-319
-#define SPHK_NSTAGES 18        // entries of sphk_stage_names (one event bracket each)
+#define SPHK_NSTAGES 19        // entries of sphk_stage_names (one event bracket each)
 
 struct DevParams {
     int N, ndim, flknl, flbndy, fli, if_move, flv, inip, step_regu;
@@ -48,6 +50,7 @@ struct DevParams {
     double st_e, st_poi;       // Para_Structure elastic constants
     double g_acc;              // |g|, interact1 (CPP_10-interact1.cpp:28)
     double art_stre_coe;       // artificial stress coefficient (0: off)
+    int bulk;                  // 1: the FP32-bulk form (pair records in FP32)
 };
 
 struct DevState {
@@ -66,6 +69,7 @@ struct DevState {
     // positions (x, y, z, h) records, ping-pong
     double *xh, *xh_next;
     double *xs;                // xh in cell-sorted order (NNPS scan)
+    float *xsf;                // xs as FP32 (x - xmin, y - ymin, z - zmin, h) records: the NNPS prefilter
     // dynamic state
     double *vx, *vx_next;      // vx: velocity after the step; vx_next: before XSPH
     double *vxp, *axp, *ax, *ux;
@@ -83,7 +87,6 @@ struct DevState {
     double *pp;                // pore-pressure term / rho^2, N
     double *eps_in;            // strain the constitutive pass starts from: eps, or eps_tmp after strain_regu
     double *eps_tmp, *sig_tmp; // outputs of the regularisation passes, 6N each
-    double *lmat;              // inverse CSPM matrix per soil/structure particle, 9N (flknl 3/4)
     double *rij;               // artificial stress tensor R per soil particle, 9N row-major (art_stre_coe > 0)
     // NNPS
     int *cell;                 // cell id per particle
@@ -92,6 +95,9 @@ struct DevState {
     int *cstart, *cend;        // [ctotal + 4]
     int *nnb;                  // neighbour count (may exceed the cap: error 5)
     int *nbr;                  // [SPH_NB_CAP * N]
+    double *nbw;               // pair records (grad W, W) of the neighbour-list slots, [SPH_NB_CAP * N]
+                               // records of 32 bytes (FP64), or 16 bytes (FP32, bulk form) in the
+                               // first half of the same buffer
     // control words
     int *err;                  // first error code raised (0 = none)
     int *step;                 // Para_Pro::l of the step being run
@@ -119,101 +125,146 @@ __device__ __forceinline__ void store_pos(double* xh, int i, const Pos& q)
 }
 
 // the normalisation constant a1 of weight() / weight2() for support ra
-// (CPP_3-NNPS.cpp:24-29, 58-63)
-__device__ __forceinline__ double kernel_a1(double ra, int ndim, int flknl)
+// (CPP_3-NNPS.cpp:24-29, 58-63), in the pair arithmetic's type R
+template <typename R>
+__device__ __forceinline__ R kernel_a1(R ra, int ndim, int flknl)
 {
     if (flknl == 1 || flknl == 3)
-        return (ndim == 2) ? 0.682092613250980 / ra / ra : 0.477464829275686 / ra / ra / ra;
-    return (ndim == 2) ? 0.106103295394597 / (ra * ra) : 0.077010456334788 / (ra * ra * ra);
+        return (ndim == 2) ? R(0.682092613250980) / ra / ra : R(0.477464829275686) / ra / ra / ra;
+    return (ndim == 2) ? R(0.106103295394597) / (ra * ra) : R(0.077010456334788) / (ra * ra * ra);
 }
 
-// Particle i's side of every pair: position, h and a1 for ra = h_i (the
-// reference's ra = (h_i + h_j) / 2 equals h_i exactly when h_j == h_i).
-struct PairI {
-    double x[3];
-    double h, a1;
-    bool corr;                 // kernel gradient correction applies (flknl 3/4, soil or structure)
-    double L[9];               // its inverse CSPM matrix, row-major
+// A pair sum.  In FP64 it is the plain running sum the reference forms; in
+// FP32 (the bulk form) it is Kahan-compensated, and the compensation is folded
+// back in FP64 when the sum is read.
+template <typename R> struct Sum;
+template <> struct Sum<double> {
+    double s = 0.0;
+    __device__ __forceinline__ void add(double x) { s = s + x; }
+    __device__ __forceinline__ double v() const { return s; }
+};
+template <> struct Sum<float> {
+    float s = 0.f, c = 0.f;
+    __device__ __forceinline__ void add(float x)
+    {
+        const float y = x - c;
+        const float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ double v() const { return (double)s - (double)c; }
 };
 
-template <int ND, int KGC>
-__device__ __forceinline__ PairI pair_i(const Dev& d, int i)
+// Particle i's side of every pair: position (FP64: pair differences are
+// taken in FP64 and then rounded to R), h and a1 for ra = h_i (the
+// reference's ra = (h_i + h_j) / 2 equals h_i exactly when h_j == h_i).
+template <typename R>
+struct PairI {
+    double x[3];
+    R h, a1;
+};
+
+template <int ND, typename R>
+__device__ __forceinline__ PairI<R> pair_i(const Dev& d, int i)
 {
     Pos q = load_pos(d.s.xh, i);
-    PairI I;
-    I.x[0] = q.x; I.x[1] = q.y; I.x[2] = q.z; I.h = q.h;
-    I.a1 = kernel_a1(q.h, ND, d.p.flknl);
-    I.corr = false;
-    if (KGC) {
-        const int t = d.s.type[i];
-        I.corr = (t == 2 || t == 4);
-        for (int k = 0; k < 9; k++) I.L[k] = I.corr ? d.s.lmat[(size_t)k * d.p.N + i] : 0.0;
-    }
+    PairI<R> I;
+    I.x[0] = q.x; I.x[1] = q.y; I.x[2] = q.z; I.h = (R)q.h;
+    I.a1 = kernel_a1<R>(I.h, ND, d.p.flknl);
     return I;
 }
 
 // Kernel value and gradient of pair (i, j) exactly as partisearching stored
 // them: weight() / weight2() (CPP_3-NNPS.cpp:17-82) with the same
 // differences, summation order and sqrt, recomputed from this step's
-// positions.  w[0..2] gradient, w[3] value.
-template <int ND>
-__device__ __forceinline__ void pair_w_raw(const Dev& d, const PairI& I, const Pos& pj, double w[4]);
-
-// Kernel value and gradient as the consumers read them: with flknl 3/4 the
-// gradient of a soil or structure particle's pairs is corrected in place by
-// kernel_gradient_correction (CPP_3-NNPS.cpp:464-493): grad' = L^-1 grad,
-// in mat_multiply's order (:85-90).
-template <int ND, int KGC>
-__device__ __forceinline__ void pair_w(const Dev& d, const PairI& I, const Pos& pj, double w[4])
+// positions.  w[0..2] gradient, w[3] value.  In FP32 the gradient's common
+// factor is divided once per pair instead of once per component.
+template <int ND, typename R>
+__device__ __forceinline__ void pair_w_raw(const Dev& d, const PairI<R>& I, const Pos& pj, R w[4])
 {
-    pair_w_raw<ND>(d, I, pj, w);
-    if (KGC && I.corr) {
-        const double* a = I.L;
-        double c0 = a[0] * w[0] + a[1] * w[1] + a[2] * w[2];
-        double c1 = a[3] * w[0] + a[4] * w[1] + a[5] * w[2];
-        double c2 = a[6] * w[0] + a[7] * w[1] + a[8] * w[2];
-        w[0] = c0; w[1] = c1; w[2] = c2;
+    constexpr int nd = ND;
+    constexpr bool f32 = sizeof(R) == 4;
+    const double xj[3] = {pj.x, pj.y, pj.z};
+    R dx[3] = {R(0), R(0), R(0)}, dst = R(0);
+    for (int k = 0; k < nd; k++) {
+        const R t = (R)(I.x[k] - xj[k]);
+        dst = dst + t * t;
+        dx[k] = t;
+    }
+    dst = sqrt(dst);
+    const R hj = (R)pj.h;
+    const R ra = (hj == I.h) ? I.h : (I.h + hj) / 2;
+    const R a1 = (hj == I.h) ? I.a1 : kernel_a1<R>(ra, nd, d.p.flknl);
+    const R s = dst / ra;
+    w[0] = w[1] = w[2] = w[3] = R(0);
+    if (d.p.flknl == 1 || d.p.flknl == 3) {
+        if (s == R(0)) {
+            w[3] = a1 * (R(0.66666667) - s * s + R(0.5) * s * s * s);
+        }
+        if (s > R(0) && s <= R(1)) {
+            if (f32) {
+                const R g = a1 * (-2 * s + R(1.5) * s * s) / (ra * dst);
+                for (int k = 0; k < nd; k++) w[k] = dx[k] * g;
+            } else {
+                for (int k = 0; k < nd; k++) w[k] = a1 * dx[k] * (-2 * s + R(1.5) * s * s) / (ra * dst);
+            }
+            w[3] = a1 * (R(0.66666667) - s * s + R(0.5) * s * s * s);
+        } else if (s > R(1) && s <= R(2)) {
+            if (f32) {
+                const R g = a1 * R(-0.5) * (R(2.0) - s) * (R(2.0) - s) / (ra * dst);
+                for (int k = 0; k < nd; k++) w[k] = dx[k] * g;
+            } else {
+                for (int k = 0; k < nd; k++) w[k] = a1 * R(-0.5) * dx[k] * (R(2.0) - s) * (R(2.0) - s) / (ra * dst);
+            }
+            w[3] = a1 * (R(2.0) - s) * (R(2.0) - s) * (R(2.0) - s) / R(6.0);
+        }
+    } else {
+        if (s == R(0)) {
+            w[3] = a1 * (R(6.0) - R(6.0) * s + R(1.0) * s * s * s);
+        }
+        if (s > R(0) && s <= R(1)) {
+            if (f32) {
+                const R g = a1 * (R(-6.0) + R(3.0) * s * s) / (ra * dst);
+                for (int k = 0; k < nd; k++) w[k] = dx[k] * g;
+            } else {
+                for (int k = 0; k < nd; k++) w[k] = a1 * dx[k] * (R(-6.0) + R(3.0) * s * s) / (ra * dst);
+            }
+            w[3] = a1 * (R(6.0) - R(6.0) * s + R(1.0) * s * s * s);
+        } else if (s > R(1) && s <= R(2)) {
+            if (f32) {
+                const R g = a1 * R(-3.0) * (R(2.0) - s) * (R(2.0) - s) / (ra * dst);
+                for (int k = 0; k < nd; k++) w[k] = dx[k] * g;
+            } else {
+                for (int k = 0; k < nd; k++) w[k] = a1 * R(-3.0) * dx[k] * (R(2.0) - s) * (R(2.0) - s) / (ra * dst);
+            }
+            w[3] = a1 * (R(2.0) - s) * (R(2.0) - s) * (R(2.0) - s);
+        }
     }
 }
 
-template <int ND>
-__device__ __forceinline__ void pair_w_raw(const Dev& d, const PairI& I, const Pos& pj, double w[4])
+// The stored pair record of slot s of particle i: kernel gradient w[0..2] and
+// value w[3], as partisearching stores Par_Cell::wij (CPP_3-NNPS.cpp:339-345),
+// corrected in place by kernel_gradient_correction when flknl is 3 or 4.
+__device__ __forceinline__ void load_w(const Dev& d, int s, int i, double w[4])
 {
-    constexpr int nd = ND;
-    const double xj[3] = {pj.x, pj.y, pj.z};
-    double dx[3] = {0.0, 0.0, 0.0}, dst = 0.0;
-    for (int k = 0; k < nd; k++) {
-        dst = dst + (I.x[k] - xj[k]) * (I.x[k] - xj[k]);
-        dx[k] = I.x[k] - xj[k];
-    }
-    dst = sqrt(dst);
-    const double ra = (pj.h == I.h) ? I.h : (I.h + pj.h) / 2;
-    const double a1 = (pj.h == I.h) ? I.a1 : kernel_a1(ra, nd, d.p.flknl);
-    const double s = dst / ra;
-    w[0] = w[1] = w[2] = w[3] = 0.0;
-    if (d.p.flknl == 1 || d.p.flknl == 3) {
-        if (s == 0.0) {
-            w[3] = a1 * (0.66666667 - s * s + 0.5 * s * s * s);
-        }
-        if (s > 0.0 && s <= 1.0) {
-            for (int k = 0; k < nd; k++) w[k] = a1 * dx[k] * (-2 * s + 1.5 * s * s) / (ra * dst);
-            w[3] = a1 * (0.66666667 - s * s + 0.5 * s * s * s);
-        } else if (s > 1.0 && s <= 2.0) {
-            for (int k = 0; k < nd; k++) w[k] = a1 * (-0.5) * dx[k] * (2.0 - s) * (2.0 - s) / (ra * dst);
-            w[3] = a1 * (2.0 - s) * (2.0 - s) * (2.0 - s) / 6.0;
-        }
-    } else {
-        if (s == 0.0) {
-            w[3] = a1 * (6.0 - 6.0 * s + 1.0 * s * s * s);
-        }
-        if (s > 0.0 && s <= 1.0) {
-            for (int k = 0; k < nd; k++) w[k] = a1 * dx[k] * (-6.0 + 3.0 * s * s) / (ra * dst);
-            w[3] = a1 * (6.0 - 6.0 * s + 1.0 * s * s * s);
-        } else if (s > 1.0 && s <= 2.0) {
-            for (int k = 0; k < nd; k++) w[k] = a1 * (-3.0) * dx[k] * (2.0 - s) * (2.0 - s) / (ra * dst);
-            w[3] = a1 * (2.0 - s) * (2.0 - s) * (2.0 - s);
-        }
-    }
+    const double2* p = reinterpret_cast<const double2*>(d.s.nbw) + 2 * ((size_t)s * d.p.N + i);
+    const double2 a = p[0], b = p[1];
+    w[0] = a.x; w[1] = a.y; w[2] = b.x; w[3] = b.y;
+}
+__device__ __forceinline__ void load_w(const Dev& d, int s, int i, float w[4])
+{
+    const float4 f = reinterpret_cast<const float4*>(d.s.nbw)[(size_t)s * d.p.N + i];
+    w[0] = f.x; w[1] = f.y; w[2] = f.z; w[3] = f.w;
+}
+__device__ __forceinline__ void store_w(const Dev& d, int s, int i, const double w[4])
+{
+    double2* p = reinterpret_cast<double2*>(d.s.nbw) + 2 * ((size_t)s * d.p.N + i);
+    p[0] = make_double2(w[0], w[1]);
+    p[1] = make_double2(w[2], w[3]);
+}
+__device__ __forceinline__ void store_w(const Dev& d, int s, int i, const float w[4])
+{
+    reinterpret_cast<float4*>(d.s.nbw)[(size_t)s * d.p.N + i] = make_float4(w[0], w[1], w[2], w[3]);
 }
 
 // x^7 rounded to nearest from a double-double product chain (Dekker's exact

@@ -23,15 +23,38 @@
 // Every pair sum is gathered by the particle that owns it, in the reference's
 // neighbour order, with no atomics: results are deterministic and, with
 // -fmad=false, equal to the reference's FP64 arithmetic.  Kernel values are
-// recomputed per pair from the positions (pair_w) instead of being stored.
+// computed once per pair by the neighbour search and stored with the list,
+// as partisearching stores Par_Cell::wij.
 // All kernels return immediately once an error code is set, so a failing step
 // leaves the state as the reference leaves it when it returns the code.
+//
+// The file is compiled twice.  Built plainly it is the FP64 drop-in form:
+// -fmad=false, every pair sum in the reference's FP64 order.  Built with
+// SPH_BULK32 defined (sph_kernels_bulk32.cu) it is the FP32-bulk form: the
+// pair arithmetic of the neighbour passes (kernel values and gradients, pair
+// terms, their sums) runs in FP32 with Kahan-compensated sums, while
+// positions, velocities, densities, stresses, their time integration and the
+// constitutive update stay FP64; pair differences of positions and velocities
+// are taken in FP64 before they are rounded.  The neighbour search is shared
+// by both forms and lives in the FP64 build only.
 #include <cub/cub.cuh>
 #include <climits>
 #include "sph_device.cuh"
 #include "sph_constitutive.cuh"
 
+#ifdef SPH_BULK32
+typedef float real;            // pair arithmetic of the neighbour passes
+#define SPH_NS sph_bulk32
+#define SPHK_ENTRY(name) name##_bulk32
+#else
+typedef double real;
+#define SPH_NS sph_fp64
+#define SPHK_ENTRY(name) name
+#endif
+
 #define IDX (blockIdx.x * blockDim.x + threadIdx.x)
+
+namespace SPH_NS {
 
 // minimum resident 128-thread blocks per SM requested from the register
 // allocator for the neighbour-loop kernels (an occupancy / spill trade-off)
@@ -81,6 +104,7 @@ __device__ __forceinline__ int nbr_count(const Dev& d, int i)
 }
 
 // ---------------------------------------------------------------------------
+#ifndef SPH_BULK32
 template <int ND>
 __global__ void k_cellkey(Dev d)
 {
@@ -139,13 +163,29 @@ __global__ void k_cellrange(Dev d)
         if (first) d.s.cstart[c] = q;
         if (last) d.s.cend[c] = q;
     }
-    store_pos(d.s.xs, q, load_pos(d.s.xh, d.s.pid_sorted[q]));
+    const Pos r = load_pos(d.s.xh, d.s.pid_sorted[q]);
+    store_pos(d.s.xs, q, r);
+    reinterpret_cast<float4*>(d.s.xsf)[q] =
+        make_float4((float)(r.x - d.p.xmin), (float)(r.y - d.p.ymin), (float)(r.z - d.p.zmin), (float)r.h);
 }
 
 // partisearching (CPP_3-NNPS.cpp:265-374): neighbours of i in stencil order,
 // descending index inside each cell; inclusion dst <= h_i + h_j decided as the
-// reference decides it (sqrt of the FP64 sum of squares), with the sqrt only
-// evaluated when the squared distance is within 1e-10 of the squared radius.
+// reference decides it (sqrt of the FP64 sum of squares).
+//
+// Each candidate is first tested in FP32 on the (x - xmin, y - ymin, z - zmin,
+// h) records, against a margin M that bounds every rounding between the FP32
+// squared distance d2f and the exact one: the coordinates' rounding to FP32
+// (at most 2^-24 |coordinate|, and |x_j - xmin| <= |x_i - xmin| + |x_i - x_j|),
+// the subtraction, squares and sum, and the rounding of T = h_i + h_j and T^2.
+// With F_i the particle's largest |coordinate - min| and e = 2.2 u (F_i + 2 T),
+// u = 2^-24, every candidate with d2f <= 4 T^2 has |d2f - d2| <= nd e (4 T + e)
+// + 12.4 u T^2; M adds 32 u T^2 on top of that.  Candidates with d2f > 4 T^2
+// are outside whenever h_i > 10 u F_i (the error then grows more slowly than
+// d2f - T^2); the test requires h_i > 64 u F_i and otherwise sends every
+// candidate to the FP64 path.  Only candidates within M of T^2 take the FP64
+// path, where the sqrt is evaluated only within 1e-10 of the squared radius,
+// so the decisions are those of the reference.
 template <int ND>
 __global__ void __launch_bounds__(128, SPH_MINB) k_nnps(Dev d)
 {
@@ -154,24 +194,54 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_nnps(Dev d)
     int cnt = 0;
     if (d.s.type[i] != 7) {
         constexpr int nd = ND, nst = (ND == 2) ? 9 : 27;
+        constexpr float U = 5.9604645e-8f;     // 2^-24
         const int nc = d.s.cell[i];
         const Pos pi = load_pos(d.s.xh, i);
         const double xi[3] = {pi.x, pi.y, pi.z};
+        const float fx = (float)(pi.x - d.p.xmin), fy = (float)(pi.y - d.p.ymin);
+        const float fz = (ND == 3) ? (float)(pi.z - d.p.zmin) : 0.f, fh = (float)pi.h;
+        float Fi = fmaxf(fabsf(fx), fabsf(fy));
+        if (ND == 3) Fi = fmaxf(Fi, fabsf(fz));
+        const bool fast = fh > 64.f * U * Fi;
+        const float ce = 2.2f * U * Fi, ct = 32.f * U;
+        const float4* xsf = reinterpret_cast<const float4*>(d.s.xsf);
         for (int nj = 0; nj < nst; nj++) {
             const int nl = cell_link(d.p, nc, nj);
             if (nl <= 0) continue;
             const int start = d.s.cstart[nl], end = d.s.cend[nl];
             for (int q = start; q <= end; q++) {
-                const Pos pj = load_pos(d.s.xs, q);
-                const double xj[3] = {pj.x, pj.y, pj.z};
-                double d2 = 0.0;
-                for (int k = 0; k < nd; k++) d2 = d2 + (xi[k] - xj[k]) * (xi[k] - xj[k]);
-                const double ra = (pi.h + pj.h) / 2;
-                const double T = 2 * ra, T2 = T * T;
-                bool in;
-                if (d2 < T2 * (1.0 - 1.0e-10)) in = true;
-                else if (d2 > T2 * (1.0 + 1.0e-10)) in = false;
-                else in = (sqrt(d2) <= T);
+                bool in = false, decided = false;
+                if (fast) {
+                    const float4 fj = xsf[q];
+                    float t = fx - fj.x;
+                    float d2f = t * t;
+                    t = fy - fj.y;
+                    d2f = d2f + t * t;
+                    if (ND == 3) {
+                        t = fz - fj.z;
+                        d2f = d2f + t * t;
+                    }
+                    const float Tf = fh + fj.w, T2f = Tf * Tf;
+                    if (d2f > 4.f * T2f) {
+                        decided = true;
+                    } else {
+                        const float e = ce + 4.4f * U * Tf;
+                        const float M = nd * e * (4.f * Tf + e) + ct * T2f;
+                        if (d2f < T2f - M) in = decided = true;
+                        else if (d2f > T2f + M) decided = true;
+                    }
+                }
+                if (!decided) {
+                    const Pos pj = load_pos(d.s.xs, q);
+                    const double xj[3] = {pj.x, pj.y, pj.z};
+                    double d2 = 0.0;
+                    for (int k = 0; k < nd; k++) d2 = d2 + (xi[k] - xj[k]) * (xi[k] - xj[k]);
+                    const double ra = (pi.h + pj.h) / 2;
+                    const double T = 2 * ra, T2 = T * T;
+                    if (d2 < T2 * (1.0 - 1.0e-10)) in = true;
+                    else if (d2 > T2 * (1.0 + 1.0e-10)) in = false;
+                    else in = (sqrt(d2) <= T);
+                }
                 if (in) {
                     const int j = d.s.pid_sorted[q];
                     if (i != j) {
@@ -186,9 +256,36 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_nnps(Dev d)
     d.s.nnb[i] = cnt;
 }
 
+// The pair records of every list slot, as partisearching stores wij with the
+// list (CPP_3-NNPS.cpp:339-345): weight() / weight2() of the pair in FP64, or
+// in FP32 from the FP64 position differences in the bulk form.  One thread per
+// particle walks its list, so for each slot a warp writes consecutive records.
+template <int ND, typename R>
+__device__ __forceinline__ void pairw_particle(const Dev& d, int i)
+{
+    const int N = d.p.N, nn = nbr_count(d, i);
+    const PairI<R> I = pair_i<ND, R>(d, i);
+    for (int s = 0; s < nn; s++) {
+        const int j = d.s.nbr[(size_t)s * N + i];
+        R w[4];
+        pair_w_raw<ND, R>(d, I, load_pos(d.s.xh, j), w);
+        store_w(d, s, i, w);
+    }
+}
+
+template <int ND>
+__global__ void __launch_bounds__(128, SPH_MINB) k_pairw(Dev d)
+{
+    const int i = IDX;
+    if (i >= d.p.N || *d.s.err) return;
+    if (d.p.bulk) pairw_particle<ND, float>(d, i);
+    else pairw_particle<ND, double>(d, i);
+}
+#endif  // !SPH_BULK32
+
 // ---------------------------------------------------------------------------
 // density(): fluid porosity (:25-54) and continuity (:57-165) -> rho_c
-template <int ND, int KGC>
+template <int ND>
 __global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
 {
     const int i = IDX, N = d.p.N;
@@ -196,20 +293,23 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
     constexpr int nd = ND;
     const int ti = d.s.type[i], nn = nbr_count(d, i);
     const int l = *d.s.step;
-    const PairI I = pair_i<ND, KGC>(d, i);
+    const Pos P = load_pos(d.s.xh, i);
+    const double xi[3] = {P.x, P.y, P.z};
     double por = d.s.porosity[i];
     double pcop = d.s.poro_cop[i];
     if (ti == 1) {
-        double up = 0.0, down = 0.0;
+        Sum<real> sup, sdown;
         for (int s = 0; s < nn; s++) {
             const int j = d.s.nbr[(size_t)s * N + i];
             if (d.s.type[j] == 2) {
-                double w[4];
-                pair_w<ND, KGC>(d, I, load_pos(d.s.xh, j), w);
-                up = up + d.s.mass[j] * d.s.porosity[j] / d.s.rho[j] * w[3];
-                down = down + d.s.mass[j] / d.s.rho[j] * w[3];
+                real w[4];
+                load_w(d, s, i, w);
+                const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
+                sup.add(mj * (real)d.s.porosity[j] / rj * w[3]);
+                sdown.add(mj / rj * w[3]);
             }
         }
+        const double up = sup.v(), down = sdown.v();
         if (fabs(down) > 1.0e-7) {
             pcop = por;
             por = up / down;
@@ -222,7 +322,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
     }
     double rnew = d.s.rho[i];
     if (ti != 7) {
-        double up[3] = {0.0, 0.0, 0.0}, down[3] = {0.0, 0.0, 0.0};
+        Sum<real> sup[3], sdown[3];
         double vi[3];
         for (int k = 0; k < 3; k++) vi[k] = d.s.vxp[k * N + i];
         const bool solid = (ti == 2 || ti == 4), fluid = (ti == 1 || ti == 3);
@@ -239,21 +339,23 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
             } else {
                 continue;
             }
-            const Pos pj = load_pos(d.s.xh, j);
-            const double xj[3] = {pj.x, pj.y, pj.z};
-            double w[4];
-            pair_w<ND, KGC>(d, I, pj, w);
-            const double mj = d.s.mass[j];
+            real w[4];
+            load_w(d, s, i, w);
+            const real mj = (real)d.s.mass[j];
             if (solid) {
+                const Pos pj = load_pos(d.s.xh, j);
+                const double xj[3] = {pj.x, pj.y, pj.z};
                 for (int k = 0; k < nd; k++) {
-                    up[k] = up[k] + mj * (vi[k] - vxj[k]) * w[k];
-                    down[k] = down[k] + mj * (I.x[k] - xj[k]) * w[k];
+                    sup[k].add(mj * (real)(vi[k] - vxj[k]) * w[k]);
+                    sdown[k].add(mj * (real)(xi[k] - xj[k]) * w[k]);
                 }
             }
             if (fluid) {
-                for (int k = 0; k < nd; k++) up[k] = up[k] + mj * (vi[k] - vxj[k]) * w[k];
+                for (int k = 0; k < nd; k++) sup[k].add(mj * (real)(vi[k] - vxj[k]) * w[k]);
             }
         }
+        double up[3], down[3];
+        for (int k = 0; k < 3; k++) { up[k] = sup[k].v(); down[k] = sdown[k].v(); }
         double drhot = 0.0;
         if (solid) {
             for (int k = 0; k < nd; k++) {
@@ -274,23 +376,24 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
 
 // Shepard filter (:168-188) reading every neighbour's continuity density
 // (Jacobi order), then the local equation of state (CPP_7-1-eos_CR.cpp:22-43).
-template <int ND, int KGC>
+template <int ND>
 __global__ void __launch_bounds__(128, SPH_MINB) k_shepard_eos(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
     const int ti = d.s.type[i], nn = nbr_count(d, i);
-    const PairI I = pair_i<ND, KGC>(d, i);
-    double up = 0.0, down = 0.0;
+    Sum<real> sup, sdown;
     for (int s = 0; s < nn; s++) {
         const int j = d.s.nbr[(size_t)s * N + i];
         if (d.s.type[j] == ti) {
-            double w[4];
-            pair_w<ND, KGC>(d, I, load_pos(d.s.xh, j), w);
-            up = up + d.s.mass[j] * w[3];
-            down = down + d.s.mass[j] / d.s.rho_c[j] * w[3];
+            real w[4];
+            load_w(d, s, i, w);
+            const real mj = (real)d.s.mass[j];
+            sup.add(mj * w[3]);
+            sdown.add(mj / (real)d.s.rho_c[j] * w[3]);
         }
     }
+    const double up = sup.v(), down = sdown.v();
     double r = d.s.rho_c[i];
     if (ti != 7 && fabs(down) > 1.0e-7) r = up / down;
     d.s.rho[i] = r;
@@ -315,22 +418,22 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_shepard_eos(Dev d)
 // neighbour list, each sum in list order.  Writes de, we, color, prew, prea,
 // and the walls' gathered stress into sig_next (reads the soil stresses of
 // the previous step from sig).
-template <int ND, int KGC>
+template <int ND>
 __global__ void __launch_bounds__(128, SPH_MINB) k_strain(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
     constexpr int nd = ND;
     const int ti = d.s.type[i], nn = nbr_count(d, i);
-    const PairI I = pair_i<ND, KGC>(d, i);
+    const Pos P = load_pos(d.s.xh, i);
     double vi[3];
     for (int k = 0; k < 3; k++) vi[k] = d.s.vxp[k * N + i];
     const bool solid = (ti == 2 || ti == 4);
     const bool moving = (ti >= 1 && ti <= 4);
-    double up[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, down[3] = {0, 0, 0};
-    double u1 = 0, u2 = 0, u3 = 0, u4 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0;
-    double us[6] = {0, 0, 0, 0, 0, 0}, dsw = 0;
-    double color = 0.0;
+    Sum<real> sup[9], sdown[3];
+    Sum<real> su1, su2, su3, su4, sd1, sd2, sd3, sd4;
+    Sum<real> sus[6], sdsw;
+    Sum<real> scolor;
     for (int q = 0; q < nn; q++) {
         const int j = d.s.nbr[(size_t)q * N + i];
         const int tj = d.s.type[j];
@@ -338,46 +441,54 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_strain(Dev d)
         const bool wallj = (moving && tj == 0);
         const bool gath = (ti != tj) && ((ti == 2 || ti == 4 || ti == 0) && (tj == 1 || tj == 3 || (ti == 0 && tj == 2)));
         if (!(same || wallj || gath)) continue;
-        const Pos pj = load_pos(d.s.xh, j);
-        double w[4];
-        pair_w<ND, KGC>(d, I, pj, w);
-        const double mj = d.s.mass[j], rj = d.s.rho[j];
+        real w[4];
+        load_w(d, q, i, w);
+        const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
         if (same || wallj) {
-            double dvx[3];
+            real dvx[3];
             for (int k = 0; k < 3; k++) {
                 double vj = same ? d.s.vxp[k * N + j] : ((d.p.flbndy == 1) ? vi[k] : 0.0);
-                dvx[k] = vi[k] - vj;
+                dvx[k] = (real)(vi[k] - vj);
             }
-            up[0] = up[0] + mj / rj * dvx[0] * w[0];
-            up[1] = up[1] + mj / rj * dvx[0] * w[1];
-            up[2] = up[2] + mj / rj * dvx[0] * w[2];
-            up[3] = up[3] + mj / rj * dvx[1] * w[0];
-            up[4] = up[4] + mj / rj * dvx[1] * w[1];
-            up[5] = up[5] + mj / rj * dvx[1] * w[2];
-            up[6] = up[6] + mj / rj * dvx[2] * w[0];
-            up[7] = up[7] + mj / rj * dvx[2] * w[1];
-            up[8] = up[8] + mj / rj * dvx[2] * w[2];
+            sup[0].add(mj / rj * dvx[0] * w[0]);
+            sup[1].add(mj / rj * dvx[0] * w[1]);
+            sup[2].add(mj / rj * dvx[0] * w[2]);
+            sup[3].add(mj / rj * dvx[1] * w[0]);
+            sup[4].add(mj / rj * dvx[1] * w[1]);
+            sup[5].add(mj / rj * dvx[1] * w[2]);
+            sup[6].add(mj / rj * dvx[2] * w[0]);
+            sup[7].add(mj / rj * dvx[2] * w[1]);
+            sup[8].add(mj / rj * dvx[2] * w[2]);
             if (solid) {
-                down[0] = down[0] + mj / rj * (I.x[0] - pj.x) * w[0];
-                down[1] = down[1] + mj / rj * (I.x[1] - pj.y) * w[1];
-                down[2] = down[2] + mj / rj * (I.x[2] - pj.z) * w[2];
+                const Pos pj = load_pos(d.s.xh, j);
+                sdown[0].add(mj / rj * (real)(P.x - pj.x) * w[0]);
+                sdown[1].add(mj / rj * (real)(P.y - pj.y) * w[1]);
+                sdown[2].add(mj / rj * (real)(P.z - pj.z) * w[2]);
             }
-            color = color + mj / rj * 1.0 * w[3];
+            scolor.add(mj / rj * real(1.0) * w[3]);
         }
         if (gath) {
-            const double w3 = w[3];
-            if (ti == 2 && tj == 1) { u1 = u1 + mj * d.s.pre[j] * w3 / rj; d1 = d1 + mj * w3 / rj; }
-            if (ti == 2 && tj == 3) { u2 = u2 + mj * d.s.pre[j] * w3 / rj; d2 = d2 + mj * w3 / rj; }
-            if (ti == 4 && tj == 1) { u3 = u3 + mj * d.s.pre[j] * w3 / rj; d3 = d3 + mj * w3 / rj; }
-            if (ti == 4 && tj == 3) { u4 = u4 + mj * d.s.pre[j] * w3 / rj; d4 = d4 + mj * w3 / rj; }
-            if (ti == 0 && tj == 1) { u1 = u1 + mj * d.s.pre[j] * w3 / rj; d1 = d1 + mj * w3 / rj; }
-            if (ti == 0 && tj == 3) { u2 = u2 + mj * d.s.pre[j] * w3 / rj; d2 = d2 + mj * w3 / rj; }
+            const real w3 = w[3];
+            const real pj_ = (ti == 0 && tj == 2) ? real(0) : (real)d.s.pre[j];
+            if (ti == 2 && tj == 1) { su1.add(mj * pj_ * w3 / rj); sd1.add(mj * w3 / rj); }
+            if (ti == 2 && tj == 3) { su2.add(mj * pj_ * w3 / rj); sd2.add(mj * w3 / rj); }
+            if (ti == 4 && tj == 1) { su3.add(mj * pj_ * w3 / rj); sd3.add(mj * w3 / rj); }
+            if (ti == 4 && tj == 3) { su4.add(mj * pj_ * w3 / rj); sd4.add(mj * w3 / rj); }
+            if (ti == 0 && tj == 1) { su1.add(mj * pj_ * w3 / rj); sd1.add(mj * w3 / rj); }
+            if (ti == 0 && tj == 3) { su2.add(mj * pj_ * w3 / rj); sd2.add(mj * w3 / rj); }
             if (ti == 0 && tj == 2) {
-                for (int k = 0; k < 6; k++) us[k] = us[k] + mj * d.s.sig[k * N + j] * w3 / rj;
-                dsw = dsw + mj * w3 / rj;
+                for (int k = 0; k < 6; k++) sus[k].add(mj * (real)d.s.sig[k * N + j] * w3 / rj);
+                sdsw.add(mj * w3 / rj);
             }
         }
     }
+    double up[9], down[3], us[6];
+    for (int k = 0; k < 9; k++) up[k] = sup[k].v();
+    for (int k = 0; k < 3; k++) down[k] = sdown[k].v();
+    for (int k = 0; k < 6; k++) us[k] = sus[k].v();
+    const double u1 = su1.v(), u2 = su2.v(), u3 = su3.v(), u4 = su4.v();
+    const double d1 = sd1.v(), d2 = sd2.v(), d3 = sd3.v(), d4 = sd4.v();
+    const double dsw = sdsw.v(), color = scolor.v();
     // velocity gradient (:148-181), strain rate and spin (:183-218)
     double dv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     if (ti == 1 || ti == 3) {
@@ -669,7 +780,7 @@ __global__ void __launch_bounds__(128) k_art_rij(Dev d)
 // stress-divergence sums, whose per-pair stress / rho^2 halves were evaluated
 // once per particle by k_stress.  Writes ax = g + sums for particle types 1-4;
 // k_accel_b continues from this value in the reference's order.
-template <int ND, int KGC>
+template <int ND>
 __global__ void __launch_bounds__(128, SPH_MINB) k_accel_a(Dev d)
 {
     const int i = IDX, N = d.p.N;
@@ -679,13 +790,12 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_a(Dev d)
     const bool solid = (ti == 2 || ti == 4);
     if (!fluid && !solid) return;
     const int nn = nbr_count(d, i);
-    const PairI I = pair_i<ND, KGC>(d, i);
     const double ri = d.s.rho[i];
     const int other = (ti == 1) ? 3 : 1;
     const bool minor = (ti == 1) ? d.p.water_minor : d.p.air_minor;
-    double sri[6];
-    for (int k = 0; k < 6; k++) sri[k] = d.s.sr[k * N + i];
-    double tf[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    real sri[6];
+    for (int k = 0; k < 6; k++) sri[k] = (real)d.s.sr[k * N + i];
+    Sum<real> tf[3][3];
     const double satu_i = d.s.satu[i];
     const double prew_i = solid ? d.s.prew[i] : 0.0, prea_i = solid ? d.s.prea[i] : 0.0;
     const double poro_f = fluid ? d.s.f_por[i] : 0.0;
@@ -702,36 +812,36 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_a(Dev d)
         const bool f_pair = fluid && (tj == ti || tj == other);
         const bool s_pair = solid && tj == ti;
         if (!(f_pair || s_pair)) continue;
-        double w[4];
-        pair_w<ND, KGC>(d, I, load_pos(d.s.xh, j), w);
-        const double mj = d.s.mass[j];
-        double srj[6];
+        real w[4];
+        load_w(d, q, i, w);
+        const real mj = (real)d.s.mass[j];
+        real srj[6];
         if (s_pair || same_bits(d.s.f_por[j], poro_f)) {
-            for (int k = 0; k < 6; k++) srj[k] = d.s.sr[k * N + j];
+            for (int k = 0; k < 6; k++) srj[k] = (real)d.s.sr[k * N + j];
         } else {
             const double rj = d.s.rho[j];
-            for (int k = 0; k < 6; k++) srj[k] = poro_f * d.s.sig_next[k * N + j] / rj / rj;
+            for (int k = 0; k < 6; k++) srj[k] = (real)(poro_f * d.s.sig_next[k * N + j] / rj / rj);
         }
         if (f_pair && minor) {
-            tf[0][0] = tf[0][0] + mj * (srj[0] - sri[0]) * w[0];
-            tf[0][1] = tf[0][1] + mj * (srj[3] - sri[3]) * w[1];
-            tf[0][2] = tf[0][2] + mj * (srj[5] - sri[5]) * w[2];
-            tf[1][0] = tf[1][0] + mj * (srj[3] - sri[3]) * w[0];
-            tf[1][1] = tf[1][1] + mj * (srj[1] - sri[1]) * w[1];
-            tf[1][2] = tf[1][2] + mj * (srj[4] - sri[4]) * w[2];
-            tf[2][0] = tf[2][0] + mj * (srj[5] - sri[5]) * w[0];
-            tf[2][1] = tf[2][1] + mj * (srj[4] - sri[4]) * w[1];
-            tf[2][2] = tf[2][2] + mj * (srj[2] - sri[2]) * w[2];
+            tf[0][0].add(mj * (srj[0] - sri[0]) * w[0]);
+            tf[0][1].add(mj * (srj[3] - sri[3]) * w[1]);
+            tf[0][2].add(mj * (srj[5] - sri[5]) * w[2]);
+            tf[1][0].add(mj * (srj[3] - sri[3]) * w[0]);
+            tf[1][1].add(mj * (srj[1] - sri[1]) * w[1]);
+            tf[1][2].add(mj * (srj[4] - sri[4]) * w[2]);
+            tf[2][0].add(mj * (srj[5] - sri[5]) * w[0]);
+            tf[2][1].add(mj * (srj[4] - sri[4]) * w[1]);
+            tf[2][2].add(mj * (srj[2] - sri[2]) * w[2]);
         } else {
-            tf[0][0] = tf[0][0] + mj * (srj[0] + sri[0]) * w[0];
-            tf[0][1] = tf[0][1] + mj * (srj[3] + sri[3]) * w[1];
-            tf[0][2] = tf[0][2] + mj * (srj[5] + sri[5]) * w[2];
-            tf[1][0] = tf[1][0] + mj * (srj[3] + sri[3]) * w[0];
-            tf[1][1] = tf[1][1] + mj * (srj[1] + sri[1]) * w[1];
-            tf[1][2] = tf[1][2] + mj * (srj[4] + sri[4]) * w[2];
-            tf[2][0] = tf[2][0] + mj * (srj[5] + sri[5]) * w[0];
-            tf[2][1] = tf[2][1] + mj * (srj[4] + sri[4]) * w[1];
-            tf[2][2] = tf[2][2] + mj * (srj[2] + sri[2]) * w[2];
+            tf[0][0].add(mj * (srj[0] + sri[0]) * w[0]);
+            tf[0][1].add(mj * (srj[3] + sri[3]) * w[1]);
+            tf[0][2].add(mj * (srj[5] + sri[5]) * w[2]);
+            tf[1][0].add(mj * (srj[3] + sri[3]) * w[0]);
+            tf[1][1].add(mj * (srj[1] + sri[1]) * w[1]);
+            tf[1][2].add(mj * (srj[4] + sri[4]) * w[2]);
+            tf[2][0].add(mj * (srj[5] + sri[5]) * w[0]);
+            tf[2][1].add(mj * (srj[4] + sri[4]) * w[1]);
+            tf[2][2].add(mj * (srj[2] + sri[2]) * w[2]);
         }
         if (s_pair) {
             const double satu = d.s.satu[j];
@@ -745,25 +855,27 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_a(Dev d)
                 }
                 pi_ = same_bits(satu, satu_i) ? pi_own
                     : (1 - poro_s) * (-satu * prew_i + (1 - satu) * prea_i) / dens_s / dens_s;
-                tf[0][0] = tf[0][0] + mj * (pj_ + pi_) * w[0];
-                tf[1][1] = tf[1][1] + mj * (pj_ + pi_) * w[1];
-                tf[2][2] = tf[2][2] + mj * (pj_ + pi_) * w[2];
+                const real pq = (real)(pj_ + pi_);
+                tf[0][0].add(mj * pq * w[0]);
+                tf[1][1].add(mj * pq * w[1]);
+                tf[2][2].add(mj * pq * w[2]);
             } else {
                 const double pj_ = d.s.pp[j];
                 const double pi_ = same_bits(satu, satu_i) ? pi_own
                     : (-satu * prew_i + (1 - satu) * prea_i) / ri / ri;
-                tf[0][0] = tf[0][0] + mj * (pj_ - pi_) * w[0];
-                tf[1][1] = tf[1][1] + mj * (pj_ - pi_) * w[1];
-                tf[2][2] = tf[2][2] + mj * (pj_ - pi_) * w[2];
+                const real pq = (real)(pj_ - pi_);
+                tf[0][0].add(mj * pq * w[0]);
+                tf[1][1].add(mj * pq * w[1]);
+                tf[2][2].add(mj * pq * w[2]);
             }
         }
     }
     const double g[3] = {d.p.gx, d.p.gy, d.p.gz};
     double ax[3];
     for (int k = 0; k < 3; k++) ax[k] = g[k];
-    ax[0] += tf[0][0] + tf[0][1] + tf[0][2];
-    ax[1] += tf[1][0] + tf[1][1] + tf[1][2];
-    ax[2] += tf[2][0] + tf[2][1] + tf[2][2];
+    ax[0] += tf[0][0].v() + tf[0][1].v() + tf[0][2].v();
+    ax[1] += tf[1][0].v() + tf[1][1].v() + tf[1][2].v();
+    ax[2] += tf[2][0].v() + tf[2][1].v() + tf[2][2].v();
     for (int k = 0; k < 3; k++) d.s.ax[k * N + i] = ax[k];
 }
 
@@ -805,46 +917,51 @@ __device__ __noinline__ double drag_beta(int form, double por, double ds, double
 // stress-divergence result of k_accel_a in the reference's call order.
 // Writes ax, interf, interfss and the updated velocity into vx_next (the
 // reference's vx before XSPH).
-template <int ND, int KGC, int ART = 0>
+template <int ND, int ART = 0>
 __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
     constexpr int nd = ND;
     const int ti = d.s.type[i], nn = nbr_count(d, i);
-    const PairI I = pair_i<ND, KGC>(d, i);
+    const PairI<real> I = pair_i<ND, real>(d, i);
     const double ri = d.s.rho[i];
+    const real riR = (real)ri;
     double vi[3];
     for (int k = 0; k < 3; k++) vi[k] = d.s.vxp[k * N + i];
     const bool fluid = (ti == 1 || ti == 3);
     const bool solid = (ti == 2 || ti == 4);
     const bool moving = (ti >= 1 && ti <= 4);
-    double tb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};   // wall stress
-    double tav[3] = {0, 0, 0}, tin[3] = {0, 0, 0}, tdm[3] = {0, 0, 0}, tu[3] = {0, 0, 0};
+    Sum<real> tb[3][3];   // wall stress
+    Sum<real> tav[3], tin[3], tdm[3], tu[3];
     const bool damping = (*d.s.step <= d.p.inip) && solid;
     const bool art = ART && ti == 2;   // artificial stress (art_stre_coe > 0)
-    const double cdi = damping ? d.s.cd[i] : 0.0;
+    const real cdi = damping ? (real)d.s.cd[i] : real(0);
     // artificial viscosity coefficients of particle i
-    double ca = 0.0, aa = 0.0, bb = 0.0;
-    if (ti == 1) { ca = d.s.f_vpu[i]; aa = d.p.av[0][0]; bb = d.p.av[0][1]; }
-    if (ti == 2) { ca = d.s.s_vpu[i]; aa = d.p.av[1][0]; bb = d.p.av[1][1]; }
-    if (ti == 3) { ca = d.s.f_vpu[i]; aa = d.p.av[2][0]; bb = d.p.av[2][1]; }
+    real ca = 0, aa = 0, bb = 0;
+    if (ti == 1) { ca = (real)d.s.f_vpu[i]; aa = (real)d.p.av[0][0]; bb = (real)d.p.av[0][1]; }
+    if (ti == 2) { ca = (real)d.s.s_vpu[i]; aa = (real)d.p.av[1][0]; bb = (real)d.p.av[1][1]; }
+    if (ti == 3) { ca = (real)d.s.f_vpu[i]; aa = (real)d.p.av[2][0]; bb = (real)d.p.av[2][1]; }
     // wall-stress operand of particle i (:668-700) and its own half
-    double ab[6] = {0, 0, 0, 0, 0, 0}, abr[6] = {0, 0, 0, 0, 0, 0};
+    real ab[6] = {0, 0, 0, 0, 0, 0}, abr[6] = {0, 0, 0, 0, 0, 0};
     const double satu_i = d.s.satu[i];
     if (moving) {
         double si[6];
         for (int k = 0; k < 6; k++) si[k] = d.s.sig_next[k * N + i];
+        double abd[6];
         if (fluid) {
-            for (int k = 0; k < 6; k++) ab[k] = si[k];
+            for (int k = 0; k < 6; k++) abd[k] = si[k];
         } else {
             const double prew_i = d.s.prew[i], prea_i = d.s.prea[i];
-            ab[0] = si[0] - satu_i * prew_i + (1 - satu_i) * prea_i;
-            ab[1] = si[1] - satu_i * prew_i + (1 - satu_i) * prea_i;
-            ab[2] = si[2] - satu_i * prew_i + (1 - satu_i) * prea_i;
-            ab[3] = si[3]; ab[4] = si[4]; ab[5] = si[5];
+            abd[0] = si[0] - satu_i * prew_i + (1 - satu_i) * prea_i;
+            abd[1] = si[1] - satu_i * prew_i + (1 - satu_i) * prea_i;
+            abd[2] = si[2] - satu_i * prew_i + (1 - satu_i) * prea_i;
+            abd[3] = si[3]; abd[4] = si[4]; abd[5] = si[5];
         }
-        for (int k = 0; k < 6; k++) abr[k] = ab[k] / ri / ri;
+        for (int k = 0; k < 6; k++) {
+            ab[k] = (real)abd[k];
+            abr[k] = (real)(abd[k] / ri / ri);
+        }
     }
     for (int q = 0; q < nn; q++) {
         const int j = d.s.nbr[(size_t)q * N + i];
@@ -856,100 +973,107 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
         const bool as_pair = art && tj == 2;
         if (!(av_pair || b_pair || in_pair || dm_pair)) continue;
         const Pos pj = load_pos(d.s.xh, j);
-        double w[4];
-        pair_w<ND, KGC>(d, I, pj, w);
-        const double mj = d.s.mass[j], rj = d.s.rho[j];
+        real w[4];
+        load_w(d, q, i, w);
+        const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
         const double xj[3] = {pj.x, pj.y, pj.z};
         if (av_pair) {
-            double inprod = 0.0, dst = 0.0, dx[3];
+            real inprod = 0, dst = 0, dx[3];
             for (int k = 0; k < nd; k++) {
-                double dvx = vi[k] - d.s.vxp[k * N + j];
-                dx[k] = I.x[k] - xj[k];
+                const real dvx = (real)(vi[k] - d.s.vxp[k * N + j]);
+                dx[k] = (real)(I.x[k] - xj[k]);
                 dst = dst + dx[k] * dx[k];
                 inprod = inprod + dvx * dx[k];
             }
-            const double hl = (pj.h + I.h) * 0.5;
-            const double rou = (rj + ri) * 0.5;
-            double paix;
-            if (inprod < 0.0) {
+            const real hl = ((real)pj.h + I.h) * real(0.5);
+            const real rou = (rj + riR) * real(0.5);
+            real paix;
+            if (inprod < real(0)) {
                 dst = sqrt(dst);
-                double myu = hl * inprod / (dst * dst + 0.01 * hl * hl);
+                real myu = hl * inprod / (dst * dst + real(0.01) * hl * hl);
                 paix = (-aa * ca * myu + bb * myu * myu) / rou;
             } else
-                paix = 0.0;
-            for (int k = 0; k < nd; k++) tav[k] = tav[k] + mj * paix * w[k];
+                paix = 0;
+            for (int k = 0; k < nd; k++) tav[k].add(mj * paix * w[k]);
         }
         if (b_pair) {
-            double abj[6];
+            real abj[6];
             for (int k = 0; k < 6; k++) abj[k] = ab[k] / rj / rj;
-            tb[0][0] = tb[0][0] + mj * (abj[0] + abr[0]) * w[0];
-            tb[0][1] = tb[0][1] + mj * (abj[3] + abr[3]) * w[1];
-            tb[0][2] = tb[0][2] + mj * (abj[5] + abr[5]) * w[2];
-            tb[1][0] = tb[1][0] + mj * (abj[3] + abr[3]) * w[0];
-            tb[1][1] = tb[1][1] + mj * (abj[1] + abr[1]) * w[1];
-            tb[1][2] = tb[1][2] + mj * (abj[4] + abr[4]) * w[2];
-            tb[2][0] = tb[2][0] + mj * (abj[5] + abr[5]) * w[0];
-            tb[2][1] = tb[2][1] + mj * (abj[4] + abr[4]) * w[1];
-            tb[2][2] = tb[2][2] + mj * (abj[2] + abr[2]) * w[2];
+            tb[0][0].add(mj * (abj[0] + abr[0]) * w[0]);
+            tb[0][1].add(mj * (abj[3] + abr[3]) * w[1]);
+            tb[0][2].add(mj * (abj[5] + abr[5]) * w[2]);
+            tb[1][0].add(mj * (abj[3] + abr[3]) * w[0]);
+            tb[1][1].add(mj * (abj[1] + abr[1]) * w[1]);
+            tb[1][2].add(mj * (abj[4] + abr[4]) * w[2]);
+            tb[2][0].add(mj * (abj[5] + abr[5]) * w[0]);
+            tb[2][1].add(mj * (abj[4] + abr[4]) * w[1]);
+            tb[2][2].add(mj * (abj[2] + abr[2]) * w[2]);
         }
         if (in_pair) {
-            double inprod = 0.0, dvx[3];
+            real inprod = 0, dvx[3];
             for (int k = 0; k < nd; k++) {
-                double dxk = I.x[k] - xj[k];
-                dvx[k] = vi[k] - d.s.vxp[k * N + j];
+                const real dxk = (real)(I.x[k] - xj[k]);
+                dvx[k] = (real)(vi[k] - d.s.vxp[k * N + j]);
                 inprod = inprod + dxk * dvx[k];
             }
             if (inprod < 0) {
-                const double w3 = w[3], ga = d.p.g_acc;
+                const real w3 = w[3], ga = (real)d.p.g_acc;
                 if (d.p.fli > 1 && ((ti == 2 && tj == 1) || (ti == 1 && tj == 2))) {
                     // interact2/3 soil-water drag, m_j / rho_j W beta (v_i - v_j)
                     double mv = 0.0;
-                    for (int k = 0; k < nd; k++) mv = mv + dvx[k] * dvx[k];
+                    for (int k = 0; k < nd; k++) mv = mv + (double)dvx[k] * (double)dvx[k];
                     mv = sqrt(mv);
                     const int so = (ti == 2) ? i : j, wa = (ti == 2) ? j : i;
-                    const double beta = drag_beta(d.p.fli, d.s.porosity[so], d.s.s_ds[so], d.s.f_dens[wa],
-                                                  d.s.f_vis[wa], mv, (ti == 2) ? rj : ri);
-                    for (int k = 0; k < nd; k++) tin[k] = tin[k] + mj / rj * w3 * beta * dvx[k];
+                    const real beta = (real)drag_beta(d.p.fli, d.s.porosity[so], d.s.s_ds[so], d.s.f_dens[wa],
+                                                      d.s.f_vis[wa], mv, (ti == 2) ? d.s.rho[j] : ri);
+                    for (int k = 0; k < nd; k++) tin[k].add(mj / rj * w3 * beta * dvx[k]);
                 } else if (ti == 2 && tj == 1) {
-                    const double sa = satu_i, po = d.s.porosity[i], cp = d.s.cop[i], fd = d.s.f_dens[j];
+                    const real sa = (real)satu_i, po = (real)d.s.porosity[i], cp = (real)d.s.cop[i],
+                               fd = (real)d.s.f_dens[j];
                     for (int k = 0; k < nd; k++)
-                        tin[k] = tin[k] + sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3;
+                        tin[k].add(sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3);
                 } else if (ti == 1 && tj == 2) {
-                    const double sa = d.s.satu[j], po = d.s.porosity[j], cp = d.s.cop[j], fd = d.s.f_dens[i];
+                    const real sa = (real)d.s.satu[j], po = (real)d.s.porosity[j], cp = (real)d.s.cop[j],
+                               fd = (real)d.s.f_dens[i];
                     for (int k = 0; k < nd; k++)
-                        tin[k] = tin[k] + sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3;
+                        tin[k].add(sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3);
                 } else if (ti == 2 && tj == 3) {
-                    const double sa = satu_i, po = d.s.porosity[i], fd = d.s.f_dens[j];
+                    const real sa = (real)satu_i, po = (real)d.s.porosity[i], fd = (real)d.s.f_dens[j];
                     for (int k = 0; k < nd; k++)
-                        tin[k] = tin[k] + (1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3;
+                        tin[k].add((1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3);
                 } else if (ti == 3 && tj == 2) {
-                    const double sa = d.s.satu[j], po = d.s.porosity[j], fd = d.s.f_dens[i];
+                    const real sa = (real)d.s.satu[j], po = (real)d.s.porosity[j], fd = (real)d.s.f_dens[i];
                     for (int k = 0; k < nd; k++)
-                        tin[k] = tin[k] + (1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3;
+                        tin[k].add((1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3);
                 }
             }
         }
         if (dm_pair)
             for (int k = 0; k < nd; k++)
-                tdm[k] = tdm[k] + mj / rj * cdi * (vi[k] - d.s.vxp[k * N + j]) * w[3];
+                tdm[k].add(mj / rj * cdi * (real)(vi[k] - d.s.vxp[k * N + j]) * w[3]);
         if (as_pair) {
             // artificial_stress_2d/_3d pair sum (CPP_9-5-artificialstress.cpp:
             // 100-140, 248-290): f_ij = (W(q) / W(dr))^2.55 of the cubic
             // spline, m_j f_ij (R_i + R_j) grad W_ij
-            double dst = 0.0;
-            for (int k = 0; k < 3; k++) dst = dst + (I.x[k] - xj[k]) * (I.x[k] - xj[k]);
+            real dst = 0;
+            for (int k = 0; k < 3; k++) {
+                const real t = (real)(I.x[k] - xj[k]);
+                dst = dst + t * t;
+            }
             dst = sqrt(dst);
-            const double hl = (I.h + pj.h) * 0.5;
-            const double qd = dst / hl;
-            double f;
-            if (qd >= 0.0 && qd < 1.0) f = pow((0.666666666666667 - qd * qd + 0.5 * qd * qd * qd) * 3.82300884955752, 2.55);
-            else if (qd >= 1.0 && qd < 2.0) f = pow((2.0 - qd) * (2.0 - qd) * (2.0 - qd) * 0.629737609329447, 2.55);
-            else f = 0.0;
+            const real hl = (I.h + (real)pj.h) * real(0.5);
+            const real qd = dst / hl;
+            real f;
+            if (qd >= real(0) && qd < real(1))
+                f = pow((real(0.666666666666667) - qd * qd + real(0.5) * qd * qd * qd) * real(3.82300884955752), real(2.55));
+            else if (qd >= real(1) && qd < real(2))
+                f = pow((real(2.0) - qd) * (real(2.0) - qd) * (real(2.0) - qd) * real(0.629737609329447), real(2.55));
+            else f = 0;
             for (int a = 0; a < nd; a++) {
-                double acc = tu[a];
+                Sum<real> acc = tu[a];
                 for (int b = 0; b < nd; b++) {
                     const int c = a * 3 + b;
-                    acc = acc + mj * f * (d.s.rij[(size_t)c * N + i] + d.s.rij[(size_t)c * N + j]) * w[b];
+                    acc.add(mj * f * (real)(d.s.rij[(size_t)c * N + i] + d.s.rij[(size_t)c * N + j]) * w[b]);
                 }
                 tu[a] = acc;
             }
@@ -958,13 +1082,13 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
     double ax[3];
     for (int k = 0; k < 3; k++) ax[k] = d.s.ax[k * N + i];   // g + stress divergence (k_accel_a) or the old value
     if (ti != 7)
-        for (int k = 0; k < nd; k++) ax[k] = ax[k] - tav[k];
+        for (int k = 0; k < nd; k++) ax[k] = ax[k] - tav[k].v();
     if (art)
-        for (int k = 0; k < nd; k++) ax[k] = ax[k] + tu[k];
+        for (int k = 0; k < nd; k++) ax[k] = ax[k] + tu[k].v();
     if (moving) {
-        ax[0] += tb[0][0] + tb[0][1] + tb[0][2];
-        ax[1] += tb[1][0] + tb[1][1] + tb[1][2];
-        ax[2] += tb[2][0] + tb[2][1] + tb[2][2];
+        ax[0] += tb[0][0].v() + tb[0][1].v() + tb[0][2].v();
+        ax[1] += tb[1][0].v() + tb[1][1].v() + tb[1][2].v();
+        ax[2] += tb[2][0].v() + tb[2][1].v() + tb[2][2].v();
     }
     const double dt = d.p.dt;
     double axp[3];
@@ -972,7 +1096,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
     if (d.p.fli >= 1 && moving) {
         const double xishu = d.p.interc;
         for (int k = 0; k < nd; k++) {
-            double itf = tin[k];
+            double itf = tin[k].v();
             double vx1 = vi[k] + 0.5 * (axp[k] + ax[k]) * dt;
             double vx2 = vi[k] + 0.5 * (axp[k] + ax[k] - itf * xishu / ri) * dt;
             if (vx1 * vx2 <= 0.0) {
@@ -986,9 +1110,9 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
     if (damping) {
         for (int k = 0; k < nd; k++) {
             double vx1 = vi[k] + 0.5 * (axp[k] + ax[k]) * dt;
-            double vx2 = vi[k] + 0.5 * (axp[k] + ax[k] - tdm[k]) * dt;
+            double vx2 = vi[k] + 0.5 * (axp[k] + ax[k] - tdm[k].v()) * dt;
             if (vx1 * vx2 <= 0.0) ax[k] = -2.0 * vi[k] / dt - axp[k];
-            else ax[k] -= tdm[k];
+            else ax[k] -= tdm[k].v();
         }
     }
     // veocity_update, if_move 0 and 1
@@ -1036,7 +1160,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
 // before XSPH), tmboundary (CPP_13-boundary.cpp:125-177), check_domain
 // (CPP_13-boundary.cpp:20-68) and update (CPP_12-1-update.cpp:11-55).
 // Reads xh / vx_next, writes xh_next / vx.
-template <int ND, int KGC>
+template <int ND>
 __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
 {
     const int i = IDX, N = d.p.N;
@@ -1044,31 +1168,36 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
     constexpr int nd = ND;
     const int ti = d.s.type[i], nn = nbr_count(d, i);
     const double dt = d.p.dt;
-    const PairI I = pair_i<ND, KGC>(d, i);
+    const PairI<real> I = pair_i<ND, real>(d, i);
     double vm[3];
     for (int k = 0; k < 3; k++) vm[k] = d.s.vx_next[k * N + i];
     const bool moving = (ti >= 1 && ti <= 4);
     double vn[3] = {vm[0], vm[1], vm[2]};
     if (d.p.if_move != 2 && moving) {
-        double tu[3] = {0, 0, 0}, down = 0.0;
+        const real xs_same = (real)((ti == 1) ? d.p.xsph0 : (ti == 3) ? d.p.xsph2 : d.p.xsph1);
+        const real xs_wall = (real)((ti == 1 || ti == 3) ? 0.006 : d.p.xsph1 / 5.0);
+        Sum<real> stu[3], sdown;
         for (int q = 0; q < nn; q++) {
             const int j = d.s.nbr[(size_t)q * N + i];
             const int tj = d.s.type[j];
-            double xishu;
+            real xishu;
             if (ti == tj) {
-                xishu = (ti == 1) ? d.p.xsph0 : (ti == 3) ? d.p.xsph2 : d.p.xsph1;
+                xishu = xs_same;
             } else if (tj == 0) {
-                xishu = (ti == 1 || ti == 3) ? 0.006 : d.p.xsph1 / 5.0;
+                xishu = xs_wall;
             } else {
                 continue;
             }
-            double w[4];
-            pair_w<ND, KGC>(d, I, load_pos(d.s.xh, j), w);
-            const double mj = d.s.mass[j], rj = d.s.rho[j];
+            real w[4];
+            load_w(d, q, i, w);
+            const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
             for (int k = 0; k < nd; k++)
-                tu[k] = tu[k] + xishu * mj * (d.s.vx_next[k * N + j] - vm[k]) * w[3] / rj;
-            down = down + mj * w[3] / rj;
+                stu[k].add(xishu * mj * (real)(d.s.vx_next[k * N + j] - vm[k]) * w[3] / rj);
+            sdown.add(mj * w[3] / rj);
         }
+        double tu[3];
+        for (int k = 0; k < 3; k++) tu[k] = stu[k].v();
+        const double down = sdown.v();
         if (fabs(down) > 1.0e-7 && (ti == 2 || ti == 4))
             for (int k = 0; k < nd; k++) vn[k] = vm[k] + tu[k] / down;
         else
@@ -1139,7 +1268,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
             d.s.prep[i] = d.s.pre[i];
         }
     }
-    store_pos(d.s.xh_next, i, Pos{xn[0], xn[1], xn[2], I.h});
+    store_pos(d.s.xh_next, i, Pos{xn[0], xn[1], xn[2], load_pos(d.s.xh, i).h});
     for (int k = 0; k < 3; k++) d.s.vx[k * N + i] = vn[k];
 }
 
@@ -1151,18 +1280,19 @@ __global__ void k_step_done(Dev d)
 // kernel_gradient_correction (CPP_3-NNPS.cpp:376-496): the inverse of
 // L = sum_j m_j / rho_j (x_j - x_i) (x) grad W_ij over same-phase, wall and
 // soil/structure neighbours of each soil (type 2) or structure (type 4)
-// particle, inverted as inverse_mat_2D / inverse_mat_3D do (:499-558); the
-// pair kernels apply it to the gradients (pair_w).  Uses the densities of the
-// previous step, as the reference does (it runs before density()).
-template <int ND>
-__global__ void __launch_bounds__(128, SPH_MINB) k_kgc(Dev d)
+// particle, inverted as inverse_mat_2D / inverse_mat_3D do (:499-558), then
+// applied in place to the gradients of all the particle's pair records in
+// mat_multiply's order (:85-90), as the reference rewrites wij.  Uses the
+// densities of the previous step, as the reference does (it runs before
+// density()).  In the bulk form L is formed in FP64 from the FP32 records.
+template <int ND, typename R>
+__device__ __forceinline__ void kgc_particle(const Dev& d, int i)
 {
-    const int i = IDX, N = d.p.N;
-    if (i >= N || *d.s.err) return;
+    const int N = d.p.N;
     const int ti = d.s.type[i];
-    if (!(ti == 2 || ti == 4)) return;
     const int nn = nbr_count(d, i);
-    const PairI I = pair_i<ND, 0>(d, i);
+    const Pos P = load_pos(d.s.xh, i);
+    const double xi[3] = {P.x, P.y, P.z};
     double L[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     for (int q = 0; q < nn; q++) {
         const int j = d.s.nbr[(size_t)q * N + i];
@@ -1171,11 +1301,12 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_kgc(Dev d)
         if (!take) continue;
         const Pos pj = load_pos(d.s.xh, j);
         const double xj[3] = {pj.x, pj.y, pj.z};
-        double w[4];
-        pair_w<ND, 0>(d, I, pj, w);
+        R wr[4];
+        load_w(d, q, i, wr);
+        const double w[3] = {wr[0], wr[1], wr[2]};
         const double mr = d.s.mass[j] / d.s.rho[j];
         double xij[3];
-        for (int k = 0; k < ND; k++) xij[k] = xj[k] - I.x[k];
+        for (int k = 0; k < ND; k++) xij[k] = xj[k] - xi[k];
         for (int a = 0; a < ND; a++)
             for (int b = 0; b < ND; b++) L[a][b] = L[a][b] + mr * xij[a] * w[b];
     }
@@ -1205,15 +1336,36 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_kgc(Dev d)
             B[0][0] = 1.0; B[1][1] = 1.0; B[2][2] = 1.0;
         }
     }
-    for (int a = 0; a < 3; a++)
-        for (int b = 0; b < 3; b++) d.s.lmat[(size_t)(a * 3 + b) * N + i] = B[a][b];
+    R a[9];
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) a[r * 3 + c] = (R)B[r][c];
+    for (int q = 0; q < nn; q++) {
+        R w[4];
+        load_w(d, q, i, w);
+        const R c0 = a[0] * w[0] + a[1] * w[1] + a[2] * w[2];
+        const R c1 = a[3] * w[0] + a[4] * w[1] + a[5] * w[2];
+        const R c2 = a[6] * w[0] + a[7] * w[1] + a[8] * w[2];
+        w[0] = c0; w[1] = c1; w[2] = c2;
+        store_w(d, q, i, w);
+    }
+}
+
+template <int ND>
+__global__ void __launch_bounds__(128, SPH_MINB) k_kgc(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    const int ti = d.s.type[i];
+    if (!(ti == 2 || ti == 4)) return;
+    if (d.p.bulk) kgc_particle<ND, float>(d, i);
+    else kgc_particle<ND, double>(d, i);
 }
 
 // strain_regu / stress_regu (CPP_7-2-constitutive.cpp:385-450) in Jacobi
 // order: on steps with l % step_regu == 0, dst = the same-phase Shepard
 // average of src; otherwise dst = src.  For the strain, the values read are
 // those after strain_noreg's reset at l == inip (zero_at_inip).
-template <int ND, int KGC>
+template <int ND>
 __global__ void __launch_bounds__(128, SPH_MINB) k_regu(Dev d, const double* src, double* dst, int zero_at_inip)
 {
     const int i = IDX, N = d.p.N;
@@ -1225,26 +1377,32 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_regu(Dev d, const double* src
         return;
     }
     const int ti = d.s.type[i], nn = nbr_count(d, i);
-    const PairI I = pair_i<ND, 0>(d, i);
     double up[6] = {0, 0, 0, 0, 0, 0}, down = 0.0;
     for (int q = 0; q < nn; q++) {
         const int j = d.s.nbr[(size_t)q * N + i];
         if (d.s.type[j] != ti) continue;
-        double w[4];
-        pair_w<ND, 0>(d, I, load_pos(d.s.xh, j), w);
+        real wr[4];
+        load_w(d, q, i, wr);
+        const double w3 = wr[3];
         const double mr = d.s.mass[j] / d.s.rho[j];
-        for (int k = 0; k < 6; k++) up[k] = up[k] + mr * w[3] * (zero ? 0.0 : src[(size_t)k * N + j]);
-        down = down + mr * w[3];
+        for (int k = 0; k < 6; k++) up[k] = up[k] + mr * w3 * (zero ? 0.0 : src[(size_t)k * N + j]);
+        down = down + mr * w3;
     }
     for (int k = 0; k < 6; k++)
         dst[(size_t)k * N + i] = (fabs(down) > 1.0e-6) ? up[k] / down : (zero ? 0.0 : src[(size_t)k * N + i]);
 }
 
+}  // namespace SPH_NS
+
 // ---------------------------------------------------------------------------
 // host-side launch sequences (enqueued on `st`, capturable into a graph)
+using namespace SPH_NS;
 
 static inline unsigned nblk(long n, int b) { return (unsigned)((n + b - 1) / b); }
 
+#define REC(k) do { if (ev) cudaEventRecord(ev[k], st); } while (0)
+
+#ifndef SPH_BULK32
 extern "C" size_t sphk_sort_temp_bytes(int N, int end_bit)
 {
     size_t bytes = 0;
@@ -1257,30 +1415,19 @@ extern "C" size_t sphk_sort_temp_bytes(int N, int end_bit)
 // before stage k and ev[SPHK_NSTAGES] after the last one (stages a run does
 // not need are recorded with no work between their events).
 extern "C" const char* const sphk_stage_names[] = {
-    "k_cellkey", "radix_sort", "k_cellreset", "k_cellrange", "k_nnps", "k_kgc",
+    "k_cellkey", "radix_sort", "k_cellreset", "k_cellrange", "k_nnps", "k_pairw", "k_kgc",
     "k_density", "k_shepard_eos", "k_strain", "k_regu_eps", "k_stress", "k_regu_sig", "k_stress_2",
     "k_art_rij", "k_accel_a", "k_accel_b", "k_xsph_update", "k_step_done"};
 static_assert(sizeof(sphk_stage_names) / sizeof(sphk_stage_names[0]) == SPHK_NSTAGES, "stage table");
-#define REC(k) do { if (ev) cudaEventRecord(ev[k], st); } while (0)
+#endif  // !SPH_BULK32
 
-// launch K<ND> or K<ND, KGC> for the run's dimension and kernel-gradient mode
+// launch K<ND> for the run's dimension
 #define LAUNCH_ND(K, blocks, threads, ...)                                          \
     do {                                                                           \
         if (d.p.ndim == 2) K<2><<<blocks, threads, 0, st>>>(__VA_ARGS__);          \
         else K<3><<<blocks, threads, 0, st>>>(__VA_ARGS__);                        \
     } while (0)
-#define LAUNCH_PAIR(K, blocks, threads, ...)                                        \
-    do {                                                                           \
-        const bool kgc = d.p.flknl > 2;                                            \
-        if (d.p.ndim == 2) {                                                       \
-            if (kgc) K<2, 1><<<blocks, threads, 0, st>>>(__VA_ARGS__);             \
-            else K<2, 0><<<blocks, threads, 0, st>>>(__VA_ARGS__);                 \
-        } else {                                                                   \
-            if (kgc) K<3, 1><<<blocks, threads, 0, st>>>(__VA_ARGS__);             \
-            else K<3, 0><<<blocks, threads, 0, st>>>(__VA_ARGS__);                 \
-        }                                                                          \
-    } while (0)
-
+#ifndef SPH_BULK32
 // the NNPS stage (+ kernel gradient correction); returns the number of this
 // library's kernels it launched
 extern "C" int sphk_enqueue_nnps(const Dev* dp, void* sort_tmp, size_t sort_bytes, int end_bit, cudaStream_t st,
@@ -1302,27 +1449,31 @@ extern "C" int sphk_enqueue_nnps(const Dev* dp, void* sort_tmp, size_t sort_byte
     REC(4);
     LAUNCH_ND(k_nnps, nblk(N, 128), 128, d); n++;
     REC(5);
+    LAUNCH_ND(k_pairw, nblk(N, 128), 128, d); n++;
+    REC(6);
     if (d.p.flknl > 2) { LAUNCH_ND(k_kgc, nblk(N, 128), 128, d); n++; }
     return n;
 }
+#endif  // !SPH_BULK32
 
 // the rest of the step; `regu` includes the strain/stress regularisation
-// passes (which act on steps l with l % step_regu == 0)
-extern "C" int sphk_enqueue_physics(const Dev* dp, cudaStream_t st, cudaEvent_t* ev, int regu)
+// passes (which act on steps l with l % step_regu == 0).  The FP32-bulk build
+// exports it as sphk_enqueue_physics_bulk32.
+extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, cudaEvent_t* ev, int regu)
 {
     Dev d = *dp;
     d.s.eps_in = regu ? d.s.eps_tmp : d.s.eps;
     const int N = d.p.N;
     int n = 0;
-    REC(6);
-    LAUNCH_PAIR(k_density, nblk(N, 128), 128, d); n++;
     REC(7);
-    LAUNCH_PAIR(k_shepard_eos, nblk(N, 128), 128, d); n++;
+    LAUNCH_ND(k_density, nblk(N, 128), 128, d); n++;
     REC(8);
-    LAUNCH_PAIR(k_strain, nblk(N, 128), 128, d); n++;
+    LAUNCH_ND(k_shepard_eos, nblk(N, 128), 128, d); n++;
     REC(9);
-    if (regu) { LAUNCH_PAIR(k_regu, nblk(N, 128), 128, d, d.s.eps, d.s.eps_tmp, 1); n++; }
+    LAUNCH_ND(k_strain, nblk(N, 128), 128, d); n++;
     REC(10);
+    if (regu) { LAUNCH_ND(k_regu, nblk(N, 128), 128, d, d.s.eps, d.s.eps_tmp, 1); n++; }
+    REC(11);
     if (regu) {
         if (d.p.ndim == 2) k_stress<2, 1><<<nblk(N, 128), 128, 0, st>>>(d);
         else k_stress<3, 1><<<nblk(N, 128), 128, 0, st>>>(d);
@@ -1331,37 +1482,31 @@ extern "C" int sphk_enqueue_physics(const Dev* dp, cudaStream_t st, cudaEvent_t*
         else k_stress<3, 0><<<nblk(N, 128), 128, 0, st>>>(d);
     }
     n++;
-    REC(11);
-    if (regu) { LAUNCH_PAIR(k_regu, nblk(N, 128), 128, d, d.s.sig_next, d.s.sig_tmp, 0); n++; }
     REC(12);
+    if (regu) { LAUNCH_ND(k_regu, nblk(N, 128), 128, d, d.s.sig_next, d.s.sig_tmp, 0); n++; }
+    REC(13);
     if (regu) {
         if (d.p.ndim == 2) k_stress<2, 2><<<nblk(N, 128), 128, 0, st>>>(d);
         else k_stress<3, 2><<<nblk(N, 128), 128, 0, st>>>(d);
         n++;
     }
-    REC(13);
+    REC(14);
     const bool art = d.p.art_stre_coe > 0.0;
     if (art) { LAUNCH_ND(k_art_rij, nblk(N, 128), 128, d); n++; }
-    REC(14);
-    LAUNCH_PAIR(k_accel_a, nblk(N, 128), 128, d); n++;
     REC(15);
+    LAUNCH_ND(k_accel_a, nblk(N, 128), 128, d); n++;
+    REC(16);
     if (art) {
-        const bool kgc = d.p.flknl > 2;
-        if (d.p.ndim == 2) {
-            if (kgc) k_accel_b<2, 1, 1><<<nblk(N, 128), 128, 0, st>>>(d);
-            else k_accel_b<2, 0, 1><<<nblk(N, 128), 128, 0, st>>>(d);
-        } else {
-            if (kgc) k_accel_b<3, 1, 1><<<nblk(N, 128), 128, 0, st>>>(d);
-            else k_accel_b<3, 0, 1><<<nblk(N, 128), 128, 0, st>>>(d);
-        }
+        if (d.p.ndim == 2) k_accel_b<2, 1><<<nblk(N, 128), 128, 0, st>>>(d);
+        else k_accel_b<3, 1><<<nblk(N, 128), 128, 0, st>>>(d);
     } else {
-        LAUNCH_PAIR(k_accel_b, nblk(N, 128), 128, d);
+        LAUNCH_ND(k_accel_b, nblk(N, 128), 128, d);
     }
     n++;
-    REC(16);
-    LAUNCH_PAIR(k_xsph_update, nblk(N, 128), 128, d); n++;
     REC(17);
-    k_step_done<<<1, 32, 0, st>>>(d); n++;
+    LAUNCH_ND(k_xsph_update, nblk(N, 128), 128, d); n++;
     REC(18);
+    k_step_done<<<1, 32, 0, st>>>(d); n++;
+    REC(19);
     return n;
 }

@@ -112,6 +112,9 @@ FIELDS = {
 }
 INT_FIELDS = {"type", "matype", "permtype", "etype"}
 
+PREC_FP64 = 0          # SPHGPU_PREC_FP64
+PREC_FP32_BULK = 1     # SPHGPU_PREC_FP32_BULK
+
 ERRORS = {0: "ok", 3: "particle outside the cell grid", 5: "more than 99 neighbours",
           100: "bad argument", 101: "CUDA error", 102: "no CUDA device", 103: "unsupported flags",
           104: "call order"}
@@ -164,6 +167,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_stage_name.restype = C.c_char_p
     lib.sphgpu_stage_name.argtypes = [C.c_int]
     lib.sphgpu_step_profiled.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    lib.sphgpu_set_precision.argtypes = [C.c_void_p, C.c_int]
+    lib.sphgpu_get_precision.argtypes = [C.c_void_p]
     _lib = lib
     return lib
 
@@ -225,6 +230,14 @@ class Engine:
                 self.set_field(name, v)
         if fluid is not None or soil is not None:
             self.set_materials(fluid, soil)
+
+    def set_precision(self, mode: int) -> None:
+        """PREC_FP64 (the reference's arithmetic) or PREC_FP32_BULK."""
+        self._check(self.lib.sphgpu_set_precision(self.h, int(mode)), "sphgpu_set_precision")
+
+    @property
+    def precision(self) -> int:
+        return int(self.lib.sphgpu_get_precision(self.h))
 
     def step(self, nsteps: int = 1) -> None:
         self._check(self.lib.sphgpu_step(self.h, int(nsteps)), "sphgpu_step")
