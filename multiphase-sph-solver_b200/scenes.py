@@ -674,3 +674,33 @@ def initialise(scene: Scene) -> InitialState:
         structure=st,
     )
     return InitialState(params=params, fields=f, fluid=fl, soil=so)
+
+
+def kl_domain(scene: Scene) -> dict:
+    """The values the K-L generators take from Cell_Con (input_par,
+    CPP_2-initialf.cpp:933-1010; SpatialVariables_Generate_2D/3D,
+    CPP_17-1_K-L_expansion_non.cpp:66-90, 160-186): the half extents `a` and
+    centre `x_trans` of the non-boundary particles' box widened by 20% per
+    side, and soil_max / water_max along y (2-D) or z (3-D).  input_par forms
+    those maxima as fmax(running min, x), so they hold the coordinate of the
+    last soil / water particle in particle order, not the maximum."""
+    nd = scene.ndim
+    t = scene.ptype
+    nb = (t != 0) & (t != 7)
+    lo, hi = np.full(3, 10000.0), np.full(3, -10000.0)
+    if nb.any():
+        lo = np.minimum(lo, scene.xp[nb].min(axis=0))
+        hi = np.maximum(hi, scene.xp[nb].max(axis=0))
+    axis = 1 if nd == 2 else 2
+    soil = np.flatnonzero(t == 2)
+    water = np.flatnonzero(t == 1)
+    soil_max = float(scene.xp[soil[-1], axis]) if len(soil) else -100000.0
+    water_max = float(scene.xp[water[-1], axis]) if len(water) else -100000.0
+    a, xt = np.zeros(3), np.zeros(3)
+    for d in range(nd):
+        xmin = lo[d] - 0.2 * (hi[d] - lo[d])
+        xmax = hi[d] + 0.2 * (hi[d] - lo[d])
+        xt[d] = (xmax + xmin) / 2.0
+        a[d] = (xmax - xmin) / 2.0
+    return {"a": a, "x_trans": xt, "soil_max": soil_max, "water_max": water_max,
+            "nb_min": lo, "nb_max": hi}

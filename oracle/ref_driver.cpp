@@ -15,7 +15,14 @@
 #include <stdlib.h>
 #include <string.h>
 
+// The K-L generator's steps (solve_wi, solve_ramdai, solve_h_2D/3D) are
+// private members of clFSpatialVariability_Fun; this harness calls them
+// directly so that the standard-normal coefficients can be injected in place
+// of the generator's time-seeded draw.  The class has no data members, so
+// widening access in this translation unit changes nothing else.
+#define private public
 #include "Class_Functions.h"
+#undef private
 
 #include "../include/sphgpu.h"
 
@@ -309,3 +316,74 @@ void ref_destroy(void* h)
 }
 
 }  // extern "C"
+
+/*
+ * The reference's K-L random field (CPP_17-1_K-L_expansion_non.cpp) for one
+ * field with injected standard-normal coefficients uu[klterm]: solve_wi,
+ * solve_ramdai and solve_h_2D / solve_h_3D as SpatialVariables_Generate_2D /
+ * _3D call them (CPP_17-1:138-157, 250-269).  n particles with positions xp
+ * (n x 3) and types; a[3], x_trans[3], soil_max, water_max as the generator
+ * derives them.  Returns the reference's code; out[i] receives the member the
+ * field writes (NaN where it writes none), wi (200 x 3), eigval (200) and
+ * order (200 x 3) the intermediate results.
+ */
+extern "C" int ref_kl_field(int ndim, int n, const double* xp, const int* type, int no, int dist_type,
+                            double mean_value, double sd_value, double coe_depth, const double* rl,
+                            const double* a, const double* x_trans, double soil_max, double water_max,
+                            const double* uu, double* out, double* wi_out, double* eigval_out, int* order_out)
+{
+    const int K = 200;
+    Particle* par = new Particle[n];
+    Para_Fluid* fl = new Para_Fluid[n];
+    Para_Soil* so = new Para_Soil[n];
+    const double nan = 0.0 / 0.0;
+    for (int i = 0; i < n; i++) {
+        for (int d = 0; d < 3; d++) par[i].xp[d] = xp[(size_t)i * 3 + d];
+        par[i].type = type[i];
+        fl[i].fai = fl[i].c = nan;
+        so[i].fai = so[i].c = so[i].cop = so[i].ds = nan;
+    }
+    Para_Pro pro;
+    pro.ndim = ndim;
+    pro.ntotal = n;
+    Para_SpatialVariability psv;
+    psv.no = no;
+    psv.type = dist_type;
+    psv.mean_value = mean_value;
+    psv.sd_value = sd_value;
+    psv.coe_depth = coe_depth;
+    for (int d = 0; d < 3; d++) { psv.rl_value[d] = rl[d]; psv.a[d] = a[d]; }
+    double wi[200][3], eigval[200], xt[3] = {x_trans[0], x_trans[1], x_trans[2]};
+    int order_id[200][3];
+    double u[200];
+    for (int j = 0; j < K; j++) u[j] = uu[j];
+    clFSpatialVariability_Fun f;
+    f.solve_wi(wi, psv.a, psv.rl_value, ndim);
+    int err = f.solve_ramdai(eigval, wi, psv.rl_value, order_id, ndim);
+    if (!err) {
+        if (ndim == 2)
+            err = f.solve_h_2D(par, fl, so, pro, wi, eigval, u, xt, order_id, psv, soil_max, water_max, no);
+        else
+            err = f.solve_h_3D(par, fl, so, pro, wi, eigval, u, xt, order_id, psv, soil_max, water_max, no);
+    }
+    for (int i = 0; i < n; i++) {
+        double v = nan;
+        switch (no) {
+        case 0: v = so[i].fai; break;
+        case 1: v = so[i].c; break;
+        case 2: v = so[i].cop; break;
+        case 3: v = so[i].ds; break;
+        case 4: v = fl[i].fai; break;
+        case 5: v = fl[i].c; break;
+        }
+        out[i] = v;
+    }
+    for (int j = 0; j < K; j++) {
+        eigval_out[j] = eigval[j];
+        for (int d = 0; d < 3; d++) { wi_out[j * 3 + d] = wi[j][d]; order_out[j * 3 + d] = order_id[j][d]; }
+    }
+    delete[] par;
+    delete[] fl;
+    delete[] so;
+    return err;
+}

@@ -52,6 +52,8 @@ def oracle_lib():
         lib.orc_set_field.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t]
         lib.orc_get_field.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t]
         lib.orc_set_materials.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        lib.orc_kl_solve_wi.argtypes = [C.c_void_p, C.c_double * 3, C.c_double * 3, C.c_int, C.c_int]
+        lib.orc_kl_ramdai.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double * 3, C.c_int, C.c_int]
         lib.orc_set_mode.argtypes = [C.c_void_p, C.c_int]
         lib.orc_set_pow_mode.argtypes = [C.c_void_p, C.c_int]
         lib.orc_pow7.restype = C.c_double
@@ -206,3 +208,76 @@ STATE_FIELDS = ("x", "xp", "vx", "vxp", "ax", "axp", "ux", "strep", "interf", "i
 
 def snapshot(obj, names=STATE_FIELDS):
     return {k: obj.get_field(k) for k in names}
+
+
+# --------------------------------------------------------------------------
+# K-L random fields (CPP_17-1_K-L_expansion_non.cpp)
+
+class OrcKLSpec(C.Structure):
+    _fields_ = [("no", C.c_int), ("type", C.c_int), ("mean_value", C.c_double), ("sd_value", C.c_double),
+                ("coe_depth", C.c_double), ("rl", C.c_double * 3), ("a", C.c_double * 3),
+                ("x_trans", C.c_double * 3), ("soil_max", C.c_double), ("water_max", C.c_double)]
+
+
+def kl_spec(field: dict, dom: dict) -> OrcKLSpec:
+    s = OrcKLSpec()
+    s.no, s.type = int(field["no"]), int(field["type"])
+    s.mean_value, s.sd_value, s.coe_depth = field["mean"], field["sd"], field.get("coe_depth", 0.0)
+    for d in range(3):
+        s.rl[d] = field["rl"][d]
+        s.a[d] = dom["a"][d]
+        s.x_trans[d] = dom["x_trans"][d]
+    s.soil_max, s.water_max = dom["soil_max"], dom["water_max"]
+    return s
+
+
+def kl_oracle(ndim, xp, ptype, field, dom, xi, K=200):
+    """The oracle's field: (out, written, wi, eigval, order)."""
+    lib = oracle_lib()
+    n = len(ptype)
+    xp = np.ascontiguousarray(xp, dtype=np.float64).reshape(n, 3)
+    ptype = np.ascontiguousarray(ptype, dtype=np.int32)
+    s = kl_spec(field, dom)
+    wi = np.zeros((K, 3))
+    lib.orc_kl_solve_wi(_ptr(wi), s.a, s.rl, C.c_int(ndim), C.c_int(K))
+    eig = np.zeros(K)
+    order = np.zeros((K, 3), np.int32)
+    assert lib.orc_kl_ramdai(_ptr(eig), _ptr(order), _ptr(wi), s.rl, C.c_int(ndim), C.c_int(K)) == 0
+    out = np.full(n, np.nan)
+    written = np.zeros(n, np.int32)
+    xi = np.ascontiguousarray(xi, dtype=np.float64)
+    err = lib.orc_kl_field(C.c_int(ndim), C.c_int(n), _ptr(xp), _ptr(ptype), C.byref(s), _ptr(wi), _ptr(eig),
+                           _ptr(order), _ptr(xi), C.c_int(K), _ptr(out), _ptr(written))
+    assert err == 0
+    out[written == 0] = np.nan
+    return out, written, wi, eig, order
+
+
+def kl_correlate(u2, coefficient, K=200):
+    lib = oracle_lib()
+    u2 = np.ascontiguousarray(u2, dtype=np.float64).reshape(K, 2)
+    a, b = np.zeros(K), np.zeros(K)
+    lib.orc_kl_correlate(_ptr(u2), C.c_double(coefficient), _ptr(a), _ptr(b), C.c_int(K))
+    return a, b
+
+
+def kl_reference(ndim, xp, ptype, field, dom, xi):
+    """The reference's own solve_wi / solve_ramdai / solve_h (klterm = 200)."""
+    lib = reference_lib()
+    n = len(ptype)
+    xp = np.ascontiguousarray(xp, dtype=np.float64).reshape(n, 3)
+    ptype = np.ascontiguousarray(ptype, dtype=np.int32)
+    out = np.zeros(n)
+    wi, eig, order = np.zeros((200, 3)), np.zeros(200), np.zeros((200, 3), np.int32)
+    rl = np.ascontiguousarray(field["rl"], dtype=np.float64)
+    a = np.ascontiguousarray(dom["a"], dtype=np.float64)
+    xt = np.ascontiguousarray(dom["x_trans"], dtype=np.float64)
+    xi = np.ascontiguousarray(xi, dtype=np.float64)
+    f = lib.ref_kl_field
+    f.restype = C.c_int
+    err = f(C.c_int(ndim), C.c_int(n), _ptr(xp), _ptr(ptype), C.c_int(int(field["no"])), C.c_int(int(field["type"])),
+            C.c_double(field["mean"]), C.c_double(field["sd"]), C.c_double(field.get("coe_depth", 0.0)),
+            _ptr(rl), _ptr(a), _ptr(xt), C.c_double(dom["soil_max"]), C.c_double(dom["water_max"]),
+            _ptr(xi), _ptr(out), _ptr(wi), _ptr(eig), _ptr(order))
+    assert err == 0
+    return out, wi, eig, order

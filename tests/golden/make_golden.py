@@ -25,7 +25,7 @@ sys.path[:0] = [os.path.join(REPO, "multiphase-sph-solver_b200"), os.path.join(R
 
 import scenes  # noqa: E402
 import sphgpu  # noqa: E402
-from checkers import STATE_FIELDS, Reference  # noqa: E402
+from checkers import STATE_FIELDS, Reference, kl_reference  # noqa: E402
 
 def _kgc_regu():
     """The soil column with the Yang-Liu kernel, kernel gradient correction
@@ -93,7 +93,43 @@ CASES = {
 }
 
 
+# K-L random fields (CPP_17-1_K-L_expansion_non.cpp) through the reference's
+# own solve_wi / solve_ramdai / solve_h with injected standard normals:
+# name: (scene factory, field, seed of the normals)
+KL_CASES = {
+    "kl_slope_2d_cohesion_lognormal": (
+        lambda: scenes.slope_2d(H=5.0, dx=0.1),
+        {"no": 1, "type": 2, "mean": 10.0e3, "sd": 3.0e3, "rl": [10.0, 1.0, 0.0], "coe_depth": 0.0}, 1),
+    "kl_slope_2d_friction_normal_depth": (
+        lambda: scenes.slope_2d(H=5.0, dx=0.1),
+        {"no": 0, "type": 1, "mean": 25.0, "sd": 2.5, "rl": [5.0, 2.0, 0.0], "coe_depth": 0.4}, 2),
+    "kl_column_3d_friction_normal_depth": (
+        lambda: scenes.soil_column_3d(dx=0.05, steps=100),
+        {"no": 0, "type": 1, "mean": 30.0, "sd": 3.0, "rl": [0.5, 0.3, 0.2], "coe_depth": 2.0}, 3),
+    "kl_column_3d_fluid_cohesion_lognormal": (
+        lambda: scenes.soil_column_3d(dx=0.05, steps=100),
+        {"no": 5, "type": 2, "mean": 50.0, "sd": 10.0, "rl": [0.4, 0.4, 0.3], "coe_depth": 0.0}, 4),
+}
+
+
+def make_kl(name: str) -> str:
+    factory, field, seed = KL_CASES[name]
+    sc = factory()
+    dom = scenes.kl_domain(sc)
+    xi = np.random.default_rng(seed).standard_normal(200)
+    out, wi, eig, order = kl_reference(sc.ndim, sc.xp, sc.ptype, field, dom, xi)
+    fn = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(fn, ndim=sc.ndim, xp=sc.xp, type=sc.ptype, xi=xi,
+                        field=np.array([field["no"], field["type"]]),
+                        field_vals=np.array([field["mean"], field["sd"], field["coe_depth"]] + list(field["rl"])),
+                        a=dom["a"], x_trans=dom["x_trans"], soil_max=dom["soil_max"], water_max=dom["water_max"],
+                        out=out, wi=wi[:, :sc.ndim], eigval=eig, order=order[:, :sc.ndim])
+    return fn
+
+
 def make(name: str) -> str:
+    if name in KL_CASES:
+        return make_kl(name)
     factory, steps = CASES[name]
     sc = factory()
     out = {}
@@ -126,7 +162,7 @@ if __name__ == "__main__":
     saved = os.dup(1)
     os.dup2(devnull, 1)   # the reference prints progress lines
     try:
-        files = [make(n) for n in (sys.argv[1:] or CASES)]
+        files = [make(n) for n in (sys.argv[1:] or list(CASES) + list(KL_CASES))]
     finally:
         os.dup2(saved, 1)
     for f in files:
