@@ -227,6 +227,54 @@ const char* sphgpu_stage_name(int k);
 int         sphgpu_step_profiled(sphgpu_ctx* ctx, int nsteps, double* stage_ms);
 
 /*
+ * Karhunen-Loeve random fields (flspv 1 and 2): the reference's
+ * clFSpatialVariability_Fun::SpatialVariables_Generate_2D / _3D and
+ * SpatialVariables_Generate_2D_corr / _3D_corr
+ * (Class_spatial_variability.h:79-86, CPP_17-1_K-L_expansion_non.cpp:62-272,
+ * CPP_17-2_K-L_expansion_corr.cpp:55-473).
+ *
+ * sphgpu_kl_field is Para_SpatialVariability (Class_spatial_variability.h:46-66)
+ * without its derived half extents; `no` selects the member written:
+ * 0 soil fai, 1 soil c, 2 soil cop, 3 soil ds (type-2 particles), 4 fluid fai,
+ * 5 fluid c (type-1 particles).  sphgpu_kl_domain holds the Cell_Con members
+ * the generators read (Class_NNPS.h): the extents of the non-boundary
+ * particles (xmin_nb .. zmax_nb) and soil_max / water_max as input_par stores
+ * them (CPP_2-initialf.cpp:954-961).
+ *
+ * The reference draws the standard normals from a time-seeded generator
+ * (generate_SND, CPP_17-1:24-33); here the caller passes them: xi holds K
+ * values per field (sphgpu_kl_generate) or K x 2 values per correlated pair
+ * (sphgpu_kl_generate_corr, the uu_cfai matrix of CPP_17-2:121).  K is the
+ * number of terms, the reference's klterm (200); other K are accepted.
+ * The fields are written into the context's material records for the
+ * particles each field covers (sphgpu_set_materials must have been called)
+ * and the constants the step derives from them are evaluated again; out, if
+ * non-NULL, receives nfields x ntotal values (NaN where a field writes none).
+ * Returns 0, 13 (a zero half extent, as the reference), 14 (a distribution
+ * type other than 1 or 2), or an engine code.
+ */
+typedef struct sphgpu_kl_field {
+    int    no;                /* member written (above) */
+    int    type;              /* 1 normal, 2 lognormal */
+    double mean_value, sd_value;
+    double rl_value[3];       /* correlation lengths */
+    double coe_depth;         /* mean + (top - y) * coe_depth */
+} sphgpu_kl_field;
+
+typedef struct sphgpu_kl_domain {
+    double xmin_nb, xmax_nb, ymin_nb, ymax_nb, zmin_nb, zmax_nb;
+    double soil_max[3], water_max[3];
+} sphgpu_kl_domain;
+
+int sphgpu_kl_generate(sphgpu_ctx* ctx, const sphgpu_kl_domain* dom, const sphgpu_kl_field* fields, int nfields,
+                       const double* xi, int K, double* out);
+/* Correlated friction / cohesion (flspv 2): pairs[0] is the friction field
+ * (no 0 or 4) and pairs[1] the cohesion field (no 1 or 5) of one phase;
+ * coe_frict_cohesion is Flag_SpatialVariability::coe_frict_cohesion. */
+int sphgpu_kl_generate_corr(sphgpu_ctx* ctx, const sphgpu_kl_domain* dom, const sphgpu_kl_field pair[2],
+                            double coe_frict_cohesion, const double* u2, int K, double* out);
+
+/*
  * Neighbour search that allocates no device memory (no counterpart in the
  * reference: an addition of this library).
  *

@@ -23,6 +23,14 @@ extern "C" int sphk_enqueue_nnps(const Dev* d, void* sort_tmp, size_t sort_bytes
 extern "C" int sphk_enqueue_physics(const Dev* d, cudaStream_t st, cudaEvent_t* ev, int regu);
 extern "C" int sphk_enqueue_physics_bulk32(const Dev* d, cudaStream_t st, cudaEvent_t* ev, int regu);
 extern "C" const char* const sphk_stage_names[];
+extern "C" size_t sphk_kl_sort_bytes(size_t total);
+extern "C" int sphk_kl_order(const double* d_r, int K, int ndim, double* keys_in, double* keys_out, uint32_t* vals_in,
+                             uint32_t* vals_out, void* sort_tmp, size_t sort_bytes, cudaStream_t st);
+extern "C" int sphk_kl_field(int n, int ndim, int K, int no, int type, const double* x_trans, double mean_value,
+                             double sd_value, double coe_depth, double soil_max, double water_max, const double* d_xh,
+                             const int* d_type, const void* d_terms, const double* d_sqrt_eig, const double* d_xi,
+                             double* d_out, cudaStream_t st);
+extern "C" size_t sphk_kl_term_bytes(void);
 
 namespace {
 
@@ -93,6 +101,8 @@ struct sphgpu_ctx {
     size_t pinned_bytes = 0;
     bool regu = false;     // graphs include the strain/stress regularisation passes
     int precision = SPHGPU_PREC_FP64;
+    std::vector<sphgpu_fluid> h_fluid;   // the material records last set (K-L fields rewrite members)
+    std::vector<sphgpu_soil> h_soil;
 };
 
 namespace {
@@ -518,6 +528,8 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
 {
     if (!c || n != c->N) return SPHGPU_E_ARG;
     cudaSetDevice(c->device);
+    if (fl && fl != c->h_fluid.data()) c->h_fluid.assign(fl, fl + n);
+    if (so && so != c->h_soil.data()) c->h_soil.assign(so, so + n);
     const int N = c->N;
     DevState& s = c->d[0].s;
     std::vector<double> buf((size_t)N);
@@ -748,5 +760,231 @@ int sphgpu_step_profiled(sphgpu_ctx* c, int nsteps, double* stage_ms)
 double sphgpu_last_step_ms(const sphgpu_ctx* c) { return c ? c->last_ms : 0.0; }
 long sphgpu_last_step_launches(const sphgpu_ctx* c) { return c ? c->last_launches : 0; }
 void* sphgpu_stream(sphgpu_ctx* c) { return c ? (void*)c->st : nullptr; }
+
+
+// ---------------------------------------------------------------------------
+// Karhunen-Loeve random fields (CPP_17-1_K-L_expansion_non.cpp)
+
+namespace {
+
+const double kKlPi = 3.141592653;     // Header_Parameters.h:10
+const double kKlPrec = 1.0e-6;        // CPP_17-1:21
+
+// solve_wi (CPP_17-1:275-345): the positive roots w of 2/l - w tan(w a)
+// (odd terms) and 2/l tan(w a) + w (even terms) per axis, by bisection
+// between the reference's bounds, in FP64 with the C library's tan.
+void kl_solve_wi(std::vector<double>& wi, const double a_x[3], const double rl[3], int ndim, int K)
+{
+    wi.assign((size_t)K * 3, 0.0);
+    std::vector<double> up(K), lo(K);
+    for (int d = 0; d < ndim; d++) {
+        const double a = a_x[d], dira = rl[d];
+        for (int i = 0; i < K; i++) {
+            if ((i + 1) % 2 == 1) { up[i] = (i + 0.5) * kKlPi / a; lo[i] = i * kKlPi / a; }
+            else { up[i] = (i + 1.0) * kKlPi / a; lo[i] = (i + 0.5) * kKlPi / a; }
+        }
+        for (int i = 0; i < K; i++) {
+            double x1 = lo[i] + kKlPrec, x2 = up[i] - kKlPrec, xm, f1, fm;
+            const bool odd = (i + 1) % 2 == 1;
+            xm = odd ? (x1 + x2) * 0.5 : (x1 + x2) / 2.0;
+            do {
+                if (odd) {
+                    f1 = 2.0 / dira - x1 * std::tan(x1 * a);
+                    fm = 2.0 / dira - xm * std::tan(xm * a);
+                } else {
+                    f1 = 2.0 / dira * std::tan(x1 * a) + x1;
+                    fm = 2.0 / dira * std::tan(xm * a) + xm;
+                }
+                if ((f1 * fm) < 0.0) x2 = xm;
+                else x1 = xm;
+                xm = (x1 + x2) * 0.5;
+            } while (std::fabs(fm) > kKlPrec);
+            wi[(size_t)i * 3 + d] = xm;
+        }
+    }
+}
+
+struct HostKLTerm { double w, alpha; int use_cos; int pad; };
+
+// One field of SpatialVariables_Generate_2D / _3D for the context's
+// particles; d_out receives the values (NaN where the field writes none).
+int kl_one_field(sphgpu_ctx* c, const double a[3], const double x_trans[3], double soil_max, double water_max,
+                 const sphgpu_kl_field& f, const double* xi, int K, double* d_out)
+{
+    const int nd = c->P.ndim;
+    if (f.type != 1 && f.type != 2) return 14;
+    std::vector<double> wi;
+    kl_solve_wi(wi, a, f.rl_value, nd, K);
+    // 1-D eigenvalues (equation_ramdai, CPP_17-1:36-41)
+    std::vector<double> r((size_t)K * 3, 0.0);
+    for (int d = 0; d < nd; d++)
+        for (int i = 0; i < K; i++) {
+            const double w = wi[(size_t)i * 3 + d], dirac = f.rl_value[d];
+            r[(size_t)i * 3 + d] = 4.0 * dirac / (4.0 + w * w * dirac * dirac);
+        }
+    const size_t total = (nd == 2) ? (size_t)K * K : (size_t)K * K * K;
+    if (total > 0xffffffffull) return SPHGPU_E_ARG;
+    const size_t sort_bytes = sphk_kl_sort_bytes(total);
+    void* buf = nullptr;
+    const size_t off_r = 0, off_ki = 256 * ((sizeof(double) * 3 * K + 255) / 256);
+    const size_t off_ko = off_ki + 256 * ((8 * total + 255) / 256);
+    const size_t off_vi = off_ko + 256 * ((8 * total + 255) / 256);
+    const size_t off_vo = off_vi + 256 * ((4 * total + 255) / 256);
+    const size_t off_tmp = off_vo + 256 * ((4 * total + 255) / 256);
+    const size_t off_terms = off_tmp + 256 * ((sort_bytes + 255) / 256);
+    const size_t off_se = off_terms + 256 * ((sphk_kl_term_bytes() * 3 * K + 255) / 256);
+    const size_t off_xi = off_se + 256 * ((8 * (size_t)K + 255) / 256);
+    const size_t bytes = off_xi + 8 * (size_t)K;
+    CK(cudaMalloc(&buf, bytes));
+    char* b = (char*)buf;
+    int rc = 0;
+    do {
+        if (cuda_fail(c, cudaMemcpyAsync(b + off_r, r.data(), sizeof(double) * 3 * K, cudaMemcpyHostToDevice, c->st),
+                      "cudaMemcpyAsync")) { rc = SPHGPU_E_CUDA; break; }
+        if (sphk_kl_order((const double*)(b + off_r), K, nd, (double*)(b + off_ki), (double*)(b + off_ko),
+                          (uint32_t*)(b + off_vi), (uint32_t*)(b + off_vo), b + off_tmp, sort_bytes, c->st)) {
+            rc = cuda_fail(c, cudaGetLastError(), "K-L eigenvalue ordering");
+            if (!rc) rc = SPHGPU_E_CUDA;
+            break;
+        }
+        std::vector<double> eig(K);
+        std::vector<uint32_t> idx(K);
+        if (cuda_fail(c, cudaMemcpyAsync(eig.data(), b + off_ko, 8 * (size_t)K, cudaMemcpyDeviceToHost, c->st),
+                      "cudaMemcpyAsync") ||
+            cuda_fail(c, cudaMemcpyAsync(idx.data(), b + off_vo, 4 * (size_t)K, cudaMemcpyDeviceToHost, c->st),
+                      "cudaMemcpyAsync") ||
+            cuda_fail(c, cudaStreamSynchronize(c->st), "cudaStreamSynchronize")) { rc = SPHGPU_E_CUDA; break; }
+        // the terms: per axis the root of the selected 1-D index, its
+        // normalisation (solve_faii, CPP_17-1:44-59) and cos / sin parity
+        std::vector<HostKLTerm> terms((size_t)K * nd);
+        std::vector<double> se(K);
+        for (int j = 0; j < K; j++) {
+            int id[3];
+            if (nd == 2) { id[0] = (int)(idx[j] / K); id[1] = (int)(idx[j] % K); }
+            else {
+                id[0] = (int)(idx[j] / ((uint32_t)K * K));
+                id[1] = (int)((idx[j] / K) % K);
+                id[2] = (int)(idx[j] % K);
+            }
+            for (int d = 0; d < nd; d++) {
+                const double w = wi[(size_t)id[d] * 3 + d], ad = a[d];
+                HostKLTerm& t = terms[(size_t)j * nd + d];
+                t.w = w;
+                t.use_cos = ((id[d] + 1) % 2 == 1) ? 1 : 0;
+                t.alpha = t.use_cos ? 1.0 / std::sqrt(std::sin(2.0 * w * ad) / 2.0 / w + ad)
+                                    : 1.0 / std::sqrt(-std::sin(2.0 * w * ad) / 2.0 / w + ad);
+                t.pad = 0;
+            }
+            se[j] = std::sqrt(eig[j]);
+        }
+        if (cuda_fail(c, cudaMemcpyAsync(b + off_terms, terms.data(), sizeof(HostKLTerm) * terms.size(),
+                                         cudaMemcpyHostToDevice, c->st), "cudaMemcpyAsync") ||
+            cuda_fail(c, cudaMemcpyAsync(b + off_se, se.data(), 8 * (size_t)K, cudaMemcpyHostToDevice, c->st),
+                      "cudaMemcpyAsync") ||
+            cuda_fail(c, cudaMemcpyAsync(b + off_xi, xi, 8 * (size_t)K, cudaMemcpyHostToDevice, c->st),
+                      "cudaMemcpyAsync")) { rc = SPHGPU_E_CUDA; break; }
+        const DevState& s = c->d[c->parity].s;
+        if (sphk_kl_field(c->N, nd, K, f.no, f.type, x_trans, f.mean_value, f.sd_value, f.coe_depth, soil_max,
+                          water_max, s.xh, s.type, b + off_terms, (const double*)(b + off_se),
+                          (const double*)(b + off_xi), d_out, c->st)) { rc = SPHGPU_E_CUDA; break; }
+        if (cuda_fail(c, cudaStreamSynchronize(c->st), "cudaStreamSynchronize")) { rc = SPHGPU_E_CUDA; break; }
+    } while (0);
+    cudaFree(buf);
+    return rc;
+}
+
+int kl_run(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_kl_field* fields, int nfields,
+           const double* const* xis, int K, double* out)
+{
+    if (!c || !dom || !fields || nfields <= 0 || K <= 0) return SPHGPU_E_ARG;
+    if (c->h_type.empty() || (c->h_soil.empty() && c->h_fluid.empty())) return SPHGPU_E_STATE;
+    for (int q = 0; q < nfields; q++) {
+        if (fields[q].no < 0 || fields[q].no > 5) return SPHGPU_E_ARG;
+        if (fields[q].no <= 3 && c->h_soil.empty()) return SPHGPU_E_STATE;
+        if (fields[q].no >= 4 && c->h_fluid.empty()) return SPHGPU_E_STATE;
+    }
+    cudaSetDevice(c->device);
+    const int nd = c->P.ndim, N = c->N;
+    // the field domain: the non-boundary box widened by 20% per side
+    // (CPP_17-1:70-90, 166-186); soil_max / water_max along y (2-D) or z (3-D)
+    const double lo[3] = {dom->xmin_nb, dom->ymin_nb, dom->zmin_nb};
+    const double hi[3] = {dom->xmax_nb, dom->ymax_nb, dom->zmax_nb};
+    double a[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
+    for (int d = 0; d < nd; d++) {
+        const double xmin = lo[d] - 0.2 * (hi[d] - lo[d]), xmax = hi[d] + 0.2 * (hi[d] - lo[d]);
+        xt[d] = (xmax + xmin) / 2.0;
+        a[d] = (xmax - xmin) / 2.0;
+    }
+    if (a[0] == 0.0 || a[1] == 0.0) return 13;
+    const double soil_max = dom->soil_max[nd == 2 ? 1 : 2], water_max = dom->water_max[nd == 2 ? 1 : 2];
+    double* d_out = nullptr;
+    CK(cudaMalloc(&d_out, sizeof(double) * N));
+    std::vector<double> v(N);
+    int rc = 0;
+    for (int q = 0; q < nfields && !rc; q++) {
+        rc = kl_one_field(c, a, xt, soil_max, water_max, fields[q], xis[q], K, d_out);
+        if (rc) break;
+        if (cuda_fail(c, cudaMemcpy(v.data(), d_out, sizeof(double) * N, cudaMemcpyDeviceToHost), "cudaMemcpy")) {
+            rc = SPHGPU_E_CUDA;
+            break;
+        }
+        if (out) std::memcpy(out + (size_t)q * N, v.data(), sizeof(double) * N);
+        const int no = fields[q].no;
+        for (int i = 0; i < N; i++) {
+            if (v[i] != v[i]) continue;
+            switch (no) {
+            case 0: c->h_soil[i].fai = v[i]; break;
+            case 1: c->h_soil[i].c = v[i]; break;
+            case 2: c->h_soil[i].cop = v[i]; break;
+            case 3: c->h_soil[i].ds = v[i]; break;
+            case 4: c->h_fluid[i].fai = v[i]; break;
+            case 5: c->h_fluid[i].c = v[i]; break;
+            }
+        }
+    }
+    cudaFree(d_out);
+    if (rc) return rc;
+    return sphgpu_set_materials(c, c->h_fluid.empty() ? nullptr : c->h_fluid.data(),
+                                c->h_soil.empty() ? nullptr : c->h_soil.data(), N);
+}
+
+}  // namespace
+
+int sphgpu_kl_generate(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_kl_field* fields, int nfields,
+                       const double* xi, int K, double* out)
+{
+    if (!xi || nfields <= 0) return SPHGPU_E_ARG;
+    std::vector<const double*> xis(nfields);
+    for (int q = 0; q < nfields; q++) xis[q] = xi + (size_t)q * K;
+    return kl_run(c, dom, fields, nfields, xis.data(), K, out);
+}
+
+int sphgpu_kl_generate_corr(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_kl_field pair[2],
+                            double coe, const double* u2, int K, double* out)
+{
+    if (!pair || !u2 || K <= 0) return SPHGPU_E_ARG;
+    // the correlation coefficient of the underlying normals
+    // (CPP_17-2:115-131): for lognormal fields from the fields' COVs
+    double coefficient = coe;
+    if (pair[0].type == 2) {
+        const double m0 = pair[0].mean_value, s0 = pair[0].sd_value, m1 = pair[1].mean_value, s1 = pair[1].sd_value;
+        coefficient = std::log(1.0 + coe * (s0 / m0) * (s1 / m1));
+        coefficient = coefficient / std::sqrt(std::log(1.0 + s0 * s0 / m0 / m0) * std::log(1.0 + s1 * s1 / m1 / m1));
+    }
+    // zeta = u2 [1, coefficient; 0, sqrt(1 - coefficient^2)] (matrix_multi, CPP_17-2:21-35, 133-140)
+    const double cm[4] = {1.0, coefficient, 0.0, std::sqrt(1.0 - coefficient * coefficient)};
+    std::vector<double> z0(K), z1(K);
+    for (int i = 0; i < K; i++) {
+        double t0 = 0.0, t1 = 0.0;
+        t0 = t0 + u2[(size_t)i * 2 + 0] * cm[0];
+        t0 = t0 + u2[(size_t)i * 2 + 1] * cm[2];
+        t1 = t1 + u2[(size_t)i * 2 + 0] * cm[1];
+        t1 = t1 + u2[(size_t)i * 2 + 1] * cm[3];
+        z0[i] = t0;
+        z1[i] = t1;
+    }
+    const double* xis[2] = {z0.data(), z1.data()};
+    return kl_run(c, dom, pair, 2, xis, K, out);
+}
 
 }  // extern "C"

@@ -115,6 +115,39 @@ INT_FIELDS = {"type", "matype", "permtype", "etype"}
 PREC_FP64 = 0          # SPHGPU_PREC_FP64
 PREC_FP32_BULK = 1     # SPHGPU_PREC_FP32_BULK
 
+class KLField(C.Structure):
+    """sphgpu_kl_field: Para_SpatialVariability's members the K-L generators read."""
+    _fields_ = [("no", C.c_int), ("type", C.c_int), ("mean_value", C.c_double), ("sd_value", C.c_double),
+                ("rl_value", C.c_double * 3), ("coe_depth", C.c_double)]
+
+
+class KLDomain(C.Structure):
+    """sphgpu_kl_domain: the Cell_Con members the K-L generators read."""
+    _fields_ = [("xmin_nb", C.c_double), ("xmax_nb", C.c_double), ("ymin_nb", C.c_double),
+                ("ymax_nb", C.c_double), ("zmin_nb", C.c_double), ("zmax_nb", C.c_double),
+                ("soil_max", C.c_double * 3), ("water_max", C.c_double * 3)]
+
+
+def kl_field(no: int, type: int, mean: float, sd: float, rl, coe_depth: float = 0.0) -> KLField:
+    f = KLField()
+    f.no, f.type, f.mean_value, f.sd_value, f.coe_depth = int(no), int(type), float(mean), float(sd), float(coe_depth)
+    for d in range(3):
+        f.rl_value[d] = float(rl[d]) if d < len(rl) else 0.0
+    return f
+
+
+def kl_domain(nb_min, nb_max, soil_max, water_max) -> KLDomain:
+    """soil_max / water_max: 3 values each, or one value for the depth axis
+    (y in 2-D, z in 3-D), which is the only component the generators read."""
+    d = KLDomain()
+    d.xmin_nb, d.ymin_nb, d.zmin_nb = (float(v) for v in nb_min)
+    d.xmax_nb, d.ymax_nb, d.zmax_nb = (float(v) for v in nb_max)
+    for k in range(3):
+        d.soil_max[k] = float(soil_max[k]) if hasattr(soil_max, "__len__") else float(soil_max)
+        d.water_max[k] = float(water_max[k]) if hasattr(water_max, "__len__") else float(water_max)
+    return d
+
+
 ERRORS = {0: "ok", 3: "particle outside the cell grid", 5: "more than 99 neighbours",
           100: "bad argument", 101: "CUDA error", 102: "no CUDA device", 103: "unsupported flags",
           104: "call order"}
@@ -168,6 +201,10 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_stage_name.argtypes = [C.c_int]
     lib.sphgpu_step_profiled.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
     lib.sphgpu_set_precision.argtypes = [C.c_void_p, C.c_int]
+    lib.sphgpu_kl_generate.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_int, C.c_void_p,
+                                       C.c_int, C.c_void_p]
+    lib.sphgpu_kl_generate_corr.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_double,
+                                            C.c_void_p, C.c_int, C.c_void_p]
     lib.sphgpu_get_precision.argtypes = [C.c_void_p]
     _lib = lib
     return lib
@@ -230,6 +267,28 @@ class Engine:
                 self.set_field(name, v)
         if fluid is not None or soil is not None:
             self.set_materials(fluid, soil)
+
+    def kl_generate(self, domain: KLDomain, fields, xi, K: int = 200) -> np.ndarray:
+        """SpatialVariables_Generate_2D / _3D with the standard normals xi
+        (len(fields) x K); returns the fields (len(fields) x ntotal, NaN where a
+        field writes none), which also become the particles' material values."""
+        fields = list(fields)
+        arr = (KLField * len(fields))(*fields)
+        x = np.ascontiguousarray(np.asarray(xi, dtype=np.float64).reshape(len(fields) * K))
+        out = np.empty(len(fields) * self.n)
+        self._check(self.lib.sphgpu_kl_generate(self.h, C.byref(domain), arr, len(fields), _ptr(x), int(K), _ptr(out)),
+                    "sphgpu_kl_generate")
+        return out.reshape(len(fields), self.n)
+
+    def kl_generate_corr(self, domain: KLDomain, friction: KLField, cohesion: KLField, coe: float, u2,
+                         K: int = 200) -> np.ndarray:
+        """SpatialVariables_Generate_*_corr for one phase; u2: K x 2 normals."""
+        arr = (KLField * 2)(friction, cohesion)
+        u = np.ascontiguousarray(np.asarray(u2, dtype=np.float64).reshape(2 * K))
+        out = np.empty(2 * self.n)
+        self._check(self.lib.sphgpu_kl_generate_corr(self.h, C.byref(domain), arr, float(coe), _ptr(u), int(K),
+                                                     _ptr(out)), "sphgpu_kl_generate_corr")
+        return out.reshape(2, self.n)
 
     def set_precision(self, mode: int) -> None:
         """PREC_FP64 (the reference's arithmetic) or PREC_FP32_BULK."""
