@@ -275,6 +275,23 @@ int sphgpu_kl_generate_corr(sphgpu_ctx* ctx, const sphgpu_kl_domain* dom, const 
                             double coe_frict_cohesion, const double* u2, int K, double* out);
 
 /*
+ * Batched synthesis of R realisations of one field on the context's particles
+ * (the Monte Carlo use of the generator above: R runs of
+ * SpatialVariables_Generate_2D / _3D on one geometry, each with its own
+ * normals).  xi: R x K standard normals (host); d_out: a DEVICE buffer of
+ * R x ntotal floats receiving field value [r * ntotal + i] (NaN where the
+ * field writes none).  The sum over the K terms runs on the tensor cores as
+ * an FP32-accurate product of TF32 operand halves; values agree with the FP64
+ * generator to FP32 rounding.  R must be a multiple of 16 and K of 8.
+ * kernel_ms, if non-NULL, receives the device time of the synthesis kernels.
+ * Returns 0, 13, 14, SPHGPU_E_ARG, or SPHGPU_E_KL_TIMEOUT if a tensor-core
+ * completion wait expired (the outputs are then incomplete).
+ */
+#define SPHGPU_E_KL_TIMEOUT 105
+int sphgpu_kl_synthesize(sphgpu_ctx* ctx, const sphgpu_kl_domain* dom, const sphgpu_kl_field* field,
+                         const double* xi, int R, int K, float* d_out, double* kernel_ms);
+
+/*
  * Neighbour search that allocates no device memory (no counterpart in the
  * reference: an addition of this library).
  *

@@ -31,6 +31,12 @@ extern "C" int sphk_kl_field(int n, int ndim, int K, int no, int type, const dou
                              const int* d_type, const void* d_terms, const double* d_sqrt_eig, const double* d_xi,
                              double* d_out, cudaStream_t st);
 extern "C" size_t sphk_kl_term_bytes(void);
+extern "C" size_t sphk_kl_tc_term_bytes(void);
+extern "C" int sphk_kl_synthesize(int n, int ndim, int K, int R, int no, int type, const double* x_trans,
+                                  double mean_value, double sd_value, double coe_depth, double soil_max,
+                                  double water_max, const double* d_xh, const int* d_type, const void* d_terms,
+                                  const double* d_sqrt_eig, const double* d_xi, float* c_hi, float* c_lo,
+                                  float* d_out, int* d_err, cudaStream_t st);
 
 namespace {
 
@@ -267,6 +273,7 @@ const char* sphgpu_error_string(int code)
     case SPHGPU_E_NODEVICE: return "no CUDA device";
     case SPHGPU_E_UNSUPPORTED: return "flag combination not supported by the engine";
     case SPHGPU_E_STATE: return "call order (state not uploaded)";
+    case SPHGPU_E_KL_TIMEOUT: return "a tensor-core completion wait expired";
     default: return "unknown error";
     }
 }
@@ -806,13 +813,16 @@ void kl_solve_wi(std::vector<double>& wi, const double a_x[3], const double rl[3
 
 struct HostKLTerm { double w, alpha; int use_cos; int pad; };
 
-// One field of SpatialVariables_Generate_2D / _3D for the context's
-// particles; d_out receives the values (NaN where the field writes none).
-int kl_one_field(sphgpu_ctx* c, const double a[3], const double x_trans[3], double soil_max, double water_max,
-                 const sphgpu_kl_field& f, const double* xi, int K, double* d_out)
+// The expansion of one field: per term the selected 1-D root, normalisation
+// and parity on each axis, and sqrt(lambda); terms in the reference's order.
+struct KLPlan {
+    std::vector<HostKLTerm> terms;   // K x ndim
+    std::vector<double> sqrt_eig;    // K
+};
+
+int kl_plan(sphgpu_ctx* c, const double a[3], const sphgpu_kl_field& f, int K, KLPlan& plan)
 {
     const int nd = c->P.ndim;
-    if (f.type != 1 && f.type != 2) return 14;
     std::vector<double> wi;
     kl_solve_wi(wi, a, f.rl_value, nd, K);
     // 1-D eigenvalues (equation_ramdai, CPP_17-1:36-41)
@@ -831,10 +841,7 @@ int kl_one_field(sphgpu_ctx* c, const double a[3], const double x_trans[3], doub
     const size_t off_vi = off_ko + 256 * ((8 * total + 255) / 256);
     const size_t off_vo = off_vi + 256 * ((4 * total + 255) / 256);
     const size_t off_tmp = off_vo + 256 * ((4 * total + 255) / 256);
-    const size_t off_terms = off_tmp + 256 * ((sort_bytes + 255) / 256);
-    const size_t off_se = off_terms + 256 * ((sphk_kl_term_bytes() * 3 * K + 255) / 256);
-    const size_t off_xi = off_se + 256 * ((8 * (size_t)K + 255) / 256);
-    const size_t bytes = off_xi + 8 * (size_t)K;
+    const size_t bytes = off_tmp + sort_bytes;
     CK(cudaMalloc(&buf, bytes));
     char* b = (char*)buf;
     int rc = 0;
@@ -856,8 +863,10 @@ int kl_one_field(sphgpu_ctx* c, const double a[3], const double x_trans[3], doub
             cuda_fail(c, cudaStreamSynchronize(c->st), "cudaStreamSynchronize")) { rc = SPHGPU_E_CUDA; break; }
         // the terms: per axis the root of the selected 1-D index, its
         // normalisation (solve_faii, CPP_17-1:44-59) and cos / sin parity
-        std::vector<HostKLTerm> terms((size_t)K * nd);
-        std::vector<double> se(K);
+        std::vector<HostKLTerm>& terms = plan.terms;
+        std::vector<double>& se = plan.sqrt_eig;
+        terms.assign((size_t)K * nd, HostKLTerm{});
+        se.assign(K, 0.0);
         for (int j = 0; j < K; j++) {
             int id[3];
             if (nd == 2) { id[0] = (int)(idx[j] / K); id[1] = (int)(idx[j] % K); }
@@ -877,20 +886,58 @@ int kl_one_field(sphgpu_ctx* c, const double a[3], const double x_trans[3], doub
             }
             se[j] = std::sqrt(eig[j]);
         }
-        if (cuda_fail(c, cudaMemcpyAsync(b + off_terms, terms.data(), sizeof(HostKLTerm) * terms.size(),
+    } while (0);
+    cudaFree(buf);
+    return rc;
+}
+
+// One field of SpatialVariables_Generate_2D / _3D for the context's
+// particles; d_out receives the values (NaN where the field writes none).
+int kl_one_field(sphgpu_ctx* c, const double a[3], const double x_trans[3], double soil_max, double water_max,
+                 const sphgpu_kl_field& f, const double* xi, int K, double* d_out)
+{
+    const int nd = c->P.ndim;
+    if (f.type != 1 && f.type != 2) return 14;
+    KLPlan plan;
+    int rc = kl_plan(c, a, f, K, plan);
+    if (rc) return rc;
+    void* buf = nullptr;
+    const size_t off_se = 256 * ((sizeof(HostKLTerm) * plan.terms.size() + 255) / 256);
+    const size_t off_xi = off_se + 256 * ((8 * (size_t)K + 255) / 256);
+    CK(cudaMalloc(&buf, off_xi + 8 * (size_t)K));
+    char* b = (char*)buf;
+    do {
+        if (cuda_fail(c, cudaMemcpyAsync(b, plan.terms.data(), sizeof(HostKLTerm) * plan.terms.size(),
                                          cudaMemcpyHostToDevice, c->st), "cudaMemcpyAsync") ||
-            cuda_fail(c, cudaMemcpyAsync(b + off_se, se.data(), 8 * (size_t)K, cudaMemcpyHostToDevice, c->st),
-                      "cudaMemcpyAsync") ||
+            cuda_fail(c, cudaMemcpyAsync(b + off_se, plan.sqrt_eig.data(), 8 * (size_t)K, cudaMemcpyHostToDevice,
+                                         c->st), "cudaMemcpyAsync") ||
             cuda_fail(c, cudaMemcpyAsync(b + off_xi, xi, 8 * (size_t)K, cudaMemcpyHostToDevice, c->st),
                       "cudaMemcpyAsync")) { rc = SPHGPU_E_CUDA; break; }
         const DevState& s = c->d[c->parity].s;
         if (sphk_kl_field(c->N, nd, K, f.no, f.type, x_trans, f.mean_value, f.sd_value, f.coe_depth, soil_max,
-                          water_max, s.xh, s.type, b + off_terms, (const double*)(b + off_se),
-                          (const double*)(b + off_xi), d_out, c->st)) { rc = SPHGPU_E_CUDA; break; }
+                          water_max, s.xh, s.type, b, (const double*)(b + off_se), (const double*)(b + off_xi),
+                          d_out, c->st)) { rc = SPHGPU_E_CUDA; break; }
         if (cuda_fail(c, cudaStreamSynchronize(c->st), "cudaStreamSynchronize")) { rc = SPHGPU_E_CUDA; break; }
     } while (0);
     cudaFree(buf);
     return rc;
+}
+
+// the field domain: the non-boundary box widened by 20% per side
+// (CPP_17-1:70-90, 166-186); soil_max / water_max along y (2-D) or z (3-D)
+int kl_dom(int nd, const sphgpu_kl_domain* dom, double a[3], double xt[3], double* soil_max, double* water_max)
+{
+    const double lo[3] = {dom->xmin_nb, dom->ymin_nb, dom->zmin_nb};
+    const double hi[3] = {dom->xmax_nb, dom->ymax_nb, dom->zmax_nb};
+    for (int d = 0; d < 3; d++) a[d] = xt[d] = 0.0;
+    for (int d = 0; d < nd; d++) {
+        const double xmin = lo[d] - 0.2 * (hi[d] - lo[d]), xmax = hi[d] + 0.2 * (hi[d] - lo[d]);
+        xt[d] = (xmax + xmin) / 2.0;
+        a[d] = (xmax - xmin) / 2.0;
+    }
+    *soil_max = dom->soil_max[nd == 2 ? 1 : 2];
+    *water_max = dom->water_max[nd == 2 ? 1 : 2];
+    return (a[0] == 0.0 || a[1] == 0.0) ? 13 : 0;
 }
 
 int kl_run(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_kl_field* fields, int nfields,
@@ -905,18 +952,8 @@ int kl_run(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_kl_field* fi
     }
     cudaSetDevice(c->device);
     const int nd = c->P.ndim, N = c->N;
-    // the field domain: the non-boundary box widened by 20% per side
-    // (CPP_17-1:70-90, 166-186); soil_max / water_max along y (2-D) or z (3-D)
-    const double lo[3] = {dom->xmin_nb, dom->ymin_nb, dom->zmin_nb};
-    const double hi[3] = {dom->xmax_nb, dom->ymax_nb, dom->zmax_nb};
-    double a[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
-    for (int d = 0; d < nd; d++) {
-        const double xmin = lo[d] - 0.2 * (hi[d] - lo[d]), xmax = hi[d] + 0.2 * (hi[d] - lo[d]);
-        xt[d] = (xmax + xmin) / 2.0;
-        a[d] = (xmax - xmin) / 2.0;
-    }
-    if (a[0] == 0.0 || a[1] == 0.0) return 13;
-    const double soil_max = dom->soil_max[nd == 2 ? 1 : 2], water_max = dom->water_max[nd == 2 ? 1 : 2];
+    double a[3], xt[3], soil_max, water_max;
+    if (kl_dom(nd, dom, a, xt, &soil_max, &water_max)) return 13;
     double* d_out = nullptr;
     CK(cudaMalloc(&d_out, sizeof(double) * N));
     std::vector<double> v(N);
@@ -985,6 +1022,75 @@ int sphgpu_kl_generate_corr(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sp
     }
     const double* xis[2] = {z0.data(), z1.data()};
     return kl_run(c, dom, pair, 2, xis, K, out);
+}
+
+
+int sphgpu_kl_synthesize(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_kl_field* f, const double* xi,
+                         int R, int K, float* d_out, double* kernel_ms)
+{
+    if (!c || !dom || !f || !xi || !d_out || R <= 0 || R % 16 != 0 || K < 8 || K % 8 != 0) return SPHGPU_E_ARG;
+    if (f->no < 0 || f->no > 5) return SPHGPU_E_ARG;
+    if (f->type != 1 && f->type != 2) return 14;
+    if (c->h_type.empty()) return SPHGPU_E_STATE;
+    cudaSetDevice(c->device);
+    const int nd = c->P.ndim, N = c->N;
+    double a[3], xt[3], soil_max, water_max;
+    if (kl_dom(nd, dom, a, xt, &soil_max, &water_max)) return 13;
+    KLPlan plan;
+    int rc = kl_plan(c, a, *f, K, plan);
+    if (rc) return rc;
+    // the tensor-core kernel's term record: w (FP64), alpha (FP32), parity
+    struct TCTerm { double w; float alpha; int use_cos; };
+    if (sphk_kl_tc_term_bytes() != sizeof(TCTerm)) return SPHGPU_E_ARG;
+    std::vector<TCTerm> tc(plan.terms.size());
+    for (size_t q = 0; q < tc.size(); q++)
+        tc[q] = TCTerm{plan.terms[q].w, (float)plan.terms[q].alpha, plan.terms[q].use_cos};
+    const int Rc = R < 256 ? R : 256;   // realisations per launch
+    const size_t off_se = 256 * ((sizeof(TCTerm) * tc.size() + 255) / 256);
+    const size_t off_xi = off_se + 256 * ((8 * (size_t)K + 255) / 256);
+    const size_t off_ch = off_xi + 256 * ((8 * (size_t)Rc * K + 255) / 256);
+    const size_t off_cl = off_ch + 256 * ((4 * (size_t)Rc * K + 255) / 256);
+    const size_t off_err = off_cl + 256 * ((4 * (size_t)Rc * K + 255) / 256);
+    void* buf = nullptr;
+    CK(cudaMalloc(&buf, off_err + 16));
+    char* b = (char*)buf;
+    float total_ms = 0.f;
+    do {
+        if (cuda_fail(c, cudaMemcpyAsync(b, tc.data(), sizeof(TCTerm) * tc.size(), cudaMemcpyHostToDevice, c->st),
+                      "cudaMemcpyAsync") ||
+            cuda_fail(c, cudaMemcpyAsync(b + off_se, plan.sqrt_eig.data(), 8 * (size_t)K, cudaMemcpyHostToDevice,
+                                         c->st), "cudaMemcpyAsync") ||
+            cuda_fail(c, cudaMemsetAsync(b + off_err, 0, 16, c->st), "cudaMemsetAsync")) { rc = SPHGPU_E_CUDA; break; }
+        const DevState& s = c->d[c->parity].s;
+        for (int r0 = 0; r0 < R && !rc; r0 += Rc) {
+            const int rr = (R - r0) < Rc ? (R - r0) : Rc;
+            if (cuda_fail(c, cudaMemcpyAsync(b + off_xi, xi + (size_t)r0 * K, 8 * (size_t)rr * K,
+                                             cudaMemcpyHostToDevice, c->st), "cudaMemcpyAsync")) { rc = SPHGPU_E_CUDA; break; }
+            cudaEventRecord(c->ev0, c->st);
+            if (sphk_kl_synthesize(N, nd, K, rr, f->no, f->type, xt, f->mean_value, f->sd_value, f->coe_depth,
+                                   soil_max, water_max, s.xh, s.type, b, (const double*)(b + off_se),
+                                   (const double*)(b + off_xi), (float*)(b + off_ch), (float*)(b + off_cl),
+                                   d_out + (size_t)r0 * N, (int*)(b + off_err), c->st)) {
+                rc = cuda_fail(c, cudaGetLastError(), "K-L synthesis launch");
+                if (!rc) rc = SPHGPU_E_ARG;
+                break;
+            }
+            cudaEventRecord(c->ev1, c->st);
+            if (cuda_fail(c, cudaStreamSynchronize(c->st), "cudaStreamSynchronize")) { rc = SPHGPU_E_CUDA; break; }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+            total_ms += ms;
+            int err = 0;
+            if (cuda_fail(c, cudaMemcpy(&err, b + off_err, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy")) {
+                rc = SPHGPU_E_CUDA;
+                break;
+            }
+            if (err) rc = err;
+        }
+    } while (0);
+    cudaFree(buf);
+    if (kernel_ms) *kernel_ms = total_ms;
+    return rc;
 }
 
 }  // extern "C"

@@ -150,7 +150,7 @@ def kl_domain(nb_min, nb_max, soil_max, water_max) -> KLDomain:
 
 ERRORS = {0: "ok", 3: "particle outside the cell grid", 5: "more than 99 neighbours",
           100: "bad argument", 101: "CUDA error", 102: "no CUDA device", 103: "unsupported flags",
-          104: "call order"}
+          104: "call order", 105: "tensor-core wait expired"}
 
 
 class SPHError(RuntimeError):
@@ -203,6 +203,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_set_precision.argtypes = [C.c_void_p, C.c_int]
     lib.sphgpu_kl_generate.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_int, C.c_void_p,
                                        C.c_int, C.c_void_p]
+    lib.sphgpu_kl_synthesize.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_void_p, C.c_int,
+                                         C.c_int, C.c_void_p, C.POINTER(C.c_double)]
     lib.sphgpu_kl_generate_corr.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_double,
                                             C.c_void_p, C.c_int, C.c_void_p]
     lib.sphgpu_get_precision.argtypes = [C.c_void_p]
@@ -279,6 +281,17 @@ class Engine:
         self._check(self.lib.sphgpu_kl_generate(self.h, C.byref(domain), arr, len(fields), _ptr(x), int(K), _ptr(out)),
                     "sphgpu_kl_generate")
         return out.reshape(len(fields), self.n)
+
+    def kl_synthesize(self, domain: KLDomain, field: KLField, xi, d_out: int, K: int = 200) -> float:
+        """R realisations of one field (xi: R x K normals) into the device
+        buffer at address d_out (R x ntotal float32) on the tensor cores;
+        returns the kernels' device time in ms."""
+        x = np.ascontiguousarray(np.asarray(xi, dtype=np.float64))
+        R = x.size // K
+        ms = C.c_double(0.0)
+        self._check(self.lib.sphgpu_kl_synthesize(self.h, C.byref(domain), C.byref(field), _ptr(x), int(R), int(K),
+                                                  C.c_void_p(int(d_out)), C.byref(ms)), "sphgpu_kl_synthesize")
+        return ms.value
 
     def kl_generate_corr(self, domain: KLDomain, friction: KLField, cohesion: KLField, coe: float, u2,
                          K: int = 200) -> np.ndarray:
