@@ -27,6 +27,9 @@ struct orc_ctx {
     double *satu, *dsatu, *suct, *cop, *vsig, *veps, *divq, *divr, *meps;
     double *prew, *prea, *porosity, *cd, *poro_cop, *beta, *beta_ts;
     int *type, *matype, *permtype, *etype;
+    /* cl_bndy_pair::vel_bndy and clVar_Boundary::vx_* (Class_particle.h:172-207),
+     * the wall virtual velocities of flbndy 2 */
+    double *vel_bndy, *vb_water, *vb_soil, *vb_air, *vb_struct;
     /* per-particle material records (pVFluid, pParti_ConsPara) */
     sphgpu_fluid* fl;
     sphgpu_soil* so;
@@ -58,6 +61,7 @@ static const field_desc k_fields[] = {
     FD(divq, 1), FD(divr, 1), FD(meps, 1), FD(prew, 1), FD(prea, 1), FD(porosity, 1),
     FD(cd, 1), FD(poro_cop, 1), FD(beta, 9), FD(beta_ts, 9),
     FI(type), FI(matype), FI(permtype), FI(etype),
+    FD(vel_bndy, 3), FD(vb_water, 3), FD(vb_soil, 3), FD(vb_air, 3), FD(vb_struct, 3),
 };
 #define NFIELDS (sizeof(k_fields) / sizeof(k_fields[0]))
 
@@ -358,10 +362,26 @@ static int partisearching(orc_ctx* c)
 
 /* ------------------------------------------------------------------------- */
 /* density: CPP_6-density.cpp:11-189                                          */
+/* the virtual velocity of wall particle j seen by particle i: its own
+ * velocity (flbndy 1) or the wall's clVar_Boundary velocity for i's phase
+ * (flbndy 2/3/4/13/14), CPP_6-density.cpp:89-121, CPP_7-1-strain.cpp:92-124 */
+static void wall_velocity(const orc_ctx* c, int i, int j, double vxj[3])
+{
+    const int bt = c->P.flbndy, ti = c->type[i];
+    vxj[0] = vxj[1] = vxj[2] = 0.0;
+    if (bt == 1) {
+        for (int k = 0; k < 3; k++) vxj[k] = c->vxp[i * 3 + k];
+    } else if (bt == 2 || bt == 3 || bt == 4 || bt == 13 || bt == 14) {
+        const double* v = ti == 1 ? c->vb_water : ti == 2 ? c->vb_soil : ti == 3 ? c->vb_air : ti == 4 ? c->vb_struct : 0;
+        if (v)
+            for (int k = 0; k < 3; k++) vxj[k] = v[j * 3 + k];
+    }
+}
+
 static void density(orc_ctx* c)
 {
     const sphgpu_params* P = &c->P;
-    int n = c->n, ndim = P->ndim, l = c->l, bndytype = P->flbndy;
+    int n = c->n, ndim = P->ndim, l = c->l;
     double dt = P->dt;
     /* fluid porosity from soil neighbours (:25-54) */
     for (int i = 0; i < n; i++) {
@@ -399,11 +419,7 @@ static void density(orc_ctx* c)
                         up[k] = up[k] + c->mass[j] * (c->vxp[i * 3 + k] - c->vxp[j * 3 + k]) * W(i, nj, k);
                 }
             } else if ((ti == 1 || ti == 2 || ti == 3 || ti == 4) && c->type[j] == 0) {
-                vxj[0] = vxj[1] = vxj[2] = 0.0;
-                if (bndytype == 1) {
-                    vxj[0] = c->vxp[i * 3 + 0]; vxj[1] = c->vxp[i * 3 + 1]; vxj[2] = c->vxp[i * 3 + 2];
-                }
-                /* bndytype 2/3/4/13/14 read clVar_Boundary: not restated (flbndy 1 only) */
+                wall_velocity(c, i, j, vxj);
                 if (ti == 2 || ti == 4) {
                     for (k = 0; k < ndim; k++) {
                         up[k] = up[k] + c->mass[j] * (c->vxp[i * 3 + k] - vxj[k]) * W(i, nj, k);
@@ -460,7 +476,7 @@ static void density(orc_ctx* c)
 static void strain_noreg(orc_ctx* c)
 {
     const sphgpu_params* P = &c->P;
-    int n = c->n, dim = P->ndim, bndytype = P->flbndy;
+    int n = c->n, dim = P->ndim;
     for (int i = 0; i < n; i++) {
         double dvx[3], up[9], vxj[3], down[3];
         int j, k;
@@ -478,10 +494,7 @@ static void strain_noreg(orc_ctx* c)
                 for (k = 0; k < 3; k++) dvx[k] = c->vxp[i * 3 + k] - c->vxp[j * 3 + k];
                 touch = 1;
             } else if ((ti == 1 || ti == 2 || ti == 3 || ti == 4) && c->type[j] == 0) {
-                vxj[0] = vxj[1] = vxj[2] = 0.0;
-                if (bndytype == 1) {
-                    vxj[0] = c->vxp[i * 3 + 0]; vxj[1] = c->vxp[i * 3 + 1]; vxj[2] = c->vxp[i * 3 + 2];
-                }
+                wall_velocity(c, i, j, vxj);
                 for (k = 0; k < 3; k++) dvx[k] = c->vxp[i * 3 + k] - vxj[k];
                 touch = 1;
             }
@@ -1638,6 +1651,167 @@ static void tmboundary(orc_ctx* c)
     }
 }
 
+/* velocity_set_domain: CPP_13-boundary.cpp:71-122, fluid particles only, with
+ * a = b = coe_bndy */
+static void velocity_set_domain(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    int ndim = P->ndim;
+    double dr = P->dr, a = P->coe_bndy, b = P->coe_bndy;
+    for (int i = 0; i < c->n; i++) {
+        if (!(c->type[i] == 1 || c->type[i] == 3)) continue;
+        double tu[3] = {0, 0, 0};
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj), k;
+            if (c->type[j] != 0) continue;
+            double inprod = 0.0, dst = 0.0;
+            for (k = 0; k < ndim; k++) {
+                inprod = inprod + (c->vx[i * 3 + k] - c->interfss[j * 3 + k]) * (c->xp[i * 3 + k] - c->xp[j * 3 + k]);
+                dst = dst + (c->xp[i * 3 + k] - c->xp[j * 3 + k]) * (c->xp[i * 3 + k] - c->xp[j * 3 + k]);
+            }
+            if (inprod < 0.0) {
+                dst = sqrt(dst);
+                double db = a * dr;
+                double beta = 1 + db / (dst - b * dr);
+                beta = fmin(1.5, beta);
+                for (k = 0; k < ndim; k++)
+                    tu[k] = tu[k] + (1 - beta) * (c->xp[i * 3 + k] - c->xp[j * 3 + k]) * inprod / dst / dst;
+            }
+        }
+        for (int k = 0; k < ndim; k++) c->vx[i * 3 + k] = c->vx[i * 3 + k] + tu[k];
+    }
+}
+
+/* the wall particles of i's list in list order with their distances, sorted
+ * as clParti_Pair::dist_sorting does (Class_particle.cpp:343-359): four
+ * passes that swap the ids but not the distances */
+static int wall_pairs_sorted(const orc_ctx* c, int i, int* ids, int* last_id)
+{
+    double dsts[NB];
+    int k = 0;
+    *last_id = 0;
+    for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+        int j = NBR(i, nj);
+        if (c->type[j] != 0) continue;
+        double dx = c->xp[i * 3] - c->xp[j * 3], dy = c->xp[i * 3 + 1] - c->xp[j * 3 + 1];
+        double dz = c->xp[i * 3 + 2] - c->xp[j * 3 + 2];
+        double d = dx * dx + dy * dy + dz * dz;
+        ids[k] = j;
+        dsts[k] = sqrt(d);
+        k++;
+        if (c->matype[j] > 2) *last_id = j;
+    }
+    for (int a = 0; a < 4; a++)
+        for (int b = a + 1; b < k; b++)
+            if (dsts[a] > dsts[b]) { int t = ids[a]; ids[a] = ids[b]; ids[b] = t; }
+    return k;
+}
+
+/* tm_boundary_2d / tm_boundary_3d: CPP_13-boundary.cpp:179-615.  The line of
+ * the two nearest walls (2-D) keeps the C = 1 of clLine() (cal_line sets only
+ * A and B); the plane through the three nearest walls (3-D) keeps the D its
+ * variable last held: 1 from clPlane(), or the value plane_two_points set,
+ * which persists through later particles of the same loop in the reference
+ * (ORC_INPLACE); in ORC_JACOBI order every particle starts from D = 1.  The
+ * walls' Shepard sums keep the reference's [0][0] index in components 1 and 2. */
+static void tm_boundary(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    const int nd = P->ndim;
+    const double dr = P->dr;
+    double plane_d = 1.0;
+    int ids[NB];
+    for (int i = 0; i < c->n; i++) {
+        int ti = c->type[i];
+        if (ti == 0 || ti == 7) continue;
+        int id = 0;
+        int total = wall_pairs_sorted(c, i, ids, &id);
+        double* vb = &c->vel_bndy[i * 3];
+        const double* vi = &c->vx[i * 3];
+        if (total >= (nd == 2 ? 2 : 3)) {
+            const double* p4 = &c->xp[i * 3];
+            const double* p1 = &c->xp[ids[0] * 3];
+            const double* p2 = &c->xp[ids[1] * 3];
+            double dst;
+            if (nd == 2) {
+                /* cal_line (:645-650) and cal_dpline (:617-628) */
+                double den = p2[1] * p1[0] - p1[1] * p2[0];
+                double A = (p1[1] - p2[1]) / den, B = (p2[0] - p1[0]) / den, C = 1.0;
+                double num = fabs(A * p4[0] + B * p4[1] + C);
+                double tmp = sqrt(A * A + B * B);
+                dst = (tmp > 1.0e-3) ? num / tmp : 0.0;
+            } else {
+                const double* p3 = &c->xp[ids[2] * 3];
+                double pc1[3], pc2[3], A, B, C;
+                /* cal_plane (:653-666) of (p1, p2, p4) and (p1, p3, p4) */
+                double den1 = -p1[0] * (p2[1] * p4[2] - p4[1] * p2[2]) - p2[0] * (p4[1] * p1[2] - p1[1] * p4[2]) -
+                              p4[0] * (p1[1] * p2[2] - p2[1] * p1[2]);
+                pc1[0] = p1[1] * (p2[2] - p4[2]) + p2[1] * (p4[2] - p1[2]) + p4[1] * (p1[2] - p2[2]);
+                pc1[1] = p1[2] * (p2[0] - p4[0]) + p2[2] * (p4[0] - p1[0]) + p4[2] * (p1[0] - p2[0]);
+                pc1[2] = p1[0] * (p2[1] - p4[1]) + p2[0] * (p4[1] - p1[1]) + p4[0] * (p1[1] - p2[1]);
+                pc1[0] = pc1[0] / den1; pc1[1] = pc1[1] / den1; pc1[2] = pc1[2] / den1;
+                double den2 = -p1[0] * (p3[1] * p4[2] - p4[1] * p3[2]) - p3[0] * (p4[1] * p1[2] - p1[1] * p4[2]) -
+                              p4[0] * (p1[1] * p3[2] - p3[1] * p1[2]);
+                pc2[0] = p1[1] * (p3[2] - p4[2]) + p3[1] * (p4[2] - p1[2]) + p4[1] * (p1[2] - p3[2]);
+                pc2[1] = p1[2] * (p3[0] - p4[0]) + p3[2] * (p4[0] - p1[0]) + p4[2] * (p1[0] - p3[0]);
+                pc2[2] = p1[0] * (p3[1] - p4[1]) + p3[0] * (p4[1] - p1[1]) + p4[0] * (p1[1] - p3[1]);
+                pc2[0] = pc2[0] / den2; pc2[1] = pc2[1] / den2; pc2[2] = pc2[2] / den2;
+                double cs = pc1[0] * pc2[0] + pc1[1] * pc2[1] + pc1[2] * pc2[2];
+                cs = cs / sqrt(pc1[0] * pc1[0] + pc1[1] * pc1[1] + pc1[2] * pc1[2]) /
+                     sqrt(pc2[0] * pc2[0] + pc2[1] * pc2[1] + pc2[2] * pc2[2]);
+                if (c->mode == ORC_JACOBI) plane_d = 1.0;
+                if (fabs(cs) > 0.999999) {
+                    /* plane_two_points(p4, p1) (:684-708) */
+                    double a = p4[0] - p1[0], b = p4[1] - p1[1], cc = p4[2] - p1[2];
+                    double tmp = -a * p1[0] - b * p1[1] - cc * p1[2];
+                    if (fabs(tmp) > 1.0e-6) { A = a / tmp; B = b / tmp; C = cc / tmp; plane_d = 1.0; }
+                    else { A = a; B = b; C = cc; plane_d = 0.0; }
+                } else {
+                    double den = -p1[0] * (p2[1] * p3[2] - p3[1] * p2[2]) - p2[0] * (p3[1] * p1[2] - p1[1] * p3[2]) -
+                                 p3[0] * (p1[1] * p2[2] - p2[1] * p1[2]);
+                    A = p1[1] * (p2[2] - p3[2]) + p2[1] * (p3[2] - p1[2]) + p3[1] * (p1[2] - p2[2]);
+                    B = p1[2] * (p2[0] - p3[0]) + p2[2] * (p3[0] - p1[0]) + p3[2] * (p1[0] - p2[0]);
+                    C = p1[0] * (p2[1] - p3[1]) + p2[0] * (p3[1] - p1[1]) + p3[0] * (p1[1] - p2[1]);
+                    A = A / den; B = B / den; C = C / den;
+                }
+                /* cal_dpplane (:631-642) */
+                double num = fabs(A * p4[0] + B * p4[1] + C * p4[2] + plane_d);
+                double tmp = sqrt(A * A + B * B + C * C);
+                dst = (tmp > 1.0e-3) ? num / tmp : 0.0;
+            }
+            double da = (dst > 0.6 * dr) ? dst - 0.5 * dr : 0.1 * dr;
+            double db = 0.5 * dr, beta;
+            if (fabs(da) > 1.0e-6) { beta = 1.0 + db / da; beta = fmin(1.5, beta); }
+            else beta = 1.5;
+            const double* its = &c->interfss[id * 3];
+            vb[0] = (1.0 - beta) * vi[0] + beta * its[0];
+            vb[1] = (1.0 - beta) * vi[1] + beta * its[1];
+            vb[2] = (nd == 2) ? 0.0 : (1.0 - beta) * vi[2] + beta * its[2];
+        } else {
+            vb[0] = vi[0]; vb[1] = vi[1]; vb[2] = vi[2];
+        }
+    }
+    /* the walls: Shepard sums of the moving particles' virtual velocities per phase */
+    for (int i = 0; i < c->n; i++) {
+        if (c->type[i] != 0) continue;
+        double up[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, down[4] = {0, 0, 0, 0};
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj), tj = c->type[j];
+            if (tj < 1 || tj > 4) continue;
+            int p = tj - 1;
+            const double* vb = &c->vel_bndy[j * 3];
+            double w3 = W(i, nj, 3), mj = c->mass[j], rj = c->rho[j];
+            up[p][0] = up[p][0] + mj * vb[0] * w3 / rj;
+            up[p][1] = up[p][0] + mj * vb[1] * w3 / rj;
+            up[p][2] = up[p][0] + mj * vb[2] * w3 / rj;
+            down[p] = down[p] + mj * w3 / rj;
+        }
+        double* out[4] = {c->vb_water, c->vb_soil, c->vb_air, c->vb_struct};
+        for (int p = 0; p < 4; p++)
+            for (int k = 0; k < 3; k++) out[p][i * 3 + k] = (fabs(down[p]) > 1.0e-6) ? up[p][k] / down[p] : 0.0;
+    }
+}
+
 /* check_domain: CPP_13-boundary.cpp:20-68, in the sequential order (vbx is
  * taken from the first wall particle with matype > 2 and applies to the
  * particles after it) */
@@ -1777,7 +1951,7 @@ static void kernel_gradient_correction(orc_ctx* c)
 
 static int check_supported(const sphgpu_params* P)
 {
-    if (P->flbndy != 1) return SPHGPU_E_UNSUPPORTED;
+    if (P->flbndy != 1 && P->flbndy != 2) return SPHGPU_E_UNSUPPORTED;
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
     if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
     if (P->fli < 0 || P->fli > 3 || P->ss_type != 0) return SPHGPU_E_UNSUPPORTED;
@@ -1813,12 +1987,13 @@ int orc_step(orc_ctx* c, int nsteps)
         structure_acceleration(c);
         artificial_viscosity(c);
         if (P->art_stre_coe > 0.0) artificial_stress(c);
-        boundary_moving_stress_effect(c);    /* flv == 0, flbndy 1 */
+        boundary_moving_stress_effect(c);    /* flv == 0, flbndy 1 or 2 */
         if (P->fli >= 1) interact(c, P->fli);
         if (c->l <= P->inip) soil_damping_geostress(c);
         velocity_update(c);
         if (P->if_move != 2) xsph(c);
-        tmboundary(c);                        /* flbndy == 1 */
+        if (P->flbndy == 1) tmboundary(c);
+        else if (P->flbndy == 2) { velocity_set_domain(c); tm_boundary(c); }
         check_domain(c);
         update(c);
         c->l++;

@@ -30,7 +30,8 @@ ORC_POW_LIBM, ORC_POW_CR = 0, 1
 
 ORACLE_FIELDS = dict(FIELDS)
 ORACLE_FIELDS.update({"divx": 9, "deps": 6, "dsig": 6, "weps": 9, "dsatu": 1, "suct": 1,
-                      "cd": 1, "beta": 9, "beta_ts": 9})
+                      "cd": 1, "beta": 9, "beta_ts": 9, "vel_bndy": 3, "vb_water": 3, "vb_soil": 3,
+                      "vb_air": 3, "vb_struct": 3})
 
 
 def _ptr(a):

@@ -78,6 +78,16 @@ def _column_model(matype, **record):
     return lambda: scenes.set_soil_model(scenes.soil_column_3d(dx=0.1, steps=200), matype, **record)
 
 
+def _tm_boundary(factory):
+    """A scene with the Takeda-Morris wall treatment of flbndy 2
+    (velocity_set_domain + tm_boundary_2d / tm_boundary_3d, coe_bndy 0.3)."""
+    def make():
+        sc = factory()
+        sc.flags["flbndy"] = 2
+        return sc
+    return make
+
+
 CASES = {
     # name: (scene factory, steps)
     "dam_break_2d_dx0.04": (lambda: scenes.dam_break_2d(dx=0.04, steps=200), 25),
@@ -90,6 +100,8 @@ CASES = {
     "soil_column_3d_dx0.1_camclay": (_column_model(1, **MCC), 20),
     "soil_column_3d_dx0.1_mohr_coulomb": (_column_model(9, c=0.0, fai=30.0, e=1.0e7), 20),
     "soil_column_3d_dx0.1_visco_elastic": (_column_model(7, c=1.0e5, e=1.0e7), 20),
+    "dam_break_2d_dx0.04_tm_boundary": (_tm_boundary(lambda: scenes.dam_break_2d(dx=0.04, steps=200)), 25),
+    "soil_column_3d_dx0.1_tm_boundary": (_tm_boundary(lambda: scenes.soil_column_3d(dx=0.1, steps=200)), 15),
 }
 
 

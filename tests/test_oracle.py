@@ -17,7 +17,8 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ["dam_break_2d_dx0.04", "soil_column_3d_dx0.1", "soil_column_3d_dx0.1_kgc_regu",
          "slope_2d_H1_dx0.05_art_stress", "soil_column_3d_dx0.1_art_stress",
          "soil_column_3d_dx0.1_drag_tsuji_dilute", "soil_column_3d_dx0.1_drag_peng",
-         "soil_column_3d_dx0.1_camclay", "soil_column_3d_dx0.1_mohr_coulomb", "soil_column_3d_dx0.1_visco_elastic"]
+         "soil_column_3d_dx0.1_camclay", "soil_column_3d_dx0.1_mohr_coulomb", "soil_column_3d_dx0.1_visco_elastic",
+         "dam_break_2d_dx0.04_tm_boundary", "soil_column_3d_dx0.1_tm_boundary"]
 
 
 def _golden(name):
