@@ -43,29 +43,33 @@ import scenes  # noqa: E402
 METRIC = "particle-updates/s"
 WORKLOAD = "3d_saturated_soil_column_collapse"
 
-# Algorithmic bytes per particle and launch (FP64, 3-D), each kernel reading
-# its own particle's fields and neighbour-list row once and writing its
-# outputs once; neighbour fields are counted as cache-served.  NB is the mean
-# listed neighbours per particle (65 for co-located soil and water).
+# Algorithmic bytes per particle and launch (3-D), each kernel reading its
+# own particle's fields, its neighbour-list row and its pair records once and
+# writing its outputs once; neighbour fields are counted as cache-served.  NB
+# is the mean listed neighbours per particle (65 for co-located soil and
+# water); a pair record (grad W, W) is 32 bytes in FP64 and 16 in the
+# FP32-bulk form.
 NB_MEAN = 65
 
 
-def algorithmic_bytes(stage: str, nb: float = NB_MEAN) -> float:
+def algorithmic_bytes(stage: str, nb: float = NB_MEAN, rec_bytes: float = 32.0) -> float:
     row = 4.0 * nb                       # the particle's neighbour-list row
+    rec = rec_bytes * nb                 # the particle's pair records
     table = {
         # reads | writes
         "k_cellkey": 32 + 12,                                   # (x,y,z,h) | cell, key, value
         "radix_sort": 3 * 16,                                   # 3 digit passes of (key, value) in + out
-        "k_cellrange": 4 + 4 + 32 + 32 + 8,                     # key, pid, record | sorted record, range
+        "k_cellrange": 4 + 4 + 32 + 32 + 16 + 8,                # key, pid, record | sorted FP64 + FP32 records, range
         "k_nnps": 32 + 4 + 4 + 4 + row,                         # record, cell, type | count, list row
-        "k_density": 4 + 4 + 32 + 8 + 8 + 8 + 24 + 8 + row + 8 + 16,
-        "k_shepard_eos": 4 + 4 + 32 + 8 + 8 + 8 + 8 + row + 8 + 8,
-        "k_strain": 4 + 4 + 32 + 24 + row + 48 + 48 + 8 + 16,
+        "k_pairw": 32 + 4 + row + rec,                          # record, count, list row | pair records
+        "k_density": 4 + 4 + 32 + 8 + 8 + 8 + 24 + 8 + row + rec + 8 + 16,
+        "k_shepard_eos": 4 + 4 + 32 + 8 + 8 + 8 + 8 + row + rec + 8 + 8,
+        "k_strain": 4 + 4 + 32 + 24 + row + rec + 48 + 48 + 8 + 16,
         "k_stress": 48 + 48 + 48 + 48 + 8 + 4 + 4 + 8 + 8 + 88 + 48 + 8
                     + 48 + 48 + 48 + 8 + 8 + 40 + 24 + 48 + 8,
-        "k_accel_a": 4 + 4 + 32 + 8 + 48 + 8 + 8 + 8 + 8 + 8 + row + 24,
-        "k_accel_b": 4 + 4 + 32 + 8 + 24 + 48 + 24 + 24 + 24 + 24 + 4 + 8 + 8 + 8 + 24 + row + 24 + 24 + 24,
-        "k_xsph_update": 4 + 4 + 32 + 24 + 24 + 24 + 24 + 8 + 8 + 8 + 8 + 4 + row + 32 + 24 + 24 + 24 + 24 + 8,
+        "k_accel_a": 4 + 4 + 8 + 48 + 8 + 8 + 8 + 8 + 8 + row + rec + 24,
+        "k_accel_b": 4 + 4 + 32 + 8 + 24 + 48 + 24 + 24 + 24 + 24 + 4 + 8 + 8 + 8 + 24 + row + rec + 24 + 24 + 24,
+        "k_xsph_update": 4 + 4 + 32 + 24 + 24 + 24 + 24 + 8 + 8 + 8 + 8 + 4 + row + rec + 32 + 24 + 24 + 24 + 24 + 8,
     }
     return float(table.get(stage, 0.0))
 
@@ -260,12 +264,58 @@ STATE_DOWN = ("xp", "vxp", "axp", "ax", "vx", "ux", "rho", "rhop", "pre", "prep"
               "interfss", "vsig", "veps", "divq", "divr", "meps")
 
 
+def _rel_l2(a, b, m):
+    a, b = a[m], b[m]
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def bulk_form(st, args, device, ref_fields, moving):
+    """The FP32-bulk form on the same workload: K timed steps after the same
+    warm-up, and its state after warm-up + K steps against the FP64 form's."""
+    import sphgpu
+    eng = sphgpu.Engine(st.params, device=device)
+    eng.load_state(st.fields, st.fluid, st.soil)
+    eng.set_precision(sphgpu.PREC_FP32_BULK)
+    eng.step(args.warmup)
+    eng.synchronize()
+    eng.step(args.steps)
+    ms = eng.last_step_ms()
+    err = {k: _rel_l2(eng.get_field(k), ref_fields[k], moving) for k in ref_fields}
+    prof = eng.step_profiled(args.steps)
+    eng.close()
+    return ms, err, prof
+
+
+def kl_synthesis(eng, scene, device, R=32, K=400):
+    """R realisations of a K-term friction-angle field (normal, mean 30 deg,
+    COV 0.1, correlation lengths 0.5 / 0.25 / 0.25 m, depth trend) on the
+    workload's particles, on the tensor cores, into device memory."""
+    import sphgpu
+    import torch
+    d = scenes.kl_domain(scene)
+    dom = sphgpu.kl_domain(d["nb_min"], d["nb_max"], d["soil_max"], d["water_max"])
+    field = sphgpu.kl_field(0, 1, 30.0, 3.0, [0.5, 0.25, 0.25], 2.0)
+    xi = np.random.default_rng(20261203).standard_normal((R, K))
+    out = torch.empty(R * eng.n, dtype=torch.float32, device=f"cuda:{device}")
+    eng.kl_synthesize(dom, field, xi, out.data_ptr(), K)           # warm-up (plan + launch)
+    t0 = time.perf_counter()
+    ms = eng.kl_synthesize(dom, field, xi, out.data_ptr(), K)
+    wall = time.perf_counter() - t0
+    flops = 2.0 * eng.n * K * R * 3            # three TF32 products per term
+    del out
+    return {"realisations": R, "terms": K, "particles": eng.n, "kernel_ms": ms, "call_s": wall,
+            "tensor_tflops": flops / (ms / 1e3) / 1e12,
+            "fields_per_s": R / wall,
+            "what": "tcgen05 kind::tf32 split-operand product, eigenfunction tiles generated in shared memory"}
+
+
 def engine_arm(args, world, rank, local):
     import sphgpu
     scene = scenes.soil_column_3d(dx=args.dx, steps=5000)
     st = scenes.initialise(scene)
     n_active = scene.n_active()
-    eng = sphgpu.Engine(st.params, device=local if world > 1 else args.device)
+    device = local if world > 1 else args.device
+    eng = sphgpu.Engine(st.params, device=device)
     eng.load_state(st.fields, st.fluid, st.soil)
     eng.step(args.warmup)
     barrier(world)
@@ -280,6 +330,8 @@ def engine_arm(args, world, rank, local):
     total_active = dist_sum(float(n_active), world)
     value = total_active * args.steps / (ms_max / 1e3)
 
+    moving = (st.fields["type"] >= 1) & (st.fields["type"] <= 4)
+    ref_fields = {k: eng.get_field(k) for k in ("sig", "ux", "vx", "rho", "xp")}
     # stage durations with an event between stages, over the same number of steps
     prof = eng.step_profiled(args.steps)
     dominant = max((k for k in prof if k != "k_step_done"), key=lambda k: prof[k])
@@ -304,6 +356,10 @@ def engine_arm(args, world, rank, local):
     d2h = sum(v.nbytes for v in out.values())
     e2e_value = total_active * args.steps / t_e2e
     eng2.close()
+
+    bulk_ms, bulk_err, bulk_prof = bulk_form(st, args, device, ref_fields, moving)
+    bulk_ms = dist_max(bulk_ms, world)
+    kl = kl_synthesis(eng, scene, device) if not args.no_kl else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -332,6 +388,16 @@ def engine_arm(args, world, rank, local):
                          "algorithmic_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
                          "traffic": (traffic * scene.n) if traffic else None},
             "stage_ms_per_step": {k: v / args.steps for k, v in prof.items()},
+            "forms": {
+                "fp64": {"value": value, "ms_per_step": ms_max / args.steps,
+                         "error": "bit-identical to the FP64 oracle (tests/test_gpu_parity.py)"},
+                "fp32_bulk": {"value": total_active * args.steps / (bulk_ms / 1e3),
+                              "ms_per_step": bulk_ms / args.steps,
+                              "speedup_vs_fp64": ms_max / bulk_ms,
+                              "rel_l2_vs_fp64_after_warmup_plus_steps": bulk_err,
+                              "stage_ms_per_step": {k: v / args.steps for k, v in bulk_prof.items() if v > 0.01}},
+            },
+            "kl_synthesis": kl,
             "e2e": {"value": e2e_value, "unit": "particle-updates/s",
                     "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                     "what": "state upload + K steps + full state download through the C ABI"},
@@ -351,6 +417,7 @@ def main():
     ap.add_argument("--dx", type=float, default=0.005)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-kl", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         # host-only arm: rank 0 runs it, the other ranks exit without work
