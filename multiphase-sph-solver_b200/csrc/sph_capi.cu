@@ -143,7 +143,7 @@ int check_params(const sphgpu_params* P)
     if (!(P->dr > 0.0) || !(P->dt > 0.0)) return SPHGPU_E_ARG;
     if (P->step_regu <= 0) return SPHGPU_E_ARG;
     // flag combinations this engine runs (the others are rejected loudly)
-    if (P->flbndy != 1) return SPHGPU_E_UNSUPPORTED;
+    if (P->flbndy != 1 && P->flbndy != 2) return SPHGPU_E_UNSUPPORTED;
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
     if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
     if (P->fli < 0 || P->fli > 3) return SPHGPU_E_UNSUPPORTED;
@@ -332,6 +332,11 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.sr, 6 * (size_t)N); r |= dalloc(c, &s.pp, N);
     r |= dalloc(c, &s.eps_tmp, 6 * (size_t)N); r |= dalloc(c, &s.sig_tmp, 6 * (size_t)N);
     if (P->art_stre_coe > 0.0) r |= dalloc(c, &s.rij, 9 * (size_t)N);
+    if (P->flbndy != 1) {
+        r |= dalloc(c, &s.vel_bndy, 3 * (size_t)N);
+        r |= dalloc(c, &s.vb, 12 * (size_t)N);
+        r |= dalloc(c, &s.vx_vb, 3 * (size_t)N);
+    }
     r |= dalloc(c, &s.vx, 3 * (size_t)N); r |= dalloc(c, &s.vx_next, 3 * (size_t)N);
     r |= dalloc(c, &s.vxp, 3 * (size_t)N); r |= dalloc(c, &s.axp, 3 * (size_t)N); r |= dalloc(c, &s.ax, 3 * (size_t)N);
     r |= dalloc(c, &s.ux, 3 * (size_t)N);

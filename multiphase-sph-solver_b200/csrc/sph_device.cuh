@@ -30,7 +30,7 @@
 #define SPH_NB_CAP 99          // Par_Cell::influ[100], slots 1..99 (Class_NNPS.h:71)
 #define SPH_ERR_CELL 3         // parttocell, CPP_3-NNPS.cpp:247-257
 #define SPH_ERR_NEIGH 5        // partisearching, CPP_3-NNPS.cpp:313-319
-#define SPHK_NSTAGES 19        // entries of sphk_stage_names (one event bracket each)
+#define SPHK_NSTAGES 20        // entries of sphk_stage_names (one event bracket each)
 
 struct DevParams {
     int N, ndim, flknl, flbndy, fli, if_move, flv, inip, step_regu;
@@ -88,6 +88,11 @@ struct DevState {
     double *eps_in;            // strain the constitutive pass starts from: eps, or eps_tmp after strain_regu
     double *eps_tmp, *sig_tmp; // outputs of the regularisation passes, 6N each
     double *rij;               // artificial stress tensor R per soil particle, 9N row-major (art_stre_coe > 0)
+    // flbndy 2: cl_bndy_pair::vel_bndy of the moving particles (3N), the
+    // walls' clVar_Boundary velocities per phase vb[(p * 3 + k) * N + i],
+    // p = water, soil, air, structure (12N), and the velocity tm_boundary
+    // reads (after XSPH and velocity_set_domain, before check_domain; 3N)
+    double *vel_bndy, *vb, *vx_vb;
     // NNPS
     int *cell;                 // cell id per particle
     uint32_t *key_in, *key_out;
@@ -240,6 +245,19 @@ __device__ __forceinline__ void pair_w_raw(const Dev& d, const PairI<R>& I, cons
             w[3] = a1 * (R(2.0) - s) * (R(2.0) - s) * (R(2.0) - s);
         }
     }
+}
+
+// The virtual velocity component k of wall particle j seen by particle i of
+// type ti (CPP_6-density.cpp:89-121, CPP_7-1-strain.cpp:92-124): i's own
+// velocity with flbndy 1, the wall's per-phase velocity of tm_boundary with
+// flbndy 2/3/4/13/14, zero otherwise.
+__device__ __forceinline__ double wall_vel(const Dev& d, int ti, int j, const double vi[3], int k)
+{
+    const int bt = d.p.flbndy;
+    if (bt == 1) return vi[k];
+    if ((bt == 2 || bt == 3 || bt == 4 || bt == 13 || bt == 14) && ti >= 1 && ti <= 4)
+        return d.s.vb[(size_t)((ti - 1) * 3 + k) * d.p.N + j];
+    return 0.0;
 }
 
 // The stored pair record of slot s of particle i: kernel gradient w[0..2] and

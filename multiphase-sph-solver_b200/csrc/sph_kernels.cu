@@ -334,8 +334,8 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
             if (ti == tj && ti != 0) {
                 for (int k = 0; k < 3; k++) vxj[k] = d.s.vxp[k * N + j];
             } else if (moving && tj == 0) {
-                // virtual wall velocity, flbndy 1: the particle's own (:94-98)
-                for (int k = 0; k < 3; k++) vxj[k] = (d.p.flbndy == 1) ? vi[k] : 0.0;
+                // virtual wall velocity (:89-121)
+                for (int k = 0; k < 3; k++) vxj[k] = wall_vel(d, ti, j, vi, k);
             } else {
                 continue;
             }
@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_strain(Dev d)
         if (same || wallj) {
             real dvx[3];
             for (int k = 0; k < 3; k++) {
-                double vj = same ? d.s.vxp[k * N + j] : ((d.p.flbndy == 1) ? vi[k] : 0.0);
+                double vj = same ? d.s.vxp[k * N + j] : wall_vel(d, ti, j, vi, k);
                 dvx[k] = (real)(vi[k] - vj);
             }
             sup[0].add(mj / rj * dvx[0] * w[0]);
@@ -1203,8 +1203,12 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
         else
             for (int k = 0; k < nd; k++) vn[k] = vm[k] + tu[k];
     }
-    if (moving && d.p.flbndy == 1) {
-        const double a = 0.30, b = 0.30, dr = d.p.dr;
+    // tmboundary (flbndy 1, moving particles, a = b = 0.3) or
+    // velocity_set_domain (flbndy 2, fluid particles, a = b = coe_bndy,
+    // CPP_13-boundary.cpp:71-122): the same correction
+    const bool vcorr = (d.p.flbndy == 1 && moving) || (d.p.flbndy == 2 && (ti == 1 || ti == 3));
+    if (vcorr) {
+        const double a = (d.p.flbndy == 1) ? 0.30 : d.p.coe_bndy, b = a, dr = d.p.dr;
         double tb[3] = {0, 0, 0};
         for (int q = 0; q < nn; q++) {
             const int j = d.s.nbr[(size_t)q * N + i];
@@ -1227,6 +1231,8 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
         }
         for (int k = 0; k < nd; k++) vn[k] = vn[k] + tb[k];
     }
+    if (d.p.flbndy == 2 && moving)
+        for (int k = 0; k < 3; k++) d.s.vx_vb[k * N + i] = vn[k];
     if (ti != 0 && ti != 7) {
         const double dr = d.p.dr;
         const double bmax[3] = {d.p.xmax, d.p.ymax, d.p.zmax}, bmin[3] = {d.p.xmin, d.p.ymin, d.p.zmin};
@@ -1270,6 +1276,134 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
     }
     store_pos(d.s.xh_next, i, Pos{xn[0], xn[1], xn[2], load_pos(d.s.xh, i).h});
     for (int k = 0; k < 3; k++) d.s.vx[k * N + i] = vn[k];
+}
+
+// tm_boundary_2d / tm_boundary_3d, first pass (CPP_13-boundary.cpp:200-297,
+// 410-508): for each moving particle the wall particles of its list with
+// their distances, sorted as clParti_Pair::dist_sorting does (four passes
+// swapping ids, not distances, Class_particle.cpp:343-359); the line through
+// the two nearest (2-D, with clLine's C = 1 that cal_line leaves) or the plane
+// through the three nearest (3-D; plane_two_points when they are collinear,
+// D = 1 from clPlane() unless plane_two_points sets it), the particle's
+// distance to it, and vel_bndy = (1 - beta) v + beta v_wall, v_wall the
+// interfss of the last wall of matype > 2 in the list (particle 0 if none).
+template <int ND>
+__global__ void __launch_bounds__(128) k_tm_vb(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    const int ti = d.s.type[i];
+    if (ti == 0 || ti == 7) return;
+    const int nn = nbr_count(d, i);
+    int ids[SPH_NB_CAP];
+    double dsts[SPH_NB_CAP];
+    int total = 0, id = 0;
+    const Pos P = load_pos(d.s.xh, i);
+    for (int q = 0; q < nn; q++) {
+        const int j = d.s.nbr[(size_t)q * N + i];
+        if (d.s.type[j] != 0) continue;
+        const Pos pj = load_pos(d.s.xh, j);
+        const double d2 = (P.x - pj.x) * (P.x - pj.x) + (P.y - pj.y) * (P.y - pj.y) + (P.z - pj.z) * (P.z - pj.z);
+        ids[total] = j;
+        dsts[total] = sqrt(d2);
+        total++;
+        if (d.s.matype[j] > 2) id = j;
+    }
+    for (int a = 0; a < 4; a++)
+        for (int b = a + 1; b < total; b++)
+            if (dsts[a] > dsts[b]) { const int t = ids[a]; ids[a] = ids[b]; ids[b] = t; }
+    double vi[3], vb[3];
+    for (int k = 0; k < 3; k++) vi[k] = d.s.vx_vb[k * N + i];
+    const double dr = d.p.dr;
+    if (total >= (ND == 2 ? 2 : 3)) {
+        const Pos q1 = load_pos(d.s.xh, ids[0]), q2 = load_pos(d.s.xh, ids[1]);
+        const double p4[3] = {P.x, P.y, P.z}, p1[3] = {q1.x, q1.y, q1.z}, p2[3] = {q2.x, q2.y, q2.z};
+        double dst;
+        if (ND == 2) {
+            // cal_line (:645-650), cal_dpline (:617-628)
+            const double den = p2[1] * p1[0] - p1[1] * p2[0];
+            const double A = (p1[1] - p2[1]) / den, B = (p2[0] - p1[0]) / den, C = 1.0;
+            const double num = fabs(A * p4[0] + B * p4[1] + C);
+            const double tmp = sqrt(A * A + B * B);
+            dst = (tmp > 1.0e-3) ? num / tmp : 0.0;
+        } else {
+            const Pos q3 = load_pos(d.s.xh, ids[2]);
+            const double p3[3] = {q3.x, q3.y, q3.z};
+            double pc1[3], pc2[3], A, B, C, D = 1.0;
+            // cal_plane (:653-666) of (p1, p2, p4) and (p1, p3, p4)
+            const double den1 = -p1[0] * (p2[1] * p4[2] - p4[1] * p2[2]) - p2[0] * (p4[1] * p1[2] - p1[1] * p4[2]) -
+                                p4[0] * (p1[1] * p2[2] - p2[1] * p1[2]);
+            pc1[0] = p1[1] * (p2[2] - p4[2]) + p2[1] * (p4[2] - p1[2]) + p4[1] * (p1[2] - p2[2]);
+            pc1[1] = p1[2] * (p2[0] - p4[0]) + p2[2] * (p4[0] - p1[0]) + p4[2] * (p1[0] - p2[0]);
+            pc1[2] = p1[0] * (p2[1] - p4[1]) + p2[0] * (p4[1] - p1[1]) + p4[0] * (p1[1] - p2[1]);
+            pc1[0] = pc1[0] / den1; pc1[1] = pc1[1] / den1; pc1[2] = pc1[2] / den1;
+            const double den2 = -p1[0] * (p3[1] * p4[2] - p4[1] * p3[2]) - p3[0] * (p4[1] * p1[2] - p1[1] * p4[2]) -
+                                p4[0] * (p1[1] * p3[2] - p3[1] * p1[2]);
+            pc2[0] = p1[1] * (p3[2] - p4[2]) + p3[1] * (p4[2] - p1[2]) + p4[1] * (p1[2] - p3[2]);
+            pc2[1] = p1[2] * (p3[0] - p4[0]) + p3[2] * (p4[0] - p1[0]) + p4[2] * (p1[0] - p3[0]);
+            pc2[2] = p1[0] * (p3[1] - p4[1]) + p3[0] * (p4[1] - p1[1]) + p4[0] * (p1[1] - p3[1]);
+            pc2[0] = pc2[0] / den2; pc2[1] = pc2[1] / den2; pc2[2] = pc2[2] / den2;
+            double cs = pc1[0] * pc2[0] + pc1[1] * pc2[1] + pc1[2] * pc2[2];
+            cs = cs / sqrt(pc1[0] * pc1[0] + pc1[1] * pc1[1] + pc1[2] * pc1[2]) /
+                 sqrt(pc2[0] * pc2[0] + pc2[1] * pc2[1] + pc2[2] * pc2[2]);
+            if (fabs(cs) > 0.999999) {
+                // plane_two_points(p4, p1) (:684-708)
+                const double a = p4[0] - p1[0], b = p4[1] - p1[1], c = p4[2] - p1[2];
+                const double tmp = -a * p1[0] - b * p1[1] - c * p1[2];
+                if (fabs(tmp) > 1.0e-6) { A = a / tmp; B = b / tmp; C = c / tmp; D = 1.0; }
+                else { A = a; B = b; C = c; D = 0.0; }
+            } else {
+                const double den = -p1[0] * (p2[1] * p3[2] - p3[1] * p2[2]) - p2[0] * (p3[1] * p1[2] - p1[1] * p3[2]) -
+                                   p3[0] * (p1[1] * p2[2] - p2[1] * p1[2]);
+                A = p1[1] * (p2[2] - p3[2]) + p2[1] * (p3[2] - p1[2]) + p3[1] * (p1[2] - p2[2]);
+                B = p1[2] * (p2[0] - p3[0]) + p2[2] * (p3[0] - p1[0]) + p3[2] * (p1[0] - p2[0]);
+                C = p1[0] * (p2[1] - p3[1]) + p2[0] * (p3[1] - p1[1]) + p3[0] * (p1[1] - p2[1]);
+                A = A / den; B = B / den; C = C / den;
+            }
+            // cal_dpplane (:631-642)
+            const double num = fabs(A * p4[0] + B * p4[1] + C * p4[2] + D);
+            const double tmp = sqrt(A * A + B * B + C * C);
+            dst = (tmp > 1.0e-3) ? num / tmp : 0.0;
+        }
+        const double da = (dst > 0.6 * dr) ? dst - 0.5 * dr : 0.1 * dr;
+        const double db = 0.5 * dr;
+        double beta;
+        if (fabs(da) > 1.0e-6) { beta = 1.0 + db / da; beta = fmin(1.5, beta); }
+        else beta = 1.5;
+        for (int k = 0; k < 2; k++) vb[k] = (1.0 - beta) * vi[k] + beta * d.s.interfss[(size_t)k * N + id];
+        vb[2] = (ND == 2) ? 0.0 : (1.0 - beta) * vi[2] + beta * d.s.interfss[(size_t)2 * N + id];
+    } else {
+        for (int k = 0; k < 3; k++) vb[k] = vi[k];
+    }
+    for (int k = 0; k < 3; k++) d.s.vel_bndy[k * N + i] = vb[k];
+}
+
+// tm_boundary second pass (CPP_13-boundary.cpp:298-386, 509-614): each wall
+// particle's Shepard sums of the moving neighbours' vel_bndy per phase, with
+// the reference's [0][0] operand in components 1 and 2.
+__global__ void __launch_bounds__(128) k_tm_wall(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    if (d.s.type[i] != 0) return;
+    const int nn = nbr_count(d, i);
+    double up[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, down[4] = {0, 0, 0, 0};
+    for (int q = 0; q < nn; q++) {
+        const int j = d.s.nbr[(size_t)q * N + i];
+        const int tj = d.s.type[j];
+        if (tj < 1 || tj > 4) continue;
+        const int p = tj - 1;
+        real w[4];
+        load_w(d, q, i, w);
+        const double w3 = w[3], mj = d.s.mass[j], rj = d.s.rho[j];
+        up[p][0] = up[p][0] + mj * d.s.vel_bndy[j] * w3 / rj;
+        up[p][1] = up[p][0] + mj * d.s.vel_bndy[(size_t)N + j] * w3 / rj;
+        up[p][2] = up[p][0] + mj * d.s.vel_bndy[(size_t)2 * N + j] * w3 / rj;
+        down[p] = down[p] + mj * w3 / rj;
+    }
+    for (int p = 0; p < 4; p++)
+        for (int k = 0; k < 3; k++)
+            d.s.vb[(size_t)(p * 3 + k) * N + i] = (fabs(down[p]) > 1.0e-6) ? up[p][k] / down[p] : 0.0;
 }
 
 __global__ void k_step_done(Dev d)
@@ -1417,7 +1551,7 @@ extern "C" size_t sphk_sort_temp_bytes(int N, int end_bit)
 extern "C" const char* const sphk_stage_names[] = {
     "k_cellkey", "radix_sort", "k_cellreset", "k_cellrange", "k_nnps", "k_pairw", "k_kgc",
     "k_density", "k_shepard_eos", "k_strain", "k_regu_eps", "k_stress", "k_regu_sig", "k_stress_2",
-    "k_art_rij", "k_accel_a", "k_accel_b", "k_xsph_update", "k_step_done"};
+    "k_art_rij", "k_accel_a", "k_accel_b", "k_xsph_update", "k_tm_boundary", "k_step_done"};
 static_assert(sizeof(sphk_stage_names) / sizeof(sphk_stage_names[0]) == SPHK_NSTAGES, "stage table");
 #endif  // !SPH_BULK32
 
@@ -1506,7 +1640,12 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
     REC(17);
     LAUNCH_ND(k_xsph_update, nblk(N, 128), 128, d); n++;
     REC(18);
-    k_step_done<<<1, 32, 0, st>>>(d); n++;
+    if (d.p.flbndy == 2) {
+        LAUNCH_ND(k_tm_vb, nblk(N, 128), 128, d); n++;
+        k_tm_wall<<<nblk(N, 128), 128, 0, st>>>(d); n++;
+    }
     REC(19);
+    k_step_done<<<1, 32, 0, st>>>(d); n++;
+    REC(20);
     return n;
 }

@@ -282,3 +282,18 @@ def test_soil_models(label, factory, steps, tol):
     worst = _compare(eng, orc, tol=tol)
     if worst:
         print(f"soil model {label}, worst relative error per field:", max(worst.values()))
+
+
+@pytest.mark.parametrize("name,steps", [("dam_break_2d", 40), ("soil_column_3d", 30)])
+def test_tm_boundary_walls(name, steps):
+    """flbndy 2: velocity_set_domain and tm_boundary_2d / 3d (the per-phase
+    wall virtual velocities read by density and strain_noreg in the next
+    step): bit-identical to the oracle, whose same runs are bit-identical to
+    the reference (golden *_tm_boundary fixtures)."""
+    sc = SCENES[name]()
+    sc.flags["flbndy"] = 2
+    _, eng, orc = _engine_and_oracle(sc)
+    for chunk in (1, steps - 1):
+        eng.step(chunk)
+        assert orc.step(chunk) == 0
+    _compare(eng, orc)
