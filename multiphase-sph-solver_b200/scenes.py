@@ -258,6 +258,74 @@ def slope_2d(H: float = 5.0, dx: float = 0.05, crest: float = 6.25, gradient: fl
     )
 
 
+def footing(ndim: int = 2, dx: float = 0.04, bed=(2.0, 1.0, 1.0), width: float = 0.4, height: float = 0.12,
+            gap: float = 0.8, v: float = 0.5, ss_type: int = 3, myu: float = 0.3, zeta: float = 0.0,
+            layers: int = 3, steps: int = 10000, matype: int = 2) -> Scene:
+    """A rigid strip footing pushed into a soil bed: the soil (type 2,
+    Drucker-Prager by default) fills bed[0] x bed[1] (x bed[2] in 3-D) on a
+    3-layer floor between side walls (type 0); the footing (type 4, etype 5,
+    E = 30 GPa) is `width` wide (and bed[2] long in 3-D), `height` tall, centred
+    over the bed, its lowest layer `gap` spacings above the top soil layer; it
+    moves down at v m/s (if_move 3) and meets the soil through the
+    soil-structure contact of type ss_type (1 rigid, 2 deformable, 3 penalty)
+    with friction coefficient myu and damping zeta."""
+    g = 9.81
+    L, D = bed[0], bed[1]
+    nx, ny = int(round(L / dx)), int(round(D / dx))
+    nf, nh = int(round(width / dx)), int(round(height / dx))
+    x0f = (nx - nf) // 2 * dx
+    yf = (ny - 0.5 + gap) * dx          # the footing's lowest layer, gap spacings above the soil's top layer
+    wall_h = D + height + 4 * dx
+    nwy = int(round(wall_h / dx))
+    if ndim == 2:
+        soil = _grid2(nx, ny, dx, (0.0, 0.0))
+        foot = _grid2(nf, nh, dx, (x0f, 0.0))
+        foot[:, 1] += yf - foot[:, 1].min()
+        parts = [(soil, 2, matype), (foot, 4, 0)]
+        parts.append((_grid2(nx + 2 * layers, layers, dx, (-layers * dx, -layers * dx)), 0, 0))
+        parts.append((_grid2(layers, nwy, dx, (-layers * dx, 0.0)), 0, 0))
+        parts.append((_grid2(layers, nwy, dx, (nx * dx, 0.0)), 0, 0))
+        gvec, mv = (0.0, -g, 0.0), (0.0, -v, 0.0)
+    else:
+        nz = int(round(bed[2] / dx))
+        soil = _grid(nx, ny, nz, dx, (0.0, 0.0, 0.0))
+        foot = _grid(nf, nh, nz, dx, (x0f, 0.0, 0.0))
+        foot[:, 1] += yf - foot[:, 1].min()
+        parts = [(soil, 2, matype), (foot, 4, 0)]
+        parts.append((_grid(nx + 2 * layers, layers, nz + 2 * layers, dx, (-layers * dx, -layers * dx, -layers * dx)), 0, 0))
+        parts.append((_grid(layers, nwy, nz, dx, (-layers * dx, 0.0, 0.0)), 0, 0))
+        parts.append((_grid(layers, nwy, nz, dx, (nx * dx, 0.0, 0.0)), 0, 0))
+        parts.append((_grid(nx, nwy, layers, dx, (0.0, 0.0, -layers * dx)), 0, 0))
+        parts.append((_grid(nx, nwy, layers, dx, (0.0, 0.0, nz * dx)), 0, 0))
+        gvec, mv = (0.0, -g, 0.0), (0.0, -v, 0.0)
+    xp, vxp, ptype, mt, permtype, etype = _assemble(parts)
+    etype[ptype == 4] = 5
+    dp = soil_default()
+    dp.update(kapa=0.05, poi=0.3, dens=2000.0, c=5.0e3, fai=30.0, fs=1.0, beta=0.0,
+              damp1=0.0, damp2=0.0, cop=1.0e-4, eps0=0.0, e=2.0e7, ds=1.0e-3)
+    w = fluid_default()
+    w.update(dens=1000.0, vis=1.0e-3, vpu=30.0, press_type=0, acc_type=0, bhtype=0,
+             pre_coe=30.0 * 30.0 / (7.0 * g * dx), strain_min=1.0e-3)
+    mflags = [0] * 10
+    mflags[matype % 10] = 1
+    return Scene(
+        name=f"footing_{ndim}d_dx{dx:g}_ss{ss_type}", ndim=ndim, dr=dx, dt=0.25 * dx / 600.0 * steps, loop=steps,
+        xp=xp, vxp=vxp, ptype=ptype, matype=mt, permtype=permtype, etype=etype,
+        flags=dict(fla=0, fls=1, flr=0, fli=0, flv=0, fleob=0, flts=0, flspv=0, flknl=1,
+                   ntd=1, flbndy=1),
+        problem=dict(threshold_min=0.1, threshold_max=0.12, fop=max(steps, 1), inip=0,
+                     step_regu=100000000, dttype=2,
+                     xsph=(0.5, 0.1, 0.0), art_vis=((0.1, 0.0), (0.1, 0.0), (0.0, 0.0)),
+                     art_stre_coe=0.0, g=gvec,
+                     interc=0.0, permtype=0, pers=0.0, perl=0.0, perm=0.0,
+                     ss=(ss_type, myu, zeta, 0), if_cal=0, if_move=3, coe_bndy=0.3, move_vx=mv),
+        water=[w, copy.deepcopy(w), copy.deepcopy(w)],
+        model_flags=tuple(mflags),
+        soils={matype: dp},
+        structure=dict(dens=2500.0, eps0=0.0, cop=0.0, e=3.0e10, poi=0.2),
+    )
+
+
 def uplift(scene: Scene, axis: int, above: float, v: float = 0.5) -> Scene:
     """Give the soil particles (type 2) above coordinate `above` along `axis`
     an initial velocity v along that axis, which stretches the soil body and

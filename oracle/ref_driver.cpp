@@ -76,6 +76,7 @@ struct RefRun {
     clVel_Fun vel;
     clUpdate_Fun upd;
     clBndy_Fun bnd;
+    clSoilStruct_Fun ssinter;
 };
 
 int g_last_error = 0;
@@ -240,7 +241,7 @@ int ref_nnps(void* h, int* ninflu, int* influ, double* wij)
 }
 
 /* the body of the main loop, CPP_1-SPHLoops.cpp:481-753, for the flag set the
- * engine covers (no rain, excavation, vibration or soil-structure contact) */
+ * engine covers (no rain, excavation or vibration) */
 int ref_step(void* h, int nsteps)
 {
     RefRun* r = (RefRun*)h;
@@ -278,9 +279,19 @@ int ref_step(void* h, int nsteps)
         else if (F.flbndy == 3 || F.flbndy == 4 || F.flbndy == 13 || F.flbndy == 14)
             r->acc.boundary_stress_effect_tran(r->par, r->parcell, r->varibndy, P, F.ntd);
         else r->acc.boundary_effect_free_struct(r->par, r->parcell, P, F.ntd);
+        if (r->ssi.type >= 1 && r->ssi.type <= 3 && r->ssi.acc_type == 2)
+            r->acc.coupled_Water_Soil_Structure(r->par, r->parcell, r->vfluid, r->conspara, P, r->gf, F.ntd);
         if (F.fli == 1) r->itf.interact1(r->par, r->parcell, r->inter, r->vfluid, P, r->gf, F.ntd);
         else if (F.fli == 2) r->itf.interact2(r->par, r->parcell, r->inter, r->conspara, r->vfluid, P, r->gf, F.ntd);
         else if (F.fli == 3) r->itf.interact3(r->par, r->parcell, r->inter, r->conspara, r->vfluid, P, r->gf, F.ntd);
+        if (r->ssi.type == 1)
+            err = r->ssinter.interaction_ss_rigid(r->par, r->parcell, r->pair_ss, r->interf_ss, r->partipair, r->ssi, P, F.ntd);
+        else if (r->ssi.type == 2)
+            err = r->ssinter.interaction_ss_deformable(r->par, r->parcell, r->pair_ss, r->interf_ss, r->partipair, r->ssi, P,
+                                                       F.ntd);
+        else if (r->ssi.type == 3)
+            err = r->ssinter.interaction_ss_penalty(r->par, r->parcell, r->pair_ss, r->interf_ss, r->partipair, r->ssi, P, F.ntd);
+        if (err > 0) return err;
         if (P.l <= P.inip) r->acc.soil_damping_geostress(r->par, r->parcell, P, F.ntd);
         if (F.flbndy == 5) r->bnd.boundary_free_solid(r->par, r->parcell, P, r->ssi, F.ntd);
         r->vel.veocity_update(r->par, P, r->bou, F.flv);
@@ -292,6 +303,13 @@ int ref_step(void* h, int nsteps)
             else r->bnd.tm_boundary_3d(r->par, r->parcell, r->bndy, r->varibndy, P, F.ntd);
         } else if (F.flbndy == 3) r->bnd.no_slip_tran(r->par, r->parcell, r->varibndy, P, F.ntd);
         else if (F.flbndy == 4) r->bnd.free_slip_tran(r->par, r->parcell, r->varibndy, P, F.ntd);
+        else if (F.flbndy == 13) {
+            r->bnd.velocity_set_domain(r->par, r->parcell, r->bndy, P, r->bou.coe_bndy);
+            r->bnd.no_slip_tran(r->par, r->parcell, r->varibndy, P, F.ntd);
+        } else if (F.flbndy == 14) {
+            r->bnd.velocity_set_domain(r->par, r->parcell, r->bndy, P, r->bou.coe_bndy);
+            r->bnd.free_slip_tran(r->par, r->parcell, r->varibndy, P, F.ntd);
+        }
         r->bnd.check_domain(r->par, r->cellc, r->bou, P);
         r->upd.update(r->par, P, r->bou, F.ntd);
         P.l++;

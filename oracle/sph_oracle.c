@@ -30,6 +30,8 @@ struct orc_ctx {
     /* cl_bndy_pair::vel_bndy and clVar_Boundary::vx_* (Class_particle.h:172-207),
      * the wall virtual velocities of flbndy 2 */
     double *vel_bndy, *vb_water, *vb_soil, *vb_air, *vb_struct;
+    /* clInterf_SS of the one thread (f_n, f_t) of the soil-structure contact */
+    double *ss_fn, *ss_ft;
     /* per-particle material records (pVFluid, pParti_ConsPara) */
     sphgpu_fluid* fl;
     sphgpu_soil* so;
@@ -62,6 +64,7 @@ static const field_desc k_fields[] = {
     FD(cd, 1), FD(poro_cop, 1), FD(beta, 9), FD(beta_ts, 9),
     FI(type), FI(matype), FI(permtype), FI(etype),
     FD(vel_bndy, 3), FD(vb_water, 3), FD(vb_soil, 3), FD(vb_air, 3), FD(vb_struct, 3),
+    FD(ss_fn, 3), FD(ss_ft, 3),
 };
 #define NFIELDS (sizeof(k_fields) / sizeof(k_fields[0]))
 
@@ -1812,6 +1815,236 @@ static void tm_boundary(orc_ctx* c)
     }
 }
 
+/* ------------------------------------------------------------------------- */
+/* soil-structure contact: interaction_ss_rigid / _deformable / _penalty      */
+/* (CPP_10-1-interact_ss.cpp:17-1036) with their geometry helpers (:1039-1369) */
+/* in the order one thread runs them: the forces a structure particle takes   */
+/* from its contacting particles accumulate in particle order.               */
+
+typedef struct { double x, y, z; } orc_pt;
+
+static double ss_dpline(orc_pt p, double A, double B, double C)
+{   /* cal_dpline (:1224-1236) */
+    double dst = fabs(A * p.x + B * p.y + C), tmp = sqrt(A * A + B * B);
+    return (tmp > 1.0e-3) ? dst / tmp : 0.0;
+}
+
+static double ss_dpplane(orc_pt p, double A, double B, double C, double D)
+{   /* cal_dpplane (:1238-1250) */
+    double dst = fabs(A * p.x + B * p.y + C * p.z + D), tmp = sqrt(A * A + B * B + C * C);
+    return (tmp > 1.0e-3) ? dst / tmp : 0.0;
+}
+
+/* linear_interpolate (:1187-1202) */
+static void ss_interp(orc_pt P1, orc_pt P2, orc_pt r, double m1, double m2, const double* v1, const double* v2,
+                      double* m, double* v)
+{
+    double xk1 = 0.0;
+    double xk2 = sqrt((P2.x - P1.x) * (P2.x - P1.x) + (P2.y - P1.y) * (P2.y - P1.y) + (P2.z - P1.z) * (P2.z - P1.z));
+    double xp = sqrt((r.x - P1.x) * (r.x - P1.x) + (r.y - P1.y) * (r.y - P1.y) + (r.z - P1.z) * (r.z - P1.z));
+    *m = (m1 * fabs(xp - xk2) + m2 * fabs(xp - xk1)) / fabs(xk2 - xk1);
+    for (int k = 0; k < 3; k++) v[k] = (v1[k] * fabs(xp - xk2) + v2[k] * fabs(xp - xk1)) / fabs(xk2 - xk1);
+}
+
+/* linear_interpolate_force (:1204-1222) */
+static void ss_interp_force(orc_pt P1, orc_pt P2, orc_pt r, const double* f, double* f1, double* f2)
+{
+    double xk1 = 0.0;
+    double xk2 = sqrt((P2.x - P1.x) * (P2.x - P1.x) + (P2.y - P1.y) * (P2.y - P1.y) + (P2.z - P1.z) * (P2.z - P1.z));
+    double xp = sqrt((r.x - P1.x) * (r.x - P1.x) + (r.y - P1.y) * (r.y - P1.y) + (r.z - P1.z) * (r.z - P1.z));
+    for (int k = 0; k < 3; k++) f1[k] = -fabs(xp - xk2) / fabs(xk1 - xk2) * f[k];
+    for (int k = 0; k < 3; k++) f2[k] = -fabs(xp - xk1) / fabs(xk1 - xk2) * f[k];
+}
+
+static orc_pt ss_point(const orc_ctx* c, int i) { orc_pt p = {c->xp[i * 3], c->xp[i * 3 + 1], c->xp[i * 3 + 2]}; return p; }
+
+static void interaction_ss(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    const int form = P->ss_type, nd = P->ndim, n = c->n;
+    const double dt = P->dt, dr = P->dr, myu = P->ss_myu, zeta = P->ss_zeta;
+    const double reach = (form == 1) ? 0.5 * dr : dr;
+    int ids[NB];
+    double dsts[NB];
+    for (int i = 0; i < n * 3; i++) { c->ss_fn[i] = 0.0; c->ss_ft[i] = 0.0; }
+    for (int i = 0; i < n; i++) {
+        int ti = c->type[i];
+        if (!(ti == 1 || ti == 2)) continue;
+        int total = 0;
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj);
+            if (c->type[j] != 4) continue;
+            double d = (c->xp[i * 3] - c->xp[j * 3]) * (c->xp[i * 3] - c->xp[j * 3]) +
+                       (c->xp[i * 3 + 1] - c->xp[j * 3 + 1]) * (c->xp[i * 3 + 1] - c->xp[j * 3 + 1]) +
+                       (c->xp[i * 3 + 2] - c->xp[j * 3 + 2]) * (c->xp[i * 3 + 2] - c->xp[j * 3 + 2]);
+            ids[total] = j;
+            dsts[total] = sqrt(d);
+            total++;
+        }
+        for (int a = 0; a < 4; a++)   /* clParti_Pair::dist_sorting */
+            for (int b = a + 1; b < total; b++)
+                if (dsts[a] > dsts[b]) { int t = ids[a]; ids[a] = ids[b]; ids[b] = t; }
+        if (total < (nd == 2 ? 2 : 3)) continue;
+        const double mi = c->mass[i];
+        const double* vpi = &c->vxp[i * 3];
+        double* fn = &c->ss_fn[i * 3];
+        double* ft = &c->ss_ft[i * 3];
+        orc_pt p4 = ss_point(c, i);
+        int id1 = ids[0], id2 = ids[1];
+        orc_pt p1 = ss_point(c, id1), p2 = ss_point(c, id2);
+        if (nd == 2) {
+            /* cal_line (:1055-1060), C = 1 from clLine() */
+            double den = p2.y * p1.x - p1.y * p2.x;
+            double A = (p1.y - p2.y) / den, B = (p2.x - p1.x) / den, C = 1.0;
+            double dp = ss_dpline(p4, A, B, C);
+            /* cal_mappoint_line (:1094-1125) */
+            double tmp = sqrt(A * A + B * B);
+            orc_pt P1 = {p4.x + dp * A / tmp, p4.y + dp * B / tmp, 0.0}, P2 = {p4.x - dp * A / tmp, p4.y - dp * B / tmp, 0.0};
+            orc_pt outp = (ss_dpline(P1, A, B, C) < 1.0e-3) ? P1 : P2;
+            outp.z = 0.0;
+            /* check_ifinside_line (:1290-1305) on (p1, p2, outp with z = 0) */
+            double v0x = p2.x - p1.x, v0y = p2.y - p1.y, v0z = p2.z - p1.z;
+            double v1x = outp.x - p1.x, v1y = outp.y - p1.y, v1z = 0.0 - p1.z;
+            double dot00 = v0x * v0x + v0y * v0y + v0z * v0z, dot01 = v0x * v1x + v0y * v1y + v0z * v1z;
+            double u = 1.0 / dot00 * dot01;
+            int inside = !(u < 0 || u > 1);
+            if (!(inside && dp < reach)) continue;
+            /* clLine::set_normal, check_ifoutward2D (:1252-1270) */
+            double nx = 0.0, ny = 0.0, tot = sqrt(A * A + B * B);
+            if (tot > 1.0e-10) { nx = A / tot; ny = B / tot; }
+            double dot = (outp.x - p4.x) * nx + (outp.y - p4.y) * ny + 0.0 * 0.0;
+            if (!(dot <= 0.0)) { nx = -nx; ny = -ny; }
+            double ms, vs[3];
+            ss_interp(p1, p2, outp, c->mass[id1], c->mass[id2], &c->vxp[id1 * 3], &c->vxp[id2 * 3], &ms, vs);
+            vs[0] -= vpi[0];
+            vs[1] -= vpi[1];
+            if (form != 1) {
+                vs[0] *= ms / (ms + mi);
+                vs[1] *= ms / (ms + mi);
+            }
+            /* decomposition_velocity2D (:1346-1356) */
+            double v = vs[0] * nx + vs[1] * ny;
+            double vn[2] = {v * nx, v * ny}, vt[2] = {vs[0] - vn[0], vs[1] - vn[1]};
+            if (form == 3) {
+                double mag = (1.0 - zeta) * 2.0 * mi * (dr - dp) / dt / dt;
+                fn[0] = mag * nx; fn[1] = mag * ny;
+            } else {
+                fn[0] = mi * vn[0] / dt; fn[1] = mi * vn[1] / dt;
+            }
+            ft[0] = mi * vt[0] / dt; ft[1] = mi * vt[1] / dt;
+            double mag_fn = sqrt(fn[0] * fn[0] + fn[1] * fn[1]);
+            double mag_ft = sqrt(ft[0] * ft[0] + ft[1] * ft[1]);
+            if (mag_ft > (mag_fn * myu)) {
+                vt[0] = vt[0] * myu * mag_fn / mag_ft;
+                vt[1] = vt[1] * myu * mag_fn / mag_ft;
+                ft[0] = mi * vt[0] / dt; ft[1] = mi * vt[1] / dt;
+            }
+            double f1n[3], f2n[3], f1t[3], f2t[3];
+            ss_interp_force(p1, p2, outp, fn, f1n, f2n);
+            ss_interp_force(p1, p2, outp, ft, f1t, f2t);
+            for (int k = 0; k < 3; k++) c->ss_fn[id1 * 3 + k] += f1n[k];
+            for (int k = 0; k < 3; k++) c->ss_fn[id2 * 3 + k] += f2n[k];
+            for (int k = 0; k < 3; k++) c->ss_ft[id1 * 3 + k] += f1t[k];
+            for (int k = 0; k < 3; k++) c->ss_ft[id2 * 3 + k] += f2t[k];
+        } else {
+            int id3 = ids[2];
+            orc_pt p3 = ss_point(c, id3);
+            /* cal_plane (:1063-1076), D = 1 from clPlane() */
+            double den = -p1.x * (p2.y * p3.z - p3.y * p2.z) - p2.x * (p3.y * p1.z - p1.y * p3.z) - p3.x * (p1.y * p2.z - p2.y * p1.z);
+            double A = p1.y * (p2.z - p3.z) + p2.y * (p3.z - p1.z) + p3.y * (p1.z - p2.z);
+            double B = p1.z * (p2.x - p3.x) + p2.z * (p3.x - p1.x) + p3.z * (p1.x - p2.x);
+            double C = p1.x * (p2.y - p3.y) + p2.x * (p3.y - p1.y) + p3.x * (p1.y - p2.y);
+            A = A / den; B = B / den; C = C / den;
+            const double D = 1.0;
+            double dp = ss_dpplane(p4, A, B, C, D);
+            /* cal_mappoint_plane (:1127-1160) */
+            double tmp = sqrt(A * A + B * B + C * C);
+            orc_pt P1 = {p4.x + dp * A / tmp, p4.y + dp * B / tmp, p4.z + dp * C / tmp};
+            orc_pt P2 = {p4.x - dp * A / tmp, p4.y - dp * B / tmp, p4.z - dp * C / tmp};
+            orc_pt outp = (ss_dpplane(P1, A, B, C, D) < 1.0e-3) ? P1 : P2;
+            /* check_ifinside_triangle (:1307-1344) of (p1, p2, p3, outp) */
+            double v0[3] = {p3.x - p1.x, p3.y - p1.y, p3.z - p1.z};
+            double v1[3] = {p2.x - p1.x, p2.y - p1.y, p2.z - p1.z};
+            double v2[3] = {outp.x - p1.x, outp.y - p1.y, outp.z - p1.z};
+            double dot00 = v0[0] * v0[0] + v0[1] * v0[1] + v0[2] * v0[2];
+            double dot01 = v0[0] * v1[0] + v0[1] * v1[1] + v0[2] * v1[2];
+            double dot02 = v0[0] * v2[0] + v0[1] * v2[1] + v0[2] * v2[2];
+            double dot11 = v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2];
+            double dot12 = v1[0] * v2[0] + v1[1] * v2[1] + v1[2] * v2[2];
+            double inv = 1 / (dot00 * dot11 - dot01 * dot01);
+            double u = (dot11 * dot02 - dot01 * dot12) * inv;
+            int inside = 1;
+            if (u < 0 || u > 1) inside = 0;
+            else {
+                double v = (dot00 * dot12 - dot01 * dot02) * inv;
+                if (v < 0 || v > 1) inside = 0;
+                else inside = (u + v <= 1);
+            }
+            if (!(inside && dp < reach)) continue;
+            /* clPlane::set_normal, check_ifoutward3D (:1272-1288) */
+            double nx = 0.0, ny = 0.0, nz = 0.0, tot = sqrt(A * A + B * B + C * C);
+            if (tot > 1.0e-10) { nx = A / tot; ny = B / tot; nz = C / tot; }
+            double dot = (outp.x - p4.x) * nx + (outp.y - p4.y) * ny + (outp.z - p4.z) * nz;
+            if (!(dot <= 0.0)) { nx = -nx; ny = -ny; nz = -nz; }
+            /* cal_line3D (:1078-1092) of (p1, p2) and (p3, outp); cal_intersect_lines3D (:1162-1185) */
+            double d1 = sqrt((p2.x - p1.x) * (p2.x - p1.x) + (p2.y - p1.y) * (p2.y - p1.y) + (p2.z - p1.z) * (p2.z - p1.z));
+            double a1 = (p2.x - p1.x) / d1, b1 = (p2.y - p1.y) / d1, c1 = (p2.z - p1.z) / d1;
+            double d2 = sqrt((outp.x - p3.x) * (outp.x - p3.x) + (outp.y - p3.y) * (outp.y - p3.y) + (outp.z - p3.z) * (outp.z - p3.z));
+            double a2 = (outp.x - p3.x) / d2, b2 = (outp.y - p3.y) / d2;
+            double flag = a1 * b2 - a2 * b1;
+            if (!(fabs(flag) > 1.0e-3)) continue;
+            double tu = a2 * (p1.y - p3.y) - b2 * (p1.x - p3.x);
+            double t = tu / flag;
+            orc_pt sectp = {p1.x + a1 * t, p1.y + b1 * t, p1.z + c1 * t};
+            double tms, tvs[3], ms, vs[3];
+            ss_interp(p1, p2, sectp, c->mass[id1], c->mass[id2], &c->vxp[id1 * 3], &c->vxp[id2 * 3], &tms, tvs);
+            ss_interp(p3, sectp, outp, c->mass[id3], tms, &c->vxp[id3 * 3], tvs, &ms, vs);
+            for (int k = 0; k < 3; k++) {
+                vs[k] -= vpi[k];
+                if (form != 1) vs[k] *= ms / (ms + mi);
+            }
+            /* decomposition_velocity3D (:1358-1369) */
+            double v = vs[0] * nx + vs[1] * ny + vs[2] * nz;
+            double vn[3] = {v * nx, v * ny, v * nz}, vt[3] = {vs[0] - vn[0], vs[1] - vn[1], vs[2] - vn[2]};
+            if (form == 3) {
+                double mag = (1.0 - zeta) * 2.0 * mi * (dr - dp) / dt / dt;
+                fn[0] = mag * nx; fn[1] = mag * ny; fn[2] = mag * nz;
+            } else {
+                for (int k = 0; k < 3; k++) fn[k] = mi * vn[k] / dt;
+            }
+            for (int k = 0; k < 3; k++) ft[k] = mi * vt[k] / dt;
+            double mag_fn = sqrt(fn[0] * fn[0] + fn[1] * fn[1] + fn[2] * fn[2]);
+            double mag_ft = sqrt(ft[0] * ft[0] + ft[1] * ft[1] + ft[2] * ft[2]);
+            if (mag_ft > (mag_fn * myu)) {
+                for (int k = 0; k < 3; k++) vt[k] = vt[k] * myu * mag_fn / mag_ft;
+                for (int k = 0; k < 3; k++) ft[k] = mi * vt[k] / dt;
+            }
+            double f1n[3], f3n[3], f1t[3], f3t[3], g1n[3], g2n[3], g1t[3], g2t[3];
+            ss_interp_force(p3, sectp, outp, fn, f1n, f3n);
+            ss_interp_force(p3, sectp, outp, ft, f1t, f3t);
+            for (int k = 0; k < 3; k++) c->ss_fn[id3 * 3 + k] += f1n[k];
+            for (int k = 0; k < 3; k++) c->ss_ft[id3 * 3 + k] += f1t[k];
+            ss_interp_force(p1, p2, sectp, f3n, g1n, g2n);
+            ss_interp_force(p1, p2, sectp, f3t, g1t, g2t);
+            for (int k = 0; k < 3; k++) c->ss_fn[id1 * 3 + k] -= g1n[k];
+            for (int k = 0; k < 3; k++) c->ss_fn[id2 * 3 + k] -= g2n[k];
+            for (int k = 0; k < 3; k++) c->ss_ft[id1 * 3 + k] -= g1t[k];
+            for (int k = 0; k < 3; k++) c->ss_ft[id2 * 3 + k] -= g2t[k];
+        }
+    }
+    /* the per-thread sums into interfss and the acceleration (:1008-1034) */
+    for (int i = 0; i < n; i++) {
+        int ti = c->type[i];
+        if (!(ti == 1 || ti == 2 || ti == 4)) continue;
+        for (int k = 0; k < 3; k++) {
+            c->interfss[i * 3 + k] = 0.0;
+            if (form != 3) c->interfss[i * 3 + k] += zeta * (c->ss_ft[i * 3 + k] + c->ss_fn[i * 3 + k]);
+            else c->interfss[i * 3 + k] += c->ss_ft[i * 3 + k] + c->ss_fn[i * 3 + k];
+        }
+        for (int k = 0; k < 3; k++) c->ax[i * 3 + k] += c->interfss[i * 3 + k] / c->mass[i];
+    }
+}
+
 /* check_domain: CPP_13-boundary.cpp:20-68, in the sequential order (vbx is
  * taken from the first wall particle with matype > 2 and applies to the
  * particles after it) */
@@ -1954,7 +2187,8 @@ static int check_supported(const sphgpu_params* P)
     if (P->flbndy != 1 && P->flbndy != 2) return SPHGPU_E_UNSUPPORTED;
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
     if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
-    if (P->fli < 0 || P->fli > 3 || P->ss_type != 0) return SPHGPU_E_UNSUPPORTED;
+    if (P->fli < 0 || P->fli > 3 || P->ss_type < 0 || P->ss_type > 3) return SPHGPU_E_UNSUPPORTED;
+    if (P->ss_type >= 1 && P->ss_acc_type == 2) return SPHGPU_E_UNSUPPORTED;
     return 0;
 }
 
@@ -1989,6 +2223,7 @@ int orc_step(orc_ctx* c, int nsteps)
         if (P->art_stre_coe > 0.0) artificial_stress(c);
         boundary_moving_stress_effect(c);    /* flv == 0, flbndy 1 or 2 */
         if (P->fli >= 1) interact(c, P->fli);
+        if (P->ss_type >= 1 && P->ss_type <= 3) interaction_ss(c);
         if (c->l <= P->inip) soil_damping_geostress(c);
         velocity_update(c);
         if (P->if_move != 2) xsph(c);

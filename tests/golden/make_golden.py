@@ -88,6 +88,14 @@ def _tm_boundary(factory):
     return make
 
 
+def _footing(ndim, dx, ss_type):
+    """A strip footing (type 4, pushed down at 0.5 m/s, if_move 3) 0.4 spacings
+    above a Drucker-Prager soil bed, with soil-structure contact ss_type
+    (1 rigid, 2 deformable, 3 penalty), friction 0.3, zeta 0.1."""
+    return lambda: scenes.footing(ndim=ndim, dx=dx, bed=(1.2, 0.6, 0.5), width=0.4, height=0.2, gap=0.4,
+                                  ss_type=ss_type, zeta=0.1, v=0.5)
+
+
 CASES = {
     # name: (scene factory, steps)
     "dam_break_2d_dx0.04": (lambda: scenes.dam_break_2d(dx=0.04, steps=200), 25),
@@ -102,6 +110,11 @@ CASES = {
     "soil_column_3d_dx0.1_visco_elastic": (_column_model(7, c=1.0e5, e=1.0e7), 20),
     "dam_break_2d_dx0.04_tm_boundary": (_tm_boundary(lambda: scenes.dam_break_2d(dx=0.04, steps=200)), 25),
     "soil_column_3d_dx0.1_tm_boundary": (_tm_boundary(lambda: scenes.soil_column_3d(dx=0.1, steps=200)), 15),
+    "footing_2d_rigid": (_footing(2, 0.04, 1), 12),
+    "footing_2d_deformable": (_footing(2, 0.04, 2), 12),
+    "footing_2d_penalty": (_footing(2, 0.04, 3), 12),
+    "footing_3d_deformable": (_footing(3, 0.1, 2), 12),
+    "footing_3d_penalty": (_footing(3, 0.1, 3), 12),
 }
 
 

@@ -18,7 +18,9 @@ CASES = ["dam_break_2d_dx0.04", "soil_column_3d_dx0.1", "soil_column_3d_dx0.1_kg
          "slope_2d_H1_dx0.05_art_stress", "soil_column_3d_dx0.1_art_stress",
          "soil_column_3d_dx0.1_drag_tsuji_dilute", "soil_column_3d_dx0.1_drag_peng",
          "soil_column_3d_dx0.1_camclay", "soil_column_3d_dx0.1_mohr_coulomb", "soil_column_3d_dx0.1_visco_elastic",
-         "dam_break_2d_dx0.04_tm_boundary", "soil_column_3d_dx0.1_tm_boundary"]
+         "dam_break_2d_dx0.04_tm_boundary", "soil_column_3d_dx0.1_tm_boundary",
+         "footing_2d_rigid", "footing_2d_deformable", "footing_2d_penalty", "footing_3d_deformable",
+         "footing_3d_penalty"]
 
 
 def _golden(name):
