@@ -147,8 +147,9 @@ int check_params(const sphgpu_params* P)
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
     if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
     if (P->fli < 0 || P->fli > 3) return SPHGPU_E_UNSUPPORTED;
-    if (P->ss_type != 0) return SPHGPU_E_UNSUPPORTED;
-    if (P->if_move != 0 && P->if_move != 1) return SPHGPU_E_UNSUPPORTED;
+    if (P->ss_type < 0 || P->ss_type > 3) return SPHGPU_E_UNSUPPORTED;
+    if (P->ss_type >= 1 && P->ss_acc_type == 2) return SPHGPU_E_UNSUPPORTED;
+    if (P->if_move < 0 || P->if_move > 3) return SPHGPU_E_UNSUPPORTED;
     return 0;
 }
 
@@ -315,6 +316,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     p.st_e = P->structure.e; p.st_poi = P->structure.poi;
     p.g_acc = std::sqrt(P->gx * P->gx + P->gy * P->gy + P->gz * P->gz);   // CPP_10-interact1.cpp:28
     p.art_stre_coe = P->art_stre_coe;
+    p.ss_type = P->ss_type; p.ss_myu = P->ss_myu; p.ss_zeta = P->ss_zeta;
     DevState& s = d.s;
     int r = 0;
     r |= dalloc(c, &s.type, N); r |= dalloc(c, &s.matype, N); r |= dalloc(c, &s.etype, N); r |= dalloc(c, &s.permtype, N);
@@ -332,6 +334,12 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.sr, 6 * (size_t)N); r |= dalloc(c, &s.pp, N);
     r |= dalloc(c, &s.eps_tmp, 6 * (size_t)N); r |= dalloc(c, &s.sig_tmp, 6 * (size_t)N);
     if (P->art_stre_coe > 0.0) r |= dalloc(c, &s.rij, 9 * (size_t)N);
+    if (P->ss_type >= 1) {
+        r |= dalloc(c, &s.ss_id, 3 * (size_t)N);
+        r |= dalloc(c, &s.ss_con, 18 * (size_t)N);
+        r |= dalloc(c, &s.ss_own, 6 * (size_t)N);
+        r |= dalloc(c, &s.ss_fs, 6 * (size_t)N);
+    }
     if (P->flbndy != 1) {
         r |= dalloc(c, &s.vel_bndy, 3 * (size_t)N);
         r |= dalloc(c, &s.vb, 12 * (size_t)N);

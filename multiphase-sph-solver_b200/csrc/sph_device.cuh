@@ -50,6 +50,8 @@ struct DevParams {
     double st_e, st_poi;       // Para_Structure elastic constants
     double g_acc;              // |g|, interact1 (CPP_10-interact1.cpp:28)
     double art_stre_coe;       // artificial stress coefficient (0: off)
+    int ss_type;               // soil-structure contact: 0 none, 1 rigid, 2 deformable, 3 penalty
+    double ss_myu, ss_zeta;
     int bulk;                  // 1: the FP32-bulk form (pair records in FP32)
 };
 
@@ -93,6 +95,14 @@ struct DevState {
     // p = water, soil, air, structure (12N), and the velocity tm_boundary
     // reads (after XSPH and velocity_set_domain, before check_domain; 3N)
     double *vel_bndy, *vb, *vx_vb;
+    // soil-structure contact (ss_type 1-3): per water/soil particle the
+    // structure particles it pushes (ss_id, 3N, -1 = none) with the forces
+    // they take from it (ss_con, 18N: per slot q the normal then the
+    // tangential force, component k at (q * 6 + c) * N + i, signed as the
+    // reference applies them) and its own forces (ss_own, 6N: normal, then
+    // tangential); per structure particle the gathered forces (ss_fs, 6N)
+    int *ss_id;
+    double *ss_con, *ss_own, *ss_fs;
     // NNPS
     int *cell;                 // cell id per particle
     uint32_t *key_in, *key_out;

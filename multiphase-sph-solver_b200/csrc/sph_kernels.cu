@@ -1107,6 +1107,26 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
             d.s.interf[k * N + i] = itf;
         }
     }
+    if (d.p.ss_type >= 1 && (ti == 1 || ti == 2 || ti == 4)) {
+        // the contact forces into interfss and the acceleration
+        // (CPP_10-1-interact_ss.cpp:1008-1034 and the same sums of the rigid
+        // and deformable forms, which scale them by zeta)
+        const bool own = (ti != 4) && d.s.ss_id[i] >= 0;
+        double fn[3] = {0, 0, 0}, ft[3] = {0, 0, 0};
+        if (ti == 4) {
+            for (int k = 0; k < 3; k++) { fn[k] = d.s.ss_fs[(size_t)k * N + i]; ft[k] = d.s.ss_fs[(size_t)(3 + k) * N + i]; }
+        } else if (own) {
+            for (int k = 0; k < 3; k++) { fn[k] = d.s.ss_own[(size_t)k * N + i]; ft[k] = d.s.ss_own[(size_t)(3 + k) * N + i]; }
+        }
+        const double mi = d.s.mass[i];
+        for (int k = 0; k < 3; k++) {
+            double f = 0.0;
+            if (d.p.ss_type != 3) f += d.p.ss_zeta * (ft[k] + fn[k]);
+            else f += ft[k] + fn[k];
+            d.s.interfss[k * N + i] = f;
+            ax[k] += f / mi;
+        }
+    }
     if (damping) {
         for (int k = 0; k < nd; k++) {
             double vx1 = vi[k] + 0.5 * (axp[k] + ax[k]) * dt;
@@ -1138,7 +1158,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
                 vout[k] = vi[k] + ath * dt;
             }
         }
-    } else {   // if_move == 1 (2 and 3 are rejected at create)
+    } else if (d.p.if_move == 1) {
         if (ti == 0 && mt == 2 && *d.s.step > d.p.inip) {
             for (int k = 0; k < nd; k++) d.s.interfss[k * N + i] = d.p.move_vx[k];
         } else if (ti == 0) {
@@ -1148,6 +1168,24 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
                 double ath = (axp[k] + ax[k]) * 0.5;
                 vout[k] = vi[k] + ath * dt;
             }
+        }
+    } else {
+        // if_move 2 (soil) / 3 (structure) with etype 5 driven at move_vx after
+        // inip (CPP_11-xsph.cpp:92-141); every particle then takes
+        // v = vxp + (axp + ax) dt / 2, walls included
+        const int tmove = (d.p.if_move == 2) ? 2 : 4;
+        double vp[3] = {vi[0], vi[1], vi[2]};
+        if (ti == tmove && d.s.etype[i] == 5 && *d.s.step > d.p.inip) {
+            for (int k = 0; k < nd; k++) {
+                axp[k] = 0.0;
+                vp[k] = d.p.move_vx[k];
+                vout[k] = d.p.move_vx[k];
+                ax[k] = 0.0;
+            }
+        }
+        for (int k = 0; k < nd; k++) {
+            double ath = (axp[k] + ax[k]) * 0.5;
+            vout[k] = vp[k] + ath * dt;
         }
     }
     for (int k = 0; k < 3; k++) {
@@ -1248,12 +1286,14 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
             for (int k = 0; k < 3; k++) vn[k] = (i > w0) ? d.s.interfss[k * N + w0] : 0.0;
         }
     }
-    // update
+    // update (vxp is move_vx for the particles if_move 2 / 3 drives)
     const int loop = *d.s.step - d.p.inip;
     double xn[3] = {I.x[0], I.x[1], I.x[2]};
+    const bool driven = d.p.if_move >= 2 && ti == ((d.p.if_move == 2) ? 2 : 4) && d.s.etype[i] == 5 &&
+                        *d.s.step > d.p.inip;
     if (ti != 0) {
         for (int k = 0; k < nd; k++) {
-            const double vp = d.s.vxp[k * N + i];
+            const double vp = driven ? d.p.move_vx[k] : d.s.vxp[k * N + i];
             xn[k] = I.x[k] + (vn[k] + vp) * dt * 0.5;
             double u = d.s.ux[k * N + i];
             u = (loop == 0) ? 0.0 : u + (vn[k] + vp) * dt * 0.5;
@@ -1404,6 +1444,271 @@ __global__ void __launch_bounds__(128) k_tm_wall(Dev d)
     for (int p = 0; p < 4; p++)
         for (int k = 0; k < 3; k++)
             d.s.vb[(size_t)(p * 3 + k) * N + i] = (fabs(down[p]) > 1.0e-6) ? up[p][k] / down[p] : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// Soil-structure contact: interaction_ss_rigid / _deformable / _penalty
+// (CPP_10-1-interact_ss.cpp:17-1036, geometry helpers :1039-1369).  The
+// reference scatters each contact's reaction onto the two (2-D) or three
+// (3-D) structure particles it touches, accumulating per thread; here each
+// water / soil particle records its contact (k_ss_pair) and each structure
+// particle gathers its reactions in ascending particle order (k_ss_struct),
+// the order one reference thread applies them in.
+
+struct SSPt { double x, y, z; };
+
+__device__ __forceinline__ SSPt ss_pt(const Dev& d, int i)
+{
+    const Pos p = load_pos(d.s.xh, i);
+    return SSPt{p.x, p.y, p.z};
+}
+
+// linear_interpolate (:1187-1202)
+__device__ __forceinline__ void ss_interp(SSPt P1, SSPt P2, SSPt r, double m1, double m2, const double v1[3],
+                                          const double v2[3], double* m, double v[3])
+{
+    const double xk1 = 0.0;
+    const double xk2 = sqrt((P2.x - P1.x) * (P2.x - P1.x) + (P2.y - P1.y) * (P2.y - P1.y) + (P2.z - P1.z) * (P2.z - P1.z));
+    const double xp = sqrt((r.x - P1.x) * (r.x - P1.x) + (r.y - P1.y) * (r.y - P1.y) + (r.z - P1.z) * (r.z - P1.z));
+    *m = (m1 * fabs(xp - xk2) + m2 * fabs(xp - xk1)) / fabs(xk2 - xk1);
+    for (int k = 0; k < 3; k++) v[k] = (v1[k] * fabs(xp - xk2) + v2[k] * fabs(xp - xk1)) / fabs(xk2 - xk1);
+}
+
+// linear_interpolate_force (:1204-1222)
+__device__ __forceinline__ void ss_interp_force(SSPt P1, SSPt P2, SSPt r, const double f[3], double f1[3], double f2[3])
+{
+    const double xk1 = 0.0;
+    const double xk2 = sqrt((P2.x - P1.x) * (P2.x - P1.x) + (P2.y - P1.y) * (P2.y - P1.y) + (P2.z - P1.z) * (P2.z - P1.z));
+    const double xp = sqrt((r.x - P1.x) * (r.x - P1.x) + (r.y - P1.y) * (r.y - P1.y) + (r.z - P1.z) * (r.z - P1.z));
+    for (int k = 0; k < 3; k++) f1[k] = -fabs(xp - xk2) / fabs(xk1 - xk2) * f[k];
+    for (int k = 0; k < 3; k++) f2[k] = -fabs(xp - xk1) / fabs(xk1 - xk2) * f[k];
+}
+
+template <int ND>
+__global__ void __launch_bounds__(128) k_ss_pair(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    for (int q = 0; q < 3; q++) d.s.ss_id[(size_t)q * N + i] = -1;
+    const int ti = d.s.type[i];
+    if (!(ti == 1 || ti == 2)) return;
+    const int form = d.p.ss_type, nn = nbr_count(d, i);
+    const double dt = d.p.dt, dr = d.p.dr, myu = d.p.ss_myu, zeta = d.p.ss_zeta;
+    const double reach = (form == 1) ? 0.5 * dr : dr;
+    int ids[SPH_NB_CAP];
+    double dsts[SPH_NB_CAP];
+    int total = 0;
+    const SSPt p4 = ss_pt(d, i);
+    for (int q = 0; q < nn; q++) {
+        const int j = d.s.nbr[(size_t)q * N + i];
+        if (d.s.type[j] != 4) continue;
+        const SSPt pj = ss_pt(d, j);
+        const double dd = (p4.x - pj.x) * (p4.x - pj.x) + (p4.y - pj.y) * (p4.y - pj.y) + (p4.z - pj.z) * (p4.z - pj.z);
+        ids[total] = j;
+        dsts[total] = sqrt(dd);
+        total++;
+    }
+    for (int a = 0; a < 4; a++)   // clParti_Pair::dist_sorting
+        for (int b = a + 1; b < total; b++)
+            if (dsts[a] > dsts[b]) { const int t = ids[a]; ids[a] = ids[b]; ids[b] = t; }
+    if (total < ND) return;
+    const double mi = d.s.mass[i];
+    double vpi[3];
+    for (int k = 0; k < 3; k++) vpi[k] = d.s.vxp[(size_t)k * N + i];
+    const int id1 = ids[0], id2 = ids[1];
+    const SSPt p1 = ss_pt(d, id1), p2 = ss_pt(d, id2);
+    double v1[3], v2[3];
+    for (int k = 0; k < 3; k++) { v1[k] = d.s.vxp[(size_t)k * N + id1]; v2[k] = d.s.vxp[(size_t)k * N + id2]; }
+    double fn[3] = {0, 0, 0}, ft[3] = {0, 0, 0};
+    double con[3][6];                // reactions per slot: normal (3), tangential (3)
+    int sid[3] = {-1, -1, -1};
+    if (ND == 2) {
+        // cal_line (:1055-1060) with clLine()'s C = 1, cal_dpline, cal_mappoint_line (:1094-1125)
+        const double den = p2.y * p1.x - p1.y * p2.x;
+        const double A = (p1.y - p2.y) / den, B = (p2.x - p1.x) / den, C = 1.0;
+        const double tmp0 = sqrt(A * A + B * B);
+        const double dp = (tmp0 > 1.0e-3) ? fabs(A * p4.x + B * p4.y + C) / tmp0 : 0.0;
+        const double tmp = sqrt(A * A + B * B);
+        const SSPt P1 = {p4.x + dp * A / tmp, p4.y + dp * B / tmp, 0.0}, P2 = {p4.x - dp * A / tmp, p4.y - dp * B / tmp, 0.0};
+        const double dp1 = (tmp0 > 1.0e-3) ? fabs(A * P1.x + B * P1.y + C) / tmp0 : 0.0;
+        SSPt outp = (dp1 < 1.0e-3) ? P1 : P2;
+        outp.z = 0.0;
+        // check_ifinside_line (:1290-1305) with the mapped point's z = 0
+        const double v0x = p2.x - p1.x, v0y = p2.y - p1.y, v0z = p2.z - p1.z;
+        const double w1x = outp.x - p1.x, w1y = outp.y - p1.y, w1z = 0.0 - p1.z;
+        const double dot00 = v0x * v0x + v0y * v0y + v0z * v0z, dot01 = v0x * w1x + v0y * w1y + v0z * w1z;
+        const double u = 1.0 / dot00 * dot01;
+        if ((u < 0 || u > 1) || !(dp < reach)) return;
+        // clLine::set_normal, check_ifoutward2D (:1252-1270)
+        double nx = 0.0, ny = 0.0;
+        const double tot = sqrt(A * A + B * B);
+        if (tot > 1.0e-10) { nx = A / tot; ny = B / tot; }
+        const double dot = (outp.x - p4.x) * nx + (outp.y - p4.y) * ny + 0.0 * 0.0;
+        if (!(dot <= 0.0)) { nx = -nx; ny = -ny; }
+        double ms, vs[3];
+        ss_interp(p1, p2, outp, d.s.mass[id1], d.s.mass[id2], v1, v2, &ms, vs);
+        vs[0] -= vpi[0];
+        vs[1] -= vpi[1];
+        if (form != 1) {
+            vs[0] *= ms / (ms + mi);
+            vs[1] *= ms / (ms + mi);
+        }
+        const double v = vs[0] * nx + vs[1] * ny;   // decomposition_velocity2D (:1346-1356)
+        double vt[2] = {vs[0] - v * nx, vs[1] - v * ny};
+        const double vn[2] = {v * nx, v * ny};
+        if (form == 3) {
+            const double mag = (1.0 - zeta) * 2.0 * mi * (dr - dp) / dt / dt;
+            fn[0] = mag * nx; fn[1] = mag * ny;
+        } else {
+            fn[0] = mi * vn[0] / dt; fn[1] = mi * vn[1] / dt;
+        }
+        ft[0] = mi * vt[0] / dt; ft[1] = mi * vt[1] / dt;
+        const double mag_fn = sqrt(fn[0] * fn[0] + fn[1] * fn[1]);
+        const double mag_ft = sqrt(ft[0] * ft[0] + ft[1] * ft[1]);
+        if (mag_ft > (mag_fn * myu)) {
+            vt[0] = vt[0] * myu * mag_fn / mag_ft;
+            vt[1] = vt[1] * myu * mag_fn / mag_ft;
+            ft[0] = mi * vt[0] / dt; ft[1] = mi * vt[1] / dt;
+        }
+        double f1n[3], f2n[3], f1t[3], f2t[3];
+        ss_interp_force(p1, p2, outp, fn, f1n, f2n);
+        ss_interp_force(p1, p2, outp, ft, f1t, f2t);
+        sid[0] = id1; sid[1] = id2;
+        for (int k = 0; k < 3; k++) {
+            con[0][k] = f1n[k]; con[0][3 + k] = f1t[k];
+            con[1][k] = f2n[k]; con[1][3 + k] = f2t[k];
+        }
+    } else {
+        const int id3 = ids[2];
+        const SSPt p3 = ss_pt(d, id3);
+        // cal_plane (:1063-1076) with clPlane()'s D = 1
+        const double den = -p1.x * (p2.y * p3.z - p3.y * p2.z) - p2.x * (p3.y * p1.z - p1.y * p3.z) -
+                           p3.x * (p1.y * p2.z - p2.y * p1.z);
+        double A = p1.y * (p2.z - p3.z) + p2.y * (p3.z - p1.z) + p3.y * (p1.z - p2.z);
+        double B = p1.z * (p2.x - p3.x) + p2.z * (p3.x - p1.x) + p3.z * (p1.x - p2.x);
+        double C = p1.x * (p2.y - p3.y) + p2.x * (p3.y - p1.y) + p3.x * (p1.y - p2.y);
+        A = A / den; B = B / den; C = C / den;
+        const double D = 1.0;
+        const double tmp0 = sqrt(A * A + B * B + C * C);
+        const double dp = (tmp0 > 1.0e-3) ? fabs(A * p4.x + B * p4.y + C * p4.z + D) / tmp0 : 0.0;
+        // cal_mappoint_plane (:1127-1160)
+        const double tmp = sqrt(A * A + B * B + C * C);
+        const SSPt P1 = {p4.x + dp * A / tmp, p4.y + dp * B / tmp, p4.z + dp * C / tmp};
+        const SSPt P2 = {p4.x - dp * A / tmp, p4.y - dp * B / tmp, p4.z - dp * C / tmp};
+        const double dp1 = (tmp0 > 1.0e-3) ? fabs(A * P1.x + B * P1.y + C * P1.z + D) / tmp0 : 0.0;
+        const SSPt outp = (dp1 < 1.0e-3) ? P1 : P2;
+        // check_ifinside_triangle (:1307-1344)
+        const double a0[3] = {p3.x - p1.x, p3.y - p1.y, p3.z - p1.z};
+        const double a1[3] = {p2.x - p1.x, p2.y - p1.y, p2.z - p1.z};
+        const double a2[3] = {outp.x - p1.x, outp.y - p1.y, outp.z - p1.z};
+        const double dot00 = a0[0] * a0[0] + a0[1] * a0[1] + a0[2] * a0[2];
+        const double dot01 = a0[0] * a1[0] + a0[1] * a1[1] + a0[2] * a1[2];
+        const double dot02 = a0[0] * a2[0] + a0[1] * a2[1] + a0[2] * a2[2];
+        const double dot11 = a1[0] * a1[0] + a1[1] * a1[1] + a1[2] * a1[2];
+        const double dot12 = a1[0] * a2[0] + a1[1] * a2[1] + a1[2] * a2[2];
+        const double inv = 1 / (dot00 * dot11 - dot01 * dot01);
+        const double u = (dot11 * dot02 - dot01 * dot12) * inv;
+        bool inside;
+        if (u < 0 || u > 1) inside = false;
+        else {
+            const double v = (dot00 * dot12 - dot01 * dot02) * inv;
+            inside = (v < 0 || v > 1) ? false : (u + v <= 1);
+        }
+        if (!(inside && dp < reach)) return;
+        // clPlane::set_normal, check_ifoutward3D (:1272-1288)
+        double nx = 0.0, ny = 0.0, nz = 0.0;
+        const double tot = sqrt(A * A + B * B + C * C);
+        if (tot > 1.0e-10) { nx = A / tot; ny = B / tot; nz = C / tot; }
+        const double dot = (outp.x - p4.x) * nx + (outp.y - p4.y) * ny + (outp.z - p4.z) * nz;
+        if (!(dot <= 0.0)) { nx = -nx; ny = -ny; nz = -nz; }
+        // cal_line3D (:1078-1092) of (p1, p2) and (p3, outp); cal_intersect_lines3D (:1162-1185)
+        const double d1 = sqrt((p2.x - p1.x) * (p2.x - p1.x) + (p2.y - p1.y) * (p2.y - p1.y) + (p2.z - p1.z) * (p2.z - p1.z));
+        const double la = (p2.x - p1.x) / d1, lb = (p2.y - p1.y) / d1, lc = (p2.z - p1.z) / d1;
+        const double d2 = sqrt((outp.x - p3.x) * (outp.x - p3.x) + (outp.y - p3.y) * (outp.y - p3.y) +
+                               (outp.z - p3.z) * (outp.z - p3.z));
+        const double ma = (outp.x - p3.x) / d2, mb = (outp.y - p3.y) / d2;
+        const double flag = la * mb - ma * lb;
+        if (!(fabs(flag) > 1.0e-3)) return;
+        const double tu = ma * (p1.y - p3.y) - mb * (p1.x - p3.x);
+        const double t = tu / flag;
+        const SSPt sectp = {p1.x + la * t, p1.y + lb * t, p1.z + lc * t};
+        double v3[3];
+        for (int k = 0; k < 3; k++) v3[k] = d.s.vxp[(size_t)k * N + id3];
+        double tms, tvs[3], ms, vs[3];
+        ss_interp(p1, p2, sectp, d.s.mass[id1], d.s.mass[id2], v1, v2, &tms, tvs);
+        ss_interp(p3, sectp, outp, d.s.mass[id3], tms, v3, tvs, &ms, vs);
+        for (int k = 0; k < 3; k++) {
+            vs[k] -= vpi[k];
+            if (form != 1) vs[k] *= ms / (ms + mi);
+        }
+        const double v = vs[0] * nx + vs[1] * ny + vs[2] * nz;   // decomposition_velocity3D (:1358-1369)
+        const double vn[3] = {v * nx, v * ny, v * nz};
+        double vt[3] = {vs[0] - vn[0], vs[1] - vn[1], vs[2] - vn[2]};
+        if (form == 3) {
+            const double mag = (1.0 - zeta) * 2.0 * mi * (dr - dp) / dt / dt;
+            fn[0] = mag * nx; fn[1] = mag * ny; fn[2] = mag * nz;
+        } else {
+            for (int k = 0; k < 3; k++) fn[k] = mi * vn[k] / dt;
+        }
+        for (int k = 0; k < 3; k++) ft[k] = mi * vt[k] / dt;
+        const double mag_fn = sqrt(fn[0] * fn[0] + fn[1] * fn[1] + fn[2] * fn[2]);
+        const double mag_ft = sqrt(ft[0] * ft[0] + ft[1] * ft[1] + ft[2] * ft[2]);
+        if (mag_ft > (mag_fn * myu)) {
+            for (int k = 0; k < 3; k++) vt[k] = vt[k] * myu * mag_fn / mag_ft;
+            for (int k = 0; k < 3; k++) ft[k] = mi * vt[k] / dt;
+        }
+        double f1n[3], f3n[3], f1t[3], f3t[3], g1n[3], g2n[3], g1t[3], g2t[3];
+        ss_interp_force(p3, sectp, outp, fn, f1n, f3n);
+        ss_interp_force(p3, sectp, outp, ft, f1t, f3t);
+        ss_interp_force(p1, p2, sectp, f3n, g1n, g2n);
+        ss_interp_force(p1, p2, sectp, f3t, g1t, g2t);
+        // id3 takes + (f1n, f1t); id1 and id2 take - (g1, g2), as the reference applies them
+        sid[0] = id3; sid[1] = id1; sid[2] = id2;
+        for (int k = 0; k < 3; k++) {
+            con[0][k] = f1n[k]; con[0][3 + k] = f1t[k];
+            con[1][k] = -g1n[k]; con[1][3 + k] = -g1t[k];
+            con[2][k] = -g2n[k]; con[2][3 + k] = -g2t[k];
+        }
+    }
+    for (int q = 0; q < 3; q++) {
+        d.s.ss_id[(size_t)q * N + i] = sid[q];
+        if (sid[q] >= 0)
+            for (int c = 0; c < 6; c++) d.s.ss_con[(size_t)(q * 6 + c) * N + i] = con[q][c];
+    }
+    for (int k = 0; k < 3; k++) {
+        d.s.ss_own[(size_t)k * N + i] = fn[k];
+        d.s.ss_own[(size_t)(3 + k) * N + i] = ft[k];
+    }
+}
+
+// each structure particle's reactions, added in ascending order of the
+// particles they come from (x - y is x + (-y) in IEEE arithmetic, so the
+// reference's "-=" reactions are stored negated and added)
+__global__ void __launch_bounds__(128) k_ss_struct(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    if (d.s.type[i] != 4) return;
+    const int nn = nbr_count(d, i);
+    int src[SPH_NB_CAP], slot[SPH_NB_CAP];
+    int m = 0;
+    for (int q = 0; q < nn; q++) {
+        const int j = d.s.nbr[(size_t)q * N + i];
+        const int tj = d.s.type[j];
+        if (!(tj == 1 || tj == 2)) continue;
+        for (int s = 0; s < 3; s++)
+            if (d.s.ss_id[(size_t)s * N + j] == i) {
+                // insertion by source index
+                int p = m++;
+                while (p > 0 && src[p - 1] > j) { src[p] = src[p - 1]; slot[p] = slot[p - 1]; p--; }
+                src[p] = j;
+                slot[p] = s;
+            }
+    }
+    double f[6] = {0, 0, 0, 0, 0, 0};
+    for (int e = 0; e < m; e++)
+        for (int c = 0; c < 6; c++) f[c] += d.s.ss_con[(size_t)(slot[e] * 6 + c) * N + src[e]];
+    for (int c = 0; c < 6; c++) d.s.ss_fs[(size_t)c * N + i] = f[c];
 }
 
 __global__ void k_step_done(Dev d)
@@ -1629,6 +1934,10 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
     if (art) { LAUNCH_ND(k_art_rij, nblk(N, 128), 128, d); n++; }
     REC(15);
     LAUNCH_ND(k_accel_a, nblk(N, 128), 128, d); n++;
+    if (d.p.ss_type >= 1) {
+        LAUNCH_ND(k_ss_pair, nblk(N, 128), 128, d); n++;
+        k_ss_struct<<<nblk(N, 128), 128, 0, st>>>(d); n++;
+    }
     REC(16);
     if (art) {
         if (d.p.ndim == 2) k_accel_b<2, 1><<<nblk(N, 128), 128, 0, st>>>(d);

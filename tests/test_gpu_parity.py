@@ -297,3 +297,23 @@ def test_tm_boundary_walls(name, steps):
         eng.step(chunk)
         assert orc.step(chunk) == 0
     _compare(eng, orc)
+
+
+@pytest.mark.parametrize("ndim,dx,ss_type", [(2, 0.04, 1), (2, 0.04, 2), (2, 0.04, 3), (3, 0.1, 2), (3, 0.1, 3)])
+def test_soil_structure_contact(ndim, dx, ss_type):
+    """A footing (type 4) driven into soil (if_move 3) with the rigid (1),
+    deformable (2) or penalty (3) soil-structure contact: bit-identical to the
+    oracle, whose same runs are bit-identical to the reference (golden
+    footing_* fixtures).  The contact forces gathered by the structure
+    particles follow the order one reference thread accumulates them in."""
+    sc = scenes.footing(ndim=ndim, dx=dx, bed=(1.2, 0.6, 0.5), width=0.4, height=0.2, gap=0.4,
+                        ss_type=ss_type, zeta=0.1, v=0.5)
+    st, eng, orc = _engine_and_oracle(sc)
+    touched = 0
+    for _ in range(12):
+        eng.step(1)
+        assert orc.step(1) == 0
+        f = eng.get_field("interfss")
+        touched += int((np.abs(f[st.fields["type"] == 2]).sum(axis=1) > 0).sum())
+    _compare(eng, orc)
+    assert touched > 0
