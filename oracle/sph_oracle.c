@@ -30,6 +30,8 @@ struct orc_ctx {
     /* cl_bndy_pair::vel_bndy and clVar_Boundary::vx_* (Class_particle.h:172-207),
      * the wall virtual velocities of flbndy 2 */
     double *vel_bndy, *vb_water, *vb_soil, *vb_air, *vb_struct;
+    /* clVar_Boundary::sig_* (flbndy 3/4/13/14) */
+    double *sb_water, *sb_soil, *sb_air, *sb_struct;
     /* clInterf_SS of the one thread (f_n, f_t) of the soil-structure contact */
     double *ss_fn, *ss_ft;
     /* per-particle material records (pVFluid, pParti_ConsPara) */
@@ -65,6 +67,7 @@ static const field_desc k_fields[] = {
     FI(type), FI(matype), FI(permtype), FI(etype),
     FD(vel_bndy, 3), FD(vb_water, 3), FD(vb_soil, 3), FD(vb_air, 3), FD(vb_struct, 3),
     FD(ss_fn, 3), FD(ss_ft, 3),
+    FD(sb_water, 6), FD(sb_soil, 6), FD(sb_air, 6), FD(sb_struct, 6),
 };
 #define NFIELDS (sizeof(k_fields) / sizeof(k_fields[0]))
 
@@ -1429,6 +1432,40 @@ static void boundary_moving_stress_effect(orc_ctx* c)
     }
 }
 
+/* boundary_stress_effect_tran: CPP_9-4-derivation_stress.cpp:725-846, the wall
+ * stress of flbndy 3/4/13/14 with the wall's Shepard-extrapolated stress of
+ * the particle's phase */
+static void boundary_stress_effect_tran(orc_ctx* c)
+{
+    for (int i = 0; i < c->n; i++) {
+        int ti = c->type[i];
+        if (ti == 0 || ti == 7) continue;
+        double tu[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        const double* wall = ti == 1 ? c->sb_water : ti == 2 ? c->sb_soil : ti == 3 ? c->sb_air : ti == 4 ? c->sb_struct : 0;
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj);
+            if (c->type[j] != 0) continue;
+            double ai[6] = {0, 0, 0, 0, 0, 0}, aj[6] = {0, 0, 0, 0, 0, 0};
+            const double* s = &c->sig[i * 6];
+            if (ti == 2) {
+                double satu = c->satu[i];
+                ai[0] = s[0] - satu * c->prew[i] + (1 - satu) * c->prea[i];
+                ai[1] = s[1] - satu * c->prew[i] + (1 - satu) * c->prea[i];
+                ai[2] = s[2] - satu * c->prew[i] + (1 - satu) * c->prea[i];
+                ai[3] = s[3]; ai[4] = s[4]; ai[5] = s[5];
+            } else if (ti == 1 || ti == 3 || ti == 4) {
+                for (int k = 0; k < 6; k++) ai[k] = s[k];
+            }
+            if (wall)
+                for (int k = 0; k < 6; k++) aj[k] = wall[j * 6 + k];
+            stress_pair(tu, c->mass[j], aj, ai, c->rho[j], c->rho[i], &W(i, nj, 0), 1.0);
+        }
+        c->ax[i * 3 + 0] += tu[0][0] + tu[0][1] + tu[0][2];
+        c->ax[i * 3 + 1] += tu[1][0] + tu[1][1] + tu[1][2];
+        c->ax[i * 3 + 2] += tu[2][0] + tu[2][1] + tu[2][2];
+    }
+}
+
 /* Soil-water drag coefficient beta of interact2 (Tsuji et al. 1993 / Shi et al.
  * 2018, CPP_10-interact1.cpp:154-176) and interact3 (Peng et al. 2017,
  * :294-306), for soil particle s and water particle w; rho_w is the density
@@ -2045,6 +2082,68 @@ static void interaction_ss(orc_ctx* c)
     }
 }
 
+/* no_slip_tran / free_slip_tran: CPP_13-boundary.cpp:711-958 and 960-1237.
+ * Each wall particle's Shepard sums over its water, soil, air and structure
+ * neighbours give its stress per phase (soil with the pore terms) and its
+ * virtual velocity per phase: the wall's own velocity minus the phase's mean
+ * velocity (no-slip), or plus the phase's mean tangential velocity taken from
+ * neighbours more than 0.1 dr away (free-slip).  (The reference's rho_* are
+ * formed but never read; they are not kept.) */
+static void tran_walls(orc_ctx* c, int free_slip)
+{
+    const double dr = c->P.dr;
+    double* sig_out[4] = {c->sb_water, c->sb_soil, c->sb_air, c->sb_struct};
+    double* vel_out[4] = {c->vb_water, c->vb_soil, c->vb_air, c->vb_struct};
+    for (int i = 0; i < c->n; i++) {
+        if (c->type[i] != 0) continue;
+        double us[4][6], uv[4][3], down[4];
+        for (int p = 0; p < 4; p++) {
+            for (int k = 0; k < 6; k++) us[p][k] = 0.0;
+            for (int k = 0; k < 3; k++) uv[p][k] = 0.0;
+            down[p] = 0.0;
+        }
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj), tj = c->type[j];
+            if (tj < 1 || tj > 4) continue;
+            int p = tj - 1;
+            double mj = c->mass[j], rj = c->rho[j], w3 = W(i, nj, 3);
+            const double* sj = &c->sig[j * 6];
+            const double* vj = &c->vx[j * 3];
+            if (tj == 2) {
+                double satu = c->satu[j];
+                for (int k = 0; k < 3; k++)
+                    us[p][k] = us[p][k] + mj * (sj[k] - satu * c->prew[j] + (1 - satu) * c->prea[j]) * w3 / rj;
+                for (int k = 3; k < 6; k++) us[p][k] = us[p][k] + mj * sj[k] * w3 / rj;
+            } else {
+                for (int k = 0; k < 6; k++) us[p][k] = us[p][k] + mj * sj[k] * w3 / rj;
+            }
+            if (free_slip) {
+                double v1[3] = {c->xp[i * 3] - c->xp[j * 3], c->xp[i * 3 + 1] - c->xp[j * 3 + 1],
+                                c->xp[i * 3 + 2] - c->xp[j * 3 + 2]};
+                double dst = sqrt(v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2]);
+                double inprod = vj[0] * v1[0] + vj[1] * v1[1] + vj[2] * v1[2];
+                if (dst > 0.1 * dr)
+                    for (int k = 0; k < 3; k++)
+                        uv[p][k] = uv[p][k] + mj * (vj[k] - inprod * v1[k] / dst / dst) * w3 / rj;
+            } else {
+                for (int k = 0; k < 3; k++) uv[p][k] = uv[p][k] + mj * vj[k] * w3 / rj;
+            }
+            down[p] = down[p] + mj * w3 / rj;
+        }
+        const double* its = &c->interfss[i * 3];
+        for (int p = 0; p < 4; p++) {
+            if (fabs(down[p]) > 1.0e-6) {
+                for (int k = 0; k < 6; k++) sig_out[p][i * 6 + k] = us[p][k] / down[p];
+                for (int k = 0; k < 3; k++)
+                    vel_out[p][i * 3 + k] = free_slip ? its[k] + uv[p][k] / down[p] : its[k] - uv[p][k] / down[p];
+            } else {
+                for (int k = 0; k < 6; k++) sig_out[p][i * 6 + k] = 0.0;
+                for (int k = 0; k < 3; k++) vel_out[p][i * 3 + k] = its[k];
+            }
+        }
+    }
+}
+
 /* check_domain: CPP_13-boundary.cpp:20-68, in the sequential order (vbx is
  * taken from the first wall particle with matype > 2 and applies to the
  * particles after it) */
@@ -2184,7 +2283,7 @@ static void kernel_gradient_correction(orc_ctx* c)
 
 static int check_supported(const sphgpu_params* P)
 {
-    if (P->flbndy != 1 && P->flbndy != 2) return SPHGPU_E_UNSUPPORTED;
+    if (!(P->flbndy >= 1 && P->flbndy <= 4) && P->flbndy != 13 && P->flbndy != 14) return SPHGPU_E_UNSUPPORTED;
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
     if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
     if (P->fli < 0 || P->fli > 3 || P->ss_type < 0 || P->ss_type > 3) return SPHGPU_E_UNSUPPORTED;
@@ -2221,7 +2320,8 @@ int orc_step(orc_ctx* c, int nsteps)
         structure_acceleration(c);
         artificial_viscosity(c);
         if (P->art_stre_coe > 0.0) artificial_stress(c);
-        boundary_moving_stress_effect(c);    /* flv == 0, flbndy 1 or 2 */
+        if (P->flbndy == 1 || P->flbndy == 2) boundary_moving_stress_effect(c);   /* flv == 0 */
+        else boundary_stress_effect_tran(c);
         if (P->fli >= 1) interact(c, P->fli);
         if (P->ss_type >= 1 && P->ss_type <= 3) interaction_ss(c);
         if (c->l <= P->inip) soil_damping_geostress(c);
@@ -2229,6 +2329,10 @@ int orc_step(orc_ctx* c, int nsteps)
         if (P->if_move != 2) xsph(c);
         if (P->flbndy == 1) tmboundary(c);
         else if (P->flbndy == 2) { velocity_set_domain(c); tm_boundary(c); }
+        else if (P->flbndy == 3) tran_walls(c, 0);
+        else if (P->flbndy == 4) tran_walls(c, 1);
+        else if (P->flbndy == 13) { velocity_set_domain(c); tran_walls(c, 0); }
+        else if (P->flbndy == 14) { velocity_set_domain(c); tran_walls(c, 1); }
         check_domain(c);
         update(c);
         c->l++;

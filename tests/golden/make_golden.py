@@ -78,12 +78,14 @@ def _column_model(matype, **record):
     return lambda: scenes.set_soil_model(scenes.soil_column_3d(dx=0.1, steps=200), matype, **record)
 
 
-def _tm_boundary(factory):
-    """A scene with the Takeda-Morris wall treatment of flbndy 2
-    (velocity_set_domain + tm_boundary_2d / tm_boundary_3d, coe_bndy 0.3)."""
+def _tm_boundary(factory, flbndy=2):
+    """A scene with another wall treatment: flbndy 2 (velocity_set_domain +
+    tm_boundary_2d / tm_boundary_3d), 3 / 4 (no_slip_tran / free_slip_tran)
+    or 13 / 14 (velocity_set_domain + no_slip_tran / free_slip_tran),
+    coe_bndy 0.3."""
     def make():
         sc = factory()
-        sc.flags["flbndy"] = 2
+        sc.flags["flbndy"] = flbndy
         return sc
     return make
 
@@ -110,6 +112,10 @@ CASES = {
     "soil_column_3d_dx0.1_visco_elastic": (_column_model(7, c=1.0e5, e=1.0e7), 20),
     "dam_break_2d_dx0.04_tm_boundary": (_tm_boundary(lambda: scenes.dam_break_2d(dx=0.04, steps=200)), 25),
     "soil_column_3d_dx0.1_tm_boundary": (_tm_boundary(lambda: scenes.soil_column_3d(dx=0.1, steps=200)), 15),
+    "dam_break_2d_dx0.04_no_slip": (_tm_boundary(lambda: scenes.dam_break_2d(dx=0.04, steps=200), 3), 25),
+    "dam_break_2d_dx0.04_free_slip_vsd": (_tm_boundary(lambda: scenes.dam_break_2d(dx=0.04, steps=200), 14), 25),
+    "soil_column_3d_dx0.1_free_slip": (_tm_boundary(lambda: scenes.soil_column_3d(dx=0.1, steps=200), 4), 15),
+    "soil_column_3d_dx0.1_no_slip_vsd": (_tm_boundary(lambda: scenes.soil_column_3d(dx=0.1, steps=200), 13), 15),
     "footing_2d_rigid": (_footing(2, 0.04, 1), 12),
     "footing_2d_deformable": (_footing(2, 0.04, 2), 12),
     "footing_2d_penalty": (_footing(2, 0.04, 3), 12),
