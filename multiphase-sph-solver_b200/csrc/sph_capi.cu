@@ -143,7 +143,7 @@ int check_params(const sphgpu_params* P)
     if (!(P->dr > 0.0) || !(P->dt > 0.0)) return SPHGPU_E_ARG;
     if (P->step_regu <= 0) return SPHGPU_E_ARG;
     // flag combinations this engine runs (the others are rejected loudly)
-    if (P->flbndy != 1 && P->flbndy != 2) return SPHGPU_E_UNSUPPORTED;
+    if (!(P->flbndy >= 1 && P->flbndy <= 4) && P->flbndy != 13 && P->flbndy != 14) return SPHGPU_E_UNSUPPORTED;
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
     if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
     if (P->fli < 0 || P->fli > 3) return SPHGPU_E_UNSUPPORTED;
@@ -344,6 +344,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
         r |= dalloc(c, &s.vel_bndy, 3 * (size_t)N);
         r |= dalloc(c, &s.vb, 12 * (size_t)N);
         r |= dalloc(c, &s.vx_vb, 3 * (size_t)N);
+        if (P->flbndy != 2) r |= dalloc(c, &s.sb, 24 * (size_t)N);
     }
     r |= dalloc(c, &s.vx, 3 * (size_t)N); r |= dalloc(c, &s.vx_next, 3 * (size_t)N);
     r |= dalloc(c, &s.vxp, 3 * (size_t)N); r |= dalloc(c, &s.axp, 3 * (size_t)N); r |= dalloc(c, &s.ax, 3 * (size_t)N);

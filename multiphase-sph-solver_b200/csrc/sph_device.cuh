@@ -95,6 +95,9 @@ struct DevState {
     // p = water, soil, air, structure (12N), and the velocity tm_boundary
     // reads (after XSPH and velocity_set_domain, before check_domain; 3N)
     double *vel_bndy, *vb, *vx_vb;
+    // flbndy 3/4/13/14: the walls' clVar_Boundary stresses per phase,
+    // sb[(p * 6 + k) * N + i] (24N)
+    double *sb;
     // soil-structure contact (ss_type 1-3): per water/soil particle the
     // structure particles it pushes (ss_id, 3N, -1 = none) with the forces
     // they take from it (ss_con, 18N: per slot q the normal then the

@@ -945,11 +945,15 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
     // wall-stress operand of particle i (:668-700) and its own half
     real ab[6] = {0, 0, 0, 0, 0, 0}, abr[6] = {0, 0, 0, 0, 0, 0};
     const double satu_i = d.s.satu[i];
+    // flbndy 3/4/13/14: boundary_stress_effect_tran (CPP_9-4:725-846) takes the
+    // wall's stress for i's phase, and a structure particle's own stress
+    // without the pore terms
+    const bool tran = d.p.flbndy == 3 || d.p.flbndy == 4 || d.p.flbndy == 13 || d.p.flbndy == 14;
     if (moving) {
         double si[6];
         for (int k = 0; k < 6; k++) si[k] = d.s.sig_next[k * N + i];
         double abd[6];
-        if (fluid) {
+        if (fluid || (tran && ti == 4)) {
             for (int k = 0; k < 6; k++) abd[k] = si[k];
         } else {
             const double prew_i = d.s.prew[i], prea_i = d.s.prea[i];
@@ -998,7 +1002,11 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
         }
         if (b_pair) {
             real abj[6];
-            for (int k = 0; k < 6; k++) abj[k] = ab[k] / rj / rj;
+            if (tran)
+                for (int k = 0; k < 6; k++)
+                    abj[k] = (real)(d.s.sb[(size_t)((ti - 1) * 6 + k) * N + j] / d.s.rho[j] / d.s.rho[j]);
+            else
+                for (int k = 0; k < 6; k++) abj[k] = ab[k] / rj / rj;
             tb[0][0].add(mj * (abj[0] + abr[0]) * w[0]);
             tb[0][1].add(mj * (abj[3] + abr[3]) * w[1]);
             tb[0][2].add(mj * (abj[5] + abr[5]) * w[2]);
@@ -1244,7 +1252,8 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
     // tmboundary (flbndy 1, moving particles, a = b = 0.3) or
     // velocity_set_domain (flbndy 2, fluid particles, a = b = coe_bndy,
     // CPP_13-boundary.cpp:71-122): the same correction
-    const bool vcorr = (d.p.flbndy == 1 && moving) || (d.p.flbndy == 2 && (ti == 1 || ti == 3));
+    const bool vsd = d.p.flbndy == 2 || d.p.flbndy == 13 || d.p.flbndy == 14;
+    const bool vcorr = (d.p.flbndy == 1 && moving) || (vsd && (ti == 1 || ti == 3));
     if (vcorr) {
         const double a = (d.p.flbndy == 1) ? 0.30 : d.p.coe_bndy, b = a, dr = d.p.dr;
         double tb[3] = {0, 0, 0};
@@ -1269,7 +1278,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
         }
         for (int k = 0; k < nd; k++) vn[k] = vn[k] + tb[k];
     }
-    if (d.p.flbndy == 2 && moving)
+    if (d.p.flbndy != 1 && moving)
         for (int k = 0; k < 3; k++) d.s.vx_vb[k * N + i] = vn[k];
     if (ti != 0 && ti != 7) {
         const double dr = d.p.dr;
@@ -1711,6 +1720,70 @@ __global__ void __launch_bounds__(128) k_ss_struct(Dev d)
     for (int c = 0; c < 6; c++) d.s.ss_fs[(size_t)c * N + i] = f[c];
 }
 
+// no_slip_tran / free_slip_tran (CPP_13-boundary.cpp:711-958, 960-1237): each
+// wall particle's Shepard sums over its water, soil, air and structure
+// neighbours give its stress per phase (soil with the pore terms) and its
+// virtual velocity per phase: its own velocity minus the phase's mean velocity
+// (no-slip), or plus the mean velocity with the component along the
+// wall-particle line removed, from neighbours beyond 0.1 dr (free-slip).  The
+// velocities are those after XSPH (and velocity_set_domain), before
+// check_domain.
+__global__ void __launch_bounds__(128) k_tran_wall(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    if (d.s.type[i] != 0) return;
+    const bool free_slip = d.p.flbndy == 4 || d.p.flbndy == 14;
+    const int nn = nbr_count(d, i);
+    const Pos P = load_pos(d.s.xh, i);
+    const double dr = d.p.dr;
+    double us[4][6], uv[4][3], down[4];
+    for (int p = 0; p < 4; p++) {
+        for (int k = 0; k < 6; k++) us[p][k] = 0.0;
+        for (int k = 0; k < 3; k++) uv[p][k] = 0.0;
+        down[p] = 0.0;
+    }
+    for (int q = 0; q < nn; q++) {
+        const int j = d.s.nbr[(size_t)q * N + i];
+        const int tj = d.s.type[j];
+        if (tj < 1 || tj > 4) continue;
+        const int p = tj - 1;
+        real wr[4];
+        load_w(d, q, i, wr);
+        const double w3 = wr[3], mj = d.s.mass[j], rj = d.s.rho[j];
+        double sj[6], vj[3];
+        for (int k = 0; k < 6; k++) sj[k] = d.s.sig_next[(size_t)k * N + j];
+        for (int k = 0; k < 3; k++) vj[k] = d.s.vx_vb[(size_t)k * N + j];
+        if (tj == 2) {
+            const double satu = d.s.satu[j], pw = d.s.prew[j], pa = d.s.prea[j];
+            for (int k = 0; k < 3; k++) us[p][k] = us[p][k] + mj * (sj[k] - satu * pw + (1 - satu) * pa) * w3 / rj;
+            for (int k = 3; k < 6; k++) us[p][k] = us[p][k] + mj * sj[k] * w3 / rj;
+        } else {
+            for (int k = 0; k < 6; k++) us[p][k] = us[p][k] + mj * sj[k] * w3 / rj;
+        }
+        if (free_slip) {
+            const Pos pj = load_pos(d.s.xh, j);
+            const double v1[3] = {P.x - pj.x, P.y - pj.y, P.z - pj.z};
+            const double dst = sqrt(v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2]);
+            const double inprod = vj[0] * v1[0] + vj[1] * v1[1] + vj[2] * v1[2];
+            if (dst > 0.1 * dr)
+                for (int k = 0; k < 3; k++) uv[p][k] = uv[p][k] + mj * (vj[k] - inprod * v1[k] / dst / dst) * w3 / rj;
+        } else {
+            for (int k = 0; k < 3; k++) uv[p][k] = uv[p][k] + mj * vj[k] * w3 / rj;
+        }
+        down[p] = down[p] + mj * w3 / rj;
+    }
+    double its[3];
+    for (int k = 0; k < 3; k++) its[k] = d.s.interfss[(size_t)k * N + i];
+    for (int p = 0; p < 4; p++) {
+        const bool some = fabs(down[p]) > 1.0e-6;
+        for (int k = 0; k < 6; k++) d.s.sb[(size_t)(p * 6 + k) * N + i] = some ? us[p][k] / down[p] : 0.0;
+        for (int k = 0; k < 3; k++)
+            d.s.vb[(size_t)(p * 3 + k) * N + i] =
+                some ? (free_slip ? its[k] + uv[p][k] / down[p] : its[k] - uv[p][k] / down[p]) : its[k];
+    }
+}
+
 __global__ void k_step_done(Dev d)
 {
     if (threadIdx.x == 0 && blockIdx.x == 0 && *d.s.err == 0) *d.s.step += 1;
@@ -1952,6 +2025,8 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
     if (d.p.flbndy == 2) {
         LAUNCH_ND(k_tm_vb, nblk(N, 128), 128, d); n++;
         k_tm_wall<<<nblk(N, 128), 128, 0, st>>>(d); n++;
+    } else if (d.p.flbndy != 1) {
+        k_tran_wall<<<nblk(N, 128), 128, 0, st>>>(d); n++;
     }
     REC(19);
     k_step_done<<<1, 32, 0, st>>>(d); n++;

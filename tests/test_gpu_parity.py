@@ -317,3 +317,19 @@ def test_soil_structure_contact(ndim, dx, ss_type):
         touched += int((np.abs(f[st.fields["type"] == 2]).sum(axis=1) > 0).sum())
     _compare(eng, orc)
     assert touched > 0
+
+
+@pytest.mark.parametrize("flbndy", [3, 4, 13, 14])
+@pytest.mark.parametrize("name,steps", [("dam_break_2d", 30), ("soil_column_3d", 20)])
+def test_slip_walls(name, steps, flbndy):
+    """no_slip_tran / free_slip_tran walls (flbndy 3 / 4, and 13 / 14 with
+    velocity_set_domain first), with boundary_stress_effect_tran: bit-identical
+    to the oracle, whose same runs are bit-identical to the reference (golden
+    *_slip*.npz fixtures)."""
+    sc = SCENES[name]()
+    sc.flags["flbndy"] = flbndy
+    _, eng, orc = _engine_and_oracle(sc)
+    for chunk in (1, steps - 1):
+        eng.step(chunk)
+        assert orc.step(chunk) == 0
+    _compare(eng, orc)
