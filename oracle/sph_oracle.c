@@ -1466,6 +1466,41 @@ static void boundary_stress_effect_tran(orc_ctx* c)
     }
 }
 
+/* boundary_effect_free_struct: CPP_9-4-derivation_stress.cpp:900-990, the wall
+ * stress of flbndy 5 (and any flbndy outside 1-4, 13, 14): the particle's own
+ * stress mirrored into the wall, with the shear components of a fluid's
+ * mirror negated */
+static void boundary_effect_free_struct(orc_ctx* c)
+{
+    for (int i = 0; i < c->n; i++) {
+        int ti = c->type[i];
+        if (ti == 0 || ti == 7) continue;
+        double tu[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj);
+            if (c->type[j] != 0) continue;
+            double ai[6] = {0, 0, 0, 0, 0, 0}, aj[6] = {0, 0, 0, 0, 0, 0};
+            const double* s = &c->sig[i * 6];
+            if (ti == 1 || ti == 3) {
+                for (int k = 0; k < 6; k++) ai[k] = s[k];
+                aj[0] = ai[0]; aj[1] = ai[1]; aj[2] = ai[2];
+                aj[3] = -ai[3]; aj[4] = -ai[4]; aj[5] = -ai[5];
+            } else if (ti == 2 || ti == 4) {
+                double satu = c->satu[i];
+                ai[0] = s[0] - satu * c->prew[i] + (1 - satu) * c->prea[i];
+                ai[1] = s[1] - satu * c->prew[i] + (1 - satu) * c->prea[i];
+                ai[2] = s[2] - satu * c->prew[i] + (1 - satu) * c->prea[i];
+                ai[3] = s[3]; ai[4] = s[4]; ai[5] = s[5];
+                for (int k = 0; k < 6; k++) aj[k] = ai[k];
+            }
+            stress_pair(tu, c->mass[j], aj, ai, c->rho[j], c->rho[i], &W(i, nj, 0), 1.0);
+        }
+        c->ax[i * 3 + 0] += tu[0][0] + tu[0][1] + tu[0][2];
+        c->ax[i * 3 + 1] += tu[1][0] + tu[1][1] + tu[1][2];
+        c->ax[i * 3 + 2] += tu[2][0] + tu[2][1] + tu[2][2];
+    }
+}
+
 /* Soil-water drag coefficient beta of interact2 (Tsuji et al. 1993 / Shi et al.
  * 2018, CPP_10-interact1.cpp:154-176) and interact3 (Peng et al. 2017,
  * :294-306), for soil particle s and water particle w; rho_w is the density
@@ -2082,6 +2117,138 @@ static void interaction_ss(orc_ctx* c)
     }
 }
 
+/* boundary_free_solid (flbndy 5): CPP_13-boundary.cpp:1239-1516.  The rigid
+ * contact of interaction_ss_rigid against the wall particles, with the walls'
+ * velocities (interfss), applied to the particle's own acceleration only:
+ * types 1-4 in 2-D; every particle in 3-D, as the reference's 3-D loop has no
+ * type test. */
+static void boundary_free_solid(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    const int nd = P->ndim, n = c->n;
+    const double dt = P->dt, dr = P->dr, myu = P->ss_myu, zeta = P->ss_zeta;
+    int ids[NB];
+    double dsts[NB];
+    for (int i = 0; i < n; i++) {
+        int ti = c->type[i];
+        if (nd == 2 && !(ti == 1 || ti == 2 || ti == 3 || ti == 4)) continue;
+        int total = 0;
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj);
+            if (c->type[j] != 0) continue;
+            double d = (c->xp[i * 3] - c->xp[j * 3]) * (c->xp[i * 3] - c->xp[j * 3]) +
+                       (c->xp[i * 3 + 1] - c->xp[j * 3 + 1]) * (c->xp[i * 3 + 1] - c->xp[j * 3 + 1]) +
+                       (c->xp[i * 3 + 2] - c->xp[j * 3 + 2]) * (c->xp[i * 3 + 2] - c->xp[j * 3 + 2]);
+            ids[total] = j;
+            dsts[total] = sqrt(d);
+            total++;
+        }
+        for (int a = 0; a < 4; a++)
+            for (int b = a + 1; b < total; b++)
+                if (dsts[a] > dsts[b]) { int t = ids[a]; ids[a] = ids[b]; ids[b] = t; }
+        if (total < (nd == 2 ? 2 : 3)) continue;
+        const double mi = c->mass[i];
+        const double* vpi = &c->vxp[i * 3];
+        double fn[3] = {0, 0, 0}, ft[3] = {0, 0, 0};
+        orc_pt p4 = ss_point(c, i);
+        int id1 = ids[0], id2 = ids[1];
+        orc_pt p1 = ss_point(c, id1), p2 = ss_point(c, id2);
+        if (nd == 2) {
+            double den = p2.y * p1.x - p1.y * p2.x;
+            double A = (p1.y - p2.y) / den, B = (p2.x - p1.x) / den, C = 1.0;
+            double dp = ss_dpline(p4, A, B, C);
+            double tmp = sqrt(A * A + B * B);
+            orc_pt Q1 = {p4.x + dp * A / tmp, p4.y + dp * B / tmp, 0.0}, Q2 = {p4.x - dp * A / tmp, p4.y - dp * B / tmp, 0.0};
+            orc_pt outp = (ss_dpline(Q1, A, B, C) < 1.0e-3) ? Q1 : Q2;
+            outp.z = 0.0;
+            double v0x = p2.x - p1.x, v0y = p2.y - p1.y, v0z = p2.z - p1.z;
+            double v1x = outp.x - p1.x, v1y = outp.y - p1.y, v1z = 0.0 - p1.z;
+            double dot00 = v0x * v0x + v0y * v0y + v0z * v0z, dot01 = v0x * v1x + v0y * v1y + v0z * v1z;
+            double u = 1.0 / dot00 * dot01;
+            if ((u < 0 || u > 1) || !(dp < 0.5 * dr)) continue;
+            double nx = 0.0, ny = 0.0, tot = sqrt(A * A + B * B);
+            if (tot > 1.0e-10) { nx = A / tot; ny = B / tot; }
+            double dot = (outp.x - p4.x) * nx + (outp.y - p4.y) * ny + 0.0 * 0.0;
+            if (!(dot <= 0.0)) { nx = -nx; ny = -ny; }
+            double ms, vs[3];
+            ss_interp(p1, p2, outp, c->mass[id1], c->mass[id2], &c->interfss[id1 * 3], &c->interfss[id2 * 3], &ms, vs);
+            vs[0] -= vpi[0];
+            vs[1] -= vpi[1];
+            double v = vs[0] * nx + vs[1] * ny;
+            double vn[2] = {v * nx, v * ny}, vt[2] = {vs[0] - vn[0], vs[1] - vn[1]};
+            fn[0] = mi * vn[0] / dt; fn[1] = mi * vn[1] / dt;
+            ft[0] = mi * vt[0] / dt; ft[1] = mi * vt[1] / dt;
+            double mag_fn = sqrt(fn[0] * fn[0] + fn[1] * fn[1]), mag_ft = sqrt(ft[0] * ft[0] + ft[1] * ft[1]);
+            if (mag_ft > (mag_fn * myu)) {
+                vt[0] = vt[0] * myu * mag_fn / mag_ft;
+                vt[1] = vt[1] * myu * mag_fn / mag_ft;
+                ft[0] = mi * vt[0] / dt; ft[1] = mi * vt[1] / dt;
+            }
+            c->ax[i * 3 + 0] += zeta * (ft[0] + fn[0]) / mi;
+            c->ax[i * 3 + 1] += zeta * (ft[1] + fn[1]) / mi;
+            c->ax[i * 3 + 2] += 0.0;
+        } else {
+            int id3 = ids[2];
+            orc_pt p3 = ss_point(c, id3);
+            double den = -p1.x * (p2.y * p3.z - p3.y * p2.z) - p2.x * (p3.y * p1.z - p1.y * p3.z) - p3.x * (p1.y * p2.z - p2.y * p1.z);
+            double A = p1.y * (p2.z - p3.z) + p2.y * (p3.z - p1.z) + p3.y * (p1.z - p2.z);
+            double B = p1.z * (p2.x - p3.x) + p2.z * (p3.x - p1.x) + p3.z * (p1.x - p2.x);
+            double C = p1.x * (p2.y - p3.y) + p2.x * (p3.y - p1.y) + p3.x * (p1.y - p2.y);
+            A = A / den; B = B / den; C = C / den;
+            const double D = 1.0;
+            double dp = ss_dpplane(p4, A, B, C, D);
+            double tmp = sqrt(A * A + B * B + C * C);
+            orc_pt Q1 = {p4.x + dp * A / tmp, p4.y + dp * B / tmp, p4.z + dp * C / tmp};
+            orc_pt Q2 = {p4.x - dp * A / tmp, p4.y - dp * B / tmp, p4.z - dp * C / tmp};
+            orc_pt outp = (ss_dpplane(Q1, A, B, C, D) < 1.0e-3) ? Q1 : Q2;
+            double a0[3] = {p3.x - p1.x, p3.y - p1.y, p3.z - p1.z};
+            double a1[3] = {p2.x - p1.x, p2.y - p1.y, p2.z - p1.z};
+            double a2[3] = {outp.x - p1.x, outp.y - p1.y, outp.z - p1.z};
+            double dot00 = a0[0] * a0[0] + a0[1] * a0[1] + a0[2] * a0[2];
+            double dot01 = a0[0] * a1[0] + a0[1] * a1[1] + a0[2] * a1[2];
+            double dot02 = a0[0] * a2[0] + a0[1] * a2[1] + a0[2] * a2[2];
+            double dot11 = a1[0] * a1[0] + a1[1] * a1[1] + a1[2] * a1[2];
+            double dot12 = a1[0] * a2[0] + a1[1] * a2[1] + a1[2] * a2[2];
+            double inv = 1 / (dot00 * dot11 - dot01 * dot01);
+            double u = (dot11 * dot02 - dot01 * dot12) * inv;
+            int inside = 1;
+            if (u < 0 || u > 1) inside = 0;
+            else {
+                double v = (dot00 * dot12 - dot01 * dot02) * inv;
+                inside = (v < 0 || v > 1) ? 0 : (u + v <= 1);
+            }
+            if (!(inside && dp < 0.5 * dr)) continue;
+            double nx = 0.0, ny = 0.0, nz = 0.0, tot = sqrt(A * A + B * B + C * C);
+            if (tot > 1.0e-10) { nx = A / tot; ny = B / tot; nz = C / tot; }
+            double dot = (outp.x - p4.x) * nx + (outp.y - p4.y) * ny + (outp.z - p4.z) * nz;
+            if (!(dot <= 0.0)) { nx = -nx; ny = -ny; nz = -nz; }
+            double d1 = sqrt((p2.x - p1.x) * (p2.x - p1.x) + (p2.y - p1.y) * (p2.y - p1.y) + (p2.z - p1.z) * (p2.z - p1.z));
+            double la = (p2.x - p1.x) / d1, lb = (p2.y - p1.y) / d1, lc = (p2.z - p1.z) / d1;
+            double d2 = sqrt((outp.x - p3.x) * (outp.x - p3.x) + (outp.y - p3.y) * (outp.y - p3.y) + (outp.z - p3.z) * (outp.z - p3.z));
+            double ma = (outp.x - p3.x) / d2, mb = (outp.y - p3.y) / d2;
+            double flag = la * mb - ma * lb;
+            if (!(fabs(flag) > 1.0e-3)) continue;
+            double tu = ma * (p1.y - p3.y) - mb * (p1.x - p3.x);
+            double t = tu / flag;
+            orc_pt sectp = {p1.x + la * t, p1.y + lb * t, p1.z + lc * t};
+            double tms, tvs[3], ms, vs[3];
+            ss_interp(p1, p2, sectp, c->mass[id1], c->mass[id2], &c->interfss[id1 * 3], &c->interfss[id2 * 3], &tms, tvs);
+            ss_interp(p3, sectp, outp, c->mass[id3], tms, &c->interfss[id3 * 3], tvs, &ms, vs);
+            for (int k = 0; k < 3; k++) vs[k] -= vpi[k];
+            double v = vs[0] * nx + vs[1] * ny + vs[2] * nz;
+            double vn[3] = {v * nx, v * ny, v * nz}, vt[3] = {vs[0] - vn[0], vs[1] - vn[1], vs[2] - vn[2]};
+            for (int k = 0; k < 3; k++) { fn[k] = mi * vn[k] / dt; ft[k] = mi * vt[k] / dt; }
+            double mag_fn = sqrt(fn[0] * fn[0] + fn[1] * fn[1] + fn[2] * fn[2]);
+            double mag_ft = sqrt(ft[0] * ft[0] + ft[1] * ft[1] + ft[2] * ft[2]);
+            if (mag_ft > (mag_fn * myu)) {
+                for (int k = 0; k < 3; k++) vt[k] = vt[k] * myu * mag_fn / mag_ft;
+                for (int k = 0; k < 3; k++) ft[k] = mi * vt[k] / dt;
+            }
+            for (int k = 0; k < 3; k++) c->ax[i * 3 + k] += zeta * (ft[k] + fn[k]) / mi;
+        }
+    }
+}
+
 /* no_slip_tran / free_slip_tran: CPP_13-boundary.cpp:711-958 and 960-1237.
  * Each wall particle's Shepard sums over its water, soil, air and structure
  * neighbours give its stress per phase (soil with the pore terms) and its
@@ -2283,7 +2450,7 @@ static void kernel_gradient_correction(orc_ctx* c)
 
 static int check_supported(const sphgpu_params* P)
 {
-    if (!(P->flbndy >= 1 && P->flbndy <= 4) && P->flbndy != 13 && P->flbndy != 14) return SPHGPU_E_UNSUPPORTED;
+    if (!(P->flbndy >= 1 && P->flbndy <= 5) && P->flbndy != 13 && P->flbndy != 14) return SPHGPU_E_UNSUPPORTED;
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
     if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
     if (P->fli < 0 || P->fli > 3 || P->ss_type < 0 || P->ss_type > 3) return SPHGPU_E_UNSUPPORTED;
@@ -2321,10 +2488,12 @@ int orc_step(orc_ctx* c, int nsteps)
         artificial_viscosity(c);
         if (P->art_stre_coe > 0.0) artificial_stress(c);
         if (P->flbndy == 1 || P->flbndy == 2) boundary_moving_stress_effect(c);   /* flv == 0 */
-        else boundary_stress_effect_tran(c);
+        else if (P->flbndy == 3 || P->flbndy == 4 || P->flbndy == 13 || P->flbndy == 14) boundary_stress_effect_tran(c);
+        else boundary_effect_free_struct(c);
         if (P->fli >= 1) interact(c, P->fli);
         if (P->ss_type >= 1 && P->ss_type <= 3) interaction_ss(c);
         if (c->l <= P->inip) soil_damping_geostress(c);
+        if (P->flbndy == 5) boundary_free_solid(c);
         velocity_update(c);
         if (P->if_move != 2) xsph(c);
         if (P->flbndy == 1) tmboundary(c);

@@ -90,6 +90,23 @@ def _tm_boundary(factory, flbndy=2):
     return make
 
 
+def _free_solid(factory, shift):
+    """flbndy 5: boundary_effect_free_struct and boundary_free_solid (friction
+    0.3, zeta 0.5).  With `shift` the water starts 0.45 spacings from the left
+    wall so that the wall contact acts.  (In 3-D the reference's contact also
+    runs over wall particles and yields NaN accelerations on degenerate
+    triangles, which reach moving particles in the second step.)"""
+    def make():
+        sc = factory()
+        sc.flags["flbndy"] = 5
+        sc.problem["ss"] = (0, 0.3, 0.5, 0)
+        if shift:
+            w = sc.ptype == 1
+            sc.xp[w, 0] -= 0.55 * sc.dr
+        return sc
+    return make
+
+
 def _footing(ndim, dx, ss_type):
     """A strip footing (type 4, pushed down at 0.5 m/s, if_move 3) 0.4 spacings
     above a Drucker-Prager soil bed, with soil-structure contact ss_type
@@ -116,6 +133,8 @@ CASES = {
     "dam_break_2d_dx0.04_free_slip_vsd": (_tm_boundary(lambda: scenes.dam_break_2d(dx=0.04, steps=200), 14), 25),
     "soil_column_3d_dx0.1_free_slip": (_tm_boundary(lambda: scenes.soil_column_3d(dx=0.1, steps=200), 4), 15),
     "soil_column_3d_dx0.1_no_slip_vsd": (_tm_boundary(lambda: scenes.soil_column_3d(dx=0.1, steps=200), 13), 15),
+    "dam_break_2d_dx0.04_free_solid": (_free_solid(lambda: scenes.dam_break_2d(dx=0.04, steps=200), True), 15),
+    "soil_column_3d_dx0.1_free_solid": (_free_solid(lambda: scenes.soil_column_3d(dx=0.1, steps=200), False), 3),
     "footing_2d_rigid": (_footing(2, 0.04, 1), 12),
     "footing_2d_deformable": (_footing(2, 0.04, 2), 12),
     "footing_2d_penalty": (_footing(2, 0.04, 3), 12),
