@@ -143,12 +143,11 @@ int check_params(const sphgpu_params* P)
     if (!(P->dr > 0.0) || !(P->dt > 0.0)) return SPHGPU_E_ARG;
     if (P->step_regu <= 0) return SPHGPU_E_ARG;
     // flag combinations this engine runs (the others are rejected loudly)
-    if (!(P->flbndy >= 1 && P->flbndy <= 4) && P->flbndy != 13 && P->flbndy != 14) return SPHGPU_E_UNSUPPORTED;
+    if (!(P->flbndy >= 1 && P->flbndy <= 5) && P->flbndy != 13 && P->flbndy != 14) return SPHGPU_E_UNSUPPORTED;
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
     if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
     if (P->fli < 0 || P->fli > 3) return SPHGPU_E_UNSUPPORTED;
     if (P->ss_type < 0 || P->ss_type > 3) return SPHGPU_E_UNSUPPORTED;
-    if (P->ss_type >= 1 && P->ss_acc_type == 2) return SPHGPU_E_UNSUPPORTED;
     if (P->if_move < 0 || P->if_move > 3) return SPHGPU_E_UNSUPPORTED;
     return 0;
 }
@@ -317,6 +316,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     p.g_acc = std::sqrt(P->gx * P->gx + P->gy * P->gy + P->gz * P->gz);   // CPP_10-interact1.cpp:28
     p.art_stre_coe = P->art_stre_coe;
     p.ss_type = P->ss_type; p.ss_myu = P->ss_myu; p.ss_zeta = P->ss_zeta;
+    p.ss_coupled = (P->ss_type >= 1 && P->ss_type <= 3 && P->ss_acc_type == 2) ? 1 : 0;
     DevState& s = d.s;
     int r = 0;
     r |= dalloc(c, &s.type, N); r |= dalloc(c, &s.matype, N); r |= dalloc(c, &s.etype, N); r |= dalloc(c, &s.permtype, N);
@@ -340,7 +340,12 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
         r |= dalloc(c, &s.ss_own, 6 * (size_t)N);
         r |= dalloc(c, &s.ss_fs, 6 * (size_t)N);
     }
-    if (P->flbndy != 1) {
+    if (P->ss_type >= 1 && P->ss_type <= 3 && P->ss_acc_type == 2) r |= dalloc(c, &s.cpl, 3 * (size_t)N);
+    if (P->flbndy == 5) {
+        r |= dalloc(c, &s.fsol, 3 * (size_t)N);
+        r |= dalloc(c, &s.fsol_on, N);
+    }
+    if (P->flbndy != 1 && P->flbndy != 5) {
         r |= dalloc(c, &s.vel_bndy, 3 * (size_t)N);
         r |= dalloc(c, &s.vb, 12 * (size_t)N);
         r |= dalloc(c, &s.vx_vb, 3 * (size_t)N);

@@ -51,6 +51,7 @@ struct DevParams {
     double g_acc;              // |g|, interact1 (CPP_10-interact1.cpp:28)
     double art_stre_coe;       // artificial stress coefficient (0: off)
     int ss_type;               // soil-structure contact: 0 none, 1 rigid, 2 deformable, 3 penalty
+    int ss_coupled;            // 1: coupled_Water_Soil_Structure (ss_type 1-3 with acc_type 2)
     double ss_myu, ss_zeta;
     int bulk;                  // 1: the FP32-bulk form (pair records in FP32)
 };
@@ -98,6 +99,12 @@ struct DevState {
     // flbndy 3/4/13/14: the walls' clVar_Boundary stresses per phase,
     // sb[(p * 6 + k) * N + i] (24N)
     double *sb;
+    // flbndy 5: boundary_free_solid's force per particle, zeta (f_t + f_n)
+    // (3N), and whether the particle touches the walls (N)
+    double *fsol;
+    int *fsol_on;
+    // ss acc_type 2: coupled_Water_Soil_Structure's row sums per particle (3N)
+    double *cpl;
     // soil-structure contact (ss_type 1-3): per water/soil particle the
     // structure particles it pushes (ss_id, 3N, -1 = none) with the forces
     // they take from it (ss_con, 18N: per slot q the normal then the

@@ -949,6 +949,9 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
     // wall's stress for i's phase, and a structure particle's own stress
     // without the pore terms
     const bool tran = d.p.flbndy == 3 || d.p.flbndy == 4 || d.p.flbndy == 13 || d.p.flbndy == 14;
+    // boundary_effect_free_struct (CPP_9-4:900-990) for the other flbndy
+    // values: a fluid's mirrored stress has its shear components negated
+    const bool free_struct = !(tran || d.p.flbndy == 1 || d.p.flbndy == 2);
     if (moving) {
         double si[6];
         for (int k = 0; k < 6; k++) si[k] = d.s.sig_next[k * N + i];
@@ -1002,7 +1005,9 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
         }
         if (b_pair) {
             real abj[6];
-            if (tran)
+            if (free_struct && fluid)
+                for (int k = 0; k < 6; k++) abj[k] = ((k < 3) ? ab[k] : -ab[k]) / rj / rj;
+            else if (tran)
                 for (int k = 0; k < 6; k++)
                     abj[k] = (real)(d.s.sb[(size_t)((ti - 1) * 6 + k) * N + j] / d.s.rho[j] / d.s.rho[j]);
             else
@@ -1098,6 +1103,8 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
         ax[1] += tb[1][0].v() + tb[1][1].v() + tb[1][2].v();
         ax[2] += tb[2][0].v() + tb[2][1].v() + tb[2][2].v();
     }
+    if (d.p.ss_coupled && (ti == 1 || ti == 2 || ti == 4))
+        for (int k = 0; k < 3; k++) ax[k] += d.s.cpl[(size_t)k * N + i];
     const double dt = d.p.dt;
     double axp[3];
     for (int k = 0; k < 3; k++) axp[k] = d.s.axp[k * N + i];
@@ -1142,6 +1149,11 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
             if (vx1 * vx2 <= 0.0) ax[k] = -2.0 * vi[k] / dt - axp[k];
             else ax[k] -= tdm[k].v();
         }
+    }
+    if (d.p.flbndy == 5 && d.s.fsol_on[i]) {
+        // boundary_free_solid (CPP_13-boundary.cpp:1239-1516), after the damping
+        const double mi = d.s.mass[i];
+        for (int k = 0; k < 3; k++) ax[k] += d.s.fsol[(size_t)k * N + i] / mi;
     }
     // veocity_update, if_move 0 and 1
     double vout[3];
@@ -1278,7 +1290,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
         }
         for (int k = 0; k < nd; k++) vn[k] = vn[k] + tb[k];
     }
-    if (d.p.flbndy != 1 && moving)
+    if (d.p.flbndy != 1 && d.p.flbndy != 5 && moving)
         for (int k = 0; k < 3; k++) d.s.vx_vb[k * N + i] = vn[k];
     if (ti != 0 && ti != 7) {
         const double dr = d.p.dr;
@@ -1784,6 +1796,193 @@ __global__ void __launch_bounds__(128) k_tran_wall(Dev d)
     }
 }
 
+// boundary_free_solid (flbndy 5, CPP_13-boundary.cpp:1239-1516): the rigid
+// contact of interaction_ss_rigid against the wall particles, with their
+// interfss velocities, for the particle's own acceleration; types 1-4 in 2-D,
+// every particle in 3-D (the reference's 3-D loop has no type test).  Stores
+// zeta (f_t + f_n); k_accel_b divides by the mass after the damping.
+template <int ND>
+__global__ void __launch_bounds__(128) k_free_solid(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    d.s.fsol_on[i] = 0;
+    const int ti = d.s.type[i];
+    if (ND == 2 && !(ti >= 1 && ti <= 4)) return;
+    const int nn = nbr_count(d, i);
+    const double dt = d.p.dt, dr = d.p.dr, myu = d.p.ss_myu, zeta = d.p.ss_zeta;
+    int ids[SPH_NB_CAP];
+    double dsts[SPH_NB_CAP];
+    int total = 0;
+    const SSPt p4 = ss_pt(d, i);
+    for (int q = 0; q < nn; q++) {
+        const int j = d.s.nbr[(size_t)q * N + i];
+        if (d.s.type[j] != 0) continue;
+        const SSPt pj = ss_pt(d, j);
+        const double dd = (p4.x - pj.x) * (p4.x - pj.x) + (p4.y - pj.y) * (p4.y - pj.y) + (p4.z - pj.z) * (p4.z - pj.z);
+        ids[total] = j;
+        dsts[total] = sqrt(dd);
+        total++;
+    }
+    for (int a = 0; a < 4; a++)
+        for (int b = a + 1; b < total; b++)
+            if (dsts[a] > dsts[b]) { const int t = ids[a]; ids[a] = ids[b]; ids[b] = t; }
+    if (total < ND) return;
+    const double mi = d.s.mass[i];
+    double vpi[3];
+    for (int k = 0; k < 3; k++) vpi[k] = d.s.vxp[(size_t)k * N + i];
+    const int id1 = ids[0], id2 = ids[1];
+    const SSPt p1 = ss_pt(d, id1), p2 = ss_pt(d, id2);
+    double v1[3], v2[3];
+    for (int k = 0; k < 3; k++) { v1[k] = d.s.interfss[(size_t)k * N + id1]; v2[k] = d.s.interfss[(size_t)k * N + id2]; }
+    double fn[3] = {0, 0, 0}, ft[3] = {0, 0, 0}, f[3];
+    if (ND == 2) {
+        const double den = p2.y * p1.x - p1.y * p2.x;
+        const double A = (p1.y - p2.y) / den, B = (p2.x - p1.x) / den, C = 1.0;
+        const double tmp0 = sqrt(A * A + B * B);
+        const double dp = (tmp0 > 1.0e-3) ? fabs(A * p4.x + B * p4.y + C) / tmp0 : 0.0;
+        const double tmp = sqrt(A * A + B * B);
+        const SSPt Q1 = {p4.x + dp * A / tmp, p4.y + dp * B / tmp, 0.0}, Q2 = {p4.x - dp * A / tmp, p4.y - dp * B / tmp, 0.0};
+        const double dq = (tmp0 > 1.0e-3) ? fabs(A * Q1.x + B * Q1.y + C) / tmp0 : 0.0;
+        SSPt outp = (dq < 1.0e-3) ? Q1 : Q2;
+        outp.z = 0.0;
+        const double v0x = p2.x - p1.x, v0y = p2.y - p1.y, v0z = p2.z - p1.z;
+        const double w1x = outp.x - p1.x, w1y = outp.y - p1.y, w1z = 0.0 - p1.z;
+        const double dot00 = v0x * v0x + v0y * v0y + v0z * v0z, dot01 = v0x * w1x + v0y * w1y + v0z * w1z;
+        const double u = 1.0 / dot00 * dot01;
+        if ((u < 0 || u > 1) || !(dp < 0.5 * dr)) return;
+        double nx = 0.0, ny = 0.0;
+        const double tot = sqrt(A * A + B * B);
+        if (tot > 1.0e-10) { nx = A / tot; ny = B / tot; }
+        const double dot = (outp.x - p4.x) * nx + (outp.y - p4.y) * ny + 0.0 * 0.0;
+        if (!(dot <= 0.0)) { nx = -nx; ny = -ny; }
+        double ms, vs[3];
+        ss_interp(p1, p2, outp, d.s.mass[id1], d.s.mass[id2], v1, v2, &ms, vs);
+        vs[0] -= vpi[0];
+        vs[1] -= vpi[1];
+        const double v = vs[0] * nx + vs[1] * ny;
+        const double vn[2] = {v * nx, v * ny};
+        double vt[2] = {vs[0] - vn[0], vs[1] - vn[1]};
+        fn[0] = mi * vn[0] / dt; fn[1] = mi * vn[1] / dt;
+        ft[0] = mi * vt[0] / dt; ft[1] = mi * vt[1] / dt;
+        const double mag_fn = sqrt(fn[0] * fn[0] + fn[1] * fn[1]), mag_ft = sqrt(ft[0] * ft[0] + ft[1] * ft[1]);
+        if (mag_ft > (mag_fn * myu)) {
+            vt[0] = vt[0] * myu * mag_fn / mag_ft;
+            vt[1] = vt[1] * myu * mag_fn / mag_ft;
+            ft[0] = mi * vt[0] / dt; ft[1] = mi * vt[1] / dt;
+        }
+        f[0] = zeta * (ft[0] + fn[0]);
+        f[1] = zeta * (ft[1] + fn[1]);
+        f[2] = 0.0;
+    } else {
+        const int id3 = ids[2];
+        const SSPt p3 = ss_pt(d, id3);
+        const double den = -p1.x * (p2.y * p3.z - p3.y * p2.z) - p2.x * (p3.y * p1.z - p1.y * p3.z) -
+                           p3.x * (p1.y * p2.z - p2.y * p1.z);
+        double A = p1.y * (p2.z - p3.z) + p2.y * (p3.z - p1.z) + p3.y * (p1.z - p2.z);
+        double B = p1.z * (p2.x - p3.x) + p2.z * (p3.x - p1.x) + p3.z * (p1.x - p2.x);
+        double C = p1.x * (p2.y - p3.y) + p2.x * (p3.y - p1.y) + p3.x * (p1.y - p2.y);
+        A = A / den; B = B / den; C = C / den;
+        const double D = 1.0;
+        const double tmp0 = sqrt(A * A + B * B + C * C);
+        const double dp = (tmp0 > 1.0e-3) ? fabs(A * p4.x + B * p4.y + C * p4.z + D) / tmp0 : 0.0;
+        const double tmp = sqrt(A * A + B * B + C * C);
+        const SSPt Q1 = {p4.x + dp * A / tmp, p4.y + dp * B / tmp, p4.z + dp * C / tmp};
+        const SSPt Q2 = {p4.x - dp * A / tmp, p4.y - dp * B / tmp, p4.z - dp * C / tmp};
+        const double dq = (tmp0 > 1.0e-3) ? fabs(A * Q1.x + B * Q1.y + C * Q1.z + D) / tmp0 : 0.0;
+        const SSPt outp = (dq < 1.0e-3) ? Q1 : Q2;
+        const double a0[3] = {p3.x - p1.x, p3.y - p1.y, p3.z - p1.z};
+        const double a1[3] = {p2.x - p1.x, p2.y - p1.y, p2.z - p1.z};
+        const double a2[3] = {outp.x - p1.x, outp.y - p1.y, outp.z - p1.z};
+        const double dot00 = a0[0] * a0[0] + a0[1] * a0[1] + a0[2] * a0[2];
+        const double dot01 = a0[0] * a1[0] + a0[1] * a1[1] + a0[2] * a1[2];
+        const double dot02 = a0[0] * a2[0] + a0[1] * a2[1] + a0[2] * a2[2];
+        const double dot11 = a1[0] * a1[0] + a1[1] * a1[1] + a1[2] * a1[2];
+        const double dot12 = a1[0] * a2[0] + a1[1] * a2[1] + a1[2] * a2[2];
+        const double inv = 1 / (dot00 * dot11 - dot01 * dot01);
+        const double u = (dot11 * dot02 - dot01 * dot12) * inv;
+        bool inside;
+        if (u < 0 || u > 1) inside = false;
+        else {
+            const double v = (dot00 * dot12 - dot01 * dot02) * inv;
+            inside = (v < 0 || v > 1) ? false : (u + v <= 1);
+        }
+        if (!(inside && dp < 0.5 * dr)) return;
+        double nx = 0.0, ny = 0.0, nz = 0.0;
+        const double tot = sqrt(A * A + B * B + C * C);
+        if (tot > 1.0e-10) { nx = A / tot; ny = B / tot; nz = C / tot; }
+        const double dot = (outp.x - p4.x) * nx + (outp.y - p4.y) * ny + (outp.z - p4.z) * nz;
+        if (!(dot <= 0.0)) { nx = -nx; ny = -ny; nz = -nz; }
+        const double d1 = sqrt((p2.x - p1.x) * (p2.x - p1.x) + (p2.y - p1.y) * (p2.y - p1.y) + (p2.z - p1.z) * (p2.z - p1.z));
+        const double la = (p2.x - p1.x) / d1, lb = (p2.y - p1.y) / d1, lc = (p2.z - p1.z) / d1;
+        const double d2 = sqrt((outp.x - p3.x) * (outp.x - p3.x) + (outp.y - p3.y) * (outp.y - p3.y) +
+                               (outp.z - p3.z) * (outp.z - p3.z));
+        const double ma = (outp.x - p3.x) / d2, mb = (outp.y - p3.y) / d2;
+        const double flag = la * mb - ma * lb;
+        if (!(fabs(flag) > 1.0e-3)) return;
+        const double tu = ma * (p1.y - p3.y) - mb * (p1.x - p3.x);
+        const double t = tu / flag;
+        const SSPt sectp = {p1.x + la * t, p1.y + lb * t, p1.z + lc * t};
+        double v3[3];
+        for (int k = 0; k < 3; k++) v3[k] = d.s.interfss[(size_t)k * N + id3];
+        double tms, tvs[3], ms, vs[3];
+        ss_interp(p1, p2, sectp, d.s.mass[id1], d.s.mass[id2], v1, v2, &tms, tvs);
+        ss_interp(p3, sectp, outp, d.s.mass[id3], tms, v3, tvs, &ms, vs);
+        for (int k = 0; k < 3; k++) vs[k] -= vpi[k];
+        const double v = vs[0] * nx + vs[1] * ny + vs[2] * nz;
+        const double vn[3] = {v * nx, v * ny, v * nz};
+        double vt[3] = {vs[0] - vn[0], vs[1] - vn[1], vs[2] - vn[2]};
+        for (int k = 0; k < 3; k++) { fn[k] = mi * vn[k] / dt; ft[k] = mi * vt[k] / dt; }
+        const double mag_fn = sqrt(fn[0] * fn[0] + fn[1] * fn[1] + fn[2] * fn[2]);
+        const double mag_ft = sqrt(ft[0] * ft[0] + ft[1] * ft[1] + ft[2] * ft[2]);
+        if (mag_ft > (mag_fn * myu)) {
+            for (int k = 0; k < 3; k++) vt[k] = vt[k] * myu * mag_fn / mag_ft;
+            for (int k = 0; k < 3; k++) ft[k] = mi * vt[k] / dt;
+        }
+        for (int k = 0; k < 3; k++) f[k] = zeta * (ft[k] + fn[k]);
+    }
+    for (int k = 0; k < 3; k++) d.s.fsol[(size_t)k * N + i] = f[k];
+    d.s.fsol_on[i] = 1;
+}
+
+// coupled_Water_Soil_Structure (ss acc_type 2, CPP_9-4-derivation_stress.cpp:
+// 507-629): the stress divergence between structure and soil / water pairs
+// with plain stresses (a water particle with a structure neighbour takes the
+// difference form); k_accel_b adds each row sum after the wall stress.
+__global__ void __launch_bounds__(128) k_coupled(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    const int ti = d.s.type[i];
+    if (!(ti == 4 || ti == 2 || ti == 1)) return;
+    const int nn = nbr_count(d, i);
+    double si[6];
+    for (int k = 0; k < 6; k++) si[k] = d.s.sig_next[(size_t)k * N + i];
+    const double ri = d.s.rho[i];
+    double tu[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int q = 0; q < nn; q++) {
+        const int j = d.s.nbr[(size_t)q * N + i];
+        const int tj = d.s.type[j];
+        const bool plus = (ti == 4 && tj == 2) || (ti == 2 && tj == 4) || (ti == 4 && tj == 1);
+        const bool minus = (ti == 1 && tj == 4);
+        if (!(plus || minus)) continue;
+        real wr[4];
+        load_w(d, q, i, wr);
+        const double w[3] = {wr[0], wr[1], wr[2]};
+        const double mj = d.s.mass[j], rj = d.s.rho[j];
+        double sj[6], a[6], b[6];
+        for (int k = 0; k < 6; k++) sj[k] = d.s.sig_next[(size_t)k * N + j];
+        for (int k = 0; k < 6; k++) { a[k] = sj[k] / rj / rj; b[k] = si[k] / ri / ri; }
+        const int cmap[3][3] = {{0, 3, 5}, {3, 1, 4}, {5, 4, 2}};
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) {
+                const int m = cmap[r][c];
+                tu[r][c] = tu[r][c] + mj * (plus ? a[m] + b[m] : a[m] - b[m]) * w[c];
+            }
+    }
+    for (int r = 0; r < 3; r++) d.s.cpl[(size_t)r * N + i] = tu[r][0] + tu[r][1] + tu[r][2];
+}
+
 __global__ void k_step_done(Dev d)
 {
     if (threadIdx.x == 0 && blockIdx.x == 0 && *d.s.err == 0) *d.s.step += 1;
@@ -2007,6 +2206,8 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
     if (art) { LAUNCH_ND(k_art_rij, nblk(N, 128), 128, d); n++; }
     REC(15);
     LAUNCH_ND(k_accel_a, nblk(N, 128), 128, d); n++;
+    if (d.p.flbndy == 5) { LAUNCH_ND(k_free_solid, nblk(N, 128), 128, d); n++; }
+    if (d.p.ss_coupled) { k_coupled<<<nblk(N, 128), 128, 0, st>>>(d); n++; }
     if (d.p.ss_type >= 1) {
         LAUNCH_ND(k_ss_pair, nblk(N, 128), 128, d); n++;
         k_ss_struct<<<nblk(N, 128), 128, 0, st>>>(d); n++;
@@ -2025,7 +2226,7 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
     if (d.p.flbndy == 2) {
         LAUNCH_ND(k_tm_vb, nblk(N, 128), 128, d); n++;
         k_tm_wall<<<nblk(N, 128), 128, 0, st>>>(d); n++;
-    } else if (d.p.flbndy != 1) {
+    } else if (d.p.flbndy == 3 || d.p.flbndy == 4 || d.p.flbndy == 13 || d.p.flbndy == 14) {
         k_tran_wall<<<nblk(N, 128), 128, 0, st>>>(d); n++;
     }
     REC(19);

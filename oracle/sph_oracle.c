@@ -1501,6 +1501,29 @@ static void boundary_effect_free_struct(orc_ctx* c)
     }
 }
 
+/* coupled_Water_Soil_Structure (ss acc_type 2): CPP_9-4-derivation_stress.cpp:
+ * 507-629, the stress divergence between structure and soil / water pairs
+ * (plain stresses; water with a structure neighbour takes the difference form) */
+static void coupled_water_soil_structure(orc_ctx* c)
+{
+    for (int i = 0; i < c->n; i++) {
+        int ti = c->type[i];
+        if (!(ti == 4 || ti == 2 || ti == 1)) continue;
+        double tu[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj), tj = c->type[j];
+            double sg = 0.0;
+            if ((ti == 4 && tj == 2) || (ti == 2 && tj == 4) || (ti == 4 && tj == 1)) sg = 1.0;
+            else if (ti == 1 && tj == 4) sg = -1.0;
+            else continue;
+            stress_pair(tu, c->mass[j], &c->sig[j * 6], &c->sig[i * 6], c->rho[j], c->rho[i], &W(i, nj, 0), sg);
+        }
+        c->ax[i * 3 + 0] += tu[0][0] + tu[0][1] + tu[0][2];
+        c->ax[i * 3 + 1] += tu[1][0] + tu[1][1] + tu[1][2];
+        c->ax[i * 3 + 2] += tu[2][0] + tu[2][1] + tu[2][2];
+    }
+}
+
 /* Soil-water drag coefficient beta of interact2 (Tsuji et al. 1993 / Shi et al.
  * 2018, CPP_10-interact1.cpp:154-176) and interact3 (Peng et al. 2017,
  * :294-306), for soil particle s and water particle w; rho_w is the density
@@ -2454,7 +2477,6 @@ static int check_supported(const sphgpu_params* P)
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
     if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
     if (P->fli < 0 || P->fli > 3 || P->ss_type < 0 || P->ss_type > 3) return SPHGPU_E_UNSUPPORTED;
-    if (P->ss_type >= 1 && P->ss_acc_type == 2) return SPHGPU_E_UNSUPPORTED;
     return 0;
 }
 
@@ -2490,6 +2512,7 @@ int orc_step(orc_ctx* c, int nsteps)
         if (P->flbndy == 1 || P->flbndy == 2) boundary_moving_stress_effect(c);   /* flv == 0 */
         else if (P->flbndy == 3 || P->flbndy == 4 || P->flbndy == 13 || P->flbndy == 14) boundary_stress_effect_tran(c);
         else boundary_effect_free_struct(c);
+        if (P->ss_type >= 1 && P->ss_type <= 3 && P->ss_acc_type == 2) coupled_water_soil_structure(c);
         if (P->fli >= 1) interact(c, P->fli);
         if (P->ss_type >= 1 && P->ss_type <= 3) interaction_ss(c);
         if (c->l <= P->inip) soil_damping_geostress(c);

@@ -107,12 +107,18 @@ def _free_solid(factory, shift):
     return make
 
 
-def _footing(ndim, dx, ss_type):
+def _footing(ndim, dx, ss_type, coupled=False):
     """A strip footing (type 4, pushed down at 0.5 m/s, if_move 3) 0.4 spacings
     above a Drucker-Prager soil bed, with soil-structure contact ss_type
-    (1 rigid, 2 deformable, 3 penalty), friction 0.3, zeta 0.1."""
-    return lambda: scenes.footing(ndim=ndim, dx=dx, bed=(1.2, 0.6, 0.5), width=0.4, height=0.2, gap=0.4,
-                                  ss_type=ss_type, zeta=0.1, v=0.5)
+    (1 rigid, 2 deformable, 3 penalty), friction 0.3, zeta 0.1; `coupled`
+    adds coupled_Water_Soil_Structure (acc_type 2)."""
+    def make():
+        sc = scenes.footing(ndim=ndim, dx=dx, bed=(1.2, 0.6, 0.5), width=0.4, height=0.2, gap=0.4,
+                            ss_type=ss_type, zeta=0.1, v=0.5)
+        if coupled:
+            sc.problem["ss"] = (ss_type, 0.3, 0.1, 2)
+        return sc
+    return make
 
 
 CASES = {
@@ -140,6 +146,8 @@ CASES = {
     "footing_2d_penalty": (_footing(2, 0.04, 3), 12),
     "footing_3d_deformable": (_footing(3, 0.1, 2), 12),
     "footing_3d_penalty": (_footing(3, 0.1, 3), 12),
+    "footing_2d_penalty_coupled": (_footing(2, 0.04, 3, True), 12),
+    "footing_3d_deformable_coupled": (_footing(3, 0.1, 2, True), 12),
 }
 
 

@@ -299,8 +299,9 @@ def test_tm_boundary_walls(name, steps):
     _compare(eng, orc)
 
 
-@pytest.mark.parametrize("ndim,dx,ss_type", [(2, 0.04, 1), (2, 0.04, 2), (2, 0.04, 3), (3, 0.1, 2), (3, 0.1, 3)])
-def test_soil_structure_contact(ndim, dx, ss_type):
+@pytest.mark.parametrize("ndim,dx,ss_type,acc_type", [(2, 0.04, 1, 0), (2, 0.04, 2, 0), (2, 0.04, 3, 0), (3, 0.1, 2, 0),
+                                                     (3, 0.1, 3, 0), (2, 0.04, 3, 2), (3, 0.1, 2, 2)])
+def test_soil_structure_contact(ndim, dx, ss_type, acc_type):
     """A footing (type 4) driven into soil (if_move 3) with the rigid (1),
     deformable (2) or penalty (3) soil-structure contact: bit-identical to the
     oracle, whose same runs are bit-identical to the reference (golden
@@ -308,6 +309,7 @@ def test_soil_structure_contact(ndim, dx, ss_type):
     particles follow the order one reference thread accumulates them in."""
     sc = scenes.footing(ndim=ndim, dx=dx, bed=(1.2, 0.6, 0.5), width=0.4, height=0.2, gap=0.4,
                         ss_type=ss_type, zeta=0.1, v=0.5)
+    sc.problem["ss"] = (ss_type, 0.3, 0.1, acc_type)     # acc_type 2: coupled_Water_Soil_Structure
     st, eng, orc = _engine_and_oracle(sc)
     touched = 0
     for _ in range(12):
@@ -332,4 +334,22 @@ def test_slip_walls(name, steps, flbndy):
     for chunk in (1, steps - 1):
         eng.step(chunk)
         assert orc.step(chunk) == 0
+    _compare(eng, orc)
+
+
+@pytest.mark.parametrize("name,steps,shift", [("dam_break_2d", 15, True), ("soil_column_3d", 3, False)])
+def test_free_solid_walls(name, steps, shift):
+    """flbndy 5: boundary_effect_free_struct and boundary_free_solid (the rigid
+    wall contact; in 3-D over every particle, as the reference does, NaN
+    where its triangles degenerate): bit-identical to the oracle, whose same
+    runs are bit-identical to the reference (golden *_free_solid fixtures)."""
+    sc = SCENES[name]()
+    sc.flags["flbndy"] = 5
+    sc.problem["ss"] = (0, 0.3, 0.5, 0)
+    if shift:
+        w = sc.ptype == 1
+        sc.xp[w, 0] -= 0.55 * sc.dr
+    _, eng, orc = _engine_and_oracle(sc)
+    eng.step(steps)
+    assert orc.step(steps) == 0
     _compare(eng, orc)

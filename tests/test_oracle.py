@@ -22,7 +22,8 @@ CASES = ["dam_break_2d_dx0.04", "soil_column_3d_dx0.1", "soil_column_3d_dx0.1_kg
          "footing_2d_rigid", "footing_2d_deformable", "footing_2d_penalty", "footing_3d_deformable",
          "footing_3d_penalty", "dam_break_2d_dx0.04_no_slip", "dam_break_2d_dx0.04_free_slip_vsd",
          "soil_column_3d_dx0.1_free_slip", "soil_column_3d_dx0.1_no_slip_vsd",
-         "dam_break_2d_dx0.04_free_solid", "soil_column_3d_dx0.1_free_solid"]
+         "dam_break_2d_dx0.04_free_solid", "soil_column_3d_dx0.1_free_solid",
+         "footing_2d_penalty_coupled", "footing_3d_deformable_coupled"]
 
 
 def _golden(name):
