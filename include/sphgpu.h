@@ -168,7 +168,11 @@ int sphgpu_get_field(sphgpu_ctx* ctx, const char* name, void* host, size_t count
  * Per-particle material records, as SPH_Calculation keeps them
  * (pVFluid / pParti_ConsPara, CPP_1-SPHLoops.cpp:371-372; filled by
  * setting_vis_cons, CPP_2-initialf.cpp:1021-1058).  Either pointer may be
- * NULL (the corresponding records stay zero).
+ * NULL (the corresponding records stay zero).  Call it after the particles'
+ * matype is set: the members only unsaturated (matype % 10 == 3) and
+ * fractional-order (8) Cam-clay and the saturation pass (flagum == 1) read
+ * are uploaded when such particles are present, and a step that needs them
+ * without them returns SPHGPU_E_STATE.
  */
 int sphgpu_set_materials(sphgpu_ctx* ctx, const sphgpu_fluid* fluid,
                          const sphgpu_soil* soil, int n);

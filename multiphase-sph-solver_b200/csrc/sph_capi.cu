@@ -53,7 +53,8 @@ const FieldDef kFields[] = {
     {"x", 3, 0}, {"xp", 3, 0}, {"vx", 3, 0}, {"vxp", 3, 0}, {"ax", 3, 0}, {"axp", 3, 0},
     {"ux", 3, 0}, {"strep", 3, 0}, {"interf", 3, 0}, {"interfss", 3, 0},
     {"rho", 1, 0}, {"rhop", 1, 0}, {"mass", 1, 0}, {"hl", 1, 0}, {"pre", 1, 0}, {"prep", 1, 0},
-    {"e", 1, 0}, {"eps", 6, 0}, {"sig", 6, 0}, {"adps", 6, 0}, {"satu", 1, 0}, {"cop", 1, 0},
+    {"e", 1, 0}, {"eps", 6, 0}, {"sig", 6, 0}, {"adps", 6, 0}, {"tssig", 6, 0}, {"tsqc", 1, 0},
+    {"satu", 1, 0}, {"dsatu", 1, 0}, {"suct", 1, 0}, {"cop", 1, 0},
     {"vsig", 1, 0}, {"veps", 1, 0}, {"divq", 1, 0}, {"divr", 1, 0}, {"meps", 1, 0},
     {"prew", 1, 0}, {"prea", 1, 0}, {"porosity", 1, 0}, {"poro_cop", 1, 0}, {"cd", 1, 0},
     {"type", 1, 1}, {"matype", 1, 1}, {"permtype", 1, 1}, {"etype", 1, 1},
@@ -73,7 +74,8 @@ const AosMember kAos[] = {
     {"x", 0}, {"xp", 24}, {"vx", 48}, {"vxp", 72}, {"ax", 96}, {"axp", 120}, {"ux", 144},
     {"strep", 168}, {"interf", 264}, {"interfss", 288}, {"rho", 312}, {"rhop", 320},
     {"mass", 328}, {"hl", 336}, {"pre", 344}, {"prep", 352}, {"e", 360}, {"eps", 368},
-    {"sig", 464}, {"adps", 656}, {"satu", 760}, {"cop", 784}, {"vsig", 792}, {"veps", 800},
+    {"sig", 464}, {"adps", 656}, {"tssig", 704}, {"tsqc", 752}, {"satu", 760}, {"dsatu", 768},
+    {"suct", 776}, {"cop", 784}, {"vsig", 792}, {"veps", 800},
     {"divq", 808}, {"divr", 816}, {"meps", 824}, {"prew", 864}, {"prea", 872},
     {"porosity", 880}, {"cd", 888}, {"poro_cop", 896}, {"type", 1048}, {"matype", 1052},
     {"permtype", 1056}, {"etype", 1060},
@@ -145,7 +147,7 @@ int check_params(const sphgpu_params* P)
     // flag combinations this engine runs (the others are rejected loudly)
     if (!(P->flbndy >= 1 && P->flbndy <= 5) && P->flbndy != 13 && P->flbndy != 14) return SPHGPU_E_UNSUPPORTED;
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
-    if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
+    if (P->flv != 0) return SPHGPU_E_UNSUPPORTED;
     if (P->fli < 0 || P->fli > 3) return SPHGPU_E_UNSUPPORTED;
     if (P->ss_type < 0 || P->ss_type > 3) return SPHGPU_E_UNSUPPORTED;
     if (P->if_move < 0 || P->if_move > 3) return SPHGPU_E_UNSUPPORTED;
@@ -211,7 +213,8 @@ void* field_ptr(sphgpu_ctx* c, const char* name)
         {"vx", s.vx}, {"vxp", s.vxp}, {"ax", s.ax}, {"axp", s.axp}, {"ux", s.ux},
         {"strep", s.strep}, {"interf", s.interf}, {"interfss", s.interfss}, {"rho", s.rho},
         {"rhop", s.rhop}, {"mass", s.mass}, {"pre", s.pre}, {"prep", s.prep},
-        {"e", s.e}, {"eps", s.eps}, {"sig", s.sig}, {"adps", s.adps}, {"satu", s.satu}, {"cop", s.cop},
+        {"e", s.e}, {"eps", s.eps}, {"sig", s.sig}, {"adps", s.adps}, {"tssig", s.tssig}, {"tsqc", s.tsqc},
+        {"satu", s.satu}, {"dsatu", s.dsatu}, {"suct", s.suct}, {"cop", s.cop},
         {"vsig", s.vsig}, {"veps", s.veps}, {"divq", s.divq}, {"divr", s.divr}, {"meps", s.meps},
         {"prew", s.prew}, {"prea", s.prea}, {"porosity", s.porosity}, {"poro_cop", s.poro_cop},
         {"cd", s.cd}, {"type", s.type}, {"matype", s.matype}, {"permtype", s.permtype}, {"etype", s.etype},
@@ -234,15 +237,19 @@ void update_static_params(sphgpu_ctx* c)
 int check_particles(sphgpu_ctx* c)
 {
     if (c->h_type.empty() || c->h_matype.empty()) return SPHGPU_E_STATE;
+    bool ext = c->P.flagum == 1;
     for (int i = 0; i < c->N; i++) {
         const int t = c->h_type[i], m = c->h_matype[i];
+        // matype 30-49 and >= 60 match no branch of strain_to_stress
         if (t == 2) {
-            const int mt = m % 10;
-            if (!(mt == 0 || mt == 1 || mt == 2 || mt == 5 || mt == 6 || mt == 7 || mt == 9) || (m >= 30 && m < 50) ||
-                m >= 60)
+            if ((m >= 30 && m < 50) || m >= 60)
                 return SPHGPU_E_UNSUPPORTED;
+            if (m % 10 == 3 || m % 10 == 8) ext = true;
         }
     }
+    // those models and the saturation pass read material members that
+    // sphgpu_set_materials uploads once it has seen them in use
+    if (ext && !c->d[0].s.s_ext) return SPHGPU_E_STATE;
     return 0;
 }
 
@@ -317,6 +324,9 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     p.art_stre_coe = P->art_stre_coe;
     p.ss_type = P->ss_type; p.ss_myu = P->ss_myu; p.ss_zeta = P->ss_zeta;
     p.ss_coupled = (P->ss_type >= 1 && P->ss_type <= 3 && P->ss_acc_type == 2) ? 1 : 0;
+    p.flts = P->flts;
+    p.flagum = P->flagum;
+    p.alphats = P->alphats;
     DevState& s = d.s;
     int r = 0;
     r |= dalloc(c, &s.type, N); r |= dalloc(c, &s.matype, N); r |= dalloc(c, &s.etype, N); r |= dalloc(c, &s.permtype, N);
@@ -358,6 +368,8 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.prep, N); r |= dalloc(c, &s.porosity, N); r |= dalloc(c, &s.poro_cop, N); r |= dalloc(c, &s.e, N);
     r |= dalloc(c, &s.sig, 6 * (size_t)N); r |= dalloc(c, &s.sig_next, 6 * (size_t)N);
     r |= dalloc(c, &s.eps, 6 * (size_t)N); r |= dalloc(c, &s.adps, 6 * (size_t)N);
+    r |= dalloc(c, &s.tssig, 6 * (size_t)N); r |= dalloc(c, &s.tsqc, N);
+    r |= dalloc(c, &s.dsatu, N); r |= dalloc(c, &s.suct, N);
     r |= dalloc(c, &s.satu, N); r |= dalloc(c, &s.cop, N); r |= dalloc(c, &s.prew, N); r |= dalloc(c, &s.prea, N);
     r |= dalloc(c, &s.interf, 3 * (size_t)N); r |= dalloc(c, &s.interfss, 3 * (size_t)N); r |= dalloc(c, &s.strep, 3 * (size_t)N);
     r |= dalloc(c, &s.vsig, N); r |= dalloc(c, &s.veps, N); r |= dalloc(c, &s.divq, N); r |= dalloc(c, &s.divr, N);
@@ -613,6 +625,32 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
         buf = ya; r |= put(s.s_yalf);
         buf = yk; r |= put(s.s_ykap);
         buf = yd; r |= put(s.s_yalf_dil);
+        // the members only unsaturated Cam-clay (matype % 10 == 3), the
+        // saturation pass and fractional-order Cam-clay (8) read, allocated
+        // on first use; pow(c, 4) of fractional_mcc with the host's libm
+        // (CPP_8-5-consfactor-focc.cpp:158)
+        bool need = c->P.flagum == 1;
+        for (int i = 0; i < N && !need && i < (int)c->h_matype.size(); i++) {
+            const int mt = c->h_matype[i] % 10;
+            need = (mt == 3 || mt == 8);
+        }
+        if (need && !s.s_ext) {
+            double* q = nullptr;
+            if (dalloc(c, &q, (size_t)SX_COUNT * N)) return SPHGPU_E_CUDA;
+            for (int p = 0; p < 2; p++) c->d[p].s.s_ext = q;
+            invalidate_graphs(c);
+        }
+        if (s.s_ext) {
+            std::vector<double> ext((size_t)SX_COUNT * N);
+            for (int i = 0; i < N; i++) {
+                const sphgpu_soil& m = so[i];
+                const double v[SX_COUNT] = {m.epss, m.epsr, m.bnn, m.beta, m.sd, m.sw, m.c1, m.c2,
+                                            m.g0, m.etao, m.zet, m.damp1, m.damp2, std::pow(m.c, 4)};
+                for (int k = 0; k < SX_COUNT; k++) ext[(size_t)k * N + i] = v[k];
+            }
+            CK(cudaMemcpyAsync(s.s_ext, ext.data(), sizeof(double) * ext.size(), cudaMemcpyHostToDevice, c->st));
+            CK(cudaStreamSynchronize(c->st));
+        }
     }
     return r ? SPHGPU_E_CUDA : 0;
 }

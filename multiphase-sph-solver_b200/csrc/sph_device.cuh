@@ -54,6 +54,18 @@ struct DevParams {
     int ss_coupled;            // 1: coupled_Water_Soil_Structure (ss_type 1-3 with acc_type 2)
     double ss_myu, ss_zeta;
     int bulk;                  // 1: the FP32-bulk form (pair records in FP32)
+    int flts;                  // >= 1: TSSMP stress transformation around the soil models
+    int flagum;                // 1: the saturation pass (one unsaturated Cam-clay layer)
+    double alphats;            // TSSMP alpha
+};
+
+// Members of the soil record that only the unsaturated Cam-clay model, the
+// saturation pass and the fractional-order Cam-clay read, in one block
+// s_ext[k * N + i] (allocated when a particle uses them)
+enum SoilExt {
+    SX_EPSS, SX_EPSR, SX_BNN, SX_BETA, SX_SD, SX_SW, SX_C1, SX_C2,
+    SX_G0, SX_ETAO, SX_ZET, SX_DAMP1, SX_DAMP2, SX_C4,   // SX_C4 = pow(c, 4), host libm
+    SX_COUNT
 };
 
 struct DevState {
@@ -69,6 +81,7 @@ struct DevState {
     double *s_c, *s_fs;        // cohesion (viscous-elastic: shear modulus), strength reduction factor
     double *s_ann, *s_zmf, *s_ramda, *s_sme0;   // subloading Cam-clay
     double *s_yalf, *s_ykap, *s_yalf_dil;   // Drucker-Prager constants, host-evaluated
+    double *s_ext;             // SoilExt members, SX_COUNT * N (or null)
     // positions (x, y, z, h) records, ping-pong
     double *xh, *xh_next;
     double *xs;                // xh in cell-sorted order (NNPS scan)
@@ -79,7 +92,8 @@ struct DevState {
     double *rho, *rho_c, *rhop, *pre, *prep, *porosity, *poro_cop, *e;
     double *sig, *sig_next;    // 6N each, ping-pong
     double *eps, *adps;
-    double *satu, *cop, *prew, *prea;
+    double *tssig, *tsqc;      // TSSMP: the transformed stress and its q (flts >= 1)
+    double *satu, *dsatu, *suct, *cop, *prew, *prea;
     double *interf, *interfss, *strep;
     double *vsig, *veps, *divq, *divr, *meps;
     // per-step intermediates

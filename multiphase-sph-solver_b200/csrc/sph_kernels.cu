@@ -103,6 +103,35 @@ __device__ __forceinline__ int nbr_count(const Dev& d, int i)
     return c > SPH_NB_CAP ? SPH_NB_CAP : c;
 }
 
+// The list slots of particle i in order, each slot's particle index loaded
+// two slots ahead and its type one slot ahead.  A neighbour pass is a chain of
+// dependent loads per slot (list -> type -> the neighbour's fields); issuing
+// the first two for later slots while the current slot's gathers are in
+// flight leaves one load latency per slot instead of three.
+struct NbrIter {
+    const int* nbr;
+    const int* type;
+    size_t N;
+    int i, nn, s, j1, j2, t1;
+    __device__ __forceinline__ NbrIter(const Dev& d, int i_, int nn_)
+        : nbr(d.s.nbr), type(d.s.type), N((size_t)d.p.N), i(i_), nn(nn_), s(0)
+    {
+        j1 = (nn > 0) ? nbr[i] : 0;
+        j2 = (nn > 1) ? nbr[N + i] : 0;
+        t1 = (nn > 0) ? type[j1] : 0;
+    }
+    // slot s's particle and type; issues the loads of the slots after it
+    __device__ __forceinline__ void next(int& j, int& tj)
+    {
+        j = j1;
+        tj = t1;
+        j1 = j2;
+        t1 = (s + 1 < nn) ? type[j1] : 0;
+        j2 = (s + 2 < nn) ? nbr[(size_t)(s + 2) * N + i] : 0;
+        s++;
+    }
+};
+
 // ---------------------------------------------------------------------------
 #ifndef SPH_BULK32
 template <int ND>
@@ -186,6 +215,104 @@ __global__ void k_cellrange(Dev d)
 // candidate to the FP64 path.  Only candidates within M of T^2 take the FP64
 // path, where the sqrt is evaluated only within 1e-10 of the squared radius,
 // so the decisions are those of the reference.
+// The FP64 inclusion test of one candidate, as partisearching decides it:
+// sqrt of the FP64 sum of squares against h_i + h_j, the sqrt evaluated only
+// within 1e-10 of the squared radius (outside that band the comparison of the
+// squares gives the same answer).
+template <int ND>
+__device__ __forceinline__ bool nnps_in_fp64(const double xi[3], double hi, const Pos& pj)
+{
+    const double xj[3] = {pj.x, pj.y, pj.z};
+    double d2 = 0.0;
+    for (int k = 0; k < ND; k++) d2 = d2 + (xi[k] - xj[k]) * (xi[k] - xj[k]);
+    const double ra = (hi + pj.h) / 2;
+    const double T = 2 * ra, T2 = T * T;
+    if (d2 < T2 * (1.0 - 1.0e-10)) return true;
+    if (d2 > T2 * (1.0 + 1.0e-10)) return false;
+    return sqrt(d2) <= T;
+}
+
+// FP32 prefilter verdict of one candidate: 1 inside, 0 outside, -1 undecided
+// (within the rounding margin of the radius)
+template <int ND>
+__device__ __forceinline__ int nnps_prefilter(float fx, float fy, float fz, float fh, float ce, float ct, float4 fj)
+{
+    constexpr float U = 5.9604645e-8f;     // 2^-24
+    float t = fx - fj.x;
+    float d2f = t * t;
+    t = fy - fj.y;
+    d2f = d2f + t * t;
+    if (ND == 3) {
+        t = fz - fj.z;
+        d2f = d2f + t * t;
+    }
+    const float Tf = fh + fj.w, T2f = Tf * Tf;
+    if (d2f > 4.f * T2f) return 0;
+    const float e = ce + 4.4f * U * Tf;
+    const float M = ND * e * (4.f * Tf + e) + ct * T2f;
+    if (d2f < T2f - M) return 1;
+    if (d2f > T2f + M) return 0;
+    return -1;
+}
+
+// partisearching with every candidate decided in FP64 as soon as it is met
+// (used when the FP32 prefilter does not apply to the particle, or when its
+// provisional list below overflows); returns the neighbour count
+template <int ND>
+__device__ __forceinline__ int nnps_direct(const Dev& d, int i, int nc, const Pos& pi, bool fast, float fx, float fy,
+                                        float fz, float fh, float ce, float ct)
+{
+    const int N = d.p.N;
+    constexpr int nst = (ND == 2) ? 9 : 27;
+    const double xi[3] = {pi.x, pi.y, pi.z};
+    const float4* xsf = reinterpret_cast<const float4*>(d.s.xsf);
+    int cnt = 0;
+    for (int nj = 0; nj < nst; nj++) {
+        const int nl = cell_link(d.p, nc, nj);
+        if (nl <= 0) continue;
+        const int start = d.s.cstart[nl], end = d.s.cend[nl];
+        for (int q = start; q <= end; q++) {
+            int v = fast ? nnps_prefilter<ND>(fx, fy, fz, fh, ce, ct, xsf[q]) : -1;
+            if (v < 0) v = nnps_in_fp64<ND>(xi, pi.h, load_pos(d.s.xs, q)) ? 1 : 0;
+            if (v) {
+                const int j = d.s.pid_sorted[q];
+                if (i != j) {
+                    cnt++;
+                    if (cnt <= SPH_NB_CAP) d.s.nbr[(size_t)(cnt - 1) * N + i] = j;
+                    else raise_err(d.s.err, SPH_ERR_NEIGH);
+                }
+            }
+        }
+    }
+    return cnt;
+}
+
+// partisearching (CPP_3-NNPS.cpp:265-374): neighbours of i in stencil order,
+// descending index inside each cell; inclusion dst <= h_i + h_j decided as the
+// reference decides it (sqrt of the FP64 sum of squares).
+//
+// Each candidate is first tested in FP32 on the (x - xmin, y - ymin, z - zmin,
+// h) records, against a margin M that bounds every rounding between the FP32
+// squared distance d2f and the exact one: the coordinates' rounding to FP32
+// (at most 2^-24 |coordinate|, and |x_j - xmin| <= |x_i - xmin| + |x_i - x_j|),
+// the subtraction, squares and sum, and the rounding of T = h_i + h_j and T^2.
+// With F_i the particle's largest |coordinate - min| and e = 2.2 u (F_i + 2 T),
+// u = 2^-24, every candidate with d2f <= 4 T^2 has |d2f - d2| <= nd e (4 T + e)
+// + 12.4 u T^2; M adds 32 u T^2 on top of that.  Candidates with d2f > 4 T^2
+// are outside whenever h_i > 10 u F_i (the error then grows more slowly than
+// d2f - T^2); the test requires h_i > 64 u F_i and otherwise takes every
+// candidate to the FP64 test.
+//
+// Two passes keep the FP64 work out of the candidate scan, where a lattice's
+// many candidates at exactly the support radius would stall the whole warp
+// on nearly every step: the scan stores, in candidate order, the sorted
+// position q of each candidate inside (q) or undecided (~q) into the
+// particle's list slots; the second pass walks that list, decides the
+// undecided ones in FP64 and compacts the list in place to particle indices.
+// The order, and so the list, is the one the single pass gives.  A
+// provisional list longer than the capacity (possible only when undecided
+// candidates or the particle itself push it over) is redone by the direct
+// form, which also raises the reference's error for a true overflow.
 template <int ND>
 __global__ void __launch_bounds__(128, SPH_MINB) k_nnps(Dev d)
 {
@@ -193,61 +320,45 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_nnps(Dev d)
     if (i >= N || *d.s.err) return;
     int cnt = 0;
     if (d.s.type[i] != 7) {
-        constexpr int nd = ND, nst = (ND == 2) ? 9 : 27;
+        constexpr int nst = (ND == 2) ? 9 : 27;
         constexpr float U = 5.9604645e-8f;     // 2^-24
         const int nc = d.s.cell[i];
         const Pos pi = load_pos(d.s.xh, i);
-        const double xi[3] = {pi.x, pi.y, pi.z};
         const float fx = (float)(pi.x - d.p.xmin), fy = (float)(pi.y - d.p.ymin);
         const float fz = (ND == 3) ? (float)(pi.z - d.p.zmin) : 0.f, fh = (float)pi.h;
         float Fi = fmaxf(fabsf(fx), fabsf(fy));
         if (ND == 3) Fi = fmaxf(Fi, fabsf(fz));
         const bool fast = fh > 64.f * U * Fi;
         const float ce = 2.2f * U * Fi, ct = 32.f * U;
-        const float4* xsf = reinterpret_cast<const float4*>(d.s.xsf);
-        for (int nj = 0; nj < nst; nj++) {
-            const int nl = cell_link(d.p, nc, nj);
-            if (nl <= 0) continue;
-            const int start = d.s.cstart[nl], end = d.s.cend[nl];
-            for (int q = start; q <= end; q++) {
-                bool in = false, decided = false;
-                if (fast) {
-                    const float4 fj = xsf[q];
-                    float t = fx - fj.x;
-                    float d2f = t * t;
-                    t = fy - fj.y;
-                    d2f = d2f + t * t;
-                    if (ND == 3) {
-                        t = fz - fj.z;
-                        d2f = d2f + t * t;
-                    }
-                    const float Tf = fh + fj.w, T2f = Tf * Tf;
-                    if (d2f > 4.f * T2f) {
-                        decided = true;
-                    } else {
-                        const float e = ce + 4.4f * U * Tf;
-                        const float M = nd * e * (4.f * Tf + e) + ct * T2f;
-                        if (d2f < T2f - M) in = decided = true;
-                        else if (d2f > T2f + M) decided = true;
+        if (!fast) {
+            cnt = nnps_direct<ND>(d, i, nc, pi, false, fx, fy, fz, fh, ce, ct);
+        } else {
+            const float4* xsf = reinterpret_cast<const float4*>(d.s.xsf);
+            int np = 0;   // provisional entries
+            for (int nj = 0; nj < nst; nj++) {
+                const int nl = cell_link(d.p, nc, nj);
+                if (nl <= 0) continue;
+                const int start = d.s.cstart[nl], end = d.s.cend[nl];
+                for (int q = start; q <= end; q++) {
+                    const int v = nnps_prefilter<ND>(fx, fy, fz, fh, ce, ct, xsf[q]);
+                    if (v != 0) {
+                        if (np < SPH_NB_CAP) d.s.nbr[(size_t)np * N + i] = (v > 0) ? q : ~q;
+                        np++;
                     }
                 }
-                if (!decided) {
-                    const Pos pj = load_pos(d.s.xs, q);
-                    const double xj[3] = {pj.x, pj.y, pj.z};
-                    double d2 = 0.0;
-                    for (int k = 0; k < nd; k++) d2 = d2 + (xi[k] - xj[k]) * (xi[k] - xj[k]);
-                    const double ra = (pi.h + pj.h) / 2;
-                    const double T = 2 * ra, T2 = T * T;
-                    if (d2 < T2 * (1.0 - 1.0e-10)) in = true;
-                    else if (d2 > T2 * (1.0 + 1.0e-10)) in = false;
-                    else in = (sqrt(d2) <= T);
-                }
-                if (in) {
+            }
+            if (np > SPH_NB_CAP) {
+                cnt = nnps_direct<ND>(d, i, nc, pi, true, fx, fy, fz, fh, ce, ct);
+            } else {
+                const double xi[3] = {pi.x, pi.y, pi.z};
+                for (int s = 0; s < np; s++) {
+                    const int v = d.s.nbr[(size_t)s * N + i];
+                    const int q = (v < 0) ? ~v : v;
+                    const bool in = (v >= 0) || nnps_in_fp64<ND>(xi, pi.h, load_pos(d.s.xs, q));
                     const int j = d.s.pid_sorted[q];
-                    if (i != j) {
+                    if (in && j != i) {
+                        d.s.nbr[(size_t)cnt * N + i] = j;
                         cnt++;
-                        if (cnt <= SPH_NB_CAP) d.s.nbr[(size_t)(cnt - 1) * N + i] = j;
-                        else raise_err(d.s.err, SPH_ERR_NEIGH);
                     }
                 }
             }
@@ -265,10 +376,15 @@ __device__ __forceinline__ void pairw_particle(const Dev& d, int i)
 {
     const int N = d.p.N, nn = nbr_count(d, i);
     const PairI<R> I = pair_i<ND, R>(d, i);
+    // the next slot's index and position are loaded one slot ahead
+    int jn = (nn > 1) ? d.s.nbr[(size_t)N + i] : 0;
+    Pos pn = load_pos(d.s.xh, (nn > 0) ? d.s.nbr[i] : i);
     for (int s = 0; s < nn; s++) {
-        const int j = d.s.nbr[(size_t)s * N + i];
+        const Pos pj = pn;
+        if (s + 1 < nn) pn = load_pos(d.s.xh, jn);
+        if (s + 2 < nn) jn = d.s.nbr[(size_t)(s + 2) * N + i];
         R w[4];
-        pair_w_raw<ND, R>(d, I, load_pos(d.s.xh, j), w);
+        pair_w_raw<ND, R>(d, I, pj, w);
         store_w(d, s, i, w);
     }
 }
@@ -299,9 +415,11 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
     double pcop = d.s.poro_cop[i];
     if (ti == 1) {
         Sum<real> sup, sdown;
+        NbrIter it(d, i, nn);
         for (int s = 0; s < nn; s++) {
-            const int j = d.s.nbr[(size_t)s * N + i];
-            if (d.s.type[j] == 2) {
+            int j, tj;
+            it.next(j, tj);
+            if (tj == 2) {
                 real w[4];
                 load_w(d, s, i, w);
                 const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
@@ -327,9 +445,10 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
         for (int k = 0; k < 3; k++) vi[k] = d.s.vxp[k * N + i];
         const bool solid = (ti == 2 || ti == 4), fluid = (ti == 1 || ti == 3);
         const bool moving = (ti >= 1 && ti <= 4);
+        NbrIter it(d, i, nn);
         for (int s = 0; s < nn; s++) {
-            const int j = d.s.nbr[(size_t)s * N + i];
-            const int tj = d.s.type[j];
+            int j, tj;
+            it.next(j, tj);
             double vxj[3];
             if (ti == tj && ti != 0) {
                 for (int k = 0; k < 3; k++) vxj[k] = d.s.vxp[k * N + j];
@@ -383,9 +502,11 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_shepard_eos(Dev d)
     if (i >= N || *d.s.err) return;
     const int ti = d.s.type[i], nn = nbr_count(d, i);
     Sum<real> sup, sdown;
+    NbrIter it(d, i, nn);
     for (int s = 0; s < nn; s++) {
-        const int j = d.s.nbr[(size_t)s * N + i];
-        if (d.s.type[j] == ti) {
+        int j, tj;
+        it.next(j, tj);
+        if (tj == ti) {
             real w[4];
             load_w(d, s, i, w);
             const real mj = (real)d.s.mass[j];
@@ -434,9 +555,10 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_strain(Dev d)
     Sum<real> su1, su2, su3, su4, sd1, sd2, sd3, sd4;
     Sum<real> sus[6], sdsw;
     Sum<real> scolor;
+    NbrIter it(d, i, nn);
     for (int q = 0; q < nn; q++) {
-        const int j = d.s.nbr[(size_t)q * N + i];
-        const int tj = d.s.type[j];
+        int j, tj;
+        it.next(j, tj);
         const bool same = (ti == tj && ti != 7 && ti != 0);
         const bool wallj = (moving && tj == 0);
         const bool gath = (ti != tj) && ((ti == 2 || ti == 4 || ti == 0) && (tj == 1 || tj == 3 || (ti == 0 && tj == 2)));
@@ -529,6 +651,42 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_strain(Dev d)
 // PHASE 0 does all of it.  Where stress_regu can run (step_regu within the
 // run), PHASE 1 stops after the constitutive update (writing sig_next), the
 // smoothing pass runs, and PHASE 2 continues from the smoothed stresses.
+// saturation (flagum == 1, CPP_7-1-strain.cpp:222-281): each soil particle's
+// degree of saturation from the Shepard ratio of its water neighbours, its
+// change dsatu (a decrease is undone), the clamp to [sitar, sitas] and the
+// suction of moisturesuct.  Reads only the particle's own satu, so the
+// in-place and Jacobi orders agree.
+__global__ void __launch_bounds__(128, SPH_MINB) k_saturation(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err || d.s.type[i] != 2) return;
+    const double sitas = d.s.s_sitas[i], sitar = d.s.s_sitar[i], cof = sitas - sitar;
+    const int nn = nbr_count(d, i);
+    Sum<real> up, down;
+    for (int s = 0; s < nn; s++) {
+        const int j = d.s.nbr[(size_t)s * N + i];
+        if (d.s.type[j] != 1) continue;
+        real w[4];
+        load_w(d, s, i, w);
+        const double mr = d.s.mass[j] / d.s.rho[j];
+        up.add((real)(mr * cof) * w[3]);
+        down.add((real)mr * w[3]);
+    }
+    const double tempup = up.v(), tempdown = down.v();
+    const double psatu = d.s.satu[i];
+    double satu = (tempdown != 0.0) ? tempup / tempdown + sitar : tempup + sitar;
+    double dsatu = satu - psatu;
+    if (dsatu < 0) {
+        satu = satu - dsatu;
+        dsatu = 0.0;
+    }
+    if (satu > sitas) satu = sitas;
+    else if (satu < sitar) satu = sitar;
+    d.s.satu[i] = satu;
+    d.s.dsatu[i] = dsatu;
+    d.s.suct[i] = moisture_suction(satu, dsatu, sitas, sitar, d.s.s_ext + i, N);
+}
+
 template <int ND, int PHASE>
 __global__ void __launch_bounds__(128, SPH_MINB_STRESS) k_stress(Dev d)
 {
@@ -600,26 +758,68 @@ __global__ void __launch_bounds__(128, SPH_MINB_STRESS) k_stress(Dev d)
         for (int a = 0; a < 6; a++) s[a] = (a < 3) ? -pr - viscos1 * dd_[a] : -viscos1 * dd_[a];
     } else if (ti == 2 || ti == 4) {
         double D[6][6], adps[6] = {0, 0, 0, 0, 0, 0}, ds[6] = {0, 0, 0, 0, 0, 0};
+        double erfs[6] = {0, 0, 0, 0, 0, 0};
         double dlam, dmu, sm;
-        const int mt = d.s.matype[i] % 10;
+        const int m = d.s.matype[i], mt = m % 10;
         const bool plastic = (ti == 2) && !(l < d.p.inip);
         const bool dp = plastic && (mt == 2 || mt == 5);
+        // TSSMP step 1 (CPP_7-2-constitutive.cpp:99-101): the model and the
+        // Jaumann terms see the transformed stress
+        const bool ts = (ti == 2) && d.p.flts >= 1;
+        double ts_s[6], qc = 0.0;
+        if (ts) {
+            const double sp[3] = {d.s.strep[i], d.s.strep[N + i], d.s.strep[2 * N + i]};
+            qc = tssmp_before(s, ts_s, sp, d.s.vsig[i], d.s.divq[i], d.p.alphats);
+        }
         if (ti == 2) {
-            // elastic_plastic (M-C, matype 9) takes its mean stress with 0.333333333
+            // elastic_plastic (M-C, matype 9) and sub_camunsatu (3) take their
+            // mean stress with 0.333333333
             elastic_consts(s, d.s.s_e[i], d.s.s_poi[i], d.s.s_eps0[i], d.s.s_kapa[i], &dlam, &dmu, &sm,
-                           (plastic && mt == 9) ? 0.333333333 : 0.3333333333);
+                           (plastic && (mt == 9 || mt == 3)) ? 0.333333333 : 0.3333333333);
         } else {
             const double e0 = d.p.st_e, poi = d.p.st_poi;
             dlam = e0 * poi / (1.0 + poi) / (1.0 - 2.0 * poi);
             dmu = e0 * 0.5 / (1.0 + poi);
             sm = 0.0;
         }
-        fill_elastic(D, dlam, dmu);
+        // sub_camanisotropy (matype 4, CPP_8-2-consfactor-amcc.cpp:17-99) has
+        // its body commented out: its dept stays zero
+        fill_elastic(D, (plastic && mt == 4) ? 0.0 : dlam, (plastic && mt == 4) ? 0.0 : dmu);
         if (dp) dp_tangent(D, adps, s, de, dlam, dmu, sm, d.s.s_yalf[i], d.s.s_ykap[i], (mt == 5) ? d.s.s_yalf_dil[i] : 0.0);
         if (plastic && mt == 9) dp_tangent<true>(D, adps, s, de, dlam, dmu, sm, d.s.s_yalf[i], d.s.s_ykap[i], 0.0);
         if (plastic && mt == 1)
             subcam_tangent(D, adps, s, de, dlam, dmu, sm, d.s.s_ann[i], d.s.s_zmf[i], d.s.s_ramda[i], d.s.s_kapa[i],
                            d.s.s_eps0[i], d.s.s_sme0[i], d.s.s_fs[i]);
+        // the two rarely used models run out of line on copies in local
+        // memory, so that D, s and de of the other models stay in registers
+        if (plastic && mt == 3) {
+            double Dl[6][6], sl[6], dl[6], al[6], el[6];
+            for (int a = 0; a < 6; a++) {
+                sl[a] = s[a]; dl[a] = de[a]; al[a] = 0.0; el[a] = 0.0;
+                for (int b = 0; b < 6; b++) Dl[a][b] = D[a][b];
+            }
+            unsat_tangent(Dl, al, el, sl, dl, dlam, dmu, sm, d.s.satu[i], d.s.dsatu[i], d.s.s_zmf[i], d.s.s_fs[i],
+                          d.s.s_ramda[i], d.s.s_kapa[i], d.s.s_eps0[i], d.s.s_sme0[i], d.s.s_ann[i],
+                          d.s.s_sitas[i], d.s.s_sitar[i], d.s.s_ext + i, N);
+            for (int a = 0; a < 6; a++) {
+                adps[a] = al[a]; erfs[a] = el[a];
+                for (int b = 0; b < 6; b++) D[a][b] = Dl[a][b];
+            }
+        }
+        // fractional-order Cam-clay (matype 8): D and the elastic compliance C
+        double C[6][6];
+        const bool fo_plastic = (ti == 2) && (m == 8 || m == 18 || m == 28);
+        if (fo_plastic || (plastic && mt == 8))
+            for (int a = 0; a < 6; a++)
+                for (int b = 0; b < 6; b++) C[a][b] = 0.0;
+        if (plastic && mt == 8) {
+            double Dl[6][6], sl[6], dl[6];
+            for (int a = 0; a < 6; a++) { sl[a] = s[a]; dl[a] = de[a]; }
+            focc_tangent(Dl, C, sl, dl, d.s.e[i], d.s.s_poi[i], d.s.s_zmf[i], d.s.s_ramda[i], d.s.s_ann[i],
+                         d.s.s_ext + i, N);
+            for (int a = 0; a < 6; a++)
+                for (int b = 0; b < 6; b++) D[a][b] = Dl[a][b];
+        }
         if (plastic && mt == 7) {
             double smv;
             const double e0 = elastic_e0(s, d.s.s_e[i], d.s.s_poi[i], d.s.s_eps0[i], d.s.s_kapa[i], &smv);
@@ -628,12 +828,23 @@ __global__ void __launch_bounds__(128, SPH_MINB_STRESS) k_stress(Dev d)
             add_dense(ds, D, de);
         if (dp) dp_check(s, ds, d.s.s_yalf[i], d.s.s_ykap[i], dt);
         jaumann(ds, s, we9);
+        // fractional_plastic for matype 8, 18, 28 (:255-258).  In elastic steps
+        // (l < inip) the reference reads its compliance uninitialised there;
+        // only the output-only adps depends on it, and a zero compliance is
+        // taken.
+        if (fo_plastic) fractional_plastic(ds, de, adps, C);
+        if (ts) {
+            // TSSMP step 2 (:261-262): the rate back to the real stress space
+            tssmp_after(ds, s, ts_s, d.s.divq[i], qc);
+            for (int a = 0; a < 6; a++) d.s.tssig[a * N + i] = ts_s[a];
+            d.s.tsqc[i] = qc;
+        }
         if (ti == 2) {
             for (int a = 0; a < 6; a++) {
                 double ad = d.s.adps[a * N + i];
                 d.s.adps[a * N + i] = ad + adps[a] * dt;
                 ep[a] = ep[a] + de[a] * dt;
-                s[a] = s[a] + ds[a] * dt + 0.0;
+                s[a] = s[a] + ds[a] * dt + erfs[a];
             }
         } else {
             for (int a = 0; a < 6; a++) {
@@ -806,9 +1017,10 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_a(Dev d)
     double pi_own = 0.0;
     if (ti == 2) pi_own = (1 - poro_s) * (-satu_i * prew_i + (1 - satu_i) * prea_i) / dens_s / dens_s;
     if (ti == 4) pi_own = (-satu_i * prew_i + (1 - satu_i) * prea_i) / ri / ri;
+    NbrIter it(d, i, nn);
     for (int q = 0; q < nn; q++) {
-        const int j = d.s.nbr[(size_t)q * N + i];
-        const int tj = d.s.type[j];
+        int j, tj;
+        it.next(j, tj);
         const bool f_pair = fluid && (tj == ti || tj == other);
         const bool s_pair = solid && tj == ti;
         if (!(f_pair || s_pair)) continue;
@@ -970,9 +1182,10 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
             abr[k] = (real)(abd[k] / ri / ri);
         }
     }
+    NbrIter it(d, i, nn);
     for (int q = 0; q < nn; q++) {
-        const int j = d.s.nbr[(size_t)q * N + i];
-        const int tj = d.s.type[j];
+        int j, tj;
+        it.next(j, tj);
         const bool av_pair = (ti == tj && ti != 7);
         const bool b_pair = moving && tj == 0;
         const bool in_pair = d.p.fli >= 1 && ti != tj;
@@ -1235,9 +1448,10 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
         const real xs_same = (real)((ti == 1) ? d.p.xsph0 : (ti == 3) ? d.p.xsph2 : d.p.xsph1);
         const real xs_wall = (real)((ti == 1 || ti == 3) ? 0.006 : d.p.xsph1 / 5.0);
         Sum<real> stu[3], sdown;
+        NbrIter it(d, i, nn);
         for (int q = 0; q < nn; q++) {
-            const int j = d.s.nbr[(size_t)q * N + i];
-            const int tj = d.s.type[j];
+            int j, tj;
+            it.next(j, tj);
             real xishu;
             if (ti == tj) {
                 xishu = xs_same;
@@ -2182,6 +2396,7 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
     LAUNCH_ND(k_shepard_eos, nblk(N, 128), 128, d); n++;
     REC(9);
     LAUNCH_ND(k_strain, nblk(N, 128), 128, d); n++;
+    if (d.p.flagum == 1) { k_saturation<<<nblk(N, 128), 128, 0, st>>>(d); n++; }
     REC(10);
     if (regu) { LAUNCH_ND(k_regu, nblk(N, 128), 128, d, d.s.eps, d.s.eps_tmp, 1); n++; }
     REC(11);

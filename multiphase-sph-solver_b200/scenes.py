@@ -343,17 +343,40 @@ MODEL_FIELDS = {
     0: ("kapa", "poi", "dens") + _BASE,
     1: ("poi", "dens", "eps0", "zmf", "sme0", "fs", "ramda", "kapa", "damp1", "damp2", "cop", "ann", "ocr", "e", "ds"),
     2: ("kapa", "poi", "dens", "c", "fai", "fs") + _BASE,
+    3: ("poi", "dens", "eps0", "zmf", "sme0", "fs", "ramda", "kapa", "damp1", "damp2", "cop",
+        "ann", "bnn", "beta", "epss", "epsr", "sitas", "sitar", "sd", "sw", "kse", "c1", "c2", "c3",
+        "e", "ds"),
+    4: ("poi", "dens", "eps0", "zmf", "sme0", "fs", "ramda", "kapa", "damp1", "damp2", "cop",
+        "mzm", "azm", "r0", "bl", "bz", "zet", "e", "ds"),
     5: ("kapa", "poi", "dens", "c", "fai", "beta", "fs") + _BASE,
     6: ("kapa", "poi", "dens") + _BASE,
     7: ("kapa", "poi", "dens", "c") + _BASE,
+    8: ("dens", "c", "eps0", "cop", "sme0", "g0", "poi", "zmf", "ramda", "etao", "zet", "ann", "bnn",
+        "damp1", "damp2", "ds"),
     9: ("kapa", "poi", "dens", "c", "fai", "fs") + _BASE,
+}
+
+# the input blocks of models 3, 4 and 8, line by line (CPP_2-initialf.cpp:
+# 573-639, 719-740); model 8's reader then sets e = 5e6
+_BLOCKS = {
+    3: ("UM unsaturated cam-clay", (("poi", "dens", "eps0", "zmf", "sme0", "fs"),
+                                    ("ramda", "kapa", "damp1", "damp2", "cop"),
+                                    ("ann", "bnn", "beta", "epss", "epsr", "sitas", "sitar"),
+                                    ("sd", "sw", "kse", "c1", "c2", "c3"), ("e", "ds"))),
+    4: ("AM anisotropic cam-clay", (("poi", "dens", "eps0", "zmf", "sme0", "fs"),
+                                    ("ramda", "kapa", "damp1", "damp2", "cop"),
+                                    ("mzm", "azm", "r0", "bl", "bz", "zet"), ("e", "ds"))),
+    8: ("FC fractional order cam-clay", (("dens", "c", "eps0", "cop", "sme0"),
+                                         ("g0", "poi", "zmf", "ramda", "etao"),
+                                         ("zet", "ann", "bnn", "damp1", "damp2"), ("ds",))),
 }
 
 
 def set_soil_model(scene: Scene, matype: int, **record) -> Scene:
     """Switch every soil particle (type 2) to constitutive model `matype`
-    (0 elastic, 1 subloading Cam-clay, 2 Drucker-Prager, 5 Bui DP, 6 elastic,
-    7 viscous-elastic, 9 Mohr-Coulomb; one layer).  The record holds the
+    (0 elastic, 1 subloading Cam-clay, 2 Drucker-Prager, 3 unsaturated
+    Cam-clay, 4 anisotropic Cam-clay, 5 Bui DP, 6 elastic, 7 viscous-elastic,
+    8 fractional-order Cam-clay, 9 Mohr-Coulomb; one layer).  The record holds the
     members that model's input block reads, from `record`, else from the
     previous soil record; the others keep Para_Soil's defaults."""
     old = next(iter(scene.soils.values())) if scene.soils else soil_default()
@@ -368,6 +391,14 @@ def set_soil_model(scene: Scene, matype: int, **record) -> Scene:
     flags = [0] * 10
     flags[matype % 10] = 1
     scene.model_flags = tuple(flags)
+    return scene
+
+
+def keep(scene: Scene, mask: np.ndarray) -> Scene:
+    """The scene with only the particles where `mask` is true, in their order."""
+    m = np.asarray(mask, bool)
+    for name in ("xp", "vxp", "ptype", "matype", "permtype", "etype"):
+        setattr(scene, name, getattr(scene, name)[m].copy())
     return scene
 
 
@@ -452,8 +483,19 @@ def write_input_dat(scene: Scene, path: str, ntd: int = 1) -> None:
     add("MS soil models")
     add("A data")
     add(" ".join(str(v) for v in scene.model_flags))
+    if F["flts"] >= 1:
+        add(" ".join(_f(v) for v in P.get("ts", (0.0, 0.0))))     # alphats, damp_coe
     add("E end")
     mf = scene.model_flags
+    for flag, (title, lines) in _BLOCKS.items():
+        if mf[flag] >= 1:
+            add(title)
+            add("A data")
+            for layer in range(mf[flag]):
+                s = scene.soils[layer * 10 + flag]
+                for keys in lines:
+                    add(" ".join(_f(s[k]) for k in keys))
+            add("E end")
     if mf[0] >= 1:
         add("EM elastic")
         add("A data")
@@ -540,9 +582,12 @@ def material_tables(scene: Scene):
     soils = [soil_default() for _ in range(30)]
     for idx, s in scene.soils.items():
         soils[idx] = dict(s)
+    damp_coe = scene.problem.get("ts", (0.0, 0.0))[1] if scene.flags["flts"] >= 1 else 0.0
     for s in soils:
         s["vpu"] = 600.0
-        s["damp_coe"] = 0.0
+        s["damp_coe"] = damp_coe
+    for layer in range(scene.model_flags[8]):
+        soils[layer * 10 + 8]["e"] = 5.0e6
     water = [dict(fluid_default(), **w) for w in scene.water]
     for k in (1, 2):
         for key in ("press_type", "bhtype", "pre_coe", "strain_min"):
@@ -571,6 +616,15 @@ def material_tables(scene: Scene):
     st["vpu"] = 600.0
     st["porosity"] = st["eps0"] / (1 + st["eps0"])
     return soils, water, air, st
+
+
+def moisturesuct(satu: float, dsatu: float, soil) -> float:
+    """Suction on the wetting (dsatu > 0) or drying curve,
+    CPP_7-2-constitutive.cpp:323-338, with pi = 3.141592653."""
+    temp = math.tan(3.141592653 * (soil["sitas"] - satu) / (soil["sitas"] - soil["sitar"]) / 2.0)
+    if dsatu > 0.0:
+        return math.log(1 + math.exp(soil["c2"] * soil["sw"]) * temp) / soil["c2"]
+    return math.log(1 + math.exp(soil["c1"] * soil["sd"]) * temp) / soil["c1"]
 
 
 @dataclass
@@ -620,8 +674,9 @@ def initialise(scene: Scene) -> InitialState:
     f = {name: np.zeros((n, nc)) for name, nc in
          (("x", 3), ("vx", 3), ("ax", 3), ("axp", 3), ("ux", 3), ("strep", 3), ("interf", 3),
           ("interfss", 3), ("eps", 6), ("sig", 6), ("adps", 6))}
-    for name in ("rho", "rhop", "mass", "hl", "pre", "prep", "e", "satu", "cop", "porosity", "cd",
-                 "poro_cop", "prew", "prea", "vsig", "veps", "divq", "divr", "meps"):
+    f["tssig"] = np.zeros((n, 6))
+    for name in ("rho", "rhop", "mass", "hl", "pre", "prep", "e", "satu", "dsatu", "suct", "cop", "porosity",
+                 "cd", "poro_cop", "prew", "prea", "vsig", "veps", "divq", "divr", "meps", "tsqc"):
         f[name] = np.zeros(n)
     f["xp"] = scene.xp.copy()
     f["vxp"] = scene.vxp.copy()
@@ -706,6 +761,10 @@ def initialise(scene: Scene) -> InitialState:
     a1 = air_ & (fl["press_type"] != 0)
     f["prep"][a1] = fl["dens"][a1] * (-g) * np.abs(z[a1] - hmaxw - fl["pre_coe"][a1] * dr)
     f["pre"][air_] = f["prep"][air_]
+    # suction of unsaturated Cam-clay soil, moisturesuct(satu, -1e-4) with the
+    # C library's tan / exp / log (:1345-1346, 1356-1357)
+    for i in np.nonzero(is_s & np.isin(mt, (3, 13, 23)))[0]:
+        f["suct"][i] = moisturesuct(f["satu"][i], -0.0001, so[i])
     f.pop("roue", None)
     # input_par domain box (:917-1002) and celllist_ini1 (CPP_3-NNPS.cpp:96-121)
     bmax = np.maximum(scene.xp.max(axis=0), -10000.0)
@@ -737,7 +796,8 @@ def initialise(scene: Scene) -> InitialState:
         move_vx=tuple(P.get("move_vx", (0.0, 0.0, 0.0))),
         xmin=bmin[0], xmax=bmax[0], ymin=bmin[1], ymax=bmax[1], zmin=bmin[2], zmax=bmax[2],
         cxm=cxm, cym=cym, czm=czm, ctotal=cxm * cym * czm,
-        flagum=scene.model_flags[3], alphats=0.0,
+        flagum=scene.model_flags[3],
+        alphats=P.get("ts", (0.0, 0.0))[0] if scene.flags["flts"] >= 1 else 0.0,
         water_acc_type=water[0]["acc_type"], air_acc_type=air["acc_type"],
         structure=st,
     )

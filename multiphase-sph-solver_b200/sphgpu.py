@@ -106,7 +106,8 @@ def params_to_dict(p: Params) -> dict:
 FIELDS = {
     "x": 3, "xp": 3, "vx": 3, "vxp": 3, "ax": 3, "axp": 3, "ux": 3, "strep": 3,
     "interf": 3, "interfss": 3, "rho": 1, "rhop": 1, "mass": 1, "hl": 1, "pre": 1, "prep": 1,
-    "e": 1, "eps": 6, "sig": 6, "adps": 6, "satu": 1, "cop": 1, "vsig": 1, "veps": 1,
+    "e": 1, "eps": 6, "sig": 6, "adps": 6, "tssig": 6, "tsqc": 1, "satu": 1, "dsatu": 1,
+    "suct": 1, "cop": 1, "vsig": 1, "veps": 1,
     "divq": 1, "divr": 1, "meps": 1, "prew": 1, "prea": 1, "porosity": 1, "poro_cop": 1,
     "cd": 1, "type": 1, "matype": 1, "permtype": 1, "etype": 1,
 }

@@ -211,7 +211,7 @@ int ref_get_field(void* h, const char* name, void* out)
     DV(x, 3) DV(xp, 3) DV(vx, 3) DV(vxp, 3) DV(ax, 3) DV(axp, 3) DV(ux, 3) DV(strep, 3)
     DV(divx, 9) DV(interf, 3) DV(interfss, 3) DV(rho, 1) DV(rhop, 1) DV(mass, 1) DV(hl, 1)
     DV(pre, 1) DV(prep, 1) DV(e, 1) DV(eps, 6) DV(deps, 6) DV(sig, 6) DV(dsig, 6) DV(weps, 9)
-    DV(adps, 6) DV(satu, 1) DV(dsatu, 1) DV(suct, 1) DV(cop, 1) DV(vsig, 1) DV(veps, 1)
+    DV(adps, 6) DV(tssig, 6) DV(tsqc, 1) DV(satu, 1) DV(dsatu, 1) DV(suct, 1) DV(cop, 1) DV(vsig, 1) DV(veps, 1)
     DV(divq, 1) DV(divr, 1) DV(meps, 1) DV(prew, 1) DV(prea, 1) DV(porosity, 1) DV(cd, 1)
     DV(poro_cop, 1) DV(beta, 9) DV(beta_ts, 9)
     IV(type) IV(matype) IV(permtype) IV(etype)

@@ -23,7 +23,7 @@ struct orc_ctx {
     /* Particle members (Class_particle.h:13-103), particle-major */
     double *x, *xp, *vx, *vxp, *ax, *axp, *ux, *strep, *divx, *interf, *interfss;
     double *rho, *rhop, *mass, *hl, *pre, *prep, *e;
-    double *eps, *deps, *sig, *dsig, *weps, *adps;
+    double *eps, *deps, *sig, *dsig, *weps, *adps, *tssig, *tsqc;
     double *satu, *dsatu, *suct, *cop, *vsig, *veps, *divq, *divr, *meps;
     double *prew, *prea, *porosity, *cd, *poro_cop, *beta, *beta_ts;
     int *type, *matype, *permtype, *etype;
@@ -60,7 +60,7 @@ static const field_desc k_fields[] = {
     FD(x, 3), FD(xp, 3), FD(vx, 3), FD(vxp, 3), FD(ax, 3), FD(axp, 3), FD(ux, 3),
     FD(strep, 3), FD(divx, 9), FD(interf, 3), FD(interfss, 3),
     FD(rho, 1), FD(rhop, 1), FD(mass, 1), FD(hl, 1), FD(pre, 1), FD(prep, 1), FD(e, 1),
-    FD(eps, 6), FD(deps, 6), FD(sig, 6), FD(dsig, 6), FD(weps, 9), FD(adps, 6),
+    FD(eps, 6), FD(deps, 6), FD(sig, 6), FD(dsig, 6), FD(weps, 9), FD(adps, 6), FD(tssig, 6), FD(tsqc, 1),
     FD(satu, 1), FD(dsatu, 1), FD(suct, 1), FD(cop, 1), FD(vsig, 1), FD(veps, 1),
     FD(divq, 1), FD(divr, 1), FD(meps, 1), FD(prew, 1), FD(prea, 1), FD(porosity, 1),
     FD(cd, 1), FD(poro_cop, 1), FD(beta, 9), FD(beta_ts, 9),
@@ -892,6 +892,306 @@ static void dpmodel(double dept[6][6], const double* sig, const double* deps, co
     }
 }
 
+/* sub_camunsatu: unsaturated subloading Cam-clay, CPP_8-4-consfactor-umcc.cpp:
+ * 17-180.  Its elastic part takes the mean stress with 0.333333333; the
+ * suction term rous follows the particle's degree of saturation, and the
+ * plastic branch also sets the stress correction erfs. */
+static void sub_camunsatu(double dept[6][6], double* erfs, const double* sig, const double* deps,
+                          double satu, double dsatu, const sphgpu_soil* so, double* adps)
+{
+    double zkapa = so->kapa, poi = so->poi, eps0 = so->eps0;
+    double qq = (so->epsr - so->epss) / (so->sitas - so->sitar);
+    double sigct[6];
+    for (int a = 0; a < 6; a++) sigct[a] = -sig[a];
+    double ymf = 3.0 * (so->zmf - 1.0) / (so->zmf + 2.0) / so->fs;
+    double sm = (sigct[0] + sigct[1] + sigct[2]) * 0.333333333;
+    if (sm < 1.0) sm = 1.0;
+    double e0;
+    if (so->e > 1.0) e0 = so->e;
+    else e0 = 3 * (1 - 2 * poi) * (1 + eps0) * fabs(sm) / zkapa;
+    double hee = (so->ramda - so->kapa) / (1.0 + eps0);
+    double dlam = e0 * poi / (1.0 + poi) / (1.0 - 2.0 * poi);
+    double dmu = e0 * 0.5 / (1.0 + poi);
+    double dmu2 = dmu * 2.0;
+    dept[0][0] = dlam + dmu2; dept[1][1] = dlam + dmu2; dept[2][2] = dlam + dmu2;
+    dept[0][1] = dlam; dept[0][2] = dlam; dept[1][0] = dlam;
+    dept[1][2] = dlam; dept[2][0] = dlam; dept[2][1] = dlam;
+    dept[3][3] = dmu; dept[4][4] = dmu; dept[5][5] = dmu;
+    double dx = sigct[0] - sm, dy = sigct[1] - sm, dz = sigct[2] - sm;
+    double dxy = sigct[3], dyz = sigct[4], dzx = sigct[5];
+    double sjj = 0.5 * (dx * dx + dy * dy + dz * dz) + dxy * dxy + dyz * dyz + dzx * dzx;
+    double tt1 = 1.0 / (ymf * ymf * sm * sm + 3.0 * sjj);
+    double tt2 = 2.0 * ymf * ymf * sm * tt1 - 1.0 / sm;
+    double f11 = tt2 * 0.333333333 + dx * tt1 * 3.0;
+    double f22 = tt2 * 0.333333333 + dy * tt1 * 3.0;
+    double f33 = tt2 * 0.333333333 + dz * tt1 * 3.0;
+    double f12 = 3.0 * dxy * tt1, f23 = 3.0 * dyz * tt1, f31 = 3.0 * dzx * tt1;
+    double rous = qq * (so->sitas - satu);
+    double roue = hee * (1.0 + so->eps0) * log(so->sme0 / sm);
+    double ttt = so->ann * roue + so->bnn * rous;
+    ttt = pow(ttt, so->beta);
+    double hdd = f11 + f22 + f33 + ttt / sm;
+    double fkk = f11 + f22 + f33;
+    double fij = 2.0 * (f11 * f11 + f22 * f22 + f33 * f33) + f12 * f12 + f23 * f23 + f31 * f31;
+    double cc7 = dlam * (fkk * fkk) + dmu * fij + hdd / hee;
+    double d = 1.0 / cc7;
+    double df = dlam * fkk, dg = dlam * fkk;
+    double ramda = (dmu2 * f11 + dlam * fkk) * deps[0] + (dmu2 * f22 + dlam * fkk) * deps[1]
+        + (dmu2 * f33 + dlam * fkk) * deps[2] + dmu * (f12 * deps[3] + f23 * deps[4] + f31 * deps[5]);
+    double omake = qq * dsatu / (so->ramda - so->kapa);
+    ramda = ramda + omake;
+    if (ramda < 0.0) {
+        erfs[0] = omake * d * (dept[0][0] * f11 + dept[0][1] * f22 + dept[0][2] * f33);
+        erfs[1] = omake * d * (dept[1][0] * f11 + dept[1][1] * f22 + dept[1][2] * f33);
+        erfs[2] = omake * d * (dept[2][0] * f11 + dept[2][1] * f22 + dept[2][2] * f33);
+        erfs[3] = omake * d * (dept[3][3] * f12);
+        erfs[4] = omake * d * (dept[4][4] * f23);
+        erfs[5] = omake * d * (dept[5][5] * f31);
+        double ww[6] = {dg + dmu2 * f11, dg + dmu2 * f22, dg + dmu2 * f33, dmu * f12, dmu * f23, dmu * f31};
+        double zz[6] = {df + dmu2 * f11, df + dmu2 * f22, df + dmu2 * f33, dmu * f12, dmu * f23, dmu * f31};
+        plastic_update(dept, d, ww, zz);
+        adps[0] = ramda * d * f11; adps[1] = ramda * d * f22; adps[2] = ramda * d * f33;
+        adps[3] = ramda * d * f12; adps[4] = ramda * d * f23; adps[5] = ramda * d * f31;
+    }
+}
+
+/* detA: determinant by cofactor expansion along the first row, recursively
+ * (CPP_8-5-consfactor-focc.cpp:265-290) */
+static double fo_det(double a[6][6], int n)
+{
+    double bak[6][6], sum = 0;
+    if (n == 1) return a[0][0];
+    for (int i = 0; i < n; i++) {
+        for (int j = 1; j < n; j++) {
+            int cc = 0;
+            for (int k = 0; k < n; k++) {
+                if (k == i) continue;
+                bak[j - 1][cc++] = a[j][k];
+            }
+        }
+        sum += (i % 2 == 0 ? 1 : -1) * a[0][i] * fo_det(bak, n - 1);
+    }
+    return sum;
+}
+
+/* getAStart: the adjugate, ans[j][i] = (-1)^(i+j) det(minor i, j)
+ * (CPP_8-5-consfactor-focc.cpp:293-322) */
+static void fo_adjugate(double a[6][6], int n, double ans[6][6])
+{
+    double tmp[6][6];
+    if (n == 1) { ans[0][0] = 1.0; return; }
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) {
+            for (int k = 0; k < n - 1; k++)
+                for (int t = 0; t < n - 1; t++) tmp[k][t] = a[k >= i ? k + 1 : k][t >= j ? t + 1 : t];
+            ans[j][i] = fo_det(tmp, n - 1);
+            if ((i + j) % 2 == 1) ans[j][i] = -ans[j][i];
+        }
+}
+
+/* fractional_mcc: fractional-order plastic model of MCC,
+ * CPP_8-5-consfactor-focc.cpp:13-247.  dept is the inverse of the compliance
+ * (elastic, plus the plastic part n m / hp when the Cam-clay loading index
+ * ramda_cc is negative) by adjugate / determinant; cijkl keeps the elastic
+ * compliance for fractional_plastic. */
+static void fractional_mcc(double dept[6][6], double cijkl[6][6], const double* sig, const double* deps,
+                           double e, const sphgpu_soil* so)
+{
+    double sigct[6], sij[6], smn[3][3], mij[6], nij[6], pijkl[6][6], total[6][6], adjoint[6][6];
+    double p0 = 98000, pa = 98000;
+    double poi = so->poi, h1 = so->damp1, h2 = so->damp2, ramda = so->ramda, mc = so->zmf;
+    double alpha = so->ann, beta = so->bnn, c = so->c, zeta = so->zet, etao = so->etao, g0 = so->g0;
+    for (int a = 0; a < 6; a++) {
+        sigct[a] = -sig[a];
+        for (int b = 0; b < 6; b++) { cijkl[a][b] = 0.0; pijkl[a][b] = 0.0; }
+    }
+    double sm = (sigct[0] + sigct[1] + sigct[2]) / 0.33333333;
+    for (int a = 0; a < 6; a++) sij[a] = (a < 3) ? sigct[a] - sm : sigct[a];
+    double q = 0.5 * (sij[0] * sij[0] + sij[1] * sij[1] + sij[2] * sij[2]) + sij[3] * sij[3] + sij[4] * sij[4] + sij[5] * sij[5];
+    q = sqrt(3.0 * q);
+    double ita = q / sm;
+    if (ita == 0.0) {
+        ita = 0.000001;
+        q = ita * sm;
+    }
+    double g = g0 * (2.97 - e) * (2.97 - e) / (1.0 + e) * sqrt(sm * pa);
+    double e0 = 2.0 * g * (1.0 + poi);
+    double ymf = mc;
+    double dlam = e0 * poi / (1.0 + poi) / (1.0 - 2.0 * poi);
+    double dmu = e0 * 0.5 / (1.0 + poi);
+    double dmu2 = dmu * 2.0;
+    double tt1 = 1.0 / (ymf * ymf * sm * sm + q * q);
+    double tt2 = 2.0 * ymf * ymf * sm * tt1 - 1.0 / sm;
+    double f11 = tt2 * 0.33333333 + sij[0] * tt1 * 3.0;
+    double f22 = tt2 * 0.33333333 + sij[1] * tt1 * 3.0;
+    double f33 = tt2 * 0.33333333 + sij[2] * tt1 * 3.0;
+    double f12 = 3.0 * sij[3] * tt1, f23 = 3.0 * sij[4] * tt1, f31 = 3.0 * sij[5] * tt1;
+    double fkk = f11 + f22 + f33;
+    double ramda_cc = (dmu2 * f11 + dlam * fkk) * deps[0] + (dmu2 * f22 + dlam * fkk) * deps[1]
+        + (dmu2 * f33 + dlam * fkk) * deps[2] + dmu * (f12 * deps[3] + f23 * deps[4] + f31 * deps[5]);
+    /* Lode angle */
+    smn[0][0] = sij[0]; smn[0][1] = sij[3]; smn[0][2] = sij[5];
+    smn[1][0] = sij[3]; smn[1][1] = sij[1]; smn[1][2] = sij[4];
+    smn[2][0] = sij[5]; smn[2][1] = sij[4]; smn[2][2] = sij[2];
+    double s_val = 0.0, skl = 0.0;
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++)
+            for (int k = 0; k < 3; k++) s_val = s_val + smn[a][b] * smn[b][k] * smn[k][a];
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) skl = skl + smn[a][b] * smn[b][a];
+    if (skl == 0.0) skl = 0.000001;
+    double sita = 9.0 * s_val * 0.5 / pow(1.5 * skl, 1.5);
+    if (sita < -1.0) sita = -1.0;
+    else if (sita > 1.0) sita = 1.0;
+    sita = asin(sita) * 0.33333333;
+    c = pow(c, 4);
+    double m = 2 * c / (1 + c + (1 - c) * sin(3.0 * sita));
+    m = pow(m, 0.25);
+    m = mc * m;
+    double pc = pa * pow((etao - e) / ramda, 1 / zeta);
+    double qc = q + m * (sm - pc);
+    double df = (sm - p0 / 2) * mc * mc / q;
+    double dg = ((sm - pc) + (2 - alpha) * (pc - sm * 0.5 - q * q / mc / mc / sm / 2)) / ((q - qc) + (2 - alpha) * qc);
+    dg = pow(m, alpha + 1) * dg;
+    for (int a = 0; a < 6; a++) {
+        mij[a] = 1.0 / sqrt(1.0 + df * df) * ((a < 3) ? 3.0 * sij[a] * 0.5 / q + df * 0.33333333 : 3.0 * sij[a] * 0.5 / q);
+        nij[a] = 1.0 / sqrt(1.0 + dg * dg) * ((a < 3) ? 3.0 * sij[a] * 0.5 / q + dg * 0.33333333 : 3.0 * sij[a] * 0.5 / q);
+    }
+    double order = beta * (e - etao + ramda * pow(sm / pa, zeta));
+    double mf = mc * pow(2.71828, -order);
+    double hp = (h1 - h2 * e) * (1 - e) * g * (mf - ita) / ita * pow(2.71828, order);
+    cijkl[0][0] = 1.0 / e0; cijkl[1][1] = 1.0 / e0; cijkl[2][2] = 1.0 / e0;
+    cijkl[0][1] = -poi / e0; cijkl[0][2] = -poi / e0; cijkl[1][0] = -poi / e0;
+    cijkl[1][2] = -poi / e0; cijkl[2][0] = -poi / e0; cijkl[2][1] = -poi / e0;
+    cijkl[3][3] = 1.0 / g; cijkl[4][4] = 1.0 / g; cijkl[5][5] = 1.0 / g;
+    for (int a = 0; a < 6; a++)
+        for (int b = 0; b < 6; b++) pijkl[a][b] = nij[a] * mij[b] / hp;
+    for (int a = 0; a < 6; a++)
+        for (int b = 0; b < 6; b++) total[a][b] = (ramda_cc < 0.0) ? cijkl[a][b] + pijkl[a][b] : cijkl[a][b];
+    double det_a = fo_det(total, 6);
+    fo_adjugate(total, 6, adjoint);
+    /* a singular total falls back to the elastic compliance; the reference
+     * switches on the first element, so every element takes it */
+    if (det_a == 0.0) {
+        det_a = fo_det(cijkl, 6);
+        fo_adjugate(cijkl, 6, adjoint);
+    }
+    for (int a = 0; a < 6; a++)
+        for (int b = 0; b < 6; b++) dept[a][b] = adjoint[a][b] / det_a;
+}
+
+/* fractional_plastic: plastic strain rate = strain rate - C dsig,
+ * CPP_8-5-consfactor-focc.cpp:250-264 */
+static void fractional_plastic(const double* dsig, const double* deps, double* adps, double cijkl[6][6])
+{
+    double eeps[6];
+    for (int a = 0; a < 6; a++) {
+        eeps[a] = 0.0;
+        for (int b = 0; b < 6; b++) eeps[a] = eeps[a] + cijkl[a][b] * dsig[b];
+    }
+    for (int a = 0; a < 6; a++) adps[a] = deps[a] - eeps[a];
+}
+
+/* TSSMP_before: the transformed stress of the SMP criterion from the
+ * principal stresses of the last Stress_eigValue, CPP_7-3-TS.cpp:14-67 */
+static void tssmp_before(orc_ctx* c, int i, double alpha)
+{
+    double* s = &c->sig[i * 6];
+    const double* sp = &c->strep[i * 3];
+    double qc = 0.0, sx[6];
+    c->tsqc[i] = 0.0;
+    sx[0] = -s[0] + c->vsig[i];
+    sx[1] = -s[1] + c->vsig[i];
+    sx[2] = -s[2] + c->vsig[i];
+    sx[3] = -s[3]; sx[4] = -s[4]; sx[5] = -s[5];
+    double q = c->divq[i];
+    double I1 = -(sp[0] + sp[1] + sp[2]);
+    double I2 = sp[0] * sp[1] + sp[1] * sp[2] + sp[2] * sp[1];
+    double I3 = -sp[0] * sp[1] * sp[2];
+    if ((I1 * I1 - 3.0 * I2) >= 1.0e-7) {
+        double temp = 3.0 * sqrt((I1 * I2 - I3) / (I1 * I2 - 9.0 * I3)) - 1.0;
+        if (fabs(temp) >= 1.0e-7)
+            qc = alpha * sqrt(I1 * I1 - 3.0 * I2) + 2.0 * (1.0 - alpha) * I1 / (3.0 * sqrt((I1 * I2 - I3) / (I1 * I2 - 9.0 * I3)) - 1.0);
+        else
+            qc = 0.0;
+    } else
+        qc = 0.0;
+    c->tsqc[i] = qc;
+    for (int a = 0; a < 6; a++) c->tssig[i * 6 + a] = s[a];
+    if (q != 0.0) {
+        s[0] = -I1 * 0.33333333 - qc / q * sx[0];
+        s[1] = -I1 * 0.33333333 - qc / q * sx[1];
+        s[2] = -I1 * 0.33333333 - qc / q * sx[2];
+        s[3] = -qc / q * sx[3];
+        s[4] = -qc / q * sx[4];
+        s[5] = -qc / q * sx[5];
+    }
+}
+
+/* TSSMP_after: the stress rate back to the real stress space; sig and tssig
+ * exchange, CPP_7-3-TS.cpp:69-105 */
+static void tssmp_after(orc_ctx* c, int i, double* ds)
+{
+    double q = c->divq[i], qc = c->tsqc[i], temp[6];
+    double* s = &c->sig[i * 6];
+    double* ts = &c->tssig[i * 6];
+    double dvsig = (ds[0] + ds[1] + ds[2]) / 3.0;
+    if (qc != 0.0) {
+        ds[0] = dvsig + q / qc * (ds[0] - dvsig);
+        ds[1] = dvsig + q / qc * (ds[1] - dvsig);
+        ds[2] = dvsig + q / qc * (ds[2] - dvsig);
+        ds[3] = q / qc * ds[3];
+        ds[4] = q / qc * ds[4];
+        ds[5] = q / qc * ds[5];
+    }
+    for (int a = 0; a < 6; a++) temp[a] = ts[a];
+    for (int a = 0; a < 6; a++) ts[a] = s[a];
+    for (int a = 0; a < 6; a++) s[a] = temp[a];
+}
+
+/* moisturesuct: suction from the degree of saturation on the wetting or
+ * drying curve, CPP_7-2-constitutive.cpp:323-338 (its first tan, for
+ * saturations within 1e-4 of the residual one, is overwritten) */
+static double moisturesuct(double satu, double dsatu, const sphgpu_soil* so)
+{
+    const double pi_ = 3.141592653;   /* Header_Parameters.h:10 */
+    double temp = tan(pi_ * (so->sitas - satu) / (so->sitas - so->sitar) / 2.0);
+    if (dsatu > 0.0) return log(1 + exp(so->c2 * so->sw) * temp) / so->c2;
+    return log(1 + exp(so->c1 * so->sd) * temp) / so->c1;
+}
+
+/* saturation: degree of saturation of soil particles from their water
+ * neighbours (flagum == 1), CPP_7-1-strain.cpp:222-281 */
+static void saturation(orc_ctx* c)
+{
+    for (int i = 0; i < c->n; i++) {
+        if (c->type[i] != 2) continue;   /* the sums of other particles are unused */
+        const sphgpu_soil* so = &c->so[i];
+        double cof = so->sitas - so->sitar, sitas = so->sitas, sitar = so->sitar;
+        double tempup = 0.0, tempdown = 0.0;
+        int nc = c->ninflu[i];
+        for (int nj = 1; nj <= nc; nj++) {
+            int j = c->influ[i * NB + nj];
+            if (c->type[j] == 1) {
+                double w = c->wij[((size_t)i * NB + nj) * 4 + 3];
+                tempup = tempup + c->mass[j] / c->rho[j] * cof * w;
+                tempdown = tempdown + c->mass[j] / c->rho[j] * w;
+            }
+        }
+        double psatu = c->satu[i];
+        if (tempdown != 0.0) c->satu[i] = tempup / tempdown + sitar;
+        else c->satu[i] = tempup + sitar;
+        c->dsatu[i] = c->satu[i] - psatu;
+        if (c->dsatu[i] < 0) {
+            c->satu[i] = c->satu[i] - c->dsatu[i];
+            c->dsatu[i] = 0.0;
+        }
+        if (c->satu[i] > sitas) c->satu[i] = sitas;
+        else if (c->satu[i] < sitar) c->satu[i] = sitar;
+        c->suct[i] = moisturesuct(c->satu[i], c->dsatu[i], so);
+    }
+}
+
 /* DPModel_check: stress-scaling return, CPP_8-1-consfactor.cpp:779-819 */
 static void dp_check(double* sig, double* dsig, const sphgpu_soil* so, double dt)
 {
@@ -933,8 +1233,10 @@ static void jaumann(double* ds, const double* s, const double* w)
 
 /* strain_to_stress: CPP_7-2-constitutive.cpp:13-321.  Soil models restated:
  * elastic (matype%10 = 0, 6), subloading Cam-clay (1), Drucker-Prager (2,
- * with DPModel_check), Bui DP (5, with DPModel_check), viscous-elastic (7) and
- * Mohr-Coulomb (9). */
+ * with DPModel_check), unsaturated Cam-clay (3), anisotropic Cam-clay (4, an
+ * empty model), Bui DP (5, with DPModel_check), viscous-elastic (7),
+ * fractional-order MCC (8) and Mohr-Coulomb (9), each inside the TSSMP
+ * transformation when flts >= 1. */
 static int strain_to_stress(orc_ctx* c)
 {
     const sphgpu_params* P = &c->P;
@@ -974,31 +1276,46 @@ static int strain_to_stress(orc_ctx* c)
             d[3] = de[3]; d[4] = de[4]; d[5] = de[5];
             for (int a = 0; a < 6; a++) s[a] = (a < 3) ? -c->pre[i] - viscos1 * d[a] : -viscos1 * d[a];
         } else if (ti == 2) {
-            double dept[6][6], adps[6] = {0, 0, 0, 0, 0, 0}, erfs[6] = {0, 0, 0, 0, 0, 0};
+            double dept[6][6], adps[6] = {0, 0, 0, 0, 0, 0}, erfs[6] = {0, 0, 0, 0, 0, 0}, cijkl[6][6];
             double dl, dm, sm;
             double* ds = &c->dsig[i * 6];
             int mt = c->matype[i] % 10;
-            if (P->flts >= 1) return SPHGPU_E_UNSUPPORTED;
+            const int m = c->matype[i];
             /* matype 30-49 and >= 60 match no branch of the reference's dispatch */
-            if ((c->matype[i] >= 30 && c->matype[i] < 50) || c->matype[i] >= 60) return SPHGPU_E_UNSUPPORTED;
+            if ((m >= 30 && m < 50) || m >= 60) return SPHGPU_E_UNSUPPORTED;
+            for (int a = 0; a < 6; a++)
+                for (int b = 0; b < 6; b++) { dept[a][b] = 0.0; cijkl[a][b] = 0.0; }
+            /* transformed stress of the SMP criterion, step 1 (:99-101) */
+            if (P->flts >= 1) tssmp_before(c, i, P->alphats);
             if (c->l < P->inip || mt == 0 || mt == 6) {
                 elastic_d(dept, s, &c->so[i], &dl, &dm, &sm);
             } else if (mt == 1) {
                 sub_camclay(dept, s, de, &c->so[i], adps);
             } else if (mt == 2 || mt == 5) {
                 dpmodel(dept, s, de, &c->so[i], adps, mt == 5);
+            } else if (mt == 3) {
+                sub_camunsatu(dept, erfs, s, de, c->satu[i], c->dsatu[i], &c->so[i], adps);
+            } else if (mt == 4) {
+                /* sub_camanisotropy (CPP_8-2-consfactor-amcc.cpp:17-99): its body is
+                 * commented out, so dept stays zero */
+            } else if (mt == 8) {
+                fractional_mcc(dept, cijkl, s, de, c->e[i], &c->so[i]);
             } else if (mt == 9) {
                 mc_model(dept, s, de, &c->so[i], adps);
-            } else if (mt == 7) {
-                visco_elastic(ds, s, de, &c->so[i]);
             } else {
-                return SPHGPU_E_UNSUPPORTED;
+                visco_elastic(ds, s, de, &c->so[i]);
             }
             if (c->l < P->inip || mt != 7)
                 for (int a = 0; a < 6; a++)
                     for (int b = 0; b < 6; b++) ds[a] += dept[a][b] * de[b];
             if (!(c->l < P->inip) && (mt == 2 || mt == 5)) dp_check(s, ds, &c->so[i], dt);
             jaumann(ds, s, &c->weps[i * 9]);
+            /* fractional_plastic for matype 8, 18, 28 (:255-258).  In elastic steps
+             * (l < inip) the reference reads cijkl uninitialised there; only the
+             * output-only adps depends on it, and a zero compliance is taken. */
+            if (m == 8 || m == 18 || m == 28) fractional_plastic(ds, de, adps, cijkl);
+            /* step 2: the rate back to the real stress; sig restored (:261-262) */
+            if (P->flts >= 1) tssmp_after(c, i, ds);
             for (int a = 0; a < 6; a++) {
                 c->adps[i * 6 + a] = c->adps[i * 6 + a] + adps[a] * dt;
                 ep[a] = ep[a] + de[a] * dt;
@@ -2475,7 +2792,7 @@ static int check_supported(const sphgpu_params* P)
 {
     if (!(P->flbndy >= 1 && P->flbndy <= 5) && P->flbndy != 13 && P->flbndy != 14) return SPHGPU_E_UNSUPPORTED;
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
-    if (P->flv != 0 || P->flts != 0 || P->flagum != 0) return SPHGPU_E_UNSUPPORTED;
+    if (P->flv != 0) return SPHGPU_E_UNSUPPORTED;
     if (P->fli < 0 || P->fli > 3 || P->ss_type < 0 || P->ss_type > 3) return SPHGPU_E_UNSUPPORTED;
     return 0;
 }
@@ -2496,6 +2813,7 @@ int orc_step(orc_ctx* c, int nsteps)
         density(c);
         strain_noreg(c);
         if (c->l % P->step_regu == 0) regularise(c, c->eps);
+        if (P->flagum == 1) saturation(c);
         if (P->fli == 1) cal_permeability(c);
         eos(c);
         err = strain_to_stress(c);

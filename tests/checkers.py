@@ -29,7 +29,7 @@ ORC_JACOBI, ORC_INPLACE = 0, 1
 ORC_POW_LIBM, ORC_POW_CR = 0, 1
 
 ORACLE_FIELDS = dict(FIELDS)
-ORACLE_FIELDS.update({"divx": 9, "deps": 6, "dsig": 6, "weps": 9, "dsatu": 1, "suct": 1,
+ORACLE_FIELDS.update({"divx": 9, "deps": 6, "dsig": 6, "weps": 9,
                       "cd": 1, "beta": 9, "beta_ts": 9, "vel_bndy": 3, "vb_water": 3, "vb_soil": 3,
                       "vb_air": 3, "vb_struct": 3})
 
@@ -202,7 +202,7 @@ class Reference:
 
 
 STATE_FIELDS = ("x", "xp", "vx", "vxp", "ax", "axp", "ux", "strep", "interf", "interfss", "rho",
-                "rhop", "mass", "hl", "pre", "prep", "e", "eps", "sig", "adps", "satu", "cop",
+                "rhop", "mass", "hl", "pre", "prep", "e", "eps", "sig", "adps", "tssig", "tsqc", "satu", "dsatu", "suct", "cop",
                 "vsig", "veps", "divq", "divr", "meps", "prew", "prea", "porosity", "poro_cop",
                 "type", "matype", "permtype", "etype")
 

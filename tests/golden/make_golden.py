@@ -74,7 +74,8 @@ MCC = dict(ramda=0.2, kapa=0.04, zmf=1.2, eps0=0.9, poi=0.3, sme0=50.0e3, ann=1.
 def _column_model(matype, **record):
     """The soil column with its soil switched to another constitutive model:
     subloading Cam-clay (1; lambda 0.2, kappa 0.04, M 1.2, e0 0.9, p0 50 kPa,
-    E from kappa and p), viscous-elastic (7) or Mohr-Coulomb (9)."""
+    E from kappa and p), anisotropic Cam-clay (4), viscous-elastic (7),
+    fractional-order Cam-clay (8) or Mohr-Coulomb (9)."""
     return lambda: scenes.set_soil_model(scenes.soil_column_3d(dx=0.1, steps=200), matype, **record)
 
 
@@ -121,6 +122,41 @@ def _footing(ndim, dx, ss_type, coupled=False):
     return make
 
 
+# unsaturated Cam-clay (3): saturation between 0.95 and 1 with the pore
+# water below z = 0.15 only, so that the saturation pass leaves the upper
+# soil at the residual saturation; beta = 2 keeps pow() of the hardening term
+# real when roue turns negative
+UMCC = dict(poi=0.3, dens=2650.0, eps0=0.9, zmf=1.2, sme0=50.0e3, fs=1.0, ramda=0.2, kapa=0.04, damp1=0.0,
+            damp2=0.0, cop=1.0e-4, ann=1.0, bnn=0.5, beta=2.0, epss=0.9, epsr=0.905, sitas=1.0, sitar=0.95,
+            sd=20.0, sw=10.0, kse=0.0, c1=0.05, c2=0.1, c3=0.0, e=0.0, ds=1.0e-3)
+# anisotropic Cam-clay (4): its model body is empty in the reference
+AMCC = dict(poi=0.3, dens=2650.0, eps0=0.9, zmf=1.2, sme0=50.0e3, fs=1.0, ramda=0.2, kapa=0.04, damp1=0.0,
+            damp2=0.0, cop=1.0e-4, mzm=1.0, azm=0.5, r0=0.8, bl=0.95, bz=1.0, zet=0.1, e=1.0e7, ds=1.0e-3)
+# fractional-order Cam-clay (8): a sand-like parameter set (G0 125, M 1.25,
+# lambda 0.019, e_Gamma 0.934, xi 0.7, alpha 1.2, beta 1, h1 1.8, h2 1.1)
+FOCC = dict(dens=2650.0, c=0.75, eps0=0.8, cop=1.0e-4, sme0=50.0e3, g0=125.0, poi=0.25, zmf=1.25, ramda=0.019,
+            etao=0.934, zet=0.7, ann=1.2, bnn=1.0, damp1=1.8, damp2=1.1, ds=1.0e-3)
+
+
+def _column_unsat():
+    """The soil column with unsaturated Cam-clay soil and the saturation pass
+    (flagum 1); pore water only below z = 0.15."""
+    sc = scenes.set_soil_model(scenes.soil_column_3d(dx=0.1, steps=200), 3, **UMCC)
+    return scenes.keep(sc, ~((sc.ptype == 1) & (sc.xp[:, 2] > 0.15)))
+
+
+def _column_tssmp():
+    """The Drucker-Prager soil column inside the TSSMP stress transformation
+    (flts 1, alpha 0.5, damping coefficient 0.05).  Over more steps, or at
+    finer spacing, the reference's TSSMP around Drucker-Prager diverges (NaN
+    stresses after about 15 steps at dx = 0.05); around Cam-clay, the pairing
+    the transformation is meant for, it stays bounded."""
+    sc = scenes.soil_column_3d(dx=0.1, steps=200)
+    sc.flags["flts"] = 1
+    sc.problem["ts"] = (0.5, 0.05)
+    return sc
+
+
 CASES = {
     # name: (scene factory, steps)
     "dam_break_2d_dx0.04": (lambda: scenes.dam_break_2d(dx=0.04, steps=200), 25),
@@ -148,6 +184,10 @@ CASES = {
     "footing_3d_penalty": (_footing(3, 0.1, 3), 12),
     "footing_2d_penalty_coupled": (_footing(2, 0.04, 3, True), 12),
     "footing_3d_deformable_coupled": (_footing(3, 0.1, 2, True), 12),
+    "soil_column_3d_dx0.1_unsat": (_column_unsat, 20),
+    "soil_column_3d_dx0.1_amcc": (_column_model(4, **AMCC), 20),
+    "soil_column_3d_dx0.1_focc": (_column_model(8, **FOCC), 20),
+    "soil_column_3d_dx0.1_tssmp": (_column_tssmp, 20),
 }
 
 

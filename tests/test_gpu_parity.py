@@ -12,6 +12,7 @@ lists are compared exactly: same neighbours in the same order.
 import numpy as np
 import pytest
 
+import make_golden
 import scenes
 import sphgpu
 from checkers import ORC_JACOBI, ORC_POW_CR, ORC_POW_LIBM, STATE_FIELDS, Oracle
@@ -263,6 +264,20 @@ MCC = dict(ramda=0.2, kapa=0.04, zmf=1.2, eps0=0.9, poi=0.3, sme0=50.0e3, ann=1.
 # Mohr-Coulomb and viscous-elastic use no transcendental function on the
 # device and are compared bit for bit.
 MCC_REL_TOL = 1e-12
+# unsaturated Cam-clay adds pow() to its hardening term and the saturation
+# pass tan / exp / log to the suction; fractional-order Cam-clay takes pow,
+# asin and sin, and inverts its 6x6 compliance: both held to a tolerance.
+# The anisotropic Cam-clay (an empty model in the reference) and the TSSMP
+# transformation around Drucker-Prager use none and are compared bit for bit.
+UMCC_REL_TOL = 1e-12
+FOCC_REL_TOL = 1e-10
+
+
+def _tssmp(sc, alpha=0.5):
+    """The scene inside the TSSMP stress transformation (flts 1)."""
+    sc.flags["flts"] = 1
+    sc.problem["ts"] = (alpha, 0.05)
+    return sc
 
 
 @pytest.mark.parametrize("label,factory,steps,tol", [
@@ -272,10 +287,18 @@ MCC_REL_TOL = 1e-12
                                                    c=0.0, fai=30.0, e=1.0e7), 20, 0.0),
     ("visco_elastic", lambda: scenes.set_soil_model(scenes.soil_column_3d(dx=0.05, steps=100), 7,
                                                     c=1.0e5, e=1.0e7), 20, 0.0),
+    ("unsat_camclay", make_golden.CASES["soil_column_3d_dx0.1_unsat"][0], 20, UMCC_REL_TOL),
+    ("aniso_camclay", make_golden.CASES["soil_column_3d_dx0.1_amcc"][0], 20, 0.0),
+    ("fractional_camclay", make_golden.CASES["soil_column_3d_dx0.1_focc"][0], 20, FOCC_REL_TOL),
+    ("tssmp_dp", make_golden.CASES["soil_column_3d_dx0.1_tssmp"][0], 20, 0.0),
+    ("tssmp_camclay", lambda: _tssmp(scenes.set_soil_model(scenes.soil_column_3d(dx=0.05, steps=100), 1, **MCC)),
+     40, MCC_REL_TOL),
 ])
 def test_soil_models(label, factory, steps, tol):
-    """Subloading Cam-clay, Mohr-Coulomb and viscous-elastic soil against the
-    oracle (whose same runs are bit-identical to the reference)."""
+    """Subloading, unsaturated (with the saturation pass), anisotropic and
+    fractional-order Cam-clay, Mohr-Coulomb, viscous-elastic soil, and the
+    TSSMP transformation, against the oracle (whose same runs are
+    bit-identical to the reference)."""
     _, eng, orc = _engine_and_oracle(factory())
     eng.step(steps)
     assert orc.step(steps) == 0

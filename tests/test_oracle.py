@@ -23,7 +23,9 @@ CASES = ["dam_break_2d_dx0.04", "soil_column_3d_dx0.1", "soil_column_3d_dx0.1_kg
          "footing_3d_penalty", "dam_break_2d_dx0.04_no_slip", "dam_break_2d_dx0.04_free_slip_vsd",
          "soil_column_3d_dx0.1_free_slip", "soil_column_3d_dx0.1_no_slip_vsd",
          "dam_break_2d_dx0.04_free_solid", "soil_column_3d_dx0.1_free_solid",
-         "footing_2d_penalty_coupled", "footing_3d_deformable_coupled"]
+         "footing_2d_penalty_coupled", "footing_3d_deformable_coupled",
+         "soil_column_3d_dx0.1_unsat", "soil_column_3d_dx0.1_amcc", "soil_column_3d_dx0.1_focc",
+         "soil_column_3d_dx0.1_tssmp"]
 
 
 def _golden(name):
