@@ -1144,8 +1144,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
     const bool fluid = (ti == 1 || ti == 3);
     const bool solid = (ti == 2 || ti == 4);
     const bool moving = (ti >= 1 && ti <= 4);
-    Sum<real> tb[3][3];   // wall stress
-    Sum<real> tav[3], tin[3], tdm[3], tu[3];
+    Sum<real> tav[3], tin[3], tdm[3];
     const bool damping = (*d.s.step <= d.p.inip) && solid;
     const bool art = ART && ti == 2;   // artificial stress (art_stre_coe > 0)
     const real cdi = damping ? (real)d.s.cd[i] : real(0);
@@ -1155,7 +1154,6 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
     if (ti == 2) { ca = (real)d.s.s_vpu[i]; aa = (real)d.p.av[1][0]; bb = (real)d.p.av[1][1]; }
     if (ti == 3) { ca = (real)d.s.f_vpu[i]; aa = (real)d.p.av[2][0]; bb = (real)d.p.av[2][1]; }
     // wall-stress operand of particle i (:668-700) and its own half
-    real ab[6] = {0, 0, 0, 0, 0, 0}, abr[6] = {0, 0, 0, 0, 0, 0};
     const double satu_i = d.s.satu[i];
     // flbndy 3/4/13/14: boundary_stress_effect_tran (CPP_9-4:725-846) takes the
     // wall's stress for i's phase, and a structure particle's own stress
@@ -1164,34 +1162,18 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
     // boundary_effect_free_struct (CPP_9-4:900-990) for the other flbndy
     // values: a fluid's mirrored stress has its shear components negated
     const bool free_struct = !(tran || d.p.flbndy == 1 || d.p.flbndy == 2);
-    if (moving) {
-        double si[6];
-        for (int k = 0; k < 6; k++) si[k] = d.s.sig_next[k * N + i];
-        double abd[6];
-        if (fluid || (tran && ti == 4)) {
-            for (int k = 0; k < 6; k++) abd[k] = si[k];
-        } else {
-            const double prew_i = d.s.prew[i], prea_i = d.s.prea[i];
-            abd[0] = si[0] - satu_i * prew_i + (1 - satu_i) * prea_i;
-            abd[1] = si[1] - satu_i * prew_i + (1 - satu_i) * prea_i;
-            abd[2] = si[2] - satu_i * prew_i + (1 - satu_i) * prea_i;
-            abd[3] = si[3]; abd[4] = si[4]; abd[5] = si[5];
-        }
-        for (int k = 0; k < 6; k++) {
-            ab[k] = (real)abd[k];
-            abr[k] = (real)(abd[k] / ri / ri);
-        }
-    }
+    // the common sums (artificial viscosity, soil-water drag, geostatic
+    // damping), and whether a wall particle is in the list
+    bool any_wall = false;
     NbrIter it(d, i, nn);
     for (int q = 0; q < nn; q++) {
         int j, tj;
         it.next(j, tj);
         const bool av_pair = (ti == tj && ti != 7);
-        const bool b_pair = moving && tj == 0;
         const bool in_pair = d.p.fli >= 1 && ti != tj;
         const bool dm_pair = damping && tj == ti;
-        const bool as_pair = art && tj == 2;
-        if (!(av_pair || b_pair || in_pair || dm_pair)) continue;
+        any_wall = any_wall || tj == 0;
+        if (!(av_pair || in_pair || dm_pair)) continue;
         const Pos pj = load_pos(d.s.xh, j);
         real w[4];
         load_w(d, q, i, w);
@@ -1215,25 +1197,6 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
             } else
                 paix = 0;
             for (int k = 0; k < nd; k++) tav[k].add(mj * paix * w[k]);
-        }
-        if (b_pair) {
-            real abj[6];
-            if (free_struct && fluid)
-                for (int k = 0; k < 6; k++) abj[k] = ((k < 3) ? ab[k] : -ab[k]) / rj / rj;
-            else if (tran)
-                for (int k = 0; k < 6; k++)
-                    abj[k] = (real)(d.s.sb[(size_t)((ti - 1) * 6 + k) * N + j] / d.s.rho[j] / d.s.rho[j]);
-            else
-                for (int k = 0; k < 6; k++) abj[k] = ab[k] / rj / rj;
-            tb[0][0].add(mj * (abj[0] + abr[0]) * w[0]);
-            tb[0][1].add(mj * (abj[3] + abr[3]) * w[1]);
-            tb[0][2].add(mj * (abj[5] + abr[5]) * w[2]);
-            tb[1][0].add(mj * (abj[3] + abr[3]) * w[0]);
-            tb[1][1].add(mj * (abj[1] + abr[1]) * w[1]);
-            tb[1][2].add(mj * (abj[4] + abr[4]) * w[2]);
-            tb[2][0].add(mj * (abj[5] + abr[5]) * w[0]);
-            tb[2][1].add(mj * (abj[4] + abr[4]) * w[1]);
-            tb[2][2].add(mj * (abj[2] + abr[2]) * w[2]);
         }
         if (in_pair) {
             real inprod = 0, dvx[3];
@@ -1277,7 +1240,69 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
         if (dm_pair)
             for (int k = 0; k < nd; k++)
                 tdm[k].add(mj / rj * cdi * (real)(vi[k] - d.s.vxp[k * N + j]) * w[3]);
-        if (as_pair) {
+    }
+    // the wall stress of moving particles with a wall in their list, in a
+    // loop of its own so that its nine sums do not hold registers in the
+    // common loop (each sum still runs over the list in order)
+    Sum<real> tb[3][3];
+    if (moving && any_wall) {
+        real ab[6], abr[6];
+        double si[6];
+        for (int k = 0; k < 6; k++) si[k] = d.s.sig_next[k * N + i];
+        double abd[6];
+        if (fluid || (tran && ti == 4)) {
+            for (int k = 0; k < 6; k++) abd[k] = si[k];
+        } else {
+            const double prew_i = d.s.prew[i], prea_i = d.s.prea[i];
+            abd[0] = si[0] - satu_i * prew_i + (1 - satu_i) * prea_i;
+            abd[1] = si[1] - satu_i * prew_i + (1 - satu_i) * prea_i;
+            abd[2] = si[2] - satu_i * prew_i + (1 - satu_i) * prea_i;
+            abd[3] = si[3]; abd[4] = si[4]; abd[5] = si[5];
+        }
+        for (int k = 0; k < 6; k++) {
+            ab[k] = (real)abd[k];
+            abr[k] = (real)(abd[k] / ri / ri);
+        }
+        NbrIter itw(d, i, nn);
+        for (int q = 0; q < nn; q++) {
+            int j, tj;
+            itw.next(j, tj);
+            if (tj != 0) continue;
+            real w[4];
+            load_w(d, q, i, w);
+            const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
+            real abj[6];
+            if (free_struct && fluid)
+                for (int k = 0; k < 6; k++) abj[k] = ((k < 3) ? ab[k] : -ab[k]) / rj / rj;
+            else if (tran)
+                for (int k = 0; k < 6; k++)
+                    abj[k] = (real)(d.s.sb[(size_t)((ti - 1) * 6 + k) * N + j] / d.s.rho[j] / d.s.rho[j]);
+            else
+                for (int k = 0; k < 6; k++) abj[k] = ab[k] / rj / rj;
+            tb[0][0].add(mj * (abj[0] + abr[0]) * w[0]);
+            tb[0][1].add(mj * (abj[3] + abr[3]) * w[1]);
+            tb[0][2].add(mj * (abj[5] + abr[5]) * w[2]);
+            tb[1][0].add(mj * (abj[3] + abr[3]) * w[0]);
+            tb[1][1].add(mj * (abj[1] + abr[1]) * w[1]);
+            tb[1][2].add(mj * (abj[4] + abr[4]) * w[2]);
+            tb[2][0].add(mj * (abj[5] + abr[5]) * w[0]);
+            tb[2][1].add(mj * (abj[4] + abr[4]) * w[1]);
+            tb[2][2].add(mj * (abj[2] + abr[2]) * w[2]);
+        }
+    }
+    // the artificial-stress pair sum (ART), likewise in a loop of its own
+    Sum<real> tu[3];
+    if (art) {
+        NbrIter ita(d, i, nn);
+        for (int q = 0; q < nn; q++) {
+            int j, tj;
+            ita.next(j, tj);
+            if (tj != 2) continue;
+            const Pos pj = load_pos(d.s.xh, j);
+            real w[4];
+            load_w(d, q, i, w);
+            const real mj = (real)d.s.mass[j];
+            const double xj[3] = {pj.x, pj.y, pj.z};
             // artificial_stress_2d/_3d pair sum (CPP_9-5-artificialstress.cpp:
             // 100-140, 248-290): f_ij = (W(q) / W(dr))^2.55 of the cubic
             // spline, m_j f_ij (R_i + R_j) grad W_ij
