@@ -297,17 +297,19 @@ __device__ __forceinline__ double wall_vel(const Dev& d, int ti, int j, const do
 // The stored pair record of slot s of particle i: kernel gradient w[0..2] and
 // value w[3], as partisearching stores Par_Cell::wij (CPP_3-NNPS.cpp:339-345),
 // corrected in place by kernel_gradient_correction when flknl is 3 or 4.
-__device__ __forceinline__ void load_w(const Dev& d, int s, int i, double w[4])
+__device__ __forceinline__ void load_w_raw(const double* nbw, int N, int s, int i, double w[4])
 {
-    const double2* p = reinterpret_cast<const double2*>(d.s.nbw) + 2 * ((size_t)s * d.p.N + i);
+    const double2* p = reinterpret_cast<const double2*>(nbw) + 2 * ((size_t)s * N + i);
     const double2 a = p[0], b = p[1];
     w[0] = a.x; w[1] = a.y; w[2] = b.x; w[3] = b.y;
 }
-__device__ __forceinline__ void load_w(const Dev& d, int s, int i, float w[4])
+__device__ __forceinline__ void load_w_raw(const double* nbw, int N, int s, int i, float w[4])
 {
-    const float4 f = reinterpret_cast<const float4*>(d.s.nbw)[(size_t)s * d.p.N + i];
+    const float4 f = reinterpret_cast<const float4*>(nbw)[(size_t)s * N + i];
     w[0] = f.x; w[1] = f.y; w[2] = f.z; w[3] = f.w;
 }
+__device__ __forceinline__ void load_w(const Dev& d, int s, int i, double w[4]) { load_w_raw(d.s.nbw, d.p.N, s, i, w); }
+__device__ __forceinline__ void load_w(const Dev& d, int s, int i, float w[4]) { load_w_raw(d.s.nbw, d.p.N, s, i, w); }
 __device__ __forceinline__ void store_w(const Dev& d, int s, int i, const double w[4])
 {
     double2* p = reinterpret_cast<double2*>(d.s.nbw) + 2 * ((size_t)s * d.p.N + i);

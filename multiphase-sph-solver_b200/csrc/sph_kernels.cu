@@ -232,26 +232,57 @@ __device__ __forceinline__ bool nnps_in_fp64(const double xi[3], double hi, cons
     return sqrt(d2) <= T;
 }
 
-// FP32 prefilter verdict of one candidate: 1 inside, 0 outside, -1 undecided
-// (within the rounding margin of the radius)
+// FP32 prefilter of the candidates of one particle: its (x - xmin, y - ymin,
+// z - zmin, h) in FP32, the margin terms, and the decision bounds lo / hi of a
+// candidate with the same h (the usual case), so that such a candidate costs
+// its squared distance and two comparisons.  The squared distance is summed
+// with fused multiply-adds: one rounding per term instead of two, inside the
+// margin derived for separate roundings.
+struct Prefilter {
+    float fx, fy, fz, fh, ce, ct, lo0, hi0;
+};
+
 template <int ND>
-__device__ __forceinline__ int nnps_prefilter(float fx, float fy, float fz, float fh, float ce, float ct, float4 fj)
+__device__ __forceinline__ void prefilter_bounds(const Prefilter& P, float hj, float* lo, float* hi)
 {
     constexpr float U = 5.9604645e-8f;     // 2^-24
-    float t = fx - fj.x;
+    const float Tf = P.fh + hj, T2f = Tf * Tf;
+    const float e = P.ce + 4.4f * U * Tf;
+    const float M = ND * e * (4.f * Tf + e) + P.ct * T2f;
+    *lo = T2f - M;
+    *hi = T2f + M;
+}
+
+template <int ND>
+__device__ __forceinline__ Prefilter make_prefilter(float fx, float fy, float fz, float fh, float ce, float ct)
+{
+    Prefilter P{fx, fy, fz, fh, ce, ct, 0.f, 0.f};
+    prefilter_bounds<ND>(P, fh, &P.lo0, &P.hi0);
+    return P;
+}
+
+// verdict of one candidate: 1 inside, 0 outside, -1 undecided (within the
+// rounding margin of the radius).  A candidate beyond twice the radius is
+// outside; hi < 4 T^2, so the bounds test covers that case too.
+template <int ND>
+__device__ __forceinline__ int nnps_prefilter(const Prefilter& P, float4 fj)
+{
+    float t = P.fx - fj.x;
     float d2f = t * t;
-    t = fy - fj.y;
-    d2f = d2f + t * t;
+    t = P.fy - fj.y;
+    d2f = __fmaf_rn(t, t, d2f);
     if (ND == 3) {
-        t = fz - fj.z;
-        d2f = d2f + t * t;
+        t = P.fz - fj.z;
+        d2f = __fmaf_rn(t, t, d2f);
     }
-    const float Tf = fh + fj.w, T2f = Tf * Tf;
-    if (d2f > 4.f * T2f) return 0;
-    const float e = ce + 4.4f * U * Tf;
-    const float M = ND * e * (4.f * Tf + e) + ct * T2f;
-    if (d2f < T2f - M) return 1;
-    if (d2f > T2f + M) return 0;
+    float lo = P.lo0, hi = P.hi0;
+    if (fj.w != P.fh) {
+        const float Tf = P.fh + fj.w;
+        if (d2f > 4.f * (Tf * Tf)) return 0;
+        prefilter_bounds<ND>(P, fj.w, &lo, &hi);
+    }
+    if (d2f < lo) return 1;
+    if (d2f > hi) return 0;
     return -1;
 }
 
@@ -259,8 +290,7 @@ __device__ __forceinline__ int nnps_prefilter(float fx, float fy, float fz, floa
 // (used when the FP32 prefilter does not apply to the particle, or when its
 // provisional list below overflows); returns the neighbour count
 template <int ND>
-__device__ __forceinline__ int nnps_direct(const Dev& d, int i, int nc, const Pos& pi, bool fast, float fx, float fy,
-                                        float fz, float fh, float ce, float ct)
+__device__ __forceinline__ int nnps_direct(const Dev& d, int i, int nc, const Pos& pi, bool fast, const Prefilter& P)
 {
     const int N = d.p.N;
     constexpr int nst = (ND == 2) ? 9 : 27;
@@ -272,7 +302,7 @@ __device__ __forceinline__ int nnps_direct(const Dev& d, int i, int nc, const Po
         if (nl <= 0) continue;
         const int start = d.s.cstart[nl], end = d.s.cend[nl];
         for (int q = start; q <= end; q++) {
-            int v = fast ? nnps_prefilter<ND>(fx, fy, fz, fh, ce, ct, xsf[q]) : -1;
+            int v = fast ? nnps_prefilter<ND>(P, xsf[q]) : -1;
             if (v < 0) v = nnps_in_fp64<ND>(xi, pi.h, load_pos(d.s.xs, q)) ? 1 : 0;
             if (v) {
                 const int j = d.s.pid_sorted[q];
@@ -329,9 +359,9 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_nnps(Dev d)
         float Fi = fmaxf(fabsf(fx), fabsf(fy));
         if (ND == 3) Fi = fmaxf(Fi, fabsf(fz));
         const bool fast = fh > 64.f * U * Fi;
-        const float ce = 2.2f * U * Fi, ct = 32.f * U;
+        const Prefilter P = make_prefilter<ND>(fx, fy, fz, fh, 2.2f * U * Fi, 32.f * U);
         if (!fast) {
-            cnt = nnps_direct<ND>(d, i, nc, pi, false, fx, fy, fz, fh, ce, ct);
+            cnt = nnps_direct<ND>(d, i, nc, pi, false, P);
         } else {
             const float4* xsf = reinterpret_cast<const float4*>(d.s.xsf);
             int np = 0;   // provisional entries
@@ -340,7 +370,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_nnps(Dev d)
                 if (nl <= 0) continue;
                 const int start = d.s.cstart[nl], end = d.s.cend[nl];
                 for (int q = start; q <= end; q++) {
-                    const int v = nnps_prefilter<ND>(fx, fy, fz, fh, ce, ct, xsf[q]);
+                    const int v = nnps_prefilter<ND>(P, xsf[q]);
                     if (v != 0) {
                         if (np < SPH_NB_CAP) d.s.nbr[(size_t)np * N + i] = (v > 0) ? q : ~q;
                         np++;
@@ -348,7 +378,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_nnps(Dev d)
                 }
             }
             if (np > SPH_NB_CAP) {
-                cnt = nnps_direct<ND>(d, i, nc, pi, true, fx, fy, fz, fh, ce, ct);
+                cnt = nnps_direct<ND>(d, i, nc, pi, true, P);
             } else {
                 const double xi[3] = {pi.x, pi.y, pi.z};
                 for (int s = 0; s < np; s++) {
@@ -644,13 +674,6 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_strain(Dev d)
     }
 }
 
-// cal_permeability (CPP_7-2-constitutive.cpp:355-382), strain_to_stress
-// (:13-321), free_surface_check's correction (:482-504) and Stress_eigValue
-// (CPP_7-1-strain.cpp:283-332), per particle.  Also evaluates the particle's
-// own stress / rho^2 and pore-pressure / rho^2 terms the momentum pass uses.
-// PHASE 0 does all of it.  Where stress_regu can run (step_regu within the
-// run), PHASE 1 stops after the constitutive update (writing sig_next), the
-// smoothing pass runs, and PHASE 2 continues from the smoothed stresses.
 // saturation (flagum == 1, CPP_7-1-strain.cpp:222-281): each soil particle's
 // degree of saturation from the Shepard ratio of its water neighbours, its
 // change dsatu (a decrease is undone), the clamp to [sitar, sitas] and the
@@ -687,6 +710,13 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_saturation(Dev d)
     d.s.suct[i] = moisture_suction(satu, dsatu, sitas, sitar, d.s.s_ext + i, N);
 }
 
+// cal_permeability (CPP_7-2-constitutive.cpp:355-382), strain_to_stress
+// (:13-321), free_surface_check's correction (:482-504) and Stress_eigValue
+// (CPP_7-1-strain.cpp:283-332), per particle.  Also evaluates the particle's
+// own stress / rho^2 and pore-pressure / rho^2 terms the momentum pass uses.
+// PHASE 0 does all of it.  Where stress_regu can run (step_regu within the
+// run), PHASE 1 stops after the constitutive update (writing sig_next), the
+// smoothing pass runs, and PHASE 2 continues from the smoothed stresses.
 template <int ND, int PHASE>
 __global__ void __launch_bounds__(128, SPH_MINB_STRESS) k_stress(Dev d)
 {
@@ -1120,6 +1150,64 @@ __device__ __noinline__ double drag_beta(int form, double por, double ds, double
     return beta;
 }
 
+// The wall-stress sums of one moving particle (boundary_moving_stress_effect,
+// CPP_9-4-derivation_stress.cpp:631-721; boundary_stress_effect_tran,
+// :725-846; boundary_effect_free_struct, :900-990) over the wall particles of
+// its list, in list order: the rows (t_k0 + t_k1) + t_k2 that are added to the
+// acceleration.  Out of line, so that its nine sums and the particle's
+// stress operands hold registers only for particles next to a wall.
+template <int ND>
+__device__ __noinline__ void wall_stress_rows(int i, int N, int nn, int ti, bool fluid, bool tran, bool free_struct,
+                                              double ri, double satu_i, const int* nbr, const int* type,
+                                              const double* nbw, const double* mass, const double* rho,
+                                              const double* sb, const double* sig_next, const double* prew,
+                                              const double* prea, double rows[3])
+{
+    Sum<real> tb[3][3];
+    real ab[6], abr[6];
+    double si[6];
+    for (int k = 0; k < 6; k++) si[k] = sig_next[k * N + i];
+    double abd[6];
+    if (fluid || (tran && ti == 4)) {
+        for (int k = 0; k < 6; k++) abd[k] = si[k];
+    } else {
+        const double prew_i = prew[i], prea_i = prea[i];
+        abd[0] = si[0] - satu_i * prew_i + (1 - satu_i) * prea_i;
+        abd[1] = si[1] - satu_i * prew_i + (1 - satu_i) * prea_i;
+        abd[2] = si[2] - satu_i * prew_i + (1 - satu_i) * prea_i;
+        abd[3] = si[3]; abd[4] = si[4]; abd[5] = si[5];
+    }
+    for (int k = 0; k < 6; k++) {
+        ab[k] = (real)abd[k];
+        abr[k] = (real)(abd[k] / ri / ri);
+    }
+    for (int q = 0; q < nn; q++) {
+        const int j = nbr[(size_t)q * N + i];
+        if (type[j] != 0) continue;
+        real w[4];
+        load_w_raw(nbw, N, q, i, w);
+        const real mj = (real)mass[j], rj = (real)rho[j];
+        real abj[6];
+        if (free_struct && fluid)
+            for (int k = 0; k < 6; k++) abj[k] = ((k < 3) ? ab[k] : -ab[k]) / rj / rj;
+        else if (tran)
+            for (int k = 0; k < 6; k++)
+                abj[k] = (real)(sb[(size_t)((ti - 1) * 6 + k) * N + j] / rho[j] / rho[j]);
+        else
+            for (int k = 0; k < 6; k++) abj[k] = ab[k] / rj / rj;
+        tb[0][0].add(mj * (abj[0] + abr[0]) * w[0]);
+        tb[0][1].add(mj * (abj[3] + abr[3]) * w[1]);
+        tb[0][2].add(mj * (abj[5] + abr[5]) * w[2]);
+        tb[1][0].add(mj * (abj[3] + abr[3]) * w[0]);
+        tb[1][1].add(mj * (abj[1] + abr[1]) * w[1]);
+        tb[1][2].add(mj * (abj[4] + abr[4]) * w[2]);
+        tb[2][0].add(mj * (abj[5] + abr[5]) * w[0]);
+        tb[2][1].add(mj * (abj[4] + abr[4]) * w[1]);
+        tb[2][2].add(mj * (abj[2] + abr[2]) * w[2]);
+    }
+    for (int k = 0; k < 3; k++) rows[k] = tb[k][0].v() + tb[k][1].v() + tb[k][2].v();
+}
+
 // artificial_viscosity (CPP_9-3-artificialvis.cpp:12-99), the pair sum of
 // artificial_stress_2d/_3d (CPP_9-5-artificialstress.cpp, ART = 1),
 // boundary_moving_stress_effect (CPP_9-4-derivation_stress.cpp:631-721),
@@ -1128,8 +1216,9 @@ __device__ __noinline__ double drag_beta(int form, double por, double ds, double
 // over the neighbour list with one accumulator set per sum, combined with the
 // stress-divergence result of k_accel_a in the reference's call order.
 // Writes ax, interf, interfss and the updated velocity into vx_next (the
-// reference's vx before XSPH).
-template <int ND, int ART = 0>
+// reference's vx before XSPH).  DRAG = 1 carries the interact2/3 drag
+// coefficient (fli 2, 3), whose out-of-line call the Darcy form does without.
+template <int ND, int ART = 0, int DRAG = 0>
 __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
 {
     const int i = IDX, N = d.p.N;
@@ -1170,23 +1259,29 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
         int j, tj;
         it.next(j, tj);
         const bool av_pair = (ti == tj && ti != 7);
-        const bool in_pair = d.p.fli >= 1 && ti != tj;
+        // the soil-water (and soil-air) pairs interact1/2/3 add a term for;
+        // the reference visits every other pair of different types too, but
+        // adds nothing for them
+        const bool in_pair = d.p.fli >= 1 &&
+            ((ti == 2 && (tj == 1 || tj == 3)) || ((ti == 1 || ti == 3) && tj == 2));
         const bool dm_pair = damping && tj == ti;
         any_wall = any_wall || tj == 0;
-        if (!(av_pair || in_pair || dm_pair)) continue;
+        if (!(av_pair || in_pair)) continue;
         const Pos pj = load_pos(d.s.xh, j);
         real w[4];
         load_w(d, q, i, w);
         const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
         const double xj[3] = {pj.x, pj.y, pj.z};
+        // the relative position and velocity and their inner product, which
+        // artificial_viscosity and interact form alike (products commute)
+        real inprod = 0, dst = 0, dx[3], dvx[3];
+        for (int k = 0; k < nd; k++) {
+            dvx[k] = (real)(vi[k] - d.s.vxp[k * N + j]);
+            dx[k] = (real)(I.x[k] - xj[k]);
+            dst = dst + dx[k] * dx[k];
+            inprod = inprod + dvx[k] * dx[k];
+        }
         if (av_pair) {
-            real inprod = 0, dst = 0, dx[3];
-            for (int k = 0; k < nd; k++) {
-                const real dvx = (real)(vi[k] - d.s.vxp[k * N + j]);
-                dx[k] = (real)(I.x[k] - xj[k]);
-                dst = dst + dx[k] * dx[k];
-                inprod = inprod + dvx * dx[k];
-            }
             const real hl = ((real)pj.h + I.h) * real(0.5);
             const real rou = (rj + riR) * real(0.5);
             real paix;
@@ -1197,99 +1292,47 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
             } else
                 paix = 0;
             for (int k = 0; k < nd; k++) tav[k].add(mj * paix * w[k]);
-        }
-        if (in_pair) {
-            real inprod = 0, dvx[3];
-            for (int k = 0; k < nd; k++) {
-                const real dxk = (real)(I.x[k] - xj[k]);
-                dvx[k] = (real)(vi[k] - d.s.vxp[k * N + j]);
-                inprod = inprod + dxk * dvx[k];
-            }
-            if (inprod < 0) {
-                const real w3 = w[3], ga = (real)d.p.g_acc;
-                if (d.p.fli > 1 && ((ti == 2 && tj == 1) || (ti == 1 && tj == 2))) {
-                    // interact2/3 soil-water drag, m_j / rho_j W beta (v_i - v_j)
-                    double mv = 0.0;
-                    for (int k = 0; k < nd; k++) mv = mv + (double)dvx[k] * (double)dvx[k];
-                    mv = sqrt(mv);
-                    const int so = (ti == 2) ? i : j, wa = (ti == 2) ? j : i;
-                    const real beta = (real)drag_beta(d.p.fli, d.s.porosity[so], d.s.s_ds[so], d.s.f_dens[wa],
-                                                      d.s.f_vis[wa], mv, (ti == 2) ? d.s.rho[j] : ri);
-                    for (int k = 0; k < nd; k++) tin[k].add(mj / rj * w3 * beta * dvx[k]);
-                } else if (ti == 2 && tj == 1) {
-                    const real sa = (real)satu_i, po = (real)d.s.porosity[i], cp = (real)d.s.cop[i],
-                               fd = (real)d.s.f_dens[j];
-                    for (int k = 0; k < nd; k++)
-                        tin[k].add(sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3);
-                } else if (ti == 1 && tj == 2) {
-                    const real sa = (real)d.s.satu[j], po = (real)d.s.porosity[j], cp = (real)d.s.cop[j],
-                               fd = (real)d.s.f_dens[i];
-                    for (int k = 0; k < nd; k++)
-                        tin[k].add(sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3);
-                } else if (ti == 2 && tj == 3) {
-                    const real sa = (real)satu_i, po = (real)d.s.porosity[i], fd = (real)d.s.f_dens[j];
-                    for (int k = 0; k < nd; k++)
-                        tin[k].add((1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3);
-                } else if (ti == 3 && tj == 2) {
-                    const real sa = (real)d.s.satu[j], po = (real)d.s.porosity[j], fd = (real)d.s.f_dens[i];
-                    for (int k = 0; k < nd; k++)
-                        tin[k].add((1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3);
-                }
+            if (dm_pair)
+                for (int k = 0; k < nd; k++) tdm[k].add(mj / rj * cdi * dvx[k] * w[3]);
+        } else if (inprod < 0) {
+            const real w3 = w[3], ga = (real)d.p.g_acc;
+            if (DRAG && d.p.fli > 1 && ((ti == 2 && tj == 1) || (ti == 1 && tj == 2))) {
+                // interact2/3 soil-water drag, m_j / rho_j W beta (v_i - v_j)
+                double mv = 0.0;
+                for (int k = 0; k < nd; k++) mv = mv + (double)dvx[k] * (double)dvx[k];
+                mv = sqrt(mv);
+                const int so = (ti == 2) ? i : j, wa = (ti == 2) ? j : i;
+                const real beta = (real)drag_beta(d.p.fli, d.s.porosity[so], d.s.s_ds[so], d.s.f_dens[wa],
+                                                  d.s.f_vis[wa], mv, (ti == 2) ? d.s.rho[j] : ri);
+                for (int k = 0; k < nd; k++) tin[k].add(mj / rj * w3 * beta * dvx[k]);
+            } else if (ti == 2 && tj == 1) {
+                const real sa = (real)satu_i, po = (real)d.s.porosity[i], cp = (real)d.s.cop[i],
+                           fd = (real)d.s.f_dens[j];
+                for (int k = 0; k < nd; k++)
+                    tin[k].add(sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3);
+            } else if (ti == 1 && tj == 2) {
+                const real sa = (real)d.s.satu[j], po = (real)d.s.porosity[j], cp = (real)d.s.cop[j],
+                           fd = (real)d.s.f_dens[i];
+                for (int k = 0; k < nd; k++)
+                    tin[k].add(sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3);
+            } else if (ti == 2 && tj == 3) {
+                const real sa = (real)satu_i, po = (real)d.s.porosity[i], fd = (real)d.s.f_dens[j];
+                for (int k = 0; k < nd; k++)
+                    tin[k].add((1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3);
+            } else if (ti == 3 && tj == 2) {
+                const real sa = (real)d.s.satu[j], po = (real)d.s.porosity[j], fd = (real)d.s.f_dens[i];
+                for (int k = 0; k < nd; k++)
+                    tin[k].add((1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3);
             }
         }
-        if (dm_pair)
-            for (int k = 0; k < nd; k++)
-                tdm[k].add(mj / rj * cdi * (real)(vi[k] - d.s.vxp[k * N + j]) * w[3]);
     }
-    // the wall stress of moving particles with a wall in their list, in a
-    // loop of its own so that its nine sums do not hold registers in the
-    // common loop (each sum still runs over the list in order)
-    Sum<real> tb[3][3];
-    if (moving && any_wall) {
-        real ab[6], abr[6];
-        double si[6];
-        for (int k = 0; k < 6; k++) si[k] = d.s.sig_next[k * N + i];
-        double abd[6];
-        if (fluid || (tran && ti == 4)) {
-            for (int k = 0; k < 6; k++) abd[k] = si[k];
-        } else {
-            const double prew_i = d.s.prew[i], prea_i = d.s.prea[i];
-            abd[0] = si[0] - satu_i * prew_i + (1 - satu_i) * prea_i;
-            abd[1] = si[1] - satu_i * prew_i + (1 - satu_i) * prea_i;
-            abd[2] = si[2] - satu_i * prew_i + (1 - satu_i) * prea_i;
-            abd[3] = si[3]; abd[4] = si[4]; abd[5] = si[5];
-        }
-        for (int k = 0; k < 6; k++) {
-            ab[k] = (real)abd[k];
-            abr[k] = (real)(abd[k] / ri / ri);
-        }
-        NbrIter itw(d, i, nn);
-        for (int q = 0; q < nn; q++) {
-            int j, tj;
-            itw.next(j, tj);
-            if (tj != 0) continue;
-            real w[4];
-            load_w(d, q, i, w);
-            const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
-            real abj[6];
-            if (free_struct && fluid)
-                for (int k = 0; k < 6; k++) abj[k] = ((k < 3) ? ab[k] : -ab[k]) / rj / rj;
-            else if (tran)
-                for (int k = 0; k < 6; k++)
-                    abj[k] = (real)(d.s.sb[(size_t)((ti - 1) * 6 + k) * N + j] / d.s.rho[j] / d.s.rho[j]);
-            else
-                for (int k = 0; k < 6; k++) abj[k] = ab[k] / rj / rj;
-            tb[0][0].add(mj * (abj[0] + abr[0]) * w[0]);
-            tb[0][1].add(mj * (abj[3] + abr[3]) * w[1]);
-            tb[0][2].add(mj * (abj[5] + abr[5]) * w[2]);
-            tb[1][0].add(mj * (abj[3] + abr[3]) * w[0]);
-            tb[1][1].add(mj * (abj[1] + abr[1]) * w[1]);
-            tb[1][2].add(mj * (abj[4] + abr[4]) * w[2]);
-            tb[2][0].add(mj * (abj[5] + abr[5]) * w[0]);
-            tb[2][1].add(mj * (abj[4] + abr[4]) * w[1]);
-            tb[2][2].add(mj * (abj[2] + abr[2]) * w[2]);
-        }
-    }
+    // the wall stress of moving particles with a wall in their list, out of
+    // line (its nine sums take registers only there); each sum still runs
+    // over the list in order
+    double tbrow[3] = {0.0, 0.0, 0.0};
+    if (moving && any_wall)
+        wall_stress_rows<ND>(i, N, nn, ti, fluid, tran, free_struct, ri, satu_i, d.s.nbr, d.s.type, d.s.nbw,
+                             d.s.mass, d.s.rho, d.s.sb, d.s.sig_next, d.s.prew, d.s.prea, tbrow);
     // the artificial-stress pair sum (ART), likewise in a loop of its own
     Sum<real> tu[3];
     if (art) {
@@ -1336,11 +1379,8 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
         for (int k = 0; k < nd; k++) ax[k] = ax[k] - tav[k].v();
     if (art)
         for (int k = 0; k < nd; k++) ax[k] = ax[k] + tu[k].v();
-    if (moving) {
-        ax[0] += tb[0][0].v() + tb[0][1].v() + tb[0][2].v();
-        ax[1] += tb[1][0].v() + tb[1][1].v() + tb[1][2].v();
-        ax[2] += tb[2][0].v() + tb[2][1].v() + tb[2][2].v();
-    }
+    if (moving)
+        for (int k = 0; k < 3; k++) ax[k] += tbrow[k];
     if (d.p.ss_coupled && (ti == 1 || ti == 2 || ti == 4))
         for (int k = 0; k < 3; k++) ax[k] += d.s.cpl[(size_t)k * N + i];
     const double dt = d.p.dt;
@@ -1469,7 +1509,9 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
     for (int k = 0; k < 3; k++) vm[k] = d.s.vx_next[k * N + i];
     const bool moving = (ti >= 1 && ti <= 4);
     double vn[3] = {vm[0], vm[1], vm[2]};
+    bool any_wall = true;      // whether a wall particle is in the list (known after the XSPH loop)
     if (d.p.if_move != 2 && moving) {
+        any_wall = false;
         const real xs_same = (real)((ti == 1) ? d.p.xsph0 : (ti == 3) ? d.p.xsph2 : d.p.xsph1);
         const real xs_wall = (real)((ti == 1 || ti == 3) ? 0.006 : d.p.xsph1 / 5.0);
         Sum<real> stu[3], sdown;
@@ -1482,6 +1524,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
                 xishu = xs_same;
             } else if (tj == 0) {
                 xishu = xs_wall;
+                any_wall = true;
             } else {
                 continue;
             }
@@ -1505,12 +1548,14 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
     // CPP_13-boundary.cpp:71-122): the same correction
     const bool vsd = d.p.flbndy == 2 || d.p.flbndy == 13 || d.p.flbndy == 14;
     const bool vcorr = (d.p.flbndy == 1 && moving) || (vsd && (ti == 1 || ti == 3));
-    if (vcorr) {
+    if (vcorr && any_wall) {
         const double a = (d.p.flbndy == 1) ? 0.30 : d.p.coe_bndy, b = a, dr = d.p.dr;
         double tb[3] = {0, 0, 0};
+        NbrIter itw(d, i, nn);
         for (int q = 0; q < nn; q++) {
-            const int j = d.s.nbr[(size_t)q * N + i];
-            if (d.s.type[j] != 0) continue;
+            int j, tj;
+            itw.next(j, tj);
+            if (tj != 0) continue;
             const Pos pj = load_pos(d.s.xh, j);
             const double xj[3] = {pj.x, pj.y, pj.z};
             double inprod = 0.0, dst = 0.0;
@@ -1528,6 +1573,10 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
             }
         }
         for (int k = 0; k < nd; k++) vn[k] = vn[k] + tb[k];
+    }
+    else if (vcorr) {
+        // no wall in the list: the correction adds zeros (kept, for -0.0)
+        for (int k = 0; k < nd; k++) vn[k] = vn[k] + 0.0;
     }
     if (d.p.flbndy != 1 && d.p.flbndy != 5 && moving)
         for (int k = 0; k < 3; k++) d.s.vx_vb[k * N + i] = vn[k];
@@ -2453,11 +2502,20 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
         k_ss_struct<<<nblk(N, 128), 128, 0, st>>>(d); n++;
     }
     REC(16);
-    if (art) {
-        if (d.p.ndim == 2) k_accel_b<2, 1><<<nblk(N, 128), 128, 0, st>>>(d);
-        else k_accel_b<3, 1><<<nblk(N, 128), 128, 0, st>>>(d);
-    } else {
-        LAUNCH_ND(k_accel_b, nblk(N, 128), 128, d);
+    {
+        const int v = (art ? 1 : 0) + (d.p.fli > 1 ? 2 : 0);
+        const dim3 g(nblk(N, 128)), b(128);
+        if (d.p.ndim == 2) {
+            if (v == 0) k_accel_b<2, 0, 0><<<g, b, 0, st>>>(d);
+            else if (v == 1) k_accel_b<2, 1, 0><<<g, b, 0, st>>>(d);
+            else if (v == 2) k_accel_b<2, 0, 1><<<g, b, 0, st>>>(d);
+            else k_accel_b<2, 1, 1><<<g, b, 0, st>>>(d);
+        } else {
+            if (v == 0) k_accel_b<3, 0, 0><<<g, b, 0, st>>>(d);
+            else if (v == 1) k_accel_b<3, 1, 0><<<g, b, 0, st>>>(d);
+            else if (v == 2) k_accel_b<3, 0, 1><<<g, b, 0, st>>>(d);
+            else k_accel_b<3, 1, 1><<<g, b, 0, st>>>(d);
+        }
     }
     n++;
     REC(17);

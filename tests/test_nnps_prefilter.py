@@ -5,7 +5,7 @@ grid minimum and only falls back to the FP64 test of partisearching
 (CPP_3-NNPS.cpp:300-312: sqrt of the FP64 sum of squares <= h_i + h_j) when the
 FP32 squared distance lies within a rounding margin M of T^2.  This file
 restates that prefilter in numpy float32 arithmetic, operation for
-operation, and checks on adversarial pairs (distances within a few ulps of the
+operation (fused multiply-adds emulated), and checks on adversarial pairs (distances within a few ulps of the
 support radius, far from the grid origin) that every pair it decides without
 the fallback is decided as the FP64 test decides it.
 """
@@ -22,8 +22,27 @@ def fp64_inside(xi, xj, hi, hj):
     return np.sqrt(d2) <= T
 
 
+def _fma32(a, b, c):
+    """float32 fused multiply-add: the product of two float32 values is exact
+    in float64, so one float64 sum rounded to float32 (a double rounding that
+    differs from the single rounding only on exact ties) stands in for it."""
+    return (a.astype(np.float64) * b.astype(np.float64) + c.astype(np.float64)).astype(np.float32)
+
+
+def _bounds(nd, fh, hj, ce, ct):
+    f32 = np.float32
+    Tf = (fh + hj).astype(f32)
+    T2f = (Tf * Tf).astype(f32)
+    e = (ce + (f32(4.4) * U * Tf).astype(f32)).astype(f32)
+    M = (f32(nd) * e * (f32(4.0) * Tf + e).astype(f32) + (ct * T2f).astype(f32)).astype(f32)
+    return (T2f - M).astype(f32), (T2f + M).astype(f32), T2f
+
+
 def prefilter(xi, xj, hi, hj, xmin):
-    """(decided, inside) of the FP32 stage of k_nnps for each pair."""
+    """(decided, inside) of the FP32 stage of k_nnps for each pair: the squared
+    distance summed with fused multiply-adds; a candidate with the particle's
+    own h is decided by the bounds alone, any other is first tested against
+    twice the radius."""
     f32 = np.float32
     nd = xi.shape[1]
     fi = (xi - xmin).astype(f32)
@@ -37,17 +56,17 @@ def prefilter(xi, xj, hi, hj, xmin):
     d2f = (t * t).astype(f32)
     for k in range(1, nd):
         t = (fi[:, k] - fj[:, k]).astype(f32)
-        d2f = (d2f + (t * t).astype(f32)).astype(f32)
-    Tf = (fh + fjh).astype(f32)
-    T2f = (Tf * Tf).astype(f32)
-    far = d2f > f32(4.0) * T2f
-    e = (ce + (f32(4.4) * U * Tf).astype(f32)).astype(f32)
-    M = (f32(nd) * e * (f32(4.0) * Tf + e).astype(f32) + (ct * T2f).astype(f32)).astype(f32)
-    lo = d2f < (T2f - M).astype(f32)
-    hi_ = d2f > (T2f + M).astype(f32)
-    decided = fast & (far | lo | hi_)
-    inside = fast & ~far & lo
-    return decided, inside
+        d2f = _fma32(t, t, d2f)
+    lo0, hi0, _ = _bounds(nd, fh, fh, ce, ct)
+    lo1, hi1, T2f = _bounds(nd, fh, fjh, ce, ct)
+    same = fjh == fh
+    lo = np.where(same, lo0, lo1)
+    hi = np.where(same, hi0, hi1)
+    far = ~same & (d2f > f32(4.0) * T2f)
+    inside = ~far & (d2f < lo)
+    out = far | (d2f > hi)
+    decided = fast & (inside | out)
+    return decided, fast & inside
 
 
 def _pairs_near_radius(rng, n, nd, origin_scale, h, rel):
