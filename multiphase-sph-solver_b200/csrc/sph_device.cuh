@@ -213,13 +213,29 @@ __device__ __forceinline__ PairI<R> pair_i(const Dev& d, int i)
     return I;
 }
 
+// x / y correctly rounded, from yr = RN(1 / y): q = RN(x yr) lies within one
+// ulp of x / y, the residual x - q y is then exact as a fused multiply-add,
+// and RN(q + r yr) is RN(x / y) (Markstein's correction).  A zero residual
+// means q is exact and is returned as it is, which also keeps the sign of a
+// zero quotient.  One multiply and two fused multiply-adds in place of an
+// IEEE division wherever the reciprocal is shared.
+__device__ __forceinline__ double div_rcp(double x, double y, double yr)
+{
+    const double q = __dmul_rn(x, yr);
+    const double r = __fma_rn(-q, y, x);
+    return (r == 0.0) ? q : __fma_rn(r, yr, q);
+}
+
 // Kernel value and gradient of pair (i, j) exactly as partisearching stored
 // them: weight() / weight2() (CPP_3-NNPS.cpp:17-82) with the same
 // differences, summation order and sqrt, recomputed from this step's
-// positions.  w[0..2] gradient, w[3] value.  In FP32 the gradient's common
-// factor is divided once per pair instead of once per component.
+// positions.  w[0..2] gradient, w[3] value.  In FP64 the quotients by ra
+// (rra = RN(1 / h_i) when h_j = h_i), by ra * dst (one reciprocal for the
+// components) and by 6 are taken with div_rcp, which gives the IEEE
+// quotients.  In FP32 the gradient's common factor is divided once per pair
+// instead of once per component.
 template <int ND, typename R>
-__device__ __forceinline__ void pair_w_raw(const Dev& d, const PairI<R>& I, const Pos& pj, R w[4])
+__device__ __forceinline__ void pair_w_raw(const Dev& d, const PairI<R>& I, R rra, const Pos& pj, R w[4])
 {
     constexpr int nd = ND;
     constexpr bool f32 = sizeof(R) == 4;
@@ -232,9 +248,16 @@ __device__ __forceinline__ void pair_w_raw(const Dev& d, const PairI<R>& I, cons
     }
     dst = sqrt(dst);
     const R hj = (R)pj.h;
-    const R ra = (hj == I.h) ? I.h : (I.h + hj) / 2;
-    const R a1 = (hj == I.h) ? I.a1 : kernel_a1<R>(ra, nd, d.p.flknl);
-    const R s = dst / ra;
+    const bool same_h = (hj == I.h);
+    const R ra = same_h ? I.h : (I.h + hj) / 2;
+    const R a1 = same_h ? I.a1 : kernel_a1<R>(ra, nd, d.p.flknl);
+    R s;
+    if (!f32 && same_h) s = (R)div_rcp(dst, ra, rra);
+    else s = dst / ra;
+    // the gradient's quotients by ra * dst
+    const R D = ra * dst;
+    const R rD = f32 ? R(0) : R(1.0) / D;
+    auto grad = [&](R num) -> R { return f32 ? num / D : (R)div_rcp(num, D, rD); };
     w[0] = w[1] = w[2] = w[3] = R(0);
     if (d.p.flknl == 1 || d.p.flknl == 3) {
         if (s == R(0)) {
@@ -242,20 +265,22 @@ __device__ __forceinline__ void pair_w_raw(const Dev& d, const PairI<R>& I, cons
         }
         if (s > R(0) && s <= R(1)) {
             if (f32) {
-                const R g = a1 * (-2 * s + R(1.5) * s * s) / (ra * dst);
+                const R g = a1 * (-2 * s + R(1.5) * s * s) / D;
                 for (int k = 0; k < nd; k++) w[k] = dx[k] * g;
             } else {
-                for (int k = 0; k < nd; k++) w[k] = a1 * dx[k] * (-2 * s + R(1.5) * s * s) / (ra * dst);
+                for (int k = 0; k < nd; k++) w[k] = grad(a1 * dx[k] * (-2 * s + R(1.5) * s * s));
             }
             w[3] = a1 * (R(0.66666667) - s * s + R(0.5) * s * s * s);
         } else if (s > R(1) && s <= R(2)) {
             if (f32) {
-                const R g = a1 * R(-0.5) * (R(2.0) - s) * (R(2.0) - s) / (ra * dst);
+                const R g = a1 * R(-0.5) * (R(2.0) - s) * (R(2.0) - s) / D;
                 for (int k = 0; k < nd; k++) w[k] = dx[k] * g;
+                w[3] = a1 * (R(2.0) - s) * (R(2.0) - s) * (R(2.0) - s) / R(6.0);
             } else {
-                for (int k = 0; k < nd; k++) w[k] = a1 * R(-0.5) * dx[k] * (R(2.0) - s) * (R(2.0) - s) / (ra * dst);
+                for (int k = 0; k < nd; k++) w[k] = grad(a1 * R(-0.5) * dx[k] * (R(2.0) - s) * (R(2.0) - s));
+                constexpr double r6 = 1.0 / 6.0;
+                w[3] = (R)div_rcp(a1 * (R(2.0) - s) * (R(2.0) - s) * (R(2.0) - s), 6.0, r6);
             }
-            w[3] = a1 * (R(2.0) - s) * (R(2.0) - s) * (R(2.0) - s) / R(6.0);
         }
     } else {
         if (s == R(0)) {
@@ -263,18 +288,18 @@ __device__ __forceinline__ void pair_w_raw(const Dev& d, const PairI<R>& I, cons
         }
         if (s > R(0) && s <= R(1)) {
             if (f32) {
-                const R g = a1 * (R(-6.0) + R(3.0) * s * s) / (ra * dst);
+                const R g = a1 * (R(-6.0) + R(3.0) * s * s) / D;
                 for (int k = 0; k < nd; k++) w[k] = dx[k] * g;
             } else {
-                for (int k = 0; k < nd; k++) w[k] = a1 * dx[k] * (R(-6.0) + R(3.0) * s * s) / (ra * dst);
+                for (int k = 0; k < nd; k++) w[k] = grad(a1 * dx[k] * (R(-6.0) + R(3.0) * s * s));
             }
             w[3] = a1 * (R(6.0) - R(6.0) * s + R(1.0) * s * s * s);
         } else if (s > R(1) && s <= R(2)) {
             if (f32) {
-                const R g = a1 * R(-3.0) * (R(2.0) - s) * (R(2.0) - s) / (ra * dst);
+                const R g = a1 * R(-3.0) * (R(2.0) - s) * (R(2.0) - s) / D;
                 for (int k = 0; k < nd; k++) w[k] = dx[k] * g;
             } else {
-                for (int k = 0; k < nd; k++) w[k] = a1 * R(-3.0) * dx[k] * (R(2.0) - s) * (R(2.0) - s) / (ra * dst);
+                for (int k = 0; k < nd; k++) w[k] = grad(a1 * R(-3.0) * dx[k] * (R(2.0) - s) * (R(2.0) - s));
             }
             w[3] = a1 * (R(2.0) - s) * (R(2.0) - s) * (R(2.0) - s);
         }

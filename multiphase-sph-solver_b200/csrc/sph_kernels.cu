@@ -406,6 +406,7 @@ __device__ __forceinline__ void pairw_particle(const Dev& d, int i)
 {
     const int N = d.p.N, nn = nbr_count(d, i);
     const PairI<R> I = pair_i<ND, R>(d, i);
+    const R rra = R(1.0) / I.h;     // RN(1 / h_i), the reciprocal of ra when h_j = h_i
     // the next slot's index and position are loaded one slot ahead
     int jn = (nn > 1) ? d.s.nbr[(size_t)N + i] : 0;
     Pos pn = load_pos(d.s.xh, (nn > 0) ? d.s.nbr[i] : i);
@@ -414,7 +415,7 @@ __device__ __forceinline__ void pairw_particle(const Dev& d, int i)
         if (s + 1 < nn) pn = load_pos(d.s.xh, jn);
         if (s + 2 < nn) jn = d.s.nbr[(size_t)(s + 2) * N + i];
         R w[4];
-        pair_w_raw<ND, R>(d, I, pj, w);
+        pair_w_raw<ND, R>(d, I, rra, pj, w);
         store_w(d, s, i, w);
     }
 }
