@@ -90,6 +90,7 @@ struct DevState {
     double *vx, *vx_next;      // vx: velocity after the step; vx_next: before XSPH
     double *vxp, *axp, *ax, *ux;
     double *rho, *rho_c, *rhop, *pre, *prep, *porosity, *poro_cop, *e;
+    double *rrho;              // RN(1 / rho) at the start of the step (k_pairw), for k_density
     double *sig, *sig_next;    // 6N each, ping-pong
     double *eps, *adps;
     double *tssig, *tsqc;      // TSSMP: the transformed stress and its q (flts >= 1)
@@ -217,14 +218,23 @@ __device__ __forceinline__ PairI<R> pair_i(const Dev& d, int i)
 // ulp of x / y, the residual x - q y is then exact as a fused multiply-add,
 // and RN(q + r yr) is RN(x / y) (Markstein's correction).  A zero residual
 // means q is exact and is returned as it is, which also keeps the sign of a
-// zero quotient.  One multiply and two fused multiply-adds in place of an
-// IEEE division wherever the reciprocal is shared.
+// zero quotient.  A residual that is not finite comes from an infinite or
+// NaN operand or a zero or infinite divisor; those take the IEEE division,
+// so that inf / y stays inf.  One multiply and two fused multiply-adds in
+// place of an IEEE division wherever the reciprocal is shared.
 __device__ __forceinline__ double div_rcp(double x, double y, double yr)
 {
     const double q = __dmul_rn(x, yr);
     const double r = __fma_rn(-q, y, x);
-    return (r == 0.0) ? q : __fma_rn(r, yr, q);
+    if (r == 0.0) return q;
+    if (!isfinite(r)) return x / y;
+    return __fma_rn(r, yr, q);
 }
+
+// x / rho_j: in FP64 the IEEE quotient from the stored reciprocal of rho_j
+// (div_rcp), in the FP32 bulk form a plain division
+__device__ __forceinline__ double div_rho(double x, double rj, double rrj) { return div_rcp(x, rj, rrj); }
+__device__ __forceinline__ float div_rho(float x, float rj, double) { return x / rj; }
 
 // Kernel value and gradient of pair (i, j) exactly as partisearching stored
 // them: weight() / weight2() (CPP_3-NNPS.cpp:17-82) with the same

@@ -425,6 +425,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_pairw(Dev d)
 {
     const int i = IDX;
     if (i >= d.p.N || *d.s.err) return;
+    d.s.rrho[i] = 1.0 / d.s.rho[i];     // for the divisions by rho_j of k_density (rho of the last step)
     if (d.p.bulk) pairw_particle<ND, float>(d, i);
     else pairw_particle<ND, double>(d, i);
 }
@@ -454,8 +455,9 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
                 real w[4];
                 load_w(d, s, i, w);
                 const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
-                sup.add(mj * (real)d.s.porosity[j] / rj * w[3]);
-                sdown.add(mj / rj * w[3]);
+                const double rrj = d.s.rrho[j];
+                sup.add(div_rho(mj * (real)d.s.porosity[j], rj, rrj) * w[3]);
+                sdown.add(div_rho(mj, rj, rrj) * w[3]);
             }
         }
         const double up = sup.v(), down = sdown.v();

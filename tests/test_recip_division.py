@@ -9,6 +9,7 @@ Checked here on the CPU with exact rational arithmetic standing in for the
 device's rounded multiply and fused multiply-adds, against IEEE division,
 on random operands over many binades and on quotients near rounding ties.
 """
+import math
 from fractions import Fraction
 
 import numpy as np
@@ -18,22 +19,45 @@ def rn(v: Fraction) -> float:
     return float(v)            # Fraction -> float rounds to nearest, ties to even
 
 
+def _ieee_div(x: float, y: float) -> float:
+    if y == 0.0:
+        if x == 0.0 or math.isnan(x):
+            return math.nan
+        return math.copysign(math.inf, x) * math.copysign(1.0, y)
+    return x / y
+
+
+def _fma_residual(x: float, y: float, q: float) -> float:
+    """RN(x - q y), with the IEEE results for infinite and NaN operands."""
+    if not (math.isfinite(x) and math.isfinite(y) and math.isfinite(q)):
+        with np.errstate(all="ignore"):
+            return float(np.float64(x) - np.float64(q) * np.float64(y))
+    return rn(Fraction(x) - Fraction(q) * Fraction(y))
+
+
 def div_by_recip(x: float, y: float, yr: float) -> float:
-    q = x * yr                 # an IEEE double product, signed zeros included
-    r = rn(Fraction(x) - Fraction(q) * Fraction(y))
+    with np.errstate(all="ignore"):
+        q = float(np.float64(x) * np.float64(yr))    # IEEE product, signed zeros and infinities included
+    r = _fma_residual(x, y, q)
     if r == 0.0:
         return q
+    if not math.isfinite(r):
+        return _ieee_div(x, y)
     return rn(Fraction(r) * Fraction(yr) + Fraction(q))
+
+
+def _same(a: float, b: float) -> bool:
+    if math.isnan(a) or math.isnan(b):
+        return math.isnan(a) and math.isnan(b)
+    return a == b and np.signbit(a) == np.signbit(b)
 
 
 def _check(xs, ys):
     bad = 0
     for x, y in zip(xs, ys):
         x, y = float(x), float(y)
-        yr = 1.0 / y
-        got = div_by_recip(x, y, yr)
-        want = x / y
-        if got != want or np.signbit(got) != np.signbit(want):
+        yr = _ieee_div(1.0, y)
+        if not _same(div_by_recip(x, y, yr), _ieee_div(x, y)):
             bad += 1
     return bad
 
@@ -73,4 +97,13 @@ def test_near_ties_and_zeros():
         ys += [y, y, y, y]
     xs += [0.0, -0.0, 3.0, -3.0]
     ys += [7.0, 7.0, 3.0, 6.0]
+    assert _check(xs, ys) == 0
+
+
+def test_infinities_nans_and_zero_divisors():
+    """Operands a diverging run produces (the reference's own 3-D penalty
+    contact drives velocities to infinity): inf / y stays inf, NaN stays NaN,
+    x / 0 and x / inf are the IEEE results."""
+    xs = [math.inf, -math.inf, math.nan, 1.0, -1.0, 0.0, 2.0, -2.0, math.inf]
+    ys = [1590.0, 3.0, 2.0, 0.0, 0.0, 0.0, math.inf, math.inf, math.inf]
     assert _check(xs, ys) == 0
