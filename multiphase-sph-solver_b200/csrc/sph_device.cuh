@@ -134,6 +134,10 @@ struct DevState {
     int *val_in, *pid_sorted;
     int *cstart, *cend;        // [ctotal + 4]
     int *nnb;                  // neighbour count (may exceed the cap: error 5)
+    // per particle and particle type t = 0..4, bit s set when list slot s
+    // holds a particle of type t: nbm[(2 t + w) * N + i], word w = 0 for
+    // slots 0-63, 1 for slots 64-98 (written by k_pairw)
+    unsigned long long* nbm;
     int *nbr;                  // [SPH_NB_CAP * N]
     double *nbw;               // pair records (grad W, W) of the neighbour-list slots, [SPH_NB_CAP * N]
                                // records of 32 bytes (FP64), or 16 bytes (FP32, bulk form) in the

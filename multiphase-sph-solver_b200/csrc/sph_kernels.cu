@@ -103,6 +103,55 @@ __device__ __forceinline__ int nbr_count(const Dev& d, int i)
     return c > SPH_NB_CAP ? SPH_NB_CAP : c;
 }
 
+// The slot mask of particles of type t in particle i's list (word 0: slots
+// 0-63, word 1: slots 64-98); types 0-4 only (type 7 has none)
+struct SlotMask {
+    unsigned long long lo, hi;
+    __device__ __forceinline__ SlotMask operator|(const SlotMask& o) const { return SlotMask{lo | o.lo, hi | o.hi}; }
+    __device__ __forceinline__ bool any() const { return (lo | hi) != 0ull; }
+    __device__ __forceinline__ bool has(int s) const { return ((s < 64 ? lo >> s : hi >> (s - 64)) & 1ull) != 0; }
+};
+__device__ __forceinline__ SlotMask type_mask(const Dev& d, int i, int t)
+{
+    if (t < 0 || t > 4) return SlotMask{0ull, 0ull};
+    const size_t N = (size_t)d.p.N;
+    return SlotMask{d.s.nbm[(2 * t) * N + i], d.s.nbm[(2 * t + 1) * N + i]};
+}
+
+// The slots of particle i's list whose bits are set in a mask (from nbm:
+// one type's slots or a union), in slot order, with the next slot's particle index
+// loaded one slot ahead.  Lanes of a warp then take their k-th slot of the
+// class together, whatever the slots of other classes between them, so the
+// pass body runs with its lanes in step instead of idling on other classes.
+struct MaskIter {
+    const int* nbr;
+    size_t N;
+    int i, jn, sn;
+    unsigned long long m0, m1;
+    __device__ __forceinline__ int pop()
+    {
+        if (m0) { const int s = __ffsll(m0) - 1; m0 &= m0 - 1; return s; }
+        if (m1) { const int s = 63 + __ffsll(m1); m1 &= m1 - 1; return s; }
+        return -1;
+    }
+    __device__ __forceinline__ MaskIter(const Dev& d, int i_, SlotMask m)
+        : nbr(d.s.nbr), N((size_t)d.p.N), i(i_), m0(m.lo), m1(m.hi)
+    {
+        sn = pop();
+        jn = (sn >= 0) ? nbr[(size_t)sn * N + i] : 0;
+    }
+    // the next slot s and its particle j; false when the mask is exhausted
+    __device__ __forceinline__ bool next(int& s, int& j)
+    {
+        if (sn < 0) return false;
+        s = sn;
+        j = jn;
+        sn = pop();
+        if (sn >= 0) jn = nbr[(size_t)sn * N + i];
+        return true;
+    }
+};
+
 // The list slots of particle i in order, each slot's particle index loaded
 // two slots ahead and its type one slot ahead.  A neighbour pass is a chain of
 // dependent loads per slot (list -> type -> the neighbour's fields); issuing
@@ -407,17 +456,32 @@ __device__ __forceinline__ void pairw_particle(const Dev& d, int i)
     const int N = d.p.N, nn = nbr_count(d, i);
     const PairI<R> I = pair_i<ND, R>(d, i);
     const R rra = R(1.0) / I.h;     // RN(1 / h_i), the reciprocal of ra when h_j = h_i
-    // the next slot's index and position are loaded one slot ahead
+    unsigned long long tm[5][2] = {{0ull, 0ull}, {0ull, 0ull}, {0ull, 0ull}, {0ull, 0ull}, {0ull, 0ull}};
+    // the next slot's index, position and type are loaded one slot ahead
     int jn = (nn > 1) ? d.s.nbr[(size_t)N + i] : 0;
-    Pos pn = load_pos(d.s.xh, (nn > 0) ? d.s.nbr[i] : i);
+    const int j0 = (nn > 0) ? d.s.nbr[i] : i;
+    Pos pn = load_pos(d.s.xh, j0);
+    int tn = d.s.type[j0];
     for (int s = 0; s < nn; s++) {
         const Pos pj = pn;
-        if (s + 1 < nn) pn = load_pos(d.s.xh, jn);
+        const int tj = tn;
+        if (s + 1 < nn) { pn = load_pos(d.s.xh, jn); tn = d.s.type[jn]; }
         if (s + 2 < nn) jn = d.s.nbr[(size_t)(s + 2) * N + i];
         R w[4];
         pair_w_raw<ND, R>(d, I, rra, pj, w);
         store_w(d, s, i, w);
+        const unsigned long long lo = (s < 64) ? (1ull << s) : 0ull, hi = (s < 64) ? 0ull : (1ull << (s - 64));
+#pragma unroll
+        for (int t = 0; t < 5; t++)
+            if (tj == t) {
+                tm[t][0] |= lo;
+                tm[t][1] |= hi;
+            }
     }
+#pragma unroll
+    for (int t = 0; t < 5; t++)
+#pragma unroll
+        for (int w = 0; w < 2; w++) d.s.nbm[(size_t)(2 * t + w) * N + i] = tm[t][w];
 }
 
 template <int ND>
@@ -447,18 +511,15 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
     double pcop = d.s.poro_cop[i];
     if (ti == 1) {
         Sum<real> sup, sdown;
-        NbrIter it(d, i, nn);
-        for (int s = 0; s < nn; s++) {
-            int j, tj;
-            it.next(j, tj);
-            if (tj == 2) {
-                real w[4];
-                load_w(d, s, i, w);
-                const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
-                const double rrj = d.s.rrho[j];
-                sup.add(div_rho(mj * (real)d.s.porosity[j], rj, rrj) * w[3]);
-                sdown.add(div_rho(mj, rj, rrj) * w[3]);
-            }
+        MaskIter it(d, i, type_mask(d, i, 2));
+        int s, j;
+        while (it.next(s, j)) {
+            real w[4];
+            load_w(d, s, i, w);
+            const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
+            const double rrj = d.s.rrho[j];
+            sup.add(div_rho(mj * (real)d.s.porosity[j], rj, rrj) * w[3]);
+            sdown.add(div_rho(mj, rj, rrj) * w[3]);
         }
         const double up = sup.v(), down = sdown.v();
         if (fabs(down) > 1.0e-7) {
@@ -478,14 +539,15 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
         for (int k = 0; k < 3; k++) vi[k] = d.s.vxp[k * N + i];
         const bool solid = (ti == 2 || ti == 4), fluid = (ti == 1 || ti == 3);
         const bool moving = (ti >= 1 && ti <= 4);
-        NbrIter it(d, i, nn);
-        for (int s = 0; s < nn; s++) {
-            int j, tj;
-            it.next(j, tj);
+        // slots of i's own type (not for walls) and, for moving i, wall slots
+        const SlotMask wallm = moving ? type_mask(d, i, 0) : SlotMask{0ull, 0ull};
+        MaskIter it(d, i, (ti != 0 ? type_mask(d, i, ti) : SlotMask{0ull, 0ull}) | wallm);
+        int s, j;
+        while (it.next(s, j)) {
             double vxj[3];
-            if (ti == tj && ti != 0) {
+            if (!wallm.has(s)) {
                 for (int k = 0; k < 3; k++) vxj[k] = d.s.vxp[k * N + j];
-            } else if (moving && tj == 0) {
+            } else if (moving) {
                 // virtual wall velocity (:89-121)
                 for (int k = 0; k < 3; k++) vxj[k] = wall_vel(d, ti, j, vi, k);
             } else {
@@ -535,17 +597,14 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_shepard_eos(Dev d)
     if (i >= N || *d.s.err) return;
     const int ti = d.s.type[i], nn = nbr_count(d, i);
     Sum<real> sup, sdown;
-    NbrIter it(d, i, nn);
-    for (int s = 0; s < nn; s++) {
-        int j, tj;
-        it.next(j, tj);
-        if (tj == ti) {
-            real w[4];
-            load_w(d, s, i, w);
-            const real mj = (real)d.s.mass[j];
-            sup.add(mj * w[3]);
-            sdown.add(mj / (real)d.s.rho_c[j] * w[3]);
-        }
+    MaskIter it(d, i, type_mask(d, i, ti));
+    int s, j;
+    while (it.next(s, j)) {
+        real w[4];
+        load_w(d, s, i, w);
+        const real mj = (real)d.s.mass[j];
+        sup.add(mj * w[3]);
+        sdown.add(mj / (real)d.s.rho_c[j] * w[3]);
     }
     const double up = sup.v(), down = sdown.v();
     double r = d.s.rho_c[i];
@@ -588,18 +647,17 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_strain(Dev d)
     Sum<real> su1, su2, su3, su4, sd1, sd2, sd3, sd4;
     Sum<real> sus[6], sdsw;
     Sum<real> scolor;
-    NbrIter it(d, i, nn);
-    for (int q = 0; q < nn; q++) {
-        int j, tj;
-        it.next(j, tj);
-        const bool same = (ti == tj && ti != 7 && ti != 0);
-        const bool wallj = (moving && tj == 0);
-        const bool gath = (ti != tj) && ((ti == 2 || ti == 4 || ti == 0) && (tj == 1 || tj == 3 || (ti == 0 && tj == 2)));
-        if (!(same || wallj || gath)) continue;
+    // the velocity-gradient and colour sums over i's own type (not walls,
+    // not type 7) and, for moving i, the walls
+    const SlotMask wallm = moving ? type_mask(d, i, 0) : SlotMask{0ull, 0ull};
+    MaskIter it(d, i, ((ti != 0 && ti != 7) ? type_mask(d, i, ti) : SlotMask{0ull, 0ull}) | wallm);
+    int q, j;
+    while (it.next(q, j)) {
+        const bool same = !wallm.has(q);
         real w[4];
         load_w(d, q, i, w);
         const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
-        if (same || wallj) {
+        {
             real dvx[3];
             for (int k = 0; k < 3; k++) {
                 double vj = same ? d.s.vxp[k * N + j] : wall_vel(d, ti, j, vi, k);
@@ -622,7 +680,17 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_strain(Dev d)
             }
             scolor.add(mj / rj * real(1.0) * w[3]);
         }
-        if (gath) {
+    }
+    // the pressure (and, for walls, stress) gathers of eos from the fluids
+    // (and, for walls, the soil), in a loop of their own over those slots
+    if (ti == 2 || ti == 4 || ti == 0) {
+        const SlotMask m1 = type_mask(d, i, 1), m3 = type_mask(d, i, 3);
+        MaskIter itg(d, i, m1 | m3 | (ti == 0 ? type_mask(d, i, 2) : SlotMask{0ull, 0ull}));
+        while (itg.next(q, j)) {
+            const int tj = m1.has(q) ? 1 : m3.has(q) ? 3 : 2;
+            real w[4];
+            load_w(d, q, i, w);
+            const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
             const real w3 = w[3];
             const real pj_ = (ti == 0 && tj == 2) ? real(0) : (real)d.s.pre[j];
             if (ti == 2 && tj == 1) { su1.add(mj * pj_ * w3 / rj); sd1.add(mj * w3 / rj); }
@@ -1050,13 +1118,12 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_a(Dev d)
     double pi_own = 0.0;
     if (ti == 2) pi_own = (1 - poro_s) * (-satu_i * prew_i + (1 - satu_i) * prea_i) / dens_s / dens_s;
     if (ti == 4) pi_own = (-satu_i * prew_i + (1 - satu_i) * prea_i) / ri / ri;
-    NbrIter it(d, i, nn);
-    for (int q = 0; q < nn; q++) {
-        int j, tj;
-        it.next(j, tj);
-        const bool f_pair = fluid && (tj == ti || tj == other);
-        const bool s_pair = solid && tj == ti;
-        if (!(f_pair || s_pair)) continue;
+    // fluid: its own and the other fluid's slots; solid: its own type's
+    MaskIter it(d, i, fluid ? (type_mask(d, i, ti) | type_mask(d, i, other)) : type_mask(d, i, ti));
+    int q, j;
+    while (it.next(q, j)) {
+        const bool f_pair = fluid;
+        const bool s_pair = solid;
         real w[4];
         load_w(d, q, i, w);
         const real mj = (real)d.s.mass[j];
@@ -1254,37 +1321,28 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
     // boundary_effect_free_struct (CPP_9-4:900-990) for the other flbndy
     // values: a fluid's mirrored stress has its shear components negated
     const bool free_struct = !(tran || d.p.flbndy == 1 || d.p.flbndy == 2);
-    // the common sums (artificial viscosity, soil-water drag, geostatic
-    // damping), and whether a wall particle is in the list
-    bool any_wall = false;
-    NbrIter it(d, i, nn);
-    for (int q = 0; q < nn; q++) {
-        int j, tj;
-        it.next(j, tj);
-        const bool av_pair = (ti == tj && ti != 7);
-        // the soil-water (and soil-air) pairs interact1/2/3 add a term for;
-        // the reference visits every other pair of different types too, but
-        // adds nothing for them
-        const bool in_pair = d.p.fli >= 1 &&
-            ((ti == 2 && (tj == 1 || tj == 3)) || ((ti == 1 || ti == 3) && tj == 2));
-        const bool dm_pair = damping && tj == ti;
-        any_wall = any_wall || tj == 0;
-        if (!(av_pair || in_pair)) continue;
-        const Pos pj = load_pos(d.s.xh, j);
-        real w[4];
-        load_w(d, q, i, w);
-        const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
-        const double xj[3] = {pj.x, pj.y, pj.z};
-        // the relative position and velocity and their inner product, which
-        // artificial_viscosity and interact form alike (products commute)
-        real inprod = 0, dst = 0, dx[3], dvx[3];
-        for (int k = 0; k < nd; k++) {
-            dvx[k] = (real)(vi[k] - d.s.vxp[k * N + j]);
-            dx[k] = (real)(I.x[k] - xj[k]);
-            dst = dst + dx[k] * dx[k];
-            inprod = inprod + dvx[k] * dx[k];
-        }
-        if (av_pair) {
+    // artificial viscosity and geostatic damping over i's own type's slots,
+    // then the soil-water (soil-air) drag of interact1/2/3 over the slots of
+    // the types it pairs (the reference visits every other pair of different
+    // types too, but adds nothing for them); each sum in list order
+    const bool any_wall = type_mask(d, i, 0).any();
+    {
+        MaskIter it(d, i, (ti != 7) ? type_mask(d, i, ti) : SlotMask{0ull, 0ull});
+        int q, j;
+        while (it.next(q, j)) {
+            const bool dm_pair = damping;
+            const Pos pj = load_pos(d.s.xh, j);
+            real w[4];
+            load_w(d, q, i, w);
+            const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
+            const double xj[3] = {pj.x, pj.y, pj.z};
+            real inprod = 0, dst = 0, dx[3], dvx[3];
+            for (int k = 0; k < nd; k++) {
+                dvx[k] = (real)(vi[k] - d.s.vxp[k * N + j]);
+                dx[k] = (real)(I.x[k] - xj[k]);
+                dst = dst + dx[k] * dx[k];
+                inprod = inprod + dvx[k] * dx[k];
+            }
             const real hl = ((real)pj.h + I.h) * real(0.5);
             const real rou = (rj + riR) * real(0.5);
             real paix;
@@ -1297,35 +1355,55 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
             for (int k = 0; k < nd; k++) tav[k].add(mj * paix * w[k]);
             if (dm_pair)
                 for (int k = 0; k < nd; k++) tdm[k].add(mj / rj * cdi * dvx[k] * w[3]);
-        } else if (inprod < 0) {
-            const real w3 = w[3], ga = (real)d.p.g_acc;
-            if (DRAG && d.p.fli > 1 && ((ti == 2 && tj == 1) || (ti == 1 && tj == 2))) {
-                // interact2/3 soil-water drag, m_j / rho_j W beta (v_i - v_j)
-                double mv = 0.0;
-                for (int k = 0; k < nd; k++) mv = mv + (double)dvx[k] * (double)dvx[k];
-                mv = sqrt(mv);
-                const int so = (ti == 2) ? i : j, wa = (ti == 2) ? j : i;
-                const real beta = (real)drag_beta(d.p.fli, d.s.porosity[so], d.s.s_ds[so], d.s.f_dens[wa],
-                                                  d.s.f_vis[wa], mv, (ti == 2) ? d.s.rho[j] : ri);
-                for (int k = 0; k < nd; k++) tin[k].add(mj / rj * w3 * beta * dvx[k]);
-            } else if (ti == 2 && tj == 1) {
-                const real sa = (real)satu_i, po = (real)d.s.porosity[i], cp = (real)d.s.cop[i],
-                           fd = (real)d.s.f_dens[j];
-                for (int k = 0; k < nd; k++)
-                    tin[k].add(sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3);
-            } else if (ti == 1 && tj == 2) {
-                const real sa = (real)d.s.satu[j], po = (real)d.s.porosity[j], cp = (real)d.s.cop[j],
-                           fd = (real)d.s.f_dens[i];
-                for (int k = 0; k < nd; k++)
-                    tin[k].add(sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3);
-            } else if (ti == 2 && tj == 3) {
-                const real sa = (real)satu_i, po = (real)d.s.porosity[i], fd = (real)d.s.f_dens[j];
-                for (int k = 0; k < nd; k++)
-                    tin[k].add((1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3);
-            } else if (ti == 3 && tj == 2) {
-                const real sa = (real)d.s.satu[j], po = (real)d.s.porosity[j], fd = (real)d.s.f_dens[i];
-                for (int k = 0; k < nd; k++)
-                    tin[k].add((1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3);
+        }
+    }
+    if (d.p.fli >= 1 && (ti == 1 || ti == 2 || ti == 3)) {
+        const SlotMask m1 = type_mask(d, i, 1);
+        MaskIter it(d, i, (ti == 2) ? (m1 | type_mask(d, i, 3)) : type_mask(d, i, 2));
+        int q, j;
+        while (it.next(q, j)) {
+            const int tj = (ti != 2) ? 2 : m1.has(q) ? 1 : 3;
+            const Pos pj = load_pos(d.s.xh, j);
+            real w[4];
+            load_w(d, q, i, w);
+            const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
+            const double xj[3] = {pj.x, pj.y, pj.z};
+            real inprod = 0, dvx[3];
+            for (int k = 0; k < nd; k++) {
+                dvx[k] = (real)(vi[k] - d.s.vxp[k * N + j]);
+                const real dxk = (real)(I.x[k] - xj[k]);
+                inprod = inprod + dvx[k] * dxk;
+            }
+            if (inprod < 0) {
+                const real w3 = w[3], ga = (real)d.p.g_acc;
+                if (DRAG && d.p.fli > 1 && ((ti == 2 && tj == 1) || (ti == 1 && tj == 2))) {
+                    // interact2/3 soil-water drag, m_j / rho_j W beta (v_i - v_j)
+                    double mv = 0.0;
+                    for (int k = 0; k < nd; k++) mv = mv + (double)dvx[k] * (double)dvx[k];
+                    mv = sqrt(mv);
+                    const int so = (ti == 2) ? i : j, wa = (ti == 2) ? j : i;
+                    const real beta = (real)drag_beta(d.p.fli, d.s.porosity[so], d.s.s_ds[so], d.s.f_dens[wa],
+                                                      d.s.f_vis[wa], mv, (ti == 2) ? d.s.rho[j] : ri);
+                    for (int k = 0; k < nd; k++) tin[k].add(mj / rj * w3 * beta * dvx[k]);
+                } else if (ti == 2 && tj == 1) {
+                    const real sa = (real)satu_i, po = (real)d.s.porosity[i], cp = (real)d.s.cop[i],
+                               fd = (real)d.s.f_dens[j];
+                    for (int k = 0; k < nd; k++)
+                        tin[k].add(sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3);
+                } else if (ti == 1 && tj == 2) {
+                    const real sa = (real)d.s.satu[j], po = (real)d.s.porosity[j], cp = (real)d.s.cop[j],
+                               fd = (real)d.s.f_dens[i];
+                    for (int k = 0; k < nd; k++)
+                        tin[k].add(sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3);
+                } else if (ti == 2 && tj == 3) {
+                    const real sa = (real)satu_i, po = (real)d.s.porosity[i], fd = (real)d.s.f_dens[j];
+                    for (int k = 0; k < nd; k++)
+                        tin[k].add((1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3);
+                } else if (ti == 3 && tj == 2) {
+                    const real sa = (real)d.s.satu[j], po = (real)d.s.porosity[j], fd = (real)d.s.f_dens[i];
+                    for (int k = 0; k < nd; k++)
+                        tin[k].add((1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3);
+                }
             }
         }
     }
@@ -1339,11 +1417,9 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
     // the artificial-stress pair sum (ART), likewise in a loop of its own
     Sum<real> tu[3];
     if (art) {
-        NbrIter ita(d, i, nn);
-        for (int q = 0; q < nn; q++) {
-            int j, tj;
-            ita.next(j, tj);
-            if (tj != 2) continue;
+        MaskIter ita(d, i, type_mask(d, i, 2));
+        int q, j;
+        while (ita.next(q, j)) {
             const Pos pj = load_pos(d.s.xh, j);
             real w[4];
             load_w(d, q, i, w);
@@ -1512,25 +1588,17 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
     for (int k = 0; k < 3; k++) vm[k] = d.s.vx_next[k * N + i];
     const bool moving = (ti >= 1 && ti <= 4);
     double vn[3] = {vm[0], vm[1], vm[2]};
-    bool any_wall = true;      // whether a wall particle is in the list (known after the XSPH loop)
+    const SlotMask wallm = type_mask(d, i, 0);
+    const bool any_wall = wallm.any();
     if (d.p.if_move != 2 && moving) {
-        any_wall = false;
         const real xs_same = (real)((ti == 1) ? d.p.xsph0 : (ti == 3) ? d.p.xsph2 : d.p.xsph1);
         const real xs_wall = (real)((ti == 1 || ti == 3) ? 0.006 : d.p.xsph1 / 5.0);
         Sum<real> stu[3], sdown;
-        NbrIter it(d, i, nn);
-        for (int q = 0; q < nn; q++) {
-            int j, tj;
-            it.next(j, tj);
-            real xishu;
-            if (ti == tj) {
-                xishu = xs_same;
-            } else if (tj == 0) {
-                xishu = xs_wall;
-                any_wall = true;
-            } else {
-                continue;
-            }
+        // same-type and wall slots in list order (disjoint for moving i)
+        MaskIter it(d, i, type_mask(d, i, ti) | wallm);
+        int q, j;
+        while (it.next(q, j)) {
+            const real xishu = wallm.has(q) ? xs_wall : xs_same;
             real w[4];
             load_w(d, q, i, w);
             const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
@@ -1554,11 +1622,9 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
     if (vcorr && any_wall) {
         const double a = (d.p.flbndy == 1) ? 0.30 : d.p.coe_bndy, b = a, dr = d.p.dr;
         double tb[3] = {0, 0, 0};
-        NbrIter itw(d, i, nn);
-        for (int q = 0; q < nn; q++) {
-            int j, tj;
-            itw.next(j, tj);
-            if (tj != 0) continue;
+        MaskIter itw(d, i, wallm);
+        int q, j;
+        while (itw.next(q, j)) {
             const Pos pj = load_pos(d.s.xh, j);
             const double xj[3] = {pj.x, pj.y, pj.z};
             double inprod = 0.0, dst = 0.0;
