@@ -30,7 +30,7 @@
 #define SPH_NB_CAP 99          // Par_Cell::influ[100], slots 1..99 (Class_NNPS.h:71)
 #define SPH_ERR_CELL 3         // parttocell, CPP_3-NNPS.cpp:247-257
 #define SPH_ERR_NEIGH 5        // partisearching, CPP_3-NNPS.cpp:313-319
-#define SPHK_NSTAGES 20        // entries of sphk_stage_names (one event bracket each)
+#define SPHK_NSTAGES 21        // entries of sphk_stage_names (one event bracket each)
 
 struct DevParams {
     int N, ndim, flknl, flbndy, fli, if_move, flv, inip, step_regu;
@@ -136,7 +136,7 @@ struct DevState {
     int *nnb;                  // neighbour count (may exceed the cap: error 5)
     // per particle and particle type t = 0..4, bit s set when list slot s
     // holds a particle of type t: nbm[(2 t + w) * N + i], word w = 0 for
-    // slots 0-63, 1 for slots 64-98 (written by k_pairw)
+    // slots 0-63, 1 for slots 64-98 (written by k_slotmask after the search)
     unsigned long long* nbm;
     int *nbr;                  // [SPH_NB_CAP * N]
     double *nbw;               // pair records (grad W, W) of the neighbour-list slots, [SPH_NB_CAP * N]

@@ -264,6 +264,36 @@ __global__ void k_cellrange(Dev d)
 // candidate to the FP64 path.  Only candidates within M of T^2 take the FP64
 // path, where the sqrt is evaluated only within 1e-10 of the squared radius,
 // so the decisions are those of the reference.
+// The per-type slot masks of one particle's list (nbm), built as the list
+// is written: bit s of word (t, s / 64) set when slot s holds type t (0-4)
+struct TypeMasks {
+    unsigned long long m[5][2];
+    __device__ __forceinline__ TypeMasks()
+    {
+#pragma unroll
+        for (int t = 0; t < 5; t++) m[t][0] = m[t][1] = 0ull;
+    }
+    __device__ __forceinline__ void add(int t, int s)
+    {
+        const unsigned long long lo = (s < 64) ? (1ull << s) : 0ull, hi = (s < 64) ? 0ull : (1ull << (s - 64));
+#pragma unroll
+        for (int k = 0; k < 5; k++)
+            if (t == k) {
+                m[k][0] |= lo;
+                m[k][1] |= hi;
+            }
+    }
+    __device__ __forceinline__ void store(const Dev& d, int i) const
+    {
+        const size_t N = (size_t)d.p.N;
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            d.s.nbm[(2 * k) * N + i] = m[k][0];
+            d.s.nbm[(2 * k + 1) * N + i] = m[k][1];
+        }
+    }
+};
+
 // The FP64 inclusion test of one candidate, as partisearching decides it:
 // sqrt of the FP64 sum of squares against h_i + h_j, the sqrt evaluated only
 // within 1e-10 of the squared radius (outside that band the comparison of the
@@ -446,6 +476,24 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_nnps(Dev d)
     d.s.nnb[i] = cnt;
 }
 
+// The per-type slot masks of each particle's list (nbm), from the list and
+// the neighbours' types, with the list entries loaded two slots ahead and the
+// types one slot ahead
+__global__ void __launch_bounds__(256) k_slotmask(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    const int nn = nbr_count(d, i);
+    TypeMasks tm;
+    NbrIter it(d, i, nn);
+    for (int s = 0; s < nn; s++) {
+        int j, tj;
+        it.next(j, tj);
+        tm.add(tj, s);
+    }
+    tm.store(d, i);
+}
+
 // The pair records of every list slot, as partisearching stores wij with the
 // list (CPP_3-NNPS.cpp:339-345): weight() / weight2() of the pair in FP64, or
 // in FP32 from the FP64 position differences in the bulk form.  One thread per
@@ -456,32 +504,17 @@ __device__ __forceinline__ void pairw_particle(const Dev& d, int i)
     const int N = d.p.N, nn = nbr_count(d, i);
     const PairI<R> I = pair_i<ND, R>(d, i);
     const R rra = R(1.0) / I.h;     // RN(1 / h_i), the reciprocal of ra when h_j = h_i
-    unsigned long long tm[5][2] = {{0ull, 0ull}, {0ull, 0ull}, {0ull, 0ull}, {0ull, 0ull}, {0ull, 0ull}};
-    // the next slot's index, position and type are loaded one slot ahead
+    // the next slot's index and position are loaded one slot ahead
     int jn = (nn > 1) ? d.s.nbr[(size_t)N + i] : 0;
-    const int j0 = (nn > 0) ? d.s.nbr[i] : i;
-    Pos pn = load_pos(d.s.xh, j0);
-    int tn = d.s.type[j0];
+    Pos pn = load_pos(d.s.xh, (nn > 0) ? d.s.nbr[i] : i);
     for (int s = 0; s < nn; s++) {
         const Pos pj = pn;
-        const int tj = tn;
-        if (s + 1 < nn) { pn = load_pos(d.s.xh, jn); tn = d.s.type[jn]; }
+        if (s + 1 < nn) pn = load_pos(d.s.xh, jn);
         if (s + 2 < nn) jn = d.s.nbr[(size_t)(s + 2) * N + i];
         R w[4];
         pair_w_raw<ND, R>(d, I, rra, pj, w);
         store_w(d, s, i, w);
-        const unsigned long long lo = (s < 64) ? (1ull << s) : 0ull, hi = (s < 64) ? 0ull : (1ull << (s - 64));
-#pragma unroll
-        for (int t = 0; t < 5; t++)
-            if (tj == t) {
-                tm[t][0] |= lo;
-                tm[t][1] |= hi;
-            }
     }
-#pragma unroll
-    for (int t = 0; t < 5; t++)
-#pragma unroll
-        for (int w = 0; w < 2; w++) d.s.nbm[(size_t)(2 * t + w) * N + i] = tm[t][w];
 }
 
 template <int ND>
@@ -2483,7 +2516,7 @@ extern "C" size_t sphk_sort_temp_bytes(int N, int end_bit)
 // before stage k and ev[SPHK_NSTAGES] after the last one (stages a run does
 // not need are recorded with no work between their events).
 extern "C" const char* const sphk_stage_names[] = {
-    "k_cellkey", "radix_sort", "k_cellreset", "k_cellrange", "k_nnps", "k_pairw", "k_kgc",
+    "k_cellkey", "radix_sort", "k_cellreset", "k_cellrange", "k_nnps", "k_pairw", "k_slotmask", "k_kgc",
     "k_density", "k_shepard_eos", "k_strain", "k_regu_eps", "k_stress", "k_regu_sig", "k_stress_2",
     "k_art_rij", "k_accel_a", "k_accel_b", "k_xsph_update", "k_tm_boundary", "k_step_done"};
 static_assert(sizeof(sphk_stage_names) / sizeof(sphk_stage_names[0]) == SPHK_NSTAGES, "stage table");
@@ -2519,6 +2552,8 @@ extern "C" int sphk_enqueue_nnps(const Dev* dp, void* sort_tmp, size_t sort_byte
     REC(5);
     LAUNCH_ND(k_pairw, nblk(N, 128), 128, d); n++;
     REC(6);
+    k_slotmask<<<nblk(N, 256), 256, 0, st>>>(d); n++;
+    REC(7);
     if (d.p.flknl > 2) { LAUNCH_ND(k_kgc, nblk(N, 128), 128, d); n++; }
     return n;
 }
@@ -2533,16 +2568,16 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
     d.s.eps_in = regu ? d.s.eps_tmp : d.s.eps;
     const int N = d.p.N;
     int n = 0;
-    REC(7);
-    LAUNCH_ND(k_density, nblk(N, 128), 128, d); n++;
     REC(8);
-    LAUNCH_ND(k_shepard_eos, nblk(N, 128), 128, d); n++;
+    LAUNCH_ND(k_density, nblk(N, 128), 128, d); n++;
     REC(9);
+    LAUNCH_ND(k_shepard_eos, nblk(N, 128), 128, d); n++;
+    REC(10);
     LAUNCH_ND(k_strain, nblk(N, 128), 128, d); n++;
     if (d.p.flagum == 1) { k_saturation<<<nblk(N, 128), 128, 0, st>>>(d); n++; }
-    REC(10);
-    if (regu) { LAUNCH_ND(k_regu, nblk(N, 128), 128, d, d.s.eps, d.s.eps_tmp, 1); n++; }
     REC(11);
+    if (regu) { LAUNCH_ND(k_regu, nblk(N, 128), 128, d, d.s.eps, d.s.eps_tmp, 1); n++; }
+    REC(12);
     if (regu) {
         if (d.p.ndim == 2) k_stress<2, 1><<<nblk(N, 128), 128, 0, st>>>(d);
         else k_stress<3, 1><<<nblk(N, 128), 128, 0, st>>>(d);
@@ -2551,18 +2586,18 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
         else k_stress<3, 0><<<nblk(N, 128), 128, 0, st>>>(d);
     }
     n++;
-    REC(12);
-    if (regu) { LAUNCH_ND(k_regu, nblk(N, 128), 128, d, d.s.sig_next, d.s.sig_tmp, 0); n++; }
     REC(13);
+    if (regu) { LAUNCH_ND(k_regu, nblk(N, 128), 128, d, d.s.sig_next, d.s.sig_tmp, 0); n++; }
+    REC(14);
     if (regu) {
         if (d.p.ndim == 2) k_stress<2, 2><<<nblk(N, 128), 128, 0, st>>>(d);
         else k_stress<3, 2><<<nblk(N, 128), 128, 0, st>>>(d);
         n++;
     }
-    REC(14);
+    REC(15);
     const bool art = d.p.art_stre_coe > 0.0;
     if (art) { LAUNCH_ND(k_art_rij, nblk(N, 128), 128, d); n++; }
-    REC(15);
+    REC(16);
     LAUNCH_ND(k_accel_a, nblk(N, 128), 128, d); n++;
     if (d.p.flbndy == 5) { LAUNCH_ND(k_free_solid, nblk(N, 128), 128, d); n++; }
     if (d.p.ss_coupled) { k_coupled<<<nblk(N, 128), 128, 0, st>>>(d); n++; }
@@ -2570,7 +2605,7 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
         LAUNCH_ND(k_ss_pair, nblk(N, 128), 128, d); n++;
         k_ss_struct<<<nblk(N, 128), 128, 0, st>>>(d); n++;
     }
-    REC(16);
+    REC(17);
     {
         const int v = (art ? 1 : 0) + (d.p.fli > 1 ? 2 : 0);
         const dim3 g(nblk(N, 128)), b(128);
@@ -2587,17 +2622,17 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
         }
     }
     n++;
-    REC(17);
-    LAUNCH_ND(k_xsph_update, nblk(N, 128), 128, d); n++;
     REC(18);
+    LAUNCH_ND(k_xsph_update, nblk(N, 128), 128, d); n++;
+    REC(19);
     if (d.p.flbndy == 2) {
         LAUNCH_ND(k_tm_vb, nblk(N, 128), 128, d); n++;
         k_tm_wall<<<nblk(N, 128), 128, 0, st>>>(d); n++;
     } else if (d.p.flbndy == 3 || d.p.flbndy == 4 || d.p.flbndy == 13 || d.p.flbndy == 14) {
         k_tran_wall<<<nblk(N, 128), 128, 0, st>>>(d); n++;
     }
-    REC(19);
-    k_step_done<<<1, 32, 0, st>>>(d); n++;
     REC(20);
+    k_step_done<<<1, 32, 0, st>>>(d); n++;
+    REC(21);
     return n;
 }
