@@ -660,8 +660,10 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_shepard_eos(Dev d)
 // ---------------------------------------------------------------------------
 // strain_noreg (CPP_7-1-strain.cpp:20-220), the gathered pore pressures and
 // wall stresses of eos (CPP_7-1-eos_CR.cpp:46-177) and the colour sum of
-// free_surface_check (CPP_7-2-constitutive.cpp:462-480): one pass over the
-// neighbour list, each sum in list order.  Writes de, we, color, prew, prea,
+// free_surface_check (CPP_7-2-constitutive.cpp:462-480): a loop over the
+// slots of the particle's own type and the walls, then one over the fluid
+// (and, for walls, soil) slots, each sum in list order.  Writes de, we,
+// color, prew, prea,
 // and the walls' gathered stress into sig_next (reads the soil stresses of
 // the previous step from sig).
 template <int ND>
@@ -1315,9 +1317,11 @@ __device__ __noinline__ void wall_stress_rows(int i, int N, int nn, int ti, bool
 // artificial_stress_2d/_3d (CPP_9-5-artificialstress.cpp, ART = 1),
 // boundary_moving_stress_effect (CPP_9-4-derivation_stress.cpp:631-721),
 // interact1/2/3 (CPP_10-interact1.cpp:15-405), soil_damping_geostress
-// (CPP_9-4:849-896) and veocity_update (CPP_11-xsph.cpp:11-142): one pass
-// over the neighbour list with one accumulator set per sum, combined with the
-// stress-divergence result of k_accel_a in the reference's call order.
+// (CPP_9-4:849-896) and veocity_update (CPP_11-xsph.cpp:11-142): one loop
+// per group of sums over the list slots that group takes (its own type; the
+// types the drag pairs; walls; soil), each sum over its pairs in list order,
+// combined with the stress-divergence result of k_accel_a in the reference's
+// call order.
 // Writes ax, interf, interfss and the updated velocity into vx_next (the
 // reference's vx before XSPH).  DRAG = 1 carries the interact2/3 drag
 // coefficient (fli 2, 3), whose out-of-line call the Darcy form does without.
