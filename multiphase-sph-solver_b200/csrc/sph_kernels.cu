@@ -68,6 +68,11 @@ namespace SPH_NS {
 #ifndef SPH_MINB_STRESS
 #define SPH_MINB_STRESS 2
 #endif
+// the momentum pass: its neighbour loops need about 100 registers, its
+// per-particle tail more; a cap of 96 (5 blocks per SM) spills only the tail
+#ifndef SPH_MINB_ACCB
+#define SPH_MINB_ACCB 5
+#endif
 
 __device__ __forceinline__ void raise_err(int* err, int code) { atomicCAS(err, 0, code); }
 
@@ -1326,7 +1331,7 @@ __device__ __noinline__ void wall_stress_rows(int i, int N, int nn, int ti, bool
 // reference's vx before XSPH).  DRAG = 1 carries the interact2/3 drag
 // coefficient (fli 2, 3), whose out-of-line call the Darcy form does without.
 template <int ND, int ART = 0, int DRAG = 0>
-__global__ void __launch_bounds__(128, SPH_MINB) k_accel_b(Dev d)
+__global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
