@@ -73,6 +73,21 @@ namespace SPH_NS {
 #ifndef SPH_MINB_ACCB
 #define SPH_MINB_ACCB 5
 #endif
+// the same trade for the strain pass (96 registers, a few spills), the
+// density pass (72, none) and XSPH (72, a few); the stress-divergence pass
+// ran slower at 5 blocks (2.2 -> 2.5 ms) and keeps 4
+#ifndef SPH_MINB_STRAIN
+#define SPH_MINB_STRAIN 5
+#endif
+#ifndef SPH_MINB_ACCA
+#define SPH_MINB_ACCA 4
+#endif
+#ifndef SPH_MINB_DENS
+#define SPH_MINB_DENS 6
+#endif
+#ifndef SPH_MINB_XSPH
+#define SPH_MINB_XSPH 7
+#endif
 
 __device__ __forceinline__ void raise_err(int* err, int code) { atomicCAS(err, 0, code); }
 
@@ -536,7 +551,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_pairw(Dev d)
 // ---------------------------------------------------------------------------
 // density(): fluid porosity (:25-54) and continuity (:57-165) -> rho_c
 template <int ND>
-__global__ void __launch_bounds__(128, SPH_MINB) k_density(Dev d)
+__global__ void __launch_bounds__(128, SPH_MINB_DENS) k_density(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
@@ -672,7 +687,7 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_shepard_eos(Dev d)
 // and the walls' gathered stress into sig_next (reads the soil stresses of
 // the previous step from sig).
 template <int ND>
-__global__ void __launch_bounds__(128, SPH_MINB) k_strain(Dev d)
+__global__ void __launch_bounds__(128, SPH_MINB_STRAIN) k_strain(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
@@ -1133,7 +1148,7 @@ __global__ void __launch_bounds__(128) k_art_rij(Dev d)
 // once per particle by k_stress.  Writes ax = g + sums for particle types 1-4;
 // k_accel_b continues from this value in the reference's order.
 template <int ND>
-__global__ void __launch_bounds__(128, SPH_MINB) k_accel_a(Dev d)
+__global__ void __launch_bounds__(128, SPH_MINB_ACCA) k_accel_a(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
@@ -1618,7 +1633,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b(Dev d)
 // (CPP_13-boundary.cpp:20-68) and update (CPP_12-1-update.cpp:11-55).
 // Reads xh / vx_next, writes xh_next / vx.
 template <int ND>
-__global__ void __launch_bounds__(128, SPH_MINB) k_xsph_update(Dev d)
+__global__ void __launch_bounds__(128, SPH_MINB_XSPH) k_xsph_update(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
