@@ -260,9 +260,6 @@ def reference_arm(args, world, rank):
 STATE_UP = ("xp", "vxp", "axp", "ax", "vx", "ux", "rho", "rhop", "mass", "hl", "pre", "prep", "e",
             "eps", "sig", "adps", "satu", "cop", "porosity", "poro_cop", "cd", "interf", "interfss",
             "type", "matype", "permtype", "etype")
-STATE_DOWN = ("xp", "vxp", "axp", "ax", "vx", "ux", "rho", "rhop", "pre", "prep", "e", "eps", "sig",
-              "adps", "satu", "cop", "porosity", "poro_cop", "prew", "prea", "strep", "interf",
-              "interfss", "vsig", "veps", "divq", "divr", "meps")
 
 
 def _rel_l2(a, b, m):
@@ -342,19 +339,25 @@ def engine_arm(args, world, rank, local):
     achieved = alg / (avg_ms / 1e3) / 1e9
     traffic = ncu_traffic().get(dominant)
 
-    # end to end through the C ABI from host buffers
-    host = {k: np.ascontiguousarray(st.fields[k]) for k in STATE_UP}
-    fluid, soil = st.fluid, st.soil
+    # end to end through the C ABI from host buffers, as a caller holding the
+    # reference's own arrays uses it: its Particle records (sphgpu_upload /
+    # download_particles) and its material records (sphgpu_set_materials)
+    recs = sphgpu.particle_records({k: st.fields[k] for k in STATE_UP}, scene.n)
+    out_recs = np.zeros_like(recs)
+    fluid, soil = np.ascontiguousarray(st.fluid), np.ascontiguousarray(st.soil)
     eng2 = sphgpu.Engine(st.params, device=local if world > 1 else args.device)
     barrier(world)
     t0 = time.perf_counter()
-    eng2.load_state(host, fluid, soil)
+    eng2.upload_particles(recs)
+    eng2.set_materials(fluid, soil)
     eng2.step(args.steps)
-    out = {k: eng2.get_field(k) for k in STATE_DOWN}
+    eng2.download_particles(out_recs)
     t_e2e = time.perf_counter() - t0
     t_e2e = dist_max(t_e2e, world)
-    h2d = sum(v.nbytes for v in host.values()) + fluid.nbytes + soil.nbytes
-    d2h = sum(v.nbytes for v in out.values())
+    h2d = recs.nbytes + fluid.nbytes + soil.nbytes
+    # the download moves the device-owned members only (all but x), ints in
+    # 8-byte slots
+    d2h = scene.n * sum(8 * nc if k not in sphgpu.INT_FIELDS else 8 for k, nc in sphgpu.FIELDS.items() if k != "x")
     e2e_value = total_active * args.steps / t_e2e
     eng2.close()
 
@@ -401,7 +404,8 @@ def engine_arm(args, world, rank, local):
             "kl_synthesis": kl,
             "e2e": {"value": e2e_value, "unit": "particle-updates/s",
                     "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-                    "what": "state upload + K steps + full state download through the C ABI"},
+                    "what": "Particle-record upload, material upload, K steps and Particle-record download "
+                            "through the C ABI"},
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))

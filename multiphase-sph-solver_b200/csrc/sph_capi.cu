@@ -7,11 +7,15 @@
 // alternate the ping-pong buffers of positions and stresses).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <functional>
+#include <thread>
 #include <vector>
 
 #include "../../include/sphgpu.h"
@@ -107,6 +111,11 @@ struct sphgpu_ctx {
     int sticky = 0;
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
+    // record transfer staging: two pinned host and two device chunks
+    void* rec_pinned[2] = {nullptr, nullptr};
+    void* rec_dev[2] = {nullptr, nullptr};
+    size_t rec_bytes = 0;
+    cudaEvent_t rec_ev[2] = {nullptr, nullptr};
     bool regu = false;     // graphs include the strain/stress regularisation passes
     int precision = SPHGPU_PREC_FP64;
     std::vector<sphgpu_fluid> h_fluid;   // the material records last set (K-L fields rewrite members)
@@ -192,6 +201,23 @@ void invalidate_graphs(sphgpu_ctx* c)
 {
     for (int p = 0; p < 2; p++)
         if (c->exec[p]) { cudaGraphExecDestroy(c->exec[p]); c->exec[p] = nullptr; }
+}
+
+// a loop over [0, n) split across host threads (gathers and copies of large
+// host arrays run at the host's memory bandwidth, not one core's)
+void par_for(size_t n, const std::function<void(size_t, size_t)>& body)
+{
+    unsigned T = std::thread::hardware_concurrency();
+    if (T == 0) T = 4;
+    if (T > 16) T = 16;
+    if (n < 4096 || T == 1) { body(0, n); return; }
+    std::vector<std::thread> th;
+    const size_t per = (n + T - 1) / T;
+    for (unsigned t = 0; t < T; t++) {
+        const size_t a = t * per, b = std::min(n, a + per);
+        if (a < b) th.emplace_back(body, a, b);
+    }
+    for (auto& x : th) x.join();
 }
 
 int ensure_pinned(sphgpu_ctx* c, size_t bytes)
@@ -410,6 +436,11 @@ void sphgpu_destroy(sphgpu_ctx* c)
     invalidate_graphs(c);
     for (void* p : c->allocs) cudaFree(p);
     if (c->pinned) cudaFreeHost(c->pinned);
+    for (int b = 0; b < 2; b++) {
+        if (c->rec_pinned[b]) cudaFreeHost(c->rec_pinned[b]);
+        if (c->rec_dev[b]) cudaFree(c->rec_dev[b]);
+        if (c->rec_ev[b]) cudaEventDestroy(c->rec_ev[b]);
+    }
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->st) cudaStreamDestroy(c->st);
@@ -580,41 +611,42 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
     };
     int r = 0;
     if (fl) {
-        for (int i = 0; i < N; i++) buf[i] = fl[i].dens; r |= put(s.f_dens);
-        for (int i = 0; i < N; i++) buf[i] = fl[i].porosity; r |= put(s.f_por);
-        for (int i = 0; i < N; i++) buf[i] = fl[i].vpu; r |= put(s.f_vpu);
-        for (int i = 0; i < N; i++) buf[i] = fl[i].vis; r |= put(s.f_vis);
-        for (int i = 0; i < N; i++) buf[i] = fl[i].c; r |= put(s.f_c);
-        for (int i = 0; i < N; i++) buf[i] = fl[i].strain_min; r |= put(s.f_smin);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = fl[i].dens; }); r |= put(s.f_dens);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = fl[i].porosity; }); r |= put(s.f_por);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = fl[i].vpu; }); r |= put(s.f_vpu);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = fl[i].vis; }); r |= put(s.f_vis);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = fl[i].c; }); r |= put(s.f_c);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = fl[i].strain_min; }); r |= put(s.f_smin);
         // Bingham friction: tan of the angle, CPP_7-2-constitutive.cpp:42-43
-        for (int i = 0; i < N; i++) buf[i] = std::tan(fl[i].fai * 0.0174532925199); r |= put(s.f_tanfai);
-        for (int i = 0; i < N; i++) ibuf[i] = fl[i].bhtype;
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = std::tan(fl[i].fai * 0.0174532925199); }); r |= put(s.f_tanfai);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) ibuf[i] = fl[i].bhtype; });
         CK(cudaMemcpyAsync(s.f_bhtype, ibuf.data(), sizeof(int) * N, cudaMemcpyHostToDevice, c->st));
         CK(cudaStreamSynchronize(c->st));
     }
     if (so) {
-        for (int i = 0; i < N; i++) buf[i] = so[i].e; r |= put(s.s_e);
-        for (int i = 0; i < N; i++) buf[i] = so[i].poi; r |= put(s.s_poi);
-        for (int i = 0; i < N; i++) buf[i] = so[i].eps0; r |= put(s.s_eps0);
-        for (int i = 0; i < N; i++) buf[i] = so[i].dens; r |= put(s.s_dens);
-        for (int i = 0; i < N; i++) buf[i] = so[i].kapa; r |= put(s.s_kapa);
-        for (int i = 0; i < N; i++) buf[i] = so[i].porosity; r |= put(s.s_por);
-        for (int i = 0; i < N; i++) buf[i] = so[i].vpu; r |= put(s.s_vpu);
-        for (int i = 0; i < N; i++) buf[i] = so[i].cop; r |= put(s.s_cop);
-        for (int i = 0; i < N; i++) buf[i] = so[i].sitas; r |= put(s.s_sitas);
-        for (int i = 0; i < N; i++) buf[i] = so[i].sitar; r |= put(s.s_sitar);
-        for (int i = 0; i < N; i++) buf[i] = so[i].ds; r |= put(s.s_ds);
-        for (int i = 0; i < N; i++) buf[i] = so[i].c; r |= put(s.s_c);
-        for (int i = 0; i < N; i++) buf[i] = so[i].fs; r |= put(s.s_fs);
-        for (int i = 0; i < N; i++) buf[i] = so[i].ann; r |= put(s.s_ann);
-        for (int i = 0; i < N; i++) buf[i] = so[i].zmf; r |= put(s.s_zmf);
-        for (int i = 0; i < N; i++) buf[i] = so[i].ramda; r |= put(s.s_ramda);
-        for (int i = 0; i < N; i++) buf[i] = so[i].sme0; r |= put(s.s_sme0);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].e; }); r |= put(s.s_e);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].poi; }); r |= put(s.s_poi);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].eps0; }); r |= put(s.s_eps0);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].dens; }); r |= put(s.s_dens);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].kapa; }); r |= put(s.s_kapa);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].porosity; }); r |= put(s.s_por);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].vpu; }); r |= put(s.s_vpu);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].cop; }); r |= put(s.s_cop);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].sitas; }); r |= put(s.s_sitas);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].sitar; }); r |= put(s.s_sitar);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].ds; }); r |= put(s.s_ds);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].c; }); r |= put(s.s_c);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].fs; }); r |= put(s.s_fs);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].ann; }); r |= put(s.s_ann);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].zmf; }); r |= put(s.s_zmf);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].ramda; }); r |= put(s.s_ramda);
+        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].sme0; }); r |= put(s.s_sme0);
         // Drucker-Prager cone constants with the reference's own libm calls
         // (dpmodel1 / dpmodel_bui / DPModel_check, CPP_8-1-consfactor.cpp:294-349,
         // 461-529, 783-803); they depend only on the material record.
         std::vector<double> ya(N), yk(N), yd(N);
-        for (int i = 0; i < N; i++) {
+        par_for(N, [&](size_t a, size_t b) {
+        for (size_t i = a; i < b; i++) {
             const double fai = std::atan(std::tan(so[i].fai * 0.0174532925166667) / so[i].fs);
             const double fai_dil = std::atan(std::tan(so[i].beta * 0.0174532925166667) / so[i].fs);
             const double ci = so[i].c / so[i].fs;
@@ -623,6 +655,7 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
             // dilatancy slope, used by the Bui form (matype % 10 == 5) only
             yd[i] = std::sin(fai_dil) / std::sqrt(9.0 + 3.0 * std::sin(fai_dil) * std::sin(fai_dil));
         }
+        });
         buf = ya; r |= put(s.s_yalf);
         buf = yk; r |= put(s.s_ykap);
         buf = yd; r |= put(s.s_yalf_dil);
@@ -668,10 +701,121 @@ int sphgpu_particle_layout(const char* name, size_t* offset, int* ncomp)
     return SPHGPU_E_ARG;
 }
 
-int sphgpu_upload_particles(sphgpu_ctx* c, const void* particles, int n, size_t stride)
+}  // extern "C"
+
+namespace {
+
+// One device-owned Particle member in the record transfer: its byte offset
+// in the caller's record, its components, where it lives on the device
+// (kind 0: doubles, component-major; 1: int; 2: x, y, z of the position
+// records xh; 3: h of xh) and its byte offset in the packed download record.
+struct RecMember {
+    int off, nc, kind, pk;
+    void* dst;
+};
+constexpr int kMaxRecMembers = 48;
+constexpr int kRecChunk = 65536;          // records per staged chunk
+
+// caller records -> SoA state, one thread per record of the chunk
+__global__ void k_rec_unpack(const char* recs, size_t stride, int i0, int cnt, int N, const RecMember* tab, int nt)
 {
-    if (!c || !particles || n != c->N || stride < kParticleBytes) return SPHGPU_E_ARG;
-    const char* base = (const char*)particles;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= cnt) return;
+    const char* r = recs + (size_t)t * stride;
+    const size_t i = (size_t)i0 + t;
+    for (int m = 0; m < nt; m++) {
+        const RecMember e = tab[m];
+        const double* v = reinterpret_cast<const double*>(r + e.off);
+        if (e.kind == 0) {
+            for (int k = 0; k < e.nc; k++) static_cast<double*>(e.dst)[(size_t)k * N + i] = v[k];
+        } else if (e.kind == 1) {
+            static_cast<int*>(e.dst)[i] = *reinterpret_cast<const int*>(r + e.off);
+        } else if (e.kind == 2) {
+            for (int k = 0; k < 3; k++) static_cast<double*>(e.dst)[i * 4 + k] = v[k];
+        } else {
+            static_cast<double*>(e.dst)[i * 4 + 3] = v[0];
+        }
+    }
+}
+
+// SoA state -> packed records of the owned members (P bytes each)
+__global__ void k_rec_pack(char* out, size_t P, int i0, int cnt, int N, const RecMember* tab, int nt)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= cnt) return;
+    char* r = out + (size_t)t * P;
+    const size_t i = (size_t)i0 + t;
+    for (int m = 0; m < nt; m++) {
+        const RecMember e = tab[m];
+        double* v = reinterpret_cast<double*>(r + e.pk);
+        if (e.kind == 0) {
+            for (int k = 0; k < e.nc; k++) v[k] = static_cast<const double*>(e.dst)[(size_t)k * N + i];
+        } else if (e.kind == 1) {
+            *reinterpret_cast<int*>(r + e.pk) = static_cast<const int*>(e.dst)[i];
+        } else if (e.kind == 2) {
+            for (int k = 0; k < 3; k++) v[k] = static_cast<const double*>(e.dst)[i * 4 + k];
+        } else {
+            v[0] = static_cast<const double*>(e.dst)[i * 4 + 3];
+        }
+    }
+}
+
+// the table of device-owned members (all but x, which the host keeps) for
+// the current parity, and the packed record size
+int rec_table(sphgpu_ctx* c, std::vector<RecMember>& tab, size_t* packed)
+{
+    tab.clear();
+    size_t pk = 0;
+    for (const AosMember& m : kAos) {
+        if (std::strcmp(m.name, "x") == 0) continue;
+        const FieldDef* f = find_field(m.name);
+        RecMember e;
+        e.off = (int)m.off;
+        e.nc = f->ncomp;
+        e.pk = (int)pk;
+        if (std::strcmp(m.name, "xp") == 0) { e.kind = 2; e.dst = c->d[c->parity].s.xh; }
+        else if (std::strcmp(m.name, "hl") == 0) { e.kind = 3; e.dst = c->d[c->parity].s.xh; }
+        else { e.kind = f->is_int ? 1 : 0; e.dst = field_ptr(c, m.name); }
+        if (!e.dst) return SPHGPU_E_ARG;
+        pk += f->is_int ? 8 : 8 * (size_t)f->ncomp;   // ints keep an 8-byte slot
+        tab.push_back(e);
+    }
+    if ((int)tab.size() > kMaxRecMembers) return SPHGPU_E_ARG;
+    *packed = pk;
+    return 0;
+}
+
+int ensure_rec_staging(sphgpu_ctx* c, size_t bytes)
+{
+    if (c->rec_bytes >= bytes) return 0;
+    for (int b = 0; b < 2; b++) {
+        if (c->rec_pinned[b]) cudaFreeHost(c->rec_pinned[b]);
+        if (c->rec_dev[b]) cudaFree(c->rec_dev[b]);
+        c->rec_pinned[b] = c->rec_dev[b] = nullptr;
+    }
+    c->rec_bytes = 0;
+    for (int b = 0; b < 2; b++) {
+        CK(cudaMallocHost(&c->rec_pinned[b], bytes));
+        CK(cudaMalloc(&c->rec_dev[b], bytes + sizeof(RecMember) * kMaxRecMembers));
+        if (!c->rec_ev[b]) CK(cudaEventCreateWithFlags(&c->rec_ev[b], cudaEventDisableTiming));
+    }
+    c->rec_bytes = bytes;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Records are moved in chunks through two pinned and two device buffers: the
+// host copies a chunk of whole records (on several threads) while the
+// previous chunk crosses PCIe and a kernel scatters its members into the
+// device's component-major arrays (the reverse on download, where only the
+// device-owned members of the caller's records are written).
+// member by member through the field calls, for records that are not 8-byte
+// aligned
+int upload_by_fields(sphgpu_ctx* c, const char* base, int n, size_t stride)
+{
     for (const AosMember& m : kAos) {
         const FieldDef* f = find_field(m.name);
         const size_t nc = f->ncomp;
@@ -690,10 +834,8 @@ int sphgpu_upload_particles(sphgpu_ctx* c, const void* particles, int n, size_t 
     return 0;
 }
 
-int sphgpu_download_particles(sphgpu_ctx* c, void* particles, int n, size_t stride)
+int download_by_fields(sphgpu_ctx* c, char* base, int n, size_t stride)
 {
-    if (!c || !particles || n != c->N || stride < kParticleBytes) return SPHGPU_E_ARG;
-    char* base = (char*)particles;
     for (const AosMember& m : kAos) {
         const FieldDef* f = find_field(m.name);
         const size_t nc = f->ncomp;
@@ -708,6 +850,123 @@ int sphgpu_download_particles(sphgpu_ctx* c, void* particles, int n, size_t stri
             if (r) return r;
             for (int i = 0; i < n; i++) std::memcpy(base + (size_t)i * stride + m.off, &v[(size_t)i * nc], 8 * nc);
         }
+    }
+    return 0;
+}
+
+int sphgpu_upload_particles(sphgpu_ctx* c, const void* particles, int n, size_t stride)
+{
+    if (!c || !particles || n != c->N || stride < kParticleBytes) return SPHGPU_E_ARG;
+    if (stride % 8 != 0 || ((uintptr_t)particles) % 8 != 0)
+        return upload_by_fields(c, (const char*)particles, n, stride);
+    cudaSetDevice(c->device);
+    const char* base = (const char*)particles;
+    std::vector<RecMember> tab;
+    size_t P = 0;
+    int r = rec_table(c, tab, &P);
+    if (r) return r;
+    const size_t chunk_bytes = (size_t)kRecChunk * stride;
+    r = ensure_rec_staging(c, std::max(chunk_bytes, (size_t)kRecChunk * P));
+    if (r) return r;
+    // the host copies of x, type and matype
+    c->h_x.resize((size_t)n * 3);
+    c->h_type.resize(n);
+    c->h_matype.resize(n);
+    par_for((size_t)n, [&](size_t a, size_t b) {
+        for (size_t i = a; i < b; i++) {
+            const char* rec = base + i * stride;
+            std::memcpy(&c->h_x[i * 3], rec + 0, 24);
+            std::memcpy(&c->h_type[i], rec + 1048, 4);
+            std::memcpy(&c->h_matype[i], rec + 1052, 4);
+        }
+    });
+    c->x_tracked = true;
+    CK(cudaStreamSynchronize(c->st));
+    RecMember* dtab[2];
+    for (int b = 0; b < 2; b++) {
+        dtab[b] = reinterpret_cast<RecMember*>(static_cast<char*>(c->rec_dev[b]) + c->rec_bytes);
+        CK(cudaMemcpy(dtab[b], tab.data(), sizeof(RecMember) * tab.size(), cudaMemcpyHostToDevice));
+    }
+    int k = 0;
+    for (int i0 = 0; i0 < n; i0 += kRecChunk, k++) {
+        const int b = k & 1, cnt = std::min(kRecChunk, n - i0);
+        if (k >= 2) CK(cudaEventSynchronize(c->rec_ev[b]));
+        char* pin = static_cast<char*>(c->rec_pinned[b]);
+        const char* src = base + (size_t)i0 * stride;
+        const size_t bytes = (size_t)cnt * stride;
+        par_for(bytes, [&](size_t a, size_t e) { std::memcpy(pin + a, src + a, e - a); });
+        CK(cudaMemcpyAsync(c->rec_dev[b], pin, bytes, cudaMemcpyHostToDevice, c->st));
+        k_rec_unpack<<<(cnt + 255) / 256, 256, 0, c->st>>>(static_cast<const char*>(c->rec_dev[b]), stride, i0, cnt,
+                                                           c->N, dtab[b], (int)tab.size());
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(c->rec_ev[b], c->st));
+    }
+    CK(cudaStreamSynchronize(c->st));
+    update_static_params(c);
+    return 0;
+}
+
+int sphgpu_download_particles(sphgpu_ctx* c, void* particles, int n, size_t stride)
+{
+    if (!c || !particles || n != c->N || stride < kParticleBytes) return SPHGPU_E_ARG;
+    if (stride % 8 != 0 || ((uintptr_t)particles) % 8 != 0)
+        return download_by_fields(c, (char*)particles, n, stride);
+    cudaSetDevice(c->device);
+    char* base = (char*)particles;
+    std::vector<RecMember> tab;
+    size_t P = 0;
+    int r = rec_table(c, tab, &P);
+    if (r) return r;
+    r = ensure_rec_staging(c, std::max((size_t)kRecChunk * stride, (size_t)kRecChunk * P));
+    if (r) return r;
+    CK(cudaStreamSynchronize(c->st));
+    RecMember* dtab[2];
+    for (int b = 0; b < 2; b++) {
+        dtab[b] = reinterpret_cast<RecMember*>(static_cast<char*>(c->rec_dev[b]) + c->rec_bytes);
+        CK(cudaMemcpy(dtab[b], tab.data(), sizeof(RecMember) * tab.size(), cudaMemcpyHostToDevice));
+    }
+    // Particle::x as get_field("x") reports it: the uploaded x, and xp for
+    // the particles update() moves once a step has run
+    const bool moved = c->l_host > 1 && !c->h_type.empty();
+    const int nd = c->P.ndim;
+    auto scatter = [&](int i0, int cnt, const char* pin) {
+        par_for((size_t)cnt, [&](size_t a, size_t e) {
+            for (size_t t = a; t < e; t++) {
+                const char* src = pin + t * P;
+                const size_t i = (size_t)i0 + t;
+                char* rec = base + i * stride;
+                for (const RecMember& m : tab) {
+                    const size_t len = (m.kind == 1) ? 4 : 8 * (size_t)m.nc;
+                    std::memcpy(rec + m.off, src + m.pk, len);
+                }
+                double x[3];
+                for (int q = 0; q < 3; q++) x[q] = c->x_tracked ? c->h_x[i * 3 + q] : 0.0;
+                if (moved) {
+                    const int ty = c->h_type[i], ma = c->h_matype.empty() ? 0 : c->h_matype[i];
+                    if (ty != 0 || ma == 2 || ma == 3 || ma == 4 || ma == 5)
+                        std::memcpy(x, rec + 24, sizeof(double) * nd);
+                }
+                std::memcpy(rec, x, 24);
+            }
+        });
+    };
+    int k = 0, prev_i0 = -1, prev_cnt = 0, prev_b = 0;
+    for (int i0 = 0; i0 < n; i0 += kRecChunk, k++) {
+        const int b = k & 1, cnt = std::min(kRecChunk, n - i0);
+        k_rec_pack<<<(cnt + 255) / 256, 256, 0, c->st>>>(static_cast<char*>(c->rec_dev[b]), P, i0, cnt, c->N, dtab[b],
+                                                         (int)tab.size());
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(c->rec_pinned[b], c->rec_dev[b], (size_t)cnt * P, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaEventRecord(c->rec_ev[b], c->st));
+        if (prev_i0 >= 0) {
+            CK(cudaEventSynchronize(c->rec_ev[prev_b]));
+            scatter(prev_i0, prev_cnt, static_cast<const char*>(c->rec_pinned[prev_b]));
+        }
+        prev_i0 = i0; prev_cnt = cnt; prev_b = b;
+    }
+    if (prev_i0 >= 0) {
+        CK(cudaEventSynchronize(c->rec_ev[prev_b]));
+        scatter(prev_i0, prev_cnt, static_cast<const char*>(c->rec_pinned[prev_b]));
     }
     return 0;
 }

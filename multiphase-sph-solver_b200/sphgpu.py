@@ -113,6 +113,29 @@ FIELDS = {
 }
 INT_FIELDS = {"type", "matype", "permtype", "etype"}
 
+PARTICLE_BYTES = 1064  # sizeof(Particle) of the reference (Class_particle.h)
+
+
+def particle_records(fields: dict, n: int, stride: int = PARTICLE_BYTES) -> np.ndarray:
+    """Particle records (n x stride bytes, zero elsewhere) holding `fields`
+    at the offsets sphgpu_particle_layout reports, as the reference's own
+    Particle array would hold them."""
+    lib = load_library()
+    buf = np.zeros(n * stride, np.uint8)
+    for name, v in fields.items():
+        if name not in FIELDS:
+            continue
+        off, nc = C.c_size_t(), C.c_int()
+        if lib.sphgpu_particle_layout(name.encode(), C.byref(off), C.byref(nc)) != 0:
+            continue
+        dt = np.int32 if name in INT_FIELDS else np.float64
+        a = np.ascontiguousarray(np.asarray(v, dtype=dt).reshape(n, nc.value))
+        view = np.lib.stride_tricks.as_strided(buf[off.value:], shape=(n, a.itemsize * nc.value),
+                                               strides=(stride, 1))
+        view[:] = a.view(np.uint8).reshape(n, a.itemsize * nc.value)
+    return buf
+
+
 PREC_FP64 = 0          # SPHGPU_PREC_FP64
 PREC_FP32_BULK = 1     # SPHGPU_PREC_FP32_BULK
 
@@ -187,6 +210,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_get_field.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t]
     lib.sphgpu_set_materials.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
     lib.sphgpu_upload_particles.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_size_t]
+    lib.sphgpu_particle_layout.argtypes = [C.c_char_p, C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
     lib.sphgpu_download_particles.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_size_t]
     lib.sphgpu_step.argtypes = [C.c_void_p, C.c_int]
     lib.sphgpu_nnps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
@@ -263,6 +287,14 @@ class Engine:
         fp = _ptr(np.ascontiguousarray(fluid)) if fluid is not None else None
         sp = _ptr(np.ascontiguousarray(soil)) if soil is not None else None
         self._check(self.lib.sphgpu_set_materials(self.h, fp, sp, self.n), "set_materials")
+
+    def upload_particles(self, records: np.ndarray, stride: int = PARTICLE_BYTES) -> None:
+        """sphgpu_upload_particles: whole Particle records (n x stride bytes)."""
+        self._check(self.lib.sphgpu_upload_particles(self.h, _ptr(records), self.n, stride), "upload_particles")
+
+    def download_particles(self, records: np.ndarray, stride: int = PARTICLE_BYTES) -> None:
+        """sphgpu_download_particles: the device-owned members of each record."""
+        self._check(self.lib.sphgpu_download_particles(self.h, _ptr(records), self.n, stride), "download_particles")
 
     def load_state(self, fields: dict, fluid=None, soil=None) -> None:
         for name, v in fields.items():
