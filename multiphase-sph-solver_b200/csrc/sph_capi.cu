@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -16,6 +17,7 @@
 #include <string>
 #include <functional>
 #include <thread>
+#include <utility>
 #include <vector>
 
 #include "../../include/sphgpu.h"
@@ -88,6 +90,23 @@ constexpr size_t kParticleBytes = 1064;
 
 }  // namespace
 
+// An allocator whose elements start uninitialised: a resize of a large host
+// array then leaves its pages untouched until the copy that fills it, which
+// runs on several threads (zero-filling first would cost a single-threaded
+// pass over the whole array)
+template <typename T>
+struct UninitAlloc {
+    typedef T value_type;
+    UninitAlloc() = default;
+    template <typename U> UninitAlloc(const UninitAlloc<U>&) {}
+    T* allocate(size_t n) { return static_cast<T*>(::operator new(n * sizeof(T))); }
+    void deallocate(T* p, size_t) { ::operator delete(p); }
+    template <typename U> void construct(U*) {}
+    template <typename U, typename... A> void construct(U* p, A&&... a) { ::new ((void*)p) U(std::forward<A>(a)...); }
+    template <typename U> bool operator==(const UninitAlloc<U>&) const { return true; }
+    template <typename U> bool operator!=(const UninitAlloc<U>&) const { return false; }
+};
+
 struct sphgpu_ctx {
     sphgpu_params P;
     int device = 0;
@@ -118,8 +137,8 @@ struct sphgpu_ctx {
     cudaEvent_t rec_ev[2] = {nullptr, nullptr};
     bool regu = false;     // graphs include the strain/stress regularisation passes
     int precision = SPHGPU_PREC_FP64;
-    std::vector<sphgpu_fluid> h_fluid;   // the material records last set (K-L fields rewrite members)
-    std::vector<sphgpu_soil> h_soil;
+    std::vector<sphgpu_fluid, UninitAlloc<sphgpu_fluid>> h_fluid;   // the material records last set
+    std::vector<sphgpu_soil, UninitAlloc<sphgpu_soil>> h_soil;      // (K-L fields rewrite members)
 };
 
 namespace {
@@ -276,6 +295,139 @@ int check_particles(sphgpu_ctx* c)
     // those models and the saturation pass read material members that
     // sphgpu_set_materials uploads once it has seen them in use
     if (ext && !c->d[0].s.s_ext) return SPHGPU_E_STATE;
+    return 0;
+}
+
+}  // namespace
+
+namespace {
+
+// One device-owned Particle member in the record transfer: its byte offset
+// in the caller's record, its components, where it lives on the device
+// (kind 0: doubles, component-major; 1: int; 2: x, y, z of the position
+// records xh; 3: h of xh) and its byte offset in the packed download record.
+struct RecMember {
+    int off, nc, kind, pk;
+    void* dst;
+};
+constexpr int kMaxRecMembers = 48;
+constexpr int kRecChunk = 65536;          // records per staged chunk
+
+// caller records -> SoA state, one thread per record of the chunk
+__global__ void k_rec_unpack(const char* recs, size_t stride, int i0, int cnt, int N, const RecMember* tab, int nt)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= cnt) return;
+    const char* r = recs + (size_t)t * stride;
+    const size_t i = (size_t)i0 + t;
+    for (int m = 0; m < nt; m++) {
+        const RecMember e = tab[m];
+        const double* v = reinterpret_cast<const double*>(r + e.off);
+        if (e.kind == 0) {
+            for (int k = 0; k < e.nc; k++) static_cast<double*>(e.dst)[(size_t)k * N + i] = v[k];
+        } else if (e.kind == 1) {
+            static_cast<int*>(e.dst)[i] = *reinterpret_cast<const int*>(r + e.off);
+        } else if (e.kind == 2) {
+            for (int k = 0; k < 3; k++) static_cast<double*>(e.dst)[i * 4 + k] = v[k];
+        } else {
+            static_cast<double*>(e.dst)[i * 4 + 3] = v[0];
+        }
+    }
+}
+
+// SoA state -> packed records of the owned members (P bytes each)
+__global__ void k_rec_pack(char* out, size_t P, int i0, int cnt, int N, const RecMember* tab, int nt)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= cnt) return;
+    char* r = out + (size_t)t * P;
+    const size_t i = (size_t)i0 + t;
+    for (int m = 0; m < nt; m++) {
+        const RecMember e = tab[m];
+        double* v = reinterpret_cast<double*>(r + e.pk);
+        if (e.kind == 0) {
+            for (int k = 0; k < e.nc; k++) v[k] = static_cast<const double*>(e.dst)[(size_t)k * N + i];
+        } else if (e.kind == 1) {
+            *reinterpret_cast<int*>(r + e.pk) = static_cast<const int*>(e.dst)[i];
+        } else if (e.kind == 2) {
+            for (int k = 0; k < 3; k++) v[k] = static_cast<const double*>(e.dst)[i * 4 + k];
+        } else {
+            v[0] = static_cast<const double*>(e.dst)[i * 4 + 3];
+        }
+    }
+}
+
+// the table of device-owned members (all but x, which the host keeps) for
+// the current parity, and the packed record size
+int rec_table(sphgpu_ctx* c, std::vector<RecMember>& tab, size_t* packed)
+{
+    tab.clear();
+    size_t pk = 0;
+    for (const AosMember& m : kAos) {
+        if (std::strcmp(m.name, "x") == 0) continue;
+        const FieldDef* f = find_field(m.name);
+        RecMember e;
+        e.off = (int)m.off;
+        e.nc = f->ncomp;
+        e.pk = (int)pk;
+        if (std::strcmp(m.name, "xp") == 0) { e.kind = 2; e.dst = c->d[c->parity].s.xh; }
+        else if (std::strcmp(m.name, "hl") == 0) { e.kind = 3; e.dst = c->d[c->parity].s.xh; }
+        else { e.kind = f->is_int ? 1 : 0; e.dst = field_ptr(c, m.name); }
+        if (!e.dst) return SPHGPU_E_ARG;
+        pk += f->is_int ? 8 : 8 * (size_t)f->ncomp;   // ints keep an 8-byte slot
+        tab.push_back(e);
+    }
+    if ((int)tab.size() > kMaxRecMembers) return SPHGPU_E_ARG;
+    *packed = pk;
+    return 0;
+}
+
+int ensure_rec_staging(sphgpu_ctx* c, size_t bytes)
+{
+    if (c->rec_bytes >= bytes) return 0;
+    for (int b = 0; b < 2; b++) {
+        if (c->rec_pinned[b]) cudaFreeHost(c->rec_pinned[b]);
+        if (c->rec_dev[b]) cudaFree(c->rec_dev[b]);
+        c->rec_pinned[b] = c->rec_dev[b] = nullptr;
+    }
+    c->rec_bytes = 0;
+    for (int b = 0; b < 2; b++) {
+        CK(cudaMallocHost(&c->rec_pinned[b], bytes));
+        CK(cudaMalloc(&c->rec_dev[b], bytes + sizeof(RecMember) * kMaxRecMembers));
+        if (!c->rec_ev[b]) CK(cudaEventCreateWithFlags(&c->rec_ev[b], cudaEventDisableTiming));
+    }
+    c->rec_bytes = bytes;
+    return 0;
+}
+
+// n caller records of `stride` bytes (8-byte aligned) -> the device arrays of
+// `tab`, in chunks: a chunk is copied into a pinned buffer on several host
+// threads while the previous one crosses PCIe and k_rec_unpack scatters it
+int push_records(sphgpu_ctx* c, const char* base, int n, size_t stride, const std::vector<RecMember>& tab)
+{
+    int r = ensure_rec_staging(c, std::max((size_t)kRecChunk * stride, c->rec_bytes));
+    if (r) return r;
+    CK(cudaStreamSynchronize(c->st));
+    RecMember* dtab[2];
+    for (int b = 0; b < 2; b++) {
+        dtab[b] = reinterpret_cast<RecMember*>(static_cast<char*>(c->rec_dev[b]) + c->rec_bytes);
+        CK(cudaMemcpy(dtab[b], tab.data(), sizeof(RecMember) * tab.size(), cudaMemcpyHostToDevice));
+    }
+    int k = 0;
+    for (int i0 = 0; i0 < n; i0 += kRecChunk, k++) {
+        const int b = k & 1, cnt = std::min(kRecChunk, n - i0);
+        if (k >= 2) CK(cudaEventSynchronize(c->rec_ev[b]));
+        char* pin = static_cast<char*>(c->rec_pinned[b]);
+        const char* src = base + (size_t)i0 * stride;
+        const size_t bytes = (size_t)cnt * stride;
+        par_for(bytes, [&](size_t a, size_t e) { std::memcpy(pin + a, src + a, e - a); });
+        CK(cudaMemcpyAsync(c->rec_dev[b], pin, bytes, cudaMemcpyHostToDevice, c->st));
+        k_rec_unpack<<<(cnt + 255) / 256, 256, 0, c->st>>>(static_cast<const char*>(c->rec_dev[b]), stride, i0, cnt,
+                                                           c->N, dtab[b], (int)tab.size());
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(c->rec_ev[b], c->st));
+    }
+    CK(cudaStreamSynchronize(c->st));
     return 0;
 }
 
@@ -598,53 +750,61 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
 {
     if (!c || n != c->N) return SPHGPU_E_ARG;
     cudaSetDevice(c->device);
-    if (fl && fl != c->h_fluid.data()) c->h_fluid.assign(fl, fl + n);
-    if (so && so != c->h_soil.data()) c->h_soil.assign(so, so + n);
+    // the host copies (K-L fields rewrite members of them and upload them
+    // again), copied on all cores; the device arrays come from these aligned
+    // copies through the record pipeline of sphgpu_upload_particles
+    if (fl && fl != c->h_fluid.data()) {
+        c->h_fluid.resize(n);
+        char* dst = reinterpret_cast<char*>(c->h_fluid.data());
+        const char* src = reinterpret_cast<const char*>(fl);
+        par_for(sizeof(sphgpu_fluid) * n, [&](size_t a, size_t e) { std::memcpy(dst + a, src + a, e - a); });
+    }
+    if (so && so != c->h_soil.data()) {
+        c->h_soil.resize(n);
+        char* dst = reinterpret_cast<char*>(c->h_soil.data());
+        const char* src = reinterpret_cast<const char*>(so);
+        par_for(sizeof(sphgpu_soil) * n, [&](size_t a, size_t e) { std::memcpy(dst + a, src + a, e - a); });
+    }
+    if (fl) fl = c->h_fluid.data();
+    if (so) so = c->h_soil.data();
     const int N = c->N;
     DevState& s = c->d[0].s;
-    std::vector<double> buf((size_t)N);
-    std::vector<int> ibuf((size_t)N);
+    std::vector<double, UninitAlloc<double>> buf((size_t)N);
     auto put = [&](double* dst) -> int {
         CK(cudaMemcpyAsync(dst, buf.data(), sizeof(double) * N, cudaMemcpyHostToDevice, c->st));
         CK(cudaStreamSynchronize(c->st));
         return 0;
     };
+    auto m = [](size_t off, void* dst, int kind = 0) { return RecMember{(int)off, 1, kind, 0, dst}; };
     int r = 0;
     if (fl) {
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = fl[i].dens; }); r |= put(s.f_dens);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = fl[i].porosity; }); r |= put(s.f_por);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = fl[i].vpu; }); r |= put(s.f_vpu);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = fl[i].vis; }); r |= put(s.f_vis);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = fl[i].c; }); r |= put(s.f_c);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = fl[i].strain_min; }); r |= put(s.f_smin);
+        const std::vector<RecMember> tab = {
+            m(offsetof(sphgpu_fluid, dens), s.f_dens), m(offsetof(sphgpu_fluid, porosity), s.f_por),
+            m(offsetof(sphgpu_fluid, vpu), s.f_vpu), m(offsetof(sphgpu_fluid, vis), s.f_vis),
+            m(offsetof(sphgpu_fluid, c), s.f_c), m(offsetof(sphgpu_fluid, strain_min), s.f_smin),
+            m(offsetof(sphgpu_fluid, bhtype), s.f_bhtype, 1)};
+        r = push_records(c, reinterpret_cast<const char*>(fl), N, sizeof(sphgpu_fluid), tab);
+        if (r) return r;
         // Bingham friction: tan of the angle, CPP_7-2-constitutive.cpp:42-43
         par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = std::tan(fl[i].fai * 0.0174532925199); }); r |= put(s.f_tanfai);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) ibuf[i] = fl[i].bhtype; });
-        CK(cudaMemcpyAsync(s.f_bhtype, ibuf.data(), sizeof(int) * N, cudaMemcpyHostToDevice, c->st));
-        CK(cudaStreamSynchronize(c->st));
     }
     if (so) {
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].e; }); r |= put(s.s_e);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].poi; }); r |= put(s.s_poi);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].eps0; }); r |= put(s.s_eps0);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].dens; }); r |= put(s.s_dens);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].kapa; }); r |= put(s.s_kapa);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].porosity; }); r |= put(s.s_por);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].vpu; }); r |= put(s.s_vpu);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].cop; }); r |= put(s.s_cop);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].sitas; }); r |= put(s.s_sitas);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].sitar; }); r |= put(s.s_sitar);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].ds; }); r |= put(s.s_ds);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].c; }); r |= put(s.s_c);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].fs; }); r |= put(s.s_fs);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].ann; }); r |= put(s.s_ann);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].zmf; }); r |= put(s.s_zmf);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].ramda; }); r |= put(s.s_ramda);
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = so[i].sme0; }); r |= put(s.s_sme0);
+        const std::vector<RecMember> tab = {
+            m(offsetof(sphgpu_soil, e), s.s_e), m(offsetof(sphgpu_soil, poi), s.s_poi),
+            m(offsetof(sphgpu_soil, eps0), s.s_eps0), m(offsetof(sphgpu_soil, dens), s.s_dens),
+            m(offsetof(sphgpu_soil, kapa), s.s_kapa), m(offsetof(sphgpu_soil, porosity), s.s_por),
+            m(offsetof(sphgpu_soil, vpu), s.s_vpu), m(offsetof(sphgpu_soil, cop), s.s_cop),
+            m(offsetof(sphgpu_soil, sitas), s.s_sitas), m(offsetof(sphgpu_soil, sitar), s.s_sitar),
+            m(offsetof(sphgpu_soil, ds), s.s_ds), m(offsetof(sphgpu_soil, c), s.s_c),
+            m(offsetof(sphgpu_soil, fs), s.s_fs), m(offsetof(sphgpu_soil, ann), s.s_ann),
+            m(offsetof(sphgpu_soil, zmf), s.s_zmf), m(offsetof(sphgpu_soil, ramda), s.s_ramda),
+            m(offsetof(sphgpu_soil, sme0), s.s_sme0)};
+        r = push_records(c, reinterpret_cast<const char*>(so), N, sizeof(sphgpu_soil), tab);
+        if (r) return r;
         // Drucker-Prager cone constants with the reference's own libm calls
         // (dpmodel1 / dpmodel_bui / DPModel_check, CPP_8-1-consfactor.cpp:294-349,
         // 461-529, 783-803); they depend only on the material record.
-        std::vector<double> ya(N), yk(N), yd(N);
+        std::vector<double, UninitAlloc<double>> ya(N), yk(N), yd(N);
         par_for(N, [&](size_t a, size_t b) {
         for (size_t i = a; i < b; i++) {
             const double fai = std::atan(std::tan(so[i].fai * 0.0174532925166667) / so[i].fs);
@@ -676,12 +836,14 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
         }
         if (s.s_ext) {
             std::vector<double> ext((size_t)SX_COUNT * N);
-            for (int i = 0; i < N; i++) {
-                const sphgpu_soil& m = so[i];
-                const double v[SX_COUNT] = {m.epss, m.epsr, m.bnn, m.beta, m.sd, m.sw, m.c1, m.c2,
-                                            m.g0, m.etao, m.zet, m.damp1, m.damp2, std::pow(m.c, 4)};
-                for (int k = 0; k < SX_COUNT; k++) ext[(size_t)k * N + i] = v[k];
-            }
+            par_for(N, [&](size_t a, size_t b) {
+                for (size_t i = a; i < b; i++) {
+                    const sphgpu_soil& q = so[i];
+                    const double v[SX_COUNT] = {q.epss, q.epsr, q.bnn, q.beta, q.sd, q.sw, q.c1, q.c2,
+                                                q.g0, q.etao, q.zet, q.damp1, q.damp2, std::pow(q.c, 4)};
+                    for (int k = 0; k < SX_COUNT; k++) ext[(size_t)k * N + i] = v[k];
+                }
+            });
             CK(cudaMemcpyAsync(s.s_ext, ext.data(), sizeof(double) * ext.size(), cudaMemcpyHostToDevice, c->st));
             CK(cudaStreamSynchronize(c->st));
         }
@@ -700,112 +862,6 @@ int sphgpu_particle_layout(const char* name, size_t* offset, int* ncomp)
         }
     return SPHGPU_E_ARG;
 }
-
-}  // extern "C"
-
-namespace {
-
-// One device-owned Particle member in the record transfer: its byte offset
-// in the caller's record, its components, where it lives on the device
-// (kind 0: doubles, component-major; 1: int; 2: x, y, z of the position
-// records xh; 3: h of xh) and its byte offset in the packed download record.
-struct RecMember {
-    int off, nc, kind, pk;
-    void* dst;
-};
-constexpr int kMaxRecMembers = 48;
-constexpr int kRecChunk = 65536;          // records per staged chunk
-
-// caller records -> SoA state, one thread per record of the chunk
-__global__ void k_rec_unpack(const char* recs, size_t stride, int i0, int cnt, int N, const RecMember* tab, int nt)
-{
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= cnt) return;
-    const char* r = recs + (size_t)t * stride;
-    const size_t i = (size_t)i0 + t;
-    for (int m = 0; m < nt; m++) {
-        const RecMember e = tab[m];
-        const double* v = reinterpret_cast<const double*>(r + e.off);
-        if (e.kind == 0) {
-            for (int k = 0; k < e.nc; k++) static_cast<double*>(e.dst)[(size_t)k * N + i] = v[k];
-        } else if (e.kind == 1) {
-            static_cast<int*>(e.dst)[i] = *reinterpret_cast<const int*>(r + e.off);
-        } else if (e.kind == 2) {
-            for (int k = 0; k < 3; k++) static_cast<double*>(e.dst)[i * 4 + k] = v[k];
-        } else {
-            static_cast<double*>(e.dst)[i * 4 + 3] = v[0];
-        }
-    }
-}
-
-// SoA state -> packed records of the owned members (P bytes each)
-__global__ void k_rec_pack(char* out, size_t P, int i0, int cnt, int N, const RecMember* tab, int nt)
-{
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= cnt) return;
-    char* r = out + (size_t)t * P;
-    const size_t i = (size_t)i0 + t;
-    for (int m = 0; m < nt; m++) {
-        const RecMember e = tab[m];
-        double* v = reinterpret_cast<double*>(r + e.pk);
-        if (e.kind == 0) {
-            for (int k = 0; k < e.nc; k++) v[k] = static_cast<const double*>(e.dst)[(size_t)k * N + i];
-        } else if (e.kind == 1) {
-            *reinterpret_cast<int*>(r + e.pk) = static_cast<const int*>(e.dst)[i];
-        } else if (e.kind == 2) {
-            for (int k = 0; k < 3; k++) v[k] = static_cast<const double*>(e.dst)[i * 4 + k];
-        } else {
-            v[0] = static_cast<const double*>(e.dst)[i * 4 + 3];
-        }
-    }
-}
-
-// the table of device-owned members (all but x, which the host keeps) for
-// the current parity, and the packed record size
-int rec_table(sphgpu_ctx* c, std::vector<RecMember>& tab, size_t* packed)
-{
-    tab.clear();
-    size_t pk = 0;
-    for (const AosMember& m : kAos) {
-        if (std::strcmp(m.name, "x") == 0) continue;
-        const FieldDef* f = find_field(m.name);
-        RecMember e;
-        e.off = (int)m.off;
-        e.nc = f->ncomp;
-        e.pk = (int)pk;
-        if (std::strcmp(m.name, "xp") == 0) { e.kind = 2; e.dst = c->d[c->parity].s.xh; }
-        else if (std::strcmp(m.name, "hl") == 0) { e.kind = 3; e.dst = c->d[c->parity].s.xh; }
-        else { e.kind = f->is_int ? 1 : 0; e.dst = field_ptr(c, m.name); }
-        if (!e.dst) return SPHGPU_E_ARG;
-        pk += f->is_int ? 8 : 8 * (size_t)f->ncomp;   // ints keep an 8-byte slot
-        tab.push_back(e);
-    }
-    if ((int)tab.size() > kMaxRecMembers) return SPHGPU_E_ARG;
-    *packed = pk;
-    return 0;
-}
-
-int ensure_rec_staging(sphgpu_ctx* c, size_t bytes)
-{
-    if (c->rec_bytes >= bytes) return 0;
-    for (int b = 0; b < 2; b++) {
-        if (c->rec_pinned[b]) cudaFreeHost(c->rec_pinned[b]);
-        if (c->rec_dev[b]) cudaFree(c->rec_dev[b]);
-        c->rec_pinned[b] = c->rec_dev[b] = nullptr;
-    }
-    c->rec_bytes = 0;
-    for (int b = 0; b < 2; b++) {
-        CK(cudaMallocHost(&c->rec_pinned[b], bytes));
-        CK(cudaMalloc(&c->rec_dev[b], bytes + sizeof(RecMember) * kMaxRecMembers));
-        if (!c->rec_ev[b]) CK(cudaEventCreateWithFlags(&c->rec_ev[b], cudaEventDisableTiming));
-    }
-    c->rec_bytes = bytes;
-    return 0;
-}
-
-}  // namespace
-
-extern "C" {
 
 // Records are moved in chunks through two pinned and two device buffers: the
 // host copies a chunk of whole records (on several threads) while the
@@ -865,9 +921,6 @@ int sphgpu_upload_particles(sphgpu_ctx* c, const void* particles, int n, size_t 
     size_t P = 0;
     int r = rec_table(c, tab, &P);
     if (r) return r;
-    const size_t chunk_bytes = (size_t)kRecChunk * stride;
-    r = ensure_rec_staging(c, std::max(chunk_bytes, (size_t)kRecChunk * P));
-    if (r) return r;
     // the host copies of x, type and matype
     c->h_x.resize((size_t)n * 3);
     c->h_type.resize(n);
@@ -881,27 +934,8 @@ int sphgpu_upload_particles(sphgpu_ctx* c, const void* particles, int n, size_t 
         }
     });
     c->x_tracked = true;
-    CK(cudaStreamSynchronize(c->st));
-    RecMember* dtab[2];
-    for (int b = 0; b < 2; b++) {
-        dtab[b] = reinterpret_cast<RecMember*>(static_cast<char*>(c->rec_dev[b]) + c->rec_bytes);
-        CK(cudaMemcpy(dtab[b], tab.data(), sizeof(RecMember) * tab.size(), cudaMemcpyHostToDevice));
-    }
-    int k = 0;
-    for (int i0 = 0; i0 < n; i0 += kRecChunk, k++) {
-        const int b = k & 1, cnt = std::min(kRecChunk, n - i0);
-        if (k >= 2) CK(cudaEventSynchronize(c->rec_ev[b]));
-        char* pin = static_cast<char*>(c->rec_pinned[b]);
-        const char* src = base + (size_t)i0 * stride;
-        const size_t bytes = (size_t)cnt * stride;
-        par_for(bytes, [&](size_t a, size_t e) { std::memcpy(pin + a, src + a, e - a); });
-        CK(cudaMemcpyAsync(c->rec_dev[b], pin, bytes, cudaMemcpyHostToDevice, c->st));
-        k_rec_unpack<<<(cnt + 255) / 256, 256, 0, c->st>>>(static_cast<const char*>(c->rec_dev[b]), stride, i0, cnt,
-                                                           c->N, dtab[b], (int)tab.size());
-        CK(cudaGetLastError());
-        CK(cudaEventRecord(c->rec_ev[b], c->st));
-    }
-    CK(cudaStreamSynchronize(c->st));
+    r = push_records(c, base, n, stride, tab);
+    if (r) return r;
     update_static_params(c);
     return 0;
 }
