@@ -59,10 +59,11 @@ def algorithmic_bytes(stage: str, nb: float = NB_MEAN, rec_bytes: float = 32.0) 
         # reads | writes
         "k_cellkey": 32 + 12,                                   # (x,y,z,h) | cell, key, value
         "radix_sort": 3 * 16,                                   # 3 digit passes of (key, value) in + out
-        "k_cellrange": 4 + 4 + 32 + 32 + 16 + 8,                # key, pid, record | sorted FP64 + FP32 records, range
-        "k_nnps": 32 + 4 + 4 + 4 + row,                         # record, cell, type | count, list row
+        "k_cellrange": 4 + 4 + 4 + 32 + 32 + 16 + 4 + 4 + 8,    # key, pid, type, record | sorted FP64 + FP32 records, word, position, range
+        "k_nnps": 16 + 4 + 4 + 4 + 4 + row,                     # FP32 record, cell, pid, type | count, provisional row
+        "k_nnps_resolve": 4 + 4 + 4 + 32 + row + 4 + row + 80,  # type, position, count, record, provisional row
+                                                                # | count, list row, five two-word type masks
         "k_pairw": 32 + 4 + row + rec,                          # record, count, list row | pair records
-        "k_slotmask": 4 + row + 80,                             # count, list row | five two-word type masks
         "k_density": 4 + 4 + 32 + 8 + 8 + 8 + 24 + 8 + row + rec + 8 + 16,
         "k_shepard_eos": 4 + 4 + 32 + 8 + 8 + 8 + 8 + row + rec + 8 + 8,
         "k_strain": 4 + 4 + 32 + 24 + row + rec + 48 + 48 + 8 + 16,

@@ -169,6 +169,8 @@ int check_params(const sphgpu_params* P)
     if (!P) return SPHGPU_E_ARG;
     if (P->ndim != 2 && P->ndim != 3) return SPHGPU_E_ARG;
     if (P->ntotal <= 0 || P->ctotal <= 0 || P->cxm <= 0 || P->cym <= 0 || P->czm <= 0) return SPHGPU_E_ARG;
+    // the search packs a particle index and its type code into one 32-bit word
+    if (P->ntotal >= (1 << 28)) return SPHGPU_E_UNSUPPORTED;
     if ((long long)P->cxm * P->cym * P->czm != P->ctotal) return SPHGPU_E_ARG;
     if (!(P->dr > 0.0) || !(P->dt > 0.0)) return SPHGPU_E_ARG;
     if (P->step_regu <= 0) return SPHGPU_E_ARG;
@@ -556,6 +558,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.val_in, N); r |= dalloc(c, &s.pid_sorted, N);
     r |= dalloc(c, &s.cstart, M); r |= dalloc(c, &s.cend, M);
     r |= dalloc(c, &s.nnb, N); r |= dalloc(c, &s.nbr, (size_t)SPH_NB_CAP * N);
+    r |= dalloc(c, &s.nps, N); r |= dalloc(c, &s.sortpos, N); r |= dalloc(c, &s.pts, N); r |= dalloc(c, &s.nbrs, (size_t)SPH_NB_CAP * N);
     r |= dalloc(c, &s.nbm, 10 * (size_t)N);
     r |= dalloc(c, &s.nbw, 4 * (size_t)SPH_NB_CAP * N);
     r |= dalloc(c, &s.err, 1); r |= dalloc(c, &s.step, 1);

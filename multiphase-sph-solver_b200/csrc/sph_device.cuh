@@ -134,9 +134,15 @@ struct DevState {
     int *val_in, *pid_sorted;
     int *cstart, *cend;        // [ctotal + 4]
     int *nnb;                  // neighbour count (may exceed the cap: error 5)
+    // the neighbour search by cell-sorted position q: pts[q] = the particle
+    // index << 3 | its type code (the type for types 0-4, else 7); the scan's
+    // provisional count (-1: the particle takes the direct FP64 search) and
+    // provisional list nbrs[s * N + q] of candidates' pts words (~word for a
+    // candidate within the FP32 margin of the radius); sortpos[i] = q
+    int *nps, *nbrs, *sortpos, *pts;
     // per particle and particle type t = 0..4, bit s set when list slot s
     // holds a particle of type t: nbm[(2 t + w) * N + i], word w = 0 for
-    // slots 0-63, 1 for slots 64-98 (written by k_slotmask after the search)
+    // slots 0-63, 1 for slots 64-98 (written by the search with the list)
     unsigned long long* nbm;
     int *nbr;                  // [SPH_NB_CAP * N]
     double *nbw;               // pair records (grad W, W) of the neighbour-list slots, [SPH_NB_CAP * N]

@@ -9,7 +9,8 @@
 //   radix sort     Binary_Sort's order: cell ascending, index descending
 //   k_cellreset    cell_info reset                              (CPP_3-NNPS.cpp:196-201)
 //   k_cellrange    cell_info start/end (:621-629) + the cell-sorted copy of positions
-//   k_nnps         partisearching: stencil scan, FP64 distance test, neighbour list
+//   k_nnps         partisearching: stencil scan in cell-sorted order, FP32 prefilter
+//   k_nnps_resolve FP64 decisions of the undecided candidates, neighbour list, slot masks
 //   k_density      fluid porosity + continuity                  (CPP_6-density.cpp:25-165)
 //   k_shepard_eos  Shepard filter (Jacobi) + local EOS          (CPP_6-density.cpp:168-188, CPP_7-1-eos_CR.cpp:22-43)
 //   k_strain       velocity gradient, strain rate and spin, gathered pore pressures and
@@ -261,7 +262,11 @@ __global__ void k_cellrange(Dev d)
         if (first) d.s.cstart[c] = q;
         if (last) d.s.cend[c] = q;
     }
-    const Pos r = load_pos(d.s.xh, d.s.pid_sorted[q]);
+    const int pid = d.s.pid_sorted[q];
+    d.s.sortpos[pid] = q;
+    const int t = d.s.type[pid];
+    d.s.pts[q] = (pid << 3) | ((t >= 0 && t <= 4) ? t : 7);
+    const Pos r = load_pos(d.s.xh, pid);
     store_pos(d.s.xs, q, r);
     reinterpret_cast<float4*>(d.s.xsf)[q] =
         make_float4((float)(r.x - d.p.xmin), (float)(r.y - d.p.ymin), (float)(r.z - d.p.zmin), (float)r.h);
@@ -432,85 +437,103 @@ __device__ __forceinline__ int nnps_direct(const Dev& d, int i, int nc, const Po
 // d2f - T^2); the test requires h_i > 64 u F_i and otherwise takes every
 // candidate to the FP64 test.
 //
-// Two passes keep the FP64 work out of the candidate scan, where a lattice's
-// many candidates at exactly the support radius would stall the whole warp
-// on nearly every step: the scan stores, in candidate order, the sorted
-// position q of each candidate inside (q) or undecided (~q) into the
-// particle's list slots; the second pass walks that list, decides the
-// undecided ones in FP64 and compacts the list in place to particle indices.
-// The order, and so the list, is the one the single pass gives.  A
-// provisional list longer than the capacity (possible only when undecided
-// candidates or the particle itself push it over) is redone by the direct
-// form, which also raises the reference's error for a true overflow.
+// Two passes.  The scan (k_nnps) runs one thread per cell-sorted position,
+// so the lanes of a warp belong to one or two cells, walk the same stencil
+// cells and load the same candidate records (one broadcast per load instead
+// of a line per lane).  It stores, in candidate order, the index-and-type
+// word w of each candidate inside (w) or undecided (~w) into the provisional
+// list of its own sorted position, nbrs[s * N + q], which the lanes of a warp
+// fill row by row.  The resolve pass (k_nnps_resolve) runs one thread per
+// particle in the caller's order: it reads its provisional list, decides the
+// undecided candidates in FP64, and writes the list nbr[s * N + i] and the
+// per-type slot masks.  The order, and so the
+// list, is the one a single pass in candidate order gives.  A provisional list
+// longer than the capacity (possible only when undecided candidates or the
+// particle itself push it over), and a particle the FP32 test does not apply
+// to, are searched again by the direct form, which also raises the
+// reference's error for a true overflow.
 template <int ND>
 __global__ void __launch_bounds__(128, SPH_MINB) k_nnps(Dev d)
 {
-    const int i = IDX, N = d.p.N;
-    if (i >= N || *d.s.err) return;
-    int cnt = 0;
-    if (d.s.type[i] != 7) {
+    const int q = IDX, N = d.p.N;
+    if (q >= N || *d.s.err) return;
+    int np = 0;   // provisional entries
+    if (d.s.type[d.s.pid_sorted[q]] != 7) {
         constexpr int nst = (ND == 2) ? 9 : 27;
         constexpr float U = 5.9604645e-8f;     // 2^-24
-        const int nc = d.s.cell[i];
-        const Pos pi = load_pos(d.s.xh, i);
-        const float fx = (float)(pi.x - d.p.xmin), fy = (float)(pi.y - d.p.ymin);
-        const float fz = (ND == 3) ? (float)(pi.z - d.p.zmin) : 0.f, fh = (float)pi.h;
-        float Fi = fmaxf(fabsf(fx), fabsf(fy));
+        const float4* xsf = reinterpret_cast<const float4*>(d.s.xsf);
+        const int nc = (int)d.s.key_out[q];
+        const float4 fi = xsf[q];              // the particle's own FP32 record
+        const float fz = (ND == 3) ? fi.z : 0.f;
+        float Fi = fmaxf(fabsf(fi.x), fabsf(fi.y));
         if (ND == 3) Fi = fmaxf(Fi, fabsf(fz));
-        const bool fast = fh > 64.f * U * Fi;
-        const Prefilter P = make_prefilter<ND>(fx, fy, fz, fh, 2.2f * U * Fi, 32.f * U);
-        if (!fast) {
-            cnt = nnps_direct<ND>(d, i, nc, pi, false, P);
+        if (!(fi.w > 64.f * U * Fi)) {
+            np = -1;
         } else {
-            const float4* xsf = reinterpret_cast<const float4*>(d.s.xsf);
-            int np = 0;   // provisional entries
+            const Prefilter P = make_prefilter<ND>(fi.x, fi.y, fz, fi.w, 2.2f * U * Fi, 32.f * U);
+            int* row = d.s.nbrs + q;
             for (int nj = 0; nj < nst; nj++) {
                 const int nl = cell_link(d.p, nc, nj);
                 if (nl <= 0) continue;
                 const int start = d.s.cstart[nl], end = d.s.cend[nl];
-                for (int q = start; q <= end; q++) {
-                    const int v = nnps_prefilter<ND>(P, xsf[q]);
+                for (int c = start; c <= end; c++) {
+                    const float4 fc = xsf[c];
+                    const int w = d.s.pts[c];
+                    const int v = nnps_prefilter<ND>(P, fc);
                     if (v != 0) {
-                        if (np < SPH_NB_CAP) d.s.nbr[(size_t)np * N + i] = (v > 0) ? q : ~q;
+                        if (np < SPH_NB_CAP) row[(size_t)np * N] = (v > 0) ? w : ~w;
                         np++;
-                    }
-                }
-            }
-            if (np > SPH_NB_CAP) {
-                cnt = nnps_direct<ND>(d, i, nc, pi, true, P);
-            } else {
-                const double xi[3] = {pi.x, pi.y, pi.z};
-                for (int s = 0; s < np; s++) {
-                    const int v = d.s.nbr[(size_t)s * N + i];
-                    const int q = (v < 0) ? ~v : v;
-                    const bool in = (v >= 0) || nnps_in_fp64<ND>(xi, pi.h, load_pos(d.s.xs, q));
-                    const int j = d.s.pid_sorted[q];
-                    if (in && j != i) {
-                        d.s.nbr[(size_t)cnt * N + i] = j;
-                        cnt++;
                     }
                 }
             }
         }
     }
-    d.s.nnb[i] = cnt;
+    d.s.nps[q] = np;
 }
 
-// The per-type slot masks of each particle's list (nbm), from the list and
-// the neighbours' types, with the list entries loaded two slots ahead and the
-// types one slot ahead
-__global__ void __launch_bounds__(256) k_slotmask(Dev d)
+// The resolve pass of the search (see k_nnps), one thread per particle, with
+// the per-type slot masks of the list written beside it.
+template <int ND>
+__global__ void __launch_bounds__(128, SPH_MINB) k_nnps_resolve(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
-    const int nn = nbr_count(d, i);
+    int cnt = 0;
     TypeMasks tm;
-    NbrIter it(d, i, nn);
-    for (int s = 0; s < nn; s++) {
-        int j, tj;
-        it.next(j, tj);
-        tm.add(tj, s);
+    if (d.s.type[i] != 7) {
+        const int q0 = d.s.sortpos[i];
+        const int np = d.s.nps[q0];
+        const Pos pi = load_pos(d.s.xh, i);
+        if (np < 0 || np > SPH_NB_CAP) {
+            constexpr float U = 5.9604645e-8f;     // 2^-24
+            const float4 fi = reinterpret_cast<const float4*>(d.s.xsf)[q0];
+            const float fz = (ND == 3) ? fi.z : 0.f;
+            float Fi = fmaxf(fabsf(fi.x), fabsf(fi.y));
+            if (ND == 3) Fi = fmaxf(Fi, fabsf(fz));
+            const Prefilter P = make_prefilter<ND>(fi.x, fi.y, fz, fi.w, 2.2f * U * Fi, 32.f * U);
+            cnt = nnps_direct<ND>(d, i, d.s.cell[i], pi, np >= 0, P);
+            const int nn = cnt < SPH_NB_CAP ? cnt : SPH_NB_CAP;
+            for (int s = 0; s < nn; s++) tm.add(d.s.type[d.s.nbr[(size_t)s * N + i]], s);
+        } else {
+            const double xi[3] = {pi.x, pi.y, pi.z};
+            const int* row = d.s.nbrs + q0;
+            // provisional entries two slots ahead
+            int v1 = (np > 0) ? row[0] : 0, v2 = (np > 1) ? row[N] : 0;
+            for (int s = 0; s < np; s++) {
+                const int v = v1;
+                v1 = v2;
+                if (s + 2 < np) v2 = row[(size_t)(s + 2) * N];
+                const int w = (v < 0) ? ~v : v, j = w >> 3;
+                const bool in = (v >= 0) || nnps_in_fp64<ND>(xi, pi.h, load_pos(d.s.xh, j));
+                if (in && j != i) {
+                    d.s.nbr[(size_t)cnt * N + i] = j;
+                    tm.add(w & 7, cnt);
+                    cnt++;
+                }
+            }
+        }
     }
+    d.s.nnb[i] = cnt;
     tm.store(d, i);
 }
 
@@ -2540,7 +2563,7 @@ extern "C" size_t sphk_sort_temp_bytes(int N, int end_bit)
 // before stage k and ev[SPHK_NSTAGES] after the last one (stages a run does
 // not need are recorded with no work between their events).
 extern "C" const char* const sphk_stage_names[] = {
-    "k_cellkey", "radix_sort", "k_cellreset", "k_cellrange", "k_nnps", "k_pairw", "k_slotmask", "k_kgc",
+    "k_cellkey", "radix_sort", "k_cellreset", "k_cellrange", "k_nnps", "k_nnps_resolve", "k_pairw", "k_kgc",
     "k_density", "k_shepard_eos", "k_strain", "k_regu_eps", "k_stress", "k_regu_sig", "k_stress_2",
     "k_art_rij", "k_accel_a", "k_accel_b", "k_xsph_update", "k_tm_boundary", "k_step_done"};
 static_assert(sizeof(sphk_stage_names) / sizeof(sphk_stage_names[0]) == SPHK_NSTAGES, "stage table");
@@ -2574,9 +2597,9 @@ extern "C" int sphk_enqueue_nnps(const Dev* dp, void* sort_tmp, size_t sort_byte
     REC(4);
     LAUNCH_ND(k_nnps, nblk(N, 128), 128, d); n++;
     REC(5);
-    LAUNCH_ND(k_pairw, nblk(N, 128), 128, d); n++;
+    LAUNCH_ND(k_nnps_resolve, nblk(N, 128), 128, d); n++;
     REC(6);
-    k_slotmask<<<nblk(N, 256), 256, 0, st>>>(d); n++;
+    LAUNCH_ND(k_pairw, nblk(N, 128), 128, d); n++;
     REC(7);
     if (d.p.flknl > 2) { LAUNCH_ND(k_kgc, nblk(N, 128), 128, d); n++; }
     return n;
