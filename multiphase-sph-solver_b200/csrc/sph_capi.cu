@@ -558,7 +558,8 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.val_in, N); r |= dalloc(c, &s.pid_sorted, N);
     r |= dalloc(c, &s.cstart, M); r |= dalloc(c, &s.cend, M);
     r |= dalloc(c, &s.nnb, N); r |= dalloc(c, &s.nbr, (size_t)SPH_NB_CAP * N);
-    r |= dalloc(c, &s.nps, N); r |= dalloc(c, &s.sortpos, N); r |= dalloc(c, &s.pts, N); r |= dalloc(c, &s.nbrs, (size_t)SPH_NB_CAP * N);
+    r |= dalloc(c, &s.nps, N); r |= dalloc(c, &s.sortpos, N); r |= dalloc(c, &s.pts, N);
+    r |= dalloc(c, &s.accb, 9 * (size_t)N); r |= dalloc(c, &s.nbrs, (size_t)SPH_NB_CAP * N);
     r |= dalloc(c, &s.nbm, 10 * (size_t)N);
     r |= dalloc(c, &s.nbw, 4 * (size_t)SPH_NB_CAP * N);
     r |= dalloc(c, &s.err, 1); r |= dalloc(c, &s.step, 1);

@@ -140,6 +140,9 @@ struct DevState {
     // provisional list nbrs[s * N + q] of candidates' pts words (~word for a
     // candidate within the FP32 margin of the radius); sortpos[i] = q
     int *nps, *nbrs, *sortpos, *pts;
+    // the momentum pass's artificial-viscosity, drag and damping sums, from
+    // its loop kernel to its tail kernel: accb[(3 g + k) * N + i] (9N)
+    double* accb;
     // per particle and particle type t = 0..4, bit s set when list slot s
     // holds a particle of type t: nbm[(2 t + w) * N + i], word w = 0 for
     // slots 0-63, 1 for slots 64-98 (written by the search with the list)

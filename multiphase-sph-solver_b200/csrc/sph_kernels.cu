@@ -69,10 +69,13 @@ namespace SPH_NS {
 #ifndef SPH_MINB_STRESS
 #define SPH_MINB_STRESS 2
 #endif
-// the momentum pass: its neighbour loops need about 100 registers, its
-// per-particle tail more; a cap of 96 (5 blocks per SM) spills only the tail
+// the momentum pass: its neighbour loops (k_accel_b) at 6 blocks per SM, its
+// per-particle tail (k_accel_b_tail) at 5
 #ifndef SPH_MINB_ACCB
 #define SPH_MINB_ACCB 5
+#endif
+#ifndef SPH_MINB_ACCB1
+#define SPH_MINB_ACCB1 6
 #endif
 // the same trade for the strain pass (96 registers, a few spills), the
 // density pass (72, none) and XSPH (72, a few); the stress-divergence pass
@@ -1368,8 +1371,8 @@ __device__ __noinline__ void wall_stress_rows(int i, int N, int nn, int ti, bool
 // Writes ax, interf, interfss and the updated velocity into vx_next (the
 // reference's vx before XSPH).  DRAG = 1 carries the interact2/3 drag
 // coefficient (fli 2, 3), whose out-of-line call the Darcy form does without.
-template <int ND, int ART = 0, int DRAG = 0>
-__global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b(Dev d)
+template <int ND, int DRAG = 0>
+__global__ void __launch_bounds__(128, SPH_MINB_ACCB1) k_accel_b(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
@@ -1380,32 +1383,20 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b(Dev d)
     const real riR = (real)ri;
     double vi[3];
     for (int k = 0; k < 3; k++) vi[k] = d.s.vxp[k * N + i];
-    const bool fluid = (ti == 1 || ti == 3);
     const bool solid = (ti == 2 || ti == 4);
-    const bool moving = (ti >= 1 && ti <= 4);
     Sum<real> tav[3], tin[3], tdm[3];
     const bool damping = (*d.s.step <= d.p.inip) && solid;
-    const bool art = ART && ti == 2;   // artificial stress (art_stre_coe > 0)
     const real cdi = damping ? (real)d.s.cd[i] : real(0);
     // artificial viscosity coefficients of particle i
     real ca = 0, aa = 0, bb = 0;
     if (ti == 1) { ca = (real)d.s.f_vpu[i]; aa = (real)d.p.av[0][0]; bb = (real)d.p.av[0][1]; }
     if (ti == 2) { ca = (real)d.s.s_vpu[i]; aa = (real)d.p.av[1][0]; bb = (real)d.p.av[1][1]; }
     if (ti == 3) { ca = (real)d.s.f_vpu[i]; aa = (real)d.p.av[2][0]; bb = (real)d.p.av[2][1]; }
-    // wall-stress operand of particle i (:668-700) and its own half
     const double satu_i = d.s.satu[i];
-    // flbndy 3/4/13/14: boundary_stress_effect_tran (CPP_9-4:725-846) takes the
-    // wall's stress for i's phase, and a structure particle's own stress
-    // without the pore terms
-    const bool tran = d.p.flbndy == 3 || d.p.flbndy == 4 || d.p.flbndy == 13 || d.p.flbndy == 14;
-    // boundary_effect_free_struct (CPP_9-4:900-990) for the other flbndy
-    // values: a fluid's mirrored stress has its shear components negated
-    const bool free_struct = !(tran || d.p.flbndy == 1 || d.p.flbndy == 2);
     // artificial viscosity and geostatic damping over i's own type's slots,
     // then the soil-water (soil-air) drag of interact1/2/3 over the slots of
     // the types it pairs (the reference visits every other pair of different
     // types too, but adds nothing for them); each sum in list order
-    const bool any_wall = type_mask(d, i, 0).any();
     {
         MaskIter it(d, i, (ti != 7) ? type_mask(d, i, ti) : SlotMask{0ull, 0ull});
         int q, j;
@@ -1487,6 +1478,52 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b(Dev d)
             }
         }
     }
+    for (int k = 0; k < 3; k++) {
+        d.s.accb[(size_t)k * N + i] = (double)tav[k].v();
+        d.s.accb[(size_t)(3 + k) * N + i] = (double)tin[k].v();
+        d.s.accb[(size_t)(6 + k) * N + i] = (double)tdm[k].v();
+    }
+}
+
+// The rest of the momentum pass, per particle: the wall stress and the
+// artificial-stress sums (each over the list in order), then the combination
+// with the sums of k_accel_b (accb) and k_accel_a in the reference's call
+// order, the velocity update and the writes of ax, interf, interfss and the
+// velocity before XSPH (vx_next).  In a kernel of its own so that the loops of
+// k_accel_b run under a smaller register budget than this straight-line code.
+template <int ND, int ART = 0>
+__global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b_tail(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    constexpr int nd = ND;
+    const int ti = d.s.type[i], nn = nbr_count(d, i);
+    const PairI<real> I = pair_i<ND, real>(d, i);
+    const double ri = d.s.rho[i];
+    double vi[3];
+    for (int k = 0; k < 3; k++) vi[k] = d.s.vxp[k * N + i];
+    const bool fluid = (ti == 1 || ti == 3);
+    const bool solid = (ti == 2 || ti == 4);
+    const bool moving = (ti >= 1 && ti <= 4);
+    const bool damping = (*d.s.step <= d.p.inip) && solid;
+    const bool art = ART && ti == 2;   // artificial stress (art_stre_coe > 0)
+    // wall-stress operand of particle i (:668-700) and its own half
+    const double satu_i = d.s.satu[i];
+    // flbndy 3/4/13/14: boundary_stress_effect_tran (CPP_9-4:725-846) takes the
+    // wall's stress for i's phase, and a structure particle's own stress
+    // without the pore terms
+    const bool tran = d.p.flbndy == 3 || d.p.flbndy == 4 || d.p.flbndy == 13 || d.p.flbndy == 14;
+    // boundary_effect_free_struct (CPP_9-4:900-990) for the other flbndy
+    // values: a fluid's mirrored stress has its shear components negated
+    const bool free_struct = !(tran || d.p.flbndy == 1 || d.p.flbndy == 2);
+    const bool any_wall = type_mask(d, i, 0).any();
+    // the artificial-viscosity, drag and damping sums of k_accel_b
+    double tav[3], tin[3], tdm[3];
+    for (int k = 0; k < 3; k++) {
+        tav[k] = d.s.accb[(size_t)k * N + i];
+        tin[k] = d.s.accb[(size_t)(3 + k) * N + i];
+        tdm[k] = d.s.accb[(size_t)(6 + k) * N + i];
+    }
     // the wall stress of moving particles with a wall in their list, out of
     // line (its nine sums take registers only there); each sum still runs
     // over the list in order
@@ -1535,7 +1572,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b(Dev d)
     double ax[3];
     for (int k = 0; k < 3; k++) ax[k] = d.s.ax[k * N + i];   // g + stress divergence (k_accel_a) or the old value
     if (ti != 7)
-        for (int k = 0; k < nd; k++) ax[k] = ax[k] - tav[k].v();
+        for (int k = 0; k < nd; k++) ax[k] = ax[k] - tav[k];
     if (art)
         for (int k = 0; k < nd; k++) ax[k] = ax[k] + tu[k].v();
     if (moving)
@@ -1548,7 +1585,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b(Dev d)
     if (d.p.fli >= 1 && moving) {
         const double xishu = d.p.interc;
         for (int k = 0; k < nd; k++) {
-            double itf = tin[k].v();
+            double itf = tin[k];
             double vx1 = vi[k] + 0.5 * (axp[k] + ax[k]) * dt;
             double vx2 = vi[k] + 0.5 * (axp[k] + ax[k] - itf * xishu / ri) * dt;
             if (vx1 * vx2 <= 0.0) {
@@ -1582,9 +1619,9 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b(Dev d)
     if (damping) {
         for (int k = 0; k < nd; k++) {
             double vx1 = vi[k] + 0.5 * (axp[k] + ax[k]) * dt;
-            double vx2 = vi[k] + 0.5 * (axp[k] + ax[k] - tdm[k].v()) * dt;
+            double vx2 = vi[k] + 0.5 * (axp[k] + ax[k] - tdm[k]) * dt;
             if (vx1 * vx2 <= 0.0) ax[k] = -2.0 * vi[k] / dt - axp[k];
-            else ax[k] -= tdm[k].v();
+            else ax[k] -= tdm[k];
         }
     }
     if (d.p.flbndy == 5 && d.s.fsol_on[i]) {
@@ -2654,21 +2691,21 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
     }
     REC(17);
     {
-        const int v = (art ? 1 : 0) + (d.p.fli > 1 ? 2 : 0);
+        const bool drag = d.p.fli > 1;
         const dim3 g(nblk(N, 128)), b(128);
         if (d.p.ndim == 2) {
-            if (v == 0) k_accel_b<2, 0, 0><<<g, b, 0, st>>>(d);
-            else if (v == 1) k_accel_b<2, 1, 0><<<g, b, 0, st>>>(d);
-            else if (v == 2) k_accel_b<2, 0, 1><<<g, b, 0, st>>>(d);
-            else k_accel_b<2, 1, 1><<<g, b, 0, st>>>(d);
+            if (drag) k_accel_b<2, 1><<<g, b, 0, st>>>(d);
+            else k_accel_b<2, 0><<<g, b, 0, st>>>(d);
+            if (art) k_accel_b_tail<2, 1><<<g, b, 0, st>>>(d);
+            else k_accel_b_tail<2, 0><<<g, b, 0, st>>>(d);
         } else {
-            if (v == 0) k_accel_b<3, 0, 0><<<g, b, 0, st>>>(d);
-            else if (v == 1) k_accel_b<3, 1, 0><<<g, b, 0, st>>>(d);
-            else if (v == 2) k_accel_b<3, 0, 1><<<g, b, 0, st>>>(d);
-            else k_accel_b<3, 1, 1><<<g, b, 0, st>>>(d);
+            if (drag) k_accel_b<3, 1><<<g, b, 0, st>>>(d);
+            else k_accel_b<3, 0><<<g, b, 0, st>>>(d);
+            if (art) k_accel_b_tail<3, 1><<<g, b, 0, st>>>(d);
+            else k_accel_b_tail<3, 0><<<g, b, 0, st>>>(d);
         }
     }
-    n++;
+    n += 2;
     REC(18);
     LAUNCH_ND(k_xsph_update, nblk(N, 128), 128, d); n++;
     REC(19);
