@@ -69,19 +69,23 @@ namespace SPH_NS {
 #ifndef SPH_MINB_STRESS
 #define SPH_MINB_STRESS 2
 #endif
-// the momentum pass: its neighbour loops (k_accel_b) at 6 blocks per SM, its
-// per-particle tail (k_accel_b_tail) at 5
+// the momentum pass: its neighbour loops (k_accel_b) at 7 blocks per SM
+// (72 registers, a few spills: faster than 6 or 5), its per-particle tail
+// (k_accel_b_tail) at 5 (faster than 4)
 #ifndef SPH_MINB_ACCB
 #define SPH_MINB_ACCB 5
 #endif
 #ifndef SPH_MINB_ACCB1
-#define SPH_MINB_ACCB1 6
+#define SPH_MINB_ACCB1 7
 #endif
-// the same trade for the strain pass (96 registers, a few spills), the
-// density pass (72, none) and XSPH (72, a few); the stress-divergence pass
-// ran slower at 5 blocks (2.2 -> 2.5 ms) and keeps 4
+#ifndef SPH_MINB_PAIRW
+#define SPH_MINB_PAIRW SPH_MINB
+#endif
+// the same trade for the strain pass (6 blocks: 80 registers, a few spills),
+// the density pass (72, none) and XSPH (72, a few); the stress-divergence
+// pass ran slower at 5 blocks (2.2 -> 2.5 ms) and keeps 4
 #ifndef SPH_MINB_STRAIN
-#define SPH_MINB_STRAIN 5
+#define SPH_MINB_STRAIN 6
 #endif
 #ifndef SPH_MINB_ACCA
 #define SPH_MINB_ACCA 4
@@ -564,7 +568,7 @@ __device__ __forceinline__ void pairw_particle(const Dev& d, int i)
 }
 
 template <int ND>
-__global__ void __launch_bounds__(128, SPH_MINB) k_pairw(Dev d)
+__global__ void __launch_bounds__(128, SPH_MINB_PAIRW) k_pairw(Dev d)
 {
     const int i = IDX;
     if (i >= d.p.N || *d.s.err) return;
@@ -725,8 +729,6 @@ __global__ void __launch_bounds__(128, SPH_MINB_STRAIN) k_strain(Dev d)
     const bool solid = (ti == 2 || ti == 4);
     const bool moving = (ti >= 1 && ti <= 4);
     Sum<real> sup[9], sdown[3];
-    Sum<real> su1, su2, su3, su4, sd1, sd2, sd3, sd4;
-    Sum<real> sus[6], sdsw;
     Sum<real> scolor;
     // the velocity-gradient and colour sums over i's own type (not walls,
     // not type 7) and, for moving i, the walls
@@ -762,9 +764,41 @@ __global__ void __launch_bounds__(128, SPH_MINB_STRAIN) k_strain(Dev d)
             scolor.add(mj / rj * real(1.0) * w[3]);
         }
     }
+    // velocity gradient (:148-181), strain rate and spin (:183-218), written
+    // before the gathers below so that their sums are not held across them
+    {
+        double up[9], down[3];
+        for (int k = 0; k < 9; k++) up[k] = sup[k].v();
+        for (int k = 0; k < 3; k++) down[k] = sdown[k].v();
+        double dv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (ti == 1 || ti == 3) {
+            for (int k = 0; k < 9; k++) dv[k] = up[k];
+        } else {
+            if (fabs(down[0]) > 1.0e-7) { dv[0] = up[0] / down[0]; dv[3] = up[3] / down[0]; dv[6] = up[6] / down[0]; }
+            if (fabs(down[1]) > 1.0e-7) { dv[1] = up[1] / down[1]; dv[4] = up[4] / down[1]; dv[7] = up[7] / down[1]; }
+            if (fabs(down[2]) > 1.0e-7) { dv[2] = up[2] / down[2]; dv[5] = up[5] / down[2]; dv[8] = up[8] / down[2]; }
+        }
+        double de[6] = {dv[0], dv[4], dv[8], dv[1] + dv[3], dv[5] + dv[7], dv[6] + dv[2]};
+        double we[6] = {0.5 * (dv[1] - dv[3]), 0.5 * (dv[2] - dv[6]), 0.5 * (dv[3] - dv[1]),
+                        0.5 * (dv[5] - dv[7]), 0.5 * (dv[6] - dv[2]), 0.5 * (dv[7] - dv[5])};
+        if (nd == 2) {
+            de[2] = 0.0; de[4] = 0.0; de[5] = 0.0;
+            we[1] = 0.0; we[3] = 0.0; we[4] = 0.0; we[5] = 0.0;
+        }
+        for (int k = 0; k < 6; k++) {
+            d.s.de[k * N + i] = de[k];
+            d.s.we[k * N + i] = we[k];
+        }
+        d.s.color[i] = scolor.v();
+    }
     // the pressure (and, for walls, stress) gathers of eos from the fluids
-    // (and, for walls, the soil), in a loop of their own over those slots
+    // (and, for walls, the soil), in a loop of their own over those slots:
+    // per particle the water (type 1) and air (type 3) pressure sums u1 / d1
+    // and u2 / d2, which the reference keeps in separate variables for soil
+    // and structure particles (only one of which a particle is)
     if (ti == 2 || ti == 4 || ti == 0) {
+        Sum<real> su1, su2, sd1, sd2;
+        Sum<real> sus[6], sdsw;
         const SlotMask m1 = type_mask(d, i, 1), m3 = type_mask(d, i, 3);
         MaskIter itg(d, i, m1 | m3 | (ti == 0 ? type_mask(d, i, 2) : SlotMask{0ull, 0ull}));
         while (itg.next(q, j)) {
@@ -774,55 +808,24 @@ __global__ void __launch_bounds__(128, SPH_MINB_STRAIN) k_strain(Dev d)
             const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
             const real w3 = w[3];
             const real pj_ = (ti == 0 && tj == 2) ? real(0) : (real)d.s.pre[j];
-            if (ti == 2 && tj == 1) { su1.add(mj * pj_ * w3 / rj); sd1.add(mj * w3 / rj); }
-            if (ti == 2 && tj == 3) { su2.add(mj * pj_ * w3 / rj); sd2.add(mj * w3 / rj); }
-            if (ti == 4 && tj == 1) { su3.add(mj * pj_ * w3 / rj); sd3.add(mj * w3 / rj); }
-            if (ti == 4 && tj == 3) { su4.add(mj * pj_ * w3 / rj); sd4.add(mj * w3 / rj); }
-            if (ti == 0 && tj == 1) { su1.add(mj * pj_ * w3 / rj); sd1.add(mj * w3 / rj); }
-            if (ti == 0 && tj == 3) { su2.add(mj * pj_ * w3 / rj); sd2.add(mj * w3 / rj); }
+            if (tj == 1) { su1.add(mj * pj_ * w3 / rj); sd1.add(mj * w3 / rj); }
+            if (tj == 3) { su2.add(mj * pj_ * w3 / rj); sd2.add(mj * w3 / rj); }
             if (ti == 0 && tj == 2) {
                 for (int k = 0; k < 6; k++) sus[k].add(mj * (real)d.s.sig[k * N + j] * w3 / rj);
                 sdsw.add(mj * w3 / rj);
             }
         }
-    }
-    double up[9], down[3], us[6];
-    for (int k = 0; k < 9; k++) up[k] = sup[k].v();
-    for (int k = 0; k < 3; k++) down[k] = sdown[k].v();
-    for (int k = 0; k < 6; k++) us[k] = sus[k].v();
-    const double u1 = su1.v(), u2 = su2.v(), u3 = su3.v(), u4 = su4.v();
-    const double d1 = sd1.v(), d2 = sd2.v(), d3 = sd3.v(), d4 = sd4.v();
-    const double dsw = sdsw.v(), color = scolor.v();
-    // velocity gradient (:148-181), strain rate and spin (:183-218)
-    double dv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    if (ti == 1 || ti == 3) {
-        for (int k = 0; k < 9; k++) dv[k] = up[k];
-    } else {
-        if (fabs(down[0]) > 1.0e-7) { dv[0] = up[0] / down[0]; dv[3] = up[3] / down[0]; dv[6] = up[6] / down[0]; }
-        if (fabs(down[1]) > 1.0e-7) { dv[1] = up[1] / down[1]; dv[4] = up[4] / down[1]; dv[7] = up[7] / down[1]; }
-        if (fabs(down[2]) > 1.0e-7) { dv[2] = up[2] / down[2]; dv[5] = up[5] / down[2]; dv[8] = up[8] / down[2]; }
-    }
-    double de[6] = {dv[0], dv[4], dv[8], dv[1] + dv[3], dv[5] + dv[7], dv[6] + dv[2]};
-    double we[6] = {0.5 * (dv[1] - dv[3]), 0.5 * (dv[2] - dv[6]), 0.5 * (dv[3] - dv[1]),
-                    0.5 * (dv[5] - dv[7]), 0.5 * (dv[6] - dv[2]), 0.5 * (dv[7] - dv[5])};
-    if (nd == 2) {
-        de[2] = 0.0; de[4] = 0.0; de[5] = 0.0;
-        we[1] = 0.0; we[3] = 0.0; we[4] = 0.0; we[5] = 0.0;
-    }
-    for (int k = 0; k < 6; k++) {
-        d.s.de[k * N + i] = de[k];
-        d.s.we[k * N + i] = we[k];
-    }
-    d.s.color[i] = color;
-    // gathered pressures (eos :122-176)
-    if (ti == 2 || ti == 0) {
+        // gathered pressures (eos :122-176)
+        const double u1 = su1.v(), u2 = su2.v(), d1 = sd1.v(), d2 = sd2.v();
         d.s.prew[i] = (d1 != 0.0) ? u1 / d1 : u1;
         d.s.prea[i] = (d2 != 0.0) ? u2 / d2 : u2;
-        if (ti == 0)
-            for (int k = 0; k < 6; k++) d.s.sig_next[k * N + i] = (dsw != 0.0) ? us[k] / dsw : us[k];
-    } else if (ti == 4) {
-        d.s.prew[i] = (d3 != 0.0) ? u3 / d3 : u3;
-        d.s.prea[i] = (d4 != 0.0) ? u4 / d4 : u4;
+        if (ti == 0) {
+            const double dsw = sdsw.v();
+            for (int k = 0; k < 6; k++) {
+                const double us = sus[k].v();
+                d.s.sig_next[k * N + i] = (dsw != 0.0) ? us / dsw : us;
+            }
+        }
     }
 }
 
