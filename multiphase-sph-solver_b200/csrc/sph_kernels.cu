@@ -70,10 +70,10 @@ namespace SPH_NS {
 #define SPH_MINB_STRESS 2
 #endif
 // the momentum pass: its neighbour loops (k_accel_b) at 7 blocks per SM
-// (72 registers, a few spills: faster than 6 or 5), its per-particle tail
-// (k_accel_b_tail) at 5 (faster than 4)
+// (72 registers, a few spills: faster than 8, 6 or 5), its per-particle tail
+// (k_accel_b_tail) at 6 (faster than 5 and 4)
 #ifndef SPH_MINB_ACCB
-#define SPH_MINB_ACCB 5
+#define SPH_MINB_ACCB 6
 #endif
 #ifndef SPH_MINB_ACCB1
 #define SPH_MINB_ACCB1 7
@@ -82,8 +82,8 @@ namespace SPH_NS {
 #define SPH_MINB_PAIRW SPH_MINB
 #endif
 // the same trade for the strain pass (6 blocks: 80 registers, a few spills),
-// the density pass (72, none) and XSPH (72, a few); the stress-divergence
-// pass ran slower at 5 blocks (2.2 -> 2.5 ms) and keeps 4
+// the density pass (6: 72, none; 7 no faster) and XSPH (8: 64); the
+// stress-divergence pass ran slower at 5 blocks (2.2 -> 2.5 ms) and keeps 4
 #ifndef SPH_MINB_STRAIN
 #define SPH_MINB_STRAIN 6
 #endif
@@ -94,7 +94,7 @@ namespace SPH_NS {
 #define SPH_MINB_DENS 6
 #endif
 #ifndef SPH_MINB_XSPH
-#define SPH_MINB_XSPH 7
+#define SPH_MINB_XSPH 8
 #endif
 
 __device__ __forceinline__ void raise_err(int* err, int code) { atomicCAS(err, 0, code); }
