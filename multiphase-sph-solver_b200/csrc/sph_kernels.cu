@@ -1311,8 +1311,9 @@ __device__ __noinline__ double drag_beta(int form, double por, double ds, double
 // acceleration.  Out of line, so that its nine sums and the particle's
 // stress operands hold registers only for particles next to a wall.
 template <int ND>
-__device__ __noinline__ void wall_stress_rows(int i, int N, int nn, int ti, bool fluid, bool tran, bool free_struct,
-                                              double ri, double satu_i, const int* nbr, const int* type,
+__device__ __noinline__ void wall_stress_rows(int i, int N, unsigned long long wlo, unsigned long long whi, int ti,
+                                              bool fluid, bool tran, bool free_struct,
+                                              double ri, double satu_i, const int* nbr,
                                               const double* nbw, const double* mass, const double* rho,
                                               const double* sb, const double* sig_next, const double* prew,
                                               const double* prea, double rows[3])
@@ -1335,9 +1336,13 @@ __device__ __noinline__ void wall_stress_rows(int i, int N, int nn, int ti, bool
         ab[k] = (real)abd[k];
         abr[k] = (real)(abd[k] / ri / ri);
     }
-    for (int q = 0; q < nn; q++) {
+    // the wall slots (type 0) of the list, in slot order
+    for (int wd = 0; wd < 2; wd++) {
+      unsigned long long m = wd ? whi : wlo;
+      while (m) {
+        const int q = wd * 64 + __ffsll((long long)m) - 1;
+        m &= m - 1;
         const int j = nbr[(size_t)q * N + i];
-        if (type[j] != 0) continue;
         real w[4];
         load_w_raw(nbw, N, q, i, w);
         const real mj = (real)mass[j], rj = (real)rho[j];
@@ -1358,6 +1363,7 @@ __device__ __noinline__ void wall_stress_rows(int i, int N, int nn, int ti, bool
         tb[2][0].add(mj * (abj[5] + abr[5]) * w[0]);
         tb[2][1].add(mj * (abj[4] + abr[4]) * w[1]);
         tb[2][2].add(mj * (abj[2] + abr[2]) * w[2]);
+      }
     }
     for (int k = 0; k < 3; k++) rows[k] = tb[k][0].v() + tb[k][1].v() + tb[k][2].v();
 }
@@ -1519,7 +1525,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b_tail(Dev d)
     // boundary_effect_free_struct (CPP_9-4:900-990) for the other flbndy
     // values: a fluid's mirrored stress has its shear components negated
     const bool free_struct = !(tran || d.p.flbndy == 1 || d.p.flbndy == 2);
-    const bool any_wall = type_mask(d, i, 0).any();
+    const SlotMask wallm = type_mask(d, i, 0);
     // the artificial-viscosity, drag and damping sums of k_accel_b
     double tav[3], tin[3], tdm[3];
     for (int k = 0; k < 3; k++) {
@@ -1531,8 +1537,8 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b_tail(Dev d)
     // line (its nine sums take registers only there); each sum still runs
     // over the list in order
     double tbrow[3] = {0.0, 0.0, 0.0};
-    if (moving && any_wall)
-        wall_stress_rows<ND>(i, N, nn, ti, fluid, tran, free_struct, ri, satu_i, d.s.nbr, d.s.type, d.s.nbw,
+    if (moving && wallm.any())
+        wall_stress_rows<ND>(i, N, wallm.lo, wallm.hi, ti, fluid, tran, free_struct, ri, satu_i, d.s.nbr, d.s.nbw,
                              d.s.mass, d.s.rho, d.s.sb, d.s.sig_next, d.s.prew, d.s.prea, tbrow);
     // the artificial-stress pair sum (ART), likewise in a loop of its own
     Sum<real> tu[3];
