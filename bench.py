@@ -338,7 +338,11 @@ def engine_arm(args, world, rank, local):
     peaks, peak_kind = measured_peaks()
     alg = algorithmic_bytes(dominant) * scene.n
     achieved = alg / (avg_ms / 1e3) / 1e9
-    traffic = ncu_traffic().get(dominant)
+    # the kernels a stage launches (the momentum pass is a loop and a tail kernel)
+    stage_kernels = {"k_accel_b": ("k_accel_b", "k_accel_b_tail")}.get(dominant, (dominant,))
+    per_kernel = ncu_traffic()
+    traffic = (sum(per_kernel[k] for k in stage_kernels)
+               if all(k in per_kernel for k in stage_kernels) else None)
 
     # end to end through the C ABI from host buffers, as a caller holding the
     # reference's own arrays uses it: its Particle records (sphgpu_upload /
@@ -387,7 +391,7 @@ def engine_arm(args, world, rank, local):
                        "timing": "CUDA events on the engine stream around K graph launches"},
             "gpu_launches": int(launches),
             "clocks": clk,
-            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": dominant, "kernels": list(stage_kernels), "achieved": achieved,
                          "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                          "frac": achieved / peaks.get("hbm_gbs"), "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
