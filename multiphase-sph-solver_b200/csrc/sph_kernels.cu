@@ -78,6 +78,9 @@ namespace SPH_NS {
 #ifndef SPH_MINB_ACCB1
 #define SPH_MINB_ACCB1 7
 #endif
+#ifndef SPH_MINB_ACCB2
+#define SPH_MINB_ACCB2 7
+#endif
 #ifndef SPH_MINB_PAIRW
 #define SPH_MINB_PAIRW SPH_MINB
 #endif
@@ -1380,8 +1383,8 @@ __device__ __noinline__ void wall_stress_rows(int i, int N, unsigned long long w
 // Writes ax, interf, interfss and the updated velocity into vx_next (the
 // reference's vx before XSPH).  DRAG = 1 carries the interact2/3 drag
 // coefficient (fli 2, 3), whose out-of-line call the Darcy form does without.
-template <int ND, int DRAG = 0>
-__global__ void __launch_bounds__(128, SPH_MINB_ACCB1) k_accel_b(Dev d)
+template <int ND, int DRAG = 0, int LOOP = 0>
+__global__ void __launch_bounds__(128, LOOP ? SPH_MINB_ACCB2 : SPH_MINB_ACCB1) k_accel_b(Dev d)
 {
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
@@ -1406,7 +1409,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB1) k_accel_b(Dev d)
     // then the soil-water (soil-air) drag of interact1/2/3 over the slots of
     // the types it pairs (the reference visits every other pair of different
     // types too, but adds nothing for them); each sum in list order
-    {
+    if (LOOP == 0) {
         MaskIter it(d, i, (ti != 7) ? type_mask(d, i, ti) : SlotMask{0ull, 0ull});
         int q, j;
         while (it.next(q, j)) {
@@ -1437,7 +1440,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB1) k_accel_b(Dev d)
                 for (int k = 0; k < nd; k++) tdm[k].add(mj / rj * cdi * dvx[k] * w[3]);
         }
     }
-    if (d.p.fli >= 1 && (ti == 1 || ti == 2 || ti == 3)) {
+    if (LOOP == 1 && d.p.fli >= 1 && (ti == 1 || ti == 2 || ti == 3)) {
         const SlotMask m1 = type_mask(d, i, 1);
         MaskIter it(d, i, (ti == 2) ? (m1 | type_mask(d, i, 3)) : type_mask(d, i, 2));
         int q, j;
@@ -1488,9 +1491,12 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB1) k_accel_b(Dev d)
         }
     }
     for (int k = 0; k < 3; k++) {
-        d.s.accb[(size_t)k * N + i] = (double)tav[k].v();
-        d.s.accb[(size_t)(3 + k) * N + i] = (double)tin[k].v();
-        d.s.accb[(size_t)(6 + k) * N + i] = (double)tdm[k].v();
+        if (LOOP == 0) {
+            d.s.accb[(size_t)k * N + i] = (double)tav[k].v();
+            d.s.accb[(size_t)(6 + k) * N + i] = (double)tdm[k].v();
+        } else {
+            d.s.accb[(size_t)(3 + k) * N + i] = (double)tin[k].v();
+        }
     }
 }
 
@@ -2703,18 +2709,20 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
         const bool drag = d.p.fli > 1;
         const dim3 g(nblk(N, 128)), b(128);
         if (d.p.ndim == 2) {
-            if (drag) k_accel_b<2, 1><<<g, b, 0, st>>>(d);
-            else k_accel_b<2, 0><<<g, b, 0, st>>>(d);
+            k_accel_b<2, 0, 0><<<g, b, 0, st>>>(d);
+            if (drag) k_accel_b<2, 1, 1><<<g, b, 0, st>>>(d);
+            else k_accel_b<2, 0, 1><<<g, b, 0, st>>>(d);
             if (art) k_accel_b_tail<2, 1><<<g, b, 0, st>>>(d);
             else k_accel_b_tail<2, 0><<<g, b, 0, st>>>(d);
         } else {
-            if (drag) k_accel_b<3, 1><<<g, b, 0, st>>>(d);
-            else k_accel_b<3, 0><<<g, b, 0, st>>>(d);
+            k_accel_b<3, 0, 0><<<g, b, 0, st>>>(d);
+            if (drag) k_accel_b<3, 1, 1><<<g, b, 0, st>>>(d);
+            else k_accel_b<3, 0, 1><<<g, b, 0, st>>>(d);
             if (art) k_accel_b_tail<3, 1><<<g, b, 0, st>>>(d);
             else k_accel_b_tail<3, 0><<<g, b, 0, st>>>(d);
         }
     }
-    n += 2;
+    n += 3;
     REC(18);
     LAUNCH_ND(k_xsph_update, nblk(N, 128), 128, d); n++;
     REC(19);
