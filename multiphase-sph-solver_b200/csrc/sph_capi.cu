@@ -120,8 +120,9 @@ struct sphgpu_ctx {
     size_t sort_bytes = 0;
     int end_bit = 1;
     std::vector<void*> allocs;
-    std::vector<int> h_type, h_matype;
-    std::vector<double> h_x;          // x as uploaded (the reference writes it only in update)
+    // filled whole by whoever sizes them, so left uninitialised until then
+    std::vector<int, UninitAlloc<int>> h_type, h_matype;
+    std::vector<double, UninitAlloc<double>> h_x;   // x as uploaded (the reference writes it only in update)
     bool x_tracked = false;
     int l_host = 1;
     double last_ms = 0.0;
@@ -577,6 +578,11 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     c->sort_bytes = sphk_sort_temp_bytes(N, c->end_bit);
     if (cudaMalloc(&c->sort_tmp, c->sort_bytes + 256) != cudaSuccess) return fail(SPHGPU_E_CUDA);
     c->allocs.push_back(c->sort_tmp);
+    // the staging buffers of the record transfers, sized for Particle and
+    // material records, allocated with the rest of the state
+    if (ensure_rec_staging(c, (size_t)kRecChunk * std::max({(size_t)kParticleBytes, sizeof(sphgpu_fluid),
+                                                             sizeof(sphgpu_soil)})))
+        return fail(SPHGPU_E_CUDA);
     c->d[1] = c->d[0];
     std::swap(c->d[1].s.xh, c->d[1].s.xh_next);
     std::swap(c->d[1].s.sig, c->d[1].s.sig_next);
