@@ -416,7 +416,10 @@ int ensure_rec_staging(sphgpu_ctx* c, size_t bytes)
 // n caller records of `stride` bytes (8-byte aligned) -> the device arrays of
 // `tab`, in chunks: a chunk is copied into a pinned buffer on several host
 // threads while the previous one crosses PCIe and k_rec_unpack scatters it
-int push_records(sphgpu_ctx* c, const char* base, int n, size_t stride, const std::vector<RecMember>& tab)
+// With `keep` non-null the records are also copied there (n x stride bytes),
+// in the same pass over the caller's array.
+int push_records(sphgpu_ctx* c, const char* base, int n, size_t stride, const std::vector<RecMember>& tab,
+                 char* keep = nullptr)
 {
     int r = ensure_rec_staging(c, std::max((size_t)kRecChunk * stride, c->rec_bytes));
     if (r) return r;
@@ -433,7 +436,11 @@ int push_records(sphgpu_ctx* c, const char* base, int n, size_t stride, const st
         char* pin = static_cast<char*>(c->rec_pinned[b]);
         const char* src = base + (size_t)i0 * stride;
         const size_t bytes = (size_t)cnt * stride;
-        par_for(bytes, [&](size_t a, size_t e) { std::memcpy(pin + a, src + a, e - a); });
+        char* kp = keep ? keep + (size_t)i0 * stride : nullptr;
+        par_for(bytes, [&](size_t a, size_t e) {
+            std::memcpy(pin + a, src + a, e - a);
+            if (kp) std::memcpy(kp + a, src + a, e - a);
+        });
         CK(cudaMemcpyAsync(c->rec_dev[b], pin, bytes, cudaMemcpyHostToDevice, c->st));
         k_rec_unpack<<<(cnt + 255) / 256, 256, 0, c->st>>>(static_cast<const char*>(c->rec_dev[b]), stride, i0, cnt,
                                                            c->N, dtab[b], (int)tab.size());
@@ -786,22 +793,18 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
     if (!c || n != c->N) return SPHGPU_E_ARG;
     cudaSetDevice(c->device);
     // the host copies (K-L fields rewrite members of them and upload them
-    // again), copied on all cores; the device arrays come from these aligned
-    // copies through the record pipeline of sphgpu_upload_particles
+    // again), written in the same pass that stages the caller's records for
+    // the device; the per-particle constants below read the caller's records
+    char* keep_f = nullptr;
+    char* keep_s = nullptr;
     if (fl && fl != c->h_fluid.data()) {
         c->h_fluid.resize(n);
-        char* dst = reinterpret_cast<char*>(c->h_fluid.data());
-        const char* src = reinterpret_cast<const char*>(fl);
-        par_for(sizeof(sphgpu_fluid) * n, [&](size_t a, size_t e) { std::memcpy(dst + a, src + a, e - a); });
+        keep_f = reinterpret_cast<char*>(c->h_fluid.data());
     }
     if (so && so != c->h_soil.data()) {
         c->h_soil.resize(n);
-        char* dst = reinterpret_cast<char*>(c->h_soil.data());
-        const char* src = reinterpret_cast<const char*>(so);
-        par_for(sizeof(sphgpu_soil) * n, [&](size_t a, size_t e) { std::memcpy(dst + a, src + a, e - a); });
+        keep_s = reinterpret_cast<char*>(c->h_soil.data());
     }
-    if (fl) fl = c->h_fluid.data();
-    if (so) so = c->h_soil.data();
     const int N = c->N;
     DevState& s = c->d[0].s;
     std::vector<double, UninitAlloc<double>> buf((size_t)N);
@@ -818,8 +821,11 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
             m(offsetof(sphgpu_fluid, vpu), s.f_vpu), m(offsetof(sphgpu_fluid, vis), s.f_vis),
             m(offsetof(sphgpu_fluid, c), s.f_c), m(offsetof(sphgpu_fluid, strain_min), s.f_smin),
             m(offsetof(sphgpu_fluid, bhtype), s.f_bhtype, 1)};
-        r = push_records(c, reinterpret_cast<const char*>(fl), N, sizeof(sphgpu_fluid), tab);
-        if (r) return r;
+        r = push_records(c, reinterpret_cast<const char*>(fl), N, sizeof(sphgpu_fluid), tab, keep_f);
+        if (r) {
+            if (keep_f) c->h_fluid.clear();   // not filled
+            return r;
+        }
         // Bingham friction: tan of the angle, CPP_7-2-constitutive.cpp:42-43
         par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = std::tan(fl[i].fai * 0.0174532925199); }); r |= put(s.f_tanfai);
     }
@@ -834,8 +840,11 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
             m(offsetof(sphgpu_soil, fs), s.s_fs), m(offsetof(sphgpu_soil, ann), s.s_ann),
             m(offsetof(sphgpu_soil, zmf), s.s_zmf), m(offsetof(sphgpu_soil, ramda), s.s_ramda),
             m(offsetof(sphgpu_soil, sme0), s.s_sme0)};
-        r = push_records(c, reinterpret_cast<const char*>(so), N, sizeof(sphgpu_soil), tab);
-        if (r) return r;
+        r = push_records(c, reinterpret_cast<const char*>(so), N, sizeof(sphgpu_soil), tab, keep_s);
+        if (r) {
+            if (keep_s) c->h_soil.clear();   // not filled
+            return r;
+        }
         // Drucker-Prager cone constants with the reference's own libm calls
         // (dpmodel1 / dpmodel_bui / DPModel_check, CPP_8-1-consfactor.cpp:294-349,
         // 461-529, 783-803); they depend only on the material record.
