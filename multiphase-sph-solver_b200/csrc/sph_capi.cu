@@ -140,6 +140,7 @@ struct sphgpu_ctx {
     int precision = SPHGPU_PREC_FP64;
     std::vector<sphgpu_fluid, UninitAlloc<sphgpu_fluid>> h_fluid;   // the material records last set
     std::vector<sphgpu_soil, UninitAlloc<sphgpu_soil>> h_soil;      // (K-L fields rewrite members)
+    double* mat_pinned = nullptr;     // pinned, 4N: the per-particle material constants set_materials uploads
 };
 
 namespace {
@@ -605,6 +606,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     // the transfers copy at memory speed instead of taking a page fault per
     // 4 KB.  They stay empty (not set) until a call fills them, and sizing
     // them to N then reuses this storage.
+    if (cudaMallocHost(&c->mat_pinned, sizeof(double) * 4 * (size_t)N) != cudaSuccess) return fail(SPHGPU_E_CUDA);
     c->h_x.reserve((size_t)N * 3);
     c->h_type.reserve(N);
     c->h_matype.reserve(N);
@@ -630,6 +632,7 @@ void sphgpu_destroy(sphgpu_ctx* c)
     invalidate_graphs(c);
     for (void* p : c->allocs) cudaFree(p);
     if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->mat_pinned) cudaFreeHost(c->mat_pinned);
     for (int b = 0; b < 2; b++) {
         if (c->rec_pinned[b]) cudaFreeHost(c->rec_pinned[b]);
         if (c->rec_dev[b]) cudaFree(c->rec_dev[b]);
@@ -807,12 +810,16 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
     }
     const int N = c->N;
     DevState& s = c->d[0].s;
-    std::vector<double, UninitAlloc<double>> buf((size_t)N);
-    auto put = [&](double* dst) -> int {
-        CK(cudaMemcpyAsync(dst, buf.data(), sizeof(double) * N, cudaMemcpyHostToDevice, c->st));
+    // the per-particle constants, in the pinned block (N doubles each)
+    double* buf = c->mat_pinned;
+    auto put = [&](double* dst, const double* src) -> int {
+        CK(cudaMemcpyAsync(dst, src, sizeof(double) * N, cudaMemcpyHostToDevice, c->st));
         CK(cudaStreamSynchronize(c->st));
         return 0;
     };
+    // a particle whose inputs have the bits of the previous particle's takes
+    // its results (particles of one material share their records)
+    auto same = [](double a, double b) { return std::memcmp(&a, &b, sizeof(double)) == 0; };
     auto m = [](size_t off, void* dst, int kind = 0) { return RecMember{(int)off, 1, kind, 0, dst}; };
     int r = 0;
     if (fl) {
@@ -827,7 +834,14 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
             return r;
         }
         // Bingham friction: tan of the angle, CPP_7-2-constitutive.cpp:42-43
-        par_for(N, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) buf[i] = std::tan(fl[i].fai * 0.0174532925199); }); r |= put(s.f_tanfai);
+        par_for(N, [&](size_t a, size_t b) {
+            double lf = 0.0, v = 0.0;
+            for (size_t i = a; i < b; i++) {
+                if (i == a || !same(fl[i].fai, lf)) { lf = fl[i].fai; v = std::tan(lf * 0.0174532925199); }
+                buf[i] = v;
+            }
+        });
+        r |= put(s.f_tanfai, buf);
     }
     if (so) {
         const std::vector<RecMember> tab = {
@@ -848,21 +862,30 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
         // Drucker-Prager cone constants with the reference's own libm calls
         // (dpmodel1 / dpmodel_bui / DPModel_check, CPP_8-1-consfactor.cpp:294-349,
         // 461-529, 783-803); they depend only on the material record.
-        std::vector<double, UninitAlloc<double>> ya(N), yk(N), yd(N);
+        double* ya = buf + N;
+        double* yk = buf + 2 * (size_t)N;
+        double* yd = buf + 3 * (size_t)N;
         par_for(N, [&](size_t a, size_t b) {
-        for (size_t i = a; i < b; i++) {
-            const double fai = std::atan(std::tan(so[i].fai * 0.0174532925166667) / so[i].fs);
-            const double fai_dil = std::atan(std::tan(so[i].beta * 0.0174532925166667) / so[i].fs);
-            const double ci = so[i].c / so[i].fs;
-            ya[i] = std::sin(fai) / std::sqrt(9.0 + 3.0 * std::sin(fai) * std::sin(fai));
-            yk[i] = 3.0 * ci * std::cos(fai) / std::sqrt(9.0 + 3.0 * std::sin(fai) * std::sin(fai));
-            // dilatancy slope, used by the Bui form (matype % 10 == 5) only
-            yd[i] = std::sin(fai_dil) / std::sqrt(9.0 + 3.0 * std::sin(fai_dil) * std::sin(fai_dil));
-        }
+            double lf = 0.0, lb = 0.0, lc = 0.0, ls = 0.0, va = 0.0, vk = 0.0, vd = 0.0;
+            for (size_t i = a; i < b; i++) {
+                const sphgpu_soil& q = so[i];
+                if (i == a || !same(q.fai, lf) || !same(q.beta, lb) || !same(q.c, lc) || !same(q.fs, ls)) {
+                    lf = q.fai; lb = q.beta; lc = q.c; ls = q.fs;
+                    const double fai = std::atan(std::tan(q.fai * 0.0174532925166667) / q.fs);
+                    const double fai_dil = std::atan(std::tan(q.beta * 0.0174532925166667) / q.fs);
+                    const double ci = q.c / q.fs;
+                    const double sf = std::sin(fai), sd = std::sin(fai_dil);
+                    va = sf / std::sqrt(9.0 + 3.0 * sf * sf);
+                    vk = 3.0 * ci * std::cos(fai) / std::sqrt(9.0 + 3.0 * sf * sf);
+                    // dilatancy slope, used by the Bui form (matype % 10 == 5) only
+                    vd = sd / std::sqrt(9.0 + 3.0 * sd * sd);
+                }
+                ya[i] = va; yk[i] = vk; yd[i] = vd;
+            }
         });
-        buf = ya; r |= put(s.s_yalf);
-        buf = yk; r |= put(s.s_ykap);
-        buf = yd; r |= put(s.s_yalf_dil);
+        r |= put(s.s_yalf, ya);
+        r |= put(s.s_ykap, yk);
+        r |= put(s.s_yalf_dil, yd);
         // the members only unsaturated Cam-clay (matype % 10 == 3), the
         // saturation pass and fractional-order Cam-clay (8) read, allocated
         // on first use; pow(c, 4) of fractional_mcc with the host's libm
