@@ -307,19 +307,28 @@ int sphgpu_kl_synthesize(sphgpu_ctx* ctx, const sphgpu_kl_domain* dom, const sph
  * Particle::xp), d_hl (n doubles), d_type (n ints) in, and d_ninflu (n ints)
  * and d_influ (n * 100 ints, Par_Cell::influ layout: slots 1..ninflu) out;
  * `grid` supplies ndim, dr, xmin/ymin/zmin and cxm/cym/czm/ctotal.  The
- * result equals sphgpu_nnps on the same positions (parttocell +
- * partisearching, CPP_3-NNPS.cpp:175-374).
+ * result equals what sphgpu_nnps returns on the same positions for the first
+ * search after the particles are loaded (parttocell + partisearching,
+ * CPP_3-NNPS.cpp:175-374).  The reference, and the context engine, carry the
+ * cell range of the extra cell ctotal over from step to step
+ * (CPP_3-NNPS.cpp:196-201); each call here starts it afresh.
  *
  * Every intermediate lives in one fixed device array of
  * sphgpu_nnps_noalloc_scratch_bytes() bytes inside the library, held by each
  * GPU that loads the library until the process exits; n is limited to
  * SPHGPU_NOALLOC_MAX_PARTICLES and ctotal to SPHGPU_NOALLOC_MAX_CELLS (larger
  * sizes return SPHGPU_E_ARG).  The first call on a device looks the array up
- * with that device current; make it before any stream capture.  All calls on
+ * with that device current and keeps it for the rest of the process; make it
+ * before any stream capture, and do not call the search again on a device the
+ * process has reset (cudaDeviceReset discards the array).  All calls on
  * a device share the array: calls that overlap on the GPU race and must not
  * be issued.  The call runs on `stream` (a cudaStream_t, NULL for the default
- * stream), waits for it, and returns 0, 3 (a particle outside the grid; the
- * outputs are not written) or 5 (more than 99 neighbours).
+ * stream) and waits for that stream, so it is synchronous and cannot be
+ * captured into a CUDA graph.  Returns 0, 3 (a particle outside the grid; the
+ * outputs are not written), 5 (more than 99 neighbours: every count in
+ * d_ninflu is written, lists hold their first 99 slots) or SPHGPU_E_CUDA
+ * (also when an error of the caller's earlier work is pending; it is left
+ * pending and nothing is launched).
  */
 #define SPHGPU_NOALLOC_MAX_PARTICLES 65536
 #define SPHGPU_NOALLOC_MAX_CELLS     262144

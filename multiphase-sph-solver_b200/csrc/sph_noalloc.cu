@@ -14,8 +14,12 @@
 //
 // The array exists once per GPU that loads this library and stays allocated
 // until the process exits.  Its device address is looked up once per device,
-// with that device current, by the first call made on it; that first call
-// should therefore be made before any stream capture.  Every call on a
+// with that device current, by the first call made on it, and kept for the
+// rest of the process; that first call should therefore be made before any
+// stream capture, and a process that resets a device (cudaDeviceReset, which
+// discards the module and so the array) must not call the search on that
+// device again.  Each call waits for its own stream to read its status, so it
+// is synchronous and cannot be captured into a graph.  Every call on a
 // device uses the same array and it keeps the previous call's contents: each
 // call clears the words that must start at zero (the error word and the cell
 // ranges) itself.  Calls that overlap on the GPU (on different streams, or
@@ -161,8 +165,10 @@ __global__ void __launch_bounds__(128) na_search(NaArgs a)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
+    // a particle outside the grid stops the search (outputs not written);
+    // more than 99 neighbours does not, so that every count is written
     const int* err = reinterpret_cast<const int*>(a.scratch + kOffErr);
-    if (*err) return;
+    if (*err == SPH_ERR_CELL) return;
     int* errw = reinterpret_cast<int*>(a.scratch + kOffErr);
     const int* cell = reinterpret_cast<const int*>(a.scratch + kOffCell);
     const int* pid = reinterpret_cast<const int*>(a.scratch + kOffValOut);
@@ -229,6 +235,9 @@ extern "C" int sphgpu_nnps_noalloc(const sphgpu_params* grid, int n, const doubl
                                     (const int*)nullptr, (int*)nullptr, n, 0, end_bit);
     if (need > kSortBytes) return SPHGPU_E_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // an error the caller's own earlier work left pending is reported, not
+    // taken over: nothing is launched and the error stays where it was
+    if (cudaPeekAtLastError() != cudaSuccess) return SPHGPU_E_CUDA;
     NaArgs a;
     a.n = n; a.ndim = grid->ndim; a.cxm = grid->cxm; a.cym = grid->cym; a.czm = grid->czm;
     a.ctotal = grid->ctotal; a.dr = grid->dr; a.xmin = grid->xmin; a.ymin = grid->ymin; a.zmin = grid->zmin;
@@ -236,20 +245,26 @@ extern "C" int sphgpu_nnps_noalloc(const sphgpu_params* grid, int n, const doubl
     const int threads = 256;
     const int cover = (n > grid->ctotal + 1) ? n : grid->ctotal + 1;
     na_clear_err<<<1, 32, 0, st>>>(a);
+    if (cudaPeekAtLastError() != cudaSuccess) return SPHGPU_E_CUDA;
     na_keys<<<(cover + threads - 1) / threads, threads, 0, st>>>(a);
+    if (cudaPeekAtLastError() != cudaSuccess) return SPHGPU_E_CUDA;
     size_t bytes = kSortBytes;
-    cub::DeviceRadixSort::SortPairs(scratch + kOffSort, bytes, reinterpret_cast<uint32_t*>(scratch + kOffKeyIn),
-                                    reinterpret_cast<uint32_t*>(scratch + kOffKeyOut),
-                                    reinterpret_cast<int*>(scratch + kOffValIn),
-                                    reinterpret_cast<int*>(scratch + kOffValOut), n, 0, end_bit, st);
-    na_ranges<<<(n + threads - 1) / threads, threads, 0, st>>>(a);
-    na_search<<<(n + 127) / 128, 128, 0, st>>>(a);
-    if (cudaGetLastError() != cudaSuccess) return SPHGPU_E_CUDA;
-    // the search is synchronous: its status is the error word of this call
-    if (cudaStreamSynchronize(st) != cudaSuccess) return SPHGPU_E_CUDA;
-    int err = 0;
-    if (cudaMemcpy(&err, scratch + kOffErr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    if (cub::DeviceRadixSort::SortPairs(scratch + kOffSort, bytes, reinterpret_cast<uint32_t*>(scratch + kOffKeyIn),
+                                        reinterpret_cast<uint32_t*>(scratch + kOffKeyOut),
+                                        reinterpret_cast<int*>(scratch + kOffValIn),
+                                        reinterpret_cast<int*>(scratch + kOffValOut), n, 0, end_bit,
+                                        st) != cudaSuccess)
         return SPHGPU_E_CUDA;
+    na_ranges<<<(n + threads - 1) / threads, threads, 0, st>>>(a);
+    if (cudaPeekAtLastError() != cudaSuccess) return SPHGPU_E_CUDA;
+    na_search<<<(n + 127) / 128, 128, 0, st>>>(a);
+    if (cudaPeekAtLastError() != cudaSuccess) return SPHGPU_E_CUDA;
+    // the call is synchronous: its status is the error word of this search,
+    // read on the caller's stream (no wait on other streams of the device)
+    int err = 0;
+    if (cudaMemcpyAsync(&err, scratch + kOffErr, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return SPHGPU_E_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return SPHGPU_E_CUDA;
     return err;
 }
 

@@ -3,7 +3,7 @@
     python tests/golden/make_golden.py [case ...]     (default: every case)
 
 Needs oracle/_ref/libsphref.so, i.e. the reference solver compiled from its own
-sources (make -C oracle ref, which reads the reference source tree).  For each
+sources (make -C oracle ref REF=<reference source tree>).  For each
 case the reference parses the input deck written by scenes.write_input_dat,
 initialises itself, and runs one thread (its deterministic, sequential order).
 Saved per case (.npz): the input deck parameters the reference parsed, the
