@@ -43,37 +43,59 @@ import scenes  # noqa: E402
 METRIC = "particle-updates/s"
 WORKLOAD = "3d_saturated_soil_column_collapse"
 
-# Algorithmic bytes per particle and launch (3-D), each kernel reading its
-# own particle's fields, its neighbour-list row and its pair records once and
-# writing its outputs once; neighbour fields are counted as cache-served.  NB
-# is the mean listed neighbours per particle (65 for co-located soil and
-# water); a pair record (grad W, W) is 32 bytes in FP64 and 16 in the
-# FP32-bulk form.
-NB_MEAN = 65
+# Algorithmic bytes per particle per step: each barrier-level pass of the
+# step reads its own particle's fields once and writes its outputs once,
+# neighbour fields are served from cache after the cell sort, and no
+# neighbour list is stored.  The per-pass figures are those of the 2-D FP64
+# dam break (806 B in all); the 3-D soil column with co-located water (soil
+# state sigma, eps, adps, e, n, satu, cop and its material fields) comes to
+# 1,870 B by the same rule, and its per-pass figures are the 2-D ones scaled
+# by 1870 / 806.  Each pass is listed with the kernels of this engine that do
+# its work.  The engine's neighbour search and pair records have no
+# counterpart in this count (their traffic is the engine's own choice), and it
+# keeps the state in the caller's order, so the reorder pass has no kernel.
+PASS_BYTES_2D = {
+    "key": 24.0,
+    "radix sort": 32.0,
+    "reorder": 196.0,
+    "cell ranges": 14.0,
+    "porosity + continuity": 68.0,
+    "Shepard + EOS": 36.0,
+    "strain + stress + free surface + eigen": 124.0,
+    "stress divergence + viscosity + walls + velocity update": 132.0,
+    "XSPH + walls + check_domain + update": 180.0,
+}
+STEP_BYTES_3D = 1870.0
+PASS_KERNELS = {
+    "key": ("k_cellkey",),
+    "radix sort": ("radix_sort",),
+    "reorder": (),
+    "cell ranges": ("k_cellreset", "k_cellrange"),
+    "porosity + continuity": ("k_density",),
+    "Shepard + EOS": ("k_shepard_eos",),
+    "strain + stress + free surface + eigen": ("k_strain", "k_regu_eps", "k_saturation", "k_stress",
+                                               "k_regu_sig", "k_stress_2", "k_art_rij"),
+    "stress divergence + viscosity + walls + velocity update": ("k_accel_a", "k_accel_b", "k_ss", "k_tran_wall",
+                                                                "k_coupled", "k_free_solid"),
+    "XSPH + walls + check_domain + update": ("k_xsph_update", "k_tm_boundary"),
+}
 
 
-def algorithmic_bytes(stage: str, nb: float = NB_MEAN, rec_bytes: float = 32.0) -> float:
-    row = 4.0 * nb                       # the particle's neighbour-list row
-    rec = rec_bytes * nb                 # the particle's pair records
-    table = {
-        # reads | writes
-        "k_cellkey": 32 + 12,                                   # (x,y,z,h) | cell, key, value
-        "radix_sort": 3 * 16,                                   # 3 digit passes of (key, value) in + out
-        "k_cellrange": 4 + 4 + 4 + 32 + 32 + 16 + 4 + 4 + 8,    # key, pid, type, record | sorted FP64 + FP32 records, word, position, range
-        "k_nnps": 16 + 4 + 4 + 4 + 4 + row,                     # FP32 record, cell, pid, type | count, provisional row
-        "k_nnps_resolve": 4 + 4 + 4 + 32 + row + 4 + row + 80,  # type, position, count, record, provisional row
-                                                                # | count, list row, five two-word type masks
-        "k_pairw": 32 + 4 + row + rec,                          # record, count, list row | pair records
-        "k_density": 4 + 4 + 32 + 8 + 8 + 8 + 24 + 8 + row + rec + 8 + 16,
-        "k_shepard_eos": 4 + 4 + 32 + 8 + 8 + 8 + 8 + row + rec + 8 + 8,
-        "k_strain": 4 + 4 + 32 + 24 + row + rec + 48 + 48 + 8 + 16,
-        "k_stress": 48 + 48 + 48 + 48 + 8 + 4 + 4 + 8 + 8 + 88 + 48 + 8
-                    + 48 + 48 + 48 + 8 + 8 + 40 + 24 + 48 + 8,
-        "k_accel_a": 4 + 4 + 8 + 48 + 8 + 8 + 8 + 8 + 8 + row + rec + 24,
-        "k_accel_b": 4 + 4 + 32 + 8 + 24 + 48 + 24 + 24 + 24 + 24 + 4 + 8 + 8 + 8 + 24 + row + rec + 24 + 24 + 24,
-        "k_xsph_update": 4 + 4 + 32 + 24 + 24 + 24 + 24 + 8 + 8 + 8 + 8 + 4 + row + rec + 32 + 24 + 24 + 24 + 24 + 8,
-    }
-    return float(table.get(stage, 0.0))
+def pass_bytes(ndim: int = 3) -> dict:
+    scale = 1.0 if ndim == 2 else STEP_BYTES_3D / sum(PASS_BYTES_2D.values())
+    return {k: v * scale for k, v in PASS_BYTES_2D.items()}
+
+
+def pass_roofline(stage_ms: dict, n: int, peak_gbs: float, ndim: int = 3) -> dict:
+    """Per pass: its algorithmic bytes for n particles, the summed device time
+    of its kernels (ms per step) and the achieved GB/s and fraction of peak."""
+    out = {}
+    for name, b in pass_bytes(ndim).items():
+        ms = sum(stage_ms.get(k, 0.0) for k in PASS_KERNELS[name])
+        gbs = b * n / (ms / 1e3) / 1e9 if ms > 0 else None
+        out[name] = {"bytes_per_particle": b, "kernels": list(PASS_KERNELS[name]), "ms": ms,
+                     "achieved_gbs": gbs, "frac": gbs / peak_gbs if gbs else None}
+    return out
 
 
 def measured_peaks() -> tuple[dict, str]:
@@ -333,16 +355,25 @@ def engine_arm(args, world, rank, local):
     ref_fields = {k: eng.get_field(k) for k in ("sig", "ux", "vx", "rho", "xp")}
     # stage durations with an event between stages, over the same number of steps
     prof = eng.step_profiled(args.steps)
-    dominant = max((k for k in prof if k != "k_step_done"), key=lambda k: prof[k])
-    avg_ms = prof[dominant] / args.steps
+    stage_ms = {k: v / args.steps for k, v in prof.items()}
     peaks, peak_kind = measured_peaks()
-    alg = algorithmic_bytes(dominant) * scene.n
-    achieved = alg / (avg_ms / 1e3) / 1e9
-    # the kernels a stage launches (the momentum pass is a loop and a tail kernel)
-    stage_kernels = {"k_accel_b": ("k_accel_b", "k_accel_b_tail")}.get(dominant, (dominant,))
+    hbm = peaks.get("hbm_gbs")
+    passes = pass_roofline(stage_ms, scene.n, hbm)
+    # the roofline line is the pass that takes the most device time
+    dominant = max((k for k in passes if passes[k]["ms"] > 0), key=lambda k: passes[k]["ms"])
+    dom = passes[dominant]
+    avg_ms = dom["ms"]
+    alg = dom["bytes_per_particle"] * scene.n
+    achieved = dom["achieved_gbs"]
+    # the pass's kernels as ncu names them (the momentum stage launches two
+    # loop kernels and a tail kernel under the stage name k_accel_b)
+    ncu_names = {"k_accel_b": ("k_accel_b", "k_accel_b_tail")}
+    pass_kernels = [q for k in dom["kernels"] if stage_ms.get(k, 0.0) > 0.01 for q in ncu_names.get(k, (k,))]
     per_kernel = ncu_traffic()
-    traffic = (sum(per_kernel[k] for k in stage_kernels)
-               if all(k in per_kernel for k in stage_kernels) else None)
+    traffic = (sum(per_kernel[k] for k in pass_kernels)
+               if pass_kernels and all(k in per_kernel for k in pass_kernels) else None)
+    step_ms = ms_max / args.steps
+    step_gbs = STEP_BYTES_3D * scene.n / (step_ms / 1e3) / 1e9
 
     # end to end through the C ABI from host buffers, as a caller holding the
     # reference's own arrays uses it: its Particle records (sphgpu_upload /
@@ -391,12 +422,15 @@ def engine_arm(args, world, rank, local):
                        "timing": "CUDA events on the engine stream around K graph launches"},
             "gpu_launches": int(launches),
             "clocks": clk,
-            "roofline": {"bound": "hbm", "kernel": dominant, "kernels": list(stage_kernels), "achieved": achieved,
-                         "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
-                         "frac": achieved / peaks.get("hbm_gbs"), "peak_kind": peak_kind,
+            "roofline": {"bound": "hbm", "pass": dominant, "kernels": pass_kernels, "achieved": achieved,
+                         "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
-                         "traffic": (traffic * scene.n) if traffic else None},
-            "stage_ms_per_step": {k: v / args.steps for k, v in prof.items()},
+                         "traffic": (traffic * scene.n) if traffic else None,
+                         "traffic_over_algorithmic": (traffic * scene.n / alg) if traffic else None,
+                         "step": {"algorithmic_bytes": STEP_BYTES_3D * scene.n, "ms": step_ms,
+                                  "achieved": step_gbs, "frac": step_gbs / hbm}},
+            "passes": passes,
+            "stage_ms_per_step": stage_ms,
             "forms": {
                 "fp64": {"value": value, "ms_per_step": ms_max / args.steps,
                          "error": "bit-identical to the FP64 oracle (tests/test_gpu_parity.py)"},

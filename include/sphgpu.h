@@ -199,11 +199,69 @@ int sphgpu_particle_layout(const char* name, size_t* offset, int* ncomp);
 int sphgpu_step(sphgpu_ctx* ctx, int nsteps);
 
 /*
+ * Step l in the reference's method granularity, for the C++ shim classes that
+ * keep SPH_Calculation's own loop (CPP_1-SPHLoops.cpp:523-753) as the caller:
+ *   sphgpu_parttocell      clNNPS_Fun::parttocell (CPP_3-NNPS.cpp:175-263):
+ *                          cell keys, the radix sort in Binary_Sort's order and
+ *                          the cell ranges; returns 0 or 3
+ *   sphgpu_partisearching  clNNPS_Fun::partisearching (CPP_3-NNPS.cpp:265-374):
+ *                          the neighbour lists and their kernel values; runs
+ *                          parttocell first if the step has not; returns 0 or 5
+ *   sphgpu_update          every method SPH_Calculation calls after
+ *                          partisearching, through clUpdate_Fun::update
+ *                          (kernel_gradient_correction, density, strain_noreg,
+ *                          strain_regu, saturation, cal_permeability, eos,
+ *                          strain_to_stress, stress_regu, free_surface_check,
+ *                          Stress_eigValue, the clAcce_Fun accelerations,
+ *                          artificial viscosity and stress, the wall stresses,
+ *                          coupled_Water_Soil_Structure, interact1/2/3,
+ *                          interaction_ss_*, soil_damping_geostress,
+ *                          boundary_free_solid, veocity_update, xsph, the wall
+ *                          treatments of clBndy_Fun, check_domain, update): the
+ *                          engine fuses these methods into passes that cross the
+ *                          methods' boundaries (the local equation of state
+ *                          runs with the Shepard filter, seven momentum methods
+ *                          share one neighbour pass), so they run together
+ *                          when the step completes; advances l.  Runs the
+ *                          search first if the step has not.
+ * The results equal sphgpu_step's.  sphgpu_parttocell on a step whose cell
+ * lists are built returns SPHGPU_E_STATE; sphgpu_step completes a step these
+ * entries began before it runs its own.
+ */
+int sphgpu_parttocell(sphgpu_ctx* ctx);
+int sphgpu_partisearching(sphgpu_ctx* ctx);
+int sphgpu_update(sphgpu_ctx* ctx);
+
+/*
+ * Replace the run flags and parameters of a context between steps (a caller
+ * that learns them method by method, as the shim classes do).  The particle
+ * count, dimension and cell grid must be those the context was created with
+ * (else SPHGPU_E_ARG); buffers new flags need are allocated here.
+ */
+int sphgpu_update_params(sphgpu_ctx* ctx, const sphgpu_params* params);
+
+/*
  * The NNPS stage alone (parttocell + partisearching for step l), leaving the
  * neighbour lists on the device; ninflu[n] and influ[n * 100] (1-based slots
  * 1..ninflu, as Par_Cell::influ) are copied out if non-NULL.
  */
 int sphgpu_nnps(sphgpu_ctx* ctx, int* ninflu, int* influ);
+
+/*
+ * Adaptive time step (an addition of this library: the reference's dt is
+ * constant, clUpdate_Fun::timestep, CPP_12-2-dt.cpp:13-20).  With cfl > 0 the
+ * last kernels of every step reduce, over the water, soil, air and structure
+ * particles, min(cfl h / (c + |v|), cfl_force sqrt(h / |a|)) -- c the sound
+ * speed of the particle's material (Para_Fluid / Para_Soil / Para_Structure
+ * vpu), v and a its velocity and acceleration after the update -- with warp
+ * shuffles on the device, and the next step runs with that dt, capped at the
+ * input dt (no host round trip: the steps stay in their CUDA graphs).  The
+ * first step after the call uses the input dt.  cfl <= 0 turns it off, the
+ * default; every parity statement of this library is for the constant dt.
+ * sphgpu_get_dt reads the dt the next step will use.
+ */
+int sphgpu_set_cfl(sphgpu_ctx* ctx, double cfl, double cfl_force);
+int sphgpu_get_dt(sphgpu_ctx* ctx, double* dt);
 
 /* Block until the context's stream is idle; returns the sticky error, if any. */
 int sphgpu_synchronize(sphgpu_ctx* ctx);

@@ -26,6 +26,8 @@
 extern "C" size_t sphk_sort_temp_bytes(int N, int end_bit);
 extern "C" int sphk_enqueue_nnps(const Dev* d, void* sort_tmp, size_t sort_bytes, int end_bit, cudaStream_t st,
                                  cudaEvent_t* ev);
+extern "C" int sphk_enqueue_nnps_parts(const Dev* d, void* sort_tmp, size_t sort_bytes, int end_bit,
+                                       cudaStream_t st, cudaEvent_t* ev, int parts);
 extern "C" int sphk_enqueue_physics(const Dev* d, cudaStream_t st, cudaEvent_t* ev, int regu);
 extern "C" int sphk_enqueue_physics_bulk32(const Dev* d, cudaStream_t st, cudaEvent_t* ev, int regu);
 extern "C" const char* const sphk_stage_names[];
@@ -141,6 +143,7 @@ struct sphgpu_ctx {
     std::vector<sphgpu_fluid, UninitAlloc<sphgpu_fluid>> h_fluid;   // the material records last set
     std::vector<sphgpu_soil, UninitAlloc<sphgpu_soil>> h_soil;      // (K-L fields rewrite members)
     double* mat_pinned = nullptr;     // pinned, 4N: the per-particle material constants set_materials uploads
+    int part_done = 0;     // parts of step l run through the method entries: 1 parttocell, 2 partisearching
 };
 
 namespace {
@@ -184,6 +187,72 @@ int check_params(const sphgpu_params* P)
     if (P->ss_type < 0 || P->ss_type > 3) return SPHGPU_E_UNSUPPORTED;
     if (P->if_move < 0 || P->if_move > 3) return SPHGPU_E_UNSUPPORTED;
     return 0;
+}
+
+// the kernels' copy of the run parameters
+void fill_dev_params(DevParams& p, const sphgpu_params* P)
+{
+    const int N = P->ntotal;
+    p.N = N; p.ndim = P->ndim; p.flknl = P->flknl; p.flbndy = P->flbndy; p.fli = P->fli;
+    p.if_move = P->if_move; p.flv = P->flv; p.inip = P->inip; p.step_regu = P->step_regu;
+    p.cxm = P->cxm; p.cym = P->cym; p.czm = P->czm; p.ctotal = P->ctotal;
+    p.water_minor = P->water_acc_type != 0; p.air_minor = P->air_acc_type != 0;
+    p.first_vbx_wall = N;
+    p.dr = P->dr; p.dt = P->dt;
+    p.xsph0 = P->xsph[0]; p.xsph1 = P->xsph[1]; p.xsph2 = P->xsph[2];
+    for (int a = 0; a < 3; a++) for (int b = 0; b < 2; b++) p.av[a][b] = P->art_vis[a][b];
+    p.gx = P->gx; p.gy = P->gy; p.gz = P->gz;
+    p.thr_min = P->threshold_min; p.thr_max = P->threshold_max;
+    p.interc = P->interc; p.pers = P->pers; p.perl = P->perl; p.perm = P->perm; p.permtype = P->permtype;
+    p.coe_bndy = P->coe_bndy;
+    for (int k = 0; k < 3; k++) p.move_vx[k] = P->move_vx[k];
+    p.xmin = P->xmin; p.xmax = P->xmax; p.ymin = P->ymin; p.ymax = P->ymax; p.zmin = P->zmin; p.zmax = P->zmax;
+    p.st_e = P->structure.e; p.st_poi = P->structure.poi;
+    p.g_acc = std::sqrt(P->gx * P->gx + P->gy * P->gy + P->gz * P->gz);   // CPP_10-interact1.cpp:28
+    p.art_stre_coe = P->art_stre_coe;
+    p.ss_type = P->ss_type; p.ss_myu = P->ss_myu; p.ss_zeta = P->ss_zeta;
+    p.ss_coupled = (P->ss_type >= 1 && P->ss_type <= 3 && P->ss_acc_type == 2) ? 1 : 0;
+    p.flts = P->flts;
+    p.flagum = P->flagum;
+    p.alphats = P->alphats;
+    p.cfl_on = 0; p.cfl_c = 0.0; p.cfl_f = 0.0;
+    p.st_vpu = P->structure.vpu;
+}
+
+// the buffers only some flag settings use, allocated when the flags first
+// need them (at create, or when sphgpu_update_params turns the flags on)
+int alloc_optional(sphgpu_ctx* c, const sphgpu_params* P)
+{
+    DevState& s = c->d[0].s;
+    const int N = c->N;
+    int r = 0;
+    auto need = [&](auto*& ptr, size_t count) {
+        if (!ptr) r |= dalloc(c, &ptr, count);
+    };
+    if (P->art_stre_coe > 0.0) need(s.rij, 9 * (size_t)N);
+    if (P->ss_type >= 1) {
+        need(s.ss_id, 3 * (size_t)N);
+        need(s.ss_con, 18 * (size_t)N);
+        need(s.ss_own, 6 * (size_t)N);
+        need(s.ss_fs, 6 * (size_t)N);
+    }
+    if (P->ss_type >= 1 && P->ss_type <= 3 && P->ss_acc_type == 2) need(s.cpl, 3 * (size_t)N);
+    if (P->flbndy == 5) {
+        need(s.fsol, 3 * (size_t)N);
+        need(s.fsol_on, (size_t)N);
+    }
+    if (P->flbndy != 1 && P->flbndy != 5) {
+        need(s.vel_bndy, 3 * (size_t)N);
+        need(s.vb, 12 * (size_t)N);
+        need(s.vx_vb, 3 * (size_t)N);
+        if (P->flbndy != 2) need(s.sb, 24 * (size_t)N);
+    }
+    // the other parity variant shares them
+    DevState& t = c->d[1].s;
+    t.rij = s.rij; t.ss_id = s.ss_id; t.ss_con = s.ss_con; t.ss_own = s.ss_own; t.ss_fs = s.ss_fs;
+    t.cpl = s.cpl; t.fsol = s.fsol; t.fsol_on = s.fsol_on;
+    t.vel_bndy = s.vel_bndy; t.vb = s.vb; t.vx_vb = s.vx_vb; t.sb = s.sb;
+    return r;
 }
 
 int end_bit_for(int m)
@@ -503,29 +572,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     cudaEventCreate(&c->ev1);
     const int N = c->N, M = P->ctotal + 4;
     Dev& d = c->d[0];
-    DevParams& p = d.p;
-    p.N = N; p.ndim = P->ndim; p.flknl = P->flknl; p.flbndy = P->flbndy; p.fli = P->fli;
-    p.if_move = P->if_move; p.flv = P->flv; p.inip = P->inip; p.step_regu = P->step_regu;
-    p.cxm = P->cxm; p.cym = P->cym; p.czm = P->czm; p.ctotal = P->ctotal;
-    p.water_minor = P->water_acc_type != 0; p.air_minor = P->air_acc_type != 0;
-    p.first_vbx_wall = N;
-    p.dr = P->dr; p.dt = P->dt;
-    p.xsph0 = P->xsph[0]; p.xsph1 = P->xsph[1]; p.xsph2 = P->xsph[2];
-    for (int a = 0; a < 3; a++) for (int b = 0; b < 2; b++) p.av[a][b] = P->art_vis[a][b];
-    p.gx = P->gx; p.gy = P->gy; p.gz = P->gz;
-    p.thr_min = P->threshold_min; p.thr_max = P->threshold_max;
-    p.interc = P->interc; p.pers = P->pers; p.perl = P->perl; p.perm = P->perm; p.permtype = P->permtype;
-    p.coe_bndy = P->coe_bndy;
-    for (int k = 0; k < 3; k++) p.move_vx[k] = P->move_vx[k];
-    p.xmin = P->xmin; p.xmax = P->xmax; p.ymin = P->ymin; p.ymax = P->ymax; p.zmin = P->zmin; p.zmax = P->zmax;
-    p.st_e = P->structure.e; p.st_poi = P->structure.poi;
-    p.g_acc = std::sqrt(P->gx * P->gx + P->gy * P->gy + P->gz * P->gz);   // CPP_10-interact1.cpp:28
-    p.art_stre_coe = P->art_stre_coe;
-    p.ss_type = P->ss_type; p.ss_myu = P->ss_myu; p.ss_zeta = P->ss_zeta;
-    p.ss_coupled = (P->ss_type >= 1 && P->ss_type <= 3 && P->ss_acc_type == 2) ? 1 : 0;
-    p.flts = P->flts;
-    p.flagum = P->flagum;
-    p.alphats = P->alphats;
+    fill_dev_params(d.p, P);
     DevState& s = d.s;
     int r = 0;
     r |= dalloc(c, &s.type, N); r |= dalloc(c, &s.matype, N); r |= dalloc(c, &s.etype, N); r |= dalloc(c, &s.permtype, N);
@@ -542,24 +589,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.de, 6 * (size_t)N); r |= dalloc(c, &s.we, 6 * (size_t)N); r |= dalloc(c, &s.color, N);
     r |= dalloc(c, &s.sr, 6 * (size_t)N); r |= dalloc(c, &s.pp, N);
     r |= dalloc(c, &s.eps_tmp, 6 * (size_t)N); r |= dalloc(c, &s.sig_tmp, 6 * (size_t)N);
-    if (P->art_stre_coe > 0.0) r |= dalloc(c, &s.rij, 9 * (size_t)N);
-    if (P->ss_type >= 1) {
-        r |= dalloc(c, &s.ss_id, 3 * (size_t)N);
-        r |= dalloc(c, &s.ss_con, 18 * (size_t)N);
-        r |= dalloc(c, &s.ss_own, 6 * (size_t)N);
-        r |= dalloc(c, &s.ss_fs, 6 * (size_t)N);
-    }
-    if (P->ss_type >= 1 && P->ss_type <= 3 && P->ss_acc_type == 2) r |= dalloc(c, &s.cpl, 3 * (size_t)N);
-    if (P->flbndy == 5) {
-        r |= dalloc(c, &s.fsol, 3 * (size_t)N);
-        r |= dalloc(c, &s.fsol_on, N);
-    }
-    if (P->flbndy != 1 && P->flbndy != 5) {
-        r |= dalloc(c, &s.vel_bndy, 3 * (size_t)N);
-        r |= dalloc(c, &s.vb, 12 * (size_t)N);
-        r |= dalloc(c, &s.vx_vb, 3 * (size_t)N);
-        if (P->flbndy != 2) r |= dalloc(c, &s.sb, 24 * (size_t)N);
-    }
+    r |= alloc_optional(c, P);
     r |= dalloc(c, &s.vx, 3 * (size_t)N); r |= dalloc(c, &s.vx_next, 3 * (size_t)N);
     r |= dalloc(c, &s.vxp, 3 * (size_t)N); r |= dalloc(c, &s.axp, 3 * (size_t)N); r |= dalloc(c, &s.ax, 3 * (size_t)N);
     r |= dalloc(c, &s.ux, 3 * (size_t)N);
@@ -582,6 +612,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.nbm, 10 * (size_t)N);
     r |= dalloc(c, &s.nbw, 4 * (size_t)SPH_NB_CAP * N);
     r |= dalloc(c, &s.err, 1); r |= dalloc(c, &s.step, 1);
+    r |= dalloc(c, &s.dtv, 1); r |= dalloc(c, &s.dtmin, 1);
     if (r) return fail(SPHGPU_E_CUDA);
     // cell_info() constructor values (Class_NNPS.cpp:68-72): the range of the
     // last cell, which the reference never resets, starts from them
@@ -675,6 +706,7 @@ int sphgpu_set_step(sphgpu_ctx* c, int l)
     CK(cudaMemcpyAsync(c->d[0].s.step, &l, sizeof(int), cudaMemcpyHostToDevice, c->st));
     CK(cudaStreamSynchronize(c->st));
     c->l_host = l;
+    c->part_done = 0;
     return 0;
 }
 
@@ -1072,6 +1104,95 @@ int sphgpu_download_particles(sphgpu_ctx* c, void* particles, int n, size_t stri
     return 0;
 }
 
+namespace {
+
+// Runs step l up to and including `upto` (1 parttocell, 2 partisearching,
+// 3 the rest of the step through update) from where the method entries left
+// it, with direct launches on the context's stream; returns the step's error
+// code.  A completed step advances l and the parity as sphgpu_step does.
+int run_parts(sphgpu_ctx* c, int upto)
+{
+    if (c->sticky) return c->sticky;
+    if (upto >= 3) {
+        int r = check_particles(c);
+        if (r) return r;
+    }
+    cudaSetDevice(c->device);
+    const Dev* d = &c->d[c->parity];
+    int parts = 0;
+    if (c->part_done < 1 && upto >= 1) parts |= 1;
+    if (c->part_done < 2 && upto >= 2) parts |= 2;
+    if (upto >= 3) parts |= 4;
+    if (parts) sphk_enqueue_nnps_parts(d, c->sort_tmp, c->sort_bytes, c->end_bit, c->st, nullptr, parts);
+    if (upto >= 3) {
+        if (!c->regu && c->l_host % c->P.step_regu == 0) { c->regu = true; invalidate_graphs(c); }
+        enqueue_physics(c, d, nullptr);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->st));
+    int err = 0, l = 0;
+    CK(cudaMemcpy(&err, c->d[0].s.err, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&l, c->d[0].s.step, sizeof(int), cudaMemcpyDeviceToHost));
+    if (upto >= 3) {
+        c->parity = (c->parity + (l - c->l_host)) & 1;
+        c->l_host = l;
+        if (err == 0) c->part_done = 0;
+    } else if (err == 0) {
+        c->part_done = upto;
+    }
+    return err;
+}
+
+}  // namespace
+
+int sphgpu_parttocell(sphgpu_ctx* c)
+{
+    if (!c) return SPHGPU_E_ARG;
+    if (c->part_done >= 1) return SPHGPU_E_STATE;     // step l's cell lists are already built
+    return run_parts(c, 1);
+}
+
+int sphgpu_partisearching(sphgpu_ctx* c)
+{
+    if (!c) return SPHGPU_E_ARG;
+    if (c->part_done >= 2) return SPHGPU_E_STATE;
+    return run_parts(c, 2);
+}
+
+int sphgpu_update(sphgpu_ctx* c)
+{
+    if (!c) return SPHGPU_E_ARG;
+    return run_parts(c, 3);
+}
+
+int sphgpu_update_params(sphgpu_ctx* c, const sphgpu_params* P)
+{
+    if (!c) return SPHGPU_E_ARG;
+    int r = check_params(P);
+    if (r) return r;
+    const sphgpu_params& Q = c->P;
+    // the particle count and the cell grid the buffers were sized for stay
+    if (P->ndim != Q.ndim || P->ntotal != Q.ntotal || P->cxm != Q.cxm || P->cym != Q.cym || P->czm != Q.czm ||
+        P->ctotal != Q.ctotal || P->xmin != Q.xmin || P->ymin != Q.ymin || P->zmin != Q.zmin ||
+        P->xmax != Q.xmax || P->ymax != Q.ymax || P->zmax != Q.zmax)
+        return SPHGPU_E_ARG;
+    cudaSetDevice(c->device);
+    r = alloc_optional(c, P);
+    if (r) return r;
+    for (int p = 0; p < 2; p++) {
+        DevParams& dp = c->d[p].p;
+        const DevParams keep = dp;
+        fill_dev_params(dp, P);
+        dp.first_vbx_wall = keep.first_vbx_wall;
+        dp.bulk = keep.bulk;
+        dp.cfl_on = keep.cfl_on; dp.cfl_c = keep.cfl_c; dp.cfl_f = keep.cfl_f;
+    }
+    c->P = *P;
+    invalidate_graphs(c);
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
 int sphgpu_step(sphgpu_ctx* c, int nsteps)
 {
     if (!c || nsteps < 0) return SPHGPU_E_ARG;
@@ -1079,6 +1200,12 @@ int sphgpu_step(sphgpu_ctx* c, int nsteps)
     if (nsteps == 0) return 0;
     int r = check_particles(c);
     if (r) return r;
+    // a step the method entries began is completed first
+    if (c->part_done) {
+        r = run_parts(c, 3);
+        if (r || nsteps == 1) return r;
+        nsteps--;
+    }
     // the regularisation passes (strain_regu / stress_regu) join the step
     // graphs from the first call whose steps include one with l % step_regu == 0
     if (!c->regu)
@@ -1104,6 +1231,37 @@ int sphgpu_step(sphgpu_ctx* c, int nsteps)
     c->parity = (c->parity + (l - l0)) & 1;
     c->l_host = l;
     return err;
+}
+
+int sphgpu_set_cfl(sphgpu_ctx* c, double cfl, double cfl_force)
+{
+    if (!c) return SPHGPU_E_ARG;
+    if (cfl > 0.0 && !(cfl_force > 0.0)) return SPHGPU_E_ARG;
+    cudaSetDevice(c->device);
+    const int on = cfl > 0.0 ? 1 : 0;
+    // the first step after turning it on runs with the input dt
+    const double dt0 = c->P.dt;
+    const unsigned long long inf = 0x7ff0000000000000ULL;
+    CK(cudaMemcpyAsync(c->d[0].s.dtv, &dt0, sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d[0].s.dtmin, &inf, sizeof(inf), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int p = 0; p < 2; p++) {
+        c->d[p].p.cfl_on = on;
+        c->d[p].p.cfl_c = on ? cfl : 0.0;
+        c->d[p].p.cfl_f = on ? cfl_force : 0.0;
+    }
+    invalidate_graphs(c);
+    return 0;
+}
+
+int sphgpu_get_dt(sphgpu_ctx* c, double* dt)
+{
+    if (!c || !dt) return SPHGPU_E_ARG;
+    if (!c->d[0].p.cfl_on) { *dt = c->P.dt; return 0; }
+    cudaSetDevice(c->device);
+    CK(cudaMemcpyAsync(dt, c->d[0].s.dtv, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
 }
 
 int sphgpu_nnps(sphgpu_ctx* c, int* ninflu, int* influ)

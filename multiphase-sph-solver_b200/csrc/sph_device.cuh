@@ -57,6 +57,13 @@ struct DevParams {
     int flts;                  // >= 1: TSSMP stress transformation around the soil models
     int flagum;                // 1: the saturation pass (one unsaturated Cam-clay layer)
     double alphats;            // TSSMP alpha
+    // adaptive time step (an extension, off unless sphgpu_set_cfl turns it
+    // on; the reference's dt is constant, CPP_12-2-dt.cpp:13-20): the step
+    // reads its dt from the device word dtv, which the last kernel of the
+    // previous step set from the CFL and force limits, capped at dt
+    int cfl_on;
+    double cfl_c, cfl_f;       // factors of h / (c + |v|) and sqrt(h / |a|)
+    double st_vpu;             // Para_Structure::vpu, the structure's sound speed
 };
 
 // Members of the soil record that only the unsaturated Cam-clay model, the
@@ -154,6 +161,8 @@ struct DevState {
     // control words
     int *err;                  // first error code raised (0 = none)
     int *step;                 // Para_Pro::l of the step being run
+    double *dtv;               // dt of the step being run (cfl_on)
+    unsigned long long *dtmin; // running minimum of the per-particle limits (bits of a positive double)
 };
 
 struct Dev {
@@ -162,6 +171,10 @@ struct Dev {
 };
 
 struct Pos { double x, y, z, h; };
+
+// the step's time increment: the input dt, or with the adaptive step on the
+// value the previous step's limit reduction left in dtv
+__device__ __forceinline__ double step_dt(const Dev& d) { return d.p.cfl_on ? *d.s.dtv : d.p.dt; }
 
 __device__ __forceinline__ Pos load_pos(const double* xh, int i)
 {

@@ -665,7 +665,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_DENS) k_density(Dev d)
         }
         if (fluid)
             for (int k = 0; k < nd; k++) drhot += up[k];
-        const double rhop = d.s.rhop[i], dt = d.p.dt;
+        const double rhop = d.s.rhop[i], dt = step_dt(d);
         if (ti == 1 && fabs(por) > 0.0001)
             rnew = rhop + drhot * dt + rhop * (por - pcop) / (1.0 - pcop);
         else
@@ -881,7 +881,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_STRESS) k_stress(Dev d)
     const int i = IDX, N = d.p.N;
     if (i >= N || *d.s.err) return;
     const int ti = d.s.type[i], l = *d.s.step;
-    const double dt = d.p.dt;
+    const double dt = step_dt(d);
     double s[6], ep[6], de[6], we9[9];
     for (int k = 0; k < 6; k++) {
         if (PHASE == 2) s[k] = d.s.sig_tmp[k * N + i];
@@ -1594,7 +1594,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b_tail(Dev d)
         for (int k = 0; k < 3; k++) ax[k] += tbrow[k];
     if (d.p.ss_coupled && (ti == 1 || ti == 2 || ti == 4))
         for (int k = 0; k < 3; k++) ax[k] += d.s.cpl[(size_t)k * N + i];
-    const double dt = d.p.dt;
+    const double dt = step_dt(d);
     double axp[3];
     for (int k = 0; k < 3; k++) axp[k] = d.s.axp[k * N + i];
     if (d.p.fli >= 1 && moving) {
@@ -1714,7 +1714,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_XSPH) k_xsph_update(Dev d)
     if (i >= N || *d.s.err) return;
     constexpr int nd = ND;
     const int ti = d.s.type[i], nn = nbr_count(d, i);
-    const double dt = d.p.dt;
+    const double dt = step_dt(d);
     const PairI<real> I = pair_i<ND, real>(d, i);
     double vm[3];
     for (int k = 0; k < 3; k++) vm[k] = d.s.vx_next[k * N + i];
@@ -2003,7 +2003,7 @@ __global__ void __launch_bounds__(128) k_ss_pair(Dev d)
     const int ti = d.s.type[i];
     if (!(ti == 1 || ti == 2)) return;
     const int form = d.p.ss_type, nn = nbr_count(d, i);
-    const double dt = d.p.dt, dr = d.p.dr, myu = d.p.ss_myu, zeta = d.p.ss_zeta;
+    const double dt = step_dt(d), dr = d.p.dr, myu = d.p.ss_myu, zeta = d.p.ss_zeta;
     const double reach = (form == 1) ? 0.5 * dr : dr;
     int ids[SPH_NB_CAP];
     double dsts[SPH_NB_CAP];
@@ -2299,7 +2299,7 @@ __global__ void __launch_bounds__(128) k_free_solid(Dev d)
     const int ti = d.s.type[i];
     if (ND == 2 && !(ti >= 1 && ti <= 4)) return;
     const int nn = nbr_count(d, i);
-    const double dt = d.p.dt, dr = d.p.dr, myu = d.p.ss_myu, zeta = d.p.ss_zeta;
+    const double dt = step_dt(d), dr = d.p.dr, myu = d.p.ss_myu, zeta = d.p.ss_zeta;
     int ids[SPH_NB_CAP];
     double dsts[SPH_NB_CAP];
     int total = 0;
@@ -2474,7 +2474,55 @@ __global__ void __launch_bounds__(128) k_coupled(Dev d)
 
 __global__ void k_step_done(Dev d)
 {
-    if (threadIdx.x == 0 && blockIdx.x == 0 && *d.s.err == 0) *d.s.step += 1;
+    if (threadIdx.x == 0 && blockIdx.x == 0 && *d.s.err == 0) {
+        *d.s.step += 1;
+        if (d.p.cfl_on) {
+            // the next step's dt: the reduced limit, capped at the input dt;
+            // the running minimum starts again from +inf
+            const double lim = __longlong_as_double((long long)*d.s.dtmin);
+            *d.s.dtv = (lim < d.p.dt) ? lim : d.p.dt;
+            *d.s.dtmin = 0x7ff0000000000000ULL;      // +inf
+        }
+    }
+}
+
+// Adaptive time step (an extension: the reference keeps dt constant,
+// CPP_12-2-dt.cpp:13-20).  For every water, soil, air and structure particle
+// after the update, the CFL limit cfl_c h / (c + |v|), c the sound speed of
+// its material (Para_Fluid / Para_Soil / Para_Structure::vpu), and the force
+// limit cfl_f sqrt(h / |a|); their minimum over the particles, reduced with
+// warp shuffles and one 64-bit atomicMin per warp on the bits of the positive
+// double (which order as the values do), becomes the next step's dt in
+// k_step_done.  Off (not launched) unless sphgpu_set_cfl turns it on.
+__global__ void __launch_bounds__(256) k_cfl(Dev d)
+{
+    const int N = d.p.N, nd = d.p.ndim;
+    if (*d.s.err) return;
+    double m = __longlong_as_double(0x7ff0000000000000LL);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const int t = d.s.type[i];
+        if (t < 1 || t > 4) continue;
+        const double c = (t == 1 || t == 3) ? d.s.f_vpu[i] : (t == 2) ? d.s.s_vpu[i] : d.p.st_vpu;
+        double v2 = 0.0, a2 = 0.0;
+        for (int k = 0; k < nd; k++) {
+            const double v = d.s.vxp[k * N + i], a = d.s.axp[k * N + i];
+            v2 = v2 + v * v;
+            a2 = a2 + a * a;
+        }
+        const double h = load_pos(d.s.xh, i).h;
+        double lim = d.p.cfl_c * (h / (c + sqrt(v2)));
+        if (a2 > 0.0) {
+            const double lf = d.p.cfl_f * sqrt(h / sqrt(a2));
+            if (lf < lim) lim = lf;
+        }
+        if (lim < m) m = lim;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double q = __shfl_xor_sync(0xffffffffu, m, o);
+        if (q < m) m = q;
+    }
+    if ((threadIdx.x & 31) == 0 && m > 0.0)
+        atomicMin(d.s.dtmin, (unsigned long long)__double_as_longlong(m));
 }
 
 // kernel_gradient_correction (CPP_3-NNPS.cpp:376-496): the inverse of
@@ -2628,33 +2676,47 @@ static_assert(sizeof(sphk_stage_names) / sizeof(sphk_stage_names[0]) == SPHK_NST
         else K<3><<<blocks, threads, 0, st>>>(__VA_ARGS__);                        \
     } while (0)
 #ifndef SPH_BULK32
-// the NNPS stage (+ kernel gradient correction); returns the number of this
-// library's kernels it launched
-extern "C" int sphk_enqueue_nnps(const Dev* dp, void* sort_tmp, size_t sort_bytes, int end_bit, cudaStream_t st,
-                                 cudaEvent_t* ev)
+// the NNPS stage (+ kernel gradient correction) as three parts, selected by
+// the bits of `parts`: 1 parttocell (cell keys, the sort, cell ranges),
+// 2 partisearching (the search and the pair records), 4 the kernel gradient
+// correction; returns the number of this library's kernels it launched
+extern "C" int sphk_enqueue_nnps_parts(const Dev* dp, void* sort_tmp, size_t sort_bytes, int end_bit,
+                                       cudaStream_t st, cudaEvent_t* ev, int parts)
 {
     const Dev& d = *dp;
     const int N = d.p.N;
     int n = 0;
-    REC(0);
-    LAUNCH_ND(k_cellkey, nblk(N, 256), 256, d); n++;
-    REC(1);
-    size_t bytes = sort_bytes;
-    cub::DeviceRadixSort::SortPairs(sort_tmp, bytes, d.s.key_in, d.s.key_out, d.s.val_in, d.s.pid_sorted,
-                                    N, 0, end_bit, st);
-    REC(2);
-    k_cellreset<<<nblk(d.p.ctotal, 256), 256, 0, st>>>(d); n++;
-    REC(3);
-    k_cellrange<<<nblk(N, 256), 256, 0, st>>>(d); n++;
-    REC(4);
-    LAUNCH_ND(k_nnps, nblk(N, 128), 128, d); n++;
-    REC(5);
-    LAUNCH_ND(k_nnps_resolve, nblk(N, 128), 128, d); n++;
-    REC(6);
-    LAUNCH_ND(k_pairw, nblk(N, 128), 128, d); n++;
-    REC(7);
-    if (d.p.flknl > 2) { LAUNCH_ND(k_kgc, nblk(N, 128), 128, d); n++; }
+    if (parts & 1) {
+        REC(0);
+        LAUNCH_ND(k_cellkey, nblk(N, 256), 256, d); n++;
+        REC(1);
+        size_t bytes = sort_bytes;
+        cub::DeviceRadixSort::SortPairs(sort_tmp, bytes, d.s.key_in, d.s.key_out, d.s.val_in, d.s.pid_sorted,
+                                        N, 0, end_bit, st);
+        REC(2);
+        k_cellreset<<<nblk(d.p.ctotal, 256), 256, 0, st>>>(d); n++;
+        REC(3);
+        k_cellrange<<<nblk(N, 256), 256, 0, st>>>(d); n++;
+    }
+    if (parts & 2) {
+        REC(4);
+        LAUNCH_ND(k_nnps, nblk(N, 128), 128, d); n++;
+        REC(5);
+        LAUNCH_ND(k_nnps_resolve, nblk(N, 128), 128, d); n++;
+        REC(6);
+        LAUNCH_ND(k_pairw, nblk(N, 128), 128, d); n++;
+    }
+    if (parts & 4) {
+        REC(7);
+        if (d.p.flknl > 2) { LAUNCH_ND(k_kgc, nblk(N, 128), 128, d); n++; }
+    }
     return n;
+}
+
+extern "C" int sphk_enqueue_nnps(const Dev* dp, void* sort_tmp, size_t sort_bytes, int end_bit, cudaStream_t st,
+                                 cudaEvent_t* ev)
+{
+    return sphk_enqueue_nnps_parts(dp, sort_tmp, sort_bytes, end_bit, st, ev, 7);
 }
 #endif  // !SPH_BULK32
 
@@ -2732,6 +2794,7 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
     } else if (d.p.flbndy == 3 || d.p.flbndy == 4 || d.p.flbndy == 13 || d.p.flbndy == 14) {
         k_tran_wall<<<nblk(N, 128), 128, 0, st>>>(d); n++;
     }
+    if (d.p.cfl_on) { k_cfl<<<148 * 8, 256, 0, st>>>(d); n++; }
     REC(20);
     k_step_done<<<1, 32, 0, st>>>(d); n++;
     REC(21);

@@ -226,6 +226,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_stage_name.argtypes = [C.c_int]
     lib.sphgpu_step_profiled.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
     lib.sphgpu_set_precision.argtypes = [C.c_void_p, C.c_int]
+    lib.sphgpu_set_cfl.argtypes = [C.c_void_p, C.c_double, C.c_double]
+    lib.sphgpu_get_dt.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     lib.sphgpu_kl_generate.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_int, C.c_void_p,
                                        C.c_int, C.c_void_p]
     lib.sphgpu_kl_synthesize.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_void_p, C.c_int,
@@ -339,6 +341,17 @@ class Engine:
     def set_precision(self, mode: int) -> None:
         """PREC_FP64 (the reference's arithmetic) or PREC_FP32_BULK."""
         self._check(self.lib.sphgpu_set_precision(self.h, int(mode)), "sphgpu_set_precision")
+
+    def set_cfl(self, cfl: float, cfl_force: float = 0.25) -> None:
+        """Adaptive dt from the CFL and force limits (cfl <= 0: off, the
+        reference's constant dt)."""
+        self._check(self.lib.sphgpu_set_cfl(self.h, float(cfl), float(cfl_force)), "sphgpu_set_cfl")
+
+    def dt(self) -> float:
+        """The dt the next step uses."""
+        v = C.c_double()
+        self._check(self.lib.sphgpu_get_dt(self.h, C.byref(v)), "sphgpu_get_dt")
+        return v.value
 
     @property
     def precision(self) -> int:

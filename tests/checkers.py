@@ -121,17 +121,23 @@ class Oracle:
         return err, ninflu, influ.reshape(self.n, 100), (wij.reshape(self.n, 100, 4) if with_wij else None)
 
 
-_rlib = None
+SHIM_SO = os.path.join(REPO, "oracle", "_ref", "libsphshim.so")
+_rlibs = {}
 
 
 def have_reference() -> bool:
     return os.path.exists(REF_SO)
 
 
-def reference_lib():
-    global _rlib
-    if _rlib is None:
-        lib = C.CDLL(REF_SO)
+def have_shim() -> bool:
+    return os.path.exists(SHIM_SO)
+
+
+def reference_lib(so: str = REF_SO):
+    """The reference driver library: REF_SO (the reference's own classes) or
+    SHIM_SO (the same driver with the step classes of the engine's shim)."""
+    if so not in _rlibs:
+        lib = C.CDLL(so)
         lib.ref_create.restype = C.c_void_p
         lib.ref_create.argtypes = [C.c_char_p, C.c_int]
         lib.ref_last_error.restype = C.c_int
@@ -146,15 +152,16 @@ def reference_lib():
         lib.ref_step.argtypes = [C.c_void_p, C.c_int]
         lib.ref_get_step.argtypes = [C.c_void_p]
         lib.ref_destroy.argtypes = [C.c_void_p]
-        _rlib = lib
-    return _rlib
+        _rlibs[so] = lib
+    return _rlibs[so]
 
 
 class Reference:
-    """The reference solver, initialised from an input.dat by its own code."""
+    """The reference solver, initialised from an input.dat by its own code
+    (with so=SHIM_SO: its step methods run on the GPU through the shim)."""
 
-    def __init__(self, input_dat: str, nthreads: int = 1):
-        self.lib = reference_lib()
+    def __init__(self, input_dat: str, nthreads: int = 1, so: str = REF_SO):
+        self.lib = reference_lib(so)
         h = self.lib.ref_create(input_dat.encode(), int(nthreads))
         if not h:
             raise RuntimeError(f"ref_create failed: {self.lib.ref_last_error()}")

@@ -157,6 +157,84 @@ def _column_tssmp():
     return sc
 
 
+# pore air (type 3, input block AP): density 1.293, initial pressure 100 Pa,
+# sound speed 30 m/s; the reference's air equation of state makes the
+# pressure -0.403 paa0 whatever the density (CPP_7-1-eos_CR.cpp:34)
+AIR = dict(dens=1.293, paa0=100.0, vis=1.8e-5, vpu=30.0, press_type=0, acc_type=0, pre_coe=0.0)
+
+
+def _three_phase(acc_type=0, unsat=True):
+    """The soil column with three phases (fla 1): pore water below z = 0.15 and
+    pore air (type 3) above it, both co-located with the soil; unsaturated
+    Cam-clay soil with the saturation pass (saturation 0.95-1, so that the
+    soil-air drag of interact1, weighted by (1 - satu)^2, is not zero) or
+    Drucker-Prager soil; acc_type 1 selects the minor momentum forms of both
+    fluids (fluid_acceleration_minorwater / _minorair)."""
+    def make():
+        sc = scenes.soil_column_3d(dx=0.1, steps=200)
+        if unsat:
+            sc = scenes.set_soil_model(sc, 3, **UMCC)
+        up = (sc.ptype == 1) & (sc.xp[:, 2] > 0.15)
+        sc.ptype[up] = 3
+        sc.flags["fla"] = 1
+        sc.air = dict(AIR, acc_type=acc_type)
+        sc.water[0]["acc_type"] = acc_type
+        return sc
+    return make
+
+
+def _dam_break_variant(acc_type=0, bhtype=0, moving=False, dx=0.04):
+    """The dam break with the minor water momentum form (acc_type 1), a
+    Bingham water (bhtype 1: friction angle 20 deg, yield stress 50 Pa,
+    strain_min 1e-3), or a moving right wall (if_move 1: the wall's particles
+    get matype 2 and move at -0.2 m/s along x from the first step,
+    veocity_update / update, CPP_11-xsph.cpp:61-84, CPP_12-1-update.cpp:38-47)."""
+    def make():
+        sc = scenes.dam_break_2d(dx=dx, steps=200)
+        sc.water[0]["acc_type"] = acc_type
+        if bhtype:
+            sc.water[0].update(bhtype=1, fai=20.0, c=50.0, strain_min=1.0e-3)
+        if moving:
+            right = (sc.ptype == 0) & (sc.xp[:, 0] > 1.6)
+            sc.matype[right] = 2
+            sc.problem["if_move"] = 1
+            sc.problem["move_vx"] = (-0.2, 0.0, 0.0)
+        return sc
+    return make
+
+
+def _column_moving_wall():
+    """The soil column whose far side wall (y > 0.5) moves towards the soil at
+    0.1 m/s (if_move 1, matype 2 wall particles)."""
+    sc = scenes.soil_column_3d(dx=0.1, steps=200)
+    wall = (sc.ptype == 0) & (sc.xp[:, 1] > 0.5)
+    sc.matype[wall] = 2
+    sc.problem["if_move"] = 1
+    sc.problem["move_vx"] = (0.0, -0.1, 0.0)
+    return sc
+
+
+def _geostatic(factory, inip, camclay=False, step_regu=100000000):
+    """A geostatic stage of `inip` steps (Para_Pro::inip): elastic stresses
+    while l < inip (CPP_7-2-constitutive.cpp:104-115), the damping of
+    soil_damping_geostress while l <= inip (CPP_9-4-derivation_stress.cpp:
+    850-897), strains reset at l == inip (CPP_7-1-strain.cpp:35-39) and
+    displacements restarted by update (CPP_12-1-update.cpp:19-28).  With
+    `camclay` the soil is subloading Cam-clay inside the TSSMP transformation
+    (flts 1), whose input line also carries the damping coefficient 0.05 that
+    gives the damping a nonzero cd."""
+    def make():
+        sc = factory()
+        if camclay:
+            sc = scenes.set_soil_model(sc, 1, **MCC)
+            sc.flags["flts"] = 1
+            sc.problem["ts"] = (0.5, 0.05)
+        sc.problem["inip"] = inip
+        sc.problem["step_regu"] = step_regu
+        return sc
+    return make
+
+
 CASES = {
     # name: (scene factory, steps)
     "dam_break_2d_dx0.04": (lambda: scenes.dam_break_2d(dx=0.04, steps=200), 25),
@@ -188,6 +266,16 @@ CASES = {
     "soil_column_3d_dx0.1_amcc": (_column_model(4, **AMCC), 20),
     "soil_column_3d_dx0.1_focc": (_column_model(8, **FOCC), 20),
     "soil_column_3d_dx0.1_tssmp": (_column_tssmp, 20),
+    "three_phase_column_3d_dx0.1_unsat": (_three_phase(0, True), 15),
+    "three_phase_column_3d_dx0.1_minor": (_three_phase(1, False), 15),
+    "dam_break_2d_dx0.04_minor": (_dam_break_variant(acc_type=1), 25),
+    "dam_break_2d_dx0.04_bingham": (_dam_break_variant(bhtype=1), 25),
+    "dam_break_2d_dx0.04_moving_wall": (_dam_break_variant(moving=True), 25),
+    "soil_column_3d_dx0.1_moving_wall": (_column_moving_wall, 15),
+    "soil_column_3d_dx0.1_geostatic": (_geostatic(lambda: scenes.soil_column_3d(dx=0.1, steps=200), 6), 12),
+    "soil_column_3d_dx0.1_geostatic_camclay": (
+        _geostatic(lambda: scenes.soil_column_3d(dx=0.1, steps=200), 6, camclay=True, step_regu=4), 12),
+    "slope_2d_H1_dx0.05_geostatic": (_geostatic(lambda: scenes.slope_2d(H=1.0, dx=0.05), 8), 16),
 }
 
 

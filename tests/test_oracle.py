@@ -25,7 +25,11 @@ CASES = ["dam_break_2d_dx0.04", "soil_column_3d_dx0.1", "soil_column_3d_dx0.1_kg
          "dam_break_2d_dx0.04_free_solid", "soil_column_3d_dx0.1_free_solid",
          "footing_2d_penalty_coupled", "footing_3d_deformable_coupled",
          "soil_column_3d_dx0.1_unsat", "soil_column_3d_dx0.1_amcc", "soil_column_3d_dx0.1_focc",
-         "soil_column_3d_dx0.1_tssmp"]
+         "soil_column_3d_dx0.1_tssmp",
+         "three_phase_column_3d_dx0.1_unsat", "three_phase_column_3d_dx0.1_minor",
+         "dam_break_2d_dx0.04_minor", "dam_break_2d_dx0.04_bingham", "dam_break_2d_dx0.04_moving_wall",
+         "soil_column_3d_dx0.1_moving_wall", "soil_column_3d_dx0.1_geostatic",
+         "soil_column_3d_dx0.1_geostatic_camclay", "slope_2d_H1_dx0.05_geostatic"]
 
 
 def _golden(name):
@@ -304,3 +308,22 @@ def test_live_reference_soil_models(label, factory, steps):
     if label in ("camclay", "camclay_2d", "mohr_coulomb"):
         t = ref.get_field("type")
         assert (np.abs(ref.get_field("adps")[t == 2]).sum(axis=1) > 0).any()
+
+
+@needs_ref
+def test_live_reference_dam_break_full_size():
+    """The 2-D dam break at its stated size (dx = 5 mm, 12,800 water and 2,178
+    wall particles) for 200 steps: the oracle in the reference's sequential
+    order is bit-identical to the reference."""
+    sc = scenes.dam_break_2d(dx=0.005, steps=2000)
+    ref = _live(sc)
+    fl, so = ref.materials()
+    orc = Oracle(ref.params, ORC_INPLACE)
+    orc.load_state({k: ref.get_field(k) for k in STATE_FIELDS}, fl, so)
+    assert ref.n == 14978
+    assert ref.step(200) == 0
+    assert orc.step(200) == 0
+    for k in STATE_FIELDS:
+        a, b = orc.get_field(k), ref.get_field(k)
+        same = (a == b) | (np.isnan(a) & np.isnan(b)) if a.dtype.kind == "f" else (a == b)
+        assert same.all(), k
