@@ -330,6 +330,94 @@ def kl_synthesis(eng, scene, device, R=32, K=400):
             "what": "tcgen05 kind::tf32 split-operand product, eigenfunction tiles generated in shared memory"}
 
 
+def slope_heights(count: int = 256, dx: float = 0.05, seed: int = 20261203) -> np.ndarray:
+    """Heights H = 5 + 7 u of the batched slopes, u uniform from a Philox
+    stream of the given seed, rounded to the particle spacing."""
+    u = np.random.Generator(np.random.Philox(seed)).random(count)
+    return np.round((5.0 + 7.0 * u) / dx) * dx
+
+
+def batched_slopes(args, device: int, count: int = 256, dx: float = 0.05, steps_run: int = 20000, K: int = 200):
+    """The batched Monte Carlo slope workload: `count` 2-D cohesive-frictional
+    slopes (1:1.5 face, 6.25 m crest, H from slope_heights, Drucker-Prager,
+    phi = 25 deg, E = 20 MPa, dry) in one batched context, each with its own
+    lognormal K-L cohesion field (mean 10 kPa, COV 0.3, correlation lengths
+    10 m / 1 m, K terms, its own standard normals).  Times K-L generation for
+    all instances, then args.steps steps after args.warmup, in the FP64 and
+    FP32-bulk forms; realisations per hour = count x 3600 / (K-L time +
+    steps_run x step time)."""
+    import sphgpu
+    H = slope_heights(count, dx)
+    insts, parts, first = [], [], 0
+    shared = None
+    keep = ("xp", "vxp", "axp", "rho", "rhop", "mass", "hl", "pre", "prep", "e", "sig", "satu", "porosity",
+            "cd", "type", "matype", "permtype", "etype")
+    cols = {k: [] for k in keep}
+    fl, so, doms = [], [], []
+    n_active = 0
+    for h in H:
+        sc = scenes.slope_2d(H=float(h), dx=dx, c=10.0e3, fai=25.0, E=2.0e7)
+        st = scenes.initialise(sc)
+        p = st.params
+        if shared is None:
+            shared = dict(p)
+        insts.append(sphgpu.Instance(first, sc.n, p["xmin"], p["xmax"], p["ymin"], p["ymax"], p["zmin"], p["zmax"],
+                                     p["cxm"], p["cym"], p["czm"], p["ctotal"]))
+        first += sc.n
+        n_active += sc.n_active()
+        for k in keep:
+            cols[k].append(st.fields[k])
+        fl.append(st.fluid)
+        so.append(st.soil)
+        d = scenes.kl_domain(sc)
+        doms.append(sphgpu.kl_domain(d["nb_min"], d["nb_max"], d["soil_max"], d["water_max"]))
+        del st
+    fields = {k: np.concatenate(v) for k, v in cols.items()}
+    del cols
+    fluid, soil = np.concatenate(fl), np.concatenate(so)
+    del fl, so
+    shared["ntotal"] = first
+    xi = np.random.Generator(np.random.Philox(20261204)).standard_normal((count, K))
+    field = sphgpu.kl_field(1, 2, 10.0e3, 3.0e3, [10.0, 1.0, 0.0])
+    out = {"instances": count, "particles": first, "active_particles": n_active, "dx": dx,
+           "heights_m": [float(H.min()), float(H.max())],
+           "particles_per_instance": [int(min(q.count for q in insts)), int(max(q.count for q in insts))]}
+    for form in ("fp64", "fp32_bulk"):
+        eng = sphgpu.Engine(shared, device=device, instances=insts)
+        eng.load_state(fields, fluid, soil)
+        t0 = time.perf_counter()
+        eng.kl_generate_batched(doms, field, xi)
+        kl_s = time.perf_counter() - t0
+        if form == "fp32_bulk":
+            eng.set_precision(sphgpu.PREC_FP32_BULK)
+        eng.step(args.warmup)
+        eng.synchronize()
+        eng.step(args.steps)
+        ms = eng.last_step_ms() / args.steps
+        eng.close()
+        runs_hr = count * 3600.0 / (kl_s + steps_run * ms / 1e3)
+        out[form] = {"ms_per_step": ms, "value": n_active / (ms / 1e3), "unit": "particle-updates/s",
+                     "kl_generate_s": kl_s, "rf_runs_per_hour": runs_hr}
+    out["fp32_bulk"]["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["fp32_bulk"]["ms_per_step"]
+    out["what"] = (f"{count} slopes in one batched context (one graph per step over all instances), "
+                   f"runs/hr for {steps_run} steps each with K-L generation")
+    return out
+
+
+def batched_slopes_cpu(threads: int, dx: float = 0.05, steps_run: int = 20000):
+    """The reference on one slope of the median height, on the host cores:
+    realisations per hour when each runs alone for steps_run steps."""
+    H = float(np.median(slope_heights()))
+    sc = scenes.slope_2d(H=H, dx=dx, c=10.0e3, fai=25.0, E=2.0e7)
+    r = run_reference(sc, 3, 1, threads)
+    if "unavailable" in r:
+        return None
+    return {"value": sc.n_active() / r["step_s"], "unit": "particle-updates/s", "ms_per_step": r["step_s"] * 1e3,
+            "rf_runs_per_hour": 3600.0 / (steps_run * r["step_s"]), "cores": threads, "kind": "reference",
+            "sample": f"3 steps (after 1 warm-up) of one slope, H = {H:g} m ({sc.n} particles); "
+                      f"its K-L generation not included"}
+
+
 def engine_arm(args, world, rank, local):
     import sphgpu
     scene = scenes.soil_column_3d(dx=args.dx, steps=5000)
@@ -400,6 +488,8 @@ def engine_arm(args, world, rank, local):
     bulk_ms, bulk_err, bulk_prof = bulk_form(st, args, device, ref_fields, moving)
     bulk_ms = dist_max(bulk_ms, world)
     kl = kl_synthesis(eng, scene, device) if not args.no_kl else None
+    eng.close()
+    batched = batched_slopes(args, device) if not args.no_batched else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -410,6 +500,8 @@ def engine_arm(args, world, rank, local):
             cpu = {"value": r["value"], "unit": "particle-updates/s", "cores": thr, "kind": "reference",
                    "sample": f"2 steps (after 1 warm-up) of the same scene at dx={2 * args.dx:g} "
                              f"({small.n} particles, {small.n_active()} active)"}
+        if batched is not None:
+            batched["cpu_baseline"] = batched_slopes_cpu(thr)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "particle-updates/s", "n_gpus": world,
@@ -441,6 +533,7 @@ def engine_arm(args, world, rank, local):
                               "stage_ms_per_step": {k: v / args.steps for k, v in bulk_prof.items() if v > 0.01}},
             },
             "kl_synthesis": kl,
+            "batched_slopes": batched,
             "e2e": {"value": e2e_value, "unit": "particle-updates/s",
                     "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                     "what": "Particle-record upload, material upload, K steps and Particle-record download "
@@ -448,7 +541,6 @@ def engine_arm(args, world, rank, local):
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))
-    eng.close()
     return 0
 
 
@@ -462,6 +554,7 @@ def main():
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kl", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         # host-only arm: rank 0 runs it, the other ranks exit without work

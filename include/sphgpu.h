@@ -131,6 +131,34 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* params, int device);
 int         sphgpu_last_create_error(void);
 void        sphgpu_destroy(sphgpu_ctx* ctx);
 int         sphgpu_get_params(const sphgpu_ctx* ctx, sphgpu_params* out);
+
+/*
+ * Batched context: many instances of the step (Monte Carlo realisations,
+ * slope geometries of uneven particle counts) in one particle system, each
+ * step running every instance in the same kernel launches (one CUDA graph per
+ * step), driven by a per-instance table of particle offsets and cell grids.
+ * The reference runs each instance as a project of its own (CPP_0-main.cpp,
+ * one SPH_Calculation per directory); here instance q holds particles
+ * [first, first + count) of the context, in the order of its own Particle
+ * array, and the cell grid its Cell_Con gives (celllist_ini1,
+ * CPP_3-NNPS.cpp:96-121); the instances follow one another (first of the
+ * first is 0, each next starts where the last ends).  `shared` holds every
+ * other parameter, the same for all instances (its ntotal and grid members
+ * are ignored).  Each instance evolves exactly as a context of its own would:
+ * its neighbours come from its own cells only, and every absolute particle
+ * index the reference uses (check_domain's first moving wall, tm_boundary's
+ * particle 0) is taken within the instance.  Fields, records and neighbour
+ * lists are indexed by the context's particle index.  sphgpu_update_params
+ * is not available for a batched context.
+ */
+typedef struct sphgpu_instance {
+    int    first, count;
+    double xmin, xmax, ymin, ymax, zmin, zmax;    /* Cell_Con domain box */
+    int    cxm, cym, czm, ctotal;                 /* Cell_Con cell counts */
+} sphgpu_instance;
+sphgpu_ctx* sphgpu_create_batched(const sphgpu_params* shared, const sphgpu_instance* inst, int ninst,
+                                  int device);
+int         sphgpu_instance_count(const sphgpu_ctx* ctx);
 /* Current step counter l (Para_Pro::l); starts at 1 like the reference. */
 int         sphgpu_get_step(const sphgpu_ctx* ctx);
 int         sphgpu_set_step(sphgpu_ctx* ctx, int l);
@@ -335,6 +363,16 @@ int sphgpu_kl_generate(sphgpu_ctx* ctx, const sphgpu_kl_domain* dom, const sphgp
  * coe_frict_cohesion is Flag_SpatialVariability::coe_frict_cohesion. */
 int sphgpu_kl_generate_corr(sphgpu_ctx* ctx, const sphgpu_kl_domain* dom, const sphgpu_kl_field pair[2],
                             double coe_frict_cohesion, const double* u2, int K, double* out);
+
+/*
+ * K-L fields of a batched context: one field per instance, each over the
+ * instance's own particles with its own domain doms[q] and its own standard
+ * normals xi[q * K .. q * K + K - 1] (what sphgpu_kl_generate does for one
+ * system, for every instance in one call, with one update of the material
+ * records at the end).  out, if non-NULL, receives ntotal values.
+ */
+int sphgpu_kl_generate_batched(sphgpu_ctx* ctx, const sphgpu_kl_domain* doms, const sphgpu_kl_field* field,
+                               const double* xi, int K, double* out);
 
 /*
  * Batched synthesis of R realisations of one field on the context's particles

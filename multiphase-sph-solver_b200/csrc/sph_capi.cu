@@ -144,6 +144,8 @@ struct sphgpu_ctx {
     std::vector<sphgpu_soil, UninitAlloc<sphgpu_soil>> h_soil;      // (K-L fields rewrite members)
     double* mat_pinned = nullptr;     // pinned, 4N: the per-particle material constants set_materials uploads
     int part_done = 0;     // parts of step l run through the method entries: 1 parttocell, 2 partisearching
+    std::vector<InstGrid> h_inst;     // batched context: the instance table (empty: one system)
+    InstGrid* d_inst = nullptr;
 };
 
 namespace {
@@ -217,6 +219,7 @@ void fill_dev_params(DevParams& p, const sphgpu_params* P)
     p.alphats = P->alphats;
     p.cfl_on = 0; p.cfl_c = 0.0; p.cfl_f = 0.0;
     p.st_vpu = P->structure.vpu;
+    p.ninst = 0;
 }
 
 // the buffers only some flag settings use, allocated when the flags first
@@ -352,13 +355,25 @@ void* field_ptr(sphgpu_ctx* c, const char* name)
     return nullptr;
 }
 
+// the first wall (index order) with matype > 2 in [a, b), or b
+int first_vbx_wall(const sphgpu_ctx* c, int a, int b)
+{
+    if (!c->h_type.empty() && !c->h_matype.empty())
+        for (int i = a; i < b; i++)
+            if (c->h_type[i] == 0 && c->h_matype[i] > 2) return i;
+    return b;
+}
+
 void update_static_params(sphgpu_ctx* c)
 {
-    int w0 = c->N;
-    if (!c->h_type.empty() && !c->h_matype.empty())
-        for (int i = 0; i < c->N; i++)
-            if (c->h_type[i] == 0 && c->h_matype[i] > 2) { w0 = i; break; }
+    const int w0 = first_vbx_wall(c, 0, c->N);
     for (int p = 0; p < 2; p++) c->d[p].p.first_vbx_wall = w0;
+    if (!c->h_inst.empty()) {
+        for (InstGrid& g : c->h_inst) g.first_vbx_wall = first_vbx_wall(c, g.first, g.first + g.count);
+        cuda_fail(c, cudaMemcpyAsync(c->d_inst, c->h_inst.data(), sizeof(InstGrid) * c->h_inst.size(),
+                                     cudaMemcpyHostToDevice, c->st), "cudaMemcpyAsync");
+        cuda_fail(c, cudaStreamSynchronize(c->st), "cudaStreamSynchronize");
+    }
     invalidate_graphs(c);
 }
 
@@ -1168,6 +1183,7 @@ int sphgpu_update(sphgpu_ctx* c)
 int sphgpu_update_params(sphgpu_ctx* c, const sphgpu_params* P)
 {
     if (!c) return SPHGPU_E_ARG;
+    if (!c->h_inst.empty()) return SPHGPU_E_STATE;   // a batched context keeps its instances' grids
     int r = check_params(P);
     if (r) return r;
     const sphgpu_params& Q = c->P;
@@ -1192,6 +1208,66 @@ int sphgpu_update_params(sphgpu_ctx* c, const sphgpu_params* P)
     CK(cudaStreamSynchronize(c->st));
     return 0;
 }
+
+sphgpu_ctx* sphgpu_create_batched(const sphgpu_params* shared, const sphgpu_instance* inst, int ninst, int device)
+{
+    g_create_error = SPHGPU_E_ARG;
+    if (!shared || !inst || ninst <= 0) return nullptr;
+    // the instances follow one another in the particle order, each with a
+    // grid of its own; the context numbers their cells one after another
+    std::vector<InstGrid> tab(ninst);
+    long long total = 0, cells = 0;
+    for (int q = 0; q < ninst; q++) {
+        const sphgpu_instance& a = inst[q];
+        if (a.first != total || a.count <= 0) return nullptr;
+        if (a.cxm <= 0 || a.cym <= 0 || a.czm <= 0 || (long long)a.cxm * a.cym * a.czm != a.ctotal) return nullptr;
+        InstGrid& g = tab[q];
+        g.xmin = a.xmin; g.ymin = a.ymin; g.zmin = a.zmin; g.xmax = a.xmax; g.ymax = a.ymax; g.zmax = a.zmax;
+        g.cxm = a.cxm; g.cym = a.cym; g.czm = a.czm; g.ctotal = a.ctotal;
+        g.cell_base = (int)cells;
+        g.first = a.first; g.count = a.count;
+        g.first_vbx_wall = a.first + a.count;
+        total += a.count;
+        cells += (long long)a.ctotal + 1;
+        if (total >= (1LL << 28) || cells >= (1LL << 30)) { g_create_error = SPHGPU_E_UNSUPPORTED; return nullptr; }
+    }
+    sphgpu_params P = *shared;
+    P.ntotal = (int)total;
+    P.cxm = (int)cells; P.cym = 1; P.czm = 1; P.ctotal = (int)cells;
+    P.xmin = tab[0].xmin; P.ymin = tab[0].ymin; P.zmin = tab[0].zmin;
+    P.xmax = tab[0].xmax; P.ymax = tab[0].ymax; P.zmax = tab[0].zmax;
+    sphgpu_ctx* c = sphgpu_create(&P, device);
+    if (!c) return nullptr;
+    c->h_inst = tab;
+    std::vector<int> pinst((size_t)total);
+    for (int q = 0; q < ninst; q++)
+        for (int i = tab[q].first; i < tab[q].first + tab[q].count; i++) pinst[i] = q;
+    int* d_pinst = nullptr;
+    int r = dalloc(c, &c->d_inst, (size_t)ninst);
+    r |= dalloc(c, &d_pinst, (size_t)total);
+    if (!r) r |= cuda_fail(c, cudaMemcpyAsync(d_pinst, pinst.data(), sizeof(int) * total, cudaMemcpyHostToDevice,
+                                              c->st), "cudaMemcpyAsync");
+    if (r) {
+        sphgpu_destroy(c);
+        g_create_error = SPHGPU_E_CUDA;
+        return nullptr;
+    }
+    for (int p = 0; p < 2; p++) {
+        c->d[p].p.ninst = ninst;
+        c->d[p].s.inst = c->d_inst;
+        c->d[p].s.pinst = d_pinst;
+    }
+    update_static_params(c);
+    if (c->sticky) {
+        sphgpu_destroy(c);
+        g_create_error = SPHGPU_E_CUDA;
+        return nullptr;
+    }
+    g_create_error = 0;
+    return c;
+}
+
+int sphgpu_instance_count(const sphgpu_ctx* c) { return c ? (int)c->h_inst.size() : -1; }
 
 int sphgpu_step(sphgpu_ctx* c, int nsteps)
 {
@@ -1470,8 +1546,9 @@ int kl_plan(sphgpu_ctx* c, const double a[3], const sphgpu_kl_field& f, int K, K
 // One field of SpatialVariables_Generate_2D / _3D for the context's
 // particles; d_out receives the values (NaN where the field writes none).
 int kl_one_field(sphgpu_ctx* c, const double a[3], const double x_trans[3], double soil_max, double water_max,
-                 const sphgpu_kl_field& f, const double* xi, int K, double* d_out)
+                 const sphgpu_kl_field& f, const double* xi, int K, double* d_out, int first = 0, int count = -1)
 {
+    if (count < 0) count = c->N - first;
     const int nd = c->P.ndim;
     if (f.type != 1 && f.type != 2) return 14;
     KLPlan plan;
@@ -1490,9 +1567,9 @@ int kl_one_field(sphgpu_ctx* c, const double a[3], const double x_trans[3], doub
             cuda_fail(c, cudaMemcpyAsync(b + off_xi, xi, 8 * (size_t)K, cudaMemcpyHostToDevice, c->st),
                       "cudaMemcpyAsync")) { rc = SPHGPU_E_CUDA; break; }
         const DevState& s = c->d[c->parity].s;
-        if (sphk_kl_field(c->N, nd, K, f.no, f.type, x_trans, f.mean_value, f.sd_value, f.coe_depth, soil_max,
-                          water_max, s.xh, s.type, b, (const double*)(b + off_se), (const double*)(b + off_xi),
-                          d_out, c->st)) { rc = SPHGPU_E_CUDA; break; }
+        if (sphk_kl_field(count, nd, K, f.no, f.type, x_trans, f.mean_value, f.sd_value, f.coe_depth, soil_max,
+                          water_max, s.xh + 4 * (size_t)first, s.type + first, b, (const double*)(b + off_se),
+                          (const double*)(b + off_xi), d_out + first, c->st)) { rc = SPHGPU_E_CUDA; break; }
         if (cuda_fail(c, cudaStreamSynchronize(c->st), "cudaStreamSynchronize")) { rc = SPHGPU_E_CUDA; break; }
     } while (0);
     cudaFree(buf);
@@ -1514,6 +1591,22 @@ int kl_dom(int nd, const sphgpu_kl_domain* dom, double a[3], double xt[3], doubl
     *soil_max = dom->soil_max[nd == 2 ? 1 : 2];
     *water_max = dom->water_max[nd == 2 ? 1 : 2];
     return (a[0] == 0.0 || a[1] == 0.0) ? 13 : 0;
+}
+
+// the field's values written into the host copies of the material records
+void kl_store(sphgpu_ctx* c, int no, const double* v, int first, int count)
+{
+    for (int i = first; i < first + count; i++) {
+        if (v[i] != v[i]) continue;
+        switch (no) {
+        case 0: c->h_soil[i].fai = v[i]; break;
+        case 1: c->h_soil[i].c = v[i]; break;
+        case 2: c->h_soil[i].cop = v[i]; break;
+        case 3: c->h_soil[i].ds = v[i]; break;
+        case 4: c->h_fluid[i].fai = v[i]; break;
+        case 5: c->h_fluid[i].c = v[i]; break;
+        }
+    }
 }
 
 int kl_run(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_kl_field* fields, int nfields,
@@ -1542,18 +1635,7 @@ int kl_run(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_kl_field* fi
             break;
         }
         if (out) std::memcpy(out + (size_t)q * N, v.data(), sizeof(double) * N);
-        const int no = fields[q].no;
-        for (int i = 0; i < N; i++) {
-            if (v[i] != v[i]) continue;
-            switch (no) {
-            case 0: c->h_soil[i].fai = v[i]; break;
-            case 1: c->h_soil[i].c = v[i]; break;
-            case 2: c->h_soil[i].cop = v[i]; break;
-            case 3: c->h_soil[i].ds = v[i]; break;
-            case 4: c->h_fluid[i].fai = v[i]; break;
-            case 5: c->h_fluid[i].c = v[i]; break;
-            }
-        }
+        kl_store(c, fields[q].no, v.data(), 0, N);
     }
     cudaFree(d_out);
     if (rc) return rc;
@@ -1562,6 +1644,38 @@ int kl_run(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_kl_field* fi
 }
 
 }  // namespace
+
+int sphgpu_kl_generate_batched(sphgpu_ctx* c, const sphgpu_kl_domain* doms, const sphgpu_kl_field* f,
+                               const double* xi, int K, double* out)
+{
+    if (!c || !doms || !f || !xi || K <= 0 || c->h_inst.empty()) return SPHGPU_E_ARG;
+    if (f->no < 0 || f->no > 5) return SPHGPU_E_ARG;
+    if (c->h_type.empty() || (f->no <= 3 && c->h_soil.empty()) || (f->no >= 4 && c->h_fluid.empty()))
+        return SPHGPU_E_STATE;
+    cudaSetDevice(c->device);
+    const int nd = c->P.ndim, N = c->N;
+    double* d_out = nullptr;
+    CK(cudaMalloc(&d_out, sizeof(double) * N));
+    int rc = 0;
+    for (size_t q = 0; q < c->h_inst.size() && !rc; q++) {
+        double a[3], xt[3], soil_max, water_max;
+        if (kl_dom(nd, &doms[q], a, xt, &soil_max, &water_max)) { rc = 13; break; }
+        rc = kl_one_field(c, a, xt, soil_max, water_max, *f, xi + q * (size_t)K, K, d_out, c->h_inst[q].first,
+                          c->h_inst[q].count);
+    }
+    std::vector<double> v;
+    if (!rc) {
+        v.resize(N);
+        if (cuda_fail(c, cudaMemcpy(v.data(), d_out, sizeof(double) * N, cudaMemcpyDeviceToHost), "cudaMemcpy"))
+            rc = SPHGPU_E_CUDA;
+    }
+    cudaFree(d_out);
+    if (rc) return rc;
+    if (out) std::memcpy(out, v.data(), sizeof(double) * N);
+    kl_store(c, f->no, v.data(), 0, N);
+    return sphgpu_set_materials(c, c->h_fluid.empty() ? nullptr : c->h_fluid.data(),
+                                c->h_soil.empty() ? nullptr : c->h_soil.data(), N);
+}
 
 int sphgpu_kl_generate(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_kl_field* fields, int nfields,
                        const double* xi, int K, double* out)

@@ -32,6 +32,17 @@
 #define SPH_ERR_NEIGH 5        // partisearching, CPP_3-NNPS.cpp:313-319
 #define SPHK_NSTAGES 21        // entries of sphk_stage_names (one event bracket each)
 
+// One instance of a batched context: its particle range, its own cell grid
+// (Cell_Con, celllist_ini1) and where its cells start in the context's cell
+// numbering.  The instances share every other parameter.
+struct InstGrid {
+    double xmin, ymin, zmin, xmax, ymax, zmax;
+    int cxm, cym, czm, ctotal;
+    int cell_base;             // context cell id of the instance's cell 0
+    int first, count;          // particles [first, first + count)
+    int first_vbx_wall;        // its first wall (index order) with matype > 2, or first + count
+};
+
 struct DevParams {
     int N, ndim, flknl, flbndy, fli, if_move, flv, inip, step_regu;
     int cxm, cym, czm, ctotal;
@@ -64,6 +75,7 @@ struct DevParams {
     int cfl_on;
     double cfl_c, cfl_f;       // factors of h / (c + |v|) and sqrt(h / |a|)
     double st_vpu;             // Para_Structure::vpu, the structure's sound speed
+    int ninst;                 // batched context: number of instances (0: one system)
 };
 
 // Members of the soil record that only the unsaturated Cam-clay model, the
@@ -161,6 +173,8 @@ struct DevState {
     // control words
     int *err;                  // first error code raised (0 = none)
     int *step;                 // Para_Pro::l of the step being run
+    const InstGrid *inst;      // batched context: the instance table (ninst)
+    int *pinst;                // batched context: each particle's instance
     double *dtv;               // dt of the step being run (cfl_on)
     unsigned long long *dtmin; // running minimum of the per-particle limits (bits of a positive double)
 };
@@ -171,6 +185,24 @@ struct Dev {
 };
 
 struct Pos { double x, y, z, h; };
+
+// The cell grid and domain box of particle i: the context's, or in a batched
+// context those of the particle's instance, whose cells are numbered from
+// `base` in the context's cell ids.
+struct CellGrid {
+    int cxm, cym, czm, ctotal, base, w0;
+    double xmin, ymin, zmin, xmax, ymax, zmax;
+};
+
+__device__ __forceinline__ CellGrid cell_grid(const Dev& d, int i)
+{
+    if (d.p.ninst == 0)
+        return CellGrid{d.p.cxm, d.p.cym, d.p.czm, d.p.ctotal, 0, d.p.first_vbx_wall,
+                        d.p.xmin, d.p.ymin, d.p.zmin, d.p.xmax, d.p.ymax, d.p.zmax};
+    const InstGrid& g = d.s.inst[d.s.pinst[i]];
+    return CellGrid{g.cxm, g.cym, g.czm, g.ctotal, g.cell_base, g.first_vbx_wall,
+                    g.xmin, g.ymin, g.zmin, g.xmax, g.ymax, g.zmax};
+}
 
 // the step's time increment: the input dt, or with the adaptive step on the
 // value the previous step's limit reduction left in dtv

@@ -114,18 +114,21 @@ __device__ __forceinline__ int to_int_x86(double v)
     return (v >= -2147483648.0 && v < 2147483648.0) ? (int)v : INT_MIN;
 }
 
-// cell_link slot p of cell c (celllist_ini2, CPP_3-NNPS.cpp:124-171).
-__device__ __forceinline__ int cell_link(const DevParams& p, int c, int slot)
+// cell_link slot p of cell c (celllist_ini2, CPP_3-NNPS.cpp:124-171) on the
+// grid g, in the context's cell ids (0: no cell)
+template <int ND>
+__device__ __forceinline__ int cell_link(const CellGrid& g, int c, int slot)
 {
     int v;
-    if (p.ndim == 2) {
+    const int lc = c - g.base;
+    if (ND == 2) {
         int ky = slot / 3 + 1, kx = slot % 3 + 1;
-        v = (kx - 2) * p.cym + ky - 2 + c;
+        v = (kx - 2) * g.cym + ky - 2 + lc;
     } else {
         int kz = slot / 9 + 1, kx = (slot / 3) % 3 + 1, ky = slot % 3 + 1;
-        v = (ky - 2) * p.cxm * p.czm + (kx - 2) * p.czm + kz - 2 + c;
+        v = (ky - 2) * g.cxm * g.czm + (kx - 2) * g.czm + kz - 2 + lc;
     }
-    return (v < 0 || v > p.ctotal) ? 0 : v;
+    return (v <= 0 || v > g.ctotal) ? 0 : v + g.base;
 }
 
 __device__ __forceinline__ int nbr_count(const Dev& d, int i)
@@ -221,7 +224,8 @@ __global__ void k_cellkey(Dev d)
     if (i >= N || *d.s.err) return;
     const Pos q = load_pos(d.s.xh, i);
     const double xp[3] = {q.x, q.y, q.z};
-    const double xmin[3] = {d.p.xmin, d.p.ymin, d.p.zmin};
+    const CellGrid g = cell_grid(d, i);
+    const double xmin[3] = {g.xmin, g.ymin, g.zmin};
     const double dr = 2.0 * d.p.dr;
     int nx_t[3] = {0, 0, 0};
     for (int j = 0; j < ND; j++) {
@@ -231,15 +235,16 @@ __global__ void k_cellkey(Dev d)
     }
     unsigned key;
     if (ND == 2)
-        key = (unsigned)d.p.cym * (unsigned)(nx_t[0] - 1) + (unsigned)nx_t[1];
+        key = (unsigned)g.cym * (unsigned)(nx_t[0] - 1) + (unsigned)nx_t[1];
     else
-        key = (unsigned)d.p.cxm * (unsigned)d.p.czm * (unsigned)(nx_t[1] - 1) +
-              (unsigned)d.p.czm * (unsigned)(nx_t[0] - 1) + (unsigned)nx_t[2];
+        key = (unsigned)g.cxm * (unsigned)g.czm * (unsigned)(nx_t[1] - 1) +
+              (unsigned)g.czm * (unsigned)(nx_t[0] - 1) + (unsigned)nx_t[2];
     int c = (int)key;
-    if (!(c > 0 && c <= d.p.ctotal)) {
+    if (!(c > 0 && c <= g.ctotal)) {
         raise_err(d.s.err, SPH_ERR_CELL);
         c = 0;
     }
+    c += g.base;
     d.s.cell[i] = c;
     // reversed input order: the stable radix sort then keeps equal keys in
     // descending particle index, the order Binary_Sort's merge produces
@@ -251,6 +256,16 @@ __global__ void k_cellreset(Dev d)
 {
     const int c = IDX;
     if (c >= d.p.ctotal || *d.s.err) return;
+    if (d.p.ninst > 0) {
+        // each instance's own cell ctotal keeps its range, as in one system
+        int lo = 0, hi = d.p.ninst - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (d.s.inst[mid].cell_base <= c) lo = mid;
+            else hi = mid - 1;
+        }
+        if (c - d.s.inst[lo].cell_base == d.s.inst[lo].ctotal) return;
+    }
     d.s.cstart[c] = 10000000;
     d.s.cend[c] = -10000000;
 }
@@ -265,21 +280,22 @@ __global__ void k_cellrange(Dev d)
     const uint32_t c = d.s.key_out[q];
     const bool first = (q == 0) || d.s.key_out[q - 1] != c;
     const bool last = (q == N - 1) || d.s.key_out[q + 1] != c;
-    if ((int)c == d.p.ctotal) {
+    const int pid = d.s.pid_sorted[q];
+    const CellGrid g = cell_grid(d, pid);
+    if ((int)c - g.base == g.ctotal) {
         if (first) atomicMin(&d.s.cstart[c], q);
         if (last) atomicMax(&d.s.cend[c], q);
     } else {
         if (first) d.s.cstart[c] = q;
         if (last) d.s.cend[c] = q;
     }
-    const int pid = d.s.pid_sorted[q];
     d.s.sortpos[pid] = q;
     const int t = d.s.type[pid];
     d.s.pts[q] = (pid << 3) | ((t >= 0 && t <= 4) ? t : 7);
     const Pos r = load_pos(d.s.xh, pid);
     store_pos(d.s.xs, q, r);
     reinterpret_cast<float4*>(d.s.xsf)[q] =
-        make_float4((float)(r.x - d.p.xmin), (float)(r.y - d.p.ymin), (float)(r.z - d.p.zmin), (float)r.h);
+        make_float4((float)(r.x - g.xmin), (float)(r.y - g.ymin), (float)(r.z - g.zmin), (float)r.h);
 }
 
 // partisearching (CPP_3-NNPS.cpp:265-374): neighbours of i in stencil order,
@@ -410,9 +426,10 @@ __device__ __forceinline__ int nnps_direct(const Dev& d, int i, int nc, const Po
     constexpr int nst = (ND == 2) ? 9 : 27;
     const double xi[3] = {pi.x, pi.y, pi.z};
     const float4* xsf = reinterpret_cast<const float4*>(d.s.xsf);
+    const CellGrid g = cell_grid(d, i);
     int cnt = 0;
     for (int nj = 0; nj < nst; nj++) {
-        const int nl = cell_link(d.p, nc, nj);
+        const int nl = cell_link<ND>(g, nc, nj);
         if (nl <= 0) continue;
         const int start = d.s.cstart[nl], end = d.s.cend[nl];
         for (int q = start; q <= end; q++) {
@@ -468,7 +485,8 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_nnps(Dev d)
     const int q = IDX, N = d.p.N;
     if (q >= N || *d.s.err) return;
     int np = 0;   // provisional entries
-    if (d.s.type[d.s.pid_sorted[q]] != 7) {
+    const int pid = d.s.pid_sorted[q];
+    if (d.s.type[pid] != 7) {
         constexpr int nst = (ND == 2) ? 9 : 27;
         constexpr float U = 5.9604645e-8f;     // 2^-24
         const float4* xsf = reinterpret_cast<const float4*>(d.s.xsf);
@@ -481,9 +499,10 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_nnps(Dev d)
             np = -1;
         } else {
             const Prefilter P = make_prefilter<ND>(fi.x, fi.y, fz, fi.w, 2.2f * U * Fi, 32.f * U);
+            const CellGrid g = cell_grid(d, pid);
             int* row = d.s.nbrs + q;
             for (int nj = 0; nj < nst; nj++) {
-                const int nl = cell_link(d.p, nc, nj);
+                const int nl = cell_link<ND>(g, nc, nj);
                 if (nl <= 0) continue;
                 const int start = d.s.cstart[nl], end = d.s.cend[nl];
                 for (int c = start; c <= end; c++) {
@@ -1783,7 +1802,8 @@ __global__ void __launch_bounds__(128, SPH_MINB_XSPH) k_xsph_update(Dev d)
         for (int k = 0; k < 3; k++) d.s.vx_vb[k * N + i] = vn[k];
     if (ti != 0 && ti != 7) {
         const double dr = d.p.dr;
-        const double bmax[3] = {d.p.xmax, d.p.ymax, d.p.zmax}, bmin[3] = {d.p.xmin, d.p.ymin, d.p.zmin};
+        const CellGrid g = cell_grid(d, i);
+        const double bmax[3] = {g.xmax, g.ymax, g.zmax}, bmin[3] = {g.xmin, g.ymin, g.zmin};
         bool hit = false;
         if (I.x[0] - bmax[0] >= -0.5 * dr) hit = true;
         if (I.x[0] - bmin[0] <= 0.5 * dr) hit = true;
@@ -1792,7 +1812,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_XSPH) k_xsph_update(Dev d)
         if (I.x[2] - bmax[2] >= -0.5 * dr && nd == 3) hit = true;
         if (I.x[2] - bmin[2] <= 0.5 * dr && nd == 3) hit = true;
         if (hit) {
-            const int w0 = d.p.first_vbx_wall;
+            const int w0 = g.w0;
             for (int k = 0; k < 3; k++) vn[k] = (i > w0) ? d.s.interfss[k * N + w0] : 0.0;
         }
     }
@@ -1836,7 +1856,8 @@ __global__ void __launch_bounds__(128, SPH_MINB_XSPH) k_xsph_update(Dev d)
 // through the three nearest (3-D; plane_two_points when they are collinear,
 // D = 1 from clPlane() unless plane_two_points sets it), the particle's
 // distance to it, and vel_bndy = (1 - beta) v + beta v_wall, v_wall the
-// interfss of the last wall of matype > 2 in the list (particle 0 if none).
+// interfss of the last wall of matype > 2 in the list (particle 0 if none;
+// in a batched context the instance's first particle).
 template <int ND>
 __global__ void __launch_bounds__(128) k_tm_vb(Dev d)
 {
@@ -1847,7 +1868,8 @@ __global__ void __launch_bounds__(128) k_tm_vb(Dev d)
     const int nn = nbr_count(d, i);
     int ids[SPH_NB_CAP];
     double dsts[SPH_NB_CAP];
-    int total = 0, id = 0;
+    // without such a wall the reference reads particle 0 (of the instance)
+    int total = 0, id = (d.p.ninst > 0) ? d.s.inst[d.s.pinst[i]].first : 0;
     const Pos P = load_pos(d.s.xh, i);
     for (int q = 0; q < nn; q++) {
         const int j = d.s.nbr[(size_t)q * N + i];

@@ -66,6 +66,14 @@ class Params(C.Structure):
     ]
 
 
+class Instance(C.Structure):
+    """sphgpu_instance: one instance of a batched context."""
+    _fields_ = [("first", C.c_int), ("count", C.c_int),
+                ("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double), ("ymax", C.c_double),
+                ("zmin", C.c_double), ("zmax", C.c_double),
+                ("cxm", C.c_int), ("cym", C.c_int), ("czm", C.c_int), ("ctotal", C.c_int)]
+
+
 def params_from_dict(d: dict) -> Params:
     p = Params()
     for name, ctype in Params._fields_:
@@ -235,6 +243,15 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_kl_generate_corr.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_double,
                                             C.c_void_p, C.c_int, C.c_void_p]
     lib.sphgpu_get_precision.argtypes = [C.c_void_p]
+    lib.sphgpu_create_batched.restype = C.c_void_p
+    lib.sphgpu_create_batched.argtypes = [C.POINTER(Params), C.POINTER(Instance), C.c_int, C.c_int]
+    lib.sphgpu_instance_count.argtypes = [C.c_void_p]
+    lib.sphgpu_kl_generate_batched.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_void_p,
+                                               C.c_int, C.c_void_p]
+    lib.sphgpu_update_params.argtypes = [C.c_void_p, C.POINTER(Params)]
+    lib.sphgpu_parttocell.argtypes = [C.c_void_p]
+    lib.sphgpu_partisearching.argtypes = [C.c_void_p]
+    lib.sphgpu_update.argtypes = [C.c_void_p]
     _lib = lib
     return lib
 
@@ -244,18 +261,29 @@ def _ptr(a: np.ndarray) -> C.c_void_p:
 
 
 class Engine:
-    """One particle system on one GPU (sphgpu_ctx)."""
+    """One particle system on one GPU (sphgpu_ctx); with `instances`, a
+    batched context of several systems that share `params` but for their
+    particle ranges and cell grids (sphgpu_create_batched)."""
 
-    def __init__(self, params: dict | Params, device: int = 0):
+    def __init__(self, params: dict | Params, device: int = 0, instances=None):
         self.lib = load_library()
         if self.lib.sphgpu_device_count() <= 0:
             raise SPHError(102, "sphgpu_device_count")
         self.params = params if isinstance(params, Params) else params_from_dict(params)
-        h = self.lib.sphgpu_create(C.byref(self.params), int(device))
+        if instances is None:
+            h = self.lib.sphgpu_create(C.byref(self.params), int(device))
+            what = "sphgpu_create"
+        else:
+            arr = (Instance * len(instances))(*instances)
+            h = self.lib.sphgpu_create_batched(C.byref(self.params), arr, len(instances), int(device))
+            what = "sphgpu_create_batched"
+            if h:
+                self.params.ntotal = sum(int(q.count) for q in instances)
         if not h:
-            raise SPHError(self.lib.sphgpu_last_create_error(), "sphgpu_create")
+            raise SPHError(self.lib.sphgpu_last_create_error(), what)
         self.h = C.c_void_p(h)
         self.n = int(self.params.ntotal)
+        self.instances = instances
 
     def close(self):
         if getattr(self, "h", None):
@@ -342,6 +370,30 @@ class Engine:
         """PREC_FP64 (the reference's arithmetic) or PREC_FP32_BULK."""
         self._check(self.lib.sphgpu_set_precision(self.h, int(mode)), "sphgpu_set_precision")
 
+    def kl_generate_batched(self, doms, field: "KLField", xi: np.ndarray) -> np.ndarray:
+        """One K-L field per instance, doms[q] its domain and xi[q] its K
+        standard normals; returns the n values written (NaN where none)."""
+        xi = np.ascontiguousarray(xi, dtype=np.float64)
+        arr = (KLDomain * len(doms))(*doms)
+        out = np.empty(self.n)
+        self._check(self.lib.sphgpu_kl_generate_batched(self.h, arr, C.byref(field), _ptr(xi), xi.shape[1],
+                                                        _ptr(out)), "sphgpu_kl_generate_batched")
+        return out
+
+    def update_params(self, params: dict | Params) -> None:
+        p = params if isinstance(params, Params) else params_from_dict(params)
+        self._check(self.lib.sphgpu_update_params(self.h, C.byref(p)), "sphgpu_update_params")
+        self.params = p
+
+    def parttocell(self) -> int:
+        return int(self.lib.sphgpu_parttocell(self.h))
+
+    def partisearching(self) -> int:
+        return int(self.lib.sphgpu_partisearching(self.h))
+
+    def update(self) -> int:
+        return int(self.lib.sphgpu_update(self.h))
+
     def set_cfl(self, cfl: float, cfl_force: float = 0.25) -> None:
         """Adaptive dt from the CFL and force limits (cfl <= 0: off, the
         reference's constant dt)."""
@@ -386,3 +438,22 @@ class Engine:
         ms = np.zeros(k)
         self._check(self.lib.sphgpu_step_profiled(self.h, int(nsteps), _ptr(ms)), "sphgpu_step_profiled")
         return {self.lib.sphgpu_stage_name(i).decode(): float(ms[i]) for i in range(k)}
+
+
+def batch(states) -> tuple:
+    """Concatenate initial states (scenes.initialise results of scenes that
+    share every parameter but their geometry) into the arguments of a batched
+    Engine: (shared params, instances, fields, fluid records, soil records)."""
+    insts, first = [], 0
+    for st in states:
+        p = st.params
+        n = int(p["ntotal"])
+        insts.append(Instance(first, n, p["xmin"], p["xmax"], p["ymin"], p["ymax"], p["zmin"], p["zmax"],
+                              p["cxm"], p["cym"], p["czm"], p["ctotal"]))
+        first += n
+    fields = {k: np.concatenate([st.fields[k] for st in states]) for k in states[0].fields}
+    fluid = np.concatenate([st.fluid for st in states])
+    soil = np.concatenate([st.soil for st in states])
+    shared = dict(states[0].params)
+    shared["ntotal"] = first
+    return shared, insts, fields, fluid, soil
