@@ -388,6 +388,15 @@ int sphgpu_kl_generate_batched(sphgpu_ctx* ctx, const sphgpu_kl_domain* doms, co
  * completion wait expired (the outputs are then incomplete).
  */
 #define SPHGPU_E_KL_TIMEOUT 105
+/*
+ * Self-test of the synthesis kernel's failure path (no counterpart in the
+ * reference): one CTA of the kernel takes its tensor memory and waits
+ * budget_cycles SM clocks on a completion barrier that nothing will signal,
+ * before it has issued any MMA; the wait must expire, the kernel must record
+ * the timeout and release the memory, and the context stays usable.  Returns
+ * SPHGPU_E_KL_TIMEOUT when that happened (the expected result).
+ */
+int sphgpu_kl_wait_check(sphgpu_ctx* ctx, long long budget_cycles);
 int sphgpu_kl_synthesize(sphgpu_ctx* ctx, const sphgpu_kl_domain* dom, const sphgpu_kl_field* field,
                          const double* xi, int R, int K, float* d_out, double* kernel_ms);
 

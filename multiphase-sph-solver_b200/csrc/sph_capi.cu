@@ -39,6 +39,7 @@ extern "C" int sphk_kl_field(int n, int ndim, int K, int no, int type, const dou
                              const int* d_type, const void* d_terms, const double* d_sqrt_eig, const double* d_xi,
                              double* d_out, cudaStream_t st);
 extern "C" size_t sphk_kl_term_bytes(void);
+extern "C" int sphk_kl_wait_probe(long long budget, int* d_err, cudaStream_t st);
 extern "C" size_t sphk_kl_tc_term_bytes(void);
 extern "C" int sphk_kl_synthesize(int n, int ndim, int K, int R, int no, int type, const double* x_trans,
                                   double mean_value, double sd_value, double coe_depth, double soil_max,
@@ -1714,6 +1715,22 @@ int sphgpu_kl_generate_corr(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sp
     return kl_run(c, dom, pair, 2, xis, K, out);
 }
 
+
+int sphgpu_kl_wait_check(sphgpu_ctx* c, long long budget_cycles)
+{
+    if (!c || budget_cycles <= 0) return SPHGPU_E_ARG;
+    cudaSetDevice(c->device);
+    int* d_err = nullptr;
+    CK(cudaMalloc(&d_err, sizeof(int)));
+    int rc = 0, err = 0;
+    if (cuda_fail(c, cudaMemsetAsync(d_err, 0, sizeof(int), c->st), "cudaMemsetAsync") ||
+        sphk_kl_wait_probe(budget_cycles, d_err, c->st) ||
+        cuda_fail(c, cudaMemcpyAsync(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st), "cudaMemcpyAsync") ||
+        cuda_fail(c, cudaStreamSynchronize(c->st), "cudaStreamSynchronize"))
+        rc = SPHGPU_E_CUDA;
+    cudaFree(d_err);
+    return rc ? rc : err;
+}
 
 int sphgpu_kl_synthesize(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_kl_field* f, const double* xi,
                          int R, int K, float* d_out, double* kernel_ms)

@@ -47,6 +47,8 @@ struct KLTCArgs {
     const float* c_lo;
     float* out;                // R x n
     int* err;
+    long long budget;          // SM clocks one completion wait may take
+    int probe;                 // 1: the wait self-test (below), no synthesis
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
@@ -144,8 +146,19 @@ __global__ void __launch_bounds__(KL_TILE_M, 1) k_kl_synth(KLTCArgs a)
     const double two_pi = 6.283185307179586, inv_two_pi = 0.15915494309189535;
     uint32_t phase = 0;
     bool ok = true;
-    const long long budget = 2000000000ll;   // SM clocks, about one second
-    for (int k0 = 0; k0 < a.K && ok; k0 += KL_K_TILE) {
+    const long long budget = a.budget;
+    if (a.probe) {
+        // the failure path on demand: a wait on the completion barrier before
+        // any MMA has been issued, which nothing will signal, must expire
+        // within the budget, record the code and leave through the normal
+        // teardown (tensor memory released, nothing in flight)
+        const bool got = mbar_wait(smem_u32(bar), phase, budget);
+        if (__syncthreads_or(!got)) {
+            ok = false;
+            if (t == 0) atomicCAS(a.err, 0, KL_TIMEOUT_CODE);
+        }
+    }
+    for (int k0 = 0; k0 < a.K && ok && !a.probe; k0 += KL_K_TILE) {
         const int kt = min(KL_K_TILE, a.K - k0);
         // this thread's Phi row for terms k0 .. k0 + kt
         for (int k = 0; k < KL_K_TILE; k++) {
@@ -211,7 +224,7 @@ __global__ void __launch_bounds__(KL_TILE_M, 1) k_kl_synth(KLTCArgs a)
         phase ^= 1u;
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (ok) {
+    if (ok && !a.probe) {
         // epilogue: warp w holds accumulator lanes 32 w .. 32 w + 31 (particle t)
         const int ptype = live ? a.ptype[i] : -1;
         const bool soil_field = a.no >= 0 && a.no <= 3;
@@ -287,9 +300,28 @@ extern "C" int sphk_kl_synthesize(int n, int ndim, int K, int R, int no, int typ
     a.soil_max = soil_max; a.water_max = water_max;
     a.xh = d_xh; a.ptype = d_type; a.terms = (const KLTCTerm*)d_terms; a.c_hi = c_hi; a.c_lo = c_lo;
     a.out = d_out; a.err = d_err;
+    a.budget = 2000000000ll;     // SM clocks, about one second
+    a.probe = 0;
     const size_t smem = sphk_kl_tc_smem_bytes(R);
     if (cudaFuncSetAttribute(k_kl_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return 1;
     k_kl_synth<<<(n + KL_TILE_M - 1) / KL_TILE_M, KL_TILE_M, smem, st>>>(a);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// One CTA of the synthesis kernel in its wait self-test: it allocates its
+// tensor memory, waits `budget` SM clocks on a completion barrier nothing
+// signals, records the timeout code in *d_err and releases the memory.
+extern "C" int sphk_kl_wait_probe(long long budget, int* d_err, cudaStream_t st)
+{
+    KLTCArgs a = {};
+    a.n = 0; a.ndim = 2; a.K = 8; a.R = 16;
+    a.err = d_err;
+    a.budget = budget;
+    a.probe = 1;
+    const size_t smem = sphk_kl_tc_smem_bytes(a.R);
+    if (cudaFuncSetAttribute(k_kl_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return 1;
+    k_kl_synth<<<1, KL_TILE_M, smem, st>>>(a);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }

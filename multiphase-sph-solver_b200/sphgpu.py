@@ -252,6 +252,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_parttocell.argtypes = [C.c_void_p]
     lib.sphgpu_partisearching.argtypes = [C.c_void_p]
     lib.sphgpu_update.argtypes = [C.c_void_p]
+    lib.sphgpu_kl_wait_check.argtypes = [C.c_void_p, C.c_longlong]
     _lib = lib
     return lib
 

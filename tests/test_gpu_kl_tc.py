@@ -61,3 +61,24 @@ def test_synthesis_rejects_bad_shapes():
     with pytest.raises(sphgpu.SPHError) as e:
         eng.kl_synthesize(dom, sphgpu.kl_field(1, 1, 1.0, 0.1, [1.0, 1.0]), np.zeros((24, 200)), out.data_ptr())
     assert e.value.code == 100
+
+
+def test_bounded_wait_expires_and_context_stays_usable():
+    """The synthesis kernel's bounded completion wait, made to run out on a
+    barrier that nothing signals (sphgpu_kl_wait_check, about 0.5 ms of SM
+    clock): the call reports SPHGPU_E_KL_TIMEOUT (105), and the next synthesis
+    on the same context, which needs the tensor memory the timed-out CTA held,
+    runs and is correct."""
+    sc = scenes.slope_2d(H=5.0, dx=0.1)
+    eng, dom = _setup(sc)
+    for _ in range(2):
+        assert eng.lib.sphgpu_kl_wait_check(eng.h, 1_000_000) == 105
+    field = sphgpu.kl_field(1, 2, 10.0e3, 3.0e3, [10.0, 1.0])
+    R, K = 16, 200
+    xi = np.random.default_rng(5).standard_normal((R, K))
+    out = torch.full((R * eng.n,), float("nan"), dtype=torch.float32, device="cuda")
+    eng.kl_synthesize(dom, field, xi, out.data_ptr(), K)
+    got = out.cpu().numpy().reshape(R, eng.n).astype(np.float64)
+    ref = eng.kl_generate(dom, [field], xi[3][None, :], K)[0]
+    m = ~np.isnan(ref)
+    assert float(np.abs(got[3][m] - ref[m]).max() / np.abs(ref[m]).max()) <= TC_REL_TOL
