@@ -291,6 +291,28 @@ int sphgpu_nnps(sphgpu_ctx* ctx, int* ninflu, int* influ);
 int sphgpu_set_cfl(sphgpu_ctx* ctx, double cfl, double cfl_force);
 int sphgpu_get_dt(sphgpu_ctx* ctx, double* dt);
 
+/*
+ * Rainfall (flr == 1): the reference's Para_Rain (Class_Problem.h) as its
+ * input block RP sets it, with nrain the number of rain particles still
+ * waiting (type 7, etype 1; input_par counts them, CPP_2-initialf.cpp:979-
+ * 1017).  The rain particles sit at the end of the particle array, row after
+ * row in the order they fall.  Every lp steps (rainini, CPP_15-1-rain.cpp:
+ * 11-23: lp = (loop - inip) / (nrain / nhor + 1)) the top of the step
+ * releases the next row (rainpro, :43-85), and after the update water beyond
+ * the domain's x ends is taken out (partidel, CPP_15-2-partidel.cpp:19-58);
+ * both run on the device inside the step's CUDA graph, with no host round
+ * trip.  rtype 1 (rain) is supported; 2-4 (water-level lowering, cement
+ * injection) return SPHGPU_E_UNSUPPORTED.  sphgpu_get_rain reports nrain as
+ * the steps have left it.  A context created with flr == 1 steps only after
+ * sphgpu_set_rain (SPHGPU_E_STATE before).
+ */
+typedef struct sphgpu_rain {
+    int    rtype, nrain, nhor;
+    double press_factor, drop_velocity;
+} sphgpu_rain;
+int sphgpu_set_rain(sphgpu_ctx* ctx, const sphgpu_rain* rain);
+int sphgpu_get_rain(sphgpu_ctx* ctx, sphgpu_rain* rain);
+
 /* Block until the context's stream is idle; returns the sticky error, if any. */
 int sphgpu_synchronize(sphgpu_ctx* ctx);
 

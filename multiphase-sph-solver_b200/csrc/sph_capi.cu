@@ -145,6 +145,8 @@ struct sphgpu_ctx {
     std::vector<sphgpu_soil, UninitAlloc<sphgpu_soil>> h_soil;      // (K-L fields rewrite members)
     double* mat_pinned = nullptr;     // pinned, 4N: the per-particle material constants set_materials uploads
     int part_done = 0;     // parts of step l run through the method entries: 1 parttocell, 2 partisearching
+    sphgpu_rain rain = {};            // the rainfall record (flr 1), nrain as last set
+    bool rain_set = false;
     std::vector<InstGrid> h_inst;     // batched context: the instance table (empty: one system)
     InstGrid* d_inst = nullptr;
 };
@@ -221,6 +223,8 @@ void fill_dev_params(DevParams& p, const sphgpu_params* P)
     p.cfl_on = 0; p.cfl_c = 0.0; p.cfl_f = 0.0;
     p.st_vpu = P->structure.vpu;
     p.ninst = 0;
+    p.flr = P->flr == 1 ? 1 : 0;
+    p.rain_lp = 0; p.rain_vrain = 0.0; p.rain_press = 0.0;
 }
 
 // the buffers only some flag settings use, allocated when the flags first
@@ -381,6 +385,7 @@ void update_static_params(sphgpu_ctx* c)
 int check_particles(sphgpu_ctx* c)
 {
     if (c->h_type.empty() || c->h_matype.empty()) return SPHGPU_E_STATE;
+    if (c->P.flr == 1 && !c->rain_set) return SPHGPU_E_STATE;
     bool ext = c->P.flagum == 1;
     for (int i = 0; i < c->N; i++) {
         const int t = c->h_type[i], m = c->h_matype[i];
@@ -628,7 +633,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.nbm, 10 * (size_t)N);
     r |= dalloc(c, &s.nbw, 4 * (size_t)SPH_NB_CAP * N);
     r |= dalloc(c, &s.err, 1); r |= dalloc(c, &s.step, 1);
-    r |= dalloc(c, &s.dtv, 1); r |= dalloc(c, &s.dtmin, 1);
+    r |= dalloc(c, &s.dtv, 1); r |= dalloc(c, &s.dtmin, 1); r |= dalloc(c, &s.nrain, 1);
     if (r) return fail(SPHGPU_E_CUDA);
     // cell_info() constructor values (Class_NNPS.cpp:68-72): the range of the
     // last cell, which the reference never resets, starts from them
@@ -1203,6 +1208,7 @@ int sphgpu_update_params(sphgpu_ctx* c, const sphgpu_params* P)
         dp.first_vbx_wall = keep.first_vbx_wall;
         dp.bulk = keep.bulk;
         dp.cfl_on = keep.cfl_on; dp.cfl_c = keep.cfl_c; dp.cfl_f = keep.cfl_f;
+        dp.rain_lp = keep.rain_lp; dp.rain_vrain = keep.rain_vrain; dp.rain_press = keep.rain_press;
     }
     c->P = *P;
     invalidate_graphs(c);
@@ -1214,6 +1220,8 @@ sphgpu_ctx* sphgpu_create_batched(const sphgpu_params* shared, const sphgpu_inst
 {
     g_create_error = SPHGPU_E_ARG;
     if (!shared || !inst || ninst <= 0) return nullptr;
+    // rain rows are released from the end of the whole particle array
+    if (shared->flr == 1) { g_create_error = SPHGPU_E_UNSUPPORTED; return nullptr; }
     // the instances follow one another in the particle order, each with a
     // grid of its own; the context numbers their cells one after another
     std::vector<InstGrid> tab(ninst);
@@ -1328,6 +1336,42 @@ int sphgpu_set_cfl(sphgpu_ctx* c, double cfl, double cfl_force)
         c->d[p].p.cfl_f = on ? cfl_force : 0.0;
     }
     invalidate_graphs(c);
+    return 0;
+}
+
+int sphgpu_set_rain(sphgpu_ctx* c, const sphgpu_rain* rain)
+{
+    if (!c || !rain) return SPHGPU_E_ARG;
+    if (c->P.flr != 1) return SPHGPU_E_STATE;
+    if (rain->rtype != 1) return SPHGPU_E_UNSUPPORTED;
+    if (rain->nrain < 0 || rain->nrain > c->N || rain->nhor < 0) return SPHGPU_E_ARG;
+    sphgpu_rain r = *rain;
+    if (r.nhor == 0) r.nhor = 35;            // initial_pro's default (CPP_2-initialf.cpp:201-202)
+    // rainini (CPP_15-1-rain.cpp:11-23): nrain / nhor in integer arithmetic
+    const double temp = r.nrain / r.nhor + 1.0;
+    const int lp = (int)((c->P.loop - c->P.inip) / temp);
+    cudaSetDevice(c->device);
+    CK(cudaMemcpyAsync(c->d[0].s.nrain, &r.nrain, sizeof(int), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int p = 0; p < 2; p++) {
+        c->d[p].p.rain_lp = lp;
+        c->d[p].p.rain_vrain = r.drop_velocity;
+        c->d[p].p.rain_press = r.press_factor;
+    }
+    c->rain = r;
+    c->rain_set = true;
+    invalidate_graphs(c);
+    return 0;
+}
+
+int sphgpu_get_rain(sphgpu_ctx* c, sphgpu_rain* rain)
+{
+    if (!c || !rain) return SPHGPU_E_ARG;
+    if (!c->rain_set) return SPHGPU_E_STATE;
+    *rain = c->rain;
+    cudaSetDevice(c->device);
+    CK(cudaMemcpyAsync(&rain->nrain, c->d[0].s.nrain, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
     return 0;
 }
 

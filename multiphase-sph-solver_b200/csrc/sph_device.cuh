@@ -76,6 +76,9 @@ struct DevParams {
     double cfl_c, cfl_f;       // factors of h / (c + |v|) and sqrt(h / |a|)
     double st_vpu;             // Para_Structure::vpu, the structure's sound speed
     int ninst;                 // batched context: number of instances (0: one system)
+    // rainfall (flr 1, rtype 1): rainini's lp and vrain, Para_Rain::press_factor
+    int flr, rain_lp;
+    double rain_vrain, rain_press;
 };
 
 // Members of the soil record that only the unsaturated Cam-clay model, the
@@ -175,6 +178,7 @@ struct DevState {
     int *step;                 // Para_Pro::l of the step being run
     const InstGrid *inst;      // batched context: the instance table (ninst)
     int *pinst;                // batched context: each particle's instance
+    int *nrain;                // rain particles still waiting (Para_Rain::nrain)
     double *dtv;               // dt of the step being run (cfl_on)
     unsigned long long *dtmin; // running minimum of the per-particle limits (bits of a positive double)
 };

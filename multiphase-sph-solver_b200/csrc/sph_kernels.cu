@@ -252,6 +252,64 @@ __global__ void k_cellkey(Dev d)
     d.s.val_in[N - 1 - i] = i;
 }
 
+// rainpro (CPP_15-1-rain.cpp:43-85), at the top of the steps with
+// (l - inip) > 0 and (l - inip) % lp == 0: the next row of waiting rain
+// particles -- from index N - nrain on while each next particle's vertical
+// coordinate stays within 0.1 dr of the one before it -- becomes water:
+// lowered to 0.95 of its height, falling at vrain, with its density, mass and
+// pressure set as the reference sets them.  One block: the row's end is the
+// first break found over windows of the block's width, then each thread
+// releases its share of the row.
+template <int ND>
+__global__ void __launch_bounds__(256) k_rain(Dev d)
+{
+    if (*d.s.err) return;
+    const int rel = *d.s.step - d.p.inip;
+    if (!(rel > 0 && d.p.rain_lp > 0 && rel % d.p.rain_lp == 0)) return;
+    const int nrain = *d.s.nrain;
+    if (nrain <= 0) return;
+    const int N = d.p.N, k0 = N - nrain;
+    const double dr = d.p.dr;
+    __shared__ int s_end;
+    if (threadIdx.x == 0) s_end = N - 1;
+    __syncthreads();
+    for (int base = k0; base < N - 1; base += blockDim.x) {
+        const int e = base + threadIdx.x;
+        if (e < N - 1) {
+            const Pos a = load_pos(d.s.xh, e), b = load_pos(d.s.xh, e + 1);
+            const double za = (ND == 2) ? a.y : a.z, zb = (ND == 2) ? b.y : b.z;
+            if (!(fabs(zb - za) < 0.1 * dr)) atomicMin(&s_end, e);
+        }
+        __syncthreads();
+        const bool found = s_end < N - 1 && s_end < base + (int)blockDim.x;
+        __syncthreads();
+        if (found) break;
+    }
+    const int end = s_end;
+    const double g = (ND == 2) ? d.p.gy : d.p.gz;
+    for (int k = k0 + threadIdx.x; k <= end; k += blockDim.x) {
+        Pos p = load_pos(d.s.xh, k);
+        if (ND == 2) p.y = 0.95 * p.y;
+        else p.z = 0.95 * p.z;
+        p.h = dr;
+        store_pos(d.s.xh, k, p);
+        d.s.type[k] = 1;
+        d.s.matype[k] = 0;
+        d.s.etype[k] = 7;
+        const double rhop = d.s.f_por[k] * d.s.f_dens[k];
+        d.s.rhop[k] = rhop;
+        d.s.mass[k] = (ND == 2) ? rhop * p.h * p.h : rhop * p.h * p.h * p.h;
+        for (int c = 0; c < 3; c++) {
+            d.s.vxp[c * N + k] = 0.0;
+            d.s.vx[c * N + k] = 0.0;
+        }
+        d.s.vxp[(ND - 1) * N + k] = d.p.rain_vrain;
+        d.s.prep[k] = rhop * dr * (-g) * d.p.rain_press;
+        d.s.satu[k] = 0.99;
+    }
+    if (threadIdx.x == 0) *d.s.nrain = nrain - (end - k0 + 1);
+}
+
 __global__ void k_cellreset(Dev d)
 {
     const int c = IDX;
@@ -2508,6 +2566,30 @@ __global__ void k_step_done(Dev d)
     }
 }
 
+// partidel (CPP_15-2-partidel.cpp:19-58), after the update: water within dr
+// of 7 dr past either x end of the domain box (of its instance) and above
+// y = 0.12 stops and leaves the calculation as type 7
+__global__ void __launch_bounds__(256) k_partidel(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    if (d.s.type[i] != 1) return;
+    const CellGrid g = cell_grid(d, i);
+    const Pos p = load_pos(d.s.xh_next, i);
+    const double dr = d.p.dr;
+    const double dx1 = fabs(p.x - g.xmax - 7.0 * dr);
+    const double dx2 = fabs(p.x - g.xmin + 7.0 * dr);
+    const double dy1 = p.y - 0.12;
+    if ((dx1 < dr || dx2 < dr) && dy1 > 0.0) {
+        d.s.type[i] = 7;
+        for (int c = 0; c < 3; c++) {
+            d.s.vxp[c * N + i] = 0.0;
+            d.s.vx[c * N + i] = 0.0;
+            d.s.ax[c * N + i] = 0.0;
+        }
+    }
+}
+
 // Adaptive time step (an extension: the reference keeps dt constant,
 // CPP_12-2-dt.cpp:13-20).  For every water, soil, air and structure particle
 // after the update, the CFL limit cfl_c h / (c + |v|), c the sound speed of
@@ -2710,6 +2792,7 @@ extern "C" int sphk_enqueue_nnps_parts(const Dev* dp, void* sort_tmp, size_t sor
     int n = 0;
     if (parts & 1) {
         REC(0);
+        if (d.p.flr) { LAUNCH_ND(k_rain, 1, 256, d); n++; }
         LAUNCH_ND(k_cellkey, nblk(N, 256), 256, d); n++;
         REC(1);
         size_t bytes = sort_bytes;
@@ -2816,6 +2899,7 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
     } else if (d.p.flbndy == 3 || d.p.flbndy == 4 || d.p.flbndy == 13 || d.p.flbndy == 14) {
         k_tran_wall<<<nblk(N, 128), 128, 0, st>>>(d); n++;
     }
+    if (d.p.flr) { k_partidel<<<nblk(N, 256), 256, 0, st>>>(d); n++; }
     if (d.p.cfl_on) { k_cfl<<<148 * 8, 256, 0, st>>>(d); n++; }
     REC(20);
     k_step_done<<<1, 32, 0, st>>>(d); n++;

@@ -70,6 +70,7 @@ class Scene:
     model_flags: tuple = (0,) * 10                # block MS: em sb dp um am bui pl ve focc ep
     soils: dict = field(default_factory=dict)     # {index: Para_Soil dict}, index = layer*10 + model
     structure: dict | None = None                 # block SM
+    rain: dict | None = None                      # block RP (flr = 1)
 
     @property
     def n(self) -> int:
@@ -326,6 +327,41 @@ def footing(ndim: int = 2, dx: float = 0.04, bed=(2.0, 1.0, 1.0), width: float =
     )
 
 
+def add_rain(scene: Scene, x0: float, x1: float, rows: int, top: float, press_factor: float = 1.0,
+             drop_velocity: float = -1.0) -> Scene:
+    """Rain particles (type 7, etype 1: water waiting to fall) appended to
+    the scene in `rows` rows of one spacing's pitch above height `top` (y in
+    2-D, z in 3-D), each row spanning [x0, x1) at the spacing (and the
+    scene's z or y extent in 3-D), the lowest row first since the reference
+    releases them in array order (rainpro, CPP_15-1-rain.cpp:43-85); rainfall
+    type 1 with nhor = the row's particle count (input block RP)."""
+    dx = scene.dr
+    nx = int(round((x1 - x0) / dx))
+    blocks = []
+    for r in range(rows):
+        h = top + (r + 0.5) * dx
+        if scene.ndim == 2:
+            row = _grid2(nx, 1, dx, (x0, 0.0))
+            row[:, 1] = h
+        else:
+            lo, hi = scene.xp[:, 1].min(), scene.xp[:, 1].max()
+            ny = max(int(round((hi - lo) / dx)), 1)
+            row = _grid(nx, ny, 1, dx, (x0, lo, 0.0))
+            row[:, 2] = h
+        blocks.append(row)
+    rain = np.concatenate(blocks)
+    m = rain.shape[0]
+    scene.xp = np.concatenate([scene.xp, rain])
+    scene.vxp = np.concatenate([scene.vxp, np.zeros((m, 3))])
+    scene.ptype = np.concatenate([scene.ptype, np.full(m, 7, np.int32)])
+    scene.matype = np.concatenate([scene.matype, np.zeros(m, np.int32)])
+    scene.permtype = np.concatenate([scene.permtype, np.zeros(m, np.int32)])
+    scene.etype = np.concatenate([scene.etype, np.ones(m, np.int32)])
+    scene.flags["flr"] = 1
+    scene.rain = dict(rtype=1, nrain=m, nhor=m // rows, press_factor=press_factor, drop_velocity=drop_velocity)
+    return scene
+
+
 def uplift(scene: Scene, axis: int, above: float, v: float = 0.5) -> Scene:
     """Give the soil particles (type 2) above coordinate `above` along `axis`
     an initial velocity v along that axis, which stretches the soil body and
@@ -464,6 +500,12 @@ def write_input_dat(scene: Scene, path: str, ntd: int = 1) -> None:
     if P["if_move"] >= 1:
         add(" ".join(_f(v) for v in P.get("move_vx", (0.0, 0.0, 0.0))))
     add("E end")
+    if F["flr"] == 1 and scene.rain is not None:
+        rn = scene.rain
+        add("RP rain")
+        add("A data")
+        add(f"{rn['rtype']} {rn['nrain']} {rn['nhor']} {_f(rn['press_factor'])} {_f(rn['drop_velocity'])}")
+        add("E end")
     add("WP water")
     add("A data")
     w0 = scene.water[0]
@@ -633,6 +675,7 @@ class InitialState:
     fields: dict          # Particle member name -> array (n,) or (n, ncomp)
     fluid: np.ndarray     # (n, 12) records as sphgpu_fluid (structured dtype)
     soil: np.ndarray      # (n,) structured sphgpu_soil
+    rain: dict | None = None   # sphgpu_rain members (flr = 1)
 
 
 FLUID_DTYPE = np.dtype([(k, np.int32 if k in ("bhtype", "press_type", "acc_type") else np.float64)
@@ -801,7 +844,13 @@ def initialise(scene: Scene) -> InitialState:
         water_acc_type=water[0]["acc_type"], air_acc_type=air["acc_type"],
         structure=st,
     )
-    return InitialState(params=params, fields=f, fluid=fl, soil=so)
+    rain = None
+    if scene.flags.get("flr", 0) == 1 and scene.rain is not None:
+        # input_par counts the waiting rain particles (CPP_2-initialf.cpp:979-1017)
+        rain = dict(scene.rain, nrain=int(np.count_nonzero((t == 7) & (et == 1))))
+        if rain["nhor"] == 0:
+            rain["nhor"] = 35
+    return InitialState(params=params, fields=f, fluid=fl, soil=so, rain=rain)
 
 
 def kl_domain(scene: Scene) -> dict:

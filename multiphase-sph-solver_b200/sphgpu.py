@@ -74,6 +74,17 @@ class Instance(C.Structure):
                 ("cxm", C.c_int), ("cym", C.c_int), ("czm", C.c_int), ("ctotal", C.c_int)]
 
 
+class Rain(C.Structure):
+    """sphgpu_rain: the reference's Para_Rain as the step uses it."""
+    _fields_ = [("rtype", C.c_int), ("nrain", C.c_int), ("nhor", C.c_int),
+                ("press_factor", C.c_double), ("drop_velocity", C.c_double)]
+
+
+def rain_record(d: dict) -> Rain:
+    return Rain(int(d["rtype"]), int(d["nrain"]), int(d["nhor"]), float(d["press_factor"]),
+                float(d["drop_velocity"]))
+
+
 def params_from_dict(d: dict) -> Params:
     p = Params()
     for name, ctype in Params._fields_:
@@ -253,6 +264,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_partisearching.argtypes = [C.c_void_p]
     lib.sphgpu_update.argtypes = [C.c_void_p]
     lib.sphgpu_kl_wait_check.argtypes = [C.c_void_p, C.c_longlong]
+    lib.sphgpu_set_rain.argtypes = [C.c_void_p, C.POINTER(Rain)]
+    lib.sphgpu_get_rain.argtypes = [C.c_void_p, C.POINTER(Rain)]
     _lib = lib
     return lib
 
@@ -327,12 +340,14 @@ class Engine:
         """sphgpu_download_particles: the device-owned members of each record."""
         self._check(self.lib.sphgpu_download_particles(self.h, _ptr(records), self.n, stride), "download_particles")
 
-    def load_state(self, fields: dict, fluid=None, soil=None) -> None:
+    def load_state(self, fields: dict, fluid=None, soil=None, rain=None) -> None:
         for name, v in fields.items():
             if name in FIELDS:
                 self.set_field(name, v)
         if fluid is not None or soil is not None:
             self.set_materials(fluid, soil)
+        if rain is not None:
+            self.set_rain(rain)
 
     def kl_generate(self, domain: KLDomain, fields, xi, K: int = 200) -> np.ndarray:
         """SpatialVariables_Generate_2D / _3D with the standard normals xi
@@ -394,6 +409,15 @@ class Engine:
 
     def update(self) -> int:
         return int(self.lib.sphgpu_update(self.h))
+
+    def set_rain(self, rain: dict) -> None:
+        """sphgpu_set_rain: the rainfall record of a run with flr = 1."""
+        self._check(self.lib.sphgpu_set_rain(self.h, C.byref(rain_record(rain))), "sphgpu_set_rain")
+
+    def rain(self) -> dict:
+        r = Rain()
+        self._check(self.lib.sphgpu_get_rain(self.h, C.byref(r)), "sphgpu_get_rain")
+        return {k: getattr(r, k) for k, _ in Rain._fields_}
 
     def set_cfl(self, cfl: float, cfl_force: float = 0.25) -> None:
         """Adaptive dt from the CFL and force limits (cfl <= 0: off, the

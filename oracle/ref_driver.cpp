@@ -77,6 +77,9 @@ struct RefRun {
     clUpdate_Fun upd;
     clBndy_Fun bnd;
     clSoilStruct_Fun ssinter;
+    clRain_Fun rainf;
+    int lp = 0;
+    double vrain = 0.0, cement_base[3] = {0.0, 0.0, 0.0};
 };
 
 int g_last_error = 0;
@@ -126,7 +129,23 @@ void* ref_create(const char* input_dat_path, int nthreads)
     r->cinfo = new cell_info[r->cellc.ctotal + 4];
     r->clink = new cell_link[r->cellc.ctotal + 4];
     r->nnps.celllist_ini2(r->clink, r->cellc, r->pro.ndim, r->fl.ntd);
+    // rainfall set-up as SPH_Calculation does it (CPP_1-SPHLoops.cpp:457-467)
+    if (r->fl.flr == 1 && r->rain.rtype <= 7 && r->rain.rtype >= 1) {
+        r->rainf.rainini(r->rain, r->pro, &r->lp, &r->vrain);
+        r->rainf.center_cement(r->par, r->pro, r->cement_base);
+    }
     return r;
+}
+
+int ref_get_rain(void* h, sphgpu_rain* o)
+{
+    RefRun* r = (RefRun*)h;
+    o->rtype = r->rain.rtype;
+    o->nrain = r->rain.nrain;
+    o->nhor = r->rain.nhor;
+    o->press_factor = r->rain.press_factor;
+    o->drop_velocity = r->rain.drop_velocity;
+    return 0;
 }
 
 int ref_last_error(void) { return g_last_error; }
@@ -240,8 +259,8 @@ int ref_nnps(void* h, int* ninflu, int* influ, double* wij)
     return err;
 }
 
-/* the body of the main loop, CPP_1-SPHLoops.cpp:481-753, for the flag set the
- * engine covers (no rain, excavation or vibration) */
+/* the body of the main loop, CPP_1-SPHLoops.cpp:481-760, for the flag set the
+ * engine covers (rain, no excavation or vibration) */
 int ref_step(void* h, int nsteps)
 {
     RefRun* r = (RefRun*)h;
@@ -250,6 +269,14 @@ int ref_step(void* h, int nsteps)
     for (int s = 0; s < nsteps; s++) {
         if (!(P.t < P.tt)) return 0;
         P.t = P.t + P.dt;
+        // rainfall (CPP_1-SPHLoops.cpp:497-513)
+        if (F.flr == 1 && (P.l - P.inip) > 0 && (P.l - P.inip) % r->lp == 0) {
+            if (r->rain.rtype == 1) r->rainf.rainpro(r->par, &r->rain, &P, r->vfluid, r->gf, r->vrain);
+            else if (r->rain.rtype == 2) r->rainf.waterdel_min(r->par, &r->rain, &P);
+            else if (r->rain.rtype == 3) r->rainf.waterdel_max(r->par, &r->rain, &P);
+            else if (r->rain.rtype == 4)
+                r->rainf.cementpro(r->par, &r->rain, &P, r->vfluid, r->gf, r->vrain, r->cement_base);
+        }
         int err = r->nnps.parttocell(r->parcell, r->cinfo, r->cellc, r->sorted, r->temp, P, r->par, P.ndim,
                                      F.ntd, r->size_m, r->k);
         if (err > 0) return err;
@@ -312,6 +339,7 @@ int ref_step(void* h, int nsteps)
         }
         r->bnd.check_domain(r->par, r->cellc, r->bou, P);
         r->upd.update(r->par, P, r->bou, F.ntd);
+        if (F.flr == 1) r->rainf.partidel(r->par, &r->rain, &P, r->cellc, F.ntd);
         P.l++;
     }
     return 0;

@@ -47,6 +47,10 @@ struct orc_ctx {
     double* vx_temp;
     double* snap;                        /* Jacobi snapshots */
     double* rij;                         /* clRaij per particle (9), persistent */
+    /* rainfall (flr == 1): Para_Rain and rainini's lp / vrain */
+    sphgpu_rain rain;
+    int rain_set, lp;
+    double vrain;
 };
 
 /* ------------------------------------------------------------------------- */
@@ -2788,6 +2792,77 @@ static void kernel_gradient_correction(orc_ctx* c)
     }
 }
 
+/* rainini (CPP_15-1-rain.cpp:11-23) for rtype 1: lp steps between rows,
+ * nrain / nhor in integer arithmetic */
+int orc_set_rain(orc_ctx* c, const sphgpu_rain* rain)
+{
+    if (!rain) return SPHGPU_E_ARG;
+    if (rain->rtype != 1) return SPHGPU_E_UNSUPPORTED;
+    c->rain = *rain;
+    if (c->rain.nhor == 0) c->rain.nhor = 35;      /* initial_pro's default, CPP_2-initialf.cpp:201-202 */
+    double temp = c->rain.nrain / c->rain.nhor + 1.0;
+    c->lp = (int)((c->P.loop - c->P.inip) / temp);
+    c->vrain = c->rain.drop_velocity;
+    c->rain_set = 1;
+    return 0;
+}
+
+int orc_get_rain(const orc_ctx* c, sphgpu_rain* rain)
+{
+    if (!rain) return SPHGPU_E_ARG;
+    *rain = c->rain;
+    return 0;
+}
+
+/* rainpro (CPP_15-1-rain.cpp:43-85): the next row of waiting rain
+ * particles, from index ntotal - nrain on while each next particle's vertical
+ * coordinate stays within 0.1 dr of the one before it (compared before that
+ * one is lowered), becomes water falling at vrain, lowered to 0.95 of its
+ * height; the reference's loop reads one particle past the array after the
+ * last one, which this restatement does not */
+static void rainpro(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    const int nd = P->ndim, n = c->n;
+    const double g = (nd == 2) ? P->gy : P->gz;
+    int k = n - c->rain.nrain;
+    if (c->rain.nrain <= 0) return;
+    for (;;) {
+        c->rain.nrain = c->rain.nrain - 1;
+        const double temp_xp = c->xp[k * 3 + nd - 1];
+        c->xp[k * 3 + nd - 1] = 0.95 * c->xp[k * 3 + nd - 1];
+        c->type[k] = 1;
+        c->matype[k] = 0;
+        c->etype[k] = 7;
+        c->rhop[k] = c->fl[k].porosity * c->fl[k].dens;
+        c->hl[k] = P->dr;
+        c->mass[k] = (nd == 2) ? c->rhop[k] * c->hl[k] * c->hl[k] : c->rhop[k] * c->hl[k] * c->hl[k] * c->hl[k];
+        for (int d = 0; d < 3; d++) { c->vxp[k * 3 + d] = 0.0; c->vx[k * 3 + d] = 0.0; }
+        c->vxp[k * 3 + nd - 1] = c->vrain;
+        c->prep[k] = c->rhop[k] * P->dr * (-g) * c->rain.press_factor;
+        c->satu[k] = 0.99;
+        k++;
+        if (!(k <= n - 1 && fabs(c->xp[k * 3 + nd - 1] - temp_xp) < 0.1 * P->dr)) break;
+    }
+}
+
+/* partidel (CPP_15-2-partidel.cpp:19-58): water within dr of 7 dr past
+ * either x end of the domain box and above y = 0.12 stops and leaves the
+ * calculation as type 7 */
+static void partidel(orc_ctx* c)
+{
+    const sphgpu_params* P = &c->P;
+    for (int i = 0; i < c->n; i++) {
+        const double dx1 = fabs(c->xp[i * 3] - P->xmax - 7.0 * P->dr);
+        const double dx2 = fabs(c->xp[i * 3] - P->xmin + 7.0 * P->dr);
+        const double dy1 = c->xp[i * 3 + 1] - 0.12;
+        if (c->type[i] == 1 && (dx1 < P->dr || dx2 < P->dr) && dy1 > 0.0) {
+            c->type[i] = 7;
+            for (int d = 0; d < 3; d++) { c->vxp[i * 3 + d] = 0.0; c->vx[i * 3 + d] = 0.0; c->ax[i * 3 + d] = 0.0; }
+        }
+    }
+}
+
 static int check_supported(const sphgpu_params* P)
 {
     if (!(P->flbndy >= 1 && P->flbndy <= 5) && P->flbndy != 13 && P->flbndy != 14) return SPHGPU_E_UNSUPPORTED;
@@ -2803,8 +2878,10 @@ int orc_step(orc_ctx* c, int nsteps)
     const sphgpu_params* P = &c->P;
     int err = check_supported(P);
     if (err) return err;
+    if (P->flr == 1 && !c->rain_set) return SPHGPU_E_STATE;
     for (int s = 0; s < nsteps; s++) {
         c->t = c->t + P->dt;
+        if (P->flr == 1 && (c->l - P->inip) > 0 && c->lp > 0 && (c->l - P->inip) % c->lp == 0) rainpro(c);
         err = parttocell(c);
         if (err) return err;
         err = partisearching(c);
@@ -2845,6 +2922,7 @@ int orc_step(orc_ctx* c, int nsteps)
         else if (P->flbndy == 14) { velocity_set_domain(c); tran_walls(c, 1); }
         check_domain(c);
         update(c);
+        if (P->flr == 1) partidel(c);
         c->l++;
     }
     return 0;

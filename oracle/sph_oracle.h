@@ -54,6 +54,9 @@ int      orc_get_step(const orc_ctx* c);
  * out as in Par_Cell (influ 1-based, 100 slots per particle). */
 int      orc_nnps(orc_ctx* c, int* ninflu, int* influ, double* wij);
 int      orc_step(orc_ctx* c, int nsteps);
+/* rainfall (flr == 1): the Para_Rain record, and its nrain as the steps leave it */
+int      orc_set_rain(orc_ctx* c, const sphgpu_rain* rain);
+int      orc_get_rain(const orc_ctx* c, sphgpu_rain* rain);
 
 #ifdef __cplusplus
 }

@@ -62,6 +62,8 @@ def oracle_lib():
         lib.orc_get_step.argtypes = [C.c_void_p]
         lib.orc_nnps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.orc_step.argtypes = [C.c_void_p, C.c_int]
+        lib.orc_set_rain.argtypes = [C.c_void_p, C.c_void_p]
+        lib.orc_get_rain.argtypes = [C.c_void_p, C.c_void_p]
         _olib = lib
     return _olib
 
@@ -104,14 +106,25 @@ class Oracle:
         sp = _ptr(np.ascontiguousarray(soil)) if soil is not None else None
         assert self.lib.orc_set_materials(self.h, fp, sp, self.n) == 0
 
-    def load_state(self, fields, fluid=None, soil=None):
+    def load_state(self, fields, fluid=None, soil=None, rain=None):
         for name, v in fields.items():
             if name in ORACLE_FIELDS:
                 self.set_field(name, v)
         self.set_materials(fluid, soil)
+        if rain is not None:
+            self.set_rain(rain)
 
     def step(self, nsteps=1):
         return self.lib.orc_step(self.h, int(nsteps))
+
+    def set_rain(self, rain: dict):
+        r = sphgpu.rain_record(rain)
+        assert self.lib.orc_set_rain(self.h, C.byref(r)) == 0
+
+    def rain(self) -> dict:
+        r = sphgpu.Rain()
+        assert self.lib.orc_get_rain(self.h, C.byref(r)) == 0
+        return {k: getattr(r, k) for k, _ in sphgpu.Rain._fields_}
 
     def nnps(self, with_wij=False):
         ninflu = np.zeros(self.n, np.int32)
@@ -152,6 +165,7 @@ def reference_lib(so: str = REF_SO):
         lib.ref_step.argtypes = [C.c_void_p, C.c_int]
         lib.ref_get_step.argtypes = [C.c_void_p]
         lib.ref_destroy.argtypes = [C.c_void_p]
+        lib.ref_get_rain.argtypes = [C.c_void_p, C.c_void_p]
         _rlibs[so] = lib
     return _rlibs[so]
 
@@ -188,6 +202,11 @@ class Reference:
         so = np.zeros(self.n, SOIL_DTYPE)
         self.lib.ref_get_materials(self.h, _ptr(fl), _ptr(so))
         return fl, so
+
+    def rain(self) -> dict:
+        r = sphgpu.Rain()
+        self.lib.ref_get_rain(self.h, C.byref(r))
+        return {k: getattr(r, k) for k, _ in sphgpu.Rain._fields_}
 
     def set_threads(self, n):
         self.lib.ref_set_threads(self.h, int(n))

@@ -235,6 +235,30 @@ def _geostatic(factory, inip, camclay=False, step_regu=100000000):
     return make
 
 
+def _rain(partidel=True):
+    """The dam break (dx = 0.04, 40 steps) with three rows of ten rain
+    particles above the tank (rainfall type 1, falling at 1 m/s, pressure
+    factor 1): lp = 40 / (30 / 10 + 1) = 10, so rows fall at steps 10, 20 and
+    30 (rainpro, CPP_15-1-rain.cpp:43-85).  With `partidel` one water particle
+    stands alone 0.4 m left of the tank moving left at 9 spacings per step:
+    after its first update it lies 7 spacings beyond the domain's left end and
+    partidel (CPP_15-2-partidel.cpp:19-58) takes it out; the reference's
+    parttocell folds coordinates below the grid's minimum back (the fabs of
+    CPP_3-NNPS.cpp:213), so it stays in the grid."""
+    def make():
+        sc = scenes.dam_break_2d(dx=0.04, steps=40)
+        if partidel:
+            dt = sc.dt
+            sc.xp = np.concatenate([sc.xp, [[-0.5, 0.5, 0.0]]])
+            sc.vxp = np.concatenate([sc.vxp, [[-9.0 * sc.dr / dt, 0.0, 0.0]]])
+            sc.ptype = np.concatenate([sc.ptype, np.array([1], np.int32)])
+            sc.matype = np.concatenate([sc.matype, np.array([0], np.int32)])
+            sc.permtype = np.concatenate([sc.permtype, np.array([0], np.int32)])
+            sc.etype = np.concatenate([sc.etype, np.array([1], np.int32)])
+        return scenes.add_rain(sc, 0.6, 1.0, 3, 0.9)
+    return make
+
+
 CASES = {
     # name: (scene factory, steps)
     "dam_break_2d_dx0.04": (lambda: scenes.dam_break_2d(dx=0.04, steps=200), 25),
@@ -276,6 +300,7 @@ CASES = {
     "soil_column_3d_dx0.1_geostatic_camclay": (
         _geostatic(lambda: scenes.soil_column_3d(dx=0.1, steps=200), 6, camclay=True, step_regu=4), 12),
     "slope_2d_H1_dx0.05_geostatic": (_geostatic(lambda: scenes.slope_2d(H=1.0, dx=0.05), 8), 16),
+    "dam_break_2d_dx0.04_rain": (_rain(), 35),
 }
 
 
@@ -324,6 +349,9 @@ def make(name: str) -> str:
         scenes.write_input_dat(sc, path)
         ref = Reference(path, 1)
         out["params"] = np.frombuffer(bytes(ref.params), dtype=np.uint8)
+        if sc.flags.get("flr", 0) == 1:
+            rn = ref.rain()
+            out["rain"] = np.array([rn["rtype"], rn["nrain"], rn["nhor"], rn["press_factor"], rn["drop_velocity"]])
         fl, so = ref.materials()
         out["fluid"], out["soil"] = fl, so
         for k in STATE_FIELDS:
@@ -336,6 +364,8 @@ def make(name: str) -> str:
         out["nnps_wij"] = np.where(mask[:, :, None], wij, 0.0)
         assert ref.step(steps) == 0
         out["steps"] = np.array(steps)
+        if sc.flags.get("flr", 0) == 1:
+            out["final_nrain"] = np.array(ref.rain()["nrain"])
         for k in STATE_FIELDS:
             out["final_" + k] = ref.get_field(k)
     fn = os.path.join(HERE, name + ".npz")

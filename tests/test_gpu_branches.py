@@ -19,7 +19,10 @@ named per case.
   (CPP_9-4-derivation_stress.cpp:850-897), the strain reset
   (CPP_7-1-strain.cpp:35-39) and the displacement restart
   (CPP_12-1-update.cpp:19-28), with Drucker-Prager soil (cd = 0) and with
-  Cam-clay under TSSMP (cd > 0) and regularisation every 4 steps.
+  Cam-clay under TSSMP (cd > 0) and regularisation every 4 steps;
+* rainfall (flr 1): three rows of rain particles released on the device every
+  lp steps (rainpro, CPP_15-1-rain.cpp:43-85) and a water particle taken out
+  past the domain's left end (partidel, CPP_15-2-partidel.cpp:19-58).
 """
 import numpy as np
 import pytest
@@ -46,6 +49,7 @@ CASES = {
     "soil_column_3d_dx0.1_geostatic": 0.0,
     "soil_column_3d_dx0.1_geostatic_camclay": 1e-12,
     "slope_2d_H1_dx0.05_geostatic": 0.0,
+    "dam_break_2d_dx0.04_rain": 0.0,
 }
 RATIO_FIELDS = {"divr"}
 
@@ -77,13 +81,15 @@ def test_branch_against_oracle(name):
     factory, steps = make_golden.CASES[name]
     st = scenes.initialise(factory())
     eng = sphgpu.Engine(st.params, device=0)
-    eng.load_state(st.fields, st.fluid, st.soil)
+    eng.load_state(st.fields, st.fluid, st.soil, st.rain)
     orc = Oracle(st.params, ORC_JACOBI, ORC_POW_CR)
-    orc.load_state(st.fields, st.fluid, st.soil)
+    orc.load_state(st.fields, st.fluid, st.soil, st.rain)
     for chunk in (1, steps - 1):
         eng.step(chunk)
         assert orc.step(chunk) == 0
     assert eng.step_index == orc.step_index
+    if st.rain is not None:
+        assert eng.rain()["nrain"] == orc.rain()["nrain"] == 0
     worst = _compare(eng, orc, CASES[name])
     print(f"{name}: worst relative error {worst:.3g}")
     n1, i1 = eng.nnps()

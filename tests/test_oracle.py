@@ -29,7 +29,8 @@ CASES = ["dam_break_2d_dx0.04", "soil_column_3d_dx0.1", "soil_column_3d_dx0.1_kg
          "three_phase_column_3d_dx0.1_unsat", "three_phase_column_3d_dx0.1_minor",
          "dam_break_2d_dx0.04_minor", "dam_break_2d_dx0.04_bingham", "dam_break_2d_dx0.04_moving_wall",
          "soil_column_3d_dx0.1_moving_wall", "soil_column_3d_dx0.1_geostatic",
-         "soil_column_3d_dx0.1_geostatic_camclay", "slope_2d_H1_dx0.05_geostatic"]
+         "soil_column_3d_dx0.1_geostatic_camclay", "slope_2d_H1_dx0.05_geostatic",
+         "dam_break_2d_dx0.04_rain"]
 
 
 def _golden(name):
@@ -38,9 +39,18 @@ def _golden(name):
     return g, p
 
 
+def golden_rain(g):
+    """The rainfall record a golden case was made with (None without rain)."""
+    if "rain" not in g:
+        return None
+    r = g["rain"]
+    return dict(rtype=int(r[0]), nrain=int(r[1]), nhor=int(r[2]), press_factor=float(r[3]),
+                drop_velocity=float(r[4]))
+
+
 def _oracle_from_golden(g, p, mode=ORC_INPLACE, pow_mode=ORC_POW_LIBM):
     orc = Oracle(p, mode, pow_mode)
-    orc.load_state({k: g["init_" + k] for k in STATE_FIELDS}, g["fluid"], g["soil"])
+    orc.load_state({k: g["init_" + k] for k in STATE_FIELDS}, g["fluid"], g["soil"], golden_rain(g))
     return orc
 
 
@@ -65,6 +75,8 @@ def test_golden_steps_bit_identical(name):
     g, p = _golden(name)
     orc = _oracle_from_golden(g, p)
     assert orc.step(int(g["steps"])) == 0
+    if "final_nrain" in g:
+        assert orc.rain()["nrain"] == int(g["final_nrain"])
     for k in STATE_FIELDS:
         a, b = orc.get_field(k), g["final_" + k]
         same = (a == b) | (np.isnan(a) & np.isnan(b)) if a.dtype.kind == "f" else (a == b)
