@@ -313,6 +313,22 @@ typedef struct sphgpu_rain {
 int sphgpu_set_rain(sphgpu_ctx* ctx, const sphgpu_rain* rain);
 int sphgpu_get_rain(sphgpu_ctx* ctx, sphgpu_rain* rain);
 
+/*
+ * Checkpoint and restart (the reference has none: a run restarts only from
+ * its input deck).  sphgpu_checkpoint_save writes, between steps, the step
+ * counter, every device-owned Particle member, the material records, the
+ * precision form, the rain and adaptive-step settings, and the device state
+ * outside Particle that the next step reads (the walls' per-phase virtual
+ * velocities and stresses of flbndy 2-4 / 13 / 14, the range of the cell
+ * ctotal that the reference never resets, the rain and time-step words).
+ * sphgpu_checkpoint_load restores it into a context created with the same
+ * parameters; the run then continues bit for bit as it would have.  Returns
+ * 0, SPHGPU_E_ARG (unreadable file or another particle count or grid), or an
+ * engine code.
+ */
+int sphgpu_checkpoint_save(sphgpu_ctx* ctx, const char* path);
+int sphgpu_checkpoint_load(sphgpu_ctx* ctx, const char* path);
+
 /* Block until the context's stream is idle; returns the sticky error, if any. */
 int sphgpu_synchronize(sphgpu_ctx* ctx);
 

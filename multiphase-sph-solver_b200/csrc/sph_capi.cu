@@ -1339,6 +1339,153 @@ int sphgpu_set_cfl(sphgpu_ctx* c, double cfl, double cfl_force)
     return 0;
 }
 
+namespace {
+
+// Checkpoint file: a header, every device-owned Particle member (as
+// sphgpu_get_field gives it), the material records, and the device state
+// outside Particle that a later step reads: the walls' per-phase velocities
+// and stresses (cl_bndy_pair / clVar_Boundary), the range of the cell the
+// reference never resets, and the rain and time-step words.
+constexpr char kCkMagic[8] = {'S', 'P', 'H', 'G', 'P', 'U', 'C', 'K'};
+constexpr uint32_t kCkVersion = 1;
+
+struct CkHeader {
+    char magic[8];
+    uint32_t version, ndim;
+    int32_t n, ctotal, step, precision, regu, cfl_on;
+    double cfl_c, cfl_f;
+    int32_t rain_set, has_fluid, has_soil, nextra;
+    sphgpu_rain rain;
+};
+
+struct CkExtra { const char* name; void* ptr; size_t bytes; };
+
+std::vector<CkExtra> ck_extras(sphgpu_ctx* c)
+{
+    const DevState& s = c->d[c->parity].s;
+    const size_t N = (size_t)c->N;
+    const size_t last = (size_t)c->P.ctotal;
+    std::vector<CkExtra> v;
+    auto add = [&](const char* name, void* p, size_t bytes) { if (p) v.push_back({name, p, bytes}); };
+    add("vel_bndy", s.vel_bndy, 3 * N * 8);
+    add("vb", s.vb, 12 * N * 8);
+    add("vx_vb", s.vx_vb, 3 * N * 8);
+    add("sb", s.sb, 24 * N * 8);
+    add("cstart_last", s.cstart + last, 4);
+    add("cend_last", s.cend + last, 4);
+    add("nrain", s.nrain, 4);
+    add("dtv", s.dtv, 8);
+    add("dtmin", s.dtmin, 8);
+    return v;
+}
+
+}  // namespace
+
+int sphgpu_checkpoint_save(sphgpu_ctx* c, const char* path)
+{
+    if (!c || !path) return SPHGPU_E_ARG;
+    if (c->sticky) return c->sticky;
+    if (c->part_done) return SPHGPU_E_STATE;          // between steps only
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return SPHGPU_E_ARG;
+    int rc = 0;
+    CkHeader h = {};
+    std::memcpy(h.magic, kCkMagic, 8);
+    h.version = kCkVersion;
+    h.ndim = (uint32_t)c->P.ndim;
+    h.n = c->N; h.ctotal = c->P.ctotal; h.step = c->l_host; h.precision = c->precision; h.regu = c->regu;
+    h.cfl_on = c->d[0].p.cfl_on; h.cfl_c = c->d[0].p.cfl_c; h.cfl_f = c->d[0].p.cfl_f;
+    h.rain_set = c->rain_set; h.rain = c->rain;
+    h.has_fluid = c->h_fluid.empty() ? 0 : 1;
+    h.has_soil = c->h_soil.empty() ? 0 : 1;
+    std::vector<CkExtra> ex = ck_extras(c);
+    h.nextra = (int32_t)ex.size();
+    bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1;
+    std::vector<char> buf;
+    for (const FieldDef& fd : kFields) {
+        if (!ok) break;
+        const size_t count = (size_t)c->N * fd.ncomp, bytes = count * (fd.is_int ? 4 : 8);
+        buf.resize(bytes);
+        rc = sphgpu_get_field(c, fd.name, buf.data(), count);
+        if (rc) break;
+        ok = std::fwrite(buf.data(), 1, bytes, f) == bytes;
+    }
+    if (!rc && ok && h.has_fluid) ok = std::fwrite(c->h_fluid.data(), sizeof(sphgpu_fluid), c->N, f) == (size_t)c->N;
+    if (!rc && ok && h.has_soil) ok = std::fwrite(c->h_soil.data(), sizeof(sphgpu_soil), c->N, f) == (size_t)c->N;
+    for (const CkExtra& e : ex) {
+        if (rc || !ok) break;
+        buf.resize(e.bytes);
+        if (cuda_fail(c, cudaMemcpy(buf.data(), e.ptr, e.bytes, cudaMemcpyDeviceToHost), "cudaMemcpy")) {
+            rc = SPHGPU_E_CUDA;
+            break;
+        }
+        char name[16] = {};
+        std::strncpy(name, e.name, 15);
+        const uint64_t b = e.bytes;
+        ok = std::fwrite(name, 1, 16, f) == 16 && std::fwrite(&b, 8, 1, f) == 1 &&
+             std::fwrite(buf.data(), 1, e.bytes, f) == e.bytes;
+    }
+    if (std::fclose(f) != 0) ok = false;
+    if (rc) return rc;
+    return ok ? 0 : SPHGPU_E_ARG;
+}
+
+int sphgpu_checkpoint_load(sphgpu_ctx* c, const char* path)
+{
+    if (!c || !path) return SPHGPU_E_ARG;
+    if (c->sticky) return c->sticky;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return SPHGPU_E_ARG;
+    CkHeader h;
+    int rc = 0;
+    if (std::fread(&h, sizeof(h), 1, f) != 1 || std::memcmp(h.magic, kCkMagic, 8) != 0 ||
+        h.version != kCkVersion || (int)h.ndim != c->P.ndim || h.n != c->N || h.ctotal != c->P.ctotal) {
+        std::fclose(f);
+        return SPHGPU_E_ARG;
+    }
+    std::vector<char> buf;
+    for (const FieldDef& fd : kFields) {
+        const size_t count = (size_t)c->N * fd.ncomp, bytes = count * (fd.is_int ? 4 : 8);
+        buf.resize(bytes);
+        if (std::fread(buf.data(), 1, bytes, f) != bytes) { rc = SPHGPU_E_ARG; break; }
+        rc = sphgpu_set_field(c, fd.name, buf.data(), count);
+        if (rc) break;
+    }
+    std::vector<sphgpu_fluid> fl;
+    std::vector<sphgpu_soil> so;
+    if (!rc && h.has_fluid) {
+        fl.resize(c->N);
+        if (std::fread(fl.data(), sizeof(sphgpu_fluid), c->N, f) != (size_t)c->N) rc = SPHGPU_E_ARG;
+    }
+    if (!rc && h.has_soil) {
+        so.resize(c->N);
+        if (std::fread(so.data(), sizeof(sphgpu_soil), c->N, f) != (size_t)c->N) rc = SPHGPU_E_ARG;
+    }
+    if (!rc && (h.has_fluid || h.has_soil))
+        rc = sphgpu_set_materials(c, h.has_fluid ? fl.data() : nullptr, h.has_soil ? so.data() : nullptr, c->N);
+    if (!rc) rc = sphgpu_set_step(c, h.step);
+    if (!rc) rc = sphgpu_set_precision(c, h.precision);
+    if (!rc && h.rain_set) rc = sphgpu_set_rain(c, &h.rain);
+    if (!rc && h.cfl_on) rc = sphgpu_set_cfl(c, h.cfl_c, h.cfl_f);
+    // the device words and arrays last, over what the calls above set
+    std::vector<CkExtra> ex = ck_extras(c);
+    for (int q = 0; q < h.nextra && !rc; q++) {
+        char name[16];
+        uint64_t b = 0;
+        if (std::fread(name, 1, 16, f) != 16 || std::fread(&b, 8, 1, f) != 1) { rc = SPHGPU_E_ARG; break; }
+        name[15] = 0;
+        buf.resize(b);
+        if (std::fread(buf.data(), 1, b, f) != b) { rc = SPHGPU_E_ARG; break; }
+        for (const CkExtra& e : ex)
+            if (std::strcmp(e.name, name) == 0 && e.bytes == b &&
+                cuda_fail(c, cudaMemcpy(e.ptr, buf.data(), b, cudaMemcpyHostToDevice), "cudaMemcpy"))
+                rc = SPHGPU_E_CUDA;
+    }
+    std::fclose(f);
+    if (!rc && h.regu && !c->regu) { c->regu = true; invalidate_graphs(c); }
+    return rc;
+}
+
 int sphgpu_set_rain(sphgpu_ctx* c, const sphgpu_rain* rain)
 {
     if (!c || !rain) return SPHGPU_E_ARG;

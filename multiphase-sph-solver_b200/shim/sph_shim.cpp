@@ -164,6 +164,15 @@ int ensure_context(Particle* par, const Cell_Con& cc, const Para_Pro& pro)
         g_run.ctx = nullptr;
     }
     if (!g_run.ctx) {
+        // a new run: nothing recorded for an earlier array carries over
+        const sphgpu_params keep = P;
+        P = sphgpu_params{};
+        take_pro(pro);
+        P.xmin = keep.xmin; P.xmax = keep.xmax; P.ymin = keep.ymin; P.ymax = keep.ymax;
+        P.zmin = keep.zmin; P.zmax = keep.zmax;
+        P.cxm = keep.cxm; P.cym = keep.cym; P.czm = keep.czm; P.ctotal = keep.ctotal;
+        g_run.fluid = nullptr;
+        g_run.soil = nullptr;
         // what the methods of the first step have not told yet: the
         // reference's defaults (velocity-correction walls, the cubic spline,
         // the free-surface thresholds of CPP_1-SPHLoops.cpp:83-84)
@@ -229,6 +238,14 @@ int clNNPS_Fun::parttocell(Par_Cell*, cell_info*, const Cell_Con& pCellc, parti_
         download();
         return rc;
     }
+    // what the presence of a call tells (a drag form, a soil-structure
+    // contact, the saturation pass) is learnt afresh every step: a step that
+    // makes no such call runs without it
+    sphgpu_params& P = g_run.P;
+    P.fli = 0;
+    P.interc = 0.0; P.permtype = 0; P.pers = 0.0; P.perl = 0.0; P.perm = 0.0;
+    P.ss_type = 0; P.ss_myu = 0.0; P.ss_zeta = 0.0; P.ss_acc_type = 0;
+    P.flagum = 0;
     rc = ensure_context(pPar, pCellc, pPPro);
     if (rc) return rc;
     rc = sphgpu_parttocell(g_run.ctx);

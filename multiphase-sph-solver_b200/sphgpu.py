@@ -265,6 +265,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_update.argtypes = [C.c_void_p]
     lib.sphgpu_kl_wait_check.argtypes = [C.c_void_p, C.c_longlong]
     lib.sphgpu_set_rain.argtypes = [C.c_void_p, C.POINTER(Rain)]
+    lib.sphgpu_checkpoint_save.argtypes = [C.c_void_p, C.c_char_p]
+    lib.sphgpu_checkpoint_load.argtypes = [C.c_void_p, C.c_char_p]
     lib.sphgpu_get_rain.argtypes = [C.c_void_p, C.POINTER(Rain)]
     _lib = lib
     return lib
@@ -409,6 +411,12 @@ class Engine:
 
     def update(self) -> int:
         return int(self.lib.sphgpu_update(self.h))
+
+    def checkpoint_save(self, path: str) -> None:
+        self._check(self.lib.sphgpu_checkpoint_save(self.h, path.encode()), "sphgpu_checkpoint_save")
+
+    def checkpoint_load(self, path: str) -> None:
+        self._check(self.lib.sphgpu_checkpoint_load(self.h, path.encode()), "sphgpu_checkpoint_load")
 
     def set_rain(self, rain: dict) -> None:
         """sphgpu_set_rain: the rainfall record of a run with flr = 1."""
