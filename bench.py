@@ -297,6 +297,8 @@ def bulk_form(st, args, device, ref_fields, moving):
     eng = sphgpu.Engine(st.params, device=device)
     eng.load_state(st.fields, st.fluid, st.soil)
     eng.set_precision(sphgpu.PREC_FP32_BULK)
+    if not args.no_autotune:
+        eng.autotune(steps=1)
     eng.step(args.warmup)
     eng.synchronize()
     eng.step(args.steps)
@@ -390,6 +392,8 @@ def batched_slopes(args, device: int, count: int = 256, dx: float = 0.05, steps_
         kl_s = time.perf_counter() - t0
         if form == "fp32_bulk":
             eng.set_precision(sphgpu.PREC_FP32_BULK)
+        if not args.no_autotune:
+            eng.autotune(steps=1)
         eng.step(args.warmup)
         eng.synchronize()
         eng.step(args.steps)
@@ -426,6 +430,14 @@ def engine_arm(args, world, rank, local):
     device = local if world > 1 else args.device
     eng = sphgpu.Engine(st.params, device=device)
     eng.load_state(st.fields, st.fluid, st.soil)
+    tune = None
+    if not args.no_autotune:
+        # the project's autotuner: threads per block of each neighbour pass,
+        # timed over steps of the run (4 candidates x 1 step)
+        table = eng.autotune(steps=1)
+        tune = {"passes": list(sphgpu.Engine.TUNE_PASSES), "threads_per_block": [int(v) for v in eng.launch()],
+                "ms_per_step_by_candidate": {str(b): [round(float(x), 4) for x in table[a]]
+                                             for a, b in enumerate((32, 64, 96, 128))}}
     eng.step(args.warmup)
     barrier(world)
     eng.synchronize()
@@ -513,6 +525,7 @@ def engine_arm(args, world, rank, local):
                        "l2": "inputs larger than L2 (state ~%.1f GB per GPU)" % (scene.n * 1.0e3 / 1e9),
                        "timing": "CUDA events on the engine stream around K graph launches"},
             "gpu_launches": int(launches),
+            "autotune": tune,
             "clocks": clk,
             "roofline": {"bound": "hbm", "pass": dominant, "kernels": pass_kernels, "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
@@ -555,6 +568,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kl", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         # host-only arm: rank 0 runs it, the other ranks exit without work

@@ -339,6 +339,29 @@ int sphgpu_synchronize(sphgpu_ctx* ctx);
 double sphgpu_last_step_ms(const sphgpu_ctx* ctx);
 long   sphgpu_last_step_launches(const sphgpu_ctx* ctx);
 
+/*
+ * Launch shapes and their autotuner (no counterpart in the reference, whose
+ * OpenMP loops take their thread count from the input deck).  Each of the
+ * SPHGPU_TUNE_PASSES neighbour passes -- the search scan, its resolve pass,
+ * the pair records, density, Shepard + EOS, strain, the constitutive update,
+ * the two momentum stages, XSPH + update, in that order -- runs one particle
+ * per thread with 32 to 128 threads per block (a multiple of 32).
+ * sphgpu_set_launch / sphgpu_get_launch set and read those sizes;
+ * sphgpu_autotune runs `steps` steps of the run with each of 32, 64, 96 and
+ * 128 threads per block, times every pass with CUDA events, and keeps for
+ * each pass the fastest (ties keep 128).  The steps it runs are steps of the
+ * run: a launch shape changes no result, bit for bit.  With cache_path the
+ * choice is kept in that text file under a key of the GPU model and the
+ * run's shape (dimension, particle count, wall, drag and contact types,
+ * precision form, instances), and a later call with the same key applies it
+ * without measuring.  table, if non-NULL, receives the mean ms per step of
+ * each pass for each candidate (4 x SPHGPU_TUNE_PASSES, candidate-major).
+ */
+#define SPHGPU_TUNE_PASSES 10
+int sphgpu_set_launch(sphgpu_ctx* ctx, const int* threads_per_block, int n);
+int sphgpu_get_launch(const sphgpu_ctx* ctx, int* threads_per_block, int n);
+int sphgpu_autotune(sphgpu_ctx* ctx, int steps, const char* cache_path, double* table);
+
 /* The context's CUDA stream (a cudaStream_t), for callers that order their own
  * work after the engine's. */
 void*  sphgpu_stream(sphgpu_ctx* ctx);

@@ -223,6 +223,7 @@ void fill_dev_params(DevParams& p, const sphgpu_params* P)
     p.cfl_on = 0; p.cfl_c = 0.0; p.cfl_f = 0.0;
     p.st_vpu = P->structure.vpu;
     p.ninst = 0;
+    for (int q = 0; q < TP_COUNT; q++) p.tb[q] = 128;
     p.flr = P->flr == 1 ? 1 : 0;
     p.rain_lp = 0; p.rain_vrain = 0.0; p.rain_press = 0.0;
 }
@@ -1209,6 +1210,7 @@ int sphgpu_update_params(sphgpu_ctx* c, const sphgpu_params* P)
         dp.bulk = keep.bulk;
         dp.cfl_on = keep.cfl_on; dp.cfl_c = keep.cfl_c; dp.cfl_f = keep.cfl_f;
         dp.rain_lp = keep.rain_lp; dp.rain_vrain = keep.rain_vrain; dp.rain_press = keep.rain_press;
+        for (int q = 0; q < TP_COUNT; q++) dp.tb[q] = keep.tb[q];
     }
     c->P = *P;
     invalidate_graphs(c);
@@ -1606,6 +1608,122 @@ int sphgpu_step_profiled(sphgpu_ctx* c, int nsteps, double* stage_ms)
     }
     for (int k = 0; k <= SPHK_NSTAGES; k++) cudaEventDestroy(ev[k]);
     return err;
+}
+
+namespace {
+
+static_assert(TP_COUNT == SPHGPU_TUNE_PASSES, "tuned passes");
+
+// the stages (sphk_stage_names) whose device time each tuned pass is
+const char* const kTuneStages[TP_COUNT][2] = {
+    {"k_nnps", nullptr}, {"k_nnps_resolve", nullptr}, {"k_pairw", nullptr}, {"k_density", nullptr},
+    {"k_shepard_eos", nullptr}, {"k_strain", nullptr}, {"k_stress", "k_stress_2"}, {"k_accel_a", nullptr},
+    {"k_accel_b", nullptr}, {"k_xsph_update", nullptr},
+};
+
+int stage_index(const char* name)
+{
+    for (int k = 0; k < SPHK_NSTAGES; k++)
+        if (std::strcmp(sphk_stage_names[k], name) == 0) return k;
+    return -1;
+}
+
+void set_tb(sphgpu_ctx* c, const int* tb)
+{
+    for (int p = 0; p < 2; p++)
+        for (int q = 0; q < TP_COUNT; q++) c->d[p].p.tb[q] = tb[q];
+    invalidate_graphs(c);
+}
+
+// what a tuned shape is kept for: the GPU model and the run's shape
+std::string tune_key(const sphgpu_ctx* c)
+{
+    cudaDeviceProp prop;
+    std::string name = "unknown";
+    if (cudaGetDeviceProperties(&prop, c->device) == cudaSuccess) name = prop.name;
+    for (char& ch : name)
+        if (ch == ' ') ch = '_';
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), "%s/ndim%d/n%d/flbndy%d/fli%d/ss%d/prec%d/inst%d", name.c_str(), c->P.ndim,
+                  c->N, c->P.flbndy, c->P.fli, c->P.ss_type, c->precision, (int)c->h_inst.size());
+    return buf;
+}
+
+}  // namespace
+
+int sphgpu_set_launch(sphgpu_ctx* c, const int* tb, int n)
+{
+    if (!c || !tb || n != TP_COUNT) return SPHGPU_E_ARG;
+    for (int q = 0; q < n; q++)
+        if (tb[q] < 32 || tb[q] > 128 || tb[q] % 32 != 0) return SPHGPU_E_ARG;
+    set_tb(c, tb);
+    return 0;
+}
+
+int sphgpu_get_launch(const sphgpu_ctx* c, int* tb, int n)
+{
+    if (!c || !tb || n != TP_COUNT) return SPHGPU_E_ARG;
+    for (int q = 0; q < n; q++) tb[q] = c->d[0].p.tb[q];
+    return 0;
+}
+
+int sphgpu_autotune(sphgpu_ctx* c, int steps, const char* cache_path, double* table)
+{
+    if (!c || steps <= 0) return SPHGPU_E_ARG;
+    const std::string key = tune_key(c);
+    if (cache_path) {
+        if (FILE* f = std::fopen(cache_path, "r")) {
+            char line[512];
+            int found = 0, tb[TP_COUNT];
+            while (std::fgets(line, sizeof(line), f)) {
+                char k[300];
+                int v[TP_COUNT];
+                if (std::sscanf(line, "%299s %d %d %d %d %d %d %d %d %d %d", k, &v[0], &v[1], &v[2], &v[3], &v[4],
+                                &v[5], &v[6], &v[7], &v[8], &v[9]) == 1 + TP_COUNT && key == k) {
+                    std::memcpy(tb, v, sizeof(tb));
+                    found = 1;
+                }
+            }
+            std::fclose(f);
+            if (found && sphgpu_set_launch(c, tb, TP_COUNT) == 0) return 0;
+        }
+    }
+    const int cand[4] = {32, 64, 96, 128};
+    double t[4][TP_COUNT];
+    std::vector<double> stage_ms(SPHK_NSTAGES);
+    for (int a = 0; a < 4; a++) {
+        int tb[TP_COUNT];
+        for (int q = 0; q < TP_COUNT; q++) tb[q] = cand[a];
+        set_tb(c, tb);
+        int rc = sphgpu_step_profiled(c, steps, stage_ms.data());
+        if (rc) return rc;
+        for (int q = 0; q < TP_COUNT; q++) {
+            t[a][q] = 0.0;
+            for (int e = 0; e < 2; e++)
+                if (kTuneStages[q][e]) {
+                    const int k = stage_index(kTuneStages[q][e]);
+                    if (k >= 0) t[a][q] += stage_ms[k] / steps;
+                }
+            if (table) table[a * TP_COUNT + q] = t[a][q];
+        }
+    }
+    int best[TP_COUNT];
+    for (int q = 0; q < TP_COUNT; q++) {
+        int b = 3;                          // ties keep the default of 128
+        for (int a = 0; a < 4; a++)
+            if (t[a][q] < t[b][q]) b = a;
+        best[q] = cand[b];
+    }
+    set_tb(c, best);
+    if (cache_path) {
+        if (FILE* f = std::fopen(cache_path, "a")) {
+            std::fprintf(f, "%s", key.c_str());
+            for (int q = 0; q < TP_COUNT; q++) std::fprintf(f, " %d", best[q]);
+            std::fprintf(f, "\n");
+            std::fclose(f);
+        }
+    }
+    return 0;
 }
 
 double sphgpu_last_step_ms(const sphgpu_ctx* c) { return c ? c->last_ms : 0.0; }

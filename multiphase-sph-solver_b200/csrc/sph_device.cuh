@@ -43,6 +43,14 @@ struct InstGrid {
     int first_vbx_wall;        // its first wall (index order) with matype > 2, or first + count
 };
 
+// Passes whose threads per block the autotuner picks (one particle per
+// thread; every pass is written for any multiple of 32 up to its launch
+// bound of 128)
+enum TunePass {
+    TP_NNPS, TP_RESOLVE, TP_PAIRW, TP_DENSITY, TP_SHEPARD, TP_STRAIN, TP_STRESS, TP_ACCEL_A, TP_ACCEL_B,
+    TP_XSPH, TP_COUNT
+};
+
 struct DevParams {
     int N, ndim, flknl, flbndy, fli, if_move, flv, inip, step_regu;
     int cxm, cym, czm, ctotal;
@@ -76,6 +84,7 @@ struct DevParams {
     double cfl_c, cfl_f;       // factors of h / (c + |v|) and sqrt(h / |a|)
     double st_vpu;             // Para_Structure::vpu, the structure's sound speed
     int ninst;                 // batched context: number of instances (0: one system)
+    int tb[TP_COUNT];          // threads per block of the tuned passes
     // rainfall (flr 1, rtype 1): rainini's lp and vrain, Para_Rain::press_factor
     int flr, rain_lp;
     double rain_vrain, rain_press;

@@ -2752,6 +2752,14 @@ using namespace SPH_NS;
 
 static inline unsigned nblk(long n, int b) { return (unsigned)((n + b - 1) / b); }
 
+// threads per block of a tuned pass (128 unless the autotuner chose another
+// multiple of 32)
+static inline int tbk(const Dev& d, int pass)
+{
+    const int b = d.p.tb[pass];
+    return (b >= 32 && b <= 128 && b % 32 == 0) ? b : 128;
+}
+
 #define REC(k) do { if (ev) cudaEventRecord(ev[k], st); } while (0)
 
 #ifndef SPH_BULK32
@@ -2805,11 +2813,11 @@ extern "C" int sphk_enqueue_nnps_parts(const Dev* dp, void* sort_tmp, size_t sor
     }
     if (parts & 2) {
         REC(4);
-        LAUNCH_ND(k_nnps, nblk(N, 128), 128, d); n++;
+        LAUNCH_ND(k_nnps, nblk(N, tbk(d, TP_NNPS)), tbk(d, TP_NNPS), d); n++;
         REC(5);
-        LAUNCH_ND(k_nnps_resolve, nblk(N, 128), 128, d); n++;
+        LAUNCH_ND(k_nnps_resolve, nblk(N, tbk(d, TP_RESOLVE)), tbk(d, TP_RESOLVE), d); n++;
         REC(6);
-        LAUNCH_ND(k_pairw, nblk(N, 128), 128, d); n++;
+        LAUNCH_ND(k_pairw, nblk(N, tbk(d, TP_PAIRW)), tbk(d, TP_PAIRW), d); n++;
     }
     if (parts & 4) {
         REC(7);
@@ -2835,36 +2843,36 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
     const int N = d.p.N;
     int n = 0;
     REC(8);
-    LAUNCH_ND(k_density, nblk(N, 128), 128, d); n++;
+    LAUNCH_ND(k_density, nblk(N, tbk(d, TP_DENSITY)), tbk(d, TP_DENSITY), d); n++;
     REC(9);
-    LAUNCH_ND(k_shepard_eos, nblk(N, 128), 128, d); n++;
+    LAUNCH_ND(k_shepard_eos, nblk(N, tbk(d, TP_SHEPARD)), tbk(d, TP_SHEPARD), d); n++;
     REC(10);
-    LAUNCH_ND(k_strain, nblk(N, 128), 128, d); n++;
+    LAUNCH_ND(k_strain, nblk(N, tbk(d, TP_STRAIN)), tbk(d, TP_STRAIN), d); n++;
     if (d.p.flagum == 1) { k_saturation<<<nblk(N, 128), 128, 0, st>>>(d); n++; }
     REC(11);
     if (regu) { LAUNCH_ND(k_regu, nblk(N, 128), 128, d, d.s.eps, d.s.eps_tmp, 1); n++; }
     REC(12);
     if (regu) {
-        if (d.p.ndim == 2) k_stress<2, 1><<<nblk(N, 128), 128, 0, st>>>(d);
-        else k_stress<3, 1><<<nblk(N, 128), 128, 0, st>>>(d);
+        if (d.p.ndim == 2) k_stress<2, 1><<<nblk(N, tbk(d, TP_STRESS)), tbk(d, TP_STRESS), 0, st>>>(d);
+        else k_stress<3, 1><<<nblk(N, tbk(d, TP_STRESS)), tbk(d, TP_STRESS), 0, st>>>(d);
     } else {
-        if (d.p.ndim == 2) k_stress<2, 0><<<nblk(N, 128), 128, 0, st>>>(d);
-        else k_stress<3, 0><<<nblk(N, 128), 128, 0, st>>>(d);
+        if (d.p.ndim == 2) k_stress<2, 0><<<nblk(N, tbk(d, TP_STRESS)), tbk(d, TP_STRESS), 0, st>>>(d);
+        else k_stress<3, 0><<<nblk(N, tbk(d, TP_STRESS)), tbk(d, TP_STRESS), 0, st>>>(d);
     }
     n++;
     REC(13);
     if (regu) { LAUNCH_ND(k_regu, nblk(N, 128), 128, d, d.s.sig_next, d.s.sig_tmp, 0); n++; }
     REC(14);
     if (regu) {
-        if (d.p.ndim == 2) k_stress<2, 2><<<nblk(N, 128), 128, 0, st>>>(d);
-        else k_stress<3, 2><<<nblk(N, 128), 128, 0, st>>>(d);
+        if (d.p.ndim == 2) k_stress<2, 2><<<nblk(N, tbk(d, TP_STRESS)), tbk(d, TP_STRESS), 0, st>>>(d);
+        else k_stress<3, 2><<<nblk(N, tbk(d, TP_STRESS)), tbk(d, TP_STRESS), 0, st>>>(d);
         n++;
     }
     REC(15);
     const bool art = d.p.art_stre_coe > 0.0;
     if (art) { LAUNCH_ND(k_art_rij, nblk(N, 128), 128, d); n++; }
     REC(16);
-    LAUNCH_ND(k_accel_a, nblk(N, 128), 128, d); n++;
+    LAUNCH_ND(k_accel_a, nblk(N, tbk(d, TP_ACCEL_A)), tbk(d, TP_ACCEL_A), d); n++;
     if (d.p.flbndy == 5) { LAUNCH_ND(k_free_solid, nblk(N, 128), 128, d); n++; }
     if (d.p.ss_coupled) { k_coupled<<<nblk(N, 128), 128, 0, st>>>(d); n++; }
     if (d.p.ss_type >= 1) {
@@ -2874,7 +2882,7 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
     REC(17);
     {
         const bool drag = d.p.fli > 1;
-        const dim3 g(nblk(N, 128)), b(128);
+        const dim3 g(nblk(N, tbk(d, TP_ACCEL_B))), b(tbk(d, TP_ACCEL_B));
         if (d.p.ndim == 2) {
             k_accel_b<2, 0, 0><<<g, b, 0, st>>>(d);
             if (drag) k_accel_b<2, 1, 1><<<g, b, 0, st>>>(d);
@@ -2891,7 +2899,7 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
     }
     n += 3;
     REC(18);
-    LAUNCH_ND(k_xsph_update, nblk(N, 128), 128, d); n++;
+    LAUNCH_ND(k_xsph_update, nblk(N, tbk(d, TP_XSPH)), tbk(d, TP_XSPH), d); n++;
     REC(19);
     if (d.p.flbndy == 2) {
         LAUNCH_ND(k_tm_vb, nblk(N, 128), 128, d); n++;

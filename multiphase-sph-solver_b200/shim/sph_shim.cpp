@@ -98,6 +98,26 @@ void shim_fail(const char* what, int code)
     std::fprintf(stderr, "sphgpu shim: %s failed: %d (%s)\n", what, code, sphgpu_error_string(code));
 }
 
+// SPHGPU_SHIM_TRACE=1: the parameters each push hands the engine, on stderr
+void trace_params(const char* when, const sphgpu_params& P)
+{
+    const char* t = std::getenv("SPHGPU_SHIM_TRACE");
+    if (!t || t[0] != '1') return;
+    std::fprintf(stderr,
+                 "sphgpu shim %s: ndim %d n %d flknl %d flbndy %d fli %d flv %d flts %d flagum %d inip %d "
+                 "step_regu %d loop %d fop %d dr %.17g dt %.17g g %.17g %.17g %.17g thr %.17g %.17g "
+                 "interc %.17g permtype %d pers %.17g perl %.17g perm %.17g ss %d %.17g %.17g %d coe_bndy %.17g "
+                 "if_cal %d if_move %d move %.17g %.17g %.17g alphats %.17g acc %d %d art %.17g xsph %.17g %.17g %.17g "
+                 "st %.17g %.17g %.17g %.17g %.17g %.17g %.17g\n",
+                 when, P.ndim, P.ntotal, P.flknl, P.flbndy, P.fli, P.flv, P.flts, P.flagum, P.inip, P.step_regu,
+                 P.loop, P.fop, P.dr, P.dt, P.gx, P.gy, P.gz, P.threshold_min, P.threshold_max, P.interc,
+                 P.permtype, P.pers, P.perl, P.perm, P.ss_type, P.ss_myu, P.ss_zeta, P.ss_acc_type, P.coe_bndy,
+                 P.if_cal, P.if_move, P.move_vx[0], P.move_vx[1], P.move_vx[2], P.alphats, P.water_acc_type,
+                 P.air_acc_type, P.art_stre_coe, P.xsph[0], P.xsph[1], P.xsph[2], P.structure.dens,
+                 P.structure.eps0, P.structure.e, P.structure.poi, P.structure.vpu, P.structure.porosity,
+                 P.structure.cop);
+}
+
 void take_pro(const Para_Pro& pro)
 {
     sphgpu_params& P = g_run.P;
@@ -487,6 +507,7 @@ void clUpdate_Fun::update(Particle* pPar, const Para_Pro& pPPro, const Para_Boun
     for (int k = 0; k < 3; k++) P.move_vx[k] = pPBou.move_vx[k];
     int rc = 0;
     if (std::memcmp(&P, &g_run.pushed, sizeof(P)) != 0) {
+        trace_params("update_params", P);
         rc = sphgpu_update_params(g_run.ctx, &P);
         if (rc) shim_fail("sphgpu_update_params", rc);
         else g_run.pushed = P;

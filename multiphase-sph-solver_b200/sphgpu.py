@@ -265,6 +265,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_update.argtypes = [C.c_void_p]
     lib.sphgpu_kl_wait_check.argtypes = [C.c_void_p, C.c_longlong]
     lib.sphgpu_set_rain.argtypes = [C.c_void_p, C.POINTER(Rain)]
+    lib.sphgpu_set_launch.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    lib.sphgpu_get_launch.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    lib.sphgpu_autotune.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_void_p]
     lib.sphgpu_checkpoint_save.argtypes = [C.c_void_p, C.c_char_p]
     lib.sphgpu_checkpoint_load.argtypes = [C.c_void_p, C.c_char_p]
     lib.sphgpu_get_rain.argtypes = [C.c_void_p, C.POINTER(Rain)]
@@ -411,6 +414,27 @@ class Engine:
 
     def update(self) -> int:
         return int(self.lib.sphgpu_update(self.h))
+
+    TUNE_PASSES = ("k_nnps", "k_nnps_resolve", "k_pairw", "k_density", "k_shepard_eos", "k_strain", "k_stress",
+                   "k_accel_a", "k_accel_b", "k_xsph_update")
+
+    def set_launch(self, threads_per_block) -> None:
+        tb = np.ascontiguousarray(threads_per_block, dtype=np.int32)
+        self._check(self.lib.sphgpu_set_launch(self.h, _ptr(tb), tb.size), "sphgpu_set_launch")
+
+    def launch(self) -> np.ndarray:
+        tb = np.zeros(len(self.TUNE_PASSES), np.int32)
+        self._check(self.lib.sphgpu_get_launch(self.h, _ptr(tb), tb.size), "sphgpu_get_launch")
+        return tb
+
+    def autotune(self, steps: int = 2, cache_path: str | None = None) -> np.ndarray:
+        """Threads per block of each tuned pass picked by timing (runs 4 x steps
+        steps of the run); returns the ms per step measured (candidates 32, 64,
+        96, 128 by pass), zeros when the choice came from cache_path."""
+        table = np.zeros((4, len(self.TUNE_PASSES)))
+        path = cache_path.encode() if cache_path else None
+        self._check(self.lib.sphgpu_autotune(self.h, int(steps), path, _ptr(table)), "sphgpu_autotune")
+        return table
 
     def checkpoint_save(self, path: str) -> None:
         self._check(self.lib.sphgpu_checkpoint_save(self.h, path.encode()), "sphgpu_checkpoint_save")
