@@ -173,24 +173,36 @@ def dist_setup():
     return world, rank, local
 
 
-def dist_max(x: float, world: int) -> float:
-    if world == 1:
-        return x
+def _reduce(x: float, op) -> float:
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    # NCCL reduces device tensors; the gloo backend (CPU runs) host tensors
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def dist_max(x: float, world: int) -> float:
+    """The slowest replica's time: the max over ranks."""
+    if world == 1:
+        return x
+    import torch.distributed as dist
+    return _reduce(x, dist.ReduceOp.MAX)
 
 
 def dist_sum(x: float, world: int) -> float:
+    """The particles of all replicas: the sum over ranks."""
     if world == 1:
         return x
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(x, dist.ReduceOp.SUM)
+
+
+def replica_value(n_active: float, steps: int, ms: float, world: int) -> float:
+    """Whole-job particle-updates/s of independent replicas: every rank's
+    active particles times the steps, over the slowest rank's time."""
+    return dist_sum(float(n_active), world) * steps / (dist_max(ms, world) / 1e3)
 
 
 def barrier(world: int):
