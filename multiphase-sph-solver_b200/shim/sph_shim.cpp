@@ -24,8 +24,9 @@
 //     and runs the rest of the step as the engine's fused passes
 //     (sphgpu_update).  An error from that work, which update cannot return,
 //     is returned by the next parttocell.
-//   * host copy: the Particle array is uploaded when the shim first sees it
-//     (or sees a different array or particle count) and downloaded after the
+//   * host copy: the Particle array is uploaded when a run starts (an array,
+//     a particle count or a step counter the device's state does not
+//     continue: l = 1, or an l other than the device's) and downloaded after the
 //     steps whose state SPH_Calculation writes out (l % fop == 0, l == 1, and
 //     the step after which the time runs out, CPP_1-SPHLoops.cpp:761-783).
 //     With SPHGPU_SHIM_SYNC=always in the environment it is uploaded before
@@ -179,7 +180,11 @@ int ensure_context(Particle* par, const Cell_Con& cc, const Para_Pro& pro)
     P.cxm = cc.cxm; P.cym = cc.cym; P.czm = cc.czm; P.ctotal = cc.ctotal;
     const char* mode = std::getenv("SPHGPU_SHIM_SYNC");
     g_run.sync_always = mode && std::strcmp(mode, "always") == 0;
-    if (g_run.ctx && (g_run.par != par || g_run.n != pro.ntotal)) {
+    // a new run: another array, another particle count, or a step counter
+    // that does not continue the device's (a run that starts again at l = 1
+    // may be handed an array at the address the previous run's had)
+    if (g_run.ctx && (g_run.par != par || g_run.n != pro.ntotal || pro.l == 1 ||
+                      pro.l != sphgpu_get_step(g_run.ctx))) {
         sphgpu_destroy(g_run.ctx);
         g_run.ctx = nullptr;
     }
