@@ -45,7 +45,8 @@ extern "C" int sphk_kl_synthesize(int n, int ndim, int K, int R, int no, int typ
                                   double mean_value, double sd_value, double coe_depth, double soil_max,
                                   double water_max, const double* d_xh, const int* d_type, const void* d_terms,
                                   const double* d_sqrt_eig, const double* d_xi, float* c_hi, float* c_lo,
-                                  float* d_out, int* d_err, cudaStream_t st);
+                                  float* d_out, int* d_err, cudaStream_t st, const void* d_modes,
+                                  const int* nmode, const unsigned short* d_tidx);
 
 namespace {
 
@@ -1780,6 +1781,7 @@ struct HostKLTerm { double w, alpha; int use_cos; int pad; };
 struct KLPlan {
     std::vector<HostKLTerm> terms;   // K x ndim
     std::vector<double> sqrt_eig;    // K
+    std::vector<int> ids;            // K x ndim: the 1-D eigenfunction index of each term on each axis
 };
 
 int kl_plan(sphgpu_ctx* c, const double a[3], const sphgpu_kl_field& f, int K, KLPlan& plan)
@@ -1829,6 +1831,7 @@ int kl_plan(sphgpu_ctx* c, const double a[3], const sphgpu_kl_field& f, int K, K
         std::vector<double>& se = plan.sqrt_eig;
         terms.assign((size_t)K * nd, HostKLTerm{});
         se.assign(K, 0.0);
+        plan.ids.assign((size_t)K * nd, 0);
         for (int j = 0; j < K; j++) {
             int id[3];
             if (nd == 2) { id[0] = (int)(idx[j] / K); id[1] = (int)(idx[j] % K); }
@@ -1838,6 +1841,7 @@ int kl_plan(sphgpu_ctx* c, const double a[3], const sphgpu_kl_field& f, int K, K
                 id[2] = (int)(idx[j] % K);
             }
             for (int d = 0; d < nd; d++) {
+                plan.ids[(size_t)j * nd + d] = id[d];
                 const double w = wi[(size_t)id[d] * 3 + d], ad = a[d];
                 HostKLTerm& t = terms[(size_t)j * nd + d];
                 t.w = w;
@@ -2061,14 +2065,32 @@ int sphgpu_kl_synthesize(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgp
     std::vector<TCTerm> tc(plan.terms.size());
     for (size_t q = 0; q < tc.size(); q++)
         tc[q] = TCTerm{plan.terms[q].w, (float)plan.terms[q].alpha, plan.terms[q].use_cos};
+    // the separable form: per axis the distinct 1-D eigenfunctions the terms
+    // use (in order of first use) and each term's index among them
+    std::vector<TCTerm> modes;
+    std::vector<unsigned short> tidx((size_t)K * nd);
+    int nmode[3] = {0, 0, 0};
+    for (int d = 0; d < nd; d++) {
+        std::vector<int> slot(K, -1);
+        for (int j = 0; j < K; j++) {
+            const int id = plan.ids[(size_t)j * nd + d];
+            if (slot[id] < 0) {
+                slot[id] = nmode[d]++;
+                modes.push_back(tc[(size_t)j * nd + d]);
+            }
+            tidx[(size_t)j * nd + d] = (unsigned short)slot[id];
+        }
+    }
     const int Rc = R < 256 ? R : 256;   // realisations per launch
     const size_t off_se = 256 * ((sizeof(TCTerm) * tc.size() + 255) / 256);
     const size_t off_xi = off_se + 256 * ((8 * (size_t)K + 255) / 256);
     const size_t off_ch = off_xi + 256 * ((8 * (size_t)Rc * K + 255) / 256);
     const size_t off_cl = off_ch + 256 * ((4 * (size_t)Rc * K + 255) / 256);
     const size_t off_err = off_cl + 256 * ((4 * (size_t)Rc * K + 255) / 256);
+    const size_t off_md = off_err + 256;
+    const size_t off_ti = off_md + 256 * ((sizeof(TCTerm) * modes.size() + 255) / 256);
     void* buf = nullptr;
-    CK(cudaMalloc(&buf, off_err + 16));
+    CK(cudaMalloc(&buf, off_ti + 2 * tidx.size() + 16));
     char* b = (char*)buf;
     float total_ms = 0.f;
     do {
@@ -2076,7 +2098,11 @@ int sphgpu_kl_synthesize(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgp
                       "cudaMemcpyAsync") ||
             cuda_fail(c, cudaMemcpyAsync(b + off_se, plan.sqrt_eig.data(), 8 * (size_t)K, cudaMemcpyHostToDevice,
                                          c->st), "cudaMemcpyAsync") ||
-            cuda_fail(c, cudaMemsetAsync(b + off_err, 0, 16, c->st), "cudaMemsetAsync")) { rc = SPHGPU_E_CUDA; break; }
+            cuda_fail(c, cudaMemsetAsync(b + off_err, 0, 16, c->st), "cudaMemsetAsync") ||
+            cuda_fail(c, cudaMemcpyAsync(b + off_md, modes.data(), sizeof(TCTerm) * modes.size(),
+                                         cudaMemcpyHostToDevice, c->st), "cudaMemcpyAsync") ||
+            cuda_fail(c, cudaMemcpyAsync(b + off_ti, tidx.data(), 2 * tidx.size(), cudaMemcpyHostToDevice, c->st),
+                      "cudaMemcpyAsync")) { rc = SPHGPU_E_CUDA; break; }
         const DevState& s = c->d[c->parity].s;
         for (int r0 = 0; r0 < R && !rc; r0 += Rc) {
             const int rr = (R - r0) < Rc ? (R - r0) : Rc;
@@ -2086,7 +2112,8 @@ int sphgpu_kl_synthesize(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgp
             if (sphk_kl_synthesize(N, nd, K, rr, f->no, f->type, xt, f->mean_value, f->sd_value, f->coe_depth,
                                    soil_max, water_max, s.xh, s.type, b, (const double*)(b + off_se),
                                    (const double*)(b + off_xi), (float*)(b + off_ch), (float*)(b + off_cl),
-                                   d_out + (size_t)r0 * N, (int*)(b + off_err), c->st)) {
+                                   d_out + (size_t)r0 * N, (int*)(b + off_err), c->st, b + off_md, nmode,
+                                   (const unsigned short*)(b + off_ti))) {
                 rc = cuda_fail(c, cudaGetLastError(), "K-L synthesis launch");
                 if (!rc) rc = SPHGPU_E_ARG;
                 break;

@@ -49,6 +49,13 @@ struct KLTCArgs {
     int* err;
     long long budget;          // SM clocks one completion wait may take
     int probe;                 // 1: the wait self-test (below), no synthesis
+    // the separable form: the distinct 1-D eigenfunctions of each axis
+    // (nmode[d] of them, from modes + moff[d]) and, per term and axis, the
+    // index of its factor among them (tidx, K x ndim); null: each term's
+    // factors are evaluated in the tile loop
+    const KLTCTerm* modes;
+    int nmode[3], moff[3];
+    const unsigned short* tidx;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
@@ -109,6 +116,11 @@ __global__ void __launch_bounds__(KL_TILE_M, 1) k_kl_synth(KLTCArgs a)
     unsigned char* B_lo = B_hi + b_bytes;
     uint64_t* bar = reinterpret_cast<uint64_t*>(B_lo + b_bytes);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+    // separable form: each particle's values of the distinct 1-D factors,
+    // table[m * 128 + thread], then the factor indices of the K terms
+    float* table = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(bar) + 16);
+    const int nmodes = a.modes ? a.nmode[0] + a.nmode[1] + a.nmode[2] : 0;
+    unsigned short* tix = reinterpret_cast<unsigned short*>(table + (size_t)nmodes * KL_TILE_M);
 
     const int t = threadIdx.x, warp = t >> 5;
     int ncols = 32;
@@ -140,6 +152,26 @@ __global__ void __launch_bounds__(KL_TILE_M, 1) k_kl_synth(KLTCArgs a)
         xa[2] = r1.x - a.x_trans[2];
         yp = r0.y;
     }
+    if (a.modes && !a.probe) {
+        // each distinct factor once per particle and axis: alpha cos / sin of
+        // w x reduced modulo 2 pi in FP64, the values the tile loop below
+        // multiplies (the same operations as the direct form, so the same
+        // floats)
+        const double two_pi_ = 6.283185307179586, inv_two_pi_ = 0.15915494309189535;
+        for (int d = 0; d < a.ndim; d++)
+            for (int m = 0; m < a.nmode[d]; m++) {
+                float v = 0.f;
+                if (live) {
+                    const KLTCTerm q = a.modes[a.moff[d] + m];
+                    const double arg = q.w * xa[d];
+                    const float red = (float)(arg - rint(arg * inv_two_pi_) * two_pi_);
+                    v = q.alpha * (q.use_cos ? cosf(red) : sinf(red));
+                }
+                table[(size_t)(a.moff[d] + m) * KL_TILE_M + t] = v;
+            }
+        for (int e = t; e < a.K * a.ndim; e += KL_TILE_M) tix[e] = a.tidx[e];
+        __syncthreads();
+    }
     // instruction descriptor: D F32, A and B TF32, both K-major, N = R, M = 128
     const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(R >> 3) << 17) |
                            ((uint32_t)(KL_TILE_M >> 4) << 24);
@@ -165,11 +197,16 @@ __global__ void __launch_bounds__(KL_TILE_M, 1) k_kl_synth(KLTCArgs a)
             float phi = 0.f;
             if (live && k < kt) {
                 phi = 1.f;
-                for (int d = 0; d < a.ndim; d++) {
-                    const KLTCTerm q = a.terms[(size_t)(k0 + k) * a.ndim + d];
-                    const double arg = q.w * xa[d];
-                    const float red = (float)(arg - rint(arg * inv_two_pi) * two_pi);
-                    phi *= q.alpha * (q.use_cos ? cosf(red) : sinf(red));
+                if (a.modes) {
+                    for (int d = 0; d < a.ndim; d++)
+                        phi *= table[(size_t)(a.moff[d] + tix[(k0 + k) * a.ndim + d]) * KL_TILE_M + t];
+                } else {
+                    for (int d = 0; d < a.ndim; d++) {
+                        const KLTCTerm q = a.terms[(size_t)(k0 + k) * a.ndim + d];
+                        const double arg = q.w * xa[d];
+                        const float red = (float)(arg - rint(arg * inv_two_pi) * two_pi);
+                        phi *= q.alpha * (q.use_cos ? cosf(red) : sinf(red));
+                    }
                 }
             }
             const float hi = tf32_hi(phi);
@@ -281,6 +318,16 @@ extern "C" size_t sphk_kl_tc_smem_bytes(int R)
     return (size_t)2 * KL_TILE_M * KL_K_TILE * 4 + (size_t)2 * R * KL_K_TILE * 4 + 16;
 }
 
+// shared memory of the separable form: the above, the factor table of
+// nmodes factors per particle and the K x ndim factor indices
+static size_t kl_tc_smem_table(int R, int nmodes, int K, int ndim)
+{
+    return sphk_kl_tc_smem_bytes(R) + (size_t)nmodes * KL_TILE_M * 4 + ((size_t)K * ndim * 2 + 15) / 16 * 16;
+}
+
+// the largest dynamic shared memory a CTA of this kernel may take
+#define KL_SMEM_MAX (227 * 1024)
+
 extern "C" size_t sphk_kl_tc_term_bytes(void) { return sizeof(KLTCTerm); }
 
 // R: multiple of 16 in [16, 256]; K: multiple of 8.  d_terms K x ndim
@@ -289,7 +336,8 @@ extern "C" int sphk_kl_synthesize(int n, int ndim, int K, int R, int no, int typ
                                   double mean_value, double sd_value, double coe_depth, double soil_max,
                                   double water_max, const double* d_xh, const int* d_type, const void* d_terms,
                                   const double* d_sqrt_eig, const double* d_xi, float* c_hi, float* c_lo,
-                                  float* d_out, int* d_err, cudaStream_t st)
+                                  float* d_out, int* d_err, cudaStream_t st, const void* d_modes,
+                                  const int* nmode, const unsigned short* d_tidx)
 {
     if (R < 16 || R > 256 || R % 16 != 0 || K < 8 || K % 8 != 0) return 1;
     k_kl_coef<<<(K * R + 255) / 256, 256, 0, st>>>(K, R, d_sqrt_eig, d_xi, c_hi, c_lo);
@@ -302,7 +350,23 @@ extern "C" int sphk_kl_synthesize(int n, int ndim, int K, int R, int no, int typ
     a.out = d_out; a.err = d_err;
     a.budget = 2000000000ll;     // SM clocks, about one second
     a.probe = 0;
-    const size_t smem = sphk_kl_tc_smem_bytes(R);
+    a.modes = nullptr;
+    a.tidx = nullptr;
+    a.nmode[0] = a.nmode[1] = a.nmode[2] = 0;
+    a.moff[0] = a.moff[1] = a.moff[2] = 0;
+    size_t smem = sphk_kl_tc_smem_bytes(R);
+    if (d_modes && d_tidx && nmode) {
+        const int total = nmode[0] + nmode[1] + nmode[2];
+        const size_t with = kl_tc_smem_table(R, total, K, ndim);
+        if (with <= KL_SMEM_MAX) {       // else the factors are evaluated per term
+            a.modes = (const KLTCTerm*)d_modes;
+            a.tidx = d_tidx;
+            for (int d = 0; d < 3; d++) a.nmode[d] = nmode[d];
+            a.moff[1] = nmode[0];
+            a.moff[2] = nmode[0] + nmode[1];
+            smem = with;
+        }
+    }
     if (cudaFuncSetAttribute(k_kl_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return 1;
     k_kl_synth<<<(n + KL_TILE_M - 1) / KL_TILE_M, KL_TILE_M, smem, st>>>(a);
@@ -316,6 +380,8 @@ extern "C" int sphk_kl_wait_probe(long long budget, int* d_err, cudaStream_t st)
 {
     KLTCArgs a = {};
     a.n = 0; a.ndim = 2; a.K = 8; a.R = 16;
+    a.modes = nullptr;
+    a.tidx = nullptr;
     a.err = d_err;
     a.budget = budget;
     a.probe = 1;
