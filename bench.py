@@ -310,7 +310,7 @@ def bulk_form(st, args, device, ref_fields, moving):
     eng.load_state(st.fields, st.fluid, st.soil)
     eng.set_precision(sphgpu.PREC_FP32_BULK)
     if not args.no_autotune:
-        eng.autotune(steps=1)
+        eng.autotune(steps=2)
     eng.step(args.warmup)
     eng.synchronize()
     eng.step(args.steps)
@@ -405,7 +405,7 @@ def batched_slopes(args, device: int, count: int = 256, dx: float = 0.05, steps_
         if form == "fp32_bulk":
             eng.set_precision(sphgpu.PREC_FP32_BULK)
         if not args.no_autotune:
-            eng.autotune(steps=1)
+            eng.autotune(steps=2)
         eng.step(args.warmup)
         eng.synchronize()
         eng.step(args.steps)
@@ -445,8 +445,8 @@ def engine_arm(args, world, rank, local):
     tune = None
     if not args.no_autotune:
         # the project's autotuner: threads per block of each neighbour pass,
-        # timed over steps of the run (4 candidates x 1 step)
-        table = eng.autotune(steps=1)
+        # timed over steps of the run (4 candidates x 2 steps)
+        table = eng.autotune(steps=2)
         tune = {"passes": list(sphgpu.Engine.TUNE_PASSES), "threads_per_block": [int(v) for v in eng.launch()],
                 "ms_per_step_by_candidate": {str(b): [round(float(x), 4) for x in table[a]]
                                              for a, b in enumerate((32, 64, 96, 128))}}

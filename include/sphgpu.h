@@ -349,7 +349,8 @@ long   sphgpu_last_step_launches(const sphgpu_ctx* ctx);
  * sphgpu_set_launch / sphgpu_get_launch set and read those sizes;
  * sphgpu_autotune runs `steps` steps of the run with each of 32, 64, 96 and
  * 128 threads per block, times every pass with CUDA events, and keeps for
- * each pass the fastest (ties keep 128).  The steps it runs are steps of the
+ * each pass the fastest, a shape other than 128 only when it is more than 3%
+ * faster (the spread of the timings).  The steps it runs are steps of the
  * run: a launch shape changes no result, bit for bit.  With cache_path the
  * choice is kept in that text file under a key of the GPU model and the
  * run's shape (dimension, particle count, wall, drag and contact types,

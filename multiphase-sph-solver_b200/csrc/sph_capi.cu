@@ -1710,9 +1710,11 @@ int sphgpu_autotune(sphgpu_ctx* c, int steps, const char* cache_path, double* ta
     }
     int best[TP_COUNT];
     for (int q = 0; q < TP_COUNT; q++) {
-        int b = 3;                          // ties keep the default of 128
-        for (int a = 0; a < 4; a++)
-            if (t[a][q] < t[b][q]) b = a;
+        // another shape replaces the default of 128 only when it is faster by
+        // more than the step-to-step spread of the timings (3%)
+        int b = 3;
+        for (int a = 0; a < 3; a++)
+            if (t[a][q] < 0.97 * t[3][q] && t[a][q] < t[b][q]) b = a;
         best[q] = cand[b];
     }
     set_tb(c, best);

@@ -1,6 +1,7 @@
 """Launch shapes and the autotuner (sphgpu_set_launch / sphgpu_autotune): the
 threads per block of the neighbour passes change no result, bit for bit, and
-the autotuner keeps, per pass, the fastest of the shapes it timed, and applies
+the autotuner keeps, per pass, the fastest of the shapes it timed (the default
+of 128 unless another is more than 3% faster), and applies
 a cached choice without timing again."""
 import os
 import tempfile
@@ -47,7 +48,9 @@ def test_autotune_picks_the_fastest_and_caches_it():
     cand = np.array([32, 64, 96, 128])
     assert (table > 0).all()
     for q in range(table.shape[1]):
-        assert table[list(cand).index(chosen[q]), q] == table[:, q].min()
+        best = int(np.argmin(table[:3, q]))
+        want = cand[best] if table[best, q] < 0.97 * table[3, q] else 128
+        assert chosen[q] == want, q
     print("autotune ms per pass (rows 32/64/96/128):\n", np.round(table, 4), "\nchosen", chosen)
     assert os.path.exists(cache)
     eng.close()
