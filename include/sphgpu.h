@@ -329,6 +329,23 @@ int sphgpu_get_rain(sphgpu_ctx* ctx, sphgpu_rain* rain);
 int sphgpu_checkpoint_save(sphgpu_ctx* ctx, const char* path);
 int sphgpu_checkpoint_load(sphgpu_ctx* ctx, const char* path);
 
+/*
+ * Result files, written while the steps go on (the reference writes them on
+ * the host between steps, clOutput_Fun::output_total, CPP_14-2-output.cpp:
+ * 15-136).  sphgpu_output_total takes a snapshot of the state after the last
+ * completed step l on the step stream (the next step starts after it), copies
+ * it to pinned host memory on a stream of its own and writes
+ * dir/data-<l, 10 digits>.odb from a host thread, in output_total's format
+ * byte for byte (rows formatted on several threads), while later steps run.
+ * Two files may be in flight; a third call waits for the older.
+ * sphgpu_output_wait waits for every file and returns the first error of
+ * their writing (0 if none).  The snapshot memory (two buffers of 49 doubles
+ * per particle on the device and in pinned host memory) is allocated at the
+ * first call.
+ */
+int sphgpu_output_total(sphgpu_ctx* ctx, const char* dir);
+int sphgpu_output_wait(sphgpu_ctx* ctx);
+
 /* Block until the context's stream is idle; returns the sticky error, if any. */
 int sphgpu_synchronize(sphgpu_ctx* ctx);
 

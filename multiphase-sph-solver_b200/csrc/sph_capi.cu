@@ -148,6 +148,15 @@ struct sphgpu_ctx {
     int part_done = 0;     // parts of step l run through the method entries: 1 parttocell, 2 partisearching
     sphgpu_rain rain = {};            // the rainfall record (flr 1), nrain as last set
     bool rain_set = false;
+    // the output writer: two slots of device staging, pinned host copy,
+    // completion event and writer thread
+    double* out_dev[2] = {nullptr, nullptr};
+    double* out_host[2] = {nullptr, nullptr};
+    cudaEvent_t out_ev[2] = {nullptr, nullptr};
+    cudaStream_t out_st = nullptr;
+    std::thread out_th[2];
+    int out_next = 0;
+    int out_err = 0;
     std::vector<InstGrid> h_inst;     // batched context: the instance table (empty: one system)
     InstGrid* d_inst = nullptr;
 };
@@ -635,7 +644,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.nbm, 10 * (size_t)N);
     r |= dalloc(c, &s.nbw, 4 * (size_t)SPH_NB_CAP * N);
     r |= dalloc(c, &s.err, 1); r |= dalloc(c, &s.step, 1);
-    r |= dalloc(c, &s.dtv, 1); r |= dalloc(c, &s.dtmin, 1); r |= dalloc(c, &s.nrain, 1);
+    r |= dalloc(c, &s.dtv, 1); r |= dalloc(c, &s.dtmin, 1); r |= dalloc(c, &s.nrain, 1); r |= dalloc(c, &s.tsim, 1);
     if (r) return fail(SPHGPU_E_CUDA);
     // cell_info() constructor values (Class_NNPS.cpp:68-72): the range of the
     // last cell, which the reference never resets, starts from them
@@ -682,6 +691,13 @@ void sphgpu_destroy(sphgpu_ctx* c)
 {
     if (!c) return;
     cudaSetDevice(c->device);
+    for (int b = 0; b < 2; b++)
+        if (c->out_th[b].joinable()) c->out_th[b].join();
+    for (int b = 0; b < 2; b++) {
+        if (c->out_host[b]) cudaFreeHost(c->out_host[b]);
+        if (c->out_ev[b]) cudaEventDestroy(c->out_ev[b]);
+    }
+    if (c->out_st) cudaStreamDestroy(c->out_st);
     if (c->st) cudaStreamSynchronize(c->st);
     invalidate_graphs(c);
     for (void* p : c->allocs) cudaFree(p);
@@ -1379,6 +1395,7 @@ std::vector<CkExtra> ck_extras(sphgpu_ctx* c)
     add("nrain", s.nrain, 4);
     add("dtv", s.dtv, 8);
     add("dtmin", s.dtmin, 8);
+    add("tsim", s.tsim, 8);
     return v;
 }
 
@@ -1486,6 +1503,144 @@ int sphgpu_checkpoint_load(sphgpu_ctx* c, const char* path)
     }
     std::fclose(f);
     if (!rc && h.regu && !c->regu) { c->regu = true; invalidate_graphs(c); }
+    return rc;
+}
+
+namespace {
+
+constexpr int kOutCols = 49;    // output_total's 47 values, type and matype, per particle
+
+// one row of output_total (CPP_14-2-output.cpp:78-131) per particle, as
+// doubles in its column order: xp, ux, |ux|, then ax and vx for moving
+// particles or interfss and interf for walls, pre, prea, prew, sig, strep,
+// eps, adps, vsig, veps, meps, divq, divr, satu, suct, interfss, type, matype
+__global__ void k_out_pack(Dev d, double* out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, N = d.p.N;
+    if (i == 0) out[(size_t)N * kOutCols] = *d.s.tsim;
+    if (i >= N) return;
+    const DevState& s = d.s;
+    double* o = out + (size_t)i * kOutCols;
+    const Pos p = load_pos(s.xh, i);
+    o[0] = p.x; o[1] = p.y; o[2] = p.z;
+    const double u0 = s.ux[i], u1 = s.ux[N + i], u2 = s.ux[2 * N + i];
+    o[3] = u0; o[4] = u1; o[5] = u2;
+    o[6] = sqrt(u0 * u0 + u1 * u1 + u2 * u2);
+    const int t = s.type[i];
+    for (int k = 0; k < 3; k++) {
+        o[7 + k] = (t != 0) ? s.ax[k * N + i] : s.interfss[k * N + i];
+        o[10 + k] = (t != 0) ? s.vx[k * N + i] : s.interf[k * N + i];
+    }
+    o[13] = s.pre[i]; o[14] = s.prea[i]; o[15] = s.prew[i];
+    for (int k = 0; k < 6; k++) o[16 + k] = s.sig[k * N + i];
+    for (int k = 0; k < 3; k++) o[22 + k] = s.strep[k * N + i];
+    for (int k = 0; k < 6; k++) o[25 + k] = s.eps[k * N + i];
+    for (int k = 0; k < 6; k++) o[31 + k] = s.adps[k * N + i];
+    o[37] = s.vsig[i]; o[38] = s.veps[i]; o[39] = s.meps[i]; o[40] = s.divq[i]; o[41] = s.divr[i];
+    o[42] = s.satu[i]; o[43] = s.suct[i];
+    for (int k = 0; k < 3; k++) o[44 + k] = s.interfss[k * N + i];
+    o[47] = (double)t;
+    o[48] = (double)s.matype[i];
+}
+
+// output_total's file, written from the packed rows (its name, header and
+// row format are the reference's, so the two files compare byte for byte)
+int write_odb(const char* dir, int l, const double* rows, int n)
+{
+    char path[1024];
+    std::snprintf(path, sizeof(path), "%s/data-%010d.odb", dir, l);
+    FILE* f = std::fopen(path, "w");
+    if (!f) return SPHGPU_E_ARG;
+    static const char* kStars =
+        "*************************************************************************************************\n";
+    std::fputs(kStars, f);
+    std::fprintf(f, "%10d %14.6e\n", l, rows[(size_t)n * kOutCols]);
+    // rows formatted in parallel, in chunks, and written in order
+    const int chunk = 65536;
+    const int nchunk = (n + chunk - 1) / chunk;
+    std::vector<std::string> text(nchunk);
+    par_for((size_t)nchunk, [&](size_t a, size_t b) {
+        char line[1024];
+        for (size_t q = a; q < b; q++) {
+            std::string& out = text[q];
+            const int i0 = (int)q * chunk, i1 = std::min(n, i0 + chunk);
+            out.reserve((size_t)(i1 - i0) * 700);
+            for (int i = i0; i < i1; i++) {
+                const double* o = rows + (size_t)i * kOutCols;
+                const int len = std::snprintf(line, sizeof(line),
+                    "%5d %14.6e %14.6e %14.6e %14.6e %14.6e %14.6e "
+                    "%14.6e %14.6e %14.6e %14.6e %14.6e %14.6e %14.6e "
+                    "%14.6e %14.6e %14.6e %14.6e %14.6e %14.6e "
+                    "%14.6e %14.6e %14.6e %14.6e %14.6e %14.6e "
+                    "%14.6e %14.6e %14.6e %14.6e %14.6e %14.6e "
+                    "%14.6e %14.6e %14.6e %14.6e %14.6e %14.6e "
+                    "%14.6e %14.6e %14.6e %14.6e  %14.6e %14.6e "
+                    "%14.6e %14.6e %14.6e "
+                    "%14.6e %4d %4d\n",
+                    i + 1, o[0], o[1], o[2], o[3], o[4], o[5], o[6], o[7], o[8], o[9], o[10], o[11], o[12],
+                    o[13], o[14], o[15], o[16], o[17], o[18], o[19], o[20], o[21], o[22], o[23], o[24],
+                    o[25], o[26], o[27], o[28], o[29], o[30], o[31], o[32], o[33], o[34], o[35], o[36],
+                    o[37], o[38], o[39], o[40], o[41], o[42], o[43], o[44], o[45], o[46], (int)o[47],
+                    (int)o[48]);
+                out.append(line, (size_t)len);
+            }
+        }
+    });
+    bool ok = true;
+    for (const std::string& t : text) ok = ok && std::fwrite(t.data(), 1, t.size(), f) == t.size();
+    std::fputs(kStars, f);
+    if (std::fclose(f) != 0) ok = false;
+    return ok ? 0 : SPHGPU_E_ARG;
+}
+
+}  // namespace
+
+int sphgpu_output_total(sphgpu_ctx* c, const char* dir)
+{
+    if (!c || !dir || std::strlen(dir) > 900) return SPHGPU_E_ARG;
+    if (c->sticky) return c->sticky;
+    if (c->part_done) return SPHGPU_E_STATE;          // between steps only
+    cudaSetDevice(c->device);
+    const int slot = c->out_next;
+    if (c->out_th[slot].joinable()) c->out_th[slot].join();      // the slot's previous file
+    const size_t bytes = sizeof(double) * ((size_t)c->N * kOutCols + 1);
+    if (!c->out_dev[slot]) {
+        if (!c->out_st) CK(cudaStreamCreateWithFlags(&c->out_st, cudaStreamNonBlocking));
+        int r = dalloc(c, &c->out_dev[slot], (size_t)c->N * kOutCols + 1);
+        if (r) return r;
+        CK(cudaMallocHost(&c->out_host[slot], bytes));
+        CK(cudaEventCreateWithFlags(&c->out_ev[slot], cudaEventDisableTiming));
+    }
+    // the snapshot on the step stream (the next step waits for it); the copy
+    // to the host on the writer's stream, overlapping the next steps
+    k_out_pack<<<(c->N + 255) / 256, 256, 0, c->st>>>(c->d[c->parity], c->out_dev[slot]);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->out_ev[slot], c->st));
+    CK(cudaStreamWaitEvent(c->out_st, c->out_ev[slot], 0));
+    CK(cudaMemcpyAsync(c->out_host[slot], c->out_dev[slot], bytes, cudaMemcpyDeviceToHost, c->out_st));
+    CK(cudaEventRecord(c->out_ev[slot], c->out_st));
+    const int l = c->l_host - 1, n = c->N, dev = c->device;
+    std::string where(dir);
+    double* host = c->out_host[slot];
+    cudaEvent_t ev = c->out_ev[slot];
+    int* err = &c->out_err;
+    c->out_th[slot] = std::thread([=]() {
+        cudaSetDevice(dev);
+        int rc = (cudaEventSynchronize(ev) == cudaSuccess) ? 0 : SPHGPU_E_CUDA;
+        if (!rc) rc = write_odb(where.c_str(), l, host, n);
+        if (rc && *err == 0) *err = rc;
+    });
+    c->out_next ^= 1;
+    return 0;
+}
+
+int sphgpu_output_wait(sphgpu_ctx* c)
+{
+    if (!c) return SPHGPU_E_ARG;
+    for (int b = 0; b < 2; b++)
+        if (c->out_th[b].joinable()) c->out_th[b].join();
+    const int rc = c->out_err;
+    c->out_err = 0;
     return rc;
 }
 

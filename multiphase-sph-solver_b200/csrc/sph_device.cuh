@@ -188,6 +188,7 @@ struct DevState {
     const InstGrid *inst;      // batched context: the instance table (ninst)
     int *pinst;                // batched context: each particle's instance
     int *nrain;                // rain particles still waiting (Para_Rain::nrain)
+    double *tsim;              // Para_Pro::t, the simulated time after the last completed step
     double *dtv;               // dt of the step being run (cfl_on)
     unsigned long long *dtmin; // running minimum of the per-particle limits (bits of a positive double)
 };

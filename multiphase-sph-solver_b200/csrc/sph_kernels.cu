@@ -2556,6 +2556,7 @@ __global__ void k_step_done(Dev d)
 {
     if (threadIdx.x == 0 && blockIdx.x == 0 && *d.s.err == 0) {
         *d.s.step += 1;
+        *d.s.tsim = *d.s.tsim + step_dt(d);     // t = t + dt (CPP_1-SPHLoops.cpp:485)
         if (d.p.cfl_on) {
             // the next step's dt: the reduced limit, capped at the input dt;
             // the running minimum starts again from +inf

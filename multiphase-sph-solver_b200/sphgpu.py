@@ -268,6 +268,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_set_launch.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
     lib.sphgpu_get_launch.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
     lib.sphgpu_autotune.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_void_p]
+    lib.sphgpu_output_total.argtypes = [C.c_void_p, C.c_char_p]
+    lib.sphgpu_output_wait.argtypes = [C.c_void_p]
     lib.sphgpu_checkpoint_save.argtypes = [C.c_void_p, C.c_char_p]
     lib.sphgpu_checkpoint_load.argtypes = [C.c_void_p, C.c_char_p]
     lib.sphgpu_get_rain.argtypes = [C.c_void_p, C.POINTER(Rain)]
@@ -435,6 +437,14 @@ class Engine:
         path = cache_path.encode() if cache_path else None
         self._check(self.lib.sphgpu_autotune(self.h, int(steps), path, _ptr(table)), "sphgpu_autotune")
         return table
+
+    def output_total(self, directory: str) -> None:
+        """Write directory/data-<l>.odb (the reference's output_total format)
+        for the last completed step, in the background."""
+        self._check(self.lib.sphgpu_output_total(self.h, directory.encode()), "sphgpu_output_total")
+
+    def output_wait(self) -> None:
+        self._check(self.lib.sphgpu_output_wait(self.h), "sphgpu_output_wait")
 
     def checkpoint_save(self, path: str) -> None:
         self._check(self.lib.sphgpu_checkpoint_save(self.h, path.encode()), "sphgpu_checkpoint_save")
