@@ -433,3 +433,88 @@ extern "C" int ref_kl_field(int ndim, int n, const double* xp, const int* type, 
     delete[] so;
     return err;
 }
+
+/*
+ * The reference's correlation-matrix random field (nonstationary_random_2D /
+ * _3D, CPP_17-3-Nonstationary-RF.cpp:76-849) for one field, with the cell
+ * normals injected: that translation unit is compiled without inlining
+ * (oracle/Makefile), so its calls of the time-seeded generate_SND
+ * (CPP_17-3:32-43) reach the definition below, which hands out zeta.
+ */
+namespace {
+const double* g_zeta = nullptr;
+int g_zeta_n = 0;
+}  // namespace
+
+void generate_SND(double* kexi, int n)
+{
+    for (int i = 0; i < n; i++) kexi[i] = (g_zeta && i < g_zeta_n) ? g_zeta[i] : 0.0 / 0.0;
+}
+
+extern "C" int ref_rf_cholesky(int ndim, int n, const double* xp, const int* type, double dr, int no, int dist_type,
+                               double mean_value, double sd_value, double coe_depth, const double* rl,
+                               double cell_ndx, int flag_auto, double beta, double beta_1, const double* nb_min,
+                               const double* nb_max, double soil_max, double water_max, const double* zeta,
+                               int nzeta, double* out)
+{
+    Particle* par = new Particle[n];
+    Para_Fluid* fl = new Para_Fluid[n];
+    Para_Soil* so = new Para_Soil[n];
+    const double nan = 0.0 / 0.0;
+    for (int i = 0; i < n; i++) {
+        for (int d = 0; d < 3; d++) par[i].xp[d] = xp[(size_t)i * 3 + d];
+        par[i].type = type[i];
+        fl[i].fai = fl[i].c = nan;
+        so[i].fai = so[i].c = so[i].cop = so[i].ds = nan;
+    }
+    Para_Pro pro;
+    pro.ndim = ndim;
+    pro.ntotal = n;
+    pro.dr = dr;
+    Flag_SpatialVariability fsv;
+    fsv.flag_fai = no == 0; fsv.flag_c = no == 1; fsv.flag_cop = no == 2; fsv.flag_ds = no == 3;
+    fsv.flag_faiw = no == 4; fsv.flag_cw = no == 5;
+    fsv.cell_ndx = cell_ndx;
+    fsv.flag_auto = flag_auto;
+    fsv.beta = beta;
+    fsv.beta_1 = beta_1;
+    Para_SpatialVariability psv[6];
+    psv[no].no = no;
+    psv[no].type = dist_type;
+    psv[no].mean_value = mean_value;
+    psv[no].sd_value = sd_value;
+    psv[no].coe_depth = coe_depth;
+    for (int d = 0; d < 3; d++) psv[no].rl_value[d] = rl[d];
+    Cell_Con cc;
+    cc.xmin_nb = nb_min[0]; cc.ymin_nb = nb_min[1]; cc.zmin_nb = nb_min[2];
+    cc.xmax_nb = nb_max[0]; cc.ymax_nb = nb_max[1]; cc.zmax_nb = nb_max[2];
+    for (int d = 0; d < 3; d++) { cc.soil_max[d] = soil_max; cc.water_max[d] = water_max; }
+    g_zeta = zeta;
+    g_zeta_n = nzeta;
+    // one thread: the Cholesky diagonal is an OpenMP reduction whose order
+    // depends on the team size (CPP_17-3:52-55); sequential here
+    const int threads = omp_get_max_threads();
+    omp_set_num_threads(1);
+    clFSpatialVariability_Fun f;
+    const int err = (ndim == 2) ? f.nonstationary_random_2D(par, fl, so, pro, fsv, psv, cc)
+                                : f.nonstationary_random_3D(par, fl, so, pro, fsv, psv, cc);
+    omp_set_num_threads(threads);
+    g_zeta = nullptr;
+    g_zeta_n = 0;
+    for (int i = 0; i < n; i++) {
+        double v = nan;
+        switch (no) {
+        case 0: v = so[i].fai; break;
+        case 1: v = so[i].c; break;
+        case 2: v = so[i].cop; break;
+        case 3: v = so[i].ds; break;
+        case 4: v = fl[i].fai; break;
+        case 5: v = fl[i].c; break;
+        }
+        out[i] = v;
+    }
+    delete[] par;
+    delete[] fl;
+    delete[] so;
+    return err;
+}

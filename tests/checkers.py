@@ -63,6 +63,7 @@ def oracle_lib():
         lib.orc_nnps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.orc_step.argtypes = [C.c_void_p, C.c_int]
         lib.orc_set_rain.argtypes = [C.c_void_p, C.c_void_p]
+        lib.orc_rf_cholesky.restype = C.c_int
         lib.orc_get_rain.argtypes = [C.c_void_p, C.c_void_p]
         _olib = lib
     return _olib
@@ -308,3 +309,65 @@ def kl_reference(ndim, xp, ptype, field, dom, xi):
             _ptr(xi), _ptr(out), _ptr(wi), _ptr(eig), _ptr(order))
     assert err == 0
     return out, wi, eig, order
+
+
+# --------------------------------------------------------------------------
+# correlation-matrix (Cholesky) random fields (CPP_17-3-Nonstationary-RF.cpp)
+
+class OrcRFSpec(C.Structure):
+    _fields_ = [("no", C.c_int), ("type", C.c_int), ("mean_value", C.c_double), ("sd_value", C.c_double),
+                ("coe_depth", C.c_double), ("rl", C.c_double * 3), ("cell_ndx", C.c_double),
+                ("flag_auto", C.c_int), ("beta", C.c_double), ("beta_1", C.c_double),
+                ("nb_min", C.c_double * 3), ("nb_max", C.c_double * 3), ("soil_max", C.c_double),
+                ("water_max", C.c_double)]
+
+
+def rf_spec(field: dict, dom: dict) -> OrcRFSpec:
+    s = OrcRFSpec()
+    s.no, s.type = int(field["no"]), int(field["type"])
+    s.mean_value, s.sd_value, s.coe_depth = field["mean"], field["sd"], field.get("coe_depth", 0.0)
+    for d in range(3):
+        s.rl[d] = field["rl"][d]
+        s.nb_min[d] = dom["nb_min"][d]
+        s.nb_max[d] = dom["nb_max"][d]
+    s.cell_ndx, s.flag_auto = field["cell_ndx"], int(field["flag_auto"])
+    s.beta, s.beta_1 = field.get("beta", 0.0), field.get("beta_1", 0.0)
+    s.soil_max, s.water_max = dom["soil_max"], dom["water_max"]
+    return s
+
+
+def rf_oracle(ndim, xp, ptype, dr, field, dom, zeta):
+    """The oracle's correlation-matrix field: (code, out, number of cells)."""
+    lib = oracle_lib()
+    n = len(ptype)
+    xp = np.ascontiguousarray(xp, dtype=np.float64).reshape(n, 3)
+    ptype = np.ascontiguousarray(ptype, dtype=np.int32)
+    zeta = np.ascontiguousarray(zeta, dtype=np.float64)
+    out = np.zeros(n)
+    ncell = C.c_int(0)
+    s = rf_spec(field, dom)
+    err = lib.orc_rf_cholesky(C.c_int(ndim), C.c_int(n), _ptr(xp), _ptr(ptype), C.c_double(dr), C.byref(s),
+                              _ptr(zeta), C.c_int(len(zeta)), _ptr(out), C.byref(ncell))
+    return err, out, ncell.value
+
+
+def rf_reference(ndim, xp, ptype, dr, field, dom, zeta):
+    """The reference's nonstationary_random_2D / _3D with the normals zeta."""
+    lib = reference_lib()
+    n = len(ptype)
+    xp = np.ascontiguousarray(xp, dtype=np.float64).reshape(n, 3)
+    ptype = np.ascontiguousarray(ptype, dtype=np.int32)
+    zeta = np.ascontiguousarray(zeta, dtype=np.float64)
+    out = np.zeros(n)
+    rl = np.ascontiguousarray(field["rl"], dtype=np.float64)
+    lo = np.ascontiguousarray(dom["nb_min"], dtype=np.float64)
+    hi = np.ascontiguousarray(dom["nb_max"], dtype=np.float64)
+    f = lib.ref_rf_cholesky
+    f.restype = C.c_int
+    err = f(C.c_int(ndim), C.c_int(n), _ptr(xp), _ptr(ptype), C.c_double(dr), C.c_int(int(field["no"])),
+            C.c_int(int(field["type"])), C.c_double(field["mean"]), C.c_double(field["sd"]),
+            C.c_double(field.get("coe_depth", 0.0)), _ptr(rl), C.c_double(field["cell_ndx"]),
+            C.c_int(int(field["flag_auto"])), C.c_double(field.get("beta", 0.0)), C.c_double(field.get("beta_1", 0.0)),
+            _ptr(lo), _ptr(hi), C.c_double(dom["soil_max"]), C.c_double(dom["water_max"]), _ptr(zeta),
+            C.c_int(len(zeta)), _ptr(out))
+    return err, out

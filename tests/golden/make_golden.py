@@ -323,6 +323,57 @@ KL_CASES = {
 }
 
 
+def _column_no_walls():
+    """The soil column's soil and water only (the 3-D generator puts every
+    particle into a cell, and the walls reach past the cells)."""
+    sc = scenes.soil_column_3d(dx=0.05, steps=100)
+    return scenes.keep(sc, sc.ptype != 0)
+
+
+# correlation-matrix (Cholesky) random fields, nonstationary_random_2D / _3D
+# (CPP_17-3-Nonstationary-RF.cpp) through the reference's own routine with
+# injected cell normals: name: (scene factory, field, seed of the normals)
+RF_CASES = {
+    "rf_slope_2d_cohesion_lognormal": (
+        lambda: scenes.slope_2d(H=5.0, dx=0.1),
+        {"no": 1, "type": 2, "mean": 10.0e3, "sd": 3.0e3, "rl": [10.0, 1.0, 0.0], "cell_ndx": 5.0, "flag_auto": 1},
+        11),
+    "rf_slope_2d_friction_normal_gauss": (
+        lambda: scenes.slope_2d(H=5.0, dx=0.1),
+        {"no": 0, "type": 1, "mean": 25.0, "sd": 2.5, "rl": [5.0, 2.0, 0.0], "coe_depth": 0.4, "cell_ndx": 4.0,
+         "flag_auto": 2}, 12),
+    "rf_slope_2d_cohesion_rotated": (
+        lambda: scenes.slope_2d(H=5.0, dx=0.1),
+        {"no": 1, "type": 1, "mean": 10.0e3, "sd": 2.0e3, "rl": [6.0, 2.0, 0.0], "cell_ndx": 5.0, "flag_auto": 3,
+         "beta": 10.0}, 13),
+    "rf_column_3d_friction_rotated": (
+        _column_no_walls,
+        {"no": 0, "type": 1, "mean": 30.0, "sd": 3.0, "rl": [0.5, 0.3, 0.2], "coe_depth": 2.0, "cell_ndx": 2.0,
+         "flag_auto": 3, "beta": 15.0, "beta_1": 30.0}, 14),
+    "rf_column_3d_fluid_cohesion_lognormal": (
+        _column_no_walls,
+        {"no": 5, "type": 2, "mean": 50.0, "sd": 10.0, "rl": [0.4, 0.4, 0.3], "coe_depth": 20.0, "cell_ndx": 2.0,
+         "flag_auto": 1}, 15),
+}
+
+
+def make_rf(name: str) -> str:
+    from checkers import rf_oracle, rf_reference
+    factory, field, seed = RF_CASES[name]
+    sc = factory()
+    dom = scenes.kl_domain(sc)
+    err, _, ncell = rf_oracle(sc.ndim, sc.xp, sc.ptype, sc.dr, field, dom, np.zeros(15000))
+    assert err == 0, err
+    zeta = np.random.default_rng(seed).standard_normal(ncell)
+    err, out = rf_reference(sc.ndim, sc.xp, sc.ptype, sc.dr, field, dom, zeta)
+    assert err == 0, err
+    fn = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(fn, ndim=sc.ndim, xp=sc.xp, type=sc.ptype, dr=sc.dr, zeta=zeta, out=out,
+                        nb_min=dom["nb_min"], nb_max=dom["nb_max"], soil_max=dom["soil_max"],
+                        water_max=dom["water_max"])
+    return fn
+
+
 def make_kl(name: str) -> str:
     factory, field, seed = KL_CASES[name]
     sc = factory()
@@ -341,6 +392,8 @@ def make_kl(name: str) -> str:
 def make(name: str) -> str:
     if name in KL_CASES:
         return make_kl(name)
+    if name in RF_CASES:
+        return make_rf(name)
     factory, steps = CASES[name]
     sc = factory()
     out = {}
@@ -378,7 +431,7 @@ if __name__ == "__main__":
     saved = os.dup(1)
     os.dup2(devnull, 1)   # the reference prints progress lines
     try:
-        files = [make(n) for n in (sys.argv[1:] or list(CASES) + list(KL_CASES))]
+        files = [make(n) for n in (sys.argv[1:] or list(CASES) + list(KL_CASES) + list(RF_CASES))]
     finally:
         os.dup2(saved, 1)
     for f in files:
