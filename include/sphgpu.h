@@ -444,6 +444,60 @@ int sphgpu_kl_generate_corr(sphgpu_ctx* ctx, const sphgpu_kl_domain* dom, const 
                             double coe_frict_cohesion, const double* u2, int K, double* out);
 
 /*
+ * Correlation-matrix random fields: the reference's
+ * clFSpatialVariability_Fun::nonstationary_random_2D / _3D (flspv 3,
+ * Class_spatial_variability.h:92-103, CPP_17-3-Nonstationary-RF.cpp:76-458,
+ * 460-849), nonstationary_correlated_random_2D / _3D (flspv 4,
+ * CPP_17-5-Nonstationary-Correlated-RF.cpp:87-406, 409-735) and
+ * random_variable_generate (flspv 5, CPP_17-5:738-863).
+ *
+ * The non-boundary box (sphgpu_kl_domain), widened by 10% per side, is cut
+ * into cells of cell_ndx particle spacings; the correlation matrix of the
+ * cell centres is factored (Cholesky, the diagonal's radicand floored at
+ * 1e-6), multiplied by one standard normal per cell, and every particle of a
+ * cell takes the cell's value (2-D: water and soil particles are placed in
+ * cells; 3-D: every particle).  sphgpu_rf_flags holds the
+ * Flag_SpatialVariability members the generators read
+ * (Class_spatial_variability.h:9-36).
+ *
+ * The reference draws the normals from a time-seeded generator
+ * (generate_SND, CPP_17-3:31-41); here the caller passes them:
+ * sphgpu_rf_cells gives the number of cells C, and zeta holds C values per
+ * field in the reference's cell order (x fastest, then y, then z).  The
+ * fields are written into the material records (sphgpu_set_materials must
+ * have been called) as sphgpu_kl_generate writes them; out, if non-NULL,
+ * receives nfields x ntotal values (NaN where a field writes none).
+ * Returns 0, 41 (no cells, or 15,000 or more), 42 (a cell holding more than
+ * 39 particles), SPHGPU_E_ARG (a particle outside the cells, where the
+ * reference would index past its cell array; or ncell is not C),
+ * SPHGPU_E_UNSUPPORTED for a batched context, or an engine code.
+ */
+typedef struct sphgpu_rf_flags {
+    double cell_ndx;             /* cell edge in particle spacings */
+    int    flag_auto;            /* 1 exponential, 2 Gaussian, 3 rotated exponential */
+    double beta, beta_1;         /* rotation angles (flag_auto 3), degrees */
+    double coe_frict_cohesion;   /* correlation of friction and cohesion (flspv 4 and 5) */
+} sphgpu_rf_flags;
+
+int sphgpu_rf_cells(sphgpu_ctx* ctx, const sphgpu_kl_domain* dom, const sphgpu_rf_flags* flags, int* ncell);
+/* flspv 3: fields in the caller's order, each with its own factor (as the
+ * reference, which factors again per field; consecutive fields of equal
+ * correlation lengths share one here) */
+int sphgpu_rf_generate(sphgpu_ctx* ctx, const sphgpu_kl_domain* dom, const sphgpu_kl_field* fields, int nfields,
+                       const sphgpu_rf_flags* flags, const double* zeta, int ncell, double* out);
+/* flspv 4: pair[0] the friction field (no 0 or 4), pair[1] the cohesion field
+ * (no 1 or 5) of one phase; u2 holds ncell x 2 normals (the reference's
+ * vec_zeta_1), correlated through the 2 x 2 factor of coe_frict_cohesion.
+ * Both members use the friction field's correlation lengths and distribution
+ * type; out receives 2 x ntotal values. */
+int sphgpu_rf_generate_corr(sphgpu_ctx* ctx, const sphgpu_kl_domain* dom, const sphgpu_kl_field pair[2],
+                            const sphgpu_rf_flags* flags, const double* u2, int ncell, double* out);
+/* flspv 5: one correlated pair of random variables for the whole phase from
+ * the two normals u2; out receives the friction and cohesion values. */
+int sphgpu_rv_generate_corr(sphgpu_ctx* ctx, const sphgpu_kl_field pair[2], double coe_frict_cohesion,
+                            const double u2[2], double out[2]);
+
+/*
  * K-L fields of a batched context: one field per instance, each over the
  * instance's own particles with its own domain doms[q] and its own standard
  * normals xi[q * K .. q * K + K - 1] (what sphgpu_kl_generate does for one

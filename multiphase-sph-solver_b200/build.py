@@ -18,7 +18,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsphgpu.so")
-SOURCES = ["sph_kernels.cu", "sph_capi.cu", "sph_noalloc.cu", "sph_kernels_bulk32.cu", "sph_kl.cu", "sph_kl_tc.cu"]
+SOURCES = ["sph_kernels.cu", "sph_capi.cu", "sph_noalloc.cu", "sph_kernels_bulk32.cu", "sph_kl.cu", "sph_kl_tc.cu",
+           "sph_rf.cu"]
 # per-source flags on top of NVCC_FLAGS
 SOURCE_FLAGS = {"sph_kernels_bulk32.cu": ["-fmad=true"]}
 HEADERS = ["sph_device.cuh", "sph_constitutive.cuh", os.path.join("..", "..", "include", "sphgpu.h")]

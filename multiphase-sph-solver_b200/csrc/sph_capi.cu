@@ -47,6 +47,11 @@ extern "C" int sphk_kl_synthesize(int n, int ndim, int K, int R, int no, int typ
                                   const double* d_sqrt_eig, const double* d_xi, float* c_hi, float* c_lo,
                                   float* d_out, int* d_err, cudaStream_t st, const void* d_modes,
                                   const int* nmode, const unsigned short* d_tidx);
+extern "C" int sphk_rf_cells(const int* ip, const double* dp, const double* d_xh, const int* d_type, int* d_cell,
+                             int* d_count, int* d_err, cudaStream_t st);
+extern "C" int sphk_rf_factor(const int* ip, const double* dp, double* d_C, cudaStream_t st);
+extern "C" int sphk_rf_assign(const int* ip, const double* dp, const double* d_L, const double* d_zeta, double* d_E,
+                              const int* d_cell, const int* d_type, double* d_out, cudaStream_t st);
 
 namespace {
 
@@ -2183,6 +2188,264 @@ int sphgpu_kl_generate_corr(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sp
     }
     const double* xis[2] = {z0.data(), z1.data()};
     return kl_run(c, dom, pair, 2, xis, K, out);
+}
+
+// ---------------------------------------------------------------------------
+// correlation-matrix random fields (flspv 3, 4 and 5)
+
+namespace {
+
+// the cells: the non-boundary box widened by 10% per side, cells of
+// cell_ndx spacings, their base offset as CPP_17-3:100-132 (2-D) and
+// :482-517 (3-D) compute it.  41: no cells, or 15,000 or more.
+struct RFGeom { int nc[3]; double base[3]; double cdx; int total; };
+
+int rf_geom(int nd, double dr, const sphgpu_kl_domain* dom, double cell_ndx, RFGeom& g)
+{
+    const double lo[3] = {dom->xmin_nb, dom->ymin_nb, dom->zmin_nb};
+    const double hi[3] = {dom->xmax_nb, dom->ymax_nb, dom->zmax_nb};
+    double xmin[3] = {0, 0, 0}, xmax[3] = {0, 0, 0};
+    g.cdx = cell_ndx * dr;
+    g.total = 0;
+    for (int d = 0; d < 3; d++) { g.nc[d] = 1; g.base[d] = 0.0; }
+    for (int d = 0; d < nd; d++) {
+        xmin[d] = lo[d] - 0.1 * (hi[d] - lo[d]);
+        xmax[d] = hi[d] + 0.1 * (hi[d] - lo[d]);
+        const double q = (xmax[d] - xmin[d]) / g.cdx;
+        if (!(q >= 0.0 && q < 15000.0)) return 41;      // also a zero, negative or NaN cell edge
+        g.nc[d] = (int)q + 1;
+    }
+    const long long total = (long long)g.nc[0] * g.nc[1] * g.nc[2];
+    if (!(total > 0 && total < 15000)) return 41;
+    g.total = (int)total;
+    for (int d = 0; d < nd; d++) g.base[d] = -(g.nc[d] * g.cdx - (xmax[d] - xmin[d])) / 2.0 + 0.01 * dr + xmin[d];
+    return 0;
+}
+
+void rf_pack(const sphgpu_ctx* c, const RFGeom& g, const sphgpu_kl_field& f, const sphgpu_rf_flags& fl,
+             int depth_axis, int log_exp, int ip[10], double dp[15])
+{
+    const int nd = c->P.ndim;
+    ip[0] = nd; ip[1] = c->N; ip[2] = f.no; ip[3] = f.type; ip[4] = fl.flag_auto;
+    for (int d = 0; d < 3; d++) ip[5 + d] = g.nc[d];
+    ip[8] = depth_axis; ip[9] = log_exp;
+    const double pi = 3.141592653;                       // Header_Parameters.h:10
+    for (int d = 0; d < 3; d++) { dp[d] = g.base[d]; dp[3 + d] = f.rl_value[d]; }
+    dp[6] = g.cdx; dp[7] = c->P.dr;
+    dp[8] = f.mean_value; dp[9] = f.sd_value; dp[10] = f.coe_depth;
+    dp[11] = fl.beta * pi / 180.0; dp[12] = fl.beta_1 * pi / 180.0;
+    dp[13] = 0.0; dp[14] = 0.0;
+}
+
+// The device side of one call: cells once, then for every field its factor
+// (re-used while the correlation lengths stay the same), E = L zeta and the
+// particles' values.  zetas[q] holds the normals of field q (total values);
+// out receives nfields x N values.
+int rf_run(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_kl_field* fields, int nfields,
+           const sphgpu_rf_flags* fl, const double* const* zetas, const int* depth_axis, int log_exp, double* out)
+{
+    cudaSetDevice(c->device);
+    const int nd = c->P.ndim, N = c->N;
+    RFGeom g;
+    int rc = rf_geom(nd, c->P.dr, dom, fl->cell_ndx, g);
+    if (rc) return rc;
+    const double soil_max = dom->soil_max[nd == 2 ? 1 : 2], water_max = dom->water_max[nd == 2 ? 1 : 2];
+    const size_t T = (size_t)g.total;
+    const size_t off_count = 256 * ((4 * (size_t)N + 255) / 256);
+    const size_t off_err = off_count + 256 * ((4 * T + 255) / 256);
+    const size_t off_zeta = off_err + 256;
+    const size_t off_E = off_zeta + 256 * ((8 * T + 255) / 256);
+    const size_t off_out = off_E + 256 * ((8 * T + 255) / 256);
+    const size_t off_C = off_out + 256 * ((8 * (size_t)N + 255) / 256);
+    void* buf = nullptr;
+    CK(cudaMalloc(&buf, off_C + 8 * T * T));
+    char* b = (char*)buf;
+    int* d_cell = (int*)b;
+    int* d_count = (int*)(b + off_count);
+    int* d_err = (int*)(b + off_err);
+    double* d_zeta = (double*)(b + off_zeta);
+    double* d_E = (double*)(b + off_E);
+    double* d_out = (double*)(b + off_out);
+    double* d_C = (double*)(b + off_C);
+    const DevState& s = c->d[c->parity].s;
+    int ip[10];
+    double dp[15];
+    do {
+        rf_pack(c, g, fields[0], *fl, nd - 1, log_exp, ip, dp);
+        int herr[2] = {0, 0};
+        if (cuda_fail(c, cudaMemsetAsync(d_count, 0, off_zeta - off_count, c->st), "cudaMemsetAsync") ||
+            sphk_rf_cells(ip, dp, s.xh, s.type, d_cell, d_count, d_err, c->st) ||
+            cuda_fail(c, cudaMemcpyAsync(herr, d_err, sizeof(herr), cudaMemcpyDeviceToHost, c->st), "cudaMemcpyAsync") ||
+            cuda_fail(c, cudaStreamSynchronize(c->st), "cudaStreamSynchronize")) { rc = SPHGPU_E_CUDA; break; }
+        // a particle outside the cells, where the reference would index past
+        // its cell array; else a cell over its 39 places (error 42)
+        if (herr[0]) { rc = SPHGPU_E_ARG; break; }
+        if (herr[1]) { rc = 42; break; }
+        const sphgpu_kl_field* factored = nullptr;
+        for (int q = 0; q < nfields && !rc; q++) {
+            const sphgpu_kl_field& f = fields[q];
+            rf_pack(c, g, f, *fl, depth_axis[q], log_exp, ip, dp);
+            dp[13] = soil_max; dp[14] = water_max;
+            if (!factored || std::memcmp(factored->rl_value, f.rl_value, sizeof(f.rl_value)) != 0) {
+                if (sphk_rf_factor(ip, dp, d_C, c->st)) { rc = SPHGPU_E_CUDA; break; }
+                factored = &f;
+            }
+            if (cuda_fail(c, cudaMemcpyAsync(d_zeta, zetas[q], 8 * T, cudaMemcpyHostToDevice, c->st),
+                          "cudaMemcpyAsync") ||
+                sphk_rf_assign(ip, dp, d_C, d_zeta, d_E, d_cell, s.type, d_out, c->st) ||
+                cuda_fail(c, cudaMemcpyAsync(out + (size_t)q * N, d_out, 8 * (size_t)N, cudaMemcpyDeviceToHost,
+                                             c->st), "cudaMemcpyAsync") ||
+                cuda_fail(c, cudaStreamSynchronize(c->st), "cudaStreamSynchronize")) { rc = SPHGPU_E_CUDA; break; }
+        }
+    } while (0);
+    cudaFree(buf);
+    return rc;
+}
+
+int rf_check(const sphgpu_ctx* c, const sphgpu_kl_field* fields, int nfields)
+{
+    if (c->h_type.empty() || (c->h_soil.empty() && c->h_fluid.empty())) return SPHGPU_E_STATE;
+    if (!c->h_inst.empty()) return SPHGPU_E_UNSUPPORTED;     // one system per context
+    for (int q = 0; q < nfields; q++) {
+        if (fields[q].no < 0 || fields[q].no > 5) return SPHGPU_E_ARG;
+        if (fields[q].no <= 3 && c->h_soil.empty()) return SPHGPU_E_STATE;
+        if (fields[q].no >= 4 && c->h_fluid.empty()) return SPHGPU_E_STATE;
+    }
+    return 0;
+}
+
+int rf_finish(sphgpu_ctx* c, const sphgpu_kl_field* fields, int nfields, const double* v)
+{
+    for (int q = 0; q < nfields; q++) kl_store(c, fields[q].no, v + (size_t)q * c->N, 0, c->N);
+    return sphgpu_set_materials(c, c->h_fluid.empty() ? nullptr : c->h_fluid.data(),
+                                c->h_soil.empty() ? nullptr : c->h_soil.data(), c->N);
+}
+
+// the correlation coefficient of the underlying normals and the 2 x 2 factor
+// (CPP_17-5:206-225): for lognormal fields from the fields' COVs
+void rf_pair_factor(const sphgpu_kl_field pair[2], double coe, double cm[4])
+{
+    double coefficient = coe;
+    if (pair[0].type == 2) {
+        const double m0 = pair[0].mean_value, s0 = pair[0].sd_value, m1 = pair[1].mean_value, s1 = pair[1].sd_value;
+        coefficient = std::log(1.0 + coe * (s0 / m0) * (s1 / m1));
+        coefficient = coefficient / std::sqrt(std::log(1.0 + s0 * s0 / m0 / m0) * std::log(1.0 + s1 * s1 / m1 / m1));
+    }
+    cm[0] = 1.0; cm[1] = coefficient; cm[2] = 0.0; cm[3] = std::sqrt(1.0 - coefficient * coefficient);
+}
+
+int rf_pair_check(const sphgpu_kl_field pair[2])
+{
+    // friction then cohesion of one phase
+    if (!((pair[0].no == 0 && pair[1].no == 1) || (pair[0].no == 4 && pair[1].no == 5))) return SPHGPU_E_ARG;
+    return 0;
+}
+
+}  // namespace
+
+int sphgpu_rf_cells(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_rf_flags* fl, int* ncell)
+{
+    if (!c || !dom || !fl || !ncell) return SPHGPU_E_ARG;
+    RFGeom g;
+    const int rc = rf_geom(c->P.ndim, c->P.dr, dom, fl->cell_ndx, g);
+    *ncell = g.total;
+    return rc;
+}
+
+int sphgpu_rf_generate(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_kl_field* fields, int nfields,
+                       const sphgpu_rf_flags* fl, const double* zeta, int ncell, double* out)
+{
+    if (!c || !dom || !fields || !fl || !zeta || nfields <= 0) return SPHGPU_E_ARG;
+    int rc = rf_check(c, fields, nfields);
+    if (rc) return rc;
+    RFGeom g;
+    if ((rc = rf_geom(c->P.ndim, c->P.dr, dom, fl->cell_ndx, g))) return rc;
+    if (ncell != g.total) return SPHGPU_E_ARG;
+    const int N = c->N;
+    std::vector<double> v((size_t)nfields * N);
+    std::vector<const double*> zetas(nfields);
+    std::vector<int> axis(nfields, c->P.ndim - 1);
+    for (int q = 0; q < nfields; q++) zetas[q] = zeta + (size_t)q * ncell;
+    rc = rf_run(c, dom, fields, nfields, fl, zetas.data(), axis.data(), 0, v.data());
+    if (rc) return rc;
+    if (out) std::memcpy(out, v.data(), sizeof(double) * v.size());
+    return rf_finish(c, fields, nfields, v.data());
+}
+
+int sphgpu_rf_generate_corr(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_kl_field pair[2],
+                            const sphgpu_rf_flags* fl, const double* u2, int ncell, double* out)
+{
+    if (!c || !dom || !pair || !fl || !u2) return SPHGPU_E_ARG;
+    int rc = rf_pair_check(pair);
+    if (rc || (rc = rf_check(c, pair, 2))) return rc;
+    RFGeom g;
+    if ((rc = rf_geom(c->P.ndim, c->P.dr, dom, fl->cell_ndx, g))) return rc;
+    if (ncell != g.total) return SPHGPU_E_ARG;
+    // zeta = u2 [1, coefficient; 0, sqrt(1 - coefficient^2)] (matrix_multi,
+    // CPP_17-5:21-33, 225-227)
+    double cm[4];
+    rf_pair_factor(pair, fl->coe_frict_cohesion, cm);
+    std::vector<double> z0(ncell), z1(ncell);
+    for (int i = 0; i < ncell; i++) {
+        double t0 = 0.0, t1 = 0.0;
+        t0 = t0 + u2[(size_t)i * 2 + 0] * cm[0];
+        t0 = t0 + u2[(size_t)i * 2 + 1] * cm[2];
+        t1 = t1 + u2[(size_t)i * 2 + 0] * cm[1];
+        t1 = t1 + u2[(size_t)i * 2 + 1] * cm[3];
+        z0[i] = t0;
+        z1[i] = t1;
+    }
+    // both members take the friction field's lengths and distribution type
+    // (psv_temp, CPP_17-5:177-186); the fluid members of the 3-D field read
+    // their depth on y (17-5:650-735)
+    sphgpu_kl_field two[2] = {pair[0], pair[1]};
+    for (int d = 0; d < 3; d++) two[1].rl_value[d] = pair[0].rl_value[d];
+    two[1].type = pair[0].type;
+    const int nd = c->P.ndim;
+    const int axis[2] = {(nd == 3 && pair[0].no == 4) ? 1 : nd - 1, (nd == 3 && pair[1].no == 5) ? 1 : nd - 1};
+    const double* zetas[2] = {z0.data(), z1.data()};
+    const int N = c->N;
+    std::vector<double> v(2 * (size_t)N);
+    rc = rf_run(c, dom, two, 2, fl, zetas, axis, 1, v.data());
+    if (rc) return rc;
+    if (out) std::memcpy(out, v.data(), sizeof(double) * v.size());
+    return rf_finish(c, pair, 2, v.data());
+}
+
+int sphgpu_rv_generate_corr(sphgpu_ctx* c, const sphgpu_kl_field pair[2], double coe_frict_cohesion,
+                            const double u2[2], double out[2])
+{
+    if (!c || !pair || !u2) return SPHGPU_E_ARG;
+    int rc = rf_pair_check(pair);
+    if (rc || (rc = rf_check(c, pair, 2))) return rc;
+    // the correlated pair [zeta_c, zeta_fai] (random_variable_generate,
+    // CPP_17-5:738-863): friction takes the second, cohesion the first
+    double cm[4];
+    rf_pair_factor(pair, coe_frict_cohesion, cm);
+    double t0 = 0.0, t1 = 0.0;
+    t0 = t0 + u2[0] * cm[0];
+    t0 = t0 + u2[1] * cm[2];
+    t1 = t1 + u2[0] * cm[1];
+    t1 = t1 + u2[1] * cm[3];
+    const double z[2] = {t1, t0};
+    double val[2];
+    const int dist = pair[0].type;
+    for (int k = 0; k < 2; k++) {
+        double mean = pair[k].mean_value, sd = pair[k].sd_value;
+        if (dist == 1) val[k] = mean + sd * z[k];
+        else if (dist == 2) {
+            sd = std::sqrt(std::log(1.0 + (sd / mean) * (sd / mean)));
+            mean = std::log(mean) - 0.5 * sd * sd;
+            val[k] = std::exp(mean + sd * z[k]);
+        } else val[k] = std::nan("");
+    }
+    if (out) { out[0] = val[0]; out[1] = val[1]; }
+    const int want = pair[0].no == 0 ? 2 : 1;
+    const int N = c->N;
+    std::vector<double> v(2 * (size_t)N, std::nan(""));
+    for (int i = 0; i < N; i++)
+        if (c->h_type[i] == want) { v[i] = val[0]; v[(size_t)N + i] = val[1]; }
+    return rf_finish(c, pair, 2, v.data());
 }
 
 

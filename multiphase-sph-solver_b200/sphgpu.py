@@ -191,7 +191,23 @@ def kl_domain(nb_min, nb_max, soil_max, water_max) -> KLDomain:
     return d
 
 
-ERRORS = {0: "ok", 3: "particle outside the cell grid", 5: "more than 99 neighbours",
+class RFFlags(C.Structure):
+    """sphgpu_rf_flags: the Flag_SpatialVariability members the correlation-
+    matrix generators read."""
+    _fields_ = [("cell_ndx", C.c_double), ("flag_auto", C.c_int), ("beta", C.c_double), ("beta_1", C.c_double),
+                ("coe_frict_cohesion", C.c_double)]
+
+
+def rf_flags(cell_ndx: float, flag_auto: int = 1, beta: float = 0.0, beta_1: float = 0.0,
+             coe_frict_cohesion: float = 0.0) -> RFFlags:
+    f = RFFlags()
+    f.cell_ndx, f.flag_auto, f.beta, f.beta_1 = float(cell_ndx), int(flag_auto), float(beta), float(beta_1)
+    f.coe_frict_cohesion = float(coe_frict_cohesion)
+    return f
+
+
+ERRORS = {0: "ok", 3: "particle outside the cell grid", 41: "no random-field cells, or 15,000 or more",
+          42: "a random-field cell holds more than 39 particles", 5: "more than 99 neighbours",
           100: "bad argument", 101: "CUDA error", 102: "no CUDA device", 103: "unsupported flags",
           104: "call order", 105: "tensor-core wait expired"}
 
@@ -249,6 +265,12 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_get_dt.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     lib.sphgpu_kl_generate.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_int, C.c_void_p,
                                        C.c_int, C.c_void_p]
+    lib.sphgpu_rf_cells.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(RFFlags), C.POINTER(C.c_int)]
+    lib.sphgpu_rf_generate.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_int,
+                                       C.POINTER(RFFlags), C.c_void_p, C.c_int, C.c_void_p]
+    lib.sphgpu_rf_generate_corr.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.POINTER(RFFlags),
+                                            C.c_void_p, C.c_int, C.c_void_p]
+    lib.sphgpu_rv_generate_corr.argtypes = [C.c_void_p, C.POINTER(KLField), C.c_double, C.c_void_p, C.c_void_p]
     lib.sphgpu_kl_synthesize.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_void_p, C.c_int,
                                          C.c_int, C.c_void_p, C.POINTER(C.c_double)]
     lib.sphgpu_kl_generate_corr.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_double,
@@ -388,6 +410,45 @@ class Engine:
         self._check(self.lib.sphgpu_kl_generate_corr(self.h, C.byref(domain), arr, float(coe), _ptr(u), int(K),
                                                      _ptr(out)), "sphgpu_kl_generate_corr")
         return out.reshape(2, self.n)
+
+    def rf_cells(self, domain: KLDomain, flags: RFFlags) -> int:
+        """The number of correlation-matrix cells (the normals each field takes)."""
+        n = C.c_int(0)
+        self._check(self.lib.sphgpu_rf_cells(self.h, C.byref(domain), C.byref(flags), C.byref(n)), "sphgpu_rf_cells")
+        return n.value
+
+    def rf_generate(self, domain: KLDomain, fields, flags: RFFlags, zeta) -> np.ndarray:
+        """nonstationary_random_2D / _3D (flspv 3) with the cell normals zeta
+        (len(fields) x cells); returns len(fields) x ntotal values (NaN where a
+        field writes none), which also become the particles' material values."""
+        fields = list(fields)
+        arr = (KLField * len(fields))(*fields)
+        z = np.ascontiguousarray(np.asarray(zeta, dtype=np.float64).reshape(len(fields), -1))
+        out = np.empty(len(fields) * self.n)
+        self._check(self.lib.sphgpu_rf_generate(self.h, C.byref(domain), arr, len(fields), C.byref(flags), _ptr(z),
+                                                z.shape[1], _ptr(out)), "sphgpu_rf_generate")
+        return out.reshape(len(fields), self.n)
+
+    def rf_generate_corr(self, domain: KLDomain, friction: KLField, cohesion: KLField, flags: RFFlags,
+                         u2) -> np.ndarray:
+        """nonstationary_correlated_random_2D / _3D (flspv 4) for one phase;
+        u2: cells x 2 normals; returns 2 x ntotal values."""
+        arr = (KLField * 2)(friction, cohesion)
+        u = np.ascontiguousarray(np.asarray(u2, dtype=np.float64).reshape(-1, 2))
+        out = np.empty(2 * self.n)
+        self._check(self.lib.sphgpu_rf_generate_corr(self.h, C.byref(domain), arr, C.byref(flags), _ptr(u), len(u),
+                                                     _ptr(out)), "sphgpu_rf_generate_corr")
+        return out.reshape(2, self.n)
+
+    def rv_generate_corr(self, friction: KLField, cohesion: KLField, coe: float, u2) -> np.ndarray:
+        """random_variable_generate (flspv 5): one correlated pair for the
+        phase from two normals; returns (friction, cohesion)."""
+        arr = (KLField * 2)(friction, cohesion)
+        u = np.ascontiguousarray(np.asarray(u2, dtype=np.float64).reshape(2))
+        out = np.empty(2)
+        self._check(self.lib.sphgpu_rv_generate_corr(self.h, arr, float(coe), _ptr(u), _ptr(out)),
+                    "sphgpu_rv_generate_corr")
+        return out
 
     def set_precision(self, mode: int) -> None:
         """PREC_FP64 (the reference's arithmetic) or PREC_FP32_BULK."""

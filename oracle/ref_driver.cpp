@@ -435,20 +435,30 @@ extern "C" int ref_kl_field(int ndim, int n, const double* xp, const int* type, 
 }
 
 /*
- * The reference's correlation-matrix random field (nonstationary_random_2D /
- * _3D, CPP_17-3-Nonstationary-RF.cpp:76-849) for one field, with the cell
- * normals injected: that translation unit is compiled without inlining
- * (oracle/Makefile), so its calls of the time-seeded generate_SND
- * (CPP_17-3:32-43) reach the definition below, which hands out zeta.
+ * The reference's correlation-matrix random fields (nonstationary_random_2D /
+ * _3D, CPP_17-3-Nonstationary-RF.cpp:76-849; nonstationary_correlated_random_
+ * 2D / _3D and random_variable_generate, CPP_17-5-Nonstationary-Correlated-
+ * RF.cpp:87-863) with the normals injected: both translation units are
+ * compiled without inlining for this library (oracle/Makefile), so their
+ * calls of the time-seeded generate_SND (CPP_17-3:32-43, which fills n
+ * values; CPP_17-5:35-46, which fills n pairs) reach the definition below,
+ * which hands out zeta (g_zeta_per values per requested unit).
  */
 namespace {
 const double* g_zeta = nullptr;
 int g_zeta_n = 0;
+int g_zeta_per = 1;
+int g_rf_threads = 1;
 }  // namespace
+
+/* The OpenMP team the random-field routines run with (1 by default: their
+ * Cholesky diagonal is an OpenMP reduction whose order follows the team size,
+ * CPP_17-3:52-55, so only one thread makes the result reproducible). */
+extern "C" void ref_rf_threads(int n) { g_rf_threads = n > 0 ? n : 1; }
 
 void generate_SND(double* kexi, int n)
 {
-    for (int i = 0; i < n; i++) kexi[i] = (g_zeta && i < g_zeta_n) ? g_zeta[i] : 0.0 / 0.0;
+    for (int i = 0; i < n * g_zeta_per; i++) kexi[i] = (g_zeta && i < g_zeta_n) ? g_zeta[i] : 0.0 / 0.0;
 }
 
 extern "C" int ref_rf_cholesky(int ndim, int n, const double* xp, const int* type, double dr, int no, int dist_type,
@@ -491,10 +501,8 @@ extern "C" int ref_rf_cholesky(int ndim, int n, const double* xp, const int* typ
     for (int d = 0; d < 3; d++) { cc.soil_max[d] = soil_max; cc.water_max[d] = water_max; }
     g_zeta = zeta;
     g_zeta_n = nzeta;
-    // one thread: the Cholesky diagonal is an OpenMP reduction whose order
-    // depends on the team size (CPP_17-3:52-55); sequential here
     const int threads = omp_get_max_threads();
-    omp_set_num_threads(1);
+    omp_set_num_threads(g_rf_threads);
     clFSpatialVariability_Fun f;
     const int err = (ndim == 2) ? f.nonstationary_random_2D(par, fl, so, pro, fsv, psv, cc)
                                 : f.nonstationary_random_3D(par, fl, so, pro, fsv, psv, cc);
@@ -516,5 +524,116 @@ extern "C" int ref_rf_cholesky(int ndim, int n, const double* xp, const int* typ
     delete[] par;
     delete[] fl;
     delete[] so;
+    return err;
+}
+
+namespace {
+
+struct RFRun {
+    Particle* par;
+    Para_Fluid* fl;
+    Para_Soil* so;
+    Para_Pro pro;
+    RFRun(int ndim, int n, const double* xp, const int* type, double dr)
+    {
+        par = new Particle[n];
+        fl = new Para_Fluid[n];
+        so = new Para_Soil[n];
+        const double nan = 0.0 / 0.0;
+        for (int i = 0; i < n; i++) {
+            for (int d = 0; d < 3; d++) par[i].xp[d] = xp ? xp[(size_t)i * 3 + d] : 0.0;
+            par[i].type = type[i];
+            fl[i].fai = fl[i].c = nan;
+            so[i].fai = so[i].c = so[i].cop = so[i].ds = nan;
+        }
+        pro.ndim = ndim;
+        pro.ntotal = n;
+        pro.dr = dr;
+    }
+    ~RFRun() { delete[] par; delete[] fl; delete[] so; }
+    // friction then cohesion of the pair's phase
+    void pair_out(int soil, double* out) const
+    {
+        for (int i = 0; i < pro.ntotal; i++) {
+            out[i] = soil ? so[i].fai : fl[i].fai;
+            out[(size_t)pro.ntotal + i] = soil ? so[i].c : fl[i].c;
+        }
+    }
+};
+
+void pair_setup(int no0, int dist_type, const double* mean, const double* sd, const double* coe_depth, const double* rl,
+                double coe, Flag_SpatialVariability& fsv, Para_SpatialVariability* psv)
+{
+    const int soil = no0 == 0;
+    fsv.flag_fai = soil; fsv.flag_c = soil; fsv.flag_cop = 0; fsv.flag_ds = 0;
+    fsv.flag_faiw = !soil; fsv.flag_cw = !soil;
+    fsv.coe_frict_cohesion = coe;
+    for (int k = 0; k < 2; k++) {
+        Para_SpatialVariability& p = psv[no0 + k];
+        p.no = no0 + k;
+        p.type = dist_type;
+        p.mean_value = mean[k];
+        p.sd_value = sd[k];
+        p.coe_depth = coe_depth[k];
+        for (int d = 0; d < 3; d++) p.rl_value[d] = rl[d];
+    }
+}
+
+}  // namespace
+
+/* flspv 4 with the pair normals u2 (cells x 2): friction and cohesion of the
+ * phase of no0 (0 soil, 4 fluid) into out (2 x n) */
+extern "C" int ref_rf_cholesky_corr(int ndim, int n, const double* xp, const int* type, double dr, int no0,
+                                    int dist_type, const double* mean, const double* sd, const double* coe_depth,
+                                    const double* rl, double cell_ndx, int flag_auto, double beta, double beta_1,
+                                    double coe, const double* nb_min, const double* nb_max, double soil_max,
+                                    double water_max, const double* u2, int nu, double* out)
+{
+    RFRun r(ndim, n, xp, type, dr);
+    Flag_SpatialVariability fsv;
+    Para_SpatialVariability psv[6];
+    pair_setup(no0, dist_type, mean, sd, coe_depth, rl, coe, fsv, psv);
+    fsv.cell_ndx = cell_ndx;
+    fsv.flag_auto = flag_auto;
+    fsv.beta = beta;
+    fsv.beta_1 = beta_1;
+    Cell_Con cc;
+    cc.xmin_nb = nb_min[0]; cc.ymin_nb = nb_min[1]; cc.zmin_nb = nb_min[2];
+    cc.xmax_nb = nb_max[0]; cc.ymax_nb = nb_max[1]; cc.zmax_nb = nb_max[2];
+    for (int d = 0; d < 3; d++) { cc.soil_max[d] = soil_max; cc.water_max[d] = water_max; }
+    g_zeta = u2;
+    g_zeta_n = 2 * nu;
+    g_zeta_per = 2;
+    const int threads = omp_get_max_threads();
+    omp_set_num_threads(g_rf_threads);
+    clFSpatialVariability_Fun f;
+    const int err = (ndim == 2) ? f.nonstationary_correlated_random_2D(r.par, r.fl, r.so, r.pro, fsv, psv, cc)
+                                : f.nonstationary_correlated_random_3D(r.par, r.fl, r.so, r.pro, fsv, psv, cc);
+    omp_set_num_threads(threads);
+    g_zeta = nullptr;
+    g_zeta_n = 0;
+    g_zeta_per = 1;
+    r.pair_out(no0 == 0, out);
+    return err;
+}
+
+/* flspv 5 with the two normals u2 */
+extern "C" int ref_rv_corr(int n, const int* type, int no0, int dist_type, const double* mean, const double* sd,
+                           double coe, const double* u2, double* out)
+{
+    RFRun r(2, n, nullptr, type, 1.0);
+    Flag_SpatialVariability fsv;
+    Para_SpatialVariability psv[6];
+    const double zero[2] = {0.0, 0.0}, rl[3] = {1.0, 1.0, 1.0};
+    pair_setup(no0, dist_type, mean, sd, zero, rl, coe, fsv, psv);
+    g_zeta = u2;
+    g_zeta_n = 2;
+    g_zeta_per = 2;
+    clFSpatialVariability_Fun f;
+    const int err = f.random_variable_generate(r.par, r.fl, r.so, r.pro, fsv, psv);
+    g_zeta = nullptr;
+    g_zeta_n = 0;
+    g_zeta_per = 1;
+    r.pair_out(no0 == 0, out);
     return err;
 }

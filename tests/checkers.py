@@ -351,6 +351,88 @@ def rf_oracle(ndim, xp, ptype, dr, field, dom, zeta):
     return err, out, ncell.value
 
 
+def rf_oracle_corr(ndim, xp, ptype, dr, pair, coe, dom, u2):
+    """The oracle's correlated field (flspv 4): (code, out 2 x n, cells).
+    pair: the friction and cohesion field dicts; the cell and kernel keys are
+    read from pair[0]."""
+    lib = oracle_lib()
+    n = len(ptype)
+    xp = np.ascontiguousarray(xp, dtype=np.float64).reshape(n, 3)
+    ptype = np.ascontiguousarray(ptype, dtype=np.int32)
+    u2 = np.ascontiguousarray(u2, dtype=np.float64).reshape(-1, 2)
+    out = np.zeros(2 * n)
+    ncell = C.c_int(0)
+    cells = {k: pair[0][k] for k in ("cell_ndx", "flag_auto", "beta", "beta_1") if k in pair[0]}
+    s0, s1 = rf_spec(pair[0], dom), rf_spec(dict(pair[1], **cells), dom)
+    lib.orc_rf_cholesky_corr.restype = C.c_int
+    err = lib.orc_rf_cholesky_corr(C.c_int(ndim), C.c_int(n), _ptr(xp), _ptr(ptype), C.c_double(dr), C.byref(s0),
+                                   C.byref(s1), C.c_double(coe), _ptr(u2), C.c_int(len(u2)), _ptr(out),
+                                   C.byref(ncell))
+    return err, out.reshape(2, n), ncell.value
+
+
+def rv_oracle(ptype, pair, coe, u2):
+    """The oracle's correlated random variables (flspv 5): out 2 x n."""
+    lib = oracle_lib()
+    n = len(ptype)
+    ptype = np.ascontiguousarray(ptype, dtype=np.int32)
+    u2 = np.ascontiguousarray(u2, dtype=np.float64)
+    out = np.zeros(2 * n)
+    dom = {"nb_min": [0, 0, 0], "nb_max": [0, 0, 0], "soil_max": 0.0, "water_max": 0.0}
+    s0, s1 = rf_spec(dict(pair[0], cell_ndx=1.0, flag_auto=1), dom), rf_spec(dict(pair[1], cell_ndx=1.0, flag_auto=1), dom)
+    lib.orc_rv_corr.restype = C.c_int
+    err = lib.orc_rv_corr(C.c_int(n), _ptr(ptype), C.byref(s0), C.byref(s1), C.c_double(coe), _ptr(u2), _ptr(out))
+    assert err == 0
+    return out.reshape(2, n)
+
+
+def _pair_arrays(pair):
+    mean = np.array([pair[0]["mean"], pair[1]["mean"]], dtype=np.float64)
+    sd = np.array([pair[0]["sd"], pair[1]["sd"]], dtype=np.float64)
+    cd = np.array([pair[0].get("coe_depth", 0.0), pair[1].get("coe_depth", 0.0)], dtype=np.float64)
+    return mean, sd, cd
+
+
+def rf_reference_corr(ndim, xp, ptype, dr, pair, coe, dom, u2):
+    """The reference's nonstationary_correlated_random_2D / _3D with the pair
+    normals u2: (code, out 2 x n)."""
+    lib = reference_lib()
+    n = len(ptype)
+    xp = np.ascontiguousarray(xp, dtype=np.float64).reshape(n, 3)
+    ptype = np.ascontiguousarray(ptype, dtype=np.int32)
+    u2 = np.ascontiguousarray(u2, dtype=np.float64).reshape(-1, 2)
+    out = np.zeros(2 * n)
+    f0 = pair[0]
+    mean, sd, cd = _pair_arrays(pair)
+    rl = np.ascontiguousarray(f0["rl"], dtype=np.float64)
+    lo = np.ascontiguousarray(dom["nb_min"], dtype=np.float64)
+    hi = np.ascontiguousarray(dom["nb_max"], dtype=np.float64)
+    f = lib.ref_rf_cholesky_corr
+    f.restype = C.c_int
+    err = f(C.c_int(ndim), C.c_int(n), _ptr(xp), _ptr(ptype), C.c_double(dr), C.c_int(int(f0["no"])),
+            C.c_int(int(f0["type"])), _ptr(mean), _ptr(sd), _ptr(cd), _ptr(rl), C.c_double(f0["cell_ndx"]),
+            C.c_int(int(f0["flag_auto"])), C.c_double(f0.get("beta", 0.0)), C.c_double(f0.get("beta_1", 0.0)),
+            C.c_double(coe), _ptr(lo), _ptr(hi), C.c_double(dom["soil_max"]), C.c_double(dom["water_max"]),
+            _ptr(u2), C.c_int(len(u2)), _ptr(out))
+    return err, out.reshape(2, n)
+
+
+def rv_reference(ptype, pair, coe, u2):
+    """The reference's random_variable_generate with the normals u2."""
+    lib = reference_lib()
+    n = len(ptype)
+    ptype = np.ascontiguousarray(ptype, dtype=np.int32)
+    u2 = np.ascontiguousarray(u2, dtype=np.float64)
+    out = np.zeros(2 * n)
+    mean, sd, _ = _pair_arrays(pair)
+    f = lib.ref_rv_corr
+    f.restype = C.c_int
+    err = f(C.c_int(n), _ptr(ptype), C.c_int(int(pair[0]["no"])), C.c_int(int(pair[0]["type"])), _ptr(mean), _ptr(sd),
+            C.c_double(coe), _ptr(u2), _ptr(out))
+    assert err == 0
+    return out.reshape(2, n)
+
+
 def rf_reference(ndim, xp, ptype, dr, field, dom, zeta):
     """The reference's nonstationary_random_2D / _3D with the normals zeta."""
     lib = reference_lib()

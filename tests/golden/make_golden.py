@@ -367,10 +367,88 @@ def make_rf(name: str) -> str:
     zeta = np.random.default_rng(seed).standard_normal(ncell)
     err, out = rf_reference(sc.ndim, sc.xp, sc.ptype, sc.dr, field, dom, zeta)
     assert err == 0, err
+    spread = _rf_thread_spread(lambda: rf_reference(sc.ndim, sc.xp, sc.ptype, sc.dr, field, dom, zeta)[1], out)
     fn = os.path.join(HERE, name + ".npz")
     np.savez_compressed(fn, ndim=sc.ndim, xp=sc.xp, type=sc.ptype, dr=sc.dr, zeta=zeta, out=out,
                         nb_min=dom["nb_min"], nb_max=dom["nb_max"], soil_max=dom["soil_max"],
-                        water_max=dom["water_max"])
+                        water_max=dom["water_max"], ref_thread_spread=spread)
+    return fn
+
+
+def _rf_thread_spread(run, out1):
+    """The reference's own spread: the largest relative change of the field
+    when its OpenMP team has 2 to 8 threads instead of one (its Cholesky
+    diagonal is an OpenMP reduction whose order follows the team size,
+    CPP_17-3:52-55)."""
+    from checkers import reference_lib
+    lib = reference_lib()
+    ok = np.isfinite(out1)
+    scale = np.abs(out1[ok]).max()
+    worst = 0.0
+    try:
+        for t in range(2, 9):
+            lib.ref_rf_threads(t)
+            o = run()
+            worst = max(worst, float(np.abs(o[ok] - out1[ok]).max() / scale))
+    finally:
+        lib.ref_rf_threads(1)
+    return np.array(worst)
+
+
+# the correlated forms of CPP_17-5-Nonstationary-Correlated-RF.cpp, through the
+# reference's own routines with injected normals:
+# name: (scene factory, (friction field, cohesion field), coe_frict_cohesion, seed)
+_FAI_SOIL = {"no": 0, "type": 2, "mean": 25.0, "sd": 5.0, "rl": [8.0, 1.5, 0.0], "coe_depth": 0.5, "cell_ndx": 5.0,
+             "flag_auto": 1}
+_C_SOIL = {"no": 1, "type": 2, "mean": 10.0e3, "sd": 3.0e3, "rl": [1.0, 1.0, 0.0], "coe_depth": 200.0}
+RF_CORR_CASES = {
+    "rfc_slope_2d_soil_lognormal": (lambda: scenes.slope_2d(H=5.0, dx=0.1), (_FAI_SOIL, _C_SOIL), -0.5, 21),
+    "rfc_slope_2d_soil_normal_gauss": (
+        lambda: scenes.slope_2d(H=5.0, dx=0.1),
+        (dict(_FAI_SOIL, type=1, flag_auto=2, rl=[5.0, 2.0, 0.0], cell_ndx=4.0), dict(_C_SOIL, type=1)), -0.3, 22),
+    "rfc_column_3d_fluid_normal_rotated": (
+        _column_no_walls,
+        ({"no": 4, "type": 1, "mean": 5.0, "sd": 1.0, "rl": [0.5, 0.3, 0.2], "coe_depth": 2.0, "cell_ndx": 2.0,
+          "flag_auto": 3, "beta": 15.0, "beta_1": 30.0},
+         {"no": 5, "type": 1, "mean": 50.0, "sd": 10.0, "rl": [9.0, 9.0, 9.0], "coe_depth": 20.0}), 0.4, 23),
+    "rfc_column_3d_soil_lognormal": (
+        _column_no_walls,
+        (dict(_FAI_SOIL, rl=[0.4, 0.4, 0.3], cell_ndx=2.0), _C_SOIL), -0.6, 24),
+}
+# random_variable_generate (flspv 5): name: (scene factory, pair, coe, seed)
+RV_CASES = {
+    "rv_slope_2d_soil_lognormal": (lambda: scenes.slope_2d(H=5.0, dx=0.1), (_FAI_SOIL, _C_SOIL), -0.5, 31),
+    "rv_column_3d_fluid_normal": (_column_no_walls, (dict(_FAI_SOIL, no=4, type=1), dict(_C_SOIL, no=5)), 0.3, 32),
+}
+
+
+def make_rf_corr(name: str) -> str:
+    from checkers import rf_oracle_corr, rf_reference_corr
+    factory, pair, coe, seed = RF_CORR_CASES[name]
+    sc = factory()
+    dom = scenes.kl_domain(sc)
+    err, _, ncell = rf_oracle_corr(sc.ndim, sc.xp, sc.ptype, sc.dr, pair, coe, dom, np.zeros((15000, 2)))
+    assert err == 0, err
+    u2 = np.random.default_rng(seed).standard_normal((ncell, 2))
+    err, out = rf_reference_corr(sc.ndim, sc.xp, sc.ptype, sc.dr, pair, coe, dom, u2)
+    assert err == 0, err
+    spread = _rf_thread_spread(lambda: rf_reference_corr(sc.ndim, sc.xp, sc.ptype, sc.dr, pair, coe, dom, u2)[1],
+                               out)
+    fn = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(fn, ndim=sc.ndim, xp=sc.xp, type=sc.ptype, dr=sc.dr, u2=u2, out=out,
+                        nb_min=dom["nb_min"], nb_max=dom["nb_max"], soil_max=dom["soil_max"],
+                        water_max=dom["water_max"], ref_thread_spread=spread)
+    return fn
+
+
+def make_rv(name: str) -> str:
+    from checkers import rv_reference
+    factory, pair, coe, seed = RV_CASES[name]
+    sc = factory()
+    u2 = np.random.default_rng(seed).standard_normal(2)
+    out = rv_reference(sc.ptype, pair, coe, u2)
+    fn = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(fn, type=sc.ptype, u2=u2, out=out)
     return fn
 
 
@@ -394,6 +472,10 @@ def make(name: str) -> str:
         return make_kl(name)
     if name in RF_CASES:
         return make_rf(name)
+    if name in RF_CORR_CASES:
+        return make_rf_corr(name)
+    if name in RV_CASES:
+        return make_rv(name)
     factory, steps = CASES[name]
     sc = factory()
     out = {}
@@ -431,7 +513,8 @@ if __name__ == "__main__":
     saved = os.dup(1)
     os.dup2(devnull, 1)   # the reference prints progress lines
     try:
-        files = [make(n) for n in (sys.argv[1:] or list(CASES) + list(KL_CASES) + list(RF_CASES))]
+        files = [make(n) for n in (sys.argv[1:] or list(CASES) + list(KL_CASES) + list(RF_CASES) +
+                                         list(RF_CORR_CASES) + list(RV_CASES))]
     finally:
         os.dup2(saved, 1)
     for f in files:
