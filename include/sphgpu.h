@@ -396,6 +396,32 @@ const char* sphgpu_stage_name(int k);
 int         sphgpu_step_profiled(sphgpu_ctx* ctx, int nsteps, double* stage_ms);
 
 /*
+ * Vibration loading (flv 1 and 2): Para_Vibra (Class_Problem.h:133-149) as
+ * initial_pro reads its VL block (ttime nsteps / sttime edtime,
+ * CPP_2-initialf.cpp:250-270) and initial_vib reads vibra.dat (nsteps rows of
+ * three loads, CPP_2-initialf.cpp:292-320).  With flv 1 the walls of matype 3
+ * and 5 take the load of the step's time as their acceleration
+ * (vibration_acceleration, CPP_9-1-acceleration_vibration.cpp:10-78), with
+ * flv 2 the walls of matype 4 and 5 take it as their velocity
+ * (vibration_velocity, :80-160); with either, the soil and structure
+ * particles are damped by soil_damping_vibration (:162-224, damp1 + damp2
+ * sqrt(stiffness / rho h^2) from the soil record) and the soil feels the
+ * free-field particles (free_field_solid, CPP_19-FreeFieldParticles.cpp and
+ * CPP_19-FreeFieldParticles_soil.cpp: soil of matype >= 50 and walls of
+ * matype 5, permtype the wave direction).  A context with flv >= 1 steps
+ * only after this call.  Returns 0, 7 (nsteps < 1, the reference's error),
+ * SPHGPU_E_ARG (no loads, or ttime not positive), SPHGPU_E_STATE (flv 0).
+ * sphgpu_checkpoint_save keeps the table.
+ */
+typedef struct sphgpu_vibration {
+    double ttime;                /* one period */
+    int    nsteps;               /* load entries per period */
+    double sttime, edtime;       /* the loads apply for sttime <= t <= edtime */
+} sphgpu_vibration;
+
+int sphgpu_set_vibration(sphgpu_ctx* ctx, const sphgpu_vibration* vib, const double* loads);
+
+/*
  * Karhunen-Loeve random fields (flspv 1 and 2): the reference's
  * clFSpatialVariability_Fun::SpatialVariables_Generate_2D / _3D and
  * SpatialVariables_Generate_2D_corr / _3D_corr

@@ -153,6 +153,11 @@ struct sphgpu_ctx {
     int part_done = 0;     // parts of step l run through the method entries: 1 parttocell, 2 partisearching
     sphgpu_rain rain = {};            // the rainfall record (flr 1), nrain as last set
     bool rain_set = false;
+    sphgpu_vibration vib = {};        // the vibration table (flv 1, 2) as last set
+    std::vector<double> vib_loads;
+    bool vib_set = false;
+    double vib_par[4] = {0, 0, 0, 0};   // ttime, nsteps, sttime, edtime (checkpoint record)
+    bool accb_vib = false;            // accb holds the vibration rows (19N)
     // the output writer: two slots of device staging, pinned host copy,
     // completion event and writer thread
     double* out_dev[2] = {nullptr, nullptr};
@@ -202,7 +207,7 @@ int check_params(const sphgpu_params* P)
     // flag combinations this engine runs (the others are rejected loudly)
     if (!(P->flbndy >= 1 && P->flbndy <= 5) && P->flbndy != 13 && P->flbndy != 14) return SPHGPU_E_UNSUPPORTED;
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
-    if (P->flv != 0) return SPHGPU_E_UNSUPPORTED;
+    if (P->flv < 0 || P->flv > 2) return SPHGPU_E_UNSUPPORTED;
     if (P->fli < 0 || P->fli > 3) return SPHGPU_E_UNSUPPORTED;
     if (P->ss_type < 0 || P->ss_type > 3) return SPHGPU_E_UNSUPPORTED;
     if (P->if_move < 0 || P->if_move > 3) return SPHGPU_E_UNSUPPORTED;
@@ -241,6 +246,8 @@ void fill_dev_params(DevParams& p, const sphgpu_params* P)
     for (int q = 0; q < TP_COUNT; q++) p.tb[q] = 128;
     p.flr = P->flr == 1 ? 1 : 0;
     p.rain_lp = 0; p.rain_vrain = 0.0; p.rain_press = 0.0;
+    p.vib_ttime = 0.0; p.vib_st = 0.0; p.vib_ed = 0.0; p.vib_nsteps = 0;
+    p.ff_e = 0.0; p.ff_poi = 0.0;      // pFFBound: Para_Soil() (Class_ParticleProperty.cpp:28-31)
 }
 
 // the buffers only some flag settings use, allocated when the flags first
@@ -265,6 +272,13 @@ int alloc_optional(sphgpu_ctx* c, const sphgpu_params* P)
         need(s.fsol, 3 * (size_t)N);
         need(s.fsol_on, (size_t)N);
     }
+    if (P->flv > 0) need(s.stiff, (size_t)N);
+    if (P->flv != 0 && !c->accb_vib) {
+        // the momentum pass's vibration rows: accb grows from 9N to 19N
+        double* q = nullptr;
+        r |= dalloc(c, &q, 19 * (size_t)N);
+        if (q) { s.accb = q; c->d[1].s.accb = q; c->accb_vib = true; }
+    }
     if (P->flbndy != 1 && P->flbndy != 5) {
         need(s.vel_bndy, 3 * (size_t)N);
         need(s.vb, 12 * (size_t)N);
@@ -276,6 +290,7 @@ int alloc_optional(sphgpu_ctx* c, const sphgpu_params* P)
     t.rij = s.rij; t.ss_id = s.ss_id; t.ss_con = s.ss_con; t.ss_own = s.ss_own; t.ss_fs = s.ss_fs;
     t.cpl = s.cpl; t.fsol = s.fsol; t.fsol_on = s.fsol_on;
     t.vel_bndy = s.vel_bndy; t.vb = s.vb; t.vx_vb = s.vx_vb; t.sb = s.sb;
+    t.stiff = s.stiff;
     return r;
 }
 
@@ -402,7 +417,9 @@ int check_particles(sphgpu_ctx* c)
 {
     if (c->h_type.empty() || c->h_matype.empty()) return SPHGPU_E_STATE;
     if (c->P.flr == 1 && !c->rain_set) return SPHGPU_E_STATE;
-    bool ext = c->P.flagum == 1;
+    if (c->P.flv >= 1 && !c->vib_set) return SPHGPU_E_STATE;
+    // the vibration damping reads damp1 / damp2 from the extended soil block
+    bool ext = c->P.flagum == 1 || c->P.flv > 0;
     for (int i = 0; i < c->N; i++) {
         const int t = c->h_type[i], m = c->h_matype[i];
         // matype 30-49 and >= 60 match no branch of strain_to_stress
@@ -645,7 +662,8 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.cstart, M); r |= dalloc(c, &s.cend, M);
     r |= dalloc(c, &s.nnb, N); r |= dalloc(c, &s.nbr, (size_t)SPH_NB_CAP * N);
     r |= dalloc(c, &s.nps, N); r |= dalloc(c, &s.sortpos, N); r |= dalloc(c, &s.pts, N);
-    r |= dalloc(c, &s.accb, 9 * (size_t)N); r |= dalloc(c, &s.nbrs, (size_t)SPH_NB_CAP * N);
+    if (!s.accb) r |= dalloc(c, &s.accb, 9 * (size_t)N);   // (19N when alloc_optional sized it for vibration)
+    r |= dalloc(c, &s.nbrs, (size_t)SPH_NB_CAP * N);
     r |= dalloc(c, &s.nbm, 10 * (size_t)N);
     r |= dalloc(c, &s.nbw, 4 * (size_t)SPH_NB_CAP * N);
     r |= dalloc(c, &s.err, 1); r |= dalloc(c, &s.step, 1);
@@ -966,7 +984,7 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
         // saturation pass and fractional-order Cam-clay (8) read, allocated
         // on first use; pow(c, 4) of fractional_mcc with the host's libm
         // (CPP_8-5-consfactor-focc.cpp:158)
-        bool need = c->P.flagum == 1;
+        bool need = c->P.flagum == 1 || c->P.flv > 0;
         for (int i = 0; i < N && !need && i < (int)c->h_matype.size(); i++) {
             const int mt = c->h_matype[i] % 10;
             need = (mt == 3 || mt == 8);
@@ -1232,6 +1250,8 @@ int sphgpu_update_params(sphgpu_ctx* c, const sphgpu_params* P)
         dp.bulk = keep.bulk;
         dp.cfl_on = keep.cfl_on; dp.cfl_c = keep.cfl_c; dp.cfl_f = keep.cfl_f;
         dp.rain_lp = keep.rain_lp; dp.rain_vrain = keep.rain_vrain; dp.rain_press = keep.rain_press;
+        dp.vib_ttime = keep.vib_ttime; dp.vib_st = keep.vib_st; dp.vib_ed = keep.vib_ed;
+        dp.vib_nsteps = keep.vib_nsteps;
         for (int q = 0; q < TP_COUNT; q++) dp.tb[q] = keep.tb[q];
     }
     c->P = *P;
@@ -1382,7 +1402,7 @@ struct CkHeader {
     sphgpu_rain rain;
 };
 
-struct CkExtra { const char* name; void* ptr; size_t bytes; };
+struct CkExtra { const char* name; void* ptr; size_t bytes; bool host; };
 
 std::vector<CkExtra> ck_extras(sphgpu_ctx* c)
 {
@@ -1390,7 +1410,7 @@ std::vector<CkExtra> ck_extras(sphgpu_ctx* c)
     const size_t N = (size_t)c->N;
     const size_t last = (size_t)c->P.ctotal;
     std::vector<CkExtra> v;
-    auto add = [&](const char* name, void* p, size_t bytes) { if (p) v.push_back({name, p, bytes}); };
+    auto add = [&](const char* name, void* p, size_t bytes) { if (p) v.push_back({name, p, bytes, false}); };
     add("vel_bndy", s.vel_bndy, 3 * N * 8);
     add("vb", s.vb, 12 * N * 8);
     add("vx_vb", s.vx_vb, 3 * N * 8);
@@ -1401,6 +1421,13 @@ std::vector<CkExtra> ck_extras(sphgpu_ctx* c)
     add("dtv", s.dtv, 8);
     add("dtmin", s.dtmin, 8);
     add("tsim", s.tsim, 8);
+    add("stiff", s.stiff, N * 8);
+    // the vibration table, from the host copies (sphgpu_set_vibration again
+    // on load)
+    if (c->vib_set) {
+        v.push_back({"vib_par", c->vib_par, sizeof(c->vib_par), true});
+        v.push_back({"vib_loads", c->vib_loads.data(), c->vib_loads.size() * 8, true});
+    }
     return v;
 }
 
@@ -1440,7 +1467,8 @@ int sphgpu_checkpoint_save(sphgpu_ctx* c, const char* path)
     for (const CkExtra& e : ex) {
         if (rc || !ok) break;
         buf.resize(e.bytes);
-        if (cuda_fail(c, cudaMemcpy(buf.data(), e.ptr, e.bytes, cudaMemcpyDeviceToHost), "cudaMemcpy")) {
+        if (e.host) std::memcpy(buf.data(), e.ptr, e.bytes);
+        else if (cuda_fail(c, cudaMemcpy(buf.data(), e.ptr, e.bytes, cudaMemcpyDeviceToHost), "cudaMemcpy")) {
             rc = SPHGPU_E_CUDA;
             break;
         }
@@ -1494,6 +1522,7 @@ int sphgpu_checkpoint_load(sphgpu_ctx* c, const char* path)
     if (!rc && h.cfl_on) rc = sphgpu_set_cfl(c, h.cfl_c, h.cfl_f);
     // the device words and arrays last, over what the calls above set
     std::vector<CkExtra> ex = ck_extras(c);
+    std::vector<double> vpar, vload;
     for (int q = 0; q < h.nextra && !rc; q++) {
         char name[16];
         uint64_t b = 0;
@@ -1501,10 +1530,20 @@ int sphgpu_checkpoint_load(sphgpu_ctx* c, const char* path)
         name[15] = 0;
         buf.resize(b);
         if (std::fread(buf.data(), 1, b, f) != b) { rc = SPHGPU_E_ARG; break; }
+        if (std::strcmp(name, "vib_par") == 0 || std::strcmp(name, "vib_loads") == 0) {
+            std::vector<double>& dst = (name[4] == 'p') ? vpar : vload;
+            dst.resize(b / 8);
+            std::memcpy(dst.data(), buf.data(), dst.size() * 8);
+            continue;
+        }
         for (const CkExtra& e : ex)
-            if (std::strcmp(e.name, name) == 0 && e.bytes == b &&
+            if (!e.host && std::strcmp(e.name, name) == 0 && e.bytes == b &&
                 cuda_fail(c, cudaMemcpy(e.ptr, buf.data(), b, cudaMemcpyHostToDevice), "cudaMemcpy"))
                 rc = SPHGPU_E_CUDA;
+    }
+    if (!rc && vpar.size() == 4 && c->P.flv >= 1) {
+        const sphgpu_vibration v = {vpar[0], (int)vpar[1], vpar[2], vpar[3]};
+        if (vload.size() == 3 * (size_t)v.nsteps) rc = sphgpu_set_vibration(c, &v, vload.data());
     }
     std::fclose(f);
     if (!rc && h.regu && !c->regu) { c->regu = true; invalidate_graphs(c); }
@@ -1682,6 +1721,34 @@ int sphgpu_get_rain(sphgpu_ctx* c, sphgpu_rain* rain)
     cudaSetDevice(c->device);
     CK(cudaMemcpyAsync(&rain->nrain, c->d[0].s.nrain, sizeof(int), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+int sphgpu_set_vibration(sphgpu_ctx* c, const sphgpu_vibration* v, const double* loads)
+{
+    if (!c || !v) return SPHGPU_E_ARG;
+    if (c->P.flv < 1) return SPHGPU_E_STATE;
+    if (v->nsteps < 1) return 7;                      // initial_pro's vibration steps error (CPP_2-initialf.cpp:262-268)
+    if (!loads || !(v->ttime > 0.0) || !std::isfinite(v->ttime) || v->sttime != v->sttime || v->edtime != v->edtime)
+        return SPHGPU_E_ARG;
+    cudaSetDevice(c->device);
+    const size_t n = 3 * (size_t)v->nsteps;
+    if (c->vib_loads.size() != n) {
+        double* q = nullptr;
+        if (dalloc(c, &q, n)) return SPHGPU_E_CUDA;
+        for (int p = 0; p < 2; p++) c->d[p].s.vib_loads = q;
+    }
+    c->vib_loads.assign(loads, loads + n);
+    CK(cudaMemcpyAsync(c->d[0].s.vib_loads, c->vib_loads.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int p = 0; p < 2; p++) {
+        DevParams& dp = c->d[p].p;
+        dp.vib_ttime = v->ttime; dp.vib_nsteps = v->nsteps; dp.vib_st = v->sttime; dp.vib_ed = v->edtime;
+    }
+    c->vib = *v;
+    c->vib_par[0] = v->ttime; c->vib_par[1] = v->nsteps; c->vib_par[2] = v->sttime; c->vib_par[3] = v->edtime;
+    c->vib_set = true;
+    invalidate_graphs(c);
     return 0;
 }
 

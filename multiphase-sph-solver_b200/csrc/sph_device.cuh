@@ -88,6 +88,13 @@ struct DevParams {
     // rainfall (flr 1, rtype 1): rainini's lp and vrain, Para_Rain::press_factor
     int flr, rain_lp;
     double rain_vrain, rain_press;
+    // vibration (flv 1, 2): Para_Vibra's period, steps per period, start and
+    // end time (its loads in DevState::vib_loads); the free-field walls'
+    // elastic constants (the reference's pFFBound, a default-constructed
+    // Para_Soil: e = poi = 0, CPP_1-SPHLoops.cpp:253)
+    double vib_ttime, vib_st, vib_ed;
+    int vib_nsteps;
+    double ff_e, ff_poi;
 };
 
 // Members of the soil record that only the unsaturated Cam-clay model, the
@@ -172,8 +179,16 @@ struct DevState {
     // candidate within the FP32 margin of the radius); sortpos[i] = q
     int *nps, *nbrs, *sortpos, *pts;
     // the momentum pass's artificial-viscosity, drag and damping sums, from
-    // its loop kernel to its tail kernel: accb[(3 g + k) * N + i] (9N)
+    // its loop kernel to its tail kernel: accb[(3 g + k) * N + i] (9N); with
+    // vibration (flv != 0) also the free-field sums of the walls (g = 3) and
+    // of the soil (g = 4), the vibration damping sum (g = 5) and its
+    // normaliser (row 18): 19N
     double* accb;
+    // vibration (flv > 0): per soil / structure particle the largest of 0 and
+    // the diagonal entries 0-2 of the constitutive matrix of its last stress
+    // update (StiffMat::depp0, CPP_7-2-constitutive.cpp:112-292), N; and
+    // Para_Vibra::loads, vib_nsteps x 3
+    double *stiff, *vib_loads;
     // per particle and particle type t = 0..4, bit s set when list slot s
     // holds a particle of type t: nbm[(2 t + w) * N + i], word w = 0 for
     // slots 0-63, 1 for slots 64-98 (written by the search with the list)

@@ -1085,6 +1085,15 @@ __global__ void __launch_bounds__(128, SPH_MINB_STRESS) k_stress(Dev d)
             for (int a = 0; a < 6; a++)
                 for (int b = 0; b < 6; b++) D[a][b] = Dl[a][b];
         }
+        // StiffMat::depp0 = dept (CPP_7-2-constitutive.cpp:112-229, 292), which
+        // the vibration damping reads through its largest diagonal entry; the
+        // viscous-elastic model (matype % 10 == 7) leaves it as it was
+        if (d.s.stiff && (ti == 4 || !plastic || mt != 7)) {
+            double st = fmax(0.0, D[0][0]);
+            st = fmax(st, D[1][1]);
+            st = fmax(st, D[2][2]);
+            d.s.stiff[i] = st;
+        }
         if (plastic && mt == 7) {
             double smv;
             const double e0 = elastic_e0(s, d.s.s_e[i], d.s.s_poi[i], d.s.s_eps0[i], d.s.s_kapa[i], &smv);
@@ -1448,6 +1457,37 @@ __device__ __noinline__ void wall_stress_rows(int i, int N, unsigned long long w
     for (int k = 0; k < 3; k++) rows[k] = tb[k][0].v() + tb[k][1].v() + tb[k][2].v();
 }
 
+// ff_stress_2d_solid / ff_stress_3d_solid (CPP_19-FreeFieldParticles.cpp:21-76,
+// the same in CPP_19-FreeFieldParticles_soil.cpp:21-68): the viscous stress a
+// free-field particle of elastic constants (e, poi), density dens and wave
+// direction `type` (its permtype) puts between velocities va and vb
+template <int ND>
+__device__ __forceinline__ void ff_stress(double sg[3], const double va[3], const double vb[3], double e, double poi,
+                                          double dens, int type)
+{
+    const double g = e * 0.5 / (1 + poi);
+    const double k = e * 0.333333333333333 / (1 - 2.0 * poi);
+    const double c_p = sqrt((k + 4.0 * g * 0.333333333333333) / dens);
+    const double c_s = sqrt(g / dens);
+    sg[0] = 0.0; sg[1] = 0.0; sg[2] = 0.0;
+    if (ND == 2) {
+        if (type == 1) {
+            sg[0] = -c_p * dens * (va[0] - vb[0]);
+            sg[1] = -c_s * dens * (va[1] - vb[1]);
+        } else if (type == 2) {
+            sg[0] = -c_s * dens * (va[0] - vb[0]);
+            sg[1] = -c_p * dens * (va[1] - vb[1]);
+        }
+    } else {
+        const double c0 = (type == 1) ? c_p : c_s, c1 = (type == 2) ? c_p : c_s, c2 = (type == 3) ? c_p : c_s;
+        if (type >= 1 && type <= 3) {
+            sg[0] = -c0 * dens * (va[0] - vb[0]);
+            sg[1] = -c1 * dens * (va[1] - vb[1]);
+            sg[2] = -c2 * dens * (va[2] - vb[2]);
+        }
+    }
+}
+
 // artificial_viscosity (CPP_9-3-artificialvis.cpp:12-99), the pair sum of
 // artificial_stress_2d/_3d (CPP_9-5-artificialstress.cpp, ART = 1),
 // boundary_moving_stress_effect (CPP_9-4-derivation_stress.cpp:631-721),
@@ -1482,6 +1522,39 @@ __global__ void __launch_bounds__(128, LOOP ? SPH_MINB_ACCB2 : SPH_MINB_ACCB1) k
     if (ti == 2) { ca = (real)d.s.s_vpu[i]; aa = (real)d.p.av[1][0]; bb = (real)d.p.av[1][1]; }
     if (ti == 3) { ca = (real)d.s.f_vpu[i]; aa = (real)d.p.av[2][0]; bb = (real)d.p.av[2][1]; }
     const double satu_i = d.s.satu[i];
+    // vibration (flv != 0): the free-field sums of free_field_solid over the
+    // walls of matype 5 (CPP_19-FreeFieldParticles.cpp:79-141) and of its soil
+    // form between free-field soil (matype >= 50) and the rest
+    // (CPP_19-FreeFieldParticles_soil.cpp:71-175), for soil particles; the
+    // sums of soil_damping_vibration (CPP_9-1-acceleration_vibration.cpp:
+    // 171-224) for soil and structure particles (flv > 0)
+    const bool ffree = LOOP == 0 && d.p.flv != 0 && ti == 2;
+    const bool vdamp = LOOP == 0 && d.p.flv > 0 && solid;
+    Sum<real> tfw[3], tfs[3], tdv[3], tdn;
+    real cdv = 0;
+    double vnow_i[3] = {0.0, 0.0, 0.0};
+    const int mti = d.s.matype[i];
+    if (vdamp) {
+        const double hl = d.s.xh[4 * (size_t)i + 3];
+        cdv = (real)(d.s.s_ext[(size_t)SX_DAMP1 * N + i] +
+                     d.s.s_ext[(size_t)SX_DAMP2 * N + i] * sqrt(d.s.stiff[i] / d.s.rhop[i] / hl / hl));
+    }
+    if (ffree) {
+        for (int k = 0; k < 3; k++) vnow_i[k] = d.s.vx[k * N + i];
+        MaskIter itw(d, i, type_mask(d, i, 0));
+        int q, j;
+        while (itw.next(q, j)) {
+            if (d.s.matype[j] != 5) continue;
+            real w[4];
+            load_w(d, q, i, w);
+            double vj[3], sg[3];
+            for (int k = 0; k < 3; k++) vj[k] = d.s.interfss[k * N + j];
+            const double rj = d.s.rho[j];
+            ff_stress<ND>(sg, vnow_i, vj, d.p.ff_e, d.p.ff_poi, rj, d.s.permtype[j]);
+            const real mr = (real)(d.s.mass[j] / rj);
+            for (int k = 0; k < nd; k++) tfw[k].add(mr * (real)sg[k] / riR * w[k]);
+        }
+    }
     // artificial viscosity and geostatic damping over i's own type's slots,
     // then the soil-water (soil-air) drag of interact1/2/3 over the slots of
     // the types it pairs (the reference visits every other pair of different
@@ -1515,6 +1588,22 @@ __global__ void __launch_bounds__(128, LOOP ? SPH_MINB_ACCB2 : SPH_MINB_ACCB1) k
             for (int k = 0; k < nd; k++) tav[k].add(mj * paix * w[k]);
             if (dm_pair)
                 for (int k = 0; k < nd; k++) tdm[k].add(mj / rj * cdi * dvx[k] * w[3]);
+            if (vdamp) {
+                for (int k = 0; k < nd; k++) tdv[k].add(mj / rj * cdv * dvx[k] * w[3]);
+                tdn.add(mj / rj * w[3]);
+            }
+            if (ffree) {
+                const int mtj = d.s.matype[j];
+                if ((mti < 50) != (mtj < 50)) {
+                    double vj[3], sg[3];
+                    for (int k = 0; k < 3; k++) vj[k] = d.s.vx[k * N + j];
+                    if (mti < 50)
+                        ff_stress<ND>(sg, vnow_i, vj, d.s.s_e[j], d.s.s_poi[j], d.s.rho[j], d.s.permtype[j]);
+                    else
+                        ff_stress<ND>(sg, vj, vnow_i, d.s.s_e[i], d.s.s_poi[i], ri, d.s.permtype[i]);
+                    for (int k = 0; k < nd; k++) tfs[k].add(mj / rj * (real)sg[k] / riR * w[k]);
+                }
+            }
         }
     }
     if (LOOP == 1 && d.p.fli >= 1 && (ti == 1 || ti == 2 || ti == 3)) {
@@ -1567,6 +1656,14 @@ __global__ void __launch_bounds__(128, LOOP ? SPH_MINB_ACCB2 : SPH_MINB_ACCB1) k
             }
         }
     }
+    if (LOOP == 0 && d.p.flv != 0) {
+        for (int k = 0; k < 3; k++) {
+            d.s.accb[(size_t)(9 + k) * N + i] = (double)tfw[k].v();
+            d.s.accb[(size_t)(12 + k) * N + i] = (double)tfs[k].v();
+            d.s.accb[(size_t)(15 + k) * N + i] = (double)tdv[k].v();
+        }
+        d.s.accb[(size_t)18 * N + i] = (double)tdn.v();
+    }
     for (int k = 0; k < 3; k++) {
         if (LOOP == 0) {
             d.s.accb[(size_t)k * N + i] = (double)tav[k].v();
@@ -1575,6 +1672,26 @@ __global__ void __launch_bounds__(128, LOOP ? SPH_MINB_ACCB2 : SPH_MINB_ACCB1) k
             d.s.accb[(size_t)(3 + k) * N + i] = (double)tin[k].v();
         }
     }
+}
+
+// The vibration load of the step at time t (vibration_acceleration and
+// vibration_velocity, CPP_9-1-acceleration_vibration.cpp:10-160): 0 outside
+// [sttime, edtime]; else the entry of Para_Vibra::loads the elapsed time
+// selects in v, and 1 when its largest magnitude is under 1000, 2 when not.
+__device__ __forceinline__ int vib_load(const Dev& d, double t, double v[3])
+{
+    const double time1 = t - d.p.vib_st, time2 = t - d.p.vib_ed;
+    if (!(time1 >= 0.0 && time2 <= 0.0)) return 0;
+    const int ns = d.p.vib_nsteps;
+    // (int)(time1 / ttime * nsteps), capped at nsteps - 1 (the cap taken
+    // before the conversion, which would overflow past it)
+    const double q = time1 / d.p.vib_ttime * (double)ns;
+    const int step = (q >= (double)(ns - 1)) ? ns - 1 : (int)q;
+    for (int k = 0; k < 3; k++) v[k] = d.s.vib_loads[(size_t)step * 3 + k];
+    double m = fmax(0.0, fabs(v[0]));
+    m = fmax(m, fabs(v[1]));
+    m = fmax(m, fabs(v[2]));
+    return (m < 1000.0) ? 1 : 2;
 }
 
 // The rest of the momentum pass, per particle: the wall stress and the
@@ -1669,6 +1786,11 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b_tail(Dev d)
         for (int k = 0; k < nd; k++) ax[k] = ax[k] + tu[k].v();
     if (moving)
         for (int k = 0; k < 3; k++) ax[k] += tbrow[k];
+    if (d.p.flv != 0 && ti == 2) {
+        // free_field_solid: the walls' sum, then the soil form's
+        for (int k = 0; k < nd; k++) ax[k] = ax[k] + d.s.accb[(size_t)(9 + k) * N + i];
+        for (int k = 0; k < nd; k++) ax[k] = ax[k] + d.s.accb[(size_t)(12 + k) * N + i];
+    }
     if (d.p.ss_coupled && (ti == 1 || ti == 2 || ti == 4))
         for (int k = 0; k < 3; k++) ax[k] += d.s.cpl[(size_t)k * N + i];
     const double dt = step_dt(d);
@@ -1716,6 +1838,18 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b_tail(Dev d)
             else ax[k] -= tdm[k];
         }
     }
+    if (d.p.flv > 0 && solid) {
+        // soil_damping_vibration (CPP_9-1-acceleration_vibration.cpp:171-224)
+        double td = d.s.accb[(size_t)18 * N + i];
+        for (int k = 0; k < nd; k++) {
+            if (fabs(td) < 1.0e-7) td = 1.0e-7;
+            const double dm = d.s.accb[(size_t)(15 + k) * N + i];
+            double vx1 = vi[k] + 0.5 * (axp[k] + ax[k]) * dt;
+            double vx2 = vi[k] + 0.5 * (axp[k] + ax[k] - dm / td) * dt;
+            if (vx1 * vx2 <= 0.0) ax[k] = -2.0 * vi[k] / dt - axp[k];
+            else ax[k] -= dm / td;
+        }
+    }
     if (d.p.flbndy == 5 && d.s.fsol_on[i]) {
         // boundary_free_solid (CPP_13-boundary.cpp:1239-1516), after the damping
         const double mi = d.s.mass[i];
@@ -1725,6 +1859,17 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b_tail(Dev d)
     double vout[3];
     for (int k = 0; k < 3; k++) vout[k] = d.s.vx[k * N + i];
     const int mt = d.s.matype[i];
+    if (d.p.flv == 1 && ti == 0 && (mt == 3 || mt == 5)) {
+        // vibration_acceleration: the load into the wall's interf (a load of
+        // 1000 or more, or a time outside the window, zeroes interf and
+        // interfss)
+        double v[3];
+        const int ld = vib_load(d, *d.s.tsim + dt, v);
+        for (int k = 0; k < nd; k++) {
+            if (ld == 1) d.s.interf[k * N + i] = v[k];
+            else { d.s.interf[k * N + i] = 0.0; d.s.interfss[k * N + i] = 0.0; }
+        }
+    }
     if (d.p.if_move == 0) {
         if (ti == 0 && mt < 2) {
             for (int k = 0; k < nd; k++) {
@@ -1772,6 +1917,16 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b_tail(Dev d)
         for (int k = 0; k < nd; k++) {
             double ath = (axp[k] + ax[k]) * 0.5;
             vout[k] = vp[k] + ath * dt;
+        }
+    }
+    if (d.p.flv == 2 && ti == 0 && (mt == 4 || mt == 5)) {
+        // vibration_velocity, after the velocity update: the load is the
+        // wall's velocity interfss
+        double v[3];
+        const int ld = vib_load(d, *d.s.tsim + dt, v);
+        for (int k = 0; k < nd; k++) {
+            if (ld == 1) d.s.interfss[k * N + i] = v[k];
+            else { d.s.interf[k * N + i] = 0.0; d.s.interfss[k * N + i] = 0.0; }
         }
     }
     for (int k = 0; k < 3; k++) {

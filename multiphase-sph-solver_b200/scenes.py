@@ -20,6 +20,7 @@ cell centres ``(i + 1/2) dx``; nothing is random.
 from __future__ import annotations
 
 import copy
+import os
 import math
 from dataclasses import dataclass, field
 
@@ -71,6 +72,7 @@ class Scene:
     soils: dict = field(default_factory=dict)     # {index: Para_Soil dict}, index = layer*10 + model
     structure: dict | None = None                 # block SM
     rain: dict | None = None                      # block RP (flr = 1)
+    vibration: dict | None = None                 # block VL + vibra.dat (flv >= 1): ttime nsteps sttime edtime loads
 
     @property
     def n(self) -> int:
@@ -327,6 +329,95 @@ def footing(ndim: int = 2, dx: float = 0.04, bed=(2.0, 1.0, 1.0), width: float =
     )
 
 
+def shaking_box(ndim: int = 2, flv: int = 1, dx: float = 0.05, box=(2.0, 1.0, 0.4), layers: int = 3,
+                steps: int = 40, ff_columns: int = 2, damp=(0.5, 0.02), amplitude: float | None = None,
+                window=(3, 30)) -> Scene:
+    """A soil block on a shaking base (vibration, flv 1 or 2): Drucker-Prager
+    soil (type 2, matype 2, E = 20 MPa, rho = 2000) of box[0] x box[1]
+    (x box[2] in 3-D) with free-field columns of `ff_columns` particles at
+    both x ends (matype 52, the same material; permtype 1 on the left, 2 on
+    the right: the wave direction ff_stress reads), on a `layers`-layer floor
+    between side walls.  The floor takes the vibration load: matype 3
+    (flv 1, acceleration) or 4 (flv 2, velocity), matype 5 under the
+    free-field columns; the side walls are matype 5 (permtype 1 / 2).  Soil
+    damping damp1, damp2 (soil_damping_vibration).  The load table: 20
+    entries per period of 40 steps, a sine in x with a smaller cosine in y
+    (amplitude 2 m/s^2 or 0.05 m/s), one entry of 1500 (the reference's
+    cut-off), applied between steps window[0] and window[1] (sttime and
+    edtime as multiples of dt)."""
+    g = 9.81
+    L = layers
+    nx, ny = int(round(box[0] / dx)), int(round(box[1] / dx))
+    parts = []
+    if ndim == 2:
+        soil = _grid2(nx, ny, dx, (0.0, 0.0))
+        xs = soil[:, 0]
+        ffl = xs < ff_columns * dx
+        ffr = xs > (nx - ff_columns) * dx
+        core = ~(ffl | ffr)
+        parts += [(soil[core], 2, 2), (soil[ffl], 2, 52), (soil[ffr], 2, 52)]
+        floor = _grid2(nx + 2 * L, L, dx, (-L * dx, -L * dx))
+        fx = floor[:, 0]
+        under_ff = (fx < ff_columns * dx) | (fx > (nx - ff_columns) * dx)
+        parts += [(floor[~under_ff], 0, 3 if flv == 1 else 4), (floor[under_ff], 0, 5)]
+        nwy = ny + 2
+        parts += [(_grid2(L, nwy, dx, (-L * dx, 0.0)), 0, 5), (_grid2(L, nwy, dx, (nx * dx, 0.0)), 0, 5)]
+        grav = (0.0, -g, 0.0)
+    else:
+        nz = int(round(box[2] / dx))
+        soil = _grid(nx, nz, ny, dx, (0.0, 0.0, 0.0))       # y across, z up
+        xs = soil[:, 0]
+        ffl = xs < ff_columns * dx
+        ffr = xs > (nx - ff_columns) * dx
+        core = ~(ffl | ffr)
+        parts += [(soil[core], 2, 2), (soil[ffl], 2, 52), (soil[ffr], 2, 52)]
+        floor = _grid(nx + 2 * L, nz + 2 * L, L, dx, (-L * dx, -L * dx, -L * dx))
+        fx = floor[:, 0]
+        under_ff = (fx < ff_columns * dx) | (fx > (nx - ff_columns) * dx)
+        parts += [(floor[~under_ff], 0, 3 if flv == 1 else 4), (floor[under_ff], 0, 5)]
+        nwz = ny + 2
+        parts += [(_grid(L, nz + 2 * L, nwz, dx, (-L * dx, -L * dx, 0.0)), 0, 5),
+                  (_grid(L, nz + 2 * L, nwz, dx, (nx * dx, -L * dx, 0.0)), 0, 5),
+                  (_grid(nx, L, nwz, dx, (0.0, -L * dx, 0.0)), 0, 0),
+                  (_grid(nx, L, nwz, dx, (0.0, nz * dx, 0.0)), 0, 0)]
+        grav = (0.0, 0.0, -g)
+    xp, vxp, ptype, mt, permtype, etype = _assemble(parts)
+    # wave directions: left free-field soil and left wall 1, right 2
+    left = xp[:, 0] < 0.5 * nx * dx
+    sel = (mt == 52) | (mt == 5)
+    permtype[sel & left] = 1
+    permtype[sel & ~left] = 2
+    dt = 0.25 * dx / 600.0
+    dp = soil_default()
+    dp.update(kapa=0.05, poi=0.3, dens=2000.0, c=5.0e3, fai=30.0, fs=1.0, beta=0.0,
+              damp1=damp[0], damp2=damp[1], cop=1.0e-4, eps0=0.0, e=2.0e7, ds=1.0e-3)
+    w = fluid_default()
+    w.update(dens=1000.0, vis=1.0e-3, vpu=30.0, press_type=0, acc_type=0, bhtype=0,
+             pre_coe=30.0 * 30.0 / (7.0 * g * dx), strain_min=1.0e-3)
+    nsteps = 20
+    amp = amplitude if amplitude is not None else (2.0 if flv == 1 else 0.05)
+    ph = 2.0 * np.pi * np.arange(nsteps) / nsteps
+    loads = np.stack([amp * np.sin(ph), 0.3 * amp * np.cos(ph), 0.1 * amp * np.sin(2 * ph)], axis=1)
+    loads[7, 0] = 1500.0
+    vib = dict(ttime=40 * dt, nsteps=nsteps, sttime=window[0] * dt, edtime=window[1] * dt, loads=loads)
+    return Scene(
+        name=f"shaking_box_{ndim}d_flv{flv}_dx{dx:g}", ndim=ndim, dr=dx, dt=dt, loop=steps,
+        xp=xp, vxp=vxp, ptype=ptype, matype=mt, permtype=permtype, etype=etype,
+        flags=dict(fla=0, fls=1, flr=0, fli=0, flv=flv, fleob=0, flts=0, flspv=0, flknl=1,
+                   ntd=1, flbndy=1),
+        problem=dict(threshold_min=0.1, threshold_max=0.12, fop=max(steps, 1), inip=0,
+                     step_regu=100000000, dttype=1,
+                     xsph=(0.5, 0.1, 0.0), art_vis=((0.1, 0.0), (0.1, 0.0), (0.0, 0.0)),
+                     art_stre_coe=0.0, g=grav,
+                     interc=0.0, permtype=0, pers=0.0, perl=0.0, perm=0.0,
+                     ss=(0, 0.0, 0.0, 0), if_cal=0, if_move=0, coe_bndy=0.3),
+        water=[w, copy.deepcopy(w), copy.deepcopy(w)],
+        model_flags=(0, 0, 1, 0, 0, 0, 0, 0, 0, 0),
+        soils={2: dp},
+        vibration=vib,
+    )
+
+
 def add_rain(scene: Scene, x0: float, x1: float, rows: int, top: float, press_factor: float = 1.0,
              drop_velocity: float = -1.0) -> Scene:
     """Rain particles (type 7, etype 1: water waiting to fall) appended to
@@ -500,6 +591,18 @@ def write_input_dat(scene: Scene, path: str, ntd: int = 1) -> None:
     if P["if_move"] >= 1:
         add(" ".join(_f(v) for v in P.get("move_vx", (0.0, 0.0, 0.0))))
     add("E end")
+    if F["flv"] >= 1 and scene.vibration is not None:
+        vb = scene.vibration
+        add("VL vibration")
+        add("A data")
+        add(f"{_f(vb['ttime'])} {int(vb['nsteps'])}")
+        add(f"{_f(vb['sttime'])} {_f(vb['edtime'])}")
+        add("E end")
+        # the loads, one row of three per step, in vibra.dat beside the deck
+        # (initial_vib, CPP_2-initialf.cpp:292-320)
+        with open(os.path.join(os.path.dirname(os.path.abspath(path)), "vibra.dat"), "w") as fv:
+            for row in np.asarray(vb["loads"], dtype=np.float64).reshape(-1, 3):
+                fv.write(" ".join(_f(v) for v in row) + "\n")
     if F["flr"] == 1 and scene.rain is not None:
         rn = scene.rain
         add("RP rain")
@@ -676,6 +779,7 @@ class InitialState:
     fluid: np.ndarray     # (n, 12) records as sphgpu_fluid (structured dtype)
     soil: np.ndarray      # (n,) structured sphgpu_soil
     rain: dict | None = None   # sphgpu_rain members (flr = 1)
+    vibration: dict | None = None   # Para_Vibra: ttime nsteps sttime edtime loads (flv >= 1)
 
 
 FLUID_DTYPE = np.dtype([(k, np.int32 if k in ("bhtype", "press_type", "acc_type") else np.float64)
@@ -850,7 +954,8 @@ def initialise(scene: Scene) -> InitialState:
         rain = dict(scene.rain, nrain=int(np.count_nonzero((t == 7) & (et == 1))))
         if rain["nhor"] == 0:
             rain["nhor"] = 35
-    return InitialState(params=params, fields=f, fluid=fl, soil=so, rain=rain)
+    vib = scene.vibration if scene.flags.get("flv", 0) >= 1 else None
+    return InitialState(params=params, fields=f, fluid=fl, soil=so, rain=rain, vibration=vib)
 
 
 def kl_domain(scene: Scene) -> dict:

@@ -191,6 +191,11 @@ def kl_domain(nb_min, nb_max, soil_max, water_max) -> KLDomain:
     return d
 
 
+class Vibration(C.Structure):
+    """sphgpu_vibration: Para_Vibra without its loads."""
+    _fields_ = [("ttime", C.c_double), ("nsteps", C.c_int), ("sttime", C.c_double), ("edtime", C.c_double)]
+
+
 class RFFlags(C.Structure):
     """sphgpu_rf_flags: the Flag_SpatialVariability members the correlation-
     matrix generators read."""
@@ -265,6 +270,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_get_dt.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     lib.sphgpu_kl_generate.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_int, C.c_void_p,
                                        C.c_int, C.c_void_p]
+    lib.sphgpu_set_vibration.argtypes = [C.c_void_p, C.POINTER(Vibration), C.c_void_p]
     lib.sphgpu_rf_cells.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(RFFlags), C.POINTER(C.c_int)]
     lib.sphgpu_rf_generate.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_int,
                                        C.POINTER(RFFlags), C.c_void_p, C.c_int, C.c_void_p]
@@ -369,7 +375,7 @@ class Engine:
         """sphgpu_download_particles: the device-owned members of each record."""
         self._check(self.lib.sphgpu_download_particles(self.h, _ptr(records), self.n, stride), "download_particles")
 
-    def load_state(self, fields: dict, fluid=None, soil=None, rain=None) -> None:
+    def load_state(self, fields: dict, fluid=None, soil=None, rain=None, vibration=None) -> None:
         for name, v in fields.items():
             if name in FIELDS:
                 self.set_field(name, v)
@@ -377,6 +383,17 @@ class Engine:
             self.set_materials(fluid, soil)
         if rain is not None:
             self.set_rain(rain)
+        if vibration is not None:
+            self.set_vibration(vibration)
+
+    def set_vibration(self, vib: dict) -> None:
+        """sphgpu_set_vibration: Para_Vibra of a run with flv 1 or 2 (ttime,
+        nsteps, sttime, edtime and nsteps x 3 loads)."""
+        v = Vibration()
+        v.ttime, v.nsteps, v.sttime, v.edtime = float(vib["ttime"]), int(vib["nsteps"]), float(vib["sttime"]), \
+            float(vib["edtime"])
+        loads = np.ascontiguousarray(np.asarray(vib["loads"], dtype=np.float64).reshape(-1))
+        self._check(self.lib.sphgpu_set_vibration(self.h, C.byref(v), _ptr(loads)), "sphgpu_set_vibration")
 
     def kl_generate(self, domain: KLDomain, fields, xi, K: int = 200) -> np.ndarray:
         """SpatialVariables_Generate_2D / _3D with the standard normals xi

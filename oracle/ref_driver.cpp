@@ -15,6 +15,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <string>
+
 // The K-L generator's steps (solve_wi, solve_ramdai, solve_h_2D/3D) are
 // private members of clFSpatialVariability_Fun; this harness calls them
 // directly so that the standard-normal coefficients can be injected in place
@@ -35,6 +37,9 @@ struct RefRun {
     Para_Inter inter;
     Para_Boundary bou;
     Para_Vibra vib;
+    Para_Soil ffbound;                 // SPH_Calculation's pFFBound: never read from the deck
+    clFreeFieldBndy_Fun ffb;
+    clFreeFieldBndy_Fun_soil ffs;
     Para_GF gf;
     Para_EC ec;
     Para_SSInter ssi;
@@ -123,6 +128,17 @@ void* ref_create(const char* input_dat_path, int nthreads)
     if (err > 0) { g_last_error = err; fclose(finp); return nullptr; }
     r->ini.input_par(r->par, &r->pro, &r->cellc, &r->rain, r->flog, finp);
     fclose(finp);
+    // vibra.dat beside the deck, as SPH_Calculation opens it (CPP_1-SPHLoops.cpp:306-340)
+    if (r->fl.flv >= 1) {
+        std::string dir(input_dat_path);
+        const size_t slash = dir.find_last_of('/');
+        dir = (slash == std::string::npos) ? std::string(".") : dir.substr(0, slash);
+        FILE* fvib = fopen((dir + "/vibra.dat").c_str(), "r");
+        if (!fvib) { g_last_error = 1; delete r; return nullptr; }
+        err = r->ini.initial_vib(&r->vib, r->flog, fvib);
+        fclose(fvib);
+        if (err > 0) { g_last_error = err; delete r; return nullptr; }
+    }
     r->ini.setting_vis_cons(r->par, r->pro, r->vfluid, r->water, r->air, r->conspara, r->soil, r->structure);
     r->ini.setting_par(r->par, &r->pro, r->vfluid, r->conspara, r->soil, r->gf, r->structure, r->water, &r->rain, r->flog);
     r->nnps.celllist_ini1(&r->cellc, r->pro);
@@ -306,8 +322,15 @@ int ref_step(void* h, int nsteps)
         else if (F.flbndy == 3 || F.flbndy == 4 || F.flbndy == 13 || F.flbndy == 14)
             r->acc.boundary_stress_effect_tran(r->par, r->parcell, r->varibndy, P, F.ntd);
         else r->acc.boundary_effect_free_struct(r->par, r->parcell, P, F.ntd);
+        if (F.flv != 0) {
+            // free-field boundaries (CPP_1-SPHLoops.cpp:621-635) with
+            // SPH_Calculation's default-constructed pFFBound (:253)
+            r->ffb.free_field_solid(r->par, r->bndy, r->ffbound, r->parcell, P, F.ntd);
+            r->ffs.free_field_solid(r->par, r->conspara, r->parcell, P, F.ntd);
+        }
         if (r->ssi.type >= 1 && r->ssi.type <= 3 && r->ssi.acc_type == 2)
             r->acc.coupled_Water_Soil_Structure(r->par, r->parcell, r->vfluid, r->conspara, P, r->gf, F.ntd);
+        if (F.flv == 1) r->acc.vibration_acceleration(r->par, r->vib, P, F.ntd);
         if (F.fli == 1) r->itf.interact1(r->par, r->parcell, r->inter, r->vfluid, P, r->gf, F.ntd);
         else if (F.fli == 2) r->itf.interact2(r->par, r->parcell, r->inter, r->conspara, r->vfluid, P, r->gf, F.ntd);
         else if (F.fli == 3) r->itf.interact3(r->par, r->parcell, r->inter, r->conspara, r->vfluid, P, r->gf, F.ntd);
@@ -320,8 +343,10 @@ int ref_step(void* h, int nsteps)
             err = r->ssinter.interaction_ss_penalty(r->par, r->parcell, r->pair_ss, r->interf_ss, r->partipair, r->ssi, P, F.ntd);
         if (err > 0) return err;
         if (P.l <= P.inip) r->acc.soil_damping_geostress(r->par, r->parcell, P, F.ntd);
+        if (F.flv > 0) r->acc.soil_damping_vibration(r->par, r->parcell, r->conspara, r->stiff, P);
         if (F.flbndy == 5) r->bnd.boundary_free_solid(r->par, r->parcell, P, r->ssi, F.ntd);
         r->vel.veocity_update(r->par, P, r->bou, F.flv);
+        if (F.flv == 2) r->acc.vibration_velocity(r->par, r->vib, P, F.ntd);
         if (r->bou.if_move != 2) r->vel.xsph(r->par, r->parcell, r->bndy, r->varibndy, P, r->vx_temp, F.flbndy);
         if (F.flbndy == 1) r->bnd.tmboundary(r->par, r->parcell, r->bndy, P);
         else if (F.flbndy == 2) {

@@ -51,6 +51,12 @@ struct orc_ctx {
     sphgpu_rain rain;
     int rain_set, lp;
     double vrain;
+    /* vibration (flv 1, 2): Para_Vibra, and StiffMat::depp0's largest
+     * diagonal entry (the only part soil_damping_vibration reads) */
+    double vib_ttime, vib_sttime, vib_edtime;
+    int vib_nsteps, vib_set;
+    double* vib_loads;
+    double* stiff;
 };
 
 /* ------------------------------------------------------------------------- */
@@ -97,6 +103,7 @@ orc_ctx* orc_create(const sphgpu_params* p)
     }
     c->fl = (sphgpu_fluid*)calloc(n, sizeof(sphgpu_fluid));
     c->so = (sphgpu_soil*)calloc(n, sizeof(sphgpu_soil));
+    c->stiff = (double*)calloc(n, sizeof(double));      /* StiffMat(): depp0 = 0 (Class_particle.cpp:220-228) */
     for (int i = 0; i < n; i++) {
         c->fl[i].strain_min = 1.0;   /* Para_Fluid() (Class_ParticleProperty.cpp) */
         c->so[i].fs = 1.0;            /* Para_Soil()  */
@@ -132,7 +139,7 @@ void orc_destroy(orc_ctx* c)
 {
     if (!c) return;
     for (size_t f = 0; f < NFIELDS; f++) free(*(void**)((char*)c + k_fields[f].off));
-    free(c->fl); free(c->so); free(c->pc_cell_id); free(c->ninflu); free(c->influ); free(c->wij);
+    free(c->fl); free(c->so); free(c->stiff); free(c->vib_loads); free(c->pc_cell_id); free(c->ninflu); free(c->influ); free(c->wij);
     free(c->srt_cell); free(c->srt_pid); free(c->tmp_cell); free(c->tmp_pid);
     free(c->ci_start); free(c->ci_end); free(c->vx_temp); free(c->snap); free(c->rij);
     free(c);
@@ -1309,9 +1316,16 @@ static int strain_to_stress(orc_ctx* c)
             } else {
                 visco_elastic(ds, s, de, &c->so[i]);
             }
-            if (c->l < P->inip || mt != 7)
+            if (c->l < P->inip || mt != 7) {
                 for (int a = 0; a < 6; a++)
                     for (int b = 0; b < 6; b++) ds[a] += dept[a][b] * de[b];
+                /* depp0 = dept; its largest diagonal entry 0-2, as
+                 * soil_damping_vibration takes it (CPP_9-1:186-188) */
+                double st = fmax(0.0, dept[0][0]);
+                st = fmax(st, dept[1][1]);
+                st = fmax(st, dept[2][2]);
+                c->stiff[i] = st;
+            }
             if (!(c->l < P->inip) && (mt == 2 || mt == 5)) dp_check(s, ds, &c->so[i], dt);
             jaumann(ds, s, &c->weps[i * 9]);
             /* fractional_plastic for matype 8, 18, 28 (:255-258).  In elastic steps
@@ -1340,6 +1354,12 @@ static int strain_to_stress(orc_ctx* c)
             dept[3][3] = dmu; dept[4][4] = dmu; dept[5][5] = dmu;
             for (int a = 0; a < 6; a++)
                 for (int b = 0; b < 6; b++) ds[a] += dept[a][b] * de[b];
+            {
+                double st = fmax(0.0, dept[0][0]);
+                st = fmax(st, dept[1][1]);
+                st = fmax(st, dept[2][2]);
+                c->stiff[i] = st;
+            }
             jaumann(ds, s, &c->weps[i * 9]);
             for (int a = 0; a < 6; a++) {
                 ep[a] = ep[a] + de[a] * dt;
@@ -1953,6 +1973,152 @@ static void soil_damping_geostress(orc_ctx* c)
             double vx2 = vxp + 0.5 * (axp + *ax - damp[k]) * dt;
             if (vx1 * vx2 <= 0.0) *ax = -2.0 * vxp / dt - axp;
             else *ax -= damp[k];
+        }
+    }
+}
+
+/* ff_stress_2d_solid / _3d_solid: CPP_19-FreeFieldParticles.cpp:21-76 (the
+ * soil form's copy, CPP_19-FreeFieldParticles_soil.cpp:21-68, is the same) */
+static void ff_stress(int ndim, double* sg, const double* va, const double* vb, double e, double poi, double dens,
+                      int type)
+{
+    double g = e * 0.5 / (1 + poi);
+    double k = e * 0.333333333333333 / (1 - 2.0 * poi);
+    double c_p = sqrt((k + 4.0 * g * 0.333333333333333) / dens);
+    double c_s = sqrt(g / dens);
+    sg[0] = 0.0; sg[1] = 0.0; sg[2] = 0.0;
+    if (ndim == 2) {
+        if (type == 1) {
+            sg[0] = -c_p * dens * (va[0] - vb[0]);
+            sg[1] = -c_s * dens * (va[1] - vb[1]);
+        } else if (type == 2) {
+            sg[0] = -c_s * dens * (va[0] - vb[0]);
+            sg[1] = -c_p * dens * (va[1] - vb[1]);
+        }
+    } else {
+        if (type == 1) {
+            sg[0] = -c_p * dens * (va[0] - vb[0]);
+            sg[1] = -c_s * dens * (va[1] - vb[1]);
+            sg[2] = -c_s * dens * (va[2] - vb[2]);
+        } else if (type == 2) {
+            sg[0] = -c_s * dens * (va[0] - vb[0]);
+            sg[1] = -c_p * dens * (va[1] - vb[1]);
+            sg[2] = -c_s * dens * (va[2] - vb[2]);
+        } else if (type == 3) {
+            sg[0] = -c_s * dens * (va[0] - vb[0]);
+            sg[1] = -c_s * dens * (va[1] - vb[1]);
+            sg[2] = -c_p * dens * (va[2] - vb[2]);
+        }
+    }
+}
+
+/* free_field_solid of the walls: CPP_19-FreeFieldParticles.cpp:79-141.  The
+ * elastic constants are those of pFFBound, a default-constructed Para_Soil
+ * (e = poi = 0, CPP_1-SPHLoops.cpp:253; Class_ParticleProperty.cpp:28-31) */
+static void free_field_walls(orc_ctx* c)
+{
+    const int ndim = c->P.ndim;
+    const double e = 0.0, poi = 0.0;
+    for (int i = 0; i < c->n; i++) {
+        if (c->type[i] != 2) continue;
+        double t[3] = {0, 0, 0};
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj);
+            if (!(c->type[j] == 0 && c->matype[j] == 5)) continue;
+            double sg[3];
+            ff_stress(ndim, sg, &c->vx[i * 3], &c->interfss[j * 3], e, poi, c->rho[j], c->permtype[j]);
+            for (int k = 0; k < 3; k++) t[k] = t[k] + c->mass[j] / c->rho[j] * sg[k] / c->rho[i] * W(i, nj, k);
+        }
+        for (int k = 0; k < ndim; k++) c->ax[i * 3 + k] = c->ax[i * 3 + k] + t[k];
+    }
+}
+
+/* free_field_solid of the soil: CPP_19-FreeFieldParticles_soil.cpp:71-175,
+ * between soil of matype >= 50 (the free-field columns) and the rest */
+static void free_field_soil(orc_ctx* c)
+{
+    const int ndim = c->P.ndim;
+    for (int i = 0; i < c->n; i++) {
+        if (c->type[i] != 2) continue;
+        const int ff = c->matype[i] >= 50;
+        double t[3] = {0, 0, 0};
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj);
+            if (!(c->type[j] == 2 && (c->matype[j] >= 50) != ff)) continue;
+            double sg[3];
+            if (!ff)
+                ff_stress(ndim, sg, &c->vx[i * 3], &c->vx[j * 3], c->so[j].e, c->so[j].poi, c->rho[j], c->permtype[j]);
+            else
+                ff_stress(ndim, sg, &c->vx[j * 3], &c->vx[i * 3], c->so[i].e, c->so[i].poi, c->rho[i], c->permtype[i]);
+            for (int k = 0; k < 3; k++) t[k] = t[k] + c->mass[j] / c->rho[j] * sg[k] / c->rho[i] * W(i, nj, k);
+        }
+        for (int k = 0; k < ndim; k++) c->ax[i * 3 + k] = c->ax[i * 3 + k] + t[k];
+    }
+}
+
+/* the load of time t: 0 outside [sttime, edtime], else 1 (largest magnitude
+ * under 1000) or 2, the entry in v (CPP_9-1:21-35, 85-99) */
+static int vib_load(const orc_ctx* c, double* v)
+{
+    double time1 = c->t - c->vib_sttime, time2 = c->t - c->vib_edtime;
+    if (!(time1 >= 0.0 && time2 <= 0.0)) return 0;
+    double q = time1 / c->vib_ttime * (double)c->vib_nsteps;
+    int nstep = (q >= (double)(c->vib_nsteps - 1)) ? c->vib_nsteps - 1 : (int)q;
+    for (int k = 0; k < 3; k++) v[k] = c->vib_loads[nstep * 3 + k];
+    double m = fmax(0.0, fabs(v[0]));
+    m = fmax(m, fabs(v[1]));
+    m = fmax(m, fabs(v[2]));
+    return m < 1000.0 ? 1 : 2;
+}
+
+/* vibration_acceleration (CPP_9-1:10-78, flv 1, walls of matype 3 and 5) and
+ * vibration_velocity (CPP_9-1:80-160, flv 2, walls of matype 4 and 5) */
+static void vibration_load(orc_ctx* c, int velocity)
+{
+    const int ndim = c->P.ndim;
+    double v[3];
+    const int ld = vib_load(c, v);
+    for (int i = 0; i < c->n; i++) {
+        const int m = c->matype[i];
+        if (c->type[i] != 0 || !(m == (velocity ? 4 : 3) || m == 5)) continue;
+        for (int k = 0; k < ndim; k++) {
+            if (ld == 1) {
+                if (velocity) c->interfss[i * 3 + k] = v[k];
+                else c->interf[i * 3 + k] = v[k];
+            } else {
+                c->interf[i * 3 + k] = 0.0;
+                c->interfss[i * 3 + k] = 0.0;
+            }
+        }
+    }
+}
+
+/* soil_damping_vibration: CPP_9-1-acceleration_vibration.cpp:162-224 */
+static void soil_damping_vibration(orc_ctx* c)
+{
+    const int ndim = c->P.ndim;
+    const double dt = c->P.dt;
+    for (int i = 0; i < c->n; i++) {
+        if (!(c->type[i] == 2 || c->type[i] == 4)) continue;
+        double damp[3] = {0, 0, 0}, tempdown = 0.0;
+        const double stiff = c->stiff[i];
+        const double cd = c->so[i].damp1 + c->so[i].damp2 * sqrt(stiff / c->rhop[i] / c->hl[i] / c->hl[i]);
+        for (int nj = 1; nj <= c->ninflu[i]; nj++) {
+            int j = NBR(i, nj);
+            if (c->type[i] == c->type[j]) {
+                for (int k = 0; k < ndim; k++)
+                    damp[k] = damp[k] + c->mass[j] / c->rho[j] * cd * (c->vxp[i * 3 + k] - c->vxp[j * 3 + k]) * W(i, nj, 3);
+                tempdown = tempdown + c->mass[j] / c->rho[j] * W(i, nj, 3);
+            }
+        }
+        for (int k = 0; k < ndim; k++) {
+            if (fabs(tempdown) < 1.0e-7) tempdown = 1.0e-7;
+            double* ax = &c->ax[i * 3 + k];
+            double axp = c->axp[i * 3 + k], vxp = c->vxp[i * 3 + k];
+            double vx1 = vxp + 0.5 * (axp + *ax) * dt;
+            double vx2 = vxp + 0.5 * (axp + *ax - damp[k] / tempdown) * dt;
+            if (vx1 * vx2 <= 0.0) *ax = -2.0 * vxp / dt - axp;
+            else *ax -= damp[k] / tempdown;
         }
     }
 }
@@ -2807,6 +2973,18 @@ int orc_set_rain(orc_ctx* c, const sphgpu_rain* rain)
     return 0;
 }
 
+int orc_set_vibration(orc_ctx* c, double ttime, int nsteps, double sttime, double edtime, const double* loads)
+{
+    if (nsteps < 1) return 7;
+    if (!loads || !(ttime > 0.0)) return SPHGPU_E_ARG;
+    free(c->vib_loads);
+    c->vib_loads = (double*)malloc(sizeof(double) * 3 * (size_t)nsteps);
+    memcpy(c->vib_loads, loads, sizeof(double) * 3 * (size_t)nsteps);
+    c->vib_ttime = ttime; c->vib_nsteps = nsteps; c->vib_sttime = sttime; c->vib_edtime = edtime;
+    c->vib_set = 1;
+    return 0;
+}
+
 int orc_get_rain(const orc_ctx* c, sphgpu_rain* rain)
 {
     if (!rain) return SPHGPU_E_ARG;
@@ -2867,7 +3045,7 @@ static int check_supported(const sphgpu_params* P)
 {
     if (!(P->flbndy >= 1 && P->flbndy <= 5) && P->flbndy != 13 && P->flbndy != 14) return SPHGPU_E_UNSUPPORTED;
     if (P->flknl < 1 || P->flknl > 4) return SPHGPU_E_UNSUPPORTED;
-    if (P->flv != 0) return SPHGPU_E_UNSUPPORTED;
+    if (P->flv < 0 || P->flv > 2) return SPHGPU_E_UNSUPPORTED;
     if (P->fli < 0 || P->fli > 3 || P->ss_type < 0 || P->ss_type > 3) return SPHGPU_E_UNSUPPORTED;
     return 0;
 }
@@ -2879,6 +3057,7 @@ int orc_step(orc_ctx* c, int nsteps)
     int err = check_supported(P);
     if (err) return err;
     if (P->flr == 1 && !c->rain_set) return SPHGPU_E_STATE;
+    if (P->flv >= 1 && !c->vib_set) return SPHGPU_E_STATE;
     for (int s = 0; s < nsteps; s++) {
         c->t = c->t + P->dt;
         if (P->flr == 1 && (c->l - P->inip) > 0 && c->lp > 0 && (c->l - P->inip) % c->lp == 0) rainpro(c);
@@ -2904,15 +3083,19 @@ int orc_step(orc_ctx* c, int nsteps)
         structure_acceleration(c);
         artificial_viscosity(c);
         if (P->art_stre_coe > 0.0) artificial_stress(c);
-        if (P->flbndy == 1 || P->flbndy == 2) boundary_moving_stress_effect(c);   /* flv == 0 */
+        if (P->flbndy == 1 || P->flbndy == 2) boundary_moving_stress_effect(c);
         else if (P->flbndy == 3 || P->flbndy == 4 || P->flbndy == 13 || P->flbndy == 14) boundary_stress_effect_tran(c);
         else boundary_effect_free_struct(c);
+        if (P->flv != 0) { free_field_walls(c); free_field_soil(c); }
         if (P->ss_type >= 1 && P->ss_type <= 3 && P->ss_acc_type == 2) coupled_water_soil_structure(c);
+        if (P->flv == 1) vibration_load(c, 0);
         if (P->fli >= 1) interact(c, P->fli);
         if (P->ss_type >= 1 && P->ss_type <= 3) interaction_ss(c);
         if (c->l <= P->inip) soil_damping_geostress(c);
+        if (P->flv > 0) soil_damping_vibration(c);
         if (P->flbndy == 5) boundary_free_solid(c);
         velocity_update(c);
+        if (P->flv == 2) vibration_load(c, 1);
         if (P->if_move != 2) xsph(c);
         if (P->flbndy == 1) tmboundary(c);
         else if (P->flbndy == 2) { velocity_set_domain(c); tm_boundary(c); }

@@ -57,6 +57,9 @@ int      orc_step(orc_ctx* c, int nsteps);
 /* rainfall (flr == 1): the Para_Rain record, and its nrain as the steps leave it */
 int      orc_set_rain(orc_ctx* c, const sphgpu_rain* rain);
 int      orc_get_rain(const orc_ctx* c, sphgpu_rain* rain);
+/* the vibration table (flv 1, 2): Para_Vibra's ttime, nsteps, sttime, edtime
+ * and nsteps x 3 loads; 7 for nsteps < 1, as initial_pro */
+int      orc_set_vibration(orc_ctx* c, double ttime, int nsteps, double sttime, double edtime, const double* loads);
 
 #ifdef __cplusplus
 }

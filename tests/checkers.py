@@ -107,13 +107,20 @@ class Oracle:
         sp = _ptr(np.ascontiguousarray(soil)) if soil is not None else None
         assert self.lib.orc_set_materials(self.h, fp, sp, self.n) == 0
 
-    def load_state(self, fields, fluid=None, soil=None, rain=None):
+    def load_state(self, fields, fluid=None, soil=None, rain=None, vibration=None):
         for name, v in fields.items():
             if name in ORACLE_FIELDS:
                 self.set_field(name, v)
         self.set_materials(fluid, soil)
         if rain is not None:
             self.set_rain(rain)
+        if vibration is not None:
+            self.set_vibration(vibration)
+
+    def set_vibration(self, vib: dict) -> int:
+        loads = np.ascontiguousarray(np.asarray(vib["loads"], dtype=np.float64).reshape(-1))
+        return self.lib.orc_set_vibration(self.h, C.c_double(vib["ttime"]), C.c_int(int(vib["nsteps"])),
+                                          C.c_double(vib["sttime"]), C.c_double(vib["edtime"]), _ptr(loads))
 
     def step(self, nsteps=1):
         return self.lib.orc_step(self.h, int(nsteps))

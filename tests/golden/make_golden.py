@@ -301,6 +301,11 @@ CASES = {
         _geostatic(lambda: scenes.soil_column_3d(dx=0.1, steps=200), 6, camclay=True, step_regu=4), 12),
     "slope_2d_H1_dx0.05_geostatic": (_geostatic(lambda: scenes.slope_2d(H=1.0, dx=0.05), 8), 16),
     "dam_break_2d_dx0.04_rain": (_rain(), 35),
+    # vibration (flv 1, 2): a shaking base, free-field columns, soil damping
+    "shaking_box_2d_flv1": (lambda: scenes.shaking_box(ndim=2, flv=1, dx=0.05), 36),
+    "shaking_box_2d_flv2": (lambda: scenes.shaking_box(ndim=2, flv=2, dx=0.05), 36),
+    "shaking_box_3d_flv1": (lambda: scenes.shaking_box(ndim=3, flv=1, dx=0.1), 24),
+    "shaking_box_3d_flv2": (lambda: scenes.shaking_box(ndim=3, flv=2, dx=0.1), 24),
 }
 
 
@@ -484,6 +489,10 @@ def make(name: str) -> str:
         scenes.write_input_dat(sc, path)
         ref = Reference(path, 1)
         out["params"] = np.frombuffer(bytes(ref.params), dtype=np.uint8)
+        if sc.flags.get("flv", 0) >= 1:
+            vb = sc.vibration
+            out["vib_par"] = np.array([vb["ttime"], vb["nsteps"], vb["sttime"], vb["edtime"]])
+            out["vib_loads"] = np.asarray(vb["loads"], dtype=np.float64)
         if sc.flags.get("flr", 0) == 1:
             rn = ref.rain()
             out["rain"] = np.array([rn["rtype"], rn["nrain"], rn["nhor"], rn["press_factor"], rn["drop_velocity"]])

@@ -55,7 +55,7 @@ def test_unsupported_flags_rejected():
     lib = sphgpu.load_library()
     import scenes
     st = scenes.initialise(scenes.dam_break_2d(dx=0.04, steps=10))
-    for key, val in (("flbndy", 6), ("ss_type", 4), ("flv", 1), ("if_move", 4), ("flknl", 5)):
+    for key, val in (("flbndy", 6), ("ss_type", 4), ("flv", 3), ("flv", -1), ("if_move", 4), ("flknl", 5)):
         d = dict(st.params)
         d[key] = val
         p = sphgpu.params_from_dict(d)

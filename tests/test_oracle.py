@@ -30,7 +30,8 @@ CASES = ["dam_break_2d_dx0.04", "soil_column_3d_dx0.1", "soil_column_3d_dx0.1_kg
          "dam_break_2d_dx0.04_minor", "dam_break_2d_dx0.04_bingham", "dam_break_2d_dx0.04_moving_wall",
          "soil_column_3d_dx0.1_moving_wall", "soil_column_3d_dx0.1_geostatic",
          "soil_column_3d_dx0.1_geostatic_camclay", "slope_2d_H1_dx0.05_geostatic",
-         "dam_break_2d_dx0.04_rain"]
+         "dam_break_2d_dx0.04_rain", "shaking_box_2d_flv1", "shaking_box_2d_flv2", "shaking_box_3d_flv1",
+         "shaking_box_3d_flv2"]
 
 
 def _golden(name):
@@ -48,9 +49,18 @@ def golden_rain(g):
                 drop_velocity=float(r[4]))
 
 
+def golden_vibration(g):
+    """The vibration table a golden case was made with (None without)."""
+    if "vib_par" not in g:
+        return None
+    v = g["vib_par"]
+    return dict(ttime=float(v[0]), nsteps=int(v[1]), sttime=float(v[2]), edtime=float(v[3]), loads=g["vib_loads"])
+
+
 def _oracle_from_golden(g, p, mode=ORC_INPLACE, pow_mode=ORC_POW_LIBM):
     orc = Oracle(p, mode, pow_mode)
-    orc.load_state({k: g["init_" + k] for k in STATE_FIELDS}, g["fluid"], g["soil"], golden_rain(g))
+    orc.load_state({k: g["init_" + k] for k in STATE_FIELDS}, g["fluid"], g["soil"], golden_rain(g),
+                   golden_vibration(g))
     return orc
 
 
