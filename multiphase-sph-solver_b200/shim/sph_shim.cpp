@@ -3,11 +3,12 @@
 // A drop-in for the hot-path translation units of MultiPhase-SPH-Solver
 // (CPP_3-NNPS, CPP_6-density, CPP_7-1/7-2/7-3, CPP_8-x, CPP_9-3/9-4/9-5,
 // CPP_10/10-1, CPP_11, CPP_12-1, CPP_13): it defines the public methods of
-// clNNPS_Fun, clDensity_Fun, clStraStre_Fun, clInterFor_Fun, clAcce_Fun (all
-// but the vibration methods of CPP_9-1), clVel_Fun, clUpdate_Fun::update,
-// clBndy_Fun and clSoilStruct_Fun with the signatures of the reference's own
-// Class_Functions.h (:41-185, :242-253), which this file includes from the
-// caller's source tree.  SPH_Calculation (CPP_1-SPHLoops.cpp) then links
+// clNNPS_Fun, clDensity_Fun, clStraStre_Fun, clInterFor_Fun, clAcce_Fun (the
+// vibration methods of CPP_9-1 included), clVel_Fun, clUpdate_Fun::update,
+// clBndy_Fun, clSoilStruct_Fun and the free-field classes of CPP_19
+// (clFreeFieldBndy_Fun, clFreeFieldBndy_Fun_soil) with the signatures of the
+// reference's own Class_Functions.h (:41-185, :242-253, :278-296), which this
+// file includes from the caller's source tree.  SPH_Calculation (CPP_1-SPHLoops.cpp) then links
 // against it unchanged and runs its time steps on the GPU through the sphgpu
 // C ABI (include/sphgpu.h).
 //
@@ -90,6 +91,8 @@ struct ShimRun {
     bool mats_sent = false;
     int pending = 0;                  // an error of the last update, for the next parttocell
     bool sync_always = false;
+    const Para_Vibra* vib = nullptr;  // the vibration table the vibration methods were handed
+    bool vib_sent = false;
 };
 
 ShimRun g_run;
@@ -198,6 +201,8 @@ int ensure_context(Particle* par, const Cell_Con& cc, const Para_Pro& pro)
         P.cxm = keep.cxm; P.cym = keep.cym; P.czm = keep.czm; P.ctotal = keep.ctotal;
         g_run.fluid = nullptr;
         g_run.soil = nullptr;
+        g_run.vib = nullptr;
+        g_run.vib_sent = false;
         // what the methods of the first step have not told yet: the
         // reference's defaults (velocity-correction walls, the cubic spline,
         // the free-surface thresholds of CPP_1-SPHLoops.cpp:83-84)
@@ -436,6 +441,30 @@ void clAcce_Fun::coupled_Water_Soil_Structure(Particle*, Par_Cell*, const Para_F
 }
 
 void clAcce_Fun::soil_damping_geostress(Particle*, Par_Cell*, const Para_Pro&, int) {}
+
+// vibration (flv 1, 2): the table is handed to the engine with the step's
+// parameters; the loads, the damping and the free-field terms run inside the
+// step
+void clAcce_Fun::vibration_acceleration(Particle*, const Para_Vibra& pPVib, const Para_Pro&, int) { g_run.vib = &pPVib; }
+void clAcce_Fun::vibration_velocity(Particle*, const Para_Vibra& pPVib, const Para_Pro&, int) { g_run.vib = &pPVib; }
+void clAcce_Fun::soil_damping_vibration(Particle*, Par_Cell*, const Para_Soil* pParti_ConsPara, StiffMat*,
+                                        const Para_Pro&)
+{
+    g_run.soil = pParti_ConsPara;
+}
+
+// ------------------------------------------------------ free-field boundaries
+
+void clFreeFieldBndy_Fun::free_field_solid(Particle*, cl_bndy_pair*, const Para_Soil, Par_Cell*, const Para_Pro&,
+                                           int)
+{
+}
+
+void clFreeFieldBndy_Fun_soil::free_field_solid(Particle*, const Para_Soil* pParti_ConsPara, Par_Cell*,
+                                                const Para_Pro&, int)
+{
+    g_run.soil = pParti_ConsPara;
+}
 void clAcce_Fun::boundary_stress_effect_tran(Particle*, Par_Cell*, clVar_Boundary*, const Para_Pro&, int) {}
 
 // ---------------------------------------------------------- clSoilStruct_Fun
@@ -516,6 +545,13 @@ void clUpdate_Fun::update(Particle* pPar, const Para_Pro& pPPro, const Para_Boun
         rc = sphgpu_update_params(g_run.ctx, &P);
         if (rc) shim_fail("sphgpu_update_params", rc);
         else g_run.pushed = P;
+    }
+    if (!rc && P.flv >= 1 && g_run.vib && !g_run.vib_sent) {
+        const Para_Vibra& v = *g_run.vib;
+        const sphgpu_vibration vb = {v.ttime, v.nsteps, v.sttime, v.edtime};
+        rc = sphgpu_set_vibration(g_run.ctx, &vb, v.loads ? &v.loads[0][0] : nullptr);
+        if (rc) shim_fail("sphgpu_set_vibration", rc);
+        else g_run.vib_sent = true;
     }
     if (!rc && !g_run.mats_sent) {
         rc = sphgpu_set_materials(g_run.ctx, reinterpret_cast<const sphgpu_fluid*>(g_run.fluid),

@@ -53,6 +53,8 @@ CASES = {
     "geostatic": (make_golden.CASES["soil_column_3d_dx0.1_geostatic"][0], 10, 0.0),
     "drag_peng": (make_golden.CASES["soil_column_3d_dx0.1_drag_peng"][0], 8, 1e-12),
     "kgc_regu": (make_golden.CASES["soil_column_3d_dx0.1_kgc_regu"][0], 8, 0.0),
+    "shaking_box_2d_flv1": (make_golden.CASES["shaking_box_2d_flv1"][0], 20, 0.0),
+    "shaking_box_3d_flv2": (make_golden.CASES["shaking_box_3d_flv2"][0], 15, 0.0),
 }
 
 
@@ -93,16 +95,18 @@ def test_shim_step_loop_matches_oracle(name, sync, monkeypatch):
     the oracle's.  sync 'output': the shim downloads only on output steps
     (the last step is one here); 'always': upload and download every step."""
     factory, steps, tol = CASES[name]
+    sc = factory()
     if sync == "always":
         monkeypatch.setenv("SPHGPU_SHIM_SYNC", "always")
-        path = _deck(factory(), steps, 100000)
+        path = _deck(sc, steps, 100000)
     else:
         monkeypatch.delenv("SPHGPU_SHIM_SYNC", raising=False)
-        path = _deck(factory(), steps, steps)
+        path = _deck(sc, steps, steps)
     shim = Reference(path, 1, so=SHIM_SO)
     fl, so = shim.materials()
     orc = Oracle(shim.params, ORC_JACOBI, ORC_POW_CR)
-    orc.load_state({k: shim.get_field(k) for k in STATE_FIELDS}, fl, so)
+    orc.load_state({k: shim.get_field(k) for k in STATE_FIELDS}, fl, so,
+                   vibration=sc.vibration if sc.flags.get("flv", 0) >= 1 else None)
     for chunk in (1, steps - 1):
         assert shim.step(chunk) == 0
         assert orc.step(chunk) == 0
