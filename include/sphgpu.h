@@ -345,6 +345,21 @@ int sphgpu_checkpoint_load(sphgpu_ctx* ctx, const char* path);
  */
 int sphgpu_output_total(sphgpu_ctx* ctx, const char* dir);
 int sphgpu_output_wait(sphgpu_ctx* ctx);
+/*
+ * The other result files of SPH_Calculation's output steps
+ * (CPP_1-SPHLoops.cpp:761-780), from the same snapshot: sphgpu_output_step
+ * writes the files `what` selects, the data-*.odb of output_total included,
+ * and appends to the run's files in call order.  sphgpu_output_begin creates
+ * dir's "Flowing distance.dat", Total_Force.dat and AVS_MGF.mgf (with the AVS
+ * header and the frame count loop / fop) as SPH_Calculation opens them
+ * before its loop (:185-230, 452-453).
+ */
+#define SPHGPU_OUT_ODB      1   /* data-<l>.odb (output_total, CPP_14-2-output.cpp:15-136) */
+#define SPHGPU_OUT_FLOWDIST 2   /* each phase's extent, appended to "Flowing distance.dat" (output_flowdist, :222-320) */
+#define SPHGPU_OUT_IMPACT   4   /* Impact-force<l>.inp and a Total_Force.dat line (output_impact, :139-220) */
+#define SPHGPU_OUT_MGF      8   /* a frame appended to AVS_MGF.mgf (mgf, CPP_14-1-outmgf.cpp:12-104) */
+int sphgpu_output_begin(sphgpu_ctx* ctx, const char* dir);
+int sphgpu_output_step(sphgpu_ctx* ctx, const char* dir, int what);
 
 /* Block until the context's stream is idle; returns the sticky error, if any. */
 int sphgpu_synchronize(sphgpu_ctx* ctx);

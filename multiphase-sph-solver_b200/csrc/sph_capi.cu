@@ -15,7 +15,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <condition_variable>
 #include <functional>
+#include <mutex>
 #include <thread>
 #include <utility>
 #include <vector>
@@ -167,6 +169,12 @@ struct sphgpu_ctx {
     std::thread out_th[2];
     int out_next = 0;
     int out_err = 0;
+    // the files several steps append to are appended in call order: each
+    // call takes a ticket, and its thread appends when the tickets before it
+    // have
+    std::mutex out_mu;
+    std::condition_variable out_cv;
+    long out_ticket = 0, out_turn = 0;
     std::vector<InstGrid> h_inst;     // batched context: the instance table (empty: one system)
     InstGrid* d_inst = nullptr;
 };
@@ -1637,11 +1645,168 @@ int write_odb(const char* dir, int l, const double* rows, int n)
     return ok ? 0 : SPHGPU_E_ARG;
 }
 
+// the ten-character step number of output_impact's file name
+// (CPP_14-2-output.cpp:150-181): zero-padded below 1e8, empty from there on
+std::string step10(int l)
+{
+    if (l < 0 || l >= 100000000) return std::string();
+    char b[16];
+    std::snprintf(b, sizeof(b), "%010d", l);
+    return std::string(b);
+}
+
+// output_flowdist (CPP_14-2-output.cpp:222-320): each phase's extent per axis,
+// appended to "Flowing distance.dat"
+int append_flowdist(const char* dir, int l, const double* rows, int n)
+{
+    double mx[4][3], mn[4][3];
+    for (int p = 0; p < 4; p++)
+        for (int k = 0; k < 3; k++) { mn[p][k] = 10000.0; mx[p][k] = -10000.0; }
+    for (int i = 0; i < n; i++) {
+        const double* o = rows + (size_t)i * kOutCols;
+        const int t = (int)o[47];
+        if (t < 1 || t > 4) continue;
+        for (int k = 0; k < 3; k++) {
+            mx[t - 1][k] = std::fmax(o[k], mx[t - 1][k]);
+            mn[t - 1][k] = std::fmin(o[k], mn[t - 1][k]);
+        }
+    }
+    for (int p = 0; p < 4; p++)
+        for (int k = 0; k < 3; k++) {
+            if (std::fabs(mn[p][k] - 10000.0) < 0.0001) mn[p][k] = 0.0;
+            if (std::fabs(mx[p][k] + 10000.0) < 0.0001) mx[p][k] = 0.0;
+        }
+    const std::string path = std::string(dir) + "/Flowing distance.dat";
+    FILE* f = std::fopen(path.c_str(), "a");
+    if (!f) return SPHGPU_E_ARG;
+    std::fprintf(f, "\nStep%9d            X                       Y                      Z\n", l);
+    std::fprintf(f, "-----------------------------------------------------------------------------------\n");
+    std::fprintf(f, "                  max           min        max         min        max         min   \n");
+    static const char* kRow[4] = {"Water Phase:   ", "Soil Phase:    ", "Air Phase:     ", "Structure:      "};
+    for (int p = 0; p < 4; p++)
+        std::fprintf(f, "%s%5.3e    %5.3e   %5.3e   %5.3e   %5.3e   %5.3e \n", kRow[p], mx[p][0], mn[p][0], mx[p][1],
+                     mn[p][1], mx[p][2], mn[p][2]);
+    return std::fclose(f) == 0 ? 0 : SPHGPU_E_ARG;
+}
+
+// output_impact (CPP_14-2-output.cpp:139-220): the walls of matype >= 1 into
+// Impact-force<l>.inp, their force sum prew dr^(ndim-1) as a line of
+// Total_Force.dat
+int write_impact(const char* dir, int l, const double* rows, int n, int ndim, double dr)
+{
+    const std::string path = std::string(dir) + "/Impact-force" + step10(l) + ".inp";
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) return SPHGPU_E_ARG;
+    std::fprintf(f, "No.  X   Y  Z  Pre_Dens  Pre_water  Pre_Air  SIGXX  SIGYY  SIGZZ  SIGXY  SIGYZ  SIGZX\n");
+    int row = 1;
+    double total_f = 0.0;
+    for (int i = 0; i < n; i++) {
+        const double* o = rows + (size_t)i * kOutCols;
+        if (!((int)o[47] == 0 && (int)o[48] >= 1)) continue;
+        std::fprintf(f, "%5d %14.6e %14.6e %14.6e %14.6e %14.6e %14.6e %14.6e %14.6e %14.6e %14.6e %14.6e %14.6e \n",
+                     row, o[0], o[1], o[2], o[13], o[15], o[14], o[16], o[17], o[18], o[19], o[20], o[21]);
+        row += 1;
+        total_f += o[15] * std::pow(dr, ndim - 1);
+    }
+    bool ok = std::fclose(f) == 0;
+    const std::string tot = std::string(dir) + "/Total_Force.dat";
+    FILE* g = std::fopen(tot.c_str(), "a");
+    if (!g) return SPHGPU_E_ARG;
+    std::fprintf(g, "Step%9d, Total force is %14.6e N\n", l, total_f);
+    ok = (std::fclose(g) == 0) && ok;
+    return ok ? 0 : SPHGPU_E_ARG;
+}
+
+// mgf (CPP_14-1-outmgf.cpp:12-104): a frame of AVS_MGF.mgf -- the cell box's
+// edges, then one sphere of radius 1.1 dr per particle of types 0-4 and 7 in
+// its phase's colour (the count line says every particle)
+int append_mgf(const char* dir, int l, int fop, const double* rows, int n, int ndim, double dr0, const double bmin[3],
+               const double bmax[3])
+{
+    const std::string path = std::string(dir) + "/AVS_MGF.mgf";
+    FILE* f = std::fopen(path.c_str(), "a");
+    if (!f) return SPHGPU_E_ARG;
+    const double dr = 1.1 * dr0;
+    std::fprintf(f, "step%d\n", (int)(l / fop));
+    auto edge = [&](double x, double y, double z) {
+        std::fprintf(f, "%6.4f %6.4f %6.4f %6.4f %6.4f %6.4f\n", x, y, z, 0.5, 0.5, 0.5);
+    };
+    if (ndim == 2) {
+        std::fprintf(f, " disjoint line\n boundary\n color\n 8\n");
+        const double c2[8][2] = {{bmin[0], bmin[1]}, {bmax[0], bmin[1]}, {bmax[0], bmin[1]}, {bmax[0], bmax[1]},
+                                 {bmax[0], bmax[1]}, {bmin[0], bmax[1]}, {bmin[0], bmax[1]}, {bmin[0], bmin[1]}};
+        for (int q = 0; q < 8; q++) edge(c2[q][0], c2[q][1], 0.0);
+    } else if (ndim == 3) {
+        std::fprintf(f, " disjoint line\n boundary\n color\n 24\n");
+        // bottom, top (the bottom's square at zmax), then the four verticals
+        const double sq[8][2] = {{bmin[0], bmin[1]}, {bmax[0], bmin[1]}, {bmax[0], bmin[1]}, {bmax[0], bmax[1]},
+                                 {bmax[0], bmax[1]}, {bmin[0], bmax[1]}, {bmin[0], bmax[1]}, {bmin[0], bmin[1]}};
+        for (int q = 0; q < 8; q++) edge(sq[q][0], sq[q][1], bmin[2]);
+        for (int q = 0; q < 8; q++) edge(sq[q][0], sq[q][1], bmax[2]);
+        const double vt[4][2] = {{bmin[0], bmin[1]}, {bmax[0], bmin[1]}, {bmax[0], bmax[1]}, {bmin[0], bmax[1]}};
+        for (int q = 0; q < 4; q++) { edge(vt[q][0], vt[q][1], bmin[2]); edge(vt[q][0], vt[q][1], bmax[2]); }
+    }
+    std::fprintf(f, " sphere\n particles\n color\n %d\n", n);
+    // the particle lines, formatted in parallel chunks and written in order
+    const int chunk = 65536;
+    const int nchunk = (n + chunk - 1) / chunk;
+    std::vector<std::string> text(nchunk);
+    par_for((size_t)nchunk, [&](size_t a, size_t b) {
+        char line[256];
+        for (size_t q = a; q < b; q++) {
+            std::string& out = text[q];
+            const int i0 = (int)q * chunk, i1 = std::min(n, i0 + chunk);
+            for (int i = i0; i < i1; i++) {
+                const double* o = rows + (size_t)i * kOutCols;
+                double r, g, bl;
+                switch ((int)o[47]) {
+                case 0: r = 0.80; g = 0.80; bl = 0.80; break;
+                case 1: r = 0.2; g = 0.47; bl = 0.87; break;
+                case 2: r = 0.87; g = 0.87; bl = 0.2; break;
+                case 3: r = 0.0; g = 1.0; bl = 0.67; break;
+                case 4: r = 0.73; g = 0.47; bl = 0.07; break;
+                case 7: r = 0.5; g = 0.5; bl = 0.5; break;
+                default: continue;
+                }
+                const int len = std::snprintf(line, sizeof(line), "%6.4f %6.4f %6.4f %6.4f %6.4f %6.4f %6.4f\n", o[0],
+                                              o[1], o[2], dr, r, g, bl);
+                out.append(line, (size_t)len);
+            }
+        }
+    });
+    bool ok = true;
+    for (const std::string& t : text) ok = ok && std::fwrite(t.data(), 1, t.size(), f) == t.size();
+    if (std::fclose(f) != 0) ok = false;
+    return ok ? 0 : SPHGPU_E_ARG;
+}
+
 }  // namespace
 
-int sphgpu_output_total(sphgpu_ctx* c, const char* dir)
+int sphgpu_output_begin(sphgpu_ctx* c, const char* dir)
 {
     if (!c || !dir || std::strlen(dir) > 900) return SPHGPU_E_ARG;
+    // the files SPH_Calculation opens before its loop (CPP_1-SPHLoops.cpp:
+    // 185-230), with the AVS header it writes (:452-453)
+    const std::string d(dir);
+    FILE* f = std::fopen((d + "/Flowing distance.dat").c_str(), "w");
+    if (!f) return SPHGPU_E_ARG;
+    std::fclose(f);
+    f = std::fopen((d + "/Total_Force.dat").c_str(), "w");
+    if (!f) return SPHGPU_E_ARG;
+    std::fclose(f);
+    f = std::fopen((d + "/AVS_MGF.mgf").c_str(), "w");
+    if (!f) return SPHGPU_E_ARG;
+    std::fprintf(f, "# Micro AVS Geom:2.10\n# SPH simulation\n");
+    std::fprintf(f, "%d\n", (int)(c->P.loop / c->P.fop));
+    return std::fclose(f) == 0 ? 0 : SPHGPU_E_ARG;
+}
+
+int sphgpu_output_total(sphgpu_ctx* c, const char* dir) { return sphgpu_output_step(c, dir, SPHGPU_OUT_ODB); }
+
+int sphgpu_output_step(sphgpu_ctx* c, const char* dir, int what)
+{
+    if (!c || !dir || std::strlen(dir) > 900) return SPHGPU_E_ARG;
+    if (what & ~(SPHGPU_OUT_ODB | SPHGPU_OUT_FLOWDIST | SPHGPU_OUT_IMPACT | SPHGPU_OUT_MGF)) return SPHGPU_E_ARG;
     if (c->sticky) return c->sticky;
     if (c->part_done) return SPHGPU_E_STATE;          // between steps only
     cudaSetDevice(c->device);
@@ -1663,16 +1828,29 @@ int sphgpu_output_total(sphgpu_ctx* c, const char* dir)
     CK(cudaStreamWaitEvent(c->out_st, c->out_ev[slot], 0));
     CK(cudaMemcpyAsync(c->out_host[slot], c->out_dev[slot], bytes, cudaMemcpyDeviceToHost, c->out_st));
     CK(cudaEventRecord(c->out_ev[slot], c->out_st));
-    const int l = c->l_host - 1, n = c->N, dev = c->device;
+    const int l = c->l_host - 1, n = c->N, dev = c->device, nd = c->P.ndim, fop = c->P.fop;
+    const double dr = c->P.dr;
+    const double bmin[3] = {c->P.xmin, c->P.ymin, c->P.zmin}, bmax[3] = {c->P.xmax, c->P.ymax, c->P.zmax};
     std::string where(dir);
     double* host = c->out_host[slot];
     cudaEvent_t ev = c->out_ev[slot];
-    int* err = &c->out_err;
+    const long ticket = c->out_ticket++;
     c->out_th[slot] = std::thread([=]() {
         cudaSetDevice(dev);
         int rc = (cudaEventSynchronize(ev) == cudaSuccess) ? 0 : SPHGPU_E_CUDA;
-        if (!rc) rc = write_odb(where.c_str(), l, host, n);
-        if (rc && *err == 0) *err = rc;
+        if (!rc && (what & SPHGPU_OUT_ODB)) rc = write_odb(where.c_str(), l, host, n);
+        // the appended files in call order (every ticket takes its turn,
+        // also after an error)
+        std::unique_lock<std::mutex> lk(c->out_mu);
+        c->out_cv.wait(lk, [&] { return c->out_turn == ticket; });
+        if (!rc && (what & SPHGPU_OUT_FLOWDIST)) rc = append_flowdist(where.c_str(), l, host, n);
+        if (!rc && (what & SPHGPU_OUT_IMPACT)) rc = write_impact(where.c_str(), l, host, n, nd, dr);
+        if (!rc && (what & SPHGPU_OUT_MGF) && fop > 0)
+            rc = append_mgf(where.c_str(), l, fop, host, n, nd, dr, bmin, bmax);
+        if (rc && c->out_err == 0) c->out_err = rc;
+        c->out_turn++;
+        lk.unlock();
+        c->out_cv.notify_all();
     });
     c->out_next ^= 1;
     return 0;

@@ -191,6 +191,9 @@ def kl_domain(nb_min, nb_max, soil_max, water_max) -> KLDomain:
     return d
 
 
+OUT_ODB, OUT_FLOWDIST, OUT_IMPACT, OUT_MGF = 1, 2, 4, 8
+
+
 class Vibration(C.Structure):
     """sphgpu_vibration: Para_Vibra without its loads."""
     _fields_ = [("ttime", C.c_double), ("nsteps", C.c_int), ("sttime", C.c_double), ("edtime", C.c_double)]
@@ -298,6 +301,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_autotune.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_void_p]
     lib.sphgpu_output_total.argtypes = [C.c_void_p, C.c_char_p]
     lib.sphgpu_output_wait.argtypes = [C.c_void_p]
+    lib.sphgpu_output_begin.argtypes = [C.c_void_p, C.c_char_p]
+    lib.sphgpu_output_step.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
     lib.sphgpu_checkpoint_save.argtypes = [C.c_void_p, C.c_char_p]
     lib.sphgpu_checkpoint_load.argtypes = [C.c_void_p, C.c_char_p]
     lib.sphgpu_get_rain.argtypes = [C.c_void_p, C.POINTER(Rain)]
@@ -520,6 +525,15 @@ class Engine:
         """Write directory/data-<l>.odb (the reference's output_total format)
         for the last completed step, in the background."""
         self._check(self.lib.sphgpu_output_total(self.h, directory.encode()), "sphgpu_output_total")
+
+    def output_begin(self, directory: str) -> None:
+        """Create the run's appended result files (Flowing distance.dat,
+        Total_Force.dat, AVS_MGF.mgf with its header)."""
+        self._check(self.lib.sphgpu_output_begin(self.h, directory.encode()), "sphgpu_output_begin")
+
+    def output_step(self, directory: str, what: int) -> None:
+        """The result files `what` selects (OUT_* bits) for the last step."""
+        self._check(self.lib.sphgpu_output_step(self.h, directory.encode(), int(what)), "sphgpu_output_step")
 
     def output_wait(self) -> None:
         self._check(self.lib.sphgpu_output_wait(self.h), "sphgpu_output_wait")

@@ -1,9 +1,12 @@
-"""Result files written while the steps go on (sphgpu_output_total): the
-engine's data-*.odb files must equal, byte for byte, the ones the reference's
-own output_total (CPP_14-2-output.cpp:15-136) writes from the same state --
-here through the reference's executable linked against the shim, which
-hands output_total the engine's state -- and a file must hold the state of
-the step it was asked for even when later steps run before it is written."""
+"""Result files written while the steps go on (sphgpu_output_total,
+sphgpu_output_step): the engine's data-*.odb files, and the appended "Flowing
+distance.dat", AVS_MGF.mgf and Total_Force.dat with the Impact-force files,
+must equal, byte for byte, the ones the reference's own output_total,
+output_flowdist, mgf and output_impact (CPP_14-2-output.cpp, CPP_14-1-outmgf.cpp)
+write from the same state -- here through the reference's executable linked
+against the shim, which hands those functions the engine's state -- and a
+file must hold the state of the step it was asked for even when later steps
+run before it is written."""
 import glob
 import os
 import subprocess
@@ -29,9 +32,15 @@ def _deck(sc):
     return sc
 
 
+def _impact(sc):
+    sc.problem["if_cal"] = 1
+    return sc
+
+
 @pytest.mark.skipif(not os.path.exists(SPH_SHIM_EXE), reason="reference executables not built")
 @pytest.mark.parametrize("factory", [lambda: scenes.dam_break_2d(dx=0.02, steps=100),
-                                     lambda: scenes.soil_column_3d(dx=0.1, steps=200)])
+                                     lambda: _impact(scenes.soil_column_3d(dx=0.1, steps=200)),
+                                     lambda: _impact(scenes.shaking_box(ndim=2, flv=1, dx=0.05))])
 def test_output_files_equal_the_references(factory):
     sc = _deck(factory())
     ref_dir = tempfile.mkdtemp(prefix="sphr", dir="/tmp")
@@ -41,22 +50,32 @@ def test_output_files_equal_the_references(factory):
     assert r.returncode == 0, r.stderr.decode()[-2000:]
     st = scenes.initialise(sc)
     eng = sphgpu.Engine(st.params, device=0)
-    eng.load_state(st.fields, st.fluid, st.soil)
+    eng.load_state(st.fields, st.fluid, st.soil, vibration=st.vibration)
     out_dir = tempfile.mkdtemp(prefix="sphg", dir="/tmp")
+    eng.output_begin(out_dir)
     done = 0
+    impact = sc.problem["if_cal"] == 1
     for l in (1, 4, 8, 12):
         eng.step(l - done)
         done = l
-        eng.output_total(out_dir)
+        # what SPH_Calculation writes at an output step (CPP_1-SPHLoops.cpp:761-773)
+        what = sphgpu.OUT_ODB | sphgpu.OUT_FLOWDIST | (sphgpu.OUT_IMPACT if impact else 0) | \
+            (sphgpu.OUT_MGF if l != 1 else 0)
+        eng.output_step(out_dir, what)
     eng.output_wait()
     eng.close()
     names = sorted(os.path.basename(p) for p in glob.glob(os.path.join(ref_dir, "data-*.odb")))
     assert names == sorted(os.path.basename(p) for p in glob.glob(os.path.join(out_dir, "data-*.odb")))
     assert len(names) == 4
-    for f in names:
+    others = ["Flowing distance.dat", "AVS_MGF.mgf"]
+    if impact:
+        imp = sorted(os.path.basename(p) for p in glob.glob(os.path.join(ref_dir, "Impact-force*.inp")))
+        assert len(imp) == 4
+        others += ["Total_Force.dat"] + imp
+    for f in names + others:
         a = open(os.path.join(ref_dir, f), "rb").read()
         b = open(os.path.join(out_dir, f), "rb").read()
-        assert a == b, f
+        assert len(a) > 0 and a == b, f
 
 
 def test_output_holds_its_step_while_later_steps_run():
