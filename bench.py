@@ -434,6 +434,63 @@ def batched_slopes_cpu(threads: int, dx: float = 0.05, steps_run: int = 20000):
                       f"its K-L generation not included"}
 
 
+MCC = dict(ramda=0.2, kapa=0.04, zmf=1.2, eps0=0.9, poi=0.3, sme0=50.0e3, ann=1.0, ocr=1.5, e=0.0, fs=1.0)
+
+
+def dam_break_scene(dx: float = 0.005):
+    """The 2-D dam break: a 0.4 m x 0.8 m water column in a 1.6 m x 1.0 m tank,
+    12,800 water particles at dx = 5 mm, 3 wall layers."""
+    return scenes.dam_break_2d(dx=dx, steps=2000)
+
+
+def footing_scene(dx: float = 0.04):
+    """The 3-D soil-structure case: a rigid strip footing 2 m wide, 0.28 m tall
+    and 5 m long (43,750 structure particles at dx = 40 mm) pushed down at
+    0.01 m/s into a 10 x 5 x 5 m subloading Cam-clay bed (lambda 0.2, kappa
+    0.04, M 1.2, OCR 1.5, e0 0.9; 3.9 M soil particles), penalty contact."""
+    sc = scenes.footing(ndim=3, dx=dx, bed=(10.0, 5.0, 5.0), width=2.0, height=0.28, gap=0.4, v=0.01, ss_type=3,
+                        myu=0.3, zeta=0.1, steps=5000, matype=1)
+    return scenes.set_soil_model(sc, 1, **MCC)
+
+
+def config_leg(args, device, make, cpu_make, threads):
+    """One more named workload: K steps after the warm-up in the FP64 and
+    FP32-bulk forms (the bulk form's state compared with the FP64 form's after
+    the same steps), and the reference on the host cores on a sample of it."""
+    import sphgpu
+    sc = make()
+    st = scenes.initialise(sc)
+    n_active = sc.n_active()
+    out = {"particles": sc.n, "active_particles": n_active}
+    moving = (st.fields["type"] >= 1) & (st.fields["type"] <= 4)
+    ref = None
+    for form in ("fp64", "fp32_bulk"):
+        eng = sphgpu.Engine(st.params, device=device)
+        eng.load_state(st.fields, st.fluid, st.soil)
+        if form == "fp32_bulk":
+            eng.set_precision(sphgpu.PREC_FP32_BULK)
+        eng.step(args.warmup)
+        eng.synchronize()
+        eng.step(args.steps)
+        ms = eng.last_step_ms() / args.steps
+        out[form] = {"ms_per_step": ms, "value": n_active / (ms / 1e3), "unit": "particle-updates/s"}
+        fields = {k: eng.get_field(k) for k in ("sig", "ux", "vx", "rho", "xp")}
+        if ref is None:
+            ref = fields
+        else:
+            out[form]["rel_l2_vs_fp64"] = {k: _rel_l2(fields[k], ref[k], moving) for k in ref}
+        eng.close()
+    out["fp32_bulk"]["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["fp32_bulk"]["ms_per_step"]
+    if cpu_make is not None and threads:
+        small = cpu_make()
+        r = run_reference(small, 2, 1, threads)
+        if "unavailable" not in r:
+            out["cpu_baseline"] = {"value": r["value"], "unit": "particle-updates/s", "cores": threads,
+                                   "kind": "reference",
+                                   "sample": f"2 steps (after 1 warm-up) of {small.name} ({small.n} particles)"}
+    return out
+
+
 def engine_arm(args, world, rank, local):
     import sphgpu
     scene = scenes.soil_column_3d(dx=args.dx, steps=5000)
@@ -514,6 +571,13 @@ def engine_arm(args, world, rank, local):
     kl = kl_synthesis(eng, scene, device) if not args.no_kl else None
     eng.close()
     batched = batched_slopes(args, device) if not args.no_batched else None
+    others = None
+    if not args.no_configs:
+        thr = host_threads() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else 0
+        others = {
+            "dam_break_2d_dx5mm": config_leg(args, device, dam_break_scene, dam_break_scene, thr),
+            "footing_3d_camclay_dx40mm": config_leg(args, device, footing_scene, lambda: footing_scene(0.08), thr),
+        }
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -559,6 +623,7 @@ def engine_arm(args, world, rank, local):
             },
             "kl_synthesis": kl,
             "batched_slopes": batched,
+            "configs": others,
             "e2e": {"value": e2e_value, "unit": "particle-updates/s",
                     "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                     "what": "Particle-record upload, material upload, K steps and Particle-record download "
@@ -581,6 +646,7 @@ def main():
     ap.add_argument("--no-kl", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-configs", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         # host-only arm: rank 0 runs it, the other ranks exit without work
