@@ -129,6 +129,9 @@ struct DevState {
     double *vxp, *axp, *ax, *ux;
     double *rho, *rho_c, *rhop, *pre, *prep, *porosity, *poro_cop, *e;
     double *rrho;              // RN(1 / rho) at the start of the step (k_pairw), for k_density
+    double *nv;                // per particle (vxp x, y, z, mass) as the step starts (k_pairw): the
+                               // neighbour fields the density, strain and momentum loops gather, in
+                               // one 32-byte record instead of four arrays
     double *sig, *sig_next;    // 6N each, ping-pong
     double *eps, *adps;
     double *tssig, *tsqc;      // TSSMP: the transformed stress and its q (flts >= 1)
@@ -242,6 +245,15 @@ __device__ __forceinline__ Pos load_pos(const double* xh, int i)
     const double2* p = reinterpret_cast<const double2*>(xh) + 2 * (size_t)i;
     double2 a = p[0], b = p[1];
     return Pos{a.x, a.y, b.x, b.y};
+}
+
+// the neighbour record of particle j: vxp (x, y, z) and mass
+struct NV { double vx, vy, vz, m; };
+__device__ __forceinline__ NV load_nv(const double* nv, int j)
+{
+    const double2* p = reinterpret_cast<const double2*>(nv) + 2 * (size_t)j;
+    double2 a = p[0], b = p[1];
+    return NV{a.x, a.y, b.x, b.y};
 }
 
 __device__ __forceinline__ void store_pos(double* xh, int i, const Pos& q)

@@ -653,6 +653,13 @@ __global__ void __launch_bounds__(128, SPH_MINB_PAIRW) k_pairw(Dev d)
     const int i = IDX;
     if (i >= d.p.N || *d.s.err) return;
     d.s.rrho[i] = 1.0 / d.s.rho[i];     // for the divisions by rho_j of k_density (rho of the last step)
+    {
+        // the neighbour record of this step (vxp and mass change only between steps)
+        const int N = d.p.N;
+        double2* q = reinterpret_cast<double2*>(d.s.nv) + 2 * (size_t)i;
+        q[0] = make_double2(d.s.vxp[i], d.s.vxp[N + i]);
+        q[1] = make_double2(d.s.vxp[2 * N + i], d.s.mass[i]);
+    }
     if (d.p.bulk) pairw_particle<ND, float>(d, i);
     else pairw_particle<ND, double>(d, i);
 }
@@ -708,8 +715,9 @@ __global__ void __launch_bounds__(128, SPH_MINB_DENS) k_density(Dev d)
         int s, j;
         while (it.next(s, j)) {
             double vxj[3];
+            const NV nj = load_nv(d.s.nv, j);
             if (!wallm.has(s)) {
-                for (int k = 0; k < 3; k++) vxj[k] = d.s.vxp[k * N + j];
+                vxj[0] = nj.vx; vxj[1] = nj.vy; vxj[2] = nj.vz;
             } else if (moving) {
                 // virtual wall velocity (:89-121)
                 for (int k = 0; k < 3; k++) vxj[k] = wall_vel(d, ti, j, vi, k);
@@ -718,7 +726,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_DENS) k_density(Dev d)
             }
             real w[4];
             load_w(d, s, i, w);
-            const real mj = (real)d.s.mass[j];
+            const real mj = (real)nj.m;
             if (solid) {
                 const Pos pj = load_pos(d.s.xh, j);
                 const double xj[3] = {pj.x, pj.y, pj.z};
@@ -819,11 +827,13 @@ __global__ void __launch_bounds__(128, SPH_MINB_STRAIN) k_strain(Dev d)
         const bool same = !wallm.has(q);
         real w[4];
         load_w(d, q, i, w);
-        const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
+        const NV nj = load_nv(d.s.nv, j);
+        const real mj = (real)nj.m, rj = (real)d.s.rho[j];
         {
             real dvx[3];
+            const double vjs[3] = {nj.vx, nj.vy, nj.vz};
             for (int k = 0; k < 3; k++) {
-                double vj = same ? d.s.vxp[k * N + j] : wall_vel(d, ti, j, vi, k);
+                double vj = same ? vjs[k] : wall_vel(d, ti, j, vi, k);
                 dvx[k] = (real)(vi[k] - vj);
             }
             sup[0].add(mj / rj * dvx[0] * w[0]);
@@ -1500,7 +1510,9 @@ __device__ __forceinline__ void ff_stress(double sg[3], const double va[3], cons
 // Writes ax, interf, interfss and the updated velocity into vx_next (the
 // reference's vx before XSPH).  DRAG = 1 carries the interact2/3 drag
 // coefficient (fli 2, 3), whose out-of-line call the Darcy form does without.
-template <int ND, int DRAG = 0, int LOOP = 0>
+// VIB = 1 (flv != 0) adds the vibration damping and free-field sums to the
+// first loop; runs without vibration take the variant without them.
+template <int ND, int DRAG = 0, int LOOP = 0, int VIB = 0>
 __global__ void __launch_bounds__(128, LOOP ? SPH_MINB_ACCB2 : SPH_MINB_ACCB1) k_accel_b(Dev d)
 {
     const int i = IDX, N = d.p.N;
@@ -1528,8 +1540,8 @@ __global__ void __launch_bounds__(128, LOOP ? SPH_MINB_ACCB2 : SPH_MINB_ACCB1) k
     // (CPP_19-FreeFieldParticles_soil.cpp:71-175), for soil particles; the
     // sums of soil_damping_vibration (CPP_9-1-acceleration_vibration.cpp:
     // 171-224) for soil and structure particles (flv > 0)
-    const bool ffree = LOOP == 0 && d.p.flv != 0 && ti == 2;
-    const bool vdamp = LOOP == 0 && d.p.flv > 0 && solid;
+    const bool ffree = LOOP == 0 && VIB && d.p.flv != 0 && ti == 2;
+    const bool vdamp = LOOP == 0 && VIB && d.p.flv > 0 && solid;
     Sum<real> tfw[3], tfs[3], tdv[3], tdn;
     real cdv = 0;
     double vnow_i[3] = {0.0, 0.0, 0.0};
@@ -1567,11 +1579,13 @@ __global__ void __launch_bounds__(128, LOOP ? SPH_MINB_ACCB2 : SPH_MINB_ACCB1) k
             const Pos pj = load_pos(d.s.xh, j);
             real w[4];
             load_w(d, q, i, w);
-            const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
+            const NV nj = load_nv(d.s.nv, j);
+            const real mj = (real)nj.m, rj = (real)d.s.rho[j];
             const double xj[3] = {pj.x, pj.y, pj.z};
+            const double vjs[3] = {nj.vx, nj.vy, nj.vz};
             real inprod = 0, dst = 0, dx[3], dvx[3];
             for (int k = 0; k < nd; k++) {
-                dvx[k] = (real)(vi[k] - d.s.vxp[k * N + j]);
+                dvx[k] = (real)(vi[k] - vjs[k]);
                 dx[k] = (real)(I.x[k] - xj[k]);
                 dst = dst + dx[k] * dx[k];
                 inprod = inprod + dvx[k] * dx[k];
@@ -1615,11 +1629,13 @@ __global__ void __launch_bounds__(128, LOOP ? SPH_MINB_ACCB2 : SPH_MINB_ACCB1) k
             const Pos pj = load_pos(d.s.xh, j);
             real w[4];
             load_w(d, q, i, w);
-            const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
+            const NV nj = load_nv(d.s.nv, j);
+            const real mj = (real)nj.m, rj = (real)d.s.rho[j];
             const double xj[3] = {pj.x, pj.y, pj.z};
+            const double vjs[3] = {nj.vx, nj.vy, nj.vz};
             real inprod = 0, dvx[3];
             for (int k = 0; k < nd; k++) {
-                dvx[k] = (real)(vi[k] - d.s.vxp[k * N + j]);
+                dvx[k] = (real)(vi[k] - vjs[k]);
                 const real dxk = (real)(I.x[k] - xj[k]);
                 inprod = inprod + dvx[k] * dxk;
             }
@@ -1656,7 +1672,7 @@ __global__ void __launch_bounds__(128, LOOP ? SPH_MINB_ACCB2 : SPH_MINB_ACCB1) k
             }
         }
     }
-    if (LOOP == 0 && d.p.flv != 0) {
+    if (LOOP == 0 && VIB && d.p.flv != 0) {
         for (int k = 0; k < 3; k++) {
             d.s.accb[(size_t)(9 + k) * N + i] = (double)tfw[k].v();
             d.s.accb[(size_t)(12 + k) * N + i] = (double)tfs[k].v();
@@ -1700,7 +1716,7 @@ __device__ __forceinline__ int vib_load(const Dev& d, double t, double v[3])
 // order, the velocity update and the writes of ax, interf, interfss and the
 // velocity before XSPH (vx_next).  In a kernel of its own so that the loops of
 // k_accel_b run under a smaller register budget than this straight-line code.
-template <int ND, int ART = 0>
+template <int ND, int ART = 0, int VIB = 0>
 __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b_tail(Dev d)
 {
     const int i = IDX, N = d.p.N;
@@ -1786,7 +1802,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b_tail(Dev d)
         for (int k = 0; k < nd; k++) ax[k] = ax[k] + tu[k].v();
     if (moving)
         for (int k = 0; k < 3; k++) ax[k] += tbrow[k];
-    if (d.p.flv != 0 && ti == 2) {
+    if (VIB && d.p.flv != 0 && ti == 2) {
         // free_field_solid: the walls' sum, then the soil form's
         for (int k = 0; k < nd; k++) ax[k] = ax[k] + d.s.accb[(size_t)(9 + k) * N + i];
         for (int k = 0; k < nd; k++) ax[k] = ax[k] + d.s.accb[(size_t)(12 + k) * N + i];
@@ -1838,7 +1854,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b_tail(Dev d)
             else ax[k] -= tdm[k];
         }
     }
-    if (d.p.flv > 0 && solid) {
+    if (VIB && d.p.flv > 0 && solid) {
         // soil_damping_vibration (CPP_9-1-acceleration_vibration.cpp:171-224)
         double td = d.s.accb[(size_t)18 * N + i];
         for (int k = 0; k < nd; k++) {
@@ -1859,7 +1875,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b_tail(Dev d)
     double vout[3];
     for (int k = 0; k < 3; k++) vout[k] = d.s.vx[k * N + i];
     const int mt = d.s.matype[i];
-    if (d.p.flv == 1 && ti == 0 && (mt == 3 || mt == 5)) {
+    if (VIB && d.p.flv == 1 && ti == 0 && (mt == 3 || mt == 5)) {
         // vibration_acceleration: the load into the wall's interf (a load of
         // 1000 or more, or a time outside the window, zeroes interf and
         // interfss)
@@ -1919,7 +1935,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b_tail(Dev d)
             vout[k] = vp[k] + ath * dt;
         }
     }
-    if (d.p.flv == 2 && ti == 0 && (mt == 4 || mt == 5)) {
+    if (VIB && d.p.flv == 2 && ti == 0 && (mt == 4 || mt == 5)) {
         // vibration_velocity, after the velocity update: the load is the
         // wall's velocity interfss
         double v[3];
@@ -3037,20 +3053,32 @@ extern "C" int SPHK_ENTRY(sphk_enqueue_physics)(const Dev* dp, cudaStream_t st, 
     }
     REC(17);
     {
-        const bool drag = d.p.fli > 1;
+        const bool drag = d.p.fli > 1, vib = d.p.flv != 0;
         const dim3 g(nblk(N, tbk(d, TP_ACCEL_B))), b(tbk(d, TP_ACCEL_B));
         if (d.p.ndim == 2) {
-            k_accel_b<2, 0, 0><<<g, b, 0, st>>>(d);
+            if (vib) k_accel_b<2, 0, 0, 1><<<g, b, 0, st>>>(d);
+            else k_accel_b<2, 0, 0><<<g, b, 0, st>>>(d);
             if (drag) k_accel_b<2, 1, 1><<<g, b, 0, st>>>(d);
             else k_accel_b<2, 0, 1><<<g, b, 0, st>>>(d);
-            if (art) k_accel_b_tail<2, 1><<<g, b, 0, st>>>(d);
-            else k_accel_b_tail<2, 0><<<g, b, 0, st>>>(d);
+            if (vib) {
+                if (art) k_accel_b_tail<2, 1, 1><<<g, b, 0, st>>>(d);
+                else k_accel_b_tail<2, 0, 1><<<g, b, 0, st>>>(d);
+            } else {
+                if (art) k_accel_b_tail<2, 1><<<g, b, 0, st>>>(d);
+                else k_accel_b_tail<2, 0><<<g, b, 0, st>>>(d);
+            }
         } else {
-            k_accel_b<3, 0, 0><<<g, b, 0, st>>>(d);
+            if (vib) k_accel_b<3, 0, 0, 1><<<g, b, 0, st>>>(d);
+            else k_accel_b<3, 0, 0><<<g, b, 0, st>>>(d);
             if (drag) k_accel_b<3, 1, 1><<<g, b, 0, st>>>(d);
             else k_accel_b<3, 0, 1><<<g, b, 0, st>>>(d);
-            if (art) k_accel_b_tail<3, 1><<<g, b, 0, st>>>(d);
-            else k_accel_b_tail<3, 0><<<g, b, 0, st>>>(d);
+            if (vib) {
+                if (art) k_accel_b_tail<3, 1, 1><<<g, b, 0, st>>>(d);
+                else k_accel_b_tail<3, 0, 1><<<g, b, 0, st>>>(d);
+            } else {
+                if (art) k_accel_b_tail<3, 1><<<g, b, 0, st>>>(d);
+                else k_accel_b_tail<3, 0><<<g, b, 0, st>>>(d);
+            }
         }
     }
     n += 3;
