@@ -491,6 +491,55 @@ def config_leg(args, device, make, cpu_make, threads):
     return out
 
 
+def rf_cholesky(device, threads: int):
+    """The correlation-matrix random field (flspv 3) on the 5 m slope: one
+    lognormal cohesion field over about 2,400 cells and one over about
+    13,000 (the reference refuses 15,000), timed per call on the GPU; the
+    reference's own routine on the 2,400-cell case on the host cores."""
+    import sphgpu
+    sc = scenes.slope_2d(H=5.0, dx=0.1)
+    st = scenes.initialise(sc)
+    d = scenes.kl_domain(sc)
+    dom = sphgpu.kl_domain(d["nb_min"], d["nb_max"], d["soil_max"], d["water_max"])
+    ext = 1.2 * (np.array(d["nb_max"]) - np.array(d["nb_min"]))
+    out = {}
+    eng = sphgpu.Engine(st.params, device=device)
+    eng.load_state(st.fields, st.fluid, st.soil)
+    field = sphgpu.kl_field(1, 2, 10.0e3, 3.0e3, [6.0, 1.5, 0.0], 100.0)
+    small = None
+    for target in (2500, 14000):
+        ndx = 1.03 * float(np.sqrt(ext[0] * ext[1] / target) / sc.dr)
+        fl = sphgpu.rf_flags(ndx, 1)
+        nc = eng.rf_cells(dom, fl)
+        z = np.random.default_rng(7).standard_normal((1, nc))
+        eng.rf_generate(dom, [field], fl, z)               # warm-up
+        t0 = time.perf_counter()
+        eng.rf_generate(dom, [field], fl, z)
+        out[f"cells_{nc}"] = {"cells": nc, "gpu_s": time.perf_counter() - t0,
+                              "factor_flop": nc ** 3 / 3.0}
+        if small is None:
+            small = (ndx, nc, z)
+    eng.close()
+    if threads:
+        sys.path.insert(0, os.path.join(REPO, "tests"))
+        from checkers import have_reference, reference_lib, rf_reference
+        if have_reference():
+            import ctypes
+            ndx, nc, z = small
+            lib = reference_lib()
+            f = {"no": 1, "type": 2, "mean": 10.0e3, "sd": 3.0e3, "rl": [6.0, 1.5, 0.0], "coe_depth": 100.0,
+                 "cell_ndx": ndx, "flag_auto": 1}
+            lib.ref_rf_threads(ctypes.c_int(threads))
+            try:
+                t0 = time.perf_counter()
+                rf_reference(2, sc.xp, sc.ptype, sc.dr, f, d, z[0])
+                out["cpu_baseline"] = {"cells": nc, "s": time.perf_counter() - t0, "cores": threads,
+                                       "kind": "reference"}
+            finally:
+                lib.ref_rf_threads(ctypes.c_int(1))
+    return out
+
+
 def engine_arm(args, world, rank, local):
     import sphgpu
     scene = scenes.soil_column_3d(dx=args.dx, steps=5000)
@@ -571,6 +620,9 @@ def engine_arm(args, world, rank, local):
     kl = kl_synthesis(eng, scene, device) if not args.no_kl else None
     eng.close()
     batched = batched_slopes(args, device) if not args.no_batched else None
+    rf = None
+    if rank == 0 and not args.no_configs:
+        rf = rf_cholesky(device, host_threads() if (world == 1 and not args.no_cpu_baseline) else 0)
     others = None
     if not args.no_configs:
         thr = host_threads() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else 0
@@ -624,6 +676,7 @@ def engine_arm(args, world, rank, local):
             "kl_synthesis": kl,
             "batched_slopes": batched,
             "configs": others,
+            "rf_cholesky": rf,
             "e2e": {"value": e2e_value, "unit": "particle-updates/s",
                     "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                     "what": "Particle-record upload, material upload, K steps and Particle-record download "
