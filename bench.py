@@ -447,19 +447,40 @@ def footing_scene(dx: float = 0.04):
     """The 3-D soil-structure case: a rigid strip footing 2 m wide, 0.28 m tall
     and 5 m long (43,750 structure particles at dx = 40 mm) pushed down at
     0.01 m/s into a 10 x 5 x 5 m subloading Cam-clay bed (lambda 0.2, kappa
-    0.04, M 1.2, OCR 1.5, e0 0.9; 3.9 M soil particles), penalty contact."""
-    sc = scenes.footing(ndim=3, dx=dx, bed=(10.0, 5.0, 5.0), width=2.0, height=0.28, gap=0.4, v=0.01, ss_type=3,
+    0.04, M 1.2, OCR 1.5, e0 0.9; 3.9 M soil particles), penalty contact.  The
+    footing starts two spacings above the soil."""
+    sc = scenes.footing(ndim=3, dx=dx, bed=(10.0, 5.0, 5.0), width=2.0, height=0.28, gap=2.0, v=0.01, ss_type=3,
                         myu=0.3, zeta=0.1, steps=5000, matype=1)
     return scenes.set_soil_model(sc, 1, **MCC)
 
 
-def config_leg(args, device, make, cpu_make, threads):
+def geostatic_soil(st, K0: float = 0.3 / 0.7) -> None:
+    """A K0 geostatic stress in the soil (vertical stress rho g depth below
+    the soil's top, horizontal K0 times it), so that a Cam-clay bed starts
+    from a stress state rather than from zero stiffness."""
+    t, xp = st.fields["type"], st.fields["xp"]
+    soil = t == 2
+    if not soil.any():
+        return
+    dens = np.asarray(st.soil["dens"])
+    top = xp[soil, 1].max() + 0.5 * st.params["dr"]
+    sig = np.array(st.fields["sig"], dtype=np.float64).reshape(-1, 6).copy()
+    sv = -dens * 9.81 * (top - xp[:, 1])
+    sig[soil, 1] = sv[soil]
+    sig[soil, 0] = K0 * sv[soil]
+    sig[soil, 2] = K0 * sv[soil]
+    st.fields["sig"] = sig
+
+
+def config_leg(args, device, make, cpu_make, threads, prepare=None):
     """One more named workload: K steps after the warm-up in the FP64 and
     FP32-bulk forms (the bulk form's state compared with the FP64 form's after
     the same steps), and the reference on the host cores on a sample of it."""
     import sphgpu
     sc = make()
     st = scenes.initialise(sc)
+    if prepare is not None:
+        prepare(st)
     n_active = sc.n_active()
     out = {"particles": sc.n, "active_particles": n_active}
     moving = (st.fields["type"] >= 1) & (st.fields["type"] <= 4)
@@ -628,7 +649,8 @@ def engine_arm(args, world, rank, local):
         thr = host_threads() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else 0
         others = {
             "dam_break_2d_dx5mm": config_leg(args, device, dam_break_scene, dam_break_scene, thr),
-            "footing_3d_camclay_dx40mm": config_leg(args, device, footing_scene, lambda: footing_scene(0.08), thr),
+            "footing_3d_camclay_dx40mm": config_leg(args, device, footing_scene, lambda: footing_scene(0.08), thr,
+                                                    prepare=geostatic_soil),
         }
 
     cpu = None
