@@ -649,10 +649,10 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.s_yalf, N); r |= dalloc(c, &s.s_ykap, N); r |= dalloc(c, &s.s_yalf_dil, N);
     r |= dalloc(c, &s.xh, 4 * (size_t)N); r |= dalloc(c, &s.xh_next, 4 * (size_t)N); r |= dalloc(c, &s.xs, 4 * (size_t)N); r |= dalloc(c, &s.xsf, 4 * (size_t)N);
     r |= dalloc(c, &s.de, 6 * (size_t)N); r |= dalloc(c, &s.we, 6 * (size_t)N); r |= dalloc(c, &s.color, N);
-    r |= dalloc(c, &s.sr, 6 * (size_t)N); r |= dalloc(c, &s.pp, N);
+    r |= dalloc(c, &s.sr, 8 * (size_t)N);
     r |= dalloc(c, &s.eps_tmp, 6 * (size_t)N); r |= dalloc(c, &s.sig_tmp, 6 * (size_t)N);
     r |= alloc_optional(c, P);
-    r |= dalloc(c, &s.vx, 3 * (size_t)N); r |= dalloc(c, &s.vx_next, 3 * (size_t)N);
+    r |= dalloc(c, &s.vx, 3 * (size_t)N); r |= dalloc(c, &s.vx_next, 4 * (size_t)N);
     r |= dalloc(c, &s.vxp, 3 * (size_t)N); r |= dalloc(c, &s.axp, 3 * (size_t)N); r |= dalloc(c, &s.ax, 3 * (size_t)N);
     r |= dalloc(c, &s.ux, 3 * (size_t)N);
     r |= dalloc(c, &s.rho, N); r |= dalloc(c, &s.rho_c, N); r |= dalloc(c, &s.rrho, N); r |= dalloc(c, &s.nv, 4 * (size_t)N); r |= dalloc(c, &s.rhop, N); r |= dalloc(c, &s.pre, N);

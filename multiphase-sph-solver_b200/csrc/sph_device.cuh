@@ -125,7 +125,8 @@ struct DevState {
     double *xs;                // xh in cell-sorted order (NNPS scan)
     float *xsf;                // xs as FP32 (x - xmin, y - ymin, z - zmin, h) records: the NNPS prefilter
     // dynamic state
-    double *vx, *vx_next;      // vx: velocity after the step; vx_next: before XSPH
+    double *vx;                // velocity after the step
+    double *vx_next;           // per particle (vx x, y, z before XSPH, mass): one 32-byte record
     double *vxp, *axp, *ax, *ux;
     double *rho, *rho_c, *rhop, *pre, *prep, *porosity, *poro_cop, *e;
     double *rrho;              // RN(1 / rho) at the start of the step (k_pairw), for k_density
@@ -142,8 +143,9 @@ struct DevState {
     double *de;                // strain rate, 6N
     double *we;                // spin, off-diagonal entries (0,1)(0,2)(1,0)(1,2)(2,0)(2,1): 6N
     double *color;             // free-surface colour sum
-    double *sr;                // stress / rho^2 as the momentum pass uses it, 6N
-    double *pp;                // pore-pressure term / rho^2, N
+    double *sr;                // per particle, 8 doubles in one 64-byte record: stress / rho^2 as the
+                               // momentum pass uses it (6, Voigt order), the pore-pressure term / rho^2
+                               // and the mass, so that a neighbour's part of the pass is one record
     double *eps_in;            // strain the constitutive pass starts from: eps, or eps_tmp after strain_regu
     double *eps_tmp, *sig_tmp; // outputs of the regularisation passes, 6N each
     double *rij;               // artificial stress tensor R per soil particle, 9N row-major (art_stre_coe > 0)
@@ -245,6 +247,23 @@ __device__ __forceinline__ Pos load_pos(const double* xh, int i)
     const double2* p = reinterpret_cast<const double2*>(xh) + 2 * (size_t)i;
     double2 a = p[0], b = p[1];
     return Pos{a.x, a.y, b.x, b.y};
+}
+
+// the momentum record of particle j (DevState::sr)
+struct SR { double s[6], p, m; };
+__device__ __forceinline__ SR load_sr(const double* sr, int j)
+{
+    const double2* q = reinterpret_cast<const double2*>(sr) + 4 * (size_t)j;
+    const double2 a = q[0], b = q[1], c = q[2], e = q[3];
+    return SR{{a.x, a.y, b.x, b.y, c.x, c.y}, e.x, e.y};
+}
+__device__ __forceinline__ void store_sr(double* sr, int i, const double s[6], double p, double m)
+{
+    double2* q = reinterpret_cast<double2*>(sr) + 4 * (size_t)i;
+    q[0] = make_double2(s[0], s[1]);
+    q[1] = make_double2(s[2], s[3]);
+    q[2] = make_double2(s[4], s[5]);
+    q[3] = make_double2(p, m);
 }
 
 // the neighbour record of particle j: vxp (x, y, z) and mass

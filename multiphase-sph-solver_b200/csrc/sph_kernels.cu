@@ -1203,10 +1203,11 @@ __global__ void __launch_bounds__(128, SPH_MINB_STRESS) k_stress(Dev d)
     // fluids use porosity * sigma / rho / rho, soil and structure sigma / rho / rho
     const double r = d.s.rho[i];
     const double pf = (ti == 1 || ti == 3) ? d.s.f_por[i] : 0.0;
+    double srk[6];
     for (int k = 0; k < 6; k++) {
         d.s.sig_next[k * N + i] = s[k];
         d.s.eps[k * N + i] = ep[k];
-        d.s.sr[k * N + i] = (ti == 1 || ti == 3) ? pf * s[k] / r / r : s[k] / r / r;
+        srk[k] = (ti == 1 || ti == 3) ? pf * s[k] / r / r : s[k] / r / r;
     }
     double pp = 0.0;
     if (ti == 2) {
@@ -1216,7 +1217,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_STRESS) k_stress(Dev d)
         const double satu = d.s.satu[i];
         pp = (-satu * d.s.prew[i] + (1 - satu) * d.s.prea[i]) / r / r;
     }
-    d.s.pp[i] = pp;
+    store_sr(d.s.sr, i, srk, pp, d.s.mass[i]);
 }
 
 // The per-particle tensor R_i of artificial_stress_2d / artificial_stress_3d
@@ -1289,7 +1290,10 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCA) k_accel_a(Dev d)
     const int other = (ti == 1) ? 3 : 1;
     const bool minor = (ti == 1) ? d.p.water_minor : d.p.air_minor;
     real sri[6];
-    for (int k = 0; k < 6; k++) sri[k] = (real)d.s.sr[k * N + i];
+    {
+        const SR own = load_sr(d.s.sr, i);
+        for (int k = 0; k < 6; k++) sri[k] = (real)own.s[k];
+    }
     Sum<real> tf[3][3];
     const double satu_i = d.s.satu[i];
     const double prew_i = solid ? d.s.prew[i] : 0.0, prea_i = solid ? d.s.prea[i] : 0.0;
@@ -1309,10 +1313,11 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCA) k_accel_a(Dev d)
         const bool s_pair = solid;
         real w[4];
         load_w(d, q, i, w);
-        const real mj = (real)d.s.mass[j];
+        const SR rj_ = load_sr(d.s.sr, j);
+        const real mj = (real)rj_.m;
         real srj[6];
         if (s_pair || same_bits(d.s.f_por[j], poro_f)) {
-            for (int k = 0; k < 6; k++) srj[k] = (real)d.s.sr[k * N + j];
+            for (int k = 0; k < 6; k++) srj[k] = (real)rj_.s[k];
         } else {
             const double rj = d.s.rho[j];
             for (int k = 0; k < 6; k++) srj[k] = (real)(poro_f * d.s.sig_next[k * N + j] / rj / rj);
@@ -1343,7 +1348,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCA) k_accel_a(Dev d)
             if (ti == 2) {
                 double pj_, pi_;
                 if (same_bits(d.s.s_por[j], poro_s)) {
-                    pj_ = d.s.pp[j];
+                    pj_ = rj_.p;
                 } else {
                     const double rj = d.s.rho[j];
                     pj_ = (1 - poro_s) * (-satu * d.s.prew[j] + (1 - satu) * d.s.prea[j]) / rj / rj;
@@ -1355,7 +1360,7 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCA) k_accel_a(Dev d)
                 tf[1][1].add(mj * pq * w[1]);
                 tf[2][2].add(mj * pq * w[2]);
             } else {
-                const double pj_ = d.s.pp[j];
+                const double pj_ = rj_.p;
                 const double pi_ = same_bits(satu, satu_i) ? pi_own
                     : (-satu * prew_i + (1 - satu) * prea_i) / ri / ri;
                 const real pq = (real)(pj_ - pi_);
@@ -1945,10 +1950,11 @@ __global__ void __launch_bounds__(128, SPH_MINB_ACCB) k_accel_b_tail(Dev d)
             else { d.s.interf[k * N + i] = 0.0; d.s.interfss[k * N + i] = 0.0; }
         }
     }
-    for (int k = 0; k < 3; k++) {
-        d.s.ax[k * N + i] = ax[k];
-        d.s.vx_next[k * N + i] = vout[k];   // velocity before XSPH
-    }
+    for (int k = 0; k < 3; k++) d.s.ax[k * N + i] = ax[k];
+    // the velocity before XSPH, with the mass, as one record for XSPH's gathers
+    double2* vq = reinterpret_cast<double2*>(d.s.vx_next) + 2 * (size_t)i;
+    vq[0] = make_double2(vout[0], vout[1]);
+    vq[1] = make_double2(vout[2], d.s.mass[i]);
 }
 
 // xsph (CPP_11-xsph.cpp:145-256, Jacobi by construction: reads the velocities
@@ -1965,7 +1971,10 @@ __global__ void __launch_bounds__(128, SPH_MINB_XSPH) k_xsph_update(Dev d)
     const double dt = step_dt(d);
     const PairI<real> I = pair_i<ND, real>(d, i);
     double vm[3];
-    for (int k = 0; k < 3; k++) vm[k] = d.s.vx_next[k * N + i];
+    {
+        const NV own = load_nv(d.s.vx_next, i);
+        vm[0] = own.vx; vm[1] = own.vy; vm[2] = own.vz;
+    }
     const bool moving = (ti >= 1 && ti <= 4);
     double vn[3] = {vm[0], vm[1], vm[2]};
     const SlotMask wallm = type_mask(d, i, 0);
@@ -1981,9 +1990,11 @@ __global__ void __launch_bounds__(128, SPH_MINB_XSPH) k_xsph_update(Dev d)
             const real xishu = wallm.has(q) ? xs_wall : xs_same;
             real w[4];
             load_w(d, q, i, w);
-            const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
+            const NV nj = load_nv(d.s.vx_next, j);
+            const real mj = (real)nj.m, rj = (real)d.s.rho[j];
+            const double vjs[3] = {nj.vx, nj.vy, nj.vz};
             for (int k = 0; k < nd; k++)
-                stu[k].add(xishu * mj * (real)(d.s.vx_next[k * N + j] - vm[k]) * w[3] / rj);
+                stu[k].add(xishu * mj * (real)(vjs[k] - vm[k]) * w[3] / rj);
             sdown.add(mj * w[3] / rj);
         }
         double tu[3];
