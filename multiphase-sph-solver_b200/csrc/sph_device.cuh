@@ -128,7 +128,9 @@ struct DevState {
     double *vx;                // velocity after the step
     double *vx_next;           // per particle (vx x, y, z before XSPH, mass): one 32-byte record
     double *vxp, *axp, *ax, *ux;
-    double *rho, *rho_c, *rhop, *pre, *prep, *porosity, *poro_cop, *e;
+    double *rho, *rhop, *pre, *prep, *porosity, *poro_cop, *e;
+    double *rho_c;             // per particle (continuity density, mass): one 16-byte record for Shepard
+    double *svr;               // per particle (vxp x, y, z, mass / rho) after Shepard: the strain loop's record
     double *rrho;              // RN(1 / rho) at the start of the step (k_pairw), for k_density
     double *nv;                // per particle (vxp x, y, z, mass) as the step starts (k_pairw): the
                                // neighbour fields the density, strain and momentum loops gather, in

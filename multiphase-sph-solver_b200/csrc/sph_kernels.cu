@@ -756,7 +756,8 @@ __global__ void __launch_bounds__(128, SPH_MINB_DENS) k_density(Dev d)
         else
             rnew = rhop + drhot * dt;
     }
-    d.s.rho_c[i] = rnew;
+    // the continuity density with the mass, one record for the Shepard gathers
+    reinterpret_cast<double2*>(d.s.rho_c)[i] = make_double2(rnew, d.s.mass[i]);
 }
 
 // Shepard filter (:168-188) reading every neighbour's continuity density
@@ -773,14 +774,21 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_shepard_eos(Dev d)
     while (it.next(s, j)) {
         real w[4];
         load_w(d, s, i, w);
-        const real mj = (real)d.s.mass[j];
+        const double2 cm = reinterpret_cast<const double2*>(d.s.rho_c)[j];
+        const real mj = (real)cm.y;
         sup.add(mj * w[3]);
-        sdown.add(mj / (real)d.s.rho_c[j] * w[3]);
+        sdown.add(mj / (real)cm.x * w[3]);
     }
     const double up = sup.v(), down = sdown.v();
-    double r = d.s.rho_c[i];
+    double r = reinterpret_cast<const double2*>(d.s.rho_c)[i].x;
     if (ti != 7 && fabs(down) > 1.0e-7) r = up / down;
     d.s.rho[i] = r;
+    {
+        // the strain loop's neighbour record: vxp and mass / rho of this step
+        double2* q = reinterpret_cast<double2*>(d.s.svr) + 2 * (size_t)i;
+        q[0] = make_double2(d.s.vxp[i], d.s.vxp[N + i]);
+        q[1] = make_double2(d.s.vxp[2 * N + i], d.s.mass[i] / r);
+    }
     const double prep = d.s.prep[i];
     if (ti == 1) {
         double pr = prep * (pow7(r / d.s.f_dens[i] / d.s.f_por[i]) - 1.0);
@@ -827,8 +835,10 @@ __global__ void __launch_bounds__(128, SPH_MINB_STRAIN) k_strain(Dev d)
         const bool same = !wallm.has(q);
         real w[4];
         load_w(d, q, i, w);
-        const NV nj = load_nv(d.s.nv, j);
-        const real mj = (real)nj.m, rj = (real)d.s.rho[j];
+        // vxp and m_j / rho_j (the quotient the reference forms per pair,
+        // formed once per particle by k_shepard_eos: the same value in FP64)
+        const NV nj = load_nv(d.s.svr, j);
+        const real mr = (real)nj.m;
         {
             real dvx[3];
             const double vjs[3] = {nj.vx, nj.vy, nj.vz};
@@ -836,22 +846,22 @@ __global__ void __launch_bounds__(128, SPH_MINB_STRAIN) k_strain(Dev d)
                 double vj = same ? vjs[k] : wall_vel(d, ti, j, vi, k);
                 dvx[k] = (real)(vi[k] - vj);
             }
-            sup[0].add(mj / rj * dvx[0] * w[0]);
-            sup[1].add(mj / rj * dvx[0] * w[1]);
-            sup[2].add(mj / rj * dvx[0] * w[2]);
-            sup[3].add(mj / rj * dvx[1] * w[0]);
-            sup[4].add(mj / rj * dvx[1] * w[1]);
-            sup[5].add(mj / rj * dvx[1] * w[2]);
-            sup[6].add(mj / rj * dvx[2] * w[0]);
-            sup[7].add(mj / rj * dvx[2] * w[1]);
-            sup[8].add(mj / rj * dvx[2] * w[2]);
+            sup[0].add(mr * dvx[0] * w[0]);
+            sup[1].add(mr * dvx[0] * w[1]);
+            sup[2].add(mr * dvx[0] * w[2]);
+            sup[3].add(mr * dvx[1] * w[0]);
+            sup[4].add(mr * dvx[1] * w[1]);
+            sup[5].add(mr * dvx[1] * w[2]);
+            sup[6].add(mr * dvx[2] * w[0]);
+            sup[7].add(mr * dvx[2] * w[1]);
+            sup[8].add(mr * dvx[2] * w[2]);
             if (solid) {
                 const Pos pj = load_pos(d.s.xh, j);
-                sdown[0].add(mj / rj * (real)(P.x - pj.x) * w[0]);
-                sdown[1].add(mj / rj * (real)(P.y - pj.y) * w[1]);
-                sdown[2].add(mj / rj * (real)(P.z - pj.z) * w[2]);
+                sdown[0].add(mr * (real)(P.x - pj.x) * w[0]);
+                sdown[1].add(mr * (real)(P.y - pj.y) * w[1]);
+                sdown[2].add(mr * (real)(P.z - pj.z) * w[2]);
             }
-            scolor.add(mj / rj * real(1.0) * w[3]);
+            scolor.add(mr * real(1.0) * w[3]);
         }
     }
     // velocity gradient (:148-181), strain rate and spin (:183-218), written
