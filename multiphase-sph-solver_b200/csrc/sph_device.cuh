@@ -131,7 +131,9 @@ struct DevState {
     double *rho, *rhop, *pre, *prep, *porosity, *poro_cop, *e;
     double *rho_c;             // per particle (continuity density, mass): one 16-byte record for Shepard
     double *svr;               // per particle (vxp x, y, z, mass / rho) after Shepard: the strain loop's record
-    double *rrho;              // RN(1 / rho) at the start of the step (k_pairw), for k_density
+    double *pmr;               // per particle (mass, rho, pre, 0) after Shepard: the pressure gathers' record
+    double *rrho;              // per particle (mass, porosity, rho, RN(1 / rho)) at the start of the step
+                               // (k_pairw): k_density's porosity gathers in one record
     double *nv;                // per particle (vxp x, y, z, mass) as the step starts (k_pairw): the
                                // neighbour fields the density, strain and momentum loops gather, in
                                // one 32-byte record instead of four arrays

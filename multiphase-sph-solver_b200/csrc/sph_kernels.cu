@@ -652,7 +652,14 @@ __global__ void __launch_bounds__(128, SPH_MINB_PAIRW) k_pairw(Dev d)
 {
     const int i = IDX;
     if (i >= d.p.N || *d.s.err) return;
-    d.s.rrho[i] = 1.0 / d.s.rho[i];     // for the divisions by rho_j of k_density (rho of the last step)
+    {
+        // k_density's record of the porosity gathers: mass, porosity, rho of
+        // the last step and its reciprocal (for the divisions by rho_j)
+        const double r = d.s.rho[i];
+        double2* q = reinterpret_cast<double2*>(d.s.rrho) + 2 * (size_t)i;
+        q[0] = make_double2(d.s.mass[i], d.s.porosity[i]);
+        q[1] = make_double2(r, 1.0 / r);
+    }
     {
         // the neighbour record of this step (vxp and mass change only between steps)
         const int N = d.p.N;
@@ -686,9 +693,10 @@ __global__ void __launch_bounds__(128, SPH_MINB_DENS) k_density(Dev d)
         while (it.next(s, j)) {
             real w[4];
             load_w(d, s, i, w);
-            const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
-            const double rrj = d.s.rrho[j];
-            sup.add(div_rho(mj * (real)d.s.porosity[j], rj, rrj) * w[3]);
+            const NV pj = load_nv(d.s.rrho, j);     // (mass, porosity, rho, 1 / rho)
+            const real mj = (real)pj.vx, rj = (real)pj.vz;
+            const double rrj = pj.m;
+            sup.add(div_rho(mj * (real)pj.vy, rj, rrj) * w[3]);
             sdown.add(div_rho(mj, rj, rrj) * w[3]);
         }
         const double up = sup.v(), down = sdown.v();
@@ -801,6 +809,12 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_shepard_eos(Dev d)
         double pr = prep * (pow7(r / d.s.rhop[i]) - 1.0);
         d.s.pre[i] = pr + prep;
     }
+    {
+        // the pressure gathers' record: mass, rho and pressure of this step
+        double2* q = reinterpret_cast<double2*>(d.s.pmr) + 2 * (size_t)i;
+        q[0] = make_double2(d.s.mass[i], r);
+        q[1] = make_double2(d.s.pre[i], 0.0);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -905,9 +919,10 @@ __global__ void __launch_bounds__(128, SPH_MINB_STRAIN) k_strain(Dev d)
             const int tj = m1.has(q) ? 1 : m3.has(q) ? 3 : 2;
             real w[4];
             load_w(d, q, i, w);
-            const real mj = (real)d.s.mass[j], rj = (real)d.s.rho[j];
+            const NV pm = load_nv(d.s.pmr, j);      // (mass, rho, pre, -)
+            const real mj = (real)pm.vx, rj = (real)pm.vy;
             const real w3 = w[3];
-            const real pj_ = (ti == 0 && tj == 2) ? real(0) : (real)d.s.pre[j];
+            const real pj_ = (ti == 0 && tj == 2) ? real(0) : (real)pm.vz;
             if (tj == 1) { su1.add(mj * pj_ * w3 / rj); sd1.add(mj * w3 / rj); }
             if (tj == 3) { su2.add(mj * pj_ * w3 / rj); sd2.add(mj * w3 / rj); }
             if (ti == 0 && tj == 2) {
