@@ -655,7 +655,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.vx, 3 * (size_t)N); r |= dalloc(c, &s.vx_next, 4 * (size_t)N);
     r |= dalloc(c, &s.vxp, 3 * (size_t)N); r |= dalloc(c, &s.axp, 3 * (size_t)N); r |= dalloc(c, &s.ax, 3 * (size_t)N);
     r |= dalloc(c, &s.ux, 3 * (size_t)N);
-    r |= dalloc(c, &s.rho, N); r |= dalloc(c, &s.rho_c, 2 * (size_t)N); r |= dalloc(c, &s.svr, 4 * (size_t)N); r |= dalloc(c, &s.pmr, 4 * (size_t)N); r |= dalloc(c, &s.rrho, 4 * (size_t)N); r |= dalloc(c, &s.nv, 4 * (size_t)N); r |= dalloc(c, &s.rhop, N); r |= dalloc(c, &s.pre, N);
+    r |= dalloc(c, &s.rho, N); r |= dalloc(c, &s.rho_c, 2 * (size_t)N); r |= dalloc(c, &s.svr, 4 * (size_t)N); r |= dalloc(c, &s.pmr, 4 * (size_t)N); r |= dalloc(c, &s.dr4, 4 * (size_t)N); r |= dalloc(c, &s.rrho, 4 * (size_t)N); r |= dalloc(c, &s.nv, 4 * (size_t)N); r |= dalloc(c, &s.rhop, N); r |= dalloc(c, &s.pre, N);
     r |= dalloc(c, &s.prep, N); r |= dalloc(c, &s.porosity, N); r |= dalloc(c, &s.poro_cop, N); r |= dalloc(c, &s.e, N);
     r |= dalloc(c, &s.sig, 6 * (size_t)N); r |= dalloc(c, &s.sig_next, 6 * (size_t)N);
     r |= dalloc(c, &s.eps, 6 * (size_t)N); r |= dalloc(c, &s.adps, 6 * (size_t)N);

@@ -132,6 +132,8 @@ struct DevState {
     double *rho_c;             // per particle (continuity density, mass): one 16-byte record for Shepard
     double *svr;               // per particle (vxp x, y, z, mass / rho) after Shepard: the strain loop's record
     double *pmr;               // per particle (mass, rho, pre, 0) after Shepard: the pressure gathers' record
+    double *dr4;               // per particle (rho, satu, porosity, soil: cop | fluid: f_dens) after the
+                               // constitutive pass: the drag loop's record
     double *rrho;              // per particle (mass, porosity, rho, RN(1 / rho)) at the start of the step
                                // (k_pairw): k_density's porosity gathers in one record
     double *nv;                // per particle (vxp x, y, z, mass) as the step starts (k_pairw): the

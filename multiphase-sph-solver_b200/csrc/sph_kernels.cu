@@ -850,9 +850,17 @@ __global__ void __launch_bounds__(128, SPH_MINB_STRAIN) k_strain(Dev d)
         real w[4];
         load_w(d, q, i, w);
         // vxp and m_j / rho_j (the quotient the reference forms per pair,
-        // formed once per particle by k_shepard_eos: the same value in FP64)
-        const NV nj = load_nv(d.s.svr, j);
-        const real mr = (real)nj.m;
+        // formed once per particle by k_shepard_eos: the same value in FP64;
+        // the FP32-bulk form divides its FP32 operands per pair)
+        NV nj;
+        real mr;
+        if constexpr (sizeof(real) == 8) {
+            nj = load_nv(d.s.svr, j);
+            mr = (real)nj.m;
+        } else {
+            nj = load_nv(d.s.nv, j);
+            mr = (real)nj.m / (real)d.s.rho[j];
+        }
         {
             real dvx[3];
             const double vjs[3] = {nj.vx, nj.vy, nj.vz};
@@ -1243,6 +1251,13 @@ __global__ void __launch_bounds__(128, SPH_MINB_STRESS) k_stress(Dev d)
         pp = (-satu * d.s.prew[i] + (1 - satu) * d.s.prea[i]) / r / r;
     }
     store_sr(d.s.sr, i, srk, pp, d.s.mass[i]);
+    {
+        // the drag loop's record: rho, saturation, porosity, and the soil's
+        // permeability or the fluid's density
+        double2* q = reinterpret_cast<double2*>(d.s.dr4) + 2 * (size_t)i;
+        q[0] = make_double2(r, d.s.satu[i]);
+        q[1] = make_double2(d.s.porosity[i], (ti == 2) ? d.s.cop[i] : d.s.f_dens[i]);
+    }
 }
 
 // The per-particle tensor R_i of artificial_stress_2d / artificial_stress_3d
@@ -1660,7 +1675,8 @@ __global__ void __launch_bounds__(128, LOOP ? SPH_MINB_ACCB2 : SPH_MINB_ACCB1) k
             real w[4];
             load_w(d, q, i, w);
             const NV nj = load_nv(d.s.nv, j);
-            const real mj = (real)nj.m, rj = (real)d.s.rho[j];
+            const NV dj = load_nv(d.s.dr4, j);      // (rho, satu, porosity, cop | f_dens)
+            const real mj = (real)nj.m, rj = (real)dj.vx;
             const double xj[3] = {pj.x, pj.y, pj.z};
             const double vjs[3] = {nj.vx, nj.vy, nj.vz};
             real inprod = 0, dvx[3];
@@ -1678,24 +1694,24 @@ __global__ void __launch_bounds__(128, LOOP ? SPH_MINB_ACCB2 : SPH_MINB_ACCB1) k
                     mv = sqrt(mv);
                     const int so = (ti == 2) ? i : j, wa = (ti == 2) ? j : i;
                     const real beta = (real)drag_beta(d.p.fli, d.s.porosity[so], d.s.s_ds[so], d.s.f_dens[wa],
-                                                      d.s.f_vis[wa], mv, (ti == 2) ? d.s.rho[j] : ri);
+                                                      d.s.f_vis[wa], mv, (ti == 2) ? dj.vx : ri);
                     for (int k = 0; k < nd; k++) tin[k].add(mj / rj * w3 * beta * dvx[k]);
                 } else if (ti == 2 && tj == 1) {
                     const real sa = (real)satu_i, po = (real)d.s.porosity[i], cp = (real)d.s.cop[i],
-                               fd = (real)d.s.f_dens[j];
+                               fd = (real)dj.m;
                     for (int k = 0; k < nd; k++)
                         tin[k].add(sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3);
                 } else if (ti == 1 && tj == 2) {
-                    const real sa = (real)d.s.satu[j], po = (real)d.s.porosity[j], cp = (real)d.s.cop[j],
+                    const real sa = (real)dj.vy, po = (real)dj.vz, cp = (real)dj.m,
                                fd = (real)d.s.f_dens[i];
                     for (int k = 0; k < nd; k++)
                         tin[k].add(sa * sa * po * po * fd * ga * dvx[k] / cp * mj / rj * w3);
                 } else if (ti == 2 && tj == 3) {
-                    const real sa = (real)satu_i, po = (real)d.s.porosity[i], fd = (real)d.s.f_dens[j];
+                    const real sa = (real)satu_i, po = (real)d.s.porosity[i], fd = (real)dj.m;
                     for (int k = 0; k < nd; k++)
                         tin[k].add((1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3);
                 } else if (ti == 3 && tj == 2) {
-                    const real sa = (real)d.s.satu[j], po = (real)d.s.porosity[j], fd = (real)d.s.f_dens[i];
+                    const real sa = (real)dj.vy, po = (real)dj.vz, fd = (real)d.s.f_dens[i];
                     for (int k = 0; k < nd; k++)
                         tin[k].add((1 - sa) * (1 - sa) * po * po * fd * ga * dvx[k] * 2000 * mj / rj * w3);
                 }
