@@ -390,7 +390,10 @@ __device__ __forceinline__ void pair_w_raw(const Dev& d, const PairI<R>& I, R rr
     else s = dst / ra;
     // the gradient's quotients by ra * dst
     const R D = ra * dst;
-    const R rD = f32 ? R(0) : R(1.0) / D;
+    // RN(1 / D): the correctly rounded reciprocal, the value of the IEEE
+    // quotient 1.0 / D, without the general division's scaling steps
+    R rD = R(0);
+    if constexpr (sizeof(R) == 8) rD = __drcp_rn(D);
     auto grad = [&](R num) -> R { return f32 ? num / D : (R)div_rcp(num, D, rD); };
     w[0] = w[1] = w[2] = w[3] = R(0);
     if (d.p.flknl == 1 || d.p.flknl == 3) {
