@@ -512,6 +512,52 @@ def config_leg(args, device, make, cpu_make, threads, prepare=None):
     return out
 
 
+def rain_slope_leg(args, device, threads: int, steps_run: int = 20000, K: int = 400):
+    """The 3-D rainfall slope (three phases: Drucker-Prager soil with
+    co-located pore air, rain rows over the crest falling as water, Darcy
+    drag; 8.65 M particles at dx = 50 mm) with correlated K-L friction and
+    cohesion fields (K terms, correlation 0.5, depth trend): one realisation's
+    field generation and K steps in the FP64 and FP32-bulk forms; realisations
+    per hour for steps_run steps each.  The reference on the host cores runs
+    the same scene at dx = 100 mm."""
+    import sphgpu
+    sc = scenes.rain_slope_3d(dx=0.05, steps=steps_run)
+    st = scenes.initialise(sc)
+    n_active = sc.n_active()
+    d = scenes.kl_domain(sc)
+    dom = sphgpu.kl_domain(d["nb_min"], d["nb_max"], d["soil_max"], d["water_max"])
+    fai = sphgpu.kl_field(0, 1, 25.0, 2.5, [10.0, 10.0, 1.0], 0.5)
+    coh = sphgpu.kl_field(1, 2, 10.0e3, 3.0e3, [10.0, 10.0, 1.0], 500.0)
+    u2 = np.random.Generator(np.random.Philox(20261205)).standard_normal((K, 2))
+    out = {"particles": sc.n, "active_particles": n_active, "rain_particles": int((sc.ptype == 7).sum()),
+           "kl_terms": K}
+    for form in ("fp64", "fp32_bulk"):
+        eng = sphgpu.Engine(st.params, device=device)
+        eng.load_state(st.fields, st.fluid, st.soil, st.rain)
+        t0 = time.perf_counter()
+        eng.kl_generate_corr(dom, fai, coh, 0.5, u2, K)
+        kl_s = time.perf_counter() - t0
+        if form == "fp32_bulk":
+            eng.set_precision(sphgpu.PREC_FP32_BULK)
+        eng.step(args.warmup)
+        eng.synchronize()
+        eng.step(args.steps)
+        ms = eng.last_step_ms() / args.steps
+        eng.close()
+        out[form] = {"ms_per_step": ms, "value": n_active / (ms / 1e3), "unit": "particle-updates/s",
+                     "kl_generate_s": kl_s, "rf_runs_per_hour": 3600.0 / (kl_s + steps_run * ms / 1e3)}
+    out["fp32_bulk"]["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["fp32_bulk"]["ms_per_step"]
+    if threads:
+        small = scenes.rain_slope_3d(dx=0.1, steps=steps_run)
+        r = run_reference(small, 2, 1, threads)
+        if "unavailable" not in r:
+            out["cpu_baseline"] = {"value": r["value"], "unit": "particle-updates/s", "cores": threads,
+                                   "kind": "reference", "ms_per_step": r["step_s"] * 1e3,
+                                   "sample": f"2 steps (after 1 warm-up) of {small.name} ({small.n} particles); "
+                                             f"its K-L generation not included"}
+    return out
+
+
 def rf_cholesky(device, threads: int):
     """The correlation-matrix random field (flspv 3) on the 5 m slope: one
     lognormal cohesion field over about 2,400 cells and one over about
@@ -651,6 +697,7 @@ def engine_arm(args, world, rank, local):
             "dam_break_2d_dx5mm": config_leg(args, device, dam_break_scene, dam_break_scene, thr),
             "footing_3d_camclay_dx40mm": config_leg(args, device, footing_scene, lambda: footing_scene(0.08), thr,
                                                     prepare=geostatic_soil),
+            "rain_slope_3d_dx50mm": rain_slope_leg(args, device, thr),
         }
 
     cpu = None

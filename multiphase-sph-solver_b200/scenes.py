@@ -418,6 +418,59 @@ def shaking_box(ndim: int = 2, flv: int = 1, dx: float = 0.05, box=(2.0, 1.0, 0.
     )
 
 
+def rain_slope_3d(dx: float = 0.05, H: float = 5.0, crest: float = 6.25, gradient: float = 1.5,
+                  width: float = 10.0, length: float = 20.0, rows: int = 3, steps: int = 20000,
+                  layers: int = 3) -> Scene:
+    """A 3-D rainfall slope with three phases (fla 1): the 1:`gradient` slope
+    of height H behind a `crest`-metre crest, extruded `width` metres across
+    (y; z up), in a `length`-metre box with a `layers`-layer floor, a back
+    wall and two side walls (type 0).  Drucker-Prager soil (type 2, phi 25
+    deg, c 10 kPa, E 20 MPa, rho 2000, porosity 0.4) holds co-located pore
+    air (type 3); `rows` rows of rain (type 7) over the crest fall as water
+    (rainfall type 1, lp = steps / (rows + 1)) and drain through the soil by
+    Darcy drag (fli 1, permeability 1e-4 m/s)."""
+    g = 9.81
+    nx, nw = int(round(length / dx)), int(round(width / dx))
+    nz = int(round((H + 2 * dx) / dx))
+    grid = _grid(nx, nw, nz, dx, (0.0, 0.0, 0.0))
+    x, z = grid[:, 0], grid[:, 2]
+    inside = (z < H) & ((x < crest) | (z < H - (x - crest) / gradient))
+    soil = grid[inside]
+    L = layers
+    wall_h = H + 6 * dx
+    nwz = int(round(wall_h / dx))
+    parts = [(soil, 2, 2), (soil.copy(), 3, 0)]
+    parts.append((_grid(nx + L, nw + 2 * L, L, dx, (-L * dx, -L * dx, -L * dx)), 0, 0))
+    parts.append((_grid(L, nw + 2 * L, nwz, dx, (-L * dx, -L * dx, 0.0)), 0, 0))
+    parts.append((_grid(nx, L, nwz, dx, (0.0, -L * dx, 0.0)), 0, 0))
+    parts.append((_grid(nx, L, nwz, dx, (0.0, nw * dx, 0.0)), 0, 0))
+    xp, vxp, ptype, mt, permtype, etype = _assemble(parts)
+    dp = soil_default()
+    dp.update(kapa=0.05, poi=0.3, dens=2000.0, c=10.0e3, fai=25.0, fs=1.0, beta=0.0,
+              damp1=0.0, damp2=0.0, cop=1.0e-4, eps0=0.6667, e=2.0e7, ds=1.0e-3)
+    w = fluid_default()
+    w.update(dens=1000.0, vis=1.0e-3, vpu=30.0, press_type=0, acc_type=0, bhtype=0,
+             pre_coe=30.0 * 30.0 / (7.0 * g * dx), strain_min=1.0e-3)
+    air = dict(dens=1.293, paa0=100.0, vis=1.8e-5, vpu=30.0, press_type=0, acc_type=0, pre_coe=0.0)
+    sc = Scene(
+        name=f"rain_slope_3d_dx{dx:g}", ndim=3, dr=dx, dt=0.25 * dx / 600.0 * steps, loop=steps,
+        xp=xp, vxp=vxp, ptype=ptype, matype=mt, permtype=permtype, etype=etype,
+        flags=dict(fla=1, fls=1, flr=0, fli=1, flv=0, fleob=0, flts=0, flspv=0, flknl=1,
+                   ntd=1, flbndy=1),
+        problem=dict(threshold_min=0.1, threshold_max=0.12, fop=max(steps, 1), inip=0,
+                     step_regu=100000000, dttype=2,
+                     xsph=(0.5, 0.1, 0.0), art_vis=((0.1, 0.0), (0.1, 0.0), (0.0, 0.0)),
+                     art_stre_coe=0.0, g=(0.0, 0.0, -g),
+                     interc=1.0, permtype=0, pers=1.0e-4, perl=1.0e-4, perm=1.0e-4,
+                     ss=(0, 0.0, 0.0, 0), if_cal=0, if_move=0, coe_bndy=0.3),
+        water=[w, copy.deepcopy(w), copy.deepcopy(w)],
+        air=air,
+        model_flags=(0, 0, 1, 0, 0, 0, 0, 0, 0, 0),
+        soils={2: dp},
+    )
+    return add_rain(sc, 0.0, crest, rows, H + 2 * dx)
+
+
 def add_rain(scene: Scene, x0: float, x1: float, rows: int, top: float, press_factor: float = 1.0,
              drop_velocity: float = -1.0) -> Scene:
     """Rain particles (type 7, etype 1: water waiting to fall) appended to

@@ -306,6 +306,10 @@ CASES = {
     "shaking_box_2d_flv2": (lambda: scenes.shaking_box(ndim=2, flv=2, dx=0.05), 36),
     "shaking_box_3d_flv1": (lambda: scenes.shaking_box(ndim=3, flv=1, dx=0.1), 24),
     "shaking_box_3d_flv2": (lambda: scenes.shaking_box(ndim=3, flv=2, dx=0.1), 24),
+    # the 3-D rainfall slope, reduced: three phases (soil, pore air, rain
+    # falling as water), Darcy drag, rows released every lp = 15 steps
+    "rain_slope_3d_dx0.25": (lambda: scenes.rain_slope_3d(dx=0.25, H=2.0, crest=2.0, width=1.5, length=5.0,
+                                                          steps=60), 50),
 }
 
 

@@ -22,7 +22,10 @@ named per case.
   Cam-clay under TSSMP (cd > 0) and regularisation every 4 steps;
 * rainfall (flr 1): three rows of rain particles released on the device every
   lp steps (rainpro, CPP_15-1-rain.cpp:43-85) and a water particle taken out
-  past the domain's left end (partidel, CPP_15-2-partidel.cpp:19-58).
+  past the domain's left end (partidel, CPP_15-2-partidel.cpp:19-58);
+* the 3-D rainfall slope, reduced: soil with co-located pore air (fla 1),
+  rain rows over the crest falling as water onto it, Darcy drag between all
+  three phases.
 """
 import numpy as np
 import pytest
@@ -50,6 +53,7 @@ CASES = {
     "soil_column_3d_dx0.1_geostatic_camclay": 1e-12,
     "slope_2d_H1_dx0.05_geostatic": 0.0,
     "dam_break_2d_dx0.04_rain": 0.0,
+    "rain_slope_3d_dx0.25": 0.0,
 }
 RATIO_FIELDS = {"divr"}
 

@@ -31,7 +31,7 @@ CASES = ["dam_break_2d_dx0.04", "soil_column_3d_dx0.1", "soil_column_3d_dx0.1_kg
          "soil_column_3d_dx0.1_moving_wall", "soil_column_3d_dx0.1_geostatic",
          "soil_column_3d_dx0.1_geostatic_camclay", "slope_2d_H1_dx0.05_geostatic",
          "dam_break_2d_dx0.04_rain", "shaking_box_2d_flv1", "shaking_box_2d_flv2", "shaking_box_3d_flv1",
-         "shaking_box_3d_flv2"]
+         "shaking_box_3d_flv2", "rain_slope_3d_dx0.25"]
 
 
 def _golden(name):
