@@ -682,6 +682,26 @@ def engine_arm(args, world, rank, local):
     e2e_value = total_active * args.steps / t_e2e
     eng2.close()
 
+    shuffled = None
+    if not args.no_configs:
+        # the same workload with the particles in a random order (a caller's
+        # Particle array need not be spatial): the neighbour gathers then hit
+        # scattered records
+        perm = np.random.Generator(np.random.Philox(20261206)).permutation(scene.n)
+        fields_p = {k: np.asarray(v)[perm] for k, v in st.fields.items()}
+        eng3 = sphgpu.Engine(st.params, device=device)
+        eng3.load_state(fields_p, np.asarray(st.fluid)[perm], np.asarray(st.soil)[perm])
+        del fields_p
+        eng3.step(args.warmup)
+        eng3.synchronize()
+        eng3.step(args.steps)
+        sh_ms = eng3.last_step_ms() / args.steps
+        sh_prof = eng3.step_profiled(args.steps)
+        eng3.close()
+        shuffled = {"ms_per_step": sh_ms, "value": n_active / (sh_ms / 1e3), "unit": "particle-updates/s",
+                    "slowdown_vs_spatial_order": sh_ms / (ms_max / args.steps),
+                    "stage_ms_per_step": {k: v / args.steps for k, v in sh_prof.items() if v > 0.01},
+                    "what": "the same particles in a random order (Philox seed 20261206)"}
     bulk_ms, bulk_err, bulk_prof = bulk_form(st, args, device, ref_fields, moving)
     bulk_ms = dist_max(bulk_ms, world)
     kl = kl_synthesis(eng, scene, device) if not args.no_kl else None
@@ -745,6 +765,7 @@ def engine_arm(args, world, rank, local):
             "kl_synthesis": kl,
             "batched_slopes": batched,
             "configs": others,
+            "shuffled_order": shuffled,
             "rf_cholesky": rf,
             "e2e": {"value": e2e_value, "unit": "particle-updates/s",
                     "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
