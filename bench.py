@@ -652,7 +652,7 @@ def engine_arm(args, world, rank, local):
     achieved = dom["achieved_gbs"]
     # the pass's kernels as ncu names them (the momentum stage launches two
     # loop kernels and a tail kernel under the stage name k_accel_b)
-    ncu_names = {"k_accel_b": ("k_accel_b", "k_accel_b_tail")}
+    ncu_names = {"k_accel_b": ("k_accel_b", "k_accel_b_drag", "k_accel_b_tail")}
     pass_kernels = [q for k in dom["kernels"] if stage_ms.get(k, 0.0) > 0.01 for q in ncu_names.get(k, (k,))]
     per_kernel = ncu_traffic()
     traffic = (sum(per_kernel[k] for k in pass_kernels)

@@ -49,6 +49,8 @@ extern "C" {
 #define SPHGPU_E_NODEVICE   102   /* no CUDA device or the kernels failed to load */
 #define SPHGPU_E_UNSUPPORTED 103  /* a flag combination this engine does not run */
 #define SPHGPU_E_STATE      104   /* call order (e.g. step before upload)        */
+#define SPHGPU_E_CHECK      106   /* bounds-checked build (libsphgpu_check.so): an index of the
+                                     neighbour search out of range or inconsistent */
 
 /* Para_Fluid, field for field (Class_ParticleProperty.h:107-133). */
 typedef struct sphgpu_fluid {

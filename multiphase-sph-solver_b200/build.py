@@ -18,6 +18,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsphgpu.so")
+# the bounds-checked build (SPHGPU_CHECK=1): the same sources with an index
+# check after the neighbour search that sets an error code instead of trapping
+LIB_CHECK = os.path.join(HERE, "libsphgpu_check.so")
 SOURCES = ["sph_kernels.cu", "sph_capi.cu", "sph_noalloc.cu", "sph_kernels_bulk32.cu", "sph_kl.cu", "sph_kl_tc.cu",
            "sph_rf.cu"]
 # per-source flags on top of NVCC_FLAGS
@@ -31,24 +34,25 @@ NVCC_FLAGS = [
 ]
 
 
-def _stale() -> bool:
-    if not os.path.exists(LIB):
+def _stale(lib: str = LIB) -> bool:
+    if not os.path.exists(lib):
         return True
-    t = os.path.getmtime(LIB)
+    t = os.path.getmtime(lib)
     deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS] + [__file__]
     return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not _stale():
-        return LIB
+def build(force: bool = False, verbose: bool = False, check: bool = False) -> str:
+    lib = LIB_CHECK if check else LIB
+    if not force and not _stale(lib):
+        return lib
     nvcc = os.environ.get("NVCC", "nvcc")
-    objdir = os.path.join(HERE, "_build")
+    objdir = os.path.join(HERE, "_build_check" if check else "_build")
     os.makedirs(objdir, exist_ok=True)
     procs, objs = [], []
     for src in SOURCES:
         obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
-        flags = SOURCE_FLAGS.get(src, ["-fmad=false"])
+        flags = SOURCE_FLAGS.get(src, ["-fmad=false"]) + (["-DSPHGPU_CHECK=1"] if check else [])
         cmd = [nvcc] + NVCC_FLAGS + flags + ["-c", "-o", obj, os.path.join(CSRC, src)]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
@@ -58,10 +62,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
     for p in procs:
         if p.wait() != 0:
             raise subprocess.CalledProcessError(p.returncode, "nvcc")
-    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB] + objs, check=True)
-    return LIB
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", lib] + objs, check=True)
+    return lib
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
-    print(LIB)
+    check = "--check" in sys.argv
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv, check=check))

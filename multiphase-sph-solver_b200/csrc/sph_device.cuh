@@ -31,6 +31,10 @@
 #define SPH_ERR_CELL 3         // parttocell, CPP_3-NNPS.cpp:247-257
 #define SPH_ERR_NEIGH 5        // partisearching, CPP_3-NNPS.cpp:313-319
 #define SPHK_NSTAGES 21        // entries of sphk_stage_names (one event bracket each)
+#ifndef SPHGPU_CHECK
+#define SPHGPU_CHECK 0         // 1: the bounds-checked build (k_check_lists after the search)
+#endif
+#define SPH_ERR_CHECK 106      // its error code (SPHGPU_E_CHECK)
 
 // One instance of a batched context: its particle range, its own cell grid
 // (Cell_Con, celllist_ini1) and where its cells start in the context's cell

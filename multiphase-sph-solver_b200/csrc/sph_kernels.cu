@@ -3016,6 +3016,40 @@ static_assert(sizeof(sphk_stage_names) / sizeof(sphk_stage_names[0]) == SPHK_NST
 // the bits of `parts`: 1 parttocell (cell keys, the sort, cell ranges),
 // 2 partisearching (the search and the pair records), 4 the kernel gradient
 // correction; returns the number of this library's kernels it launched
+#if SPHGPU_CHECK
+// The bounds-checked build (SPHGPU_CHECK=1): after the search, every index the
+// later passes take from it is checked -- each list slot holds a particle
+// other than i within [0, N), the slot masks mark exactly the slots of their
+// type, the sorted order is a permutation and the cell ranges stay within the
+// sorted positions.  A violation sets the error word to SPH_ERR_CHECK (the
+// passes after it then return at once) instead of trapping.
+__global__ void k_check_lists(Dev d)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N || *d.s.err) return;
+    bool bad = false;
+    const int nn = nbr_count(d, i);
+    if (nn < 0 || nn > SPH_NB_CAP) bad = true;
+    const int q = d.s.sortpos[i];
+    if (q < 0 || q >= N || d.s.pid_sorted[q] != i) bad = true;
+    for (int s = 0; s < nn && !bad; s++) {
+        const int j = d.s.nbr[(size_t)s * N + i];
+        if (j < 0 || j >= N || j == i) { bad = true; break; }
+        const int tj = d.s.type[j];
+        for (int t = 0; t <= 4; t++) {
+            const SlotMask m = type_mask(d, i, t);
+            if (m.has(s) != (tj == t)) bad = true;
+        }
+    }
+    const int c = d.s.cell[i];
+    if (c >= 0 && c < d.p.ctotal + 4) {
+        const int a = d.s.cstart[c], b = d.s.cend[c];
+        if (a <= b && (a < 0 || b >= N)) bad = true;
+    }
+    if (bad) atomicCAS(d.s.err, 0, SPH_ERR_CHECK);
+}
+#endif
+
 extern "C" int sphk_enqueue_nnps_parts(const Dev* dp, void* sort_tmp, size_t sort_bytes, int end_bit,
                                        cudaStream_t st, cudaEvent_t* ev, int parts)
 {
@@ -3041,6 +3075,9 @@ extern "C" int sphk_enqueue_nnps_parts(const Dev* dp, void* sort_tmp, size_t sor
         REC(5);
         LAUNCH_ND(k_nnps_resolve, nblk(N, tbk(d, TP_RESOLVE)), tbk(d, TP_RESOLVE), d); n++;
         REC(6);
+#if SPHGPU_CHECK
+        k_check_lists<<<nblk(N, 128), 128, 0, st>>>(d); n++;
+#endif
         LAUNCH_ND(k_pairw, nblk(N, tbk(d, TP_PAIRW)), tbk(d, TP_PAIRW), d); n++;
     }
     if (parts & 4) {

@@ -217,7 +217,7 @@ def rf_flags(cell_ndx: float, flag_auto: int = 1, beta: float = 0.0, beta_1: flo
 ERRORS = {0: "ok", 3: "particle outside the cell grid", 41: "no random-field cells, or 15,000 or more",
           42: "a random-field cell holds more than 39 particles", 5: "more than 99 neighbours",
           100: "bad argument", 101: "CUDA error", 102: "no CUDA device", 103: "unsupported flags",
-          104: "call order", 105: "tensor-core wait expired"}
+          104: "call order", 105: "tensor-core wait expired", 106: "index check failed (bounds-checked build)"}
 
 
 class SPHError(RuntimeError):
@@ -229,11 +229,18 @@ class SPHError(RuntimeError):
 _lib = None
 
 
+CHECK_LIB_PATH = os.path.join(HERE, "libsphgpu_check.so")
+_libs: dict = {}
+
+
 def load_library(path: str = LIB_PATH) -> C.CDLL:
-    """Load libsphgpu.so (raises if it was not built)."""
+    """Load libsphgpu.so, or another build of it such as the bounds-checked
+    libsphgpu_check.so (raises if it was not built)."""
     global _lib
-    if _lib is not None:
+    if path == LIB_PATH and _lib is not None:
         return _lib
+    if path in _libs:
+        return _libs[path]
     if not os.path.exists(path):
         raise FileNotFoundError(f"{path} is not built; run __graft_entry__.build()")
     lib = C.CDLL(path)
@@ -306,7 +313,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_checkpoint_save.argtypes = [C.c_void_p, C.c_char_p]
     lib.sphgpu_checkpoint_load.argtypes = [C.c_void_p, C.c_char_p]
     lib.sphgpu_get_rain.argtypes = [C.c_void_p, C.POINTER(Rain)]
-    _lib = lib
+    if path == LIB_PATH:
+        _lib = lib
+    _libs[path] = lib
     return lib
 
 
@@ -319,8 +328,8 @@ class Engine:
     batched context of several systems that share `params` but for their
     particle ranges and cell grids (sphgpu_create_batched)."""
 
-    def __init__(self, params: dict | Params, device: int = 0, instances=None):
-        self.lib = load_library()
+    def __init__(self, params: dict | Params, device: int = 0, instances=None, library: str | None = None):
+        self.lib = load_library(library) if library else load_library()
         if self.lib.sphgpu_device_count() <= 0:
             raise SPHError(102, "sphgpu_device_count")
         self.params = params if isinstance(params, Params) else params_from_dict(params)
