@@ -294,6 +294,34 @@ int sphgpu_set_cfl(sphgpu_ctx* ctx, double cfl, double cfl_force);
 int sphgpu_get_dt(sphgpu_ctx* ctx, double* dt);
 
 /*
+ * Re-sorted state (an addition of this library; the reference keeps its
+ * particle array in input order and only sorts an index list, Binary_Sort,
+ * CPP_3-NNPS.cpp:561-630).  With every_steps > 0, sphgpu_step and
+ * sphgpu_step_profiled gather the whole particle state on the device into a
+ * spatial order -- by type and material, then rows of a lattice of spacing dr
+ * over the grid (over each batched instance's own grid) along the search's
+ * fastest axis -- before the
+ * next step and then every every_steps steps, so the neighbour gathers of the
+ * passes read nearby records whatever order the caller's particles came in or
+ * have mixed into.  Every result stays the one of the caller's order, bit for bit: the
+ * device keeps the map between the orders, and the passes whose result
+ * depends on the particle numbering (the search's order inside a cell, the
+ * rain rows, check_domain's first wall, tm_boundary's default wall, the order
+ * of a structure particle's contact reactions) go through it.  Every call that
+ * exchanges per-particle data with the host, or runs part of a step through
+ * the method entries, first gathers the state back into the caller's order
+ * (on the device; the result-file snapshot of sphgpu_output_step writes its
+ * rows through the map instead).  0 (the default) keeps the caller's order.
+ * sphgpu_get_order copies the map out: i2o[i] = the caller's index of the
+ * particle held at i (N ints).  sphgpu_last_reorder_ms is the device time the
+ * re-sorts of the last sphgpu_step_profiled call took.
+ */
+int sphgpu_set_reorder(sphgpu_ctx* ctx, int every_steps);
+int sphgpu_get_reorder(const sphgpu_ctx* ctx);
+int sphgpu_get_order(sphgpu_ctx* ctx, int* i2o);
+double sphgpu_last_reorder_ms(const sphgpu_ctx* ctx);
+
+/*
  * Rainfall (flr == 1): the reference's Para_Rain (Class_Problem.h) as its
  * input block RP sets it, with nrain the number of rain particles still
  * waiting (type 7, etype 1; input_par counts them, CPP_2-initialf.cpp:979-

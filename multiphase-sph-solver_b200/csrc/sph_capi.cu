@@ -40,6 +40,9 @@ extern "C" int sphk_kl_field(int n, int ndim, int K, int no, int type, const dou
                              double sd_value, double coe_depth, double soil_max, double water_max, const double* d_xh,
                              const int* d_type, const void* d_terms, const double* d_sqrt_eig, const double* d_xi,
                              double* d_out, cudaStream_t st);
+extern "C" size_t sphk_order_temp_bytes(int N, int end_bit);
+extern "C" int sphk_order_sort(const Dev* dp, void* tmp, size_t bytes, int end_bit, unsigned long long* kin,
+                               unsigned long long* kout, int* vin, int* vout, cudaStream_t st);
 extern "C" size_t sphk_kl_term_bytes(void);
 extern "C" int sphk_kl_wait_probe(long long budget, int* d_err, cudaStream_t st);
 extern "C" size_t sphk_kl_tc_term_bytes(void);
@@ -58,6 +61,13 @@ extern "C" int sphk_rf_assign(const int* ip, const double* dp, const double* d_L
 namespace {
 
 thread_local int g_create_error = 0;
+
+// the held order equal to the caller's
+__global__ void k_order_identity(int* i2o, int* o2i, int N)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) { i2o[i] = i; o2i[i] = i; }
+}
 
 struct FieldDef {
     const char* name;
@@ -177,6 +187,21 @@ struct sphgpu_ctx {
     long out_ticket = 0, out_turn = 0;
     std::vector<InstGrid> h_inst;     // batched context: the instance table (empty: one system)
     InstGrid* d_inst = nullptr;
+    // the re-sorted state (sphgpu_set_reorder): re-sort every reorder_every
+    // steps (0: never), steps run since the last re-sort, whether the state
+    // is held out of the caller's order; the gather buffer, and the order
+    // keys, their sort's permutation and its work space
+    int reorder_every = 0;
+    long since_sort = 0;
+    bool permuted = false;
+    void* perm_tmp = nullptr;
+    size_t perm_tmp_bytes = 0;
+    unsigned long long *ord_kin = nullptr, *ord_kout = nullptr;
+    int *ord_vin = nullptr, *ord_vout = nullptr;
+    void* ord_tmp = nullptr;
+    size_t ord_bytes = 0;
+    int ord_end_bit = 0;
+    double reorder_ms = 0.0;          // device time of the re-sorts of the last sphgpu_step_profiled
 };
 
 namespace {
@@ -340,6 +365,189 @@ void invalidate_graphs(sphgpu_ctx* c)
 {
     for (int p = 0; p < 2; p++)
         if (c->exec[p]) { cudaGraphExecDestroy(c->exec[p]); c->exec[p] = nullptr; }
+}
+
+// ---------------------------------------------------------------------------
+// Re-sorted state.  With sphgpu_set_reorder(c, R), R > 0, sphgpu_step gathers
+// the whole particle state on the device every R steps into a spatial order
+// (k_order_key: by type and material, then rows of a lattice of spacing dr),
+// so that the neighbour gathers of every pass read nearby records whatever
+// order the caller's particles came in or have mixed into.  i2o / o2i map
+// between the held order and the caller's; the kernels whose result depends
+// on the caller's numbering (the cell keys' tie order, the rain rows,
+// check_domain's first wall, tm_boundary's default wall, the structure's
+// reaction order) read them, so every result is the caller's order's.  The
+// entries that exchange per-particle data with the host or run part of a
+// step first put the state back in the caller's order; the result-file
+// snapshot writes its rows through i2o instead.
+
+// one array of the state: cols columns of esz-byte elements, column-major
+// (element (i, k) at k N + i) or, with aos set, records of cols elements
+struct PermArr { void* p; int esz; int cols; int aos; };
+
+// the arrays a later step reads (every device-owned Particle member, the
+// material constants, the walls' per-phase records, the stiffness of the
+// last stress update, the batched instance of each particle); the per-step
+// intermediates and the search's arrays are rewritten by the next step
+std::vector<PermArr> perm_arrays(const sphgpu_ctx* c, int parity)
+{
+    const DevState& s = c->d[parity].s;
+    std::vector<PermArr> v;
+    auto i4 = [&](void* p) { if (p) v.push_back({p, 4, 1, 0}); };
+    auto f8 = [&](void* p, int cols) { if (p) v.push_back({p, 8, cols, 0}); };
+    i4(s.type); i4(s.matype); i4(s.etype); i4(s.permtype); i4(s.f_bhtype); i4(s.pinst);
+    for (double* p : {s.mass, s.cd, s.f_dens, s.f_por, s.f_vpu, s.f_vis, s.f_c, s.f_smin, s.f_tanfai,
+                      s.s_e, s.s_poi, s.s_eps0, s.s_dens, s.s_kapa, s.s_por, s.s_vpu, s.s_cop, s.s_sitas,
+                      s.s_sitar, s.s_ds, s.s_c, s.s_fs, s.s_ann, s.s_zmf, s.s_ramda, s.s_sme0, s.s_yalf,
+                      s.s_ykap, s.s_yalf_dil})
+        f8(p, 1);
+    f8(s.s_ext, SX_COUNT);
+    if (s.xh) v.push_back({s.xh, 8, 4, 1});
+    for (double* p : {s.vx, s.vxp, s.axp, s.ax, s.ux, s.interf, s.interfss, s.strep, s.vel_bndy, s.vx_vb})
+        f8(p, 3);
+    for (double* p : {s.rho, s.rhop, s.pre, s.prep, s.porosity, s.poro_cop, s.e, s.tsqc, s.satu, s.dsatu,
+                      s.suct, s.cop, s.prew, s.prea, s.vsig, s.veps, s.divq, s.divr, s.meps, s.stiff})
+        f8(p, 1);
+    for (double* p : {s.sig, s.eps, s.adps, s.tssig}) f8(p, 6);
+    f8(s.vb, 12);
+    f8(s.sb, 24);
+    return v;
+}
+
+// dst = src gathered by perm: the new i-th particle is the old perm[i]-th
+template <typename T>
+__global__ void k_perm_gather(const T* __restrict__ src, T* __restrict__ dst, const int* __restrict__ perm, int N,
+                              int cols, int aos)
+{
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t >= (size_t)N * cols) return;
+    if (aos) {
+        const size_t q = t / cols, k = t - q * cols;
+        dst[t] = src[(size_t)perm[q] * cols + k];
+    } else {
+        const size_t k = t / N, q = t - k * N;
+        dst[t] = src[k * N + perm[q]];
+    }
+}
+
+template <typename T>
+__global__ void k_perm_copy(const T* __restrict__ src, T* __restrict__ dst, size_t n)
+{
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t < n) dst[t] = src[t];
+}
+
+// after a re-sort by perm: the held particle i is the caller's i2o[perm[i]]
+__global__ void k_order_compose(const int* __restrict__ perm, const int* __restrict__ i2o, int* __restrict__ out,
+                                int N)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) out[i] = i2o[perm[i]];
+}
+
+__global__ void k_order_inverse(const int* __restrict__ i2o, int* __restrict__ o2i, int N)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) o2i[i2o[i]] = i;
+}
+
+unsigned perm_blocks(size_t n) { return (unsigned)((n + 255) / 256); }
+
+int ensure_perm_tmp(sphgpu_ctx* c, size_t bytes)
+{
+    if (c->perm_tmp_bytes >= bytes) return 0;
+    if (c->perm_tmp) {
+        CK(cudaStreamSynchronize(c->st));
+        cudaFree(c->perm_tmp);
+    }
+    c->perm_tmp = nullptr;
+    c->perm_tmp_bytes = 0;
+    CK(cudaMalloc(&c->perm_tmp, bytes));
+    c->perm_tmp_bytes = bytes;
+    return 0;
+}
+
+// every array of the state (the buffers of `parity`) gathered by perm, on
+// the context's stream, and the maps moved with them
+int enqueue_permute(sphgpu_ctx* c, int parity, const int* perm)
+{
+    const std::vector<PermArr> arr = perm_arrays(c, parity);
+    const int N = c->N;
+    size_t most = 4 * (size_t)N;
+    for (const PermArr& a : arr) most = std::max(most, (size_t)a.esz * a.cols * N);
+    int r = ensure_perm_tmp(c, most);
+    if (r) return r;
+    for (const PermArr& a : arr) {
+        const size_t n = (size_t)a.cols * N;
+        if (a.esz == 8) {
+            k_perm_gather<double><<<perm_blocks(n), 256, 0, c->st>>>((const double*)a.p, (double*)c->perm_tmp,
+                                                                     perm, N, a.cols, a.aos);
+            k_perm_copy<double><<<perm_blocks(n), 256, 0, c->st>>>((const double*)c->perm_tmp, (double*)a.p, n);
+        } else {
+            k_perm_gather<int><<<perm_blocks(n), 256, 0, c->st>>>((const int*)a.p, (int*)c->perm_tmp, perm, N,
+                                                                  a.cols, a.aos);
+            k_perm_copy<int><<<perm_blocks(n), 256, 0, c->st>>>((const int*)c->perm_tmp, (int*)a.p, n);
+        }
+    }
+    const DevState& s = c->d[parity].s;
+    int* tmp = (int*)c->perm_tmp;
+    k_order_compose<<<perm_blocks(N), 256, 0, c->st>>>(perm, s.i2o, tmp, N);
+    k_perm_copy<int><<<perm_blocks(N), 256, 0, c->st>>>(tmp, s.i2o, (size_t)N);
+    k_order_inverse<<<perm_blocks(N), 256, 0, c->st>>>(s.i2o, s.o2i, N);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+// the state re-sorted into the order of k_order_key over its current
+// positions (the buffers of `parity`)
+int sort_state(sphgpu_ctx* c, int parity)
+{
+    const int N = c->N;
+    if (!c->ord_kin) {
+        int r = dalloc(c, &c->ord_kin, (size_t)N);
+        r |= dalloc(c, &c->ord_kout, (size_t)N);
+        r |= dalloc(c, &c->ord_vin, (size_t)N);
+        r |= dalloc(c, &c->ord_vout, (size_t)N);
+        if (r) return r;
+        // keys stay below 512 groups x 8 (ctotal + 1): the bits the sort looks at
+        const unsigned long long top = 512ull * 8ull * ((unsigned long long)c->P.ctotal + 1);
+        int b = 1;
+        while (b < 64 && (1ull << b) <= top) b++;
+        c->ord_end_bit = b;
+        c->ord_bytes = sphk_order_temp_bytes(N, b);
+        CK(cudaMalloc(&c->ord_tmp, c->ord_bytes + 256));
+        c->allocs.push_back(c->ord_tmp);
+    }
+    sphk_order_sort(&c->d[parity], c->ord_tmp, c->ord_bytes, c->ord_end_bit, c->ord_kin, c->ord_kout, c->ord_vin,
+                    c->ord_vout, c->st);
+    int r = enqueue_permute(c, parity, c->ord_vout);
+    if (r) return r;
+    c->permuted = true;
+    c->since_sort = 0;
+    return 0;
+}
+
+// the state put back in the caller's order (a no-op when it is there), done
+// when the call returns
+int to_caller_order(sphgpu_ctx* c)
+{
+    if (!c->permuted) return 0;
+    cudaSetDevice(c->device);
+    // perm = o2i: the gathers and the new i2o (the identity) read it before
+    // the last launch of enqueue_permute rewrites it (the identity too)
+    int r = enqueue_permute(c, c->parity, c->d[c->parity].s.o2i);
+    if (r) return r;
+    CK(cudaStreamSynchronize(c->st));
+    c->permuted = false;
+    c->since_sort = 1L << 40;
+    return 0;
+}
+
+// the re-sort due before the next step, if any
+int sort_if_due(sphgpu_ctx* c, int parity)
+{
+    if (c->reorder_every <= 0 || c->since_sort < c->reorder_every) return 0;
+    return sort_state(c, parity);
 }
 
 // a loop over [0, n) split across host threads (gathers and copies of large
@@ -665,6 +873,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     r |= dalloc(c, &s.interf, 3 * (size_t)N); r |= dalloc(c, &s.interfss, 3 * (size_t)N); r |= dalloc(c, &s.strep, 3 * (size_t)N);
     r |= dalloc(c, &s.vsig, N); r |= dalloc(c, &s.veps, N); r |= dalloc(c, &s.divq, N); r |= dalloc(c, &s.divr, N);
     r |= dalloc(c, &s.meps, N);
+    r |= dalloc(c, &s.i2o, N); r |= dalloc(c, &s.o2i, N);
     r |= dalloc(c, &s.cell, N); r |= dalloc(c, &s.key_in, N); r |= dalloc(c, &s.key_out, N);
     r |= dalloc(c, &s.val_in, N); r |= dalloc(c, &s.pid_sorted, N);
     r |= dalloc(c, &s.cstart, M); r |= dalloc(c, &s.cend, M);
@@ -686,6 +895,8 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     int one = 1;
     if (cudaMemcpyAsync(s.step, &one, sizeof(int), cudaMemcpyHostToDevice, c->st) != cudaSuccess)
         return fail(SPHGPU_E_CUDA);
+    k_order_identity<<<(N + 255) / 256, 256, 0, c->st>>>(s.i2o, s.o2i, N);
+    if (cudaGetLastError() != cudaSuccess) return fail(SPHGPU_E_CUDA);
     c->end_bit = end_bit_for(P->ctotal);
     c->sort_bytes = sphk_sort_temp_bytes(N, c->end_bit);
     if (cudaMalloc(&c->sort_tmp, c->sort_bytes + 256) != cudaSuccess) return fail(SPHGPU_E_CUDA);
@@ -732,6 +943,7 @@ void sphgpu_destroy(sphgpu_ctx* c)
     if (c->st) cudaStreamSynchronize(c->st);
     invalidate_graphs(c);
     for (void* p : c->allocs) cudaFree(p);
+    if (c->perm_tmp) cudaFree(c->perm_tmp);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->mat_pinned) cudaFreeHost(c->mat_pinned);
     for (int b = 0; b < 2; b++) {
@@ -796,6 +1008,7 @@ int sphgpu_set_field(sphgpu_ctx* c, const char* name, const void* host, size_t c
     const int N = c->N, nc = f->ncomp;
     if (count != (size_t)N * nc) return SPHGPU_E_ARG;
     cudaSetDevice(c->device);
+    if (const int ro = to_caller_order(c)) return ro;
     if (std::strcmp(name, "x") == 0) {
         c->h_x.assign((const double*)host, (const double*)host + (size_t)N * 3);
         c->x_tracked = true;
@@ -845,6 +1058,7 @@ int sphgpu_get_field(sphgpu_ctx* c, const char* name, void* host, size_t count)
     const int N = c->N, nc = f->ncomp;
     if (count != (size_t)N * nc) return SPHGPU_E_ARG;
     cudaSetDevice(c->device);
+    if (const int ro = to_caller_order(c)) return ro;
     if (std::strcmp(name, "x") == 0) {
         // Particle::x is written only by update (CPP_12-1-update.cpp:30-47):
         // after a step it equals xp for moving particles and keeps its
@@ -897,6 +1111,7 @@ int sphgpu_set_materials(sphgpu_ctx* c, const sphgpu_fluid* fl, const sphgpu_soi
 {
     if (!c || n != c->N) return SPHGPU_E_ARG;
     cudaSetDevice(c->device);
+    if (const int ro = to_caller_order(c)) return ro;
     // the host copies (K-L fields rewrite members of them and upload them
     // again), written in the same pass that stages the caller's records for
     // the device; the per-particle constants below read the caller's records
@@ -1082,6 +1297,7 @@ int download_by_fields(sphgpu_ctx* c, char* base, int n, size_t stride)
 int sphgpu_upload_particles(sphgpu_ctx* c, const void* particles, int n, size_t stride)
 {
     if (!c || !particles || n != c->N || stride < kParticleBytes) return SPHGPU_E_ARG;
+    if (const int ro = to_caller_order(c)) return ro;
     if (stride % 8 != 0 || ((uintptr_t)particles) % 8 != 0)
         return upload_by_fields(c, (const char*)particles, n, stride);
     cudaSetDevice(c->device);
@@ -1112,6 +1328,7 @@ int sphgpu_upload_particles(sphgpu_ctx* c, const void* particles, int n, size_t 
 int sphgpu_download_particles(sphgpu_ctx* c, void* particles, int n, size_t stride)
 {
     if (!c || !particles || n != c->N || stride < kParticleBytes) return SPHGPU_E_ARG;
+    if (const int ro = to_caller_order(c)) return ro;
     if (stride % 8 != 0 || ((uintptr_t)particles) % 8 != 0)
         return download_by_fields(c, (char*)particles, n, stride);
     cudaSetDevice(c->device);
@@ -1188,6 +1405,11 @@ int run_parts(sphgpu_ctx* c, int upto)
         if (r) return r;
     }
     cudaSetDevice(c->device);
+    if (c->part_done == 0) {
+        // the method entries run on the caller's order
+        int r = to_caller_order(c);
+        if (r) return r;
+    }
     const Dev* d = &c->d[c->parity];
     int parts = 0;
     if (c->part_done < 1 && upto >= 1) parts |= 1;
@@ -1355,7 +1577,13 @@ int sphgpu_step(sphgpu_ctx* c, int nsteps)
     }
     const int l0 = c->l_host;
     CK(cudaEventRecord(c->ev0, c->st));
-    for (int s = 0; s < nsteps; s++) CK(cudaGraphLaunch(c->exec[(c->parity + s) & 1], c->st));
+    for (int s = 0; s < nsteps; s++) {
+        const int p = (c->parity + s) & 1;
+        r = sort_if_due(c, p);
+        if (r) return r;
+        CK(cudaGraphLaunch(c->exec[p], c->st));
+        c->since_sort++;
+    }
     CK(cudaEventRecord(c->ev1, c->st));
     CK(cudaStreamSynchronize(c->st));
     float ms = 0.f;
@@ -1369,6 +1597,27 @@ int sphgpu_step(sphgpu_ctx* c, int nsteps)
     c->l_host = l;
     return err;
 }
+
+int sphgpu_set_reorder(sphgpu_ctx* c, int every_steps)
+{
+    if (!c || every_steps < 0) return SPHGPU_E_ARG;
+    c->reorder_every = every_steps;
+    c->since_sort = 1L << 40;        // the first re-sort before the next step
+    return 0;
+}
+
+int sphgpu_get_reorder(const sphgpu_ctx* c) { return c ? c->reorder_every : -1; }
+
+int sphgpu_get_order(sphgpu_ctx* c, int* i2o)
+{
+    if (!c || !i2o) return SPHGPU_E_ARG;
+    cudaSetDevice(c->device);
+    CK(cudaMemcpyAsync(i2o, c->d[0].s.i2o, sizeof(int) * (size_t)c->N, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+double sphgpu_last_reorder_ms(const sphgpu_ctx* c) { return c ? c->reorder_ms : 0.0; }
 
 int sphgpu_set_cfl(sphgpu_ctx* c, double cfl, double cfl_force)
 {
@@ -1446,6 +1695,7 @@ int sphgpu_checkpoint_save(sphgpu_ctx* c, const char* path)
     if (!c || !path) return SPHGPU_E_ARG;
     if (c->sticky) return c->sticky;
     if (c->part_done) return SPHGPU_E_STATE;          // between steps only
+    if (const int ro = to_caller_order(c)) return ro;
     FILE* f = std::fopen(path, "wb");
     if (!f) return SPHGPU_E_ARG;
     int rc = 0;
@@ -1495,6 +1745,7 @@ int sphgpu_checkpoint_load(sphgpu_ctx* c, const char* path)
 {
     if (!c || !path) return SPHGPU_E_ARG;
     if (c->sticky) return c->sticky;
+    if (const int ro = to_caller_order(c)) return ro;
     FILE* f = std::fopen(path, "rb");
     if (!f) return SPHGPU_E_ARG;
     CkHeader h;
@@ -1572,7 +1823,7 @@ __global__ void k_out_pack(Dev d, double* out)
     if (i == 0) out[(size_t)N * kOutCols] = *d.s.tsim;
     if (i >= N) return;
     const DevState& s = d.s;
-    double* o = out + (size_t)i * kOutCols;
+    double* o = out + (size_t)s.i2o[i] * kOutCols;     // row of the caller's index
     const Pos p = load_pos(s.xh, i);
     o[0] = p.x; o[1] = p.y; o[2] = p.z;
     const double u0 = s.ux[i], u1 = s.ux[N + i], u2 = s.ux[2 * N + i];
@@ -1945,6 +2196,7 @@ int sphgpu_nnps(sphgpu_ctx* c, int* ninflu, int* influ)
     if (!c) return SPHGPU_E_ARG;
     if (c->sticky) return c->sticky;
     cudaSetDevice(c->device);
+    if (const int ro = to_caller_order(c)) return ro;
     sphk_enqueue_nnps(&c->d[c->parity], c->sort_tmp, c->sort_bytes, c->end_bit, c->st, nullptr);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(c->st));
@@ -1995,12 +2247,24 @@ int sphgpu_step_profiled(sphgpu_ctx* c, int nsteps, double* stage_ms)
     for (int k = 0; k <= SPHK_NSTAGES; k++) CK(cudaEventCreate(&ev[k]));
     for (int k = 0; k < SPHK_NSTAGES; k++) stage_ms[k] = 0.0;
     int err = 0;
+    c->reorder_ms = 0.0;
     for (int s = 0; s < nsteps && err == 0; s++) {
         const Dev* d = &c->d[c->parity];
+        if (c->reorder_every > 0 && c->since_sort >= c->reorder_every) {
+            CK(cudaEventRecord(c->ev0, c->st));
+            r = sort_state(c, c->parity);
+            if (r) return r;
+            CK(cudaEventRecord(c->ev1, c->st));
+            CK(cudaEventSynchronize(c->ev1));
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+            c->reorder_ms += ms;
+        }
         sphk_enqueue_nnps(d, c->sort_tmp, c->sort_bytes, c->end_bit, c->st, ev);
         enqueue_physics(c, d, ev);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(c->st));
+        c->since_sort++;
         for (int k = 0; k < SPHK_NSTAGES; k++) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
@@ -2341,6 +2605,7 @@ int kl_run(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_kl_field* fi
         if (fields[q].no >= 4 && c->h_fluid.empty()) return SPHGPU_E_STATE;
     }
     cudaSetDevice(c->device);
+    if (const int ro = to_caller_order(c)) return ro;
     const int nd = c->P.ndim, N = c->N;
     double a[3], xt[3], soil_max, water_max;
     if (kl_dom(nd, dom, a, xt, &soil_max, &water_max)) return 13;
@@ -2374,6 +2639,7 @@ int sphgpu_kl_generate_batched(sphgpu_ctx* c, const sphgpu_kl_domain* doms, cons
     if (c->h_type.empty() || (f->no <= 3 && c->h_soil.empty()) || (f->no >= 4 && c->h_fluid.empty()))
         return SPHGPU_E_STATE;
     cudaSetDevice(c->device);
+    if (const int ro = to_caller_order(c)) return ro;
     const int nd = c->P.ndim, N = c->N;
     double* d_out = nullptr;
     CK(cudaMalloc(&d_out, sizeof(double) * N));
@@ -2490,6 +2756,7 @@ int rf_run(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgpu_kl_field* fi
            const sphgpu_rf_flags* fl, const double* const* zetas, const int* depth_axis, int log_exp, double* out)
 {
     cudaSetDevice(c->device);
+    if (const int ro = to_caller_order(c)) return ro;
     const int nd = c->P.ndim, N = c->N;
     RFGeom g;
     int rc = rf_geom(nd, c->P.dr, dom, fl->cell_ndx, g);
@@ -2718,6 +2985,7 @@ int sphgpu_kl_synthesize(sphgpu_ctx* c, const sphgpu_kl_domain* dom, const sphgp
     if (f->type != 1 && f->type != 2) return 14;
     if (c->h_type.empty()) return SPHGPU_E_STATE;
     cudaSetDevice(c->device);
+    if (const int ro = to_caller_order(c)) return ro;
     const int nd = c->P.ndim, N = c->N;
     double a[3], xt[3], soil_max, water_max;
     if (kl_dom(nd, dom, a, xt, &soil_max, &water_max)) return 13;

@@ -181,6 +181,10 @@ struct DevState {
     // tangential); per structure particle the gathered forces (ss_fs, 6N)
     int *ss_id;
     double *ss_con, *ss_own, *ss_fs;
+    // the order the state is held in: the particle at i is the caller's
+    // particle i2o[i] (its index in the reference's particle array), and
+    // o2i is the inverse; identity until the state is re-sorted by cell
+    int *i2o, *o2i;
     // NNPS
     int *cell;                 // cell id per particle
     uint32_t *key_in, *key_out;

@@ -246,15 +246,19 @@ __global__ void k_cellkey(Dev d)
     }
     c += g.base;
     d.s.cell[i] = c;
-    // reversed input order: the stable radix sort then keeps equal keys in
-    // descending particle index, the order Binary_Sort's merge produces
-    d.s.key_in[N - 1 - i] = (uint32_t)c;
-    d.s.val_in[N - 1 - i] = i;
+    // placed by the particle's index in the caller's order, reversed: the
+    // stable radix sort then keeps equal keys in descending caller's index,
+    // the order Binary_Sort's merge produces, in whatever order the state is
+    // held
+    const int o = d.s.i2o[i];
+    d.s.key_in[N - 1 - o] = (uint32_t)c;
+    d.s.val_in[N - 1 - o] = i;
 }
 
 // rainpro (CPP_15-1-rain.cpp:43-85), at the top of the steps with
 // (l - inip) > 0 and (l - inip) % lp == 0: the next row of waiting rain
-// particles -- from index N - nrain on while each next particle's vertical
+// particles -- from index N - nrain on (in the caller's order, mapped to
+// where the state holds them) while each next particle's vertical
 // coordinate stays within 0.1 dr of the one before it -- becomes water:
 // lowered to 0.95 of its height, falling at vrain, with its density, mass and
 // pressure set as the reference sets them.  One block: the row's end is the
@@ -276,7 +280,7 @@ __global__ void __launch_bounds__(256) k_rain(Dev d)
     for (int base = k0; base < N - 1; base += blockDim.x) {
         const int e = base + threadIdx.x;
         if (e < N - 1) {
-            const Pos a = load_pos(d.s.xh, e), b = load_pos(d.s.xh, e + 1);
+            const Pos a = load_pos(d.s.xh, d.s.o2i[e]), b = load_pos(d.s.xh, d.s.o2i[e + 1]);
             const double za = (ND == 2) ? a.y : a.z, zb = (ND == 2) ? b.y : b.z;
             if (!(fabs(zb - za) < 0.1 * dr)) atomicMin(&s_end, e);
         }
@@ -287,7 +291,8 @@ __global__ void __launch_bounds__(256) k_rain(Dev d)
     }
     const int end = s_end;
     const double g = (ND == 2) ? d.p.gy : d.p.gz;
-    for (int k = k0 + threadIdx.x; k <= end; k += blockDim.x) {
+    for (int ko = k0 + threadIdx.x; ko <= end; ko += blockDim.x) {
+        const int k = d.s.o2i[ko];
         Pos p = load_pos(d.s.xh, k);
         if (ND == 2) p.y = 0.95 * p.y;
         else p.z = 0.95 * p.z;
@@ -2093,8 +2098,11 @@ __global__ void __launch_bounds__(128, SPH_MINB_XSPH) k_xsph_update(Dev d)
         if (I.x[2] - bmax[2] >= -0.5 * dr && nd == 3) hit = true;
         if (I.x[2] - bmin[2] <= 0.5 * dr && nd == 3) hit = true;
         if (hit) {
+            // w0 and the comparison in the caller's order
             const int w0 = g.w0;
-            for (int k = 0; k < 3; k++) vn[k] = (i > w0) ? d.s.interfss[k * N + w0] : 0.0;
+            const bool after = d.s.i2o[i] > w0;
+            const int wi = after ? d.s.o2i[w0] : 0;
+            for (int k = 0; k < 3; k++) vn[k] = after ? d.s.interfss[k * N + wi] : 0.0;
         }
     }
     // update (vxp is move_vx for the particles if_move 2 / 3 drives)
@@ -2150,7 +2158,7 @@ __global__ void __launch_bounds__(128) k_tm_vb(Dev d)
     int ids[SPH_NB_CAP];
     double dsts[SPH_NB_CAP];
     // without such a wall the reference reads particle 0 (of the instance)
-    int total = 0, id = (d.p.ninst > 0) ? d.s.inst[d.s.pinst[i]].first : 0;
+    int total = 0, id = d.s.o2i[(d.p.ninst > 0) ? d.s.inst[d.s.pinst[i]].first : 0];
     const Pos P = load_pos(d.s.xh, i);
     for (int q = 0; q < nn; q++) {
         const int j = d.s.nbr[(size_t)q * N + i];
@@ -2495,7 +2503,7 @@ __global__ void __launch_bounds__(128) k_ss_pair(Dev d)
 }
 
 // each structure particle's reactions, added in ascending order of the
-// particles they come from (x - y is x + (-y) in IEEE arithmetic, so the
+// caller's indices of the particles they come from (x - y is x + (-y) in IEEE arithmetic, so the
 // reference's "-=" reactions are stored negated and added)
 __global__ void __launch_bounds__(128) k_ss_struct(Dev d)
 {
@@ -2503,7 +2511,7 @@ __global__ void __launch_bounds__(128) k_ss_struct(Dev d)
     if (i >= N || *d.s.err) return;
     if (d.s.type[i] != 4) return;
     const int nn = nbr_count(d, i);
-    int src[SPH_NB_CAP], slot[SPH_NB_CAP];
+    int src[SPH_NB_CAP], srco[SPH_NB_CAP], slot[SPH_NB_CAP];
     int m = 0;
     for (int q = 0; q < nn; q++) {
         const int j = d.s.nbr[(size_t)q * N + i];
@@ -2511,10 +2519,14 @@ __global__ void __launch_bounds__(128) k_ss_struct(Dev d)
         if (!(tj == 1 || tj == 2)) continue;
         for (int s = 0; s < 3; s++)
             if (d.s.ss_id[(size_t)s * N + j] == i) {
-                // insertion by source index
+                // insertion by source index in the caller's order
+                const int jo = d.s.i2o[j];
                 int p = m++;
-                while (p > 0 && src[p - 1] > j) { src[p] = src[p - 1]; slot[p] = slot[p - 1]; p--; }
+                while (p > 0 && srco[p - 1] > jo) {
+                    src[p] = src[p - 1]; srco[p] = srco[p - 1]; slot[p] = slot[p - 1]; p--;
+                }
                 src[p] = j;
+                srco[p] = jo;
                 slot[p] = s;
             }
     }
@@ -2993,6 +3005,71 @@ extern "C" size_t sphk_sort_temp_bytes(int N, int end_bit)
     cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr,
                                     (const int*)nullptr, (int*)nullptr, N, 0, end_bit);
     return bytes;
+}
+
+// The order sphgpu_set_reorder re-sorts the particle state into: by type
+// and material (so that a warp's particles take the same branches of the
+// constitutive and momentum passes: co-located phases, such as the water
+// and soil particles of a saturated soil, would otherwise alternate), then
+// by place on a lattice of spacing dr over the particle's grid (each batched
+// instance's own grid, the instances one after another), in rows along the
+// grid's longest axis, planes across its shortest.  On a regular arrangement
+// the neighbours at one lattice offset from consecutive particles then sit at
+// consecutive positions, so the gathers of one list slot by a warp read one
+// contiguous run of records, and long rows keep the warps that straddle two
+// rows few.  Lattice places are clamped to the grid, so the place key of a
+// particle in instance q stays below 8 times the context cell id of instance
+// q + 1, and below span = 8 (ctotal + 1) for all.
+__global__ void k_order_key(Dev d, unsigned long long span, unsigned long long* key, int* val)
+{
+    const int i = IDX, N = d.p.N;
+    if (i >= N) return;
+    const Pos p = load_pos(d.s.xh, i);
+    const CellGrid g = cell_grid(d, i);
+    const double dr = d.p.dr;
+    auto lat = [dr](double x, double lo, int cells) -> unsigned long long {
+        const double t = fabs(x - lo) / dr;
+        const int n = 2 * cells;
+        return (t < (double)n) ? (unsigned long long)t : (unsigned long long)(n - 1);
+    };
+    const int nd = d.p.ndim;
+    const unsigned long long q[3] = {lat(p.x, g.xmin, g.cxm), lat(p.y, g.ymin, g.cym),
+                                     nd == 3 ? lat(p.z, g.zmin, g.czm) : 0ull};
+    const unsigned long long n[3] = {2ull * g.cxm, 2ull * g.cym, nd == 3 ? 2ull * g.czm : 1ull};
+    // axes by extent, longest last (the fastest); ties keep x fastest
+    int a[3] = {2, 1, 0};
+    for (int u = 0; u < 3; u++)
+        for (int v = u + 1; v < 3; v++)
+            if (n[a[u]] > n[a[v]]) { const int w = a[u]; a[u] = a[v]; a[v] = w; }
+    const unsigned long long k = (q[a[0]] * n[a[1]] + q[a[1]]) * n[a[2]] + q[a[2]];
+    const int t = d.s.type[i], m = d.s.matype[i];
+    const unsigned long long group = (unsigned long long)((t >= 0 && t < 8) ? t : 7) * 64ull +
+                                     (unsigned long long)((m >= 0 && m < 64) ? m : 63);
+    key[i] = group * span + 8ull * (unsigned long long)g.base + k;
+    val[i] = i;
+}
+
+extern "C" size_t sphk_order_temp_bytes(int N, int end_bit)
+{
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned long long*)nullptr,
+                                    (unsigned long long*)nullptr, (const int*)nullptr, (int*)nullptr, N, 0,
+                                    end_bit);
+    return bytes;
+}
+
+// the re-sort's permutation into vout (vout[i] = the held index that moves
+// to i), from the positions of the buffers of *dp; returns the kernels it
+// launched
+extern "C" int sphk_order_sort(const Dev* dp, void* tmp, size_t bytes, int end_bit, unsigned long long* kin,
+                               unsigned long long* kout, int* vin, int* vout, cudaStream_t st)
+{
+    const Dev& d = *dp;
+    const int N = d.p.N;
+    const unsigned long long span = 8ull * ((unsigned long long)d.p.ctotal + 1);
+    k_order_key<<<nblk(N, 256), 256, 0, st>>>(d, span, kin, vin);
+    cub::DeviceRadixSort::SortPairs(tmp, bytes, kin, kout, vin, vout, N, 0, end_bit, st);
+    return 1;
 }
 
 // Stage names, in launch order; with `ev` non-null, event ev[k] is recorded

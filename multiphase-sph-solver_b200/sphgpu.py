@@ -298,6 +298,11 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_kl_generate_batched.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_void_p,
                                                C.c_int, C.c_void_p]
     lib.sphgpu_update_params.argtypes = [C.c_void_p, C.POINTER(Params)]
+    lib.sphgpu_set_reorder.argtypes = [C.c_void_p, C.c_int]
+    lib.sphgpu_get_reorder.argtypes = [C.c_void_p]
+    lib.sphgpu_get_order.argtypes = [C.c_void_p, C.c_void_p]
+    lib.sphgpu_last_reorder_ms.restype = C.c_double
+    lib.sphgpu_last_reorder_ms.argtypes = [C.c_void_p]
     lib.sphgpu_parttocell.argtypes = [C.c_void_p]
     lib.sphgpu_partisearching.argtypes = [C.c_void_p]
     lib.sphgpu_update.argtypes = [C.c_void_p]
@@ -567,6 +572,22 @@ class Engine:
         reference's constant dt)."""
         self._check(self.lib.sphgpu_set_cfl(self.h, float(cfl), float(cfl_force)), "sphgpu_set_cfl")
 
+    def set_reorder(self, every_steps: int) -> None:
+        """Hold the particle state in cell order, re-sorted every every_steps
+        steps (0: the caller's order, the default); results are unchanged."""
+        self._check(self.lib.sphgpu_set_reorder(self.h, int(every_steps)), "sphgpu_set_reorder")
+
+    @property
+    def reorder(self) -> int:
+        return int(self.lib.sphgpu_get_reorder(self.h))
+
+    def order(self) -> np.ndarray:
+        """i2o: the caller's index of the particle the device holds at each
+        position."""
+        out = np.empty(self.n, dtype=np.int32)
+        self._check(self.lib.sphgpu_get_order(self.h, _ptr(out)), "sphgpu_get_order")
+        return out
+
     def dt(self) -> float:
         """The dt the next step uses."""
         v = C.c_double()
@@ -605,7 +626,9 @@ class Engine:
         k = self.lib.sphgpu_stage_count()
         ms = np.zeros(k)
         self._check(self.lib.sphgpu_step_profiled(self.h, int(nsteps), _ptr(ms)), "sphgpu_step_profiled")
-        return {self.lib.sphgpu_stage_name(i).decode(): float(ms[i]) for i in range(k)}
+        out = {self.lib.sphgpu_stage_name(i).decode(): float(ms[i]) for i in range(k)}
+        out["reorder"] = float(self.lib.sphgpu_last_reorder_ms(self.h))
+        return out
 
 
 def batch(states) -> tuple:
