@@ -102,6 +102,28 @@ def pass_roofline(stage_ms: dict, n: int, peak_gbs: float, ndim: int = 3) -> dic
     return out
 
 
+# Algorithmic FP64 flops per particle per step of the 3-D soil column with
+# co-located water: about 14,000 (the pair arithmetic of the neighbour passes
+# for 65 neighbours, the constitutive update and the eigenvalues), the figure
+# the HBM bound is weighed against (about 7.6 flop per algorithmic byte).
+STEP_FLOPS_3D = 14000.0
+
+
+def fp64_roofline(device: int, n: int, step_ms: float) -> dict:
+    """The whole step against the device's measured FP64 multiply-add rate
+    (sphgpu_pipe_peaks), beside the HBM roofline: the drop-in form's pair and
+    constitutive arithmetic runs on the FP64 pipe."""
+    import sphgpu
+    try:
+        f64, f32 = sphgpu.pipe_peaks(device)
+    except sphgpu.SPHError as e:
+        return {"unavailable": str(e)}
+    achieved = STEP_FLOPS_3D * n / (step_ms / 1e3) / 1e12
+    return {"bound": "fp64", "algorithmic_flops_per_particle": STEP_FLOPS_3D, "achieved": achieved,
+            "peak": f64, "unit": "TFLOP/s", "frac": achieved / f64, "peak_kind": "measured (sphgpu_pipe_peaks)",
+            "fp32_peak": f32}
+
+
 def measured_peaks() -> tuple[dict, str]:
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -687,7 +709,7 @@ def engine_arm(args, world, rank, local):
     eng2.close()
 
     shuffled = None
-    if not args.no_configs:
+    if not args.no_shuffled:
         # the same workload with the particles in a random order (a caller's
         # Particle array need not be spatial): the neighbour gathers then hit
         # scattered records
@@ -769,6 +791,7 @@ def engine_arm(args, world, rank, local):
                          "traffic_over_algorithmic": (traffic * scene.n / alg) if traffic else None,
                          "step": {"algorithmic_bytes": STEP_BYTES_3D * scene.n, "ms": step_ms,
                                   "achieved": step_gbs, "frac": step_gbs / hbm}},
+            "roofline_fp64": fp64_roofline(device, scene.n, step_ms),
             "passes": passes,
             "stage_ms_per_step": stage_ms,
             "forms": {
@@ -808,6 +831,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-configs", action="store_true")
+    ap.add_argument("--no-shuffled", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         # host-only arm: rank 0 runs it, the other ranks exit without work

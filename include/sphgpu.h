@@ -601,6 +601,14 @@ int sphgpu_kl_generate_batched(sphgpu_ctx* ctx, const sphgpu_kl_domain* doms, co
  * SPHGPU_E_KL_TIMEOUT when that happened (the expected result).
  */
 int sphgpu_kl_wait_check(sphgpu_ctx* ctx, long long budget_cycles);
+
+/*
+ * The device's FP64 and FP32 multiply-add rates in TFLOP/s (two flops per
+ * fused multiply-add), measured by a kernel of independent multiply-add
+ * chains on every SM (no counterpart in the reference): the denominators of
+ * the compute side of the step's roofline.  Takes a few milliseconds.
+ */
+int sphgpu_pipe_peaks(int device, double* fp64_tflops, double* fp32_tflops);
 int sphgpu_kl_synthesize(sphgpu_ctx* ctx, const sphgpu_kl_domain* dom, const sphgpu_kl_field* field,
                          const double* xi, int R, int K, float* d_out, double* kernel_ms);
 

@@ -22,7 +22,7 @@ LIB = os.path.join(HERE, "libsphgpu.so")
 # check after the neighbour search that sets an error code instead of trapping
 LIB_CHECK = os.path.join(HERE, "libsphgpu_check.so")
 SOURCES = ["sph_kernels.cu", "sph_capi.cu", "sph_noalloc.cu", "sph_kernels_bulk32.cu", "sph_kl.cu", "sph_kl_tc.cu",
-           "sph_rf.cu"]
+           "sph_rf.cu", "sph_peaks.cu"]
 # per-source flags on top of NVCC_FLAGS
 SOURCE_FLAGS = {"sph_kernels_bulk32.cu": ["-fmad=true"]}
 HEADERS = ["sph_device.cuh", "sph_constitutive.cuh", os.path.join("..", "..", "include", "sphgpu.h")]

@@ -298,6 +298,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_kl_generate_batched.argtypes = [C.c_void_p, C.POINTER(KLDomain), C.POINTER(KLField), C.c_void_p,
                                                C.c_int, C.c_void_p]
     lib.sphgpu_update_params.argtypes = [C.c_void_p, C.POINTER(Params)]
+    lib.sphgpu_pipe_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.sphgpu_set_reorder.argtypes = [C.c_void_p, C.c_int]
     lib.sphgpu_get_reorder.argtypes = [C.c_void_p]
     lib.sphgpu_get_order.argtypes = [C.c_void_p, C.c_void_p]
@@ -326,6 +327,17 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
 
 def _ptr(a: np.ndarray) -> C.c_void_p:
     return C.c_void_p(a.ctypes.data)
+
+
+def pipe_peaks(device: int = 0) -> tuple:
+    """sphgpu_pipe_peaks: the device's measured FP64 and FP32 multiply-add
+    rates, TFLOP/s."""
+    lib = load_library()
+    f64, f32 = C.c_double(), C.c_double()
+    rc = lib.sphgpu_pipe_peaks(int(device), C.byref(f64), C.byref(f32))
+    if rc:
+        raise SPHError(rc, "sphgpu_pipe_peaks")
+    return f64.value, f32.value
 
 
 class Engine:
