@@ -837,6 +837,10 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     c->N = P->ntotal;
     auto fail = [&](int code) { g_create_error = code; sphgpu_destroy(c); return (sphgpu_ctx*)nullptr; };
     if (cudaSetDevice(device) != cudaSuccess) return fail(SPHGPU_E_NODEVICE);
+    // an error an earlier, unrelated call left as the last error (not a
+    // sticky one, which every call below would report) is not this
+    // context's: cleared, so that the launch checks below see their own
+    cudaGetLastError();
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) return fail(SPHGPU_E_CUDA);
     cudaEventCreate(&c->ev0);
     cudaEventCreate(&c->ev1);
@@ -896,7 +900,7 @@ sphgpu_ctx* sphgpu_create(const sphgpu_params* P, int device)
     if (cudaMemcpyAsync(s.step, &one, sizeof(int), cudaMemcpyHostToDevice, c->st) != cudaSuccess)
         return fail(SPHGPU_E_CUDA);
     k_order_identity<<<(N + 255) / 256, 256, 0, c->st>>>(s.i2o, s.o2i, N);
-    if (cudaGetLastError() != cudaSuccess) return fail(SPHGPU_E_CUDA);
+    if (cudaPeekAtLastError() != cudaSuccess) return fail(SPHGPU_E_CUDA);
     c->end_bit = end_bit_for(P->ctotal);
     c->sort_bytes = sphk_sort_temp_bytes(N, c->end_bit);
     if (cudaMalloc(&c->sort_tmp, c->sort_bytes + 256) != cudaSuccess) return fail(SPHGPU_E_CUDA);

@@ -68,7 +68,11 @@ int rate(int sms, cudaStream_t st, T* sink, double* tflops)
 extern "C" int sphgpu_pipe_peaks(int device, double* fp64_tflops, double* fp32_tflops)
 {
     if (!fp64_tflops || !fp32_tflops) return SPHGPU_E_ARG;
-    if (cudaSetDevice(device) != cudaSuccess) return SPHGPU_E_NODEVICE;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();      // this call's own error: not left for the caller's next check
+        return SPHGPU_E_NODEVICE;
+    }
+    cudaGetLastError();          // an earlier call's last error is not this measurement's
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms <= 0)
         return SPHGPU_E_CUDA;
