@@ -414,26 +414,86 @@ std::vector<PermArr> perm_arrays(const sphgpu_ctx* c, int parity)
     return v;
 }
 
-// dst = src gathered by perm: the new i-th particle is the old perm[i]-th
-template <typename T>
-__global__ void k_perm_gather(const T* __restrict__ src, T* __restrict__ dst, const int* __restrict__ perm, int N,
-                              int cols, int aos)
+// One array of the state on the device for the fused gather: the array, its
+// gather buffer (a part of the context's scratch), element size, columns and
+// layout as PermArr.
+struct PermDev { void* arr; void* tmp; int esz, cols, aos, pad; };
+
+// tmp = arr gathered by perm, for every array of the table in one launch: one
+// thread per particle position q takes element(s) perm[q] of each array in
+// turn, four loads in flight before their stores.  The reads are gathers of a
+// nearly sorted permutation, the writes coalesced.  An AoS array (the
+// position records) has an even number of doubles per record, moved as pairs.
+__global__ void __launch_bounds__(256) k_perm_gather_all(const PermDev* __restrict__ tab, int na,
+                                                         const int* __restrict__ perm, int N)
 {
-    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (t >= (size_t)N * cols) return;
-    if (aos) {
-        const size_t q = t / cols, k = t - q * cols;
-        dst[t] = src[(size_t)perm[q] * cols + k];
-    } else {
-        const size_t k = t / N, q = t - k * N;
-        dst[t] = src[k * N + perm[q]];
+    const int qi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (qi >= N) return;
+    const size_t q = (size_t)qi, p = (size_t)perm[qi], n = (size_t)N;
+    for (int a = 0; a < na; a++) {
+        const PermDev e = tab[a];
+        if (e.esz == 4) {
+            const int* s = static_cast<const int*>(e.arr);
+            int* d = static_cast<int*>(e.tmp);
+            for (int k = 0; k < e.cols; k++) d[k * n + q] = s[k * n + p];
+        } else if (e.aos) {
+            const double2* s = static_cast<const double2*>(e.arr);
+            double2* d = static_cast<double2*>(e.tmp);
+            const int h = e.cols / 2;
+            for (int k = 0; k < h; k++) d[q * h + k] = s[p * h + k];
+        } else {
+            const double* s = static_cast<const double*>(e.arr);
+            double* d = static_cast<double*>(e.tmp);
+            for (int k0 = 0; k0 < e.cols; k0 += 4) {
+                double v[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                    if (k0 + u < e.cols) v[u] = s[(size_t)(k0 + u) * n + p];
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                    if (k0 + u < e.cols) d[(size_t)(k0 + u) * n + q] = v[u];
+            }
+        }
     }
 }
 
-template <typename T>
-__global__ void k_perm_copy(const T* __restrict__ src, T* __restrict__ dst, size_t n)
+// arr = tmp for every array of the table (the gathered state back into the
+// arrays the step graphs were captured with), one thread per position
+__global__ void __launch_bounds__(256) k_perm_copy_all(const PermDev* __restrict__ tab, int na, int N)
 {
-    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const int qi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (qi >= N) return;
+    const size_t q = (size_t)qi, n = (size_t)N;
+    for (int a = 0; a < na; a++) {
+        const PermDev e = tab[a];
+        if (e.esz == 4) {
+            const int* s = static_cast<const int*>(e.tmp);
+            int* d = static_cast<int*>(e.arr);
+            for (int k = 0; k < e.cols; k++) d[k * n + q] = s[k * n + q];
+        } else if (e.aos) {
+            const double2* s = static_cast<const double2*>(e.tmp);
+            double2* d = static_cast<double2*>(e.arr);
+            const int h = e.cols / 2;
+            for (int k = 0; k < h; k++) d[q * h + k] = s[q * h + k];
+        } else {
+            const double* s = static_cast<const double*>(e.tmp);
+            double* d = static_cast<double*>(e.arr);
+            for (int k0 = 0; k0 < e.cols; k0 += 4) {
+                double v[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                    if (k0 + u < e.cols) v[u] = s[(size_t)(k0 + u) * n + q];
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                    if (k0 + u < e.cols) d[(size_t)(k0 + u) * n + q] = v[u];
+            }
+        }
+    }
+}
+
+__global__ void k_copy_int(const int* __restrict__ src, int* __restrict__ dst, int n)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) dst[t] = src[t];
 }
 
@@ -468,31 +528,38 @@ int ensure_perm_tmp(sphgpu_ctx* c, size_t bytes)
 }
 
 // every array of the state (the buffers of `parity`) gathered by perm, on
-// the context's stream, and the maps moved with them
+// the context's stream, and the maps moved with them.  The scratch holds the
+// device table of the arrays, each array's gather buffer and the new i2o.
 int enqueue_permute(sphgpu_ctx* c, int parity, const int* perm)
 {
     const std::vector<PermArr> arr = perm_arrays(c, parity);
     const int N = c->N;
-    size_t most = 4 * (size_t)N;
-    for (const PermArr& a : arr) most = std::max(most, (size_t)a.esz * a.cols * N);
-    int r = ensure_perm_tmp(c, most);
-    if (r) return r;
-    for (const PermArr& a : arr) {
-        const size_t n = (size_t)a.cols * N;
-        if (a.esz == 8) {
-            k_perm_gather<double><<<perm_blocks(n), 256, 0, c->st>>>((const double*)a.p, (double*)c->perm_tmp,
-                                                                     perm, N, a.cols, a.aos);
-            k_perm_copy<double><<<perm_blocks(n), 256, 0, c->st>>>((const double*)c->perm_tmp, (double*)a.p, n);
-        } else {
-            k_perm_gather<int><<<perm_blocks(n), 256, 0, c->st>>>((const int*)a.p, (int*)c->perm_tmp, perm, N,
-                                                                  a.cols, a.aos);
-            k_perm_copy<int><<<perm_blocks(n), 256, 0, c->st>>>((const int*)c->perm_tmp, (int*)a.p, n);
-        }
+    auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t table_bytes = up(sizeof(PermDev) * arr.size());
+    std::vector<PermDev> tab(arr.size());
+    size_t off = table_bytes;
+    for (size_t a = 0; a < arr.size(); a++) {
+        if (arr[a].aos && arr[a].cols % 2 != 0) return SPHGPU_E_ARG;
+        tab[a] = PermDev{arr[a].p, nullptr, arr[a].esz, arr[a].cols, arr[a].aos, 0};
+        off += up((size_t)arr[a].esz * arr[a].cols * N);
     }
+    const size_t i2o_off = off;
+    int r = ensure_perm_tmp(c, i2o_off + up(4 * (size_t)N));
+    if (r) return r;
+    char* base = static_cast<char*>(c->perm_tmp);
+    off = table_bytes;
+    for (size_t a = 0; a < arr.size(); a++) {
+        tab[a].tmp = base + off;
+        off += up((size_t)arr[a].esz * arr[a].cols * N);
+    }
+    const PermDev* dtab = reinterpret_cast<const PermDev*>(base);
+    CK(cudaMemcpyAsync(base, tab.data(), sizeof(PermDev) * tab.size(), cudaMemcpyHostToDevice, c->st));
+    k_perm_gather_all<<<perm_blocks(N), 256, 0, c->st>>>(dtab, (int)tab.size(), perm, N);
+    k_perm_copy_all<<<perm_blocks(N), 256, 0, c->st>>>(dtab, (int)tab.size(), N);
     const DevState& s = c->d[parity].s;
-    int* tmp = (int*)c->perm_tmp;
+    int* tmp = reinterpret_cast<int*>(base + i2o_off);
     k_order_compose<<<perm_blocks(N), 256, 0, c->st>>>(perm, s.i2o, tmp, N);
-    k_perm_copy<int><<<perm_blocks(N), 256, 0, c->st>>>(tmp, s.i2o, (size_t)N);
+    k_copy_int<<<perm_blocks(N), 256, 0, c->st>>>(tmp, s.i2o, N);
     k_order_inverse<<<perm_blocks(N), 256, 0, c->st>>>(s.i2o, s.o2i, N);
     CK(cudaGetLastError());
     return 0;
