@@ -648,7 +648,10 @@ def engine_arm(args, world, rank, local):
         table = eng.autotune(steps=2)
         tune = {"passes": list(sphgpu.Engine.TUNE_PASSES), "threads_per_block": [int(v) for v in eng.launch()],
                 "ms_per_step_by_candidate": {str(b): [round(float(x), 4) for x in table[a]]
-                                             for a, b in enumerate((32, 64, 96, 128))}}
+                                             for a, b in enumerate((32, 64, 96, 128))},
+                # whether to hold the state re-sorted (the caller's order here is
+                # a spatial lattice already)
+                "reorder": eng.autotune_reorder(steps=2, every=RESORT_EVERY)}
     eng.step(args.warmup)
     barrier(world)
     eng.synchronize()
@@ -724,7 +727,9 @@ def engine_arm(args, world, rank, local):
         sh_ms = eng3.last_step_ms() / args.steps
         sh_prof = eng3.step_profiled(args.steps)
         # the engine re-sorting its state (sphgpu_set_reorder) every 20
-        # steps: the re-sorts that fall in the timed steps are timed with them
+        # steps: the re-sorts that fall in the timed steps are timed with them;
+        # beside it, what the reorder autotuner chooses for this order
+        sh_tune = eng3.autotune_reorder(steps=2, every=RESORT_EVERY)
         eng3.set_reorder(RESORT_EVERY)
         eng3.step(args.warmup)
         eng3.synchronize()
@@ -736,6 +741,7 @@ def engine_arm(args, world, rank, local):
         shuffled = {"ms_per_step": sh_ms, "value": n_active / (sh_ms / 1e3), "unit": "particle-updates/s",
                     "slowdown_vs_spatial_order": sh_ms / spatial_ms,
                     "stage_ms_per_step": {k: v / args.steps for k, v in sh_prof.items() if v > 0.01},
+                    "autotune_reorder": sh_tune,
                     "resorted": {"every_steps": RESORT_EVERY, "ms_per_step": rs_ms,
                                  "value": n_active / (rs_ms / 1e3), "slowdown_vs_spatial_order": rs_ms / spatial_ms,
                                  "resort_ms_per_step": rs_prof.get("reorder", 0.0) / args.steps,

@@ -320,6 +320,17 @@ int sphgpu_set_reorder(sphgpu_ctx* ctx, int every_steps);
 int sphgpu_get_reorder(const sphgpu_ctx* ctx);
 int sphgpu_get_order(sphgpu_ctx* ctx, int* i2o);
 double sphgpu_last_reorder_ms(const sphgpu_ctx* ctx);
+/*
+ * Chooses between the two by timing (the steps are real steps of the run):
+ * `steps` steps in the caller's order, then a re-sort and `steps` more, and
+ * keeps re-sorting every `every` steps only when the re-sorted steps, with one
+ * re-sort's time charged per `every` steps, are more than 3% faster.  *chosen
+ * is the interval set (every or 0); ms[0..2], if non-NULL, the caller's-order
+ * step, the re-sorted step and the re-sort's share per step (device ms, the
+ * per-stage sums of sphgpu_step_profiled).  With 0 chosen the state is back in
+ * the caller's order.
+ */
+int sphgpu_autotune_reorder(sphgpu_ctx* ctx, int steps, int every, int* chosen, double* ms);
 
 /*
  * Rainfall (flr == 1): the reference's Para_Rain (Class_Problem.h) as its

@@ -2469,6 +2469,41 @@ int sphgpu_autotune(sphgpu_ctx* c, int steps, const char* cache_path, double* ta
     return 0;
 }
 
+int sphgpu_autotune_reorder(sphgpu_ctx* c, int steps, int every, int* chosen, double* ms)
+{
+    if (!c || steps <= 0 || every <= 0 || !chosen) return SPHGPU_E_ARG;
+    if (c->part_done) return SPHGPU_E_STATE;
+    std::vector<double> stage_ms(SPHK_NSTAGES);
+    auto sum = [&]() {
+        double t = 0.0;
+        for (double v : stage_ms) t += v;
+        return t / steps;
+    };
+    // the caller's order, no re-sorts
+    int rc = to_caller_order(c);
+    if (rc) return rc;
+    c->reorder_every = 0;
+    rc = sphgpu_step_profiled(c, steps, stage_ms.data());
+    if (rc) return rc;
+    const double plain = sum();
+    // re-sorted before the first of the same number of steps; the re-sort's
+    // own time is charged at one per `every` steps
+    sphgpu_set_reorder(c, every);
+    rc = sphgpu_step_profiled(c, steps, stage_ms.data());
+    if (rc) return rc;
+    const double sorted = sum(), cost = c->reorder_ms / every;
+    // the re-sorted order is kept only when it is faster by more than the
+    // step-to-step spread of the timings (3%)
+    *chosen = (sorted + cost < 0.97 * plain) ? every : 0;
+    if (ms) { ms[0] = plain; ms[1] = sorted; ms[2] = cost; }
+    if (*chosen == 0) {
+        rc = to_caller_order(c);
+        if (rc) return rc;
+    }
+    c->reorder_every = *chosen;
+    return 0;
+}
+
 double sphgpu_last_step_ms(const sphgpu_ctx* c) { return c ? c->last_ms : 0.0; }
 long sphgpu_last_step_launches(const sphgpu_ctx* c) { return c ? c->last_launches : 0; }
 void* sphgpu_stream(sphgpu_ctx* c) { return c ? (void*)c->st : nullptr; }

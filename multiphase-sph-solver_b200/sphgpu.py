@@ -302,6 +302,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.sphgpu_set_reorder.argtypes = [C.c_void_p, C.c_int]
     lib.sphgpu_get_reorder.argtypes = [C.c_void_p]
     lib.sphgpu_get_order.argtypes = [C.c_void_p, C.c_void_p]
+    lib.sphgpu_autotune_reorder.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_void_p]
     lib.sphgpu_last_reorder_ms.restype = C.c_double
     lib.sphgpu_last_reorder_ms.argtypes = [C.c_void_p]
     lib.sphgpu_parttocell.argtypes = [C.c_void_p]
@@ -592,6 +593,16 @@ class Engine:
     @property
     def reorder(self) -> int:
         return int(self.lib.sphgpu_get_reorder(self.h))
+
+    def autotune_reorder(self, steps: int = 2, every: int = 20) -> dict:
+        """sphgpu_autotune_reorder: time the caller's order against the
+        re-sorted one and keep the faster; returns the choice and the times."""
+        chosen = C.c_int()
+        ms = np.zeros(3)
+        self._check(self.lib.sphgpu_autotune_reorder(self.h, int(steps), int(every), C.byref(chosen), _ptr(ms)),
+                    "sphgpu_autotune_reorder")
+        return {"every_steps": int(chosen.value), "caller_order_ms": float(ms[0]), "resorted_ms": float(ms[1]),
+                "resort_ms_per_step": float(ms[2])}
 
     def order(self) -> np.ndarray:
         """i2o: the caller's index of the particle the device holds at each

@@ -244,3 +244,26 @@ def test_step_profiled_resorts_and_reports():
     _assert_equal_runs(plain, sorted_, "profiled")
     plain.close()
     sorted_.close()
+
+
+@pytest.mark.parametrize("shuffle", [False, True])
+def test_reorder_autotuner_keeps_results(shuffle):
+    """sphgpu_autotune_reorder times both orders over real steps and keeps
+    one; whichever it keeps, the run stays the plain run bit for bit, and with
+    0 chosen the state is back in the caller's order."""
+    st = scenes.initialise(scenes.soil_column_3d(dx=0.05, steps=200))
+    if shuffle:
+        st = _shuffled(st, 11)
+    plain, tuned = _engine(st, 0), _engine(st, 0)
+    got = tuned.autotune_reorder(steps=2, every=5)
+    assert got["every_steps"] in (0, 5)
+    assert got["caller_order_ms"] > 0 and got["resorted_ms"] > 0 and got["resort_ms_per_step"] > 0
+    assert tuned.reorder == got["every_steps"]
+    if got["every_steps"] == 0:
+        assert not _held_out_of_order(tuned)
+    plain.step(4)               # the autotuner's own 2 + 2 steps
+    tuned.step(7)
+    plain.step(7)
+    _assert_equal_runs(plain, tuned, "autotuned")
+    plain.close()
+    tuned.close()
