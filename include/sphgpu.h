@@ -323,8 +323,9 @@ double sphgpu_last_reorder_ms(const sphgpu_ctx* ctx);
 /*
  * Chooses between the two by timing (the steps are real steps of the run):
  * `steps` steps in the caller's order, then a re-sort and `steps` more, and
- * keeps re-sorting every `every` steps only when the re-sorted steps, with one
- * re-sort's time charged per `every` steps, are more than 3% faster.  *chosen
+ * keeps re-sorting every `every` steps only when the re-sorted steps, with the
+ * time of a further re-sort (of the re-sorted state, as every re-sort after
+ * the first is) charged per `every` steps, are more than 3% faster.  *chosen
  * is the interval set (every or 0); ms[0..2], if non-NULL, the caller's-order
  * step, the re-sorted step and the re-sort's share per step (device ms, the
  * per-stage sums of sphgpu_step_profiled).  With 0 chosen the state is back in

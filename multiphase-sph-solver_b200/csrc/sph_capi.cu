@@ -2486,12 +2486,23 @@ int sphgpu_autotune_reorder(sphgpu_ctx* c, int steps, int every, int* chosen, do
     rc = sphgpu_step_profiled(c, steps, stage_ms.data());
     if (rc) return rc;
     const double plain = sum();
-    // re-sorted before the first of the same number of steps; the re-sort's
-    // own time is charged at one per `every` steps
+    // re-sorted before the first of the same number of steps
     sphgpu_set_reorder(c, every);
     rc = sphgpu_step_profiled(c, steps, stage_ms.data());
     if (rc) return rc;
-    const double sorted = sum(), cost = c->reorder_ms / every;
+    const double sorted = sum();
+    // the re-sort's own time, charged at one per `every` steps: a re-sort of
+    // the re-sorted state, as every re-sort after the first is (the first,
+    // from the caller's order, moves every record and is paid once)
+    cudaSetDevice(c->device);
+    CK(cudaEventRecord(c->ev0, c->st));
+    rc = sort_state(c, c->parity);
+    if (rc) return rc;
+    CK(cudaEventRecord(c->ev1, c->st));
+    CK(cudaEventSynchronize(c->ev1));
+    float resort_ms = 0.f;
+    cudaEventElapsedTime(&resort_ms, c->ev0, c->ev1);
+    const double cost = resort_ms / every;
     // the re-sorted order is kept only when it is faster by more than the
     // step-to-step spread of the timings (3%)
     *chosen = (sorted + cost < 0.97 * plain) ? every : 0;
