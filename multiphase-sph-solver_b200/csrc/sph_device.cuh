@@ -480,6 +480,18 @@ __device__ __forceinline__ void load_w_raw(const double* nbw, int N, int s, int 
 }
 __device__ __forceinline__ void load_w(const Dev& d, int s, int i, double w[4]) { load_w_raw(d.s.nbw, d.p.N, s, i, w); }
 __device__ __forceinline__ void load_w(const Dev& d, int s, int i, float w[4]) { load_w_raw(d.s.nbw, d.p.N, s, i, w); }
+// Slot s's pair record for a pass that needs only the kernel value w[3]:
+// with no kernel gradient correction (flknl 1, 2) recomputed from the
+// neighbour's position exactly as k_pairw computed it (the same operations on
+// the same values, so the same bits; the gradient's arithmetic, unused, is
+// dropped by the compiler), else the corrected record k_kgc left in nbw.
+template <int ND, typename R>
+__device__ __forceinline__ void pair_value(const Dev& d, const PairI<R>& I, R rra, int j, int s, int i, R w[4])
+{
+    if (d.p.flknl <= 2) pair_w_raw<ND, R>(d, I, rra, load_pos(d.s.xh, j), w);
+    else load_w(d, s, i, w);
+}
+
 __device__ __forceinline__ void store_w(const Dev& d, int s, int i, const double w[4])
 {
     double2* p = reinterpret_cast<double2*>(d.s.nbw) + 2 * ((size_t)s * d.p.N + i);

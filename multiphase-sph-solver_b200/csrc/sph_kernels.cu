@@ -678,7 +678,10 @@ __global__ void __launch_bounds__(128, SPH_MINB_PAIRW) k_pairw(Dev d)
 #endif  // !SPH_BULK32
 
 // ---------------------------------------------------------------------------
-// density(): fluid porosity (:25-54) and continuity (:57-165) -> rho_c
+// density(): fluid porosity (:25-54) and continuity (:57-165) -> rho_c.  The
+// porosity loop needs only the kernel values and recomputes them from the
+// neighbours' positions (pair_value); the continuity loop reads the gradients
+// from the pair records.
 template <int ND>
 __global__ void __launch_bounds__(128, SPH_MINB_DENS) k_density(Dev d)
 {
@@ -693,11 +696,13 @@ __global__ void __launch_bounds__(128, SPH_MINB_DENS) k_density(Dev d)
     double pcop = d.s.poro_cop[i];
     if (ti == 1) {
         Sum<real> sup, sdown;
+        const PairI<real> I = pair_i<ND, real>(d, i);
+        const real rra = real(1.0) / I.h;
         MaskIter it(d, i, type_mask(d, i, 2));
         int s, j;
         while (it.next(s, j)) {
             real w[4];
-            load_w(d, s, i, w);
+            pair_value<ND, real>(d, I, rra, j, s, i, w);
             const NV pj = load_nv(d.s.rrho, j);     // (mass, porosity, rho, 1 / rho)
             const real mj = (real)pj.vx, rj = (real)pj.vz;
             const double rrj = pj.m;
@@ -775,6 +780,9 @@ __global__ void __launch_bounds__(128, SPH_MINB_DENS) k_density(Dev d)
 
 // Shepard filter (:168-188) reading every neighbour's continuity density
 // (Jacobi order), then the local equation of state (CPP_7-1-eos_CR.cpp:22-43).
+// The pass needs only the kernel values, which it recomputes from the
+// neighbours' positions (pair_value) instead of streaming the 32-byte pair
+// records for them.
 template <int ND>
 __global__ void __launch_bounds__(128, SPH_MINB) k_shepard_eos(Dev d)
 {
@@ -782,11 +790,13 @@ __global__ void __launch_bounds__(128, SPH_MINB) k_shepard_eos(Dev d)
     if (i >= N || *d.s.err) return;
     const int ti = d.s.type[i], nn = nbr_count(d, i);
     Sum<real> sup, sdown;
+    const PairI<real> I = pair_i<ND, real>(d, i);
+    const real rra = real(1.0) / I.h;
     MaskIter it(d, i, type_mask(d, i, ti));
     int s, j;
     while (it.next(s, j)) {
         real w[4];
-        load_w(d, s, i, w);
+        pair_value<ND, real>(d, I, rra, j, s, i, w);
         const double2 cm = reinterpret_cast<const double2*>(d.s.rho_c)[j];
         const real mj = (real)cm.y;
         sup.add(mj * w[3]);
