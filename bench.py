@@ -336,7 +336,10 @@ def bulk_form(st, args, device, ref_fields, moving):
     eng.load_state(st.fields, st.fluid, st.soil)
     eng.set_precision(sphgpu.PREC_FP32_BULK)
     if not args.no_autotune:
+        # the FP64 engine's autotuning steps, so that both states are compared
+        # after the same number of steps
         eng.autotune(steps=2)
+        eng.autotune_reorder(steps=2, every=RESORT_EVERY)
     eng.step(args.warmup)
     eng.synchronize()
     eng.step(args.steps)
