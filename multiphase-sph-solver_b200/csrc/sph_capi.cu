@@ -570,11 +570,13 @@ int enqueue_permute(sphgpu_ctx* c, int parity, const int* perm)
 int sort_state(sphgpu_ctx* c, int parity)
 {
     const int N = c->N;
-    if (!c->ord_kin) {
-        int r = dalloc(c, &c->ord_kin, (size_t)N);
-        r |= dalloc(c, &c->ord_kout, (size_t)N);
-        r |= dalloc(c, &c->ord_vin, (size_t)N);
-        r |= dalloc(c, &c->ord_vout, (size_t)N);
+    if (!c->ord_tmp) {
+        // each buffer allocated once (a failed call leaves the others for the next)
+        int r = 0;
+        if (!c->ord_kin) r |= dalloc(c, &c->ord_kin, (size_t)N);
+        if (!c->ord_kout) r |= dalloc(c, &c->ord_kout, (size_t)N);
+        if (!c->ord_vin) r |= dalloc(c, &c->ord_vin, (size_t)N);
+        if (!c->ord_vout) r |= dalloc(c, &c->ord_vout, (size_t)N);
         if (r) return r;
         // keys stay below 512 groups x 8 (ctotal + 1): the bits the sort looks at
         const unsigned long long top = 512ull * 8ull * ((unsigned long long)c->P.ctotal + 1);
@@ -582,8 +584,10 @@ int sort_state(sphgpu_ctx* c, int parity)
         while (b < 64 && (1ull << b) <= top) b++;
         c->ord_end_bit = b;
         c->ord_bytes = sphk_order_temp_bytes(N, b);
-        CK(cudaMalloc(&c->ord_tmp, c->ord_bytes + 256));
-        c->allocs.push_back(c->ord_tmp);
+        void* t = nullptr;
+        CK(cudaMalloc(&t, c->ord_bytes + 256));
+        c->allocs.push_back(t);
+        c->ord_tmp = t;
     }
     sphk_order_sort(&c->d[parity], c->ord_tmp, c->ord_bytes, c->ord_end_bit, c->ord_kin, c->ord_kout, c->ord_vin,
                     c->ord_vout, c->st);
