@@ -26,7 +26,7 @@ from checkers import ORC_JACOBI, ORC_POW_CR, Oracle
 
 pytestmark = pytest.mark.gpu
 
-BULK_REL_TOL = 1e-4          # stress and displacement
+BULK_REL_TOL = 1e-4          # stress and displacement: the bound the FP32-bulk form is held to
 CONDITIONING_FACTOR = 3.0
 FIELDS = ("sig", "ux", "vx", "rho", "pre", "xp")
 
