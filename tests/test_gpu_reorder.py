@@ -267,3 +267,26 @@ def test_reorder_autotuner_keeps_results(shuffle):
     _assert_equal_runs(plain, tuned, "autotuned")
     plain.close()
     tuned.close()
+
+
+@pytest.mark.parametrize("every", [0, 3])
+@pytest.mark.parametrize("factory,steps", [
+    (lambda: scenes.dam_break_2d(dx=0.02, steps=100), 25),
+    (lambda: scenes.soil_column_3d(dx=0.05, steps=100), 12),
+])
+def test_random_order_against_the_oracle(factory, steps, every):
+    """Particles in a random order (whose results the oracle pins to the
+    reference's on the same order, tests/test_oracle.py): the engine, held in
+    that order or re-sorted, is bit-identical to the oracle."""
+    st = _shuffled(scenes.initialise(factory()), 7)
+    eng = _engine(st, every)
+    orc = Oracle(st.params, ORC_JACOBI, ORC_POW_CR)
+    orc.load_state(st.fields, st.fluid, st.soil)
+    for c in (1, steps - 1):
+        eng.step(c)
+        assert orc.step(c) == 0
+    if every:
+        assert _held_out_of_order(eng)
+    for k in STATE_FIELDS:
+        assert _same(eng.get_field(k), orc.get_field(k)), k
+    eng.close()
