@@ -114,7 +114,7 @@ def _shuffled(st, seed):
     fields = {k: np.ascontiguousarray(v[p]) for k, v in st.fields.items()}
     fluid = None if st.fluid is None else np.ascontiguousarray(st.fluid[p])
     soil = None if st.soil is None else np.ascontiguousarray(st.soil[p])
-    return scenes.InitialState(params=st.params, fields=fields, fluid=fluid, soil=soil)
+    return scenes.InitialState(params=st.params, fields=fields, fluid=fluid, soil=soil, vibration=st.vibration)
 
 
 @pytest.mark.parametrize("factory,steps", [
@@ -273,6 +273,8 @@ def test_reorder_autotuner_keeps_results(shuffle):
 @pytest.mark.parametrize("factory,steps", [
     (lambda: scenes.dam_break_2d(dx=0.02, steps=100), 25),
     (lambda: scenes.soil_column_3d(dx=0.05, steps=100), 12),
+    (make_golden.CASES["footing_3d_deformable"][0], 10),
+    (make_golden.CASES["shaking_box_2d_flv1"][0], 20),
 ])
 def test_random_order_against_the_oracle(factory, steps, every):
     """Particles in a random order (whose results the oracle pins to the
@@ -281,7 +283,7 @@ def test_random_order_against_the_oracle(factory, steps, every):
     st = _shuffled(scenes.initialise(factory()), 7)
     eng = _engine(st, every)
     orc = Oracle(st.params, ORC_JACOBI, ORC_POW_CR)
-    orc.load_state(st.fields, st.fluid, st.soil)
+    orc.load_state(st.fields, st.fluid, st.soil, vibration=st.vibration)
     for c in (1, steps - 1):
         eng.step(c)
         assert orc.step(c) == 0

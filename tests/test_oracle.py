@@ -8,6 +8,7 @@ import tempfile
 import numpy as np
 import pytest
 
+import make_golden
 import scenes
 import sphgpu
 from checkers import (ORC_INPLACE, ORC_JACOBI, ORC_POW_CR, ORC_POW_LIBM, STATE_FIELDS, Oracle,
@@ -259,10 +260,12 @@ def _shuffled_scene(sc, seed):
 @pytest.mark.parametrize("factory,steps", [
     (lambda: scenes.dam_break_2d(dx=0.02, steps=100), 25),
     (lambda: scenes.soil_column_3d(dx=0.05, steps=100), 12),
+    (make_golden.CASES["footing_3d_deformable"][0], 10),
 ])
 def test_live_reference_random_particle_order(factory, steps):
     """The reference on its particles in a random order, where its neighbour
-    order inside a cell (Binary_Sort) and its in-place Shepard sweep follow the
+    order inside a cell (Binary_Sort), its in-place Shepard sweep and the order
+    a structure particle takes its contact reactions in (the footing) follow the
     numbering: the oracle in the reference's in-place order follows it bit for
     bit, so parity is pinned for any order a caller gives."""
     sc = _shuffled_scene(factory(), 7)
