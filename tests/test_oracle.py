@@ -261,18 +261,20 @@ def _shuffled_scene(sc, seed):
     (lambda: scenes.dam_break_2d(dx=0.02, steps=100), 25),
     (lambda: scenes.soil_column_3d(dx=0.05, steps=100), 12),
     (make_golden.CASES["footing_3d_deformable"][0], 10),
+    (make_golden.CASES["shaking_box_2d_flv1"][0], 20),
 ])
 def test_live_reference_random_particle_order(factory, steps):
     """The reference on its particles in a random order, where its neighbour
-    order inside a cell (Binary_Sort), its in-place Shepard sweep and the order
-    a structure particle takes its contact reactions in (the footing) follow the
+    order inside a cell (Binary_Sort), its in-place Shepard sweep, the order
+    a structure particle takes its contact reactions in (the footing) and
+    check_domain's first wall of matype > 2 (the shaking box) follow the
     numbering: the oracle in the reference's in-place order follows it bit for
     bit, so parity is pinned for any order a caller gives."""
     sc = _shuffled_scene(factory(), 7)
     ref = _live(sc)
     fl, so = ref.materials()
     orc = Oracle(ref.params, ORC_INPLACE)
-    orc.load_state({k: ref.get_field(k) for k in STATE_FIELDS}, fl, so)
+    orc.load_state({k: ref.get_field(k) for k in STATE_FIELDS}, fl, so, vibration=sc.vibration)
     for chunk in (1, steps - 1):
         assert ref.step(chunk) == 0
         assert orc.step(chunk) == 0
