@@ -108,13 +108,16 @@ def test_resorted_every_few_steps_against_the_oracle(name, every):
 
 def _shuffled(st, seed):
     """The same scene with its particles in a random order (every per-particle
-    input permuted alike)."""
+    input permuted alike); waiting rain particles stay at the end, in their
+    rows."""
     n = int(st.params["ntotal"])
-    p = np.random.default_rng(seed).permutation(n)
+    tail = st.rain["nrain"] if st.rain else 0
+    p = np.concatenate([np.random.default_rng(seed).permutation(n - tail), np.arange(n - tail, n)])
     fields = {k: np.ascontiguousarray(v[p]) for k, v in st.fields.items()}
     fluid = None if st.fluid is None else np.ascontiguousarray(st.fluid[p])
     soil = None if st.soil is None else np.ascontiguousarray(st.soil[p])
-    return scenes.InitialState(params=st.params, fields=fields, fluid=fluid, soil=soil, vibration=st.vibration)
+    return scenes.InitialState(params=st.params, fields=fields, fluid=fluid, soil=soil, rain=st.rain,
+                               vibration=st.vibration)
 
 
 @pytest.mark.parametrize("factory,steps", [
@@ -275,6 +278,7 @@ def test_reorder_autotuner_keeps_results(shuffle):
     (lambda: scenes.soil_column_3d(dx=0.05, steps=100), 12),
     (make_golden.CASES["footing_3d_deformable"][0], 10),
     (make_golden.CASES["shaking_box_2d_flv1"][0], 20),
+    (make_golden.CASES["dam_break_2d_dx0.04_rain"][0], 35),
 ])
 def test_random_order_against_the_oracle(factory, steps, every):
     """Particles in a random order (whose results the oracle pins to the
@@ -283,7 +287,7 @@ def test_random_order_against_the_oracle(factory, steps, every):
     st = _shuffled(scenes.initialise(factory()), 7)
     eng = _engine(st, every)
     orc = Oracle(st.params, ORC_JACOBI, ORC_POW_CR)
-    orc.load_state(st.fields, st.fluid, st.soil, vibration=st.vibration)
+    orc.load_state(st.fields, st.fluid, st.soil, st.rain, vibration=st.vibration)
     for c in (1, steps - 1):
         eng.step(c)
         assert orc.step(c) == 0
@@ -291,4 +295,6 @@ def test_random_order_against_the_oracle(factory, steps, every):
         assert _held_out_of_order(eng)
     for k in STATE_FIELDS:
         assert _same(eng.get_field(k), orc.get_field(k)), k
+    if st.rain:
+        assert eng.rain()["nrain"] == orc.rain()["nrain"] == 0
     eng.close()

@@ -249,8 +249,10 @@ def test_live_reference_bit_identical(factory, steps):
 
 def _shuffled_scene(sc, seed):
     """The scene's particles in a random order (every per-particle input
-    permuted alike)."""
-    p = np.random.default_rng(seed).permutation(sc.n)
+    permuted alike); waiting rain particles stay at the end of the array, in
+    their rows, where rainpro releases them from."""
+    tail = sc.rain["nrain"] if sc.rain else 0
+    p = np.concatenate([np.random.default_rng(seed).permutation(sc.n - tail), np.arange(sc.n - tail, sc.n)])
     for k in ("xp", "vxp", "ptype", "matype", "permtype", "etype"):
         setattr(sc, k, np.ascontiguousarray(getattr(sc, k)[p]))
     return sc
@@ -262,6 +264,7 @@ def _shuffled_scene(sc, seed):
     (lambda: scenes.soil_column_3d(dx=0.05, steps=100), 12),
     (make_golden.CASES["footing_3d_deformable"][0], 10),
     (make_golden.CASES["shaking_box_2d_flv1"][0], 20),
+    (make_golden.CASES["dam_break_2d_dx0.04_rain"][0], 35),
 ])
 def test_live_reference_random_particle_order(factory, steps):
     """The reference on its particles in a random order, where its neighbour
@@ -274,7 +277,7 @@ def test_live_reference_random_particle_order(factory, steps):
     ref = _live(sc)
     fl, so = ref.materials()
     orc = Oracle(ref.params, ORC_INPLACE)
-    orc.load_state({k: ref.get_field(k) for k in STATE_FIELDS}, fl, so, vibration=sc.vibration)
+    orc.load_state({k: ref.get_field(k) for k in STATE_FIELDS}, fl, so, sc.rain, vibration=sc.vibration)
     for chunk in (1, steps - 1):
         assert ref.step(chunk) == 0
         assert orc.step(chunk) == 0
@@ -282,6 +285,8 @@ def test_live_reference_random_particle_order(factory, steps):
         a, b = orc.get_field(k), ref.get_field(k)
         same = (a == b) | (np.isnan(a) & np.isnan(b)) if a.dtype.kind == "f" else (a == b)
         assert same.all(), k
+    if sc.rain:
+        assert orc.rain()["nrain"] == 0
 
 
 def _stretched_column(dx):
