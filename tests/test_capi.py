@@ -99,3 +99,30 @@ def test_particle_layout_matches_reference_class():
         assert np.array_equal(got, want), name
         checked += 1
     assert checked == len(sphgpu.FIELDS)
+
+
+def test_header_compiles_as_c_and_links(tmp_path):
+    """include/sphgpu.h is plain C: a C99 program that takes the address of
+    every entry point it declares compiles, links against libsphgpu.so and
+    runs without a GPU (no device, no context)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    names = _declared()
+    src = tmp_path / "abi.c"
+    lines = ['#include <stdio.h>', '#include "sphgpu.h"', "int main(void) {",
+             "    void* const table[] = {"]
+    lines += ["        (void*)&%s," % n for n in names]
+    lines += ["    };",
+              '    printf("%d %d %zu\\n", sphgpu_abi_version(), sphgpu_device_count(), sizeof(table) / sizeof(table[0]));',
+              "    return sphgpu_create(NULL, 0) == NULL ? 0 : 1;", "}"]
+    src.write_text("\n".join(lines) + "\n")
+    lib_dir = os.path.dirname(sphgpu.LIB_PATH)
+    exe = tmp_path / "abi"
+    subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-I", os.path.join(REPO, "include"), str(src), "-o",
+                    str(exe), "-L", lib_dir, "-lsphgpu", "-Wl,-rpath," + lib_dir], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    assert int(out[0]) == sphgpu.load_library().sphgpu_abi_version()
+    assert int(out[2]) == len(names)
