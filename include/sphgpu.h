@@ -299,12 +299,12 @@ int sphgpu_get_dt(sphgpu_ctx* ctx, double* dt);
  * CPP_3-NNPS.cpp:561-630).  With every_steps > 0, sphgpu_step and
  * sphgpu_step_profiled gather the whole particle state on the device into a
  * spatial order -- by type and material, then rows of a lattice of spacing dr
- * over the grid (over each batched instance's own grid) along the search's
- * fastest axis -- before the
- * next step and then every every_steps steps, so the neighbour gathers of the
- * passes read nearby records whatever order the caller's particles came in or
- * have mixed into.  Every result stays the one of the caller's order, bit for bit: the
- * device keeps the map between the orders, and the passes whose result
+ * over the grid (over each batched instance's own grid) along its longest
+ * axis -- before the next step and then every every_steps steps, so the
+ * neighbour gathers of the passes read nearby records whatever order the
+ * caller's particles came in or have mixed into.  Every result stays the one
+ * of the caller's order, bit for bit: the device keeps the map between the
+ * orders, and the passes whose result
  * depends on the particle numbering (the search's order inside a cell, the
  * rain rows, check_domain's first wall, tm_boundary's default wall, the order
  * of a structure particle's contact reactions) go through it.  Every call that
